@@ -1,0 +1,183 @@
+"""ctypes wrapper of the CPU oracle (oracle/tm_oracle.cpp) -- TEST INFRASTRUCTURE ONLY.
+
+Imported only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg, as the checker; the product (libtmsolve.so and the tmsolve package)
+never loads it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libtmoracle.so")
+
+_dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.orc_model_create.restype = vp
+    L.orc_model_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _ip, _ip, _dp,
+                                   C.c_int, _ip, _ip, _ip, _ip, C.c_int, C.c_int, _ip, C.c_double,
+                                   C.c_int, _ip, C.c_int, _ip]
+    L.orc_model_destroy.argtypes = [vp]
+    L.orc_model_sizes.argtypes = [vp, np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")]
+    L.orc_model_mesh.argtypes = [vp] + [vp] * 8
+    L.orc_assemble.argtypes = [vp, C.c_int, _ip, _dp, _dp, _dp, _dp, _ip, _dp, C.c_int]
+    L.orc_get_bcsr.argtypes = [vp, vp, vp, vp, vp]
+    L.orc_matvec.argtypes = [vp, _dp, _dp]
+    L.orc_solve.restype = C.c_int
+    L.orc_solve.argtypes = [vp, _dp, _dp, C.c_double, C.c_int, C.c_int, C.c_long, _dp]
+    L.orc_clear_warm.argtypes = [vp]
+    L.orc_mg_levels.restype = C.c_int
+    L.orc_mg_levels.argtypes = [vp, _ip, C.c_int]
+    L.orc_mg_node_agg.restype = C.c_int
+    L.orc_mg_node_agg.argtypes = [vp, _ip]
+    L.orc_shape_matrices.argtypes = [vp, vp, _dp]
+    L.orc_element_k33.argtypes = [C.c_double] * 3 + [_dp, _dp]
+    L.orc_element_fth.argtypes = [C.c_double] * 3 + [vp, vp, _dp]
+    L.orc_condense33.argtypes = [_dp, vp, _dp, _dp, _dp]
+    L.orc_general_element.argtypes = [_dp, _dp, _dp, _dp]
+    L.orc_general_derivs.argtypes = [_dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
+    L.orc_anand_step.restype = C.c_double
+    L.orc_anand_step.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double, _dp, _dp, C.c_int, C.c_int]
+    L.orc_anand_uniaxial.restype = C.c_double
+    L.orc_anand_uniaxial.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int]
+    L.orc_anand_screen.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _ip, _ip, C.c_int,
+                                   _dp, _dp, _dp]
+    L.orc_last_error.restype = C.c_char_p
+    L.orc_last_error.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class OracleModel:
+    """CPU restatement of FEModel + LinearSolver (09-assembly.js, 10-solver.js) on one package."""
+
+    def __init__(self, pkg, constraints=None):
+        L = lib()
+        m = pkg.mesh
+        ncells = (m.nx - 1) * (m.ny - 1) * (m.nz - 1)
+        cg = np.full(2 * ncells, -1, np.int32); cp = np.zeros(2 * ncells, np.int32); cs = np.zeros(2 * ncells)
+        ce = m.cellElems
+        on = ce >= 0
+        cg[on] = m.eGroup[ce[on]]; cp[on] = m.ePart[ce[on]]; cs[on] = m.eScale[ce[on]]
+        con = np.ascontiguousarray(m.constraints if constraints is None else constraints, np.int32)
+        fx = np.ascontiguousarray(m.featureX, np.int32); fy = np.ascontiguousarray(m.featureY, np.int32)
+        self.pkg = pkg
+        self.h = L.orc_model_create(m.nx, m.ny, m.nz, np.ascontiguousarray(m.xs), np.ascontiguousarray(m.ys),
+                                    np.ascontiguousarray(m.zs), cg, cp, cs,
+                                    len(pkg.group_layered), np.ascontiguousarray(pkg.group_layered, np.int32),
+                                    np.ascontiguousarray(pkg.group_stage, np.int32), np.ascontiguousarray(pkg.group_pset, np.int32),
+                                    np.ascontiguousarray(pkg.sec_of_layer, np.int32), int(pkg.npset),
+                                    len(con), con, 0.0, len(fx), fx if len(fx) else np.zeros(1, np.int32),
+                                    len(fy), fy if len(fy) else np.zeros(1, np.int32))
+        sz = np.zeros(5, np.int64)
+        L.orc_model_sizes(self.h, sz)
+        self.nn, self.ne, self.nb, self.ndof, self.ncon = (int(v) for v in sz)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_model_destroy(self.h)
+            self.h = None
+
+    def mesh_arrays(self):
+        m = self.pkg.mesh
+        out = dict(nodeId=np.zeros(m.nx * m.ny * m.nz, np.int32), conn=np.zeros(8 * self.ne, np.int32),
+                   eIJK=np.zeros(3 * self.ne, np.int32), colStart=np.zeros(m.nx * m.ny + 1, np.int32),
+                   cellElems=np.zeros(2 * (m.nx - 1) * (m.ny - 1) * (m.nz - 1), np.int32),
+                   coords=np.zeros(3 * self.nn), constraints=np.zeros(self.ncon, np.int32), eGroup=np.zeros(self.ne, np.int32))
+        lib().orc_model_mesh(self.h, *[_ptr(out[k]) for k in ("nodeId", "conn", "eIJK", "colStart", "cellElems", "coords", "constraints", "eGroup")])
+        return out
+
+    def assemble(self, step, no_constraints=False):
+        rhs = np.zeros(self.ndof)
+        lib().orc_assemble(self.h, int(step.stage), np.ascontiguousarray(step.layered, np.int32), step.D, step.s0, step.W, step.V,
+                           np.ascontiguousarray(step.born, np.int32), rhs, int(no_constraints))
+        return rhs
+
+    def bcsr(self):
+        rowPtr = np.zeros(self.nn + 1, np.int32); col = np.zeros(self.nb, np.int32)
+        val = np.zeros(9 * self.nb); isC = np.zeros(self.ndof, np.uint8)
+        lib().orc_get_bcsr(self.h, _ptr(rowPtr), _ptr(col), _ptr(val), _ptr(isC))
+        return rowPtr, col, val, isC
+
+    def matvec(self, x):
+        y = np.zeros(self.ndof)
+        lib().orc_matvec(self.h, np.ascontiguousarray(x, np.float64), y)
+        return y
+
+    def solve(self, f, tol=1e-8, maxit=2000, precond="mg", key=-1):
+        """LinearSolver.solve (10-solver.js:933-994). The assembled values are scaled in place."""
+        u = np.zeros(self.ndof)
+        info = np.zeros(16)
+        rc = lib().orc_solve(self.h, np.ascontiguousarray(f, np.float64), u, float(tol), int(maxit),
+                             0 if precond == "mg" else 1, int(key), info)
+        if rc:
+            raise RuntimeError(lib().orc_last_error(self.h).decode())
+        keys = ["iters", "relres", "converged", "iters0", "ms", "pcMs", "precond", "rebuilt", "warm", "fallback",
+                "colJitter", "shellJitter", "levels"]
+        rec = {k: float(info[i]) for i, k in enumerate(keys)}
+        for k in ("iters", "converged", "rebuilt", "warm", "fallback", "colJitter", "shellJitter", "levels"):
+            rec[k] = int(rec[k])
+        rec["precond"] = "mg" if info[6] == 0 else "ic"
+        rec["u"] = u
+        return rec
+
+    def clear_warm(self):
+        lib().orc_clear_warm(self.h)
+
+    def mg_levels(self):
+        out = np.zeros(4 * 64, np.int32)
+        n = lib().orc_mg_levels(self.h, out, 64)
+        return [tuple(out[4 * l:4 * l + 4]) for l in range(n)]
+
+    def mg_node_agg(self):
+        out = np.zeros(self.nn, np.int32)
+        lib().orc_mg_node_agg(self.h, out)
+        return out
+
+
+def anand_uniaxial(params, Etab, T, rate, eps_max, nsteps):
+    return lib().orc_anand_uniaxial(np.ascontiguousarray(params, np.float64), np.ascontiguousarray(Etab, np.float64),
+                                    float(T), float(rate), float(eps_max), int(nsteps))
+
+
+def anand_step(params, Etab, state, eps, T, dt, want_tangent=True, commit=True):
+    sig = np.zeros(6); D = np.zeros(36)
+    d = lib().orc_anand_step(np.ascontiguousarray(params, np.float64), np.ascontiguousarray(Etab, np.float64), state,
+                             np.ascontiguousarray(eps, np.float64), float(T), float(dt), sig, D, int(want_tangent), int(commit))
+    return d, sig, D
+
+
+def anand_screen(params, Etab, Ftab, temps, table, hist):
+    """screenJoints' per-site loop (13-fatigue.js:395-451) for free-standing solder columns."""
+    temps = np.ascontiguousarray(temps, np.float64); table = np.ascontiguousarray(table, np.float64)
+    nsites = table.size // (6 * len(temps))
+    dW = np.zeros(nsites); dE = np.zeros(nsites); stab = np.zeros(nsites)
+    lib().orc_anand_screen(np.ascontiguousarray(params, np.float64), np.ascontiguousarray(Etab, np.float64),
+                           np.ascontiguousarray(Ftab, np.float64), nsites, len(temps), temps, table,
+                           len(hist["t"]), np.ascontiguousarray(hist["t"], np.float64), np.ascontiguousarray(hist["T"], np.float64),
+                           np.ascontiguousarray(hist["cycle"], np.int32), np.ascontiguousarray(hist["phase"], np.int32),
+                           int(hist["cycles"]), dW, dE, stab)
+    return dW, dE, stab

@@ -1,0 +1,203 @@
+"""Per-step material data that the caller hands to the solver (the reference's
+``FEModel.prepareStep`` inputs), for constant-property synthetic packages.
+
+The material database and its temperature tables stay on the caller's side of
+the boundary in the reference; this module restates the parts that synthetic
+inputs need:
+
+* ``orthoD`` / ``isoD`` / ``columnD`` (src/core/03-materials.js:222-266) with
+  ``invDense`` (src/core/01-util.js:110-134);
+* the constant-stiffness branch of ``gridStressIncrement`` (03-materials.js:394-401);
+* layered sections: ``lagrange3Integrals`` and the W_j / V_j weights of
+  ``buildBandSection`` / ``sectionVstep`` (src/core/04-homogenize.js:115-221)
+  for sub-layers of constant properties, with ``sublayerShellD`` (:115-121);
+* the 1 degC property grid and ``gridAt`` (03-materials.js:344-355) used by the
+  Anand point (E(T) and the thermal strain F(T)).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+NU_MAX_GLOBAL = 0.45          # 00-constants.js:19
+COLUMN_INPLANE_FRACTION = 1e-3  # 00-constants.js:25
+TGRID_MIN, TGRID_MAX = -80, 300
+TGRID_N = TGRID_MAX - TGRID_MIN + 1
+T_STRAIN_ORIGIN = 25.0
+
+
+def inv_dense(A: np.ndarray) -> np.ndarray:
+    """invDense (01-util.js:110-134): Gauss-Jordan with partial pivoting, same operation order."""
+    A = np.asarray(A, np.float64)
+    n = A.shape[0]
+    M = np.zeros((n, 2 * n))
+    M[:, :n] = A
+    M[np.arange(n), n + np.arange(n)] = 1.0
+    for c in range(n):
+        p = c
+        best = abs(M[c, c])
+        for r in range(c + 1, n):
+            v = abs(M[r, c])
+            if v > best:
+                best, p = v, r
+        if best == 0:
+            raise ValueError("singular matrix in invDense")
+        if p != c:
+            M[[c, p]] = M[[p, c]]
+        inv = 1.0 / M[c, c]
+        M[c] = M[c] * inv
+        for r in range(n):
+            if r == c:
+                continue
+            f = M[r, c]
+            if f == 0:
+                continue
+            M[r] = M[r] - f * M[c]
+    return M[:, n:].copy()
+
+
+def ortho_d(Ex, Ey, Ez, Gxy, Gxz, Gyz, nuxy, nuxz, nuyz, nu_max=None) -> np.ndarray:
+    """orthoD (03-materials.js:222-238): 6x6 Voigt stiffness (xx yy zz xy yz zx, engineering shear)."""
+    cl = (lambda v: min(v, 0.499 if nu_max is None else nu_max))
+    nxy, nxz, nyz = cl(nuxy), cl(nuxz), cl(nuyz)
+    S = np.zeros((3, 3))
+    S[0, 0] = 1 / Ex; S[1, 1] = 1 / Ey; S[2, 2] = 1 / Ez
+    S[0, 1] = S[1, 0] = -nxy / Ex
+    S[0, 2] = S[2, 0] = -nxz / Ex
+    S[1, 2] = S[2, 1] = -nyz / Ey
+    C = inv_dense(S)
+    D = np.zeros(36)
+    D[0], D[1], D[2] = C[0]
+    D[6], D[7], D[8] = C[1]
+    D[12], D[13], D[14] = C[2]
+    D[21] = Gxy; D[28] = Gyz; D[35] = Gxz
+    return D
+
+
+def iso_d(E, nu, nu_max=NU_MAX_GLOBAL) -> np.ndarray:
+    """isoD (03-materials.js:247-249) through isoEC (:241-244)."""
+    nu_c = min(nu, 0.499 if nu_max is None else nu_max)
+    G = E / (2 * (1 + nu_c))
+    return ortho_d(E, E, E, G, G, G, nu_c, nu_c, nu_c, nu_max)
+
+
+def column_d(E, nu) -> np.ndarray:
+    """columnD (03-materials.js:259-266): solder phase of the bump layer as separate columns."""
+    D = np.zeros(36)
+    G = E / (2 * (1 + nu))
+    fl = COLUMN_INPLANE_FRACTION
+    D[0] = D[7] = fl * E
+    D[21] = fl * G
+    D[14] = E; D[28] = G; D[35] = G
+    return D
+
+
+def thermal_stress_const(D: np.ndarray, cte_xy: float, cte_z: float, Ta: float, Tb: float) -> np.ndarray:
+    """gridStressIncrement with a constant stiffness (03-materials.js:397-400) for constant CTEs:
+    s0[r] = sum_c D[r, c] (F_c(Tb) - F_c(Ta)), F(T) = alpha (T - 25)."""
+    f = np.array([cte_xy * (Tb - T_STRAIN_ORIGIN) - cte_xy * (Ta - T_STRAIN_ORIGIN),
+                  cte_xy * (Tb - T_STRAIN_ORIGIN) - cte_xy * (Ta - T_STRAIN_ORIGIN),
+                  cte_z * (Tb - T_STRAIN_ORIGIN) - cte_z * (Ta - T_STRAIN_ORIGIN)])
+    Dm = np.asarray(D).reshape(6, 6)
+    return np.array([Dm[r, 0] * f[0] + Dm[r, 1] * f[1] + Dm[r, 2] * f[2] for r in range(6)])
+
+
+def lagrange3_integrals(a: float, b: float):
+    """lagrange3Integrals (04-homogenize.js:124-129)."""
+    Im = lambda z: z * z * z / 6 - z * z / 4
+    I0 = lambda z: z - z * z * z / 3
+    Ip = lambda z: z * z * z / 6 + z * z / 4
+    return [Im(b) - Im(a), I0(b) - I0(a), Ip(b) - Ip(a)]
+
+
+def sublayer_shell_d(D: np.ndarray) -> np.ndarray:
+    """sublayerShellD (04-homogenize.js:115-121): plane-stress in-plane block, uncoupled thickness modulus."""
+    D = np.array(D, np.float64)
+    zz = D[14]
+    P = (0, 1, 3)
+    for a in P:
+        for b in P:
+            D[a * 6 + b] -= D[a * 6 + 2] * D[2 * 6 + b] / zz
+    for a in P:
+        D[a * 6 + 2] = 0.0
+        D[2 * 6 + a] = 0.0
+    D[14] = zz
+    return D
+
+
+def layered_section(z0: float, z1: float, subs, Ta: float, Tb: float, plane_stress=True):
+    """Step weights of one layered band of constant-property sub-layers.
+
+    subs: list of (sz0, sz1, D36, cte_xy, cte_z). Returns (W 108, V 18) as in
+    buildBandSection's W_j (04-homogenize.js:172-181) averaged over the step
+    (constant here) and sectionVstep (:212-221)."""
+    h = z1 - z0
+    W = np.zeros(108)
+    V = np.zeros(18)
+    for (sz0, sz1, D, axy, az) in subs:
+        Dl = sublayer_shell_d(D) if plane_stress else np.asarray(D, np.float64)
+        L = lagrange3_integrals(2 * (sz0 - z0) / h - 1, 2 * (sz1 - z0) / h - 1)
+        s0 = thermal_stress_const(Dl, axy, az, Ta, Tb)
+        for j in range(3):
+            W[j * 36:(j + 1) * 36] += Dl * L[j]
+            V[j * 6:(j + 1) * 6] += s0 * L[j]
+    return W, V
+
+
+def grid_table(fn) -> np.ndarray:
+    """A property on the 1 degC grid TGRID_MIN..TGRID_MAX (03-materials.js:344, 424-433)."""
+    return np.array([fn(float(TGRID_MIN + i)) for i in range(TGRID_N)], np.float64)
+
+
+def grid_at(arr: np.ndarray, T: float) -> float:
+    """gridAt (03-materials.js:347-355)."""
+    x = T - TGRID_MIN
+    if x <= 0:
+        return float(arr[0])
+    if x >= TGRID_N - 1:
+        return float(arr[TGRID_N - 1])
+    i = int(np.floor(x)); t = x - i
+    return float(arr[i] + t * (arr[i + 1] - arr[i]))
+
+
+def interp_table_linear(xs, ys, x):
+    """interpTable with linear extrapolation (01-util.js:25-33)."""
+    n = len(xs)
+    if n == 1:
+        return ys[0]
+    if x <= xs[0]:
+        i = 0
+    elif x >= xs[-1]:
+        i = n - 2
+    else:
+        lo, hi = 0, n - 1
+        while hi - lo > 1:
+            mid = (lo + hi) >> 1
+            if xs[mid] <= x:
+                lo = mid
+            else:
+                hi = mid
+        i = lo
+    t = (x - xs[i]) / (xs[i + 1] - xs[i])
+    return ys[i] + t * (ys[i + 1] - ys[i])
+
+
+# SAC305 of the tool's material database (src/materials-db.json, record "sac305")
+SAC305 = dict(A=3501.0, QR=9320.0, xi=4.0, m=0.25, shat=30.2, n=0.01, h0=180000.0, a=1.78, s0=21.0, nu=0.4,
+              E_T=[-40.0, 25.0, 75.0, 125.0], E_GPa=[57.4, 46.5, 38.2, 30.0], solidus=217.0, cte=22.5e-6)
+
+
+def sac305_tables():
+    """E(T) (MPa, linear table with linear extrapolation, 1 % above the solidus; 03-materials.js:88-116)
+    and F(T) = alpha (T - 25) on the 1 degC grid."""
+    def E(T):
+        if T > SAC305["solidus"]:
+            return 0.01 * interp_table_linear(SAC305["E_T"], SAC305["E_GPa"], SAC305["solidus"]) * 1000.0
+        return interp_table_linear(SAC305["E_T"], SAC305["E_GPa"], T) * 1000.0
+    Et = grid_table(E)
+    Ft = grid_table(lambda T: SAC305["cte"] * (T - T_STRAIN_ORIGIN))
+    return Et, Ft
+
+
+def anand_params_array(p: dict) -> np.ndarray:
+    """Parameter vector (A, Q/R, xi, m, s_hat, n, h0, a, s0, nu) of the Anand entry points."""
+    return np.array([p["A"], p["QR"], p["xi"], p["m"], p["shat"], p["n"], p["h0"], p["a"], p["s0"], p["nu"]], np.float64)

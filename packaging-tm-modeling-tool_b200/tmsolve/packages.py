@@ -1,0 +1,291 @@
+"""Synthetic package models with the shapes of the tool's inputs.
+
+A package is what the tool's JavaScript side hands to the solve path: grid
+lines, a per-cell assignment of groups (``buildStructuredMesh`` input,
+src/core/06-mesher.js:14), the groups' property sets per step
+(``FEModel.prepareStep``, src/core/09-assembly.js:346-365) and the constraint
+DOFs. The reference's verification suite builds its box models the same way
+(``boxModel``, src/core/15-verify.js:11-17).
+
+Workloads (sizes of the reference's benchmark configurations, synthetic data):
+
+* ``box``: homogeneous or layered boxes of the verification tests.
+* ``fcbga_c1``: plain FCBGA, 48x48x20 elements, substrate 35x35x1.2 mm, die
+  15x15x0.775 mm, 0.08 mm bump/underfill layer with superposed solder-column
+  (30 %) and underfill (70 %) phases; voids outside the die above the
+  substrate; one 150 -> 25 degC step.
+* ``lidded_c2``: lidded FCBGA, 160x160x32 elements, 55x55 mm 8-2-8 substrate
+  in 12 layered bands, 25 mm die, TIM, Cu hat lid with adhesive foot; E and CTE
+  jittered +-10 % per material (seeded).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional
+
+import numpy as np
+
+from .materials import column_d, iso_d, layered_section, thermal_stress_const
+from .mesh import PART, Mesh, build_structured_mesh, constraints321
+
+CONSTRAINT_SPAN = 0.4   # 00-constants.js:52
+
+
+@dataclass
+class StepData:
+    """Per-step property sets: homogeneous (D 36, s0 6) or layered (W 108, V 18)."""
+    layered: np.ndarray      # (npset,) int32
+    D: np.ndarray            # (npset*36,)
+    s0: np.ndarray           # (npset*6,)
+    W: np.ndarray            # (npset*108,)
+    V: np.ndarray            # (npset*18,)
+    born: np.ndarray         # (npset,) int32: thermal load on
+    stage: int = 0
+
+
+@dataclass
+class Package:
+    name: str
+    mesh: Mesh
+    group_layered: np.ndarray   # (ngroups,) int32
+    group_stage: np.ndarray     # (ngroups,) int32
+    group_pset: np.ndarray      # (ngroups,) property set of homogeneous groups
+    sec_of_layer: np.ndarray    # (nz-1,) property set of layered groups per element layer
+    npset: int
+    step_fn: Callable[[float, float], StepData]
+    Ta: float = 150.0
+    Tb: float = 25.0
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def e_pset(self) -> np.ndarray:
+        m = self.mesh
+        k = m.eIJK[2::3]
+        lay = self.group_layered[m.eGroup] != 0
+        return np.where(lay, self.sec_of_layer[k], self.group_pset[m.eGroup]).astype(np.int32)
+
+    def step(self, Ta: Optional[float] = None, Tb: Optional[float] = None) -> StepData:
+        return self.step_fn(self.Ta if Ta is None else Ta, self.Tb if Tb is None else Tb)
+
+
+def _homog_step(mats, Ta, Tb, npset=None, layered_fn=None) -> StepData:
+    """mats: list over property sets of (D36, cte_xy, cte_z) or None for layered ones."""
+    n = len(mats) if npset is None else npset
+    lay = np.zeros(n, np.int32); D = np.zeros(n * 36); s0 = np.zeros(n * 6)
+    W = np.zeros(n * 108); V = np.zeros(n * 18)
+    for p, m in enumerate(mats):
+        if m is None:
+            lay[p] = 1
+            Wp, Vp = layered_fn(p, Ta, Tb)
+            W[108 * p:108 * p + 108] = Wp; V[18 * p:18 * p + 18] = Vp
+        else:
+            Dp, axy, az = m
+            D[36 * p:36 * p + 36] = Dp
+            s0[6 * p:6 * p + 6] = thermal_stress_const(Dp, axy, az, Ta, Tb)
+    return StepData(layered=lay, D=D, s0=s0, W=W, V=V, born=np.ones(n, np.int32))
+
+
+def linspace(a, b, n):
+    """linspace of the verification suite (15-verify.js:3): n intervals, n+1 points."""
+    return [a + (b - a) * i / n for i in range(n + 1)]
+
+
+def box_package(xs, ys, zs, mats, assign, name="box", constraints=None, Ta=25.0, Tb=125.0) -> Package:
+    """boxModel (15-verify.js:11-17): one homogeneous group per material, assign(i, j, k) -> group."""
+    nx, ny, nz = len(xs), len(ys), len(zs)
+    ncells = (nx - 1) * (ny - 1) * (nz - 1)
+    cg = np.full(2 * ncells, -1, np.int32); cp = np.zeros(2 * ncells, np.int32); cs = np.zeros(2 * ncells)
+    c = 0
+    for i in range(nx - 1):
+        for j in range(ny - 1):
+            for k in range(nz - 1):
+                cg[2 * c] = assign(i, j, k); cs[2 * c] = 1.0
+                c += 1
+    mesh = build_structured_mesh(xs, ys, zs, cg, cp, cs)
+    a = CONSTRAINT_SPAN * min((xs[-1] - xs[0]) / 2, (ys[-1] - ys[0]) / 2)
+    mesh.constraints = constraints321(mesh, a) if constraints is None else np.asarray(constraints, np.int32)
+    ng = len(mats)
+    return Package(name=name, mesh=mesh, group_layered=np.zeros(ng, np.int32), group_stage=np.zeros(ng, np.int32),
+                   group_pset=np.arange(ng, dtype=np.int32), sec_of_layer=np.zeros(nz - 1, np.int32), npset=ng,
+                   step_fn=lambda Ta_, Tb_: _homog_step(mats, Ta_, Tb_), Ta=Ta, Tb=Tb)
+
+
+def _graded_lines(segments):
+    out = [segments[0][0]]
+    for (a, b, n) in segments:
+        for q in range(1, n + 1):
+            out.append(a + (b - a) * q / n)
+    return np.array(out)
+
+
+def fcbga_c1() -> Package:
+    """Plain FP64 linear-elastic FCBGA (48x48x20 elements, voids outside the die above the substrate)."""
+    xs = _graded_lines([(-17.5, -7.5, 12), (-7.5, 7.5, 24), (7.5, 17.5, 12)])
+    ys = xs.copy()
+    z_sub = 1.2; z_bump = 0.08; z_die = 0.775
+    zs = _graded_lines([(0.0, z_sub, 10), (z_sub, z_sub + z_bump, 2), (z_sub + z_bump, z_sub + z_bump + z_die, 8)])
+    nx, ny, nz = len(xs), len(ys), len(zs)
+    ncy, ncz = ny - 1, nz - 1
+    ncells = (nx - 1) * ncy * ncz
+    cg = np.full(2 * ncells, -1, np.int32); cp = np.zeros(2 * ncells, np.int32); cs = np.zeros(2 * ncells)
+    I, J, K = np.meshgrid(np.arange(nx - 1), np.arange(ncy), np.arange(ncz), indexing="ij")
+    c = ((I * ncy + J) * ncz + K).ravel(); I = I.ravel(); J = J.ravel(); K = K.ravel()
+    in_die = (I >= 12) & (I < 36) & (J >= 12) & (J < 36)
+    sub = K < 10; bump = (K >= 10) & (K < 12); die = K >= 12
+    # groups: 0 substrate, 1 solder columns, 2 underfill (bump layer), 3 die
+    cg[2 * c[sub]] = 0; cp[2 * c[sub]] = PART["SUB"]; cs[2 * c[sub]] = 1.0
+    b = bump & in_die
+    cg[2 * c[b]] = 1; cp[2 * c[b]] = PART["SOLDER"]; cs[2 * c[b]] = 0.3
+    cg[2 * c[b] + 1] = 2; cp[2 * c[b] + 1] = PART["UF_BUMP"]; cs[2 * c[b] + 1] = 0.7
+    d = die & in_die
+    cg[2 * c[d]] = 3; cp[2 * c[d]] = PART["DIE"]; cs[2 * c[d]] = 1.0
+    mesh = build_structured_mesh(xs, ys, zs, cg, cp, cs, featureX=[12, 36], featureY=[12, 36])
+    mesh.constraints = constraints321(mesh, CONSTRAINT_SPAN * min(17.5, 17.5))
+    mats = [(iso_d(25000.0, 0.3), 15e-6, 15e-6),          # substrate
+            (column_d(40000.0, 0.4), 22.5e-6, 22.5e-6),   # SAC solder columns (E = 40 GPa)
+            (iso_d(8000.0, 0.35), 30e-6, 30e-6),          # underfill
+            (iso_d(130000.0, 0.28), 2.6e-6, 2.6e-6)]      # Si die
+    return Package(name="fcbga_c1", mesh=mesh, group_layered=np.zeros(4, np.int32), group_stage=np.zeros(4, np.int32),
+                   group_pset=np.arange(4, dtype=np.int32), sec_of_layer=np.zeros(nz - 1, np.int32), npset=4,
+                   step_fn=lambda Ta, Tb: _homog_step(mats, Ta, Tb), Ta=150.0, Tb=25.0,
+                   meta=dict(workload="fcbga_c1 48x48x20", bottom_plane=0))
+
+
+def _stack_8_2_8(rng_mat):
+    """Bottom-up substrate rows of an 8-2-8 stack (like generateStack, src/core/02-config.js:24):
+    (name, thickness)."""
+    rows = [("sr", 0.020)]
+    for _ in range(8):
+        rows += [("diel", 0.030), ("cu", 0.015)]
+    rows += [("corecu", 0.018), ("core", 0.800), ("corecu", 0.018)]
+    for _ in range(8):
+        rows += [("cu", 0.015), ("diel", 0.030)]
+    rows += [("sr", 0.020)]
+    return rows
+
+
+def lidded_c2(n_inplane: int = 160, seed: int = 20261203) -> Package:
+    """Mixed-precision benchmark package: lidded FCBGA, n x n x 32 elements, layered 8-2-8 substrate."""
+    rng = np.random.default_rng(seed)
+    names = ["sr", "diel", "cu", "corecu", "core", "solder", "uf", "die", "tim", "adh", "lid"]
+    base = {  # E (MPa), nu, CTE (1/degC): database-like 25 degC constants
+        "sr": (3000.0, 0.35, 50e-6), "diel": (5000.0, 0.34, 40e-6), "cu": (60000.0, 0.32, 17e-6),
+        "corecu": (117000.0, 0.34, 17e-6), "core": (28000.0, 0.2, 12e-6), "solder": (40000.0, 0.4, 22.5e-6),
+        "uf": (8000.0, 0.35, 30e-6), "die": (130000.0, 0.28, 2.6e-6), "tim": (10.0, 0.45, 100e-6),
+        "adh": (2000.0, 0.4, 60e-6), "lid": (117000.0, 0.34, 17e-6)}
+    jit = {k: (rng.uniform(0.9, 1.1), rng.uniform(0.9, 1.1)) for k in names}
+    mat = {k: (base[k][0] * jit[k][0], base[k][1], base[k][2] * jit[k][1]) for k in names}
+    n = n_inplane
+    L = 55.0
+    xs = np.array([-L / 2 + L * q / n for q in range(n + 1)])
+    ys = xs.copy()
+    rows = _stack_8_2_8(rng)
+    zr = np.concatenate([[0.0], np.cumsum([t for _, t in rows])])
+    z_sub = float(zr[-1])
+    # three groups (bottom build-up, core with its Cu foils, top build-up) in 4 bands each (substrateBands, 04-homogenize.js:64-105)
+    i_core = [q for q, (nm, _) in enumerate(rows) if nm == "core"][0]
+    z_lo, z_hi = zr[i_core - 1], zr[i_core + 2]
+    bands = []
+    for (g0, g1) in [(0.0, z_lo), (z_lo, z_hi), (z_hi, z_sub)]:
+        for q in range(4):
+            bands.append((g0 + (g1 - g0) * q / 4, g0 + (g1 - g0) * (q + 1) / 4))
+    zb = [bands[0][0]] + [b1 for (_, b1) in bands]
+    t_bump, t_adh, t_die, t_tim, t_lid = 0.08, 0.10, 0.775, 0.05, 0.5
+    z0 = z_sub
+    zs = list(zb)
+    zs += [z0 + t_bump / 2, z0 + t_bump, z0 + t_adh]                           # bump (2), adhesive top (1)
+    zs += list(z0 + t_adh + (t_bump + t_die - t_adh) * np.arange(1, 8) / 7)   # die above the adhesive (7)
+    zs += [z0 + t_bump + t_die + t_tim]                                       # TIM (1)
+    zs += list(z0 + t_bump + t_die + t_tim + t_lid * np.arange(1, 10) / 9)    # lid plate (9)
+    zs = np.array(zs)
+    nz = len(zs)
+    assert nz == 33, nz
+    ncz = nz - 1
+    nb = len(bands)
+    # layers: 0..11 substrate bands, 12-13 bump, 14 adhesive top / die bottom, 15-21 die, 22 TIM, 23-31 lid
+    ncells = n * n * ncz
+    cg = np.full(2 * ncells, -1, np.int32); cp = np.zeros(2 * ncells, np.int32); cs = np.zeros(2 * ncells)
+    I, J, K = np.meshgrid(np.arange(n), np.arange(n), np.arange(ncz), indexing="ij")
+    c = ((I * n + J) * ncz + K).ravel(); I = I.ravel(); J = J.ravel(); K = K.ravel()
+    d0, d1 = int(round(n * (L / 2 - 12.5) / L)), int(round(n * (L / 2 + 12.5) / L))   # die footprint cells
+    m0, m1 = max(1, n * 3 // 160), n - max(1, n * 3 // 160)                            # lid outline
+    fw = max(2, n * 9 // 160)                                                          # lid foot width
+    in_die = (I >= d0) & (I < d1) & (J >= d0) & (J < d1)
+    in_lid = (I >= m0) & (I < m1) & (J >= m0) & (J < m1)
+    in_foot = in_lid & ~((I >= m0 + fw) & (I < m1 - fw) & (J >= m0 + fw) & (J < m1 - fw))
+    G = dict(sub=0, solder=1, uf=2, die=3, tim=4, adh=5, lid=6)
+    def put(mask, g, part, scale=1.0, q=0):
+        cc = c[mask]
+        cg[2 * cc + q] = g; cp[2 * cc + q] = part; cs[2 * cc + q] = scale
+    put(K < nb, G["sub"], PART["SUB"])
+    put((K >= 12) & (K < 14) & in_die, G["solder"], PART["SOLDER"], 0.3, 0)
+    put((K >= 12) & (K < 14) & in_die, G["uf"], PART["UF_BUMP"], 0.7, 1)
+    put((K == 14) & in_die, G["die"], PART["DIE"])
+    put((K >= 12) & (K < 15) & in_foot, G["adh"], PART["LIDADH"])
+    put((K >= 15) & (K < 22) & in_die, G["die"], PART["DIE"])
+    put((K >= 15) & (K < 23) & in_foot, G["lid"], PART["LID"])
+    put((K == 22) & in_die, G["tim"], PART["TIM"])
+    put((K >= 23) & in_lid, G["lid"], PART["LID"])
+    feat = sorted({d0, d1, m0, m1, m0 + fw, m1 - fw})
+    mesh = build_structured_mesh(xs, ys, zs, cg, cp, cs, featureX=feat, featureY=feat)
+    mesh.constraints = constraints321(mesh, CONSTRAINT_SPAN * L / 2)
+    # property sets: 0..11 layered bands, then the homogeneous groups
+    def row_mat(nm):
+        E, nu, a = mat[nm]
+        return iso_d(E, nu), a, a
+    band_subs = []
+    for (b0, b1) in bands:
+        subs = []
+        for q, (nm, _) in enumerate(rows):
+            a, bb = max(b0, zr[q]), min(b1, zr[q + 1])
+            if bb - a > 1e-12:
+                D, axy, az = row_mat(nm)
+                subs.append((a, bb, D, axy, az))
+        band_subs.append((b0, b1, subs))
+    hom = [row_mat("core")]  # placeholder for pset ordering below
+    hom_names = ["solder", "uf", "die", "tim", "adh", "lid"]
+    mats: List = [None] * nb
+    for nm in hom_names:
+        E, nu, a = mat[nm]
+        mats.append((column_d(E, nu) if nm == "solder" else iso_d(E, nu), a, a))
+    del hom
+    def layered_fn(p, Ta, Tb):
+        b0, b1, subs = band_subs[p]
+        return layered_section(b0, b1, subs, Ta, Tb)
+    ng = 7
+    group_layered = np.array([1, 0, 0, 0, 0, 0, 0], np.int32)
+    group_pset = np.array([0, nb + 0, nb + 1, nb + 2, nb + 3, nb + 4, nb + 5], np.int32)
+    sec_of_layer = np.zeros(ncz, np.int32)
+    sec_of_layer[:nb] = np.arange(nb)
+    return Package(name="lidded_c2", mesh=mesh, group_layered=group_layered, group_stage=np.zeros(ng, np.int32),
+                   group_pset=group_pset, sec_of_layer=sec_of_layer, npset=nb + len(hom_names),
+                   step_fn=lambda Ta, Tb: _homog_step(mats, Ta, Tb, layered_fn=layered_fn), Ta=150.0, Tb=25.0,
+                   meta=dict(workload=f"lidded_c2 {n}x{n}x32", bottom_plane=0, seed=seed))
+
+
+def rms_warpage(mesh: Mesh, u: np.ndarray, k: int = 0) -> float:
+    """RMS of the bottom-plane z-displacement about its least-squares plane (fitPlane, src/core/01-util.js:176-190)."""
+    ids = mesh.nodeId.reshape(mesh.nx, mesh.ny, mesh.nz)[:, :, k]
+    X, Y = np.meshgrid(mesh.xs, mesh.ys, indexing="ij")
+    ok = ids >= 0
+    x = X[ok]; y = Y[ok]; w = u[3 * ids[ok] + 2]
+    mx, my, mw = x.mean(), y.mean(), w.mean()
+    dx, dy, dw = x - mx, y - my, w - mw
+    sxx, sxy, syy, sxw, syw = (dx * dx).sum(), (dx * dy).sum(), (dy * dy).sum(), (dx * dw).sum(), (dy * dw).sum()
+    det = sxx * syy - sxy * sxy
+    c1 = (sxw * syy - syw * sxy) / det if abs(det) > 1e-300 else 0.0
+    c2 = (syw * sxx - sxw * sxy) / det if abs(det) > 1e-300 else 0.0
+    r = dw - c1 * dx - c2 * dy
+    return float(np.sqrt((r * r).mean()))
+
+
+def pv_warpage(mesh: Mesh, u: np.ndarray, k: int = 0) -> float:
+    """Peak-to-valley of the bottom-plane z-displacement about its least-squares plane (as V5, 15-verify.js:228)."""
+    ids = mesh.nodeId.reshape(mesh.nx, mesh.ny, mesh.nz)[:, :, k]
+    X, Y = np.meshgrid(mesh.xs, mesh.ys, indexing="ij")
+    ok = ids >= 0
+    x = X[ok]; y = Y[ok]; w = u[3 * ids[ok] + 2]
+    A = np.stack([np.ones_like(x), x, y], 1)
+    c, *_ = np.linalg.lstsq(A, w, rcond=None)
+    r = w - A @ c
+    return float(r.max() - r.min())
