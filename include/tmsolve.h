@@ -1,0 +1,200 @@
+/*
+ * tmsolve.h -- C-ABI of the B200 solve path of the FCBGA thermomechanical tool.
+ *
+ * The reference tool (ProtonNeutronElectron69/Packaging-TM-modeling-tool) is
+ * JavaScript; its solve path runs inside the compute worker's driver thread.
+ * This library replaces, behind a thin context-aware N-API addon, the
+ * following reference interfaces (paths relative to the reference project):
+ *
+ *   tm_create          new FEModel(mesh, cfg) + new LinearSolver(model, opts)
+ *                      src/core/09-assembly.js:208-233, src/core/10-solver.js:826-841
+ *   tm_assemble_step   FEModel.assembleStep(Ta, Tb, stage, rhs) with applyConstraints
+ *                      src/core/09-assembly.js:392-424, 445-464 (prepareStep's per-group
+ *                      data, :346-365, is computed by the caller and passed in tm_step)
+ *   tm_set_bcsr        the assembled model.pattern / model.val / model.isConstrained that
+ *                      LinearSolver reads (src/core/09-assembly.js:220-223, 445-450)
+ *   tm_solve           LinearSolver.solve(f, label, key)  src/core/10-solver.js:933-994
+ *   tm_matvec          fullMatVec(P, val, x, y)           src/core/09-assembly.js:151-165
+ *   tm_anand_screen    screenJoints' per-site Anand loop  src/core/13-fatigue.js:395-451
+ *                      (AnandPoint.stepColumn / step, :13-166)
+ *   tm_anand_step      AnandPoint.step + commit           src/core/13-fatigue.js:67-143, 229-232
+ *
+ * Conventions
+ *   - Node, element and DOF numbering are the mesher's, taken verbatim
+ *     (src/core/06-mesher.js:14-72): nodes z fastest then y then x, DOF = 3*node + comp.
+ *   - Host buffers passed in are read during the call and never retained; the
+ *     context owns all device memory. Output buffers are caller-allocated.
+ *   - Every entry point returns a tm_status; TM_NOT_CONVERGED is the only
+ *     non-error status (the addon maps it to converged:false, everything else to
+ *     a thrown Error, as LinearSolver's callers expect: src/core/11-analysis.js:204).
+ *   - One context per calling thread; calls are synchronous on that thread.
+ *   - There is no CPU fallback: without a usable sm_100 GPU, tm_create returns TM_NO_DEVICE.
+ */
+#ifndef TMSOLVE_H
+#define TMSOLVE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int tm_status;
+#define TM_OK 0
+#define TM_NOT_CONVERGED 1   /* PCG did not reach tol (converged:false in the reference record) */
+#define TM_NONFINITE 2       /* NaN/Inf in the input or during the iteration */
+#define TM_TIMEOUT 3         /* a bounded device wait ran out */
+#define TM_BAD_INPUT 4       /* inconsistent sizes, indices or call order */
+#define TM_CUDA 5            /* a CUDA runtime error */
+#define TM_NO_DEVICE 6       /* no sm_100 device available: there is no CPU fallback */
+
+typedef struct tm_ctx tm_ctx;
+
+/* The mesher's output (buildStructuredMesh, 06-mesher.js:66-71) plus the element
+ * property-set map and the constraint DOFs (constraints321, 06-mesher.js:112-116). */
+typedef struct {
+  int32_t nx, ny, nz;            /* grid lines in x, y and z planes */
+  const double* xs;              /* nx */
+  const double* ys;              /* ny */
+  const double* zs;              /* nz */
+  int32_t nn, ne;                /* nodes, elements */
+  const double* coords;          /* 3*nn */
+  const int32_t* nodeId;         /* nx*ny*nz, -1 where no node */
+  const int32_t* conn;           /* 8*ne, local order loc of 06-mesher.js:49 */
+  const int32_t* eIJK;           /* 3*ne */
+  const int32_t* colStart;       /* nx*ny+1 */
+  const int32_t* cellElems;      /* 2*(nx-1)*(ny-1)*(nz-1), -1 where no phase */
+  const int32_t* eGroup;         /* ne */
+  const int8_t* ePart;           /* ne, PART ids of 06-mesher.js:3-4 */
+  const double* eScale;          /* ne */
+  int32_t ngroups;
+  const int32_t* groupStage;     /* ngroups: birth stage of every group (09-assembly.js:339) */
+  int32_t npset;                 /* property sets: homogeneous groups and layered sections */
+  const int32_t* ePset;          /* ne: property set of every element (group, or section of its layer) */
+  int32_t nconstr;
+  const int32_t* constr;         /* constrained DOFs */
+  int32_t nfeatureX, nfeatureY;  /* feature lines kept at every multigrid level (06-mesher.js:504) */
+  const int32_t* featureX;
+  const int32_t* featureY;
+} tm_mesh;
+
+/* Per-step property sets (FEModel.prepareStep's output, 09-assembly.js:346-365):
+ * homogeneous: mean stiffness D (36) and thermal stress increment s0 (6);
+ * layered: step-mean weights W_j (3 x 36) and thermal weights V_j (3 x 6). */
+typedef struct {
+  int32_t stage;                 /* element birth: group stage <= stage (09-assembly.js:401-403) */
+  const int32_t* psetLayered;    /* npset, 0 or 1 */
+  const double* D;               /* 36*npset (homogeneous sets) */
+  const double* s0;              /* 6*npset */
+  const double* W;               /* 108*npset (layered sets) */
+  const double* V;               /* 18*npset */
+  const int32_t* psetBorn;       /* npset: thermal load of the set on (sec._born / g._born) */
+} tm_step;
+
+#define TM_PC_MG 0
+#define TM_PC_JACOBI 1
+#define TM_PREC_FP64 0
+#define TM_PREC_MIXED 1
+
+typedef struct {
+  double tol;                    /* relative residual in the scaled 2-norm (PCG_TOL 1e-8) */
+  int32_t maxit;                 /* PCG_MAXIT 2000 */
+  int32_t warm;                  /* stored solutions for the warm start (WARM_START_MAX 20), 0 = off */
+  int32_t precond;               /* TM_PC_MG or TM_PC_JACOBI */
+  int32_t precision;             /* TM_PREC_FP64 or TM_PREC_MIXED */
+  int64_t key;                   /* preconditioner key (solve(f, label, key)); -1 = none */
+  void (*progress)(void* user, int32_t it, double relres);  /* called between iterations, may be NULL */
+  void* progress_user;
+  int32_t progress_every;        /* iterations between progress calls */
+} tm_solve_opts;
+
+typedef struct {
+  int32_t iters;                 /* total PCG iterations of the solve (res.iters) */
+  double relres;                 /* final relative residual */
+  double iters0;                 /* relative residual of the initial guess (res.iters0) */
+  int32_t converged;
+  double ms;                     /* wall time of the solve */
+  double pc_ms;                  /* preconditioner set-up time */
+  int32_t rebuilt;               /* a preconditioner was (re)built in this solve */
+  int32_t warm;                  /* stored solutions after the solve */
+  int32_t fallback;              /* fell back to another preconditioner */
+  int32_t jitter_count;          /* jittered pivots of the column factors (10-solver.js:61-64, 490) */
+  int32_t levels;                /* multigrid levels */
+  int32_t status;
+  int32_t refinements;           /* mixed precision: outer FP64 refinement sweeps */
+} tm_solve_info;
+
+/* Library defaults for tm_solve_opts (the reference's CONST values). */
+void tm_default_solve_opts(tm_solve_opts* opts);
+
+/* Creates the device model of a mesh (FEModel + LinearSolver). */
+tm_status tm_create(const tm_mesh* mesh, tm_ctx** out);
+
+/* Assembles K and the thermal load of one step on the device, then applies the
+ * constraints (FEModel.assembleStep + applyConstraints). rhs_out (3*nn) may be NULL. */
+tm_status tm_assemble_step(tm_ctx* ctx, const tm_step* step, double* rhs_out);
+
+/* Loads a caller-assembled operator: the full symmetric 3x3-block CSR of
+ * fullPatternFromUpper (09-assembly.js:136-148) with constraints already applied. */
+tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, const double* val,
+                      const uint8_t* isConstrained);
+
+/* Solves K u = f for the current operator (LinearSolver.solve). The operator is
+ * Jacobi-scaled in place on the first solve after an assembly, as in the reference. */
+tm_status tm_solve(tm_ctx* ctx, const double* f, double* u, const tm_solve_opts* opts, tm_solve_info* info);
+
+/* y = K x with the current operator (unscaled before the first solve of a step). */
+tm_status tm_matvec(tm_ctx* ctx, const double* x, double* y);
+
+/* Downloads the current operator as the full block CSR of the mesh (for checks). */
+tm_status tm_get_bcsr(tm_ctx* ctx, int32_t* rowPtr, int32_t* col, double* val);
+
+/* Sizes: nn, ne, nnz blocks of the full block CSR, ndof, multigrid levels, coarsest dof. */
+tm_status tm_sizes(tm_ctx* ctx, int64_t* out6);
+
+tm_status tm_destroy(tm_ctx* ctx);
+
+/* Message of the last error on this thread; returns its length. */
+int32_t tm_last_error(char* buf, size_t len);
+
+/* ---- device-resident entry points (inputs and outputs already in device memory) ---- */
+tm_status tm_solve_device(tm_ctx* ctx, const double* f_dev, double* u_dev, const tm_solve_opts* opts, tm_solve_info* info);
+tm_status tm_matvec_device(tm_ctx* ctx, const double* x_dev, double* y_dev);
+
+/* ---- Anand viscoplastic return map (13-fatigue.js:13-237) ---- */
+typedef struct {
+  double A, QR, xi, m, shat, n, h0, a, s0, nu;   /* Anand constants and Poisson ratio */
+  const double* Etab;            /* E(T) in MPa on the 1 degC grid -80..300 (381 values) */
+  const double* Ftab;            /* thermal strain F(T) on the same grid */
+} tm_anand_material;
+
+/* Screening of free-standing solder columns (screenJoints, 13-fatigue.js:379-455):
+ *   table: nsites x ntemps x 6 bump-layer total strains at the cycling temperatures temps;
+ *   the time history (t, T, cycle, phase) of cycleHistory (13-fatigue.js:275-293);
+ * outputs per site: dW (inelastic work density of the last cycle), dE (equivalent
+ * inelastic strain of the last cycle), stab (cycle-to-cycle change). Sites whose
+ * first table entry is not finite are skipped (NaN outputs). Host pointers. */
+tm_status tm_anand_screen(const tm_anand_material* mat, int32_t nsites, int32_t ntemps, const double* temps,
+                          const double* table, int32_t nsteps, const double* t, const double* T,
+                          const int32_t* cycle, const int32_t* phase, int32_t cycles,
+                          double* dW, double* dE, double* stab);
+
+/* The same with device pointers for table and outputs (time history on the host). */
+tm_status tm_anand_screen_device(const tm_anand_material* mat, int32_t nsites, int32_t ntemps, const double* temps,
+                                 const double* table_dev, int32_t nsteps, const double* t, const double* T,
+                                 const int32_t* cycle, const int32_t* phase, int32_t cycles,
+                                 double* dW_dev, double* dE_dev, double* stab_dev);
+
+/* Batched material-point steps: npts independent points, each with a 12-double state
+ * (ep[6], s, ebar, W, sigEq, lastD, spare) updated in place when commit != 0;
+ * eps (6 per point) engineering mechanical strain; sig (6 per point) and, when
+ * D != NULL, the consistent tangent (36 per point). Host pointers. */
+tm_status tm_anand_step(const tm_anand_material* mat, int32_t npts, double* state, const double* eps,
+                        double T, double dt, double* sig, double* D, int32_t commit);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMSOLVE_H */

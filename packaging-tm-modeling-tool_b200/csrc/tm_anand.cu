@@ -1,0 +1,331 @@
+// Anand viscoplastic return map on the GPU (FP64): one thread per bump site integrates the
+// whole cycle history, with the material state in registers.
+//
+// Follows src/core/13-fatigue.js:
+//   AnandPoint._solveS   :32-52    inner scalar Newton on s with bisection safeguard
+//   stepConstants        :61-65
+//   AnandPoint.step      :67-143   backward-Euler J2 radial return, consistent tangent
+//   stepColumn           :153-166  in-plane stresses of a free-standing column held at zero
+//   _dsdd                :209-218
+//   screenJoints loop    :395-451  strain interpolation, in-plane guesses, per-cycle W and ebar
+// Compiled without fused multiply-add, like the reference's JavaScript arithmetic.
+#include <cmath>
+#include <vector>
+
+#include "tm_internal.h"
+
+namespace tmg {
+
+namespace {
+
+constexpr int ANAND_NEWTON_MAXIT = 60;
+constexpr double ANAND_TOL = 1e-11;
+constexpr int COLUMN_NEWTON_MAXIT = 20;
+constexpr double COLUMN_STRESS_TOL = 1e-3;
+constexpr double KELVIN = 273.15;
+constexpr int TGRID_MIN = -80;
+constexpr int TGRID_N = 381;
+
+struct AnandConst {
+  double A, QR, xi, m, shat, n, h0, a, s0, nu;
+};
+
+struct StepK {
+  double G, K, expQ, rate0, dt;
+};
+
+__device__ __forceinline__ double sgn(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); }
+
+struct Point {
+  double ep[6], s, ebar, W, sigEq, lastD;
+  double tr_ep[6], tr_s, tr_ebar, tr_W, tr_sigEq;
+};
+
+__device__ double solve_s(const AnandConst& P, double s_n, double d, double dt, double expQ) {
+  if (d <= 0) return s_n;
+  const double sstar = P.shat * pow(d / (dt * P.A) * expQ, P.n);
+  const double sn = s_n, h0 = P.h0, a = P.a;
+  double lo = fmin(sn, sstar), hi = fmax(sn, sstar);
+  if (hi - lo < 1e-14) return sn;
+  double s = 0.5 * (lo + hi);
+  for (int it = 0; it < ANAND_NEWTON_MAXIT; it++) {
+    const double B0 = 1 - s / sstar;
+    const double f = s - sn - h0 * pow(fabs(B0), a) * sgn(B0) * d;
+    if (fabs(f) < ANAND_TOL * fmax(1.0, sn)) break;
+    if (f > 0) hi = s; else lo = s;
+    const double B = 1 - s / sstar;
+    const double dphi = 1 + h0 * a * pow(fabs(B), a - 1) * d / sstar;
+    double sn1 = s - f / dphi;
+    if (!(sn1 > lo && sn1 < hi)) sn1 = 0.5 * (lo + hi);
+    if (fabs(sn1 - s) < 1e-15 * fmax(1.0, s)) { s = sn1; break; }
+    s = sn1;
+  }
+  return s;
+}
+
+__device__ double dsdd(const AnandConst& P, double d, double s, double dt, double expQ) {
+  if (d <= 0) return 0;
+  const double sstar = P.shat * pow(d / (dt * P.A) * expQ, P.n);
+  const double B = 1 - s / sstar;
+  const double absB = fabs(B), sg = sgn(B);
+  const double h0 = P.h0, a = P.a, n = P.n;
+  const double dphi_ds = 1 + h0 * a * pow(absB, a - 1) * d / sstar;
+  const double dphi_dd = -h0 * pow(absB, a) * sg - h0 * a * pow(absB, a - 1) * s * n / sstar;
+  return -dphi_dd / dphi_ds;
+}
+
+__device__ double grid_at(const double* arr, double T) {
+  const double x = T - TGRID_MIN;
+  if (x <= 0) return arr[0];
+  if (x >= TGRID_N - 1) return arr[TGRID_N - 1];
+  const int i = (int)floor(x);
+  const double t = x - i;
+  const double a = arr[i], b = arr[i + 1];
+  return a + t * (b - a);
+}
+
+__device__ StepK step_constants(const AnandConst& P, const double* Etab, double T, double dt) {
+  const double E = grid_at(Etab, T), nu = P.nu;
+  const double expQ = exp(P.QR / (T + KELVIN));
+  StepK k;
+  k.G = E / (2 * (1 + nu)); k.K = E / (3 * (1 - 2 * nu)); k.expQ = expQ; k.rate0 = dt * P.A / expQ; k.dt = dt;
+  return k;
+}
+
+// AnandPoint.step (13-fatigue.js:67-143): fills sig (6) and D (36, when wantTangent)
+__device__ double anand_step(const AnandConst& P, Point& pt, const double* eps, const StepK& k, double* sig, double* D, bool wantTangent) {
+  const double G = k.G, K = k.K, expQ = k.expQ, rate0 = k.rate0, dt = k.dt;
+  const double vol = (eps[0] + eps[1] + eps[2]) / 3;
+  double e[6], str[6], nvec[6];
+  e[0] = eps[0] - vol - pt.ep[0]; e[1] = eps[1] - vol - pt.ep[1]; e[2] = eps[2] - vol - pt.ep[2];
+  e[3] = 0.5 * eps[3] - pt.ep[3]; e[4] = 0.5 * eps[4] - pt.ep[4]; e[5] = 0.5 * eps[5] - pt.ep[5];
+  for (int i = 0; i < 6; i++) str[i] = 2 * G * e[i];
+  const double nrm = sqrt(str[0] * str[0] + str[1] * str[1] + str[2] * str[2] + 2 * (str[3] * str[3] + str[4] * str[4] + str[5] * str[5]));
+  const double sigTr = sqrt(1.5) * nrm;
+  double d = 0, s1 = pt.s, dDdSig = 0;
+  if (sigTr > 1e-14 && dt > 0) {
+    const double dmax = sigTr / (3 * G);
+    double lo = 0, hi = dmax;
+    double dd = pt.lastD > 0 && pt.lastD < dmax ? pt.lastD : fmin(dmax, rate0 * pow(sinh(P.xi * sigTr / pt.s), 1 / P.m));
+    if (!isfinite(dd) || dd <= 0) dd = 0.5 * dmax;
+    double rg = 0, rs = pt.s, rx = 0, rsh = 0;
+    for (int it = 0; it < ANAND_NEWTON_MAXIT; it++) {
+      rs = solve_s(P, pt.s, dd, dt, expQ);
+      rx = P.xi * (sigTr - 3 * G * dd) / rs;
+      rsh = sinh(rx);
+      rg = dd - rate0 * pow(rsh, 1 / P.m);
+      if (!isfinite(rg)) { lo = dd; dd = 0.5 * (lo + hi); continue; }
+      if (fabs(rg) < ANAND_TOL * fmax(dmax, 1e-30)) break;
+      if (rg > 0) hi = dd; else lo = dd;
+      const double fx = rate0 * (1 / P.m) * pow(rsh, 1 / P.m - 1) * cosh(rx);
+      const double ds = dsdd(P, dd, rs, dt, expQ);
+      const double sg = sigTr - 3 * G * dd;
+      const double dg = 1 + fx * P.xi * (3 * G / rs + sg * ds / (rs * rs));
+      double dn = dd - rg / dg;
+      if (!(dn > lo && dn < hi) || !isfinite(dn)) dn = 0.5 * (lo + hi);
+      if (fabs(dn - dd) < 1e-16 * fmax(dmax, 1e-30)) { dd = dn; break; }
+      dd = dn;
+    }
+    d = dd; s1 = rs;
+    pt.lastD = d;
+    if (wantTangent) {
+      const double fx = rate0 * (1 / P.m) * pow(rsh, 1 / P.m - 1) * cosh(rx);
+      const double ds = dsdd(P, dd, rs, dt, expQ);
+      const double sg = sigTr - 3 * G * dd;
+      const double dg = 1 + fx * P.xi * (3 * G / rs + sg * ds / (rs * rs));
+      dDdSig = (fx * P.xi / rs) / dg;
+    }
+  }
+  const double theta = sigTr > 1e-14 ? 1 - 3 * G * d / sigTr : 1;
+  if (nrm > 0) for (int i = 0; i < 6; i++) nvec[i] = str[i] / nrm;
+  else for (int i = 0; i < 6; i++) nvec[i] = 0;
+  const double dg = sqrt(1.5) * d;
+  for (int i = 0; i < 6; i++) pt.tr_ep[i] = pt.ep[i] + dg * nvec[i];
+  const double sm = 3 * K * vol;
+  sig[0] = theta * str[0] + sm; sig[1] = theta * str[1] + sm; sig[2] = theta * str[2] + sm;
+  sig[3] = theta * str[3]; sig[4] = theta * str[4]; sig[5] = theta * str[5];
+  const double sEq = sigTr - 3 * G * d;
+  pt.tr_s = s1; pt.tr_ebar = pt.ebar + d; pt.tr_W = pt.W + 0.5 * (pt.sigEq + sEq) * d; pt.tr_sigEq = sEq;
+  if (wantTangent) {
+    const double thetaBar = 2 * G * 1.5 * dDdSig - (1 - theta);
+    const double c1 = 2 * G * theta, c2 = 2 * G * thetaBar;
+    for (int i = 0; i < 6; i++)
+      for (int j = 0; j < 6; j++) {
+        double v = -c2 * nvec[i] * nvec[j];
+        if (i < 3 && j < 3) v += K + c1 * ((i == j ? 1 : 0) - 1.0 / 3);
+        else if (i == j) v += 0.5 * c1;
+        D[i * 6 + j] = v;
+      }
+  }
+  return d;
+}
+
+__device__ void inv3(const double* J, double* out) {
+  const double a = J[0], b = J[1], c = J[2], d = J[3], e = J[4], f = J[5], g = J[6], h = J[7], i = J[8];
+  const double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+  out[0] = (e * i - f * h) / det; out[1] = (c * h - b * i) / det; out[2] = (b * f - c * e) / det;
+  out[3] = (f * g - d * i) / det; out[4] = (a * i - c * g) / det; out[5] = (c * d - a * f) / det;
+  out[6] = (d * h - e * g) / det; out[7] = (b * g - a * h) / det; out[8] = (a * e - b * d) / det;
+}
+
+// stepColumn (13-fatigue.js:153-166)
+__device__ double step_column(const AnandConst& P, Point& pt, double* eps, const StepK& k, double* sig, double* D) {
+  const int Pi[3] = {0, 1, 3};
+  double A[9], Ai[9];
+  double d = 0;
+  for (int it = 0; it < COLUMN_NEWTON_MAXIT; it++) {
+    d = anand_step(P, pt, eps, k, sig, D, true);
+    const double r0 = sig[0], r1 = sig[1], r2 = sig[3];
+    const double ref = fmax(fmax(1.0, fabs(sig[2])), fmax(fabs(sig[4]), fabs(sig[5])));
+    if (fmax(fmax(fabs(r0), fabs(r1)), fabs(r2)) < COLUMN_STRESS_TOL * ref) break;
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) A[3 * r + c] = D[6 * Pi[r] + Pi[c]];
+    inv3(A, Ai);
+    for (int r = 0; r < 3; r++) eps[Pi[r]] -= Ai[3 * r] * r0 + Ai[3 * r + 1] * r1 + Ai[3 * r + 2] * r2;
+  }
+  return d;
+}
+
+__device__ void commit(Point& pt) {
+  for (int i = 0; i < 6; i++) pt.ep[i] = pt.tr_ep[i];
+  pt.s = pt.tr_s; pt.ebar = pt.tr_ebar; pt.W = pt.tr_W; pt.sigEq = pt.tr_sigEq;
+}
+
+// screenJoints per-site loop (13-fatigue.js:416-451), thread per site
+__global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const double* __restrict__ table, int nsteps,
+                         const int* __restrict__ wi, const double* __restrict__ wt, const double* __restrict__ Fth,
+                         const StepK* __restrict__ kc, const double* __restrict__ Th, const int* __restrict__ cycle,
+                         const int* __restrict__ phase, int cycles, double* __restrict__ dW, double* __restrict__ dE,
+                         double* __restrict__ stab) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsites) return;
+  const double* tab = table + (size_t)q * ntemps * 6;
+  if (!isfinite(tab[0])) { dW[q] = NAN; dE[q] = NAN; stab[q] = NAN; return; }
+  Point pt;
+  for (int i = 0; i < 6; i++) pt.ep[i] = 0;
+  pt.s = P.s0; pt.ebar = 0; pt.W = 0; pt.sigEq = 0; pt.lastD = 0;
+  double e25[6], eps[6] = {0, 0, 0, 0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0}, sig[6], D[36];
+  for (int c = 0; c < 6; c++) e25[c] = i25 >= 0 ? tab[i25 * 6 + c] : 0;
+  const int IP[3] = {0, 1, 3};
+  const double nu = P.nu;
+  // W and ebar at the end of the last three cycles (the reference keeps every cycle)
+  double Wlast[3] = {0, 0, 0}, Elast[3] = {0, 0, 0};  // cycles nc-2, nc-1, nc
+  for (int k = 1; k < nsteps; k++) {
+    const double* a = tab + wi[k] * 6;
+    const double* b = a + 6;
+    const double t = wt[k];
+    const double ez = a[2] + t * (b[2] - a[2]) - e25[2] - Fth[k];
+    if (k > 2 && phase[k] == phase[k - 1]) {
+      for (int r = 0; r < 3; r++) eps[IP[r]] = 2 * e1[r] - e2[r];
+    } else {
+      eps[0] -= nu * (ez - eps[2]);
+      eps[1] -= nu * (ez - eps[2]);
+    }
+    eps[2] = ez;
+    eps[4] = a[4] + t * (b[4] - a[4]) - e25[4];
+    eps[5] = a[5] + t * (b[5] - a[5]) - e25[5];
+    step_column(P, pt, eps, kc[k], sig, D);
+    commit(pt);
+    for (int r = 0; r < 3; r++) { e2[r] = e1[r]; e1[r] = eps[IP[r]]; }
+    const int cyc = cycle[k];
+    const int slot = cyc - (cycles - 2);
+    if (slot >= 0 && slot < 3) { Wlast[slot] = pt.W; Elast[slot] = pt.ebar; }
+  }
+  // cycles before nc-2 stay 0 in the reference's per-cycle arrays when never reached
+  const int nc = cycles;
+  const double Wn = Wlast[2], Wn1 = nc - 1 >= 0 ? Wlast[1] : 0, Wn2 = nc - 2 >= 0 ? Wlast[0] : 0;
+  dW[q] = Wn - Wn1;
+  dE[q] = Elast[2] - Elast[1];
+  stab[q] = nc >= 2 ? fabs((Wn - Wn1) - (Wn1 - Wn2)) / fmax(Wn - Wn1, 1e-30) : NAN;
+}
+
+__global__ void k_point_step(AnandConst P, const double* __restrict__ Etab, int npts, double* __restrict__ state,
+                             const double* __restrict__ eps, double T, double dt, double* __restrict__ sig, double* __restrict__ D,
+                             int commitFlag) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  double* st = state + 12 * (size_t)q;
+  Point pt;
+  for (int i = 0; i < 6; i++) pt.ep[i] = st[i];
+  pt.s = st[6]; pt.ebar = st[7]; pt.W = st[8]; pt.sigEq = st[9]; pt.lastD = st[10];
+  const StepK k = step_constants(P, Etab, T, dt);
+  double Dl[36];
+  anand_step(P, pt, eps + 6 * (size_t)q, k, sig + 6 * (size_t)q, D ? D + 36 * (size_t)q : Dl, true);
+  if (commitFlag) commit(pt);
+  for (int i = 0; i < 6; i++) st[i] = pt.ep[i];
+  st[6] = pt.s; st[7] = pt.ebar; st[8] = pt.W; st[9] = pt.sigEq; st[10] = pt.lastD;
+}
+
+__global__ void k_step_constants(AnandConst P, const double* __restrict__ Etab, int nsteps, const double* __restrict__ t,
+                                 const double* __restrict__ T, StepK* __restrict__ kc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nsteps) return;
+  if (k == 0) { kc[0] = StepK{0, 0, 0, 0, 0}; return; }
+  kc[k] = step_constants(P, Etab, T[k], t[k] - t[k - 1]);
+}
+
+AnandConst to_const(const tm_anand_material& m) {
+  return AnandConst{m.A, m.QR, m.xi, m.m, m.shat, m.n, m.h0, m.a, m.s0, m.nu};
+}
+
+double grid_at_host(const double* arr, double T) {
+  const double x = T - TGRID_MIN;
+  if (x <= 0) return arr[0];
+  if (x >= TGRID_N - 1) return arr[TGRID_N - 1];
+  const int i = (int)std::floor(x);
+  const double t = x - i;
+  return arr[i] + t * (arr[i + 1] - arr[i]);
+}
+
+}  // namespace
+
+void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps, const double* table_d, int nsteps,
+                         const double* t_h, const double* T_h, const int* cycle_h, const int* phase_h, int cycles, double* dW_d,
+                         double* dE_d, double* stab_d, cudaStream_t s) {
+  if (nsteps < 2 || ntemps < 2 || cycles < 1) fail(TM_BAD_INPUT, "anand screening: need >= 2 time steps, >= 2 temperatures, >= 1 cycle");
+  for (int k = 0; k < nsteps; k++)
+    if (cycle_h[k] < 0 || cycle_h[k] > cycles) fail(TM_BAD_INPUT, "anand screening: cycle index out of range");
+  int i25 = -1;
+  for (int i = 0; i < ntemps; i++) if (temps[i] == 25) { i25 = i; break; }
+  // per-step interpolation weights and thermal strains (13-fatigue.js:395-401)
+  std::vector<int> wi(nsteps);
+  std::vector<double> wt(nsteps), Fth(nsteps);
+  for (int k = 0; k < nsteps; k++) {
+    int i;
+    if (T_h[k] <= temps[0]) i = 0;
+    else if (T_h[k] >= temps[ntemps - 1]) i = ntemps - 2;
+    else {
+      int lo = 0, hi = ntemps - 1;
+      while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (temps[mid] <= T_h[k]) lo = mid; else hi = mid; }
+      i = lo;
+    }
+    wi[k] = i;
+    const double tt = (T_h[k] - temps[i]) / (temps[i + 1] - temps[i]);
+    wt[k] = tt < 0 ? 0 : (tt > 1 ? 1 : tt);
+    Fth[k] = grid_at_host(mat.Ftab, T_h[k]) - grid_at_host(mat.Ftab, 25);
+  }
+  DBuf<int> d_wi, d_cycle, d_phase;
+  DBuf<double> d_wt, d_Fth, d_t, d_T, d_E;
+  DBuf<StepK> d_kc;
+  d_wi.upload(wi, s); d_wt.upload(wt, s); d_Fth.upload(Fth, s);
+  d_cycle.upload(cycle_h, nsteps, s); d_phase.upload(phase_h, nsteps, s);
+  d_t.upload(t_h, nsteps, s); d_T.upload(T_h, nsteps, s); d_E.upload(mat.Etab, TGRID_N, s);
+  d_kc.alloc(nsteps);
+  const AnandConst P = to_const(mat);
+  k_step_constants<<<(nsteps + 127) / 128, 128, 0, s>>>(P, d_E.p, nsteps, d_t.p, d_T.p, d_kc.p);
+  k_screen<<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_d, nsteps, d_wi.p, d_wt.p, d_Fth.p, d_kc.p, d_T.p, d_cycle.p,
+                                            d_phase.p, cycles, dW_d, dE_d, stab_d);
+  TM_CUDA_CHECK(cudaGetLastError());
+  TM_CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
+void anand_step_device(const tm_anand_material& mat, int npts, double* state_d, const double* eps_d, double T, double dt, double* sig_d,
+                       double* D_d, int commitFlag, cudaStream_t s) {
+  DBuf<double> d_E;
+  d_E.upload(mat.Etab, TGRID_N, s);
+  k_point_step<<<(npts + 127) / 128, 128, 0, s>>>(to_const(mat), d_E.p, npts, state_d, eps_d, T, dt, sig_d, D_d, commitFlag);
+  TM_CUDA_CHECK(cudaGetLastError());
+  TM_CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
+}  // namespace tmg

@@ -1,0 +1,576 @@
+// C-ABI of the B200 solve path (include/tmsolve.h): context management, the PCG loop with
+// the reference's warm start and rebuild policy, and the Anand entry points.
+//
+// The solve follows LinearSolver (src/core/10-solver.js:826-1043):
+//   solve            :933-994   scaling, preconditioner (re)build, warm start, stale-preconditioner
+//                               budget, rebuild on failure, rate bookkeeping, solution store
+//   _pcg             :1001-1042 PCG on the scaled system with constrained DOFs zeroed in r and z
+//   _warmStart       :885-915   Galerkin projection on <= 20 stored solutions
+//   _storeSolution   :917-926   two-pass Gram-Schmidt
+// The IC(0) fallback of the reference (:967-976, ICPC :741-800) has no device implementation:
+// a solve whose multigrid run fails after the rebuild returns TM_NOT_CONVERGED.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tm_internal.h"
+
+namespace tmg {
+
+thread_local std::string g_last_error;
+
+void fail(tm_status st, const std::string& msg) { throw Error{st, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error{TM_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+Context::~Context() {
+  for (auto* L : shells) delete L;
+  for (auto* b : basis) delete b;
+  if (stream) cudaStreamDestroy(stream);
+}
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+template <class F>
+tm_status guarded(F&& f) {
+  try {
+    f();
+    return TM_OK;
+  } catch (const Error& e) {
+    g_last_error = e.msg;
+    return e.status;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return TM_CUDA;
+  }
+}
+
+void require_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) fail(TM_NO_DEVICE, "no CUDA device: the solve path has no CPU fallback");
+  int dev = 0;
+  TM_CUDA_CHECK(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  TM_CUDA_CHECK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) fail(TM_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100: this library is built for B200 (sm_100a) only");
+}
+
+// numeric multigrid set-up for the current scaled operator (MultigridPC constructor / update)
+double build_pc(Context& c, bool mg) {
+  const double t0 = now_ms();
+  if (!mg) { c.pcReady = true; return now_ms() - t0; }
+  c.d_jitter.zero(c.stream);
+  launch_factor_columns(c);
+  launch_w01(c);
+  launch_galerkin01(c);
+  for (size_t l = 0; l < c.shells.size(); l++) {
+    ShellLevel& L = *c.shells[l];
+    if (L.coarsest) { launch_factor_coarsest(c, L); break; }
+    launch_factor_shell(c, L);
+    launch_galerkin_shell(c, (int)l);
+  }
+  int jit = 0;
+  TM_CUDA_CHECK(cudaMemcpyAsync(&jit, c.d_jitter.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  c.colJitter = jit;
+  c.pcReady = true;
+  c.needRebuild = false;
+  return now_ms() - t0;
+}
+
+void precondition(Context& c, bool mg, const double* r, double* z) {
+  if (mg) launch_vcycle(c, r, z, false);
+  else TM_CUDA_CHECK(cudaMemcpyAsync(z, r, 3 * (size_t)c.nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+}
+
+double dot_host(Context& c, const double* a, const double* b, size_t n) {
+  launch_dot(c, a, b, n, c.d_scalars.p + 15);
+  double v = 0;
+  TM_CUDA_CHECK(cudaMemcpyAsync(&v, c.d_scalars.p + 15, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  return v;
+}
+
+struct PcgResult {
+  int iters = 0;
+  double relres = 0, iters0 = 0;
+  bool converged = false;
+  bool nonfinite = false;
+};
+
+// _pcg (10-solver.js:1001-1042); device scalars: 0 rz, 1 pq, 2 alpha, 3 r.r, 4 rz2, 5 beta
+PcgResult pcg(Context& c, bool mg, const double* b, double* x, double tol, int maxit, double perDecade, const tm_solve_opts& o) {
+  const size_t n = 3 * (size_t)c.nn;
+  double* S = c.d_scalars.p;
+  PcgResult out;
+  launch_apply0(c, x, c.d_r.p, b);
+  launch_zero_constrained(c, c.d_r.p);
+  launch_zero_constrained(c, x);
+  const double bnorm = std::sqrt(dot_host(c, b, b, n));
+  double rnorm = std::sqrt(dot_host(c, c.d_r.p, c.d_r.p, n));
+  const double r0 = rnorm / bnorm;
+  out.iters0 = r0;
+  if (!std::isfinite(r0)) { out.nonfinite = true; out.relres = r0; return out; }
+  if (rnorm / bnorm < tol) { out.iters = 0; out.relres = rnorm / bnorm; out.converged = true; return out; }
+  if (perDecade > 0) maxit = std::min(maxit, std::max(30, (int)std::ceil(perDecade * std::log10(r0 / tol))));  // REBUILD_MIN_ITERS
+  precondition(c, mg, c.d_r.p, c.d_z.p);
+  launch_zero_constrained(c, c.d_z.p);
+  TM_CUDA_CHECK(cudaMemcpyAsync(c.d_p.p, c.d_z.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+  launch_dot(c, c.d_r.p, c.d_z.p, n, S + 0);
+  int it = 0;
+  double hs[4];
+  for (it = 1; it <= maxit; it++) {
+    launch_apply0(c, c.d_p.p, c.d_q.p, nullptr);
+    launch_dot(c, c.d_p.p, c.d_q.p, n, S + 1);
+    launch_div(c, S + 0, S + 1, S + 2, 1.0);
+    launch_axpy2(c, S + 2, c.d_p.p, x, c.d_q.p, c.d_r.p, n);
+    launch_finalize(c, S + 3);   // r.r from the partial sums of k_axpy2
+    TM_CUDA_CHECK(cudaMemcpyAsync(hs, S, 4 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    const double pq = hs[1];
+    if (!(pq > 0)) {
+      // the reference breaks before the update; undo it (x -= alpha p, r += alpha q)
+      double na = -hs[2];
+      TM_CUDA_CHECK(cudaMemcpyAsync(S + 2, &na, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+      launch_axpy2(c, S + 2, c.d_p.p, x, c.d_q.p, c.d_r.p, n);
+      if (!std::isfinite(pq)) out.nonfinite = true;
+      break;
+    }
+    rnorm = std::sqrt(hs[3]);
+    if (!std::isfinite(rnorm)) { out.nonfinite = true; break; }
+    if (o.progress && o.progress_every > 0 && it % o.progress_every == 0) o.progress(o.progress_user, it, rnorm / bnorm);
+    if (rnorm / bnorm < tol) { out.iters = it; out.relres = rnorm / bnorm; out.converged = true; return out; }
+    precondition(c, mg, c.d_r.p, c.d_z.p);
+    launch_zero_constrained(c, c.d_z.p);
+    launch_dot(c, c.d_r.p, c.d_z.p, n, S + 4);
+    launch_div(c, S + 4, S + 0, S + 5, 1.0);
+    TM_CUDA_CHECK(cudaMemcpyAsync(S + 0, S + 4, sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    launch_xpby(c, c.d_z.p, S + 5, c.d_p.p, n);
+  }
+  out.iters = std::min(it, maxit);
+  out.relres = rnorm / bnorm;
+  out.converged = false;
+  return out;
+}
+
+// Gauss-Jordan solve of the small warm-start system (solveDense / invDense, 01-util.js:110-142)
+bool solve_dense(const std::vector<double>& A, int n, const std::vector<double>& b, std::vector<double>& x) {
+  const int w = 2 * n;
+  std::vector<double> M((size_t)n * w, 0.0);
+  for (int i = 0; i < n; i++) {
+    for (int j = 0; j < n; j++) M[i * w + j] = A[i * n + j];
+    M[i * w + n + i] = 1;
+  }
+  for (int col = 0; col < n; col++) {
+    int p = col;
+    double best = std::fabs(M[col * w + col]);
+    for (int r = col + 1; r < n; r++) { const double v = std::fabs(M[r * w + col]); if (v > best) { best = v; p = r; } }
+    if (best == 0) return false;
+    if (p != col) for (int j = 0; j < w; j++) std::swap(M[col * w + j], M[p * w + j]);
+    const double inv = 1 / M[col * w + col];
+    for (int j = 0; j < w; j++) M[col * w + j] *= inv;
+    for (int r = 0; r < n; r++) {
+      if (r == col) continue;
+      const double f = M[r * w + col];
+      if (f == 0) continue;
+      for (int j = 0; j < w; j++) M[r * w + j] -= f * M[col * w + j];
+    }
+  }
+  x.assign(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    double s = 0;
+    for (int j = 0; j < n; j++) s += M[i * w + n + j] * b[j];
+    x[i] = s;
+  }
+  return true;
+}
+
+// _warmStart (10-solver.js:885-915) on the device
+void warm_start(Context& c, const double* fs, double* x) {
+  const size_t n = 3 * (size_t)c.nn;
+  const int m = (int)c.basis.size();
+  TM_CUDA_CHECK(cudaMemsetAsync(x, 0, n * sizeof(double), c.stream));
+  if (!m) return;
+  std::vector<DBuf<double>> KV(m);
+  for (int i = 0; i < m; i++) {
+    KV[i].alloc(n);
+    launch_scale_vec(c, c.basis[i]->p, c.d_s.p, c.d_tmp.p, true, n);
+    launch_apply0(c, c.d_tmp.p, c.d_tmp2.p, nullptr);
+    launch_scale_vec(c, c.d_tmp2.p, c.d_s.p, KV[i].p, true, n);
+  }
+  std::vector<double> A((size_t)m * m), b(m), cc;
+  launch_scale_vec(c, fs, c.d_s.p, c.d_tmp.p, true, n);
+  for (int i = 0; i < m; i++) {
+    b[i] = dot_host(c, c.basis[i]->p, c.d_tmp.p, n);
+    for (int j = 0; j < m; j++) A[i * m + j] = dot_host(c, c.basis[i]->p, KV[j].p, n);
+  }
+  for (int i = 0; i < m; i++)
+    for (int j = i + 1; j < m; j++) { const double v = 0.5 * (A[i * m + j] + A[j * m + i]); A[i * m + j] = A[j * m + i] = v; }
+  if (!solve_dense(A, m, b, cc)) return;
+  for (int i = 0; i < m; i++) if (!std::isfinite(cc[i])) return;
+  for (int i = 0; i < m; i++) launch_axpy(c, cc[i], c.basis[i]->p, x, n);
+  launch_scale_vec(c, x, c.d_s.p, x, true, n);
+}
+
+// _storeSolution (10-solver.js:917-926)
+void store_solution(Context& c, const double* u_dev, int warmMax) {
+  if (warmMax <= 0) return;
+  const size_t n = 3 * (size_t)c.nn;
+  auto* v = new DBuf<double>();
+  v->alloc(n);
+  TM_CUDA_CHECK(cudaMemcpyAsync(v->p, u_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+  for (int pass = 0; pass < 2; pass++)
+    for (auto* b : c.basis) launch_axpy(c, -dot_host(c, b->p, v->p, n), b->p, v->p, n);
+  const double nv = std::sqrt(dot_host(c, v->p, v->p, n));
+  const double nu = std::sqrt(dot_host(c, u_dev, u_dev, n));
+  if (!(nv > 1e-14 * (nu + 1e-300))) { delete v; return; }
+  launch_div_scalar(c, v->p, nv, n);
+  c.basis.push_back(v);
+  while ((int)c.basis.size() > warmMax) { delete c.basis.front(); c.basis.erase(c.basis.begin()); }
+}
+
+double pcg_rate(const PcgResult& r) { return r.iters / std::max(std::log10(r.iters0 / std::max(r.relres, 1e-300)), 0.5); }
+
+// LinearSolver.solve (10-solver.js:933-994) with f and u in device memory
+tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_solve_opts& o, tm_solve_info* info) {
+  const double t0 = now_ms();
+  if (!c.assembled) fail(TM_BAD_INPUT, "tm_solve before tm_assemble_step or tm_set_bcsr");
+  const size_t n = 3 * (size_t)c.nn;
+  const bool mg = o.precond == TM_PC_MG;
+  if (o.key != -1 && o.key != c.pcKey) c.needRebuild = true;
+  c.pcKey = o.key;
+  if (!c.scaled) {
+    launch_scale(c);
+    c.scaled = true;
+    c.pcReady = false;
+  }
+  launch_scale_rhs(c, f_dev, c.d_bs.p);
+  const double bnorm = std::sqrt(dot_host(c, c.d_bs.p, c.d_bs.p, n));
+  tm_solve_info in;
+  std::memset(&in, 0, sizeof(in));
+  in.levels = mg ? (int)c.shells.size() + 1 : 1;
+  if (!std::isfinite(bnorm)) fail(TM_NONFINITE, "non-finite load vector");
+  if (bnorm == 0) {
+    TM_CUDA_CHECK(cudaMemsetAsync(u_dev, 0, n * sizeof(double), c.stream));
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    in.converged = 1; in.ms = now_ms() - t0; in.warm = (int)c.basis.size();
+    if (info) *info = in;
+    return TM_OK;
+  }
+  bool rebuilt = false;
+  double pcMs = 0;
+  if (!c.pcReady || c.needRebuild) { pcMs = build_pc(c, mg); rebuilt = true; }
+  warm_start(c, c.d_bs.p, c.d_x.p);
+  PcgResult res = pcg(c, mg, c.d_bs.p, c.d_x.p, o.tol, o.maxit, rebuilt ? 0 : 2 * c.ratePerDecade, o);
+  int total = res.iters;
+  if (!res.converged && !rebuilt && !res.nonfinite) {
+    pcMs += build_pc(c, mg);
+    rebuilt = true;
+    res = pcg(c, mg, c.d_bs.p, c.d_x.p, o.tol, o.maxit, 0, o);
+    total += res.iters;
+  }
+  if (!res.converged) c.needRebuild = true;
+  if (res.converged) {
+    const bool known = c.ratePerDecade > 0 && !rebuilt;
+    if (known) { if (pcg_rate(res) > 2 * c.ratePerDecade) c.needRebuild = true; }
+    else c.ratePerDecade = std::log10(res.iters0 / std::max(res.relres, 1e-300)) >= 1 ? pcg_rate(res) : 0;
+  }
+  // u = x * s
+  launch_scale_vec(c, c.d_x.p, c.d_s.p, u_dev, false, n);
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  if (res.converged) store_solution(c, u_dev, o.warm);
+  in.iters = total; in.relres = res.relres; in.iters0 = res.iters0; in.converged = res.converged;
+  in.ms = now_ms() - t0; in.pc_ms = pcMs; in.rebuilt = rebuilt; in.warm = (int)c.basis.size(); in.fallback = 0;
+  in.jitter_count = c.colJitter;
+  in.status = res.nonfinite ? TM_NONFINITE : (res.converged ? TM_OK : TM_NOT_CONVERGED);
+  if (info) *info = in;
+  if (res.nonfinite) fail(TM_NONFINITE, "non-finite value in the PCG iteration");
+  return res.converged ? TM_OK : TM_NOT_CONVERGED;
+}
+
+void upload_mesh(Context& c) {
+  cudaStream_t s = c.stream;
+  c.d_nbr.upload(c.nbr, s);
+  c.d_slotMask.upload(c.slotMask, s);
+  c.d_nodeIJK.upload(c.nodeIJK, s);
+  c.d_cellElems.upload(c.cellElems, s);
+  c.d_eGroup.upload(c.eGroup, s);
+  c.d_groupStage.upload(c.groupStage, s);
+  c.d_eClass.upload(c.eClass, s);
+  c.d_colStart.upload(c.colStart, s);
+  c.d_eScale.upload(c.eScale, s);
+  c.d_clsPset.upload(c.clsPset, s);
+  c.d_clsH.upload(c.clsH, s);
+  c.d_constr.upload(c.constr, s);
+  const size_t n = 3 * (size_t)c.nn;
+  for (auto* b : {&c.d_f, &c.d_bs, &c.d_x, &c.d_r, &c.d_z, &c.d_p, &c.d_q, &c.d_tmp, &c.d_tmp2}) b->alloc(n);
+  c.d_partial.alloc(1024);
+  c.d_scalars.alloc(16);
+  c.d_jitter.alloc(1);
+}
+
+}  // namespace
+}  // namespace tmg
+
+using namespace tmg;
+
+extern "C" {
+
+void tm_default_solve_opts(tm_solve_opts* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->tol = 1e-8;
+  o->maxit = 2000;
+  o->warm = 20;
+  o->precond = TM_PC_MG;
+  o->precision = TM_PREC_FP64;
+  o->key = -1;
+}
+
+int32_t tm_last_error(char* buf, size_t len) {
+  if (buf && len) {
+    const size_t k = std::min(len - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), k);
+    buf[k] = 0;
+  }
+  return (int32_t)g_last_error.size();
+}
+
+tm_status tm_create(const tm_mesh* m, tm_ctx** out) {
+  return guarded([&] {
+    if (!m || !out) fail(TM_BAD_INPUT, "null argument");
+    *out = nullptr;
+    require_device();
+    if (m->nx < 2 || m->ny < 2 || m->nz < 2 || m->nn <= 0 || m->ne <= 0) fail(TM_BAD_INPUT, "empty mesh");
+    auto* c = new Context();
+    try {
+      TM_CUDA_CHECK(cudaGetDevice(&c->dev));
+      TM_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      c->nx = m->nx; c->ny = m->ny; c->nz = m->nz; c->nn = m->nn; c->ne = m->ne; c->npset = m->npset; c->ngroups = m->ngroups;
+      const size_t ncells = (size_t)(m->nx - 1) * (m->ny - 1) * (m->nz - 1);
+      c->xs.assign(m->xs, m->xs + m->nx); c->ys.assign(m->ys, m->ys + m->ny); c->zs.assign(m->zs, m->zs + m->nz);
+      c->coords.assign(m->coords, m->coords + 3 * (size_t)m->nn);
+      c->nodeId.assign(m->nodeId, m->nodeId + (size_t)m->nx * m->ny * m->nz);
+      c->conn.assign(m->conn, m->conn + 8 * (size_t)m->ne);
+      c->eIJK.assign(m->eIJK, m->eIJK + 3 * (size_t)m->ne);
+      c->colStart.assign(m->colStart, m->colStart + (size_t)m->nx * m->ny + 1);
+      c->cellElems.assign(m->cellElems, m->cellElems + 2 * ncells);
+      c->eGroup.assign(m->eGroup, m->eGroup + m->ne);
+      c->ePart.assign(m->ePart, m->ePart + m->ne);
+      c->eScale.assign(m->eScale, m->eScale + m->ne);
+      c->groupStage.assign(m->groupStage, m->groupStage + m->ngroups);
+      c->ePset.assign(m->ePset, m->ePset + m->ne);
+      c->constr.assign(m->constr, m->constr + m->nconstr);
+      if (m->nfeatureX > 0) c->featureX.assign(m->featureX, m->featureX + m->nfeatureX);
+      if (m->nfeatureY > 0) c->featureY.assign(m->featureY, m->featureY + m->nfeatureY);
+      // index validation (no device access is made with unchecked indices)
+      for (int v : c->conn) if (v < 0 || v >= c->nn) fail(TM_BAD_INPUT, "conn index out of range");
+      for (int v : c->nodeId) if (v >= c->nn) fail(TM_BAD_INPUT, "nodeId out of range");
+      for (int v : c->cellElems) if (v >= c->ne) fail(TM_BAD_INPUT, "cellElems out of range");
+      for (int v : c->eGroup) if (v < 0 || v >= c->ngroups) fail(TM_BAD_INPUT, "eGroup out of range");
+      for (int v : c->ePset) if (v < 0 || v >= c->npset) fail(TM_BAD_INPUT, "ePset out of range");
+      for (int v : c->constr) if (v < 0 || v >= 3 * c->nn) fail(TM_BAD_INPUT, "constraint DOF out of range");
+      if (c->colStart.back() != c->nn) fail(TM_BAD_INPUT, "colStart does not cover the nodes");
+      build_stencil(*c);
+      build_classes(*c);
+      upload_mesh(*c);
+      build_hierarchy(*c);
+      TM_CUDA_CHECK(cudaStreamSynchronize(c->stream));
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = reinterpret_cast<tm_ctx*>(c);
+  });
+}
+
+tm_status tm_destroy(tm_ctx* ctx) {
+  return guarded([&] { delete reinterpret_cast<Context*>(ctx); });
+}
+
+tm_status tm_assemble_step(tm_ctx* ctx, const tm_step* st, double* rhs_out) {
+  return guarded([&] {
+    if (!ctx || !st) fail(TM_BAD_INPUT, "null argument");
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    for (int p = 0; p < c.npset; p++) {
+      const double* src = st->psetLayered[p] ? st->W + 108 * (size_t)p : st->D + 36 * (size_t)p;
+      const int cnt = st->psetLayered[p] ? 108 : 36;
+      for (int q = 0; q < cnt; q++) if (!std::isfinite(src[q])) fail(TM_NONFINITE, "non-finite property-set stiffness");
+    }
+    launch_shape_matrices(c, *st);
+    launch_class_condense(c);
+    launch_assemble(c);
+    launch_constraints(c);
+    c.assembled = true;
+    c.scaled = false;
+    c.pcReady = false;
+    if (rhs_out) {
+      c.d_rhs.download(rhs_out, 3 * (size_t)c.nn, c.stream);
+    }
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, const double* val, const uint8_t* isConstrained) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    const int nn = c.nn;
+    std::vector<double> sv((size_t)NSLOT * 9 * nn, 0.0);
+    for (int i = 0; i < nn; i++) {
+      const int ii = c.nodeIJK[3 * (size_t)i], ij = c.nodeIJK[3 * (size_t)i + 1], ik = c.nodeIJK[3 * (size_t)i + 2];
+      for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+        const int j = col[k];
+        if (j < 0 || j >= nn) fail(TM_BAD_INPUT, "block column out of range");
+        const int di = c.nodeIJK[3 * (size_t)j] - ii, dj = c.nodeIJK[3 * (size_t)j + 1] - ij, dk = c.nodeIJK[3 * (size_t)j + 2] - ik;
+        if (std::abs(di) > 1 || std::abs(dj) > 1 || std::abs(dk) > 1) fail(TM_BAD_INPUT, "block outside the 27-point stencil of the mesh");
+        const int s = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
+        for (int v = 0; v < 9; v++) sv[((size_t)s * 9 + v) * nn + i] = val[9 * (size_t)k + v];
+      }
+    }
+    c.d_val.upload(sv, c.stream);
+    c.constr.clear();
+    for (int d = 0; d < 3 * nn; d++) if (isConstrained && isConstrained[d]) c.constr.push_back(d);
+    c.d_constr.upload(c.constr, c.stream);
+    c.assembled = true;
+    c.scaled = false;
+    c.pcReady = false;
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_get_bcsr(tm_ctx* ctx, int32_t* rowPtr, int32_t* col, double* val) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    const int nn = c.nn;
+    std::vector<double> sv((size_t)NSLOT * 9 * nn);
+    c.d_val.download(sv.data(), sv.size(), c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    int k = 0;
+    if (rowPtr) rowPtr[0] = 0;
+    for (int i = 0; i < nn; i++) {
+      for (int s = 0; s < NSLOT; s++) {
+        if (!(c.slotMask[i] >> s & 1)) continue;
+        if (col) col[k] = c.nbr[(size_t)s * nn + i];
+        if (val) for (int v = 0; v < 9; v++) val[9 * (size_t)k + v] = sv[((size_t)s * 9 + v) * nn + i];
+        k++;
+      }
+      if (rowPtr) rowPtr[i + 1] = k;
+    }
+  });
+}
+
+tm_status tm_sizes(tm_ctx* ctx, int64_t* out) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    long long nb = 0;
+    for (int i = 0; i < c.nn; i++) nb += __builtin_popcount((unsigned)c.slotMask[i]);
+    out[0] = c.nn; out[1] = c.ne; out[2] = nb; out[3] = 3LL * c.nn;
+    out[4] = (int64_t)c.shells.size() + 1;
+    out[5] = c.shells.empty() ? 0 : c.shells.back()->denseN;
+  });
+}
+
+tm_status tm_matvec_device(tm_ctx* ctx, const double* x, double* y) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!c.assembled) fail(TM_BAD_INPUT, "tm_matvec before an operator is loaded");
+    launch_apply0(c, x, y, nullptr);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_matvec(tm_ctx* ctx, const double* x, double* y) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!c.assembled) fail(TM_BAD_INPUT, "tm_matvec before an operator is loaded");
+    const size_t n = 3 * (size_t)c.nn;
+    c.d_tmp.upload(x, n, c.stream);
+    launch_apply0(c, c.d_tmp.p, c.d_tmp2.p, nullptr);
+    c.d_tmp2.download(y, n, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_solve_device(tm_ctx* ctx, const double* f_dev, double* u_dev, const tm_solve_opts* opts, tm_solve_info* info) {
+  tm_status st = TM_OK;
+  tm_status g = guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    tm_solve_opts o;
+    if (opts) o = *opts; else tm_default_solve_opts(&o);
+    st = solve_impl(c, f_dev, u_dev, o, info);
+  });
+  return g != TM_OK ? g : st;
+}
+
+tm_status tm_solve(tm_ctx* ctx, const double* f, double* u, const tm_solve_opts* opts, tm_solve_info* info) {
+  tm_status st = TM_OK;
+  tm_status g = guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    const size_t n = 3 * (size_t)c.nn;
+    for (size_t i = 0; i < n; i++) if (!std::isfinite(f[i])) fail(TM_NONFINITE, "non-finite load vector");
+    tm_solve_opts o;
+    if (opts) o = *opts; else tm_default_solve_opts(&o);
+    c.d_f.upload(f, n, c.stream);
+    DBuf<double> u_dev;
+    u_dev.alloc(n);
+    st = solve_impl(c, c.d_f.p, u_dev.p, o, info);
+    u_dev.download(u, n, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+  return g != TM_OK ? g : st;
+}
+
+tm_status tm_anand_screen_device(const tm_anand_material* mat, int32_t nsites, int32_t ntemps, const double* temps, const double* table_dev,
+                                 int32_t nsteps, const double* t, const double* T, const int32_t* cycle, const int32_t* phase, int32_t cycles,
+                                 double* dW, double* dE, double* stab) {
+  return guarded([&] {
+    require_device();
+    anand_screen_device(*mat, nsites, ntemps, temps, table_dev, nsteps, t, T, cycle, phase, cycles, dW, dE, stab, nullptr);
+  });
+}
+
+tm_status tm_anand_screen(const tm_anand_material* mat, int32_t nsites, int32_t ntemps, const double* temps, const double* table,
+                          int32_t nsteps, const double* t, const double* T, const int32_t* cycle, const int32_t* phase, int32_t cycles,
+                          double* dW, double* dE, double* stab) {
+  return guarded([&] {
+    require_device();
+    if (nsites <= 0) return;
+    DBuf<double> d_tab, d_dW, d_dE, d_st;
+    d_tab.upload(table, (size_t)nsites * ntemps * 6, nullptr);
+    d_dW.alloc(nsites); d_dE.alloc(nsites); d_st.alloc(nsites);
+    anand_screen_device(*mat, nsites, ntemps, temps, d_tab.p, nsteps, t, T, cycle, phase, cycles, d_dW.p, d_dE.p, d_st.p, nullptr);
+    d_dW.download(dW, nsites, nullptr); d_dE.download(dE, nsites, nullptr); d_st.download(stab, nsites, nullptr);
+    TM_CUDA_CHECK(cudaDeviceSynchronize());
+  });
+}
+
+tm_status tm_anand_step(const tm_anand_material* mat, int32_t npts, double* state, const double* eps, double T, double dt, double* sig,
+                        double* D, int32_t commit) {
+  return guarded([&] {
+    require_device();
+    if (npts <= 0) return;
+    DBuf<double> d_state, d_eps, d_sig, d_D;
+    d_state.upload(state, 12 * (size_t)npts, nullptr);
+    d_eps.upload(eps, 6 * (size_t)npts, nullptr);
+    d_sig.alloc(6 * (size_t)npts);
+    if (D) d_D.alloc(36 * (size_t)npts);
+    anand_step_device(*mat, npts, d_state.p, d_eps.p, T, dt, d_sig.p, D ? d_D.p : nullptr, commit, nullptr);
+    d_state.download(state, 12 * (size_t)npts, nullptr);
+    d_sig.download(sig, 6 * (size_t)npts, nullptr);
+    if (D) d_D.download(D, 36 * (size_t)npts, nullptr);
+    TM_CUDA_CHECK(cudaDeviceSynchronize());
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,208 @@
+// Internal declarations of the B200 solve-path library (not part of the C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tmsolve.h"
+
+namespace tmg {
+
+// ---- error handling --------------------------------------------------------------------
+struct Error {
+  tm_status status;
+  std::string msg;
+};
+[[noreturn]] void fail(tm_status st, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what);
+#define TM_CUDA_CHECK(x) ::tmg::cuda_check((x), #x)
+
+// ---- device buffers ---------------------------------------------------------------------
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    n = count;
+    if (count) TM_CUDA_CHECK(cudaMalloc((void**)&p, count * sizeof(T) + 16));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) TM_CUDA_CHECK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+  void zero(cudaStream_t s) {
+    if (n) TM_CUDA_CHECK(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  void download(T* h, size_t count, cudaStream_t s) const {
+    if (count) TM_CUDA_CHECK(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+};
+
+// number of stencil slots of a node: offsets (di, dj, dk) in {-1,0,1}^3, slot = (di+1)*9+(dj+1)*3+(dk+1);
+// ascending slot order is ascending neighbour node id (nodes are numbered z fastest, then y, then x)
+constexpr int NSLOT = 27;
+constexpr int SLOT_SELF = 13;
+constexpr int SLOT_DOWN = 12;  // (0, 0, -1): the node below in the same column
+
+// ---- multigrid shell level (6 DOFs per aggregate) ------------------------------------------
+struct ShellLevel {
+  int nx = 0, ny = 0, nn = 0;          // columns nx*ny, aggregates nn
+  std::vector<double> xs, ys;          // grid lines of the level's columns
+  std::vector<int> colStart;           // nx*ny+1
+  std::vector<double> zref, zlo, zhi;  // per aggregate
+  std::vector<int> keepX, keepY;
+  bool hasKeep = false;
+  // operator: block CSR with 6x6 blocks, pattern fixed by the mesh
+  std::vector<int> rowPtr, col, diag;
+  int nb = 0;
+  DBuf<int> d_rowPtr, d_col;
+  DBuf<double> d_val;                  // 36*nb
+  DBuf<float> d_val32;                 // mixed precision copy
+  // dense per-column factors
+  std::vector<long long> cfPtr;        // ncol+1 (offsets in doubles)
+  DBuf<long long> d_cfPtr;
+  DBuf<double> d_cf;
+  DBuf<int> d_colStart;
+  int maxm = 0;                        // largest column size in DOFs
+  // colours: columns with (i%2, j%2) = colour, as lists
+  DBuf<int> d_colorCols[4];
+  int colorCount[4] = {0, 0, 0, 0};
+  // prolongation from the next (coarser) level to this one: per aggregate f of this level
+  // parents idx with 6x6 weights (buildCoarseShellLevel, 10-solver.js:396-471)
+  std::vector<int> prolPtr, prolIdx;
+  std::vector<double> prolW;
+  DBuf<int> d_prolPtr, d_prolIdx;
+  DBuf<double> d_prolW;
+  // children of the next level's aggregates (transposeProl)
+  std::vector<int> chPtr, chIdx, chW;
+  DBuf<int> d_chPtr, d_chIdx, d_chW;
+  // Galerkin pattern bookkeeping for this level as a coarse level: max blocks per row
+  int maxRowBlocks = 0;
+  // work vectors
+  DBuf<double> d_b, d_x, d_res;
+  // coarsest level: banded factor and explicit inverse
+  bool coarsest = false;
+  int bandBw = 0, denseN = 0;
+  DBuf<double> d_band;                 // denseN*(bw+1)
+  DBuf<double> d_inv;                  // denseN*denseN
+  DBuf<float> d_inv32;
+};
+
+struct Context {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  // mesh (host copies of what the structure builders need)
+  int nx = 0, ny = 0, nz = 0, nn = 0, ne = 0, npset = 0, ngroups = 0;
+  std::vector<double> xs, ys, zs, coords;
+  std::vector<int> nodeId, conn, eIJK, colStart, cellElems, eGroup, ePset, groupStage, constr, featureX, featureY;
+  std::vector<int8_t> ePart;
+  std::vector<double> eScale;
+  std::vector<int> nodeIJK;            // 3*nn
+  // stencil structure
+  std::vector<int> nbr;                // 27*nn, slot-major
+  std::vector<int> slotMask;           // nn: bit s set when (n, nbr[s]) share an element (the block CSR pattern)
+  DBuf<int> d_nbr, d_slotMask, d_nodeIJK, d_cellElems, d_eGroup, d_groupStage, d_eClass, d_colStart, d_constr;
+  DBuf<double> d_eScale;
+  // element classes: (property set, hx, hy, hz)
+  int ncls = 0;
+  std::vector<int> eClass, clsPset;
+  std::vector<double> clsH;            // 3*ncls
+  DBuf<int> d_clsPset;
+  DBuf<double> d_clsH, d_clsKc, d_clsFc;   // 576, 24 per class
+  DBuf<int> d_clsBorn;
+  DBuf<double> d_psetM;                // 6*1089 per property set
+  DBuf<double> d_clsF33;               // 33 per class: uncondensed element thermal load (elementFth)
+  DBuf<int> d_psetLayered, d_psetBorn;
+  // operator (level 0): 243 values per node, slot-major ((s*9 + v)*nn + n)
+  DBuf<double> d_val;
+  DBuf<float> d_val32;
+  DBuf<double> d_rhs;
+  DBuf<uint8_t> d_isC;
+  std::vector<uint8_t> isC;
+  int stage = 0;
+  bool assembled = false, scaled = false;
+  // solver state
+  DBuf<double> d_s, d_f, d_bs, d_x, d_r, d_z, d_p, d_q, d_tmp, d_tmp2;
+  DBuf<double> d_partial, d_scalars;
+  DBuf<int> d_jitter;
+  // level 0 smoother and transfer
+  DBuf<double> d_F;                    // 18 per node (column block-tridiagonal factors)
+  DBuf<int> d_colorCols[4];
+  int colorCount[4] = {0, 0, 0, 0};
+  int maxColLen = 0;
+  std::vector<int> nodeAgg, aggStart;  // level 0 -> 1
+  std::vector<double> zp;              // z of node minus zref of its aggregate
+  DBuf<int> d_nodeAgg, d_aggStart;
+  DBuf<double> d_zp, d_W01;            // 18 per node
+  int maxRowBlocks1 = 0;
+  DBuf<double> d_res0;                 // level-0 residual
+  std::vector<ShellLevel*> shells;     // levels 1..L-1
+  bool hierarchy = false;
+  bool pcReady = false;
+  long long pcKey = -1;
+  bool needRebuild = true;
+  double ratePerDecade = 0;
+  int colJitter = 0, shellJitter = 0;
+  // warm start basis (unscaled space)
+  std::vector<DBuf<double>*> basis;
+  ~Context();
+};
+
+// ---- host structure builders (tm_hierarchy.cpp) ----------------------------------------------
+void build_stencil(Context& c);
+void build_classes(Context& c);
+void build_hierarchy(Context& c);
+
+// ---- set-up kernels (tm_setup.cu, compiled without fused multiply-add) -----------------------
+void launch_shape_matrices(Context& c, const tm_step& st);
+void launch_class_condense(Context& c);
+void launch_assemble(Context& c);
+void launch_constraints(Context& c);
+void launch_scale(Context& c);
+void launch_scale_rhs(Context& c, const double* f, double* bs);
+void launch_factor_columns(Context& c);
+void launch_w01(Context& c);
+void launch_galerkin01(Context& c);
+void launch_galerkin_shell(Context& c, int l);
+void launch_factor_shell(Context& c, ShellLevel& L);
+void launch_factor_coarsest(Context& c, ShellLevel& L);
+void launch_to_fp32(Context& c);
+
+// ---- solve kernels (tm_solve.cu) -------------------------------------------------------------
+void launch_apply0(Context& c, const double* x, double* y, const double* b);   // y = K x, or b - K x when b != nullptr
+void launch_apply0_f32(Context& c, const double* x, double* y, const double* b);
+void launch_dot(Context& c, const double* a, const double* b, size_t n, double* out_dev);
+void launch_axpy2(Context& c, const double* alpha_dev, const double* p, double* x, const double* q, double* r, size_t n);
+void launch_xpby(Context& c, const double* z, const double* beta_dev, double* p, size_t n);
+void launch_zero_constrained(Context& c, double* v);
+void launch_vcycle(Context& c, const double* r, double* z, bool mixed);
+void launch_div(Context& c, const double* num, const double* den, double* out, double sign);
+void launch_scale_vec(Context& c, const double* x, const double* s, double* y, bool divide, size_t n);
+void launch_finalize(Context& c, double* out_dev);                                  // sum of the last reduction partials
+void launch_axpy(Context& c, double alpha, const double* x, double* y, size_t n);   // y += alpha x
+void launch_div_scalar(Context& c, double* v, double d, size_t n);                  // v /= d
+
+// ---- Anand (tm_anand.cu) ---------------------------------------------------------------------
+void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps_h,
+                         const double* table_d, int nsteps, const double* t_h, const double* T_h,
+                         const int* cycle_h, const int* phase_h, int cycles, double* dW_d, double* dE_d,
+                         double* stab_d, cudaStream_t s);
+void anand_step_device(const tm_anand_material& mat, int npts, double* state_d, const double* eps_d,
+                       double T, double dt, double* sig_d, double* D_d, int commit, cudaStream_t s);
+
+}  // namespace tmg

@@ -1,0 +1,830 @@
+// Per-step numeric set-up on the GPU: element condensation, stencil assembly, constraints,
+// Jacobi scaling, column factors, Galerkin coarse operators and coarsest factor.
+//
+// This file is compiled with -fmad=false: every set-up quantity is then computed with the
+// same operations in the same order as the reference (JavaScript has no fused multiply-add),
+// so the assembled operator and the multigrid set-up are bit-identical to the FP64 oracle.
+//
+// Reference lines followed:
+//   shapeMatrices / elementK33Fast / elementFth   src/core/09-assembly.js:69-133 (UNIV :26-60)
+//   condense33 (cholDense 1e-14)                  src/core/07-element.js:88-121, 01-util.js:70-107
+//   assembleStep (element order summation)        src/core/09-assembly.js:392-424
+//   applyConstraints                              src/core/09-assembly.js:445-464
+//   LinearSolver._scale                           src/core/10-solver.js:852-866
+//   factorColumns / chol3                         src/core/10-solver.js:12-68
+//   shellWeights / galerkinProduct                src/core/10-solver.js:193-245, 337-353
+//   factorShellColumns                            src/core/10-solver.js:474-494
+//   factorCoarsest                                src/core/10-solver.js:562-600
+#include <cmath>
+#include <cstring>
+
+#include "tm_internal.h"
+
+namespace tmg {
+
+namespace {
+
+const int HEX_XI[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+const int HEX_ETA[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+const int HEX_ZETA[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+const int VOIGT[3][3] = {{0, 3, 5}, {3, 1, 4}, {5, 4, 2}};
+
+struct Univ {
+  double G[3 * 9 * 121], g[3 * 3 * 11], GH[9 * 121], gH[3 * 11];
+};
+
+// UNIV (09-assembly.js:26-60): natural-coordinate integrals of the 11 functions
+const Univ& univ() {
+  static Univ U;
+  static bool done = false;
+  if (done) return U;
+  std::memset(&U, 0, sizeof(U));
+  const double GP2 = 1 / std::sqrt(3.0);
+  const double simpson[3] = {1.0 / 3, 4.0 / 3, 1.0 / 3};
+  double d[3][11];
+  for (int j = 0; j < 3; j++) {
+    const double zeta = j - 1;
+    for (int ip = 0; ip < 4; ip++) {
+      const double xi = (ip & 1) ? GP2 : -GP2, eta = (ip & 2) ? GP2 : -GP2;
+      for (int a = 0; a < 8; a++) {
+        const double xa = HEX_XI[a], ya = HEX_ETA[a], za = HEX_ZETA[a];
+        d[0][a] = xa * (1 + ya * eta) * (1 + za * zeta) * 0.125;
+        d[1][a] = ya * (1 + xa * xi) * (1 + za * zeta) * 0.125;
+        d[2][a] = za * (1 + xa * xi) * (1 + ya * eta) * 0.125;
+      }
+      d[0][8] = -2 * xi; d[1][8] = 0; d[2][8] = 0;
+      d[0][9] = 0; d[1][9] = -2 * eta; d[2][9] = 0;
+      d[0][10] = 0; d[1][10] = 0; d[2][10] = -2 * zeta;
+      for (int r = 0; r < 3; r++)
+        for (int a = 0; a < 11; a++) {
+          U.g[(j * 3 + r) * 11 + a] += d[r][a];
+          U.gH[r * 11 + a] += simpson[j] * d[r][a];
+          for (int s = 0; s < 3; s++)
+            for (int b = 0; b < 11; b++) {
+              const double v = d[r][a] * d[s][b];
+              U.G[((j * 9 + r * 3 + s) * 121) + a * 11 + b] += v;
+              U.GH[(r * 3 + s) * 121 + a * 11 + b] += simpson[j] * v;
+            }
+        }
+    }
+  }
+  done = true;
+  return U;
+}
+
+// shapeMatrices (09-assembly.js:69-93): M (6 x 33 x 33) from D (36) or the layered weights W (108)
+void shape_matrices(const double* Wst, const double* D, double* M) {
+  const Univ& U = univ();
+  std::fill(M, M + 6 * 1089, 0.0);
+  const int nst = D ? 1 : 3;
+  const int PAIR[6][3] = {{0, 0, 0}, {1, 1, 1}, {2, 2, 2}, {3, 0, 1}, {4, 1, 2}, {5, 2, 0}};
+  for (int j = 0; j < nst; j++) {
+    const double* Wj = D ? D : Wst + 36 * j;
+    for (int pi = 0; pi < 6; pi++) {
+      const int m = PAIR[pi][0], r = PAIR[pi][1], s = PAIR[pi][2];
+      double* Mm = M + m * 1089;
+      const int rs[2][2] = {{r, s}, {s, r}};
+      const int nrs = r == s ? 1 : 2;
+      for (int t = 0; t < nrs; t++) {
+        const int rr = rs[t][0], ss = rs[t][1];
+        const double* Gb = D ? U.GH + (rr * 3 + ss) * 121 : U.G + (j * 9 + rr * 3 + ss) * 121;
+        for (int p = 0; p < 3; p++)
+          for (int q = 0; q < 3; q++) {
+            const double dv = Wj[VOIGT[p][rr] * 6 + VOIGT[q][ss]];
+            if (dv == 0) continue;
+            for (int a = 0; a < 11; a++) {
+              const int row = (3 * a + p) * 33 + q, ga = a * 11;
+              for (int b = 0; b < 11; b++) Mm[row + 3 * b] += dv * Gb[ga + b];
+            }
+          }
+      }
+    }
+  }
+}
+
+// elementFth (09-assembly.js:115-133)
+void element_fth(double hx, double hy, double hz, const double* Sst, const double* s0, double* f) {
+  const Univ& U = univ();
+  std::fill(f, f + 33, 0.0);
+  const double h[3] = {hx, hy, hz};
+  const double V8 = hx * hy * hz / 8;
+  const int nst = s0 ? 1 : 3;
+  for (int j = 0; j < nst; j++) {
+    const double* Sj = s0 ? s0 : Sst + 6 * j;
+    for (int r = 0; r < 3; r++) {
+      const double c = V8 * (2 / h[r]);
+      const double* gb = s0 ? U.gH + r * 11 : U.g + (j * 3 + r) * 11;
+      for (int p = 0; p < 3; p++) {
+        const double sv = c * Sj[VOIGT[p][r]];
+        if (sv == 0) continue;
+        for (int a = 0; a < 11; a++) f[3 * a + p] += sv * gb[a];
+      }
+    }
+  }
+}
+
+inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
+
+// ---- device helpers --------------------------------------------------------------------------
+// cholDense (01-util.js:70-91) on a 9x9 matrix, one thread
+__device__ void chol_dense9(double* A, double rel) {
+  double dmax = 0;
+  for (int i = 0; i < 9; i++) dmax = fmax(dmax, fabs(A[i * 9 + i]));
+  const double jitter = rel * (dmax != 0 ? dmax : 1);
+  for (int j = 0; j < 9; j++) {
+    const int rj = j * 9;
+    double d = A[rj + j];
+    for (int k = 0; k < j; k++) d -= A[rj + k] * A[rj + k];
+    if (!(d > jitter)) d = fmax(fabs(d), jitter);
+    const double ljj = sqrt(d);
+    A[rj + j] = ljj;
+    const double inv = 1 / ljj;
+    for (int i = j + 1; i < 9; i++) {
+      const int ri = i * 9;
+      double s = A[ri + j];
+      for (int k = 0; k < j; k++) s -= A[ri + k] * A[rj + k];
+      A[ri + j] = s * inv;
+    }
+  }
+}
+
+// cholSolveDense (01-util.js:94-107)
+__device__ void chol_solve9(const double* L, double* b) {
+  for (int i = 0; i < 9; i++) {
+    double s = b[i];
+    for (int k = 0; k < i; k++) s -= L[i * 9 + k] * b[k];
+    b[i] = s / L[i * 9 + i];
+  }
+  for (int i = 8; i >= 0; i--) {
+    double s = b[i];
+    for (int k = i + 1; k < 9; k++) s -= L[k * 9 + i] * b[k];
+    b[i] = s / L[i * 9 + i];
+  }
+}
+
+// ---- element classes: K33 = sum_m c_m M^m, condensation (one warp per class) ------------------
+__global__ void k_class_condense(int ncls, const int* __restrict__ clsPset, const double* __restrict__ clsH,
+                                 const double* __restrict__ psetM, const double* __restrict__ clsF33,
+                                 const int* __restrict__ clsBorn, double* __restrict__ clsKc, double* __restrict__ clsFc) {
+  extern __shared__ double sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cls = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (cls >= ncls) return;
+  double* K = sm + warp * 2048;        // 1089
+  double* Kc = K + 1089;               // 576
+  double* X = Kc + 576;                // 216
+  double* Kaa = X + 216;               // 81
+  double* xf = Kaa + 81;               // 9 (+ pad)
+  const double hx = clsH[3 * cls], hy = clsH[3 * cls + 1], hz = clsH[3 * cls + 2];
+  const double V8 = hx * hy * hz / 8;
+  const double c0 = V8 * 4 / (hx * hx), c1 = V8 * 4 / (hy * hy), c2 = V8 * 4 / (hz * hz);
+  const double c3 = V8 * 4 / (hx * hy), c4 = V8 * 4 / (hy * hz), c5 = V8 * 4 / (hz * hx);
+  const double* M = psetM + (size_t)clsPset[cls] * 6 * 1089;
+  // elementK33Fast (09-assembly.js:96-108): upper triangle, then mirrored
+  for (int o = lane; o < 1089; o += 32) {
+    const int i = o / 33, j = o % 33;
+    if (j >= i) K[o] = c0 * M[o] + c1 * M[1089 + o] + c2 * M[2178 + o] + c3 * M[3267 + o] + c4 * M[4356 + o] + c5 * M[5445 + o];
+  }
+  __syncwarp();
+  for (int o = lane; o < 1089; o += 32) {
+    const int i = o / 33, j = o % 33;
+    if (j < i) K[o] = K[j * 33 + i];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    for (int i = 0; i < 9; i++)
+      for (int j = 0; j < 9; j++) Kaa[i * 9 + j] = K[(24 + i) * 33 + 24 + j];
+    chol_dense9(Kaa, 1e-14);
+  }
+  __syncwarp();
+  if (lane < 24) {
+    double col[9];
+    for (int i = 0; i < 9; i++) col[i] = K[(24 + i) * 33 + lane];
+    chol_solve9(Kaa, col);
+    for (int i = 0; i < 9; i++) X[i * 24 + lane] = col[i];
+  }
+  __syncwarp();
+  for (int e = lane; e < 576; e += 32) {
+    const int i = e / 24, j = e % 24;
+    double s = K[i * 33 + j];
+    for (int q = 0; q < 9; q++) s -= K[i * 33 + 24 + q] * X[q * 24 + j];
+    Kc[e] = s;
+  }
+  __syncwarp();
+  // exact symmetry (07-element.js:108)
+  for (int e = lane; e < 576; e += 32) {
+    const int i = e / 24, j = e % 24;
+    if (j > i) {
+      const double v = 0.5 * (Kc[i * 24 + j] + Kc[j * 24 + i]);
+      Kc[i * 24 + j] = v;
+      Kc[j * 24 + i] = v;
+    }
+  }
+  __syncwarp();
+  double* outK = clsKc + (size_t)cls * 576;
+  for (int e = lane; e < 576; e += 32) outK[e] = Kc[e];
+  if (clsBorn[cls]) {
+    const double* f = clsF33 + (size_t)cls * 33;
+    if (lane == 0) {
+      for (int i = 0; i < 9; i++) xf[i] = f[24 + i];
+      chol_solve9(Kaa, xf);
+    }
+    __syncwarp();
+    if (lane < 24) {
+      double s = f[lane];
+      for (int q = 0; q < 9; q++) s -= K[lane * 33 + 24 + q] * xf[q];
+      clsFc[(size_t)cls * 24 + lane] = s;
+    }
+  } else if (lane < 24) {
+    clsFc[(size_t)cls * 24 + lane] = 0;
+  }
+}
+
+__device__ __forceinline__ int loc_index(int a, int b, int c) {
+  // local node order loc of 06-mesher.js:49 -> index
+  return c * 4 + (b ? (a ? 2 : 3) : (a ? 1 : 0));
+}
+
+// ---- stencil assembly: thread per (slot, node), contributions in element order -----------------
+__global__ void k_assemble(int nn, int nx, int ny, int nz, const int* __restrict__ nodeIJK, const int* __restrict__ nbr,
+                           const int* __restrict__ cellElems, const int* __restrict__ eClass, const double* __restrict__ eScale,
+                           const int* __restrict__ eGroup, const int* __restrict__ groupStage, int stage,
+                           const double* __restrict__ clsKc, double* __restrict__ val) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)NSLOT * nn) return;
+  const int s = (int)(t / nn), n = (int)(t % nn);
+  double acc[9];
+  for (int v = 0; v < 9; v++) acc[v] = 0;
+  const int m = nbr[t];
+  if (m >= 0) {
+    const int i = nodeIJK[3 * n], j = nodeIJK[3 * n + 1], k = nodeIJK[3 * n + 2];
+    const int di = s / 9 - 1, dj = (s / 3) % 3 - 1, dk = s % 3 - 1;
+    const int ncy = ny - 1, ncz = nz - 1;
+    const int ci0 = max(max(i, i + di) - 1, 0), ci1 = min(min(i, i + di), nx - 2);
+    const int cj0 = max(max(j, j + dj) - 1, 0), cj1 = min(min(j, j + dj), ny - 2);
+    const int ck0 = max(max(k, k + dk) - 1, 0), ck1 = min(min(k, k + dk), nz - 2);
+    for (int ci = ci0; ci <= ci1; ci++)
+      for (int cj = cj0; cj <= cj1; cj++)
+        for (int ck = ck0; ck <= ck1; ck++) {
+          const size_t cell = ((size_t)ci * ncy + cj) * ncz + ck;
+          const int a = loc_index(i - ci, j - cj, k - ck), b = loc_index(i + di - ci, j + dj - cj, k + dk - ck);
+          for (int q = 0; q < 2; q++) {
+            const int e = cellElems[2 * cell + q];
+            if (e < 0) continue;
+            const bool born = groupStage[eGroup[e]] <= stage;
+            const double scale = eScale[e] * (born ? 1.0 : 1e-6);
+            const double* Kc = clsKc + (size_t)eClass[e] * 576;
+            for (int p = 0; p < 3; p++) {
+              const int r = (3 * a + p) * 24 + 3 * b;
+              acc[3 * p] += scale * Kc[r];
+              acc[3 * p + 1] += scale * Kc[r + 1];
+              acc[3 * p + 2] += scale * Kc[r + 2];
+            }
+          }
+        }
+  }
+  for (int v = 0; v < 9; v++) val[((size_t)s * 9 + v) * nn + n] = acc[v];
+}
+
+// thermal load, thread per node (assembleStep's rhs, 09-assembly.js:417-420)
+__global__ void k_assemble_rhs(int nn, int nx, int ny, int nz, const int* __restrict__ nodeIJK, const int* __restrict__ cellElems,
+                               const int* __restrict__ eClass, const double* __restrict__ eScale, const int* __restrict__ eGroup,
+                               const int* __restrict__ groupStage, int stage, const int* __restrict__ clsBorn,
+                               const double* __restrict__ clsFc, double* __restrict__ rhs) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  const int i = nodeIJK[3 * n], j = nodeIJK[3 * n + 1], k = nodeIJK[3 * n + 2];
+  const int ncy = ny - 1, ncz = nz - 1;
+  double acc0 = 0, acc1 = 0, acc2 = 0;
+  for (int ci = max(i - 1, 0); ci <= min(i, nx - 2); ci++)
+    for (int cj = max(j - 1, 0); cj <= min(j, ny - 2); cj++)
+      for (int ck = max(k - 1, 0); ck <= min(k, nz - 2); ck++) {
+        const size_t cell = ((size_t)ci * ncy + cj) * ncz + ck;
+        const int a = loc_index(i - ci, j - cj, k - ck);
+        for (int q = 0; q < 2; q++) {
+          const int e = cellElems[2 * cell + q];
+          if (e < 0) continue;
+          const int cls = eClass[e];
+          if (!clsBorn[cls]) continue;
+          const bool born = groupStage[eGroup[e]] <= stage;
+          const double scale = eScale[e] * (born ? 1.0 : 1e-6);
+          const double* fc = clsFc + (size_t)cls * 24;
+          acc0 += scale * fc[3 * a];
+          acc1 += scale * fc[3 * a + 1];
+          acc2 += scale * fc[3 * a + 2];
+        }
+      }
+  rhs[3 * n] = acc0; rhs[3 * n + 1] = acc1; rhs[3 * n + 2] = acc2;
+}
+
+// applyConstraints (09-assembly.js:445-464), one thread walking the DOFs in order
+__global__ void k_constraints(int nn, int ncon, const int* __restrict__ dofs, const int* __restrict__ nbr,
+                              const int* __restrict__ slotMask, double* __restrict__ val, double* __restrict__ rhs,
+                              uint8_t* __restrict__ isC) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int t = 0; t < ncon; t++) isC[dofs[t]] = 1;
+  for (int t = 0; t < ncon; t++) {
+    const int d = dofs[t], i = d / 3, p = d % 3;
+    const int mask = slotMask[i];
+    for (int s = 0; s < NSLOT; s++) {
+      if (!(mask >> s & 1)) continue;
+      const int j = nbr[(size_t)s * nn + i];
+      for (int q = 0; q < 3; q++) {
+        double* v = val + ((size_t)s * 9 + 3 * p + q) * nn + i;
+        if (3 * j + q != d) *v = 0;
+        else if (*v == 0) *v = 1;
+      }
+      const int s2 = NSLOT - 1 - s;
+      for (int q = 0; q < 3; q++)
+        if (3 * j + q != d) val[((size_t)s2 * 9 + 3 * q + p) * nn + j] = 0;
+    }
+    if (rhs) rhs[d] = 0;
+  }
+}
+
+// _scale (10-solver.js:852-866)
+__global__ void k_scale_diag(int nn, const double* __restrict__ val, double* __restrict__ s) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  for (int p = 0; p < 3; p++) s[3 * n + p] = 1 / sqrt(fmax(val[((size_t)SLOT_SELF * 9 + 4 * p) * nn + n], 1e-300));
+}
+
+__global__ void k_scale_val(int nn, const int* __restrict__ nbr, const double* __restrict__ s, double* __restrict__ val) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)NSLOT * nn) return;
+  const int sl = (int)(t / nn), n = (int)(t % nn);
+  const int j = nbr[t];
+  if (j < 0) return;
+  for (int p = 0; p < 3; p++)
+    for (int q = 0; q < 3; q++) {
+      double* v = val + ((size_t)sl * 9 + 3 * p + q) * nn + n;
+      *v *= s[3 * n + p] * s[3 * j + q];
+    }
+}
+
+__global__ void k_mul(size_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ y) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a[i] * b[i];
+}
+
+// chol3 (10-solver.js:12-25)
+__device__ bool chol3(const double* A, double* L, double jit) {
+  const double a00 = A[0] + jit, a10 = A[3], a11 = A[4] + jit, a20 = A[6], a21 = A[7], a22 = A[8] + jit;
+  if (!(a00 > 0)) return false;
+  const double l00 = sqrt(a00);
+  const double l10 = a10 / l00, l20 = a20 / l00;
+  const double d11 = a11 - l10 * l10;
+  if (!(d11 > 0)) return false;
+  const double l11 = sqrt(d11);
+  const double l21 = (a21 - l20 * l10) / l11;
+  const double d22 = a22 - l20 * l20 - l21 * l21;
+  if (!(d22 > 0)) return false;
+  L[0] = l00; L[1] = 0; L[2] = 0; L[3] = l10; L[4] = l11; L[5] = 0; L[6] = l20; L[7] = l21; L[8] = sqrt(d22);
+  return true;
+}
+
+// factorColumns (10-solver.js:31-68), thread per column
+__global__ void k_factor_columns(int ncol, int nn, const int* __restrict__ colStart, const int* __restrict__ nbr,
+                                 const int* __restrict__ slotMask, const double* __restrict__ val, double* __restrict__ F,
+                                 int* __restrict__ jitterCount) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  int jitter = 0;
+  double D[9], tmp[9];
+  for (int n = colStart[c]; n < colStart[c + 1]; n++) {
+    for (int q = 0; q < 9; q++) D[q] = val[((size_t)SLOT_SELF * 9 + q) * nn + n];
+    double* Fn = F + 18 * (size_t)n;
+    const bool down = n > colStart[c] && (slotMask[n] >> SLOT_DOWN & 1) && nbr[(size_t)SLOT_DOWN * nn + n] == n - 1;
+    if (down) {
+      const double* Fp = F + 18 * (size_t)(n - 1);
+      for (int r = 0; r < 3; r++) {
+        const double b0 = val[((size_t)SLOT_DOWN * 9 + 3 * r) * nn + n], b1 = val[((size_t)SLOT_DOWN * 9 + 3 * r + 1) * nn + n],
+                     b2 = val[((size_t)SLOT_DOWN * 9 + 3 * r + 2) * nn + n];
+        const double y0 = b0 / Fp[0];
+        const double y1 = (b1 - Fp[3] * y0) / Fp[4];
+        const double y2 = (b2 - Fp[6] * y0 - Fp[7] * y1) / Fp[8];
+        tmp[3 * r] = y0; tmp[3 * r + 1] = y1; tmp[3 * r + 2] = y2;
+      }
+      for (int q = 0; q < 9; q++) Fn[9 + q] = tmp[q];
+      for (int r = 0; r < 3; r++)
+        for (int cc = 0; cc < 3; cc++)
+          D[3 * r + cc] -= tmp[3 * r] * tmp[3 * cc] + tmp[3 * r + 1] * tmp[3 * cc + 1] + tmp[3 * r + 2] * tmp[3 * cc + 2];
+    } else {
+      for (int q = 0; q < 9; q++) Fn[9 + q] = 0;
+    }
+    double jit = 0;
+    for (int t = 0; t < 8 && !chol3(D, Fn, jit); t++) {
+      jit = jit != 0 ? jit * 10 : 1e-10 * fmax(fmax(fabs(D[0]), fabs(D[4])), fmax(fabs(D[8]), 1e-300));
+      jitter++;
+    }
+  }
+  if (jitter) atomicAdd(jitterCount, jitter);
+}
+
+// shellWeights (10-solver.js:337-353): 3x6 weights per node with the scaling folded in
+__global__ void k_w01(int nn, const double* __restrict__ s, const double* __restrict__ zp, double* __restrict__ W) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  double* w = W + 18 * (size_t)n;
+  for (int q = 0; q < 18; q++) w[q] = 0;
+  const double z = zp[n];
+  w[0] = 1 / s[3 * n]; w[4] = z / s[3 * n];
+  w[7] = 1 / s[3 * n + 1]; w[9] = -z / s[3 * n + 1];
+  w[14] = 1 / s[3 * n + 2]; w[17] = z / s[3 * n + 2];
+}
+
+__device__ __forceinline__ int find_col(const int* cols, int n, int J) {
+  int lo = 0, hi = n - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = cols[mid];
+    if (v == J) return mid;
+    if (v < J) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+// galerkinProduct 0 -> 1 (10-solver.js:193-245), warp per coarse row, same summation order
+__global__ void k_galerkin01(int na, int nn, const int* __restrict__ aggStart, const int* __restrict__ nodeAgg,
+                             const int* __restrict__ nbr, const int* __restrict__ slotMask, const double* __restrict__ val,
+                             const double* __restrict__ W, const int* __restrict__ rowPtr, const int* __restrict__ col,
+                             int maxRow, double* __restrict__ out) {
+  extern __shared__ double sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (I >= na) return;
+  double* acc = sm + (size_t)warp * maxRow * 36;
+  const int r0 = rowPtr[I], nJ = rowPtr[I + 1] - r0;
+  for (int e = lane; e < nJ * 36; e += 32) acc[e] = 0;
+  __syncwarp();
+  const int e0 = lane, e1 = lane + 32;
+  const int rA = e0 / 6, cA = e0 % 6, rB = e1 / 6, cB = e1 % 6;
+  for (int i = aggStart[I]; i < aggStart[I + 1]; i++) {
+    const int mask = slotMask[i];
+    const double* Wi = W + 18 * (size_t)i;
+    for (int s = 0; s < NSLOT; s++) {
+      if (!(mask >> s & 1)) continue;
+      const int j = nbr[(size_t)s * nn + i];
+      const int loc = find_col(col + r0, nJ, nodeAgg[j]);
+      if (loc < 0) continue;   // cannot happen for a pattern built from the same mesh; never write outside acc
+      const double* Wj = W + 18 * (size_t)j;
+      double kv[9];
+      for (int v = 0; v < 9; v++) kv[v] = val[((size_t)s * 9 + v) * nn + i];
+      // T (3x6) = K_ij W_j ; acc += W_i^T T
+      {
+        double T[3];
+        for (int r = 0; r < 3; r++) {
+          double sum = 0;
+          for (int t = 0; t < 3; t++) sum += kv[r * 3 + t] * Wj[t * 6 + cA];
+          T[r] = sum;
+        }
+        double sum = 0;
+        for (int t = 0; t < 3; t++) sum += Wi[t * 6 + rA] * T[t];
+        acc[loc * 36 + e0] += sum;
+      }
+      if (e1 < 36) {
+        double T[3];
+        for (int r = 0; r < 3; r++) {
+          double sum = 0;
+          for (int t = 0; t < 3; t++) sum += kv[r * 3 + t] * Wj[t * 6 + cB];
+          T[r] = sum;
+        }
+        double sum = 0;
+        for (int t = 0; t < 3; t++) sum += Wi[t * 6 + rB] * T[t];
+        acc[loc * 36 + e1] += sum;
+      }
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < nJ * 36; e += 32) out[(size_t)r0 * 36 + e] = acc[e];
+}
+
+// galerkinProduct between shell levels (6x6 weights), warp per coarse row
+__global__ void k_galerkin_shell(int nnc, const int* __restrict__ chPtr, const int* __restrict__ chIdx, const int* __restrict__ chW,
+                                 const int* __restrict__ fRowPtr, const int* __restrict__ fCol, const double* __restrict__ fVal,
+                                 const int* __restrict__ prolPtr, const int* __restrict__ prolIdx, const double* __restrict__ W,
+                                 const int* __restrict__ rowPtr, const int* __restrict__ col, int maxRow, double* __restrict__ out) {
+  extern __shared__ double sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (I >= nnc) return;
+  double* acc = sm + (size_t)warp * maxRow * 36;
+  const int r0 = rowPtr[I], nJ = rowPtr[I + 1] - r0;
+  for (int e = lane; e < nJ * 36; e += 32) acc[e] = 0;
+  __syncwarp();
+  const int e0 = lane, e1 = lane + 32;
+  const int rA = e0 / 6, cA = e0 % 6, rB = e1 / 6, cB = e1 % 6;
+  for (int q = chPtr[I]; q < chPtr[I + 1]; q++) {
+    const int f = chIdx[q];
+    const double* Wi = W + 36 * (size_t)chW[q];
+    for (int k = fRowPtr[f]; k < fRowPtr[f + 1]; k++) {
+      const int g = fCol[k];
+      const double* Kv = fVal + 36 * (size_t)k;
+      for (int p = prolPtr[g]; p < prolPtr[g + 1]; p++) {
+        const int loc = find_col(col + r0, nJ, prolIdx[p]);
+        if (loc < 0) continue;
+        const double* Wj = W + 36 * (size_t)p;
+        {
+          double T[6];
+          for (int r = 0; r < 6; r++) {
+            double sum = 0;
+            for (int t = 0; t < 6; t++) sum += Kv[r * 6 + t] * Wj[t * 6 + cA];
+            T[r] = sum;
+          }
+          double sum = 0;
+          for (int t = 0; t < 6; t++) sum += Wi[t * 6 + rA] * T[t];
+          acc[loc * 36 + e0] += sum;
+        }
+        if (e1 < 36) {
+          double T[6];
+          for (int r = 0; r < 6; r++) {
+            double sum = 0;
+            for (int t = 0; t < 6; t++) sum += Kv[r * 6 + t] * Wj[t * 6 + cB];
+            T[r] = sum;
+          }
+          double sum = 0;
+          for (int t = 0; t < 6; t++) sum += Wi[t * 6 + rB] * T[t];
+          acc[loc * 36 + e1] += sum;
+        }
+        __syncwarp();
+      }
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < nJ * 36; e += 32) out[(size_t)r0 * 36 + e] = acc[e];
+}
+
+// factorShellColumns (10-solver.js:474-494) with cholDense (rel 1e-12), warp per column
+__global__ void k_factor_shell(int ncol, const int* __restrict__ colStart, const int* __restrict__ rowPtr, const int* __restrict__ col,
+                               const double* __restrict__ val, const long long* __restrict__ cfPtr, double* __restrict__ cf,
+                               int* __restrict__ jitterCount) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (c >= ncol) return;
+  const int n0 = colStart[c], n1 = colStart[c + 1], m = (n1 - n0) * 6;
+  if (!m) return;
+  double* A = cf + cfPtr[c];
+  for (int e = lane; e < m * m; e += 32) A[e] = 0;
+  __syncwarp();
+  for (int n = n0; n < n1; n++)
+    for (int k = rowPtr[n]; k < rowPtr[n + 1]; k++) {
+      const int j = col[k];
+      if (j < n0 || j >= n1) continue;
+      for (int e = lane; e < 36; e += 32) {
+        const int p = e / 6, q = e % 6;
+        A[((n - n0) * 6 + p) * m + (j - n0) * 6 + q] = val[36 * (size_t)k + e];
+      }
+    }
+  __syncwarp();
+  double dmax = 0;
+  for (int i = 0; i < m; i++) dmax = fmax(dmax, fabs(A[i * m + i]));
+  const double jitter = 1e-12 * (dmax != 0 ? dmax : 1);
+  int fixes = 0;
+  for (int j = 0; j < m; j++) {
+    const int rj = j * m;
+    double inv = 0;
+    if (lane == 0) {
+      double d = A[rj + j];
+      for (int k = 0; k < j; k++) d -= A[rj + k] * A[rj + k];
+      if (!(d > jitter)) { d = fmax(fabs(d), jitter); fixes++; }
+      const double ljj = sqrt(d);
+      A[rj + j] = ljj;
+      inv = 1 / ljj;
+    }
+    inv = __shfl_sync(0xffffffffu, inv, 0);
+    __syncwarp();
+    for (int i = j + 1 + lane; i < m; i += 32) {
+      const int ri = i * m;
+      double s = A[ri + j];
+      for (int k = 0; k < j; k++) s -= A[ri + k] * A[rj + k];
+      A[ri + j] = s * inv;
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && fixes) atomicAdd(jitterCount, fixes);
+}
+
+// factorCoarsest (10-solver.js:562-600): banded Cholesky in one block
+__global__ void k_factor_coarsest(int nnb, const int* __restrict__ rowPtr, const int* __restrict__ col, const double* __restrict__ val,
+                                  int n, int bw, double* __restrict__ A, int* __restrict__ jitterCount) {
+  const int w = bw + 1;
+  __shared__ double s_inv;
+  __shared__ double s_red[1024];
+  for (size_t e = threadIdx.x; e < (size_t)n * w; e += blockDim.x) A[e] = 0;
+  __syncthreads();
+  for (int i = 0; i < nnb; i++)
+    for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+      const int j = col[k];
+      if (j > i) continue;
+      for (int e = threadIdx.x; e < 36; e += blockDim.x) {
+        const int p = e / 6, q = e % 6;
+        const int r = 6 * i + p, cc = 6 * j + q;
+        if (cc <= r) A[(size_t)r * w + (cc - r + bw)] = val[36 * (size_t)k + e];
+      }
+    }
+  __syncthreads();
+  double dm = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dm = fmax(dm, fabs(A[(size_t)i * w + bw]));
+  s_red[threadIdx.x] = dm;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) s_red[threadIdx.x] = fmax(s_red[threadIdx.x], s_red[threadIdx.x + st]);
+    __syncthreads();
+  }
+  const double dmax = s_red[0];
+  const double jitter = 1e-12 * (dmax != 0 ? dmax : 1);
+  int fixes = 0;
+  for (int j = 0; j < n; j++) {
+    const int k0 = max(0, j - bw);
+    if (threadIdx.x == 0) {
+      double d = A[(size_t)j * w + bw];
+      for (int k = k0; k < j; k++) { const double l = A[(size_t)j * w + (k - j + bw)]; d -= l * l; }
+      if (!(d > jitter)) { d = fmax(fabs(d), jitter); fixes++; }
+      const double ljj = sqrt(d);
+      A[(size_t)j * w + bw] = ljj;
+      s_inv = 1 / ljj;
+    }
+    __syncthreads();
+    const double inv = s_inv;
+    const int iend = min(n, j + bw + 1);
+    for (int i = j + 1 + threadIdx.x; i < iend; i += blockDim.x) {
+      double sum = A[(size_t)i * w + (j - i + bw)];
+      const int kk0 = max(k0, i - bw);
+      for (int k = kk0; k < j; k++) sum -= A[(size_t)i * w + (k - i + bw)] * A[(size_t)j * w + (k - j + bw)];
+      A[(size_t)i * w + (j - i + bw)] = sum * inv;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && fixes) atomicAdd(jitterCount, fixes);
+}
+
+// explicit inverse of the coarsest operator from its banded factor (solveCoarsest on unit vectors)
+__global__ void k_coarsest_inverse(int n, int bw, const double* __restrict__ A, double* __restrict__ inv) {
+  const int cidx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cidx >= n) return;
+  const int w = bw + 1;
+  // forward: L y = e_c  (y_i = 0 for i < c)
+  for (int i = 0; i < n; i++) inv[(size_t)i * n + cidx] = 0;
+  for (int i = cidx; i < n; i++) {
+    double sum = i == cidx ? 1.0 : 0.0;
+    const int k0 = max(cidx, i - bw);
+    for (int k = k0; k < i; k++) sum -= A[(size_t)i * w + (k - i + bw)] * inv[(size_t)k * n + cidx];
+    inv[(size_t)i * n + cidx] = sum / A[(size_t)i * w + bw];
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    double sum = inv[(size_t)i * n + cidx];
+    const int kend = min(n, i + bw + 1);
+    for (int k = i + 1; k < kend; k++) sum -= A[(size_t)k * w + (i - k + bw)] * inv[(size_t)k * n + cidx];
+    inv[(size_t)i * n + cidx] = sum / A[(size_t)i * w + bw];
+  }
+}
+
+__global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+}  // namespace
+
+void launch_shape_matrices(Context& c, const tm_step& st) {
+  std::vector<double> M((size_t)c.npset * 6 * 1089);
+  std::vector<int> lay(c.npset), born(c.npset);
+  for (int p = 0; p < c.npset; p++) {
+    lay[p] = st.psetLayered[p] != 0;
+    born[p] = st.psetBorn[p] != 0;
+    shape_matrices(lay[p] ? st.W + 108 * (size_t)p : nullptr, lay[p] ? nullptr : st.D + 36 * (size_t)p, M.data() + (size_t)p * 6 * 1089);
+  }
+  // element thermal loads per class (elementFth) on the host: a few hundred flops per class
+  std::vector<double> f33((size_t)c.ncls * 33, 0.0);
+  std::vector<int> clsBorn(c.ncls);
+  for (int k = 0; k < c.ncls; k++) {
+    const int p = c.clsPset[k];
+    clsBorn[k] = born[p];
+    if (!born[p]) continue;
+    element_fth(c.clsH[3 * k], c.clsH[3 * k + 1], c.clsH[3 * k + 2], lay[p] ? st.V + 18 * (size_t)p : nullptr,
+                lay[p] ? nullptr : st.s0 + 6 * (size_t)p, f33.data() + 33 * (size_t)k);
+  }
+  c.d_psetM.upload(M, c.stream);
+  c.d_clsF33.upload(f33, c.stream);
+  c.d_clsBorn.upload(clsBorn, c.stream);
+  c.stage = st.stage;
+}
+
+void launch_class_condense(Context& c) {
+  c.d_clsKc.alloc((size_t)c.ncls * 576);
+  c.d_clsFc.alloc((size_t)c.ncls * 24);
+  const int warps = 2;
+  const size_t smem = (size_t)warps * 2048 * sizeof(double);
+  TM_CUDA_CHECK(cudaFuncSetAttribute(k_class_condense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_class_condense<<<grid_for(c.ncls, warps), 32 * warps, smem, c.stream>>>(c.ncls, c.d_clsPset.p, c.d_clsH.p, c.d_psetM.p, c.d_clsF33.p,
+                                                                          c.d_clsBorn.p, c.d_clsKc.p, c.d_clsFc.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_assemble(Context& c) {
+  const size_t tot = (size_t)NSLOT * c.nn;
+  c.d_val.alloc(tot * 9);
+  c.d_rhs.alloc(3 * (size_t)c.nn);
+  k_assemble<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_nodeIJK.p, c.d_nbr.p, c.d_cellElems.p, c.d_eClass.p,
+                                                      c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsKc.p, c.d_val.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+  k_assemble_rhs<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_nodeIJK.p, c.d_cellElems.p, c.d_eClass.p,
+                                                           c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsBorn.p,
+                                                           c.d_clsFc.p, c.d_rhs.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_constraints(Context& c) {
+  c.d_isC.alloc(3 * (size_t)c.nn);
+  c.d_isC.zero(c.stream);
+  DBuf<int> d;
+  d.upload(c.constr, c.stream);
+  k_constraints<<<1, 1, 0, c.stream>>>(c.nn, (int)c.constr.size(), d.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  c.isC.assign(3 * (size_t)c.nn, 0);
+  for (int d0 : c.constr) c.isC[d0] = 1;
+}
+
+void launch_scale(Context& c) {
+  c.d_s.alloc(3 * (size_t)c.nn);
+  k_scale_diag<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.d_val.p, c.d_s.p);
+  const size_t tot = (size_t)NSLOT * c.nn;
+  k_scale_val<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_s.p, c.d_val.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_scale_rhs(Context& c, const double* f, double* bs) {
+  const size_t n = 3 * (size_t)c.nn;
+  k_mul<<<grid_for(n, 256), 256, 0, c.stream>>>(n, f, c.d_s.p, bs);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_factor_columns(Context& c) {
+  const int ncol = c.nx * c.ny;
+  c.d_F.zero(c.stream);
+  k_factor_columns<<<grid_for(ncol, 128), 128, 0, c.stream>>>(ncol, c.nn, c.d_colStart.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p,
+                                                             c.d_F.p, c.d_jitter.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_w01(Context& c) {
+  k_w01<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.d_s.p, c.d_zp.p, c.d_W01.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_galerkin01(Context& c) {
+  ShellLevel& L1 = *c.shells[0];
+  const int warps = 4;
+  const size_t smem = (size_t)warps * L1.maxRowBlocks * 36 * sizeof(double);
+  TM_CUDA_CHECK(cudaFuncSetAttribute(k_galerkin01, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_galerkin01<<<grid_for(L1.nn, warps), 32 * warps, smem, c.stream>>>(L1.nn, c.nn, c.d_aggStart.p, c.d_nodeAgg.p, c.d_nbr.p, c.d_slotMask.p,
+                                                                      c.d_val.p, c.d_W01.p, L1.d_rowPtr.p, L1.d_col.p, L1.maxRowBlocks,
+                                                                      L1.d_val.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_galerkin_shell(Context& c, int l) {
+  ShellLevel& F = *c.shells[l];
+  ShellLevel& C = *c.shells[l + 1];
+  const int warps = 4;
+  const size_t smem = (size_t)warps * C.maxRowBlocks * 36 * sizeof(double);
+  TM_CUDA_CHECK(cudaFuncSetAttribute(k_galerkin_shell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_galerkin_shell<<<grid_for(C.nn, warps), 32 * warps, smem, c.stream>>>(C.nn, F.d_chPtr.p, F.d_chIdx.p, F.d_chW.p, F.d_rowPtr.p, F.d_col.p,
+                                                                         F.d_val.p, F.d_prolPtr.p, F.d_prolIdx.p, F.d_prolW.p, C.d_rowPtr.p,
+                                                                         C.d_col.p, C.maxRowBlocks, C.d_val.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_factor_shell(Context& c, ShellLevel& L) {
+  const int ncol = L.nx * L.ny;
+  const int warps = 4;
+  k_factor_shell<<<grid_for(ncol, warps), 32 * warps, 0, c.stream>>>(ncol, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_cfPtr.p,
+                                                                    L.d_cf.p, c.d_jitter.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_factor_coarsest(Context& c, ShellLevel& L) {
+  k_factor_coarsest<<<1, 1024, 0, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+  k_coarsest_inverse<<<grid_for(L.denseN, 64), 64, 0, c.stream>>>(L.denseN, L.bandBw, L.d_band.p, L.d_inv.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_to_fp32(Context& c) {
+  const size_t n0 = c.d_val.n;
+  c.d_val32.alloc(n0);
+  k_to_f32<<<grid_for(n0, 256), 256, 0, c.stream>>>(n0, c.d_val.p, c.d_val32.p);
+  for (auto* L : c.shells) {
+    L->d_val32.alloc(L->d_val.n);
+    k_to_f32<<<grid_for(L->d_val.n, 256), 256, 0, c.stream>>>(L->d_val.n, L->d_val.p, L->d_val32.p);
+    if (L->coarsest) {
+      L->d_inv32.alloc(L->d_inv.n);
+      k_to_f32<<<grid_for(L->d_inv.n, 256), 256, 0, c.stream>>>(L->d_inv.n, L->d_inv.p, L->d_inv32.p);
+    }
+  }
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace tmg

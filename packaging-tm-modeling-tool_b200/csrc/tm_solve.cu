@@ -1,0 +1,463 @@
+// Solve-phase kernels: stencil apply, PCG vector work with deterministic reductions, and
+// the multigrid V-cycle (MultigridPC._cycleOnce, src/core/10-solver.js:687-712).
+//
+// Differences from the reference, by design:
+//  * the column Gauss-Seidel sweeps (columnSweep, 10-solver.js:512-555) visit the columns in
+//    four colours (i mod 2, j mod 2) instead of lexicographically; columns of one colour do not
+//    couple, so each colour is one parallel launch. Pre-smoothing runs colours 0..3, post-
+//    smoothing 3..0, which keeps the V-cycle symmetric as the reference's forward/backward pair;
+//  * the coarsest level is applied with the explicit inverse of its banded Cholesky factor;
+//  * dot products are two-pass reductions in a fixed order (deterministic run to run).
+#include <cuda_runtime.h>
+
+#include "tm_internal.h"
+
+namespace tmg {
+
+namespace {
+
+constexpr int RED_BLOCKS = 592;   // 4 x 148 SMs
+constexpr int RED_THREADS = 256;
+
+inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
+
+// ---- level-0 stencil apply: y = K x or y = b - K x, thread per node --------------------------
+template <class T, class V>
+__global__ void k_apply0(int nn, const int* __restrict__ nbr, const T* __restrict__ val, const V* __restrict__ x,
+                         V* __restrict__ y, const V* __restrict__ b) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  T y0 = 0, y1 = 0, y2 = 0;
+#pragma unroll 3
+  for (int s = 0; s < NSLOT; s++) {
+    const int j = nbr[(size_t)s * nn + n];
+    if (j < 0) continue;
+    const T x0 = (T)x[3 * j], x1 = (T)x[3 * j + 1], x2 = (T)x[3 * j + 2];
+    const T* v = val + (size_t)s * 9 * nn + n;
+    y0 += v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
+    y1 += v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
+    y2 += v[6 * (size_t)nn] * x0 + v[7 * (size_t)nn] * x1 + v[8 * (size_t)nn] * x2;
+  }
+  if (b) {
+    y[3 * n] = b[3 * n] - (V)y0; y[3 * n + 1] = b[3 * n + 1] - (V)y1; y[3 * n + 2] = b[3 * n + 2] - (V)y2;
+  } else {
+    y[3 * n] = (V)y0; y[3 * n + 1] = (V)y1; y[3 * n + 2] = (V)y2;
+  }
+}
+
+// ---- deterministic reductions ----------------------------------------------------------------
+template <class T>
+__device__ double block_sum(double v) {
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  v = 0;
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+template <class T>
+__global__ void k_dot_partial(size_t n, const T* __restrict__ a, const T* __restrict__ b, double* __restrict__ partial) {
+  double s = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) s += (double)a[i] * (double)b[i];
+  s = block_sum<T>(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void k_reduce_final(int np, const double* __restrict__ partial, double* __restrict__ out) {
+  double s = 0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[i];
+  s = block_sum<double>(s);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// x += alpha p ; r -= alpha q ; partial sums of r.r
+template <class T>
+__global__ void k_axpy2(size_t n, const double* __restrict__ alpha, const T* __restrict__ p, T* __restrict__ x, const T* __restrict__ q,
+                        T* __restrict__ r, double* __restrict__ partial) {
+  const T a = (T)*alpha;
+  double s = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] += a * p[i];
+    const T ri = r[i] - a * q[i];
+    r[i] = ri;
+    s += (double)ri * (double)ri;
+  }
+  s = block_sum<T>(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+template <class T>
+__global__ void k_xpby(size_t n, const T* __restrict__ z, const double* __restrict__ beta, T* __restrict__ p) {
+  const T bt = (T)*beta;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = z[i] + bt * p[i];
+}
+
+__global__ void k_div(const double* __restrict__ num, const double* __restrict__ den, double* __restrict__ out, double sign) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = sign * (*num / *den);
+}
+
+template <class T>
+__global__ void k_zero_list(int n, const int* __restrict__ idx, T* __restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[idx[i]] = 0;
+}
+
+template <class T>
+__global__ void k_scale_vec(size_t n, const T* __restrict__ x, const double* __restrict__ s, T* __restrict__ y, int divide) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = divide ? (T)(x[i] / s[i]) : (T)(x[i] * s[i]);
+}
+
+// ---- level-0 column smoother: warp per column of one colour ------------------------------------
+// residual rows of the column (27-point stencil, coalesced along the column's contiguous nodes),
+// block-tridiagonal forward/backward solve with the column factors staged in shared memory
+// (solveColumn, 10-solver.js:71-104), then x += dx
+template <class T>
+__global__ void k_sweep_solid(int ncolc, const int* __restrict__ cols, const int* __restrict__ colStart, int nn,
+                              const int* __restrict__ nbr, const T* __restrict__ val, const T* __restrict__ F,
+                              const T* __restrict__ b, T* __restrict__ x, int maxLen, int zeroGuess) {
+  extern __shared__ unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (gw >= ncolc) return;
+  T* r = sm + (size_t)warp * 21 * maxLen;
+  T* Fs = r + 3 * maxLen;
+  const int c = cols[gw];
+  const int n0 = colStart[c], len = colStart[c + 1] - n0;
+  for (int e = lane; e < 18 * len; e += 32) Fs[e] = F[18 * (size_t)n0 + e];
+  for (int l = lane; l < len; l += 32) {
+    const int n = n0 + l;
+    T s0 = b[3 * n], s1 = b[3 * n + 1], s2 = b[3 * n + 2];
+    if (!zeroGuess) {
+      for (int s = 0; s < NSLOT; s++) {
+        const int j = nbr[(size_t)s * nn + n];
+        if (j < 0) continue;
+        const T x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
+        const T* v = val + (size_t)s * 9 * nn + n;
+        s0 -= v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
+        s1 -= v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
+        s2 -= v[6 * (size_t)nn] * x0 + v[7 * (size_t)nn] * x1 + v[8 * (size_t)nn] * x2;
+      }
+    }
+    r[3 * l] = s0; r[3 * l + 1] = s1; r[3 * l + 2] = s2;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    for (int l = 0; l < len; l++) {
+      const T* f = Fs + 18 * l;
+      T b0 = r[3 * l], b1 = r[3 * l + 1], b2 = r[3 * l + 2];
+      if (l > 0) {
+        const T p0 = r[3 * l - 3], p1 = r[3 * l - 2], p2 = r[3 * l - 1];
+        b0 -= f[9] * p0 + f[10] * p1 + f[11] * p2;
+        b1 -= f[12] * p0 + f[13] * p1 + f[14] * p2;
+        b2 -= f[15] * p0 + f[16] * p1 + f[17] * p2;
+      }
+      const T y0 = b0 / f[0];
+      const T y1 = (b1 - f[3] * y0) / f[4];
+      const T y2 = (b2 - f[6] * y0 - f[7] * y1) / f[8];
+      r[3 * l] = y0; r[3 * l + 1] = y1; r[3 * l + 2] = y2;
+    }
+    for (int l = len - 1; l >= 0; l--) {
+      const T* f = Fs + 18 * l;
+      T b0 = r[3 * l], b1 = r[3 * l + 1], b2 = r[3 * l + 2];
+      if (l + 1 < len) {
+        const T* g = Fs + 18 * (l + 1);
+        const T q0 = r[3 * l + 3], q1 = r[3 * l + 4], q2 = r[3 * l + 5];
+        b0 -= g[9] * q0 + g[12] * q1 + g[15] * q2;
+        b1 -= g[10] * q0 + g[13] * q1 + g[16] * q2;
+        b2 -= g[11] * q0 + g[14] * q1 + g[17] * q2;
+      }
+      const T z2 = b2 / f[8];
+      const T z1 = (b1 - f[7] * z2) / f[4];
+      const T z0 = (b0 - f[3] * z1 - f[6] * z2) / f[0];
+      r[3 * l] = z0; r[3 * l + 1] = z1; r[3 * l + 2] = z2;
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < 3 * len; e += 32) x[3 * (size_t)n0 + e] += r[e];
+}
+
+// restriction 0 -> 1: rc = P^T res, thread per aggregate (children are a contiguous node range)
+template <class T>
+__global__ void k_restrict0(int na, const int* __restrict__ aggStart, const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= na) return;
+  T acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int f = aggStart[I]; f < aggStart[I + 1]; f++) {
+    const T* w = W + 18 * (size_t)f;
+    const T r0 = res[3 * f], r1 = res[3 * f + 1], r2 = res[3 * f + 2];
+#pragma unroll
+    for (int a = 0; a < 6; a++) acc[a] += w[a] * r0 + w[6 + a] * r1 + w[12 + a] * r2;
+  }
+#pragma unroll
+  for (int a = 0; a < 6; a++) rc[6 * (size_t)I + a] = acc[a];
+}
+
+// prolongation 1 -> 0: x += P ec, thread per node
+template <class T>
+__global__ void k_prolong0(int nn, const int* __restrict__ nodeAgg, const T* __restrict__ W, const T* __restrict__ ec, T* __restrict__ x) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  const T* w = W + 18 * (size_t)n;
+  const T* e = ec + 6 * (size_t)nodeAgg[n];
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+    T s = 0;
+#pragma unroll
+    for (int a = 0; a < 6; a++) s += w[p * 6 + a] * e[a];
+    x[3 * (size_t)n + p] += s;
+  }
+}
+
+// shell-level residual res = b - K x (6x6 block CSR), thread per (row, component)
+template <class T>
+__global__ void k_apply_shell(int nrow, const int* __restrict__ rowPtr, const int* __restrict__ col, const T* __restrict__ val,
+                              const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ y) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= 6 * (size_t)nrow) return;
+  const int i = (int)(t / 6), p = (int)(t % 6);
+  T s = 0;
+  for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+    const T* v = val + 36 * (size_t)k + 6 * p;
+    const T* xj = x + 6 * (size_t)col[k];
+    s += v[0] * xj[0] + v[1] * xj[1] + v[2] * xj[2] + v[3] * xj[3] + v[4] * xj[4] + v[5] * xj[5];
+  }
+  y[t] = b ? b[t] - s : s;
+}
+
+// shell-level column sweep: warp per column of one colour (columnSweep shell branch, 10-solver.js:535-553)
+template <class T>
+__global__ void k_sweep_shell(int ncolc, const int* __restrict__ cols, const int* __restrict__ colStart, const int* __restrict__ rowPtr,
+                              const int* __restrict__ col, const T* __restrict__ val, const long long* __restrict__ cfPtr,
+                              const T* __restrict__ cf, const T* __restrict__ b, T* __restrict__ x, int maxm, int zeroGuess) {
+  extern __shared__ unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (gw >= ncolc) return;
+  T* r = sm + (size_t)warp * maxm;
+  const int c = cols[gw];
+  const int n0 = colStart[c], m = 6 * (colStart[c + 1] - n0);
+  for (int e = lane; e < m; e += 32) {
+    const int a = n0 + e / 6, p = e % 6;
+    T s = b[6 * (size_t)a + p];
+    if (!zeroGuess) {
+      for (int k = rowPtr[a]; k < rowPtr[a + 1]; k++) {
+        const T* v = val + 36 * (size_t)k + 6 * p;
+        const T* xj = x + 6 * (size_t)col[k];
+        s -= v[0] * xj[0] + v[1] * xj[1] + v[2] * xj[2] + v[3] * xj[3] + v[4] * xj[4] + v[5] * xj[5];
+      }
+    }
+    r[e] = s;
+  }
+  __syncwarp();
+  const T* L = cf + cfPtr[c];
+  for (int j = 0; j < m; j++) {
+    if (lane == 0) r[j] = r[j] / L[j * m + j];
+    __syncwarp();
+    const T xj = r[j];
+    for (int i = j + 1 + lane; i < m; i += 32) r[i] -= L[i * m + j] * xj;
+    __syncwarp();
+  }
+  for (int j = m - 1; j >= 0; j--) {
+    if (lane == 0) r[j] = r[j] / L[j * m + j];
+    __syncwarp();
+    const T xj = r[j];
+    for (int i = lane; i < j; i += 32) r[i] -= L[j * m + i] * xj;
+    __syncwarp();
+  }
+  for (int e = lane; e < m; e += 32) x[6 * (size_t)n0 + e] += r[e];
+}
+
+// shell restriction: rc = P^T res (children lists, transposeProl order)
+template <class T>
+__global__ void k_restrict_shell(int nnc, const int* __restrict__ chPtr, const int* __restrict__ chIdx, const int* __restrict__ chW,
+                                 const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= 6 * (size_t)nnc) return;
+  const int I = (int)(t / 6), a = (int)(t % 6);
+  T acc = 0;
+  for (int q = chPtr[I]; q < chPtr[I + 1]; q++) {
+    const int f = chIdx[q];
+    const T* w = W + 36 * (size_t)chW[q];
+    const T* r = res + 6 * (size_t)f;
+    acc += w[a] * r[0] + w[6 + a] * r[1] + w[12 + a] * r[2] + w[18 + a] * r[3] + w[24 + a] * r[4] + w[30 + a] * r[5];
+  }
+  rc[t] = acc;
+}
+
+// shell prolongation: x += P ec
+template <class T>
+__global__ void k_prolong_shell(int nnf, const int* __restrict__ prolPtr, const int* __restrict__ prolIdx, const T* __restrict__ W,
+                                const T* __restrict__ ec, T* __restrict__ x) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= 6 * (size_t)nnf) return;
+  const int f = (int)(t / 6), p = (int)(t % 6);
+  T v = x[t];
+  for (int q = prolPtr[f]; q < prolPtr[f + 1]; q++) {
+    const T* w = W + 36 * (size_t)q + 6 * p;
+    const T* e = ec + 6 * (size_t)prolIdx[q];
+    v += w[0] * e[0] + w[1] * e[1] + w[2] * e[2] + w[3] * e[3] + w[4] * e[4] + w[5] * e[5];
+  }
+  x[t] = v;
+}
+
+// coarsest: x = A^-1 b with the explicit inverse, warp per row
+template <class T, class M>
+__global__ void k_dense_apply(int n, const M* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (i >= n) return;
+  double s = 0;
+  for (int k = lane; k < n; k += 32) s += (double)inv[(size_t)i * n + k] * (double)b[k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) x[i] = (T)s;
+}
+
+__global__ void k_axpy_scalar(size_t n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] += alpha * x[i];
+}
+
+__global__ void k_div_scalar(size_t n, double* __restrict__ v, double d) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) v[i] /= d;
+}
+
+}  // namespace
+
+void launch_apply0(Context& c, const double* x, double* y, const double* b) {
+  k_apply0<double, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val.p, x, y, b);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_apply0_f32(Context& c, const double* x, double* y, const double* b) {
+  k_apply0<float, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val32.p, x, y, b);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_dot(Context& c, const double* a, const double* b, size_t n, double* out_dev) {
+  k_dot_partial<double><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, a, b, c.d_partial.p);
+  k_reduce_final<<<1, 1024, 0, c.stream>>>(RED_BLOCKS, c.d_partial.p, out_dev);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_finalize(Context& c, double* out_dev) {
+  k_reduce_final<<<1, 1024, 0, c.stream>>>(RED_BLOCKS, c.d_partial.p, out_dev);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_axpy(Context& c, double alpha, const double* x, double* y, size_t n) {
+  k_axpy_scalar<<<grid_for(n, 256), 256, 0, c.stream>>>(n, alpha, x, y);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_div_scalar(Context& c, double* v, double d, size_t n) {
+  k_div_scalar<<<grid_for(n, 256), 256, 0, c.stream>>>(n, v, d);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_axpy2(Context& c, const double* alpha_dev, const double* p, double* x, const double* q, double* r, size_t n) {
+  k_axpy2<double><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, alpha_dev, p, x, q, r, c.d_partial.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_xpby(Context& c, const double* z, const double* beta_dev, double* p, size_t n) {
+  k_xpby<double><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, z, beta_dev, p);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_div(Context& c, const double* num, const double* den, double* out, double sign) {
+  k_div<<<1, 32, 0, c.stream>>>(num, den, out, sign);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_zero_constrained(Context& c, double* v) {
+  if (c.constr.empty()) return;
+  k_zero_list<double><<<grid_for(c.constr.size(), 128), 128, 0, c.stream>>>((int)c.constr.size(), c.d_constr.p, v);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_scale_vec(Context& c, const double* x, const double* s, double* y, bool divide, size_t n) {
+  k_scale_vec<double><<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, s, y, divide ? 1 : 0);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+// MultigridPC._cycleOnce (10-solver.js:687-712) with zero initial guess on every level
+void launch_vcycle(Context& c, const double* r, double* z, bool mixed) {
+  (void)mixed;
+  cudaStream_t st = c.stream;
+  const int nn = c.nn;
+  // ---- level 0: pre-smoothing, 2 sweeps in colours 0..3
+  TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(double), st));
+  const int warps = 4;
+  const size_t smem0 = (size_t)warps * 21 * c.maxColLen * sizeof(double);
+  bool first = true;
+  for (int sweep = 0; sweep < 2; sweep++)
+    for (int col = 0; col < 4; col++) {
+      if (!c.colorCount[col]) continue;
+      k_sweep_solid<double><<<grid_for(c.colorCount[col], warps), 32 * warps, smem0, st>>>(
+          c.colorCount[col], c.d_colorCols[col].p, c.d_colStart.p, nn, c.d_nbr.p, c.d_val.p, c.d_F.p, r, z, c.maxColLen, first ? 1 : 0);
+      first = false;
+    }
+  // residual and restriction
+  k_apply0<double, double><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_nbr.p, c.d_val.p, z, c.d_res0.p, r);
+  ShellLevel& L1 = *c.shells[0];
+  k_restrict0<double><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, c.d_W01.p, c.d_res0.p, L1.d_b.p);
+  // ---- shell levels down
+  const size_t nl = c.shells.size();
+  for (size_t l = 0; l < nl; l++) {
+    ShellLevel& L = *c.shells[l];
+    if (L.coarsest) {
+      k_dense_apply<double, double><<<grid_for(L.denseN, 4), 128, 0, st>>>(L.denseN, L.d_inv.p, L.d_b.p, L.d_x.p);
+      break;
+    }
+    TM_CUDA_CHECK(cudaMemsetAsync(L.d_x.p, 0, 6 * (size_t)L.nn * sizeof(double), st));
+    const size_t smem = (size_t)warps * L.maxm * sizeof(double);
+    bool firstS = true;
+    for (int sweep = 0; sweep < 2; sweep++)
+      for (int col = 0; col < 4; col++) {
+        if (!L.colorCount[col]) continue;
+        k_sweep_shell<double><<<grid_for(L.colorCount[col], warps), 32 * warps, smem, st>>>(
+            L.colorCount[col], L.d_colorCols[col].p, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_cfPtr.p, L.d_cf.p, L.d_b.p,
+            L.d_x.p, L.maxm, firstS ? 1 : 0);
+        firstS = false;
+      }
+    k_apply_shell<double><<<grid_for(6 * (size_t)L.nn, 128), 128, 0, st>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_x.p, L.d_b.p, L.d_res.p);
+    ShellLevel& C = *c.shells[l + 1];
+    k_restrict_shell<double><<<grid_for(6 * (size_t)C.nn, 128), 128, 0, st>>>(C.nn, L.d_chPtr.p, L.d_chIdx.p, L.d_chW.p, L.d_prolW.p,
+                                                                               L.d_res.p, C.d_b.p);
+  }
+  // ---- shell levels up
+  for (int l = (int)nl - 2; l >= 0; l--) {
+    ShellLevel& L = *c.shells[l];
+    ShellLevel& C = *c.shells[l + 1];
+    k_prolong_shell<double><<<grid_for(6 * (size_t)L.nn, 128), 128, 0, st>>>(L.nn, L.d_prolPtr.p, L.d_prolIdx.p, L.d_prolW.p, C.d_x.p, L.d_x.p);
+    const size_t smem = (size_t)warps * L.maxm * sizeof(double);
+    for (int sweep = 0; sweep < 2; sweep++)
+      for (int col = 3; col >= 0; col--) {
+        if (!L.colorCount[col]) continue;
+        k_sweep_shell<double><<<grid_for(L.colorCount[col], warps), 32 * warps, smem, st>>>(
+            L.colorCount[col], L.d_colorCols[col].p, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_cfPtr.p, L.d_cf.p, L.d_b.p,
+            L.d_x.p, L.maxm, 0);
+      }
+  }
+  // ---- level 0: prolongation and post-smoothing, colours 3..0
+  k_prolong0<double><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_nodeAgg.p, c.d_W01.p, L1.d_x.p, z);
+  for (int sweep = 0; sweep < 2; sweep++)
+    for (int col = 3; col >= 0; col--) {
+      if (!c.colorCount[col]) continue;
+      k_sweep_solid<double><<<grid_for(c.colorCount[col], warps), 32 * warps, smem0, st>>>(
+          c.colorCount[col], c.d_colorCols[col].p, c.d_colStart.p, nn, c.d_nbr.p, c.d_val.p, c.d_F.p, r, z, c.maxColLen, 0);
+    }
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace tmg

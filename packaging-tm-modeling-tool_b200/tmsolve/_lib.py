@@ -1,0 +1,114 @@
+"""ctypes binding of libtmsolve.so (C-ABI declared in include/tmsolve.h).
+
+The library is required: there is no CPU fallback. Loading fails loudly when the
+built shared object is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libtmsolve.so")
+
+TM_OK, TM_NOT_CONVERGED, TM_NONFINITE, TM_TIMEOUT, TM_BAD_INPUT, TM_CUDA, TM_NO_DEVICE = range(7)
+STATUS_NAMES = {0: "TM_OK", 1: "TM_NOT_CONVERGED", 2: "TM_NONFINITE", 3: "TM_TIMEOUT", 4: "TM_BAD_INPUT", 5: "TM_CUDA",
+                6: "TM_NO_DEVICE"}
+
+EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bcsr", "tm_solve", "tm_matvec", "tm_get_bcsr",
+            "tm_sizes", "tm_destroy", "tm_last_error", "tm_solve_device", "tm_matvec_device", "tm_anand_screen",
+            "tm_anand_screen_device", "tm_anand_step"]
+
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int32)
+
+
+class TmMesh(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("xs", dp), ("ys", dp), ("zs", dp), ("nn", C.c_int32), ("ne", C.c_int32),
+                ("coords", dp), ("nodeId", ip), ("conn", ip), ("eIJK", ip), ("colStart", ip), ("cellElems", ip),
+                ("eGroup", ip), ("ePart", C.POINTER(C.c_int8)), ("eScale", dp), ("ngroups", C.c_int32), ("groupStage", ip),
+                ("npset", C.c_int32), ("ePset", ip), ("nconstr", C.c_int32), ("constr", ip),
+                ("nfeatureX", C.c_int32), ("nfeatureY", C.c_int32), ("featureX", ip), ("featureY", ip)]
+
+
+class TmStep(C.Structure):
+    _fields_ = [("stage", C.c_int32), ("psetLayered", ip), ("D", dp), ("s0", dp), ("W", dp), ("V", dp), ("psetBorn", ip)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, C.c_double)
+
+
+class TmSolveOpts(C.Structure):
+    _fields_ = [("tol", C.c_double), ("maxit", C.c_int32), ("warm", C.c_int32), ("precond", C.c_int32),
+                ("precision", C.c_int32), ("key", C.c_int64), ("progress", PROGRESS_FN), ("progress_user", C.c_void_p),
+                ("progress_every", C.c_int32)]
+
+
+class TmSolveInfo(C.Structure):
+    _fields_ = [("iters", C.c_int32), ("relres", C.c_double), ("iters0", C.c_double), ("converged", C.c_int32),
+                ("ms", C.c_double), ("pc_ms", C.c_double), ("rebuilt", C.c_int32), ("warm", C.c_int32),
+                ("fallback", C.c_int32), ("jitter_count", C.c_int32), ("levels", C.c_int32), ("status", C.c_int32),
+                ("refinements", C.c_int32)]
+
+
+class TmAnandMaterial(C.Structure):
+    _fields_ = [("A", C.c_double), ("QR", C.c_double), ("xi", C.c_double), ("m", C.c_double), ("shat", C.c_double),
+                ("n", C.c_double), ("h0", C.c_double), ("a", C.c_double), ("s0", C.c_double), ("nu", C.c_double),
+                ("Etab", dp), ("Ftab", dp)]
+
+
+_lib = None
+
+
+def load():
+    """Load libtmsolve.so; raises when it has not been built (there is no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libtmsolve.so not found at {LIB_PATH}: build it with `make -C {PKG_ROOT}` "
+                          "(the solve path has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.tm_default_solve_opts.argtypes = [C.POINTER(TmSolveOpts)]
+    L.tm_create.argtypes = [C.POINTER(TmMesh), C.POINTER(vp)]
+    L.tm_assemble_step.argtypes = [vp, C.POINTER(TmStep), vp]
+    L.tm_set_bcsr.argtypes = [vp, vp, vp, vp, vp]
+    L.tm_solve.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
+    L.tm_solve_device.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
+    L.tm_matvec.argtypes = [vp, vp, vp]
+    L.tm_matvec_device.argtypes = [vp, vp, vp]
+    L.tm_get_bcsr.argtypes = [vp, vp, vp, vp]
+    L.tm_sizes.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.tm_destroy.argtypes = [vp]
+    L.tm_last_error.argtypes = [C.c_char_p, C.c_size_t]
+    L.tm_last_error.restype = C.c_int32
+    L.tm_anand_screen.argtypes = [C.POINTER(TmAnandMaterial), C.c_int32, C.c_int32, vp, vp, C.c_int32, vp, vp, vp, vp,
+                                  C.c_int32, vp, vp, vp]
+    L.tm_anand_screen_device.argtypes = L.tm_anand_screen.argtypes
+    L.tm_anand_step.argtypes = [C.POINTER(TmAnandMaterial), C.c_int32, vp, vp, C.c_double, C.c_double, vp, vp, C.c_int32]
+    for name in EXPORTED:
+        getattr(L, name).restype = C.c_int32 if name not in ("tm_default_solve_opts",) else None
+    _lib = L
+    return L
+
+
+class TmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def last_error() -> str:
+    L = load()
+    buf = C.create_string_buffer(4096)
+    L.tm_last_error(buf, 4096)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, allow_not_converged: bool = False) -> int:
+    if status == TM_OK or (allow_not_converged and status == TM_NOT_CONVERGED):
+        return status
+    raise TmError(status, last_error())

@@ -1,0 +1,108 @@
+"""Anand screening of solder joints on the GPU (host side).
+
+* ``cycle_history`` restates ``cycleHistory`` (src/core/13-fatigue.js:275-293): ramps in
+  steps of at most RAMP_MAX_DT = 5 degC and DWELL_MIN_STEPS = 10 steps per dwell;
+  phases are encoded 0 start, 1 ramp up, 2 dwell hot, 3 ramp down, 4 dwell cold.
+* ``screen`` is the per-site loop of ``screenJoints`` (13-fatigue.js:395-451) through
+  ``tm_anand_screen``.
+* ``synthetic_strain_table`` builds a bump-layer strain table with the shape of
+  ``siteStrainTable`` (13-fatigue.js:318-347): sites on a die bump grid, strains linear
+  in temperature (constant-property thermoelasticity), shear growing with the distance
+  to the neutral point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from ._lib import TmAnandMaterial, check, load
+
+RAMP_MAX_DT = 5        # 00-constants.js:111
+DWELL_MIN_STEPS = 10   # 00-constants.js:112
+PHASES = {"start": 0, "ramp up": 1, "dwell hot": 2, "ramp down": 3, "dwell cold": 4}
+
+
+def cycle_history(Tmin: float, Tmax: float, ramp_c_per_min: float, dwell_min: float, cycles: int) -> dict:
+    rate = ramp_c_per_min / 60.0
+    dwell = dwell_min * 60.0
+    t, T, cyc, ph = [0.0], [25.0], [0], [0]
+    time = [0.0]
+
+    def ramp(frm, to, c):
+        n = max(1, math.ceil(abs(to - frm) / RAMP_MAX_DT))
+        dur = abs(to - frm) / rate
+        for k in range(1, n + 1):
+            time[0] += dur / n
+            t.append(time[0]); T.append(frm + (to - frm) * k / n); cyc.append(c)
+            ph.append(PHASES["ramp up"] if to > frm else PHASES["ramp down"])
+
+    def hold(Tv, c, label):
+        for _ in range(DWELL_MIN_STEPS):
+            time[0] += dwell / DWELL_MIN_STEPS
+            t.append(time[0]); T.append(Tv); cyc.append(c); ph.append(PHASES[label])
+
+    for c in range(1, cycles + 1):
+        ramp(T[-1], Tmax, c); hold(Tmax, c, "dwell hot")
+        ramp(Tmax, Tmin, c); hold(Tmin, c, "dwell cold")
+    return dict(t=np.array(t), T=np.array(T), cycle=np.array(cyc, np.int32), phase=np.array(ph, np.int32), cycles=cycles)
+
+
+def cycling_temps(Tmin: float, Tmax: float, step: float = 10.0) -> np.ndarray:
+    """Cycling sample temperatures every CYCLE_DT_STEP (00-constants.js:106) with 25 degC included."""
+    ts = set(np.arange(Tmin, Tmax + 1e-9, step).round(9).tolist()) | {Tmin, Tmax, 25.0}
+    return np.array(sorted(ts))
+
+
+def synthetic_strain_table(nsites: int, temps: np.ndarray, seed: int = 20261203, die_half: float = 7.5) -> tuple:
+    """(table nsites x ntemps x 6, x, y): strain linear in T about 25 degC per site."""
+    rng = np.random.default_rng(seed)
+    nb = int(math.ceil(math.sqrt(nsites)))
+    g = np.linspace(-die_half, die_half, nb)
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    x = X.ravel()[:nsites]; y = Y.ravel()[:nsites]
+    r = np.hypot(x, y) / (math.sqrt(2) * die_half)
+    per_deg = np.zeros((nsites, 6))
+    per_deg[:, 0] = 8e-6 * (1 + 0.1 * rng.standard_normal(nsites))
+    per_deg[:, 1] = 8e-6 * (1 + 0.1 * rng.standard_normal(nsites))
+    per_deg[:, 2] = 26e-6 * (1 + 0.05 * rng.standard_normal(nsites))          # axial (total, incl. thermal)
+    per_deg[:, 3] = 1e-6 * rng.standard_normal(nsites)
+    per_deg[:, 4] = 3.0e-5 * y / die_half * (0.5 + 0.5 * r)                      # gyz, grows with DNP
+    per_deg[:, 5] = 3.0e-5 * x / die_half * (0.5 + 0.5 * r)                      # gzx
+    e0 = 1e-4 * rng.standard_normal((nsites, 6))
+    table = e0[:, None, :] + per_deg[:, None, :] * (np.asarray(temps)[None, :, None] - 25.0)
+    return np.ascontiguousarray(table), x, y
+
+
+def material(params: dict, Etab: np.ndarray, Ftab: np.ndarray):
+    Etab = np.ascontiguousarray(Etab, np.float64); Ftab = np.ascontiguousarray(Ftab, np.float64)
+    m = TmAnandMaterial(A=params["A"], QR=params["QR"], xi=params["xi"], m=params["m"], shat=params["shat"], n=params["n"],
+                        h0=params["h0"], a=params["a"], s0=params["s0"], nu=params["nu"],
+                        Etab=Etab.ctypes.data_as(C.POINTER(C.c_double)), Ftab=Ftab.ctypes.data_as(C.POINTER(C.c_double)))
+    return m, (Etab, Ftab)
+
+
+def screen(params: dict, Etab, Ftab, temps, table, hist) -> tuple:
+    """dW, dE, stab per site (screenJoints' per-site loop on the GPU)."""
+    m, keep = material(params, Etab, Ftab)
+    temps = np.ascontiguousarray(temps, np.float64); table = np.ascontiguousarray(table, np.float64)
+    ns = table.size // (6 * len(temps))
+    t = np.ascontiguousarray(hist["t"], np.float64); T = np.ascontiguousarray(hist["T"], np.float64)
+    cyc = np.ascontiguousarray(hist["cycle"], np.int32); ph = np.ascontiguousarray(hist["phase"], np.int32)
+    dW = np.zeros(ns); dE = np.zeros(ns); stab = np.zeros(ns)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    check(load().tm_anand_screen(C.byref(m), ns, len(temps), vp(temps), vp(table), len(t), vp(t), vp(T), vp(cyc), vp(ph),
+                                 int(hist["cycles"]), vp(dW), vp(dE), vp(stab)))
+    return dW, dE, stab
+
+
+def point_step(params: dict, Etab, Ftab, state: np.ndarray, eps: np.ndarray, T: float, dt: float, commit=True):
+    """Batched AnandPoint.step (+ commit) of independent points: state (npts, 12) updated in place."""
+    m, keep = material(params, Etab, Ftab)
+    npts = state.shape[0]
+    eps = np.ascontiguousarray(eps, np.float64)
+    sig = np.zeros((npts, 6)); D = np.zeros((npts, 36))
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    check(load().tm_anand_step(C.byref(m), npts, vp(state), vp(eps), float(T), float(dt), vp(sig), vp(D), int(commit)))
+    return sig, D

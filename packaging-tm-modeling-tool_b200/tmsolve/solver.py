@@ -1,0 +1,146 @@
+"""Host-side mirror of the reference's solver interface over the GPU C-ABI.
+
+``DeviceModel`` stands for ``FEModel`` + ``LinearSolver`` of the reference
+(src/core/09-assembly.js:208, src/core/10-solver.js:826):
+
+* ``assemble_step(step)``  ->  ``FEModel.assembleStep(Ta, Tb, stage, rhs)``: the per-step
+  property sets are computed by the caller (``prepareStep``'s output) and the assembly,
+  condensation and constraints run on the GPU;
+* ``set_bcsr(...)``        ->  solving a caller-assembled ``model.pattern``/``model.val``;
+* ``solve(f, label, key)`` ->  ``LinearSolver.solve``: returns the reference's record
+  ``{u, iters, relres, converged, ms, pcMs, precond, rebuilt, warm, iters0, fallback}``;
+  non-convergence gives ``converged: False`` (the caller decides to throw, as
+  ``Analysis.solveStep`` does, src/core/11-analysis.js:204); every other failure raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import TmError, TmMesh, TmSolveInfo, TmSolveOpts, TmStep, check, load
+from .packages import Package, StepData
+
+
+def _p(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype)) if a is not None else None
+
+
+class DeviceModel:
+    def __init__(self, pkg: Package, constraints: Optional[np.ndarray] = None):
+        L = load()
+        m = pkg.mesh
+        self.pkg = pkg
+        self._keep = []
+
+        def keep(a, dtype):
+            a = np.ascontiguousarray(a, dtype)
+            self._keep.append(a)
+            return a
+
+        xs, ys, zs = keep(m.xs, np.float64), keep(m.ys, np.float64), keep(m.zs, np.float64)
+        con = keep(m.constraints if constraints is None else constraints, np.int32)
+        fx = keep(m.featureX, np.int32); fy = keep(m.featureY, np.int32)
+        mesh = TmMesh(nx=m.nx, ny=m.ny, nz=m.nz, xs=_p(xs, C.c_double), ys=_p(ys, C.c_double), zs=_p(zs, C.c_double),
+                      nn=m.nn, ne=m.ne, coords=_p(keep(m.coords, np.float64), C.c_double),
+                      nodeId=_p(keep(m.nodeId, np.int32), C.c_int32), conn=_p(keep(m.conn, np.int32), C.c_int32),
+                      eIJK=_p(keep(m.eIJK, np.int32), C.c_int32), colStart=_p(keep(m.colStart, np.int32), C.c_int32),
+                      cellElems=_p(keep(m.cellElems, np.int32), C.c_int32), eGroup=_p(keep(m.eGroup, np.int32), C.c_int32),
+                      ePart=_p(keep(m.ePart, np.int8), C.c_int8), eScale=_p(keep(m.eScale, np.float64), C.c_double),
+                      ngroups=len(pkg.group_stage), groupStage=_p(keep(pkg.group_stage, np.int32), C.c_int32),
+                      npset=int(pkg.npset), ePset=_p(keep(pkg.e_pset, np.int32), C.c_int32),
+                      nconstr=len(con), constr=_p(con, C.c_int32), nfeatureX=len(fx), nfeatureY=len(fy),
+                      featureX=_p(fx, C.c_int32) if len(fx) else None, featureY=_p(fy, C.c_int32) if len(fy) else None)
+        h = C.c_void_p()
+        check(L.tm_create(C.byref(mesh), C.byref(h)))
+        self.h = h
+        self._keep = []
+        self.ndof = 3 * m.nn
+        sz = (C.c_int64 * 6)()
+        check(L.tm_sizes(self.h, sz))
+        self.nn, self.ne, self.nb, _, self.levels, self.coarsest_dof = (int(v) for v in sz)
+        self.log = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().tm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- FEModel.assembleStep ------------------------------------------------------------
+    def assemble_step(self, step: StepData) -> np.ndarray:
+        lay = np.ascontiguousarray(step.layered, np.int32); born = np.ascontiguousarray(step.born, np.int32)
+        D = np.ascontiguousarray(step.D, np.float64); s0 = np.ascontiguousarray(step.s0, np.float64)
+        W = np.ascontiguousarray(step.W, np.float64); V = np.ascontiguousarray(step.V, np.float64)
+        st = TmStep(stage=int(step.stage), psetLayered=_p(lay, C.c_int32), D=_p(D, C.c_double), s0=_p(s0, C.c_double),
+                    W=_p(W, C.c_double), V=_p(V, C.c_double), psetBorn=_p(born, C.c_int32))
+        rhs = np.zeros(self.ndof)
+        check(load().tm_assemble_step(self.h, C.byref(st), rhs.ctypes.data_as(C.c_void_p)))
+        return rhs
+
+    def set_bcsr(self, rowPtr, col, val, isConstrained):
+        rowPtr = np.ascontiguousarray(rowPtr, np.int32); col = np.ascontiguousarray(col, np.int32)
+        val = np.ascontiguousarray(val, np.float64); isC = np.ascontiguousarray(isConstrained, np.uint8)
+        check(load().tm_set_bcsr(self.h, rowPtr.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                                 val.ctypes.data_as(C.c_void_p), isC.ctypes.data_as(C.c_void_p)))
+
+    def get_bcsr(self):
+        rowPtr = np.zeros(self.nn + 1, np.int32); col = np.zeros(self.nb, np.int32); val = np.zeros(9 * self.nb)
+        check(load().tm_get_bcsr(self.h, rowPtr.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                                 val.ctypes.data_as(C.c_void_p)))
+        return rowPtr, col, val
+
+    def matvec(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.ndof)
+        check(load().tm_matvec(self.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p)))
+        return y
+
+    # ---- LinearSolver.solve ----------------------------------------------------------------
+    @staticmethod
+    def make_opts(tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64", key=-1) -> TmSolveOpts:
+        o = TmSolveOpts()
+        load().tm_default_solve_opts(C.byref(o))
+        o.tol = tol; o.maxit = maxit; o.warm = warm
+        o.precond = 0 if precond == "mg" else 1
+        o.precision = 0 if precision == "fp64" else 1
+        o.key = -1 if key is None else int(key)
+        return o
+
+    @staticmethod
+    def record(info: TmSolveInfo, label=None, precond="mg") -> dict:
+        return dict(label=label, iters=int(info.iters), relres=float(info.relres), converged=bool(info.converged),
+                    ms=float(info.ms), pcMs=float(info.pc_ms), precond=precond, rebuilt=bool(info.rebuilt),
+                    warm=int(info.warm), iters0=float(info.iters0), fallback=None if not info.fallback else True,
+                    jitter=int(info.jitter_count), levels=int(info.levels), refinements=int(info.refinements))
+
+    def solve(self, f, label=None, key=-1, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64") -> dict:
+        f = np.ascontiguousarray(f, np.float64)
+        u = np.zeros(self.ndof)
+        info = TmSolveInfo()
+        o = self.make_opts(tol, maxit, warm, precond, precision, key)
+        check(load().tm_solve(self.h, f.ctypes.data_as(C.c_void_p), u.ctypes.data_as(C.c_void_p), C.byref(o), C.byref(info)),
+              allow_not_converged=True)
+        rec = self.record(info, label, precond)
+        self.log.append(rec)
+        rec = dict(rec)
+        rec["u"] = u
+        return rec
+
+    def solve_device(self, f_ptr: int, u_ptr: int, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64", key=-1) -> dict:
+        """The same solve with f and u already in device memory (raw device pointers)."""
+        info = TmSolveInfo()
+        o = self.make_opts(tol, maxit, warm, precond, precision, key)
+        check(load().tm_solve_device(self.h, C.c_void_p(f_ptr), C.c_void_p(u_ptr), C.byref(o), C.byref(info)),
+              allow_not_converged=True)
+        return self.record(info, None, precond)
+
+
+__all__ = ["DeviceModel", "TmError"]

@@ -1,0 +1,144 @@
+"""Parity of the CUDA solve path (through the C-ABI) with the FP64 oracle.
+
+Bars (written here as the tests use them):
+* assembled operator and load: bit-exact (the set-up kernels repeat the reference's
+  operations in the same order, without fused multiply-add);
+* operator apply: relative 2-norm difference <= 1e-13;
+* solutions at relative residual 1e-12: relative 2-norm difference <= 1e-8, warpage <= 1e-8;
+* the multigrid V-cycle visits columns in four colours (the reference sweeps them
+  lexicographically), so iteration counts may differ by a few.
+"""
+import numpy as np
+import pytest
+
+from tmsolve import _lib
+from tmsolve.materials import iso_d
+from tmsolve.packages import box_package, fcbga_c1, lidded_c2, linspace, rms_warpage
+
+pytestmark = pytest.mark.gpu
+
+
+def _models(pkg, oracle_lib):
+    from tmsolve.solver import DeviceModel
+    return DeviceModel(pkg), oracle_lib.OracleModel(pkg)
+
+
+def small_box():
+    mats = [(iso_d(110000.0, 0.34), 16.4e-6, 16.4e-6), (iso_d(130000.0, 0.28), 2.6e-6, 2.6e-6)]
+    return box_package(linspace(-5, 5, 8), linspace(-4, 4, 6), [0, 0.25, 0.5, 0.75, 1.0], mats,
+                       lambda i, j, k: 0 if k < 2 else 1, Ta=25.0, Tb=-75.0)
+
+
+@pytest.mark.parametrize("make", [small_box, fcbga_c1, lambda: lidded_c2(n_inplane=24)], ids=["box", "c1", "c2_24"])
+def test_assembly_bit_exact(make, oracle_lib):
+    pkg = make()
+    dm, om = _models(pkg, oracle_lib)
+    step = pkg.step()
+    f_gpu = dm.assemble_step(step)
+    f_orc = om.assemble(step)
+    rp, col, val = dm.get_bcsr()
+    orp, ocol, oval, isC = om.bcsr()
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol)
+    assert np.array_equal(val, oval), np.abs(val - oval).max()
+    assert np.array_equal(f_gpu, f_orc), np.abs(f_gpu - f_orc).max()
+
+
+def test_matvec(oracle_lib):
+    pkg = fcbga_c1()
+    dm, om = _models(pkg, oracle_lib)
+    step = pkg.step()
+    dm.assemble_step(step); om.assemble(step)
+    x = np.random.default_rng(1).standard_normal(dm.ndof)
+    y, yo = dm.matvec(x), om.matvec(x)
+    assert np.linalg.norm(y - yo) / np.linalg.norm(yo) <= 1e-13
+
+
+@pytest.mark.parametrize("make", [small_box, fcbga_c1], ids=["box", "c1"])
+def test_solve_parity_mg(make, oracle_lib):
+    pkg = make()
+    dm, om = _models(pkg, oracle_lib)
+    step = pkg.step()
+    f = dm.assemble_step(step)
+    fo = om.assemble(step)
+    r = dm.solve(f, tol=1e-12)
+    ro = om.solve(fo, tol=1e-12)
+    assert r["converged"] and ro["converged"]
+    u, uo = r["u"], ro["u"]
+    assert np.linalg.norm(u - uo) / np.linalg.norm(uo) <= 1e-8
+    w, wo = rms_warpage(pkg.mesh, u), rms_warpage(pkg.mesh, uo)
+    assert abs(w / wo - 1) <= 1e-8
+    assert r["iters"] <= 2 * ro["iters"] + 5
+
+
+def test_solve_v3_curvature(oracle_lib):
+    from test_oracle_known_answers import centre_curvature, timoshenko, v3_package
+    pkg = v3_package()
+    from tmsolve.solver import DeviceModel
+    dm = DeviceModel(pkg)
+    r = dm.solve(dm.assemble_step(pkg.step()), tol=1e-10)
+    kxx, _ = centre_curvature(pkg.mesh, r["u"])
+    assert abs(-kxx / timoshenko() - 1) < 0.03
+    assert f"{-kxx:.4e}" == "2.0692e-03"
+
+
+def test_jacobi_pcg(oracle_lib):
+    pkg = small_box()
+    dm, om = _models(pkg, oracle_lib)
+    step = pkg.step()
+    f = dm.assemble_step(step); fo = om.assemble(step)
+    r = dm.solve(f, tol=1e-12, precond="jacobi", maxit=20000)
+    ro = om.solve(fo, tol=1e-12)
+    assert r["converged"]
+    assert np.linalg.norm(r["u"] - ro["u"]) / np.linalg.norm(ro["u"]) <= 1e-8
+
+
+def test_set_bcsr_dropin(oracle_lib):
+    """Solve a caller-assembled operator (the reference's model.val) through tm_set_bcsr."""
+    pkg = fcbga_c1()
+    dm, om = _models(pkg, oracle_lib)
+    fo = om.assemble(pkg.step())
+    rp, col, val, isC = om.bcsr()
+    dm.set_bcsr(rp, col, val, isC)
+    r = dm.solve(fo, tol=1e-12)
+    ro = om.solve(fo, tol=1e-12)
+    assert np.linalg.norm(r["u"] - ro["u"]) / np.linalg.norm(ro["u"]) <= 1e-8
+
+
+def test_warm_start_second_solve(oracle_lib):
+    pkg = fcbga_c1()
+    from tmsolve.solver import DeviceModel
+    dm = DeviceModel(pkg)
+    f = dm.assemble_step(pkg.step())
+    r1 = dm.solve(f, tol=1e-10, key=0)
+    f2 = dm.assemble_step(pkg.step(150.0, 25.0))
+    r2 = dm.solve(f2, tol=1e-10, key=1)
+    assert r2["warm"] >= 1 and r2["iters"] <= 2
+    assert np.linalg.norm(r2["u"] - r1["u"]) / np.linalg.norm(r1["u"]) < 1e-8
+
+
+def test_nonfinite_load_is_an_error():
+    pkg = small_box()
+    from tmsolve.solver import DeviceModel
+    dm = DeviceModel(pkg)
+    f = dm.assemble_step(pkg.step())
+    f[5] = np.nan
+    with pytest.raises(_lib.TmError) as e:
+        dm.solve(f)
+    assert e.value.status == _lib.TM_NONFINITE
+
+
+def test_maxit_not_converged():
+    pkg = small_box()
+    from tmsolve.solver import DeviceModel
+    dm = DeviceModel(pkg)
+    r = dm.solve(dm.assemble_step(pkg.step()), tol=1e-14, maxit=1, warm=0)
+    assert r["converged"] is False and r["iters"] == 1
+
+
+def test_zero_load():
+    pkg = small_box()
+    from tmsolve.solver import DeviceModel
+    dm = DeviceModel(pkg)
+    dm.assemble_step(pkg.step())
+    r = dm.solve(np.zeros(dm.ndof))
+    assert r["converged"] and r["iters"] == 0 and not r["u"].any()
