@@ -1,0 +1,337 @@
+"""Benchmark of the solve path: one step = FEModel.assembleStep + LinearSolver.solve of the
+lidded FCBGA workload (160 x 160 x 32 elements, 8-2-8 layered substrate, ~2.07M DOF) to a
+relative residual of 1e-8, with a fresh multigrid preconditioner every step (as the tool's
+thermal path does) and no warm start (every step solves the same synthetic step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64]
+
+Metric: MDOF*iter/s = DOF x PCG iterations / step seconds / 1e6 (higher is better), whole
+job over all ranks; the solve seconds and iterations are in the JSON line too.
+`value` times device-resident inputs (device assembly + tm_solve_device); `e2e` goes through
+the public host API (tm_assemble_step returning the load to the host, tm_solve with host
+buffers), host<->device copies inside the timed region.
+Multi-GPU: replicas only (each rank solves its own copy; the path has no exchange step).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "packaging-tm-modeling-tool_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "PCG-MG solve s & MDOF·iter/s, mixed vs FP64 GPU at ≤1e-6 warpage err; HBM GB/s"
+UNIT = "MDOF·iter/s"
+WORKLOAD = "lidded_c2 160x160x32 (8-2-8 layered substrate, die, TIM, Cu hat lid), 150->25 degC step, tol 1e-8"
+DOMINANT = "sweep_solid"   # the level-0 z-column smoother: largest share of the ncu launch list
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--inplane", type=int, default=160)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="one assemble + one solve only (for ncu captures); prints no bench line")
+    return ap.parse_args()
+
+
+def run_profile(a):
+    """The smallest run of the hot path for ncu: model creation, one assembly, one solve."""
+    import torch
+    from tmsolve.packages import lidded_c2
+    from tmsolve.solver import DeviceModel
+    torch.cuda.set_device(0)
+    pkg = lidded_c2(n_inplane=a.inplane)
+    dm = DeviceModel(pkg)
+    f = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
+    u = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
+    dm.assemble_step_device(pkg.step(), f.data_ptr())
+    r = dm.solve_device(f.data_ptr(), u.data_ptr(), tol=1e-8, warm=0, key=1, precision=a.precision)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": True, "dof": dm.ndof, "iters": r["iters"], "converged": r["converged"], "ms": r["ms"]}))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---- clocks during the timed region -------------------------------------------------------------
+class Clocks:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if len(r) > 3]
+        mx = max(float(r[2]) for r in rows if len(r) > 3)
+        pw = [float(r[3]) for r in rows if len(r) > 3]
+        load = [s for s, p in zip(sm, pw) if p > 0.5 * max(pw)] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# ---- CPU: the oracle port of the reference's solve path --------------------------------------------
+def cpu_sample(args_tuple):
+    """Assemble + multigrid set-up + a bounded number of PCG iterations of the workload on one core."""
+    inplane, iters = args_tuple
+    for p in (ROOT, PKG):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    from oracle import oracle
+    from tmsolve.packages import lidded_c2
+    pkg = lidded_c2(n_inplane=inplane)
+    om = oracle.OracleModel(pkg)
+    t0 = time.perf_counter()
+    f = om.assemble(pkg.step())
+    r = om.solve(f, tol=1e-8, maxit=iters)
+    dt = time.perf_counter() - t0
+    return om.ndof, r["iters"], dt
+
+
+def cpu_run(inplane, iters, procs):
+    import multiprocessing as mp
+    if procs <= 1:
+        return [cpu_sample((inplane, iters))]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        return pool.map(cpu_sample, [(inplane, iters)] * procs)
+
+
+def reference_procs():
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        mem = psutil.virtual_memory().available / 4e9
+    except Exception:
+        mem = 8
+    return max(1, min(n, int(mem), 16))
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    oracle.build()
+    procs = reference_procs()
+    iters = 3
+    for _ in range(a.warmup):
+        cpu_run(a.inplane, iters, procs)
+    t0 = time.perf_counter()
+    work = 0.0
+    n = 0
+    for _ in range(a.steps):
+        res = cpu_run(a.inplane, iters, procs)
+        work += sum(nd * it for nd, it, _ in res) / 1e6
+        n = res[0][0]
+    dt = time.perf_counter() - t0
+    val = work / dt
+    sample = f"per step {procs} concurrent single-thread solves (one per worker, as the tool's runSweep farms steps out), each: assembly + multigrid set-up + {iters} PCG iterations of the {n}-DOF workload"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * dt / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "dof": n, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is JavaScript with no engine on this image; the C++ FP64 port of its solve path (oracle/) is timed"}))
+
+
+# ---- GPU -----------------------------------------------------------------------------------------
+def run_ours(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        from oracle import oracle
+        oracle.build()
+        nd, it, dt = cpu_sample((a.inplane, 3))
+        cpu = {"value": nd * it / 1e6 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"assembly + multigrid set-up + {it} PCG iterations of the {nd}-DOF workload on one core ({dt:.1f} s)"}
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from tmsolve.packages import lidded_c2, rms_warpage
+    from tmsolve.solver import DeviceModel, launch_count
+    pkg = lidded_c2(n_inplane=a.inplane)
+    dm = DeviceModel(pkg)
+    stream = torch.cuda.current_stream()
+    dm.set_stream(stream.cuda_stream)
+    n = dm.ndof
+    step = pkg.step()
+    f = torch.empty(n, dtype=torch.float64, device="cuda")
+    u = torch.empty(n, dtype=torch.float64, device="cuda")
+    u64 = torch.empty(n, dtype=torch.float64, device="cuda")
+    key = [0]
+
+    def one(precision, uu):
+        key[0] += 1
+        dm.assemble_step_device(step, f.data_ptr())
+        return dm.solve_device(f.data_ptr(), uu.data_ptr(), tol=1e-8, warm=0, key=key[0], precision=precision)
+
+    for _ in range(a.warmup):
+        one(a.precision, u)
+    # accuracy of the timed precision against the FP64 GPU solve of the same step
+    r64 = one("fp64", u64)
+    torch.cuda.synchronize()
+    w64 = rms_warpage(pkg.mesh, u64.cpu().numpy())
+    # ---- timed region (device-resident inputs)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    dm.time_kernel(DOMINANT)
+    l0 = launch_count()
+    recs = []
+    with Clocks(local) as ck:
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            recs.append(one(a.precision, u))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = launch_count() - l0
+    kcount, kms = dm.kernel_time()
+    dm.time_kernel(None)
+    ms = e0.elapsed_time(e1)
+    clocks = ck.summary()
+    wmix = rms_warpage(pkg.mesh, u.cpu().numpy())
+    iters = sum(r["iters"] for r in recs)
+    work = n * iters / 1e6
+    t = torch.tensor([ms / 1e3, work], dtype=torch.float64, device="cuda")
+    if world > 1:
+        tmax = t[:1].clone(); dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        wsum = t[1:].clone(); dist.all_reduce(wsum, op=dist.ReduceOp.SUM)
+        secs, work_all = float(tmax), float(wsum)
+    else:
+        secs, work_all = ms / 1e3, work
+    value = work_all / secs
+    # ---- end to end through the host API (pinned host buffers)
+    fh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    uh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True); e3 = torch.cuda.Event(enable_timing=True)
+    e2_iters = 0
+    e2.record(stream)
+    for _ in range(a.steps):
+        key[0] += 1
+        fh[:] = dm.assemble_step(step)
+        r = dm.solve(fh, key=key[0], tol=1e-8, warm=0, precision=a.precision)
+        uh[:] = r["u"]
+        e2_iters += r["iters"]
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = e2.elapsed_time(e3) / 1e3
+    t = torch.tensor([e2e_s, n * e2_iters / 1e6], dtype=torch.float64, device="cuda")
+    if world > 1:
+        tm_ = t[:1].clone(); dist.all_reduce(tm_, op=dist.ReduceOp.MAX)
+        ws_ = t[1:].clone(); dist.all_reduce(ws_, op=dist.ReduceOp.SUM)
+        e2e_val = float(ws_) / float(tm_)
+    else:
+        e2e_val = n * e2_iters / 1e6 / e2e_s
+    step_bytes = sum(getattr(step, k).nbytes for k in ("layered", "D", "s0", "W", "V", "born"))
+    # ---- roofline of the dominant kernel: level-0 column smoother, one colour per launch
+    nn = dm.nn
+    prec_bytes = 4 if a.precision == "mixed" else 8
+    # per full sweep (4 colours): operator rows 243 values + 27 neighbour ids + 18 factor values + b, x read, x write per node
+    sweep_bytes = nn * (243 * prec_bytes + 27 * 4 + 18 * prec_bytes + 3 * prec_bytes * 3)
+    per_launch = sweep_bytes / 4
+    hbm, hbm_kind = peaks()
+    achieved = per_launch / (kms / kcount / 1e3) / 1e9 if kcount else None
+    traffic = profile_traffic(DOMINANT, a.precision)
+    roof = {"kernel": "k_sweep_solid (level-0 z-column block-tridiagonal smoother, one colour)", "bound": "hbm", "achieved": achieved,
+            "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None, "traffic": traffic,
+            "peak_kind": hbm_kind, "launches_timed": kcount, "avg_launch_us": 1e3 * kms / kcount if kcount else None,
+            "algorithmic_bytes_per_launch": per_launch}
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 apply/smoother + f64 refinement" if a.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "dof": n, "precision": a.precision, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (1.3 GB level-0 operator)"},
+            "solve": {"iters_per_step": iters / a.steps, "solve_s": ms / 1e3 / a.steps, "refinements": recs[-1]["refinements"],
+                      "pc_ms": recs[-1]["pcMs"], "relres": recs[-1]["relres"], "fp64_iters": r64["iters"],
+                      "fp64_solve_s": r64["ms"] / 1e3, "rms_warpage_mm": wmix, "rms_warpage_rel_err_vs_fp64": abs(wmix / w64 - 1)},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(step_bytes + 8 * n), "d2h_bytes_per_step": int(16 * n)},
+            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+        }
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def profile_traffic(kernel, precision):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"k_sweep_solid_{precision}.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def main():
+    a = parse()
+    if a.profile:
+        run_profile(a)
+    elif a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

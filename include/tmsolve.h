@@ -94,15 +94,17 @@ typedef struct {
 
 #define TM_PC_MG 0
 #define TM_PC_JACOBI 1
-#define TM_PREC_FP64 0
-#define TM_PREC_MIXED 1
+#define TM_PREC_FP64 0       /* everything in FP64 */
+#define TM_PREC_MIXED 1      /* FP64 PCG (apply, residuals, dots); the whole V-cycle in FP32 except the FP64 coarsest solve */
+#define TM_PREC_MIXED_IR 2   /* FP64 iterative refinement of an FP32 MG-PCG (FP32 apply and V-cycle); on a sweep that
+                                fails to halve the FP64 residual it continues as TM_PREC_MIXED */
 
 typedef struct {
   double tol;                    /* relative residual in the scaled 2-norm (PCG_TOL 1e-8) */
   int32_t maxit;                 /* PCG_MAXIT 2000 */
   int32_t warm;                  /* stored solutions for the warm start (WARM_START_MAX 20), 0 = off */
   int32_t precond;               /* TM_PC_MG or TM_PC_JACOBI */
-  int32_t precision;             /* TM_PREC_FP64 or TM_PREC_MIXED */
+  int32_t precision;             /* TM_PREC_FP64, TM_PREC_MIXED or TM_PREC_MIXED_IR */
   int64_t key;                   /* preconditioner key (solve(f, label, key)); -1 = none */
   void (*progress)(void* user, int32_t it, double relres);  /* called between iterations, may be NULL */
   void* progress_user;
@@ -159,8 +161,31 @@ tm_status tm_destroy(tm_ctx* ctx);
 int32_t tm_last_error(char* buf, size_t len);
 
 /* ---- device-resident entry points (inputs and outputs already in device memory) ---- */
+/* tm_assemble_step with the load written to device memory (rhs_dev, 3*nn doubles, may be NULL). */
+tm_status tm_assemble_step_device(tm_ctx* ctx, const tm_step* step, double* rhs_dev);
 tm_status tm_solve_device(tm_ctx* ctx, const double* f_dev, double* u_dev, const tm_solve_opts* opts, tm_solve_info* info);
 tm_status tm_matvec_device(tm_ctx* ctx, const double* x_dev, double* y_dev);
+
+/* Runs the context's work on the caller's CUDA stream (a cudaStream_t) instead of its own
+ * (the N-API addon passes the stream of the thread's device context). */
+tm_status tm_set_stream(tm_ctx* ctx, void* stream);
+
+/* ---- measurement (no counterpart in the reference, whose timings are nowMs() stamps,
+ * src/core/11-analysis.js:192-203 and 10-solver.js:988) ---- */
+/* Number of kernels this library has launched since it was loaded. */
+int64_t tm_launch_count(void);
+/* Kernel classes that the event timer can bracket. */
+#define TM_K_APPLY0 0        /* level-0 stencil apply (fullMatVec) */
+#define TM_K_SWEEP_SOLID 1   /* level-0 column smoother sweep of one colour (columnSweep, solid) */
+#define TM_K_SWEEP_SHELL 2   /* shell-level column sweep of one colour (columnSweep, shell) */
+#define TM_K_ASSEMBLE 3      /* stencil assembly (assembleStep) */
+#define TM_K_GALERKIN01 4    /* Galerkin product solid -> shell (galerkinProduct) */
+#define TM_K_APPLY_SHELL 5   /* shell-level residual (blockMatVec, b = 6) */
+/* Brackets every following launch of one kernel class with CUDA events on the context's
+ * stream (kernel = -1 switches the timer off); tm_kernel_timer_read returns the launches and
+ * their summed device time since, and resets them. */
+tm_status tm_kernel_timer(tm_ctx* ctx, int32_t kernel);
+tm_status tm_kernel_timer_read(tm_ctx* ctx, int64_t* count, double* total_ms);
 
 /* ---- Anand viscoplastic return map (13-fatigue.js:13-237) ---- */
 typedef struct {

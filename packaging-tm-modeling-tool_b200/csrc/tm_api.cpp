@@ -30,10 +30,13 @@ void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw Error{TM_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
+long long launch_count();
+
 Context::~Context() {
   for (auto* L : shells) delete L;
   for (auto* b : basis) delete b;
-  if (stream) cudaStreamDestroy(stream);
+  for (auto& e : timerEvents) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  if (stream && ownStream) cudaStreamDestroy(stream);
 }
 
 namespace {
@@ -91,7 +94,13 @@ double build_pc(Context& c, bool mg) {
 }
 
 void precondition(Context& c, bool mg, const double* r, double* z) {
-  if (mg) launch_vcycle(c, r, z, false);
+  const size_t n = 3 * (size_t)c.nn;
+  if (mg && c.mgFp32) {
+    // FP32 V-cycle (operators, column factors, transfers and smoothing in FP32; coarsest FP64)
+    launch_d2f(c, r, c.d_r32.p, n);
+    launch_vcycle32(c, c.d_r32.p, c.d_z32.p);
+    launch_f2d(c, c.d_z32.p, z, n);
+  } else if (mg) launch_vcycle(c, r, z, false);
   else TM_CUDA_CHECK(cudaMemcpyAsync(z, r, 3 * (size_t)c.nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
 }
 
@@ -241,6 +250,95 @@ void store_solution(Context& c, const double* u_dev, int warmMax) {
   while ((int)c.basis.size() > warmMax) { delete c.basis.front(); c.basis.erase(c.basis.begin()); }
 }
 
+// FP32 PCG on K d = r32 from d = 0 (inner solve of the mixed-precision refinement): the
+// stiffness apply and the V-cycle run in FP32 with FP32 accumulation; dots accumulate in FP64.
+PcgResult pcg32(Context& c, double tol_in, int maxit) {
+  const size_t n = 3 * (size_t)c.nn;
+  double* S = c.d_scalars.p;
+  PcgResult out;
+  TM_CUDA_CHECK(cudaMemsetAsync(c.d_d32.p, 0, n * sizeof(float), c.stream));
+  const double r0n = std::sqrt([&] {
+    launch_dot32(c, c.d_r32.p, c.d_r32.p, n, S + 15);
+    double v = 0;
+    TM_CUDA_CHECK(cudaMemcpyAsync(&v, S + 15, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    return v;
+  }());
+  if (!(r0n > 0)) { out.converged = true; return out; }
+  launch_vcycle32(c, c.d_r32.p, c.d_z32.p);
+  launch_zero_constrained32(c, c.d_z32.p);
+  TM_CUDA_CHECK(cudaMemcpyAsync(c.d_p32.p, c.d_z32.p, n * sizeof(float), cudaMemcpyDeviceToDevice, c.stream));
+  launch_dot32(c, c.d_r32.p, c.d_z32.p, n, S + 0);
+  int it = 0;
+  double hs[4];
+  for (it = 1; it <= maxit; it++) {
+    launch_apply0_32(c, c.d_p32.p, c.d_q32.p, nullptr);
+    launch_dot32(c, c.d_p32.p, c.d_q32.p, n, S + 1);
+    launch_div(c, S + 0, S + 1, S + 2, 1.0);
+    launch_axpy2_32(c, S + 2, c.d_p32.p, c.d_d32.p, c.d_q32.p, c.d_r32.p, n);
+    launch_finalize(c, S + 3);
+    TM_CUDA_CHECK(cudaMemcpyAsync(hs, S, 4 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    if (!(hs[1] > 0)) {
+      double na = -hs[2];
+      TM_CUDA_CHECK(cudaMemcpyAsync(S + 2, &na, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+      launch_axpy2_32(c, S + 2, c.d_p32.p, c.d_d32.p, c.d_q32.p, c.d_r32.p, n);
+      if (!std::isfinite(hs[1])) out.nonfinite = true;
+      break;
+    }
+    const double rn = std::sqrt(hs[3]);
+    if (!std::isfinite(rn)) { out.nonfinite = true; break; }
+    out.relres = rn / r0n;
+    if (rn < tol_in * r0n) { out.iters = it; out.converged = true; return out; }
+    launch_vcycle32(c, c.d_r32.p, c.d_z32.p);
+    launch_zero_constrained32(c, c.d_z32.p);
+    launch_dot32(c, c.d_r32.p, c.d_z32.p, n, S + 4);
+    launch_div(c, S + 4, S + 0, S + 5, 1.0);
+    TM_CUDA_CHECK(cudaMemcpyAsync(S + 0, S + 4, sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    launch_xpby32(c, c.d_z32.p, S + 5, c.d_p32.p, n);
+  }
+  out.iters = std::min(it, maxit);
+  return out;
+}
+
+// TM_PREC_MIXED_IR: FP64 iterative refinement around an FP32 multigrid-PCG. Every sweep
+// recomputes the FP64 residual r = b - K x, solves K d = r in FP32 (FP32 apply and V-cycle) to a
+// relative 1e-4 and adds d to x in FP64. When a sweep fails to halve the FP64 residual (the
+// FP32 operator's rounding times the condition number reaches 1, as on finely meshed lidded
+// packages) *stalled is set and the caller continues with FP64 PCG and the FP32 V-cycle.
+PcgResult refine_mixed(Context& c, const double* b, double* x, double tol, int maxit, int* sweeps, bool* stalled, const tm_solve_opts& o) {
+  const size_t n = 3 * (size_t)c.nn;
+  PcgResult out;
+  launch_zero_constrained(c, x);
+  const double bnorm = std::sqrt(dot_host(c, b, b, n));
+  int total = 0;
+  *sweeps = 0;
+  *stalled = false;
+  double prev = 0;
+  for (int guard = 0; guard < 50; guard++) {
+    launch_apply0(c, x, c.d_r.p, b);
+    launch_zero_constrained(c, c.d_r.p);
+    const double rel = std::sqrt(dot_host(c, c.d_r.p, c.d_r.p, n)) / bnorm;
+    if (guard == 0) out.iters0 = rel;
+    out.relres = rel;
+    if (!std::isfinite(rel)) { out.nonfinite = true; break; }
+    if (rel < tol) { out.converged = true; break; }
+    if (guard > 0 && rel > 0.5 * prev) { *stalled = true; break; }
+    prev = rel;
+    if (total >= maxit) break;
+    launch_d2f(c, c.d_r.p, c.d_r32.p, n);
+    const double tol_in = std::max(1e-4, 0.3 * tol / rel);
+    PcgResult in = pcg32(c, tol_in, maxit - total);
+    total += in.iters;
+    if (in.nonfinite) { out.nonfinite = true; break; }
+    launch_add_f2d(c, c.d_d32.p, x, n);
+    (*sweeps)++;
+    if (o.progress && o.progress_every > 0) o.progress(o.progress_user, total, rel);
+  }
+  out.iters = total;
+  return out;
+}
+
 double pcg_rate(const PcgResult& r) { return r.iters / std::max(std::log10(r.iters0 / std::max(r.relres, 1e-300)), 0.5); }
 
 // LinearSolver.solve (10-solver.js:933-994) with f and u in device memory
@@ -254,7 +352,7 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   if (!c.scaled) {
     launch_scale(c);
     c.scaled = true;
-    c.pcReady = false;
+    c.fp32Ready = false;
   }
   launch_scale_rhs(c, f_dev, c.d_bs.p);
   const double bnorm = std::sqrt(dot_host(c, c.d_bs.p, c.d_bs.p, n));
@@ -271,8 +369,42 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   }
   bool rebuilt = false;
   double pcMs = 0;
-  if (!c.pcReady || c.needRebuild) { pcMs = build_pc(c, mg); rebuilt = true; }
+  const bool mixed = o.precision == TM_PREC_MIXED || o.precision == TM_PREC_MIXED_IR;
+  if (mixed && !mg) fail(TM_BAD_INPUT, "mixed precision needs the multigrid preconditioner");
+  c.mgFp32 = false;
+  if (!c.pcReady || c.needRebuild) {
+    pcMs = build_pc(c, mg);
+    rebuilt = true;
+    if (mixed) { const double t1 = now_ms(); launch_to_fp32(c); TM_CUDA_CHECK(cudaStreamSynchronize(c.stream)); pcMs += now_ms() - t1; c.fp32Ready = true; }
+  } else if (mixed && !c.fp32Ready) {
+    launch_to_fp32(c);
+    c.fp32Ready = true;
+  }
   warm_start(c, c.d_bs.p, c.d_x.p);
+  int sweeps = 0;
+  bool stalled = false;
+  if (o.precision == TM_PREC_MIXED_IR) {
+    PcgResult res = refine_mixed(c, c.d_bs.p, c.d_x.p, o.tol, o.maxit, &sweeps, &stalled, o);
+    if (stalled && !res.nonfinite) {
+      c.mgFp32 = true;
+      PcgResult r2 = pcg(c, mg, c.d_bs.p, c.d_x.p, o.tol, std::max(1, o.maxit - res.iters), 0, o);
+      r2.iters += res.iters;
+      r2.iters0 = res.iters0;
+      res = r2;
+    }
+    if (!res.converged) c.needRebuild = true;
+    launch_scale_vec(c, c.d_x.p, c.d_s.p, u_dev, false, n);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    if (res.converged) store_solution(c, u_dev, o.warm);
+    in.iters = res.iters; in.relres = res.relres; in.iters0 = res.iters0; in.converged = res.converged;
+    in.ms = now_ms() - t0; in.pc_ms = pcMs; in.rebuilt = rebuilt; in.warm = (int)c.basis.size();
+    in.jitter_count = c.colJitter; in.refinements = sweeps;
+    in.status = res.nonfinite ? TM_NONFINITE : (res.converged ? TM_OK : TM_NOT_CONVERGED);
+    if (info) *info = in;
+    if (res.nonfinite) fail(TM_NONFINITE, "non-finite value in the refinement");
+    return res.converged ? TM_OK : TM_NOT_CONVERGED;
+  }
+  c.mgFp32 = o.precision == TM_PREC_MIXED;
   PcgResult res = pcg(c, mg, c.d_bs.p, c.d_x.p, o.tol, o.maxit, rebuilt ? 0 : 2 * c.ratePerDecade, o);
   int total = res.iters;
   if (!res.converged && !rebuilt && !res.nonfinite) {
@@ -414,10 +546,19 @@ tm_status tm_assemble_step(tm_ctx* ctx, const tm_step* st, double* rhs_out) {
     launch_constraints(c);
     c.assembled = true;
     c.scaled = false;
-    c.pcReady = false;
     if (rhs_out) {
       c.d_rhs.download(rhs_out, 3 * (size_t)c.nn, c.stream);
     }
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_assemble_step_device(tm_ctx* ctx, const tm_step* st, double* rhs_dev) {
+  tm_status s = tm_assemble_step(ctx, st, nullptr);
+  if (s != TM_OK || !rhs_dev) return s;
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    TM_CUDA_CHECK(cudaMemcpyAsync(rhs_dev, c.d_rhs.p, 3 * (size_t)c.nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   });
 }
@@ -444,7 +585,6 @@ tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, co
     c.d_constr.upload(c.constr, c.stream);
     c.assembled = true;
     c.scaled = false;
-    c.pcReady = false;
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   });
 }
@@ -529,6 +669,47 @@ tm_status tm_solve(tm_ctx* ctx, const double* f, double* u, const tm_solve_opts*
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   });
   return g != TM_OK ? g : st;
+}
+
+tm_status tm_set_stream(tm_ctx* ctx, void* stream) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    if (c.ownStream && c.stream) cudaStreamDestroy(c.stream);
+    c.stream = reinterpret_cast<cudaStream_t>(stream);
+    c.ownStream = false;
+  });
+}
+
+int64_t tm_launch_count(void) { return (int64_t)launch_count(); }
+
+tm_status tm_kernel_timer(tm_ctx* ctx, int32_t kernel) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (kernel < -1 || kernel >= K_NKERNEL) fail(TM_BAD_INPUT, "unknown kernel id");
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    for (auto& e : c.timerEvents) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    c.timerEvents.clear();
+    c.timerKernel = kernel;
+  });
+}
+
+tm_status tm_kernel_timer_read(tm_ctx* ctx, int64_t* count, double* total_ms) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    double tot = 0;
+    for (auto& e : c.timerEvents) {
+      float ms = 0;
+      TM_CUDA_CHECK(cudaEventElapsedTime(&ms, e.first, e.second));
+      tot += ms;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    *count = (int64_t)c.timerEvents.size();
+    *total_ms = tot;
+    c.timerEvents.clear();
+  });
 }
 
 tm_status tm_anand_screen_device(const tm_anand_material* mat, int32_t nsites, int32_t ntemps, const double* temps, const double* table_dev,

@@ -434,6 +434,29 @@ void build_hierarchy(Context& c) {
   // ---- device upload of the structure
   cudaStream_t st = c.stream;
   color_lists(nx, ny, c.colStart, c.d_colorCols, c.colorCount, st);
+  // level-0 column panels: greedy packing of each colour's columns (in list order) into groups of
+  // at most panelCap nodes; a column longer than panelCap forms a group of its own
+  c.panelCap = std::max(128, c.maxColLen);
+  c.panelMaxCols = 0;
+  for (int k = 0; k < 4; k++) {
+    std::vector<int> cols;
+    for (int col = 0; col < nx * ny; col++) {
+      if (c.colStart[col + 1] == c.colStart[col]) continue;
+      if (((col / ny) & 1) * 2 + ((col % ny) & 1) == k) cols.push_back(col);
+    }
+    std::vector<int> gs{0};
+    int nodes = 0;
+    for (size_t q = 0; q < cols.size(); q++) {
+      const int len = c.colStart[cols[q] + 1] - c.colStart[cols[q]];
+      if (nodes > 0 && nodes + len > c.panelCap) { gs.push_back((int)q); nodes = 0; }
+      nodes += len;
+    }
+    gs.push_back((int)cols.size());
+    if (cols.empty()) gs.assign(1, 0);
+    for (size_t g = 0; g + 1 < gs.size(); g++) c.panelMaxCols = std::max(c.panelMaxCols, gs[g + 1] - gs[g]);
+    c.grpCount[k] = (int)gs.size() - 1;
+    c.d_grpStart[k].upload(gs, st);
+  }
   c.d_nodeAgg.upload(c.nodeAgg, st);
   c.d_aggStart.upload(c.aggStart, st);
   c.d_zp.upload(c.zp, st);
@@ -447,7 +470,10 @@ void build_hierarchy(Context& c) {
     L.d_val.alloc(36 * (size_t)L.nb);
     L.d_colStart.upload(L.colStart, st);
     L.d_cfPtr.upload(L.cfPtr, st);
-    if (!L.coarsest) L.d_cf.alloc((size_t)L.cfPtr.back());
+    if (!L.coarsest) {
+      L.d_cf.alloc((size_t)L.cfPtr.back());
+      L.d_cfInv.alloc((size_t)L.cfPtr.back());
+    }
     color_lists(L.nx, L.ny, L.colStart, L.d_colorCols, L.colorCount, st);
     if (l + 1 < c.shells.size()) {
       L.d_prolPtr.upload(L.prolPtr, st);

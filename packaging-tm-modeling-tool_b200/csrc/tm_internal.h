@@ -73,10 +73,11 @@ struct ShellLevel {
   DBuf<int> d_rowPtr, d_col;
   DBuf<double> d_val;                  // 36*nb
   DBuf<float> d_val32;                 // mixed precision copy
-  // dense per-column factors
+  // dense per-column factors and the explicit inverses of the column blocks
   std::vector<long long> cfPtr;        // ncol+1 (offsets in doubles)
   DBuf<long long> d_cfPtr;
-  DBuf<double> d_cf;
+  DBuf<double> d_cf, d_cfInv;
+  DBuf<float> d_cfInv32;
   DBuf<int> d_colStart;
   int maxm = 0;                        // largest column size in DOFs
   // colours: columns with (i%2, j%2) = colour, as lists
@@ -95,6 +96,7 @@ struct ShellLevel {
   int maxRowBlocks = 0;
   // work vectors
   DBuf<double> d_b, d_x, d_res;
+  DBuf<float> d_prolW32, d_b32, d_x32, d_res32;
   // coarsest level: banded factor and explicit inverse
   bool coarsest = false;
   int bandBw = 0, denseN = 0;
@@ -135,7 +137,7 @@ struct Context {
   DBuf<uint8_t> d_isC;
   std::vector<uint8_t> isC;
   int stage = 0;
-  bool assembled = false, scaled = false;
+  bool assembled = false, scaled = false, fp32Ready = false, mgFp32 = false;
   // solver state
   DBuf<double> d_s, d_f, d_bs, d_x, d_r, d_z, d_p, d_q, d_tmp, d_tmp2;
   DBuf<double> d_partial, d_scalars;
@@ -145,12 +147,24 @@ struct Context {
   DBuf<int> d_colorCols[4];
   int colorCount[4] = {0, 0, 0, 0};
   int maxColLen = 0;
+  // level-0 column panels: the columns of one colour packed into groups of at most panelCap nodes,
+  // one CTA per group (group g holds colour columns grpStart[g] .. grpStart[g+1]-1)
+  int panelCap = 128, panelMaxCols = 0;
+  DBuf<int> d_grpStart[4];
+  int grpCount[4] = {0, 0, 0, 0};
   std::vector<int> nodeAgg, aggStart;  // level 0 -> 1
   std::vector<double> zp;              // z of node minus zref of its aggregate
   DBuf<int> d_nodeAgg, d_aggStart;
   DBuf<double> d_zp, d_W01;            // 18 per node
   int maxRowBlocks1 = 0;
   DBuf<double> d_res0;                 // level-0 residual
+  DBuf<float> d_F32, d_W01_32, d_res0_32;
+  // FP32 inner solve of the mixed-precision refinement
+  DBuf<float> d_r32, d_z32, d_p32, d_q32, d_d32;
+  // caller stream, launch counter and the event timer of one kernel class
+  bool ownStream = true;
+  int timerKernel = -1;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timerEvents;
   std::vector<ShellLevel*> shells;     // levels 1..L-1
   bool hierarchy = false;
   bool pcReady = false;
@@ -183,6 +197,17 @@ void launch_factor_shell(Context& c, ShellLevel& L);
 void launch_factor_coarsest(Context& c, ShellLevel& L);
 void launch_to_fp32(Context& c);
 
+// ---- launch accounting ------------------------------------------------------------------------
+enum KernelId { K_APPLY0 = 0, K_SWEEP_SOLID = 1, K_SWEEP_SHELL = 2, K_ASSEMBLE = 3, K_GALERKIN01 = 4, K_APPLY_SHELL = 5, K_NKERNEL };
+void note_launch(int count = 1);
+struct TimedLaunch {   // brackets one launch with events when the context times this kernel class
+  Context& c;
+  bool on;
+  cudaEvent_t a = nullptr, b = nullptr;
+  TimedLaunch(Context& ctx, int kid);
+  ~TimedLaunch();
+};
+
 // ---- solve kernels (tm_solve.cu) -------------------------------------------------------------
 void launch_apply0(Context& c, const double* x, double* y, const double* b);   // y = K x, or b - K x when b != nullptr
 void launch_apply0_f32(Context& c, const double* x, double* y, const double* b);
@@ -191,6 +216,16 @@ void launch_axpy2(Context& c, const double* alpha_dev, const double* p, double* 
 void launch_xpby(Context& c, const double* z, const double* beta_dev, double* p, size_t n);
 void launch_zero_constrained(Context& c, double* v);
 void launch_vcycle(Context& c, const double* r, double* z, bool mixed);
+// FP32 inner solve of the mixed-precision path
+void launch_apply0_32(Context& c, const float* x, float* y, const float* b);
+void launch_dot32(Context& c, const float* a, const float* b, size_t n, double* out_dev);
+void launch_axpy2_32(Context& c, const double* alpha_dev, const float* p, float* x, const float* q, float* r, size_t n);
+void launch_xpby32(Context& c, const float* z, const double* beta_dev, float* p, size_t n);
+void launch_zero_constrained32(Context& c, float* v);
+void launch_vcycle32(Context& c, const float* r, float* z);
+void launch_d2f(Context& c, const double* a, float* b, size_t n);
+void launch_add_f2d(Context& c, const float* d, double* x, size_t n);
+void launch_f2d(Context& c, const float* a, double* b, size_t n);
 void launch_div(Context& c, const double* num, const double* den, double* out, double sign);
 void launch_scale_vec(Context& c, const double* x, const double* s, double* y, bool divide, size_t n);
 void launch_finalize(Context& c, double* out_dev);                                  // sum of the last reduction partials

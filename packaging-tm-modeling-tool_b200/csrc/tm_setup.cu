@@ -680,6 +680,124 @@ __global__ void k_coarsest_inverse(int n, int bw, const double* __restrict__ A, 
   }
 }
 
+// explicit inverse of every shell column block from its Cholesky factor (warp per column, lanes over
+// unit vectors); the smoother then applies A_cc^-1 as a dense product instead of two serial
+// triangular solves (cholSolveDenseOff, 10-solver.js:497-509, computes the same A_cc^-1 r)
+__global__ void k_shell_inverse(int ncol, const int* __restrict__ colStart, const long long* __restrict__ cfPtr,
+                                const double* __restrict__ cf, double* __restrict__ cfInv) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (c >= ncol) return;
+  const int m = 6 * (colStart[c + 1] - colStart[c]);
+  if (!m) return;
+  const double* L = cf + cfPtr[c];
+  double* X = cfInv + cfPtr[c];
+  for (int e = lane; e < m; e += 32) {
+    for (int i = 0; i < m; i++) {
+      double s = i == e ? 1.0 : 0.0;
+      for (int k = e; k < i; k++) s -= L[i * m + k] * X[k * m + e];
+      X[i * m + e] = i < e ? 0.0 : s / L[i * m + i];
+    }
+    for (int i = m - 1; i >= 0; i--) {
+      double s = X[i * m + e];
+      for (int k = i + 1; k < m; k++) s -= L[k * m + i] * X[k * m + e];
+      X[i * m + e] = s / L[i * m + i];
+    }
+  }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// banded Cholesky of the coarsest operator (factorCoarsest, 10-solver.js:562-600) in one block:
+// for each pivot, warp 0 reduces the pivot row and the 32 warps share the rows below it, each
+// row's dot product split over the lanes
+__global__ void k_factor_coarsest_par(int nnb, const int* __restrict__ rowPtr, const int* __restrict__ col, const double* __restrict__ val,
+                                      int n, int bw, double* __restrict__ A, int* __restrict__ jitterCount) {
+  const int w = bw + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __shared__ double s_inv;
+  __shared__ double s_red[32];
+  for (size_t e = threadIdx.x; e < (size_t)n * w; e += blockDim.x) A[e] = 0;
+  __syncthreads();
+  for (int i = 0; i < nnb; i++)
+    for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+      const int j = col[k];
+      if (j > i) continue;
+      for (int e = threadIdx.x; e < 36; e += blockDim.x) {
+        const int p = e / 6, q = e % 6;
+        const int r = 6 * i + p, cc = 6 * j + q;
+        if (cc <= r) A[(size_t)r * w + (cc - r + bw)] = val[36 * (size_t)k + e];
+      }
+    }
+  __syncthreads();
+  double dm = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dm = fmax(dm, fabs(A[(size_t)i * w + bw]));
+  for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+  if (lane == 0) s_red[warp] = dm;
+  __syncthreads();
+  double dmax = 0;
+  for (int q = 0; q < nw; q++) dmax = fmax(dmax, s_red[q]);
+  const double jitter = 1e-12 * (dmax != 0 ? dmax : 1);
+  int fixes = 0;
+  for (int j = 0; j < n; j++) {
+    const int k0 = max(0, j - bw);
+    if (warp == 0) {
+      double ss = 0;
+      for (int k = k0 + lane; k < j; k += 32) { const double l = A[(size_t)j * w + (k - j + bw)]; ss += l * l; }
+      ss = warp_sum(ss);
+      if (lane == 0) {
+        double d = A[(size_t)j * w + bw] - ss;
+        if (!(d > jitter)) { d = fmax(fabs(d), jitter); fixes++; }
+        const double ljj = sqrt(d);
+        A[(size_t)j * w + bw] = ljj;
+        s_inv = 1 / ljj;
+      }
+    }
+    __syncthreads();
+    const double inv = s_inv;
+    const int iend = min(n, j + bw + 1);
+    for (int i = j + 1 + warp; i < iend; i += nw) {
+      const int kk0 = max(k0, i - bw);
+      double ss = 0;
+      for (int k = kk0 + lane; k < j; k += 32) ss += A[(size_t)i * w + (k - i + bw)] * A[(size_t)j * w + (k - j + bw)];
+      ss = warp_sum(ss);
+      if (lane == 0) A[(size_t)i * w + (j - i + bw)] = (A[(size_t)i * w + (j - i + bw)] - ss) * inv;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && fixes) atomicAdd(jitterCount, fixes);
+}
+
+// explicit inverse of the coarsest operator from its banded factor: warp per unit vector e_c, the
+// result row c (the inverse is symmetric) doubling as the work vector of the two substitutions
+__global__ void k_coarsest_inverse_par(int n, int bw, const double* __restrict__ A, double* __restrict__ inv) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (c >= n) return;
+  const int w = bw + 1;
+  double* y = inv + (size_t)c * n;
+  for (int i = lane; i < c; i += 32) y[i] = 0;
+  __syncwarp();
+  for (int i = c; i < n; i++) {
+    double ss = 0;
+    for (int k = max(c, i - bw) + lane; k < i; k += 32) ss += A[(size_t)i * w + (k - i + bw)] * y[k];
+    ss = warp_sum(ss);
+    if (lane == 0) y[i] = ((i == c ? 1.0 : 0.0) - ss) / A[(size_t)i * w + bw];
+    __syncwarp();
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    double ss = 0;
+    const int kend = min(n, i + bw + 1);
+    for (int k = i + 1 + lane; k < kend; k += 32) ss += A[(size_t)k * w + (i - k + bw)] * y[k];
+    ss = warp_sum(ss);
+    if (lane == 0) y[i] = (y[i] - ss) / A[(size_t)i * w + bw];
+    __syncwarp();
+  }
+}
+
 __global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i < n) b[i] = (float)a[i];
@@ -717,6 +835,7 @@ void launch_class_condense(Context& c) {
   const int warps = 2;
   const size_t smem = (size_t)warps * 2048 * sizeof(double);
   TM_CUDA_CHECK(cudaFuncSetAttribute(k_class_condense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  note_launch();
   k_class_condense<<<grid_for(c.ncls, warps), 32 * warps, smem, c.stream>>>(c.ncls, c.d_clsPset.p, c.d_clsH.p, c.d_psetM.p, c.d_clsF33.p,
                                                                           c.d_clsBorn.p, c.d_clsKc.p, c.d_clsFc.p);
   TM_CUDA_CHECK(cudaGetLastError());
@@ -726,8 +845,12 @@ void launch_assemble(Context& c) {
   const size_t tot = (size_t)NSLOT * c.nn;
   c.d_val.alloc(tot * 9);
   c.d_rhs.alloc(3 * (size_t)c.nn);
+  note_launch(2);
+  {
+  TimedLaunch tl(c, K_ASSEMBLE);
   k_assemble<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_nodeIJK.p, c.d_nbr.p, c.d_cellElems.p, c.d_eClass.p,
                                                       c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsKc.p, c.d_val.p);
+  }
   TM_CUDA_CHECK(cudaGetLastError());
   k_assemble_rhs<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_nodeIJK.p, c.d_cellElems.p, c.d_eClass.p,
                                                            c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsBorn.p,
@@ -740,6 +863,7 @@ void launch_constraints(Context& c) {
   c.d_isC.zero(c.stream);
   DBuf<int> d;
   d.upload(c.constr, c.stream);
+  note_launch();
   k_constraints<<<1, 1, 0, c.stream>>>(c.nn, (int)c.constr.size(), d.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
   TM_CUDA_CHECK(cudaGetLastError());
   TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
@@ -749,6 +873,7 @@ void launch_constraints(Context& c) {
 
 void launch_scale(Context& c) {
   c.d_s.alloc(3 * (size_t)c.nn);
+  note_launch(2);
   k_scale_diag<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.d_val.p, c.d_s.p);
   const size_t tot = (size_t)NSLOT * c.nn;
   k_scale_val<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_s.p, c.d_val.p);
@@ -757,6 +882,7 @@ void launch_scale(Context& c) {
 
 void launch_scale_rhs(Context& c, const double* f, double* bs) {
   const size_t n = 3 * (size_t)c.nn;
+  note_launch();
   k_mul<<<grid_for(n, 256), 256, 0, c.stream>>>(n, f, c.d_s.p, bs);
   TM_CUDA_CHECK(cudaGetLastError());
 }
@@ -764,12 +890,14 @@ void launch_scale_rhs(Context& c, const double* f, double* bs) {
 void launch_factor_columns(Context& c) {
   const int ncol = c.nx * c.ny;
   c.d_F.zero(c.stream);
+  note_launch();
   k_factor_columns<<<grid_for(ncol, 128), 128, 0, c.stream>>>(ncol, c.nn, c.d_colStart.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p,
                                                              c.d_F.p, c.d_jitter.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_w01(Context& c) {
+  note_launch();
   k_w01<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.d_s.p, c.d_zp.p, c.d_W01.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
@@ -779,6 +907,8 @@ void launch_galerkin01(Context& c) {
   const int warps = 4;
   const size_t smem = (size_t)warps * L1.maxRowBlocks * 36 * sizeof(double);
   TM_CUDA_CHECK(cudaFuncSetAttribute(k_galerkin01, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  note_launch();
+  TimedLaunch tl(c, K_GALERKIN01);
   k_galerkin01<<<grid_for(L1.nn, warps), 32 * warps, smem, c.stream>>>(L1.nn, c.nn, c.d_aggStart.p, c.d_nodeAgg.p, c.d_nbr.p, c.d_slotMask.p,
                                                                       c.d_val.p, c.d_W01.p, L1.d_rowPtr.p, L1.d_col.p, L1.maxRowBlocks,
                                                                       L1.d_val.p);
@@ -791,6 +921,7 @@ void launch_galerkin_shell(Context& c, int l) {
   const int warps = 4;
   const size_t smem = (size_t)warps * C.maxRowBlocks * 36 * sizeof(double);
   TM_CUDA_CHECK(cudaFuncSetAttribute(k_galerkin_shell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  note_launch();
   k_galerkin_shell<<<grid_for(C.nn, warps), 32 * warps, smem, c.stream>>>(C.nn, F.d_chPtr.p, F.d_chIdx.p, F.d_chW.p, F.d_rowPtr.p, F.d_col.p,
                                                                          F.d_val.p, F.d_prolPtr.p, F.d_prolIdx.p, F.d_prolW.p, C.d_rowPtr.p,
                                                                          C.d_col.p, C.maxRowBlocks, C.d_val.p);
@@ -800,29 +931,43 @@ void launch_galerkin_shell(Context& c, int l) {
 void launch_factor_shell(Context& c, ShellLevel& L) {
   const int ncol = L.nx * L.ny;
   const int warps = 4;
+  note_launch();
   k_factor_shell<<<grid_for(ncol, warps), 32 * warps, 0, c.stream>>>(ncol, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_cfPtr.p,
                                                                     L.d_cf.p, c.d_jitter.p);
+  note_launch();
+  k_shell_inverse<<<grid_for(ncol, warps), 32 * warps, 0, c.stream>>>(ncol, L.d_colStart.p, L.d_cfPtr.p, L.d_cf.p, L.d_cfInv.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_factor_coarsest(Context& c, ShellLevel& L) {
-  k_factor_coarsest<<<1, 1024, 0, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
+  note_launch(2);
+  k_factor_coarsest_par<<<1, 1024, 0, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
   TM_CUDA_CHECK(cudaGetLastError());
-  k_coarsest_inverse<<<grid_for(L.denseN, 64), 64, 0, c.stream>>>(L.denseN, L.bandBw, L.d_band.p, L.d_inv.p);
+  k_coarsest_inverse_par<<<grid_for(L.denseN, 4), 128, 0, c.stream>>>(L.denseN, L.bandBw, L.d_band.p, L.d_inv.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
+// FP32 copies for the mixed-precision inner solve: operators, column factors and transfer weights
+// (the coarsest level keeps its FP64 inverse)
 void launch_to_fp32(Context& c) {
-  const size_t n0 = c.d_val.n;
-  c.d_val32.alloc(n0);
-  k_to_f32<<<grid_for(n0, 256), 256, 0, c.stream>>>(n0, c.d_val.p, c.d_val32.p);
+  auto conv = [&](const DBuf<double>& a, DBuf<float>& b) {
+    b.alloc(a.n);
+    if (a.n) { k_to_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.p, b.p); note_launch(); }
+  };
+  conv(c.d_val, c.d_val32);
+  conv(c.d_F, c.d_F32);
+  conv(c.d_W01, c.d_W01_32);
+  c.d_res0_32.alloc(3 * (size_t)c.nn);
+  for (auto* r : {&c.d_r32, &c.d_z32, &c.d_p32, &c.d_q32, &c.d_d32}) r->alloc(3 * (size_t)c.nn);
   for (auto* L : c.shells) {
-    L->d_val32.alloc(L->d_val.n);
-    k_to_f32<<<grid_for(L->d_val.n, 256), 256, 0, c.stream>>>(L->d_val.n, L->d_val.p, L->d_val32.p);
     if (L->coarsest) {
-      L->d_inv32.alloc(L->d_inv.n);
-      k_to_f32<<<grid_for(L->d_inv.n, 256), 256, 0, c.stream>>>(L->d_inv.n, L->d_inv.p, L->d_inv32.p);
+      L->d_b32.alloc(6 * (size_t)L->nn); L->d_x32.alloc(6 * (size_t)L->nn);
+      continue;
     }
+    conv(L->d_val, L->d_val32);
+    conv(L->d_cfInv, L->d_cfInv32);
+    conv(L->d_prolW, L->d_prolW32);
+    L->d_b32.alloc(6 * (size_t)L->nn); L->d_x32.alloc(6 * (size_t)L->nn); L->d_res32.alloc(6 * (size_t)L->nn);
   }
   TM_CUDA_CHECK(cudaGetLastError());
 }

@@ -184,6 +184,102 @@ __global__ void k_sweep_solid(int ncolc, const int* __restrict__ cols, const int
   for (int e = lane; e < 3 * len; e += 32) x[3 * (size_t)n0 + e] += r[e];
 }
 
+// level-0 column smoother on packed column panels: one CTA per group of whole z-columns of one
+// colour (at most cap nodes). Every thread computes the residual rows of one node (coalesced
+// along each column's contiguous nodes), the column factors are staged in shared memory, one
+// thread per column runs the block-tridiagonal forward/backward solve (solveColumn,
+// 10-solver.js:71-104), and every node is then updated, x += dx.
+template <class T>
+__global__ void __launch_bounds__(128) k_sweep_panel(const int* __restrict__ grpStart, const int* __restrict__ cols,
+                                                      const int* __restrict__ colStart, int nn, const int* __restrict__ nbr,
+                                                      const T* __restrict__ val, const T* __restrict__ F, const T* __restrict__ b,
+                                                      T* __restrict__ x, int cap, int maxCols, int zeroGuess) {
+  extern __shared__ unsigned char smraw[];
+  T* r = reinterpret_cast<T*>(smraw);            // 3*cap
+  T* Fs = r + 3 * cap;                           // 18*cap
+  int* off = reinterpret_cast<int*>(Fs + 18 * cap);   // maxCols+1 node offsets of the columns in the group
+  int* first = off + maxCols + 1;                // first global node of every column
+  const int g0 = grpStart[blockIdx.x], ncols = grpStart[blockIdx.x + 1] - g0;
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int q = 0; q < ncols; q++) {
+      const int c = cols[g0 + q];
+      off[q] = o;
+      first[q] = colStart[c];
+      o += colStart[c + 1] - colStart[c];
+    }
+    off[ncols] = o;
+  }
+  __syncthreads();
+  const int total = off[ncols];
+  // stage the column factors (each column's 18*len values are contiguous)
+  for (int q = 0; q < ncols; q++) {
+    const int len = off[q + 1] - off[q];
+    const T* src = F + 18 * (size_t)first[q];
+    T* dst = Fs + 18 * off[q];
+    for (int e = threadIdx.x; e < 18 * len; e += blockDim.x) dst[e] = src[e];
+  }
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int q = 0;
+    while (off[q + 1] <= t) q++;
+    const int n = first[q] + (t - off[q]);
+    T s0 = b[3 * (size_t)n], s1 = b[3 * (size_t)n + 1], s2 = b[3 * (size_t)n + 2];
+    if (!zeroGuess) {
+#pragma unroll 3
+      for (int s = 0; s < NSLOT; s++) {
+        const int j = nbr[(size_t)s * nn + n];
+        if (j < 0) continue;
+        const T x0 = x[3 * (size_t)j], x1 = x[3 * (size_t)j + 1], x2 = x[3 * (size_t)j + 2];
+        const T* v = val + (size_t)s * 9 * nn + n;
+        s0 -= v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
+        s1 -= v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
+        s2 -= v[6 * (size_t)nn] * x0 + v[7 * (size_t)nn] * x1 + v[8 * (size_t)nn] * x2;
+      }
+    }
+    r[3 * t] = s0; r[3 * t + 1] = s1; r[3 * t + 2] = s2;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < ncols; q += blockDim.x) {
+    const int l0 = off[q], l1 = off[q + 1];
+    for (int l = l0; l < l1; l++) {
+      const T* f = Fs + 18 * l;
+      T b0 = r[3 * l], b1 = r[3 * l + 1], b2 = r[3 * l + 2];
+      if (l > l0) {
+        const T p0 = r[3 * l - 3], p1 = r[3 * l - 2], p2 = r[3 * l - 1];
+        b0 -= f[9] * p0 + f[10] * p1 + f[11] * p2;
+        b1 -= f[12] * p0 + f[13] * p1 + f[14] * p2;
+        b2 -= f[15] * p0 + f[16] * p1 + f[17] * p2;
+      }
+      const T y0 = b0 / f[0];
+      const T y1 = (b1 - f[3] * y0) / f[4];
+      const T y2 = (b2 - f[6] * y0 - f[7] * y1) / f[8];
+      r[3 * l] = y0; r[3 * l + 1] = y1; r[3 * l + 2] = y2;
+    }
+    for (int l = l1 - 1; l >= l0; l--) {
+      const T* f = Fs + 18 * l;
+      T b0 = r[3 * l], b1 = r[3 * l + 1], b2 = r[3 * l + 2];
+      if (l + 1 < l1) {
+        const T* gg = Fs + 18 * (l + 1);
+        const T q0 = r[3 * l + 3], q1 = r[3 * l + 4], q2 = r[3 * l + 5];
+        b0 -= gg[9] * q0 + gg[12] * q1 + gg[15] * q2;
+        b1 -= gg[10] * q0 + gg[13] * q1 + gg[16] * q2;
+        b2 -= gg[11] * q0 + gg[14] * q1 + gg[17] * q2;
+      }
+      const T z2 = b2 / f[8];
+      const T z1 = (b1 - f[7] * z2) / f[4];
+      const T z0 = (b0 - f[3] * z1 - f[6] * z2) / f[0];
+      r[3 * l] = z0; r[3 * l + 1] = z1; r[3 * l + 2] = z2;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int q = 0;
+    while (off[q + 1] <= t) q++;
+    const size_t n = first[q] + (t - off[q]);
+    x[3 * n] += r[3 * t]; x[3 * n + 1] += r[3 * t + 1]; x[3 * n + 2] += r[3 * t + 2];
+  }
+}
+
 // restriction 0 -> 1: rc = P^T res, thread per aggregate (children are a contiguous node range)
 template <class T>
 __global__ void k_restrict0(int na, const int* __restrict__ aggStart, const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc) {
@@ -258,22 +354,14 @@ __global__ void k_sweep_shell(int ncolc, const int* __restrict__ cols, const int
     r[e] = s;
   }
   __syncwarp();
-  const T* L = cf + cfPtr[c];
-  for (int j = 0; j < m; j++) {
-    if (lane == 0) r[j] = r[j] / L[j * m + j];
-    __syncwarp();
-    const T xj = r[j];
-    for (int i = j + 1 + lane; i < m; i += 32) r[i] -= L[i * m + j] * xj;
-    __syncwarp();
+  // x_col += A_cc^-1 r_col with the explicit inverse of the column block (row e per lane)
+  const T* Ai = cf + cfPtr[c];
+  for (int e = lane; e < m; e += 32) {
+    T acc = 0;
+    const T* row = Ai + (size_t)e * m;
+    for (int k = 0; k < m; k++) acc += row[k] * r[k];
+    x[6 * (size_t)n0 + e] += acc;
   }
-  for (int j = m - 1; j >= 0; j--) {
-    if (lane == 0) r[j] = r[j] / L[j * m + j];
-    __syncwarp();
-    const T xj = r[j];
-    for (int i = lane; i < j; i += 32) r[i] -= L[j * m + i] * xj;
-    __syncwarp();
-  }
-  for (int e = lane; e < m; e += 32) x[6 * (size_t)n0 + e] += r[e];
 }
 
 // shell restriction: rc = P^T res (children lists, transposeProl order)
@@ -331,133 +419,276 @@ __global__ void k_div_scalar(size_t n, double* __restrict__ v, double d) {
   if (i < n) v[i] /= d;
 }
 
+template <class A, class B>
+__global__ void k_convert(size_t n, const A* __restrict__ a, B* __restrict__ b) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (B)a[i];
+}
+
+__global__ void k_add_f2d(size_t n, const float* __restrict__ d, double* __restrict__ x) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) x[i] += (double)d[i];
+}
+
+// buffers of one precision of the V-cycle
+template <class T>
+struct Bufs;
+template <>
+struct Bufs<double> {
+  static const double* val0(Context& c) { return c.d_val.p; }
+  static const double* F(Context& c) { return c.d_F.p; }
+  static const double* W01(Context& c) { return c.d_W01.p; }
+  static double* res0(Context& c) { return c.d_res0.p; }
+  static const double* val(ShellLevel& L) { return L.d_val.p; }
+  static const double* cf(ShellLevel& L) { return L.d_cfInv.p; }
+  static const double* prolW(ShellLevel& L) { return L.d_prolW.p; }
+  static double* b(ShellLevel& L) { return L.d_b.p; }
+  static double* x(ShellLevel& L) { return L.d_x.p; }
+  static double* res(ShellLevel& L) { return L.d_res.p; }
+};
+template <>
+struct Bufs<float> {
+  static const float* val0(Context& c) { return c.d_val32.p; }
+  static const float* F(Context& c) { return c.d_F32.p; }
+  static const float* W01(Context& c) { return c.d_W01_32.p; }
+  static float* res0(Context& c) { return c.d_res0_32.p; }
+  static const float* val(ShellLevel& L) { return L.d_val32.p; }
+  static const float* cf(ShellLevel& L) { return L.d_cfInv32.p; }
+  static const float* prolW(ShellLevel& L) { return L.d_prolW32.p; }
+  static float* b(ShellLevel& L) { return L.d_b32.p; }
+  static float* x(ShellLevel& L) { return L.d_x32.p; }
+  static float* res(ShellLevel& L) { return L.d_res32.p; }
+};
+
+// MultigridPC._cycleOnce (10-solver.js:687-712) with zero initial guess on every level
+template <class T>
+void vcycle(Context& c, const T* r, T* z) {
+  typedef Bufs<T> B;
+  cudaStream_t st = c.stream;
+  const int nn = c.nn;
+  const int warps = 4;
+  const size_t smem0 = (size_t)21 * c.panelCap * sizeof(T) + 2 * (size_t)(c.panelMaxCols + 1) * sizeof(int);
+  TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(T), st));
+  if (smem0 > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
+  auto sweep0 = [&](int col, int zero) {
+    if (!c.grpCount[col]) return;
+    TimedLaunch tl(c, K_SWEEP_SOLID);
+    k_sweep_panel<T><<<c.grpCount[col], 128, smem0, st>>>(c.d_grpStart[col].p, c.d_colorCols[col].p, c.d_colStart.p, nn, c.d_nbr.p,
+                                                         B::val0(c), B::F(c), r, z, c.panelCap, c.panelMaxCols, zero);
+    note_launch();
+  };
+  auto sweepS = [&](ShellLevel& L, int col, int zero) {
+    const size_t smem = (size_t)warps * L.maxm * sizeof(T);
+    TimedLaunch tl(c, K_SWEEP_SHELL);
+    k_sweep_shell<T><<<grid_for(L.colorCount[col], warps), 32 * warps, smem, st>>>(
+        L.colorCount[col], L.d_colorCols[col].p, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, B::val(L), L.d_cfPtr.p, B::cf(L), B::b(L),
+        B::x(L), L.maxm, zero);
+    note_launch();
+  };
+  // ---- level 0 pre-smoothing: 2 sweeps in colours 0..3
+  bool first = true;
+  for (int sw = 0; sw < 2; sw++)
+    for (int col = 0; col < 4; col++) {
+      if (!c.colorCount[col]) continue;
+      sweep0(col, first ? 1 : 0);
+      first = false;
+    }
+  {
+    TimedLaunch tl(c, K_APPLY0);
+    k_apply0<T, T><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_nbr.p, B::val0(c), z, B::res0(c), r);
+    note_launch();
+  }
+  ShellLevel& L1 = *c.shells[0];
+  k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, B::W01(c), B::res0(c), B::b(L1));
+  note_launch();
+  const size_t nl = c.shells.size();
+  for (size_t l = 0; l < nl; l++) {
+    ShellLevel& L = *c.shells[l];
+    if (L.coarsest) {
+      // coarsest-grid direct solve in FP64 whatever the precision of the cycle
+      k_dense_apply<T, double><<<grid_for(L.denseN, 4), 128, 0, st>>>(L.denseN, L.d_inv.p, B::b(L), B::x(L));
+      note_launch();
+      break;
+    }
+    TM_CUDA_CHECK(cudaMemsetAsync(B::x(L), 0, 6 * (size_t)L.nn * sizeof(T), st));
+    bool firstS = true;
+    for (int sw = 0; sw < 2; sw++)
+      for (int col = 0; col < 4; col++) {
+        if (!L.colorCount[col]) continue;
+        sweepS(L, col, firstS ? 1 : 0);
+        firstS = false;
+      }
+    {
+      TimedLaunch tl(c, K_APPLY_SHELL);
+      k_apply_shell<T><<<grid_for(6 * (size_t)L.nn, 128), 128, 0, st>>>(L.nn, L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L));
+      note_launch();
+    }
+    ShellLevel& C = *c.shells[l + 1];
+    k_restrict_shell<T><<<grid_for(6 * (size_t)C.nn, 128), 128, 0, st>>>(C.nn, L.d_chPtr.p, L.d_chIdx.p, L.d_chW.p, B::prolW(L), B::res(L), B::b(C));
+    note_launch();
+  }
+  for (int l = (int)nl - 2; l >= 0; l--) {
+    ShellLevel& L = *c.shells[l];
+    ShellLevel& C = *c.shells[l + 1];
+    k_prolong_shell<T><<<grid_for(6 * (size_t)L.nn, 128), 128, 0, st>>>(L.nn, L.d_prolPtr.p, L.d_prolIdx.p, B::prolW(L), B::x(C), B::x(L));
+    note_launch();
+    for (int sw = 0; sw < 2; sw++)
+      for (int col = 3; col >= 0; col--)
+        if (L.colorCount[col]) sweepS(L, col, 0);
+  }
+  // ---- level 0: prolongation and post-smoothing, colours 3..0
+  k_prolong0<T><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_nodeAgg.p, B::W01(c), B::x(L1), z);
+  note_launch();
+  for (int sw = 0; sw < 2; sw++)
+    for (int col = 3; col >= 0; col--)
+      if (c.colorCount[col]) sweep0(col, 0);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
 }  // namespace
 
+// ---- launch accounting and event timers ----------------------------------------------------------
+static long long g_launches = 0;
+void note_launch(int count) { __atomic_fetch_add(&g_launches, (long long)count, __ATOMIC_RELAXED); }
+long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+TimedLaunch::TimedLaunch(Context& ctx, int kid) : c(ctx), on(ctx.timerKernel == kid) {
+  if (!on) return;
+  TM_CUDA_CHECK(cudaEventCreate(&a));
+  TM_CUDA_CHECK(cudaEventCreate(&b));
+  TM_CUDA_CHECK(cudaEventRecord(a, c.stream));
+}
+TimedLaunch::~TimedLaunch() {
+  if (!on) return;
+  cudaEventRecord(b, c.stream);
+  c.timerEvents.emplace_back(a, b);
+}
+
 void launch_apply0(Context& c, const double* x, double* y, const double* b) {
+  TimedLaunch tl(c, K_APPLY0);
   k_apply0<double, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val.p, x, y, b);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_apply0_f32(Context& c, const double* x, double* y, const double* b) {
   k_apply0<float, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val32.p, x, y, b);
+  note_launch();
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_apply0_32(Context& c, const float* x, float* y, const float* b) {
+  TimedLaunch tl(c, K_APPLY0);
+  k_apply0<float, float><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val32.p, x, y, b);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_dot(Context& c, const double* a, const double* b, size_t n, double* out_dev) {
   k_dot_partial<double><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, a, b, c.d_partial.p);
   k_reduce_final<<<1, 1024, 0, c.stream>>>(RED_BLOCKS, c.d_partial.p, out_dev);
+  note_launch(2);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_dot32(Context& c, const float* a, const float* b, size_t n, double* out_dev) {
+  k_dot_partial<float><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, a, b, c.d_partial.p);
+  k_reduce_final<<<1, 1024, 0, c.stream>>>(RED_BLOCKS, c.d_partial.p, out_dev);
+  note_launch(2);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_finalize(Context& c, double* out_dev) {
   k_reduce_final<<<1, 1024, 0, c.stream>>>(RED_BLOCKS, c.d_partial.p, out_dev);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_axpy(Context& c, double alpha, const double* x, double* y, size_t n) {
   k_axpy_scalar<<<grid_for(n, 256), 256, 0, c.stream>>>(n, alpha, x, y);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_div_scalar(Context& c, double* v, double d, size_t n) {
   k_div_scalar<<<grid_for(n, 256), 256, 0, c.stream>>>(n, v, d);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_axpy2(Context& c, const double* alpha_dev, const double* p, double* x, const double* q, double* r, size_t n) {
   k_axpy2<double><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, alpha_dev, p, x, q, r, c.d_partial.p);
+  note_launch();
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_axpy2_32(Context& c, const double* alpha_dev, const float* p, float* x, const float* q, float* r, size_t n) {
+  k_axpy2<float><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, alpha_dev, p, x, q, r, c.d_partial.p);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_xpby(Context& c, const double* z, const double* beta_dev, double* p, size_t n) {
   k_xpby<double><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, z, beta_dev, p);
+  note_launch();
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_xpby32(Context& c, const float* z, const double* beta_dev, float* p, size_t n) {
+  k_xpby<float><<<RED_BLOCKS, RED_THREADS, 0, c.stream>>>(n, z, beta_dev, p);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_div(Context& c, const double* num, const double* den, double* out, double sign) {
   k_div<<<1, 32, 0, c.stream>>>(num, den, out, sign);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_zero_constrained(Context& c, double* v) {
   if (c.constr.empty()) return;
   k_zero_list<double><<<grid_for(c.constr.size(), 128), 128, 0, c.stream>>>((int)c.constr.size(), c.d_constr.p, v);
+  note_launch();
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_zero_constrained32(Context& c, float* v) {
+  if (c.constr.empty()) return;
+  k_zero_list<float><<<grid_for(c.constr.size(), 128), 128, 0, c.stream>>>((int)c.constr.size(), c.d_constr.p, v);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_scale_vec(Context& c, const double* x, const double* s, double* y, bool divide, size_t n) {
   k_scale_vec<double><<<grid_for(n, 256), 256, 0, c.stream>>>(n, x, s, y, divide ? 1 : 0);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
-// MultigridPC._cycleOnce (10-solver.js:687-712) with zero initial guess on every level
-void launch_vcycle(Context& c, const double* r, double* z, bool mixed) {
-  (void)mixed;
-  cudaStream_t st = c.stream;
-  const int nn = c.nn;
-  // ---- level 0: pre-smoothing, 2 sweeps in colours 0..3
-  TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(double), st));
-  const int warps = 4;
-  const size_t smem0 = (size_t)warps * 21 * c.maxColLen * sizeof(double);
-  bool first = true;
-  for (int sweep = 0; sweep < 2; sweep++)
-    for (int col = 0; col < 4; col++) {
-      if (!c.colorCount[col]) continue;
-      k_sweep_solid<double><<<grid_for(c.colorCount[col], warps), 32 * warps, smem0, st>>>(
-          c.colorCount[col], c.d_colorCols[col].p, c.d_colStart.p, nn, c.d_nbr.p, c.d_val.p, c.d_F.p, r, z, c.maxColLen, first ? 1 : 0);
-      first = false;
-    }
-  // residual and restriction
-  k_apply0<double, double><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_nbr.p, c.d_val.p, z, c.d_res0.p, r);
-  ShellLevel& L1 = *c.shells[0];
-  k_restrict0<double><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, c.d_W01.p, c.d_res0.p, L1.d_b.p);
-  // ---- shell levels down
-  const size_t nl = c.shells.size();
-  for (size_t l = 0; l < nl; l++) {
-    ShellLevel& L = *c.shells[l];
-    if (L.coarsest) {
-      k_dense_apply<double, double><<<grid_for(L.denseN, 4), 128, 0, st>>>(L.denseN, L.d_inv.p, L.d_b.p, L.d_x.p);
-      break;
-    }
-    TM_CUDA_CHECK(cudaMemsetAsync(L.d_x.p, 0, 6 * (size_t)L.nn * sizeof(double), st));
-    const size_t smem = (size_t)warps * L.maxm * sizeof(double);
-    bool firstS = true;
-    for (int sweep = 0; sweep < 2; sweep++)
-      for (int col = 0; col < 4; col++) {
-        if (!L.colorCount[col]) continue;
-        k_sweep_shell<double><<<grid_for(L.colorCount[col], warps), 32 * warps, smem, st>>>(
-            L.colorCount[col], L.d_colorCols[col].p, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_cfPtr.p, L.d_cf.p, L.d_b.p,
-            L.d_x.p, L.maxm, firstS ? 1 : 0);
-        firstS = false;
-      }
-    k_apply_shell<double><<<grid_for(6 * (size_t)L.nn, 128), 128, 0, st>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_x.p, L.d_b.p, L.d_res.p);
-    ShellLevel& C = *c.shells[l + 1];
-    k_restrict_shell<double><<<grid_for(6 * (size_t)C.nn, 128), 128, 0, st>>>(C.nn, L.d_chPtr.p, L.d_chIdx.p, L.d_chW.p, L.d_prolW.p,
-                                                                               L.d_res.p, C.d_b.p);
-  }
-  // ---- shell levels up
-  for (int l = (int)nl - 2; l >= 0; l--) {
-    ShellLevel& L = *c.shells[l];
-    ShellLevel& C = *c.shells[l + 1];
-    k_prolong_shell<double><<<grid_for(6 * (size_t)L.nn, 128), 128, 0, st>>>(L.nn, L.d_prolPtr.p, L.d_prolIdx.p, L.d_prolW.p, C.d_x.p, L.d_x.p);
-    const size_t smem = (size_t)warps * L.maxm * sizeof(double);
-    for (int sweep = 0; sweep < 2; sweep++)
-      for (int col = 3; col >= 0; col--) {
-        if (!L.colorCount[col]) continue;
-        k_sweep_shell<double><<<grid_for(L.colorCount[col], warps), 32 * warps, smem, st>>>(
-            L.colorCount[col], L.d_colorCols[col].p, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.d_cfPtr.p, L.d_cf.p, L.d_b.p,
-            L.d_x.p, L.maxm, 0);
-      }
-  }
-  // ---- level 0: prolongation and post-smoothing, colours 3..0
-  k_prolong0<double><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_nodeAgg.p, c.d_W01.p, L1.d_x.p, z);
-  for (int sweep = 0; sweep < 2; sweep++)
-    for (int col = 3; col >= 0; col--) {
-      if (!c.colorCount[col]) continue;
-      k_sweep_solid<double><<<grid_for(c.colorCount[col], warps), 32 * warps, smem0, st>>>(
-          c.colorCount[col], c.d_colorCols[col].p, c.d_colStart.p, nn, c.d_nbr.p, c.d_val.p, c.d_F.p, r, z, c.maxColLen, 0);
-    }
+void launch_d2f(Context& c, const double* a, float* b, size_t n) {
+  k_convert<double, float><<<grid_for(n, 256), 256, 0, c.stream>>>(n, a, b);
+  note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
+
+void launch_f2d(Context& c, const float* a, double* b, size_t n) {
+  k_convert<float, double><<<grid_for(n, 256), 256, 0, c.stream>>>(n, a, b);
+  note_launch();
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_add_f2d(Context& c, const float* d, double* x, size_t n) {
+  k_add_f2d<<<grid_for(n, 256), 256, 0, c.stream>>>(n, d, x);
+  note_launch();
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_vcycle(Context& c, const double* r, double* z, bool mixed) {
+  (void)mixed;
+  vcycle<double>(c, r, z);
+}
+
+void launch_vcycle32(Context& c, const float* r, float* z) { vcycle<float>(c, r, z); }
 
 }  // namespace tmg

@@ -18,7 +18,9 @@ STATUS_NAMES = {0: "TM_OK", 1: "TM_NOT_CONVERGED", 2: "TM_NONFINITE", 3: "TM_TIM
 
 EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bcsr", "tm_solve", "tm_matvec", "tm_get_bcsr",
             "tm_sizes", "tm_destroy", "tm_last_error", "tm_solve_device", "tm_matvec_device", "tm_anand_screen",
-            "tm_anand_screen_device", "tm_anand_step"]
+            "tm_anand_screen_device", "tm_anand_step", "tm_set_stream", "tm_launch_count", "tm_kernel_timer",
+            "tm_kernel_timer_read", "tm_assemble_step_device"]
+KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
 
 dp = C.POINTER(C.c_double)
 ip = C.POINTER(C.c_int32)
@@ -75,6 +77,7 @@ def load():
     L.tm_default_solve_opts.argtypes = [C.POINTER(TmSolveOpts)]
     L.tm_create.argtypes = [C.POINTER(TmMesh), C.POINTER(vp)]
     L.tm_assemble_step.argtypes = [vp, C.POINTER(TmStep), vp]
+    L.tm_assemble_step_device.argtypes = [vp, C.POINTER(TmStep), vp]
     L.tm_set_bcsr.argtypes = [vp, vp, vp, vp, vp]
     L.tm_solve.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
     L.tm_solve_device.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
@@ -89,8 +92,13 @@ def load():
                                   C.c_int32, vp, vp, vp]
     L.tm_anand_screen_device.argtypes = L.tm_anand_screen.argtypes
     L.tm_anand_step.argtypes = [C.POINTER(TmAnandMaterial), C.c_int32, vp, vp, C.c_double, C.c_double, vp, vp, C.c_int32]
+    L.tm_set_stream.argtypes = [vp, vp]
+    L.tm_launch_count.argtypes = []
+    L.tm_kernel_timer.argtypes = [vp, C.c_int32]
+    L.tm_kernel_timer_read.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     for name in EXPORTED:
         getattr(L, name).restype = C.c_int32 if name not in ("tm_default_solve_opts",) else None
+    L.tm_launch_count.restype = C.c_int64
     _lib = L
     return L
 

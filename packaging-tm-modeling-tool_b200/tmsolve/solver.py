@@ -85,6 +85,15 @@ class DeviceModel:
         check(load().tm_assemble_step(self.h, C.byref(st), rhs.ctypes.data_as(C.c_void_p)))
         return rhs
 
+    def assemble_step_device(self, step: StepData, rhs_ptr: int):
+        """assemble_step with the load written to device memory (raw device pointer)."""
+        lay = np.ascontiguousarray(step.layered, np.int32); born = np.ascontiguousarray(step.born, np.int32)
+        D = np.ascontiguousarray(step.D, np.float64); s0 = np.ascontiguousarray(step.s0, np.float64)
+        W = np.ascontiguousarray(step.W, np.float64); V = np.ascontiguousarray(step.V, np.float64)
+        st = TmStep(stage=int(step.stage), psetLayered=_p(lay, C.c_int32), D=_p(D, C.c_double), s0=_p(s0, C.c_double),
+                    W=_p(W, C.c_double), V=_p(V, C.c_double), psetBorn=_p(born, C.c_int32))
+        check(load().tm_assemble_step_device(self.h, C.byref(st), C.c_void_p(rhs_ptr)))
+
     def set_bcsr(self, rowPtr, col, val, isConstrained):
         rowPtr = np.ascontiguousarray(rowPtr, np.int32); col = np.ascontiguousarray(col, np.int32)
         val = np.ascontiguousarray(val, np.float64); isC = np.ascontiguousarray(isConstrained, np.uint8)
@@ -110,7 +119,7 @@ class DeviceModel:
         load().tm_default_solve_opts(C.byref(o))
         o.tol = tol; o.maxit = maxit; o.warm = warm
         o.precond = 0 if precond == "mg" else 1
-        o.precision = 0 if precision == "fp64" else 1
+        o.precision = {"fp64": 0, "mixed": 1, "mixed_ir": 2}[precision]
         o.key = -1 if key is None else int(key)
         return o
 
@@ -143,4 +152,25 @@ class DeviceModel:
         return self.record(info, None, precond)
 
 
-__all__ = ["DeviceModel", "TmError"]
+    # ---- stream and measurement hooks ----------------------------------------------------------
+    def set_stream(self, stream_ptr: int):
+        """Run on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        check(load().tm_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def time_kernel(self, name: Optional[str]):
+        """Bracket every launch of one kernel class with CUDA events (None: off)."""
+        check(load().tm_kernel_timer(self.h, -1 if name is None else _lib.KERNELS[name]))
+
+    def kernel_time(self):
+        """(launches, summed device ms) of the timed kernel class since time_kernel()."""
+        n = C.c_int64(); ms = C.c_double()
+        check(load().tm_kernel_timer_read(self.h, C.byref(n), C.byref(ms)))
+        return int(n.value), float(ms.value)
+
+
+def launch_count() -> int:
+    """Kernels launched by libtmsolve.so since it was loaded."""
+    return int(load().tm_launch_count())
+
+
+__all__ = ["DeviceModel", "TmError", "launch_count"]

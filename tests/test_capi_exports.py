@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared():
     src = open(os.path.join(ROOT, "include", "tmsolve.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:tm_status|void|int32_t)\s+(tm_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:tm_status|void|int32_t|int64_t)\s+(tm_\w+)\s*\(", src, re.M)))
 
 
 def test_header_lists_entry_points():

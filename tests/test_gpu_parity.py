@@ -142,3 +142,25 @@ def test_zero_load():
     dm.assemble_step(pkg.step())
     r = dm.solve(np.zeros(dm.ndof))
     assert r["converged"] and r["iters"] == 0 and not r["u"].any()
+
+
+@pytest.mark.parametrize("make", [fcbga_c1, lambda: lidded_c2(n_inplane=48)], ids=["c1", "c2_48"])
+@pytest.mark.parametrize("precision", ["mixed", "mixed_ir"])
+def test_mixed_precision(make, precision):
+    """FP32 multigrid (and, for mixed_ir, the FP32 apply) inside FP64 iterations: same FP64
+    residual target; RMS warpage within 1e-6 relative of the FP64 GPU solve,
+    displacements within 1e-5 (both solutions carry the 1e-10 residual of the solve)."""
+    from tmsolve.solver import DeviceModel
+    pkg = make()
+    dm = DeviceModel(pkg)
+    step = pkg.step()
+    r64 = dm.solve(dm.assemble_step(step), tol=1e-10, warm=0, key=1)
+    rmx = dm.solve(dm.assemble_step(step), tol=1e-10, warm=0, key=2, precision=precision)
+    assert r64["converged"] and rmx["converged"]
+    assert rmx["relres"] < 1e-10
+    if precision == "mixed_ir":
+        assert rmx["refinements"] >= 1
+    du = np.linalg.norm(rmx["u"] - r64["u"]) / np.linalg.norm(r64["u"])
+    assert du <= 1e-5, du
+    w64, wmx = rms_warpage(pkg.mesh, r64["u"]), rms_warpage(pkg.mesh, rmx["u"])
+    assert abs(wmx / w64 - 1) <= 1e-6
