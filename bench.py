@@ -288,7 +288,7 @@ def run_ours(a):
     hbm, hbm_kind = peaks()
     achieved = per_launch / (kms / kcount / 1e3) / 1e9 if kcount else None
     traffic = profile_traffic(DOMINANT, a.precision)
-    roof = {"kernel": "k_sweep_solid (level-0 z-column block-tridiagonal smoother, one colour)", "bound": "hbm", "achieved": achieved,
+    roof = {"kernel": "k_sweep_panel (level-0 z-column block-tridiagonal smoother on packed column panels, one colour)", "bound": "hbm", "achieved": achieved,
             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None, "traffic": traffic,
             "peak_kind": hbm_kind, "launches_timed": kcount, "avg_launch_us": 1e3 * kms / kcount if kcount else None,
             "algorithmic_bytes_per_launch": per_launch}

@@ -434,7 +434,14 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
 
 void upload_mesh(Context& c) {
   cudaStream_t s = c.stream;
-  c.d_nbr.upload(c.nbr, s);
+  {
+    std::vector<int> pn((size_t)NSLOT * c.nn);
+    for (int sl = 0; sl < NSLOT; sl++)
+      for (int n = 0; n < c.nn; n++) pn[(size_t)sl * c.nn + c.pos[n]] = c.nbr[(size_t)sl * c.nn + n];
+    c.d_nbr.upload(pn, s);
+  }
+  c.d_pos.upload(c.pos, s);
+  c.d_posNode.upload(c.posNode, s);
   c.d_slotMask.upload(c.slotMask, s);
   c.d_nodeIJK.upload(c.nodeIJK, s);
   c.d_cellElems.upload(c.cellElems, s);
@@ -576,7 +583,7 @@ tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, co
         const int di = c.nodeIJK[3 * (size_t)j] - ii, dj = c.nodeIJK[3 * (size_t)j + 1] - ij, dk = c.nodeIJK[3 * (size_t)j + 2] - ik;
         if (std::abs(di) > 1 || std::abs(dj) > 1 || std::abs(dk) > 1) fail(TM_BAD_INPUT, "block outside the 27-point stencil of the mesh");
         const int s = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
-        for (int v = 0; v < 9; v++) sv[((size_t)s * 9 + v) * nn + i] = val[9 * (size_t)k + v];
+        for (int v = 0; v < 9; v++) sv[((size_t)s * 9 + v) * nn + c.pos[i]] = val[9 * (size_t)k + v];
       }
     }
     c.d_val.upload(sv, c.stream);
@@ -602,7 +609,7 @@ tm_status tm_get_bcsr(tm_ctx* ctx, int32_t* rowPtr, int32_t* col, double* val) {
       for (int s = 0; s < NSLOT; s++) {
         if (!(c.slotMask[i] >> s & 1)) continue;
         if (col) col[k] = c.nbr[(size_t)s * nn + i];
-        if (val) for (int v = 0; v < 9; v++) val[9 * (size_t)k + v] = sv[((size_t)s * 9 + v) * nn + i];
+        if (val) for (int v = 0; v < 9; v++) val[9 * (size_t)k + v] = sv[((size_t)s * 9 + v) * nn + c.pos[i]];
         k++;
       }
       if (rowPtr) rowPtr[i + 1] = k;

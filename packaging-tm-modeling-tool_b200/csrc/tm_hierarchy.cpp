@@ -274,6 +274,16 @@ void build_stencil(Context& c) {
       }
   c.maxColLen = 0;
   for (int col = 0; col < nx * ny; col++) c.maxColLen = std::max(c.maxColLen, c.colStart[col + 1] - c.colStart[col]);
+  // colour-major positions (colour = (i%2)*2 + j%2 of the column)
+  c.pos.assign(nn, -1);
+  c.posNode.assign(nn, -1);
+  int p = 0;
+  for (int k = 0; k < 4; k++)
+    for (int col = 0; col < nx * ny; col++) {
+      if (((col / ny) & 1) * 2 + ((col % ny) & 1) != k) continue;
+      for (int n = c.colStart[col]; n < c.colStart[col + 1]; n++) { c.pos[n] = p; c.posNode[p] = n; p++; }
+    }
+  if (p != nn) fail(TM_BAD_INPUT, "columns do not cover the nodes");
 }
 
 void build_classes(Context& c) {

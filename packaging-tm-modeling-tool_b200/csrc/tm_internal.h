@@ -118,6 +118,11 @@ struct Context {
   // stencil structure
   std::vector<int> nbr;                // 27*nn, slot-major
   std::vector<int> slotMask;           // nn: bit s set when (n, nbr[s]) share an element (the block CSR pattern)
+  // device copies of the level-0 arrays are stored in colour-major position order: the nodes of all
+  // colour-0 columns first (columns in ascending order, each column contiguous), then colour 1, ...
+  // so that one colour's sweep streams a contiguous block; pos[n] is the position of node n
+  std::vector<int> pos, posNode;
+  DBuf<int> d_pos, d_posNode;
   DBuf<int> d_nbr, d_slotMask, d_nodeIJK, d_cellElems, d_eGroup, d_groupStage, d_eClass, d_colStart, d_constr;
   DBuf<double> d_eScale;
   // element classes: (property set, hx, hy, hz)

@@ -246,13 +246,13 @@ __device__ __forceinline__ int loc_index(int a, int b, int c) {
 }
 
 // ---- stencil assembly: thread per (slot, node), contributions in element order -----------------
-__global__ void k_assemble(int nn, int nx, int ny, int nz, const int* __restrict__ nodeIJK, const int* __restrict__ nbr,
+__global__ void k_assemble(int nn, int nx, int ny, int nz, const int* __restrict__ posNode, const int* __restrict__ nodeIJK, const int* __restrict__ nbr,
                            const int* __restrict__ cellElems, const int* __restrict__ eClass, const double* __restrict__ eScale,
                            const int* __restrict__ eGroup, const int* __restrict__ groupStage, int stage,
                            const double* __restrict__ clsKc, double* __restrict__ val) {
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= (size_t)NSLOT * nn) return;
-  const int s = (int)(t / nn), n = (int)(t % nn);
+  const int s = (int)(t / nn), ps = (int)(t % nn), n = posNode[ps];
   double acc[9];
   for (int v = 0; v < 9; v++) acc[v] = 0;
   const int m = nbr[t];
@@ -283,7 +283,7 @@ __global__ void k_assemble(int nn, int nx, int ny, int nz, const int* __restrict
           }
         }
   }
-  for (int v = 0; v < 9; v++) val[((size_t)s * 9 + v) * nn + n] = acc[v];
+  for (int v = 0; v < 9; v++) val[((size_t)s * 9 + v) * nn + ps] = acc[v];
 }
 
 // thermal load, thread per node (assembleStep's rhs, 09-assembly.js:417-420)
@@ -318,46 +318,48 @@ __global__ void k_assemble_rhs(int nn, int nx, int ny, int nz, const int* __rest
 }
 
 // applyConstraints (09-assembly.js:445-464), one thread walking the DOFs in order
-__global__ void k_constraints(int nn, int ncon, const int* __restrict__ dofs, const int* __restrict__ nbr,
+__global__ void k_constraints(int nn, int ncon, const int* __restrict__ dofs, const int* __restrict__ pos, const int* __restrict__ nbr,
                               const int* __restrict__ slotMask, double* __restrict__ val, double* __restrict__ rhs,
                               uint8_t* __restrict__ isC) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   for (int t = 0; t < ncon; t++) isC[dofs[t]] = 1;
   for (int t = 0; t < ncon; t++) {
-    const int d = dofs[t], i = d / 3, p = d % 3;
+    const int d = dofs[t], i = d / 3, p = d % 3, pi = pos[i];
     const int mask = slotMask[i];
     for (int s = 0; s < NSLOT; s++) {
       if (!(mask >> s & 1)) continue;
-      const int j = nbr[(size_t)s * nn + i];
+      const int j = nbr[(size_t)s * nn + pi];
       for (int q = 0; q < 3; q++) {
-        double* v = val + ((size_t)s * 9 + 3 * p + q) * nn + i;
+        double* v = val + ((size_t)s * 9 + 3 * p + q) * nn + pi;
         if (3 * j + q != d) *v = 0;
         else if (*v == 0) *v = 1;
       }
       const int s2 = NSLOT - 1 - s;
       for (int q = 0; q < 3; q++)
-        if (3 * j + q != d) val[((size_t)s2 * 9 + 3 * q + p) * nn + j] = 0;
+        if (3 * j + q != d) val[((size_t)s2 * 9 + 3 * q + p) * nn + pos[j]] = 0;
     }
     if (rhs) rhs[d] = 0;
   }
 }
 
 // _scale (10-solver.js:852-866)
-__global__ void k_scale_diag(int nn, const double* __restrict__ val, double* __restrict__ s) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= nn) return;
-  for (int p = 0; p < 3; p++) s[3 * n + p] = 1 / sqrt(fmax(val[((size_t)SLOT_SELF * 9 + 4 * p) * nn + n], 1e-300));
+__global__ void k_scale_diag(int nn, const int* __restrict__ posNode, const double* __restrict__ val, double* __restrict__ s) {
+  const int ps = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ps >= nn) return;
+  const int n = posNode[ps];
+  for (int p = 0; p < 3; p++) s[3 * n + p] = 1 / sqrt(fmax(val[((size_t)SLOT_SELF * 9 + 4 * p) * nn + ps], 1e-300));
 }
 
-__global__ void k_scale_val(int nn, const int* __restrict__ nbr, const double* __restrict__ s, double* __restrict__ val) {
+__global__ void k_scale_val(int nn, const int* __restrict__ posNode, const int* __restrict__ nbr, const double* __restrict__ s,
+                            double* __restrict__ val) {
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= (size_t)NSLOT * nn) return;
-  const int sl = (int)(t / nn), n = (int)(t % nn);
+  const int sl = (int)(t / nn), ps = (int)(t % nn), n = posNode[ps];
   const int j = nbr[t];
   if (j < 0) return;
   for (int p = 0; p < 3; p++)
     for (int q = 0; q < 3; q++) {
-      double* v = val + ((size_t)sl * 9 + 3 * p + q) * nn + n;
+      double* v = val + ((size_t)sl * 9 + 3 * p + q) * nn + ps;
       *v *= s[3 * n + p] * s[3 * j + q];
     }
 }
@@ -384,22 +386,24 @@ __device__ bool chol3(const double* A, double* L, double jit) {
 }
 
 // factorColumns (10-solver.js:31-68), thread per column
-__global__ void k_factor_columns(int ncol, int nn, const int* __restrict__ colStart, const int* __restrict__ nbr,
+__global__ void k_factor_columns(int ncol, int nn, const int* __restrict__ colStart, const int* __restrict__ pos, const int* __restrict__ nbr,
                                  const int* __restrict__ slotMask, const double* __restrict__ val, double* __restrict__ F,
                                  int* __restrict__ jitterCount) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncol) return;
   int jitter = 0;
   double D[9], tmp[9];
+  const int p0 = colStart[c] < colStart[c + 1] ? pos[colStart[c]] : 0;
   for (int n = colStart[c]; n < colStart[c + 1]; n++) {
-    for (int q = 0; q < 9; q++) D[q] = val[((size_t)SLOT_SELF * 9 + q) * nn + n];
-    double* Fn = F + 18 * (size_t)n;
-    const bool down = n > colStart[c] && (slotMask[n] >> SLOT_DOWN & 1) && nbr[(size_t)SLOT_DOWN * nn + n] == n - 1;
+    const int pn = p0 + (n - colStart[c]);
+    for (int q = 0; q < 9; q++) D[q] = val[((size_t)SLOT_SELF * 9 + q) * nn + pn];
+    double* Fn = F + 18 * (size_t)pn;
+    const bool down = n > colStart[c] && (slotMask[n] >> SLOT_DOWN & 1) && nbr[(size_t)SLOT_DOWN * nn + pn] == n - 1;
     if (down) {
-      const double* Fp = F + 18 * (size_t)(n - 1);
+      const double* Fp = F + 18 * (size_t)(pn - 1);
       for (int r = 0; r < 3; r++) {
-        const double b0 = val[((size_t)SLOT_DOWN * 9 + 3 * r) * nn + n], b1 = val[((size_t)SLOT_DOWN * 9 + 3 * r + 1) * nn + n],
-                     b2 = val[((size_t)SLOT_DOWN * 9 + 3 * r + 2) * nn + n];
+        const double b0 = val[((size_t)SLOT_DOWN * 9 + 3 * r) * nn + pn], b1 = val[((size_t)SLOT_DOWN * 9 + 3 * r + 1) * nn + pn],
+                     b2 = val[((size_t)SLOT_DOWN * 9 + 3 * r + 2) * nn + pn];
         const double y0 = b0 / Fp[0];
         const double y1 = (b1 - Fp[3] * y0) / Fp[4];
         const double y2 = (b2 - Fp[6] * y0 - Fp[7] * y1) / Fp[8];
@@ -445,7 +449,7 @@ __device__ __forceinline__ int find_col(const int* cols, int n, int J) {
 }
 
 // galerkinProduct 0 -> 1 (10-solver.js:193-245), warp per coarse row, same summation order
-__global__ void k_galerkin01(int na, int nn, const int* __restrict__ aggStart, const int* __restrict__ nodeAgg,
+__global__ void k_galerkin01(int na, int nn, const int* __restrict__ aggStart, const int* __restrict__ nodeAgg, const int* __restrict__ pos,
                              const int* __restrict__ nbr, const int* __restrict__ slotMask, const double* __restrict__ val,
                              const double* __restrict__ W, const int* __restrict__ rowPtr, const int* __restrict__ col,
                              int maxRow, double* __restrict__ out) {
@@ -461,15 +465,16 @@ __global__ void k_galerkin01(int na, int nn, const int* __restrict__ aggStart, c
   const int rA = e0 / 6, cA = e0 % 6, rB = e1 / 6, cB = e1 % 6;
   for (int i = aggStart[I]; i < aggStart[I + 1]; i++) {
     const int mask = slotMask[i];
+    const int pi = pos[i];
     const double* Wi = W + 18 * (size_t)i;
     for (int s = 0; s < NSLOT; s++) {
       if (!(mask >> s & 1)) continue;
-      const int j = nbr[(size_t)s * nn + i];
+      const int j = nbr[(size_t)s * nn + pi];
       const int loc = find_col(col + r0, nJ, nodeAgg[j]);
       if (loc < 0) continue;   // cannot happen for a pattern built from the same mesh; never write outside acc
       const double* Wj = W + 18 * (size_t)j;
       double kv[9];
-      for (int v = 0; v < 9; v++) kv[v] = val[((size_t)s * 9 + v) * nn + i];
+      for (int v = 0; v < 9; v++) kv[v] = val[((size_t)s * 9 + v) * nn + pi];
       // T (3x6) = K_ij W_j ; acc += W_i^T T
       {
         double T[3];
@@ -771,6 +776,102 @@ __global__ void k_factor_coarsest_par(int nnb, const int* __restrict__ rowPtr, c
   if (threadIdx.x == 0 && fixes) atomicAdd(jitterCount, fixes);
 }
 
+// blocked right-looking form of the same banded Cholesky: per block of NB pivots, the diagonal
+// block is factored in shared memory by one warp, the panel below it (the rows the band reaches)
+// is solved against it with one thread per row, and the trailing band window is updated with one
+// warp per row; the jitter rule of cholDense is applied to every pivot.
+constexpr int CB_NB = 32, CB_LD = 33;
+__global__ void __launch_bounds__(1024) k_factor_coarsest_blk(int nnb, const int* __restrict__ rowPtr, const int* __restrict__ col,
+                                                              const double* __restrict__ val, int n, int bw, double* __restrict__ A,
+                                                              int* __restrict__ jitterCount) {
+  extern __shared__ double smb[];
+  double* Ds = smb;                  // CB_NB x CB_LD diagonal block
+  double* P = smb + CB_NB * CB_LD;   // bw x CB_LD panel rows
+  __shared__ double s_red[32];
+  __shared__ int s_fix;
+  const int w = bw + 1, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nthr = blockDim.x, nw = nthr >> 5;
+  for (size_t e = tid; e < (size_t)n * w; e += nthr) A[e] = 0;
+  __syncthreads();
+  for (int i = 0; i < nnb; i++)
+    for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+      const int j = col[k];
+      if (j > i) continue;
+      for (int e = tid; e < 36; e += nthr) {
+        const int p = e / 6, q = e % 6;
+        const int r = 6 * i + p, cc = 6 * j + q;
+        if (cc <= r) A[(size_t)r * w + (cc - r + bw)] = val[36 * (size_t)k + e];
+      }
+    }
+  __syncthreads();
+  double dm = 0;
+  for (int i = tid; i < n; i += nthr) dm = fmax(dm, fabs(A[(size_t)i * w + bw]));
+  for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+  if (lane == 0) s_red[warp] = dm;
+  if (tid == 0) s_fix = 0;
+  __syncthreads();
+  double dmax = 0;
+  for (int q = 0; q < nw; q++) dmax = fmax(dmax, s_red[q]);
+  const double jitter = 1e-12 * (dmax != 0 ? dmax : 1);
+  for (int jb = 0; jb < n; jb += CB_NB) {
+    const int nbk = min(CB_NB, n - jb);
+    for (int e = tid; e < CB_NB * CB_NB; e += nthr) {
+      const int r = e / CB_NB, cc = e % CB_NB;
+      Ds[r * CB_LD + cc] = (r < nbk && cc <= r && r - cc <= bw) ? A[(size_t)(jb + r) * w + (cc - r + bw)] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int j = 0; j < nbk; j++) {
+        double ss = 0;
+        for (int t = lane; t < j; t += 32) ss += Ds[j * CB_LD + t] * Ds[j * CB_LD + t];
+        ss = warp_sum(ss);
+        double d = Ds[j * CB_LD + j] - ss;
+        if (!(d > jitter)) { d = fmax(fabs(d), jitter); if (lane == 0) s_fix++; }
+        const double ljj = sqrt(d), inv = 1 / ljj;
+        __syncwarp();
+        if (lane == 0) Ds[j * CB_LD + j] = ljj;
+        if (lane > j && lane < nbk) {
+          double s2 = Ds[lane * CB_LD + j];
+          for (int t = 0; t < j; t++) s2 -= Ds[lane * CB_LD + t] * Ds[j * CB_LD + t];
+          Ds[lane * CB_LD + j] = s2 * inv;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < CB_NB * CB_NB; e += nthr) {
+      const int r = e / CB_NB, cc = e % CB_NB;
+      if (r < nbk && cc <= r && r - cc <= bw) A[(size_t)(jb + r) * w + (cc - r + bw)] = Ds[r * CB_LD + cc];
+    }
+    const int i0 = jb + nbk, i1 = min(n, jb + nbk + bw), R = i1 - i0;
+    for (int ri = tid; ri < R; ri += nthr) {
+      const int i = i0 + ri;
+      double* Pr = P + (size_t)ri * CB_LD;
+      for (int k = 0; k < nbk; k++) {
+        const int kk = jb + k;
+        double a = (i - kk <= bw) ? A[(size_t)i * w + (kk - i + bw)] : 0.0;
+        for (int t = 0; t < k; t++) a -= Pr[t] * Ds[k * CB_LD + t];
+        Pr[k] = a / Ds[k * CB_LD + k];
+      }
+      for (int k = 0; k < nbk; k++)
+        if (i - (jb + k) <= bw) A[(size_t)i * w + (jb + k - i + bw)] = Pr[k];
+    }
+    __syncthreads();
+    for (int ri = warp; ri < R; ri += nw) {
+      const int gi = i0 + ri;
+      const double* Pi = P + (size_t)ri * CB_LD;
+      for (int rk = max(0, ri - bw) + lane; rk <= ri; rk += 32) {
+        const double* Pk = P + (size_t)rk * CB_LD;
+        double s2 = 0;
+        for (int t = 0; t < nbk; t++) s2 += Pi[t] * Pk[t];
+        const int gk = i0 + rk;
+        A[(size_t)gi * w + (gk - gi + bw)] -= s2;
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0 && s_fix) atomicAdd(jitterCount, s_fix);
+}
+
 // explicit inverse of the coarsest operator from its banded factor: warp per unit vector e_c, the
 // result row c (the inverse is symmetric) doubling as the work vector of the two substitutions
 __global__ void k_coarsest_inverse_par(int n, int bw, const double* __restrict__ A, double* __restrict__ inv) {
@@ -848,7 +949,7 @@ void launch_assemble(Context& c) {
   note_launch(2);
   {
   TimedLaunch tl(c, K_ASSEMBLE);
-  k_assemble<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_nodeIJK.p, c.d_nbr.p, c.d_cellElems.p, c.d_eClass.p,
+  k_assemble<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_posNode.p, c.d_nodeIJK.p, c.d_nbr.p, c.d_cellElems.p, c.d_eClass.p,
                                                       c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsKc.p, c.d_val.p);
   }
   TM_CUDA_CHECK(cudaGetLastError());
@@ -864,7 +965,7 @@ void launch_constraints(Context& c) {
   DBuf<int> d;
   d.upload(c.constr, c.stream);
   note_launch();
-  k_constraints<<<1, 1, 0, c.stream>>>(c.nn, (int)c.constr.size(), d.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
+  k_constraints<<<1, 1, 0, c.stream>>>(c.nn, (int)c.constr.size(), d.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
   TM_CUDA_CHECK(cudaGetLastError());
   TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   c.isC.assign(3 * (size_t)c.nn, 0);
@@ -874,9 +975,9 @@ void launch_constraints(Context& c) {
 void launch_scale(Context& c) {
   c.d_s.alloc(3 * (size_t)c.nn);
   note_launch(2);
-  k_scale_diag<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.d_val.p, c.d_s.p);
+  k_scale_diag<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_val.p, c.d_s.p);
   const size_t tot = (size_t)NSLOT * c.nn;
-  k_scale_val<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_s.p, c.d_val.p);
+  k_scale_val<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_s.p, c.d_val.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -891,7 +992,7 @@ void launch_factor_columns(Context& c) {
   const int ncol = c.nx * c.ny;
   c.d_F.zero(c.stream);
   note_launch();
-  k_factor_columns<<<grid_for(ncol, 128), 128, 0, c.stream>>>(ncol, c.nn, c.d_colStart.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p,
+  k_factor_columns<<<grid_for(ncol, 128), 128, 0, c.stream>>>(ncol, c.nn, c.d_colStart.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p,
                                                              c.d_F.p, c.d_jitter.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
@@ -909,7 +1010,7 @@ void launch_galerkin01(Context& c) {
   TM_CUDA_CHECK(cudaFuncSetAttribute(k_galerkin01, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   note_launch();
   TimedLaunch tl(c, K_GALERKIN01);
-  k_galerkin01<<<grid_for(L1.nn, warps), 32 * warps, smem, c.stream>>>(L1.nn, c.nn, c.d_aggStart.p, c.d_nodeAgg.p, c.d_nbr.p, c.d_slotMask.p,
+  k_galerkin01<<<grid_for(L1.nn, warps), 32 * warps, smem, c.stream>>>(L1.nn, c.nn, c.d_aggStart.p, c.d_nodeAgg.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p,
                                                                       c.d_val.p, c.d_W01.p, L1.d_rowPtr.p, L1.d_col.p, L1.maxRowBlocks,
                                                                       L1.d_val.p);
   TM_CUDA_CHECK(cudaGetLastError());
@@ -941,7 +1042,13 @@ void launch_factor_shell(Context& c, ShellLevel& L) {
 
 void launch_factor_coarsest(Context& c, ShellLevel& L) {
   note_launch(2);
-  k_factor_coarsest_par<<<1, 1024, 0, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
+  const size_t smem = (size_t)(CB_NB + L.bandBw) * CB_LD * sizeof(double);
+  if (smem <= 200 * 1024) {
+    TM_CUDA_CHECK(cudaFuncSetAttribute(k_factor_coarsest_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_factor_coarsest_blk<<<1, 1024, smem, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
+  } else {
+    k_factor_coarsest_par<<<1, 1024, 0, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
+  }
   TM_CUDA_CHECK(cudaGetLastError());
   k_coarsest_inverse_par<<<grid_for(L.denseN, 4), 128, 0, c.stream>>>(L.denseN, L.bandBw, L.d_band.p, L.d_inv.p);
   TM_CUDA_CHECK(cudaGetLastError());

@@ -23,17 +23,18 @@ inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block)
 
 // ---- level-0 stencil apply: y = K x or y = b - K x, thread per node --------------------------
 template <class T, class V>
-__global__ void k_apply0(int nn, const int* __restrict__ nbr, const T* __restrict__ val, const V* __restrict__ x,
-                         V* __restrict__ y, const V* __restrict__ b) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= nn) return;
+__global__ void k_apply0(int nn, const int* __restrict__ posNode, const int* __restrict__ nbr, const T* __restrict__ val,
+                         const V* __restrict__ x, V* __restrict__ y, const V* __restrict__ b) {
+  const int ps = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ps >= nn) return;
+  const int n = posNode[ps];
   T y0 = 0, y1 = 0, y2 = 0;
 #pragma unroll 3
   for (int s = 0; s < NSLOT; s++) {
-    const int j = nbr[(size_t)s * nn + n];
+    const int j = nbr[(size_t)s * nn + ps];
     if (j < 0) continue;
     const T x0 = (T)x[3 * j], x1 = (T)x[3 * j + 1], x2 = (T)x[3 * j + 2];
-    const T* v = val + (size_t)s * 9 * nn + n;
+    const T* v = val + (size_t)s * 9 * nn + ps;
     y0 += v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
     y1 += v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
     y2 += v[6 * (size_t)nn] * x0 + v[7 * (size_t)nn] * x1 + v[8 * (size_t)nn] * x2;
@@ -114,76 +115,6 @@ __global__ void k_scale_vec(size_t n, const T* __restrict__ x, const double* __r
   if (i < n) y[i] = divide ? (T)(x[i] / s[i]) : (T)(x[i] * s[i]);
 }
 
-// ---- level-0 column smoother: warp per column of one colour ------------------------------------
-// residual rows of the column (27-point stencil, coalesced along the column's contiguous nodes),
-// block-tridiagonal forward/backward solve with the column factors staged in shared memory
-// (solveColumn, 10-solver.js:71-104), then x += dx
-template <class T>
-__global__ void k_sweep_solid(int ncolc, const int* __restrict__ cols, const int* __restrict__ colStart, int nn,
-                              const int* __restrict__ nbr, const T* __restrict__ val, const T* __restrict__ F,
-                              const T* __restrict__ b, T* __restrict__ x, int maxLen, int zeroGuess) {
-  extern __shared__ unsigned char smraw[];
-  T* sm = reinterpret_cast<T*>(smraw);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (gw >= ncolc) return;
-  T* r = sm + (size_t)warp * 21 * maxLen;
-  T* Fs = r + 3 * maxLen;
-  const int c = cols[gw];
-  const int n0 = colStart[c], len = colStart[c + 1] - n0;
-  for (int e = lane; e < 18 * len; e += 32) Fs[e] = F[18 * (size_t)n0 + e];
-  for (int l = lane; l < len; l += 32) {
-    const int n = n0 + l;
-    T s0 = b[3 * n], s1 = b[3 * n + 1], s2 = b[3 * n + 2];
-    if (!zeroGuess) {
-      for (int s = 0; s < NSLOT; s++) {
-        const int j = nbr[(size_t)s * nn + n];
-        if (j < 0) continue;
-        const T x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
-        const T* v = val + (size_t)s * 9 * nn + n;
-        s0 -= v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
-        s1 -= v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
-        s2 -= v[6 * (size_t)nn] * x0 + v[7 * (size_t)nn] * x1 + v[8 * (size_t)nn] * x2;
-      }
-    }
-    r[3 * l] = s0; r[3 * l + 1] = s1; r[3 * l + 2] = s2;
-  }
-  __syncwarp();
-  if (lane == 0) {
-    for (int l = 0; l < len; l++) {
-      const T* f = Fs + 18 * l;
-      T b0 = r[3 * l], b1 = r[3 * l + 1], b2 = r[3 * l + 2];
-      if (l > 0) {
-        const T p0 = r[3 * l - 3], p1 = r[3 * l - 2], p2 = r[3 * l - 1];
-        b0 -= f[9] * p0 + f[10] * p1 + f[11] * p2;
-        b1 -= f[12] * p0 + f[13] * p1 + f[14] * p2;
-        b2 -= f[15] * p0 + f[16] * p1 + f[17] * p2;
-      }
-      const T y0 = b0 / f[0];
-      const T y1 = (b1 - f[3] * y0) / f[4];
-      const T y2 = (b2 - f[6] * y0 - f[7] * y1) / f[8];
-      r[3 * l] = y0; r[3 * l + 1] = y1; r[3 * l + 2] = y2;
-    }
-    for (int l = len - 1; l >= 0; l--) {
-      const T* f = Fs + 18 * l;
-      T b0 = r[3 * l], b1 = r[3 * l + 1], b2 = r[3 * l + 2];
-      if (l + 1 < len) {
-        const T* g = Fs + 18 * (l + 1);
-        const T q0 = r[3 * l + 3], q1 = r[3 * l + 4], q2 = r[3 * l + 5];
-        b0 -= g[9] * q0 + g[12] * q1 + g[15] * q2;
-        b1 -= g[10] * q0 + g[13] * q1 + g[16] * q2;
-        b2 -= g[11] * q0 + g[14] * q1 + g[17] * q2;
-      }
-      const T z2 = b2 / f[8];
-      const T z1 = (b1 - f[7] * z2) / f[4];
-      const T z0 = (b0 - f[3] * z1 - f[6] * z2) / f[0];
-      r[3 * l] = z0; r[3 * l + 1] = z1; r[3 * l + 2] = z2;
-    }
-  }
-  __syncwarp();
-  for (int e = lane; e < 3 * len; e += 32) x[3 * (size_t)n0 + e] += r[e];
-}
-
 // level-0 column smoother on packed column panels: one CTA per group of whole z-columns of one
 // colour (at most cap nodes). Every thread computes the residual rows of one node (coalesced
 // along each column's contiguous nodes), the column factors are staged in shared memory, one
@@ -191,7 +122,8 @@ __global__ void k_sweep_solid(int ncolc, const int* __restrict__ cols, const int
 // 10-solver.js:71-104), and every node is then updated, x += dx.
 template <class T>
 __global__ void __launch_bounds__(128) k_sweep_panel(const int* __restrict__ grpStart, const int* __restrict__ cols,
-                                                      const int* __restrict__ colStart, int nn, const int* __restrict__ nbr,
+                                                      const int* __restrict__ colStart, const int* __restrict__ pos, int nn,
+                                                      const int* __restrict__ nbr,
                                                       const T* __restrict__ val, const T* __restrict__ F, const T* __restrict__ b,
                                                       T* __restrict__ x, int cap, int maxCols, int zeroGuess) {
   extern __shared__ unsigned char smraw[];
@@ -212,25 +144,25 @@ __global__ void __launch_bounds__(128) k_sweep_panel(const int* __restrict__ grp
   }
   __syncthreads();
   const int total = off[ncols];
-  // stage the column factors (each column's 18*len values are contiguous)
-  for (int q = 0; q < ncols; q++) {
-    const int len = off[q + 1] - off[q];
-    const T* src = F + 18 * (size_t)first[q];
-    T* dst = Fs + 18 * off[q];
-    for (int e = threadIdx.x; e < 18 * len; e += blockDim.x) dst[e] = src[e];
+  // the group's nodes occupy the contiguous positions gp0 .. gp0+total-1 (column factors included)
+  const size_t gp0 = ncols ? pos[first[0]] : 0;
+  {
+    const T* src = F + 18 * gp0;
+    for (int e = threadIdx.x; e < 18 * total; e += blockDim.x) Fs[e] = src[e];
   }
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     int q = 0;
     while (off[q + 1] <= t) q++;
     const int n = first[q] + (t - off[q]);
+    const size_t ps = gp0 + t;
     T s0 = b[3 * (size_t)n], s1 = b[3 * (size_t)n + 1], s2 = b[3 * (size_t)n + 2];
     if (!zeroGuess) {
 #pragma unroll 3
       for (int s = 0; s < NSLOT; s++) {
-        const int j = nbr[(size_t)s * nn + n];
+        const int j = nbr[(size_t)s * nn + ps];
         if (j < 0) continue;
         const T x0 = x[3 * (size_t)j], x1 = x[3 * (size_t)j + 1], x2 = x[3 * (size_t)j + 2];
-        const T* v = val + (size_t)s * 9 * nn + n;
+        const T* v = val + (size_t)s * 9 * nn + ps;
         s0 -= v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
         s1 -= v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
         s2 -= v[6 * (size_t)nn] * x0 + v[7 * (size_t)nn] * x1 + v[8 * (size_t)nn] * x2;
@@ -320,6 +252,7 @@ __global__ void k_apply_shell(int nrow, const int* __restrict__ rowPtr, const in
   if (t >= 6 * (size_t)nrow) return;
   const int i = (int)(t / 6), p = (int)(t % 6);
   T s = 0;
+#pragma unroll 4
   for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
     const T* v = val + 36 * (size_t)k + 6 * p;
     const T* xj = x + 6 * (size_t)col[k];
@@ -345,6 +278,7 @@ __global__ void k_sweep_shell(int ncolc, const int* __restrict__ cols, const int
     const int a = n0 + e / 6, p = e % 6;
     T s = b[6 * (size_t)a + p];
     if (!zeroGuess) {
+#pragma unroll 4
       for (int k = rowPtr[a]; k < rowPtr[a + 1]; k++) {
         const T* v = val + 36 * (size_t)k + 6 * p;
         const T* xj = x + 6 * (size_t)col[k];
@@ -473,7 +407,7 @@ void vcycle(Context& c, const T* r, T* z) {
   auto sweep0 = [&](int col, int zero) {
     if (!c.grpCount[col]) return;
     TimedLaunch tl(c, K_SWEEP_SOLID);
-    k_sweep_panel<T><<<c.grpCount[col], 128, smem0, st>>>(c.d_grpStart[col].p, c.d_colorCols[col].p, c.d_colStart.p, nn, c.d_nbr.p,
+    k_sweep_panel<T><<<c.grpCount[col], 128, smem0, st>>>(c.d_grpStart[col].p, c.d_colorCols[col].p, c.d_colStart.p, c.d_pos.p, nn, c.d_nbr.p,
                                                          B::val0(c), B::F(c), r, z, c.panelCap, c.panelMaxCols, zero);
     note_launch();
   };
@@ -495,7 +429,7 @@ void vcycle(Context& c, const T* r, T* z) {
     }
   {
     TimedLaunch tl(c, K_APPLY0);
-    k_apply0<T, T><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_nbr.p, B::val0(c), z, B::res0(c), r);
+    k_apply0<T, T><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_posNode.p, c.d_nbr.p, B::val0(c), z, B::res0(c), r);
     note_launch();
   }
   ShellLevel& L1 = *c.shells[0];
@@ -566,20 +500,20 @@ TimedLaunch::~TimedLaunch() {
 
 void launch_apply0(Context& c, const double* x, double* y, const double* b) {
   TimedLaunch tl(c, K_APPLY0);
-  k_apply0<double, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val.p, x, y, b);
+  k_apply0<double, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_val.p, x, y, b);
   note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_apply0_f32(Context& c, const double* x, double* y, const double* b) {
-  k_apply0<float, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val32.p, x, y, b);
+  k_apply0<float, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_val32.p, x, y, b);
   note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_apply0_32(Context& c, const float* x, float* y, const float* b) {
   TimedLaunch tl(c, K_APPLY0);
-  k_apply0<float, float><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_nbr.p, c.d_val32.p, x, y, b);
+  k_apply0<float, float><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_val32.p, x, y, b);
   note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
