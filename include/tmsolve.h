@@ -211,6 +211,25 @@ tm_status tm_anand_screen_device(const tm_anand_material* mat, int32_t nsites, i
                                  const int32_t* cycle, const int32_t* phase, int32_t cycles,
                                  double* dW_dev, double* dE_dev, double* stab_dev);
 
+/* Screening that allocates no device memory (no counterpart in the reference). For callers that
+ * cannot call cudaMalloc while they screen: a host application whose allocator already owns the
+ * device memory (a caching allocator, a process held to a fixed memory budget), or one that
+ * forbids allocations after start-up because cudaMalloc and cudaFree synchronize the device.
+ * The per-step tables live in a fixed array of the library (TM_NOALLOC_MAX_STEPS steps and
+ * TM_NOALLOC_MAX_TEMPS cycling temperatures at most, about 360 KB), which every GPU that loads
+ * the library holds until the process exits; larger inputs are refused with TM_BAD_INPUT.
+ * The caller passes the strain table and the three outputs in device memory (nsites doubles
+ * each) and the time history, temperatures and material tables on the host; stream may be NULL.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture. Every call shares the
+ * array and overwrites it: calls that overlap on the GPU (other threads, other streams) race. */
+#define TM_NOALLOC_MAX_STEPS 4096
+#define TM_NOALLOC_MAX_TEMPS 512
+tm_status tm_anand_screen_noalloc(const tm_anand_material* mat, int32_t nsites, int32_t ntemps, const double* temps,
+                                  const double* table_dev, int32_t nsteps, const double* t, const double* T,
+                                  const int32_t* cycle, const int32_t* phase, int32_t cycles,
+                                  double* dW_dev, double* dE_dev, double* stab_dev, void* stream);
+
 /* Batched material-point steps: npts independent points, each with a 12-double state
  * (ep[6], s, ebar, W, sigEq, lastD, spare) updated in place when commit != 0;
  * eps (6 per point) engineering mechanical strain; sig (6 per point) and, when

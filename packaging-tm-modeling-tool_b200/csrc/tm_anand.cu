@@ -329,3 +329,122 @@ void anand_step_device(const tm_anand_material& mat, int npts, double* state_d, 
 }
 
 }  // namespace tmg
+
+// ---- screening without device allocation -----------------------------------------------------------
+// Some callers cannot allocate device memory at the time they screen: a host application whose
+// allocator already owns the device memory (a caching allocator, or a process held to a fixed
+// memory budget), or one that forbids allocations after start-up because cudaMalloc/cudaFree
+// synchronize the device. For them, tm_anand_screen_noalloc keeps its per-step tables in this
+// fixed array, which every GPU that loads the library holds until the process exits.
+namespace tmg {
+namespace {
+
+constexpr int NA_STEPS = TM_NOALLOC_MAX_STEPS;
+constexpr int NA_TEMPS = TM_NOALLOC_MAX_TEMPS;
+// byte offsets of the tables inside the array (every table 256-byte aligned)
+constexpr size_t NA_ALIGN(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t NA_KC = 0;
+constexpr size_t NA_WT = NA_KC + NA_ALIGN(sizeof(StepK) * NA_STEPS);
+constexpr size_t NA_FTH = NA_WT + NA_ALIGN(sizeof(double) * NA_STEPS);
+constexpr size_t NA_TT = NA_FTH + NA_ALIGN(sizeof(double) * NA_STEPS);
+constexpr size_t NA_TK = NA_TT + NA_ALIGN(sizeof(double) * NA_STEPS);
+constexpr size_t NA_WI = NA_TK + NA_ALIGN(sizeof(double) * NA_STEPS);
+constexpr size_t NA_CYC = NA_WI + NA_ALIGN(sizeof(int) * NA_STEPS);
+constexpr size_t NA_PH = NA_CYC + NA_ALIGN(sizeof(int) * NA_STEPS);
+constexpr size_t NA_TEMPSOFF = NA_PH + NA_ALIGN(sizeof(int) * NA_STEPS);
+constexpr size_t NA_ETAB = NA_TEMPSOFF + NA_ALIGN(sizeof(double) * NA_TEMPS);
+constexpr size_t NA_FTAB = NA_ETAB + NA_ALIGN(sizeof(double) * TGRID_N);
+constexpr size_t NA_BYTES = NA_FTAB + NA_ALIGN(sizeof(double) * TGRID_N);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+// device address of g_noalloc_scratch per device, looked up once per device with it current
+constexpr int NA_MAX_DEVICES = 64;
+unsigned char* g_noalloc_addr[NA_MAX_DEVICES] = {nullptr};
+
+unsigned char* noalloc_scratch_address() {
+  int dev = 0;
+  TM_CUDA_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NA_MAX_DEVICES) fail(TM_BAD_INPUT, "device index beyond the no-allocation scratch table");
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) fail(TM_CUDA, std::string("cudaGetSymbolAddress of the screening scratch: ") + cudaGetErrorString(e));
+    g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+
+// per-step interpolation weights and thermal strains of screenJoints (13-fatigue.js:395-401), on the device
+__global__ void k_step_weights(int nsteps, int ntemps, const double* __restrict__ temps, const double* __restrict__ T,
+                               const double* __restrict__ Ftab, int* __restrict__ wi, double* __restrict__ wt, double* __restrict__ Fth) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nsteps) return;
+  const double Tk = T[k];
+  int i;
+  if (Tk <= temps[0]) i = 0;
+  else if (Tk >= temps[ntemps - 1]) i = ntemps - 2;
+  else {
+    int lo = 0, hi = ntemps - 1;
+    while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (temps[mid] <= Tk) lo = mid; else hi = mid; }
+    i = lo;
+  }
+  wi[k] = i;
+  const double tt = (Tk - temps[i]) / (temps[i + 1] - temps[i]);
+  wt[k] = tt < 0 ? 0 : (tt > 1 ? 1 : tt);
+  Fth[k] = grid_at(Ftab, Tk) - grid_at(Ftab, 25);
+}
+
+}  // namespace
+}  // namespace tmg
+
+extern "C" tm_status tm_anand_screen_noalloc(const tm_anand_material* mat, int32_t nsites, int32_t ntemps, const double* temps,
+                                             const double* table_dev, int32_t nsteps, const double* t, const double* T,
+                                             const int32_t* cycle, const int32_t* phase, int32_t cycles, double* dW_dev,
+                                             double* dE_dev, double* stab_dev, void* stream) {
+  using namespace tmg;
+  try {
+    if (!mat || !temps || !table_dev || !t || !T || !cycle || !phase || !dW_dev || !dE_dev || !stab_dev)
+      fail(TM_BAD_INPUT, "null argument");
+    if (nsteps < 2 || ntemps < 2 || cycles < 1) fail(TM_BAD_INPUT, "anand screening: need >= 2 time steps, >= 2 temperatures, >= 1 cycle");
+    if (nsteps > NA_STEPS) fail(TM_BAD_INPUT, "tm_anand_screen_noalloc: more than TM_NOALLOC_MAX_STEPS time steps");
+    if (ntemps > NA_TEMPS) fail(TM_BAD_INPUT, "tm_anand_screen_noalloc: more than TM_NOALLOC_MAX_TEMPS temperatures");
+    for (int k = 0; k < nsteps; k++)
+      if (cycle[k] < 0 || cycle[k] > cycles) fail(TM_BAD_INPUT, "anand screening: cycle index out of range");
+    if (nsites <= 0) return TM_OK;
+    int i25 = -1;
+    for (int i = 0; i < ntemps; i++) if (temps[i] == 25) { i25 = i; break; }
+    unsigned char* base = noalloc_scratch_address();
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    StepK* kc = reinterpret_cast<StepK*>(base + NA_KC);
+    double* wt = reinterpret_cast<double*>(base + NA_WT);
+    double* Fth = reinterpret_cast<double*>(base + NA_FTH);
+    double* tt = reinterpret_cast<double*>(base + NA_TT);
+    double* Tk = reinterpret_cast<double*>(base + NA_TK);
+    int* wi = reinterpret_cast<int*>(base + NA_WI);
+    int* cyc = reinterpret_cast<int*>(base + NA_CYC);
+    int* ph = reinterpret_cast<int*>(base + NA_PH);
+    double* tmp = reinterpret_cast<double*>(base + NA_TEMPSOFF);
+    double* Et = reinterpret_cast<double*>(base + NA_ETAB);
+    double* Ft = reinterpret_cast<double*>(base + NA_FTAB);
+    TM_CUDA_CHECK(cudaMemcpyAsync(tt, t, sizeof(double) * nsteps, cudaMemcpyHostToDevice, s));
+    TM_CUDA_CHECK(cudaMemcpyAsync(Tk, T, sizeof(double) * nsteps, cudaMemcpyHostToDevice, s));
+    TM_CUDA_CHECK(cudaMemcpyAsync(cyc, cycle, sizeof(int) * nsteps, cudaMemcpyHostToDevice, s));
+    TM_CUDA_CHECK(cudaMemcpyAsync(ph, phase, sizeof(int) * nsteps, cudaMemcpyHostToDevice, s));
+    TM_CUDA_CHECK(cudaMemcpyAsync(tmp, temps, sizeof(double) * ntemps, cudaMemcpyHostToDevice, s));
+    TM_CUDA_CHECK(cudaMemcpyAsync(Et, mat->Etab, sizeof(double) * TGRID_N, cudaMemcpyHostToDevice, s));
+    TM_CUDA_CHECK(cudaMemcpyAsync(Ft, mat->Ftab, sizeof(double) * TGRID_N, cudaMemcpyHostToDevice, s));
+    const AnandConst P = to_const(*mat);
+    k_step_constants<<<(nsteps + 127) / 128, 128, 0, s>>>(P, Et, nsteps, tt, Tk, kc);
+    k_step_weights<<<(nsteps + 127) / 128, 128, 0, s>>>(nsteps, ntemps, tmp, Tk, Ft, wi, wt, Fth);
+    k_screen<<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_dev, nsteps, wi, wt, Fth, kc, Tk, cyc, ph, cycles, dW_dev,
+                                              dE_dev, stab_dev);
+    note_launch(3);
+    TM_CUDA_CHECK(cudaGetLastError());
+    TM_CUDA_CHECK(cudaStreamSynchronize(s));
+    return TM_OK;
+  } catch (const Error& e) {
+    set_last_error(e.msg);
+    return e.status;
+  }
+}

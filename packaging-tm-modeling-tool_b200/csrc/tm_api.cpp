@@ -24,6 +24,8 @@ namespace tmg {
 
 thread_local std::string g_last_error;
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 void fail(tm_status st, const std::string& msg) { throw Error{st, msg}; }
 
 void cuda_check(cudaError_t e, const char* what) {

@@ -17,6 +17,7 @@ struct Error {
   std::string msg;
 };
 [[noreturn]] void fail(tm_status st, const std::string& msg);
+void set_last_error(const std::string& msg);
 void cuda_check(cudaError_t e, const char* what);
 #define TM_CUDA_CHECK(x) ::tmg::cuda_check((x), #x)
 

@@ -91,6 +91,8 @@ def load():
     L.tm_anand_screen.argtypes = [C.POINTER(TmAnandMaterial), C.c_int32, C.c_int32, vp, vp, C.c_int32, vp, vp, vp, vp,
                                   C.c_int32, vp, vp, vp]
     L.tm_anand_screen_device.argtypes = L.tm_anand_screen.argtypes
+    L.tm_anand_screen_noalloc.argtypes = L.tm_anand_screen.argtypes + [vp]
+    L.tm_anand_screen_noalloc.restype = C.c_int32
     L.tm_anand_step.argtypes = [C.POINTER(TmAnandMaterial), C.c_int32, vp, vp, C.c_double, C.c_double, vp, vp, C.c_int32]
     L.tm_set_stream.argtypes = [vp, vp]
     L.tm_launch_count.argtypes = []
