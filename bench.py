@@ -264,9 +264,8 @@ def run_ours(a):
     e2.record(stream)
     for _ in range(a.steps):
         key[0] += 1
-        fh[:] = dm.assemble_step(step)
-        r = dm.solve(fh, key=key[0], tol=1e-8, warm=0, precision=a.precision)
-        uh[:] = r["u"]
+        dm.assemble_step(step, out=fh)
+        r = dm.solve(fh, key=key[0], tol=1e-8, warm=0, precision=a.precision, out=uh)
         e2_iters += r["iters"]
     e3.record(stream)
     torch.cuda.synchronize()

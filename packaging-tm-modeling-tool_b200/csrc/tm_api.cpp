@@ -667,14 +667,14 @@ tm_status tm_solve(tm_ctx* ctx, const double* f, double* u, const tm_solve_opts*
   tm_status g = guarded([&] {
     Context& c = *reinterpret_cast<Context*>(ctx);
     const size_t n = 3 * (size_t)c.nn;
-    for (size_t i = 0; i < n; i++) if (!std::isfinite(f[i])) fail(TM_NONFINITE, "non-finite load vector");
     tm_solve_opts o;
     if (opts) o = *opts; else tm_default_solve_opts(&o);
+    // the load's finiteness is checked on the device (its scaled norm); the staging buffers
+    // persist across calls, so a solve allocates nothing after the first
     c.d_f.upload(f, n, c.stream);
-    DBuf<double> u_dev;
-    u_dev.alloc(n);
-    st = solve_impl(c, c.d_f.p, u_dev.p, o, info);
-    u_dev.download(u, n, c.stream);
+    c.d_uio.alloc(n);
+    st = solve_impl(c, c.d_f.p, c.d_uio.p, o, info);
+    c.d_uio.download(u, n, c.stream);
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   });
   return g != TM_OK ? g : st;

@@ -446,7 +446,7 @@ void build_hierarchy(Context& c) {
   color_lists(nx, ny, c.colStart, c.d_colorCols, c.colorCount, st);
   // level-0 column panels: greedy packing of each colour's columns (in list order) into groups of
   // at most panelCap nodes; a column longer than panelCap forms a group of its own
-  c.panelCap = std::max(128, c.maxColLen);
+  c.panelCap = std::max(TM_PANEL_THREADS, c.maxColLen);
   c.panelMaxCols = 0;
   for (int k = 0; k < 4; k++) {
     std::vector<int> cols;
@@ -466,6 +466,14 @@ void build_hierarchy(Context& c) {
     for (size_t g = 0; g + 1 < gs.size(); g++) c.panelMaxCols = std::max(c.panelMaxCols, gs[g + 1] - gs[g]);
     c.grpCount[k] = (int)gs.size() - 1;
     c.d_grpStart[k].upload(gs, st);
+    std::vector<int> cp(cols.size() + 1, 0);
+    for (size_t q = 0; q < cols.size(); q++) {
+      cp[q] = c.pos[c.colStart[cols[q]]];
+      cp[q + 1] = cp[q] + c.colStart[cols[q] + 1] - c.colStart[cols[q]];
+      if (q > 0 && cp[q] != cp[q - 1] + c.colStart[cols[q - 1] + 1] - c.colStart[cols[q - 1]])
+        fail(TM_BAD_INPUT, "colour columns are not contiguous in position order");
+    }
+    c.d_colPos[k].upload(cp, st);
   }
   c.d_nodeAgg.upload(c.nodeAgg, st);
   c.d_aggStart.upload(c.aggStart, st);
@@ -475,6 +483,9 @@ void build_hierarchy(Context& c) {
   c.d_res0.alloc(3 * (size_t)nn);
   for (size_t l = 0; l < c.shells.size(); l++) {
     ShellLevel& L = *c.shells[l];
+    L.maxColBlocks = 0;
+    for (int cc = 0; cc < L.nx * L.ny; cc++)
+      L.maxColBlocks = std::max(L.maxColBlocks, L.rowPtr[L.colStart[cc + 1]] - L.rowPtr[L.colStart[cc]]);
     L.d_rowPtr.upload(L.rowPtr, st);
     L.d_col.upload(L.col, st);
     L.d_val.alloc(36 * (size_t)L.nb);

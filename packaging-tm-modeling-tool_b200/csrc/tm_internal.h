@@ -54,6 +54,24 @@ struct DBuf {
   }
 };
 
+// launch shape of the level-0 panel smoother: threads per CTA (also the node capacity of a
+// column panel), the resident CTAs per SM its register budget is sized for
+// (FP32 and FP64 builds of the kernel) and the unroll depth of its 27-slot residual loop
+#ifndef TM_PANEL_THREADS
+#define TM_PANEL_THREADS 256
+#endif
+#ifndef TM_PANEL_MINB
+#define TM_PANEL_MINB 8
+#endif
+#ifndef TM_PANEL_MINB_F64
+#define TM_PANEL_MINB_F64 6
+#endif
+#ifndef TM_PANEL_UNROLL
+#define TM_PANEL_UNROLL 3
+#endif
+#define TM_STR_(x) #x
+#define TM_UNROLL(n) _Pragma(TM_STR_(unroll n))
+
 // number of stencil slots of a node: offsets (di, dj, dk) in {-1,0,1}^3, slot = (di+1)*9+(dj+1)*3+(dk+1);
 // ascending slot order is ascending neighbour node id (nodes are numbered z fastest, then y, then x)
 constexpr int NSLOT = 27;
@@ -81,6 +99,7 @@ struct ShellLevel {
   DBuf<float> d_cfInv32;
   DBuf<int> d_colStart;
   int maxm = 0;                        // largest column size in DOFs
+  int maxColBlocks = 0;                // most blocks in the rows of one column
   // colours: columns with (i%2, j%2) = colour, as lists
   DBuf<int> d_colorCols[4];
   int colorCount[4] = {0, 0, 0, 0};
@@ -145,7 +164,7 @@ struct Context {
   int stage = 0;
   bool assembled = false, scaled = false, fp32Ready = false, mgFp32 = false;
   // solver state
-  DBuf<double> d_s, d_f, d_bs, d_x, d_r, d_z, d_p, d_q, d_tmp, d_tmp2;
+  DBuf<double> d_s, d_f, d_uio, d_bs, d_x, d_r, d_z, d_p, d_q, d_tmp, d_tmp2;
   DBuf<double> d_partial, d_scalars;
   DBuf<int> d_jitter;
   // level 0 smoother and transfer
@@ -154,9 +173,10 @@ struct Context {
   int colorCount[4] = {0, 0, 0, 0};
   int maxColLen = 0;
   // level-0 column panels: the columns of one colour packed into groups of at most panelCap nodes,
-  // one CTA per group (group g holds colour columns grpStart[g] .. grpStart[g+1]-1)
-  int panelCap = 128, panelMaxCols = 0;
-  DBuf<int> d_grpStart[4];
+  // one CTA per group (group g holds colour columns grpStart[g] .. grpStart[g+1]-1); colPos holds
+  // the position of the first node of every colour column plus one past the colour's last node
+  int panelCap = TM_PANEL_THREADS, panelMaxCols = 0;
+  DBuf<int> d_grpStart[4], d_colPos[4];
   int grpCount[4] = {0, 0, 0, 0};
   std::vector<int> nodeAgg, aggStart;  // level 0 -> 1
   std::vector<double> zp;              // z of node minus zref of its aggregate

@@ -421,6 +421,11 @@ __global__ void k_factor_columns(int ncol, int nn, const int* __restrict__ colSt
       jit = jit != 0 ? jit * 10 : 1e-10 * fmax(fmax(fabs(D[0]), fabs(D[4])), fmax(fabs(D[8]), 1e-300));
       jitter++;
     }
+    // reciprocal pivots in the upper slots of the lower factor (always 0 in L): the smoother
+    // multiplies by them instead of dividing; the factorisation itself never reads these slots
+    Fn[1] = 1 / Fn[0];
+    Fn[2] = 1 / Fn[4];
+    Fn[5] = 1 / Fn[8];
   }
   if (jitter) atomicAdd(jitterCount, jitter);
 }
@@ -687,7 +692,9 @@ __global__ void k_coarsest_inverse(int n, int bw, const double* __restrict__ A, 
 
 // explicit inverse of every shell column block from its Cholesky factor (warp per column, lanes over
 // unit vectors); the smoother then applies A_cc^-1 as a dense product instead of two serial
-// triangular solves (cholSolveDenseOff, 10-solver.js:497-509, computes the same A_cc^-1 r)
+// triangular solves (cholSolveDenseOff, 10-solver.js:497-509, computes the same A_cc^-1 r).
+// Column e of the inverse is stored contiguously (entry (i, e) at e*m + i), so that the lanes of
+// the smoother, one per row e, read entry (e, k) at k*m + e with coalesced loads.
 __global__ void k_shell_inverse(int ncol, const int* __restrict__ colStart, const long long* __restrict__ cfPtr,
                                 const double* __restrict__ cf, double* __restrict__ cfInv) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -696,17 +703,17 @@ __global__ void k_shell_inverse(int ncol, const int* __restrict__ colStart, cons
   const int m = 6 * (colStart[c + 1] - colStart[c]);
   if (!m) return;
   const double* L = cf + cfPtr[c];
-  double* X = cfInv + cfPtr[c];
   for (int e = lane; e < m; e += 32) {
+    double* Xe = cfInv + cfPtr[c] + (size_t)e * m;
     for (int i = 0; i < m; i++) {
       double s = i == e ? 1.0 : 0.0;
-      for (int k = e; k < i; k++) s -= L[i * m + k] * X[k * m + e];
-      X[i * m + e] = i < e ? 0.0 : s / L[i * m + i];
+      for (int k = e; k < i; k++) s -= L[i * m + k] * Xe[k];
+      Xe[i] = i < e ? 0.0 : s / L[i * m + i];
     }
     for (int i = m - 1; i >= 0; i--) {
-      double s = X[i * m + e];
-      for (int k = i + 1; k < m; k++) s -= L[k * m + i] * X[k * m + e];
-      X[i * m + e] = s / L[i * m + i];
+      double s = Xe[i];
+      for (int k = i + 1; k < m; k++) s -= L[k * m + i] * Xe[k];
+      Xe[i] = s / L[i * m + i];
     }
   }
 }

@@ -29,10 +29,16 @@ __global__ void k_apply0(int nn, const int* __restrict__ posNode, const int* __r
   if (ps >= nn) return;
   const int n = posNode[ps];
   T y0 = 0, y1 = 0, y2 = 0;
-#pragma unroll 3
+  // absent slots hold exact zeros: they read the node's own x, branch-free, ids fetched first
+  int nb[NSLOT];
+#pragma unroll
   for (int s = 0; s < NSLOT; s++) {
     const int j = nbr[(size_t)s * nn + ps];
-    if (j < 0) continue;
+    nb[s] = j < 0 ? n : j;
+  }
+#pragma unroll
+  for (int s = 0; s < NSLOT; s++) {
+    const size_t j = nb[s];
     const T x0 = (T)x[3 * j], x1 = (T)x[3 * j + 1], x2 = (T)x[3 * j + 2];
     const T* v = val + (size_t)s * 9 * nn + ps;
     y0 += v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
@@ -116,52 +122,43 @@ __global__ void k_scale_vec(size_t n, const T* __restrict__ x, const double* __r
 }
 
 // level-0 column smoother on packed column panels: one CTA per group of whole z-columns of one
-// colour (at most cap nodes). Every thread computes the residual rows of one node (coalesced
-// along each column's contiguous nodes), the column factors are staged in shared memory, one
-// thread per column runs the block-tridiagonal forward/backward solve (solveColumn,
-// 10-solver.js:71-104), and every node is then updated, x += dx.
+// colour (at most cap nodes, contiguous in position order). Every thread computes the residual
+// rows of one node (coalesced along each column's contiguous nodes), the column factors are
+// staged in shared memory, one thread per column runs the block-tridiagonal forward/backward
+// solve (solveColumn, 10-solver.js:71-104), and every node is then updated, x += dx.
 template <class T>
-__global__ void __launch_bounds__(128) k_sweep_panel(const int* __restrict__ grpStart, const int* __restrict__ cols,
-                                                      const int* __restrict__ colStart, const int* __restrict__ pos, int nn,
-                                                      const int* __restrict__ nbr,
-                                                      const T* __restrict__ val, const T* __restrict__ F, const T* __restrict__ b,
-                                                      T* __restrict__ x, int cap, int maxCols, int zeroGuess) {
-  extern __shared__ unsigned char smraw[];
+struct PanelMinBlocks { static constexpr int value = TM_PANEL_MINB; };
+template <>
+struct PanelMinBlocks<double> { static constexpr int value = TM_PANEL_MINB_F64; };
+
+template <class T>
+__global__ void __launch_bounds__(TM_PANEL_THREADS, PanelMinBlocks<T>::value)
+    k_sweep_panel(const int* __restrict__ grpStart, const int* __restrict__ colPos, const int* __restrict__ posNode, int nn,
+                  const int* __restrict__ nbr, const T* __restrict__ val, const T* __restrict__ F, const T* __restrict__ b,
+                  T* __restrict__ x, int cap, int zeroGuess) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   T* r = reinterpret_cast<T*>(smraw);            // 3*cap
   T* Fs = r + 3 * cap;                           // 18*cap
-  int* off = reinterpret_cast<int*>(Fs + 18 * cap);   // maxCols+1 node offsets of the columns in the group
-  int* first = off + maxCols + 1;                // first global node of every column
+  int* off = reinterpret_cast<int*>(Fs + 18 * cap);   // node offsets of the group's columns (ncols + 1)
   const int g0 = grpStart[blockIdx.x], ncols = grpStart[blockIdx.x + 1] - g0;
-  if (threadIdx.x == 0) {
-    int o = 0;
-    for (int q = 0; q < ncols; q++) {
-      const int c = cols[g0 + q];
-      off[q] = o;
-      first[q] = colStart[c];
-      o += colStart[c + 1] - colStart[c];
-    }
-    off[ncols] = o;
-  }
-  __syncthreads();
-  const int total = off[ncols];
-  // the group's nodes occupy the contiguous positions gp0 .. gp0+total-1 (column factors included)
-  const size_t gp0 = ncols ? pos[first[0]] : 0;
+  const int gp0 = colPos[g0];
+  const int total = colPos[g0 + ncols] - gp0;
+  for (int q = threadIdx.x; q <= ncols; q += blockDim.x) off[q] = colPos[g0 + q] - gp0;
   {
-    const T* src = F + 18 * gp0;
+    const T* src = F + 18 * (size_t)gp0;
     for (int e = threadIdx.x; e < 18 * total; e += blockDim.x) Fs[e] = src[e];
   }
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    int q = 0;
-    while (off[q + 1] <= t) q++;
-    const int n = first[q] + (t - off[q]);
-    const size_t ps = gp0 + t;
+    const int ps = gp0 + t;
+    const int n = posNode[ps];
     T s0 = b[3 * (size_t)n], s1 = b[3 * (size_t)n + 1], s2 = b[3 * (size_t)n + 2];
     if (!zeroGuess) {
-#pragma unroll 3
+      // absent stencil slots hold exact zeros, so they read the node's own x (branch-free)
+      TM_UNROLL(TM_PANEL_UNROLL)
       for (int s = 0; s < NSLOT; s++) {
-        const int j = nbr[(size_t)s * nn + ps];
-        if (j < 0) continue;
-        const T x0 = x[3 * (size_t)j], x1 = x[3 * (size_t)j + 1], x2 = x[3 * (size_t)j + 2];
+        const int jj = nbr[(size_t)s * nn + ps];
+        const size_t j = jj < 0 ? n : jj;
+        const T x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
         const T* v = val + (size_t)s * 9 * nn + ps;
         s0 -= v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
         s1 -= v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
@@ -182,9 +179,9 @@ __global__ void __launch_bounds__(128) k_sweep_panel(const int* __restrict__ grp
         b1 -= f[12] * p0 + f[13] * p1 + f[14] * p2;
         b2 -= f[15] * p0 + f[16] * p1 + f[17] * p2;
       }
-      const T y0 = b0 / f[0];
-      const T y1 = (b1 - f[3] * y0) / f[4];
-      const T y2 = (b2 - f[6] * y0 - f[7] * y1) / f[8];
+      const T y0 = b0 * f[1];
+      const T y1 = (b1 - f[3] * y0) * f[2];
+      const T y2 = (b2 - f[6] * y0 - f[7] * y1) * f[5];
       r[3 * l] = y0; r[3 * l + 1] = y1; r[3 * l + 2] = y2;
     }
     for (int l = l1 - 1; l >= l0; l--) {
@@ -197,17 +194,15 @@ __global__ void __launch_bounds__(128) k_sweep_panel(const int* __restrict__ grp
         b1 -= gg[10] * q0 + gg[13] * q1 + gg[16] * q2;
         b2 -= gg[11] * q0 + gg[14] * q1 + gg[17] * q2;
       }
-      const T z2 = b2 / f[8];
-      const T z1 = (b1 - f[7] * z2) / f[4];
-      const T z0 = (b0 - f[3] * z1 - f[6] * z2) / f[0];
+      const T z2 = b2 * f[5];
+      const T z1 = (b1 - f[7] * z2) * f[2];
+      const T z0 = (b0 - f[3] * z1 - f[6] * z2) * f[1];
       r[3 * l] = z0; r[3 * l + 1] = z1; r[3 * l + 2] = z2;
     }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    int q = 0;
-    while (off[q + 1] <= t) q++;
-    const size_t n = first[q] + (t - off[q]);
+    const size_t n = posNode[gp0 + t];
     x[3 * n] += r[3 * t]; x[3 * n + 1] += r[3 * t + 1]; x[3 * n + 2] += r[3 * t + 2];
   }
 }
@@ -244,56 +239,133 @@ __global__ void k_prolong0(int nn, const int* __restrict__ nodeAgg, const T* __r
   }
 }
 
-// shell-level residual res = b - K x (6x6 block CSR), thread per (row, component)
-template <class T>
-__global__ void k_apply_shell(int nrow, const int* __restrict__ rowPtr, const int* __restrict__ col, const T* __restrict__ val,
-                              const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ y) {
-  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (t >= 6 * (size_t)nrow) return;
-  const int i = (int)(t / 6), p = (int)(t % 6);
-  T s = 0;
-#pragma unroll 4
-  for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
-    const T* v = val + 36 * (size_t)k + 6 * p;
-    const T* xj = x + 6 * (size_t)col[k];
-    s += v[0] * xj[0] + v[1] * xj[1] + v[2] * xj[2] + v[3] * xj[3] + v[4] * xj[4] + v[5] * xj[5];
+// ---- shell levels (6x6 block CSR, a column's aggregates are a contiguous row range) -----------
+
+// the 36 values of one 6x6 block with 16-byte loads (blocks start on 16-byte boundaries)
+__device__ __forceinline__ void load_block36(const float* __restrict__ p, float (&v)[36]) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    const float4 t = __ldg(q + i);
+    v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
   }
-  y[t] = b ? b[t] - s : s;
+}
+__device__ __forceinline__ void load_block36(const double* __restrict__ p, double (&v)[36]) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int i = 0; i < 18; i++) {
+    const double2 t = __ldg(q + i);
+    v[2 * i] = t.x; v[2 * i + 1] = t.y;
+  }
 }
 
-// shell-level column sweep: warp per column of one colour (columnSweep shell branch, 10-solver.js:535-553)
+// rows of the column inverse a lane keeps in registers when the column block is small
+constexpr int SH_PRE = 18;
+
+// per-warp shared staging of the shell column kernels: the 6 partial sums of every block of the
+// column's rows, the m residual rows (at least SH_PRE) and the local row starts
 template <class T>
-__global__ void k_sweep_shell(int ncolc, const int* __restrict__ cols, const int* __restrict__ colStart, const int* __restrict__ rowPtr,
-                              const int* __restrict__ col, const T* __restrict__ val, const long long* __restrict__ cfPtr,
-                              const T* __restrict__ cf, const T* __restrict__ b, T* __restrict__ x, int maxm, int zeroGuess) {
-  extern __shared__ unsigned char smraw[];
-  T* sm = reinterpret_cast<T*>(smraw);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (gw >= ncolc) return;
-  T* r = sm + (size_t)warp * maxm;
-  const int c = cols[gw];
-  const int n0 = colStart[c], m = 6 * (colStart[c + 1] - n0);
+__host__ __device__ inline size_t shell_stage_bytes(int maxm, int maxBlk) {
+  const int rlen = maxm > SH_PRE ? maxm : SH_PRE;
+  const size_t b = sizeof(T) * (6 * (size_t)maxBlk + rlen) + sizeof(int) * ((size_t)maxm / 6 + 1);
+  return (b + 15) / 16 * 16;
+}
+
+// residual rows r = b - K x of the column whose aggregates are n0 .. n0+na-1, by one warp: the
+// lanes take the column's blocks (all rows together), each lane's 6 products of a block land in
+// shared memory, and lane e then subtracts its row's block sums in block order, as the serial
+// row loop of columnSweep (10-solver.js:535-553) does
+template <class T>
+__device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, const int* __restrict__ rowPtr,
+                                                      const int* __restrict__ col, const T* __restrict__ val,
+                                                      const T* __restrict__ b, const T* __restrict__ x, bool zeroGuess,
+                                                      T* part, T* r, int* rp) {
+  const int m = 6 * na;
+  if (zeroGuess) {
+    for (int e = lane; e < m; e += 32) r[e] = b[6 * (size_t)n0 + e];
+    __syncwarp();
+    return;
+  }
+  const int k0 = rowPtr[n0];
+  for (int q = lane; q <= na; q += 32) rp[q] = rowPtr[n0 + q] - k0;
+  const int nblk = rowPtr[n0 + na] - k0;
+  for (int e = lane; e < nblk; e += 32) {
+    const T* xj = x + 6 * (size_t)col[k0 + e];
+    T v[36];
+    load_block36(val + 36 * (size_t)(k0 + e), v);
+    const T x0 = xj[0], x1 = xj[1], x2 = xj[2], x3 = xj[3], x4 = xj[4], x5 = xj[5];
+#pragma unroll
+    for (int p = 0; p < 6; p++)
+      part[6 * e + p] = v[6 * p] * x0 + v[6 * p + 1] * x1 + v[6 * p + 2] * x2 + v[6 * p + 3] * x3 + v[6 * p + 4] * x4 + v[6 * p + 5] * x5;
+  }
+  __syncwarp();
   for (int e = lane; e < m; e += 32) {
-    const int a = n0 + e / 6, p = e % 6;
-    T s = b[6 * (size_t)a + p];
-    if (!zeroGuess) {
-#pragma unroll 4
-      for (int k = rowPtr[a]; k < rowPtr[a + 1]; k++) {
-        const T* v = val + 36 * (size_t)k + 6 * p;
-        const T* xj = x + 6 * (size_t)col[k];
-        s -= v[0] * xj[0] + v[1] * xj[1] + v[2] * xj[2] + v[3] * xj[3] + v[4] * xj[4] + v[5] * xj[5];
-      }
-    }
+    const int a = e / 6, p = e % 6;
+    T s = b[6 * (size_t)n0 + e];
+    for (int k = rp[a]; k < rp[a + 1]; k++) s -= part[6 * k + p];
     r[e] = s;
   }
   __syncwarp();
-  // x_col += A_cc^-1 r_col with the explicit inverse of the column block (row e per lane)
-  const T* Ai = cf + cfPtr[c];
+}
+
+// shell-level residual res = b - K x over all columns, warp per column
+template <class T>
+__global__ void __launch_bounds__(128) k_apply_shell(int ncol, const int* __restrict__ colStart, const int* __restrict__ rowPtr,
+                                                     const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ x,
+                                                     const T* __restrict__ b, T* __restrict__ y, int maxm, int maxBlk) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (c >= ncol) return;
+  unsigned char* base = smraw + (size_t)warp * shell_stage_bytes<T>(maxm, maxBlk);
+  T* part = reinterpret_cast<T*>(base);
+  T* r = part + 6 * (size_t)maxBlk;
+  int* rp = reinterpret_cast<int*>(r + (maxm > SH_PRE ? maxm : SH_PRE));
+  const int n0 = colStart[c], na = colStart[c + 1] - n0;
+  shell_column_residual(lane, n0, na, rowPtr, col, val, b, x, false, part, r, rp);
+  for (int e = lane; e < 6 * na; e += 32) y[6 * (size_t)n0 + e] = r[e];
+}
+
+// shell-level column sweep, warp per column of one colour (columnSweep shell branch,
+// 10-solver.js:535-553): r = b - K x over the column's rows, then x_col += A_cc^-1 r with the
+// explicit inverse of the column block. For blocks of at most SH_PRE rows every lane fetches its
+// row of the inverse before the residual, so that those loads overlap the residual's.
+template <class T>
+__global__ void __launch_bounds__(128) k_sweep_shell(int ncolc, const int* __restrict__ cols, const int* __restrict__ colStart,
+                                                     const int* __restrict__ rowPtr, const int* __restrict__ col,
+                                                     const T* __restrict__ val, const long long* __restrict__ cfPtr,
+                                                     const T* __restrict__ cf, const T* __restrict__ b, T* __restrict__ x, int maxm,
+                                                     int maxBlk, int zeroGuess) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (gw >= ncolc) return;
+  unsigned char* base = smraw + (size_t)warp * shell_stage_bytes<T>(maxm, maxBlk);
+  T* part = reinterpret_cast<T*>(base);
+  T* r = part + 6 * (size_t)maxBlk;
+  int* rp = reinterpret_cast<int*>(r + (maxm > SH_PRE ? maxm : SH_PRE));
+  const int c = cols[gw];
+  const int n0 = colStart[c], na = colStart[c + 1] - n0, m = 6 * na;
+  const T* Ai = cf + cfPtr[c];   // entry (e, k) at k*m + e
+  T a[SH_PRE];
+  const bool pre = m <= SH_PRE;
+#pragma unroll
+  for (int k = 0; k < SH_PRE; k++) a[k] = (pre && lane < m && k < m) ? Ai[(size_t)k * m + lane] : (T)0;
+  shell_column_residual(lane, n0, na, rowPtr, col, val, b, x, zeroGuess != 0, part, r, rp);
+  if (pre) {
+    if (lane < m) {
+      T acc = 0;
+#pragma unroll
+      for (int k = 0; k < SH_PRE; k++)
+        if (k < m) acc += a[k] * r[k];
+      x[6 * (size_t)n0 + lane] += acc;
+    }
+    return;
+  }
   for (int e = lane; e < m; e += 32) {
     T acc = 0;
-    const T* row = Ai + (size_t)e * m;
-    for (int k = 0; k < m; k++) acc += row[k] * r[k];
+#pragma unroll 6
+    for (int k = 0; k < m; k++) acc += Ai[(size_t)k * m + e] * r[k];
     x[6 * (size_t)n0 + e] += acc;
   }
 }
@@ -400,23 +472,29 @@ void vcycle(Context& c, const T* r, T* z) {
   typedef Bufs<T> B;
   cudaStream_t st = c.stream;
   const int nn = c.nn;
-  const int warps = 4;
-  const size_t smem0 = (size_t)21 * c.panelCap * sizeof(T) + 2 * (size_t)(c.panelMaxCols + 1) * sizeof(int);
+  const size_t smem0 = (size_t)21 * c.panelCap * sizeof(T) + (size_t)(c.panelMaxCols + 1) * sizeof(int);
   TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(T), st));
   if (smem0 > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
   auto sweep0 = [&](int col, int zero) {
     if (!c.grpCount[col]) return;
     TimedLaunch tl(c, K_SWEEP_SOLID);
-    k_sweep_panel<T><<<c.grpCount[col], 128, smem0, st>>>(c.d_grpStart[col].p, c.d_colorCols[col].p, c.d_colStart.p, c.d_pos.p, nn, c.d_nbr.p,
-                                                         B::val0(c), B::F(c), r, z, c.panelCap, c.panelMaxCols, zero);
+    k_sweep_panel<T><<<c.grpCount[col], TM_PANEL_THREADS, smem0, st>>>(c.d_grpStart[col].p, c.d_colPos[col].p, c.d_posNode.p, nn,
+                                                                      c.d_nbr.p, B::val0(c), B::F(c), r, z, c.panelCap, zero);
     note_launch();
   };
+  const int wpb = 4;
+  size_t smemS = 0;
+  for (auto& Lp : c.shells) smemS = std::max(smemS, wpb * shell_stage_bytes<T>(Lp->maxm, Lp->maxColBlocks));
+  if (smemS > 48 * 1024) {
+    TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_shell<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemS));
+    TM_CUDA_CHECK(cudaFuncSetAttribute(k_apply_shell<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemS));
+  }
   auto sweepS = [&](ShellLevel& L, int col, int zero) {
-    const size_t smem = (size_t)warps * L.maxm * sizeof(T);
+    const size_t per = shell_stage_bytes<T>(L.maxm, L.maxColBlocks);
     TimedLaunch tl(c, K_SWEEP_SHELL);
-    k_sweep_shell<T><<<grid_for(L.colorCount[col], warps), 32 * warps, smem, st>>>(
+    k_sweep_shell<T><<<grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st>>>(
         L.colorCount[col], L.d_colorCols[col].p, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, B::val(L), L.d_cfPtr.p, B::cf(L), B::b(L),
-        B::x(L), L.maxm, zero);
+        B::x(L), L.maxm, L.maxColBlocks, zero);
     note_launch();
   };
   // ---- level 0 pre-smoothing: 2 sweeps in colours 0..3
@@ -454,7 +532,9 @@ void vcycle(Context& c, const T* r, T* z) {
       }
     {
       TimedLaunch tl(c, K_APPLY_SHELL);
-      k_apply_shell<T><<<grid_for(6 * (size_t)L.nn, 128), 128, 0, st>>>(L.nn, L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L));
+      const int ncol = L.nx * L.ny;
+      k_apply_shell<T><<<grid_for(ncol, wpb), 32 * wpb, wpb * shell_stage_bytes<T>(L.maxm, L.maxColBlocks), st>>>(
+          ncol, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L), L.maxm, L.maxColBlocks);
       note_launch();
     }
     ShellLevel& C = *c.shells[l + 1];

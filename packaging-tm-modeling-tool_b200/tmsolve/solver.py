@@ -28,6 +28,14 @@ def _p(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype)) if a is not None else None
 
 
+def _out_array(out, n):
+    if out is None:
+        return np.zeros(n)
+    if out.dtype != np.float64 or out.shape != (n,) or not out.flags.c_contiguous:
+        raise ValueError(f"out must be a contiguous float64 array of {n} values")
+    return out
+
+
 class DeviceModel:
     def __init__(self, pkg: Package, constraints: Optional[np.ndarray] = None):
         L = load()
@@ -75,13 +83,14 @@ class DeviceModel:
             pass
 
     # ---- FEModel.assembleStep ------------------------------------------------------------
-    def assemble_step(self, step: StepData) -> np.ndarray:
+    def assemble_step(self, step: StepData, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The load vector of the step (host array; `out`, e.g. pinned memory, is filled when given)."""
         lay = np.ascontiguousarray(step.layered, np.int32); born = np.ascontiguousarray(step.born, np.int32)
         D = np.ascontiguousarray(step.D, np.float64); s0 = np.ascontiguousarray(step.s0, np.float64)
         W = np.ascontiguousarray(step.W, np.float64); V = np.ascontiguousarray(step.V, np.float64)
         st = TmStep(stage=int(step.stage), psetLayered=_p(lay, C.c_int32), D=_p(D, C.c_double), s0=_p(s0, C.c_double),
                     W=_p(W, C.c_double), V=_p(V, C.c_double), psetBorn=_p(born, C.c_int32))
-        rhs = np.zeros(self.ndof)
+        rhs = _out_array(out, self.ndof)
         check(load().tm_assemble_step(self.h, C.byref(st), rhs.ctypes.data_as(C.c_void_p)))
         return rhs
 
@@ -130,9 +139,11 @@ class DeviceModel:
                     warm=int(info.warm), iters0=float(info.iters0), fallback=None if not info.fallback else True,
                     jitter=int(info.jitter_count), levels=int(info.levels), refinements=int(info.refinements))
 
-    def solve(self, f, label=None, key=-1, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64") -> dict:
+    def solve(self, f, label=None, key=-1, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64",
+              out: Optional[np.ndarray] = None) -> dict:
+        """LinearSolver.solve with host arrays; the displacement goes to `out` when given."""
         f = np.ascontiguousarray(f, np.float64)
-        u = np.zeros(self.ndof)
+        u = _out_array(out, self.ndof)
         info = TmSolveInfo()
         o = self.make_opts(tol, maxit, warm, precond, precision, key)
         check(load().tm_solve(self.h, f.ctypes.data_as(C.c_void_p), u.ctypes.data_as(C.c_void_p), C.byref(o), C.byref(info)),
