@@ -231,6 +231,67 @@ ShellLevel* build_coarse_shell(ShellLevel& L) {
   return Cp;
 }
 
+// position of coarse column J in the sorted block row I, or -1
+int block_of(const ShellLevel& C, int I, int J) {
+  const int* b = C.col.data() + C.rowPtr[I];
+  const int* e = C.col.data() + C.rowPtr[I + 1];
+  const int* q = std::lower_bound(b, e, J);
+  return (q != e && *q == J) ? C.rowPtr[I] + (int)(q - b) : -1;
+}
+
+// level 0 -> 1 contribution lists (the summands of galerkinProduct, 10-solver.js:193-245, grouped
+// by the coarse block they land in); counting sort over (slot, position) keeps that order per block
+void galerkin_lists01(Context& c, cudaStream_t st) {
+  const ShellLevel& L1 = *c.shells[0];
+  const int nn = c.nn;
+  std::vector<int> start((size_t)L1.nb + 1, 0);
+  auto visit = [&](auto&& emit) {
+    for (int s = 0; s < NSLOT; s++)
+      for (int ps = 0; ps < nn; ps++) {
+        const int i = c.posNode[ps];
+        if (!(c.slotMask[i] >> s & 1)) continue;
+        const int k = block_of(L1, c.nodeAgg[i], c.nodeAgg[c.nbr[(size_t)s * nn + i]]);
+        if (k < 0) fail(TM_BAD_INPUT, "level-1 Galerkin pattern misses a stencil coupling");
+        emit(k, ps * NSLOT + s);
+      }
+  };
+  visit([&](int k, int) { start[k + 1]++; });
+  for (size_t k = 0; k < (size_t)L1.nb; k++) start[k + 1] += start[k];
+  std::vector<int> list((size_t)start.back()), fill(start.begin(), start.end() - 1);
+  visit([&](int k, int code) { list[fill[k]++] = code; });
+  c.d_g01Start.upload(start, st);
+  c.d_g01List.upload(list, st);
+}
+
+// shell level F -> C contribution lists: (fine block, row weight entry, column weight entry) per
+// summand of the 6x6 galerkinProduct, in (coarse row child, fine block, column parent) order
+void galerkin_lists_shell(const ShellLevel& F, ShellLevel& C, cudaStream_t st) {
+  std::vector<int> start((size_t)C.nb + 1, 0);
+  auto visit = [&](auto&& emit) {
+    for (int I = 0; I < C.nn; I++)
+      for (int q = F.chPtr[I]; q < F.chPtr[I + 1]; q++) {
+        const int f = F.chIdx[q];
+        for (int k = F.rowPtr[f]; k < F.rowPtr[f + 1]; k++) {
+          const int g = F.col[k];
+          for (int p = F.prolPtr[g]; p < F.prolPtr[g + 1]; p++) {
+            const int b = block_of(C, I, F.prolIdx[p]);
+            if (b < 0) fail(TM_BAD_INPUT, "shell Galerkin pattern misses a coupling");
+            emit(b, k, F.chW[q], p);
+          }
+        }
+      }
+  };
+  visit([&](int b, int, int, int) { start[b + 1]++; });
+  for (size_t b = 0; b < (size_t)C.nb; b++) start[b + 1] += start[b];
+  std::vector<int> list(3 * (size_t)start.back()), fill(start.begin(), start.end() - 1);
+  visit([&](int b, int k, int p1, int p2) {
+    const size_t t = 3 * (size_t)fill[b]++;
+    list[t] = k; list[t + 1] = p1; list[t + 2] = p2;
+  });
+  C.d_galStart.upload(start, st);
+  C.d_galList.upload(list, st);
+}
+
 void column_factor_sizes(ShellLevel& L) {
   const int ncol = L.nx * L.ny;
   L.cfPtr.assign(ncol + 1, 0);
@@ -477,6 +538,8 @@ void build_hierarchy(Context& c) {
   }
   c.d_nodeAgg.upload(c.nodeAgg, st);
   c.d_aggStart.upload(c.aggStart, st);
+  galerkin_lists01(c, st);
+  for (size_t l = 0; l + 1 < c.shells.size(); l++) galerkin_lists_shell(*c.shells[l], *c.shells[l + 1], st);
   c.d_zp.upload(c.zp, st);
   c.d_W01.alloc(18 * (size_t)nn);
   c.d_F.alloc(18 * (size_t)nn);

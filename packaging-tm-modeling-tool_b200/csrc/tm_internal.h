@@ -112,6 +112,9 @@ struct ShellLevel {
   // children of the next level's aggregates (transposeProl)
   std::vector<int> chPtr, chIdx, chW;
   DBuf<int> d_chPtr, d_chIdx, d_chW;
+  // Galerkin contributions into this level's blocks from the finer shell level: per block a list
+  // of (fine block, weight entry of the row child, weight entry of the column child) triples
+  DBuf<int> d_galStart, d_galList;
   // Galerkin pattern bookkeeping for this level as a coarse level: max blocks per row
   int maxRowBlocks = 0;
   // work vectors
@@ -120,7 +123,10 @@ struct ShellLevel {
   // coarsest level: banded factor and explicit inverse
   bool coarsest = false;
   int bandBw = 0, denseN = 0;
-  DBuf<double> d_band;                 // denseN*(bw+1)
+  DBuf<double> d_band;                 // denseN*(bw+1): the operator's lower band, then its Schur complements
+  DBuf<double> d_bandL;                // denseN*(bw+1): the banded Cholesky factor
+  DBuf<double> d_dinv;                 // inverses of the factor's 32x32 diagonal blocks
+  DBuf<double> d_jit;                  // pivot floor of the factor
   DBuf<double> d_inv;                  // denseN*denseN
   DBuf<float> d_inv32;
 };
@@ -181,6 +187,9 @@ struct Context {
   std::vector<int> nodeAgg, aggStart;  // level 0 -> 1
   std::vector<double> zp;              // z of node minus zref of its aggregate
   DBuf<int> d_nodeAgg, d_aggStart;
+  // Galerkin contributions of the solid operator to the level-1 blocks: per block the
+  // (position, slot) pairs, coded position*27 + slot, in (slot, position) order
+  DBuf<int> d_g01Start, d_g01List;
   DBuf<double> d_zp, d_W01;            // 18 per node
   int maxRowBlocks1 = 0;
   DBuf<double> d_res0;                 // level-0 residual

@@ -1,9 +1,10 @@
 // Per-step numeric set-up on the GPU: element condensation, stencil assembly, constraints,
-// Jacobi scaling, column factors, Galerkin coarse operators and coarsest factor.
+// Jacobi scaling, level-0 column factors, transfer weights and shell column factors (the
+// Galerkin products and the coarsest factor are in tm_coarse.cu).
 //
-// This file is compiled with -fmad=false: every set-up quantity is then computed with the
-// same operations in the same order as the reference (JavaScript has no fused multiply-add),
-// so the assembled operator and the multigrid set-up are bit-identical to the FP64 oracle.
+// This file is compiled with -fmad=false: every quantity here is then computed with the same
+// operations in the same order as the reference (JavaScript has no fused multiply-add), so the
+// assembled operator is bit-identical to the FP64 oracle.
 //
 // Reference lines followed:
 //   shapeMatrices / elementK33Fast / elementFth   src/core/09-assembly.js:69-133 (UNIV :26-60)
@@ -12,9 +13,8 @@
 //   applyConstraints                              src/core/09-assembly.js:445-464
 //   LinearSolver._scale                           src/core/10-solver.js:852-866
 //   factorColumns / chol3                         src/core/10-solver.js:12-68
-//   shellWeights / galerkinProduct                src/core/10-solver.js:193-245, 337-353
+//   shellWeights                                  src/core/10-solver.js:337-353
 //   factorShellColumns                            src/core/10-solver.js:474-494
-//   factorCoarsest                                src/core/10-solver.js:562-600
 #include <cmath>
 #include <cstring>
 
@@ -442,128 +442,6 @@ __global__ void k_w01(int nn, const double* __restrict__ s, const double* __rest
   w[14] = 1 / s[3 * n + 2]; w[17] = z / s[3 * n + 2];
 }
 
-__device__ __forceinline__ int find_col(const int* cols, int n, int J) {
-  int lo = 0, hi = n - 1;
-  while (lo <= hi) {
-    const int mid = (lo + hi) >> 1;
-    const int v = cols[mid];
-    if (v == J) return mid;
-    if (v < J) lo = mid + 1; else hi = mid - 1;
-  }
-  return -1;
-}
-
-// galerkinProduct 0 -> 1 (10-solver.js:193-245), warp per coarse row, same summation order
-__global__ void k_galerkin01(int na, int nn, const int* __restrict__ aggStart, const int* __restrict__ nodeAgg, const int* __restrict__ pos,
-                             const int* __restrict__ nbr, const int* __restrict__ slotMask, const double* __restrict__ val,
-                             const double* __restrict__ W, const int* __restrict__ rowPtr, const int* __restrict__ col,
-                             int maxRow, double* __restrict__ out) {
-  extern __shared__ double sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int I = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (I >= na) return;
-  double* acc = sm + (size_t)warp * maxRow * 36;
-  const int r0 = rowPtr[I], nJ = rowPtr[I + 1] - r0;
-  for (int e = lane; e < nJ * 36; e += 32) acc[e] = 0;
-  __syncwarp();
-  const int e0 = lane, e1 = lane + 32;
-  const int rA = e0 / 6, cA = e0 % 6, rB = e1 / 6, cB = e1 % 6;
-  for (int i = aggStart[I]; i < aggStart[I + 1]; i++) {
-    const int mask = slotMask[i];
-    const int pi = pos[i];
-    const double* Wi = W + 18 * (size_t)i;
-    for (int s = 0; s < NSLOT; s++) {
-      if (!(mask >> s & 1)) continue;
-      const int j = nbr[(size_t)s * nn + pi];
-      const int loc = find_col(col + r0, nJ, nodeAgg[j]);
-      if (loc < 0) continue;   // cannot happen for a pattern built from the same mesh; never write outside acc
-      const double* Wj = W + 18 * (size_t)j;
-      double kv[9];
-      for (int v = 0; v < 9; v++) kv[v] = val[((size_t)s * 9 + v) * nn + pi];
-      // T (3x6) = K_ij W_j ; acc += W_i^T T
-      {
-        double T[3];
-        for (int r = 0; r < 3; r++) {
-          double sum = 0;
-          for (int t = 0; t < 3; t++) sum += kv[r * 3 + t] * Wj[t * 6 + cA];
-          T[r] = sum;
-        }
-        double sum = 0;
-        for (int t = 0; t < 3; t++) sum += Wi[t * 6 + rA] * T[t];
-        acc[loc * 36 + e0] += sum;
-      }
-      if (e1 < 36) {
-        double T[3];
-        for (int r = 0; r < 3; r++) {
-          double sum = 0;
-          for (int t = 0; t < 3; t++) sum += kv[r * 3 + t] * Wj[t * 6 + cB];
-          T[r] = sum;
-        }
-        double sum = 0;
-        for (int t = 0; t < 3; t++) sum += Wi[t * 6 + rB] * T[t];
-        acc[loc * 36 + e1] += sum;
-      }
-      __syncwarp();
-    }
-  }
-  __syncwarp();
-  for (int e = lane; e < nJ * 36; e += 32) out[(size_t)r0 * 36 + e] = acc[e];
-}
-
-// galerkinProduct between shell levels (6x6 weights), warp per coarse row
-__global__ void k_galerkin_shell(int nnc, const int* __restrict__ chPtr, const int* __restrict__ chIdx, const int* __restrict__ chW,
-                                 const int* __restrict__ fRowPtr, const int* __restrict__ fCol, const double* __restrict__ fVal,
-                                 const int* __restrict__ prolPtr, const int* __restrict__ prolIdx, const double* __restrict__ W,
-                                 const int* __restrict__ rowPtr, const int* __restrict__ col, int maxRow, double* __restrict__ out) {
-  extern __shared__ double sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int I = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (I >= nnc) return;
-  double* acc = sm + (size_t)warp * maxRow * 36;
-  const int r0 = rowPtr[I], nJ = rowPtr[I + 1] - r0;
-  for (int e = lane; e < nJ * 36; e += 32) acc[e] = 0;
-  __syncwarp();
-  const int e0 = lane, e1 = lane + 32;
-  const int rA = e0 / 6, cA = e0 % 6, rB = e1 / 6, cB = e1 % 6;
-  for (int q = chPtr[I]; q < chPtr[I + 1]; q++) {
-    const int f = chIdx[q];
-    const double* Wi = W + 36 * (size_t)chW[q];
-    for (int k = fRowPtr[f]; k < fRowPtr[f + 1]; k++) {
-      const int g = fCol[k];
-      const double* Kv = fVal + 36 * (size_t)k;
-      for (int p = prolPtr[g]; p < prolPtr[g + 1]; p++) {
-        const int loc = find_col(col + r0, nJ, prolIdx[p]);
-        if (loc < 0) continue;
-        const double* Wj = W + 36 * (size_t)p;
-        {
-          double T[6];
-          for (int r = 0; r < 6; r++) {
-            double sum = 0;
-            for (int t = 0; t < 6; t++) sum += Kv[r * 6 + t] * Wj[t * 6 + cA];
-            T[r] = sum;
-          }
-          double sum = 0;
-          for (int t = 0; t < 6; t++) sum += Wi[t * 6 + rA] * T[t];
-          acc[loc * 36 + e0] += sum;
-        }
-        if (e1 < 36) {
-          double T[6];
-          for (int r = 0; r < 6; r++) {
-            double sum = 0;
-            for (int t = 0; t < 6; t++) sum += Kv[r * 6 + t] * Wj[t * 6 + cB];
-            T[r] = sum;
-          }
-          double sum = 0;
-          for (int t = 0; t < 6; t++) sum += Wi[t * 6 + rB] * T[t];
-          acc[loc * 36 + e1] += sum;
-        }
-        __syncwarp();
-      }
-    }
-  }
-  __syncwarp();
-  for (int e = lane; e < nJ * 36; e += 32) out[(size_t)r0 * 36 + e] = acc[e];
-}
 
 // factorShellColumns (10-solver.js:474-494) with cholDense (rel 1e-12), warp per column
 __global__ void k_factor_shell(int ncol, const int* __restrict__ colStart, const int* __restrict__ rowPtr, const int* __restrict__ col,
@@ -615,81 +493,6 @@ __global__ void k_factor_shell(int ncol, const int* __restrict__ colStart, const
   if (lane == 0 && fixes) atomicAdd(jitterCount, fixes);
 }
 
-// factorCoarsest (10-solver.js:562-600): banded Cholesky in one block
-__global__ void k_factor_coarsest(int nnb, const int* __restrict__ rowPtr, const int* __restrict__ col, const double* __restrict__ val,
-                                  int n, int bw, double* __restrict__ A, int* __restrict__ jitterCount) {
-  const int w = bw + 1;
-  __shared__ double s_inv;
-  __shared__ double s_red[1024];
-  for (size_t e = threadIdx.x; e < (size_t)n * w; e += blockDim.x) A[e] = 0;
-  __syncthreads();
-  for (int i = 0; i < nnb; i++)
-    for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
-      const int j = col[k];
-      if (j > i) continue;
-      for (int e = threadIdx.x; e < 36; e += blockDim.x) {
-        const int p = e / 6, q = e % 6;
-        const int r = 6 * i + p, cc = 6 * j + q;
-        if (cc <= r) A[(size_t)r * w + (cc - r + bw)] = val[36 * (size_t)k + e];
-      }
-    }
-  __syncthreads();
-  double dm = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dm = fmax(dm, fabs(A[(size_t)i * w + bw]));
-  s_red[threadIdx.x] = dm;
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st) s_red[threadIdx.x] = fmax(s_red[threadIdx.x], s_red[threadIdx.x + st]);
-    __syncthreads();
-  }
-  const double dmax = s_red[0];
-  const double jitter = 1e-12 * (dmax != 0 ? dmax : 1);
-  int fixes = 0;
-  for (int j = 0; j < n; j++) {
-    const int k0 = max(0, j - bw);
-    if (threadIdx.x == 0) {
-      double d = A[(size_t)j * w + bw];
-      for (int k = k0; k < j; k++) { const double l = A[(size_t)j * w + (k - j + bw)]; d -= l * l; }
-      if (!(d > jitter)) { d = fmax(fabs(d), jitter); fixes++; }
-      const double ljj = sqrt(d);
-      A[(size_t)j * w + bw] = ljj;
-      s_inv = 1 / ljj;
-    }
-    __syncthreads();
-    const double inv = s_inv;
-    const int iend = min(n, j + bw + 1);
-    for (int i = j + 1 + threadIdx.x; i < iend; i += blockDim.x) {
-      double sum = A[(size_t)i * w + (j - i + bw)];
-      const int kk0 = max(k0, i - bw);
-      for (int k = kk0; k < j; k++) sum -= A[(size_t)i * w + (k - i + bw)] * A[(size_t)j * w + (k - j + bw)];
-      A[(size_t)i * w + (j - i + bw)] = sum * inv;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0 && fixes) atomicAdd(jitterCount, fixes);
-}
-
-// explicit inverse of the coarsest operator from its banded factor (solveCoarsest on unit vectors)
-__global__ void k_coarsest_inverse(int n, int bw, const double* __restrict__ A, double* __restrict__ inv) {
-  const int cidx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cidx >= n) return;
-  const int w = bw + 1;
-  // forward: L y = e_c  (y_i = 0 for i < c)
-  for (int i = 0; i < n; i++) inv[(size_t)i * n + cidx] = 0;
-  for (int i = cidx; i < n; i++) {
-    double sum = i == cidx ? 1.0 : 0.0;
-    const int k0 = max(cidx, i - bw);
-    for (int k = k0; k < i; k++) sum -= A[(size_t)i * w + (k - i + bw)] * inv[(size_t)k * n + cidx];
-    inv[(size_t)i * n + cidx] = sum / A[(size_t)i * w + bw];
-  }
-  for (int i = n - 1; i >= 0; i--) {
-    double sum = inv[(size_t)i * n + cidx];
-    const int kend = min(n, i + bw + 1);
-    for (int k = i + 1; k < kend; k++) sum -= A[(size_t)k * w + (i - k + bw)] * inv[(size_t)k * n + cidx];
-    inv[(size_t)i * n + cidx] = sum / A[(size_t)i * w + bw];
-  }
-}
-
 // explicit inverse of every shell column block from its Cholesky factor (warp per column, lanes over
 // unit vectors); the smoother then applies A_cc^-1 as a dense product instead of two serial
 // triangular solves (cholSolveDenseOff, 10-solver.js:497-509, computes the same A_cc^-1 r).
@@ -715,194 +518,6 @@ __global__ void k_shell_inverse(int ncol, const int* __restrict__ colStart, cons
       for (int k = i + 1; k < m; k++) s -= L[k * m + i] * Xe[k];
       Xe[i] = s / L[i * m + i];
     }
-  }
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// banded Cholesky of the coarsest operator (factorCoarsest, 10-solver.js:562-600) in one block:
-// for each pivot, warp 0 reduces the pivot row and the 32 warps share the rows below it, each
-// row's dot product split over the lanes
-__global__ void k_factor_coarsest_par(int nnb, const int* __restrict__ rowPtr, const int* __restrict__ col, const double* __restrict__ val,
-                                      int n, int bw, double* __restrict__ A, int* __restrict__ jitterCount) {
-  const int w = bw + 1;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  __shared__ double s_inv;
-  __shared__ double s_red[32];
-  for (size_t e = threadIdx.x; e < (size_t)n * w; e += blockDim.x) A[e] = 0;
-  __syncthreads();
-  for (int i = 0; i < nnb; i++)
-    for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
-      const int j = col[k];
-      if (j > i) continue;
-      for (int e = threadIdx.x; e < 36; e += blockDim.x) {
-        const int p = e / 6, q = e % 6;
-        const int r = 6 * i + p, cc = 6 * j + q;
-        if (cc <= r) A[(size_t)r * w + (cc - r + bw)] = val[36 * (size_t)k + e];
-      }
-    }
-  __syncthreads();
-  double dm = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dm = fmax(dm, fabs(A[(size_t)i * w + bw]));
-  for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
-  if (lane == 0) s_red[warp] = dm;
-  __syncthreads();
-  double dmax = 0;
-  for (int q = 0; q < nw; q++) dmax = fmax(dmax, s_red[q]);
-  const double jitter = 1e-12 * (dmax != 0 ? dmax : 1);
-  int fixes = 0;
-  for (int j = 0; j < n; j++) {
-    const int k0 = max(0, j - bw);
-    if (warp == 0) {
-      double ss = 0;
-      for (int k = k0 + lane; k < j; k += 32) { const double l = A[(size_t)j * w + (k - j + bw)]; ss += l * l; }
-      ss = warp_sum(ss);
-      if (lane == 0) {
-        double d = A[(size_t)j * w + bw] - ss;
-        if (!(d > jitter)) { d = fmax(fabs(d), jitter); fixes++; }
-        const double ljj = sqrt(d);
-        A[(size_t)j * w + bw] = ljj;
-        s_inv = 1 / ljj;
-      }
-    }
-    __syncthreads();
-    const double inv = s_inv;
-    const int iend = min(n, j + bw + 1);
-    for (int i = j + 1 + warp; i < iend; i += nw) {
-      const int kk0 = max(k0, i - bw);
-      double ss = 0;
-      for (int k = kk0 + lane; k < j; k += 32) ss += A[(size_t)i * w + (k - i + bw)] * A[(size_t)j * w + (k - j + bw)];
-      ss = warp_sum(ss);
-      if (lane == 0) A[(size_t)i * w + (j - i + bw)] = (A[(size_t)i * w + (j - i + bw)] - ss) * inv;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0 && fixes) atomicAdd(jitterCount, fixes);
-}
-
-// blocked right-looking form of the same banded Cholesky: per block of NB pivots, the diagonal
-// block is factored in shared memory by one warp, the panel below it (the rows the band reaches)
-// is solved against it with one thread per row, and the trailing band window is updated with one
-// warp per row; the jitter rule of cholDense is applied to every pivot.
-constexpr int CB_NB = 32, CB_LD = 33;
-__global__ void __launch_bounds__(1024) k_factor_coarsest_blk(int nnb, const int* __restrict__ rowPtr, const int* __restrict__ col,
-                                                              const double* __restrict__ val, int n, int bw, double* __restrict__ A,
-                                                              int* __restrict__ jitterCount) {
-  extern __shared__ double smb[];
-  double* Ds = smb;                  // CB_NB x CB_LD diagonal block
-  double* P = smb + CB_NB * CB_LD;   // bw x CB_LD panel rows
-  __shared__ double s_red[32];
-  __shared__ int s_fix;
-  const int w = bw + 1, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nthr = blockDim.x, nw = nthr >> 5;
-  for (size_t e = tid; e < (size_t)n * w; e += nthr) A[e] = 0;
-  __syncthreads();
-  for (int i = 0; i < nnb; i++)
-    for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
-      const int j = col[k];
-      if (j > i) continue;
-      for (int e = tid; e < 36; e += nthr) {
-        const int p = e / 6, q = e % 6;
-        const int r = 6 * i + p, cc = 6 * j + q;
-        if (cc <= r) A[(size_t)r * w + (cc - r + bw)] = val[36 * (size_t)k + e];
-      }
-    }
-  __syncthreads();
-  double dm = 0;
-  for (int i = tid; i < n; i += nthr) dm = fmax(dm, fabs(A[(size_t)i * w + bw]));
-  for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
-  if (lane == 0) s_red[warp] = dm;
-  if (tid == 0) s_fix = 0;
-  __syncthreads();
-  double dmax = 0;
-  for (int q = 0; q < nw; q++) dmax = fmax(dmax, s_red[q]);
-  const double jitter = 1e-12 * (dmax != 0 ? dmax : 1);
-  for (int jb = 0; jb < n; jb += CB_NB) {
-    const int nbk = min(CB_NB, n - jb);
-    for (int e = tid; e < CB_NB * CB_NB; e += nthr) {
-      const int r = e / CB_NB, cc = e % CB_NB;
-      Ds[r * CB_LD + cc] = (r < nbk && cc <= r && r - cc <= bw) ? A[(size_t)(jb + r) * w + (cc - r + bw)] : 0.0;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      for (int j = 0; j < nbk; j++) {
-        double ss = 0;
-        for (int t = lane; t < j; t += 32) ss += Ds[j * CB_LD + t] * Ds[j * CB_LD + t];
-        ss = warp_sum(ss);
-        double d = Ds[j * CB_LD + j] - ss;
-        if (!(d > jitter)) { d = fmax(fabs(d), jitter); if (lane == 0) s_fix++; }
-        const double ljj = sqrt(d), inv = 1 / ljj;
-        __syncwarp();
-        if (lane == 0) Ds[j * CB_LD + j] = ljj;
-        if (lane > j && lane < nbk) {
-          double s2 = Ds[lane * CB_LD + j];
-          for (int t = 0; t < j; t++) s2 -= Ds[lane * CB_LD + t] * Ds[j * CB_LD + t];
-          Ds[lane * CB_LD + j] = s2 * inv;
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    for (int e = tid; e < CB_NB * CB_NB; e += nthr) {
-      const int r = e / CB_NB, cc = e % CB_NB;
-      if (r < nbk && cc <= r && r - cc <= bw) A[(size_t)(jb + r) * w + (cc - r + bw)] = Ds[r * CB_LD + cc];
-    }
-    const int i0 = jb + nbk, i1 = min(n, jb + nbk + bw), R = i1 - i0;
-    for (int ri = tid; ri < R; ri += nthr) {
-      const int i = i0 + ri;
-      double* Pr = P + (size_t)ri * CB_LD;
-      for (int k = 0; k < nbk; k++) {
-        const int kk = jb + k;
-        double a = (i - kk <= bw) ? A[(size_t)i * w + (kk - i + bw)] : 0.0;
-        for (int t = 0; t < k; t++) a -= Pr[t] * Ds[k * CB_LD + t];
-        Pr[k] = a / Ds[k * CB_LD + k];
-      }
-      for (int k = 0; k < nbk; k++)
-        if (i - (jb + k) <= bw) A[(size_t)i * w + (jb + k - i + bw)] = Pr[k];
-    }
-    __syncthreads();
-    for (int ri = warp; ri < R; ri += nw) {
-      const int gi = i0 + ri;
-      const double* Pi = P + (size_t)ri * CB_LD;
-      for (int rk = max(0, ri - bw) + lane; rk <= ri; rk += 32) {
-        const double* Pk = P + (size_t)rk * CB_LD;
-        double s2 = 0;
-        for (int t = 0; t < nbk; t++) s2 += Pi[t] * Pk[t];
-        const int gk = i0 + rk;
-        A[(size_t)gi * w + (gk - gi + bw)] -= s2;
-      }
-    }
-    __syncthreads();
-  }
-  if (tid == 0 && s_fix) atomicAdd(jitterCount, s_fix);
-}
-
-// explicit inverse of the coarsest operator from its banded factor: warp per unit vector e_c, the
-// result row c (the inverse is symmetric) doubling as the work vector of the two substitutions
-__global__ void k_coarsest_inverse_par(int n, int bw, const double* __restrict__ A, double* __restrict__ inv) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (c >= n) return;
-  const int w = bw + 1;
-  double* y = inv + (size_t)c * n;
-  for (int i = lane; i < c; i += 32) y[i] = 0;
-  __syncwarp();
-  for (int i = c; i < n; i++) {
-    double ss = 0;
-    for (int k = max(c, i - bw) + lane; k < i; k += 32) ss += A[(size_t)i * w + (k - i + bw)] * y[k];
-    ss = warp_sum(ss);
-    if (lane == 0) y[i] = ((i == c ? 1.0 : 0.0) - ss) / A[(size_t)i * w + bw];
-    __syncwarp();
-  }
-  for (int i = n - 1; i >= 0; i--) {
-    double ss = 0;
-    const int kend = min(n, i + bw + 1);
-    for (int k = i + 1 + lane; k < kend; k += 32) ss += A[(size_t)k * w + (i - k + bw)] * y[k];
-    ss = warp_sum(ss);
-    if (lane == 0) y[i] = (y[i] - ss) / A[(size_t)i * w + bw];
-    __syncwarp();
   }
 }
 
@@ -1010,32 +625,6 @@ void launch_w01(Context& c) {
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
-void launch_galerkin01(Context& c) {
-  ShellLevel& L1 = *c.shells[0];
-  const int warps = 4;
-  const size_t smem = (size_t)warps * L1.maxRowBlocks * 36 * sizeof(double);
-  TM_CUDA_CHECK(cudaFuncSetAttribute(k_galerkin01, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  note_launch();
-  TimedLaunch tl(c, K_GALERKIN01);
-  k_galerkin01<<<grid_for(L1.nn, warps), 32 * warps, smem, c.stream>>>(L1.nn, c.nn, c.d_aggStart.p, c.d_nodeAgg.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p,
-                                                                      c.d_val.p, c.d_W01.p, L1.d_rowPtr.p, L1.d_col.p, L1.maxRowBlocks,
-                                                                      L1.d_val.p);
-  TM_CUDA_CHECK(cudaGetLastError());
-}
-
-void launch_galerkin_shell(Context& c, int l) {
-  ShellLevel& F = *c.shells[l];
-  ShellLevel& C = *c.shells[l + 1];
-  const int warps = 4;
-  const size_t smem = (size_t)warps * C.maxRowBlocks * 36 * sizeof(double);
-  TM_CUDA_CHECK(cudaFuncSetAttribute(k_galerkin_shell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  note_launch();
-  k_galerkin_shell<<<grid_for(C.nn, warps), 32 * warps, smem, c.stream>>>(C.nn, F.d_chPtr.p, F.d_chIdx.p, F.d_chW.p, F.d_rowPtr.p, F.d_col.p,
-                                                                         F.d_val.p, F.d_prolPtr.p, F.d_prolIdx.p, F.d_prolW.p, C.d_rowPtr.p,
-                                                                         C.d_col.p, C.maxRowBlocks, C.d_val.p);
-  TM_CUDA_CHECK(cudaGetLastError());
-}
-
 void launch_factor_shell(Context& c, ShellLevel& L) {
   const int ncol = L.nx * L.ny;
   const int warps = 4;
@@ -1044,20 +633,6 @@ void launch_factor_shell(Context& c, ShellLevel& L) {
                                                                     L.d_cf.p, c.d_jitter.p);
   note_launch();
   k_shell_inverse<<<grid_for(ncol, warps), 32 * warps, 0, c.stream>>>(ncol, L.d_colStart.p, L.d_cfPtr.p, L.d_cf.p, L.d_cfInv.p);
-  TM_CUDA_CHECK(cudaGetLastError());
-}
-
-void launch_factor_coarsest(Context& c, ShellLevel& L) {
-  note_launch(2);
-  const size_t smem = (size_t)(CB_NB + L.bandBw) * CB_LD * sizeof(double);
-  if (smem <= 200 * 1024) {
-    TM_CUDA_CHECK(cudaFuncSetAttribute(k_factor_coarsest_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_factor_coarsest_blk<<<1, 1024, smem, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
-  } else {
-    k_factor_coarsest_par<<<1, 1024, 0, c.stream>>>(L.nn, L.d_rowPtr.p, L.d_col.p, L.d_val.p, L.denseN, L.bandBw, L.d_band.p, c.d_jitter.p);
-  }
-  TM_CUDA_CHECK(cudaGetLastError());
-  k_coarsest_inverse_par<<<grid_for(L.denseN, 4), 128, 0, c.stream>>>(L.denseN, L.bandBw, L.d_band.p, L.d_inv.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
