@@ -437,9 +437,10 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
 void upload_mesh(Context& c) {
   cudaStream_t s = c.stream;
   {
-    std::vector<int> pn((size_t)NSLOT * c.nn);
+    c.nnp = (c.nn + 3) / 4 * 4;
+    std::vector<int> pn((size_t)NSLOT * c.nnp, -1);
     for (int sl = 0; sl < NSLOT; sl++)
-      for (int n = 0; n < c.nn; n++) pn[(size_t)sl * c.nn + c.pos[n]] = c.nbr[(size_t)sl * c.nn + n];
+      for (int n = 0; n < c.nn; n++) pn[(size_t)sl * c.nnp + c.pos[n]] = c.nbr[(size_t)sl * c.nn + n];
     c.d_nbr.upload(pn, s);
   }
   c.d_pos.upload(c.pos, s);
@@ -575,8 +576,8 @@ tm_status tm_assemble_step_device(tm_ctx* ctx, const tm_step* st, double* rhs_de
 tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, const double* val, const uint8_t* isConstrained) {
   return guarded([&] {
     Context& c = *reinterpret_cast<Context*>(ctx);
-    const int nn = c.nn;
-    std::vector<double> sv((size_t)NSLOT * 9 * nn, 0.0);
+    const int nn = c.nn, S = c.nnp;
+    std::vector<double> sv((size_t)NSLOT * 9 * S, 0.0);
     for (int i = 0; i < nn; i++) {
       const int ii = c.nodeIJK[3 * (size_t)i], ij = c.nodeIJK[3 * (size_t)i + 1], ik = c.nodeIJK[3 * (size_t)i + 2];
       for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
@@ -585,7 +586,7 @@ tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, co
         const int di = c.nodeIJK[3 * (size_t)j] - ii, dj = c.nodeIJK[3 * (size_t)j + 1] - ij, dk = c.nodeIJK[3 * (size_t)j + 2] - ik;
         if (std::abs(di) > 1 || std::abs(dj) > 1 || std::abs(dk) > 1) fail(TM_BAD_INPUT, "block outside the 27-point stencil of the mesh");
         const int s = (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
-        for (int v = 0; v < 9; v++) sv[((size_t)s * 9 + v) * nn + c.pos[i]] = val[9 * (size_t)k + v];
+        for (int v = 0; v < 9; v++) sv[((size_t)s * 9 + v) * S + c.pos[i]] = val[9 * (size_t)k + v];
       }
     }
     c.d_val.upload(sv, c.stream);
@@ -601,8 +602,8 @@ tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, co
 tm_status tm_get_bcsr(tm_ctx* ctx, int32_t* rowPtr, int32_t* col, double* val) {
   return guarded([&] {
     Context& c = *reinterpret_cast<Context*>(ctx);
-    const int nn = c.nn;
-    std::vector<double> sv((size_t)NSLOT * 9 * nn);
+    const int nn = c.nn, S = c.nnp;
+    std::vector<double> sv((size_t)NSLOT * 9 * S);
     c.d_val.download(sv.data(), sv.size(), c.stream);
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
     int k = 0;
@@ -611,7 +612,7 @@ tm_status tm_get_bcsr(tm_ctx* ctx, int32_t* rowPtr, int32_t* col, double* val) {
       for (int s = 0; s < NSLOT; s++) {
         if (!(c.slotMask[i] >> s & 1)) continue;
         if (col) col[k] = c.nbr[(size_t)s * nn + i];
-        if (val) for (int v = 0; v < 9; v++) val[9 * (size_t)k + v] = sv[((size_t)s * 9 + v) * nn + c.pos[i]];
+        if (val) for (int v = 0; v < 9; v++) val[9 * (size_t)k + v] = sv[((size_t)s * 9 + v) * S + c.pos[i]];
         k++;
       }
       if (rowPtr) rowPtr[i + 1] = k;

@@ -50,7 +50,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 // ---- Galerkin products ---------------------------------------------------------------------
 
 // galerkinProduct 0 -> 1: summands W_i^T K_ij W_j with 3x3 K_ij (slot s of position ps) and the
-// 3x6 weights of the nodes i and j (shellWeights, 10-solver.js:337-353)
+// 3x6 weights of the nodes i and j (shellWeights, 10-solver.js:337-353); nn is the row stride of
+// the slot-major arrays
 __global__ void __launch_bounds__(128) k_galerkin01(int nblk, int nn, const int* __restrict__ start, const int* __restrict__ list,
                                                     const int* __restrict__ posNode, const int* __restrict__ nbr,
                                                     const double* __restrict__ val, const double* __restrict__ W,
@@ -382,7 +383,7 @@ void launch_galerkin01(Context& c) {
   ShellLevel& L1 = *c.shells[0];
   note_launch();
   TimedLaunch tl(c, K_GALERKIN01);
-  k_galerkin01<<<grid_for(L1.nb, 4), 128, 0, c.stream>>>(L1.nb, c.nn, c.d_g01Start.p, c.d_g01List.p, c.d_posNode.p, c.d_nbr.p, c.d_val.p,
+  k_galerkin01<<<grid_for(L1.nb, 4), 128, 0, c.stream>>>(L1.nb, c.nnp, c.d_g01Start.p, c.d_g01List.p, c.d_posNode.p, c.d_nbr.p, c.d_val.p,
                                                         c.d_W01.p, L1.d_val.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }

@@ -292,6 +292,28 @@ void galerkin_lists_shell(const ShellLevel& F, ShellLevel& C, cudaStream_t st) {
   C.d_galList.upload(list, st);
 }
 
+// column metadata of a shell level: aggregate and block ranges of every column, and per colour
+// list entry the same plus the offset of the column's inverse (lists in color_lists order)
+void shell_column_meta(ShellLevel& L, cudaStream_t st) {
+  const int ncol = L.nx * L.ny;
+  std::vector<int4> all(ncol);
+  std::vector<int4> lists[4];
+  std::vector<long long> cfs[4];
+  for (int c = 0; c < ncol; c++) {
+    const int n0 = L.colStart[c], n1 = L.colStart[c + 1];
+    all[c] = make_int4(n0, n1, L.rowPtr[n0], L.rowPtr[n1]);
+    if (n1 == n0) continue;
+    const int k = ((c / L.ny) & 1) * 2 + ((c % L.ny) & 1);
+    lists[k].push_back(all[c]);
+    cfs[k].push_back(L.cfPtr.empty() ? 0 : L.cfPtr[c]);
+  }
+  L.d_colMeta.upload(all, st);
+  for (int k = 0; k < 4; k++) {
+    L.d_colorMeta[k].upload(lists[k], st);
+    L.d_colorCf[k].upload(cfs[k], st);
+  }
+}
+
 void column_factor_sizes(ShellLevel& L) {
   const int ncol = L.nx * L.ny;
   L.cfPtr.assign(ncol + 1, 0);
@@ -559,6 +581,7 @@ void build_hierarchy(Context& c) {
       L.d_cfInv.alloc((size_t)L.cfPtr.back());
     }
     color_lists(L.nx, L.ny, L.colStart, L.d_colorCols, L.colorCount, st);
+    shell_column_meta(L, st);
     if (l + 1 < c.shells.size()) {
       L.d_prolPtr.upload(L.prolPtr, st);
       L.d_prolIdx.upload(L.prolIdx, st);

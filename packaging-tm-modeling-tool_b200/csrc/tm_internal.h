@@ -69,6 +69,17 @@ struct DBuf {
 #ifndef TM_PANEL_UNROLL
 #define TM_PANEL_UNROLL 3
 #endif
+// FP32 level-0 apply: positions per thread (1, 2 or 4; the operator rows are padded to a
+// multiple of 4), unroll depth of its slot loop and the resident CTAs its registers are sized for
+#ifndef TM_APPLY32_NPT
+#define TM_APPLY32_NPT 2
+#endif
+#ifndef TM_APPLY32_UNROLL
+#define TM_APPLY32_UNROLL 3
+#endif
+#ifndef TM_APPLY32_MINB
+#define TM_APPLY32_MINB 10
+#endif
 #define TM_STR_(x) #x
 #define TM_UNROLL(n) _Pragma(TM_STR_(unroll n))
 
@@ -103,6 +114,10 @@ struct ShellLevel {
   // colours: columns with (i%2, j%2) = colour, as lists
   DBuf<int> d_colorCols[4];
   int colorCount[4] = {0, 0, 0, 0};
+  // per column (all columns, and per colour list entry): first and one-past-last aggregate and
+  // block, and the offset of the column's inverse block
+  DBuf<int4> d_colMeta, d_colorMeta[4];
+  DBuf<long long> d_colorCf[4];
   // prolongation from the next (coarser) level to this one: per aggregate f of this level
   // parents idx with 6x6 weights (buildCoarseShellLevel, 10-solver.js:396-471)
   std::vector<int> prolPtr, prolIdx;
@@ -133,6 +148,7 @@ struct ShellLevel {
 
 struct Context {
   int dev = 0;
+  int nnp = 0;                         // row stride of the slot-major level-0 arrays
   cudaStream_t stream = nullptr;
   // mesh (host copies of what the structure builders need)
   int nx = 0, ny = 0, nz = 0, nn = 0, ne = 0, npset = 0, ngroups = 0;
@@ -161,7 +177,10 @@ struct Context {
   DBuf<double> d_psetM;                // 6*1089 per property set
   DBuf<double> d_clsF33;               // 33 per class: uncondensed element thermal load (elementFth)
   DBuf<int> d_psetLayered, d_psetBorn;
-  // operator (level 0): 243 values per node, slot-major ((s*9 + v)*nn + n)
+  // operator (level 0): 243 values per position, slot-major ((s*9 + v)*nnp + p), and its FP32
+  // copy; the slot-major device arrays (operator, neighbour ids) use the row stride nnp (nn
+  // rounded up to a multiple of 4; zero values and id -1 in the padding), so that adjacent
+  // positions of the FP32 operator load as one 8- or 16-byte vector
   DBuf<double> d_val;
   DBuf<float> d_val32;
   DBuf<double> d_rhs;

@@ -246,13 +246,18 @@ __device__ __forceinline__ int loc_index(int a, int b, int c) {
 }
 
 // ---- stencil assembly: thread per (slot, node), contributions in element order -----------------
-__global__ void k_assemble(int nn, int nx, int ny, int nz, const int* __restrict__ posNode, const int* __restrict__ nodeIJK, const int* __restrict__ nbr,
-                           const int* __restrict__ cellElems, const int* __restrict__ eClass, const double* __restrict__ eScale,
-                           const int* __restrict__ eGroup, const int* __restrict__ groupStage, int stage,
+__global__ void k_assemble(int nn, int S, int nx, int ny, int nz, const int* __restrict__ posNode, const int* __restrict__ nodeIJK,
+                           const int* __restrict__ nbr, const int* __restrict__ cellElems, const int* __restrict__ eClass,
+                           const double* __restrict__ eScale, const int* __restrict__ eGroup, const int* __restrict__ groupStage, int stage,
                            const double* __restrict__ clsKc, double* __restrict__ val) {
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (t >= (size_t)NSLOT * nn) return;
-  const int s = (int)(t / nn), ps = (int)(t % nn), n = posNode[ps];
+  if (t >= (size_t)NSLOT * S) return;
+  const int s = (int)(t / S), ps = (int)(t % S);
+  if (ps >= nn) {   // padding of the rows: zeros
+    for (int v = 0; v < 9; v++) val[((size_t)s * 9 + v) * S + ps] = 0;
+    return;
+  }
+  const int n = posNode[ps];
   double acc[9];
   for (int v = 0; v < 9; v++) acc[v] = 0;
   const int m = nbr[t];
@@ -283,7 +288,7 @@ __global__ void k_assemble(int nn, int nx, int ny, int nz, const int* __restrict
           }
         }
   }
-  for (int v = 0; v < 9; v++) val[((size_t)s * 9 + v) * nn + ps] = acc[v];
+  for (int v = 0; v < 9; v++) val[((size_t)s * 9 + v) * S + ps] = acc[v];
 }
 
 // thermal load, thread per node (assembleStep's rhs, 09-assembly.js:417-420)
@@ -317,7 +322,8 @@ __global__ void k_assemble_rhs(int nn, int nx, int ny, int nz, const int* __rest
   rhs[3 * n] = acc0; rhs[3 * n + 1] = acc1; rhs[3 * n + 2] = acc2;
 }
 
-// applyConstraints (09-assembly.js:445-464), one thread walking the DOFs in order
+// applyConstraints (09-assembly.js:445-464), one thread walking the DOFs in order (nn: the
+// row stride of the slot-major arrays)
 __global__ void k_constraints(int nn, int ncon, const int* __restrict__ dofs, const int* __restrict__ pos, const int* __restrict__ nbr,
                               const int* __restrict__ slotMask, double* __restrict__ val, double* __restrict__ rhs,
                               uint8_t* __restrict__ isC) {
@@ -343,23 +349,23 @@ __global__ void k_constraints(int nn, int ncon, const int* __restrict__ dofs, co
 }
 
 // _scale (10-solver.js:852-866)
-__global__ void k_scale_diag(int nn, const int* __restrict__ posNode, const double* __restrict__ val, double* __restrict__ s) {
+__global__ void k_scale_diag(int nn, int S, const int* __restrict__ posNode, const double* __restrict__ val, double* __restrict__ s) {
   const int ps = blockIdx.x * blockDim.x + threadIdx.x;
   if (ps >= nn) return;
   const int n = posNode[ps];
-  for (int p = 0; p < 3; p++) s[3 * n + p] = 1 / sqrt(fmax(val[((size_t)SLOT_SELF * 9 + 4 * p) * nn + ps], 1e-300));
+  for (int p = 0; p < 3; p++) s[3 * n + p] = 1 / sqrt(fmax(val[((size_t)SLOT_SELF * 9 + 4 * p) * S + ps], 1e-300));
 }
 
-__global__ void k_scale_val(int nn, const int* __restrict__ posNode, const int* __restrict__ nbr, const double* __restrict__ s,
+__global__ void k_scale_val(int nn, int S, const int* __restrict__ posNode, const int* __restrict__ nbr, const double* __restrict__ s,
                             double* __restrict__ val) {
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= (size_t)NSLOT * nn) return;
   const int sl = (int)(t / nn), ps = (int)(t % nn), n = posNode[ps];
-  const int j = nbr[t];
+  const int j = nbr[(size_t)sl * S + ps];
   if (j < 0) return;
   for (int p = 0; p < 3; p++)
     for (int q = 0; q < 3; q++) {
-      double* v = val + ((size_t)sl * 9 + 3 * p + q) * nn + ps;
+      double* v = val + ((size_t)sl * 9 + 3 * p + q) * S + ps;
       *v *= s[3 * n + p] * s[3 * j + q];
     }
 }
@@ -385,7 +391,8 @@ __device__ bool chol3(const double* A, double* L, double jit) {
   return true;
 }
 
-// factorColumns (10-solver.js:31-68), thread per column
+// factorColumns (10-solver.js:31-68), thread per column (nn: the row stride of the slot-major
+// arrays)
 __global__ void k_factor_columns(int ncol, int nn, const int* __restrict__ colStart, const int* __restrict__ pos, const int* __restrict__ nbr,
                                  const int* __restrict__ slotMask, const double* __restrict__ val, double* __restrict__ F,
                                  int* __restrict__ jitterCount) {
@@ -565,14 +572,15 @@ void launch_class_condense(Context& c) {
 }
 
 void launch_assemble(Context& c) {
-  const size_t tot = (size_t)NSLOT * c.nn;
+  const size_t tot = (size_t)NSLOT * c.nnp;
   c.d_val.alloc(tot * 9);
   c.d_rhs.alloc(3 * (size_t)c.nn);
   note_launch(2);
   {
   TimedLaunch tl(c, K_ASSEMBLE);
-  k_assemble<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_posNode.p, c.d_nodeIJK.p, c.d_nbr.p, c.d_cellElems.p, c.d_eClass.p,
-                                                      c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsKc.p, c.d_val.p);
+  k_assemble<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nnp, c.nx, c.ny, c.nz, c.d_posNode.p, c.d_nodeIJK.p, c.d_nbr.p, c.d_cellElems.p,
+                                                      c.d_eClass.p, c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsKc.p,
+                                                      c.d_val.p);
   }
   TM_CUDA_CHECK(cudaGetLastError());
   k_assemble_rhs<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_nodeIJK.p, c.d_cellElems.p, c.d_eClass.p,
@@ -587,7 +595,7 @@ void launch_constraints(Context& c) {
   DBuf<int> d;
   d.upload(c.constr, c.stream);
   note_launch();
-  k_constraints<<<1, 1, 0, c.stream>>>(c.nn, (int)c.constr.size(), d.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
+  k_constraints<<<1, 1, 0, c.stream>>>(c.nnp, (int)c.constr.size(), d.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
   TM_CUDA_CHECK(cudaGetLastError());
   TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   c.isC.assign(3 * (size_t)c.nn, 0);
@@ -597,9 +605,9 @@ void launch_constraints(Context& c) {
 void launch_scale(Context& c) {
   c.d_s.alloc(3 * (size_t)c.nn);
   note_launch(2);
-  k_scale_diag<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_val.p, c.d_s.p);
+  k_scale_diag<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.nnp, c.d_posNode.p, c.d_val.p, c.d_s.p);
   const size_t tot = (size_t)NSLOT * c.nn;
-  k_scale_val<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_s.p, c.d_val.p);
+  k_scale_val<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nnp, c.d_posNode.p, c.d_nbr.p, c.d_s.p, c.d_val.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -614,7 +622,7 @@ void launch_factor_columns(Context& c) {
   const int ncol = c.nx * c.ny;
   c.d_F.zero(c.stream);
   note_launch();
-  k_factor_columns<<<grid_for(ncol, 128), 128, 0, c.stream>>>(ncol, c.nn, c.d_colStart.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p,
+  k_factor_columns<<<grid_for(ncol, 128), 128, 0, c.stream>>>(ncol, c.nnp, c.d_colStart.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p,
                                                              c.d_F.p, c.d_jitter.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }

@@ -21,35 +21,104 @@ constexpr int RED_THREADS = 256;
 
 inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
 
-// ---- level-0 stencil apply: y = K x or y = b - K x, thread per node --------------------------
-template <class T, class V>
-__global__ void k_apply0(int nn, const int* __restrict__ posNode, const int* __restrict__ nbr, const T* __restrict__ val,
-                         const V* __restrict__ x, V* __restrict__ y, const V* __restrict__ b) {
-  const int ps = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ps >= nn) return;
-  const int n = posNode[ps];
-  T y0 = 0, y1 = 0, y2 = 0;
-  // absent slots hold exact zeros: they read the node's own x, branch-free, ids fetched first
-  int nb[NSLOT];
+// ---- level-0 stencil apply: y = K x or y = b - K x over the positions p0 .. p1-1 -------------
+// nn positions, slot-major arrays of row stride `stride`. Absent stencil slots hold exact zeros,
+// so they read the node's own x (branch-free). NPT = 1:
+// thread per position, the 27 neighbour ids fetched first. NPT = 2 or 4 (FP32 operator, row
+// stride a multiple of 4): thread per aligned group of positions, every slot value of the group
+// one vector load; the per-node arithmetic is the same for every NPT.
+template <int NPT>
+struct VecOf;
+template <>
+struct VecOf<2> { typedef float2 type; };
+template <>
+struct VecOf<4> { typedef float4 type; };
+__device__ __forceinline__ float vcomp(const float2& v, int k) { return k == 0 ? v.x : v.y; }
+__device__ __forceinline__ float vcomp(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+template <class T>
+struct ApplyMinBlocks { static constexpr int value = 16; };
+template <>
+struct ApplyMinBlocks<float> { static constexpr int value = TM_APPLY32_MINB; };
+
+template <class T, class V, int NPT>
+__global__ void __launch_bounds__(128, ApplyMinBlocks<T>::value) k_apply0(int p0, int p1, int stride, int nn, const int* __restrict__ posNode,
+                                                                         const int* __restrict__ nbr, const T* __restrict__ val,
+                                                                         const V* __restrict__ x, V* __restrict__ y,
+                                                                         const V* __restrict__ b) {
+  if constexpr (NPT == 1) {
+    const int ps = p0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (ps >= p1) return;
+    const int n = posNode[ps];
+    T y0 = 0, y1 = 0, y2 = 0;
+    int nb[NSLOT];
 #pragma unroll
-  for (int s = 0; s < NSLOT; s++) {
-    const int j = nbr[(size_t)s * nn + ps];
-    nb[s] = j < 0 ? n : j;
-  }
+    for (int s = 0; s < NSLOT; s++) {
+      const int j = nbr[(size_t)s * stride + ps];
+      nb[s] = j < 0 ? n : j;
+    }
 #pragma unroll
-  for (int s = 0; s < NSLOT; s++) {
-    const size_t j = nb[s];
-    const T x0 = (T)x[3 * j], x1 = (T)x[3 * j + 1], x2 = (T)x[3 * j + 2];
-    const T* v = val + (size_t)s * 9 * nn + ps;
-    y0 += v[0] * x0 + v[(size_t)nn] * x1 + v[2 * (size_t)nn] * x2;
-    y1 += v[3 * (size_t)nn] * x0 + v[4 * (size_t)nn] * x1 + v[5 * (size_t)nn] * x2;
-    y2 += v[6 * (size_t)nn] * x0 + v[7 * (size_t)nn] * x1 + v[8 * (size_t)nn] * x2;
-  }
-  if (b) {
-    y[3 * n] = b[3 * n] - (V)y0; y[3 * n + 1] = b[3 * n + 1] - (V)y1; y[3 * n + 2] = b[3 * n + 2] - (V)y2;
+    for (int s = 0; s < NSLOT; s++) {
+      const size_t j = nb[s];
+      const T x0 = (T)x[3 * j], x1 = (T)x[3 * j + 1], x2 = (T)x[3 * j + 2];
+      const T* v = val + (size_t)s * 9 * stride + ps;
+      y0 += v[0] * x0 + v[(size_t)stride] * x1 + v[2 * (size_t)stride] * x2;
+      y1 += v[3 * (size_t)stride] * x0 + v[4 * (size_t)stride] * x1 + v[5 * (size_t)stride] * x2;
+      y2 += v[6 * (size_t)stride] * x0 + v[7 * (size_t)stride] * x1 + v[8 * (size_t)stride] * x2;
+    }
+    if (b) {
+      y[3 * n] = b[3 * n] - (V)y0; y[3 * n + 1] = b[3 * n + 1] - (V)y1; y[3 * n + 2] = b[3 * n + 2] - (V)y2;
+    } else {
+      y[3 * n] = (V)y0; y[3 * n + 1] = (V)y1; y[3 * n + 2] = (V)y2;
+    }
   } else {
-    y[3 * n] = (V)y0; y[3 * n + 1] = (V)y1; y[3 * n + 2] = (V)y2;
+    static_assert((NPT == 2 || NPT == 4) && sizeof(T) == 4, "position groups are for the FP32 operator");
+    typedef typename VecOf<NPT>::type VT;
+    const int pa = (p0 & ~(NPT - 1)) + NPT * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (pa >= p1) return;
+    // positions outside [p0, p1) are computed on valid memory (positions < nn, or the zero
+    // padding of the operator rows) and not stored
+    int n[NPT];
+    T acc[NPT][3];
+#pragma unroll
+    for (int k = 0; k < NPT; k++) {
+      n[k] = pa + k < nn ? posNode[pa + k] : 0;
+      acc[k][0] = acc[k][1] = acc[k][2] = 0;
+    }
+    const size_t sv = (size_t)stride / NPT;
+    TM_UNROLL(TM_APPLY32_UNROLL)
+    for (int s = 0; s < NSLOT; s++) {
+      T xv[NPT][3];
+#pragma unroll
+      for (int k = 0; k < NPT; k++) {
+        const int jj = pa + k < nn ? nbr[(size_t)s * stride + pa + k] : -1;
+        const size_t j = jj < 0 ? n[k] : jj;
+        xv[k][0] = (T)x[3 * j]; xv[k][1] = (T)x[3 * j + 1]; xv[k][2] = (T)x[3 * j + 2];
+      }
+      const VT* v = reinterpret_cast<const VT*>(val + (size_t)s * 9 * stride + pa);
+      VT vq[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) vq[q] = v[q * sv];
+#pragma unroll
+      for (int k = 0; k < NPT; k++)
+#pragma unroll
+        for (int r3 = 0; r3 < 3; r3++)
+          acc[k][r3] += vcomp(vq[3 * r3], k) * xv[k][0] + vcomp(vq[3 * r3 + 1], k) * xv[k][1] + vcomp(vq[3 * r3 + 2], k) * xv[k][2];
+    }
+#pragma unroll
+    for (int k = 0; k < NPT; k++) {
+      if (pa + k < p0 || pa + k >= p1) continue;
+      const size_t m = n[k];
+      if (b) { y[3 * m] = b[3 * m] - (V)acc[k][0]; y[3 * m + 1] = b[3 * m + 1] - (V)acc[k][1]; y[3 * m + 2] = b[3 * m + 2] - (V)acc[k][2]; }
+      else { y[3 * m] = (V)acc[k][0]; y[3 * m + 1] = (V)acc[k][1]; y[3 * m + 2] = (V)acc[k][2]; }
+    }
   }
+}
+
+// threads of an apply over positions p0 .. p1-1
+template <int NPT>
+inline size_t apply_threads(int p0, int p1) {
+  return (size_t)(p1 - (p0 & ~(NPT - 1)) + NPT - 1) / NPT;
 }
 
 // ---- deterministic reductions ----------------------------------------------------------------
@@ -271,12 +340,13 @@ __host__ __device__ inline size_t shell_stage_bytes(int maxm, int maxBlk) {
   return (b + 15) / 16 * 16;
 }
 
-// residual rows r = b - K x of the column whose aggregates are n0 .. n0+na-1, by one warp: the
+// residual rows r = b - K x of the column whose aggregates are n0 .. n0+na-1 (blocks k0 ..
+// k0+nblk-1), by one warp: the
 // lanes take the column's blocks (all rows together), each lane's 6 products of a block land in
 // shared memory, and lane e then subtracts its row's block sums in block order, as the serial
 // row loop of columnSweep (10-solver.js:535-553) does
 template <class T>
-__device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, const int* __restrict__ rowPtr,
+__device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, int k0, int nblk, const int* __restrict__ rowPtr,
                                                       const int* __restrict__ col, const T* __restrict__ val,
                                                       const T* __restrict__ b, const T* __restrict__ x, bool zeroGuess,
                                                       T* part, T* r, int* rp) {
@@ -286,9 +356,7 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
     __syncwarp();
     return;
   }
-  const int k0 = rowPtr[n0];
   for (int q = lane; q <= na; q += 32) rp[q] = rowPtr[n0 + q] - k0;
-  const int nblk = rowPtr[n0 + na] - k0;
   for (int e = lane; e < nblk; e += 32) {
     const T* xj = x + 6 * (size_t)col[k0 + e];
     T v[36];
@@ -308,9 +376,10 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
   __syncwarp();
 }
 
-// shell-level residual res = b - K x over all columns, warp per column
+// shell-level residual res = b - K x over all columns, warp per column (meta: first and
+// one-past-last aggregate and block of every column)
 template <class T>
-__global__ void __launch_bounds__(128) k_apply_shell(int ncol, const int* __restrict__ colStart, const int* __restrict__ rowPtr,
+__global__ void __launch_bounds__(128) k_apply_shell(int ncol, const int4* __restrict__ meta, const int* __restrict__ rowPtr,
                                                      const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ x,
                                                      const T* __restrict__ b, T* __restrict__ y, int maxm, int maxBlk) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -321,21 +390,23 @@ __global__ void __launch_bounds__(128) k_apply_shell(int ncol, const int* __rest
   T* part = reinterpret_cast<T*>(base);
   T* r = part + 6 * (size_t)maxBlk;
   int* rp = reinterpret_cast<int*>(r + (maxm > SH_PRE ? maxm : SH_PRE));
-  const int n0 = colStart[c], na = colStart[c + 1] - n0;
-  shell_column_residual(lane, n0, na, rowPtr, col, val, b, x, false, part, r, rp);
+  const int4 mt = meta[c];
+  const int n0 = mt.x, na = mt.y - mt.x;
+  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, false, part, r, rp);
   for (int e = lane; e < 6 * na; e += 32) y[6 * (size_t)n0 + e] = r[e];
 }
 
 // shell-level column sweep, warp per column of one colour (columnSweep shell branch,
 // 10-solver.js:535-553): r = b - K x over the column's rows, then x_col += A_cc^-1 r with the
-// explicit inverse of the column block. For blocks of at most SH_PRE rows every lane fetches its
-// row of the inverse before the residual, so that those loads overlap the residual's.
+// explicit inverse of the column block. The colour's column list carries each column's aggregate
+// and block ranges and the offset of its inverse (one load). For blocks of at most SH_PRE rows
+// every lane fetches its row of the inverse before the residual, so that those loads overlap the
+// residual's.
 template <class T>
-__global__ void __launch_bounds__(128) k_sweep_shell(int ncolc, const int* __restrict__ cols, const int* __restrict__ colStart,
+__global__ void __launch_bounds__(128) k_sweep_shell(int ncolc, const int4* __restrict__ meta, const long long* __restrict__ cfOff,
                                                      const int* __restrict__ rowPtr, const int* __restrict__ col,
-                                                     const T* __restrict__ val, const long long* __restrict__ cfPtr,
-                                                     const T* __restrict__ cf, const T* __restrict__ b, T* __restrict__ x, int maxm,
-                                                     int maxBlk, int zeroGuess) {
+                                                     const T* __restrict__ val, const T* __restrict__ cf, const T* __restrict__ b,
+                                                     T* __restrict__ x, int maxm, int maxBlk, int zeroGuess) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -344,14 +415,14 @@ __global__ void __launch_bounds__(128) k_sweep_shell(int ncolc, const int* __res
   T* part = reinterpret_cast<T*>(base);
   T* r = part + 6 * (size_t)maxBlk;
   int* rp = reinterpret_cast<int*>(r + (maxm > SH_PRE ? maxm : SH_PRE));
-  const int c = cols[gw];
-  const int n0 = colStart[c], na = colStart[c + 1] - n0, m = 6 * na;
-  const T* Ai = cf + cfPtr[c];   // entry (e, k) at k*m + e
+  const int4 mt = meta[gw];
+  const int n0 = mt.x, na = mt.y - mt.x, m = 6 * na;
+  const T* Ai = cf + cfOff[gw];   // entry (e, k) at k*m + e
   T a[SH_PRE];
   const bool pre = m <= SH_PRE;
 #pragma unroll
   for (int k = 0; k < SH_PRE; k++) a[k] = (pre && lane < m && k < m) ? Ai[(size_t)k * m + lane] : (T)0;
-  shell_column_residual(lane, n0, na, rowPtr, col, val, b, x, zeroGuess != 0, part, r, rp);
+  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, zeroGuess != 0, part, r, rp);
   if (pre) {
     if (lane < m) {
       T acc = 0;
@@ -466,6 +537,20 @@ struct Bufs<float> {
   static float* res(ShellLevel& L) { return L.d_res32.p; }
 };
 
+// y = K x (or b - K x) over the positions p0 .. p1-1: FP32 operators in position groups, FP64
+// operators one position per thread
+template <class T, class V>
+void apply0_range(Context& c, const T* val, int p0, int p1, const V* x, V* y, const V* b) {
+  if (p1 <= p0) return;
+  if constexpr (sizeof(T) == 4)
+    k_apply0<T, V, TM_APPLY32_NPT><<<grid_for(apply_threads<TM_APPLY32_NPT>(p0, p1), 128), 128, 0, c.stream>>>(
+        p0, p1, c.nnp, c.nn, c.d_posNode.p, c.d_nbr.p, val, x, y, b);
+  else
+    k_apply0<T, V, 1><<<grid_for(apply_threads<1>(p0, p1), 128), 128, 0, c.stream>>>(p0, p1, c.nnp, c.nn, c.d_posNode.p, c.d_nbr.p,
+                                                                                     val, x, y, b);
+  note_launch();
+}
+
 // MultigridPC._cycleOnce (10-solver.js:687-712) with zero initial guess on every level
 template <class T>
 void vcycle(Context& c, const T* r, T* z) {
@@ -478,7 +563,7 @@ void vcycle(Context& c, const T* r, T* z) {
   auto sweep0 = [&](int col, int zero) {
     if (!c.grpCount[col]) return;
     TimedLaunch tl(c, K_SWEEP_SOLID);
-    k_sweep_panel<T><<<c.grpCount[col], TM_PANEL_THREADS, smem0, st>>>(c.d_grpStart[col].p, c.d_colPos[col].p, c.d_posNode.p, nn,
+    k_sweep_panel<T><<<c.grpCount[col], TM_PANEL_THREADS, smem0, st>>>(c.d_grpStart[col].p, c.d_colPos[col].p, c.d_posNode.p, c.nnp,
                                                                       c.d_nbr.p, B::val0(c), B::F(c), r, z, c.panelCap, zero);
     note_launch();
   };
@@ -493,8 +578,8 @@ void vcycle(Context& c, const T* r, T* z) {
     const size_t per = shell_stage_bytes<T>(L.maxm, L.maxColBlocks);
     TimedLaunch tl(c, K_SWEEP_SHELL);
     k_sweep_shell<T><<<grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st>>>(
-        L.colorCount[col], L.d_colorCols[col].p, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, B::val(L), L.d_cfPtr.p, B::cf(L), B::b(L),
-        B::x(L), L.maxm, L.maxColBlocks, zero);
+        L.colorCount[col], L.d_colorMeta[col].p, L.d_colorCf[col].p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::cf(L), B::b(L), B::x(L),
+        L.maxm, L.maxColBlocks, zero);
     note_launch();
   };
   // ---- level 0 pre-smoothing: 2 sweeps in colours 0..3
@@ -507,8 +592,7 @@ void vcycle(Context& c, const T* r, T* z) {
     }
   {
     TimedLaunch tl(c, K_APPLY0);
-    k_apply0<T, T><<<grid_for(nn, 128), 128, 0, st>>>(nn, c.d_posNode.p, c.d_nbr.p, B::val0(c), z, B::res0(c), r);
-    note_launch();
+    apply0_range<T, T>(c, B::val0(c), 0, nn, z, B::res0(c), r);
   }
   ShellLevel& L1 = *c.shells[0];
   k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, B::W01(c), B::res0(c), B::b(L1));
@@ -534,7 +618,7 @@ void vcycle(Context& c, const T* r, T* z) {
       TimedLaunch tl(c, K_APPLY_SHELL);
       const int ncol = L.nx * L.ny;
       k_apply_shell<T><<<grid_for(ncol, wpb), 32 * wpb, wpb * shell_stage_bytes<T>(L.maxm, L.maxColBlocks), st>>>(
-          ncol, L.d_colStart.p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L), L.maxm, L.maxColBlocks);
+          ncol, L.d_colMeta.p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L), L.maxm, L.maxColBlocks);
       note_launch();
     }
     ShellLevel& C = *c.shells[l + 1];
@@ -580,21 +664,18 @@ TimedLaunch::~TimedLaunch() {
 
 void launch_apply0(Context& c, const double* x, double* y, const double* b) {
   TimedLaunch tl(c, K_APPLY0);
-  k_apply0<double, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_val.p, x, y, b);
-  note_launch();
+  apply0_range<double, double>(c, c.d_val.p, 0, c.nn, x, y, b);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_apply0_f32(Context& c, const double* x, double* y, const double* b) {
-  k_apply0<float, double><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_val32.p, x, y, b);
-  note_launch();
+  apply0_range<float, double>(c, c.d_val32.p, 0, c.nn, x, y, b);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_apply0_32(Context& c, const float* x, float* y, const float* b) {
   TimedLaunch tl(c, K_APPLY0);
-  k_apply0<float, float><<<grid_for(c.nn, 128), 128, 0, c.stream>>>(c.nn, c.d_posNode.p, c.d_nbr.p, c.d_val32.p, x, y, b);
-  note_launch();
+  apply0_range<float, float>(c, c.d_val32.p, 0, c.nn, x, y, b);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
