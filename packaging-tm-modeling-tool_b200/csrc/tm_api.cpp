@@ -38,6 +38,8 @@ Context::~Context() {
   for (auto* L : shells) delete L;
   for (auto* b : basis) delete b;
   for (auto& e : timerEvents) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  for (auto& g : vcGraph) if (g) cudaGraphExecDestroy(g);
+  if (capStream) cudaStreamDestroy(capStream);
   if (stream && ownStream) cudaStreamDestroy(stream);
 }
 

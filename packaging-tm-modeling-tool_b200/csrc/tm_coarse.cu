@@ -195,23 +195,28 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
     if (lane == 0) s_fix = fixes;
   }
   __syncthreads();
-  // 2. panel rows of the tiles ti and tj: P[r][k] = (A[g][jb+k] - sum_t<k P[r][t] L[k][t]) / L[k][k]
+  // 2. panel rows of the tiles ti and tj: first the rows of A (all threads, zero outside the
+  //    band and the window), then P[r][k] = (A[g][jb+k] - sum_t<k P[r][t] L[k][t]) / L[k][k],
+  //    thread per row, in shared memory
+  for (int e = tid; e < 2 * CN * CN; e += nthr) {
+    const int which = e / (CN * CN), r = (e / CN) % CN, k = e % CN;
+    if (which == 1 && ti == tj) continue;
+    const int tile = which ? tj : ti;
+    const int g = i0 + tile * CN + r, kk = jb + k;
+    double a = 0;
+    if (tile * CN + r < R && k < nbk && g - kk <= bw) a = A[(size_t)g * w + (kk - g + bw)];
+    (which ? Pj : Pi)[r][k] = a;
+  }
+  __syncthreads();
   if (tid < 64) {
     const int which = tid >> 5, r = tid & 31;
     const int tile = which ? tj : ti;
     double* P = which ? &Pj[r][0] : &Pi[r][0];
-    const int g = i0 + tile * CN + r;
-    if (!(which == 1 && ti == tj)) {
-      const bool live = tile * CN + r < R;
-      for (int k = 0; k < CN; k++) {
-        double a = 0;
-        if (live && k < nbk) {
-          const int kk = jb + k;
-          a = (g - kk <= bw) ? A[(size_t)g * w + (kk - g + bw)] : 0.0;
-          for (int t = 0; t < k; t++) a -= P[t] * Ds[k][t];
-          a /= Ds[k][k];
-        }
-        P[k] = a;
+    if (!(which == 1 && ti == tj) && tile * CN + r < R) {
+      for (int k = 0; k < nbk; k++) {
+        double a = P[k];
+        for (int t = 0; t < k; t++) a -= P[t] * Ds[k][t];
+        P[k] = a / Ds[k][k];
       }
     }
   }

@@ -404,6 +404,7 @@ static int cell_elem_at(const Context& c, long cell, int q) {
 }
 
 void build_hierarchy(Context& c) {
+  c.structEpoch++;
   const int nx = c.nx, ny = c.ny, nz = c.nz, ncy = ny - 1, ncz = nz - 1, nn = c.nn;
   for (auto* L : c.shells) delete L;
   c.shells.clear();

@@ -228,6 +228,14 @@ struct Context {
   int colJitter = 0, shellJitter = 0;
   // warm start basis (unscaled space)
   std::vector<DBuf<double>*> basis;
+  // the V-cycle as a CUDA graph per precision (0: FP64, 1: FP32), captured on first use on a
+  // private stream and replayed on the caller's; captured again when its vectors or the
+  // hierarchy's buffers (structEpoch) change
+  cudaGraphExec_t vcGraph[2] = {nullptr, nullptr};
+  size_t vcKey[2] = {0, 0};
+  long long vcNodes[2] = {0, 0};
+  cudaStream_t capStream = nullptr;
+  long long structEpoch = 0;
   ~Context();
 };
 

@@ -779,11 +779,58 @@ void launch_add_f2d(Context& c, const float* d, double* x, size_t n) {
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
-void launch_vcycle(Context& c, const double* r, double* z, bool mixed) {
-  (void)mixed;
-  vcycle<double>(c, r, z);
+// the V-cycle replayed from a CUDA graph (about 130 launches of mostly small kernels per cycle);
+// launched directly while a kernel class is being timed (the timer's events are per launch)
+template <class T>
+void vcycle_graph(Context& c, const T* r, T* z) {
+  if (c.timerKernel >= 0) {
+    vcycle<T>(c, r, z);
+    return;
+  }
+  const int idx = sizeof(T) == 4 ? 1 : 0;
+  size_t key = 1469598103934665603ull;
+  for (size_t v : {(size_t)r, (size_t)z, (size_t)c.structEpoch, (size_t)Bufs<T>::val0(c), (size_t)c.stream})
+    key = (key ^ v) * 1099511628211ull;
+  if (!c.vcGraph[idx] || c.vcKey[idx] != key) {
+    if (c.vcGraph[idx]) {
+      TM_CUDA_CHECK(cudaGraphExecDestroy(c.vcGraph[idx]));
+      c.vcGraph[idx] = nullptr;
+    }
+    if (!c.capStream) TM_CUDA_CHECK(cudaStreamCreateWithFlags(&c.capStream, cudaStreamNonBlocking));
+    // the caller's stream may be the legacy default stream, which cannot be captured: capture
+    // on the private stream, launch on the caller's
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    cudaStream_t saved = c.stream;
+    c.stream = c.capStream;
+    const long long n0 = launch_count();
+    cudaGraph_t g = nullptr;
+    TM_CUDA_CHECK(cudaStreamBeginCapture(c.capStream, cudaStreamCaptureModeThreadLocal));
+    try {
+      vcycle<T>(c, r, z);
+    } catch (...) {
+      cudaStreamEndCapture(c.capStream, &g);
+      if (g) cudaGraphDestroy(g);
+      c.stream = saved;
+      throw;
+    }
+    c.stream = saved;
+    TM_CUDA_CHECK(cudaStreamEndCapture(c.capStream, &g));
+    c.vcNodes[idx] = launch_count() - n0;
+    note_launch((int)-c.vcNodes[idx]);   // captured, not run
+    const cudaError_t e = cudaGraphInstantiate(&c.vcGraph[idx], g, 0);
+    cudaGraphDestroy(g);
+    TM_CUDA_CHECK(e);
+    c.vcKey[idx] = key;
+  }
+  TM_CUDA_CHECK(cudaGraphLaunch(c.vcGraph[idx], c.stream));
+  note_launch((int)c.vcNodes[idx]);
 }
 
-void launch_vcycle32(Context& c, const float* r, float* z) { vcycle<float>(c, r, z); }
+void launch_vcycle(Context& c, const double* r, double* z, bool mixed) {
+  (void)mixed;
+  vcycle_graph<double>(c, r, z);
+}
+
+void launch_vcycle32(Context& c, const float* r, float* z) { vcycle_graph<float>(c, r, z); }
 
 }  // namespace tmg
