@@ -45,6 +45,8 @@ Context::~Context() {
 
 namespace {
 
+void check_device_error(Context& c);
+
 double now_ms() {
   using namespace std::chrono;
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
@@ -403,6 +405,7 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
     in.iters = res.iters; in.relres = res.relres; in.iters0 = res.iters0; in.converged = res.converged;
     in.ms = now_ms() - t0; in.pc_ms = pcMs; in.rebuilt = rebuilt; in.warm = (int)c.basis.size();
     in.jitter_count = c.colJitter; in.refinements = sweeps;
+    check_device_error(c);
     in.status = res.nonfinite ? TM_NONFINITE : (res.converged ? TM_OK : TM_NOT_CONVERGED);
     if (info) *info = in;
     if (res.nonfinite) fail(TM_NONFINITE, "non-finite value in the refinement");
@@ -430,6 +433,7 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   in.iters = total; in.relres = res.relres; in.iters0 = res.iters0; in.converged = res.converged;
   in.ms = now_ms() - t0; in.pc_ms = pcMs; in.rebuilt = rebuilt; in.warm = (int)c.basis.size(); in.fallback = 0;
   in.jitter_count = c.colJitter;
+  check_device_error(c);
   in.status = res.nonfinite ? TM_NONFINITE : (res.converged ? TM_OK : TM_NOT_CONVERGED);
   if (info) *info = in;
   if (res.nonfinite) fail(TM_NONFINITE, "non-finite value in the PCG iteration");
@@ -463,6 +467,20 @@ void upload_mesh(Context& c) {
   c.d_partial.alloc(1024);
   c.d_scalars.alloc(16);
   c.d_jitter.alloc(1);
+  c.d_err.alloc(1);
+  c.d_err.zero(s);
+}
+
+// a bounded device wait that ran out (the results of the solve are invalid)
+void check_device_error(Context& c) {
+  int err = 0;
+  TM_CUDA_CHECK(cudaMemcpyAsync(&err, c.d_err.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  if (err) {
+    c.d_err.zero(c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    fail(TM_TIMEOUT, "a bounded wait of the level-0 sweep ran out");
+  }
 }
 
 }  // namespace

@@ -532,6 +532,7 @@ void build_hierarchy(Context& c) {
   // at most panelCap nodes; a column longer than panelCap forms a group of its own
   c.panelCap = std::max(TM_PANEL_THREADS, c.maxColLen);
   c.panelMaxCols = 0;
+  std::vector<int> colPos[4];
   for (int k = 0; k < 4; k++) {
     std::vector<int> cols;
     for (int col = 0; col < nx * ny; col++) {
@@ -558,14 +559,17 @@ void build_hierarchy(Context& c) {
         fail(TM_BAD_INPUT, "colour columns are not contiguous in position order");
     }
     c.d_colPos[k].upload(cp, st);
+    colPos[k] = cp;
   }
+  plan_sweep_tma(c, colPos, st);
   c.d_nodeAgg.upload(c.nodeAgg, st);
   c.d_aggStart.upload(c.aggStart, st);
   galerkin_lists01(c, st);
   for (size_t l = 0; l + 1 < c.shells.size(); l++) galerkin_lists_shell(*c.shells[l], *c.shells[l + 1], st);
   c.d_zp.upload(c.zp, st);
   c.d_W01.alloc(18 * (size_t)nn);
-  c.d_F.alloc(18 * (size_t)nn);
+  c.d_F.alloc(18 * (size_t)c.nnp);   // position-ordered, rows to the padded stride (the sweep's bulk copies read whole 4-position groups)
+  c.d_F.zero(st);
   c.d_res0.alloc(3 * (size_t)nn);
   for (size_t l = 0; l < c.shells.size(); l++) {
     ShellLevel& L = *c.shells[l];

@@ -71,6 +71,9 @@ struct DBuf {
 #endif
 // FP32 level-0 apply: positions per thread (1, 2 or 4; the operator rows are padded to a
 // multiple of 4), unroll depth of its slot loop and the resident CTAs its registers are sized for
+#ifndef TM_SWEEP_TMA
+#define TM_SWEEP_TMA 1
+#endif
 #ifndef TM_APPLY32_NPT
 #define TM_APPLY32_NPT 2
 #endif
@@ -197,6 +200,17 @@ struct Context {
   DBuf<int> d_colorCols[4];
   int colorCount[4] = {0, 0, 0, 0};
   int maxColLen = 0;
+  // level-0 sweep of the FP32 V-cycle with TMA-streamed operator rows (tm_sweep_tma.cu): per
+  // colour the runs of whole columns of each CTA (indices into the colour's column list), the
+  // longest run, the chunk stages, the two tensor maps (operator rows, neighbour ids)
+  bool tsReady = false;
+  int tsParts = 0, tsMaxNodes = 0, tsStages = 0;
+  DBuf<int> d_tsPart[4];
+  alignas(64) unsigned char tsMapVal[128];
+  alignas(64) unsigned char tsMapNbr[128];
+  const void* tsValPtr = nullptr;
+  const void* tsNbrPtr = nullptr;
+  DBuf<int> d_err;                     // set by a bounded device wait that ran out
   // level-0 column panels: the columns of one colour packed into groups of at most panelCap nodes,
   // one CTA per group (group g holds colour columns grpStart[g] .. grpStart[g+1]-1); colPos holds
   // the position of the first node of every colour column plus one past the colour's last node
@@ -293,6 +307,10 @@ void launch_scale_vec(Context& c, const double* x, const double* s, double* y, b
 void launch_finalize(Context& c, double* out_dev);                                  // sum of the last reduction partials
 void launch_axpy(Context& c, double alpha, const double* x, double* y, size_t n);   // y += alpha x
 void launch_div_scalar(Context& c, double* v, double d, size_t n);                  // v /= d
+
+// ---- level-0 sweep of the FP32 V-cycle with TMA-streamed operator rows (tm_sweep_tma.cu)
+void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st);
+bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float* x);   // false: not available
 
 // ---- Anand (tm_anand.cu) ---------------------------------------------------------------------
 void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps_h,

@@ -563,6 +563,8 @@ void vcycle(Context& c, const T* r, T* z) {
   auto sweep0 = [&](int col, int zero) {
     if (!c.grpCount[col]) return;
     TimedLaunch tl(c, K_SWEEP_SOLID);
+    if constexpr (sizeof(T) == 4)
+      if (launch_sweep_tma(c, col, zero, r, z)) return;
     k_sweep_panel<T><<<c.grpCount[col], TM_PANEL_THREADS, smem0, st>>>(c.d_grpStart[col].p, c.d_colPos[col].p, c.d_posNode.p, c.nnp,
                                                                       c.d_nbr.p, B::val0(c), B::F(c), r, z, c.panelCap, zero);
     note_launch();

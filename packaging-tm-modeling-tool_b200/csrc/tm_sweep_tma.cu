@@ -1,0 +1,354 @@
+// Level-0 column smoother of the FP32 V-cycle (columnSweep solid branch + solveColumn,
+// src/core/10-solver.js:71-104, 512-534), one colour per launch, as a persistent per-SM sweep:
+//
+//  * every CTA (one per SM) owns a contiguous run of whole columns of the colour (about 1/148 of
+//    the colour's nodes; the colour's positions are contiguous, so the run is one position range);
+//  * the run's operator rows (243 values per position) and neighbour ids (27) stream through
+//    shared memory in chunks of 64 positions, each chunk one pair of 2-D TMA tensor loads
+//    (cp.async.bulk.tensor, no multicast) completing on an mbarrier, in a ring of stages so that
+//    the loads of later chunks are in flight while a chunk's residual rows are computed;
+//  * r starts as the run's b in shared memory; 8 threads per position take the 27 slots (a warp
+//    takes 32 consecutive positions of one slot group), their partial rows are added in a fixed
+//    order and subtracted from r;
+//  * the run's column factors then arrive with one bulk copy into the freed stage memory;
+//  * one thread per column then runs the block-tridiagonal forward/backward substitution and
+//    the run's x is updated.
+//
+// Columns of one colour do not couple, so runs never read each other's updates. Every wait on
+// an mbarrier is bounded: a wait that runs out sets the error flag, waits (bounded) for the
+// copies still in flight and leaves; the host reports TM_TIMEOUT.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "tm_internal.h"
+
+namespace tmg {
+
+namespace {
+
+constexpr int TS_THREADS = 512;
+constexpr int TS_CHUNK = 64;                                       // positions per chunk (one TMA box)
+constexpr int TS_TPP = TS_THREADS / TS_CHUNK;                      // threads per position
+constexpr int TS_ROWS = NSLOT * 9;                                 // operator rows
+constexpr int TS_STAGE_BYTES = (TS_ROWS + NSLOT) * TS_CHUNK * 4;   // values, then neighbour ids
+constexpr int TS_MAXSTAGE = 4;
+constexpr long long TS_WAIT_LIMIT = 1LL << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile(
+      "{\n"
+      " .reg .b64 st;\n"
+      " mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n"
+      "}\n" ::"r"(smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// bounded wait for the phase of the given parity
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  for (long long it = 0; it < TS_WAIT_LIMIT; it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// L2 policies: the streamed operator rows are read once per sweep (evict first), the gathered
+// x is read by every sweep (evict last)
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float ld_keep(const float* p, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+// box of a 2-D tensor map at (x, y) into shared memory, completing on bar
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+// contiguous bytes into shared memory (16-byte aligned source, destination and size)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+    k_sweep_tma(const __grid_constant__ CUtensorMap tmVal, const __grid_constant__ CUtensorMap tmNbr, const int* __restrict__ partCol,
+                const int* __restrict__ colPos, const int* __restrict__ posNode, const float* __restrict__ F, const float* __restrict__ b,
+                float* __restrict__ x, int maxNodes, int nstage, int zeroGuess, int* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smraw_t[];
+  __shared__ __align__(8) uint64_t bars[TS_MAXSTAGE + 1];   // chunk stages, then the factors
+  // 128-byte aligned start of the stages (the launch adds 128 bytes for this)
+  unsigned char* smt = smraw_t + ((128u - (smem_u32(smraw_t) & 127u)) & 127u);
+  const int tid = threadIdx.x;
+  const int c0 = partCol[blockIdx.x], c1 = partCol[blockIdx.x + 1];
+  if (c0 >= c1) return;
+  const int P0 = colPos[c0], P1 = colPos[c1];
+  const int Q0 = P0 & ~3, QE = (P1 + 3) & ~3;   // 16-byte aligned window of the run
+  const int nchunks = zeroGuess ? 0 : (QE - Q0 + TS_CHUNK - 1) / TS_CHUNK;
+  // the run's factors land in the stage memory once the operator rows have streamed through
+  const float* sF = reinterpret_cast<const float*>(smt);                                  // (QE - Q0) x 18
+  float* sr = reinterpret_cast<float*>(smt + (size_t)nstage * TS_STAGE_BYTES);            // run rows x 3
+  float* red = sr + 3 * (size_t)maxNodes;                                                 // TS_TPP x TS_CHUNK x 3 partial rows
+  uint64_t* fbar = &bars[TS_MAXSTAGE];
+  if (tid == 0) {
+    for (int s = 0; s < nstage; s++) mbar_init(&bars[s], 1);
+    mbar_init(fbar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int issued = 0;   // chunks issued (thread 0)
+  const uint64_t polStream = policy_evict_first(), polKeep = policy_evict_last();
+  auto issue = [&](int k) {
+    float* dst = reinterpret_cast<float*>(smt + (size_t)(k % nstage) * TS_STAGE_BYTES);
+    mbar_expect_tx(&bars[k % nstage], TS_STAGE_BYTES);
+    tma_load_2d(dst, &tmVal, Q0 + k * TS_CHUNK, 0, &bars[k % nstage], polStream);
+    tma_load_2d(dst + TS_ROWS * TS_CHUNK, &tmNbr, Q0 + k * TS_CHUNK, 0, &bars[k % nstage], polStream);
+  };
+  if (tid == 0)
+    for (; issued < nstage && issued < nchunks; issued++) issue(issued);
+  // r starts as b (the chunks subtract K x)
+  for (int l = tid; l < P1 - P0; l += blockDim.x) {
+    const size_t n = posNode[P0 + l];
+    sr[3 * l] = b[3 * n]; sr[3 * l + 1] = b[3 * n + 1]; sr[3 * l + 2] = b[3 * n + 2];
+  }
+  bool failed = false;
+  int k = 0;
+  // a warp takes 32 consecutive positions of one slot group: conflict-free shared-memory rows
+  const int pl = tid % TS_CHUNK, sub = tid / TS_CHUNK;
+  __shared__ int s_fail;
+  if (tid == 0) s_fail = 0;
+  __syncthreads();
+  for (; k < nchunks; k++) {
+    const bool ok = mbar_wait(&bars[k % nstage], (unsigned)(k / nstage) & 1u);
+    if (!ok) s_fail = 1;
+    const float* sv = reinterpret_cast<const float*>(smt + (size_t)(k % nstage) * TS_STAGE_BYTES);
+    const int* sn = reinterpret_cast<const int*>(sv + TS_ROWS * TS_CHUNK);
+    const int p = Q0 + k * TS_CHUNK + pl;
+    const bool live = ok && p >= P0 && p < P1;
+    float a0 = 0, a1 = 0, a2 = 0;
+    if (live) {
+#pragma unroll
+      for (int h = 0; h < (NSLOT + TS_TPP - 1) / TS_TPP; h++) {
+        const int s = sub + TS_TPP * h;
+        if (s < NSLOT) {
+          const int jj = sn[s * TS_CHUNK + pl];
+          const size_t j = jj < 0 ? 0 : jj;   // absent slots hold zeros
+          const float x0 = ld_keep(x + 3 * j, polKeep), x1 = ld_keep(x + 3 * j + 1, polKeep), x2 = ld_keep(x + 3 * j + 2, polKeep);
+          const float* v = sv + s * 9 * TS_CHUNK + pl;
+          a0 += v[0] * x0 + v[TS_CHUNK] * x1 + v[2 * TS_CHUNK] * x2;
+          a1 += v[3 * TS_CHUNK] * x0 + v[4 * TS_CHUNK] * x1 + v[5 * TS_CHUNK] * x2;
+          a2 += v[6 * TS_CHUNK] * x0 + v[7 * TS_CHUNK] * x1 + v[8 * TS_CHUNK] * x2;
+        }
+      }
+    }
+    float* rd = red + 3 * (size_t)(sub * TS_CHUNK + pl);
+    rd[0] = a0; rd[1] = a1; rd[2] = a2;
+    __syncthreads();   // the stage is read: refill it while the partial rows are added
+    if (s_fail) { failed = true; break; }
+    if (tid == 0 && issued < nchunks) {
+      fence_proxy_async();   // the stage being refilled was last read by the threads
+      issue(issued);
+      issued++;
+    }
+    // the slot groups' partial rows of a position, added in group order
+    if (tid < 3 * TS_CHUNK) {
+      const int pq = tid / 3, q = tid % 3, pp = Q0 + k * TS_CHUNK + pq;
+      if (pp >= P0 && pp < P1) {
+        float acc = red[3 * pq + q];
+#pragma unroll
+        for (int g = 1; g < TS_TPP; g++) acc += red[3 * (g * TS_CHUNK + pq) + q];
+        sr[3 * (pp - P0) + q] -= acc;
+      }
+    }
+    __syncthreads();
+  }
+  bool fIssued = false;   // thread 0
+  if (!failed && tid == 0) {
+    // the factors into the (now free) stage memory
+    const unsigned fbytes = (unsigned)(QE - Q0) * 18 * 4;
+    fence_proxy_async();
+    mbar_expect_tx(fbar, fbytes);
+    bulk_load(smt, F + 18 * (size_t)Q0, fbytes, fbar);
+    fIssued = true;
+  }
+  if (!failed) {
+    const bool ok = mbar_wait(fbar, 0);
+    failed = __syncthreads_or(!ok) != 0;
+  }
+  if (failed) {
+    // give up: flag it, let the copies still in flight land (bounded), leave
+    if (tid == 0) {
+      atomicExch(err, 1);
+      for (int kk = k; kk < issued; kk++) mbar_wait(&bars[kk % nstage], (unsigned)(kk / nstage) & 1u);
+      if (fIssued) mbar_wait(fbar, 0);
+    }
+    __syncthreads();
+    return;
+  }
+  // one thread per column: block-tridiagonal forward and backward substitution
+  for (int q = tid; q < c1 - c0; q += blockDim.x) {
+    const int cp0 = colPos[c0 + q], len = colPos[c0 + q + 1] - cp0;
+    float* rr = sr + 3 * (size_t)(cp0 - P0);
+    const float* Fc = sF + 18 * (size_t)(cp0 - Q0);
+    float p0v = 0, p1v = 0, p2v = 0;
+    for (int l = 0; l < len; l++) {
+      const float* f = Fc + 18 * l;
+      float b0 = rr[3 * l], b1 = rr[3 * l + 1], b2 = rr[3 * l + 2];
+      if (l > 0) {
+        b0 -= f[9] * p0v + f[10] * p1v + f[11] * p2v;
+        b1 -= f[12] * p0v + f[13] * p1v + f[14] * p2v;
+        b2 -= f[15] * p0v + f[16] * p1v + f[17] * p2v;
+      }
+      const float y0 = b0 * f[1];
+      const float y1 = (b1 - f[3] * y0) * f[2];
+      const float y2 = (b2 - f[6] * y0 - f[7] * y1) * f[5];
+      rr[3 * l] = y0; rr[3 * l + 1] = y1; rr[3 * l + 2] = y2;
+      p0v = y0; p1v = y1; p2v = y2;
+    }
+    float q0 = 0, q1 = 0, q2 = 0;
+    for (int l = len - 1; l >= 0; l--) {
+      const float* f = Fc + 18 * l;
+      float b0 = rr[3 * l], b1 = rr[3 * l + 1], b2 = rr[3 * l + 2];
+      if (l + 1 < len) {
+        const float* g = Fc + 18 * (l + 1);
+        b0 -= g[9] * q0 + g[12] * q1 + g[15] * q2;
+        b1 -= g[10] * q0 + g[13] * q1 + g[16] * q2;
+        b2 -= g[11] * q0 + g[14] * q1 + g[17] * q2;
+      }
+      const float z2 = b2 * f[5];
+      const float z1 = (b1 - f[7] * z2) * f[2];
+      const float z0 = (b0 - f[3] * z1 - f[6] * z2) * f[1];
+      rr[3 * l] = z0; rr[3 * l + 1] = z1; rr[3 * l + 2] = z2;
+      q0 = z0; q1 = z1; q2 = z2;
+    }
+  }
+  __syncthreads();
+  for (int l = tid; l < P1 - P0; l += blockDim.x) {
+    const size_t n = posNode[P0 + l];
+    x[3 * n] += sr[3 * l]; x[3 * n + 1] += sr[3 * l + 1]; x[3 * n + 2] += sr[3 * l + 2];
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                  const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    TM_CUDA_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) fail(TM_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D map over a slot-major array of `rows` rows of nnp 4-byte entries, box of TS_CHUNK
+// positions x all rows
+void encode_rows(CUtensorMap* map, CUtensorMapDataType type, const void* base, int nnp, int rows) {
+  const cuuint64_t dims[2] = {(cuuint64_t)nnp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)nnp * 4};
+  const cuuint32_t box[2] = {(cuuint32_t)TS_CHUNK, (cuuint32_t)rows};
+  const cuuint32_t elem[2] = {1, 1};
+  const CUresult r = encode_fn()(map, type, 2, const_cast<void*>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(TM_CUDA, "cuTensorMapEncodeTiled failed");
+}
+
+}  // namespace
+
+// shared memory of the sweep for the longest run; 0 when even two stages do not fit
+size_t sweep_tma_smem(int maxNodes, int nstage) {
+  if ((size_t)(maxNodes + 8) * 18 * 4 > (size_t)nstage * TS_STAGE_BYTES) return ~(size_t)0;   // the factors reuse the stages
+  return 128 + (size_t)nstage * TS_STAGE_BYTES + (size_t)maxNodes * 3 * 4 + (size_t)TS_THREADS * 3 * 4;
+}
+
+// runs of whole columns per colour, one per SM, with about equal node counts; the number of
+// chunk stages that fits beside the longest run's factors and rows (0: the sweep is not used)
+void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st) {
+  int sms = 0, smemMax = 0;
+  TM_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.dev));
+  TM_CUDA_CHECK(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.dev));
+  c.tsParts = std::max(1, sms);
+  c.tsMaxNodes = 0;
+  std::vector<int> parts[4];
+  for (int k = 0; k < 4; k++) {
+    const std::vector<int>& cp = colPos[k];
+    const int ncols = (int)cp.size() - 1;
+    const long long total = ncols > 0 ? cp[ncols] - cp[0] : 0;
+    std::vector<int>& part = parts[k];
+    part.assign(c.tsParts + 1, 0);
+    int q = 0;
+    for (int p = 0; p < c.tsParts; p++) {
+      part[p] = q;
+      const long long target = total * (p + 1) / c.tsParts;
+      while (q < ncols && cp[q + 1] - cp[0] <= target) q++;
+    }
+    part[c.tsParts] = std::max(ncols, 0);
+    for (int p = 0; p < c.tsParts; p++) c.tsMaxNodes = std::max(c.tsMaxNodes, cp[part[p + 1]] - cp[part[p]]);
+    c.d_tsPart[k].upload(part, st);
+  }
+  const size_t staticSmem = sizeof(uint64_t) * (TS_MAXSTAGE + 1);
+  c.tsStages = 0;
+  for (int ns = 3; ns >= 2 && !c.tsStages; ns--)
+    if (sweep_tma_smem(c.tsMaxNodes, ns) + staticSmem <= (size_t)smemMax) c.tsStages = ns;
+  c.tsReady = TM_SWEEP_TMA && c.tsStages > 0;
+}
+
+bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float* x) {
+  if (!c.tsReady) return false;
+  if (c.tsValPtr != c.d_val32.p || c.tsNbrPtr != c.d_nbr.p) {
+    static_assert(sizeof(CUtensorMap) <= sizeof(c.tsMapVal), "tensor map storage");
+    encode_rows(reinterpret_cast<CUtensorMap*>(c.tsMapVal), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, c.d_val32.p, c.nnp, TS_ROWS);
+    encode_rows(reinterpret_cast<CUtensorMap*>(c.tsMapNbr), CU_TENSOR_MAP_DATA_TYPE_INT32, c.d_nbr.p, c.nnp, NSLOT);
+    c.tsValPtr = c.d_val32.p;
+    c.tsNbrPtr = c.d_nbr.p;
+  }
+  const size_t smem = sweep_tma_smem(c.tsMaxNodes, c.tsStages);
+  TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const CUtensorMap* mv = reinterpret_cast<const CUtensorMap*>(c.tsMapVal);
+  const CUtensorMap* mn = reinterpret_cast<const CUtensorMap*>(c.tsMapNbr);
+  k_sweep_tma<<<c.tsParts, TS_THREADS, smem, c.stream>>>(*mv, *mn, c.d_tsPart[col].p, c.d_colPos[col].p, c.d_posNode.p, c.d_F32.p, b, x,
+                                                          c.tsMaxNodes, c.tsStages, zeroGuess, c.d_err.p);
+  note_launch();
+  return true;
+}
+
+}  // namespace tmg
