@@ -7,9 +7,10 @@
 //    shared memory in chunks of 64 positions, each chunk one pair of 2-D TMA tensor loads
 //    (cp.async.bulk.tensor, no multicast) completing on an mbarrier, in a ring of stages so that
 //    the loads of later chunks are in flight while a chunk's residual rows are computed;
-//  * r starts as the run's b in shared memory; 8 threads per position take the 27 slots (a warp
-//    takes 32 consecutive positions of one slot group), their partial rows are added in a fixed
-//    order and subtracted from r;
+//  * r starts as the run's b in shared memory; two warp groups take alternate chunks (one
+//    group's gathers of x overlap the other's); in a group 4 threads per position take the 27
+//    slots (a warp takes 32 consecutive positions of one slot group, conflict-free), their
+//    partial rows are added in a fixed order and subtracted from r;
 //  * the run's column factors then arrive with one bulk copy into the freed stage memory;
 //  * one thread per column then runs the block-tridiagonal forward/backward substitution and
 //    the run's x is updated.
@@ -31,10 +32,12 @@ namespace {
 
 constexpr int TS_THREADS = 512;
 constexpr int TS_CHUNK = 64;                                       // positions per chunk (one TMA box)
-constexpr int TS_TPP = TS_THREADS / TS_CHUNK;                      // threads per position
+constexpr int TS_GROUPS = 2;                                       // warp groups, alternate chunks
+constexpr int TS_GTHREADS = TS_THREADS / TS_GROUPS;
+constexpr int TS_TPP = TS_GTHREADS / TS_CHUNK;                     // threads per position in a group
 constexpr int TS_ROWS = NSLOT * 9;                                 // operator rows
 constexpr int TS_STAGE_BYTES = (TS_ROWS + NSLOT) * TS_CHUNK * 4;   // values, then neighbour ids
-constexpr int TS_MAXSTAGE = 4;
+constexpr int TS_MAXSTAGE = 8;
 constexpr long long TS_WAIT_LIMIT = 1LL << 22;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -72,6 +75,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   return false;
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// barrier of one warp group (named barrier 1 + group), and the same with an OR of a flag over
+// the group (the same result in every thread of the group)
+__device__ __forceinline__ void group_sync(int g) { asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(TS_GTHREADS) : "memory"); }
+__device__ __forceinline__ bool group_sync_or(int g, bool v) {
+  unsigned r;
+  asm volatile(
+      "{\n"
+      " .reg .pred p, q;\n"
+      " setp.ne.u32 p, %1, 0;\n"
+      " bar.red.or.pred q, %2, %3, p;\n"
+      " selp.u32 %0, 1, 0, q;\n"
+      "}\n"
+      : "=r"(r)
+      : "r"((unsigned)v), "r"(1 + g), "r"(TS_GTHREADS)
+      : "memory");
+  return r != 0;
+}
 
 // L2 policies: the streamed operator rows are read once per sweep (evict first), the gathered
 // x is read by every sweep (evict last)
@@ -131,30 +151,39 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     mbar_fence_init();
   }
   __syncthreads();
-  int issued = 0;   // chunks issued (thread 0)
   const uint64_t polStream = policy_evict_first(), polKeep = policy_evict_last();
+  __shared__ int s_fail;
+  __shared__ int s_last[TS_MAXSTAGE];   // last chunk issued into each stage
   auto issue = [&](int k) {
     float* dst = reinterpret_cast<float*>(smt + (size_t)(k % nstage) * TS_STAGE_BYTES);
     mbar_expect_tx(&bars[k % nstage], TS_STAGE_BYTES);
     tma_load_2d(dst, &tmVal, Q0 + k * TS_CHUNK, 0, &bars[k % nstage], polStream);
     tma_load_2d(dst + TS_ROWS * TS_CHUNK, &tmNbr, Q0 + k * TS_CHUNK, 0, &bars[k % nstage], polStream);
+    s_last[k % nstage] = k;
   };
-  if (tid == 0)
-    for (; issued < nstage && issued < nchunks; issued++) issue(issued);
+  if (tid == 0) {
+    s_fail = 0;
+    for (int q = 0; q < TS_MAXSTAGE; q++) s_last[q] = -1;
+    for (int q = 0; q < nstage && q < nchunks; q++) issue(q);
+  }
   // r starts as b (the chunks subtract K x)
   for (int l = tid; l < P1 - P0; l += blockDim.x) {
     const size_t n = posNode[P0 + l];
     sr[3 * l] = b[3 * n]; sr[3 * l + 1] = b[3 * n + 1]; sr[3 * l + 2] = b[3 * n + 2];
   }
-  bool failed = false;
-  int k = 0;
-  // a warp takes 32 consecutive positions of one slot group: conflict-free shared-memory rows
-  const int pl = tid % TS_CHUNK, sub = tid / TS_CHUNK;
-  __shared__ int s_fail;
-  if (tid == 0) s_fail = 0;
   __syncthreads();
-  for (; k < nchunks; k++) {
-    const bool ok = mbar_wait(&bars[k % nstage], (unsigned)(k / nstage) & 1u);
+  // two warp groups take alternate chunks, so that one group's gathers of x overlap the other's;
+  // a warp takes 32 consecutive positions of one slot group: conflict-free shared-memory rows
+  const int grp = tid / TS_GTHREADS, gtid = tid % TS_GTHREADS;
+  const int pl = gtid % TS_CHUNK, sub = gtid / TS_CHUNK;
+  float* gred = red + (size_t)grp * TS_TPP * TS_CHUNK * 3;
+  for (int k = grp; k < nchunks; k += TS_GROUPS) {
+    // the chunk's loads must have been issued before its stage is waited on: the previous chunk
+    // of the stage belongs to the other group, and a wait one phase early would see that phase
+    bool ok = false;
+    for (long long it = 0; it < TS_WAIT_LIMIT; it++)
+      if (*(volatile int*)&s_last[k % nstage] == k) { ok = true; break; }
+    if (ok) ok = mbar_wait(&bars[k % nstage], (unsigned)(k / nstage) & 1u);
     if (!ok) s_fail = 1;
     const float* sv = reinterpret_cast<const float*>(smt + (size_t)(k % nstage) * TS_STAGE_BYTES);
     const int* sn = reinterpret_cast<const int*>(sv + TS_ROWS * TS_CHUNK);
@@ -176,27 +205,32 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
         }
       }
     }
-    float* rd = red + 3 * (size_t)(sub * TS_CHUNK + pl);
+    float* rd = gred + 3 * (size_t)(sub * TS_CHUNK + pl);
     rd[0] = a0; rd[1] = a1; rd[2] = a2;
-    __syncthreads();   // the stage is read: refill it while the partial rows are added
-    if (s_fail) { failed = true; break; }
-    if (tid == 0 && issued < nchunks) {
+    // the stage is read: refill it while the partial rows are added (every thread of the group
+    // takes the same branch)
+    if (group_sync_or(grp, !ok || *(volatile int*)&s_fail != 0)) {
+      s_fail = 1;
+      break;
+    }
+    if (gtid == 0 && k + nstage < nchunks) {
       fence_proxy_async();   // the stage being refilled was last read by the threads
-      issue(issued);
-      issued++;
+      issue(k + nstage);
     }
     // the slot groups' partial rows of a position, added in group order
-    if (tid < 3 * TS_CHUNK) {
-      const int pq = tid / 3, q = tid % 3, pp = Q0 + k * TS_CHUNK + pq;
+    if (gtid < 3 * TS_CHUNK) {
+      const int pq = gtid / 3, q = gtid % 3, pp = Q0 + k * TS_CHUNK + pq;
       if (pp >= P0 && pp < P1) {
-        float acc = red[3 * pq + q];
+        float acc = gred[3 * pq + q];
 #pragma unroll
-        for (int g = 1; g < TS_TPP; g++) acc += red[3 * (g * TS_CHUNK + pq) + q];
+        for (int g = 1; g < TS_TPP; g++) acc += gred[3 * (g * TS_CHUNK + pq) + q];
         sr[3 * (pp - P0) + q] -= acc;
       }
     }
-    __syncthreads();
+    group_sync(grp);
   }
+  __syncthreads();
+  bool failed = s_fail != 0;
   bool fIssued = false;   // thread 0
   if (!failed && tid == 0) {
     // the factors into the (now free) stage memory
@@ -214,7 +248,8 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     // give up: flag it, let the copies still in flight land (bounded), leave
     if (tid == 0) {
       atomicExch(err, 1);
-      for (int kk = k; kk < issued; kk++) mbar_wait(&bars[kk % nstage], (unsigned)(kk / nstage) & 1u);
+      for (int q = 0; q < nstage; q++)
+        if (s_last[q] >= 0) mbar_wait(&bars[q], (unsigned)(s_last[q] / nstage) & 1u);
       if (fIssued) mbar_wait(fbar, 0);
     }
     __syncthreads();
@@ -325,7 +360,7 @@ void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st)
     for (int p = 0; p < c.tsParts; p++) c.tsMaxNodes = std::max(c.tsMaxNodes, cp[part[p + 1]] - cp[part[p]]);
     c.d_tsPart[k].upload(part, st);
   }
-  const size_t staticSmem = sizeof(uint64_t) * (TS_MAXSTAGE + 1);
+  const size_t staticSmem = 256;   // the kernel's barriers and flags
   c.tsStages = 0;
   for (int ns = 3; ns >= 2 && !c.tsStages; ns--)
     if (sweep_tma_smem(c.tsMaxNodes, ns) + staticSmem <= (size_t)smemMax) c.tsStages = ns;
