@@ -533,6 +533,7 @@ void build_hierarchy(Context& c) {
   c.panelCap = std::max(TM_PANEL_THREADS, c.maxColLen);
   c.panelMaxCols = 0;
   std::vector<int> colPos[4];
+  c.colourPos[0] = 0;
   for (int k = 0; k < 4; k++) {
     std::vector<int> cols;
     for (int col = 0; col < nx * ny; col++) {
@@ -560,7 +561,9 @@ void build_hierarchy(Context& c) {
     }
     c.d_colPos[k].upload(cp, st);
     colPos[k] = cp;
+    c.colourPos[k + 1] = c.colourPos[k] + (cp.empty() ? 0 : cp.back() - cp.front());
   }
+  if (c.colourPos[4] != nn) fail(TM_BAD_INPUT, "colours do not cover the positions");
   plan_sweep_tma(c, colPos, st);
   c.d_nodeAgg.upload(c.nodeAgg, st);
   c.d_aggStart.upload(c.aggStart, st);

@@ -216,6 +216,7 @@ struct Context {
   // the position of the first node of every colour column plus one past the colour's last node
   int panelCap = TM_PANEL_THREADS, panelMaxCols = 0;
   DBuf<int> d_grpStart[4], d_colPos[4];
+  int colourPos[5] = {0, 0, 0, 0, 0};  // colour k occupies positions colourPos[k] .. colourPos[k+1]-1
   int grpCount[4] = {0, 0, 0, 0};
   std::vector<int> nodeAgg, aggStart;  // level 0 -> 1
   std::vector<double> zp;              // z of node minus zref of its aggregate

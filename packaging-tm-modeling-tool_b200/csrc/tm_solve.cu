@@ -278,9 +278,12 @@ __global__ void __launch_bounds__(TM_PANEL_THREADS, PanelMinBlocks<T>::value)
 
 // restriction 0 -> 1: rc = P^T res, thread per aggregate (children are a contiguous node range)
 template <class T>
-__global__ void k_restrict0(int na, const int* __restrict__ aggStart, const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc) {
+__global__ void k_restrict0(int na, const int* __restrict__ aggStart, const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc,
+                            T* __restrict__ xc) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= na) return;
+#pragma unroll
+  for (int a = 0; a < 6; a++) xc[6 * (size_t)I + a] = 0;   // the level's iterate starts at zero
   T acc[6] = {0, 0, 0, 0, 0, 0};
   for (int f = aggStart[I]; f < aggStart[I + 1]; f++) {
     const T* w = W + 18 * (size_t)f;
@@ -444,9 +447,10 @@ __global__ void __launch_bounds__(128) k_sweep_shell(int ncolc, const int4* __re
 // shell restriction: rc = P^T res (children lists, transposeProl order)
 template <class T>
 __global__ void k_restrict_shell(int nnc, const int* __restrict__ chPtr, const int* __restrict__ chIdx, const int* __restrict__ chW,
-                                 const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc) {
+                                 const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc, T* __restrict__ xc) {
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= 6 * (size_t)nnc) return;
+  xc[t] = 0;   // the coarse level's iterate starts at zero
   const int I = (int)(t / 6), a = (int)(t % 6);
   T acc = 0;
   for (int q = chPtr[I]; q < chPtr[I + 1]; q++) {
@@ -543,11 +547,11 @@ template <class T, class V>
 void apply0_range(Context& c, const T* val, int p0, int p1, const V* x, V* y, const V* b) {
   if (p1 <= p0) return;
   if constexpr (sizeof(T) == 4)
-    k_apply0<T, V, TM_APPLY32_NPT><<<grid_for(apply_threads<TM_APPLY32_NPT>(p0, p1), 128), 128, 0, c.stream>>>(
-        p0, p1, c.nnp, c.nn, c.d_posNode.p, c.d_nbr.p, val, x, y, b);
+    k_apply0<T, V, TM_APPLY32_NPT><<<grid_for(apply_threads<TM_APPLY32_NPT>(p0, p1), 128), 128, 0, c.stream>>>(p0, p1, c.nnp, c.nn,
+        c.d_posNode.p, c.d_nbr.p, val, x, y, b);
   else
-    k_apply0<T, V, 1><<<grid_for(apply_threads<1>(p0, p1), 128), 128, 0, c.stream>>>(p0, p1, c.nnp, c.nn, c.d_posNode.p, c.d_nbr.p,
-                                                                                     val, x, y, b);
+    k_apply0<T, V, 1><<<grid_for(apply_threads<1>(p0, p1), 128), 128, 0, c.stream>>>(p0, p1, c.nnp, c.nn, c.d_posNode.p, c.d_nbr.p, val, x,
+        y, b);
   note_launch();
 }
 
@@ -558,7 +562,8 @@ void vcycle(Context& c, const T* r, T* z) {
   cudaStream_t st = c.stream;
   const int nn = c.nn;
   const size_t smem0 = (size_t)21 * c.panelCap * sizeof(T) + (size_t)(c.panelMaxCols + 1) * sizeof(int);
-  TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(T), st));
+  // the iterate starts at zero (the TMA sweep clears it itself on the first sweep)
+  if (sizeof(T) == 8 || !c.tsReady) TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(T), st));
   if (smem0 > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
   auto sweep0 = [&](int col, int zero) {
     if (!c.grpCount[col]) return;
@@ -566,7 +571,7 @@ void vcycle(Context& c, const T* r, T* z) {
     if constexpr (sizeof(T) == 4)
       if (launch_sweep_tma(c, col, zero, r, z)) return;
     k_sweep_panel<T><<<c.grpCount[col], TM_PANEL_THREADS, smem0, st>>>(c.d_grpStart[col].p, c.d_colPos[col].p, c.d_posNode.p, c.nnp,
-                                                                      c.d_nbr.p, B::val0(c), B::F(c), r, z, c.panelCap, zero);
+        c.d_nbr.p, B::val0(c), B::F(c), r, z, c.panelCap, zero);
     note_launch();
   };
   const int wpb = 4;
@@ -579,9 +584,8 @@ void vcycle(Context& c, const T* r, T* z) {
   auto sweepS = [&](ShellLevel& L, int col, int zero) {
     const size_t per = shell_stage_bytes<T>(L.maxm, L.maxColBlocks);
     TimedLaunch tl(c, K_SWEEP_SHELL);
-    k_sweep_shell<T><<<grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st>>>(
-        L.colorCount[col], L.d_colorMeta[col].p, L.d_colorCf[col].p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::cf(L), B::b(L), B::x(L),
-        L.maxm, L.maxColBlocks, zero);
+    k_sweep_shell<T><<<grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st>>>(L.colorCount[col], L.d_colorMeta[col].p,
+        (const long long*)L.d_colorCf[col].p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::cf(L), B::b(L), B::x(L), L.maxm, L.maxColBlocks, zero);
     note_launch();
   };
   // ---- level 0 pre-smoothing: 2 sweeps in colours 0..3
@@ -597,7 +601,7 @@ void vcycle(Context& c, const T* r, T* z) {
     apply0_range<T, T>(c, B::val0(c), 0, nn, z, B::res0(c), r);
   }
   ShellLevel& L1 = *c.shells[0];
-  k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, B::W01(c), B::res0(c), B::b(L1));
+  k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, B::W01(c), B::res0(c), B::b(L1), B::x(L1));
   note_launch();
   const size_t nl = c.shells.size();
   for (size_t l = 0; l < nl; l++) {
@@ -608,8 +612,7 @@ void vcycle(Context& c, const T* r, T* z) {
       note_launch();
       break;
     }
-    TM_CUDA_CHECK(cudaMemsetAsync(B::x(L), 0, 6 * (size_t)L.nn * sizeof(T), st));
-    bool firstS = true;
+    bool firstS = true;   // the level's iterate was cleared by the restriction that made its b
     for (int sw = 0; sw < 2; sw++)
       for (int col = 0; col < 4; col++) {
         if (!L.colorCount[col]) continue;
@@ -619,12 +622,13 @@ void vcycle(Context& c, const T* r, T* z) {
     {
       TimedLaunch tl(c, K_APPLY_SHELL);
       const int ncol = L.nx * L.ny;
-      k_apply_shell<T><<<grid_for(ncol, wpb), 32 * wpb, wpb * shell_stage_bytes<T>(L.maxm, L.maxColBlocks), st>>>(
-          ncol, L.d_colMeta.p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L), L.maxm, L.maxColBlocks);
+      k_apply_shell<T><<<grid_for(ncol, wpb), 32 * wpb, wpb * shell_stage_bytes<T>(L.maxm, L.maxColBlocks), st>>>(ncol, L.d_colMeta.p,
+          L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L), L.maxm, L.maxColBlocks);
       note_launch();
     }
     ShellLevel& C = *c.shells[l + 1];
-    k_restrict_shell<T><<<grid_for(6 * (size_t)C.nn, 128), 128, 0, st>>>(C.nn, L.d_chPtr.p, L.d_chIdx.p, L.d_chW.p, B::prolW(L), B::res(L), B::b(C));
+    k_restrict_shell<T><<<grid_for(6 * (size_t)C.nn, 128), 128, 0, st>>>(C.nn, L.d_chPtr.p, L.d_chIdx.p, L.d_chW.p, B::prolW(L), B::res(L),
+        B::b(C), B::x(C));
     note_launch();
   }
   for (int l = (int)nl - 2; l >= 0; l--) {

@@ -13,7 +13,8 @@
 //    partial rows are added in a fixed order and subtracted from r;
 //  * the run's column factors then arrive with one bulk copy into the freed stage memory;
 //  * one thread per column then runs the block-tridiagonal forward/backward substitution and
-//    the run's x is updated.
+//    the run's x is updated (on the cycle's first sweep, x is assigned and the other colours'
+//    nodes are cleared).
 //
 // Columns of one colour do not couple, so runs never read each other's updates. Every wait on
 // an mbarrier is bounded: a wait that runs out sets the error flag, waits (bounded) for the
@@ -129,12 +130,21 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 __global__ void __launch_bounds__(TS_THREADS, 1)
     k_sweep_tma(const __grid_constant__ CUtensorMap tmVal, const __grid_constant__ CUtensorMap tmNbr, const int* __restrict__ partCol,
                 const int* __restrict__ colPos, const int* __restrict__ posNode, const float* __restrict__ F, const float* __restrict__ b,
-                float* __restrict__ x, int maxNodes, int nstage, int zeroGuess, int* __restrict__ err) {
+                float* __restrict__ x, int maxNodes, int nstage, int zeroGuess, int nn, int zlo, int zhi, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smraw_t[];
   __shared__ __align__(8) uint64_t bars[TS_MAXSTAGE + 1];   // chunk stages, then the factors
   // 128-byte aligned start of the stages (the launch adds 128 bytes for this)
   unsigned char* smt = smraw_t + ((128u - (smem_u32(smraw_t) & 127u)) & 127u);
   const int tid = threadIdx.x;
+  if (zeroGuess) {
+    // the cycle's iterate starts at zero: the nodes of the other colours are cleared here, this
+    // colour's are assigned at the end
+    const int nOther = nn - (zhi - zlo);
+    for (int t = blockIdx.x * blockDim.x + tid; t < nOther; t += gridDim.x * blockDim.x) {
+      const size_t n = posNode[t < zlo ? t : t + (zhi - zlo)];
+      x[3 * n] = 0; x[3 * n + 1] = 0; x[3 * n + 2] = 0;
+    }
+  }
   const int c0 = partCol[blockIdx.x], c1 = partCol[blockIdx.x + 1];
   if (c0 >= c1) return;
   const int P0 = colPos[c0], P1 = colPos[c1];
@@ -295,7 +305,11 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
   __syncthreads();
   for (int l = tid; l < P1 - P0; l += blockDim.x) {
     const size_t n = posNode[P0 + l];
-    x[3 * n] += sr[3 * l]; x[3 * n + 1] += sr[3 * l + 1]; x[3 * n + 2] += sr[3 * l + 2];
+    if (zeroGuess) {
+      x[3 * n] = sr[3 * l]; x[3 * n + 1] = sr[3 * l + 1]; x[3 * n + 2] = sr[3 * l + 2];
+    } else {
+      x[3 * n] += sr[3 * l]; x[3 * n + 1] += sr[3 * l + 1]; x[3 * n + 2] += sr[3 * l + 2];
+    }
   }
 }
 
@@ -381,7 +395,7 @@ bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float*
   const CUtensorMap* mv = reinterpret_cast<const CUtensorMap*>(c.tsMapVal);
   const CUtensorMap* mn = reinterpret_cast<const CUtensorMap*>(c.tsMapNbr);
   k_sweep_tma<<<c.tsParts, TS_THREADS, smem, c.stream>>>(*mv, *mn, c.d_tsPart[col].p, c.d_colPos[col].p, c.d_posNode.p, c.d_F32.p, b, x,
-                                                          c.tsMaxNodes, c.tsStages, zeroGuess, c.d_err.p);
+      c.tsMaxNodes, c.tsStages, zeroGuess, c.nn, c.colourPos[col], c.colourPos[col + 1], c.d_err.p);
   note_launch();
   return true;
 }
