@@ -291,7 +291,10 @@ def run_ours(a):
     hbm, hbm_kind = peaks()
     achieved = per_launch / (kms / kcount / 1e3) / 1e9 if kcount else None
     traffic = profile_traffic(DOMINANT, a.precision)
-    roof = {"kernel": "k_sweep_panel (level-0 z-column block-tridiagonal smoother on packed column panels, one colour)", "bound": "hbm", "achieved": achieved,
+    kname = ("k_sweep_tma (level-0 z-column smoother, one colour: operator rows streamed by TMA through shared memory, "
+             "block-tridiagonal column solves per SM run)") if a.precision == "mixed" else \
+        "k_sweep_panel<double> (level-0 z-column block-tridiagonal smoother on packed column panels, one colour)"
+    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved,
             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None, "traffic": traffic,
             "peak_kind": hbm_kind, "launches_timed": kcount, "avg_launch_us": 1e3 * kms / kcount if kcount else None,
             "algorithmic_bytes_per_launch": per_launch}
@@ -316,7 +319,8 @@ def run_ours(a):
 
 def profile_traffic(kernel, precision):
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", f"k_sweep_panel_{precision}.md")
+    name = "k_sweep_tma" if precision == "mixed" else "k_sweep_panel"
+    path = os.path.join(ROOT, "profiles", f"{name}_{precision}.md")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch:"):
