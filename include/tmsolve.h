@@ -18,6 +18,15 @@
  *   tm_anand_screen    screenJoints' per-site Anand loop  src/core/13-fatigue.js:395-451
  *                      (AnandPoint.stepColumn / step, :13-166)
  *   tm_anand_step      AnandPoint.step + commit           src/core/13-fatigue.js:67-143, 229-232
+ *   tm_prepare_step    FEModel.stepRecovery(Ta, Tb, stage): the step's shape matrices and element
+ *                      thermal loads without an assembly (src/core/09-assembly.js:480-491)
+ *   tm_accumulate_q    Model.accumulateStep(e, rec, du, state, qOnly = true) over a list of
+ *                      elements (src/core/09-assembly.js:508-533, with stepRecovery :480-491),
+ *                      the march of Analysis.qAlong (src/core/11-analysis.js:298-316)
+ *   tm_element_strains boxStrainAt at natural points (src/core/07-element.js:127-142), the
+ *                      inner loop of siteStrainTable (src/core/13-fatigue.js:318-346)
+ *   tm_sample_plane    samplePlane(mesh, u, k, comp, x, y) at many points
+ *                      (src/core/12-post.js:30-38), the sampler of warpageJEITA (:60-109)
  *
  * Conventions
  *   - Node, element and DOF numbering are the mesher's, taken verbatim
@@ -165,6 +174,38 @@ int32_t tm_last_error(char* buf, size_t len);
 tm_status tm_assemble_step_device(tm_ctx* ctx, const tm_step* step, double* rhs_dev);
 tm_status tm_solve_device(tm_ctx* ctx, const double* f_dev, double* u_dev, const tm_solve_opts* opts, tm_solve_info* info);
 tm_status tm_matvec_device(tm_ctx* ctx, const double* x_dev, double* y_dev);
+
+/* ---- element DOF histories at screening sites ---- */
+/* Loads the per-step data that the DOF histories read (the shape matrices of every property set
+ * and the element thermal loads) for step st without assembling the operator; tm_assemble_step
+ * loads them too. */
+tm_status tm_prepare_step(tm_ctx* ctx, const tm_step* st);
+/* Adds to q (nel x 33: the 24 nodal DOFs then the 9 incompatible-mode amplitudes of every
+ * listed element) the increment of the step loaded last (tm_prepare_step, tm_assemble_step), from that
+ * step's displacement increment du (3*nn doubles): du at the element's nodes and
+ * dalpha = K_aa^-1 (f_a - K_au du) (Model.accumulateStep with qOnly). The reference keeps du
+ * of every step as Float32Array (src/core/11-analysis.js:256); the caller passes the values it
+ * keeps. An element index < 0 (no element at that site) writes NaN into its row of q; an index
+ * >= ne is TM_BAD_INPUT. Host pointers. */
+tm_status tm_accumulate_q(tm_ctx* ctx, const double* du, int32_t nel, const int32_t* elems, double* q);
+/* Engineering strain (6 per point, boxStrainAt order xx yy zz xy yz zx) of element elem[p] with
+ * the element DOFs q[33 p ..] at the natural point nat[3 p ..] (each in [-1, 1], naturalCoords
+ * of src/core/12-post.js:4-11). An element index < 0 gives NaN strains. Host pointers. */
+tm_status tm_element_strains(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* q, const double* nat, double* eps);
+/* The same with every array in device memory (element indices >= ne also give NaN rows). */
+tm_status tm_accumulate_q_device(tm_ctx* ctx, const double* du_dev, int32_t nel, const int32_t* elems_dev, double* q_dev);
+tm_status tm_element_strains_device(tm_ctx* ctx, int32_t npts, const int32_t* elem_dev, const double* q_dev,
+                                    const double* nat_dev, double* eps_dev);
+
+/* ---- field sampling ---- */
+/* samplePlane: bilinear interpolation of component comp (0..2) of the nodal field u (3*nn
+ * doubles) on mesh plane k at the points (x[p], y[p]); NaN where one of the four corner nodes
+ * does not exist. Host pointers. */
+tm_status tm_sample_plane(tm_ctx* ctx, const double* u, int32_t k, int32_t comp, int32_t npts, const double* x,
+                          const double* y, double* out);
+/* The same with u, x, y and out in device memory. */
+tm_status tm_sample_plane_device(tm_ctx* ctx, const double* u_dev, int32_t k, int32_t comp, int32_t npts,
+                                 const double* x_dev, const double* y_dev, double* out_dev);
 
 /* Runs the context's work on the caller's CUDA stream (a cudaStream_t) instead of its own
  * (the N-API addon passes the stream of the thread's device context). */

@@ -61,6 +61,12 @@ def lib():
     L.orc_anand_uniaxial.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int]
     L.orc_anand_screen.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _ip, _ip, C.c_int,
                                    _dp, _dp, _dp]
+    L.orc_accumulate_q.argtypes = [vp, _dp, C.c_int, _ip, _dp]
+    L.orc_element_strains.argtypes = [vp, C.c_int, _ip, _dp, _dp, _dp]
+    L.orc_fit_plane.argtypes = [C.c_int, _dp, _dp, _dp, _dp]
+    L.orc_sample_plane.restype = C.c_double
+    L.orc_sample_plane.argtypes = [vp, _dp, C.c_int, C.c_int, C.c_double, C.c_double]
+    L.orc_warpage_jeita.argtypes = [vp, _dp, C.c_int, _dp, _dp, _dp, _dp]
     L.orc_last_error.restype = C.c_char_p
     L.orc_last_error.argtypes = [vp]
     _lib = L
@@ -156,6 +162,40 @@ class OracleModel:
         out = np.zeros(self.nn, np.int32)
         lib().orc_mg_node_agg(self.h, out)
         return out
+
+    def accumulate_q(self, du, elems, q):
+        """Model.accumulateStep with qOnly (09-assembly.js:508-533) of the last assembled step:
+        q (nel x 33, updated in place) += the DOF increment of every element of elems."""
+        elems = np.ascontiguousarray(elems, np.int32)
+        assert q.dtype == np.float64 and q.flags.c_contiguous and q.size == 33 * len(elems)
+        lib().orc_accumulate_q(self.h, np.ascontiguousarray(du, np.float64), len(elems), elems, q)
+        return q
+
+    def element_strains(self, elem, q, nat):
+        """boxStrainAt (07-element.js:127-142) of element elem[t] with DOFs q[t] at nat[t]."""
+        elem = np.ascontiguousarray(elem, np.int32)
+        eps = np.zeros(6 * len(elem))
+        lib().orc_element_strains(self.h, len(elem), elem, np.ascontiguousarray(q, np.float64).reshape(-1),
+                                  np.ascontiguousarray(nat, np.float64).reshape(-1), eps)
+        return eps.reshape(-1, 6)
+
+    def sample_plane(self, u, k, comp, x, y):
+        return lib().orc_sample_plane(self.h, np.ascontiguousarray(u, np.float64), int(k), int(comp), float(x), float(y))
+
+    def warpage_jeita(self, u, bx, by, zone):
+        """warpageJEITA (12-post.js:60-109): dict of signed, mag, sign, signConf, plane, rmin, rmax."""
+        out = np.zeros(9)
+        bx = np.ascontiguousarray(bx, np.float64); by = np.ascontiguousarray(by, np.float64)
+        lib().orc_warpage_jeita(self.h, np.ascontiguousarray(u, np.float64), len(bx), bx, by,
+                                np.ascontiguousarray(zone, np.float64), out)
+        return dict(signed=out[0], mag=out[1], sign=out[2], signConf=out[3], plane=out[4:7].copy(), rmin=out[7], rmax=out[8])
+
+
+def fit_plane(x, y, w):
+    c = np.zeros(3)
+    lib().orc_fit_plane(len(w), np.ascontiguousarray(x, np.float64), np.ascontiguousarray(y, np.float64),
+                        np.ascontiguousarray(w, np.float64), c)
+    return c
 
 
 def anand_uniaxial(params, Etab, T, rate, eps_max, nsteps):

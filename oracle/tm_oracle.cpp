@@ -20,6 +20,7 @@
 //   dense algebra   src/core/01-util.js:70-142, 176-190
 //   assembly        src/core/08-sparse.js:7-43, src/core/09-assembly.js:23-165, 318-332, 392-464
 //   solver          src/core/10-solver.js:1-1043
+//   recovery, post  src/core/09-assembly.js:480-533, 07-element.js:127-142, 12-post.js:30-109
 //   Anand           src/core/13-fatigue.js:13-293, 379-455
 #include <cmath>
 #include <cstdint>
@@ -1685,6 +1686,159 @@ struct AnandPoint {
 // =====================================================================================
 extern "C" {
 
+// ---- stress-history recovery and post-processing readers -------------------------------------
+
+// findInterval (01-util.js:12-22)
+int findIntervalD(const dvec& a, double x) {
+  const int n = (int)a.size();
+  if (x <= a[0]) return 0;
+  if (x >= a[n - 1]) return n - 2;
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// boxStrainAt (07-element.js:127-142): engineering strain at (xi, eta, zeta) from the 24 nodal
+// DOFs u and the 9 incompatible-mode amplitudes alpha
+void boxStrainAt(double hx, double hy, double hz, const double* u, const double* alpha, double xi, double eta, double zeta, double* eps) {
+  double dx[11], dy[11], dz[11];
+  boxDerivs(hx, hy, hz, xi, eta, zeta, dx, dy, dz);
+  for (int q = 0; q < 6; q++) eps[q] = 0;
+  for (int b = 0; b < 11; b++) {
+    const double ux = b < 8 ? u[3 * b] : alpha[3 * (b - 8)];
+    const double uy = b < 8 ? u[3 * b + 1] : alpha[3 * (b - 8) + 1];
+    const double uz = b < 8 ? u[3 * b + 2] : alpha[3 * (b - 8) + 2];
+    eps[0] += dx[b] * ux; eps[1] += dy[b] * uy; eps[2] += dz[b] * uz;
+    eps[3] += dy[b] * ux + dx[b] * uy;
+    eps[4] += dz[b] * uy + dy[b] * uz;
+    eps[5] += dz[b] * ux + dx[b] * uz;
+  }
+}
+
+// cholSolveDense (01-util.js:94-107)
+void cholSolveDense(const double* L, int n, double* b) {
+  for (int i = 0; i < n; i++) {
+    double s = b[i];
+    const int ri = i * n;
+    for (int k = 0; k < i; k++) s -= L[ri + k] * b[k];
+    b[i] = s / L[ri + i];
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    double s = b[i];
+    for (int k = i + 1; k < n; k++) s -= L[k * n + i] * b[k];
+    b[i] = s / L[i * n + i];
+  }
+}
+
+// Model.accumulateStep with qOnly (09-assembly.js:508-533): adds to q (33) the DOF increment of
+// element e in the step assembled last: du at its nodes, then the incompatible modes
+// K_aa^-1 (f_a - K_au du) from the rows 24..32 of the step's shape matrices (stepRecovery
+// :480-491) and, when the material is born, of the element thermal load
+void accumulateQ(const Model& M, const double* du, int e, double* q) {
+  const Mesh& m = M.mesh;
+  const PropSet& ps = M.psets[M.ePset[e]];
+  const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+  const double hx = m.xs[i + 1] - m.xs[i], hy = m.ys[j + 1] - m.ys[j], hz = m.zs[k + 1] - m.zs[k];
+  const double V8 = hx * hy * hz / 8;
+  const double c[6] = {V8 * 4 / (hx * hx), V8 * 4 / (hy * hy), V8 * 4 / (hz * hz), V8 * 4 / (hx * hy), V8 * 4 / (hy * hz), V8 * 4 / (hz * hx)};
+  double Kr[297], f33[33], dq[33], Kaa[81], col[9];
+  for (int r = 0; r < 297; r++) {
+    const double* Ma = ps.M + 24 * 33 + r;
+    Kr[r] = c[0] * Ma[0] + c[1] * Ma[1089] + c[2] * Ma[2178] + c[3] * Ma[3267] + c[4] * Ma[4356] + c[5] * Ma[5445];
+  }
+  std::fill(f33, f33 + 33, 0.0);
+  if (ps.born) elementFth(hx, hy, hz, ps.layered ? ps.V : nullptr, ps.layered ? nullptr : ps.s0, f33);
+  for (int a = 0; a < 8; a++) {
+    const int n = m.conn[8 * e + a];
+    dq[3 * a] = du[3 * n]; dq[3 * a + 1] = du[3 * n + 1]; dq[3 * a + 2] = du[3 * n + 2];
+  }
+  for (int r = 0; r < 9; r++) for (int t = 0; t < 9; t++) Kaa[r * 9 + t] = Kr[r * 33 + 24 + t];
+  cholDense(Kaa, 9, 1e-14);
+  for (int r = 0; r < 9; r++) {
+    double s = f33[24 + r];
+    for (int t = 0; t < 24; t++) s -= Kr[r * 33 + t] * dq[t];
+    col[r] = s;
+  }
+  cholSolveDense(Kaa, 9, col);
+  for (int r = 0; r < 9; r++) dq[24 + r] = col[r];
+  for (int r = 0; r < 33; r++) q[r] += dq[r];
+}
+
+// boxStrainAt of element e (its dims from the mesh lines, Model.elementDims) with the element
+// DOFs q at the natural point nat (siteStrainTable, 13-fatigue.js:335-342)
+void elementStrain(const Model& M, int e, const double* q, const double* nat, double* eps) {
+  const Mesh& m = M.mesh;
+  const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+  boxStrainAt(m.xs[i + 1] - m.xs[i], m.ys[j + 1] - m.ys[j], m.zs[k + 1] - m.zs[k], q, q + 24, nat[0], nat[1], nat[2], eps);
+}
+
+// samplePlane (12-post.js:30-38) on plane k, component comp; NaN outside existing nodes
+double samplePlane(const Mesh& m, const double* u, int k, int comp, double x, double y) {
+  const int i = findIntervalD(m.xs, x), j = findIntervalD(m.ys, y);
+  const double tx = (x - m.xs[i]) / (m.xs[i + 1] - m.xs[i]), ty = (y - m.ys[j]) / (m.ys[j + 1] - m.ys[j]);
+  auto id = [&](int a, int b) { return m.nodeId[((size_t)(i + a) * m.ny + j + b) * m.nz + k]; };
+  const int n00 = id(0, 0), n10 = id(1, 0), n01 = id(0, 1), n11 = id(1, 1);
+  if (n00 < 0 || n10 < 0 || n01 < 0 || n11 < 0) return std::nan("");
+  return (1 - tx) * (1 - ty) * u[3 * n00 + comp] + tx * (1 - ty) * u[3 * n10 + comp] + (1 - tx) * ty * u[3 * n01 + comp] +
+         tx * ty * u[3 * n11 + comp];
+}
+
+// fitPlane (01-util.js:176-190)
+void fitPlane(int n, const double* xs, const double* ys, const double* ws, double* c) {
+  double sx = 0, sy = 0, sw = 0;
+  for (int i = 0; i < n; i++) { sx += xs[i]; sy += ys[i]; sw += ws[i]; }
+  const double mx = sx / n, my = sy / n, mw = sw / n;
+  double sxx = 0, sxy = 0, syy = 0, sxw = 0, syw = 0;
+  for (int i = 0; i < n; i++) {
+    const double dx = xs[i] - mx, dy = ys[i] - my, dw = ws[i] - mw;
+    sxx += dx * dx; sxy += dx * dy; syy += dy * dy; sxw += dx * dw; syw += dy * dw;
+  }
+  const double det = sxx * syy - sxy * sxy;
+  double c1 = 0, c2 = 0;
+  if (std::fabs(det) > 1e-300) { c1 = (sxw * syy - syw * sxy) / det; c2 = (syw * sxx - sxw * sxy) / det; }
+  c[0] = mw - c1 * mx - c2 * my; c[1] = c1; c[2] = c2;
+}
+
+// warpageJEITA (12-post.js:60-109) without the shape class and the contour grid: signed
+// magnitude, magnitude, sign, sign confidence and the fitted plane; out[7] = rmin, out[8] = rmax
+void warpageJEITA(const Mesh& m, const double* u, int nb, const double* bx, const double* by, const double* zone, double* out) {
+  const int DIAG_SAMPLES = 201;   // CONST.DIAG_SAMPLES (00-constants.js:98)
+  auto sample = [&](double x, double y) { return samplePlane(m, u, 0, 2, x, y); };
+  dvec w(nb), res(nb);
+  for (int q = 0; q < nb; q++) w[q] = sample(bx[q], by[q]);
+  double pl[3];
+  fitPlane(nb, bx, by, w.data(), pl);
+  double rmin = INFINITY, rmax = -INFINITY;
+  for (int q = 0; q < nb; q++) {
+    res[q] = w[q] - (pl[0] + pl[1] * bx[q] + pl[2] * by[q]);
+    // Math.min / Math.max: NaN once any operand is NaN
+    rmin = (std::isnan(res[q]) || std::isnan(rmin)) ? NAN : std::min(rmin, res[q]);
+    rmax = (std::isnan(res[q]) || std::isnan(rmax)) ? NAN : std::max(rmax, res[q]);
+  }
+  const double mag = rmax - rmin;
+  auto diag = [&](double xa, double ya, double xb, double yb, double& mx, double& mn) {
+    const double wa = sample(xa, ya), wb = sample(xb, yb);
+    mx = 0; mn = 0;
+    for (int q = 0; q < DIAG_SAMPLES; q++) {
+      const double t = (double)q / (DIAG_SAMPLES - 1);
+      const double x = xa + t * (xb - xa), y = ya + t * (yb - ya);
+      const double rel = sample(x, y) - (wa + t * (wb - wa));
+      if (rel > mx) mx = rel;
+      if (rel < mn) mn = rel;
+    }
+  };
+  double abx, abn, cdx, cdn;
+  diag(zone[0], zone[2], zone[1], zone[3], abx, abn);   // zone: x0, x1, y0, y1
+  diag(zone[0], zone[3], zone[1], zone[2], cdx, cdn);
+  const double sum = abx + abn + cdx + cdn;
+  const double sign = sum > 0 ? 1 : (sum < 0 ? -1 : 0);
+  out[0] = sign * mag; out[1] = mag; out[2] = sign; out[3] = mag > 0 ? std::fabs(sum) / mag : 0;
+  out[4] = pl[0]; out[5] = pl[1]; out[6] = pl[2]; out[7] = rmin; out[8] = rmax;
+}
+
 struct orc_model { Model M; std::unique_ptr<LinearSolver> solver; std::string err; };
 
 // cellGroup/cellPart/cellScale: two phases per cell (group < 0: none).
@@ -1916,6 +2070,21 @@ void orc_anand_screen(const double* params, const double* Etab, const double* Ft
     dE[q] = Ec[nc] - Ec[nc - 1];
     stab[q] = nc >= 2 ? std::fabs((Wc[nc] - Wc[nc - 1]) - (Wc[nc - 1] - Wc[nc - 2])) / std::max(Wc[nc] - Wc[nc - 1], 1e-30) : NAN;
   }
+}
+
+// strain increments of the last assembled step at np points (element, natural coordinates)
+void orc_accumulate_q(orc_model* o, const double* du, int nel, const int* elems, double* q) {
+  for (int t = 0; t < nel; t++) accumulateQ(o->M, du, elems[t], q + 33 * (size_t)t);
+}
+
+void orc_element_strains(orc_model* o, int np, const int* elem, const double* q, const double* nat, double* eps) {
+  for (int t = 0; t < np; t++) elementStrain(o->M, elem[t], q + 33 * (size_t)t, nat + 3 * (size_t)t, eps + 6 * (size_t)t);
+}
+void orc_fit_plane(int n, const double* x, const double* y, const double* w, double* c3) { fitPlane(n, x, y, w, c3); }
+double orc_sample_plane(orc_model* o, const double* u, int k, int comp, double x, double y) { return samplePlane(o->M.mesh, u, k, comp, x, y); }
+// out (9): signed, magnitude, sign, sign confidence, plane c0 c1 c2, rmin, rmax
+void orc_warpage_jeita(orc_model* o, const double* u, int nb, const double* bx, const double* by, const double* zone, double* out) {
+  warpageJEITA(o->M.mesh, u, nb, bx, by, zone, out);
 }
 
 const char* orc_last_error(orc_model* o) { return o->err.c_str(); }

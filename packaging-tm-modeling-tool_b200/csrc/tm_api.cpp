@@ -561,15 +561,31 @@ tm_status tm_destroy(tm_ctx* ctx) {
   return guarded([&] { delete reinterpret_cast<Context*>(ctx); });
 }
 
+namespace {
+void check_step(const Context& c, const tm_step& st) {
+  for (int p = 0; p < c.npset; p++) {
+    const double* src = st.psetLayered[p] ? st.W + 108 * (size_t)p : st.D + 36 * (size_t)p;
+    const int cnt = st.psetLayered[p] ? 108 : 36;
+    for (int q = 0; q < cnt; q++) if (!std::isfinite(src[q])) fail(TM_NONFINITE, "non-finite property-set stiffness");
+  }
+}
+}  // namespace
+
+tm_status tm_prepare_step(tm_ctx* ctx, const tm_step* st) {
+  return guarded([&] {
+    if (!ctx || !st) fail(TM_BAD_INPUT, "null argument");
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    check_step(c, *st);
+    launch_shape_matrices(c, *st);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
 tm_status tm_assemble_step(tm_ctx* ctx, const tm_step* st, double* rhs_out) {
   return guarded([&] {
     if (!ctx || !st) fail(TM_BAD_INPUT, "null argument");
     Context& c = *reinterpret_cast<Context*>(ctx);
-    for (int p = 0; p < c.npset; p++) {
-      const double* src = st->psetLayered[p] ? st->W + 108 * (size_t)p : st->D + 36 * (size_t)p;
-      const int cnt = st->psetLayered[p] ? 108 : 36;
-      for (int q = 0; q < cnt; q++) if (!std::isfinite(src[q])) fail(TM_NONFINITE, "non-finite property-set stiffness");
-    }
+    check_step(c, *st);
     launch_shape_matrices(c, *st);
     launch_class_condense(c);
     launch_assemble(c);
@@ -668,6 +684,103 @@ tm_status tm_matvec(tm_ctx* ctx, const double* x, double* y) {
     c.d_tmp.upload(x, n, c.stream);
     launch_apply0(c, c.d_tmp.p, c.d_tmp2.p, nullptr);
     c.d_tmp2.download(y, n, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+// ---- element DOF histories (Model.accumulateStep qOnly) and strains at points -------------------
+namespace {
+void recovery_ready(Context& c) {
+  if (!c.stepReady) fail(TM_BAD_INPUT, "element DOF histories need a step loaded by tm_prepare_step or tm_assemble_step");
+  if (!c.d_conn.p) c.d_conn.upload(c.conn, c.stream);
+}
+void check_elems(const Context& c, int32_t n, const int32_t* e) {
+  for (int32_t t = 0; t < n; t++)
+    if (e[t] >= c.ne) fail(TM_BAD_INPUT, "element index out of range");
+}
+}  // namespace
+
+tm_status tm_accumulate_q_device(tm_ctx* ctx, const double* du, int32_t nel, const int32_t* elems, double* q) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (nel < 0 || (nel > 0 && (!du || !elems || !q))) fail(TM_BAD_INPUT, "tm_accumulate_q: bad arguments");
+    recovery_ready(c);
+    launch_accumulate_q(c, du, nel, elems, q);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_accumulate_q(tm_ctx* ctx, const double* du, int32_t nel, const int32_t* elems, double* q) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (nel < 0 || (nel > 0 && (!du || !elems || !q))) fail(TM_BAD_INPUT, "tm_accumulate_q: bad arguments");
+    if (nel == 0) return;
+    check_elems(c, nel, elems);
+    recovery_ready(c);
+    DBuf<int> de;
+    DBuf<double> dq;
+    c.d_tmp.upload(du, 3 * (size_t)c.nn, c.stream);
+    de.upload(elems, nel, c.stream);
+    dq.upload(q, 33 * (size_t)nel, c.stream);
+    launch_accumulate_q(c, c.d_tmp.p, nel, de.p, dq.p);
+    dq.download(q, 33 * (size_t)nel, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_element_strains_device(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* q, const double* nat, double* eps) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (npts < 0 || (npts > 0 && (!elem || !q || !nat || !eps))) fail(TM_BAD_INPUT, "tm_element_strains: bad arguments");
+    launch_element_strains(c, npts, elem, q, nat, eps);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_element_strains(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* q, const double* nat, double* eps) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (npts < 0 || (npts > 0 && (!elem || !q || !nat || !eps))) fail(TM_BAD_INPUT, "tm_element_strains: bad arguments");
+    if (npts == 0) return;
+    check_elems(c, npts, elem);
+    DBuf<int> de;
+    DBuf<double> dq, dn, deps;
+    de.upload(elem, npts, c.stream);
+    dq.upload(q, 33 * (size_t)npts, c.stream);
+    dn.upload(nat, 3 * (size_t)npts, c.stream);
+    deps.alloc(6 * (size_t)npts);
+    launch_element_strains(c, npts, de.p, dq.p, dn.p, deps.p);
+    deps.download(eps, 6 * (size_t)npts, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+// ---- samplePlane at points ------------------------------------------------------------------------
+tm_status tm_sample_plane_device(tm_ctx* ctx, const double* u, int32_t k, int32_t comp, int32_t npts, const double* x,
+                                 const double* y, double* out) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (k < 0 || k >= c.nz || comp < 0 || comp > 2 || npts < 0 || (npts > 0 && (!u || !x || !y || !out)))
+      fail(TM_BAD_INPUT, "tm_sample_plane: bad arguments");
+    launch_sample_plane(c, u, k, comp, npts, x, y, out);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_sample_plane(tm_ctx* ctx, const double* u, int32_t k, int32_t comp, int32_t npts, const double* x, const double* y,
+                          double* out) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (k < 0 || k >= c.nz || comp < 0 || comp > 2 || npts < 0 || (npts > 0 && (!u || !x || !y || !out)))
+      fail(TM_BAD_INPUT, "tm_sample_plane: bad arguments");
+    if (npts == 0) return;
+    DBuf<double> dx, dy, dout;
+    c.d_tmp.upload(u, 3 * (size_t)c.nn, c.stream);
+    dx.upload(x, npts, c.stream);
+    dy.upload(y, npts, c.stream);
+    dout.alloc(npts);
+    launch_sample_plane(c, c.d_tmp.p, k, comp, npts, dx.p, dy.p, dout.p);
+    dout.download(out, npts, c.stream);
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   });
 }

@@ -180,6 +180,10 @@ struct Context {
   DBuf<double> d_psetM;                // 6*1089 per property set
   DBuf<double> d_clsF33;               // 33 per class: uncondensed element thermal load (elementFth)
   DBuf<int> d_psetLayered, d_psetBorn;
+  bool stepReady = false;              // shape matrices and thermal loads of an assembled step are on the device
+  DBuf<int> d_conn;                    // 8*ne, uploaded on first use by the DOF-history entry points
+  DBuf<double> d_xs, d_ys;             // mesh lines and the node index grid, uploaded on first use
+  DBuf<int> d_nodeId;                  // by the plane sampler
   // operator (level 0): 243 values per position, slot-major ((s*9 + v)*nnp + p), and its FP32
   // copy; the slot-major device arrays (operator, neighbour ids) use the row stride nnp (nn
   // rounded up to a multiple of 4; zero values and id -1 in the padding), so that adjacent
@@ -273,6 +277,10 @@ void launch_galerkin_shell(Context& c, int l);
 void launch_factor_shell(Context& c, ShellLevel& L);
 void launch_factor_coarsest(Context& c, ShellLevel& L);
 void launch_to_fp32(Context& c);
+// element DOF histories and strains at points (device pointers; elems/elem, q, nat, eps on the device)
+void launch_accumulate_q(Context& c, const double* du, int nel, const int* elems, double* q);
+void launch_element_strains(Context& c, int np, const int* elem, const double* q, const double* nat, double* eps);
+void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts, const double* x, const double* y, double* out);
 
 // ---- launch accounting ------------------------------------------------------------------------
 enum KernelId { K_APPLY0 = 0, K_SWEEP_SOLID = 1, K_SWEEP_SHELL = 2, K_ASSEMBLE = 3, K_GALERKIN01 = 4, K_APPLY_SHELL = 5, K_NKERNEL };

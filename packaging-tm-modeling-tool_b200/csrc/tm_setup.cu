@@ -18,6 +18,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <math_constants.h>
+
 #include "tm_internal.h"
 
 namespace tmg {
@@ -533,6 +535,131 @@ __global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restri
   if (i < n) b[i] = (float)a[i];
 }
 
+// ---- element DOF histories at screening sites -----------------------------------------------
+// natural coordinates of the 8 nodes in the local order of the mesher (06-mesher.js:49)
+__device__ __forceinline__ double node_xi(int a) { return ((a & 3) == 1 || (a & 3) == 2) ? 1.0 : -1.0; }
+__device__ __forceinline__ double node_eta(int a) { return (a & 3) >= 2 ? 1.0 : -1.0; }
+__device__ __forceinline__ double node_zeta(int a) { return a >= 4 ? 1.0 : -1.0; }
+
+// Model.accumulateStep with qOnly (09-assembly.js:508-533), one warp per listed element:
+// q[33 t ..] += (du at the element's nodes, K_aa^-1 (f_a - K_au du)) with K_a. the rows 24..32 of
+// the step's K33 = sum_m c_m M^m taken as stored (stepRecovery, 09-assembly.js:480-491) and f_a
+// the incompatible-mode part of the element thermal load of a born material. Same operations in
+// the same order as the reference, so q matches it bit for bit for the same du.
+__global__ void k_accumulate_q(int nel, int ne, const int* __restrict__ elems, const int* __restrict__ conn,
+                               const int* __restrict__ eClass, const int* __restrict__ clsPset,
+                               const double* __restrict__ clsH, const double* __restrict__ psetM,
+                               const double* __restrict__ clsF33, const double* __restrict__ du,
+                               double* __restrict__ q) {
+  __shared__ double sm[4][448];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * 4 + warp;
+  if (t >= nel) return;
+  double* Kr = sm[warp];               // 297
+  double* Kaa = Kr + 297;              // 81
+  double* dq = Kaa + 81;               // 24
+  double* col = dq + 24;               // 9
+  const int e = elems[t];
+  if (e < 0 || e >= ne) {              // no element at this site: its DOFs read NaN
+    for (int o = lane; o < 33; o += 32) q[33 * (size_t)t + o] = CUDART_NAN;
+    return;
+  }
+  const int cls = eClass[e];
+  const double hx = clsH[3 * cls], hy = clsH[3 * cls + 1], hz = clsH[3 * cls + 2];
+  const double V8 = hx * hy * hz / 8;
+  const double c0 = V8 * 4 / (hx * hx), c1 = V8 * 4 / (hy * hy), c2 = V8 * 4 / (hz * hz);
+  const double c3 = V8 * 4 / (hx * hy), c4 = V8 * 4 / (hy * hz), c5 = V8 * 4 / (hz * hx);
+  const double* Ma = psetM + (size_t)clsPset[cls] * 6 * 1089 + 24 * 33;
+  for (int r = lane; r < 297; r += 32)
+    Kr[r] = c0 * Ma[r] + c1 * Ma[1089 + r] + c2 * Ma[2178 + r] + c3 * Ma[3267 + r] + c4 * Ma[4356 + r] + c5 * Ma[5445 + r];
+  if (lane < 24) dq[lane] = du[3 * (size_t)conn[8 * (size_t)e + lane / 3] + lane % 3];
+  __syncwarp();
+  for (int o = lane; o < 81; o += 32) Kaa[o] = Kr[(o / 9) * 33 + 24 + o % 9];
+  if (lane < 9) {
+    double s = clsF33[(size_t)cls * 33 + 24 + lane];
+    for (int k = 0; k < 24; k++) s -= Kr[lane * 33 + k] * dq[k];
+    col[lane] = s;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    chol_dense9(Kaa, 1e-14);
+    chol_solve9(Kaa, col);
+  }
+  __syncwarp();
+  for (int o = lane; o < 33; o += 32) q[33 * (size_t)t + o] += o < 24 ? dq[o] : col[o - 24];
+}
+
+// boxStrainAt (07-element.js:127-142) with boxDerivs (:19-30), thread per point: engineering
+// strain of element elem[t] with DOFs q[33 t ..] at the natural point nat[3 t ..]
+__global__ void k_element_strains(int np, int ne, const int* __restrict__ elem, const int* __restrict__ eClass,
+                                  const double* __restrict__ clsH, const double* __restrict__ q,
+                                  const double* __restrict__ nat, double* __restrict__ eps) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np) return;
+  double* o = eps + 6 * (size_t)t;
+  const int e = elem[t];
+  if (e < 0 || e >= ne) {
+    for (int r = 0; r < 6; r++) o[r] = CUDART_NAN;
+    return;
+  }
+  const int cls = eClass[e];
+  const double sx = 2 / clsH[3 * cls], sy = 2 / clsH[3 * cls + 1], sz = 2 / clsH[3 * cls + 2];
+  const double xi = nat[3 * (size_t)t], eta = nat[3 * (size_t)t + 1], zeta = nat[3 * (size_t)t + 2];
+  const double* u = q + 33 * (size_t)t;
+  double e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0, e5 = 0;
+  for (int b = 0; b < 11; b++) {
+    double dx, dy, dz;
+    if (b < 8) {
+      const double xa = node_xi(b), ya = node_eta(b), za = node_zeta(b);
+      dx = xa * (1 + ya * eta) * (1 + za * zeta) * 0.125 * sx;
+      dy = ya * (1 + xa * xi) * (1 + za * zeta) * 0.125 * sy;
+      dz = za * (1 + xa * xi) * (1 + ya * eta) * 0.125 * sz;
+    } else {
+      dx = b == 8 ? -2 * xi * sx : 0;
+      dy = b == 9 ? -2 * eta * sy : 0;
+      dz = b == 10 ? -2 * zeta * sz : 0;
+    }
+    const double ux = u[3 * b], uy = u[3 * b + 1], uz = u[3 * b + 2];
+    e0 += dx * ux; e1 += dy * uy; e2 += dz * uz;
+    e3 += dy * ux + dx * uy;
+    e4 += dz * uy + dy * uz;
+    e5 += dz * ux + dx * uz;
+  }
+  o[0] = e0; o[1] = e1; o[2] = e2; o[3] = e3; o[4] = e4; o[5] = e5;
+}
+
+// findInterval (01-util.js:12-22): i with a[i] <= x < a[i+1], clamped to [0, n-2]
+__device__ int find_interval(const double* __restrict__ a, int n, double x) {
+  if (x <= a[0]) return 0;
+  if (x >= a[n - 1]) return n - 2;
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// samplePlane (12-post.js:30-38), thread per point: bilinear interpolation of component comp of
+// the nodal field u on mesh plane k at (x, y); NaN where a corner node does not exist
+__global__ void k_sample_plane(int npts, int nx, int ny, int nz, const double* __restrict__ xs, const double* __restrict__ ys,
+                               const int* __restrict__ nodeId, const double* __restrict__ u, int k, int comp,
+                               const double* __restrict__ px, const double* __restrict__ py, double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  const double x = px[t], y = py[t];
+  const int i = find_interval(xs, nx, x), j = find_interval(ys, ny, y);
+  const double tx = (x - xs[i]) / (xs[i + 1] - xs[i]), ty = (y - ys[j]) / (ys[j + 1] - ys[j]);
+  const size_t r0 = ((size_t)i * ny + j) * nz + k, r1 = ((size_t)(i + 1) * ny + j) * nz + k;
+  const int n00 = nodeId[r0], n10 = nodeId[r1], n01 = nodeId[r0 + nz], n11 = nodeId[r1 + nz];
+  if (n00 < 0 || n10 < 0 || n01 < 0 || n11 < 0) {
+    out[t] = CUDART_NAN;
+    return;
+  }
+  out[t] = (1 - tx) * (1 - ty) * u[3 * (size_t)n00 + comp] + tx * (1 - ty) * u[3 * (size_t)n10 + comp] +
+           (1 - tx) * ty * u[3 * (size_t)n01 + comp] + tx * ty * u[3 * (size_t)n11 + comp];
+}
+
 }  // namespace
 
 void launch_shape_matrices(Context& c, const tm_step& st) {
@@ -557,6 +684,7 @@ void launch_shape_matrices(Context& c, const tm_step& st) {
   c.d_clsF33.upload(f33, c.stream);
   c.d_clsBorn.upload(clsBorn, c.stream);
   c.stage = st.stage;
+  c.stepReady = true;
 }
 
 void launch_class_condense(Context& c) {
@@ -666,6 +794,33 @@ void launch_to_fp32(Context& c) {
     conv(L->d_prolW, L->d_prolW32);
     L->d_b32.alloc(6 * (size_t)L->nn); L->d_x32.alloc(6 * (size_t)L->nn); L->d_res32.alloc(6 * (size_t)L->nn);
   }
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_accumulate_q(Context& c, const double* du, int nel, const int* elems, double* q) {
+  if (nel <= 0) return;
+  note_launch();
+  k_accumulate_q<<<(nel + 3) / 4, 128, 0, c.stream>>>(nel, c.ne, elems, c.d_conn.p, c.d_eClass.p, c.d_clsPset.p, c.d_clsH.p, c.d_psetM.p,
+                                                      c.d_clsF33.p, du, q);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_element_strains(Context& c, int np, const int* elem, const double* q, const double* nat, double* eps) {
+  if (np <= 0) return;
+  note_launch();
+  k_element_strains<<<grid_for(np, 128), 128, 0, c.stream>>>(np, c.ne, elem, c.d_eClass.p, c.d_clsH.p, q, nat, eps);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts, const double* x, const double* y, double* out) {
+  if (npts <= 0) return;
+  if (!c.d_xs.p) {
+    c.d_xs.upload(c.xs, c.stream);
+    c.d_ys.upload(c.ys, c.stream);
+    c.d_nodeId.upload(c.nodeId, c.stream);
+  }
+  note_launch();
+  k_sample_plane<<<grid_for(npts, 128), 128, 0, c.stream>>>(npts, c.nx, c.ny, c.nz, c.d_xs.p, c.d_ys.p, c.d_nodeId.p, u, k, comp, x, y, out);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -19,7 +19,8 @@ STATUS_NAMES = {0: "TM_OK", 1: "TM_NOT_CONVERGED", 2: "TM_NONFINITE", 3: "TM_TIM
 EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bcsr", "tm_solve", "tm_matvec", "tm_get_bcsr",
             "tm_sizes", "tm_destroy", "tm_last_error", "tm_solve_device", "tm_matvec_device", "tm_anand_screen",
             "tm_anand_screen_device", "tm_anand_step", "tm_set_stream", "tm_launch_count", "tm_kernel_timer",
-            "tm_kernel_timer_read", "tm_assemble_step_device"]
+            "tm_kernel_timer_read", "tm_assemble_step_device", "tm_prepare_step", "tm_accumulate_q", "tm_accumulate_q_device",
+            "tm_element_strains", "tm_element_strains_device", "tm_sample_plane", "tm_sample_plane_device"]
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
 
 dp = C.POINTER(C.c_double)
@@ -98,6 +99,13 @@ def load():
     L.tm_launch_count.argtypes = []
     L.tm_kernel_timer.argtypes = [vp, C.c_int32]
     L.tm_kernel_timer_read.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+    L.tm_prepare_step.argtypes = [vp, C.POINTER(TmStep)]
+    L.tm_accumulate_q.argtypes = [vp, vp, C.c_int32, vp, vp]
+    L.tm_accumulate_q_device.argtypes = L.tm_accumulate_q.argtypes
+    L.tm_element_strains.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
+    L.tm_element_strains_device.argtypes = L.tm_element_strains.argtypes
+    L.tm_sample_plane.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp]
+    L.tm_sample_plane_device.argtypes = L.tm_sample_plane.argtypes
     for name in EXPORTED:
         getattr(L, name).restype = C.c_int32 if name not in ("tm_default_solve_opts",) else None
     L.tm_launch_count.restype = C.c_int64

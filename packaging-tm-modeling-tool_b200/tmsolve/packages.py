@@ -148,7 +148,12 @@ def fcbga_c1() -> Package:
     return Package(name="fcbga_c1", mesh=mesh, group_layered=np.zeros(4, np.int32), group_stage=np.zeros(4, np.int32),
                    group_pset=np.arange(4, dtype=np.int32), sec_of_layer=np.zeros(nz - 1, np.int32), npset=4,
                    step_fn=lambda Ta, Tb: _homog_step(mats, Ta, Tb), Ta=150.0, Tb=25.0,
-                   meta=dict(workload="fcbga_c1 48x48x20", bottom_plane=0))
+                   meta=dict(workload="fcbga_c1 48x48x20", bottom_plane=0,
+                             # die bump field (0.15 mm pitch over the 15 mm die), BGA (1 mm pitch) and
+                             # the bump layer (mid-height, part of the solder columns)
+                             die=dict(cx=0.0, cy=0.0, w=15.0, h=15.0, keepout=0.15, px=0.15, py=0.15),
+                             bga=dict(sx=35.0, sy=35.0, inset=0.75, pitch=1.0),
+                             bump_layer=dict(zmid=z_sub + 0.5 * z_bump, part=PART["SOLDER"])))
 
 
 def _stack_8_2_8(rng_mat):
@@ -260,7 +265,10 @@ def lidded_c2(n_inplane: int = 160, seed: int = 20261203) -> Package:
     return Package(name="lidded_c2", mesh=mesh, group_layered=group_layered, group_stage=np.zeros(ng, np.int32),
                    group_pset=group_pset, sec_of_layer=sec_of_layer, npset=nb + len(hom_names),
                    step_fn=lambda Ta, Tb: _homog_step(mats, Ta, Tb, layered_fn=layered_fn), Ta=150.0, Tb=25.0,
-                   meta=dict(workload=f"lidded_c2 {n}x{n}x32", bottom_plane=0, seed=seed))
+                   meta=dict(workload=f"lidded_c2 {n}x{n}x32", bottom_plane=0, seed=seed,
+                             die=dict(cx=0.0, cy=0.0, w=25.0, h=25.0, keepout=0.2, px=0.15, py=0.15),
+                             bga=dict(sx=L, sy=L, inset=1.0, pitch=1.0),
+                             bump_layer=dict(zmid=z0 + 0.5 * t_bump, part=PART["SOLDER"])))
 
 
 def rms_warpage(mesh: Mesh, u: np.ndarray, k: int = 0) -> float:

@@ -1,0 +1,374 @@
+"""Post-processing readers of the solve path over the GPU C-ABI: JEITA warpage of the bottom
+surface, BGA ball and die bump sites, and the bump-layer strain table that the joint screening
+integrates.
+
+The field values come from the GPU (``tm_sample_plane`` samples the displacement field where
+it lives; ``tm_accumulate_q`` / ``tm_element_strains`` march the element DOFs of the site
+elements along the thermal path); this module holds the host logic around them, which works on
+a few thousand numbers: site generation, plane fit, residual range, diagonal sign, shape class.
+Every function follows one reference function (paths within the reference project):
+
+  find_interval          src/core/01-util.js:12-22
+  fit_plane              src/core/01-util.js:176-190
+  bump_axis              src/core/05-geometry.js:23-29
+  bump_field             the site grid of bumpFieldRects, src/core/05-geometry.js:45-57
+  bga_sites              src/core/05-geometry.js:172-185
+  die_bump_sites         src/core/05-geometry.js:188-196
+  natural_coords         src/core/12-post.js:4-11
+  element_in_cell        src/core/12-post.js:19-27
+  warpage_jeita          src/core/12-post.js:60-109 (samplePlane :30-38 on the GPU)
+  classify_warpage_shape src/core/12-post.js:111-131
+  screening_sites        src/core/13-fatigue.js:296-313
+  site_elements          the site -> element lookup of siteStrainTable, 13-fatigue.js:318-331
+  q_along                Analysis.qAlong, src/core/11-analysis.js:298-316 (state25 :276-281)
+  site_strain_table      siteStrainTable, src/core/13-fatigue.js:318-346
+
+Arithmetic is plain Python floats in the reference's order of operations, so the results are
+the reference's to the last bit for the same sampled values.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from .packages import StepData
+
+# 00-constants.js:98-105
+DIAG_SAMPLES = 201
+SIGN_MARGINAL = 0.25
+SCREEN_MAX_BUMPS = 20000
+SCREEN_MAX_DDI = 5000
+SCREEN_KEEP_ROWS = 3
+SCREEN_CORNER_BLOCK = 10
+
+
+def clamp(x: float, lo: float, hi: float) -> float:
+    return lo if x < lo else (hi if x > hi else x)
+
+
+def find_interval(a: Sequence[float], x: float) -> int:
+    """Index i with a[i] <= x < a[i+1], clamped to [0, n-2]; a ascending."""
+    n = len(a)
+    if x <= a[0]:
+        return 0
+    if x >= a[n - 1]:
+        return n - 2
+    lo, hi = 0, n - 1
+    while hi - lo > 1:
+        mid = (lo + hi) >> 1
+        if a[mid] <= x:
+            lo = mid
+        else:
+            hi = mid
+    return lo
+
+
+def fit_plane(xs, ys, ws) -> tuple:
+    """Least-squares plane w = c0 + c1 x + c2 y (centred normal equations): (c0, c1, c2)."""
+    xs = [float(v) for v in xs]; ys = [float(v) for v in ys]; ws = [float(v) for v in ws]
+    n = len(ws)
+    sx = sy = sw = 0.0
+    for i in range(n):
+        sx += xs[i]; sy += ys[i]; sw += ws[i]
+    mx, my, mw = sx / n, sy / n, sw / n
+    sxx = sxy = syy = sxw = syw = 0.0
+    for i in range(n):
+        dx = xs[i] - mx; dy = ys[i] - my; dw = ws[i] - mw
+        sxx += dx * dx; sxy += dx * dy; syy += dy * dy; sxw += dx * dw; syw += dy * dw
+    det = sxx * syy - sxy * sxy
+    c1 = c2 = 0.0
+    if abs(det) > 1e-300:
+        c1 = (sxw * syy - syw * sxy) / det
+        c2 = (syw * sxx - sxw * sxy) / det
+    return (mw - c1 * mx - c2 * my, c1, c2)
+
+
+def bump_axis(c: float, L: float, k: float, p: float) -> dict:
+    """Sites along one axis of a field of length L centred at c, inset k, pitch p."""
+    span0 = L - 2 * k
+    if span0 < -1e-12 or p <= 0:
+        return dict(n=0, first=c, last=c)
+    n = math.floor(span0 / p + 1e-9) + 1
+    span = (n - 1) * p
+    return dict(n=n, first=c - span / 2, last=c + span / 2)
+
+
+def bump_field(cx: float, cy: float, w: float, h: float, keepout: float, px: float, py: float,
+               rows: int = 1, peripheral: bool = False) -> dict:
+    """Bump site grid of a w x h footprint centred at (cx, cy): {nbx, nby, bx0, by0, px, py,
+    rows, peripheral} (peripheral: only the outer rows carry bumps, when the field is wide
+    enough to leave an inner void)."""
+    ax, ay = bump_axis(cx, w, keepout, px), bump_axis(cy, h, keepout, py)
+    N = max(1, round(rows or 1))
+    per = bool(peripheral and ax["n"] > 0 and ay["n"] > 0 and ax["n"] > 2 * N and ay["n"] > 2 * N)
+    return dict(nbx=ax["n"], nby=ay["n"], bx0=ax["first"], by0=ay["first"], px=px, py=py, rows=N, peripheral=per)
+
+
+def bga_sites(sx: float, sy: float, inset: float, pitch: float, depop: Optional[dict] = None) -> dict:
+    """BGA ball sites of a substrate sx x sy centred at the origin (depop: {'on', 'sx', 'sy'}
+    removes the balls of a centred rectangle) and the JEITA measuring zone."""
+    ax, ay = bump_axis(0, sx, inset, pitch), bump_axis(0, sy, inset, pitch)
+    xs, ys = [], []
+    for i in range(ax["n"]):
+        for j in range(ay["n"]):
+            x = ax["first"] + i * pitch
+            y = ay["first"] + j * pitch
+            if depop and depop.get("on") and abs(x) < depop["sx"] / 2 and abs(y) < depop["sy"] / 2:
+                continue
+            xs.append(x); ys.append(y)
+    return dict(x=np.array(xs, np.float64), y=np.array(ys, np.float64),
+                zone=dict(x0=ax["first"], x1=ax["last"], y0=ay["first"], y1=ay["last"]), nx=ax["n"], ny=ay["n"])
+
+
+def die_bump_sites(d: dict) -> dict:
+    """All bump sites of a die field d = {nbx, nby, bx0, by0, px, py[, peripheral, rows]}:
+    {x, y, ix, iy, row}, row = distance in rows from the field edge."""
+    xs, ys, ix, iy, row = [], [], [], [], []
+    for i in range(d["nbx"]):
+        for j in range(d["nby"]):
+            r = min(i, j, d["nbx"] - 1 - i, d["nby"] - 1 - j)
+            if d.get("peripheral") and r >= d["rows"]:
+                continue
+            xs.append(d["bx0"] + i * d["px"]); ys.append(d["by0"] + j * d["py"])
+            ix.append(i); iy.append(j); row.append(r)
+    return dict(x=np.array(xs, np.float64), y=np.array(ys, np.float64), ix=np.array(ix, np.int32),
+                iy=np.array(iy, np.int32), row=np.array(row, np.int32))
+
+
+def screening_sites(d: dict, max_sites: Optional[int] = None) -> dict:
+    """Bump sites kept for screening: all of them up to the cap, else the outer rows, the corner
+    blocks and an even subsample of the rest. {sites, idx, subsampled}."""
+    a = die_bump_sites(d)
+    n = len(a["x"])
+    cap = max_sites or SCREEN_MAX_BUMPS
+    if n <= cap:
+        return dict(sites=a, idx=None, subsampled=False)
+
+    def must(q):
+        cb = SCREEN_CORNER_BLOCK
+        return (a["row"][q] < SCREEN_KEEP_ROWS or
+                ((a["ix"][q] < cb or a["ix"][q] >= d["nbx"] - cb) and (a["iy"][q] < cb or a["iy"][q] >= d["nby"] - cb)))
+    keep, rest = [], []
+    for q in range(n):
+        (keep if must(q) else rest).append(q)
+    budget = max(0, cap - len(keep))
+    stride = len(rest) / max(budget, 1)
+    k = 0
+    while k < budget and k * stride < len(rest):
+        keep.append(rest[math.floor(k * stride)])
+        k += 1
+    keep.sort()
+    idx = np.array(keep, np.int32)
+    sites = {key: a[key][idx] for key in ("x", "y", "ix", "iy", "row")}
+    return dict(sites=sites, idx=idx, subsampled=True)
+
+
+def natural_coords(mesh, e: int, x: float, y: float, z: float) -> tuple:
+    i, j, k = (int(v) for v in mesh.eIJK[3 * e:3 * e + 3])
+    xs, ys, zs = mesh.xs, mesh.ys, mesh.zs
+    return (clamp(2 * (x - xs[i]) / (xs[i + 1] - xs[i]) - 1, -1, 1),
+            clamp(2 * (y - ys[j]) / (ys[j + 1] - ys[j]) - 1, -1, 1),
+            clamp(2 * (z - zs[k]) / (zs[k + 1] - zs[k]) - 1, -1, 1))
+
+
+def element_in_cell(mesh, i: int, j: int, k: int, part: Optional[int] = None) -> int:
+    ncy, ncz = mesh.ny - 1, mesh.nz - 1
+    c = (i * ncy + j) * ncz + k
+    for q in range(2):
+        e = int(mesh.cellElems[2 * c + q])
+        if e >= 0 and (part is None or int(mesh.ePart[e]) == part):
+            return e
+    return -1
+
+
+def site_elements(mesh, sx, sy, zmid: float, part: Optional[int]) -> tuple:
+    """Element of the joint layer at mid-height zmid under every site (-1: none) and the site's
+    natural coordinates in it: (elem (n,), nat (n, 3))."""
+    xs, ys, zs = [float(v) for v in mesh.xs], [float(v) for v in mesh.ys], [float(v) for v in mesh.zs]
+    kb = find_interval(zs, zmid)
+    n = len(sx)
+    elem = np.full(n, -1, np.int32)
+    nat = np.zeros((n, 3))
+    for q in range(n):
+        x, y = float(sx[q]), float(sy[q])
+        e = element_in_cell(mesh, find_interval(xs, x), find_interval(ys, y), kb, part)
+        elem[q] = e
+        if e >= 0:
+            nat[q] = natural_coords(mesh, e, x, y, zmid)
+    return elem, nat
+
+
+# ---- JEITA warpage ---------------------------------------------------------------------------
+def _diag(sample_pts: np.ndarray, xa, ya, xb, yb):
+    """Diagonal profile from its 2 + DIAG_SAMPLES sampled values (end points first)."""
+    m = DIAG_SAMPLES
+    wa, wb = float(sample_pts[0]), float(sample_pts[1])
+    s = np.zeros(m); rel = np.zeros(m); wv = np.zeros(m)
+    mx = mn = 0.0
+    L = math.hypot(xb - xa, yb - ya)
+    for q in range(m):
+        t = q / (m - 1)
+        wv[q] = float(sample_pts[2 + q])
+        s[q] = t * L
+        rel[q] = wv[q] - (wa + t * (wb - wa))
+        if rel[q] > mx:
+            mx = float(rel[q])
+        if rel[q] < mn:
+            mn = float(rel[q])
+    return dict(s=s, w=wv, rel=rel, max=mx, min=mn)
+
+
+def _diag_points(xa, ya, xb, yb):
+    m = DIAG_SAMPLES
+    px, py = [xa, xb], [ya, yb]
+    for q in range(m):
+        t = q / (m - 1)
+        px.append(xa + t * (xb - xa)); py.append(ya + t * (yb - ya))
+    return px, py
+
+
+def classify_warpage_shape(res, pl, mag, AB, CD) -> str:
+    """'dome', 'bowl', 'ring', 'saddle' or 'flat' from the two diagonal profiles."""
+    if not (mag > 0):
+        return "flat"
+
+    def prof(D):
+        rel = D["rel"]; m = len(rel); ic = (m - 1) >> 1
+        rc = rel[ic]
+        imax = imin = 0
+        for q in range(m):
+            if rel[q] > rel[imax]:
+                imax = q
+            if rel[q] < rel[imin]:
+                imin = q
+
+        def interior(i):
+            t = i / (m - 1)
+            return (0.08 < t < 0.4) or (0.6 < t < 0.92)
+        return dict(rc=rc, max=rel[imax], min=rel[imin], maxInterior=interior(imax), minInterior=interior(imin))
+    a, c = prof(AB), prof(CD)
+    up = a["rc"] > 0.1 * mag and c["rc"] > 0.1 * mag
+    down = a["rc"] < -0.1 * mag and c["rc"] < -0.1 * mag
+    if not up and not down:
+        return "saddle"
+    if up and ((a["min"] < -0.2 * mag and a["minInterior"]) or (c["min"] < -0.2 * mag and c["minInterior"])):
+        return "ring"
+    if down and ((a["max"] > 0.2 * mag and a["maxInterior"]) or (c["max"] > 0.2 * mag and c["maxInterior"])):
+        return "ring"
+    if up and a["maxInterior"] and c["maxInterior"] and a["rc"] < 0.5 * a["max"] and c["rc"] < 0.5 * c["max"]:
+        return "ring"
+    if down and a["minInterior"] and c["minInterior"] and a["rc"] > 0.5 * a["min"] and c["rc"] > 0.5 * c["min"]:
+        return "ring"
+    return "dome" if up else "bowl"
+
+
+def warpage_jeita(bga: dict, sampler: Callable[[np.ndarray, np.ndarray], np.ndarray]) -> dict:
+    """JEITA ED-7306 / JESD22-B112 warpage of the bottom surface over the BGA measuring zone.
+
+    sampler(x, y) returns the bottom-plane z displacement at the points (x, y) in one call
+    (``model.sample_plane(u, 0, 2, x, y)`` samples on the GPU). Returns the reference's record
+    without the limit-table lookup and the contour grid: signed, mag, sign, signConf, marginal,
+    shape, plane (c0, c1, c2), ballW, ballRes, diagAB, diagCD, rmin, rmax."""
+    bx, by = np.asarray(bga["x"], np.float64), np.asarray(bga["y"], np.float64)
+    n = len(bx)
+    z = bga["zone"]
+    abx, aby = _diag_points(z["x0"], z["y0"], z["x1"], z["y1"])
+    cdx, cdy = _diag_points(z["x0"], z["y1"], z["x1"], z["y0"])
+    # one batched sample: the balls, then diagonal AB, then diagonal CD
+    px = np.concatenate([bx, np.array(abx), np.array(cdx)])
+    py = np.concatenate([by, np.array(aby), np.array(cdy)])
+    vals = np.asarray(sampler(px, py), np.float64)
+    w = vals[:n]
+    pl = fit_plane(bx, by, w)
+    res = np.zeros(n)
+    rmin, rmax = math.inf, -math.inf
+    for q in range(n):
+        r = float(w[q]) - (pl[0] + pl[1] * float(bx[q]) + pl[2] * float(by[q]))
+        res[q] = r
+        # Math.min / Math.max: NaN once any operand is NaN
+        rmin = math.nan if (math.isnan(r) or math.isnan(rmin)) else min(rmin, r)
+        rmax = math.nan if (math.isnan(r) or math.isnan(rmax)) else max(rmax, r)
+    mag = rmax - rmin
+    m2 = 2 + DIAG_SAMPLES
+    AB = _diag(vals[n:n + m2], z["x0"], z["y0"], z["x1"], z["y1"])
+    CD = _diag(vals[n + m2:], z["x0"], z["y1"], z["x1"], z["y0"])
+    s = AB["max"] + AB["min"] + CD["max"] + CD["min"]
+    sign = 1 if s > 0 else (-1 if s < 0 else 0)
+    sign_conf = abs(s) / mag if mag > 0 else 0
+    return dict(signed=sign * mag, mag=mag, sign=sign, signConf=sign_conf, marginal=sign_conf < SIGN_MARGINAL,
+                shape=classify_warpage_shape(res, pl, mag, AB, CD), plane=pl, ballW=w, ballRes=res,
+                diagAB=AB, diagCD=CD, rmin=rmin, rmax=rmax)
+
+
+# ---- element DOF histories along the thermal path and the site strain table -------------------
+@dataclass
+class ThermalPath:
+    """The steps of an analysis as Analysis keeps them for the stress histories: per step its
+    property-set data (prepareStep's output), its end temperature Tb and its displacement
+    increment du (kept as float32 by the reference, src/core/11-analysis.js:256); chain: the
+    steps from the stress-free state to the as-assembled 25 degC state; up / down: the cycling
+    branches from 25 degC to Tmax / Tmin."""
+    steps: List[StepData]
+    Tb: List[float]
+    du: List[np.ndarray]
+    chain: List[int]
+    up: List[int] = field(default_factory=list)
+    down: List[int] = field(default_factory=list)
+
+
+def q_along(model, path: ThermalPath, elems, temps) -> Dict[float, np.ndarray]:
+    """Element DOFs q (nel x 33) of every listed element at each of the given as-assembled
+    temperatures: the 25 degC state (the chain), then both branches marched from it. All
+    elements advance together, one GPU launch per step."""
+    elems = np.ascontiguousarray(elems, np.int32)
+    nel = len(elems)
+    want = set(float(t) for t in temps)
+    hi, lo = max(want), min(want)
+    base = np.zeros(33 * nel)
+    for k in path.chain:
+        model.prepare_step(path.steps[k])
+        model.accumulate_q(path.du[k], elems, base)
+    out: Dict[float, np.ndarray] = {}
+    if 25.0 in want:
+        out[25.0] = base.reshape(nel, 33).copy()
+    for br, end in ((path.up, hi), (path.down, lo)):
+        if end == 25:
+            continue
+        st = base.copy()
+        for k in br:
+            model.prepare_step(path.steps[k])
+            model.accumulate_q(path.du[k], elems, st)
+            T = float(path.Tb[k])
+            if T in want:
+                out[T] = st.reshape(nel, 33).copy()
+            if T == end:
+                break
+    return out
+
+
+def site_strain_table(model, path: ThermalPath, sites: dict, temps, zmid: float, part: Optional[int]) -> np.ndarray:
+    """Bump-layer total strain (engineering, xx yy zz xy yz zx) at every site for every sample
+    temperature: (nsites x ntemps x 6), NaN where a site has no element of the joint layer or a
+    temperature is not reached by the path."""
+    mesh = model.pkg.mesh
+    temps = [float(t) for t in temps]
+    n, nt = len(sites["x"]), len(temps)
+    out = np.full(n * nt * 6, np.nan)
+    elem, nat = site_elements(mesh, sites["x"], sites["y"], zmid, part)
+    have = elem >= 0
+    if not have.any():
+        return out
+    uniq, inv = np.unique(elem[have], return_inverse=True)
+    qs = q_along(model, path, uniq, temps)
+    idx = np.nonzero(have)[0]
+    for ti, T in enumerate(temps):
+        qv = qs.get(T)
+        if qv is None:
+            continue
+        eps = model.element_strains(elem[have], qv[inv], nat[have])
+        for r, q in enumerate(idx):
+            out[(q * nt + ti) * 6:(q * nt + ti) * 6 + 6] = eps[r]
+    return out

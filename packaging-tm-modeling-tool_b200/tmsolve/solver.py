@@ -83,25 +83,34 @@ class DeviceModel:
             pass
 
     # ---- FEModel.assembleStep ------------------------------------------------------------
-    def assemble_step(self, step: StepData, out: Optional[np.ndarray] = None) -> np.ndarray:
-        """The load vector of the step (host array; `out`, e.g. pinned memory, is filled when given)."""
-        lay = np.ascontiguousarray(step.layered, np.int32); born = np.ascontiguousarray(step.born, np.int32)
-        D = np.ascontiguousarray(step.D, np.float64); s0 = np.ascontiguousarray(step.s0, np.float64)
-        W = np.ascontiguousarray(step.W, np.float64); V = np.ascontiguousarray(step.V, np.float64)
+    @staticmethod
+    def _step_struct(step: StepData):
+        """tm_step over the step's arrays; the arrays are returned too, to keep them alive."""
+        keep = (np.ascontiguousarray(step.layered, np.int32), np.ascontiguousarray(step.born, np.int32),
+                np.ascontiguousarray(step.D, np.float64), np.ascontiguousarray(step.s0, np.float64),
+                np.ascontiguousarray(step.W, np.float64), np.ascontiguousarray(step.V, np.float64))
+        lay, born, D, s0, W, V = keep
         st = TmStep(stage=int(step.stage), psetLayered=_p(lay, C.c_int32), D=_p(D, C.c_double), s0=_p(s0, C.c_double),
                     W=_p(W, C.c_double), V=_p(V, C.c_double), psetBorn=_p(born, C.c_int32))
+        return st, keep
+
+    def assemble_step(self, step: StepData, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The load vector of the step (host array; `out`, e.g. pinned memory, is filled when given)."""
+        st, _keep = self._step_struct(step)
         rhs = _out_array(out, self.ndof)
         check(load().tm_assemble_step(self.h, C.byref(st), rhs.ctypes.data_as(C.c_void_p)))
         return rhs
 
     def assemble_step_device(self, step: StepData, rhs_ptr: int):
         """assemble_step with the load written to device memory (raw device pointer)."""
-        lay = np.ascontiguousarray(step.layered, np.int32); born = np.ascontiguousarray(step.born, np.int32)
-        D = np.ascontiguousarray(step.D, np.float64); s0 = np.ascontiguousarray(step.s0, np.float64)
-        W = np.ascontiguousarray(step.W, np.float64); V = np.ascontiguousarray(step.V, np.float64)
-        st = TmStep(stage=int(step.stage), psetLayered=_p(lay, C.c_int32), D=_p(D, C.c_double), s0=_p(s0, C.c_double),
-                    W=_p(W, C.c_double), V=_p(V, C.c_double), psetBorn=_p(born, C.c_int32))
+        st, _keep = self._step_struct(step)
         check(load().tm_assemble_step_device(self.h, C.byref(st), C.c_void_p(rhs_ptr)))
+
+    def prepare_step(self, step: StepData):
+        """FEModel.stepRecovery (src/core/09-assembly.js:480-491): loads the step's shape matrices
+        and element thermal loads for accumulate_q without assembling the operator."""
+        st, _keep = self._step_struct(step)
+        check(load().tm_prepare_step(self.h, C.byref(st)))
 
     def set_bcsr(self, rowPtr, col, val, isConstrained):
         rowPtr = np.ascontiguousarray(rowPtr, np.int32); col = np.ascontiguousarray(col, np.int32)
@@ -120,6 +129,45 @@ class DeviceModel:
         y = np.zeros(self.ndof)
         check(load().tm_matvec(self.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p)))
         return y
+
+    # ---- element DOF histories and field sampling ------------------------------------------
+    def accumulate_q(self, du, elems, q: np.ndarray) -> np.ndarray:
+        """Model.accumulateStep with qOnly (src/core/09-assembly.js:508-533) for the step
+        assembled last: q (nel x 33, float64, updated in place) += every listed element's DOF
+        increment from the step's displacement increment du. A negative element index (no
+        element at that site) gives a NaN row."""
+        du = np.ascontiguousarray(du, np.float64); elems = np.ascontiguousarray(elems, np.int32)
+        if q.dtype != np.float64 or not q.flags.c_contiguous or q.size != 33 * len(elems):
+            raise ValueError("q must be a contiguous float64 array of 33 values per element")
+        if du.size != self.ndof:
+            raise ValueError(f"du must hold {self.ndof} values")
+        check(load().tm_accumulate_q(self.h, du.ctypes.data_as(C.c_void_p), len(elems), elems.ctypes.data_as(C.c_void_p),
+                                     q.ctypes.data_as(C.c_void_p)))
+        return q
+
+    def element_strains(self, elem, q, nat) -> np.ndarray:
+        """boxStrainAt (src/core/07-element.js:127-142) of element elem[p] with DOFs q[p] at the
+        natural point nat[p]: (npts, 6) engineering strains."""
+        elem = np.ascontiguousarray(elem, np.int32)
+        q = np.ascontiguousarray(q, np.float64).reshape(-1); nat = np.ascontiguousarray(nat, np.float64).reshape(-1)
+        if q.size != 33 * len(elem) or nat.size != 3 * len(elem):
+            raise ValueError("q needs 33 and nat 3 values per point")
+        eps = np.zeros(6 * len(elem))
+        check(load().tm_element_strains(self.h, len(elem), elem.ctypes.data_as(C.c_void_p), q.ctypes.data_as(C.c_void_p),
+                                        nat.ctypes.data_as(C.c_void_p), eps.ctypes.data_as(C.c_void_p)))
+        return eps.reshape(-1, 6)
+
+    def sample_plane(self, u, k: int, comp: int, x, y) -> np.ndarray:
+        """samplePlane (src/core/12-post.js:30-38) of the nodal field u at the points (x, y)."""
+        u = np.ascontiguousarray(u, np.float64)
+        x = np.ascontiguousarray(x, np.float64).reshape(-1); y = np.ascontiguousarray(y, np.float64).reshape(-1)
+        if u.size != self.ndof or x.size != y.size:
+            raise ValueError("u must hold one value per DOF and x, y one per point")
+        out = np.zeros(len(x))
+        check(load().tm_sample_plane(self.h, u.ctypes.data_as(C.c_void_p), int(k), int(comp), len(x),
+                                     x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
+                                     out.ctypes.data_as(C.c_void_p)))
+        return out
 
     # ---- LinearSolver.solve ----------------------------------------------------------------
     @staticmethod
