@@ -17,6 +17,8 @@
  *   tm_matvec          fullMatVec(P, val, x, y)           src/core/09-assembly.js:151-165
  *   tm_anand_screen    screenJoints' per-site Anand loop  src/core/13-fatigue.js:395-451
  *                      (AnandPoint.stepColumn / step, :13-166)
+ *   tm_anand_screen_pillar  screenDdi's joints: solder caps on elastic pillars
+ *                      (AnandPoint.stepSeriesColumn, src/core/13-fatigue.js:178-206, 369-376, 404-433)
  *   tm_anand_step      AnandPoint.step + commit           src/core/13-fatigue.js:67-143, 229-232
  *   tm_prepare_step    FEModel.stepRecovery(Ta, Tb, stage): the step's shape matrices and element
  *                      thermal loads without an assembly (src/core/09-assembly.js:480-491)
@@ -251,6 +253,28 @@ tm_status tm_anand_screen_device(const tm_anand_material* mat, int32_t nsites, i
                                  const double* table_dev, int32_t nsteps, const double* t, const double* T,
                                  const int32_t* cycle, const int32_t* phase, int32_t cycles,
                                  double* dW_dev, double* dE_dev, double* stab_dev);
+
+/* An elastic pillar under each solder joint (a DDI microbump: solder cap on a Cu pillar). */
+typedef struct {
+  double fs;                     /* solder height fraction of the joint, 1 - pillarH / standoff, in (0, 1] */
+  double nu;                     /* pillar Poisson ratio */
+  const double* Etab;            /* pillar E(T) in MPa on the 1 degC grid -80..300 (381 values) */
+  const double* Ftab;            /* pillar thermal strain F(T) on the same grid */
+} tm_pillar;
+
+/* tm_anand_screen for joints that are a solder cap on an elastic pillar (screenDdi): per time
+ * step the column-average axial and shear strains of the layer (less the thermal strains of cap
+ * and pillar) are prescribed, the cap and the pillar carry the same axial and shear stresses
+ * and the cap's in-plane stresses vanish (stepSeriesColumn). Host pointers. */
+tm_status tm_anand_screen_pillar(const tm_anand_material* mat, const tm_pillar* pillar, int32_t nsites, int32_t ntemps,
+                                 const double* temps, const double* table, int32_t nsteps, const double* t, const double* T,
+                                 const int32_t* cycle, const int32_t* phase, int32_t cycles,
+                                 double* dW, double* dE, double* stab);
+/* The same with device pointers for table and outputs (time history and tables on the host). */
+tm_status tm_anand_screen_pillar_device(const tm_anand_material* mat, const tm_pillar* pillar, int32_t nsites, int32_t ntemps,
+                                        const double* temps, const double* table_dev, int32_t nsteps, const double* t,
+                                        const double* T, const int32_t* cycle, const int32_t* phase, int32_t cycles,
+                                        double* dW_dev, double* dE_dev, double* stab_dev);
 
 /* Screening that allocates no device memory (no counterpart in the reference). For callers that
  * cannot call cudaMalloc while they screen: a host application whose allocator already owns the

@@ -61,6 +61,8 @@ def lib():
     L.orc_anand_uniaxial.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int]
     L.orc_anand_screen.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _ip, _ip, C.c_int,
                                    _dp, _dp, _dp]
+    L.orc_anand_screen_pillar.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _ip, _ip, C.c_int,
+                                          C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]
     L.orc_accumulate_q.argtypes = [vp, _dp, C.c_int, _ip, _dp]
     L.orc_element_strains.argtypes = [vp, C.c_int, _ip, _dp, _dp, _dp]
     L.orc_fit_plane.argtypes = [C.c_int, _dp, _dp, _dp, _dp]
@@ -220,4 +222,19 @@ def anand_screen(params, Etab, Ftab, temps, table, hist):
                            len(hist["t"]), np.ascontiguousarray(hist["t"], np.float64), np.ascontiguousarray(hist["T"], np.float64),
                            np.ascontiguousarray(hist["cycle"], np.int32), np.ascontiguousarray(hist["phase"], np.int32),
                            int(hist["cycles"]), dW, dE, stab)
+    return dW, dE, stab
+
+
+def anand_screen_pillar(params, Etab, Ftab, temps, table, hist, fs, pnu, pEtab, pFtab):
+    """screenJoints' per-site loop for a solder cap (height fraction fs) on an elastic pillar
+    (stepSeriesColumn, 13-fatigue.js:178-206, as screenDdi drives it, :369-376)."""
+    temps = np.ascontiguousarray(temps, np.float64); table = np.ascontiguousarray(table, np.float64)
+    nsites = table.size // (6 * len(temps))
+    dW = np.zeros(nsites); dE = np.zeros(nsites); stab = np.zeros(nsites)
+    lib().orc_anand_screen_pillar(np.ascontiguousarray(params, np.float64), np.ascontiguousarray(Etab, np.float64),
+                                  np.ascontiguousarray(Ftab, np.float64), nsites, len(temps), temps, table,
+                                  len(hist["t"]), np.ascontiguousarray(hist["t"], np.float64),
+                                  np.ascontiguousarray(hist["T"], np.float64), np.ascontiguousarray(hist["cycle"], np.int32),
+                                  np.ascontiguousarray(hist["phase"], np.int32), int(hist["cycles"]), float(fs), float(pnu),
+                                  np.ascontiguousarray(pEtab, np.float64), np.ascontiguousarray(pFtab, np.float64), dW, dE, stab)
     return dW, dE, stab

@@ -1676,6 +1676,53 @@ struct AnandPoint {
     return d;
   }
 
+  // stepSeriesColumn :178-206: the solder cap (height fraction fs) in series with an elastic
+  // pillar of compliances Cp; tz = prescribed column-average (zz, yz, zx) mechanical strains
+  double stepSeriesColumn(double* eps, const double* tz, double fs, const double* Cp, double T, double dt, double* sig, double* D,
+                          const StepK* k) {
+    const int Pi[3] = {0, 1, 3}, Z[3] = {2, 4, 5}, ord[6] = {0, 1, 3, 2, 4, 5};
+    const double fp = 1 - fs;
+    double J[36], R[6];
+    const double E = gridAt(Etab, T);
+    double d = 0;
+    for (int it = 0; it < COLUMN_NEWTON_MAXIT; it++) {
+      d = step(eps, T, dt, sig, D, true, k);
+      for (int r = 0; r < 3; r++) { R[r] = sig[Pi[r]]; R[3 + r] = fs * eps[Z[r]] + fp * Cp[r] * sig[Z[r]] - tz[r]; }
+      const double ref = std::max(std::max(1.0, std::fabs(sig[2])), std::max(std::fabs(sig[4]), std::fabs(sig[5])));
+      double worst = 0;
+      for (int r = 0; r < 3; r++) worst = std::max(std::max(worst, std::fabs(R[r])), std::fabs(R[3 + r]) * E);
+      if (worst < COLUMN_STRESS_TOL * ref) break;
+      for (int r = 0; r < 6; r++)
+        for (int c = 0; c < 6; c++) {
+          const double Dv = D[6 * ord[r] + ord[c]];
+          J[6 * r + c] = r < 3 ? Dv : fp * Cp[r - 3] * Dv + (ord[r] == ord[c] ? fs : 0);
+        }
+      // Gaussian elimination with partial pivoting
+      for (int c = 0; c < 6; c++) {
+        int pr = c;
+        for (int r = c + 1; r < 6; r++) if (std::fabs(J[6 * r + c]) > std::fabs(J[6 * pr + c])) pr = r;
+        if (pr != c) {
+          for (int q = 0; q < 6; q++) std::swap(J[6 * c + q], J[6 * pr + q]);
+          std::swap(R[c], R[pr]);
+        }
+        const double piv = J[7 * c];
+        for (int r = c + 1; r < 6; r++) {
+          const double f = J[6 * r + c] / piv;
+          if (f == 0) continue;
+          for (int q = c; q < 6; q++) J[6 * r + q] -= f * J[6 * c + q];
+          R[r] -= f * R[c];
+        }
+      }
+      for (int c = 5; c >= 0; c--) {
+        double v = R[c];
+        for (int q = c + 1; q < 6; q++) v -= J[6 * c + q] * R[q];
+        R[c] = v / J[7 * c];
+      }
+      for (int c = 0; c < 6; c++) eps[ord[c]] -= R[c];
+    }
+    return d;
+  }
+
   void commit() { for (int i = 0; i < 6; i++) ep[i] = tr_ep[i]; s = tr_s; ebar = tr_ebar; W = tr_W; sigEq = tr_sigEq; }
 };
 
@@ -2013,21 +2060,27 @@ double orc_anand_uniaxial(const double* params, const double* Etab, double T, do
   return last;
 }
 
-// The per-site loop of screenJoints (13-fatigue.js:395-451) for free-standing solder columns:
-// table (nsites x ntemps x 6) of bump-layer total strains at the cycling temperatures `temps`,
-// the time history (t, T, cycle, phase) of cycleHistory, thermal strain table Ftab on the
-// 1 degC grid. Outputs dW, dE, stab per site (NaN where the table is not finite).
-void orc_anand_screen(const double* params, const double* Etab, const double* Ftab,
-                      int nsites, int ntemps, const double* temps, const double* table,
-                      int nsteps, const double* th, const double* Th, const int* cycle, const int* phase, int cycles,
-                      double* dW, double* dE, double* stab) {
+// The per-site loop of screenJoints (13-fatigue.js:395-451): table (nsites x ntemps x 6) of
+// bump-layer total strains at the cycling temperatures `temps`, the time history (t, T, cycle,
+// phase) of cycleHistory, thermal strain table Ftab on the 1 degC grid. Without a pillar
+// (pEtab == nullptr) every joint is a free-standing solder column (stepColumn); with one it is a
+// solder cap of height fraction fs on an elastic pillar (E table pEtab, Poisson ratio pNu,
+// thermal strain table pFtab) in series (stepSeriesColumn, screenDdi :369-376). Outputs dW,
+// dE, stab per site (NaN where the table is not finite).
+static void screenLoop(const double* params, const double* Etab, const double* Ftab,
+                       int nsites, int ntemps, const double* temps, const double* table,
+                       int nsteps, const double* th, const double* Th, const int* cycle, const int* phase, int cycles,
+                       double fs, double pNu, const double* pEtab, const double* pFtab,
+                       double* dW, double* dE, double* stab) {
   AnandParams P{params[0], params[1], params[2], params[3], params[4], params[5], params[6], params[7], params[8], params[9]};
   AnandPoint pt(P, Etab);
   const double nu = P.nu;
   const int IP[3] = {0, 1, 3};
+  const bool pillar = pEtab != nullptr;
+  if (!pillar) fs = 1;
   int i25 = -1;
   for (int i = 0; i < ntemps; i++) if (temps[i] == 25) { i25 = i; break; }
-  std::vector<int> wi(nsteps); dvec wt(nsteps), Fth(nsteps);
+  std::vector<int> wi(nsteps); dvec wt(nsteps), Fth(nsteps), Cps(pillar ? 3 * nsteps : 0), Fp(pillar ? nsteps : 0);
   std::vector<StepK> kc(nsteps);
   for (int k = 0; k < nsteps; k++) {
     // findInterval (01-util.js:12-22)
@@ -2040,9 +2093,14 @@ void orc_anand_screen(const double* params, const double* Etab, const double* Ft
     wt[k] = t < 0 ? 0 : (t > 1 ? 1 : t);
     Fth[k] = gridAt(Ftab, Th[k]) - gridAt(Ftab, 25);
     if (k > 0) kc[k] = pt.stepConstants(Th[k], th[k] - th[k - 1]);
+    if (pillar) {   // :410-414
+      const double Ep = gridAt(pEtab, Th[k]), Gp = Ep / (2 * (1 + pNu));
+      Cps[3 * k] = 1 / Ep; Cps[3 * k + 1] = Cps[3 * k + 2] = 1 / Gp;
+      Fp[k] = gridAt(pFtab, Th[k]) - gridAt(pFtab, 25);
+    }
   }
   dvec Wc(cycles + 1), Ec(cycles + 1);
-  double eps[6], e25[6], e1[3], e2[3], sig[6], D[36];
+  double eps[6], e25[6], e1[3], e2[3], s1[6], s2[6], tz[3], sig[6], D[36];
   for (int q = 0; q < nsites; q++) {
     const size_t base = (size_t)q * ntemps * 6;
     dW[q] = dE[q] = stab[q] = NAN;
@@ -2052,14 +2110,22 @@ void orc_anand_screen(const double* params, const double* Etab, const double* Ft
     std::fill(Wc.begin(), Wc.end(), 0.0); std::fill(Ec.begin(), Ec.end(), 0.0);
     for (auto& v : eps) v = 0;
     for (int c = 0; c < 3; c++) { e1[c] = 0; e2[c] = 0; }
+    for (int c = 0; c < 6; c++) { s1[c] = 0; s2[c] = 0; }
     for (int k = 1; k < nsteps; k++) {
       const size_t a = base + (size_t)wi[k] * 6, b = a + 6; const double t = wt[k];
       auto lay = [&](int c) { return table[a + c] + t * (table[b + c] - table[a + c]) - e25[c]; };
-      const double ez = lay(2) - Fth[k];
-      if (k > 2 && phase[k] == phase[k - 1]) for (int r = 0; r < 3; r++) eps[IP[r]] = 2 * e1[r] - e2[r];
-      else { eps[0] -= nu * (ez - eps[2]); eps[1] -= nu * (ez - eps[2]); }
-      eps[2] = ez; eps[4] = lay(4); eps[5] = lay(5);
-      pt.stepColumn(eps, Th[k], kc[k].dt, sig, D, &kc[k]);
+      if (pillar) {
+        tz[0] = lay(2) - fs * Fth[k] - (1 - fs) * Fp[k]; tz[1] = lay(4); tz[2] = lay(5);
+        if (k > 2 && phase[k] == phase[k - 1]) for (int c = 0; c < 6; c++) eps[c] = 2 * s1[c] - s2[c];
+        pt.stepSeriesColumn(eps, tz, fs, Cps.data() + 3 * k, Th[k], kc[k].dt, sig, D, &kc[k]);
+        for (int c = 0; c < 6; c++) { s2[c] = s1[c]; s1[c] = eps[c]; }
+      } else {
+        const double ez = lay(2) - Fth[k];
+        if (k > 2 && phase[k] == phase[k - 1]) for (int r = 0; r < 3; r++) eps[IP[r]] = 2 * e1[r] - e2[r];
+        else { eps[0] -= nu * (ez - eps[2]); eps[1] -= nu * (ez - eps[2]); }
+        eps[2] = ez; eps[4] = lay(4); eps[5] = lay(5);
+        pt.stepColumn(eps, Th[k], kc[k].dt, sig, D, &kc[k]);
+      }
       pt.commit();
       for (int r = 0; r < 3; r++) { e2[r] = e1[r]; e1[r] = eps[IP[r]]; }
       const int cyc = cycle[k];
@@ -2072,7 +2138,25 @@ void orc_anand_screen(const double* params, const double* Etab, const double* Ft
   }
 }
 
-// strain increments of the last assembled step at np points (element, natural coordinates)
+void orc_anand_screen(const double* params, const double* Etab, const double* Ftab,
+                      int nsites, int ntemps, const double* temps, const double* table,
+                      int nsteps, const double* th, const double* Th, const int* cycle, const int* phase, int cycles,
+                      double* dW, double* dE, double* stab) {
+  screenLoop(params, Etab, Ftab, nsites, ntemps, temps, table, nsteps, th, Th, cycle, phase, cycles, 1, 0, nullptr, nullptr, dW, dE, stab);
+}
+
+// screenDdi's joints: a solder cap of height fraction fs on an elastic pillar (pillar Poisson
+// ratio pNu, E and thermal strain tables pEtab, pFtab on the 1 degC grid)
+void orc_anand_screen_pillar(const double* params, const double* Etab, const double* Ftab,
+                             int nsites, int ntemps, const double* temps, const double* table,
+                             int nsteps, const double* th, const double* Th, const int* cycle, const int* phase, int cycles,
+                             double fs, double pNu, const double* pEtab, const double* pFtab,
+                             double* dW, double* dE, double* stab) {
+  screenLoop(params, Etab, Ftab, nsites, ntemps, temps, table, nsteps, th, Th, cycle, phase, cycles, fs, pNu, pEtab, pFtab, dW, dE, stab);
+}
+
+// ---- element DOF histories and post-processing readers ----------------------------------------
+// Model.accumulateStep (qOnly) over nel elements for the last assembled step
 void orc_accumulate_q(orc_model* o, const double* du, int nel, const int* elems, double* q) {
   for (int t = 0; t < nel; t++) accumulateQ(o->M, du, elems[t], q + 33 * (size_t)t);
 }

@@ -6,6 +6,7 @@
 //   stepConstants        :61-65
 //   AnandPoint.step      :67-143   backward-Euler J2 radial return, consistent tangent
 //   stepColumn           :153-166  in-plane stresses of a free-standing column held at zero
+//   stepSeriesColumn     :178-206  solder cap in series with an elastic pillar (screenDdi, :369-376)
 //   _dsdd                :209-218
 //   screenJoints loop    :395-451  strain interpolation, in-plane guesses, per-cycle W and ebar
 // Compiled without fused multiply-add, like the reference's JavaScript arithmetic.
@@ -186,17 +187,78 @@ __device__ double step_column(const AnandConst& P, Point& pt, double* eps, const
   return d;
 }
 
+// stepSeriesColumn (13-fatigue.js:178-206): the cap (height fraction fs) and a pillar of
+// compliances Cp carry the same axial and shear stresses; tz = the prescribed column-average
+// (zz, yz, zx) mechanical strains; the cap's in-plane stresses vanish. Newton on the cap's six
+// strains, the 6x6 system by Gaussian elimination with partial pivoting.
+__device__ double step_series_column(const AnandConst& P, Point& pt, double* eps, const double* tz, double fs, const double* Cp,
+                                     double E, const StepK& k, double* sig, double* D) {
+  const int Pi[3] = {0, 1, 3}, Z[3] = {2, 4, 5}, ord[6] = {0, 1, 3, 2, 4, 5};
+  const double fp = 1 - fs;
+  double J[36], R[6];
+  double d = 0;
+  for (int it = 0; it < COLUMN_NEWTON_MAXIT; it++) {
+    d = anand_step(P, pt, eps, k, sig, D, true);
+    for (int r = 0; r < 3; r++) {
+      R[r] = sig[Pi[r]];
+      R[3 + r] = fs * eps[Z[r]] + fp * Cp[r] * sig[Z[r]] - tz[r];
+    }
+    const double ref = fmax(fmax(1.0, fabs(sig[2])), fmax(fabs(sig[4]), fabs(sig[5])));
+    double worst = 0;
+    for (int r = 0; r < 3; r++) worst = fmax(fmax(worst, fabs(R[r])), fabs(R[3 + r]) * E);
+    if (worst < COLUMN_STRESS_TOL * ref) break;
+    for (int r = 0; r < 6; r++)
+      for (int c = 0; c < 6; c++) {
+        const double Dv = D[6 * ord[r] + ord[c]];
+        J[6 * r + c] = r < 3 ? Dv : fp * Cp[r - 3] * Dv + (ord[r] == ord[c] ? fs : 0);
+      }
+    for (int c = 0; c < 6; c++) {
+      int pr = c;
+      for (int r = c + 1; r < 6; r++) if (fabs(J[6 * r + c]) > fabs(J[6 * pr + c])) pr = r;
+      if (pr != c) {
+        for (int q = 0; q < 6; q++) { const double t = J[6 * c + q]; J[6 * c + q] = J[6 * pr + q]; J[6 * pr + q] = t; }
+        const double t = R[c]; R[c] = R[pr]; R[pr] = t;
+      }
+      const double piv = J[7 * c];
+      for (int r = c + 1; r < 6; r++) {
+        const double f = J[6 * r + c] / piv;
+        if (f == 0) continue;
+        for (int q = c; q < 6; q++) J[6 * r + q] -= f * J[6 * c + q];
+        R[r] -= f * R[c];
+      }
+    }
+    for (int c = 5; c >= 0; c--) {
+      double v = R[c];
+      for (int q = c + 1; q < 6; q++) v -= J[6 * c + q] * R[q];
+      R[c] = v / J[7 * c];
+    }
+    for (int c = 0; c < 6; c++) eps[ord[c]] -= R[c];
+  }
+  return d;
+}
+
+// an elastic pillar under the solder cap: cap height fraction, per-step pillar compliances
+// (1/E_p, 1/G_p, 1/G_p) and thermal strains, and the solder's E table (for the residual scale)
+struct PillarArgs {
+  double fs;
+  const double* Cps;
+  const double* Fp;
+  const double* Etab;
+};
+
 __device__ void commit(Point& pt) {
   for (int i = 0; i < 6; i++) pt.ep[i] = pt.tr_ep[i];
   pt.s = pt.tr_s; pt.ebar = pt.tr_ebar; pt.W = pt.tr_W; pt.sigEq = pt.tr_sigEq;
 }
 
-// screenJoints per-site loop (13-fatigue.js:416-451), thread per site
+// screenJoints per-site loop (13-fatigue.js:416-451), thread per site; SERIES: the joints are
+// solder caps on elastic pillars (stepSeriesColumn), else free-standing columns (stepColumn)
+template <bool SERIES>
 __global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const double* __restrict__ table, int nsteps,
                          const int* __restrict__ wi, const double* __restrict__ wt, const double* __restrict__ Fth,
                          const StepK* __restrict__ kc, const double* __restrict__ Th, const int* __restrict__ cycle,
                          const int* __restrict__ phase, int cycles, double* __restrict__ dW, double* __restrict__ dE,
-                         double* __restrict__ stab) {
+                         double* __restrict__ stab, PillarArgs pil) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nsites) return;
   const double* tab = table + (size_t)q * ntemps * 6;
@@ -205,6 +267,7 @@ __global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const do
   for (int i = 0; i < 6; i++) pt.ep[i] = 0;
   pt.s = P.s0; pt.ebar = 0; pt.W = 0; pt.sigEq = 0; pt.lastD = 0;
   double e25[6], eps[6] = {0, 0, 0, 0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0}, sig[6], D[36];
+  double s1[6] = {0, 0, 0, 0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
   for (int c = 0; c < 6; c++) e25[c] = i25 >= 0 ? tab[i25 * 6 + c] : 0;
   const int IP[3] = {0, 1, 3};
   const double nu = P.nu;
@@ -214,17 +277,30 @@ __global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const do
     const double* a = tab + wi[k] * 6;
     const double* b = a + 6;
     const double t = wt[k];
-    const double ez = a[2] + t * (b[2] - a[2]) - e25[2] - Fth[k];
-    if (k > 2 && phase[k] == phase[k - 1]) {
-      for (int r = 0; r < 3; r++) eps[IP[r]] = 2 * e1[r] - e2[r];
+    if (SERIES) {
+      // column-average mechanical strain: the layer strain less the thermal strains of cap and pillar
+      const double fs = pil.fs;
+      double tz[3];
+      tz[0] = a[2] + t * (b[2] - a[2]) - e25[2] - fs * Fth[k] - (1 - fs) * pil.Fp[k];
+      tz[1] = a[4] + t * (b[4] - a[4]) - e25[4];
+      tz[2] = a[5] + t * (b[5] - a[5]) - e25[5];
+      if (k > 2 && phase[k] == phase[k - 1])
+        for (int c = 0; c < 6; c++) eps[c] = 2 * s1[c] - s2[c];
+      step_series_column(P, pt, eps, tz, fs, pil.Cps + 3 * k, grid_at(pil.Etab, Th[k]), kc[k], sig, D);
+      for (int c = 0; c < 6; c++) { s2[c] = s1[c]; s1[c] = eps[c]; }
     } else {
-      eps[0] -= nu * (ez - eps[2]);
-      eps[1] -= nu * (ez - eps[2]);
+      const double ez = a[2] + t * (b[2] - a[2]) - e25[2] - Fth[k];
+      if (k > 2 && phase[k] == phase[k - 1]) {
+        for (int r = 0; r < 3; r++) eps[IP[r]] = 2 * e1[r] - e2[r];
+      } else {
+        eps[0] -= nu * (ez - eps[2]);
+        eps[1] -= nu * (ez - eps[2]);
+      }
+      eps[2] = ez;
+      eps[4] = a[4] + t * (b[4] - a[4]) - e25[4];
+      eps[5] = a[5] + t * (b[5] - a[5]) - e25[5];
+      step_column(P, pt, eps, kc[k], sig, D);
     }
-    eps[2] = ez;
-    eps[4] = a[4] + t * (b[4] - a[4]) - e25[4];
-    eps[5] = a[5] + t * (b[5] - a[5]) - e25[5];
-    step_column(P, pt, eps, kc[k], sig, D);
     commit(pt);
     for (int r = 0; r < 3; r++) { e2[r] = e1[r]; e1[r] = eps[IP[r]]; }
     const int cyc = cycle[k];
@@ -281,8 +357,10 @@ double grid_at_host(const double* arr, double T) {
 
 void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps, const double* table_d, int nsteps,
                          const double* t_h, const double* T_h, const int* cycle_h, const int* phase_h, int cycles, double* dW_d,
-                         double* dE_d, double* stab_d, cudaStream_t s) {
+                         double* dE_d, double* stab_d, cudaStream_t s, const tm_pillar* pillar) {
   if (nsteps < 2 || ntemps < 2 || cycles < 1) fail(TM_BAD_INPUT, "anand screening: need >= 2 time steps, >= 2 temperatures, >= 1 cycle");
+  if (pillar && (!(pillar->fs > 0 && pillar->fs <= 1) || !pillar->Etab || !pillar->Ftab))
+    fail(TM_BAD_INPUT, "anand screening: the pillar needs a solder fraction in (0, 1] and its E and thermal strain tables");
   for (int k = 0; k < nsteps; k++)
     if (cycle_h[k] < 0 || cycle_h[k] > cycles) fail(TM_BAD_INPUT, "anand screening: cycle index out of range");
   int i25 = -1;
@@ -304,8 +382,19 @@ void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, c
     wt[k] = tt < 0 ? 0 : (tt > 1 ? 1 : tt);
     Fth[k] = grid_at_host(mat.Ftab, T_h[k]) - grid_at_host(mat.Ftab, 25);
   }
+  // a pillar in series: its compliances and thermal strain at every step (13-fatigue.js:410-414)
+  std::vector<double> Cps, Fp;
+  if (pillar) {
+    Cps.resize(3 * (size_t)nsteps); Fp.resize(nsteps);
+    for (int k = 0; k < nsteps; k++) {
+      const double Ep = grid_at_host(pillar->Etab, T_h[k]), Gp = Ep / (2 * (1 + pillar->nu));
+      if (!(Ep > 0) || !std::isfinite(Gp)) fail(TM_BAD_INPUT, "anand screening: pillar modulus must be positive");
+      Cps[3 * k] = 1 / Ep; Cps[3 * k + 1] = Cps[3 * k + 2] = 1 / Gp;
+      Fp[k] = grid_at_host(pillar->Ftab, T_h[k]) - grid_at_host(pillar->Ftab, 25);
+    }
+  }
   DBuf<int> d_wi, d_cycle, d_phase;
-  DBuf<double> d_wt, d_Fth, d_t, d_T, d_E;
+  DBuf<double> d_wt, d_Fth, d_t, d_T, d_E, d_Cps, d_Fp;
   DBuf<StepK> d_kc;
   d_wi.upload(wi, s); d_wt.upload(wt, s); d_Fth.upload(Fth, s);
   d_cycle.upload(cycle_h, nsteps, s); d_phase.upload(phase_h, nsteps, s);
@@ -313,8 +402,16 @@ void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, c
   d_kc.alloc(nsteps);
   const AnandConst P = to_const(mat);
   k_step_constants<<<(nsteps + 127) / 128, 128, 0, s>>>(P, d_E.p, nsteps, d_t.p, d_T.p, d_kc.p);
-  k_screen<<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_d, nsteps, d_wi.p, d_wt.p, d_Fth.p, d_kc.p, d_T.p, d_cycle.p,
-                                            d_phase.p, cycles, dW_d, dE_d, stab_d);
+  if (pillar) {
+    d_Cps.upload(Cps, s); d_Fp.upload(Fp, s);
+    const PillarArgs pa{pillar->fs, d_Cps.p, d_Fp.p, d_E.p};
+    k_screen<true><<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_d, nsteps, d_wi.p, d_wt.p, d_Fth.p, d_kc.p, d_T.p,
+                                                    d_cycle.p, d_phase.p, cycles, dW_d, dE_d, stab_d, pa);
+  } else {
+    k_screen<false><<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_d, nsteps, d_wi.p, d_wt.p, d_Fth.p, d_kc.p, d_T.p,
+                                                     d_cycle.p, d_phase.p, cycles, dW_d, dE_d, stab_d, PillarArgs{1, nullptr, nullptr, nullptr});
+  }
+  note_launch(2);
   TM_CUDA_CHECK(cudaGetLastError());
   TM_CUDA_CHECK(cudaStreamSynchronize(s));
 }
@@ -323,6 +420,7 @@ void anand_step_device(const tm_anand_material& mat, int npts, double* state_d, 
                        double* D_d, int commitFlag, cudaStream_t s) {
   DBuf<double> d_E;
   d_E.upload(mat.Etab, TGRID_N, s);
+  note_launch();
   k_point_step<<<(npts + 127) / 128, 128, 0, s>>>(to_const(mat), d_E.p, npts, state_d, eps_d, T, dt, sig_d, D_d, commitFlag);
   TM_CUDA_CHECK(cudaGetLastError());
   TM_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -437,8 +535,8 @@ extern "C" tm_status tm_anand_screen_noalloc(const tm_anand_material* mat, int32
     const AnandConst P = to_const(*mat);
     k_step_constants<<<(nsteps + 127) / 128, 128, 0, s>>>(P, Et, nsteps, tt, Tk, kc);
     k_step_weights<<<(nsteps + 127) / 128, 128, 0, s>>>(nsteps, ntemps, tmp, Tk, Ft, wi, wt, Fth);
-    k_screen<<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_dev, nsteps, wi, wt, Fth, kc, Tk, cyc, ph, cycles, dW_dev,
-                                              dE_dev, stab_dev);
+    k_screen<false><<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_dev, nsteps, wi, wt, Fth, kc, Tk, cyc, ph, cycles,
+                                                     dW_dev, dE_dev, stab_dev, PillarArgs{1, nullptr, nullptr, nullptr});
     note_launch(3);
     TM_CUDA_CHECK(cudaGetLastError());
     TM_CUDA_CHECK(cudaStreamSynchronize(s));

@@ -879,6 +879,35 @@ tm_status tm_anand_screen(const tm_anand_material* mat, int32_t nsites, int32_t 
   });
 }
 
+tm_status tm_anand_screen_pillar_device(const tm_anand_material* mat, const tm_pillar* pillar, int32_t nsites, int32_t ntemps,
+                                        const double* temps, const double* table_dev, int32_t nsteps, const double* t, const double* T,
+                                        const int32_t* cycle, const int32_t* phase, int32_t cycles, double* dW, double* dE,
+                                        double* stab) {
+  return guarded([&] {
+    require_device();
+    if (!mat || !pillar) fail(TM_BAD_INPUT, "null argument");
+    if (nsites <= 0) return;
+    anand_screen_device(*mat, nsites, ntemps, temps, table_dev, nsteps, t, T, cycle, phase, cycles, dW, dE, stab, nullptr, pillar);
+  });
+}
+
+tm_status tm_anand_screen_pillar(const tm_anand_material* mat, const tm_pillar* pillar, int32_t nsites, int32_t ntemps,
+                                 const double* temps, const double* table, int32_t nsteps, const double* t, const double* T,
+                                 const int32_t* cycle, const int32_t* phase, int32_t cycles, double* dW, double* dE, double* stab) {
+  return guarded([&] {
+    require_device();
+    if (!mat || !pillar) fail(TM_BAD_INPUT, "null argument");
+    if (nsites <= 0) return;
+    DBuf<double> d_tab, d_dW, d_dE, d_st;
+    d_tab.upload(table, (size_t)nsites * ntemps * 6, nullptr);
+    d_dW.alloc(nsites); d_dE.alloc(nsites); d_st.alloc(nsites);
+    anand_screen_device(*mat, nsites, ntemps, temps, d_tab.p, nsteps, t, T, cycle, phase, cycles, d_dW.p, d_dE.p, d_st.p, nullptr,
+                        pillar);
+    d_dW.download(dW, nsites, nullptr); d_dE.download(dE, nsites, nullptr); d_st.download(stab, nsites, nullptr);
+    TM_CUDA_CHECK(cudaDeviceSynchronize());
+  });
+}
+
 tm_status tm_anand_step(const tm_anand_material* mat, int32_t npts, double* state, const double* eps, double T, double dt, double* sig,
                         double* D, int32_t commit) {
   return guarded([&] {

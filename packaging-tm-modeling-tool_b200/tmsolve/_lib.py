@@ -20,7 +20,8 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_sizes", "tm_destroy", "tm_last_error", "tm_solve_device", "tm_matvec_device", "tm_anand_screen",
             "tm_anand_screen_device", "tm_anand_step", "tm_set_stream", "tm_launch_count", "tm_kernel_timer",
             "tm_kernel_timer_read", "tm_assemble_step_device", "tm_prepare_step", "tm_accumulate_q", "tm_accumulate_q_device",
-            "tm_element_strains", "tm_element_strains_device", "tm_sample_plane", "tm_sample_plane_device"]
+            "tm_element_strains", "tm_element_strains_device", "tm_sample_plane", "tm_sample_plane_device",
+            "tm_anand_screen_pillar", "tm_anand_screen_pillar_device"]
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
 
 dp = C.POINTER(C.c_double)
@@ -62,6 +63,10 @@ class TmAnandMaterial(C.Structure):
                 ("Etab", dp), ("Ftab", dp)]
 
 
+class TmPillar(C.Structure):
+    _fields_ = [("fs", C.c_double), ("nu", C.c_double), ("Etab", dp), ("Ftab", dp)]
+
+
 _lib = None
 
 
@@ -92,6 +97,8 @@ def load():
     L.tm_anand_screen.argtypes = [C.POINTER(TmAnandMaterial), C.c_int32, C.c_int32, vp, vp, C.c_int32, vp, vp, vp, vp,
                                   C.c_int32, vp, vp, vp]
     L.tm_anand_screen_device.argtypes = L.tm_anand_screen.argtypes
+    L.tm_anand_screen_pillar.argtypes = [C.POINTER(TmAnandMaterial), C.POINTER(TmPillar)] + L.tm_anand_screen.argtypes[1:]
+    L.tm_anand_screen_pillar_device.argtypes = L.tm_anand_screen_pillar.argtypes
     L.tm_anand_screen_noalloc.argtypes = L.tm_anand_screen.argtypes + [vp]
     L.tm_anand_screen_noalloc.restype = C.c_int32
     L.tm_anand_step.argtypes = [C.POINTER(TmAnandMaterial), C.c_int32, vp, vp, C.c_double, C.c_double, vp, vp, C.c_int32]

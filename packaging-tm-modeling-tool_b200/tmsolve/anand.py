@@ -17,7 +17,7 @@ import math
 
 import numpy as np
 
-from ._lib import TmAnandMaterial, check, load
+from ._lib import TmAnandMaterial, TmPillar, check, load
 
 RAMP_MAX_DT = 5        # 00-constants.js:111
 DWELL_MIN_STEPS = 10   # 00-constants.js:112
@@ -94,6 +94,25 @@ def screen(params: dict, Etab, Ftab, temps, table, hist) -> tuple:
     vp = lambda a: a.ctypes.data_as(C.c_void_p)
     check(load().tm_anand_screen(C.byref(m), ns, len(temps), vp(temps), vp(table), len(t), vp(t), vp(T), vp(cyc), vp(ph),
                                  int(hist["cycles"]), vp(dW), vp(dE), vp(stab)))
+    return dW, dE, stab
+
+
+def screen_pillar(params: dict, Etab, Ftab, temps, table, hist, fs: float, pillar_nu: float, pEtab, pFtab) -> tuple:
+    """dW, dE, stab per site for joints that are a solder cap (height fraction fs) on an elastic
+    pillar (E table pEtab, Poisson ratio pillar_nu, thermal strain table pFtab): screenDdi's
+    loop with AnandPoint.stepSeriesColumn (13-fatigue.js:178-206, 369-376), on the GPU."""
+    m, keep = material(params, Etab, Ftab)
+    pE = np.ascontiguousarray(pEtab, np.float64); pF = np.ascontiguousarray(pFtab, np.float64)
+    pil = TmPillar(fs=float(fs), nu=float(pillar_nu), Etab=pE.ctypes.data_as(C.POINTER(C.c_double)),
+                   Ftab=pF.ctypes.data_as(C.POINTER(C.c_double)))
+    temps = np.ascontiguousarray(temps, np.float64); table = np.ascontiguousarray(table, np.float64)
+    ns = table.size // (6 * len(temps))
+    t = np.ascontiguousarray(hist["t"], np.float64); T = np.ascontiguousarray(hist["T"], np.float64)
+    cyc = np.ascontiguousarray(hist["cycle"], np.int32); ph = np.ascontiguousarray(hist["phase"], np.int32)
+    dW = np.zeros(ns); dE = np.zeros(ns); stab = np.zeros(ns)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    check(load().tm_anand_screen_pillar(C.byref(m), C.byref(pil), ns, len(temps), vp(temps), vp(table), len(t), vp(t), vp(T),
+                                        vp(cyc), vp(ph), int(hist["cycles"]), vp(dW), vp(dE), vp(stab)))
     return dW, dE, stab
 
 

@@ -201,3 +201,12 @@ def sac305_tables():
 def anand_params_array(p: dict) -> np.ndarray:
     """Parameter vector (A, Q/R, xi, m, s_hat, n, h0, a, s0, nu) of the Anand entry points."""
     return np.array([p["A"], p["QR"], p["xi"], p["m"], p["shat"], p["n"], p["h0"], p["a"], p["s0"], p["nu"]], np.float64)
+
+
+def elastic_tables(E_T, E_MPa, cte: float):
+    """E(T) (MPa, linear table with linear extrapolation) and F(T) = cte (T - 25) on the 1 degC
+    grid, for an elastic material such as a Cu pillar."""
+    Et = grid_table(lambda T: interp_table_linear(E_T, E_MPa, T))
+    Ft = grid_table(lambda T: cte * (T - T_STRAIN_ORIGIN))
+    return Et, Ft
+

@@ -4,8 +4,8 @@ history, FP64 on both sides)."""
 import numpy as np
 import pytest
 
-from tmsolve.anand import cycle_history, cycling_temps, point_step, screen, synthetic_strain_table
-from tmsolve.materials import SAC305, anand_params_array, sac305_tables
+from tmsolve.anand import cycle_history, cycling_temps, point_step, screen, screen_pillar, synthetic_strain_table
+from tmsolve.materials import SAC305, anand_params_array, elastic_tables, sac305_tables
 
 pytestmark = pytest.mark.gpu
 
@@ -24,6 +24,26 @@ def test_screen_parity(oracle_lib):
     assert np.all(oW[ok] > 0)
     assert np.allclose(dW[ok], oW[ok], rtol=1e-8, atol=0)
     assert np.allclose(dE[ok], oE[ok], rtol=1e-8, atol=0)
+
+
+def test_screen_pillar_parity(oracle_lib):
+    """DDI joints: solder caps (fs = 0.4) on Cu pillars (stepSeriesColumn)."""
+    Et, Ft = sac305_tables()
+    pE, pF = elastic_tables([-40.0, 125.0], [120000.0, 114000.0], 17e-6)
+    hist = cycle_history(-40.0, 125.0, 11.0, 15.0, 3)
+    temps = cycling_temps(-40.0, 125.0)
+    table, x, y = synthetic_strain_table(64, temps, seed=11)
+    table = table.ravel()
+    table[6 * len(temps) * 3] = np.nan
+    dW, dE, stab = screen_pillar(SAC305, Et, Ft, temps, table, hist, 0.4, 0.34, pE, pF)
+    oW, oE, ostab = oracle_lib.anand_screen_pillar(anand_params_array(SAC305), Et, Ft, temps, table, hist, 0.4, 0.34, pE, pF)
+    assert np.isnan(dW[3]) and np.isnan(oW[3])
+    ok = np.isfinite(oW)
+    assert np.all(oW[ok] > 0)
+    assert np.allclose(dW[ok], oW[ok], rtol=1e-8, atol=0)
+    assert np.allclose(dE[ok], oE[ok], rtol=1e-8, atol=0)
+    with pytest.raises(Exception):
+        screen_pillar(SAC305, Et, Ft, temps, table, hist, 0.0, 0.34, pE, pF)
 
 
 def test_point_step_parity(oracle_lib):

@@ -162,3 +162,29 @@ def test_anand_series_elastic_limit(oracle_lib):
     E = Et[25 + 80]; nu = SAC305["nu"]
     Del = iso_d(E, nu, nu_max=0.499).reshape(6, 6)
     assert np.allclose(sig, Del @ eps, rtol=1e-6, atol=1e-9)
+
+
+def test_series_column_limits(oracle_lib):
+    """stepSeriesColumn (13-fatigue.js:178-206) in its two limits: with no pillar (fs = 1) it is
+    the free-standing column of stepColumn (to the column Newton tolerance, 1e-3 of the axial
+    stress); on a rigid pillar with no thermal strain the cap takes the whole column strain,
+    i.e. the column screening of the table with zz, yz, zx divided by fs."""
+    from tmsolve.anand import cycle_history, cycling_temps, synthetic_strain_table
+    from tmsolve.materials import elastic_tables
+    Et, Ft = sac305_tables()
+    P = anand_params_array(SAC305)
+    hist = cycle_history(-40.0, 125.0, 11.0, 15.0, 3)
+    temps = cycling_temps(-40.0, 125.0)
+    table, _, _ = synthetic_strain_table(16, temps)
+    table = table.ravel()
+    dW, dE, _ = oracle_lib.anand_screen(P, Et, Ft, temps, table, hist)
+    pE, pF = elastic_tables([-40.0, 125.0], [120000.0, 114000.0], 17e-6)
+    W1, E1, _ = oracle_lib.anand_screen_pillar(P, Et, Ft, temps, table, hist, 1.0, 0.34, pE, pF)
+    assert np.allclose(W1, dW, rtol=1e-3, atol=0) and np.allclose(E1, dE, rtol=1e-3, atol=0)
+    fs = 0.4
+    W2, E2, _ = oracle_lib.anand_screen_pillar(P, Et, Ft, temps, table, hist, fs, 0.34, np.full(381, 1e13), np.zeros(381))
+    t2 = table.reshape(-1, len(temps), 6).copy()
+    t2[:, :, [2, 4, 5]] /= fs
+    W3, E3, _ = oracle_lib.anand_screen(P, Et, Ft, temps, t2.ravel(), hist)
+    assert np.allclose(W2, W3, rtol=1e-6, atol=0) and np.allclose(E2, E3, rtol=1e-6, atol=0)
+
