@@ -104,7 +104,8 @@ typedef struct {
 } tm_step;
 
 #define TM_PC_MG 0
-#define TM_PC_JACOBI 1
+#define TM_PC_JACOBI 1       /* diagonal scaling only (no counterpart in the reference; a baseline) */
+#define TM_PC_IC 2           /* IC(0) with Manteuffel shift (ICPC, src/core/10-solver.js:741-800) */
 #define TM_PREC_FP64 0       /* everything in FP64 */
 #define TM_PREC_MIXED 1      /* FP64 PCG (apply, residuals, dots); the whole V-cycle in FP32 except the FP64 coarsest solve */
 #define TM_PREC_MIXED_IR 2   /* FP64 iterative refinement of an FP32 MG-PCG (FP32 apply and V-cycle); on a sweep that
@@ -114,7 +115,8 @@ typedef struct {
   double tol;                    /* relative residual in the scaled 2-norm (PCG_TOL 1e-8) */
   int32_t maxit;                 /* PCG_MAXIT 2000 */
   int32_t warm;                  /* stored solutions for the warm start (WARM_START_MAX 20), 0 = off */
-  int32_t precond;               /* TM_PC_MG or TM_PC_JACOBI */
+  int32_t precond;               /* preferred kind: TM_PC_MG, TM_PC_IC or TM_PC_JACOBI; a run that fails after a
+                                    rebuild falls back once to the other kind (MG <-> IC, 10-solver.js:967-976) */
   int32_t precision;             /* TM_PREC_FP64, TM_PREC_MIXED or TM_PREC_MIXED_IR */
   int64_t key;                   /* preconditioner key (solve(f, label, key)); -1 = none */
   void (*progress)(void* user, int32_t it, double relres);  /* called between iterations, may be NULL */
@@ -136,6 +138,10 @@ typedef struct {
   int32_t levels;                /* multigrid levels */
   int32_t status;
   int32_t refinements;           /* mixed precision: outer FP64 refinement sweeps */
+  int32_t precond;               /* kind of the preconditioner the solve ended with (rec.precond) */
+  int32_t fallback_first;        /* with fallback: the kind that failed, its iterations and residual */
+  int32_t fallback_iters;
+  double fallback_relres;
 } tm_solve_info;
 
 /* Library defaults for tm_solve_opts (the reference's CONST values). */
@@ -176,6 +182,10 @@ int32_t tm_last_error(char* buf, size_t len);
 tm_status tm_assemble_step_device(tm_ctx* ctx, const tm_step* step, double* rhs_dev);
 tm_status tm_solve_device(tm_ctx* ctx, const double* f_dev, double* u_dev, const tm_solve_opts* opts, tm_solve_info* info);
 tm_status tm_matvec_device(tm_ctx* ctx, const double* x_dev, double* y_dev);
+/* z = M^-1 r with the preconditioner the last solve built, in the solver's scaled space (the
+ * reference's pc.apply(r, z), e.g. ICPC.apply, src/core/10-solver.js:784-798). */
+tm_status tm_pc_apply(tm_ctx* ctx, const double* r, double* z);
+tm_status tm_pc_apply_device(tm_ctx* ctx, const double* r_dev, double* z_dev);
 
 /* ---- element DOF histories at screening sites ---- */
 /* Loads the per-step data that the DOF histories read (the shape matrices of every property set

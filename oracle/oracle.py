@@ -69,6 +69,7 @@ def lib():
     L.orc_sample_plane.restype = C.c_double
     L.orc_sample_plane.argtypes = [vp, _dp, C.c_int, C.c_int, C.c_double, C.c_double]
     L.orc_warpage_jeita.argtypes = [vp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+    L.orc_pc_apply.argtypes = [vp, _dp, _dp]
     L.orc_last_error.restype = C.c_char_p
     L.orc_last_error.argtypes = [vp]
     _lib = L
@@ -151,6 +152,13 @@ class OracleModel:
         rec["precond"] = "mg" if info[6] == 0 else "ic"
         rec["u"] = u
         return rec
+
+    def pc_apply(self, r):
+        """pc.apply of the preconditioner the last solve built (scaled space)."""
+        z = np.zeros(self.ndof)
+        if lib().orc_pc_apply(self.h, np.ascontiguousarray(r, np.float64), z):
+            raise RuntimeError("no preconditioner built")
+        return z
 
     def clear_warm(self):
         lib().orc_clear_warm(self.h)

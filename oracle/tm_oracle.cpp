@@ -1986,6 +1986,13 @@ int orc_solve(orc_model* o, const double* f, double* u, double tol, int maxit, i
 
 void orc_clear_warm(orc_model* o) { o->solver->basis.clear(); }
 
+// pc.apply(r, z) of the preconditioner the last solve built (scaled space); 1 when none
+int orc_pc_apply(orc_model* o, const double* r, double* z) {
+  if (!o->solver->pc) return 1;
+  o->solver->pc->apply(r, z);
+  return 0;
+}
+
 // MG level sizes after a solve: per level (nx, ny, nn, b)
 int orc_mg_levels(orc_model* o, int* out, int cap) {
   auto* mg = dynamic_cast<MultigridPC*>(o->solver->pc.get());

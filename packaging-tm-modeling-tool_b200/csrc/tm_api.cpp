@@ -7,8 +7,8 @@
 //   _pcg             :1001-1042 PCG on the scaled system with constrained DOFs zeroed in r and z
 //   _warmStart       :885-915   Galerkin projection on <= 20 stored solutions
 //   _storeSolution   :917-926   two-pass Gram-Schmidt
-// The IC(0) fallback of the reference (:967-976, ICPC :741-800) has no device implementation:
-// a solve whose multigrid run fails after the rebuild returns TM_NOT_CONVERGED.
+//   fallback         :967-976   after a failed rebuild, one more run with the other kind (MG <-> IC(0),
+//                               ICPC on the device in tm_ic0.cu), then the preferred kind again
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -76,10 +76,18 @@ void require_device() {
   if (prop.major < 10) fail(TM_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100: this library is built for B200 (sm_100a) only");
 }
 
-// numeric multigrid set-up for the current scaled operator (MultigridPC constructor / update)
-double build_pc(Context& c, bool mg) {
+// numeric set-up of a preconditioner for the current scaled operator (_buildPC, 10-solver.js:868-882):
+// MultigridPC constructor / update, ICPC, or nothing for Jacobi (the scaled operator's diagonal is 1)
+double build_pc(Context& c, int kind) {
   const double t0 = now_ms();
-  if (!mg) { c.pcReady = true; return now_ms() - t0; }
+  c.pcKind = kind;
+  if (kind == TM_PC_JACOBI) { c.pcReady = true; c.needRebuild = false; return now_ms() - t0; }
+  if (kind == TM_PC_IC) {
+    build_ic(c);
+    c.pcReady = true;
+    c.needRebuild = false;
+    return now_ms() - t0;
+  }
   c.d_jitter.zero(c.stream);
   launch_factor_columns(c);
   launch_w01(c);
@@ -99,9 +107,11 @@ double build_pc(Context& c, bool mg) {
   return now_ms() - t0;
 }
 
-void precondition(Context& c, bool mg, const double* r, double* z) {
+void precondition(Context& c, int kind, const double* r, double* z) {
   const size_t n = 3 * (size_t)c.nn;
-  if (mg && c.mgFp32) {
+  const bool mg = kind == TM_PC_MG;
+  if (kind == TM_PC_IC) launch_ic_apply(c, r, z);
+  else if (mg && c.mgFp32) {
     // FP32 V-cycle (operators, column factors, transfers and smoothing in FP32; coarsest FP64)
     launch_d2f(c, r, c.d_r32.p, n);
     launch_vcycle32(c, c.d_r32.p, c.d_z32.p);
@@ -126,7 +136,7 @@ struct PcgResult {
 };
 
 // _pcg (10-solver.js:1001-1042); device scalars: 0 rz, 1 pq, 2 alpha, 3 r.r, 4 rz2, 5 beta
-PcgResult pcg(Context& c, bool mg, const double* b, double* x, double tol, int maxit, double perDecade, const tm_solve_opts& o) {
+PcgResult pcg(Context& c, int kind, const double* b, double* x, double tol, int maxit, double perDecade, const tm_solve_opts& o) {
   const size_t n = 3 * (size_t)c.nn;
   double* S = c.d_scalars.p;
   PcgResult out;
@@ -140,7 +150,7 @@ PcgResult pcg(Context& c, bool mg, const double* b, double* x, double tol, int m
   if (!std::isfinite(r0)) { out.nonfinite = true; out.relres = r0; return out; }
   if (rnorm / bnorm < tol) { out.iters = 0; out.relres = rnorm / bnorm; out.converged = true; return out; }
   if (perDecade > 0) maxit = std::min(maxit, std::max(30, (int)std::ceil(perDecade * std::log10(r0 / tol))));  // REBUILD_MIN_ITERS
-  precondition(c, mg, c.d_r.p, c.d_z.p);
+  precondition(c, kind, c.d_r.p, c.d_z.p);
   launch_zero_constrained(c, c.d_z.p);
   TM_CUDA_CHECK(cudaMemcpyAsync(c.d_p.p, c.d_z.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
   launch_dot(c, c.d_r.p, c.d_z.p, n, S + 0);
@@ -167,7 +177,7 @@ PcgResult pcg(Context& c, bool mg, const double* b, double* x, double tol, int m
     if (!std::isfinite(rnorm)) { out.nonfinite = true; break; }
     if (o.progress && o.progress_every > 0 && it % o.progress_every == 0) o.progress(o.progress_user, it, rnorm / bnorm);
     if (rnorm / bnorm < tol) { out.iters = it; out.relres = rnorm / bnorm; out.converged = true; return out; }
-    precondition(c, mg, c.d_r.p, c.d_z.p);
+    precondition(c, kind, c.d_r.p, c.d_z.p);
     launch_zero_constrained(c, c.d_z.p);
     launch_dot(c, c.d_r.p, c.d_z.p, n, S + 4);
     launch_div(c, S + 4, S + 0, S + 5, 1.0);
@@ -352,8 +362,11 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   const double t0 = now_ms();
   if (!c.assembled) fail(TM_BAD_INPUT, "tm_solve before tm_assemble_step or tm_set_bcsr");
   const size_t n = 3 * (size_t)c.nn;
-  const bool mg = o.precond == TM_PC_MG;
+  if (o.precond != TM_PC_MG && o.precond != TM_PC_JACOBI && o.precond != TM_PC_IC) fail(TM_BAD_INPUT, "unknown preconditioner kind");
+  const int kind = o.precond;
+  const bool mg = kind == TM_PC_MG;
   if (o.key != -1 && o.key != c.pcKey) c.needRebuild = true;
+  if (c.pcKind != kind) c.needRebuild = true;
   c.pcKey = o.key;
   if (!c.scaled) {
     launch_scale(c);
@@ -379,7 +392,7 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   if (mixed && !mg) fail(TM_BAD_INPUT, "mixed precision needs the multigrid preconditioner");
   c.mgFp32 = false;
   if (!c.pcReady || c.needRebuild) {
-    pcMs = build_pc(c, mg);
+    pcMs = build_pc(c, kind);
     rebuilt = true;
     if (mixed) { const double t1 = now_ms(); launch_to_fp32(c); TM_CUDA_CHECK(cudaStreamSynchronize(c.stream)); pcMs += now_ms() - t1; c.fp32Ready = true; }
   } else if (mixed && !c.fp32Ready) {
@@ -389,39 +402,49 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   warm_start(c, c.d_bs.p, c.d_x.p);
   int sweeps = 0;
   bool stalled = false;
+  PcgResult res;
+  int total = 0;
   if (o.precision == TM_PREC_MIXED_IR) {
-    PcgResult res = refine_mixed(c, c.d_bs.p, c.d_x.p, o.tol, o.maxit, &sweeps, &stalled, o);
+    res = refine_mixed(c, c.d_bs.p, c.d_x.p, o.tol, o.maxit, &sweeps, &stalled, o);
     if (stalled && !res.nonfinite) {
       c.mgFp32 = true;
-      PcgResult r2 = pcg(c, mg, c.d_bs.p, c.d_x.p, o.tol, std::max(1, o.maxit - res.iters), 0, o);
+      PcgResult r2 = pcg(c, kind, c.d_bs.p, c.d_x.p, o.tol, std::max(1, o.maxit - res.iters), 0, o);
       r2.iters += res.iters;
       r2.iters0 = res.iters0;
       res = r2;
     }
-    if (!res.converged) c.needRebuild = true;
-    launch_scale_vec(c, c.d_x.p, c.d_s.p, u_dev, false, n);
-    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
-    if (res.converged) store_solution(c, u_dev, o.warm);
-    in.iters = res.iters; in.relres = res.relres; in.iters0 = res.iters0; in.converged = res.converged;
-    in.ms = now_ms() - t0; in.pc_ms = pcMs; in.rebuilt = rebuilt; in.warm = (int)c.basis.size();
-    in.jitter_count = c.colJitter; in.refinements = sweeps;
-    check_device_error(c);
-    in.status = res.nonfinite ? TM_NONFINITE : (res.converged ? TM_OK : TM_NOT_CONVERGED);
-    if (info) *info = in;
-    if (res.nonfinite) fail(TM_NONFINITE, "non-finite value in the refinement");
-    return res.converged ? TM_OK : TM_NOT_CONVERGED;
+    total = res.iters;
+  } else {
+    c.mgFp32 = o.precision == TM_PREC_MIXED;
+    res = pcg(c, kind, c.d_bs.p, c.d_x.p, o.tol, o.maxit, rebuilt ? 0 : 2 * c.ratePerDecade, o);   // REBUILD_FACTOR 2
+    total = res.iters;
+    if (!res.converged && !rebuilt && !res.nonfinite) {
+      // stale preconditioner: rebuild the preferred kind and continue from the current iterate
+      pcMs += build_pc(c, kind);
+      rebuilt = true;
+      res = pcg(c, kind, c.d_bs.p, c.d_x.p, o.tol, o.maxit, 0, o);
+      total += res.iters;
+    }
   }
-  c.mgFp32 = o.precision == TM_PREC_MIXED;
-  PcgResult res = pcg(c, mg, c.d_bs.p, c.d_x.p, o.tol, o.maxit, rebuilt ? 0 : 2 * c.ratePerDecade, o);
-  int total = res.iters;
-  if (!res.converged && !rebuilt && !res.nonfinite) {
-    pcMs += build_pc(c, mg);
+  bool fellBack = false;
+  if (!res.converged && !res.nonfinite) {
+    // rebuild with the other kind once, keeping the current iterate (FP64 PCG), then return to the
+    // preferred kind on the next solve
+    const int first = c.pcKind, other = first == TM_PC_MG ? TM_PC_IC : TM_PC_MG;
+    in.fallback = 1;
+    in.fallback_first = first;
+    in.fallback_iters = total;
+    in.fallback_relres = res.relres;
+    pcMs += build_pc(c, other);
     rebuilt = true;
-    res = pcg(c, mg, c.d_bs.p, c.d_x.p, o.tol, o.maxit, 0, o);
+    c.mgFp32 = false;
+    res = pcg(c, other, c.d_bs.p, c.d_x.p, o.tol, o.maxit, 0, o);
     total += res.iters;
+    c.needRebuild = true;
+    fellBack = true;
   }
   if (!res.converged) c.needRebuild = true;
-  if (res.converged) {
+  if (res.converged && !fellBack) {
     const bool known = c.ratePerDecade > 0 && !rebuilt;
     if (known) { if (pcg_rate(res) > 2 * c.ratePerDecade) c.needRebuild = true; }
     else c.ratePerDecade = std::log10(res.iters0 / std::max(res.relres, 1e-300)) >= 1 ? pcg_rate(res) : 0;
@@ -431,8 +454,9 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   if (res.converged) store_solution(c, u_dev, o.warm);
   in.iters = total; in.relres = res.relres; in.iters0 = res.iters0; in.converged = res.converged;
-  in.ms = now_ms() - t0; in.pc_ms = pcMs; in.rebuilt = rebuilt; in.warm = (int)c.basis.size(); in.fallback = 0;
-  in.jitter_count = c.colJitter;
+  in.ms = now_ms() - t0; in.pc_ms = pcMs; in.rebuilt = rebuilt; in.warm = (int)c.basis.size();
+  in.jitter_count = c.colJitter; in.refinements = sweeps;
+  in.precond = c.pcKind;
   check_device_error(c);
   in.status = res.nonfinite ? TM_NONFINITE : (res.converged ? TM_OK : TM_NOT_CONVERGED);
   if (info) *info = in;
@@ -781,6 +805,30 @@ tm_status tm_sample_plane(tm_ctx* ctx, const double* u, int32_t k, int32_t comp,
     dout.alloc(npts);
     launch_sample_plane(c, c.d_tmp.p, k, comp, npts, dx.p, dy.p, dout.p);
     dout.download(out, npts, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_pc_apply_device(tm_ctx* ctx, const double* r, double* z) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!c.pcReady || c.pcKind < 0) fail(TM_BAD_INPUT, "tm_pc_apply before a solve built a preconditioner");
+    c.mgFp32 = false;
+    precondition(c, c.pcKind, r, z);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_pc_apply(tm_ctx* ctx, const double* r, double* z) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!c.pcReady || c.pcKind < 0) fail(TM_BAD_INPUT, "tm_pc_apply before a solve built a preconditioner");
+    const size_t n = 3 * (size_t)c.nn;
+    c.mgFp32 = false;
+    c.d_tmp.upload(r, n, c.stream);
+    c.d_tmp2.alloc(n);
+    precondition(c, c.pcKind, c.d_tmp.p, c.d_tmp2.p);
+    c.d_tmp2.download(z, n, c.stream);
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   });
 }

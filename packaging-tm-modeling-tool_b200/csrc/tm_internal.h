@@ -93,6 +93,24 @@ constexpr int SLOT_SELF = 13;
 constexpr int SLOT_DOWN = 12;  // (0, 0, -1): the node below in the same column
 
 // ---- multigrid shell level (6 DOFs per aggregate) ------------------------------------------
+// IC(0) of the scaled level-0 operator (ICPC, 10-solver.js:719-800): the scalar upper CSR of the
+// block pattern (rows 3i+p, columns j >= i with q >= p on the diagonal block, sorted), for every
+// entry its index into the slot-major operator, the column lists of U (rows i < c with U(i, c),
+// ascending, and the entry's position) and the node level schedules of the factorization /
+// forward solve (levels of increasing node ids) and of the backward solve
+struct IcFactor {
+  long long epoch = -1;                // structure built for this hierarchy epoch
+  int n = 0;
+  long long nnz = 0;
+  DBuf<int> d_rowPtr, d_col, d_gmap, d_tStart, d_tRow, d_tPos;
+  DBuf<int> d_fwdNodes, d_bwdNodes;
+  std::vector<int> fwdStart, bwdStart;
+  DBuf<double> d_U;
+  DBuf<int> d_fail;
+  double shift = 0;
+  bool ready = false;
+};
+
 struct ShellLevel {
   int nx = 0, ny = 0, nn = 0;          // columns nx*ny, aggregates nn
   std::vector<double> xs, ys;          // grid lines of the level's columns
@@ -180,6 +198,8 @@ struct Context {
   DBuf<double> d_psetM;                // 6*1089 per property set
   DBuf<double> d_clsF33;               // 33 per class: uncondensed element thermal load (elementFth)
   DBuf<int> d_psetLayered, d_psetBorn;
+  IcFactor ic;                         // the IC(0) preconditioner (tm_ic0.cu)
+  int pcKind = -1;                     // kind of the preconditioner built last (TM_PC_*)
   bool stepReady = false;              // shape matrices and thermal loads of an assembled step are on the device
   DBuf<int> d_conn;                    // 8*ne, uploaded on first use by the DOF-history entry points
   DBuf<double> d_xs, d_ys;             // mesh lines and the node index grid, uploaded on first use
@@ -281,6 +301,10 @@ void launch_to_fp32(Context& c);
 void launch_accumulate_q(Context& c, const double* du, int nel, const int* elems, double* q);
 void launch_element_strains(Context& c, int np, const int* elem, const double* q, const double* nat, double* eps);
 void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts, const double* x, const double* y, double* out);
+
+// ---- IC(0) (tm_ic0.cu) -------------------------------------------------------------------------
+void build_ic(Context& c);                                   // structure (once) + shifted factorization
+void launch_ic_apply(Context& c, const double* r, double* z);
 
 // ---- launch accounting ------------------------------------------------------------------------
 enum KernelId { K_APPLY0 = 0, K_SWEEP_SOLID = 1, K_SWEEP_SHELL = 2, K_ASSEMBLE = 3, K_GALERKIN01 = 4, K_APPLY_SHELL = 5, K_NKERNEL };

@@ -21,7 +21,9 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_anand_screen_device", "tm_anand_step", "tm_set_stream", "tm_launch_count", "tm_kernel_timer",
             "tm_kernel_timer_read", "tm_assemble_step_device", "tm_prepare_step", "tm_accumulate_q", "tm_accumulate_q_device",
             "tm_element_strains", "tm_element_strains_device", "tm_sample_plane", "tm_sample_plane_device",
-            "tm_anand_screen_pillar", "tm_anand_screen_pillar_device"]
+            "tm_anand_screen_pillar", "tm_anand_screen_pillar_device", "tm_pc_apply", "tm_pc_apply_device"]
+PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
+PRECOND_NAMES = {v: k for k, v in PRECONDS.items()}
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
 
 dp = C.POINTER(C.c_double)
@@ -54,7 +56,8 @@ class TmSolveInfo(C.Structure):
     _fields_ = [("iters", C.c_int32), ("relres", C.c_double), ("iters0", C.c_double), ("converged", C.c_int32),
                 ("ms", C.c_double), ("pc_ms", C.c_double), ("rebuilt", C.c_int32), ("warm", C.c_int32),
                 ("fallback", C.c_int32), ("jitter_count", C.c_int32), ("levels", C.c_int32), ("status", C.c_int32),
-                ("refinements", C.c_int32)]
+                ("refinements", C.c_int32), ("precond", C.c_int32), ("fallback_first", C.c_int32),
+                ("fallback_iters", C.c_int32), ("fallback_relres", C.c_double)]
 
 
 class TmAnandMaterial(C.Structure):
@@ -89,6 +92,8 @@ def load():
     L.tm_solve_device.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
     L.tm_matvec.argtypes = [vp, vp, vp]
     L.tm_matvec_device.argtypes = [vp, vp, vp]
+    L.tm_pc_apply.argtypes = [vp, vp, vp]
+    L.tm_pc_apply_device.argtypes = [vp, vp, vp]
     L.tm_get_bcsr.argtypes = [vp, vp, vp, vp]
     L.tm_sizes.argtypes = [vp, C.POINTER(C.c_int64)]
     L.tm_destroy.argtypes = [vp]

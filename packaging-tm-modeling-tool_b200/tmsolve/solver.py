@@ -175,17 +175,28 @@ class DeviceModel:
         o = TmSolveOpts()
         load().tm_default_solve_opts(C.byref(o))
         o.tol = tol; o.maxit = maxit; o.warm = warm
-        o.precond = 0 if precond == "mg" else 1
+        o.precond = _lib.PRECONDS[precond]
         o.precision = {"fp64": 0, "mixed": 1, "mixed_ir": 2}[precision]
         o.key = -1 if key is None else int(key)
         return o
 
     @staticmethod
     def record(info: TmSolveInfo, label=None, precond="mg") -> dict:
+        fb = None
+        if info.fallback:
+            fb = dict(first=_lib.PRECOND_NAMES.get(int(info.fallback_first), "?"), iters=int(info.fallback_iters),
+                      relres=float(info.fallback_relres))
         return dict(label=label, iters=int(info.iters), relres=float(info.relres), converged=bool(info.converged),
-                    ms=float(info.ms), pcMs=float(info.pc_ms), precond=precond, rebuilt=bool(info.rebuilt),
-                    warm=int(info.warm), iters0=float(info.iters0), fallback=None if not info.fallback else True,
+                    ms=float(info.ms), pcMs=float(info.pc_ms), precond=_lib.PRECOND_NAMES.get(int(info.precond), precond),
+                    rebuilt=bool(info.rebuilt), warm=int(info.warm), iters0=float(info.iters0), fallback=fb,
                     jitter=int(info.jitter_count), levels=int(info.levels), refinements=int(info.refinements))
+
+    def pc_apply(self, r) -> np.ndarray:
+        """z = M^-1 r with the preconditioner the last solve built (scaled space; pc.apply)."""
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.zeros(self.ndof)
+        check(load().tm_pc_apply(self.h, r.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p)))
+        return z
 
     def solve(self, f, label=None, key=-1, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64",
               out: Optional[np.ndarray] = None) -> dict:

@@ -132,7 +132,9 @@ def test_maxit_not_converged():
     from tmsolve.solver import DeviceModel
     dm = DeviceModel(pkg)
     r = dm.solve(dm.assemble_step(pkg.step()), tol=1e-14, maxit=1, warm=0)
-    assert r["converged"] is False and r["iters"] == 1
+    # one multigrid iteration, then the fallback's one IC(0) iteration (10-solver.js:967-976)
+    assert r["converged"] is False and r["iters"] == 2
+    assert r["fallback"]["first"] == "mg" and r["fallback"]["iters"] == 1 and r["precond"] == "ic"
 
 
 def test_zero_load():
