@@ -70,6 +70,16 @@ def lib():
     L.orc_sample_plane.argtypes = [vp, _dp, C.c_int, C.c_int, C.c_double, C.c_double]
     L.orc_warpage_jeita.argtypes = [vp, _dp, C.c_int, _dp, _dp, _dp, _dp]
     L.orc_pc_apply.argtypes = [vp, _dp, _dp]
+    L.orc_sub_create.restype = vp
+    L.orc_sub_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _ip, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int, _ip,
+                                 _dp, _dp, _dp, _dp, C.c_int, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, C.c_double,
+                                 C.c_double, C.c_double]
+    L.orc_sub_destroy.argtypes = [vp]
+    L.orc_sub_sizes.argtypes = [vp, _ip]
+    L.orc_sub_step.argtypes = [vp, C.c_double, C.c_double, _ip, _dp]
+    L.orc_sub_get_u.argtypes = [vp, _dp]
+    L.orc_sub_get_points.argtypes = [vp, _dp, _dp]
+    L.orc_sub_run.argtypes = [vp, C.c_int, _dp, _dp, _ip, _ip, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp]
     L.orc_last_error.restype = C.c_char_p
     L.orc_last_error.argtypes = [vp]
     _lib = L
@@ -246,3 +256,62 @@ def anand_screen_pillar(params, Etab, Ftab, temps, table, hist, fs, pnu, pEtab, 
                                   np.ascontiguousarray(hist["phase"], np.int32), int(hist["cycles"]), float(fs), float(pnu),
                                   np.ascontiguousarray(pEtab, np.float64), np.ascontiguousarray(pFtab, np.float64), dW, dE, stab)
     return dW, dE, stab
+
+
+class OracleSubmodel:
+    """CPU restatement of BumpSubmodel (13-fatigue.js:470-1104) on a SubmodelSpec."""
+
+    def __init__(self, spec):
+        L = lib()
+        f = lambda a: np.ascontiguousarray(a, np.float64)
+        i32 = lambda a: np.ascontiguousarray(a, np.int32)
+        self._keep = (f(spec.xs), f(spec.ys), f(spec.zs))
+        nb = len(spec.bGlob)
+        self.h = L.orc_sub_create(len(spec.xs), len(spec.ys), len(spec.zs), f(spec.xs), f(spec.ys), f(spec.zs), i32(spec.cell_mat),
+                                  spec.nglob, len(spec.ts), f(spec.ts), f(spec.fields), f(spec.u25), nb, i32(spec.bGlob).reshape(-1),
+                                  f(spec.bW).reshape(-1), f(spec.anand), f(spec.solder_E), f(spec.solder_F), int(spec.elastic_solder),
+                                  f(spec.uf_E), f(spec.uf_F), float(spec.uf_nu), f(spec.si_D), f(spec.si_F), f(spec.sub_D),
+                                  f(spec.sub_F), float(spec.nu_max), float(spec.zt), float(spec.zaf))
+        if not self.h:
+            raise ValueError("boundary node count does not match the cell")
+        sz = np.zeros(4, np.int32)
+        L.orc_sub_sizes(self.h, sz)
+        self.nn, self.ne, self.nb, self.nsolder = (int(v) for v in sz)
+        self.ndof = 3 * self.nn
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_sub_destroy(self.h)
+            self.h = None
+
+    def step(self, T, dt):
+        """stepTo (13-fatigue.js:924-956): (converged, newton, dMax)."""
+        nw = np.zeros(1, np.int32); dm = np.zeros(1)
+        ok = lib().orc_sub_step(self.h, float(T), float(dt), nw, dm)
+        return bool(ok), int(nw[0]), float(dm[0])
+
+    def u(self):
+        out = np.zeros(self.ndof)
+        lib().orc_sub_get_u(self.h, out)
+        return out
+
+    def points(self):
+        W = np.zeros(self.nsolder); E = np.zeros(self.nsolder)
+        lib().orc_sub_get_points(self.h, W, E)
+        return W, E
+
+    def run(self, hist, cphi=1.0, sphi=0.0):
+        """run (13-fatigue.js:1004-1104): dict of dW, dWdie, dWsub, dE, dEdie, dEsub, stabChange,
+        steps, cutbacks, newtonPerStep, perCycle (cycles x 2), loop (points x 4)."""
+        n, nc = len(hist["t"]), int(hist["cycles"])
+        out = np.zeros(10); pc = np.zeros(2 * nc); loop = np.zeros(4 * n)
+        rc = lib().orc_sub_run(self.h, n, np.ascontiguousarray(hist["t"], np.float64), np.ascontiguousarray(hist["T"], np.float64),
+                               np.ascontiguousarray(hist["cycle"], np.int32), np.ascontiguousarray(hist["phase"], np.int32), nc,
+                               float(cphi), float(sphi), out, pc, loop)
+        if rc:
+            raise RuntimeError("submodel run failed")
+        keys = ["dW", "dWdie", "dWsub", "dE", "dEdie", "dEsub", "stabChange", "steps", "cutbacks", "newtonPerStep"]
+        rec = {k: float(out[i]) for i, k in enumerate(keys)}
+        rec["perCycle"] = pc.reshape(nc, 2); rec["loop"] = loop.reshape(n, 4)
+        return rec
+

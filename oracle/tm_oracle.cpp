@@ -26,6 +26,8 @@
 #include <cstdint>
 #include <cstring>
 #include <algorithm>
+#include <array>
+#include <cstdio>
 #include <chrono>
 #include <map>
 #include <memory>
@@ -1726,6 +1728,524 @@ struct AnandPoint {
   void commit() { for (int i = 0; i < 6; i++) ep[i] = tr_ep[i]; s = tr_s; ebar = tr_ebar; W = tr_W; sigEq = tr_sigEq; }
 };
 
+
+// ---- bump submodel (BumpSubmodel, 13-fatigue.js:470-1104) ----------------------------------------
+const double SUB_T_AVG = 0.025;             // 00-constants.js:114
+const int SUB_NEWTON_MAXIT = 25;            // :116
+const double SUB_RES_TOL = 1e-6, SUB_DU_TOL = 1e-8, SUB_INNER_TOL = 1e-8;   // :117-119
+const double INELASTIC_STEP_MAX = 2e-4;     // :113
+
+// gridAt with stride and component (03-materials.js:347-355)
+double gridAtS(const double* arr, double T, int stride, int comp) {
+  const double x = T - TGRID_MIN;
+  if (x <= 0) return arr[comp];
+  if (x >= TGRID_N - 1) return arr[(TGRID_N - 1) * stride + comp];
+  const int i = (int)std::floor(x); const double t = x - i;
+  const double a = arr[i * stride + comp], b = arr[(i + 1) * stride + comp];
+  return a + t * (b - a);
+}
+
+// gridAddAt (03-materials.js:358-362)
+void gridAddAt(const double* grid, double T, int stride, int n, double w, double* out) {
+  double x = T - TGRID_MIN;
+  x = x < 0 ? 0 : (x > TGRID_N - 1 ? TGRID_N - 1 : x);
+  const int i = std::min((int)std::floor(x), TGRID_N - 2); const double t = x - i;
+  const int a = i * stride, b = a + stride;
+  for (int c = 0; c < n; c++) out[c] += w * (grid[a + c] + t * (grid[b + c] - grid[a + c]));
+}
+
+// forGridSegments (03-materials.js:370-377)
+template <class F> void forGridSegments(double Ta, double Tb, F fn) {
+  const double lo = std::min(Ta, Tb), hi = std::max(Ta, Tb);
+  for (double t0 = lo; t0 < hi - 1e-12;) {
+    const double t1 = std::min(hi, TGRID_MIN + std::floor(t0 - TGRID_MIN + 1e-9) + 1);
+    fn(0.5 * (t0 + t1), t0, t1);
+    t0 = t1;
+  }
+}
+
+// gridMean (03-materials.js:380-387)
+void gridMean(const double* grid, int stride, int n, double Ta, double Tb, double* out) {
+  for (int c = 0; c < n; c++) out[c] = 0;
+  const double L = std::fabs(Tb - Ta);
+  if (L < 1e-12) { gridAddAt(grid, Ta, stride, n, 1, out); return; }
+  forGridSegments(Ta, Tb, [&](double tm, double t0, double t1) { gridAddAt(grid, tm, stride, n, (t1 - t0) / L, out); });
+}
+
+// gridStressIncrement with a stiffness grid (03-materials.js:394-410)
+void gridStressIncrement(const double* Dg, const double* Fg, double Ta, double Tb, double* out) {
+  for (int r = 0; r < 6; r++) out[r] = 0;
+  const double sg = Tb >= Ta ? 1 : -1;
+  double D[36];
+  forGridSegments(Ta, Tb, [&](double tm, double t0, double t1) {
+    for (auto& v : D) v = 0;
+    gridAddAt(Dg, tm, 36, 36, 1, D);
+    const double f0 = gridAtS(Fg, t1, 3, 0) - gridAtS(Fg, t0, 3, 0), f1 = gridAtS(Fg, t1, 3, 1) - gridAtS(Fg, t0, 3, 1),
+                 f2 = gridAtS(Fg, t1, 3, 2) - gridAtS(Fg, t0, 3, 2);
+    for (int r = 0; r < 6; r++) out[r] += sg * (D[6 * r] * f0 + D[6 * r + 1] * f1 + D[6 * r + 2] * f2);
+  });
+}
+
+// gridModulusStrainIncrement (03-materials.js:413-418)
+double gridModulusStrainIncrement(const double* E, const double* F, double Ta, double Tb) {
+  const double sg = Tb >= Ta ? 1 : -1;
+  double s = 0;
+  forGridSegments(Ta, Tb, [&](double tm, double t0, double t1) { s += gridAt(E, tm) * (gridAt(F, t1) - gridAt(F, t0)); });
+  return sg * s;
+}
+
+// isoD through isoEC and orthoD (03-materials.js:222-249)
+void isoD(double E, double nu, double nuMax, double* out) {
+  const double nc = std::min(nu, nuMax);
+  const double G = E / (2 * (1 + nc));
+  const double nxy = std::min(nc, nuMax), nxz = nxy, nyz = nxy;
+  double S[9] = {0}, C[9];
+  S[0] = 1 / E; S[4] = 1 / E; S[8] = 1 / E;
+  S[1] = S[3] = -nxy / E;
+  S[2] = S[6] = -nxz / E;
+  S[5] = S[7] = -nyz / E;
+  invDense(S, 3, C);
+  for (int q = 0; q < 36; q++) out[q] = 0;
+  out[0] = C[0]; out[1] = C[1]; out[2] = C[2];
+  out[6] = C[3]; out[7] = C[4]; out[8] = C[5];
+  out[12] = C[6]; out[13] = C[7]; out[14] = C[8];
+  out[21] = G; out[28] = G; out[35] = G;
+}
+
+// bbarMatrix (13-fatigue.js:474-491): B-bar (mean dilatation) matrix of a box element at a point
+void bbarMatrix(double hx, double hy, double hz, double xi, double eta, double zeta, double* Bb) {
+  double dx[11], dy[11], dz[11], cx[11], cy[11], cz[11];
+  boxDerivs(hx, hy, hz, xi, eta, zeta, dx, dy, dz);
+  boxDerivs(hx, hy, hz, 0, 0, 0, cx, cy, cz);
+  for (int q = 0; q < 144; q++) Bb[q] = 0;
+  for (int a = 0; a < 8; a++) {
+    const int c = 3 * a;
+    const double ddx = (cx[a] - dx[a]) / 3, ddy = (cy[a] - dy[a]) / 3, ddz = (cz[a] - dz[a]) / 3;
+    Bb[0 * 24 + c] = dx[a] + ddx; Bb[0 * 24 + c + 1] = ddy; Bb[0 * 24 + c + 2] = ddz;
+    Bb[1 * 24 + c] = ddx; Bb[1 * 24 + c + 1] = dy[a] + ddy; Bb[1 * 24 + c + 2] = ddz;
+    Bb[2 * 24 + c] = ddx; Bb[2 * 24 + c + 1] = ddy; Bb[2 * 24 + c + 2] = dz[a] + ddz;
+    Bb[3 * 24 + c] = dy[a]; Bb[3 * 24 + c + 1] = dx[a];
+    Bb[4 * 24 + c + 1] = dz[a]; Bb[4 * 24 + c + 2] = dy[a];
+    Bb[5 * 24 + c] = dz[a]; Bb[5 * 24 + c + 2] = dx[a];
+  }
+}
+
+int findIntervalV(const dvec& a, double x) {
+  const int n = (int)a.size();
+  if (x <= a[0]) return 0;
+  if (x >= a[n - 1]) return n - 2;
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (a[mid] <= x) lo = mid; else hi = mid; }
+  return lo;
+}
+
+// Inputs of a submodel: the voxel cell (materials per cell: 0 substrate slice, 1 solder,
+// 2 underfill, 3 silicon), the global fields it is cut from (at the global temperatures ts, only
+// the nglob global nodes the boundary uses, plus the 25 degC field) with every boundary node's 8
+// global nodes and trilinear weights, and the material tables on the 1 degC grid.
+struct SubInput {
+  int nx, ny, nz; dvec xs, ys, zs; ivec cellMat;
+  int nglob, nt; dvec ts, fields, u25; ivec bGlob; dvec bW;
+  AnandParams anand; dvec solderE, solderF; int elasticSolder = 0;
+  dvec ufE, ufF; double ufNu = 0.35;
+  dvec siD, siF; dvec subD, subF;
+  double nuMax = 0.49, zt = 0, zaf = 0;
+};
+
+struct Submodel {
+  enum { SUB = 0, SOLDER = 1, UF = 2, SI = 3 };
+  SubInput in;
+  Mesh m;
+  Pattern P;
+  int ndof = 0;
+  ivec bmap, eBb;
+  std::vector<dvec> bbB; dvec bbW;
+  std::vector<char> isC;
+  ivec bNodes;
+  std::vector<std::unique_ptr<AnandPoint>> anand;
+  dvec u, uN, sigE, eFn, eK, eF, val, vals, s_;
+  double Tn = 25;
+  bool haveStepKey = false; double keyTn = 0, keyT = 0;
+  bool elasValid[4] = {false, false, false, false}; double elasD[4][36], elasS[4][6];
+  std::unique_ptr<ICPC> pc; bool pcStale = false; int pcIters = 0;
+
+  explicit Submodel(const SubInput& inp) : in(inp) {
+    m.nx = in.nx; m.ny = in.ny; m.nz = in.nz; m.xs = in.xs; m.ys = in.ys; m.zs = in.zs;
+    const int ncells = (in.nx - 1) * (in.ny - 1) * (in.nz - 1);
+    ivec cg(2 * ncells, -1), cp(2 * ncells, 0); dvec cs(2 * ncells, 0.0);
+    for (int c = 0; c < ncells; c++) { cg[2 * c] = in.cellMat[c]; cp[2 * c] = in.cellMat[c]; cs[2 * c] = 1; }
+    buildStructuredMesh(m, cg.data(), cp.data(), cs.data());
+    ndof = 3 * m.nn;
+    P = fullPatternFromUpper(bcsrFromElements(m.nn, m.conn, m.ne, 8));
+    val.assign((size_t)P.nb * 9, 0.0);
+    // _blockMap (13-fatigue.js:597-608)
+    bmap.assign((size_t)m.ne * 64, -1);
+    for (int e = 0; e < m.ne; e++) for (int a = 0; a < 8; a++) {
+      const int na = m.conn[8 * e + a];
+      for (int b = 0; b < 8; b++) {
+        const int nb = m.conn[8 * e + b];
+        int lo = P.rowPtr[na], hi = P.rowPtr[na + 1] - 1, k = -1;
+        while (lo <= hi) { const int mid = (lo + hi) >> 1; const int v = P.col[mid]; if (v == nb) { k = mid; break; } if (v < nb) lo = mid + 1; else hi = mid - 1; }
+        bmap[((size_t)e * 8 + a) * 8 + b] = k;
+      }
+    }
+    // Gauss-point material states
+    for (int e = 0; e < m.ne; e++) for (int g = 0; g < 8; g++)
+      anand.emplace_back(m.eGroup[e] == SOLDER && !in.elasticSolder ? new AnandPoint(in.anand, in.solderE.data()) : nullptr);
+    // _boundary: nodes on the six faces of the cell, in node order
+    isC.assign(ndof, 0);
+    std::vector<char> isB(m.nn, 0);
+    for (int i = 0; i < m.nx; i++) for (int j = 0; j < m.ny; j++) for (int k = 0; k < m.nz; k++) {
+      const int n = m.nodeId[((size_t)i * m.ny + j) * m.nz + k];
+      if (n >= 0 && (i == 0 || j == 0 || k == 0 || i == m.nx - 1 || j == m.ny - 1 || k == m.nz - 1)) isB[n] = 1;
+    }
+    for (int n = 0; n < m.nn; n++) if (isB[n]) { bNodes.push_back(n); isC[3 * n] = isC[3 * n + 1] = isC[3 * n + 2] = 1; }
+    // _bbarCache: B-bar matrices of the 8 Gauss points per distinct element size (12 digits)
+    std::map<std::string, int> keys;
+    eBb.assign(m.ne, 0);
+    const double GP = 1 / std::sqrt(3.0);
+    for (int e = 0; e < m.ne; e++) {
+      const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+      const double hx = m.xs[i + 1] - m.xs[i], hy = m.ys[j + 1] - m.ys[j], hz = m.zs[k + 1] - m.zs[k];
+      char buf[96];
+      snprintf(buf, sizeof buf, "%.11e|%.11e|%.11e", hx, hy, hz);
+      auto it = keys.find(buf);
+      if (it == keys.end()) {
+        const int idx = (int)bbB.size();
+        keys.emplace(buf, idx);
+        dvec B(8 * 144);
+        for (int g = 0; g < 8; g++) bbarMatrix(hx, hy, hz, HEX_XI[g] * GP, HEX_ETA[g] * GP, HEX_ZETA[g] * GP, B.data() + 144 * g);
+        bbB.push_back(B); bbW.push_back(hx * hy * hz / 8);
+        eBb[e] = idx;
+      } else eBb[e] = it->second;
+    }
+    u.assign(ndof, 0.0); uN.assign(ndof, 0.0);
+    sigE.assign((size_t)m.ne * 48, 0.0); eFn.assign((size_t)m.ne * 24, 0.0);
+    eK.assign((size_t)m.ne * 576, 0.0); eF.assign((size_t)m.ne * 24, 0.0);
+  }
+
+  // prescribe (13-fatigue.js:680-694) with Analysis.fieldAt (11-analysis.js:317-324)
+  void prescribe(double T, dvec& uu) const {
+    const int i = findIntervalV(in.ts, T);
+    double t = (T - in.ts[i]) / (in.ts[i + 1] - in.ts[i]);
+    t = t < 0 ? 0 : (t > 1 ? 1 : t);
+    const size_t G = 3 * (size_t)in.nglob;
+    const double* a = in.fields.data() + G * i; const double* b = a + G;
+    for (size_t q = 0; q < bNodes.size(); q++) {
+      const int n = bNodes[q];
+      double ux = 0, uy = 0, uz = 0;
+      for (int c = 0; c < 8; c++) {
+        const int gn = in.bGlob[8 * q + c]; const double w = in.bW[8 * q + c];
+        const double tx = a[3 * gn] + t * (b[3 * gn] - a[3 * gn]), ty = a[3 * gn + 1] + t * (b[3 * gn + 1] - a[3 * gn + 1]),
+                     tz = a[3 * gn + 2] + t * (b[3 * gn + 2] - a[3 * gn + 2]);
+        ux += w * (tx - in.u25[3 * gn]); uy += w * (ty - in.u25[3 * gn + 1]); uz += w * (tz - in.u25[3 * gn + 2]);
+      }
+      uu[3 * n] = ux; uu[3 * n + 1] = uy; uu[3 * n + 2] = uz;
+    }
+  }
+
+  // _elastic (13-fatigue.js:702-757) without the homogenized-layer consistency mode
+  void elastic(int mat, double Ta, double Tb, double* D, double* sth) const {
+    auto rowSum = [&](int r) { return D[r * 6] + D[r * 6 + 1] + D[r * 6 + 2]; };
+    auto isoStep = [&](const dvec& E, const dvec& F, double nu) {
+      double Em;
+      gridMean(E.data(), 1, 1, Ta, Tb, &Em);
+      const double ef = gridModulusStrainIncrement(E.data(), F.data(), Ta, Tb) / Em;
+      isoD(Em, nu, in.nuMax, D);
+      for (int r = 0; r < 6; r++) sth[r] = rowSum(r) * ef;
+    };
+    if (mat == SI) {
+      for (int q = 0; q < 36; q++) D[q] = in.siD[q];
+      const double f = gridAt(in.siF.data(), Tb) - gridAt(in.siF.data(), Ta);
+      for (int r = 0; r < 6; r++) sth[r] = rowSum(r) * f;
+      return;
+    }
+    if (mat == UF) { isoStep(in.ufE, in.ufF, in.ufNu); return; }
+    if (mat == SOLDER) { isoStep(in.solderE, in.solderF, in.anand.nu); return; }
+    gridMean(in.subD.data(), 36, 36, Ta, Tb, D);
+    gridStressIncrement(in.subD.data(), in.subF.data(), Ta, Tb, sth);
+  }
+
+  // _elasRec (13-fatigue.js:760-773): per material, cached for the step from Tn to T
+  void elasRec(int mat, double T, const double** D, const double** sth) {
+    if (!elasValid[mat]) { elastic(mat, Tn, T, elasD[mat], elasS[mat]); elasValid[mat] = true; }
+    *D = elasD[mat]; *sth = elasS[mat];
+  }
+
+  // assemble (13-fatigue.js:776-853): tangent (wantK) and internal force at u; returns max dEbar
+  double assemble(double T, double dt, const dvec& uu, dvec& rint, bool wantK) {
+    if (wantK) std::fill(val.begin(), val.end(), 0.0);
+    std::fill(rint.begin(), rint.end(), 0.0);
+    const bool fresh = !(haveStepKey && keyTn == Tn && keyT == T);
+    if (fresh) for (auto& v : elasValid) v = false;
+    AnandPoint kAn(in.anand, in.solderE.data());
+    const StepK kc = kAn.stepConstants(T, dt);
+    const double fSolder = gridAt(in.solderF.data(), T) - gridAt(in.solderF.data(), 25);
+    double dMax = 0;
+    double ue[24], Ke[576], fe[24], DB[144], eps[6], epsM[6], sig[6], Dg[36];
+    for (int e = 0; e < m.ne; e++) {
+      const double* Ball = bbB[eBb[e]].data(); const double w = bbW[eBb[e]];
+      for (int a = 0; a < 8; a++) { const int n = m.conn[8 * e + a]; ue[3 * a] = uu[3 * n]; ue[3 * a + 1] = uu[3 * n + 1]; ue[3 * a + 2] = uu[3 * n + 2]; }
+      std::fill(Ke, Ke + 576, 0.0); std::fill(fe, fe + 24, 0.0);
+      if (!anand[(size_t)e * 8]) {
+        double* Kc = eK.data() + 576 * (size_t)e; double* fc = eF.data() + 24 * (size_t)e;
+        if (fresh) {
+          const double *D, *sth;
+          elasRec(m.eGroup[e], T, &D, &sth);
+          std::fill(Kc, Kc + 576, 0.0); std::fill(fc, fc + 24, 0.0);
+          for (int g = 0; g < 8; g++) {
+            const double* Bb = Ball + 144 * g;
+            for (int c = 0; c < 24; c++) { double sum = 0; for (int r = 0; r < 6; r++) sum += Bb[r * 24 + c] * sth[r]; fc[c] += w * sum; }
+            for (int r = 0; r < 6; r++) for (int c = 0; c < 24; c++) { double sum = 0; for (int t = 0; t < 6; t++) sum += D[r * 6 + t] * Bb[t * 24 + c]; DB[r * 24 + c] = sum; }
+            for (int a = 0; a < 24; a++) for (int b = a; b < 24; b++) { double sum = 0; for (int r = 0; r < 6; r++) sum += Bb[r * 24 + a] * DB[r * 24 + b]; Kc[a * 24 + b] += w * sum; }
+          }
+          for (int a = 0; a < 24; a++) for (int b = 0; b < a; b++) Kc[a * 24 + b] = Kc[b * 24 + a];
+        }
+        for (int a = 0; a < 8; a++) { const int n = m.conn[8 * e + a]; ue[3 * a] -= uN[3 * n]; ue[3 * a + 1] -= uN[3 * n + 1]; ue[3 * a + 2] -= uN[3 * n + 2]; }
+        for (int a = 0; a < 24; a++) { double sum = eFn[24 * (size_t)e + a] - fc[a]; for (int b = 0; b < 24; b++) sum += Kc[a * 24 + b] * ue[b]; fe[a] = sum; }
+        for (int a = 0; a < 8; a++) { const int n = m.conn[8 * e + a]; rint[3 * n] += fe[3 * a]; rint[3 * n + 1] += fe[3 * a + 1]; rint[3 * n + 2] += fe[3 * a + 2]; }
+        if (wantK) for (int a = 0; a < 8; a++) for (int b = 0; b < 8; b++) {
+          const size_t v = 9 * (size_t)bmap[((size_t)e * 8 + a) * 8 + b];
+          for (int p = 0; p < 3; p++) for (int q = 0; q < 3; q++) val[v + 3 * p + q] += Kc[(3 * a + p) * 24 + 3 * b + q];
+        }
+        continue;
+      }
+      for (int g = 0; g < 8; g++) {
+        const double* Bb = Ball + 144 * g;
+        for (int r = 0; r < 6; r++) { double s = 0; for (int c = 0; c < 24; c++) s += Bb[r * 24 + c] * ue[c]; eps[r] = s; }
+        AnandPoint& pt = *anand[(size_t)e * 8 + g];
+        for (int r = 0; r < 6; r++) epsM[r] = eps[r];
+        epsM[0] -= fSolder; epsM[1] -= fSolder; epsM[2] -= fSolder;
+        const double d = pt.step(epsM, T, dt, sig, Dg, wantK, &kc);
+        if (d > dMax) dMax = d;
+        for (int c = 0; c < 24; c++) { double s = 0; for (int r = 0; r < 6; r++) s += Bb[r * 24 + c] * sig[r]; fe[c] += w * s; }
+        if (wantK) {
+          for (int r = 0; r < 6; r++) for (int c = 0; c < 24; c++) { double s = 0; for (int t = 0; t < 6; t++) s += Dg[r * 6 + t] * Bb[t * 24 + c]; DB[r * 24 + c] = s; }
+          for (int a = 0; a < 24; a++) for (int b = a; b < 24; b++) { double s = 0; for (int r = 0; r < 6; r++) s += Bb[r * 24 + a] * DB[r * 24 + b]; Ke[a * 24 + b] += w * s; }
+        }
+      }
+      for (int a = 0; a < 8; a++) { const int n = m.conn[8 * e + a]; rint[3 * n] += fe[3 * a]; rint[3 * n + 1] += fe[3 * a + 1]; rint[3 * n + 2] += fe[3 * a + 2]; }
+      if (wantK) {
+        for (int a = 0; a < 24; a++) for (int b = 0; b < a; b++) Ke[a * 24 + b] = Ke[b * 24 + a];
+        for (int a = 0; a < 8; a++) for (int b = 0; b < 8; b++) {
+          const size_t v = 9 * (size_t)bmap[((size_t)e * 8 + a) * 8 + b];
+          for (int p = 0; p < 3; p++) for (int q = 0; q < 3; q++) val[v + 3 * p + q] += Ke[(3 * a + p) * 24 + 3 * b + q];
+        }
+      }
+    }
+    haveStepKey = true; keyTn = Tn; keyT = T;
+    return dMax;
+  }
+
+  // _commitElastic (13-fatigue.js:856-872)
+  void commitElastic(double T) {
+    double due[24], de[6], sg[6];
+    for (int e = 0; e < m.ne; e++) {
+      if (anand[(size_t)e * 8]) continue;
+      const double *D, *sth;
+      elasRec(m.eGroup[e], T, &D, &sth);
+      const double* Ball = bbB[eBb[e]].data(); const double w = bbW[eBb[e]];
+      for (int a = 0; a < 8; a++) { const int n = m.conn[8 * e + a]; for (int c = 0; c < 3; c++) due[3 * a + c] = u[3 * n + c] - uN[3 * n + c]; }
+      double* fn = eFn.data() + 24 * (size_t)e;
+      std::fill(fn, fn + 24, 0.0);
+      for (int g = 0; g < 8; g++) {
+        const double* Bb = Ball + 144 * g; double* so = sigE.data() + 48 * (size_t)e + 6 * g;
+        for (int r = 0; r < 6; r++) { double s2 = 0; for (int c = 0; c < 24; c++) s2 += Bb[r * 24 + c] * due[c]; de[r] = s2; }
+        for (int r = 0; r < 6; r++) { double s2 = -sth[r]; for (int c = 0; c < 6; c++) s2 += D[r * 6 + c] * de[c]; so[r] += s2; sg[r] = so[r]; }
+        for (int c = 0; c < 24; c++) { double s2 = 0; for (int r = 0; r < 6; r++) s2 += Bb[r * 24 + c] * sg[r]; fn[c] += w * s2; }
+      }
+    }
+    uN = u; Tn = T;
+  }
+
+  // _constrain (13-fatigue.js:874-883)
+  void constrain() {
+    for (int i = 0; i < P.n; i++) for (int k = P.rowPtr[i]; k < P.rowPtr[i + 1]; k++) {
+      const int j = P.col[k];
+      for (int p = 0; p < 3; p++) for (int q = 0; q < 3; q++) {
+        const int r = 3 * i + p, c = 3 * j + q;
+        if ((isC[r] || isC[c]) && r != c) val[9 * (size_t)k + 3 * p + q] = 0;
+      }
+    }
+  }
+
+  // _solve (13-fatigue.js:886-917): IC(0)-PCG on the Jacobi-scaled tangent
+  int solve(const dvec& rhs, dvec& x, double tol) {
+    const int n = ndof;
+    vals = val;
+    s_.assign(n, 0.0);
+    for (int i = 0; i < P.n; i++) {
+      const size_t v = 9 * (size_t)P.diag[i];
+      s_[3 * i] = 1 / std::sqrt(std::max(vals[v], 1e-300)); s_[3 * i + 1] = 1 / std::sqrt(std::max(vals[v + 4], 1e-300));
+      s_[3 * i + 2] = 1 / std::sqrt(std::max(vals[v + 8], 1e-300));
+    }
+    for (int i = 0; i < P.n; i++) for (int k = P.rowPtr[i]; k < P.rowPtr[i + 1]; k++) {
+      const int j = P.col[k]; const size_t v = 9 * (size_t)k;
+      for (int p = 0; p < 3; p++) for (int q = 0; q < 3; q++) vals[v + 3 * p + q] *= s_[3 * i + p] * s_[3 * j + q];
+    }
+    dvec b(n);
+    for (int q = 0; q < n; q++) b[q] = rhs[q] * s_[q];
+    if (!pc || pcStale) { pc.reset(new ICPC(P, vals)); pcStale = false; pcIters = 0; }
+    dvec r(n), z(n), p(n), qv(n);
+    std::fill(x.begin(), x.end(), 0.0);
+    r = b;
+    const double bn = norm2(b);
+    if (bn == 0) return 0;
+    pc->apply(r.data(), z.data()); p = z;
+    double rz = dot(r, z);
+    int it;
+    for (it = 1; it <= 2000; it++) {
+      fullMatVec(P, vals.data(), p.data(), qv.data());
+      const double alpha = rz / dot(p, qv);
+      axpy(alpha, p, x); axpy(-alpha, qv, r);
+      if (norm2(r) / bn < tol) break;
+      pc->apply(r.data(), z.data());
+      const double rz2 = dot(r, z); const double beta = rz2 / rz; rz = rz2;
+      for (int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+    }
+    for (int q = 0; q < n; q++) x[q] *= s_[q];
+    if (!pcIters) pcIters = it; else if (it > 2 * pcIters) pcStale = true;
+    return it;
+  }
+
+  // stepTo (13-fatigue.js:924-956)
+  bool stepTo(double T, double dt, int* newton, double* dMaxOut) {
+    const int n = ndof;
+    dvec rint(n), du(n), rhs(n);
+    prescribe(T, u);
+    double dMax = 0, rPrev = INFINITY;
+    bool converged = false, haveK = false;
+    int it;
+    for (it = 1; it <= SUB_NEWTON_MAXIT; it++) {
+      const bool wantK = it <= 2 || !haveK;
+      dMax = assemble(T, dt, u, rint, wantK);
+      if (wantK) { constrain(); haveK = true; }
+      double rn = 0, fn = 0;
+      for (int q = 0; q < n; q++) { if (!isC[q]) rn += rint[q] * rint[q]; fn += rint[q] * rint[q]; }
+      rn = std::sqrt(rn); fn = std::sqrt(fn);
+      const double ref = std::max(fn, 1e-30);
+      if (rn / ref < SUB_RES_TOL) { converged = true; break; }
+      if (!wantK && rn > 0.5 * rPrev) { assemble(T, dt, u, rint, true); constrain(); }
+      rPrev = rn;
+      for (int q = 0; q < n; q++) rhs[q] = isC[q] ? 0 : -rint[q];
+      solve(rhs, du, std::max(SUB_INNER_TOL, std::min(1e-3, 0.01 * SUB_RES_TOL * ref / std::max(rn, 1e-300))));
+      double dun = 0, un = 0;
+      for (int q = 0; q < n; q++) { if (!isC[q]) { u[q] += du[q]; dun += du[q] * du[q]; } un += u[q] * u[q]; }
+      if (std::sqrt(dun) < SUB_DU_TOL * std::max(std::sqrt(un), 1e-30)) { converged = true; it++; break; }
+    }
+    if (converged) {
+      dMax = assemble(T, dt, u, rint, false);
+      for (auto& pt : anand) if (pt) pt->commit();
+      commitElastic(T);
+    }
+    *newton = it; *dMaxOut = dMax;
+    return converged;
+  }
+
+  struct Snap { dvec u, sigE, eFn; double Tn; std::vector<std::array<double, 11>> st; };
+  void snapshot(Snap& s) const {
+    s.u = u; s.sigE = sigE; s.eFn = eFn; s.Tn = Tn;
+    s.st.resize(anand.size());
+    for (size_t i = 0; i < anand.size(); i++) if (anand[i]) {
+      const AnandPoint& p = *anand[i];
+      for (int c = 0; c < 6; c++) s.st[i][c] = p.ep[c];
+      s.st[i][6] = p.s; s.st[i][7] = p.ebar; s.st[i][8] = p.W; s.st[i][9] = p.sigEq;
+    }
+  }
+  void restore(const Snap& s) {
+    u = s.u; uN = s.u; sigE = s.sigE; eFn = s.eFn; Tn = s.Tn;
+    for (size_t i = 0; i < anand.size(); i++) if (anand[i]) {
+      AnandPoint& p = *anand[i];
+      for (int c = 0; c < 6; c++) p.ep[c] = s.st[i][c];
+      p.s = s.st[i][6]; p.ebar = s.st[i][7]; p.W = s.st[i][8]; p.sigEq = s.st[i][9];
+    }
+  }
+
+  // run (13-fatigue.js:1004-1104): the cycle history with adaptive sub-steps, the hysteresis
+  // sampler of the two interface layers and the per-cycle inelastic work. out (10): dW, dWdie,
+  // dWsub, dE, dEdie, dEsub, stabChange, steps, cutbacks, newtonPerStep; perCycle: dWdie, dWsub
+  // per cycle; loop (4 per history point): tau, gamma (die side), tauSub, gammaSub.
+  void run(int nsteps, const double* ht, const double* hT, const int* hcycle, const int* hphase, int cycles, double cphi, double sphi,
+           double* out, double* perCycle, double* loop) {
+    struct Rec { int idx; double w; };
+    std::vector<Rec> dieLayer, subLayer;
+    for (int e = 0; e < m.ne; e++) {
+      if (m.eGroup[e] != SOLDER) continue;
+      const int k = m.eIJK[3 * e + 2]; const double zc = 0.5 * (m.zs[k] + m.zs[k + 1]);
+      const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1];
+      const double w = (m.xs[i + 1] - m.xs[i]) * (m.ys[j + 1] - m.ys[j]) * (m.zs[k + 1] - m.zs[k]) / 8;
+      for (int g = 0; g < 8; g++) {
+        if (zc > in.zaf - SUB_T_AVG) dieLayer.push_back({e * 8 + g, w});
+        if (zc < in.zt + SUB_T_AVG) subLayer.push_back({e * 8 + g, w});
+      }
+    }
+    auto avg = [&](const std::vector<Rec>& list, bool W) {
+      double sum = 0, ws = 0;
+      for (const Rec& r : list) { sum += r.w * (W ? anand[r.idx]->W : anand[r.idx]->ebar); ws += r.w; }
+      return ws ? sum / ws : NAN;
+    };
+    const double GP = 1 / std::sqrt(3.0);
+    int sample = 0;
+    auto sampleLoop = [&](double T) {
+      double tS = 0, gS = 0, tB = 0, gB = 0, wS = 0, wB = 0;
+      double Bb[144], ue[24], eps[6], sig[6], Dd[36];
+      for (int li = 0; li < 2; li++) {
+        for (const Rec& r : li == 0 ? dieLayer : subLayer) {
+          const int e = r.idx / 8, g = r.idx % 8;
+          const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+          bbarMatrix(m.xs[i + 1] - m.xs[i], m.ys[j + 1] - m.ys[j], m.zs[k + 1] - m.zs[k], HEX_XI[g] * GP, HEX_ETA[g] * GP, HEX_ZETA[g] * GP, Bb);
+          for (int a = 0; a < 8; a++) { const int nn = m.conn[8 * e + a]; ue[3 * a] = u[3 * nn]; ue[3 * a + 1] = u[3 * nn + 1]; ue[3 * a + 2] = u[3 * nn + 2]; }
+          for (int rr = 0; rr < 6; rr++) { double s2 = 0; for (int c = 0; c < 24; c++) s2 += Bb[rr * 24 + c] * ue[c]; eps[rr] = s2; }
+          AnandPoint& pt = *anand[r.idx];
+          const double f = gridAt(in.solderF.data(), T) - gridAt(in.solderF.data(), 25);
+          eps[0] -= f; eps[1] -= f; eps[2] -= f;
+          pt.step(eps, T, 1e-9, sig, Dd, false, nullptr);   // stress at the committed plastic state
+          const double tau = sig[5] * cphi + sig[4] * sphi, gam = eps[5] * cphi + eps[4] * sphi;
+          if (li == 0) { tS += r.w * tau; gS += r.w * gam; wS += r.w; } else { tB += r.w * tau; gB += r.w * gam; wB += r.w; }
+        }
+      }
+      double* L = loop + 4 * (size_t)sample++;
+      L[0] = wS ? tS / wS : NAN; L[1] = wS ? gS / wS : NAN; L[2] = wB ? tB / wB : NAN; L[3] = wB ? gB / wB : NAN;
+    };
+    dvec Wdie(cycles + 1, 0.0), Wsub(cycles + 1, 0.0), Edie(cycles + 1, 0.0), Esub(cycles + 1, 0.0);
+    long long totalNewton = 0; int cutbacks = 0, steps = 0, nsubNext = 1;
+    sampleLoop(25);
+    for (int k = 1; k < nsteps; k++) {
+      const double T0 = hT[k - 1], T1 = hT[k], t0s = ht[k - 1], t1s = ht[k];
+      int nsub = nsubNext; bool done = false; double dLast = 0;
+      for (int attempt = 0; attempt < 8 && !done; attempt++) {
+        Snap snap;
+        snapshot(snap);
+        bool ok = true;
+        for (int sI = 1; sI <= nsub; sI++) {
+          const double T = T0 + (T1 - T0) * sI / nsub, dt = (t1s - t0s) / nsub;
+          int newton; double dMax;
+          const bool conv = stepTo(T, dt, &newton, &dMax);
+          totalNewton += newton; steps++;
+          dLast = dMax;
+          if (!conv || dMax > INELASTIC_STEP_MAX) { ok = false; break; }
+        }
+        if (ok) done = true;
+        else { restore(snap); nsub *= 2; cutbacks++; }
+      }
+      nsubNext = dLast > 0.5 * INELASTIC_STEP_MAX ? std::min(nsub * 2, 64) : (dLast < 0.2 * INELASTIC_STEP_MAX ? std::max(1, nsub >> 1) : nsub);
+      if (!done) throw std::runtime_error("Submodel step failed to converge after cutbacks");
+      sampleLoop(T1);
+      const int c = hcycle[k];
+      Wdie[c] = avg(dieLayer, true); Wsub[c] = avg(subLayer, true);
+      Edie[c] = avg(dieLayer, false); Esub[c] = avg(subLayer, false);
+    }
+    const int nc = cycles;
+    const double dWdie = Wdie[nc] - Wdie[nc - 1], dWsub = Wsub[nc] - Wsub[nc - 1];
+    const double dEdie = Edie[nc] - Edie[nc - 1], dEsub = Esub[nc] - Esub[nc - 1];
+    const double dW = std::max(dWdie, dWsub), dE = dWdie >= dWsub ? dEdie : dEsub;
+    const double prev = nc >= 2 ? std::max(Wdie[nc - 1] - Wdie[nc - 2], Wsub[nc - 1] - Wsub[nc - 2]) : NAN;
+    const double stab = std::isfinite(prev) && prev > 0 ? std::fabs(dW - prev) / prev : NAN;
+    const double o[10] = {dW, dWdie, dWsub, dE, dEdie, dEsub, stab, (double)steps, (double)cutbacks, (double)totalNewton / std::max(steps, 1)};
+    std::copy(o, o + 10, out);
+    for (int c = 1; c <= nc; c++) { perCycle[2 * (c - 1)] = Wdie[c] - Wdie[c - 1]; perCycle[2 * (c - 1) + 1] = Wsub[c] - Wsub[c - 1]; }
+  }
+};
 }  // namespace
 
 // =====================================================================================
@@ -1985,6 +2505,60 @@ int orc_solve(orc_model* o, const double* f, double* u, double tol, int maxit, i
 }
 
 void orc_clear_warm(orc_model* o) { o->solver->basis.clear(); }
+
+// ---- bump submodel -------------------------------------------------------------------------------
+struct orc_sub { std::unique_ptr<Submodel> S; std::string err; };
+
+// anand: the 10 Anand constants (A, QR, xi, m, shat, n, h0, a, s0, nu); tables on the 1 degC grid
+// (381 points): solder E/F, underfill E/F, silicon F, substrate slice D (36 per point) and F (3
+// per point); siD the silicon stiffness (36)
+orc_sub* orc_sub_create(int nx, int ny, int nz, const double* xs, const double* ys, const double* zs, const int* cellMat,
+                        int nglob, int nt, const double* ts, const double* fields, const double* u25, int nb, const int* bGlob,
+                        const double* bW, const double* anand, const double* solderE, const double* solderF, int elasticSolder,
+                        const double* ufE, const double* ufF, double ufNu, const double* siD, const double* siF, const double* subD,
+                        const double* subF, double nuMax, double zt, double zaf) {
+  SubInput in;
+  in.nx = nx; in.ny = ny; in.nz = nz;
+  in.xs.assign(xs, xs + nx); in.ys.assign(ys, ys + ny); in.zs.assign(zs, zs + nz);
+  in.cellMat.assign(cellMat, cellMat + (size_t)(nx - 1) * (ny - 1) * (nz - 1));
+  in.nglob = nglob; in.nt = nt; in.ts.assign(ts, ts + nt);
+  in.fields.assign(fields, fields + (size_t)nt * nglob * 3); in.u25.assign(u25, u25 + (size_t)nglob * 3);
+  in.bGlob.assign(bGlob, bGlob + 8 * (size_t)nb); in.bW.assign(bW, bW + 8 * (size_t)nb);
+  in.anand = AnandParams{anand[0], anand[1], anand[2], anand[3], anand[4], anand[5], anand[6], anand[7], anand[8], anand[9]};
+  in.solderE.assign(solderE, solderE + TGRID_N); in.solderF.assign(solderF, solderF + TGRID_N);
+  in.elasticSolder = elasticSolder;
+  in.ufE.assign(ufE, ufE + TGRID_N); in.ufF.assign(ufF, ufF + TGRID_N); in.ufNu = ufNu;
+  in.siD.assign(siD, siD + 36); in.siF.assign(siF, siF + TGRID_N);
+  in.subD.assign(subD, subD + 36 * TGRID_N); in.subF.assign(subF, subF + 3 * TGRID_N);
+  in.nuMax = nuMax; in.zt = zt; in.zaf = zaf;
+  auto* o = new orc_sub();
+  o->S.reset(new Submodel(in));
+  if ((int)o->S->bNodes.size() != nb) { delete o; return nullptr; }
+  return o;
+}
+
+void orc_sub_destroy(orc_sub* o) { delete o; }
+// nn, ne, boundary nodes, solder Gauss points
+void orc_sub_sizes(orc_sub* o, int* out) {
+  int ns = 0;
+  for (auto& p : o->S->anand) if (p) ns++;
+  out[0] = o->S->m.nn; out[1] = o->S->m.ne; out[2] = (int)o->S->bNodes.size(); out[3] = ns;
+}
+// one stepTo; returns converged, writes the Newton count and the largest plastic increment
+int orc_sub_step(orc_sub* o, double T, double dt, int* newton, double* dMax) { return o->S->stepTo(T, dt, newton, dMax) ? 1 : 0; }
+void orc_sub_get_u(orc_sub* o, double* u) { std::copy(o->S->u.begin(), o->S->u.end(), u); }
+// W and ebar of every solder Gauss point (element-major)
+void orc_sub_get_points(orc_sub* o, double* W, double* ebar) {
+  int q = 0;
+  for (auto& p : o->S->anand) if (p) { W[q] = p->W; ebar[q] = p->ebar; q++; }
+}
+int orc_sub_run(orc_sub* o, int nsteps, const double* t, const double* T, const int* cycle, const int* phase, int cycles, double cphi,
+                double sphi, double* out, double* perCycle, double* loop) {
+  try {
+    o->S->run(nsteps, t, T, cycle, phase, cycles, cphi, sphi, out, perCycle, loop);
+    return 0;
+  } catch (std::exception& e) { o->err = e.what(); return 1; }
+}
 
 // pc.apply(r, z) of the preconditioner the last solve built (scaled space); 1 when none
 int orc_pc_apply(orc_model* o, const double* r, double* z) {
