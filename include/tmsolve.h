@@ -27,6 +27,7 @@
  *                      the march of Analysis.qAlong (src/core/11-analysis.js:298-316)
  *   tm_element_strains boxStrainAt at natural points (src/core/07-element.js:127-142), the
  *                      inner loop of siteStrainTable (src/core/13-fatigue.js:318-346)
+ *   tm_submodel_*      BumpSubmodel (src/core/13-fatigue.js:470-1104): create, stepTo, run
  *   tm_sample_plane    samplePlane(mesh, u, k, comp, x, y) at many points
  *                      (src/core/12-post.js:30-38), the sampler of warpageJEITA (:60-109)
  *
@@ -304,6 +305,58 @@ tm_status tm_anand_screen_noalloc(const tm_anand_material* mat, int32_t nsites, 
                                   const double* table_dev, int32_t nsteps, const double* t, const double* T,
                                   const int32_t* cycle, const int32_t* phase, int32_t cycles,
                                   double* dW_dev, double* dE_dev, double* stab_dev, void* stream);
+
+/* ---- bump submodel (BumpSubmodel, src/core/13-fatigue.js:470-1104) ---- */
+/* One pitch cell around a bump: B-bar hexes on the grid xs x ys x zs with a material per cell
+ * (0 substrate slice, 1 solder, 2 underfill, 3 silicon; cells in (i, j, k) order, k fastest),
+ * Anand solder Gauss points (elastic ones when elasticSolder), the other parts incremental
+ * elastic. The cut boundary (the nodes on the six faces, ascending node id (i ny + j) nz + k)
+ * moves with the global displacement fields (prescribe / fieldAt): for boundary node q its 8
+ * global nodes bGlob[8q..] (indices into the nglob global nodes the caller passes) and the
+ * trilinear weights bW[8q..]; the global fields at the nt ascending global temperatures ts
+ * (fields: nt x nglob x 3) and at 25 degC (u25). Material tables on the 1 degC grid -80..300
+ * (381 points): solder E and F in `solder`, underfill E/F and Poisson ratio, silicon F and its
+ * stiffness siD (36), substrate slice D (381 x 36) and F (381 x 3). nuMax: NU_MAX_SUBMODEL.
+ * zt / zaf: the pad and UBM heights that bound the two averaging layers (SUB_T_AVG). */
+typedef struct {
+  int32_t nx, ny, nz;
+  const double *xs, *ys, *zs;
+  const int32_t* cellMat;
+  int32_t nglob, nt;
+  const double* ts;
+  const double* fields;
+  const double* u25;
+  int32_t nb;
+  const int32_t* bGlob;
+  const double* bW;
+  tm_anand_material solder;
+  int32_t elasticSolder;
+  const double* ufE;
+  const double* ufF;
+  double ufNu;
+  const double* siD;
+  const double* siF;
+  const double* subD;
+  const double* subF;
+  double nuMax, zt, zaf;
+} tm_submodel_spec;
+typedef struct tm_sub tm_sub;
+tm_status tm_submodel_create(const tm_submodel_spec* spec, tm_sub** out);
+tm_status tm_submodel_destroy(tm_sub* sm);
+/* nn, ne, boundary nodes, solder Gauss points */
+tm_status tm_submodel_sizes(tm_sub* sm, int64_t* out4);
+/* stepTo(T, dt) (13-fatigue.js:924-956): Newton to temperature T; converged (0/1), Newton
+ * iterations and the largest plastic increment of the solder points. */
+tm_status tm_submodel_step(tm_sub* sm, double T, double dt, int32_t* converged, int32_t* newton, double* dMax);
+/* The displacement (3 nn) and the solder points' W and ebar (element-major; NULL to skip). */
+tm_status tm_submodel_get(tm_sub* sm, double* u, double* W, double* ebar);
+/* run (13-fatigue.js:1004-1104) over the cycle history (t, T, cycle of cycleHistory) with
+ * adaptive sub-steps: out (10) = dW, dWdie, dWsub, dE, dEdie, dEsub, stabChange, steps,
+ * cutbacks, newtonPerStep; perCycle (2 per cycle) = dWdie, dWsub; loop (4 per history point) =
+ * tau, gamma of the die-side layer and of the substrate-side layer along (cphi, sphi), the
+ * site's direction from the die centre. A step that fails after 8 cutbacks is TM_NOT_CONVERGED. */
+tm_status tm_submodel_run(tm_sub* sm, int32_t nsteps, const double* t, const double* T, const int32_t* cycle, int32_t cycles,
+                          double cphi, double sphi, double* out10, double* perCycle, double* loop);
 
 /* Batched material-point steps: npts independent points, each with a 12-double state
  * (ep[6], s, ebar, W, sigEq, lastD, spare) updated in place when commit != 0;

@@ -974,4 +974,51 @@ tm_status tm_anand_step(const tm_anand_material* mat, int32_t npts, double* stat
   });
 }
 
+// ---- bump submodel ----------------------------------------------------------------------------------
+tm_status tm_submodel_create(const tm_submodel_spec* spec, tm_sub** out) {
+  return guarded([&] {
+    require_device();
+    if (!spec || !out) fail(TM_BAD_INPUT, "null argument");
+    *out = reinterpret_cast<tm_sub*>(submodel_create(*spec));
+  });
+}
+
+tm_status tm_submodel_destroy(tm_sub* sm) {
+  return guarded([&] { submodel_destroy(reinterpret_cast<SubModel*>(sm)); });
+}
+
+tm_status tm_submodel_sizes(tm_sub* sm, int64_t* out) {
+  return guarded([&] {
+    if (!sm || !out) fail(TM_BAD_INPUT, "null argument");
+    submodel_sizes(*reinterpret_cast<SubModel*>(sm), out);
+  });
+}
+
+tm_status tm_submodel_step(tm_sub* sm, double T, double dt, int32_t* converged, int32_t* newton, double* dMax) {
+  return guarded([&] {
+    if (!sm) fail(TM_BAD_INPUT, "null argument");
+    int nw = 0;
+    double dm = 0;
+    const bool ok = submodel_step(*reinterpret_cast<SubModel*>(sm), T, dt, &nw, &dm);
+    if (converged) *converged = ok;
+    if (newton) *newton = nw;
+    if (dMax) *dMax = dm;
+  });
+}
+
+tm_status tm_submodel_get(tm_sub* sm, double* u, double* W, double* ebar) {
+  return guarded([&] {
+    if (!sm) fail(TM_BAD_INPUT, "null argument");
+    submodel_get(*reinterpret_cast<SubModel*>(sm), u, W, ebar);
+  });
+}
+
+tm_status tm_submodel_run(tm_sub* sm, int32_t nsteps, const double* t, const double* T, const int32_t* cycle, int32_t cycles,
+                          double cphi, double sphi, double* out10, double* perCycle, double* loop) {
+  return guarded([&] {
+    if (!sm || !t || !T || !cycle || !out10 || !perCycle || !loop) fail(TM_BAD_INPUT, "null argument");
+    submodel_run(*reinterpret_cast<SubModel*>(sm), nsteps, t, T, cycle, cycles, cphi, sphi, out10, perCycle, loop);
+  });
+}
+
 }  // extern "C"

@@ -147,17 +147,17 @@ __global__ void __launch_bounds__(32 * IC_WARPS) k_ic_backward(int cnt, const in
   }
 }
 
-// node level sets: level[i] = 1 + max level of the neighbours on the given side (lower or
-// higher ids), grouped by a counting sort; start[l] .. start[l+1]-1 index the level's nodes
-void level_sets(const Context& c, bool lower, std::vector<int>& nodes, std::vector<int>& start) {
-  const int nn = c.nn;
+// node level sets of a node pattern (rowPtr/col over nodes, sorted): level[i] = 1 + max level
+// of the neighbours on the given side (lower or higher ids), grouped by a counting sort;
+// start[l] .. start[l+1]-1 index the level's nodes
+void level_sets(int nn, const std::vector<int>& nrp, const std::vector<int>& ncol, bool lower, std::vector<int>& nodes,
+                std::vector<int>& start) {
   std::vector<int> lev(nn, 0);
   int maxLev = 0;
   auto visit = [&](int i) {
     int l = 0;
-    for (int s = 0; s < NSLOT; s++) {
-      if (!(c.slotMask[i] >> s & 1)) continue;
-      const int j = c.nbr[(size_t)s * nn + i];
+    for (int k = nrp[i]; k < nrp[i + 1]; k++) {
+      const int j = ncol[k];
       if (lower ? j < i : j > i) l = std::max(l, lev[j] + 1);
     }
     lev[i] = l;
@@ -173,18 +173,21 @@ void level_sets(const Context& c, bool lower, std::vector<int>& nodes, std::vect
   for (int i = 0; i < nn; i++) nodes[fill[lev[i]]++] = i;
 }
 
-void build_ic_structure(Context& c) {
-  IcFactor& F = c.ic;
-  const int nn = c.nn, n = 3 * nn, S = c.nnp;
+}  // namespace
+
+// scalarUpperCSR (10-solver.js:719-737) of a node pattern: nrp/ncol the sorted block columns of
+// every node, vbase[k] the index of block k's (0, 0) value and vstride the step between its
+// nine values (component 3p + q at vbase[k] + vstride (3p + q))
+void ic_build_structure(IcFactor& F, int nn, const std::vector<int>& nrp, const std::vector<int>& ncol,
+                        const std::vector<long long>& vbase, long long vstride, cudaStream_t st) {
+  const int n = 3 * nn;
   std::vector<int> rowPtr(n + 1, 0);
   for (int i = 0; i < nn; i++) {
     int up = 0;
     bool diag = false;
-    for (int s = 0; s < NSLOT; s++) {
-      if (!(c.slotMask[i] >> s & 1)) continue;
-      const int j = c.nbr[(size_t)s * nn + i];
-      if (j > i) up++;
-      else if (j == i) diag = true;
+    for (int k = nrp[i]; k < nrp[i + 1]; k++) {
+      if (ncol[k] > i) up++;
+      else if (ncol[k] == i) diag = true;
     }
     if (!diag) fail(TM_BAD_INPUT, "IC(0): a node without its diagonal block");
     for (int p = 0; p < 3; p++) rowPtr[3 * i + p + 1] = rowPtr[3 * i + p] + 3 * up + (3 - p);
@@ -192,20 +195,19 @@ void build_ic_structure(Context& c) {
   const long long nnz = rowPtr[n];
   for (int r = 0; r < n; r++)
     if (rowPtr[r + 1] - rowPtr[r] > IC_ROWMAX) fail(TM_BAD_INPUT, "IC(0): a scalar row longer than the factor kernel holds");
-  if ((long long)NSLOT * 9 * S >= (1LL << 31)) fail(TM_BAD_INPUT, "IC(0): operator too large for 32-bit entry indices");
   std::vector<int> col(nnz), gmap(nnz);
   std::vector<int> tCount(n + 1, 0);
   for (int i = 0; i < nn; i++)
     for (int p = 0; p < 3; p++) {
       int w = rowPtr[3 * i + p];
-      // the stencil slots are in ascending neighbour id, so the columns come out sorted
-      for (int s = 0; s < NSLOT; s++) {
-        if (!(c.slotMask[i] >> s & 1)) continue;
-        const int j = c.nbr[(size_t)s * nn + i];
+      for (int k = nrp[i]; k < nrp[i + 1]; k++) {
+        const int j = ncol[k];
         if (j < i) continue;
         for (int q = (j == i ? p : 0); q < 3; q++) {
+          const long long g = vbase[k] + vstride * (3 * p + q);
+          if (g >= (1LL << 31)) fail(TM_BAD_INPUT, "IC(0): operator too large for 32-bit entry indices");
           col[w] = 3 * j + q;
-          gmap[w] = (s * 9 + 3 * p + q) * S + c.pos[i];
+          gmap[w] = (int)g;
           if (w > rowPtr[3 * i + p]) tCount[3 * j + q + 1]++;
           w++;
         }
@@ -222,9 +224,8 @@ void build_ic_structure(Context& c) {
       fill[cc]++;
     }
   std::vector<int> fwd, fwdStart, bwd, bwdStart;
-  level_sets(c, true, fwd, fwdStart);
-  level_sets(c, false, bwd, bwdStart);
-  cudaStream_t st = c.stream;
+  level_sets(nn, nrp, ncol, true, fwd, fwdStart);
+  level_sets(nn, nrp, ncol, false, bwd, bwdStart);
   F.d_rowPtr.upload(rowPtr, st); F.d_col.upload(col, st); F.d_gmap.upload(gmap, st);
   F.d_tStart.upload(tCount, st); F.d_tRow.upload(tRow, st); F.d_tPos.upload(tPos, st);
   F.d_fwdNodes.upload(fwd, st); F.d_bwdNodes.upload(bwd, st);
@@ -232,34 +233,32 @@ void build_ic_structure(Context& c) {
   F.d_U.alloc(nnz);
   F.d_fail.alloc(1);
   F.n = n; F.nnz = nnz;
-  F.epoch = c.structEpoch;
+  F.ready = false;
   TM_CUDA_CHECK(cudaStreamSynchronize(st));
 }
 
-}  // namespace
-
-void build_ic(Context& c) {
-  IcFactor& F = c.ic;
-  if (F.epoch != c.structEpoch || F.n != 3 * c.nn) build_ic_structure(c);
+// ICPC.build (10-solver.js:750-761): factor of the values val (gathered through the structure's
+// map) with the shift sequence 0, 1e-3, 1e-2, ... 1
+void ic_factor(IcFactor& F, const double* val, cudaStream_t st) {
   F.ready = false;
   double shift = 0;
   for (int attempt = 0; attempt < 8; attempt++) {
-    F.d_fail.zero(c.stream);
+    F.d_fail.zero(st);
     note_launch();
-    k_ic_gather<<<grid_for(F.n, 256), 256, 0, c.stream>>>(F.n, F.d_rowPtr.p, F.d_gmap.p, c.d_val.p, shift, F.d_U.p);
+    k_ic_gather<<<grid_for(F.n, 256), 256, 0, st>>>(F.n, F.d_rowPtr.p, F.d_gmap.p, val, shift, F.d_U.p);
     TM_CUDA_CHECK(cudaGetLastError());
     const int nl = (int)F.fwdStart.size() - 1;
     for (int l = 0; l < nl; l++) {
       const int cnt = F.fwdStart[l + 1] - F.fwdStart[l];
       if (cnt <= 0) continue;
       note_launch();
-      k_ic_factor<<<grid_for(cnt, IC_WARPS), 32 * IC_WARPS, 0, c.stream>>>(cnt, F.d_fwdNodes.p + F.fwdStart[l], F.d_rowPtr.p, F.d_col.p, F.d_tStart.p,
-                                                          F.d_tRow.p, F.d_tPos.p, F.d_U.p, F.d_fail.p);
+      k_ic_factor<<<grid_for(cnt, IC_WARPS), 32 * IC_WARPS, 0, st>>>(cnt, F.d_fwdNodes.p + F.fwdStart[l], F.d_rowPtr.p, F.d_col.p,
+                                                                    F.d_tStart.p, F.d_tRow.p, F.d_tPos.p, F.d_U.p, F.d_fail.p);
     }
     TM_CUDA_CHECK(cudaGetLastError());
     int bad = 0;
-    TM_CUDA_CHECK(cudaMemcpyAsync(&bad, F.d_fail.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    TM_CUDA_CHECK(cudaMemcpyAsync(&bad, F.d_fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TM_CUDA_CHECK(cudaStreamSynchronize(st));
     if (!bad) { F.shift = shift; F.ready = true; return; }
     shift = shift == 0 ? IC_SHIFT0 : shift * 10;
     if (shift > IC_SHIFT_MAX) shift = IC_SHIFT_MAX;
@@ -267,23 +266,48 @@ void build_ic(Context& c) {
   fail(TM_BAD_INPUT, "IC(0) failed even with the maximum diagonal shift");
 }
 
-void launch_ic_apply(Context& c, const double* r, double* z) {
-  IcFactor& F = c.ic;
+// ICPC.apply (10-solver.js:784-798)
+void ic_apply(IcFactor& F, const double* r, double* z, cudaStream_t st) {
   if (!F.ready) fail(TM_BAD_INPUT, "IC(0) preconditioner not built");
   const int nl = (int)F.fwdStart.size() - 1, nb = (int)F.bwdStart.size() - 1;
   for (int l = 0; l < nl; l++) {
     const int cnt = F.fwdStart[l + 1] - F.fwdStart[l];
     if (cnt <= 0) continue;
-    k_ic_forward<<<grid_for(cnt, IC_WARPS), 32 * IC_WARPS, 0, c.stream>>>(cnt, F.d_fwdNodes.p + F.fwdStart[l], F.d_rowPtr.p, F.d_tStart.p, F.d_tRow.p,
-                                                        F.d_tPos.p, F.d_U.p, r, z);
+    k_ic_forward<<<grid_for(cnt, IC_WARPS), 32 * IC_WARPS, 0, st>>>(cnt, F.d_fwdNodes.p + F.fwdStart[l], F.d_rowPtr.p, F.d_tStart.p,
+                                                                   F.d_tRow.p, F.d_tPos.p, F.d_U.p, r, z);
   }
   for (int l = 0; l < nb; l++) {
     const int cnt = F.bwdStart[l + 1] - F.bwdStart[l];
     if (cnt <= 0) continue;
-    k_ic_backward<<<grid_for(cnt, IC_WARPS), 32 * IC_WARPS, 0, c.stream>>>(cnt, F.d_bwdNodes.p + F.bwdStart[l], F.d_rowPtr.p, F.d_col.p, F.d_U.p, z);
+    k_ic_backward<<<grid_for(cnt, IC_WARPS), 32 * IC_WARPS, 0, st>>>(cnt, F.d_bwdNodes.p + F.bwdStart[l], F.d_rowPtr.p, F.d_col.p,
+                                                                    F.d_U.p, z);
   }
   note_launch(nl + nb);
   TM_CUDA_CHECK(cudaGetLastError());
 }
+
+// the level-0 operator of a solve context: node pattern from the stencil slots (ascending
+// neighbour ids), values in the slot-major operator
+void build_ic(Context& c) {
+  IcFactor& F = c.ic;
+  if (F.epoch != c.structEpoch || F.n != 3 * c.nn) {
+    const int nn = c.nn;
+    std::vector<int> nrp(nn + 1, 0), ncol;
+    std::vector<long long> vbase;
+    for (int i = 0; i < nn; i++) {
+      for (int s = 0; s < NSLOT; s++) {
+        if (!(c.slotMask[i] >> s & 1)) continue;
+        ncol.push_back(c.nbr[(size_t)s * nn + i]);
+        vbase.push_back((long long)s * 9 * c.nnp + c.pos[i]);
+      }
+      nrp[i + 1] = (int)ncol.size();
+    }
+    ic_build_structure(F, nn, nrp, ncol, vbase, c.nnp, c.stream);
+    F.epoch = c.structEpoch;
+  }
+  ic_factor(F, c.d_val.p, c.stream);
+}
+
+void launch_ic_apply(Context& c, const double* r, double* z) { ic_apply(c.ic, r, z, c.stream); }
 
 }  // namespace tmg

@@ -305,6 +305,11 @@ void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts,
 // ---- IC(0) (tm_ic0.cu) -------------------------------------------------------------------------
 void build_ic(Context& c);                                   // structure (once) + shifted factorization
 void launch_ic_apply(Context& c, const double* r, double* z);
+// the same on any node-block pattern (the bump submodel's tangent)
+void ic_build_structure(IcFactor& F, int nn, const std::vector<int>& nrp, const std::vector<int>& ncol,
+                        const std::vector<long long>& vbase, long long vstride, cudaStream_t st);
+void ic_factor(IcFactor& F, const double* val, cudaStream_t st);
+void ic_apply(IcFactor& F, const double* r, double* z, cudaStream_t st);
 
 // ---- launch accounting ------------------------------------------------------------------------
 enum KernelId { K_APPLY0 = 0, K_SWEEP_SOLID = 1, K_SWEEP_SHELL = 2, K_ASSEMBLE = 3, K_GALERKIN01 = 4, K_APPLY_SHELL = 5, K_NKERNEL };
@@ -352,5 +357,15 @@ void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, c
                          double* stab_d, cudaStream_t s, const tm_pillar* pillar = nullptr);
 void anand_step_device(const tm_anand_material& mat, int npts, double* state_d, const double* eps_d,
                        double T, double dt, double* sig_d, double* D_d, int commit, cudaStream_t s);
+
+// ---- bump submodel (tm_submodel.cu) -------------------------------------------------------------
+struct SubModel;
+SubModel* submodel_create(const tm_submodel_spec& spec);
+void submodel_destroy(SubModel* s);
+bool submodel_step(SubModel& s, double T, double dt, int* newton, double* dMax);
+void submodel_get(SubModel& s, double* u, double* W, double* ebar);
+void submodel_sizes(SubModel& s, int64_t* out);
+void submodel_run(SubModel& s, int nsteps, const double* t, const double* T, const int* cycle, int cycles, double cphi, double sphi,
+                  double* out, double* perCycle, double* loop);
 
 }  // namespace tmg

@@ -1,0 +1,1049 @@
+// Bump submodel on the GPU (FP64): one pitch cell around a bump meshed with B-bar hexes, its
+// cut boundary moved with the global fields, Anand solder Gauss points and incremental elastic
+// parts, Newton with the algorithmic tangent and IC(0)-PCG inner solves, adaptive sub-steps
+// over the cycle history, the hysteresis sampler and the per-cycle inelastic work of the two
+// interface layers.
+//
+// Follows src/core/13-fatigue.js (BumpSubmodel):
+//   constructor, _blockMap, _bbarCache   :518-608   grid, block map, B-bar matrices per element size
+//   _boundary / prescribe                :646-694   boundary nodes, trilinear interpolation of fieldAt
+//   _elastic / _elasRec                  :702-773   step-mean D and thermal stress increment per material
+//   assemble                             :776-853   tangent and internal force (k_sub_assemble + gathers)
+//   _commitElastic                       :856-872
+//   _constrain                           :874-883
+//   _solve                               :886-917   Jacobi-scaled IC(0)-PCG (tm_ic0.cu)
+//   stepTo                               :924-956
+//   _snapshot / _restore                 :994-1002
+//   run                                  :1004-1104  sub-steps, sampleLoop, per-cycle W and ebar
+//
+// Every element is one warp: the lanes share the element's 24 x 24 matrix in shared memory and
+// every entry is summed in the reference's order, as are the assembled blocks (gathered per
+// block in element order) and the internal forces (gathered per node in element order), so the
+// tangent and the residual of one Newton iteration are the reference's for the same state. The
+// inner PCG sums its dots in a fixed order of its own. Compiled without fused multiply-add.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <math_constants.h>
+
+#include "tm_internal.h"
+#include "tm_anand_point.cuh"
+
+namespace tmg {
+
+namespace {
+
+constexpr double SUB_T_AVG = 0.025;          // 00-constants.js:114
+constexpr int SUB_NEWTON_MAXIT = 25;         // :116
+constexpr double SUB_RES_TOL = 1e-6;         // :117
+constexpr double SUB_DU_TOL = 1e-8;          // :118
+constexpr double SUB_INNER_TOL = 1e-8;       // :119
+constexpr double INELASTIC_STEP_MAX = 2e-4;  // :113
+constexpr int SA_WARPS = 4;                  // elements (warps) per block of the element kernels
+enum { M_SUB = 0, M_SOLDER = 1, M_UF = 2, M_SI = 3 };
+
+inline int blocks_for(size_t n, int per) { return (int)((n + per - 1) / per); }
+
+// ---- host helpers: the material integrals of a step (03-materials.js:347-418) ------------------
+double grid_at_s(const double* arr, double T, int stride, int comp) {
+  const double x = T - TGRID_MIN;
+  if (x <= 0) return arr[comp];
+  if (x >= TGRID_N - 1) return arr[(TGRID_N - 1) * stride + comp];
+  const int i = (int)std::floor(x);
+  const double t = x - i;
+  const double a = arr[i * stride + comp], b = arr[(i + 1) * stride + comp];
+  return a + t * (b - a);
+}
+void grid_add_at(const double* grid, double T, int stride, int n, double w, double* out) {
+  double x = T - TGRID_MIN;
+  x = x < 0 ? 0 : (x > TGRID_N - 1 ? TGRID_N - 1 : x);
+  const int i = std::min((int)std::floor(x), TGRID_N - 2);
+  const double t = x - i;
+  const int a = i * stride, b = a + stride;
+  for (int c = 0; c < n; c++) out[c] += w * (grid[a + c] + t * (grid[b + c] - grid[a + c]));
+}
+template <class F> void for_grid_segments(double Ta, double Tb, F fn) {
+  const double lo = std::min(Ta, Tb), hi = std::max(Ta, Tb);
+  for (double t0 = lo; t0 < hi - 1e-12;) {
+    const double t1 = std::min(hi, TGRID_MIN + std::floor(t0 - TGRID_MIN + 1e-9) + 1);
+    fn(0.5 * (t0 + t1), t0, t1);
+    t0 = t1;
+  }
+}
+void grid_mean(const double* grid, int stride, int n, double Ta, double Tb, double* out) {
+  for (int c = 0; c < n; c++) out[c] = 0;
+  const double L = std::fabs(Tb - Ta);
+  if (L < 1e-12) { grid_add_at(grid, Ta, stride, n, 1, out); return; }
+  for_grid_segments(Ta, Tb, [&](double tm, double t0, double t1) { grid_add_at(grid, tm, stride, n, (t1 - t0) / L, out); });
+}
+void grid_stress_increment(const double* Dg, const double* Fg, double Ta, double Tb, double* out) {
+  for (int r = 0; r < 6; r++) out[r] = 0;
+  const double sg = Tb >= Ta ? 1 : -1;
+  double D[36];
+  for_grid_segments(Ta, Tb, [&](double tm, double t0, double t1) {
+    for (auto& v : D) v = 0;
+    grid_add_at(Dg, tm, 36, 36, 1, D);
+    const double f0 = grid_at_s(Fg, t1, 3, 0) - grid_at_s(Fg, t0, 3, 0), f1 = grid_at_s(Fg, t1, 3, 1) - grid_at_s(Fg, t0, 3, 1),
+                 f2 = grid_at_s(Fg, t1, 3, 2) - grid_at_s(Fg, t0, 3, 2);
+    for (int r = 0; r < 6; r++) out[r] += sg * (D[6 * r] * f0 + D[6 * r + 1] * f1 + D[6 * r + 2] * f2);
+  });
+}
+double grid_modulus_strain_increment(const double* E, const double* F, double Ta, double Tb) {
+  const double sg = Tb >= Ta ? 1 : -1;
+  double s = 0;
+  for_grid_segments(Ta, Tb, [&](double tm, double t0, double t1) {
+    s += grid_at_s(E, tm, 1, 0) * (grid_at_s(F, t1, 1, 0) - grid_at_s(F, t0, 1, 0));
+  });
+  return sg * s;
+}
+// isoD through isoEC and orthoD (03-materials.js:222-249), invDense (01-util.js:110-134)
+void iso_d(double E, double nu, double nuMax, double* out) {
+  const double nc = std::min(nu, nuMax);
+  const double G = E / (2 * (1 + nc));
+  const double S[9] = {1 / E, -nc / E, -nc / E, -nc / E, 1 / E, -nc / E, -nc / E, -nc / E, 1 / E};
+  double M[18];
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 6; j++) M[i * 6 + j] = j < 3 ? S[i * 3 + j] : (j - 3 == i ? 1 : 0);
+  for (int c = 0; c < 3; c++) {
+    int p = c;
+    double best = std::fabs(M[c * 6 + c]);
+    for (int r = c + 1; r < 3; r++) { const double v = std::fabs(M[r * 6 + c]); if (v > best) { best = v; p = r; } }
+    if (best == 0) fail(TM_BAD_INPUT, "submodel: singular isotropic compliance");
+    if (p != c) for (int j = 0; j < 6; j++) std::swap(M[c * 6 + j], M[p * 6 + j]);
+    const double inv = 1 / M[c * 6 + c];
+    for (int j = 0; j < 6; j++) M[c * 6 + j] *= inv;
+    for (int r = 0; r < 3; r++) {
+      if (r == c) continue;
+      const double f = M[r * 6 + c];
+      if (f == 0) continue;
+      for (int j = 0; j < 6; j++) M[r * 6 + j] -= f * M[c * 6 + j];
+    }
+  }
+  for (int q = 0; q < 36; q++) out[q] = 0;
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) out[i * 6 + j] = M[i * 6 + 3 + j];
+  out[21] = G; out[28] = G; out[35] = G;
+}
+
+// boxDerivs (07-element.js:19-30) and bbarMatrix (13-fatigue.js:474-491)
+const int HX[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, HY[8] = {-1, -1, 1, 1, -1, -1, 1, 1}, HZ[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+void box_derivs(double hx, double hy, double hz, double xi, double eta, double zeta, double* dx, double* dy, double* dz) {
+  const double sx = 2 / hx, sy = 2 / hy, sz = 2 / hz;
+  for (int a = 0; a < 8; a++) {
+    const double xa = HX[a], ya = HY[a], za = HZ[a];
+    dx[a] = xa * (1 + ya * eta) * (1 + za * zeta) * 0.125 * sx;
+    dy[a] = ya * (1 + xa * xi) * (1 + za * zeta) * 0.125 * sy;
+    dz[a] = za * (1 + xa * xi) * (1 + ya * eta) * 0.125 * sz;
+  }
+}
+void bbar_matrix(double hx, double hy, double hz, double xi, double eta, double zeta, double* Bb) {
+  double dx[8], dy[8], dz[8], cx[8], cy[8], cz[8];
+  box_derivs(hx, hy, hz, xi, eta, zeta, dx, dy, dz);
+  box_derivs(hx, hy, hz, 0, 0, 0, cx, cy, cz);
+  for (int q = 0; q < 144; q++) Bb[q] = 0;
+  for (int a = 0; a < 8; a++) {
+    const int c = 3 * a;
+    const double ddx = (cx[a] - dx[a]) / 3, ddy = (cy[a] - dy[a]) / 3, ddz = (cz[a] - dz[a]) / 3;
+    Bb[0 * 24 + c] = dx[a] + ddx; Bb[0 * 24 + c + 1] = ddy; Bb[0 * 24 + c + 2] = ddz;
+    Bb[1 * 24 + c] = ddx; Bb[1 * 24 + c + 1] = dy[a] + ddy; Bb[1 * 24 + c + 2] = ddz;
+    Bb[2 * 24 + c] = ddx; Bb[2 * 24 + c + 1] = ddy; Bb[2 * 24 + c + 2] = dz[a] + ddz;
+    Bb[3 * 24 + c] = dy[a]; Bb[3 * 24 + c + 1] = dx[a];
+    Bb[4 * 24 + c + 1] = dz[a]; Bb[4 * 24 + c + 2] = dy[a];
+    Bb[5 * 24 + c] = dz[a]; Bb[5 * 24 + c + 2] = dx[a];
+  }
+}
+
+// ---- device kernels ------------------------------------------------------------------------------
+constexpr unsigned FULLMASK = 0xffffffffu;
+
+// prescribe: thread per boundary node, fieldAt blended between global temperatures i and i+1
+__global__ void k_sub_prescribe(int nb, const int* __restrict__ bNodes, const int* __restrict__ bGlob, const double* __restrict__ bW,
+                                const double* __restrict__ fa, const double* __restrict__ fb, double t, const double* __restrict__ u25,
+                                double* __restrict__ u) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nb) return;
+  double ux = 0, uy = 0, uz = 0;
+  for (int c = 0; c < 8; c++) {
+    const int gn = bGlob[8 * q + c];
+    const double w = bW[8 * q + c];
+    const double tx = fa[3 * gn] + t * (fb[3 * gn] - fa[3 * gn]), ty = fa[3 * gn + 1] + t * (fb[3 * gn + 1] - fa[3 * gn + 1]),
+                 tz = fa[3 * gn + 2] + t * (fb[3 * gn + 2] - fa[3 * gn + 2]);
+    ux += w * (tx - u25[3 * gn]); uy += w * (ty - u25[3 * gn + 1]); uz += w * (tz - u25[3 * gn + 2]);
+  }
+  const int n = bNodes[q];
+  u[3 * n] = ux; u[3 * n + 1] = uy; u[3 * n + 2] = uz;
+}
+
+// assemble, warp per element: elastic elements build K_e, f_th once per step (fresh) and give
+// f_e = f_n + K_e (u_e - u_n,e) - f_th; solder elements step their 8 Anand points (one lane each)
+// and sum f_e and, with wantK, K_e = sum_g w B^T D_g B
+__global__ void __launch_bounds__(32 * SA_WARPS)
+k_sub_assemble(int ne, const int* __restrict__ conn, const int* __restrict__ eMat, const int* __restrict__ eBb, const double* __restrict__ Bm,
+               const double* __restrict__ Bw, const int* __restrict__ eAn, Point* __restrict__ pts, const double* __restrict__ u,
+               const double* __restrict__ uN, const double* __restrict__ eFn, double* __restrict__ eK, double* __restrict__ eF,
+               double* __restrict__ fe, double* __restrict__ dmaxE, const double* __restrict__ elas, int fresh, int wantK, AnandConst P,
+               StepK kc, double fSolder) {
+  __shared__ double sK[SA_WARPS][576];
+  __shared__ double sDB[SA_WARPS][144];
+  __shared__ double sSig[SA_WARPS][48];
+  __shared__ double sD[SA_WARPS][288];
+  __shared__ double sUe[SA_WARPS][24];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * SA_WARPS + w;
+  if (e >= ne) return;
+  double* K = sK[w];
+  double* DB = sDB[w];
+  double* ue = sUe[w];
+  const double* B = Bm + (size_t)eBb[e] * 8 * 144;
+  const double wt = Bw[eBb[e]];
+  const int an = eAn[e];
+  if (lane < 24) ue[lane] = u[3 * (size_t)conn[8 * (size_t)e + lane / 3] + lane % 3];
+  __syncwarp();
+  if (an < 0) {
+    double* Kc = eK + 576 * (size_t)e;
+    double* fc = eF + 24 * (size_t)e;
+    if (fresh) {
+      const double* D = elas + 42 * eMat[e];
+      const double* sth = D + 36;
+      for (int o = lane; o < 576; o += 32) K[o] = 0;
+      double fcl = 0;
+      __syncwarp();
+      for (int g = 0; g < 8; g++) {
+        const double* Bb = B + 144 * g;
+        if (lane < 24) {
+          double sum = 0;
+          for (int r = 0; r < 6; r++) sum += Bb[r * 24 + lane] * sth[r];
+          fcl += wt * sum;
+        }
+        for (int o = lane; o < 144; o += 32) {
+          const int r = o / 24, c = o % 24;
+          double sum = 0;
+          for (int t = 0; t < 6; t++) sum += D[r * 6 + t] * Bb[t * 24 + c];
+          DB[o] = sum;
+        }
+        __syncwarp();
+        for (int o = lane; o < 576; o += 32) {
+          const int a = o / 24, b = o % 24;
+          if (b < a) continue;
+          double sum = 0;
+          for (int r = 0; r < 6; r++) sum += Bb[r * 24 + a] * DB[r * 24 + b];
+          K[o] += wt * sum;
+        }
+        __syncwarp();
+      }
+      for (int o = lane; o < 576; o += 32) {
+        const int a = o / 24, b = o % 24;
+        Kc[o] = b < a ? K[b * 24 + a] : K[o];
+      }
+      if (lane < 24) fc[lane] = fcl;
+      __syncwarp();
+    }
+    if (lane < 24) ue[lane] -= uN[3 * (size_t)conn[8 * (size_t)e + lane / 3] + lane % 3];
+    __syncwarp();
+    if (lane < 24) {
+      double sum = eFn[24 * (size_t)e + lane] - fc[lane];
+      for (int b = 0; b < 24; b++) sum += Kc[lane * 24 + b] * ue[b];
+      fe[24 * (size_t)e + lane] = sum;
+    }
+    if (lane == 0) dmaxE[e] = 0;
+    return;
+  }
+  // solder: the 8 Gauss points, one lane each
+  double d = 0;
+  if (lane < 8) {
+    const double* Bb = B + 144 * lane;
+    double eps[6];
+    for (int r = 0; r < 6; r++) {
+      double s = 0;
+      for (int c = 0; c < 24; c++) s += Bb[r * 24 + c] * ue[c];
+      eps[r] = s;
+    }
+    eps[0] -= fSolder; eps[1] -= fSolder; eps[2] -= fSolder;
+    d = anand_step(P, pts[8 * (size_t)an + lane], eps, kc, sSig[w] + 6 * lane, sD[w] + 36 * lane, wantK != 0);
+  }
+  for (int off = 16; off > 0; off >>= 1) d = fmax(d, __shfl_xor_sync(FULLMASK, d, off));
+  if (lane == 0) dmaxE[e] = d;
+  __syncwarp();
+  if (lane < 24) {
+    double f = 0;
+    for (int g = 0; g < 8; g++) {
+      const double* Bb = B + 144 * g;
+      const double* sig = sSig[w] + 6 * g;
+      double s = 0;
+      for (int r = 0; r < 6; r++) s += Bb[r * 24 + lane] * sig[r];
+      f += wt * s;
+    }
+    fe[24 * (size_t)e + lane] = f;
+  }
+  if (!wantK) return;
+  for (int o = lane; o < 576; o += 32) K[o] = 0;
+  __syncwarp();
+  for (int g = 0; g < 8; g++) {
+    const double* Bb = B + 144 * g;
+    const double* Dg = sD[w] + 36 * g;
+    for (int o = lane; o < 144; o += 32) {
+      const int r = o / 24, c = o % 24;
+      double s = 0;
+      for (int t = 0; t < 6; t++) s += Dg[r * 6 + t] * Bb[t * 24 + c];
+      DB[o] = s;
+    }
+    __syncwarp();
+    for (int o = lane; o < 576; o += 32) {
+      const int a = o / 24, b = o % 24;
+      if (b < a) continue;
+      double s = 0;
+      for (int r = 0; r < 6; r++) s += Bb[r * 24 + a] * DB[r * 24 + b];
+      K[o] += wt * s;
+    }
+    __syncwarp();
+  }
+  double* Ke = eK + 576 * (size_t)e;
+  for (int o = lane; o < 576; o += 32) {
+    const int a = o / 24, b = o % 24;
+    Ke[o] = b < a ? K[b * 24 + a] : K[o];
+  }
+}
+
+// the tangent's blocks, thread per block: the element contributions in element order, then the
+// constrained rows and columns zeroed off the diagonal (_constrain)
+__global__ void k_sub_gather_val(int nb, const int* __restrict__ blkRow, const int* __restrict__ col, const int* __restrict__ start,
+                                 const int* __restrict__ list, const double* __restrict__ eK, const uint8_t* __restrict__ isC,
+                                 double* __restrict__ val) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nb) return;
+  const int i = blkRow[k], j = col[k];
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int l = start[k]; l < start[k + 1]; l++) {
+    const int code = list[l], e = code >> 6, a = (code >> 3) & 7, b = code & 7;
+    const double* Ke = eK + 576 * (size_t)e;
+    for (int p = 0; p < 3; p++)
+      for (int q = 0; q < 3; q++) v[3 * p + q] += Ke[(3 * a + p) * 24 + 3 * b + q];
+  }
+  for (int p = 0; p < 3; p++)
+    for (int q = 0; q < 3; q++) {
+      const int r = 3 * i + p, c = 3 * j + q;
+      if ((isC[r] || isC[c]) && r != c) v[3 * p + q] = 0;
+      val[9 * (size_t)k + 3 * p + q] = v[3 * p + q];
+    }
+}
+
+// internal force, thread per DOF: the element forces in element order
+__global__ void k_sub_gather_rint(int ndof, const int* __restrict__ start, const int* __restrict__ list, const double* __restrict__ fe,
+                                  double* __restrict__ rint) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ndof) return;
+  const int n = q / 3, p = q % 3;
+  double s = 0;
+  for (int l = start[n]; l < start[n + 1]; l++) {
+    const int code = list[l], e = code >> 3, a = code & 7;
+    s += fe[24 * (size_t)e + 3 * a + p];
+  }
+  rint[q] = s;
+}
+
+// deterministic sums over one block: out[0..m) = sums of m products (pairs of arrays, or with a mask)
+// kind 0: a.a over the free DOFs, a.a over all (the Newton residual norms)
+// kind 1: a.b
+// kind 2: after u += du on the free DOFs: du.du over the free DOFs, u.u over all
+__global__ void __launch_bounds__(1024) k_sub_sums(int n, int kind, const double* __restrict__ a, double* __restrict__ b,
+                                                   const uint8_t* __restrict__ isC, double* __restrict__ out) {
+  __shared__ double s0[1024], s1[1024];
+  double x0 = 0, x1 = 0;
+  for (int q = threadIdx.x; q < n; q += 1024) {
+    if (kind == 0) {
+      const double v = a[q];
+      if (!isC[q]) x0 += v * v;
+      x1 += v * v;
+    } else if (kind == 1) {
+      x0 += a[q] * b[q];
+    } else {
+      if (!isC[q]) { b[q] += a[q]; x0 += a[q] * a[q]; }
+      x1 += b[q] * b[q];
+    }
+  }
+  s0[threadIdx.x] = x0; s1[threadIdx.x] = x1;
+  __syncthreads();
+  for (int h = 512; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) { s0[threadIdx.x] += s0[threadIdx.x + h]; s1[threadIdx.x] += s1[threadIdx.x + h]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { out[0] = s0[0]; out[1] = s1[0]; }
+}
+
+// _solve's scaling: s from the tangent's diagonal, the scaled copy, b = rhs s with rhs = -rint
+// on the free DOFs
+__global__ void k_sub_scale_s(int nn, const int* __restrict__ diag, const double* __restrict__ val, double* __restrict__ s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const double* v = val + 9 * (size_t)diag[i];
+  s[3 * i] = 1 / sqrt(fmax(v[0], 1e-300)); s[3 * i + 1] = 1 / sqrt(fmax(v[4], 1e-300)); s[3 * i + 2] = 1 / sqrt(fmax(v[8], 1e-300));
+}
+__global__ void k_sub_scale_vals(int nb, const int* __restrict__ blkRow, const int* __restrict__ col, const double* __restrict__ s,
+                                 const double* __restrict__ val, double* __restrict__ vals) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nb) return;
+  const int i = blkRow[k], j = col[k];
+  for (int p = 0; p < 3; p++)
+    for (int q = 0; q < 3; q++) vals[9 * (size_t)k + 3 * p + q] = val[9 * (size_t)k + 3 * p + q] * (s[3 * i + p] * s[3 * j + q]);
+}
+__global__ void k_sub_rhs(int n, const double* __restrict__ rint, const uint8_t* __restrict__ isC, const double* __restrict__ s,
+                          double* __restrict__ b, double* __restrict__ r, double* __restrict__ x) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const double rhs = isC[q] ? 0 : -rint[q];
+  const double v = rhs * s[q];
+  b[q] = v; r[q] = v; x[q] = 0;
+}
+// fullMatVec (09-assembly.js:151-165), thread per node
+__global__ void k_sub_spmv(int nn, const int* __restrict__ rowPtr, const int* __restrict__ col, const double* __restrict__ val,
+                           const double* __restrict__ x, double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  double y0 = 0, y1 = 0, y2 = 0;
+  for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+    const int j = col[k];
+    const double* v = val + 9 * (size_t)k;
+    const double x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
+    y0 += v[0] * x0 + v[1] * x1 + v[2] * x2;
+    y1 += v[3] * x0 + v[4] * x1 + v[5] * x2;
+    y2 += v[6] * x0 + v[7] * x1 + v[8] * x2;
+  }
+  y[3 * i] = y0; y[3 * i + 1] = y1; y[3 * i + 2] = y2;
+}
+__global__ void k_sub_axpy2(int n, double alpha, const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ x,
+                            double* __restrict__ r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] += alpha * p[i];
+  r[i] += -alpha * q[i];
+}
+__global__ void k_sub_xpby(int n, const double* __restrict__ z, double beta, double* __restrict__ p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = z[i] + beta * p[i];
+}
+__global__ void k_sub_mul(int n, const double* __restrict__ s, double* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= s[i];
+}
+
+// _commitElastic, warp per elastic element: Gauss-point stresses and the element's internal force
+__global__ void __launch_bounds__(32 * SA_WARPS)
+k_sub_commit_elastic(int ne, const int* __restrict__ conn, const int* __restrict__ eMat, const int* __restrict__ eBb,
+                     const double* __restrict__ Bm, const double* __restrict__ Bw, const int* __restrict__ eAn, const double* __restrict__ u,
+                     const double* __restrict__ uN, const double* __restrict__ elas, double* __restrict__ sigE, double* __restrict__ eFn) {
+  __shared__ double sDue[SA_WARPS][24];
+  __shared__ double sSg[SA_WARPS][6];
+  __shared__ double sDe[SA_WARPS][6];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * SA_WARPS + w;
+  if (e >= ne || eAn[e] >= 0) return;
+  const double* D = elas + 42 * eMat[e];
+  const double* sth = D + 36;
+  const double* B = Bm + (size_t)eBb[e] * 8 * 144;
+  const double wt = Bw[eBb[e]];
+  double* due = sDue[w];
+  if (lane < 24) {
+    const size_t n = 3 * (size_t)conn[8 * (size_t)e + lane / 3] + lane % 3;
+    due[lane] = u[n] - uN[n];
+  }
+  __syncwarp();
+  double fn = 0;
+  for (int g = 0; g < 8; g++) {
+    const double* Bb = B + 144 * g;
+    double* so = sigE + 48 * (size_t)e + 6 * g;
+    if (lane < 6) {
+      double s2 = 0;
+      for (int c = 0; c < 24; c++) s2 += Bb[lane * 24 + c] * due[c];
+      sDe[w][lane] = s2;
+    }
+    __syncwarp();
+    if (lane < 6) {
+      double s2 = -sth[lane];
+      for (int c = 0; c < 6; c++) s2 += D[lane * 6 + c] * sDe[w][c];
+      so[lane] += s2;
+      sSg[w][lane] = so[lane];
+    }
+    __syncwarp();
+    if (lane < 24) {
+      double s2 = 0;
+      for (int r = 0; r < 6; r++) s2 += Bb[r * 24 + lane] * sSg[w][r];
+      fn += wt * s2;
+    }
+    __syncwarp();
+  }
+  if (lane < 24) eFn[24 * (size_t)e + lane] = fn;
+}
+
+__global__ void k_sub_commit_points(int np, Point* __restrict__ pts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < np) commit(pts[i]);
+}
+
+// _snapshot / _restore of the solder points' committed state (ep, s, ebar, W, sigEq)
+__global__ void k_sub_points_copy(int np, const Point* __restrict__ from, Point* __restrict__ to) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const Point& a = from[i];
+  Point& b = to[i];
+  for (int c = 0; c < 6; c++) b.ep[c] = a.ep[c];
+  b.s = a.s; b.ebar = a.ebar; b.W = a.W; b.sigEq = a.sigEq;
+}
+
+// sampleLoop (13-fatigue.js:1032-1052) over one layer list: per entry the strain at the Gauss
+// point (its own B-bar matrix), the stress at the committed plastic state (a 1e-9 s step) and
+// the weighted shear stress and strain along the site's radial direction
+__global__ void k_sub_sample(int cnt, const int* __restrict__ gp, const double* __restrict__ Bs, const int* __restrict__ conn,
+                             const double* __restrict__ u, Point* __restrict__ pts, const int* __restrict__ eAn, AnandConst P,
+                             const double* __restrict__ Etab, double T, double f, double cphi, double sphi, double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cnt) return;
+  const int idx = gp[t], e = idx / 8, g = idx % 8;
+  const double* Bb = Bs + 144 * (size_t)t;
+  double ue[24], eps[6], sig[6];
+  for (int a = 0; a < 8; a++) {
+    const int n = conn[8 * (size_t)e + a];
+    ue[3 * a] = u[3 * n]; ue[3 * a + 1] = u[3 * n + 1]; ue[3 * a + 2] = u[3 * n + 2];
+  }
+  for (int r = 0; r < 6; r++) {
+    double s = 0;
+    for (int c = 0; c < 24; c++) s += Bb[r * 24 + c] * ue[c];
+    eps[r] = s;
+  }
+  eps[0] -= f; eps[1] -= f; eps[2] -= f;
+  const StepK k = step_constants(P, Etab, T, 1e-9);
+  anand_step(P, pts[8 * (size_t)eAn[e] + g], eps, k, sig, nullptr, false);
+  out[2 * t] = sig[5] * cphi + sig[4] * sphi;
+  out[2 * t + 1] = eps[5] * cphi + eps[4] * sphi;
+}
+
+// the layer averages of W and ebar (avg of run, :1020), in list order: one thread
+__global__ void k_sub_layer_avg(int nDie, const int* __restrict__ dieGp, const double* __restrict__ dieW, int nSub,
+                                const int* __restrict__ subGp, const double* __restrict__ subW, const Point* __restrict__ pts,
+                                const int* __restrict__ eAn, double* __restrict__ out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int li = 0; li < 2; li++) {
+    const int cnt = li == 0 ? nDie : nSub;
+    const int* gp = li == 0 ? dieGp : subGp;
+    const double* wv = li == 0 ? dieW : subW;
+    double sW = 0, sE = 0, ws = 0;
+    for (int q = 0; q < cnt; q++) {
+      const int idx = gp[q];
+      const Point& p = pts[8 * (size_t)eAn[idx / 8] + idx % 8];
+      sW += wv[q] * p.W; sE += wv[q] * p.ebar; ws += wv[q];
+    }
+    out[2 * li] = ws != 0 ? sW / ws : CUDART_NAN;
+    out[2 * li + 1] = ws != 0 ? sE / ws : CUDART_NAN;
+  }
+  // 0: W die, 1: ebar die, 2: W sub, 3: ebar sub
+}
+
+}  // namespace
+
+// ---- the submodel ----------------------------------------------------------------------------------
+struct SubModel {
+  cudaStream_t st = nullptr;
+  int nx = 0, ny = 0, nz = 0, nn = 0, ne = 0, ndof = 0, nbk = 0, nbnd = 0, nsolderE = 0;
+  std::vector<double> xs, ys, zs, ts, solderE, solderF, ufE, ufF, siD, siF, subD, subF;
+  double ufNu = 0, nuMax = 0, zt = 0, zaf = 0;
+  AnandConst P{};
+  int elasticSolder = 0;
+  std::vector<int> conn, eIJK, eMat, eAn, rowPtr, col, diag, blkRow;
+  std::vector<uint8_t> isC;
+  int nglob = 0;
+  // device
+  DBuf<int> d_conn, d_eMat, d_eBb, d_eAn, d_rowPtr, d_col, d_diag, d_blkRow, d_blkStart, d_blkList, d_nodeStart, d_nodeList;
+  DBuf<int> d_bNodes, d_bGlob;
+  DBuf<uint8_t> d_isC;
+  DBuf<double> d_Bm, d_Bw, d_bW, d_fields, d_u25, d_solderE, d_elas;
+  DBuf<double> d_u, d_uN, d_sigE, d_eFn, d_eK, d_eF, d_fe, d_dmax, d_val, d_vals, d_s, d_rint, d_b, d_r, d_z, d_p, d_q, d_x, d_sums;
+  DBuf<Point> d_pts, d_snapPts;
+  DBuf<double> d_snapU, d_snapSig, d_snapFn;
+  IcFactor ic;
+  bool pcBuilt = false, pcStale = false;
+  int pcIters = 0;
+  double Tn = 25;
+  bool haveKey = false;
+  double keyTn = 0, keyT = 0;
+  // layer lists of run(): Gauss points (e*8 + g), volume weights, their own B-bar matrices
+  std::vector<int> dieGp, subGp;
+  std::vector<double> dieW, subW;
+  DBuf<int> d_dieGp, d_subGp;
+  DBuf<double> d_dieW, d_subW, d_dieB, d_subB, d_sample, d_avg;
+
+  ~SubModel() {
+    if (st) cudaStreamDestroy(st);
+  }
+
+  void sums(int n, int kind, const double* a, double* b, double* h) {
+    note_launch();
+    k_sub_sums<<<1, 1024, 0, st>>>(n, kind, a, b, d_isC.p, d_sums.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+    TM_CUDA_CHECK(cudaMemcpyAsync(h, d_sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TM_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+
+  // _elastic (13-fatigue.js:702-757), without the homogenized-layer consistency mode
+  void elastic(int mat, double Ta, double Tb, double* D, double* sth) const {
+    auto rowSum = [&](int r) { return D[r * 6] + D[r * 6 + 1] + D[r * 6 + 2]; };
+    auto isoStep = [&](const std::vector<double>& E, const std::vector<double>& F, double nu) {
+      double Em;
+      grid_mean(E.data(), 1, 1, Ta, Tb, &Em);
+      const double ef = grid_modulus_strain_increment(E.data(), F.data(), Ta, Tb) / Em;
+      iso_d(Em, nu, nuMax, D);
+      for (int r = 0; r < 6; r++) sth[r] = rowSum(r) * ef;
+    };
+    if (mat == M_SI) {
+      for (int q = 0; q < 36; q++) D[q] = siD[q];
+      const double f = grid_at_s(siF.data(), Tb, 1, 0) - grid_at_s(siF.data(), Ta, 1, 0);
+      for (int r = 0; r < 6; r++) sth[r] = rowSum(r) * f;
+      return;
+    }
+    if (mat == M_UF) { isoStep(ufE, ufF, ufNu); return; }
+    if (mat == M_SOLDER) { isoStep(solderE, solderF, P.nu); return; }
+    grid_mean(subD.data(), 36, 36, Ta, Tb, D);
+    grid_stress_increment(subD.data(), subF.data(), Ta, Tb, sth);
+  }
+
+  void prescribe(double T) {
+    int i;
+    const int n = (int)ts.size();
+    if (T <= ts[0]) i = 0;
+    else if (T >= ts[n - 1]) i = n - 2;
+    else {
+      int lo = 0, hi = n - 1;
+      while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (ts[mid] <= T) lo = mid; else hi = mid; }
+      i = lo;
+    }
+    double t = (T - ts[i]) / (ts[i + 1] - ts[i]);
+    t = t < 0 ? 0 : (t > 1 ? 1 : t);
+    const size_t G = 3 * (size_t)nglob;
+    note_launch();
+    k_sub_prescribe<<<blocks_for(nbnd, 128), 128, 0, st>>>(nbnd, d_bNodes.p, d_bGlob.p, d_bW.p, d_fields.p + G * i, d_fields.p + G * (i + 1), t,
+                                                          d_u25.p, d_u.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+  }
+
+  // assemble (13-fatigue.js:776-853); returns the largest plastic increment
+  double assemble(double T, double dt, bool wantK) {
+    const bool fresh = !(haveKey && keyTn == Tn && keyT == T);
+    if (fresh) {
+      double h[4 * 42];
+      for (int m = 0; m < 4; m++) elastic(m, Tn, T, h + 42 * m, h + 42 * m + 36);
+      d_elas.upload(h, 4 * 42, st);
+    }
+    // the solder constants of the step and its thermal strain from 25 degC
+    const double E = grid_at_s(solderE.data(), T, 1, 0), nu = P.nu;
+    const double expQ = std::exp(P.QR / (T + 273.15));
+    const StepK kc{E / (2 * (1 + nu)), E / (3 * (1 - 2 * nu)), expQ, dt * P.A / expQ, dt};
+    const double fSolder = grid_at_s(solderF.data(), T, 1, 0) - grid_at_s(solderF.data(), 25, 1, 0);
+    note_launch(wantK ? 3 : 2);
+    k_sub_assemble<<<blocks_for(ne, SA_WARPS), 32 * SA_WARPS, 0, st>>>(ne, d_conn.p, d_eMat.p, d_eBb.p, d_Bm.p, d_Bw.p, d_eAn.p, d_pts.p, d_u.p,
+                                                                      d_uN.p, d_eFn.p, d_eK.p, d_eF.p, d_fe.p, d_dmax.p, d_elas.p, fresh,
+                                                                      wantK, P, kc, fSolder);
+    TM_CUDA_CHECK(cudaGetLastError());
+    k_sub_gather_rint<<<blocks_for(ndof, 256), 256, 0, st>>>(ndof, d_nodeStart.p, d_nodeList.p, d_fe.p, d_rint.p);
+    if (wantK)
+      k_sub_gather_val<<<blocks_for(nbk, 128), 128, 0, st>>>(nbk, d_blkRow.p, d_col.p, d_blkStart.p, d_blkList.p, d_eK.p, d_isC.p, d_val.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+    haveKey = true; keyTn = Tn; keyT = T;
+    std::vector<double> dm(ne);
+    d_dmax.download(dm.data(), ne, st);
+    TM_CUDA_CHECK(cudaStreamSynchronize(st));
+    double dMax = 0;
+    for (int e = 0; e < ne; e++) if (dm[e] > dMax) dMax = dm[e];
+    return dMax;
+  }
+
+  // _solve (13-fatigue.js:886-917): d_x = the Newton increment
+  int solve(double tol) {
+    note_launch(3);
+    k_sub_scale_s<<<blocks_for(nn, 128), 128, 0, st>>>(nn, d_diag.p, d_val.p, d_s.p);
+    k_sub_scale_vals<<<blocks_for(nbk, 128), 128, 0, st>>>(nbk, d_blkRow.p, d_col.p, d_s.p, d_val.p, d_vals.p);
+    k_sub_rhs<<<blocks_for(ndof, 256), 256, 0, st>>>(ndof, d_rint.p, d_isC.p, d_s.p, d_b.p, d_r.p, d_x.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+    if (!pcBuilt || pcStale) { ic_factor(ic, d_vals.p, st); pcBuilt = true; pcStale = false; pcIters = 0; }
+    double h[2];
+    sums(ndof, 1, d_b.p, d_b.p, h);
+    const double bn = std::sqrt(h[0]);
+    if (bn == 0) return 0;
+    ic_apply(ic, d_r.p, d_z.p, st);
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_p.p, d_z.p, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    sums(ndof, 1, d_r.p, d_z.p, h);
+    double rz = h[0];
+    int it;
+    const int nb = blocks_for(ndof, 256);
+    for (it = 1; it <= 2000; it++) {
+      note_launch();
+      k_sub_spmv<<<blocks_for(nn, 128), 128, 0, st>>>(nn, d_rowPtr.p, d_col.p, d_vals.p, d_p.p, d_q.p);
+      sums(ndof, 1, d_p.p, d_q.p, h);
+      const double alpha = rz / h[0];
+      note_launch();
+      k_sub_axpy2<<<nb, 256, 0, st>>>(ndof, alpha, d_p.p, d_q.p, d_x.p, d_r.p);
+      sums(ndof, 1, d_r.p, d_r.p, h);
+      if (std::sqrt(h[0]) / bn < tol) break;
+      ic_apply(ic, d_r.p, d_z.p, st);
+      sums(ndof, 1, d_r.p, d_z.p, h);
+      const double rz2 = h[0], beta = rz2 / rz;
+      rz = rz2;
+      note_launch();
+      k_sub_xpby<<<nb, 256, 0, st>>>(ndof, d_z.p, beta, d_p.p);
+    }
+    note_launch();
+    k_sub_mul<<<nb, 256, 0, st>>>(ndof, d_s.p, d_x.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+    if (!pcIters) pcIters = it;
+    else if (it > 2 * pcIters) pcStale = true;
+    return it;
+  }
+
+  void commit_elastic(double T) {
+    // the step's material records are those of the assembly from Tn to T
+    if (!(haveKey && keyTn == Tn && keyT == T)) {
+      double h[4 * 42];
+      for (int m = 0; m < 4; m++) elastic(m, Tn, T, h + 42 * m, h + 42 * m + 36);
+      d_elas.upload(h, 4 * 42, st);
+    }
+    note_launch();
+    k_sub_commit_elastic<<<blocks_for(ne, SA_WARPS), 32 * SA_WARPS, 0, st>>>(ne, d_conn.p, d_eMat.p, d_eBb.p, d_Bm.p, d_Bw.p, d_eAn.p, d_u.p,
+                                                                            d_uN.p, d_elas.p, d_sigE.p, d_eFn.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_uN.p, d_u.p, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    Tn = T;
+  }
+
+  // stepTo (13-fatigue.js:924-956)
+  bool step_to(double T, double dt, int* newton, double* dMaxOut) {
+    prescribe(T);
+    double dMax = 0, rPrev = INFINITY;
+    bool converged = false, haveK = false;
+    int it;
+    double h[2];
+    for (it = 1; it <= SUB_NEWTON_MAXIT; it++) {
+      const bool wantK = it <= 2 || !haveK;
+      dMax = assemble(T, dt, wantK);
+      if (wantK) haveK = true;
+      sums(ndof, 0, d_rint.p, nullptr, h);
+      const double rn = std::sqrt(h[0]), fn = std::sqrt(h[1]);
+      const double ref = std::max(fn, 1e-30);
+      if (rn / ref < SUB_RES_TOL) { converged = true; break; }
+      if (!wantK && rn > 0.5 * rPrev) assemble(T, dt, true);   // stalled with the frozen tangent: refresh it
+      rPrev = rn;
+      solve(std::max(SUB_INNER_TOL, std::min(1e-3, 0.01 * SUB_RES_TOL * ref / std::max(rn, 1e-300))));
+      sums(ndof, 2, d_x.p, d_u.p, h);   // u += du on the free DOFs
+      if (std::sqrt(h[0]) < SUB_DU_TOL * std::max(std::sqrt(h[1]), 1e-30)) { converged = true; it++; break; }
+    }
+    if (converged) {
+      dMax = assemble(T, dt, false);
+      if (nsolderE) {
+        note_launch();
+        k_sub_commit_points<<<blocks_for(8 * (size_t)nsolderE, 128), 128, 0, st>>>(8 * nsolderE, d_pts.p);
+        TM_CUDA_CHECK(cudaGetLastError());
+      }
+      commit_elastic(T);
+    }
+    *newton = it; *dMaxOut = dMax;
+    TM_CUDA_CHECK(cudaStreamSynchronize(st));
+    return converged;
+  }
+
+  void snapshot() {
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_snapU.p, d_u.p, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_snapSig.p, d_sigE.p, 48 * (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_snapFn.p, d_eFn.p, 24 * (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (nsolderE) {
+      note_launch();
+      k_sub_points_copy<<<blocks_for(8 * (size_t)nsolderE, 128), 128, 0, st>>>(8 * nsolderE, d_pts.p, d_snapPts.p);
+    }
+  }
+  void restore(double snapTn) {
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_u.p, d_snapU.p, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_uN.p, d_snapU.p, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_sigE.p, d_snapSig.p, 48 * (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    TM_CUDA_CHECK(cudaMemcpyAsync(d_eFn.p, d_snapFn.p, 24 * (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (nsolderE) {
+      note_launch();
+      k_sub_points_copy<<<blocks_for(8 * (size_t)nsolderE, 128), 128, 0, st>>>(8 * nsolderE, d_snapPts.p, d_pts.p);
+    }
+    Tn = snapTn;
+  }
+
+  // sampleLoop: the two lists in order (a point in both is stepped twice, as in the reference)
+  void sample_loop(double T, double cphi, double sphi, double* L) {
+    const double f = grid_at_s(solderF.data(), T, 1, 0) - grid_at_s(solderF.data(), 25, 1, 0);
+    double s[6] = {0, 0, 0, 0, 0, 0};   // tS, gS, wS, tB, gB, wB
+    for (int li = 0; li < 2; li++) {
+      const int cnt = li == 0 ? (int)dieGp.size() : (int)subGp.size();
+      if (!cnt) continue;
+      note_launch();
+      k_sub_sample<<<blocks_for(cnt, 64), 64, 0, st>>>(cnt, li == 0 ? d_dieGp.p : d_subGp.p, li == 0 ? d_dieB.p : d_subB.p, d_conn.p, d_u.p,
+                                                      d_pts.p, d_eAn.p, P, d_solderE.p, T, f, cphi, sphi, d_sample.p);
+      TM_CUDA_CHECK(cudaGetLastError());
+      std::vector<double> o(2 * (size_t)cnt);
+      d_sample.download(o.data(), o.size(), st);
+      TM_CUDA_CHECK(cudaStreamSynchronize(st));
+      const std::vector<double>& wv = li == 0 ? dieW : subW;
+      for (int q = 0; q < cnt; q++) {
+        s[3 * li] += wv[q] * o[2 * q]; s[3 * li + 1] += wv[q] * o[2 * q + 1]; s[3 * li + 2] += wv[q];
+      }
+    }
+    L[0] = s[2] != 0 ? s[0] / s[2] : NAN; L[1] = s[2] != 0 ? s[1] / s[2] : NAN;
+    L[2] = s[5] != 0 ? s[3] / s[5] : NAN; L[3] = s[5] != 0 ? s[4] / s[5] : NAN;
+  }
+
+  // run (13-fatigue.js:1004-1104)
+  void run(int nsteps, const double* ht, const double* hT, const int* hcycle, int cycles, double cphi, double sphi, double* out,
+           double* perCycle, double* loop) {
+    if (!nsolderE || elasticSolder) fail(TM_BAD_INPUT, "submodel run needs Anand solder points");
+    std::vector<double> Wdie(cycles + 1, 0.0), Wsub(cycles + 1, 0.0), Edie(cycles + 1, 0.0), Esub(cycles + 1, 0.0);
+    long long totalNewton = 0;
+    int cutbacks = 0, steps = 0, nsubNext = 1, sample = 0;
+    sample_loop(25, cphi, sphi, loop + 4 * (size_t)sample++);
+    double avg[4];
+    for (int k = 1; k < nsteps; k++) {
+      const double T0 = hT[k - 1], T1 = hT[k], t0s = ht[k - 1], t1s = ht[k];
+      int nsub = nsubNext;
+      bool done = false;
+      double dLast = 0;
+      for (int attempt = 0; attempt < 8 && !done; attempt++) {
+        const double snapTn = Tn;
+        snapshot();
+        bool ok = true;
+        for (int s = 1; s <= nsub; s++) {
+          const double T = T0 + (T1 - T0) * s / nsub, dt = (t1s - t0s) / nsub;
+          int newton;
+          double dMax;
+          const bool conv = step_to(T, dt, &newton, &dMax);
+          totalNewton += newton;
+          steps++;
+          dLast = dMax;
+          if (!conv || dMax > INELASTIC_STEP_MAX) { ok = false; break; }
+        }
+        if (ok) done = true;
+        else { restore(snapTn); nsub *= 2; cutbacks++; }
+      }
+      nsubNext = dLast > 0.5 * INELASTIC_STEP_MAX ? std::min(nsub * 2, 64) : (dLast < 0.2 * INELASTIC_STEP_MAX ? std::max(1, nsub >> 1) : nsub);
+      if (!done) fail(TM_NOT_CONVERGED, "submodel step failed to converge after cutbacks");
+      sample_loop(T1, cphi, sphi, loop + 4 * (size_t)sample++);
+      note_launch();
+      k_sub_layer_avg<<<1, 1, 0, st>>>((int)dieGp.size(), d_dieGp.p, d_dieW.p, (int)subGp.size(), d_subGp.p, d_subW.p, d_pts.p, d_eAn.p,
+                                      d_avg.p);
+      TM_CUDA_CHECK(cudaGetLastError());
+      d_avg.download(avg, 4, st);
+      TM_CUDA_CHECK(cudaStreamSynchronize(st));
+      const int c = hcycle[k];
+      Wdie[c] = avg[0]; Edie[c] = avg[1]; Wsub[c] = avg[2]; Esub[c] = avg[3];
+    }
+    const int nc = cycles;
+    const double dWdie = Wdie[nc] - Wdie[nc - 1], dWsub = Wsub[nc] - Wsub[nc - 1];
+    const double dEdie = Edie[nc] - Edie[nc - 1], dEsub = Esub[nc] - Esub[nc - 1];
+    const double dW = std::max(dWdie, dWsub), dE = dWdie >= dWsub ? dEdie : dEsub;
+    const double prev = nc >= 2 ? std::max(Wdie[nc - 1] - Wdie[nc - 2], Wsub[nc - 1] - Wsub[nc - 2]) : NAN;
+    const double stab = std::isfinite(prev) && prev > 0 ? std::fabs(dW - prev) / prev : NAN;
+    const double o[10] = {dW, dWdie, dWsub, dE, dEdie, dEsub, stab, (double)steps, (double)cutbacks, (double)totalNewton / std::max(steps, 1)};
+    std::copy(o, o + 10, out);
+    for (int c = 1; c <= nc; c++) { perCycle[2 * (c - 1)] = Wdie[c] - Wdie[c - 1]; perCycle[2 * (c - 1) + 1] = Wsub[c] - Wsub[c - 1]; }
+  }
+};
+
+SubModel* submodel_create(const tm_submodel_spec& sp) {
+  if (sp.nx < 2 || sp.ny < 2 || sp.nz < 2 || !sp.xs || !sp.ys || !sp.zs || !sp.cellMat || sp.nt < 2 || !sp.ts || !sp.fields ||
+      !sp.u25 || !sp.bGlob || !sp.bW || !sp.solder.Etab || !sp.solder.Ftab || !sp.ufE || !sp.ufF || !sp.siD || !sp.siF || !sp.subD ||
+      !sp.subF || sp.nglob < 1)
+    fail(TM_BAD_INPUT, "submodel: missing input");
+  std::unique_ptr<SubModel> S(new SubModel());
+  SubModel& m = *S;
+  TM_CUDA_CHECK(cudaStreamCreateWithFlags(&m.st, cudaStreamNonBlocking));
+  m.nx = sp.nx; m.ny = sp.ny; m.nz = sp.nz;
+  m.xs.assign(sp.xs, sp.xs + sp.nx); m.ys.assign(sp.ys, sp.ys + sp.ny); m.zs.assign(sp.zs, sp.zs + sp.nz);
+  m.ts.assign(sp.ts, sp.ts + sp.nt);
+  m.solderE.assign(sp.solder.Etab, sp.solder.Etab + TGRID_N); m.solderF.assign(sp.solder.Ftab, sp.solder.Ftab + TGRID_N);
+  m.ufE.assign(sp.ufE, sp.ufE + TGRID_N); m.ufF.assign(sp.ufF, sp.ufF + TGRID_N);
+  m.siD.assign(sp.siD, sp.siD + 36); m.siF.assign(sp.siF, sp.siF + TGRID_N);
+  m.subD.assign(sp.subD, sp.subD + 36 * TGRID_N); m.subF.assign(sp.subF, sp.subF + 3 * TGRID_N);
+  m.ufNu = sp.ufNu; m.nuMax = sp.nuMax; m.zt = sp.zt; m.zaf = sp.zaf;
+  m.P = AnandConst{sp.solder.A, sp.solder.QR, sp.solder.xi, sp.solder.m, sp.solder.shat, sp.solder.n, sp.solder.h0, sp.solder.a,
+                   sp.solder.s0, sp.solder.nu};
+  m.elasticSolder = sp.elasticSolder;
+  m.nglob = sp.nglob;
+  const int nx = m.nx, ny = m.ny, nz = m.nz, ncy = ny - 1, ncz = nz - 1;
+  // every cell holds one element: nodes (i ny + j) nz + k, elements in cell order (06-mesher.js:14-72)
+  m.nn = nx * ny * nz;
+  m.ne = (nx - 1) * ncy * ncz;
+  m.ndof = 3 * m.nn;
+  const int LOC[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+  m.conn.resize(8 * (size_t)m.ne); m.eIJK.resize(3 * (size_t)m.ne); m.eMat.resize(m.ne); m.eAn.assign(m.ne, -1);
+  for (int i = 0, e = 0; i < nx - 1; i++)
+    for (int j = 0; j < ncy; j++)
+      for (int k = 0; k < ncz; k++, e++) {
+        const int mat = sp.cellMat[e];
+        if (mat < 0 || mat > 3) fail(TM_BAD_INPUT, "submodel: cell material out of range");
+        m.eMat[e] = mat;
+        m.eIJK[3 * e] = i; m.eIJK[3 * e + 1] = j; m.eIJK[3 * e + 2] = k;
+        for (int a = 0; a < 8; a++) m.conn[8 * (size_t)e + a] = ((i + LOC[a][0]) * ny + j + LOC[a][1]) * nz + k + LOC[a][2];
+        if (mat == M_SOLDER && !m.elasticSolder) m.eAn[e] = m.nsolderE++;
+      }
+  // full block pattern (nodes sharing an element: the 27-point neighbourhood), sorted
+  m.rowPtr.assign(m.nn + 1, 0);
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++) {
+        const int n = (i * ny + j) * nz + k;
+        for (int di = -1; di <= 1; di++)
+          for (int dj = -1; dj <= 1; dj++)
+            for (int dk = -1; dk <= 1; dk++) {
+              const int a = i + di, b = j + dj, c = k + dk;
+              if (a < 0 || b < 0 || c < 0 || a >= nx || b >= ny || c >= nz) continue;
+              m.col.push_back((a * ny + b) * nz + c);
+              m.blkRow.push_back(n);
+            }
+        m.rowPtr[n + 1] = (int)m.col.size();
+      }
+  m.nbk = (int)m.col.size();
+  m.diag.assign(m.nn, 0);
+  for (int n = 0; n < m.nn; n++)
+    for (int k = m.rowPtr[n]; k < m.rowPtr[n + 1]; k++) if (m.col[k] == n) { m.diag[n] = k; break; }
+  // gather lists: per block the (e, a, b) contributions and per node the (e, a), in element order
+  std::vector<int> bcnt(m.nbk + 1, 0), ncnt(m.nn + 1, 0), bmap(64 * (size_t)m.ne);
+  for (int e = 0; e < m.ne; e++)
+    for (int a = 0; a < 8; a++) {
+      const int na = m.conn[8 * (size_t)e + a];
+      ncnt[na + 1]++;
+      for (int b = 0; b < 8; b++) {
+        const int nb = m.conn[8 * (size_t)e + b];
+        const int k = (int)(std::lower_bound(m.col.begin() + m.rowPtr[na], m.col.begin() + m.rowPtr[na + 1], nb) - m.col.begin());
+        bmap[64 * (size_t)e + 8 * a + b] = k;
+        bcnt[k + 1]++;
+      }
+    }
+  for (int k = 0; k < m.nbk; k++) bcnt[k + 1] += bcnt[k];
+  for (int n = 0; n < m.nn; n++) ncnt[n + 1] += ncnt[n];
+  std::vector<int> blist(bcnt[m.nbk]), nlist(ncnt[m.nn]);
+  {
+    std::vector<int> bf(bcnt.begin(), bcnt.end() - 1), nf(ncnt.begin(), ncnt.end() - 1);
+    for (int e = 0; e < m.ne; e++)
+      for (int a = 0; a < 8; a++) {
+        nlist[nf[m.conn[8 * (size_t)e + a]]++] = 8 * e + a;
+        for (int b = 0; b < 8; b++) { const int k = bmap[64 * (size_t)e + 8 * a + b]; blist[bf[k]++] = 64 * e + 8 * a + b; }
+      }
+  }
+  if ((long long)m.ne * 64 >= (1LL << 31)) fail(TM_BAD_INPUT, "submodel too large");
+  // boundary: nodes on the six faces, ascending
+  m.isC.assign(m.ndof, 0);
+  std::vector<int> bNodes;
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++)
+        if (i == 0 || j == 0 || k == 0 || i == nx - 1 || j == ny - 1 || k == nz - 1) {
+          const int n = (i * ny + j) * nz + k;
+          bNodes.push_back(n);
+          m.isC[3 * n] = m.isC[3 * n + 1] = m.isC[3 * n + 2] = 1;
+        }
+  std::sort(bNodes.begin(), bNodes.end());
+  if ((int)bNodes.size() != sp.nb) fail(TM_BAD_INPUT, "submodel: boundary node count does not match the cell");
+  m.nbnd = sp.nb;
+  for (int q = 0; q < 8 * sp.nb; q++)
+    if (sp.bGlob[q] < 0 || sp.bGlob[q] >= sp.nglob) fail(TM_BAD_INPUT, "submodel: boundary global node out of range");
+  // _bbarCache: the 8 Gauss-point B-bar matrices per distinct element size (12 significant digits)
+  std::map<std::string, int> keys;
+  std::vector<int> eBb(m.ne);
+  std::vector<double> Bm, Bw;
+  const double GP = 1 / std::sqrt(3.0);
+  for (int e = 0; e < m.ne; e++) {
+    const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+    const double hx = m.xs[i + 1] - m.xs[i], hy = m.ys[j + 1] - m.ys[j], hz = m.zs[k + 1] - m.zs[k];
+    char buf[96];
+    snprintf(buf, sizeof buf, "%.11e|%.11e|%.11e", hx, hy, hz);
+    auto it = keys.find(buf);
+    if (it != keys.end()) { eBb[e] = it->second; continue; }
+    const int idx = (int)Bw.size();
+    keys.emplace(buf, idx);
+    Bm.resize(Bm.size() + 8 * 144);
+    for (int g = 0; g < 8; g++) bbar_matrix(hx, hy, hz, HX[g] * GP, HY[g] * GP, HZ[g] * GP, Bm.data() + (size_t)idx * 8 * 144 + 144 * g);
+    Bw.push_back(hx * hy * hz / 8);
+    eBb[e] = idx;
+  }
+  // layer lists of run(): solder Gauss points in the averaging layers, with their own B-bar matrices
+  std::vector<double> dieB, subB;
+  for (int e = 0; e < m.ne; e++) {
+    if (m.eMat[e] != M_SOLDER) continue;
+    const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+    const double zc = 0.5 * (m.zs[k] + m.zs[k + 1]);
+    const double hx = m.xs[i + 1] - m.xs[i], hy = m.ys[j + 1] - m.ys[j], hz = m.zs[k + 1] - m.zs[k];
+    const double w = hx * hy * hz / 8;
+    for (int g = 0; g < 8; g++) {
+      double B[144];
+      bbar_matrix(hx, hy, hz, HX[g] * GP, HY[g] * GP, HZ[g] * GP, B);
+      if (zc > m.zaf - SUB_T_AVG) { m.dieGp.push_back(8 * e + g); m.dieW.push_back(w); dieB.insert(dieB.end(), B, B + 144); }
+      if (zc < m.zt + SUB_T_AVG) { m.subGp.push_back(8 * e + g); m.subW.push_back(w); subB.insert(subB.end(), B, B + 144); }
+    }
+  }
+  // device copies and state
+  cudaStream_t st = m.st;
+  m.d_conn.upload(m.conn, st); m.d_eMat.upload(m.eMat, st); m.d_eBb.upload(eBb, st); m.d_eAn.upload(m.eAn, st);
+  m.d_rowPtr.upload(m.rowPtr, st); m.d_col.upload(m.col, st); m.d_diag.upload(m.diag, st); m.d_blkRow.upload(m.blkRow, st);
+  m.d_blkStart.upload(bcnt, st); m.d_blkList.upload(blist, st); m.d_nodeStart.upload(ncnt, st); m.d_nodeList.upload(nlist, st);
+  m.d_bNodes.upload(bNodes, st); m.d_bGlob.upload(sp.bGlob, 8 * (size_t)sp.nb, st); m.d_bW.upload(sp.bW, 8 * (size_t)sp.nb, st);
+  m.d_isC.upload(m.isC, st);
+  m.d_Bm.upload(Bm, st); m.d_Bw.upload(Bw, st);
+  m.d_fields.upload(sp.fields, (size_t)sp.nt * sp.nglob * 3, st); m.d_u25.upload(sp.u25, 3 * (size_t)sp.nglob, st);
+  m.d_solderE.upload(m.solderE, st);
+  m.d_elas.alloc(4 * 42);
+  const size_t n = m.ndof;
+  for (DBuf<double>* b : {&m.d_u, &m.d_uN, &m.d_rint, &m.d_b, &m.d_r, &m.d_z, &m.d_p, &m.d_q, &m.d_x, &m.d_s, &m.d_snapU}) { b->alloc(n); b->zero(st); }
+  m.d_sigE.alloc(48 * (size_t)m.ne); m.d_sigE.zero(st);
+  m.d_eFn.alloc(24 * (size_t)m.ne); m.d_eFn.zero(st);
+  m.d_snapSig.alloc(48 * (size_t)m.ne); m.d_snapFn.alloc(24 * (size_t)m.ne);
+  m.d_eK.alloc(576 * (size_t)m.ne); m.d_eF.alloc(24 * (size_t)m.ne); m.d_fe.alloc(24 * (size_t)m.ne); m.d_dmax.alloc(m.ne);
+  m.d_val.alloc(9 * (size_t)m.nbk); m.d_vals.alloc(9 * (size_t)m.nbk);
+  m.d_sums.alloc(2); m.d_avg.alloc(4);
+  if (m.nsolderE) {
+    std::vector<Point> pts(8 * (size_t)m.nsolderE);
+    for (Point& p : pts) {
+      for (int c = 0; c < 6; c++) { p.ep[c] = 0; p.tr_ep[c] = 0; }
+      p.s = m.P.s0; p.ebar = 0; p.W = 0; p.sigEq = 0; p.lastD = 0;
+      p.tr_s = 0; p.tr_ebar = 0; p.tr_W = 0; p.tr_sigEq = 0;
+    }
+    m.d_pts.upload(pts, st);
+    m.d_snapPts.alloc(pts.size());
+  }
+  m.d_dieGp.upload(m.dieGp, st); m.d_subGp.upload(m.subGp, st); m.d_dieW.upload(m.dieW, st); m.d_subW.upload(m.subW, st);
+  m.d_dieB.upload(dieB, st); m.d_subB.upload(subB, st);
+  m.d_sample.alloc(2 * std::max(m.dieGp.size(), m.subGp.size()) + 2);
+  // IC(0) structure of the tangent's pattern (values at 9k + 3p + q)
+  std::vector<long long> vbase(m.nbk);
+  for (int k = 0; k < m.nbk; k++) vbase[k] = 9LL * k;
+  ic_build_structure(m.ic, m.nn, m.rowPtr, m.col, vbase, 1, st);
+  TM_CUDA_CHECK(cudaStreamSynchronize(st));
+  return S.release();
+}
+
+void submodel_destroy(SubModel* s) { delete s; }
+
+bool submodel_step(SubModel& s, double T, double dt, int* newton, double* dMax) { return s.step_to(T, dt, newton, dMax); }
+
+void submodel_get(SubModel& s, double* u, double* W, double* ebar) {
+  if (u) { s.d_u.download(u, s.ndof, s.st); }
+  if ((W || ebar) && s.nsolderE) {
+    std::vector<Point> pts(8 * (size_t)s.nsolderE);
+    s.d_pts.download(pts.data(), pts.size(), s.st);
+    TM_CUDA_CHECK(cudaStreamSynchronize(s.st));
+    for (size_t q = 0; q < pts.size(); q++) { if (W) W[q] = pts[q].W; if (ebar) ebar[q] = pts[q].ebar; }
+  }
+  TM_CUDA_CHECK(cudaStreamSynchronize(s.st));
+}
+
+void submodel_sizes(SubModel& s, int64_t* out) {
+  out[0] = s.nn; out[1] = s.ne; out[2] = s.nbnd; out[3] = 8LL * s.nsolderE;
+}
+
+void submodel_run(SubModel& s, int nsteps, const double* t, const double* T, const int* cycle, int cycles, double cphi, double sphi,
+                  double* out, double* perCycle, double* loop) {
+  if (nsteps < 2 || cycles < 1) fail(TM_BAD_INPUT, "submodel run: need >= 2 history points and >= 1 cycle");
+  for (int k = 0; k < nsteps; k++) if (cycle[k] < 0 || cycle[k] > cycles) fail(TM_BAD_INPUT, "submodel run: cycle index out of range");
+  s.run(nsteps, t, T, cycle, cycles, cphi, sphi, out, perCycle, loop);
+}
+
+}  // namespace tmg

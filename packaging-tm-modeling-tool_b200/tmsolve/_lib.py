@@ -21,7 +21,9 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_anand_screen_device", "tm_anand_step", "tm_set_stream", "tm_launch_count", "tm_kernel_timer",
             "tm_kernel_timer_read", "tm_assemble_step_device", "tm_prepare_step", "tm_accumulate_q", "tm_accumulate_q_device",
             "tm_element_strains", "tm_element_strains_device", "tm_sample_plane", "tm_sample_plane_device",
-            "tm_anand_screen_pillar", "tm_anand_screen_pillar_device", "tm_pc_apply", "tm_pc_apply_device"]
+            "tm_anand_screen_pillar", "tm_anand_screen_pillar_device", "tm_pc_apply", "tm_pc_apply_device",
+            "tm_submodel_create", "tm_submodel_destroy", "tm_submodel_sizes", "tm_submodel_step", "tm_submodel_get",
+            "tm_submodel_run"]
 PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
 PRECOND_NAMES = {v: k for k, v in PRECONDS.items()}
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
@@ -70,6 +72,14 @@ class TmPillar(C.Structure):
     _fields_ = [("fs", C.c_double), ("nu", C.c_double), ("Etab", dp), ("Ftab", dp)]
 
 
+class TmSubmodelSpec(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("xs", dp), ("ys", dp), ("zs", dp), ("cellMat", ip),
+                ("nglob", C.c_int32), ("nt", C.c_int32), ("ts", dp), ("fields", dp), ("u25", dp), ("nb", C.c_int32),
+                ("bGlob", ip), ("bW", dp), ("solder", TmAnandMaterial), ("elasticSolder", C.c_int32), ("ufE", dp), ("ufF", dp),
+                ("ufNu", C.c_double), ("siD", dp), ("siF", dp), ("subD", dp), ("subF", dp), ("nuMax", C.c_double),
+                ("zt", C.c_double), ("zaf", C.c_double)]
+
+
 _lib = None
 
 
@@ -93,6 +103,12 @@ def load():
     L.tm_matvec.argtypes = [vp, vp, vp]
     L.tm_matvec_device.argtypes = [vp, vp, vp]
     L.tm_pc_apply.argtypes = [vp, vp, vp]
+    L.tm_submodel_create.argtypes = [C.POINTER(TmSubmodelSpec), C.POINTER(vp)]
+    L.tm_submodel_destroy.argtypes = [vp]
+    L.tm_submodel_sizes.argtypes = [vp, vp]
+    L.tm_submodel_step.argtypes = [vp, C.c_double, C.c_double, vp, vp, vp]
+    L.tm_submodel_get.argtypes = [vp, vp, vp, vp]
+    L.tm_submodel_run.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_double, C.c_double, vp, vp, vp]
     L.tm_pc_apply_device.argtypes = [vp, vp, vp]
     L.tm_get_bcsr.argtypes = [vp, vp, vp, vp]
     L.tm_sizes.argtypes = [vp, C.POINTER(C.c_int64)]

@@ -238,3 +238,74 @@ def synthetic_spec(nxy: int = 16, nz: int = 14, site=(2.4, 1.2), shear: float = 
                         bGlob=bGlob, bW=bW, anand=anand_params_array(SAC305), solder_E=Et, solder_F=Ft,
                         uf_E=uf_E, uf_F=uf_F, uf_nu=0.35, si_D=iso_d(130000.0, 0.28, NU_MAX_SUBMODEL), si_F=si_F,
                         sub_D=sub_D, sub_F=sub_F, zt=zt, zaf=zaf, elastic_solder=elastic_solder)
+
+
+class DeviceSubmodel:
+    """BumpSubmodel on the GPU (tm_submodel_*): step (stepTo), run, and the state readers."""
+
+    def __init__(self, spec: SubmodelSpec):
+        L = load()
+        f = lambda a: np.ascontiguousarray(a, np.float64)
+        i32 = lambda a: np.ascontiguousarray(a, np.int32)
+        keep = [f(spec.xs), f(spec.ys), f(spec.zs), i32(spec.cell_mat), f(spec.ts), f(spec.fields), f(spec.u25),
+                i32(spec.bGlob).reshape(-1), f(spec.bW).reshape(-1), f(spec.solder_E), f(spec.solder_F), f(spec.uf_E),
+                f(spec.uf_F), f(spec.si_D), f(spec.si_F), f(spec.sub_D), f(spec.sub_F)]
+        P = spec.anand
+        dpp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        mat = _lib.TmAnandMaterial(A=P[0], QR=P[1], xi=P[2], m=P[3], shat=P[4], n=P[5], h0=P[6], a=P[7], s0=P[8], nu=P[9],
+                                   Etab=dpp(keep[9]), Ftab=dpp(keep[10]))
+        ipp = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        sp = _lib.TmSubmodelSpec(nx=len(spec.xs), ny=len(spec.ys), nz=len(spec.zs), xs=dpp(keep[0]), ys=dpp(keep[1]), zs=dpp(keep[2]),
+                                 cellMat=ipp(keep[3]), nglob=spec.nglob, nt=len(spec.ts), ts=dpp(keep[4]), fields=dpp(keep[5]),
+                                 u25=dpp(keep[6]), nb=len(spec.bGlob), bGlob=ipp(keep[7]), bW=dpp(keep[8]), solder=mat,
+                                 elasticSolder=int(spec.elastic_solder), ufE=dpp(keep[11]), ufF=dpp(keep[12]), ufNu=float(spec.uf_nu),
+                                 siD=dpp(keep[13]), siF=dpp(keep[14]), subD=dpp(keep[15]), subF=dpp(keep[16]),
+                                 nuMax=float(spec.nu_max), zt=float(spec.zt), zaf=float(spec.zaf))
+        h = C.c_void_p()
+        check(L.tm_submodel_create(C.byref(sp), C.byref(h)))
+        self.h = h
+        sz = np.zeros(4, np.int64)
+        check(L.tm_submodel_sizes(self.h, sz.ctypes.data_as(C.c_void_p)))
+        self.nn, self.ne, self.nb, self.npoints = (int(v) for v in sz)
+        self.ndof = 3 * self.nn
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().tm_submodel_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, T, dt):
+        """stepTo: (converged, newton, dMax)."""
+        cv = C.c_int32(); nw = C.c_int32(); dm = C.c_double()
+        check(load().tm_submodel_step(self.h, float(T), float(dt), C.byref(cv), C.byref(nw), C.byref(dm)))
+        return bool(cv.value), int(nw.value), float(dm.value)
+
+    def u(self):
+        out = np.zeros(self.ndof)
+        check(load().tm_submodel_get(self.h, out.ctypes.data_as(C.c_void_p), None, None))
+        return out
+
+    def points(self):
+        W = np.zeros(self.npoints); E = np.zeros(self.npoints)
+        check(load().tm_submodel_get(self.h, None, W.ctypes.data_as(C.c_void_p), E.ctypes.data_as(C.c_void_p)))
+        return W, E
+
+    def run(self, hist, cphi=1.0, sphi=0.0) -> dict:
+        """run over a cycle history (cycle_history): the reference's result record's numbers."""
+        n, nc = len(hist["t"]), int(hist["cycles"])
+        t = np.ascontiguousarray(hist["t"], np.float64); T = np.ascontiguousarray(hist["T"], np.float64)
+        cyc = np.ascontiguousarray(hist["cycle"], np.int32)
+        out = np.zeros(10); pc = np.zeros(2 * nc); loop = np.zeros(4 * n)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(load().tm_submodel_run(self.h, n, vp(t), vp(T), vp(cyc), nc, float(cphi), float(sphi), vp(out), vp(pc), vp(loop)))
+        keys = ["dW", "dWdie", "dWsub", "dE", "dEdie", "dEsub", "stabChange", "steps", "cutbacks", "newtonPerStep"]
+        rec = {k: float(out[i]) for i, k in enumerate(keys)}
+        rec["perCycle"] = pc.reshape(nc, 2); rec["loop"] = loop.reshape(n, 4)
+        return rec
+

@@ -1,0 +1,60 @@
+"""The bump submodel on the GPU (tm_submodel_*) against the oracle's BumpSubmodel.
+
+Bars: one Newton step's tangent and residual repeat the reference's sums, but the inner
+IC(0)-PCG sums its dots in another order, so the converged states agree to the solver
+tolerances: displacements to 1e-7 and Gauss-point W to 1e-6 relative after single steps; the
+cycle run's dW, dWdie, dWsub and dE to 1e-6 relative (the submodel bar), with the same sub-step
+and cutback decisions.
+"""
+import numpy as np
+import pytest
+
+from tmsolve.anand import cycle_history
+from tmsolve.submodel import DeviceSubmodel, synthetic_spec
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def test_submodel_patch_and_expansion_gpu(oracle_lib):
+    import test_oracle_submodel as T
+    spec = T._uniform_spec(2, lambda t, x: (t - 25.0) / 100.0 * (T.E @ x))
+    dm = DeviceSubmodel(spec)
+    ok, newton, dmax = dm.step(125.0, 60.0)
+    assert ok and dmax == 0
+    want = T._node_coords(spec) @ T.E.T
+    assert np.abs(dm.u().reshape(-1, 3) - want).max() <= 1e-7 * np.abs(want).max()
+    a = 30e-6
+    spec = T._uniform_spec(2, lambda t, x: a * (t - 25.0) * x, uf_cte=a)
+    dm = DeviceSubmodel(spec)
+    ok, _, _ = dm.step(125.0, 60.0)
+    want = a * 100.0 * T._node_coords(spec)
+    assert ok and np.abs(dm.u().reshape(-1, 3) - want).max() <= 1e-7 * np.abs(want).max()
+
+
+def test_submodel_steps_match_oracle(oracle_lib):
+    spec = synthetic_spec(nxy=6, nz=8)
+    dm, om = DeviceSubmodel(spec), oracle_lib.OracleSubmodel(spec)
+    assert (dm.nn, dm.ne, dm.nb, dm.npoints) == (om.nn, om.ne, om.nb, om.nsolder)
+    for T in (30.0, 35.0, 40.0, 30.0):
+        g, o = dm.step(T, 30.0), om.step(T, 30.0)
+        assert g[0] and o[0]
+        assert abs(g[1] - o[1]) <= 1
+        assert abs(g[2] - o[2]) <= 1e-6 * o[2]
+        assert _rel(dm.u(), om.u()) <= 1e-7
+        Wg, Eg = dm.points(); Wo, Eo = om.points()
+        assert _rel(Wg, Wo) <= 1e-6 and _rel(Eg, Eo) <= 1e-6
+
+
+def test_submodel_run_matches_oracle(oracle_lib):
+    spec = synthetic_spec(nxy=4, nz=8)
+    hist = cycle_history(-40.0, 125.0, 33.0, 5.0, 1)
+    rg = DeviceSubmodel(spec).run(hist, 0.8, 0.6)
+    ro = oracle_lib.OracleSubmodel(spec).run(hist, 0.8, 0.6)
+    for k in ("dW", "dWdie", "dWsub", "dE", "dEdie", "dEsub"):
+        assert abs(rg[k] - ro[k]) <= 1e-6 * abs(ro[k]), (k, rg[k], ro[k])
+    assert rg["steps"] == ro["steps"] and rg["cutbacks"] == ro["cutbacks"]
+    assert np.allclose(rg["loop"], ro["loop"], rtol=1e-5, atol=1e-9)
