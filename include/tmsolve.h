@@ -358,6 +358,14 @@ tm_status tm_submodel_get(tm_sub* sm, double* u, double* W, double* ebar);
 tm_status tm_submodel_run(tm_sub* sm, int32_t nsteps, const double* t, const double* T, const int32_t* cycle, int32_t cycles,
                           double cphi, double sphi, double* out10, double* perCycle, double* loop);
 
+/* n submodels over the same history at once (the screened sites of a die): out10, perCycle
+ * and loop hold n consecutive records; status[i] is each run's status (TM_OK or the failure),
+ * and the call returns the first failure. Runs the submodels concurrently from host threads,
+ * each on its own stream. */
+tm_status tm_submodel_run_batch(int32_t n, tm_sub* const* subs, int32_t nsteps, const double* t, const double* T,
+                                const int32_t* cycle, int32_t cycles, const double* cphi, const double* sphi, double* out10,
+                                double* perCycle, double* loop, int32_t* status);
+
 /* Batched material-point steps: npts independent points, each with a 12-double state
  * (ep[6], s, ebar, W, sigEq, lastD, spare) updated in place when commit != 0;
  * eps (6 per point) engineering mechanical strain; sig (6 per point) and, when

@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -1010,6 +1012,38 @@ tm_status tm_submodel_get(tm_sub* sm, double* u, double* W, double* ebar) {
   return guarded([&] {
     if (!sm) fail(TM_BAD_INPUT, "null argument");
     submodel_get(*reinterpret_cast<SubModel*>(sm), u, W, ebar);
+  });
+}
+
+// independent submodels (the sites of one die) run concurrently: one host thread per submodel
+// (up to the hardware threads), each on its submodel's own stream, so the GPU overlaps their
+// latency-bound Newton and PCG chains
+tm_status tm_submodel_run_batch(int32_t n, tm_sub* const* subs, int32_t nsteps, const double* t, const double* T, const int32_t* cycle,
+                                int32_t cycles, const double* cphi, const double* sphi, double* out10, double* perCycle, double* loop,
+                                int32_t* status) {
+  return guarded([&] {
+    if (n < 0 || (n > 0 && (!subs || !t || !T || !cycle || !cphi || !sphi || !out10 || !perCycle || !loop || !status)))
+      fail(TM_BAD_INPUT, "null argument");
+    int dev = 0;
+    TM_CUDA_CHECK(cudaGetDevice(&dev));
+    std::atomic<int> next(0);
+    auto worker = [&] {
+      cudaSetDevice(dev);
+      for (int i = next++; i < n; i = next++) {
+        const tm_status st = guarded([&] {
+          if (!subs[i]) fail(TM_BAD_INPUT, "null submodel");
+          submodel_run(*reinterpret_cast<SubModel*>(subs[i]), nsteps, t, T, cycle, cycles, cphi[i], sphi[i], out10 + 10 * (size_t)i,
+                       perCycle + 2 * (size_t)cycles * i, loop + 4 * (size_t)nsteps * i);
+        });
+        status[i] = st;
+      }
+    };
+    const int nth = std::max(1, std::min<int>(n, (int)std::max(1u, std::thread::hardware_concurrency())));
+    std::vector<std::thread> pool;
+    for (int q = 0; q < nth; q++) pool.emplace_back(worker);
+    for (auto& th : pool) th.join();
+    for (int i = 0; i < n; i++)
+      if (status[i] != TM_OK) fail((tm_status)status[i], "submodel " + std::to_string(i) + " of the batch failed");
   });
 }
 

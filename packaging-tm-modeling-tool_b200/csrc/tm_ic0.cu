@@ -230,6 +230,7 @@ void ic_build_structure(IcFactor& F, int nn, const std::vector<int>& nrp, const 
   F.d_tStart.upload(tCount, st); F.d_tRow.upload(tRow, st); F.d_tPos.upload(tPos, st);
   F.d_fwdNodes.upload(fwd, st); F.d_bwdNodes.upload(bwd, st);
   F.fwdStart = fwdStart; F.bwdStart = bwdStart;
+  F.drop_graph();
   F.d_U.alloc(nnz);
   F.d_fail.alloc(1);
   F.n = n; F.nnz = nnz;
@@ -266,9 +267,8 @@ void ic_factor(IcFactor& F, const double* val, cudaStream_t st) {
   fail(TM_BAD_INPUT, "IC(0) failed even with the maximum diagonal shift");
 }
 
-// ICPC.apply (10-solver.js:784-798)
-void ic_apply(IcFactor& F, const double* r, double* z, cudaStream_t st) {
-  if (!F.ready) fail(TM_BAD_INPUT, "IC(0) preconditioner not built");
+namespace {
+void ic_apply_launches(IcFactor& F, const double* r, double* z, cudaStream_t st) {
   const int nl = (int)F.fwdStart.size() - 1, nb = (int)F.bwdStart.size() - 1;
   for (int l = 0; l < nl; l++) {
     const int cnt = F.fwdStart[l + 1] - F.fwdStart[l];
@@ -282,8 +282,36 @@ void ic_apply(IcFactor& F, const double* r, double* z, cudaStream_t st) {
     k_ic_backward<<<grid_for(cnt, IC_WARPS), 32 * IC_WARPS, 0, st>>>(cnt, F.d_bwdNodes.p + F.bwdStart[l], F.d_rowPtr.p, F.d_col.p,
                                                                     F.d_U.p, z);
   }
+}
+}  // namespace
+
+// ICPC.apply (10-solver.js:784-798): the level launches, replayed from a CUDA graph captured on
+// the first apply with these vectors on this stream (a created stream; the legacy default stream
+// launches directly). The factor is updated in place, so the graph stays valid until the
+// structure changes.
+void ic_apply(IcFactor& F, const double* r, double* z, cudaStream_t st) {
+  if (!F.ready) fail(TM_BAD_INPUT, "IC(0) preconditioner not built");
+  const int nl = (int)F.fwdStart.size() - 1, nb = (int)F.bwdStart.size() - 1;
   note_launch(nl + nb);
-  TM_CUDA_CHECK(cudaGetLastError());
+  if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) {
+    ic_apply_launches(F, r, z, st);
+    TM_CUDA_CHECK(cudaGetLastError());
+    return;
+  }
+  if (!F.exec || F.gr != r || F.gz != z || F.gst != st) {
+    F.drop_graph();
+    cudaGraph_t g = nullptr;
+    TM_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    ic_apply_launches(F, r, z, st);
+    const cudaError_t le = cudaGetLastError();
+    TM_CUDA_CHECK(cudaStreamEndCapture(st, &g));
+    if (le != cudaSuccess) { cudaGraphDestroy(g); TM_CUDA_CHECK(le); }
+    const cudaError_t ie = cudaGraphInstantiate(&F.exec, g, 0);
+    cudaGraphDestroy(g);
+    TM_CUDA_CHECK(ie);
+    F.gr = r; F.gz = z; F.gst = st;
+  }
+  TM_CUDA_CHECK(cudaGraphLaunch(F.exec, st));
 }
 
 // the level-0 operator of a solve context: node pattern from the stencil slots (ascending

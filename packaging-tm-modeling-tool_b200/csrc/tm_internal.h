@@ -109,6 +109,16 @@ struct IcFactor {
   DBuf<int> d_fail;
   double shift = 0;
   bool ready = false;
+  // the level launches of one apply as a CUDA graph, for the (r, z, stream) it was captured with
+  cudaGraphExec_t exec = nullptr;
+  const double* gr = nullptr;
+  double* gz = nullptr;
+  cudaStream_t gst = nullptr;
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr; gr = nullptr; gz = nullptr; gst = nullptr;
+  }
+  ~IcFactor() { drop_graph(); }
 };
 
 struct ShellLevel {

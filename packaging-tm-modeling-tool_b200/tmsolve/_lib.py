@@ -23,7 +23,7 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_element_strains", "tm_element_strains_device", "tm_sample_plane", "tm_sample_plane_device",
             "tm_anand_screen_pillar", "tm_anand_screen_pillar_device", "tm_pc_apply", "tm_pc_apply_device",
             "tm_submodel_create", "tm_submodel_destroy", "tm_submodel_sizes", "tm_submodel_step", "tm_submodel_get",
-            "tm_submodel_run"]
+            "tm_submodel_run", "tm_submodel_run_batch"]
 PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
 PRECOND_NAMES = {v: k for k, v in PRECONDS.items()}
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
@@ -109,6 +109,7 @@ def load():
     L.tm_submodel_step.argtypes = [vp, C.c_double, C.c_double, vp, vp, vp]
     L.tm_submodel_get.argtypes = [vp, vp, vp, vp]
     L.tm_submodel_run.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_double, C.c_double, vp, vp, vp]
+    L.tm_submodel_run_batch.argtypes = [C.c_int32, vp, C.c_int32, vp, vp, vp, C.c_int32, vp, vp, vp, vp, vp, vp]
     L.tm_pc_apply_device.argtypes = [vp, vp, vp]
     L.tm_get_bcsr.argtypes = [vp, vp, vp, vp]
     L.tm_sizes.argtypes = [vp, C.POINTER(C.c_int64)]

@@ -309,3 +309,23 @@ class DeviceSubmodel:
         rec["perCycle"] = pc.reshape(nc, 2); rec["loop"] = loop.reshape(n, 4)
         return rec
 
+
+def run_batch(models, hist, cphi, sphi) -> list:
+    """run of several DeviceSubmodels over one history at once (tm_submodel_run_batch): a record per model."""
+    n, m, nc = len(models), len(hist["t"]), int(hist["cycles"])
+    t = np.ascontiguousarray(hist["t"], np.float64); T = np.ascontiguousarray(hist["T"], np.float64)
+    cyc = np.ascontiguousarray(hist["cycle"], np.int32)
+    cp = np.ascontiguousarray(cphi, np.float64); sp = np.ascontiguousarray(sphi, np.float64)
+    handles = (C.c_void_p * n)(*[md.h.value for md in models])
+    out = np.zeros((n, 10)); pc = np.zeros((n, nc, 2)); loop = np.zeros((n, m, 4)); status = np.zeros(n, np.int32)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    check(load().tm_submodel_run_batch(n, C.cast(handles, C.c_void_p), m, vp(t), vp(T), vp(cyc), nc, vp(cp), vp(sp), vp(out), vp(pc),
+                                       vp(loop), vp(status)))
+    keys = ["dW", "dWdie", "dWsub", "dE", "dEdie", "dEsub", "stabChange", "steps", "cutbacks", "newtonPerStep"]
+    recs = []
+    for i in range(n):
+        r = {k: float(out[i, j]) for j, k in enumerate(keys)}
+        r["perCycle"] = pc[i]; r["loop"] = loop[i]
+        recs.append(r)
+    return recs
+

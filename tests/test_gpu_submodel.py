@@ -58,3 +58,18 @@ def test_submodel_run_matches_oracle(oracle_lib):
         assert abs(rg[k] - ro[k]) <= 1e-6 * abs(ro[k]), (k, rg[k], ro[k])
     assert rg["steps"] == ro["steps"] and rg["cutbacks"] == ro["cutbacks"]
     assert np.allclose(rg["loop"], ro["loop"], rtol=1e-5, atol=1e-9)
+
+
+def test_submodel_batch_equals_single_runs(oracle_lib):
+    """Three sites at once (concurrent streams) give each site's single-run record."""
+    from tmsolve.submodel import run_batch
+    hist = cycle_history(-40.0, 125.0, 66.0, 2.0, 1)
+    specs = [synthetic_spec(nxy=4, nz=6, site=(0.3 * q, -0.2 * q), shear=1e-5 * (q + 1), seed=q) for q in range(3)]
+    cph, sph = [1.0, 0.6, 0.0], [0.0, 0.8, 1.0]
+    recs = run_batch([DeviceSubmodel(s) for s in specs], hist, cph, sph)
+    for q in range(3):
+        one = DeviceSubmodel(specs[q]).run(hist, cph[q], sph[q])
+        for k in ("dW", "dWdie", "dWsub", "dE", "steps", "cutbacks"):
+            assert recs[q][k] == one[k], (q, k)
+        assert np.array_equal(recs[q]["loop"], one["loop"])
+
