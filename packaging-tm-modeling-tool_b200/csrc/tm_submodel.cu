@@ -413,16 +413,21 @@ __global__ void k_sub_spmv(int nn, const int* __restrict__ rowPtr, const int* __
   }
   y[3 * i] = y0; y[3 * i + 1] = y1; y[3 * i + 2] = y2;
 }
-__global__ void k_sub_axpy2(int n, double alpha, const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ x,
-                            double* __restrict__ r) {
+// the PCG updates with their scalars read on the device: alpha = rz / (p.q), beta = rz2 / rz
+__global__ void k_sub_axpy2(int n, const double* __restrict__ rz, const double* __restrict__ pq, const double* __restrict__ p,
+                            const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const double alpha = *rz / *pq;
   x[i] += alpha * p[i];
   r[i] += -alpha * q[i];
 }
-__global__ void k_sub_xpby(int n, const double* __restrict__ z, double beta, double* __restrict__ p) {
+__global__ void k_sub_xpby(int n, const double* __restrict__ z, const double* __restrict__ rz2, const double* __restrict__ rz,
+                           double* __restrict__ p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = z[i] + beta * p[i];
+  if (i >= n) return;
+  const double beta = *rz2 / *rz;
+  p[i] = z[i] + beta * p[i];
 }
 __global__ void k_sub_mul(int n, const double* __restrict__ s, double* __restrict__ x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -558,7 +563,7 @@ struct SubModel {
   DBuf<int> d_bNodes, d_bGlob;
   DBuf<uint8_t> d_isC;
   DBuf<double> d_Bm, d_Bw, d_bW, d_fields, d_u25, d_solderE, d_elas;
-  DBuf<double> d_u, d_uN, d_sigE, d_eFn, d_eK, d_eF, d_fe, d_dmax, d_val, d_vals, d_s, d_rint, d_b, d_r, d_z, d_p, d_q, d_x, d_sums;
+  DBuf<double> d_u, d_uN, d_sigE, d_eFn, d_eK, d_eF, d_fe, d_dmax, d_val, d_vals, d_s, d_rint, d_b, d_r, d_z, d_p, d_q, d_x, d_sums, d_pcg;
   DBuf<Point> d_pts, d_snapPts;
   DBuf<double> d_snapU, d_snapSig, d_snapFn;
   IcFactor ic;
@@ -671,26 +676,31 @@ struct SubModel {
     if (bn == 0) return 0;
     ic_apply(ic, d_r.p, d_z.p, st);
     TM_CUDA_CHECK(cudaMemcpyAsync(d_p.p, d_z.p, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    sums(ndof, 1, d_r.p, d_z.p, h);
-    double rz = h[0];
+    // device scalars (k_sub_sums writes two values per result): rz at a, the next rz at 2 - a,
+    // p.q at 4, r.r at 6; one host synchronization per iteration, for the convergence test
+    double* S = d_pcg.p;
+    int a = 0;
+    note_launch();
+    k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_r.p, d_z.p, d_isC.p, S + a);
     int it;
     const int nb = blocks_for(ndof, 256);
+    double rr = 0;
     for (it = 1; it <= 2000; it++) {
-      note_launch();
+      note_launch(4);
       k_sub_spmv<<<blocks_for(nn, 128), 128, 0, st>>>(nn, d_rowPtr.p, d_col.p, d_vals.p, d_p.p, d_q.p);
-      sums(ndof, 1, d_p.p, d_q.p, h);
-      const double alpha = rz / h[0];
-      note_launch();
-      k_sub_axpy2<<<nb, 256, 0, st>>>(ndof, alpha, d_p.p, d_q.p, d_x.p, d_r.p);
-      sums(ndof, 1, d_r.p, d_r.p, h);
-      if (std::sqrt(h[0]) / bn < tol) break;
+      k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_p.p, d_q.p, d_isC.p, S + 4);
+      k_sub_axpy2<<<nb, 256, 0, st>>>(ndof, S + a, S + 4, d_p.p, d_q.p, d_x.p, d_r.p);
+      k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_r.p, d_r.p, d_isC.p, S + 6);
+      TM_CUDA_CHECK(cudaMemcpyAsync(&rr, S + 6, sizeof(double), cudaMemcpyDeviceToHost, st));
+      TM_CUDA_CHECK(cudaStreamSynchronize(st));
+      if (std::sqrt(rr) / bn < tol) break;
       ic_apply(ic, d_r.p, d_z.p, st);
-      sums(ndof, 1, d_r.p, d_z.p, h);
-      const double rz2 = h[0], beta = rz2 / rz;
-      rz = rz2;
-      note_launch();
-      k_sub_xpby<<<nb, 256, 0, st>>>(ndof, d_z.p, beta, d_p.p);
+      note_launch(2);
+      k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_r.p, d_z.p, d_isC.p, S + (2 - a));
+      k_sub_xpby<<<nb, 256, 0, st>>>(ndof, d_z.p, S + (2 - a), S + a, d_p.p);
+      a = 2 - a;
     }
+    TM_CUDA_CHECK(cudaGetLastError());
     note_launch();
     k_sub_mul<<<nb, 256, 0, st>>>(ndof, d_s.p, d_x.p);
     TM_CUDA_CHECK(cudaGetLastError());
@@ -998,7 +1008,7 @@ SubModel* submodel_create(const tm_submodel_spec& sp) {
   m.d_snapSig.alloc(48 * (size_t)m.ne); m.d_snapFn.alloc(24 * (size_t)m.ne);
   m.d_eK.alloc(576 * (size_t)m.ne); m.d_eF.alloc(24 * (size_t)m.ne); m.d_fe.alloc(24 * (size_t)m.ne); m.d_dmax.alloc(m.ne);
   m.d_val.alloc(9 * (size_t)m.nbk); m.d_vals.alloc(9 * (size_t)m.nbk);
-  m.d_sums.alloc(2); m.d_avg.alloc(4);
+  m.d_sums.alloc(2); m.d_avg.alloc(4); m.d_pcg.alloc(8);
   if (m.nsolderE) {
     std::vector<Point> pts(8 * (size_t)m.nsolderE);
     for (Point& p : pts) {
