@@ -27,6 +27,9 @@
  *                      the march of Analysis.qAlong (src/core/11-analysis.js:298-316)
  *   tm_element_strains boxStrainAt at natural points (src/core/07-element.js:127-142), the
  *                      inner loop of siteStrainTable (src/core/13-fatigue.js:318-346)
+ *   tm_accumulate_state / tm_state_stress  Model.accumulateStep and stateStress
+ *                      (src/core/09-assembly.js:508-571), the element histories of StateView.point
+ *                      (src/core/11-analysis.js:343-379) behind dieSurfaceStress and jointLoads
  *   tm_submodel_*      BumpSubmodel (src/core/13-fatigue.js:470-1104): create, stepTo, run
  *   tm_sample_plane    samplePlane(mesh, u, k, comp, x, y) at many points
  *                      (src/core/12-post.js:30-38), the sampler of warpageJEITA (:60-109)
@@ -209,6 +212,31 @@ tm_status tm_element_strains(tm_ctx* ctx, int32_t npts, const int32_t* elem, con
 tm_status tm_accumulate_q_device(tm_ctx* ctx, const double* du_dev, int32_t nel, const int32_t* elems_dev, double* q_dev);
 tm_status tm_element_strains_device(tm_ctx* ctx, int32_t npts, const int32_t* elem_dev, const double* q_dev,
                                     const double* nat_dev, double* eps_dev);
+
+/* ---- element stress histories ---- */
+/* The sub-layers of the layered property sets for the step loaded last, which the stress
+ * histories read (per sub-layer s of a section: sectionSubMeanD and sectionSubStress,
+ * src/core/04-homogenize.js:196-204, and its z range, subLayerAt, src/core/09-assembly.js:547-552):
+ * nsub per property set (0 for homogeneous sets, which use D and s0 of tm_step), then per
+ * sub-layer in set order subZ (z0, z1), subD (36), subS0 (6). Call after tm_prepare_step or
+ * tm_assemble_step for the same step. */
+tm_status tm_set_sublayers(tm_ctx* ctx, const int32_t* nsub, const double* subZ, const double* subD, const double* subS0);
+/* Model.accumulateStep without qOnly (src/core/09-assembly.js:508-544) over a list of
+ * elements: state (stride doubles per element, stride >= 33 + 48 x the largest sub-layer count)
+ * holds q (33), then per sub-layer the 7 strain-monomial stresses S_m (6 each) and the thermal
+ * stress S_th (6); the step adds dq and, for born materials, D_m E_m(dq) and the step's thermal
+ * stress increment. An element index < 0 writes NaN into its row. Host pointers. */
+tm_status tm_accumulate_state(tm_ctx* ctx, const double* du, int32_t nel, const int32_t* elems, int32_t stride, double* state);
+/* stateStress (src/core/09-assembly.js:555-571): engineering strain and stress (6 each) of
+ * element elem[p] from its state (stride doubles per point) at the natural point nat[3 p ..];
+ * NaN for an element index < 0. Host pointers. */
+tm_status tm_state_stress(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* state, int32_t stride, const double* nat,
+                          double* eps, double* sig);
+/* The same with every array in device memory (element indices >= ne also give NaN rows). */
+tm_status tm_accumulate_state_device(tm_ctx* ctx, const double* du_dev, int32_t nel, const int32_t* elems_dev, int32_t stride,
+                                     double* state_dev);
+tm_status tm_state_stress_device(tm_ctx* ctx, int32_t npts, const int32_t* elem_dev, const double* state_dev, int32_t stride,
+                                 const double* nat_dev, double* eps_dev, double* sig_dev);
 
 /* ---- field sampling ---- */
 /* samplePlane: bilinear interpolation of component comp (0..2) of the nodal field u (3*nn

@@ -64,6 +64,9 @@ def lib():
     L.orc_anand_screen_pillar.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _ip, _ip, C.c_int,
                                           C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]
     L.orc_accumulate_q.argtypes = [vp, _dp, C.c_int, _ip, _dp]
+    L.orc_set_sublayers.argtypes = [vp, _ip, _dp, _dp, _dp]
+    L.orc_accumulate_state.argtypes = [vp, _dp, C.c_int, _ip, C.c_int, _dp]
+    L.orc_state_stress.argtypes = [vp, C.c_int, _ip, _dp, C.c_int, _dp, _dp, _dp]
     L.orc_element_strains.argtypes = [vp, C.c_int, _ip, _dp, _dp, _dp]
     L.orc_fit_plane.argtypes = [C.c_int, _dp, _dp, _dp, _dp]
     L.orc_sample_plane.restype = C.c_double
@@ -190,6 +193,27 @@ class OracleModel:
         assert q.dtype == np.float64 and q.flags.c_contiguous and q.size == 33 * len(elems)
         lib().orc_accumulate_q(self.h, np.ascontiguousarray(du, np.float64), len(elems), elems, q)
         return q
+
+    def set_sublayers(self, step):
+        """The step's sub-layers of the layered property sets (for the stress histories)."""
+        f = lambda a: np.ascontiguousarray(a if a is not None and len(a) else np.zeros(1), np.float64)
+        lib().orc_set_sublayers(self.h, np.ascontiguousarray(step.sub_n, np.int32), f(step.sub_z), f(step.sub_D), f(step.sub_s0))
+
+    def accumulate_state(self, du, elems, stride, state):
+        """Model.accumulateStep (09-assembly.js:508-544) of the last assembled step: state (nel x
+        stride) += the DOF increment and the sub-layer stress monomials."""
+        elems = np.ascontiguousarray(elems, np.int32)
+        assert state.dtype == np.float64 and state.flags.c_contiguous and state.size == stride * len(elems)
+        lib().orc_accumulate_state(self.h, np.ascontiguousarray(du, np.float64), len(elems), elems, int(stride), state)
+        return state
+
+    def state_stress(self, elem, state, stride, nat):
+        """stateStress (09-assembly.js:555-571): (eps, sig), each (npts, 6)."""
+        elem = np.ascontiguousarray(elem, np.int32)
+        eps = np.zeros(6 * len(elem)); sig = np.zeros(6 * len(elem))
+        lib().orc_state_stress(self.h, len(elem), elem, np.ascontiguousarray(state, np.float64).reshape(-1), int(stride),
+                               np.ascontiguousarray(nat, np.float64).reshape(-1), eps, sig)
+        return eps.reshape(-1, 6), sig.reshape(-1, 6)
 
     def element_strains(self, elem, q, nat):
         """boxStrainAt (07-element.js:127-142) of element elem[t] with DOFs q[t] at nat[t]."""

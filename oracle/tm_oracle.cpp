@@ -575,7 +575,12 @@ int findBlock(const Pattern& P, int row, int colj) {
 
 // ---- FE model: assembly with element birth and constraints (09-assembly.js:208-464) -----
 // A property set is a homogeneous group (D 36, s0 6) or a layered section (W 108, V 18).
-struct PropSet { bool layered = false; double D[36]; double s0[6]; double W[108]; double V[18]; bool born = true; double M[6 * 1089]; };
+struct PropSet {
+  bool layered = false; double D[36]; double s0[6]; double W[108]; double V[18]; bool born = true; double M[6 * 1089];
+  // layered sets: per sub-layer its z range, step-mean stiffness and thermal stress increment
+  // (sectionSubMeanD / sectionSubStress, 04-homogenize.js:196-204), for the stress histories
+  int nsub = 0; dvec subZ, subD, subS0;
+};
 
 struct Model {
   Mesh mesh;
@@ -2300,18 +2305,18 @@ void cholSolveDense(const double* L, int n, double* b) {
   }
 }
 
-// Model.accumulateStep with qOnly (09-assembly.js:508-533): adds to q (33) the DOF increment of
-// element e in the step assembled last: du at its nodes, then the incompatible modes
+// The DOF increment of element e in the step assembled last (Model.accumulateStep,
+// 09-assembly.js:508-528): du at its nodes, then the incompatible modes
 // K_aa^-1 (f_a - K_au du) from the rows 24..32 of the step's shape matrices (stepRecovery
 // :480-491) and, when the material is born, of the element thermal load
-void accumulateQ(const Model& M, const double* du, int e, double* q) {
+void elementIncrement(const Model& M, const double* du, int e, double* dq) {
   const Mesh& m = M.mesh;
   const PropSet& ps = M.psets[M.ePset[e]];
   const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
   const double hx = m.xs[i + 1] - m.xs[i], hy = m.ys[j + 1] - m.ys[j], hz = m.zs[k + 1] - m.zs[k];
   const double V8 = hx * hy * hz / 8;
   const double c[6] = {V8 * 4 / (hx * hx), V8 * 4 / (hy * hy), V8 * 4 / (hz * hz), V8 * 4 / (hx * hy), V8 * 4 / (hy * hz), V8 * 4 / (hz * hx)};
-  double Kr[297], f33[33], dq[33], Kaa[81], col[9];
+  double Kr[297], f33[33], Kaa[81], col[9];
   for (int r = 0; r < 297; r++) {
     const double* Ma = ps.M + 24 * 33 + r;
     Kr[r] = c[0] * Ma[0] + c[1] * Ma[1089] + c[2] * Ma[2178] + c[3] * Ma[3267] + c[4] * Ma[4356] + c[5] * Ma[5445];
@@ -2331,7 +2336,81 @@ void accumulateQ(const Model& M, const double* du, int e, double* q) {
   }
   cholSolveDense(Kaa, 9, col);
   for (int r = 0; r < 9; r++) dq[24 + r] = col[r];
+}
+
+// Model.accumulateStep with qOnly (09-assembly.js:508-533): q (33) += the element's increment
+void accumulateQ(const Model& M, const double* du, int e, double* q) {
+  double dq[33];
+  elementIncrement(M, du, e, dq);
   for (int r = 0; r < 33; r++) q[r] += dq[r];
+}
+
+const int STRAIN_MONO = 7;   // 09-assembly.js:168
+
+// boxStrainPoly (09-assembly.js:176-196): strain of a box element as a polynomial in the natural
+// coordinates, E (42) = six components per monomial 1, xi, eta, zeta, xi eta, eta zeta, xi zeta
+void boxStrainPoly(double hx, double hy, double hz, const double* q, double* E) {
+  for (int t = 0; t < 42; t++) E[t] = 0;
+  const double sx = 2 / hx, sy = 2 / hy, sz = 2 / hz;
+  for (int a = 0; a < 8; a++) {
+    const double xa = HEX_XI[a], ya = HEX_ETA[a], za = HEX_ZETA[a], ux = q[3 * a], uy = q[3 * a + 1], uz = q[3 * a + 2];
+    const double cx = xa * sx / 8, cy = ya * sy / 8, cz = za * sz / 8;
+    const int mx[4] = {0, 2, 3, 5}, my[4] = {0, 1, 3, 6}, mz[4] = {0, 1, 2, 4};
+    const double vx[4] = {cx, cx * ya, cx * za, cx * ya * za}, vy[4] = {cy, cy * xa, cy * za, cy * xa * za},
+                 vz[4] = {cz, cz * xa, cz * ya, cz * xa * ya};
+    for (int t = 0; t < 4; t++) { const int mm = mx[t]; const double cc = vx[t]; E[6 * mm] += cc * ux; E[6 * mm + 3] += cc * uy; E[6 * mm + 5] += cc * uz; }
+    for (int t = 0; t < 4; t++) { const int mm = my[t]; const double cc = vy[t]; E[6 * mm + 1] += cc * uy; E[6 * mm + 3] += cc * ux; E[6 * mm + 4] += cc * uz; }
+    for (int t = 0; t < 4; t++) { const int mm = mz[t]; const double cc = vz[t]; E[6 * mm + 2] += cc * uz; E[6 * mm + 4] += cc * uy; E[6 * mm + 5] += cc * ux; }
+  }
+  const double* a1 = q + 24; const double* a2 = q + 27; const double* a3 = q + 30;
+  E[6 * 1] += -2 * sx * a1[0]; E[6 * 1 + 3] += -2 * sx * a1[1]; E[6 * 1 + 5] += -2 * sx * a1[2];
+  E[6 * 2 + 1] += -2 * sy * a2[1]; E[6 * 2 + 3] += -2 * sy * a2[0]; E[6 * 2 + 4] += -2 * sy * a2[2];
+  E[6 * 3 + 2] += -2 * sz * a3[2]; E[6 * 3 + 4] += -2 * sz * a3[1]; E[6 * 3 + 5] += -2 * sz * a3[0];
+}
+
+// Model.accumulateStep without qOnly (09-assembly.js:508-544): q += dq and, when the material is
+// born, per sub-layer S_m += D_m E_m(dq) (m < 7) and S_th += the step's thermal stress increment
+void accumulateState(const Model& M, const double* du, int e, double* state) {
+  const Mesh& m = M.mesh;
+  const PropSet& ps = M.psets[M.ePset[e]];
+  double dq[33], E[42];
+  elementIncrement(M, du, e, dq);
+  for (int r = 0; r < 33; r++) state[r] += dq[r];
+  if (!ps.born) return;
+  const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+  boxStrainPoly(m.xs[i + 1] - m.xs[i], m.ys[j + 1] - m.ys[j], m.zs[k + 1] - m.zs[k], dq, E);
+  const int ns = ps.layered ? ps.nsub : 1, blk = 6 * (STRAIN_MONO + 1);
+  for (int s = 0; s < ns; s++) {
+    const double* D = ps.layered ? ps.subD.data() + 36 * s : ps.D;
+    const double* s0 = ps.layered ? ps.subS0.data() + 6 * s : ps.s0;
+    const int o = 33 + s * blk;
+    for (int mo = 0; mo < STRAIN_MONO; mo++) {
+      for (int r = 0; r < 6; r++) { double v = 0; for (int t = 0; t < 6; t++) v += D[r * 6 + t] * E[6 * mo + t]; state[o + 6 * mo + r] += v; }
+    }
+    for (int r = 0; r < 6; r++) state[o + 6 * STRAIN_MONO + r] += s0[r];
+  }
+}
+
+// stateStress (09-assembly.js:555-571) with subLayerAt (:547-552): total strain and stress of
+// element e at the natural point nat from its history state
+void stateStress(const Model& M, int e, const double* state, const double* nat, double* eps, double* sig) {
+  const Mesh& m = M.mesh;
+  const PropSet& ps = M.psets[M.ePset[e]];
+  const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
+  boxStrainAt(m.xs[i + 1] - m.xs[i], m.ys[j + 1] - m.ys[j], m.zs[k + 1] - m.zs[k], state, state + 24, nat[0], nat[1], nat[2], eps);
+  int s = 0;
+  if (ps.layered) {
+    const double z = m.zs[k] + 0.5 * (nat[2] + 1) * (m.zs[k + 1] - m.zs[k]);
+    s = ps.nsub - 1;
+    for (int t = 0; t < ps.nsub; t++) if (z <= ps.subZ[2 * t + 1] + 1e-12) { s = t; break; }
+  }
+  const double phi[7] = {1, nat[0], nat[1], nat[2], nat[0] * nat[1], nat[1] * nat[2], nat[0] * nat[2]};
+  const int o = 33 + s * 6 * (STRAIN_MONO + 1);
+  for (int r = 0; r < 6; r++) {
+    double v = -state[o + 6 * STRAIN_MONO + r];
+    for (int mo = 0; mo < STRAIN_MONO; mo++) v += phi[mo] * state[o + 6 * mo + r];
+    sig[r] = v;
+  }
 }
 
 // boxStrainAt of element e (its dims from the mesh lines, Model.elementDims) with the element
@@ -2740,6 +2819,33 @@ void orc_anand_screen_pillar(const double* params, const double* Etab, const dou
 // Model.accumulateStep (qOnly) over nel elements for the last assembled step
 void orc_accumulate_q(orc_model* o, const double* du, int nel, const int* elems, double* q) {
   for (int t = 0; t < nel; t++) accumulateQ(o->M, du, elems[t], q + 33 * (size_t)t);
+}
+
+// sub-layers of the layered property sets for the stress histories: nsub per property set (0 for
+// homogeneous ones), then per sub-layer in set order its z range (2), mean stiffness (36) and
+// thermal stress increment (6) of the step assembled last
+void orc_set_sublayers(orc_model* o, const int* nsub, const double* subZ, const double* subD, const double* subS0) {
+  size_t q = 0;
+  for (auto& ps : o->M.psets) {
+    const int n = nsub[&ps - &o->M.psets[0]];
+    ps.nsub = n;
+    ps.subZ.assign(subZ + 2 * q, subZ + 2 * (q + n));
+    ps.subD.assign(subD + 36 * q, subD + 36 * (q + n));
+    ps.subS0.assign(subS0 + 6 * q, subS0 + 6 * (q + n));
+    q += n;
+  }
+}
+
+// element histories with stresses: state (stride doubles per element) += the step's increment
+void orc_accumulate_state(orc_model* o, const double* du, int nel, const int* elems, int stride, double* state) {
+  for (int t = 0; t < nel; t++) accumulateState(o->M, du, elems[t], state + (size_t)stride * t);
+}
+
+// stress and strain at natural points from the element states (stride doubles per point)
+void orc_state_stress(orc_model* o, int np, const int* elem, const double* state, int stride, const double* nat, double* eps,
+                      double* sig) {
+  for (int t = 0; t < np; t++)
+    stateStress(o->M, elem[t], state + (size_t)stride * t, nat + 3 * (size_t)t, eps + 6 * (size_t)t, sig + 6 * (size_t)t);
 }
 
 void orc_element_strains(orc_model* o, int np, const int* elem, const double* q, const double* nat, double* eps) {

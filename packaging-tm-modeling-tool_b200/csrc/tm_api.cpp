@@ -754,6 +754,107 @@ tm_status tm_accumulate_q(tm_ctx* ctx, const double* du, int32_t nel, const int3
   });
 }
 
+// ---- element stress histories (Model.accumulateStep without qOnly, stateStress) ---------------------
+tm_status tm_set_sublayers(tm_ctx* ctx, const int32_t* nsub, const double* subZ, const double* subD, const double* subS0) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!nsub) fail(TM_BAD_INPUT, "tm_set_sublayers: null argument");
+    if (!c.stepReady) fail(TM_BAD_INPUT, "tm_set_sublayers after tm_prepare_step or tm_assemble_step");
+    std::vector<int> off(c.npset + 1, 0);
+    int mx = 1;
+    for (int p = 0; p < c.npset; p++) {
+      if (nsub[p] < 0) fail(TM_BAD_INPUT, "tm_set_sublayers: negative sub-layer count");
+      off[p + 1] = off[p] + nsub[p];
+      mx = std::max(mx, (int)nsub[p]);
+    }
+    std::vector<int> lay(c.npset);
+    TM_CUDA_CHECK(cudaMemcpyAsync(lay.data(), c.d_psetLayered.p, c.npset * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    for (int p = 0; p < c.npset; p++)
+      if (lay[p] && nsub[p] < 1) fail(TM_BAD_INPUT, "tm_set_sublayers: a layered property set needs its sub-layers");
+    const size_t n = off[c.npset];
+    if (n && (!subZ || !subD || !subS0)) fail(TM_BAD_INPUT, "tm_set_sublayers: null sub-layer data");
+    c.d_subOff.upload(off, c.stream);
+    if (n) {
+      c.d_subZ.upload(subZ, 2 * n, c.stream); c.d_subD.upload(subD, 36 * n, c.stream); c.d_subS0.upload(subS0, 6 * n, c.stream);
+    } else {
+      c.d_subZ.alloc(2); c.d_subD.alloc(36); c.d_subS0.alloc(6);
+    }
+    c.maxSub = mx;
+    c.subReady = true;
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+namespace {
+void state_ready(Context& c, int32_t stride) {
+  recovery_ready(c);
+  if (!c.subReady) fail(TM_BAD_INPUT, "stress histories need the step's sub-layers (tm_set_sublayers)");
+  if (stride < 33 + 48 * c.maxSub) fail(TM_BAD_INPUT, "state stride below 33 + 48 x the largest sub-layer count");
+  if (!c.d_eIJK.p) { c.d_eIJK.upload(c.eIJK, c.stream); c.d_zs.upload(c.zs, c.stream); }
+}
+}  // namespace
+
+tm_status tm_accumulate_state_device(tm_ctx* ctx, const double* du, int32_t nel, const int32_t* elems, int32_t stride, double* state) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (nel < 0 || (nel > 0 && (!du || !elems || !state))) fail(TM_BAD_INPUT, "tm_accumulate_state: bad arguments");
+    state_ready(c, stride);
+    launch_accumulate_state(c, du, nel, elems, stride, state);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_accumulate_state(tm_ctx* ctx, const double* du, int32_t nel, const int32_t* elems, int32_t stride, double* state) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (nel < 0 || (nel > 0 && (!du || !elems || !state))) fail(TM_BAD_INPUT, "tm_accumulate_state: bad arguments");
+    if (nel == 0) return;
+    check_elems(c, nel, elems);
+    state_ready(c, stride);
+    DBuf<int> de;
+    DBuf<double> ds;
+    c.d_tmp.upload(du, 3 * (size_t)c.nn, c.stream);
+    de.upload(elems, nel, c.stream);
+    ds.upload(state, (size_t)stride * nel, c.stream);
+    launch_accumulate_state(c, c.d_tmp.p, nel, de.p, stride, ds.p);
+    ds.download(state, (size_t)stride * nel, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_state_stress_device(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* state, int32_t stride, const double* nat,
+                                 double* eps, double* sig) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (npts < 0 || (npts > 0 && (!elem || !state || !nat || !eps || !sig))) fail(TM_BAD_INPUT, "tm_state_stress: bad arguments");
+    state_ready(c, stride);
+    launch_state_stress(c, npts, elem, state, stride, nat, eps, sig);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_state_stress(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* state, int32_t stride, const double* nat,
+                          double* eps, double* sig) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (npts < 0 || (npts > 0 && (!elem || !state || !nat || !eps || !sig))) fail(TM_BAD_INPUT, "tm_state_stress: bad arguments");
+    if (npts == 0) return;
+    check_elems(c, npts, elem);
+    state_ready(c, stride);
+    DBuf<int> de;
+    DBuf<double> ds, dn, de6, ds6;
+    de.upload(elem, npts, c.stream);
+    ds.upload(state, (size_t)stride * npts, c.stream);
+    dn.upload(nat, 3 * (size_t)npts, c.stream);
+    de6.alloc(6 * (size_t)npts); ds6.alloc(6 * (size_t)npts);
+    launch_state_stress(c, npts, de.p, ds.p, stride, dn.p, de6.p, ds6.p);
+    de6.download(eps, 6 * (size_t)npts, c.stream);
+    ds6.download(sig, 6 * (size_t)npts, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
 tm_status tm_element_strains_device(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* q, const double* nat, double* eps) {
   return guarded([&] {
     Context& c = *reinterpret_cast<Context*>(ctx);

@@ -211,6 +211,15 @@ struct Context {
   IcFactor ic;                         // the IC(0) preconditioner (tm_ic0.cu)
   int pcKind = -1;                     // kind of the preconditioner built last (TM_PC_*)
   bool stepReady = false;              // shape matrices and thermal loads of an assembled step are on the device
+  DBuf<double> d_stepD, d_stepS0;      // the step's homogeneous D (36) and s0 (6) per property set
+  // sub-layers of the layered sets for the stress histories (tm_set_sublayers): offsets per set,
+  // z ranges (2), step-mean stiffness (36) and thermal stress increment (6) per sub-layer
+  bool subReady = false;
+  int maxSub = 1;
+  DBuf<int> d_subOff;
+  DBuf<double> d_subZ, d_subD, d_subS0;
+  DBuf<int> d_eIJK;
+  DBuf<double> d_zs;
   DBuf<int> d_conn;                    // 8*ne, uploaded on first use by the DOF-history entry points
   DBuf<double> d_xs, d_ys;             // mesh lines and the node index grid, uploaded on first use
   DBuf<int> d_nodeId;                  // by the plane sampler
@@ -311,6 +320,9 @@ void launch_to_fp32(Context& c);
 void launch_accumulate_q(Context& c, const double* du, int nel, const int* elems, double* q);
 void launch_element_strains(Context& c, int np, const int* elem, const double* q, const double* nat, double* eps);
 void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts, const double* x, const double* y, double* out);
+void launch_accumulate_state(Context& c, const double* du, int nel, const int* elems, int stride, double* state);
+void launch_state_stress(Context& c, int np, const int* elem, const double* state, int stride, const double* nat, double* eps,
+                         double* sig);
 
 // ---- IC(0) (tm_ic0.cu) -------------------------------------------------------------------------
 void build_ic(Context& c);                                   // structure (once) + shifted factorization

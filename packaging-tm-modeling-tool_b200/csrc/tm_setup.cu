@@ -589,6 +589,152 @@ __global__ void k_accumulate_q(int nel, int ne, const int* __restrict__ elems, c
   for (int o = lane; o < 33; o += 32) q[33 * (size_t)t + o] += o < 24 ? dq[o] : col[o - 24];
 }
 
+// Model.accumulateStep without qOnly (09-assembly.js:508-544), warp per listed element: the DOF
+// increment as in k_accumulate_q, state[0..32] += dq and, when the material is born, the strain
+// polynomial E of dq (boxStrainPoly, :176-196) and per sub-layer S_m += D_m E_m (m < 7) and
+// S_th += the step's thermal stress increment (homogeneous sets: one layer with the set's D, s0)
+__global__ void k_accumulate_state(int nel, int ne, const int* __restrict__ elems, const int* __restrict__ conn,
+                                   const int* __restrict__ eClass, const int* __restrict__ clsPset, const double* __restrict__ clsH,
+                                   const double* __restrict__ psetM, const double* __restrict__ clsF33, const int* __restrict__ clsBorn,
+                                   const int* __restrict__ psetLayered, const double* __restrict__ stepD, const double* __restrict__ stepS0,
+                                   const int* __restrict__ subOff, const double* __restrict__ subD, const double* __restrict__ subS0,
+                                   const double* __restrict__ du, int stride, double* __restrict__ state) {
+  __shared__ double sm[4][448];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * 4 + warp;
+  if (t >= nel) return;
+  double* Kr = sm[warp];               // 297 (then the strain polynomial, 42)
+  double* Kaa = Kr + 297;              // 81
+  double* dq = Kaa + 81;               // 33: nodal DOFs, then the incompatible modes
+  double* st = state + (size_t)stride * t;
+  const int e = elems[t];
+  if (e < 0 || e >= ne) {
+    for (int o = lane; o < stride; o += 32) st[o] = CUDART_NAN;
+    return;
+  }
+  const int cls = eClass[e];
+  const double hx = clsH[3 * cls], hy = clsH[3 * cls + 1], hz = clsH[3 * cls + 2];
+  const double V8 = hx * hy * hz / 8;
+  const double c0 = V8 * 4 / (hx * hx), c1 = V8 * 4 / (hy * hy), c2 = V8 * 4 / (hz * hz);
+  const double c3 = V8 * 4 / (hx * hy), c4 = V8 * 4 / (hy * hz), c5 = V8 * 4 / (hz * hx);
+  const int pset = clsPset[cls];
+  const double* Ma = psetM + (size_t)pset * 6 * 1089 + 24 * 33;
+  for (int r = lane; r < 297; r += 32)
+    Kr[r] = c0 * Ma[r] + c1 * Ma[1089 + r] + c2 * Ma[2178 + r] + c3 * Ma[3267 + r] + c4 * Ma[4356 + r] + c5 * Ma[5445 + r];
+  if (lane < 24) dq[lane] = du[3 * (size_t)conn[8 * (size_t)e + lane / 3] + lane % 3];
+  __syncwarp();
+  for (int o = lane; o < 81; o += 32) Kaa[o] = Kr[(o / 9) * 33 + 24 + o % 9];
+  if (lane < 9) {
+    double s = clsF33[(size_t)cls * 33 + 24 + lane];
+    for (int k = 0; k < 24; k++) s -= Kr[lane * 33 + k] * dq[k];
+    dq[24 + lane] = s;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    chol_dense9(Kaa, 1e-14);
+    chol_solve9(Kaa, dq + 24);
+  }
+  __syncwarp();
+  for (int o = lane; o < 33; o += 32) st[o] += dq[o];
+  if (!clsBorn[cls]) return;
+  double* E = Kr;
+  if (lane == 0) {
+    for (int q = 0; q < 42; q++) E[q] = 0;
+    const double sx = 2 / hx, sy = 2 / hy, sz = 2 / hz;
+    for (int a = 0; a < 8; a++) {
+      const double xa = node_xi(a), ya = node_eta(a), za = node_zeta(a);
+      const double ux = dq[3 * a], uy = dq[3 * a + 1], uz = dq[3 * a + 2];
+      const double cx = xa * sx / 8, cy = ya * sy / 8, cz = za * sz / 8;
+      const int mx[4] = {0, 2, 3, 5}, my[4] = {0, 1, 3, 6}, mz[4] = {0, 1, 2, 4};
+      const double vx[4] = {cx, cx * ya, cx * za, cx * ya * za}, vy[4] = {cy, cy * xa, cy * za, cy * xa * za},
+                   vz[4] = {cz, cz * xa, cz * ya, cz * xa * ya};
+      for (int k = 0; k < 4; k++) { const int m = mx[k]; const double c = vx[k]; E[6 * m] += c * ux; E[6 * m + 3] += c * uy; E[6 * m + 5] += c * uz; }
+      for (int k = 0; k < 4; k++) { const int m = my[k]; const double c = vy[k]; E[6 * m + 1] += c * uy; E[6 * m + 3] += c * ux; E[6 * m + 4] += c * uz; }
+      for (int k = 0; k < 4; k++) { const int m = mz[k]; const double c = vz[k]; E[6 * m + 2] += c * uz; E[6 * m + 4] += c * uy; E[6 * m + 5] += c * ux; }
+    }
+    const double* a1 = dq + 24; const double* a2 = dq + 27; const double* a3 = dq + 30;
+    E[6] += -2 * sx * a1[0]; E[6 + 3] += -2 * sx * a1[1]; E[6 + 5] += -2 * sx * a1[2];
+    E[12 + 1] += -2 * sy * a2[1]; E[12 + 3] += -2 * sy * a2[0]; E[12 + 4] += -2 * sy * a2[2];
+    E[18 + 2] += -2 * sz * a3[2]; E[18 + 4] += -2 * sz * a3[1]; E[18 + 5] += -2 * sz * a3[0];
+  }
+  __syncwarp();
+  const bool lay = psetLayered[pset] != 0;
+  const int ns = lay ? subOff[pset + 1] - subOff[pset] : 1;
+  for (int idx = lane; idx < 48 * ns; idx += 32) {
+    const int s = idx / 48, rem = idx % 48;
+    const double* D = lay ? subD + 36 * (size_t)(subOff[pset] + s) : stepD + 36 * (size_t)pset;
+    const double* s0 = lay ? subS0 + 6 * (size_t)(subOff[pset] + s) : stepS0 + 6 * (size_t)pset;
+    double* o = st + 33 + 48 * s;
+    if (rem < 42) {
+      const int mo = rem / 6, r = rem % 6;
+      double v = 0;
+      for (int k = 0; k < 6; k++) v += D[r * 6 + k] * E[6 * mo + k];
+      o[6 * mo + r] += v;
+    } else {
+      o[rem] += s0[rem - 42];
+    }
+  }
+}
+
+// stateStress (09-assembly.js:555-571) with subLayerAt (:547-552), thread per point: total strain
+// and stress of element elem[t] from its state at the natural point nat[3 t ..]
+__global__ void k_state_stress(int np, int ne, const int* __restrict__ elem, const int* __restrict__ eClass,
+                               const int* __restrict__ clsPset, const double* __restrict__ clsH, const int* __restrict__ eIJK,
+                               const double* __restrict__ zs, const int* __restrict__ psetLayered, const int* __restrict__ subOff,
+                               const double* __restrict__ subZ, const double* __restrict__ state, int stride,
+                               const double* __restrict__ nat, double* __restrict__ eps, double* __restrict__ sig) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np) return;
+  double* oe = eps + 6 * (size_t)t;
+  double* os = sig + 6 * (size_t)t;
+  const int e = elem[t];
+  if (e < 0 || e >= ne) {
+    for (int r = 0; r < 6; r++) { oe[r] = CUDART_NAN; os[r] = CUDART_NAN; }
+    return;
+  }
+  const int cls = eClass[e];
+  const double sx = 2 / clsH[3 * cls], sy = 2 / clsH[3 * cls + 1], sz = 2 / clsH[3 * cls + 2];
+  const double xi = nat[3 * (size_t)t], eta = nat[3 * (size_t)t + 1], zeta = nat[3 * (size_t)t + 2];
+  const double* u = state + (size_t)stride * t;
+  double e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0, e5 = 0;
+  for (int b = 0; b < 11; b++) {
+    double dx, dy, dz;
+    if (b < 8) {
+      const double xa = node_xi(b), ya = node_eta(b), za = node_zeta(b);
+      dx = xa * (1 + ya * eta) * (1 + za * zeta) * 0.125 * sx;
+      dy = ya * (1 + xa * xi) * (1 + za * zeta) * 0.125 * sy;
+      dz = za * (1 + xa * xi) * (1 + ya * eta) * 0.125 * sz;
+    } else {
+      dx = b == 8 ? -2 * xi * sx : 0;
+      dy = b == 9 ? -2 * eta * sy : 0;
+      dz = b == 10 ? -2 * zeta * sz : 0;
+    }
+    const double ux = u[3 * b], uy = u[3 * b + 1], uz = u[3 * b + 2];
+    e0 += dx * ux; e1 += dy * uy; e2 += dz * uz;
+    e3 += dy * ux + dx * uy;
+    e4 += dz * uy + dy * uz;
+    e5 += dz * ux + dx * uz;
+  }
+  oe[0] = e0; oe[1] = e1; oe[2] = e2; oe[3] = e3; oe[4] = e4; oe[5] = e5;
+  const int pset = clsPset[cls];
+  int s = 0;
+  if (psetLayered[pset]) {
+    const int k = eIJK[3 * (size_t)e + 2];
+    const double z = zs[k] + 0.5 * (zeta + 1) * (zs[k + 1] - zs[k]);
+    const int ns = subOff[pset + 1] - subOff[pset];
+    s = ns - 1;
+    for (int q = 0; q < ns; q++)
+      if (z <= subZ[2 * (size_t)(subOff[pset] + q) + 1] + 1e-12) { s = q; break; }
+  }
+  const double phi[7] = {1, xi, eta, zeta, xi * eta, eta * zeta, xi * zeta};
+  const double* o = u + 33 + 48 * s;
+  for (int r = 0; r < 6; r++) {
+    double v = -o[42 + r];
+    for (int mo = 0; mo < 7; mo++) v += phi[mo] * o[6 * mo + r];
+    os[r] = v;
+  }
+}
+
 // boxStrainAt (07-element.js:127-142) with boxDerivs (:19-30), thread per point: engineering
 // strain of element elem[t] with DOFs q[33 t ..] at the natural point nat[3 t ..]
 __global__ void k_element_strains(int np, int ne, const int* __restrict__ elem, const int* __restrict__ eClass,
@@ -683,8 +829,17 @@ void launch_shape_matrices(Context& c, const tm_step& st) {
   c.d_psetM.upload(M, c.stream);
   c.d_clsF33.upload(f33, c.stream);
   c.d_clsBorn.upload(clsBorn, c.stream);
+  c.d_psetLayered.upload(lay, c.stream);
+  if (st.D && st.s0) {
+    c.d_stepD.upload(st.D, 36 * (size_t)c.npset, c.stream);
+    c.d_stepS0.upload(st.s0, 6 * (size_t)c.npset, c.stream);
+  } else {   // every set layered: no homogeneous data
+    c.d_stepD.alloc(36 * (size_t)c.npset); c.d_stepD.zero(c.stream);
+    c.d_stepS0.alloc(6 * (size_t)c.npset); c.d_stepS0.zero(c.stream);
+  }
   c.stage = st.stage;
   c.stepReady = true;
+  c.subReady = false;
 }
 
 void launch_class_condense(Context& c) {
@@ -821,6 +976,24 @@ void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts,
   }
   note_launch();
   k_sample_plane<<<grid_for(npts, 128), 128, 0, c.stream>>>(npts, c.nx, c.ny, c.nz, c.d_xs.p, c.d_ys.p, c.d_nodeId.p, u, k, comp, x, y, out);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_accumulate_state(Context& c, const double* du, int nel, const int* elems, int stride, double* state) {
+  if (nel <= 0) return;
+  note_launch();
+  k_accumulate_state<<<(nel + 3) / 4, 128, 0, c.stream>>>(nel, c.ne, elems, c.d_conn.p, c.d_eClass.p, c.d_clsPset.p, c.d_clsH.p, c.d_psetM.p,
+                                                          c.d_clsF33.p, c.d_clsBorn.p, c.d_psetLayered.p, c.d_stepD.p, c.d_stepS0.p,
+                                                          c.d_subOff.p, c.d_subD.p, c.d_subS0.p, du, stride, state);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_state_stress(Context& c, int np, const int* elem, const double* state, int stride, const double* nat, double* eps,
+                         double* sig) {
+  if (np <= 0) return;
+  note_launch();
+  k_state_stress<<<grid_for(np, 128), 128, 0, c.stream>>>(np, c.ne, elem, c.d_eClass.p, c.d_clsPset.p, c.d_clsH.p, c.d_eIJK.p, c.d_zs.p,
+                                                         c.d_psetLayered.p, c.d_subOff.p, c.d_subZ.p, state, stride, nat, eps, sig);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 

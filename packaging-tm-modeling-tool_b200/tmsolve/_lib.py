@@ -23,7 +23,8 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_element_strains", "tm_element_strains_device", "tm_sample_plane", "tm_sample_plane_device",
             "tm_anand_screen_pillar", "tm_anand_screen_pillar_device", "tm_pc_apply", "tm_pc_apply_device",
             "tm_submodel_create", "tm_submodel_destroy", "tm_submodel_sizes", "tm_submodel_step", "tm_submodel_get",
-            "tm_submodel_run", "tm_submodel_run_batch"]
+            "tm_submodel_run", "tm_submodel_run_batch", "tm_set_sublayers", "tm_accumulate_state",
+            "tm_accumulate_state_device", "tm_state_stress", "tm_state_stress_device"]
 PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
 PRECOND_NAMES = {v: k for k, v in PRECONDS.items()}
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
@@ -129,6 +130,11 @@ def load():
     L.tm_kernel_timer.argtypes = [vp, C.c_int32]
     L.tm_kernel_timer_read.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     L.tm_prepare_step.argtypes = [vp, C.POINTER(TmStep)]
+    L.tm_set_sublayers.argtypes = [vp, vp, vp, vp, vp]
+    L.tm_accumulate_state.argtypes = [vp, vp, C.c_int32, vp, C.c_int32, vp]
+    L.tm_accumulate_state_device.argtypes = L.tm_accumulate_state.argtypes
+    L.tm_state_stress.argtypes = [vp, C.c_int32, vp, vp, C.c_int32, vp, vp, vp]
+    L.tm_state_stress_device.argtypes = L.tm_state_stress.argtypes
     L.tm_accumulate_q.argtypes = [vp, vp, C.c_int32, vp, vp]
     L.tm_accumulate_q_device.argtypes = L.tm_accumulate_q.argtypes
     L.tm_element_strains.argtypes = [vp, C.c_int32, vp, vp, vp, vp]

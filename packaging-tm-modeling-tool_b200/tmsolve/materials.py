@@ -124,15 +124,18 @@ def sublayer_shell_d(D: np.ndarray) -> np.ndarray:
     return D
 
 
-def layered_section(z0: float, z1: float, subs, Ta: float, Tb: float, plane_stress=True):
+def layered_section(z0: float, z1: float, subs, Ta: float, Tb: float, plane_stress=True, with_subs=False):
     """Step weights of one layered band of constant-property sub-layers.
 
     subs: list of (sz0, sz1, D36, cte_xy, cte_z). Returns (W 108, V 18) as in
     buildBandSection's W_j (04-homogenize.js:172-181) averaged over the step
-    (constant here) and sectionVstep (:212-221)."""
+    (constant here) and sectionVstep (:212-221); with_subs adds the sub-layers'
+    z ranges, step-mean stiffnesses and thermal stress increments (sectionSubMeanD,
+    sectionSubStress, :196-204), which the element stress histories read."""
     h = z1 - z0
     W = np.zeros(108)
     V = np.zeros(18)
+    sz, sD, sS = [], [], []
     for (sz0, sz1, D, axy, az) in subs:
         Dl = sublayer_shell_d(D) if plane_stress else np.asarray(D, np.float64)
         L = lagrange3_integrals(2 * (sz0 - z0) / h - 1, 2 * (sz1 - z0) / h - 1)
@@ -140,6 +143,9 @@ def layered_section(z0: float, z1: float, subs, Ta: float, Tb: float, plane_stre
         for j in range(3):
             W[j * 36:(j + 1) * 36] += Dl * L[j]
             V[j * 6:(j + 1) * 6] += s0 * L[j]
+        sz.append((sz0, sz1)); sD.append(Dl); sS.append(s0)
+    if with_subs:
+        return W, V, (np.array(sz, np.float64).reshape(-1), np.concatenate(sD), np.concatenate(sS))
     return W, V
 
 

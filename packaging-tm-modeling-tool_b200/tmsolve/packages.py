@@ -41,6 +41,13 @@ class StepData:
     V: np.ndarray            # (npset*18,)
     born: np.ndarray         # (npset,) int32: thermal load on
     stage: int = 0
+    # layered sets' sub-layers for the element stress histories: count per set (0 for homogeneous
+    # sets), then per sub-layer in set order its z range (2), mean stiffness (36) and thermal
+    # stress increment (6) of the step
+    sub_n: Optional[np.ndarray] = None
+    sub_z: Optional[np.ndarray] = None
+    sub_D: Optional[np.ndarray] = None
+    sub_s0: Optional[np.ndarray] = None
 
 
 @dataclass
@@ -73,16 +80,20 @@ def _homog_step(mats, Ta, Tb, npset=None, layered_fn=None) -> StepData:
     n = len(mats) if npset is None else npset
     lay = np.zeros(n, np.int32); D = np.zeros(n * 36); s0 = np.zeros(n * 6)
     W = np.zeros(n * 108); V = np.zeros(n * 18)
+    sub_n = np.zeros(n, np.int32); sz, sD, sS = [], [], []
     for p, m in enumerate(mats):
         if m is None:
             lay[p] = 1
-            Wp, Vp = layered_fn(p, Ta, Tb)
+            Wp, Vp, (z, d, s) = layered_fn(p, Ta, Tb)
             W[108 * p:108 * p + 108] = Wp; V[18 * p:18 * p + 18] = Vp
+            sub_n[p] = len(z) // 2; sz.append(z); sD.append(d); sS.append(s)
         else:
             Dp, axy, az = m
             D[36 * p:36 * p + 36] = Dp
             s0[6 * p:6 * p + 6] = thermal_stress_const(Dp, axy, az, Ta, Tb)
-    return StepData(layered=lay, D=D, s0=s0, W=W, V=V, born=np.ones(n, np.int32))
+    cat = lambda a: np.concatenate(a) if a else np.zeros(0)
+    return StepData(layered=lay, D=D, s0=s0, W=W, V=V, born=np.ones(n, np.int32), sub_n=sub_n, sub_z=cat(sz), sub_D=cat(sD),
+                    sub_s0=cat(sS))
 
 
 def linspace(a, b, n):
@@ -256,7 +267,7 @@ def lidded_c2(n_inplane: int = 160, seed: int = 20261203) -> Package:
     del hom
     def layered_fn(p, Ta, Tb):
         b0, b1, subs = band_subs[p]
-        return layered_section(b0, b1, subs, Ta, Tb)
+        return layered_section(b0, b1, subs, Ta, Tb, with_subs=True)
     ng = 7
     group_layered = np.array([1, 0, 0, 0, 0, 0, 0], np.int32)
     group_pset = np.array([0, nb + 0, nb + 1, nb + 2, nb + 3, nb + 4, nb + 5], np.int32)

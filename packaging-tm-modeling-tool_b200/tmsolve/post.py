@@ -22,6 +22,11 @@ Every function follows one reference function (paths within the reference projec
   site_elements          the site -> element lookup of siteStrainTable, 13-fatigue.js:318-331
   q_along                Analysis.qAlong, src/core/11-analysis.js:298-316 (state25 :276-281)
   site_strain_table      siteStrainTable, src/core/13-fatigue.js:318-346
+  state_stride           stateSize, src/core/09-assembly.js:494-499
+  states_along           StateView.state (src/core/11-analysis.js:343-375) for a set of elements
+  eig_sym3, max_principal  eigSym3 / maxPrincipal, src/core/01-util.js:148-173
+  joint_loads            jointLoads / bumpLoads, src/core/12-post.js:245-299
+  die_surface_stress     dieSurfaceStress, src/core/12-post.js:178-243
 
 Arithmetic is plain Python floats in the reference's order of operations, so the results are
 the reference's to the last bit for the same sampled values.
@@ -43,6 +48,13 @@ SCREEN_MAX_BUMPS = 20000
 SCREEN_MAX_DDI = 5000
 SCREEN_KEEP_ROWS = 3
 SCREEN_CORNER_BLOCK = 10
+DIE_EDGE_BAND = 0.5      # 00-constants.js:86-88
+CORNER_PATCH = 0.1
+PATCH_SAMPLES = 5
+GP2 = 1 / math.sqrt(3)
+_HX = (-1, 1, 1, -1, -1, 1, 1, -1)
+_HY = (-1, -1, 1, 1, -1, -1, 1, 1)
+_HZ = (-1, -1, -1, -1, 1, 1, 1, 1)
 
 
 def clamp(x: float, lo: float, hi: float) -> float:
@@ -372,3 +384,223 @@ def site_strain_table(model, path: ThermalPath, sites: dict, temps, zmid: float,
         for r, q in enumerate(idx):
             out[(q * nt + ti) * 6:(q * nt + ti) * 6 + 6] = eps[r]
     return out
+
+
+# ---- element stress histories and the stress readers ------------------------------------------
+def state_stride(step) -> int:
+    """Doubles per element state: q (33), then per sub-layer 7 monomial stresses and the thermal
+    stress (48), for the largest sub-layer count of the step's property sets."""
+    ns = int(np.max(step.sub_n)) if step.sub_n is not None and len(step.sub_n) else 1
+    return 33 + 48 * max(1, ns)
+
+
+def states_along(model, path: ThermalPath, elems, temps, stride: int) -> Dict[float, np.ndarray]:
+    """Element history states (nel x stride) at the as-assembled temperatures: the 25 degC state
+    (the chain), then each branch marched from it (StateView.state); one launch per step."""
+    elems = np.ascontiguousarray(elems, np.int32)
+    nel = len(elems)
+    want = set(float(t) for t in temps)
+    hi, lo = max(want), min(want)
+    base = np.zeros(stride * nel)
+
+    def advance(k, st):
+        model.prepare_step(path.steps[k])
+        model.set_sublayers(path.steps[k])
+        model.accumulate_state(path.du[k], elems, stride, st)
+    for k in path.chain:
+        advance(k, base)
+    out: Dict[float, np.ndarray] = {}
+    if 25.0 in want:
+        out[25.0] = base.reshape(nel, stride).copy()
+    for br, end in ((path.up, hi), (path.down, lo)):
+        if end == 25:
+            continue
+        st = base.copy()
+        for k in br:
+            advance(k, st)
+            T = float(path.Tb[k])
+            if T in want:
+                out[T] = st.reshape(nel, stride).copy()
+            if T == end:
+                break
+    return out
+
+
+def eig_sym3(s) -> tuple:
+    """Eigenvalues, descending, of the symmetric tensor in Voigt order (xx yy zz xy yz zx)."""
+    a, b, c, d, e, f = (float(v) for v in s[:6])
+    p1 = d * d + e * e + f * f
+    if p1 <= 1e-30 * (a * a + b * b + c * c + 1e-300):
+        x, y, z = a, b, c
+        if x < y:
+            x, y = y, x
+        if y < z:
+            y, z = z, y
+        if x < y:
+            x, y = y, x
+        return (x, y, z)
+    q = (a + b + c) / 3
+    p2 = (a - q) * (a - q) + (b - q) * (b - q) + (c - q) * (c - q) + 2 * p1
+    p = math.sqrt(p2 / 6)
+    B0, B1, B2, B3, B4, B5 = (a - q) / p, (b - q) / p, (c - q) / p, d / p, e / p, f / p
+    detB = B0 * (B1 * B2 - B4 * B4) - B3 * (B3 * B2 - B4 * B5) + B5 * (B3 * B4 - B1 * B5)
+    r = clamp(detB / 2, -1, 1)
+    phi = math.acos(r) / 3
+    e1 = q + 2 * p * math.cos(phi)
+    e3 = q + 2 * p * math.cos(phi + 2 * math.pi / 3)
+    return (e1, 3 * q - e1 - e3, e3)
+
+
+def max_principal(s) -> float:
+    return eig_sym3(s)[0]
+
+
+def joint_loads(model, states: np.ndarray, state_elems, stride: int, sites: dict, zmid: float, part: Optional[int], A: float) -> dict:
+    """Per-joint axial force N = szz A and shear force V = |(tyz, tzx)| A at the bump sites from the
+    element states at one temperature (states[t] the state of element state_elems[t]), with the
+    worst axial and shear joints and the ten largest |(N, V)|."""
+    mesh = model.pkg.mesh
+    n = len(sites["x"])
+    N = np.full(n, np.nan); V = np.full(n, np.nan); szz = np.full(n, np.nan)
+    elem, nat = site_elements(mesh, sites["x"], sites["y"], zmid, part)
+    have = np.nonzero(elem >= 0)[0]
+    if len(have):
+        row = {int(e): t for t, e in enumerate(np.asarray(state_elems))}
+        idx = np.array([row[int(elem[q])] for q in have])
+        _, sig = model.state_stress(elem[have], states[idx], stride, nat[have])
+        for r, q in enumerate(have):
+            szz[q] = sig[r, 2]
+            N[q] = sig[r, 2] * A
+            V[q] = math.hypot(sig[r, 4], sig[r, 5]) * A
+    worstN, worstV, iN, iV = -math.inf, -math.inf, -1, -1
+    for q in range(n):
+        if math.isfinite(N[q]) and abs(N[q]) > worstN:
+            worstN, iN = abs(N[q]), q
+        if math.isfinite(V[q]) and V[q] > worstV:
+            worstV, iV = V[q], q
+    order = sorted([q for q in range(n) if math.isfinite(V[q])], key=lambda q: -math.hypot(N[q], V[q]))[:10]
+    return dict(N=N, V=V, szz=szz, worstN=N[iN] if iN >= 0 else math.nan, worstV=V[iV] if iV >= 0 else math.nan,
+                worstNidx=iN, worstVidx=iV, worst=[dict(q=q, x=float(sites["x"][q]), y=float(sites["y"][q]), N=float(N[q]), V=float(V[q]))
+                                                   for q in order], abump=A)
+
+
+def plane_index(mesh, z: float) -> int:
+    best, bd = 0, math.inf
+    for k in range(mesh.nz):
+        d = abs(float(mesh.zs[k]) - z)
+        if d < bd:
+            bd, best = d, k
+    return best
+
+
+def _gp_to_node() -> np.ndarray:
+    s = math.sqrt(3)
+    M = np.zeros(64)
+    for n in range(8):
+        N = [0.125 * (1 + _HX[g] * _HX[n] * s) * (1 + _HY[g] * _HY[n] * s) * (1 + _HZ[g] * _HZ[n] * s) for g in range(8)]
+        for g in range(8):
+            M[n * 8 + g] = N[g]
+    return M
+
+
+def die_elements(mesh, rect: dict, k_elem: int, part: Optional[int], group: int) -> list:
+    """The elements of one silicon part on element layer k_elem over its footprint: (i, j, e)."""
+    xs, ys = [float(v) for v in mesh.xs], [float(v) for v in mesh.ys]
+    i0, i1 = find_interval(xs, rect["x0"] + 1e-9), find_interval(xs, rect["x1"] - 1e-9) + 1
+    j0, j1 = find_interval(ys, rect["y0"] + 1e-9), find_interval(ys, rect["y1"] - 1e-9) + 1
+    out = []
+    for i in range(i0, i1):
+        for j in range(j0, j1):
+            e = element_in_cell(mesh, i, j, k_elem, part)
+            if e >= 0 and int(mesh.eGroup[e]) == group:
+                out.append((i, j, e))
+    return out, (i0, i1, j0, j1)
+
+
+def die_surface_stress(model, states: np.ndarray, state_elems, stride: int, rect: dict, ztop: float, zb: float, part: Optional[int],
+                       group: int, which: str = "top") -> dict:
+    """Nodal-averaged stress on the top or bottom face of a silicon part from its adjacent
+    elements' Gauss-point stresses (extrapolated to the face nodes), the largest principal
+    stress over the part's columns, its interior peak (outside DIE_EDGE_BAND), the Gauss-point
+    peaks and the 100 um patch averages at the four corners and mid-edges."""
+    mesh = model.pkg.mesh
+    top = which == "top"
+    kp = plane_index(mesh, ztop if top else zb)
+    k_elem = kp - 1 if top else kp
+    zeta_face = 1 if top else -1
+    elems, (i0, i1, j0, j1) = die_elements(mesh, rect, k_elem, part, group)
+    nxd, nyd = i1 - i0 + 1, j1 - j0 + 1
+    total = np.zeros(nxd * nyd * 6); cnt = np.zeros(nxd * nyd, np.int64)
+    band = DIE_EDGE_BAND
+    inner = dict(x0=rect["x0"] + band, x1=rect["x1"] - band, y0=rect["y0"] + band, y1=rect["y1"] - band)
+    inrect = lambda r, x, y: r["x0"] <= x <= r["x1"] and r["y0"] <= y <= r["y1"]
+    gpPeak, gpPeakAll = -math.inf, -math.inf
+    G2N = _gp_to_node()
+    xs, ys = mesh.xs, mesh.ys
+    if elems:
+        row = {int(e): t for t, e in enumerate(np.asarray(state_elems))}
+        E = np.repeat(np.array([e for _, _, e in elems], np.int32), 8)
+        nat = np.tile(np.array([[_HX[g] * GP2, _HY[g] * GP2, _HZ[g] * GP2] for g in range(8)]), (len(elems), 1))
+        _, sig = model.state_stress(E, states[np.array([row[int(e)] for e in E])], stride, nat)
+        for t, (i, j, e) in enumerate(elems):
+            gp = sig[8 * t:8 * t + 8]
+            for g in range(8):
+                sp = max_principal(gp[g])
+                if _HZ[g] == zeta_face:
+                    gx = 0.5 * (xs[i] + xs[i + 1]) + _HX[g] * GP2 * 0.5 * (xs[i + 1] - xs[i])
+                    gy = 0.5 * (ys[j] + ys[j + 1]) + _HY[g] * GP2 * 0.5 * (ys[j + 1] - ys[j])
+                    gpPeakAll = max(gpPeakAll, sp)
+                    if inrect(inner, gx, gy):
+                        gpPeak = max(gpPeak, sp)
+            for a in range(8):
+                if _HZ[a] != zeta_face:
+                    continue
+                gi, gj = i - i0 + (1 if _HX[a] > 0 else 0), j - j0 + (1 if _HY[a] > 0 else 0)
+                o = (gi * nyd + gj) * 6
+                for c in range(6):
+                    v = 0.0
+                    for g in range(8):
+                        v += G2N[a * 8 + g] * float(gp[g, c])
+                    total[o + c] += v
+                cnt[gi * nyd + gj] += 1
+    smax = np.full(nxd * nyd, np.nan); sxx = np.full(nxd * nyd, np.nan); syy = np.full(nxd * nyd, np.nan)
+    for q in range(nxd * nyd):
+        if not cnt[q]:
+            continue
+        tens = [total[6 * q + c] / cnt[q] for c in range(6)]
+        smax[q] = max_principal(tens); sxx[q] = tens[0]; syy[q] = tens[1]
+    gxs = [float(v) for v in xs[i0:i1 + 1]]; gys = [float(v) for v in ys[j0:j1 + 1]]
+    peak, px, py = -math.inf, math.nan, math.nan
+    for a in range(nxd):
+        for b in range(nyd):
+            v = smax[a * nyd + b]
+            if not math.isfinite(v) or not inrect(inner, gxs[a], gys[b]):
+                continue
+            if v > peak:
+                peak, px, py = v, gxs[a], gys[b]
+
+    def sample_grid(x, y):
+        a, b = find_interval(gxs, x), find_interval(gys, y)
+        tx = (x - gxs[a]) / (gxs[a + 1] - gxs[a]); ty = (y - gys[b]) / (gys[b + 1] - gys[b])
+        v00, v10 = smax[a * nyd + b], smax[(a + 1) * nyd + b]
+        v01, v11 = smax[a * nyd + b + 1], smax[(a + 1) * nyd + b + 1]
+        return (1 - tx) * (1 - ty) * v00 + tx * (1 - ty) * v10 + (1 - tx) * ty * v01 + tx * ty * v11
+
+    def patch(xa, ya):
+        P, m = CORNER_PATCH, PATCH_SAMPLES
+        acc = 0.0
+        for a in range(m):
+            for b in range(m):
+                acc += sample_grid(xa + P * (a + 0.5) / m, ya + P * (b + 0.5) / m)
+        return acc / (m * m)
+    P, r = CORNER_PATCH, rect
+    corners = [(1, r["x1"], r["y0"], 1, -1), (2, r["x0"], r["y0"], -1, -1), (3, r["x0"], r["y1"], -1, 1), (4, r["x1"], r["y1"], 1, 1)]
+    corner_vals = [dict(n=n, x=x, y=y, value=patch(x - P if sx > 0 else x, y - P if sy > 0 else y)) for n, x, y, sx, sy in corners]
+    cx, cy = 0.5 * (r["x0"] + r["x1"]), 0.5 * (r["y0"] + r["y1"])
+    mid = [dict(name="1-2", x=cx, y=r["y0"], value=patch(cx - P / 2, r["y0"])),
+           dict(name="2-3", x=r["x0"], y=cy, value=patch(r["x0"], cy - P / 2)),
+           dict(name="3-4", x=cx, y=r["y1"], value=patch(cx - P / 2, r["y1"] - P)),
+           dict(name="4-1", x=r["x1"], y=cy, value=patch(r["x1"] - P, cy - P / 2))]
+    return dict(which=which, xs=np.array(gxs), ys=np.array(gys), nx=nxd, ny=nyd, smax=smax, sxx=sxx, syy=syy, peakInterior=peak,
+                peakX=px, peakY=py, gpPeakInterior=gpPeak, gpPeakAll=gpPeakAll, corners=corner_vals, midEdges=mid)
+

@@ -157,6 +157,37 @@ class DeviceModel:
                                         nat.ctypes.data_as(C.c_void_p), eps.ctypes.data_as(C.c_void_p)))
         return eps.reshape(-1, 6)
 
+    def set_sublayers(self, step: StepData):
+        """The step's sub-layers of the layered property sets, for the stress histories (call
+        after prepare_step / assemble_step of that step)."""
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        n = np.ascontiguousarray(step.sub_n if step.sub_n is not None else np.zeros(len(step.layered)), np.int32)
+        z = np.ascontiguousarray(step.sub_z if step.sub_z is not None and len(step.sub_z) else np.zeros(2), np.float64)
+        d = np.ascontiguousarray(step.sub_D if step.sub_D is not None and len(step.sub_D) else np.zeros(36), np.float64)
+        s0 = np.ascontiguousarray(step.sub_s0 if step.sub_s0 is not None and len(step.sub_s0) else np.zeros(6), np.float64)
+        check(load().tm_set_sublayers(self.h, vp(n), vp(z), vp(d), vp(s0)))
+
+    def accumulate_state(self, du, elems, stride: int, state: np.ndarray) -> np.ndarray:
+        """Model.accumulateStep (src/core/09-assembly.js:508-544): state (nel x stride, updated in
+        place) += q's increment and the sub-layer stress monomials of the step loaded last."""
+        du = np.ascontiguousarray(du, np.float64); elems = np.ascontiguousarray(elems, np.int32)
+        if state.dtype != np.float64 or not state.flags.c_contiguous or state.size != stride * len(elems):
+            raise ValueError("state must be a contiguous float64 array of stride values per element")
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(load().tm_accumulate_state(self.h, vp(du), len(elems), vp(elems), int(stride), vp(state)))
+        return state
+
+    def state_stress(self, elem, state, stride: int, nat) -> tuple:
+        """stateStress (src/core/09-assembly.js:555-571): (eps, sig), (npts, 6) each."""
+        elem = np.ascontiguousarray(elem, np.int32)
+        state = np.ascontiguousarray(state, np.float64).reshape(-1); nat = np.ascontiguousarray(nat, np.float64).reshape(-1)
+        if state.size != stride * len(elem) or nat.size != 3 * len(elem):
+            raise ValueError("state needs stride and nat 3 values per point")
+        eps = np.zeros(6 * len(elem)); sig = np.zeros(6 * len(elem))
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(load().tm_state_stress(self.h, len(elem), vp(elem), vp(state), int(stride), vp(nat), vp(eps), vp(sig)))
+        return eps.reshape(-1, 6), sig.reshape(-1, 6)
+
     def sample_plane(self, u, k: int, comp: int, x, y) -> np.ndarray:
         """samplePlane (src/core/12-post.js:30-38) of the nodal field u at the points (x, y)."""
         u = np.ascontiguousarray(u, np.float64)

@@ -130,3 +130,74 @@ def test_site_strain_table_matches_oracle(c1):
     # the strain grows with the temperature distance from 25 degC on both branches
     ezz = np.abs(table[:, :, 2] - table[:, 2:3, 2]).mean(axis=0)
     assert ezz[0] > ezz[1] > 0 and ezz[4] > ezz[3] > 0
+
+
+def test_accumulate_state_and_stress_bit_exact(oracle_lib):
+    """Element stress histories on a layered package (sub-layers of the 8-2-8 substrate bands)
+    over two steps, and the stress at points: bit-exact with the oracle."""
+    from tmsolve.packages import lidded_c2
+    from tmsolve.solver import DeviceModel
+    pkg = lidded_c2(n_inplane=24)
+    dm, om = DeviceModel(pkg), oracle_lib.OracleModel(pkg)
+    m = pkg.mesh
+    rng = np.random.default_rng(11)
+    elems = np.unique(rng.integers(0, m.ne, 400)).astype(np.int32)
+    st0 = pkg.step()
+    stride = post.state_stride(st0)
+    Sg = np.zeros(stride * len(elems)); So = np.zeros(stride * len(elems))
+    for Ta, Tb in ((150.0, 25.0), (25.0, 125.0)):
+        st = pkg.step(Ta, Tb)
+        du = rng.standard_normal(dm.ndof).astype(np.float32).astype(np.float64) * 1e-3
+        dm.prepare_step(st); dm.set_sublayers(st)
+        om.assemble(st); om.set_sublayers(st)
+        dm.accumulate_state(du, elems, stride, Sg)
+        om.accumulate_state(du, elems, stride, So)
+        assert np.array_equal(Sg, So), np.abs(Sg - So).max()
+    nat = rng.uniform(-1, 1, (len(elems), 3))
+    eg, sg = dm.state_stress(elems, Sg, stride, nat)
+    eo, so = om.state_stress(elems, So, stride, nat)
+    assert np.array_equal(eg, eo) and np.array_equal(sg, so)
+    assert np.abs(sg).max() > 0
+    with pytest.raises(_lib.TmError):
+        dm.accumulate_state(du, elems, 33, np.zeros(33 * len(elems)))     # stride below the sub-layers
+
+
+def test_joint_loads_and_die_stress_match_oracle(c1, oracle_lib):
+    """jointLoads and dieSurfaceStress (12-post.js:178-299) from the element histories of a short
+    thermal path: the host readers driven by the GPU states equal those driven by the oracle's."""
+    pkg, dm, om = c1
+    legs = [(150.0, 25.0), (25.0, 125.0)]
+    steps, du, Tb = [], [], []
+    for Ta, Tb_ in legs:
+        st = pkg.step(Ta, Tb_)
+        r = dm.solve(dm.assemble_step(st), tol=1e-10)
+        steps.append(st); du.append(r["u"].astype(np.float32).astype(np.float64)); Tb.append(Tb_)
+    path = post.ThermalPath(steps=steps, Tb=Tb, du=du, chain=[0], up=[1])
+    m = pkg.mesh
+    stride = post.state_stride(steps[0])
+    # the elements the readers visit: bump-layer solder and the die's top and bottom layers
+    s, elem, nat = _site_elems(pkg)
+    rect = dict(x0=-7.5, x1=7.5, y0=-7.5, y1=7.5)
+    zb, ztop = 1.28, float(m.zs[-1])
+    die_top, _ = post.die_elements(m, rect, post.plane_index(m, ztop) - 1, 4, 3)
+    die_bot, _ = post.die_elements(m, rect, post.plane_index(m, zb), 4, 3)
+    uniq = np.unique(np.concatenate([elem[elem >= 0], [e for _, _, e in die_top], [e for _, _, e in die_bot]])).astype(np.int32)
+    states = post.states_along(dm, path, uniq, [25.0, 125.0], stride)
+    base = np.zeros(stride * len(uniq))
+    om.assemble(steps[0]); om.set_sublayers(steps[0]); om.accumulate_state(du[0], uniq, stride, base)
+    o125 = base.copy()
+    om.assemble(steps[1]); om.set_sublayers(steps[1]); om.accumulate_state(du[1], uniq, stride, o125)
+    assert np.array_equal(states[25.0].reshape(-1), base) and np.array_equal(states[125.0].reshape(-1), o125)
+    bl = pkg.meta["bump_layer"]
+    A = 0.25 * np.pi * 0.09 ** 2
+    sites = dict(x=s["x"][::7], y=s["y"][::7])
+    jg = post.joint_loads(dm, states[125.0], uniq, stride, sites, bl["zmid"], bl["part"], A)
+    jo = post.joint_loads(om, o125.reshape(len(uniq), stride), uniq, stride, sites, bl["zmid"], bl["part"], A)
+    assert np.array_equal(jg["N"], jo["N"]) and np.array_equal(jg["V"], jo["V"]) and jg["worst"] == jo["worst"]
+    assert np.all(np.isfinite(jg["N"]))
+    for which in ("top", "bottom"):
+        dg = post.die_surface_stress(dm, states[125.0], uniq, stride, rect, ztop, zb, 4, 3, which)
+        do = post.die_surface_stress(om, o125.reshape(len(uniq), stride), uniq, stride, rect, ztop, zb, 4, 3, which)
+        assert np.array_equal(dg["smax"], do["smax"], equal_nan=True)
+        assert dg["peakInterior"] == do["peakInterior"] and dg["corners"] == do["corners"] and dg["midEdges"] == do["midEdges"]
+        assert np.isfinite(dg["peakInterior"])

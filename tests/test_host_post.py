@@ -166,3 +166,57 @@ def test_site_elements_bump_layer():
     e2, _ = post.site_elements(m, [15.0], [15.0], bl["zmid"], bl["part"])
     assert e2[0] == -1
     assert post.find_interval([0.0, 1.0, 2.0], math.nan) == 0
+
+
+def test_eig_sym3_known_answers():
+    assert post.eig_sym3([3.0, 1.0, 2.0, 0, 0, 0]) == (3.0, 2.0, 1.0)
+    rng = np.random.default_rng(9)
+    for _ in range(20):
+        s = rng.standard_normal(6)
+        M = np.array([[s[0], s[3], s[5]], [s[3], s[1], s[4]], [s[5], s[4], s[2]]])
+        assert np.allclose(post.eig_sym3(s), np.linalg.eigvalsh(M)[::-1], rtol=0, atol=1e-12)
+
+
+def test_oracle_stress_history_free_expansion(oracle_lib):
+    """A homogeneous free body heated uniformly (du = alpha dT x) carries no stress; its strain is
+    alpha dT on the diagonal (Model.accumulateStep + stateStress, 09-assembly.js:508-571)."""
+    from tmsolve.materials import iso_d
+    from tmsolve.packages import box_package, linspace
+    a = 20e-6
+    pkg = box_package(linspace(0, 2, 4), linspace(0, 1, 3), [0, 0.5, 1.0], [(iso_d(100000.0, 0.3), a, a)],
+                      lambda i, j, k: 0, Ta=25.0, Tb=125.0)
+    om = oracle_lib.OracleModel(pkg)
+    st = pkg.step()
+    om.assemble(st); om.set_sublayers(st)
+    m = pkg.mesh
+    du = (a * 100.0 * m.coords.reshape(-1, 3)).reshape(-1)
+    el = np.arange(m.ne, dtype=np.int32)
+    stride = post.state_stride(st)
+    S = np.zeros(stride * m.ne)
+    om.accumulate_state(du, el, stride, S)
+    eps, sig = om.state_stress(el, S, stride, np.random.default_rng(1).uniform(-1, 1, (m.ne, 3)))
+    assert np.abs(sig).max() <= 1e-12 * 100000.0 * a * 100.0
+    assert np.allclose(eps[:, :3], a * 100.0, rtol=1e-12) and np.abs(eps[:, 3:]).max() <= 1e-15
+
+
+def test_oracle_state_stress_picks_the_sub_layer(oracle_lib):
+    """stateStress reads the sub-layer under the natural point (subLayerAt, 09-assembly.js:547-552)."""
+    from tmsolve.packages import lidded_c2
+    pkg = lidded_c2(n_inplane=8)
+    om = oracle_lib.OracleModel(pkg)
+    st = pkg.step()
+    om.assemble(st); om.set_sublayers(st)
+    stride = post.state_stride(st)
+    m = pkg.mesh
+    p = int(np.argmax(st.sub_n))                 # a layered set with the most sub-layers
+    e = int(np.nonzero(pkg.e_pset == p)[0][0])
+    k = int(m.eIJK[3 * e + 2])
+    off = int(np.sum(st.sub_n[:p])); ns = int(st.sub_n[p])
+    S = np.zeros(stride)
+    for s in range(ns):
+        S[33 + 48 * s + 42:33 + 48 * s + 48] = -(s + 1.0)     # S_th of sub-layer s
+    for s in range(ns):
+        z0, z1 = st.sub_z[2 * (off + s)], st.sub_z[2 * (off + s) + 1]
+        zeta = 2 * (0.5 * (z0 + z1) - m.zs[k]) / (m.zs[k + 1] - m.zs[k]) - 1
+        _, sig = om.state_stress([e], S, stride, [[0.1, -0.2, zeta]])
+        assert np.all(sig == s + 1.0)
