@@ -166,6 +166,11 @@ tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, co
 /* Solves K u = f for the current operator (LinearSolver.solve). The operator is
  * Jacobi-scaled in place on the first solve after an assembly, as in the reference. */
 tm_status tm_solve(tm_ctx* ctx, const double* f, double* u, const tm_solve_opts* opts, tm_solve_info* info);
+/* tm_solve with the displacement returned as float32 (3*nn floats), rounded to nearest on the
+ * device: the step increment as the analysis keeps it (Float32Array.from(du),
+ * src/core/11-analysis.js:256) and as the results file stores it (src/core/16-results-file.js),
+ * with half the device-to-host bytes. */
+tm_status tm_solve_f32(tm_ctx* ctx, const double* f, float* u32, const tm_solve_opts* opts, tm_solve_info* info);
 
 /* y = K x with the current operator (unscaled before the first solve of a step). */
 tm_status tm_matvec(tm_ctx* ctx, const double* x, double* y);

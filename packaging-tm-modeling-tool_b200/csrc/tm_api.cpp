@@ -965,6 +965,27 @@ tm_status tm_solve(tm_ctx* ctx, const double* f, double* u, const tm_solve_opts*
   return g != TM_OK ? g : st;
 }
 
+// tm_solve with the displacement returned as float32, rounded on the device (the solution kept
+// for post-processing and the results file is Float32, 11-analysis.js:256)
+tm_status tm_solve_f32(tm_ctx* ctx, const double* f, float* u32, const tm_solve_opts* opts, tm_solve_info* info) {
+  tm_status st = TM_OK;
+  tm_status g = guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!f || !u32) fail(TM_BAD_INPUT, "null argument");
+    const size_t n = 3 * (size_t)c.nn;
+    tm_solve_opts o;
+    if (opts) o = *opts; else tm_default_solve_opts(&o);
+    c.d_f.upload(f, n, c.stream);
+    c.d_uio.alloc(n);
+    st = solve_impl(c, c.d_f.p, c.d_uio.p, o, info);
+    c.d_u32out.alloc(n);
+    launch_d2f(c, c.d_uio.p, c.d_u32out.p, n);
+    c.d_u32out.download(u32, n, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+  return g != TM_OK ? g : st;
+}
+
 tm_status tm_set_stream(tm_ctx* ctx, void* stream) {
   return guarded([&] {
     Context& c = *reinterpret_cast<Context*>(ctx);

@@ -220,6 +220,7 @@ struct Context {
   DBuf<double> d_subZ, d_subD, d_subS0;
   DBuf<int> d_eIJK;
   DBuf<double> d_zs;
+  DBuf<float> d_u32out;                // float32 copy of a solution (tm_solve_f32)
   DBuf<int> d_conn;                    // 8*ne, uploaded on first use by the DOF-history entry points
   DBuf<double> d_xs, d_ys;             // mesh lines and the node index grid, uploaded on first use
   DBuf<int> d_nodeId;                  // by the plane sampler

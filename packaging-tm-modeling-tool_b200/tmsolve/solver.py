@@ -244,6 +244,20 @@ class DeviceModel:
         rec["u"] = u
         return rec
 
+    def solve_f32(self, f, label=None, key=-1, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64") -> dict:
+        """solve with the displacement returned as float32 (the increment the analysis keeps)."""
+        f = np.ascontiguousarray(f, np.float64)
+        u = np.zeros(self.ndof, np.float32)
+        info = TmSolveInfo()
+        o = self.make_opts(tol, maxit, warm, precond, precision, key)
+        check(load().tm_solve_f32(self.h, f.ctypes.data_as(C.c_void_p), u.ctypes.data_as(C.c_void_p), C.byref(o), C.byref(info)),
+              allow_not_converged=True)
+        rec = self.record(info, label, precond)
+        self.log.append(rec)
+        rec = dict(rec)
+        rec["u"] = u
+        return rec
+
     def solve_device(self, f_ptr: int, u_ptr: int, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64", key=-1) -> dict:
         """The same solve with f and u already in device memory (raw device pointers)."""
         info = TmSolveInfo()

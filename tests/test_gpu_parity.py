@@ -166,3 +166,15 @@ def test_mixed_precision(make, precision):
     assert du <= 1e-5, du
     w64, wmx = rms_warpage(pkg.mesh, r64["u"]), rms_warpage(pkg.mesh, rmx["u"])
     assert abs(wmx / w64 - 1) <= 1e-6
+
+
+def test_solve_f32_output():
+    """tm_solve_f32 returns the same solve rounded to float32 (Float32Array.from(u))."""
+    from tmsolve.solver import DeviceModel
+    pkg = small_box()
+    dm = DeviceModel(pkg)
+    step = pkg.step()
+    u64 = dm.solve(dm.assemble_step(step), tol=1e-10, warm=0, key=1)["u"]
+    r32 = dm.solve_f32(dm.assemble_step(step), tol=1e-10, warm=0, key=2)
+    assert r32["converged"] and r32["u"].dtype == np.float32
+    assert np.array_equal(r32["u"], u64.astype(np.float32))
