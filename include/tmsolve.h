@@ -253,6 +253,18 @@ tm_status tm_sample_plane(tm_ctx* ctx, const double* u, int32_t k, int32_t comp,
 tm_status tm_sample_plane_device(tm_ctx* ctx, const double* u_dev, int32_t k, int32_t comp, int32_t npts,
                                  const double* x_dev, const double* y_dev, double* out_dev);
 
+/* ---- adjoint sensitivities (no counterpart in the reference, whose tornado charts re-run the
+ * analysis per perturbed input, src/core/14-sensitivity.js) ---- */
+/* For the solution u (3*nn, host) of the step assembled last: J = the mean squared residual of
+ * the z displacements of the nodes of mesh plane k about their least-squares plane (a smooth
+ * warpage measure), and per property set m its relative sensitivities dlogE[m] = dJ/dlog(E_m)
+ * (the set's stiffness scaled, its thermal load with it) and dlogA[m] = dJ/dlog(alpha_m) (the
+ * set's thermal strain scaled), from one adjoint solve K lambda = dJ/du with the solver and
+ * preconditioner of tm_solve (opts as there; no warm start) and element sums. A material shared
+ * by several sets has the sum over them. */
+tm_status tm_warpage_sensitivity(tm_ctx* ctx, const double* u, int32_t k, const tm_solve_opts* opts, double* J, double* dlogE,
+                                 double* dlogA, tm_solve_info* info);
+
 /* Runs the context's work on the caller's CUDA stream (a cudaStream_t) instead of its own
  * (the N-API addon passes the stream of the thread's device context). */
 tm_status tm_set_stream(tm_ctx* ctx, void* stream);

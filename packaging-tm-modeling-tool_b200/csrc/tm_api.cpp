@@ -986,6 +986,63 @@ tm_status tm_solve_f32(tm_ctx* ctx, const double* f, float* u32, const tm_solve_
   return g != TM_OK ? g : st;
 }
 
+// adjoint sensitivities of the smooth warpage measure J = mean over the nodes of plane k of the
+// squared residual of their z displacement about its least-squares plane (fitPlane,
+// 01-util.js:176-190): dJ/du = 2 r / N on those z DOFs; K lambda = dJ/du by the same solver
+// (free DOFs); per property set m, with K_m and f_m the set's share of the assembled operator and
+// load, dJ/dlog(E_m) = lambda^T (f_m - K_m u) (K_m and f_m scale with the set's stiffness) and
+// dJ/dlog(alpha_m) = lambda^T f_m (f_m scales with its thermal strain)
+tm_status tm_warpage_sensitivity(tm_ctx* ctx, const double* u, int32_t k, const tm_solve_opts* opts, double* J, double* dlogE,
+                                 double* dlogA, tm_solve_info* info) {
+  tm_status st = TM_OK;
+  tm_status g = guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!u || !J || !dlogE || !dlogA) fail(TM_BAD_INPUT, "null argument");
+    if (!c.assembled || !c.stepReady || !c.d_clsKc.p) fail(TM_BAD_INPUT, "sensitivities need a step assembled by tm_assemble_step");
+    if (k < 0 || k >= c.nz) fail(TM_BAD_INPUT, "plane index out of range");
+    const size_t n = 3 * (size_t)c.nn;
+    // the plane's nodes, the fitted plane and the measure's gradient
+    std::vector<int> nodes;
+    for (int q = 0; q < c.nn; q++) if (c.nodeIJK[3 * (size_t)q + 2] == k) nodes.push_back(q);
+    const int N = (int)nodes.size();
+    if (N < 3) fail(TM_BAD_INPUT, "plane with fewer than 3 nodes");
+    double sx = 0, sy = 0, sw = 0;
+    for (int q : nodes) { sx += c.xs[c.nodeIJK[3 * (size_t)q]]; sy += c.ys[c.nodeIJK[3 * (size_t)q + 1]]; sw += u[3 * (size_t)q + 2]; }
+    const double mx = sx / N, my = sy / N, mw = sw / N;
+    double sxx = 0, sxy = 0, syy = 0, sxw = 0, syw = 0;
+    for (int q : nodes) {
+      const double dx = c.xs[c.nodeIJK[3 * (size_t)q]] - mx, dy = c.ys[c.nodeIJK[3 * (size_t)q + 1]] - my, dw = u[3 * (size_t)q + 2] - mw;
+      sxx += dx * dx; sxy += dx * dy; syy += dy * dy; sxw += dx * dw; syw += dy * dw;
+    }
+    const double det = sxx * syy - sxy * sxy;
+    double c1 = 0, c2 = 0;
+    if (std::fabs(det) > 1e-300) { c1 = (sxw * syy - syw * sxy) / det; c2 = (syw * sxx - sxw * sxy) / det; }
+    const double c0 = mw - c1 * mx - c2 * my;
+    std::vector<double> gr(n, 0.0);
+    double Jv = 0;
+    for (int q : nodes) {
+      const double r = u[3 * (size_t)q + 2] - (c0 + c1 * c.xs[c.nodeIJK[3 * (size_t)q]] + c2 * c.ys[c.nodeIJK[3 * (size_t)q + 1]]);
+      Jv += r * r;
+      gr[3 * (size_t)q + 2] = 2 * r / N;
+    }
+    *J = Jv / N;
+    // the adjoint solve (no warm start, nothing stored)
+    tm_solve_opts o;
+    if (opts) o = *opts; else tm_default_solve_opts(&o);
+    o.warm = 0;
+    c.d_f.upload(gr.data(), n, c.stream);
+    launch_zero_constrained(c, c.d_f.p);
+    c.d_sensLam.alloc(n);
+    st = solve_impl(c, c.d_f.p, c.d_sensLam.p, o, info);
+    c.d_sensU.upload(u, n, c.stream);
+    if (!c.d_conn.p) c.d_conn.upload(c.conn, c.stream);
+    std::vector<double> sums(2 * (size_t)c.npset);
+    launch_sens(c, c.d_sensU.p, c.d_sensLam.p, sums.data());
+    for (int p = 0; p < c.npset; p++) { dlogE[p] = sums[2 * p + 1] - sums[2 * p]; dlogA[p] = sums[2 * p + 1]; }
+  });
+  return g != TM_OK ? g : st;
+}
+
 tm_status tm_set_stream(tm_ctx* ctx, void* stream) {
   return guarded([&] {
     Context& c = *reinterpret_cast<Context*>(ctx);

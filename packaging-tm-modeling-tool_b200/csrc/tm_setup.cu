@@ -735,6 +735,67 @@ __global__ void k_state_stress(int np, int ne, const int* __restrict__ elem, con
   }
 }
 
+// ---- adjoint sensitivities of a warpage measure -------------------------------------------------
+// per element e (warp per element): with s_e its assembly scale (eScale, 1e-6 before its stage),
+// out[2e] = s_e lambda_e^T Kc u_e and out[2e+1] = s_e lambda_e^T fc, from the condensed class
+// matrix and load of the step assembled last (lanes over the 24 rows, fixed-order warp sum)
+__global__ void k_sens_elements(int ne, const int* __restrict__ conn, const int* __restrict__ eClass, const double* __restrict__ eScale,
+                                const int* __restrict__ eGroup, const int* __restrict__ groupStage, int stage,
+                                const double* __restrict__ clsKc, const double* __restrict__ clsFc, const double* __restrict__ u,
+                                const double* __restrict__ lam, double* __restrict__ out) {
+  __shared__ double su[4][24];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * 4 + warp;
+  if (e >= ne) return;
+  const int cls = eClass[e];
+  double lk = 0;
+  if (lane < 24) {
+    const size_t dof = 3 * (size_t)conn[8 * (size_t)e + lane / 3] + lane % 3;
+    su[warp][lane] = u[dof];
+    lk = lam[dof];
+  }
+  __syncwarp();
+  double t1 = 0, t2 = 0;
+  if (lane < 24) {
+    const double* K = clsKc + 576 * (size_t)cls + 24 * lane;
+    double ku = 0;
+    for (int b = 0; b < 24; b++) ku += K[b] * su[warp][b];
+    t1 = lk * ku;
+    t2 = lk * clsFc[24 * (size_t)cls + lane];
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    t1 += __shfl_xor_sync(0xffffffffu, t1, off);
+    t2 += __shfl_xor_sync(0xffffffffu, t2, off);
+  }
+  if (lane == 0) {
+    const double sc = eScale[e] * (groupStage[eGroup[e]] <= stage ? 1.0 : 1e-6);
+    out[2 * (size_t)e] = sc * t1;
+    out[2 * (size_t)e + 1] = sc * t2;
+  }
+}
+
+// per property set sums of the element terms, in a fixed order: block b sums elements
+// b*chunk .. (b+1)*chunk-1 per set (thread-strided, then a tree per set), one partial per block
+constexpr int SENS_MAXSET = 64;
+__global__ void __launch_bounds__(256) k_sens_partial(int ne, int chunk, const int* __restrict__ eClass, const int* __restrict__ clsPset,
+                                                      int npset, const double* __restrict__ et, double* __restrict__ part) {
+  __shared__ double s1[256], s2[256];
+  const int e0 = blockIdx.x * chunk, e1 = min(ne, e0 + chunk);
+  for (int p = 0; p < npset; p++) {
+    double a = 0, b = 0;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x)
+      if (clsPset[eClass[e]] == p) { a += et[2 * (size_t)e]; b += et[2 * (size_t)e + 1]; }
+    s1[threadIdx.x] = a; s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+      if ((int)threadIdx.x < h) { s1[threadIdx.x] += s1[threadIdx.x + h]; s2[threadIdx.x] += s2[threadIdx.x + h]; }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[2 * ((size_t)blockIdx.x * npset + p)] = s1[0]; part[2 * ((size_t)blockIdx.x * npset + p) + 1] = s2[0]; }
+    __syncthreads();
+  }
+}
+
 // boxStrainAt (07-element.js:127-142) with boxDerivs (:19-30), thread per point: engineering
 // strain of element elem[t] with DOFs q[33 t ..] at the natural point nat[3 t ..]
 __global__ void k_element_strains(int np, int ne, const int* __restrict__ elem, const int* __restrict__ eClass,
@@ -995,6 +1056,30 @@ void launch_state_stress(Context& c, int np, const int* elem, const double* stat
   k_state_stress<<<grid_for(np, 128), 128, 0, c.stream>>>(np, c.ne, elem, c.d_eClass.p, c.d_clsPset.p, c.d_clsH.p, c.d_eIJK.p, c.d_zs.p,
                                                          c.d_psetLayered.p, c.d_subOff.p, c.d_subZ.p, state, stride, nat, eps, sig);
   TM_CUDA_CHECK(cudaGetLastError());
+}
+
+// the element terms of the warpage sensitivities summed per property set: out[2p] = sum over the
+// set's elements of s_e lambda^T K_e u, out[2p+1] = sum of s_e lambda^T f_e
+void launch_sens(Context& c, const double* u, const double* lam, double* outHost) {
+  if (c.npset > SENS_MAXSET) fail(TM_BAD_INPUT, "sensitivities: too many property sets");
+  DBuf<double> et, part;
+  et.alloc(2 * (size_t)c.ne);
+  const int chunk = 4096, nbk = (c.ne + chunk - 1) / chunk;
+  part.alloc(2 * (size_t)nbk * c.npset);
+  note_launch(2);
+  k_sens_elements<<<(c.ne + 3) / 4, 128, 0, c.stream>>>(c.ne, c.d_conn.p, c.d_eClass.p, c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage,
+                                                       c.d_clsKc.p, c.d_clsFc.p, u, lam, et.p);
+  k_sens_partial<<<nbk, 256, 0, c.stream>>>(c.ne, chunk, c.d_eClass.p, c.d_clsPset.p, c.npset, et.p, part.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+  std::vector<double> h(2 * (size_t)nbk * c.npset);
+  part.download(h.data(), h.size(), c.stream);
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  for (int p = 0; p < 2 * c.npset; p++) outHost[p] = 0;
+  for (int b = 0; b < nbk; b++)
+    for (int p = 0; p < c.npset; p++) {
+      outHost[2 * p] += h[2 * ((size_t)b * c.npset + p)];
+      outHost[2 * p + 1] += h[2 * ((size_t)b * c.npset + p) + 1];
+    }
 }
 
 }  // namespace tmg

@@ -258,6 +258,20 @@ class DeviceModel:
         rec["u"] = u
         return rec
 
+    def warpage_sensitivity(self, u, k: int = 0, tol=1e-12, maxit=2000, precond="mg") -> dict:
+        """Adjoint sensitivities of J = mean squared residual of plane k's z displacements about
+        their least-squares plane, for the solution u of the step assembled last: J and, per
+        property set, dJ/dlog(E) and dJ/dlog(alpha) (tm_warpage_sensitivity)."""
+        u = np.ascontiguousarray(u, np.float64)
+        J = C.c_double()
+        dE = np.zeros(self.pkg.npset); dA = np.zeros(self.pkg.npset)
+        info = TmSolveInfo()
+        o = self.make_opts(tol, maxit, 0, precond, "fp64", -1)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(load().tm_warpage_sensitivity(self.h, vp(u), int(k), C.byref(o), C.byref(J), vp(dE), vp(dA), C.byref(info)),
+              allow_not_converged=True)
+        return dict(J=J.value, dlogE=dE, dlogA=dA, adjoint=self.record(info, "adjoint", precond))
+
     def solve_device(self, f_ptr: int, u_ptr: int, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64", key=-1) -> dict:
         """The same solve with f and u already in device memory (raw device pointers)."""
         info = TmSolveInfo()
