@@ -264,6 +264,13 @@ tm_status tm_sample_plane_device(tm_ctx* ctx, const double* u_dev, int32_t k, in
  * by several sets has the sum over them. */
 tm_status tm_warpage_sensitivity(tm_ctx* ctx, const double* u, int32_t k, const tm_solve_opts* opts, double* J, double* dlogE,
                                  double* dlogA, tm_solve_info* info);
+/* After tm_warpage_sensitivity: dJ/dt_m per property set for one parameter t_m per set, whose
+ * effect on the step's set data is given by dir (per set the derivatives of D and s0, or of W
+ * and V for layered sets, with respect to t_m; NULL arrays are zero), e.g. a Poisson ratio's
+ * dD/dnu and ds0/dnu. base is the step assembled last. The condensed element matrices are
+ * differentiated by central differences of two condensations (relative step 1e-6), the rest
+ * from the stored adjoint; the step's own element data are restored afterwards. */
+tm_status tm_sensitivity_direction(tm_ctx* ctx, const tm_step* base, const tm_step* dir, double* dJ);
 
 /* Runs the context's work on the caller's CUDA stream (a cudaStream_t) instead of its own
  * (the N-API addon passes the stream of the thread's device context). */

@@ -1039,8 +1039,19 @@ tm_status tm_warpage_sensitivity(tm_ctx* ctx, const double* u, int32_t k, const 
     std::vector<double> sums(2 * (size_t)c.npset);
     launch_sens(c, c.d_sensU.p, c.d_sensLam.p, sums.data());
     for (int p = 0; p < c.npset; p++) { dlogE[p] = sums[2 * p + 1] - sums[2 * p]; dlogA[p] = sums[2 * p + 1]; }
+    c.sensReady = true;
   });
   return g != TM_OK ? g : st;
+}
+
+tm_status tm_sensitivity_direction(tm_ctx* ctx, const tm_step* base, const tm_step* dir, double* dJ) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!base || !dir || !dJ) fail(TM_BAD_INPUT, "null argument");
+    if (!c.sensReady) fail(TM_BAD_INPUT, "tm_sensitivity_direction after tm_warpage_sensitivity");
+    check_step(c, *base);
+    sens_direction(c, *base, *dir, c.d_sensU.p, c.d_sensLam.p, dJ);
+  });
 }
 
 tm_status tm_set_stream(tm_ctx* ctx, void* stream) {

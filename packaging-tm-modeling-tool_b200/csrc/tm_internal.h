@@ -222,6 +222,7 @@ struct Context {
   DBuf<double> d_zs;
   DBuf<float> d_u32out;                // float32 copy of a solution (tm_solve_f32)
   DBuf<double> d_sensU, d_sensLam;     // solution and adjoint of tm_warpage_sensitivity
+  bool sensReady = false;
   DBuf<int> d_conn;                    // 8*ne, uploaded on first use by the DOF-history entry points
   DBuf<double> d_xs, d_ys;             // mesh lines and the node index grid, uploaded on first use
   DBuf<int> d_nodeId;                  // by the plane sampler
@@ -324,6 +325,7 @@ void launch_element_strains(Context& c, int np, const int* elem, const double* q
 void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts, const double* x, const double* y, double* out);
 void launch_accumulate_state(Context& c, const double* du, int nel, const int* elems, int stride, double* state);
 void launch_sens(Context& c, const double* u, const double* lam, double* outHost);
+void sens_direction(Context& c, const tm_step& base, const tm_step& dir, const double* u, const double* lam, double* dJ);
 void launch_state_stress(Context& c, int np, const int* elem, const double* state, int stride, const double* nat, double* eps,
                          double* sig);
 

@@ -242,6 +242,100 @@ __global__ void k_class_condense(int ncls, const int* __restrict__ clsPset, cons
   }
 }
 
+// directional derivative of the condensation, one warp per class: with K the class's K33, dK its
+// derivative along the direction (the same shape-matrix sum over the direction's data), and
+// X = Kaa^-1 Kau, y = Kaa^-1 fa: dKc = dKuu - dKua X - X^T dKau + X^T dKaa X and
+// dfc = dfu - dKua y - X^T dfa + X^T dKaa y, then the exact symmetry of Kc
+__global__ void k_class_dcondense(int ncls, const int* __restrict__ clsPset, const double* __restrict__ clsH,
+                                  const double* __restrict__ psetM, const double* __restrict__ psetdM, const double* __restrict__ clsF33,
+                                  const double* __restrict__ clsdF33, const int* __restrict__ clsBorn, double* __restrict__ dKc,
+                                  double* __restrict__ dFc) {
+  extern __shared__ double smd[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cls = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (cls >= ncls) return;
+  double* K = smd + warp * 2560;       // 1089
+  double* dK = K + 1089;               // 1089
+  double* Kaa = dK + 1089;             // 81
+  double* X = Kaa + 81;                // 216 (9 x 24)
+  double* y = X + 216;                 // 9
+  double* t = y + 9;                   // 24
+  const double hx = clsH[3 * cls], hy = clsH[3 * cls + 1], hz = clsH[3 * cls + 2];
+  const double V8 = hx * hy * hz / 8;
+  const double c0 = V8 * 4 / (hx * hx), c1 = V8 * 4 / (hy * hy), c2 = V8 * 4 / (hz * hz);
+  const double c3 = V8 * 4 / (hx * hy), c4 = V8 * 4 / (hy * hz), c5 = V8 * 4 / (hz * hx);
+  const double* M = psetM + (size_t)clsPset[cls] * 6 * 1089;
+  const double* dM = psetdM + (size_t)clsPset[cls] * 6 * 1089;
+  for (int o = lane; o < 1089; o += 32) {
+    const int i = o / 33, j = o % 33;
+    if (j >= i) {
+      K[o] = c0 * M[o] + c1 * M[1089 + o] + c2 * M[2178 + o] + c3 * M[3267 + o] + c4 * M[4356 + o] + c5 * M[5445 + o];
+      dK[o] = c0 * dM[o] + c1 * dM[1089 + o] + c2 * dM[2178 + o] + c3 * dM[3267 + o] + c4 * dM[4356 + o] + c5 * dM[5445 + o];
+    }
+  }
+  __syncwarp();
+  for (int o = lane; o < 1089; o += 32) {
+    const int i = o / 33, j = o % 33;
+    if (j < i) { K[o] = K[j * 33 + i]; dK[o] = dK[j * 33 + i]; }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    for (int i = 0; i < 9; i++)
+      for (int j = 0; j < 9; j++) Kaa[i * 9 + j] = K[(24 + i) * 33 + 24 + j];
+    chol_dense9(Kaa, 1e-14);
+  }
+  __syncwarp();
+  if (lane < 24) {
+    double col[9];
+    for (int i = 0; i < 9; i++) col[i] = K[(24 + i) * 33 + lane];
+    chol_solve9(Kaa, col);
+    for (int i = 0; i < 9; i++) X[i * 24 + lane] = col[i];
+  }
+  const bool born = clsBorn[cls] != 0;
+  const double* f = clsF33 + (size_t)cls * 33;
+  const double* df = clsdF33 + (size_t)cls * 33;
+  if (lane == 0) {
+    for (int i = 0; i < 9; i++) y[i] = born ? f[24 + i] : 0.0;
+    chol_solve9(Kaa, y);
+  }
+  __syncwarp();
+  // dKc = dKuu - dKua X - X^T dKau + X^T dKaa X
+  double* out = dKc + (size_t)cls * 576;
+  for (int e = lane; e < 576; e += 32) {
+    const int i = e / 24, j = e % 24;
+    double v = dK[i * 33 + j];
+    for (int q = 0; q < 9; q++) v -= dK[i * 33 + 24 + q] * X[q * 24 + j] + X[q * 24 + i] * dK[(24 + q) * 33 + j];
+    for (int q = 0; q < 9; q++) {
+      double s2 = 0;
+      for (int r = 0; r < 9; r++) s2 += dK[(24 + q) * 33 + 24 + r] * X[r * 24 + j];
+      v += X[q * 24 + i] * s2;
+    }
+    out[e] = v;
+  }
+  __syncwarp();
+  for (int e = lane; e < 576; e += 32) {
+    const int i = e / 24, j = e % 24;
+    if (j > i) {
+      const double v = 0.5 * (out[i * 24 + j] + out[j * 24 + i]);
+      out[i * 24 + j] = v;
+      out[j * 24 + i] = v;
+    }
+  }
+  // dfc = dfu - dKua y - X^T dfa + X^T dKaa y
+  if (lane < 9) {
+    double s2 = 0;
+    for (int r = 0; r < 9; r++) s2 += dK[(24 + lane) * 33 + 24 + r] * y[r];
+    t[lane] = s2 - (born ? df[24 + lane] : 0.0);   // dKaa y - dfa
+  }
+  __syncwarp();
+  if (lane < 24) {
+    double v = born ? df[lane] : 0.0;
+    for (int q = 0; q < 9; q++) v -= dK[lane * 33 + 24 + q] * y[q];
+    for (int q = 0; q < 9; q++) v += X[q * 24 + lane] * t[q];
+    dFc[(size_t)cls * 24 + lane] = v;
+  }
+}
+
 __device__ __forceinline__ int loc_index(int a, int b, int c) {
   // local node order loc of 06-mesher.js:49 -> index
   return c * 4 + (b ? (a ? 2 : 3) : (a ? 1 : 0));
@@ -1058,9 +1152,8 @@ void launch_state_stress(Context& c, int np, const int* elem, const double* stat
   TM_CUDA_CHECK(cudaGetLastError());
 }
 
-// the element terms of the warpage sensitivities summed per property set: out[2p] = sum over the
-// set's elements of s_e lambda^T K_e u, out[2p+1] = sum of s_e lambda^T f_e
-void launch_sens(Context& c, const double* u, const double* lam, double* outHost) {
+namespace {
+void sens_sums(Context& c, const double* u, const double* lam, const double* Kc, const double* Fc, double* outHost) {
   if (c.npset > SENS_MAXSET) fail(TM_BAD_INPUT, "sensitivities: too many property sets");
   DBuf<double> et, part;
   et.alloc(2 * (size_t)c.ne);
@@ -1068,7 +1161,7 @@ void launch_sens(Context& c, const double* u, const double* lam, double* outHost
   part.alloc(2 * (size_t)nbk * c.npset);
   note_launch(2);
   k_sens_elements<<<(c.ne + 3) / 4, 128, 0, c.stream>>>(c.ne, c.d_conn.p, c.d_eClass.p, c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage,
-                                                       c.d_clsKc.p, c.d_clsFc.p, u, lam, et.p);
+                                                       Kc, Fc, u, lam, et.p);
   k_sens_partial<<<nbk, 256, 0, c.stream>>>(c.ne, chunk, c.d_eClass.p, c.d_clsPset.p, c.npset, et.p, part.p);
   TM_CUDA_CHECK(cudaGetLastError());
   std::vector<double> h(2 * (size_t)nbk * c.npset);
@@ -1080,6 +1173,57 @@ void launch_sens(Context& c, const double* u, const double* lam, double* outHost
       outHost[2 * p] += h[2 * ((size_t)b * c.npset + p)];
       outHost[2 * p + 1] += h[2 * ((size_t)b * c.npset + p) + 1];
     }
+}
+}  // namespace
+
+// directional sensitivities: per set a parameter t_m whose derivative of the set data (D, s0 or
+// W, V) is dir; the shape matrices and element thermal loads are linear in those data, so their
+// derivatives are the same maps applied to dir, and the condensation is differentiated exactly
+// (k_class_dcondense); dJ/dt_m = lambda^T (df_m - dK_m u) summed over the set's elements. The base
+// step's data are loaded again first (the class data of the step assembled last).
+void sens_direction(Context& c, const tm_step& base, const tm_step& dir, const double* u, const double* lam, double* dJ) {
+  const bool subWas = c.subReady;
+  launch_shape_matrices(c, base);
+  c.subReady = subWas;
+  const int np = c.npset;
+  std::vector<double> dMh((size_t)np * 6 * 1089), dF33((size_t)c.ncls * 33, 0.0);
+  std::vector<double> zero108(108, 0.0), zero36(36, 0.0), zero18(18, 0.0), zero6(6, 0.0);
+  for (int p = 0; p < np; p++) {
+    const bool lay = base.psetLayered[p] != 0;
+    const double* W = dir.W ? dir.W + 108 * (size_t)p : zero108.data();
+    const double* D = dir.D ? dir.D + 36 * (size_t)p : zero36.data();
+    shape_matrices(lay ? W : nullptr, lay ? nullptr : D, dMh.data() + (size_t)p * 6 * 1089);
+  }
+  for (int k = 0; k < c.ncls; k++) {
+    const int p = c.clsPset[k];
+    if (!base.psetBorn[p]) continue;
+    const bool lay = base.psetLayered[p] != 0;
+    const double* V = dir.V ? dir.V + 18 * (size_t)p : zero18.data();
+    const double* S = dir.s0 ? dir.s0 + 6 * (size_t)p : zero6.data();
+    element_fth(c.clsH[3 * k], c.clsH[3 * k + 1], c.clsH[3 * k + 2], lay ? V : nullptr, lay ? nullptr : S, dF33.data() + 33 * (size_t)k);
+  }
+  DBuf<double> dM, dF, dKc, dFc;
+  dM.upload(dMh, c.stream);
+  dF.upload(dF33, c.stream);
+  dKc.alloc((size_t)c.ncls * 576);
+  dFc.alloc((size_t)c.ncls * 24);
+  const int warps = 2;
+  const size_t smem = (size_t)warps * 2560 * sizeof(double);
+  TM_CUDA_CHECK(cudaFuncSetAttribute(k_class_dcondense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  note_launch();
+  k_class_dcondense<<<grid_for(c.ncls, warps), 32 * warps, smem, c.stream>>>(c.ncls, c.d_clsPset.p, c.d_clsH.p, c.d_psetM.p, dM.p,
+                                                                            c.d_clsF33.p, dF.p, c.d_clsBorn.p, dKc.p, dFc.p);
+  TM_CUDA_CHECK(cudaGetLastError());
+  std::vector<double> sums(2 * (size_t)np);
+  sens_sums(c, u, lam, dKc.p, dFc.p, sums.data());
+  for (int p = 0; p < np; p++) dJ[p] = sums[2 * p + 1] - sums[2 * p];
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+}
+
+// the element terms of the warpage sensitivities summed per property set: out[2p] = sum over the
+// set's elements of s_e lambda^T K_e u, out[2p+1] = sum of s_e lambda^T f_e
+void launch_sens(Context& c, const double* u, const double* lam, double* outHost) {
+  sens_sums(c, u, lam, c.d_clsKc.p, c.d_clsFc.p, outHost);
 }
 
 }  // namespace tmg

@@ -25,7 +25,7 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_submodel_create", "tm_submodel_destroy", "tm_submodel_sizes", "tm_submodel_step", "tm_submodel_get",
             "tm_submodel_run", "tm_submodel_run_batch", "tm_set_sublayers", "tm_accumulate_state",
             "tm_accumulate_state_device", "tm_state_stress", "tm_state_stress_device", "tm_solve_f32",
-            "tm_warpage_sensitivity"]
+            "tm_warpage_sensitivity", "tm_sensitivity_direction"]
 PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
 PRECOND_NAMES = {v: k for k, v in PRECONDS.items()}
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
@@ -103,6 +103,7 @@ def load():
     L.tm_solve.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
     L.tm_solve_device.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
     L.tm_solve_f32.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), C.POINTER(TmSolveInfo)]
+    L.tm_sensitivity_direction.argtypes = [vp, C.POINTER(TmStep), C.POINTER(TmStep), vp]
     L.tm_warpage_sensitivity.argtypes = [vp, vp, C.c_int32, C.POINTER(TmSolveOpts), vp, vp, vp, C.POINTER(TmSolveInfo)]
     L.tm_matvec.argtypes = [vp, vp, vp]
     L.tm_matvec_device.argtypes = [vp, vp, vp]

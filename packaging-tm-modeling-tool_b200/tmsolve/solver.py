@@ -272,6 +272,15 @@ class DeviceModel:
               allow_not_converged=True)
         return dict(J=J.value, dlogE=dE, dlogA=dA, adjoint=self.record(info, "adjoint", precond))
 
+    def sensitivity_direction(self, base: StepData, direction: StepData) -> np.ndarray:
+        """After warpage_sensitivity: dJ/dt per property set for the parameter whose derivative of
+        the set data (D, s0 or W, V) is `direction` (tm_sensitivity_direction)."""
+        sb, kb = self._step_struct(base)
+        sd, kd = self._step_struct(direction)
+        out = np.zeros(self.pkg.npset)
+        check(load().tm_sensitivity_direction(self.h, C.byref(sb), C.byref(sd), out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def solve_device(self, f_ptr: int, u_ptr: int, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64", key=-1) -> dict:
         """The same solve with f and u already in device memory (raw device pointers)."""
         info = TmSolveInfo()

@@ -62,3 +62,52 @@ def test_adjoint_matches_central_differences(make):
                 Js.append(warpage_measure(pkg.mesh, rr["u"]))
             fd = (Js[0] - Js[1]) / (np.log(1 + h) - np.log(1 - h))
             assert abs(g[p] - fd) <= 1e-4 * abs(fd), (kind, p, g[p], fd)
+
+
+def test_direction_sensitivities_stiffness_and_poisson():
+    """tm_sensitivity_direction: along the sets' own data it reproduces dJ/dlog(E); along dD/dnu
+    (isotropic and column stiffnesses of the homogeneous package) it matches central differences
+    of re-solves in nu."""
+    from tmsolve.materials import column_d, iso_d, thermal_stress_const
+    from tmsolve.packages import StepData
+    from tmsolve.solver import DeviceModel
+    pkg = fcbga_c1()
+    dm = DeviceModel(pkg)
+    step = pkg.step()
+    r = dm.solve(dm.assemble_step(step), tol=1e-12, warm=0, key=0)
+    s = dm.warpage_sensitivity(r["u"], 0, tol=1e-12)
+    same = dm.sensitivity_direction(step, step)
+    assert np.allclose(same, s["dlogE"], rtol=1e-6, atol=1e-9 * np.abs(s["dlogE"]).max())
+    # the package's sets: (kind, E, nu, alpha) as fcbga_c1 builds them
+    mats = [("iso", 25000.0, 0.3, 15e-6), ("col", 40000.0, 0.4, 22.5e-6), ("iso", 8000.0, 0.35, 30e-6), ("iso", 130000.0, 0.28, 2.6e-6)]
+    Dof = lambda kind, E, nu: iso_d(E, nu) if kind == "iso" else column_d(E, nu)
+    Ta, Tb = pkg.Ta, pkg.Tb
+
+    def step_with(nus):
+        D = np.concatenate([Dof(k, E, nu) for (k, E, _, _), nu in zip(mats, nus)])
+        s0 = np.concatenate([thermal_stress_const(Dof(k, E, nu), a, a, Ta, Tb) for (k, E, _, a), nu in zip(mats, nus)])
+        return StepData(layered=step.layered, D=D, s0=s0, W=step.W, V=step.V, born=step.born, stage=step.stage)
+    nus = [m[2] for m in mats]
+    d = 1e-7
+    dD = [(Dof(k, E, nu + d) - Dof(k, E, nu - d)) / (2 * d) for (k, E, nu, _) in mats]
+    direction = StepData(layered=step.layered, D=np.concatenate(dD),
+                         s0=np.concatenate([thermal_stress_const(x, a, a, Ta, Tb) for x, (_, _, _, a) in zip(dD, mats)]),
+                         W=np.zeros_like(step.W), V=np.zeros_like(step.V), born=step.born, stage=step.stage)
+    base = step_with(nus)
+    assert np.allclose(base.D, step.D, rtol=1e-14, atol=0)
+    r = dm.solve(dm.assemble_step(base), tol=1e-12, warm=0, key=1)
+    dm.warpage_sensitivity(r["u"], 0, tol=1e-12)
+    g = dm.sensitivity_direction(base, direction)
+    h = 1e-3
+    key = 2
+    for p in range(len(mats)):
+        if abs(g[p]) < 1e-3 * np.abs(g).max():
+            continue
+        Js = []
+        for sg in (1, -1):
+            nn = list(nus); nn[p] += sg * h
+            rr = dm.solve(dm.assemble_step(step_with(nn)), tol=1e-12, warm=0, key=key)
+            key += 1
+            Js.append(warpage_measure(pkg.mesh, rr["u"]))
+        fd = (Js[0] - Js[1]) / (2 * h)
+        assert abs(g[p] - fd) <= 1e-4 * abs(fd), (p, g[p], fd)
