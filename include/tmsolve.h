@@ -195,6 +195,19 @@ tm_status tm_matvec_device(tm_ctx* ctx, const double* x_dev, double* y_dev);
  * reference's pc.apply(r, z), e.g. ICPC.apply, src/core/10-solver.js:784-798). */
 tm_status tm_pc_apply(tm_ctx* ctx, const double* r, double* z);
 tm_status tm_pc_apply_device(tm_ctx* ctx, const double* r_dev, double* z_dev);
+/* Launch shapes the FP32 V-cycle's autotuner chose for the current hierarchy (no counterpart in
+ * the reference, whose cycle runs on one thread): per shell level (fine to coarse) smoothed by column
+ * sweeps, the warps per block of the sweep and of the residual kernel (2, 4 or 8; up to cap
+ * levels written, *nlevels = all), and the stage count of the TMA level-0 sweep (0: not used).
+ * TM_BAD_INPUT before a mixed-precision solve has run on this hierarchy. */
+tm_status tm_vcycle_shapes(tm_ctx* ctx, int cap, int* nlevels, int* wpb_sweep, int* wpb_apply, int* tma_stages);
+/* Fixes the FP32 V-cycle's launch shapes instead of timing them (e.g. shapes read back with
+ * tm_vcycle_shapes on an earlier context of the same mesh): per swept shell level, fine to coarse
+ * as tm_vcycle_shapes lists them, warps per block 2, 4 or 8 (levels beyond nlevels get 4);
+ * tma_stages 2 or 3, or 0 for the planner's count (a count that does not fit falls back to it).
+ * nlevels < 0 returns to autotuning. Takes effect at the next FP32 V-cycle; the shapes change
+ * no arithmetic. */
+tm_status tm_set_vcycle_shapes(tm_ctx* ctx, int nlevels, const int* wpb_sweep, const int* wpb_apply, int tma_stages);
 
 /* ---- element DOF histories at screening sites ---- */
 /* Loads the per-step data that the DOF histories read (the shape matrices of every property set

@@ -47,8 +47,6 @@ Context::~Context() {
 
 namespace {
 
-void check_device_error(Context& c);
-
 double now_ms() {
   using namespace std::chrono;
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
@@ -396,9 +394,17 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   if (!c.pcReady || c.needRebuild) {
     pcMs = build_pc(c, kind);
     rebuilt = true;
-    if (mixed) { const double t1 = now_ms(); launch_to_fp32(c); TM_CUDA_CHECK(cudaStreamSynchronize(c.stream)); pcMs += now_ms() - t1; c.fp32Ready = true; }
+    if (mixed) {
+      const double t1 = now_ms();
+      launch_to_fp32(c);
+      autotune_vcycle32(c);
+      TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+      pcMs += now_ms() - t1;
+      c.fp32Ready = true;
+    }
   } else if (mixed && !c.fp32Ready) {
     launch_to_fp32(c);
+    autotune_vcycle32(c);
     c.fp32Ready = true;
   }
   warm_start(c, c.d_bs.p, c.d_x.p);
@@ -497,6 +503,8 @@ void upload_mesh(Context& c) {
   c.d_err.zero(s);
 }
 
+}  // namespace
+
 // a bounded device wait that ran out (the results of the solve are invalid)
 void check_device_error(Context& c) {
   int err = 0;
@@ -509,7 +517,6 @@ void check_device_error(Context& c) {
   }
 }
 
-}  // namespace
 }  // namespace tmg
 
 using namespace tmg;
@@ -919,6 +926,44 @@ tm_status tm_pc_apply_device(tm_ctx* ctx, const double* r, double* z) {
     c.mgFp32 = false;
     precondition(c, c.pcKind, r, z);
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_set_vcycle_shapes(tm_ctx* ctx, int nlevels, const int* wpb_sweep, const int* wpb_apply, int tma_stages) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    auto okw = [](int w) { return w == 2 || w == 4 || w == 8; };
+    if (nlevels < 0) {
+      c.shapesPinned = false;
+    } else {
+      if (nlevels > 0 && (!wpb_sweep || !wpb_apply)) fail(TM_BAD_INPUT, "tm_set_vcycle_shapes: missing per-level arrays");
+      if (tma_stages != 0 && tma_stages != 2 && tma_stages != 3) fail(TM_BAD_INPUT, "tm_set_vcycle_shapes: TMA stages must be 0, 2 or 3");
+      for (int k = 0; k < nlevels; k++)
+        if (!okw(wpb_sweep[k]) || !okw(wpb_apply[k])) fail(TM_BAD_INPUT, "tm_set_vcycle_shapes: warps per block must be 2, 4 or 8");
+      c.pinSweep.assign(wpb_sweep, wpb_sweep + nlevels);
+      c.pinApply.assign(wpb_apply, wpb_apply + nlevels);
+      c.pinStages = tma_stages;
+      c.shapesPinned = true;
+    }
+    c.tunedEpoch = -1;   // applied (or tuned again) before the next FP32 V-cycle
+  });
+}
+
+tm_status tm_vcycle_shapes(tm_ctx* ctx, int cap, int* nlevels, int* wpb_sweep, int* wpb_apply, int* tma_stages) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (c.tunedEpoch != c.structEpoch) fail(TM_BAD_INPUT, "tm_vcycle_shapes before a mixed-precision solve tuned the V-cycle");
+    int k = 0;
+    for (auto* L : c.shells) {
+      if (L->coarsest || !L->colorCount[0]) continue;
+      if (k < cap) {
+        if (wpb_sweep) wpb_sweep[k] = L->wpbSweep;
+        if (wpb_apply) wpb_apply[k] = L->wpbApply;
+      }
+      k++;
+    }
+    if (nlevels) *nlevels = k;
+    if (tma_stages) *tma_stages = c.tsReady ? c.tsStages : 0;
   });
 }
 

@@ -123,6 +123,7 @@ struct IcFactor {
 
 struct ShellLevel {
   int nx = 0, ny = 0, nn = 0;          // columns nx*ny, aggregates nn
+  int wpbSweep = 4, wpbApply = 4;      // warps per block of the FP32 sweep and residual (autotuned)
   std::vector<double> xs, ys;          // grid lines of the level's columns
   std::vector<int> colStart;           // nx*ny+1
   std::vector<double> zref, zlo, zhi;  // per aggregate
@@ -250,6 +251,12 @@ struct Context {
   // colour the runs of whole columns of each CTA (indices into the colour's column list), the
   // longest run, the chunk stages, the two tensor maps (operator rows, neighbour ids)
   bool tsReady = false;
+  long long tunedEpoch = -1;           // hierarchy epoch the FP32 V-cycle's launch shapes were tuned for
+  long long shapeEpoch = 0;            // bumped when the launch shapes change (the cycle is captured again)
+  int tsPlanned = 0;                   // the largest TMA stage count that fits (the planner's)
+  bool shapesPinned = false;           // the caller fixed the shapes (tm_set_vcycle_shapes): no timing
+  std::vector<int> pinSweep, pinApply; // pinned warps per block per swept shell level
+  int pinStages = 0;                   // pinned TMA stage count (0: the planner's)
   int tsParts = 0, tsMaxNodes = 0, tsStages = 0;
   DBuf<int> d_tsPart[4];
   alignas(64) unsigned char tsMapVal[128];
@@ -364,6 +371,8 @@ void launch_axpy2_32(Context& c, const double* alpha_dev, const float* p, float*
 void launch_xpby32(Context& c, const float* z, const double* beta_dev, float* p, size_t n);
 void launch_zero_constrained32(Context& c, float* v);
 void launch_vcycle32(Context& c, const float* r, float* z);
+void autotune_vcycle32(Context& c);   // launch shapes of the FP32 V-cycle, once per hierarchy
+void check_device_error(Context& c);  // raises when a bounded device wait ran out
 void launch_d2f(Context& c, const double* a, float* b, size_t n);
 void launch_add_f2d(Context& c, const float* d, double* x, size_t n);
 void launch_f2d(Context& c, const float* a, double* b, size_t n);
@@ -376,6 +385,7 @@ void launch_div_scalar(Context& c, double* v, double d, size_t n);              
 // ---- level-0 sweep of the FP32 V-cycle with TMA-streamed operator rows (tm_sweep_tma.cu)
 void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st);
 bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float* x);   // false: not available
+size_t sweep_tma_smem(int maxNodes, int nstage);   // shared memory of the TMA sweep (~0: does not fit)
 
 // ---- Anand (tm_anand.cu) ---------------------------------------------------------------------
 void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps_h,

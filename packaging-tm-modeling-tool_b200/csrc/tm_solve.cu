@@ -10,6 +10,8 @@
 //  * dot products are two-pass reductions in a fixed order (deterministic run to run).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "tm_internal.h"
 
 namespace tmg {
@@ -379,10 +381,42 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
   __syncwarp();
 }
 
+// one column of a shell-level sweep by one warp: r = b - K x over the column's rows, then
+// x_col += A_cc^-1 r with the explicit inverse Ai (entry (e, k) at k*m + e). For blocks of at most
+// SH_PRE rows every lane fetches its row of the inverse before the residual, so that those loads
+// overlap the residual's.
+template <class T>
+__device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* __restrict__ Ai, const int* __restrict__ rowPtr,
+                                                   const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ b,
+                                                   T* __restrict__ x, bool zeroGuess, T* part, T* r, int* rp) {
+  const int n0 = mt.x, na = mt.y - mt.x, m = 6 * na;
+  T a[SH_PRE];
+  const bool pre = m <= SH_PRE;
+#pragma unroll
+  for (int k = 0; k < SH_PRE; k++) a[k] = (pre && lane < m && k < m) ? Ai[(size_t)k * m + lane] : (T)0;
+  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, zeroGuess, part, r, rp);
+  if (pre) {
+    if (lane < m) {
+      T acc = 0;
+#pragma unroll
+      for (int k = 0; k < SH_PRE; k++)
+        if (k < m) acc += a[k] * r[k];
+      x[6 * (size_t)n0 + lane] += acc;
+    }
+    return;
+  }
+  for (int e = lane; e < m; e += 32) {
+    T acc = 0;
+#pragma unroll 6
+    for (int k = 0; k < m; k++) acc += Ai[(size_t)k * m + e] * r[k];
+    x[6 * (size_t)n0 + e] += acc;
+  }
+}
+
 // shell-level residual res = b - K x over all columns, warp per column (meta: first and
 // one-past-last aggregate and block of every column)
 template <class T>
-__global__ void __launch_bounds__(128) k_apply_shell(int ncol, const int4* __restrict__ meta, const int* __restrict__ rowPtr,
+__global__ void __launch_bounds__(256) k_apply_shell(int ncol, const int4* __restrict__ meta, const int* __restrict__ rowPtr,
                                                      const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ x,
                                                      const T* __restrict__ b, T* __restrict__ y, int maxm, int maxBlk) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -402,11 +436,9 @@ __global__ void __launch_bounds__(128) k_apply_shell(int ncol, const int4* __res
 // shell-level column sweep, warp per column of one colour (columnSweep shell branch,
 // 10-solver.js:535-553): r = b - K x over the column's rows, then x_col += A_cc^-1 r with the
 // explicit inverse of the column block. The colour's column list carries each column's aggregate
-// and block ranges and the offset of its inverse (one load). For blocks of at most SH_PRE rows
-// every lane fetches its row of the inverse before the residual, so that those loads overlap the
-// residual's.
+// and block ranges and the offset of its inverse (one load).
 template <class T>
-__global__ void __launch_bounds__(128) k_sweep_shell(int ncolc, const int4* __restrict__ meta, const long long* __restrict__ cfOff,
+__global__ void __launch_bounds__(256) k_sweep_shell(int ncolc, const int4* __restrict__ meta, const long long* __restrict__ cfOff,
                                                      const int* __restrict__ rowPtr, const int* __restrict__ col,
                                                      const T* __restrict__ val, const T* __restrict__ cf, const T* __restrict__ b,
                                                      T* __restrict__ x, int maxm, int maxBlk, int zeroGuess) {
@@ -418,30 +450,7 @@ __global__ void __launch_bounds__(128) k_sweep_shell(int ncolc, const int4* __re
   T* part = reinterpret_cast<T*>(base);
   T* r = part + 6 * (size_t)maxBlk;
   int* rp = reinterpret_cast<int*>(r + (maxm > SH_PRE ? maxm : SH_PRE));
-  const int4 mt = meta[gw];
-  const int n0 = mt.x, na = mt.y - mt.x, m = 6 * na;
-  const T* Ai = cf + cfOff[gw];   // entry (e, k) at k*m + e
-  T a[SH_PRE];
-  const bool pre = m <= SH_PRE;
-#pragma unroll
-  for (int k = 0; k < SH_PRE; k++) a[k] = (pre && lane < m && k < m) ? Ai[(size_t)k * m + lane] : (T)0;
-  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, zeroGuess != 0, part, r, rp);
-  if (pre) {
-    if (lane < m) {
-      T acc = 0;
-#pragma unroll
-      for (int k = 0; k < SH_PRE; k++)
-        if (k < m) acc += a[k] * r[k];
-      x[6 * (size_t)n0 + lane] += acc;
-    }
-    return;
-  }
-  for (int e = lane; e < m; e += 32) {
-    T acc = 0;
-#pragma unroll 6
-    for (int k = 0; k < m; k++) acc += Ai[(size_t)k * m + e] * r[k];
-    x[6 * (size_t)n0 + e] += acc;
-  }
+  shell_sweep_column<T>(lane, meta[gw], cf + cfOff[gw], rowPtr, col, val, b, x, zeroGuess != 0, part, r, rp);
 }
 
 // shell restriction: rc = P^T res (children lists, transposeProl order)
@@ -574,15 +583,19 @@ void vcycle(Context& c, const T* r, T* z) {
         c.d_nbr.p, B::val0(c), B::F(c), r, z, c.panelCap, zero);
     note_launch();
   };
-  const int wpb = 4;
+  // warps per block of the shell kernels: 4, or the autotuned shapes of the FP32 cycle
+  auto wpbS = [&](const ShellLevel& L) { return sizeof(T) == 4 ? L.wpbSweep : 4; };
+  auto wpbA = [&](const ShellLevel& L) { return sizeof(T) == 4 ? L.wpbApply : 4; };
   size_t smemS = 0;
-  for (auto& Lp : c.shells) smemS = std::max(smemS, wpb * shell_stage_bytes<T>(Lp->maxm, Lp->maxColBlocks));
+  for (auto& Lp : c.shells)
+    smemS = std::max(smemS, (size_t)std::max(wpbS(*Lp), wpbA(*Lp)) * shell_stage_bytes<T>(Lp->maxm, Lp->maxColBlocks));
   if (smemS > 48 * 1024) {
     TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_shell<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemS));
     TM_CUDA_CHECK(cudaFuncSetAttribute(k_apply_shell<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemS));
   }
   auto sweepS = [&](ShellLevel& L, int col, int zero) {
     const size_t per = shell_stage_bytes<T>(L.maxm, L.maxColBlocks);
+    const int wpb = wpbS(L);
     TimedLaunch tl(c, K_SWEEP_SHELL);
     k_sweep_shell<T><<<grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st>>>(L.colorCount[col], L.d_colorMeta[col].p,
         (const long long*)L.d_colorCf[col].p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::cf(L), B::b(L), B::x(L), L.maxm, L.maxColBlocks, zero);
@@ -622,6 +635,7 @@ void vcycle(Context& c, const T* r, T* z) {
     {
       TimedLaunch tl(c, K_APPLY_SHELL);
       const int ncol = L.nx * L.ny;
+      const int wpb = wpbA(L);
       k_apply_shell<T><<<grid_for(ncol, wpb), 32 * wpb, wpb * shell_stage_bytes<T>(L.maxm, L.maxColBlocks), st>>>(ncol, L.d_colMeta.p,
           L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L), L.maxm, L.maxColBlocks);
       note_launch();
@@ -795,7 +809,7 @@ void vcycle_graph(Context& c, const T* r, T* z) {
   }
   const int idx = sizeof(T) == 4 ? 1 : 0;
   size_t key = 1469598103934665603ull;
-  for (size_t v : {(size_t)r, (size_t)z, (size_t)c.structEpoch, (size_t)Bufs<T>::val0(c), (size_t)c.stream})
+  for (size_t v : {(size_t)r, (size_t)z, (size_t)c.structEpoch, (size_t)c.shapeEpoch, (size_t)Bufs<T>::val0(c), (size_t)c.stream})
     key = (key ^ v) * 1099511628211ull;
   if (!c.vcGraph[idx] || c.vcKey[idx] != key) {
     if (c.vcGraph[idx]) {
@@ -832,11 +846,107 @@ void vcycle_graph(Context& c, const T* r, T* z) {
   note_launch((int)c.vcNodes[idx]);
 }
 
+// Launch-shape autotuner of the FP32 V-cycle, run once per hierarchy before the cycle is first
+// captured: per shell level the warps per block (2, 4 or 8) of the column sweep and of the
+// residual kernel, and the stage count (2 or 3) of the TMA level-0 sweep. Each candidate is
+// timed with events over ten launches on scratch vectors (the kernels' memory traffic and
+// arithmetic do not depend on the values); a candidate replaces the default (4 warps, the
+// planner's stage count) only when it is at least 3 % faster, so that timing noise does not
+// move the shapes. Shapes the caller pinned are applied without timing.
+void autotune_vcycle32(Context& c) {
+  if (c.tunedEpoch == c.structEpoch) return;
+  c.shapeEpoch++;
+  std::vector<ShellLevel*> swept;
+  for (auto* Lp : c.shells)
+    if (!Lp->coarsest && Lp->colorCount[0]) swept.push_back(Lp);
+  if (c.shapesPinned) {
+    for (size_t k = 0; k < swept.size(); k++) {
+      swept[k]->wpbSweep = k < c.pinSweep.size() ? c.pinSweep[k] : 4;
+      swept[k]->wpbApply = k < c.pinApply.size() ? c.pinApply[k] : 4;
+    }
+    c.tsStages = c.pinStages >= 2 && c.pinStages <= c.tsPlanned && sweep_tma_smem(c.tsMaxNodes, c.pinStages) != ~(size_t)0 ? c.pinStages
+                                                                                                                              : c.tsPlanned;
+    c.tunedEpoch = c.structEpoch;
+    return;
+  }
+  cudaStream_t st = c.stream;
+  cudaEvent_t ea, eb;
+  TM_CUDA_CHECK(cudaEventCreate(&ea));
+  TM_CUDA_CHECK(cudaEventCreate(&eb));
+  int smemMax = 0;
+  TM_CUDA_CHECK(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.dev));
+  const int reps = 10;
+  auto timed = [&](auto&& launch) {
+    launch();
+    TM_CUDA_CHECK(cudaEventRecord(ea, st));
+    for (int q = 0; q < reps; q++) launch();
+    TM_CUDA_CHECK(cudaEventRecord(eb, st));
+    TM_CUDA_CHECK(cudaEventSynchronize(eb));
+    note_launch(reps + 1);
+    float ms = 0;
+    TM_CUDA_CHECK(cudaEventElapsedTime(&ms, ea, eb));
+    TM_CUDA_CHECK(cudaGetLastError());
+    return 1000.0 * ms / reps;
+  };
+  const int cands[3] = {4, 2, 8};   // the default first
+  for (ShellLevel* Lp : swept) {
+    ShellLevel& L = *Lp;
+    const size_t per = shell_stage_bytes<float>(L.maxm, L.maxColBlocks);
+    DBuf<float> sx, sb, sr;
+    sx.alloc(6 * (size_t)L.nn); sx.zero(st);
+    sb.alloc(6 * (size_t)L.nn); sb.zero(st);
+    sr.alloc(6 * (size_t)L.nn);
+    L.wpbSweep = L.wpbApply = 4;
+    double bestS = 1e30, bestA = 1e30;
+    for (int wpb : cands) {
+      const size_t smem = wpb * per;
+      if (smem > (size_t)smemMax) continue;
+      const int attr = (int)std::max<size_t>(smem, 48 * 1024);
+      TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_shell<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, attr));
+      TM_CUDA_CHECK(cudaFuncSetAttribute(k_apply_shell<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, attr));
+      const double tS = timed([&] {
+        k_sweep_shell<float><<<grid_for(L.colorCount[0], wpb), 32 * wpb, smem, st>>>(L.colorCount[0], L.d_colorMeta[0].p,
+            (const long long*)L.d_colorCf[0].p, L.d_rowPtr.p, L.d_col.p, L.d_val32.p, L.d_cfInv32.p, sb.p, sx.p, L.maxm, L.maxColBlocks, 0);
+      });
+      const int ncol = L.nx * L.ny;
+      const double tA = timed([&] {
+        k_apply_shell<float><<<grid_for(ncol, wpb), 32 * wpb, smem, st>>>(ncol, L.d_colMeta.p, L.d_rowPtr.p, L.d_col.p, L.d_val32.p, sx.p,
+                                                                           sb.p, sr.p, L.maxm, L.maxColBlocks);
+      });
+      if (tS < 0.97 * bestS) { bestS = tS; L.wpbSweep = wpb; }
+      if (tA < 0.97 * bestA) { bestA = tA; L.wpbApply = wpb; }
+    }
+  }
+  if (c.tsReady && c.colorCount[0]) {
+    const size_t n = 3 * (size_t)c.nn;
+    DBuf<float> sx, sb;
+    sx.alloc(n); sx.zero(st);
+    sb.alloc(n); sb.zero(st);
+    int best = c.tsPlanned;
+    double bestT = 1e30;
+    for (int ns = c.tsPlanned; ns >= 2; ns--) {   // the planner's count first
+      if (sweep_tma_smem(c.tsMaxNodes, ns) == ~(size_t)0) continue;
+      c.tsStages = ns;
+      const double t = timed([&] { launch_sweep_tma(c, 0, 0, sb.p, sx.p); });
+      if (t < 0.97 * bestT) { bestT = t; best = ns; }
+    }
+    c.tsStages = best;
+  }
+  TM_CUDA_CHECK(cudaEventDestroy(ea));
+  TM_CUDA_CHECK(cudaEventDestroy(eb));
+  TM_CUDA_CHECK(cudaStreamSynchronize(st));
+  check_device_error(c);
+  c.tunedEpoch = c.structEpoch;
+}
+
 void launch_vcycle(Context& c, const double* r, double* z, bool mixed) {
   (void)mixed;
   vcycle_graph<double>(c, r, z);
 }
 
-void launch_vcycle32(Context& c, const float* r, float* z) { vcycle_graph<float>(c, r, z); }
+void launch_vcycle32(Context& c, const float* r, float* z) {
+  autotune_vcycle32(c);
+  vcycle_graph<float>(c, r, z);
+}
 
 }  // namespace tmg

@@ -378,6 +378,7 @@ void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st)
   c.tsStages = 0;
   for (int ns = 3; ns >= 2 && !c.tsStages; ns--)
     if (sweep_tma_smem(c.tsMaxNodes, ns) + staticSmem <= (size_t)smemMax) c.tsStages = ns;
+  c.tsPlanned = c.tsStages;
   c.tsReady = TM_SWEEP_TMA && c.tsStages > 0;
 }
 

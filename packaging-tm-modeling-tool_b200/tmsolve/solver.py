@@ -229,6 +229,25 @@ class DeviceModel:
         check(load().tm_pc_apply(self.h, r.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p)))
         return z
 
+    def vcycle_shapes(self) -> dict:
+        """Launch shapes the FP32 V-cycle's autotuner chose: warps per block of the shell sweep and
+        residual per tuned level, and the TMA level-0 sweep's stage count (0: not used)."""
+        cap = 32
+        n, st = C.c_int32(0), C.c_int32(0)
+        ws, wa = (C.c_int32 * cap)(), (C.c_int32 * cap)()
+        check(load().tm_vcycle_shapes(self.h, cap, C.byref(n), ws, wa, C.byref(st)))
+        k = min(n.value, cap)
+        return dict(wpb_sweep=list(ws[:k]), wpb_apply=list(wa[:k]), tma_stages=st.value)
+
+    def set_vcycle_shapes(self, wpb_sweep=None, wpb_apply=None, tma_stages=0):
+        """Pin the FP32 V-cycle's launch shapes (as vcycle_shapes returns them); None: autotune."""
+        if wpb_sweep is None:
+            check(load().tm_set_vcycle_shapes(self.h, -1, None, None, 0))
+            return
+        n = len(wpb_sweep)
+        ws, wa = (C.c_int32 * max(n, 1))(*wpb_sweep), (C.c_int32 * max(n, 1))(*wpb_apply)
+        check(load().tm_set_vcycle_shapes(self.h, n, ws, wa, int(tma_stages)))
+
     def solve(self, f, label=None, key=-1, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64",
               out: Optional[np.ndarray] = None) -> dict:
         """LinearSolver.solve with host arrays; the displacement goes to `out` when given."""

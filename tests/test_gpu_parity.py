@@ -178,3 +178,36 @@ def test_solve_f32_output():
     r32 = dm.solve_f32(dm.assemble_step(step), tol=1e-10, warm=0, key=2)
     assert r32["converged"] and r32["u"].dtype == np.float32
     assert np.array_equal(r32["u"], u64.astype(np.float32))
+
+
+def test_vcycle_autotuned_shapes():
+    """The FP32 V-cycle's launch shapes are tuned once per hierarchy before its first capture: every
+    swept shell level gets 2, 4 or 8 warps per block, the TMA sweep 2 or 3 stages (0: not used).
+    Shapes change no arithmetic (a warp per column, the same chunk order), so a solve with pinned
+    shapes returns the tuned solve's doubles bit for bit."""
+    from tmsolve.solver import DeviceModel
+    pkg = lidded_c2(n_inplane=48)
+    dm = DeviceModel(pkg)
+    f = dm.assemble_step(pkg.step())
+    dm.solve(f, tol=1e-10, warm=0, key=1)
+    with pytest.raises(_lib.TmError):
+        dm.vcycle_shapes()          # an FP64 solve tunes nothing
+    r = dm.solve(f, tol=1e-10, warm=0, key=2, precision="mixed")
+    assert r["converged"]
+    sh = dm.vcycle_shapes()
+    nl = len(sh["wpb_sweep"])
+    assert nl >= 1 and nl == len(sh["wpb_apply"])
+    assert set(sh["wpb_sweep"]) <= {2, 4, 8} and set(sh["wpb_apply"]) <= {2, 4, 8}
+    assert sh["tma_stages"] in (0, 2, 3)
+    for ws, wa, ts in (([2] * nl, [8] * nl, 2), ([8] * nl, [2] * nl, 0)):
+        dm.set_vcycle_shapes(ws, wa, ts)
+        rp = dm.solve(f, tol=1e-10, warm=0, key=3, precision="mixed")
+        got = dm.vcycle_shapes()
+        assert got["wpb_sweep"] == ws and got["wpb_apply"] == wa
+        assert ts == 0 or got["tma_stages"] in (0, ts)
+        assert rp["iters"] == r["iters"] and np.array_equal(rp["u"], r["u"])
+    with pytest.raises(_lib.TmError):
+        dm.set_vcycle_shapes([3] * nl, [4] * nl)
+    dm.set_vcycle_shapes(None)      # back to autotuning
+    r2 = dm.solve(f, tol=1e-10, warm=0, key=4, precision="mixed")
+    assert np.array_equal(r2["u"], r["u"])
