@@ -40,6 +40,7 @@ constexpr int TS_ROWS = NSLOT * 9;                                 // operator r
 constexpr int TS_STAGE_BYTES = (TS_ROWS + NSLOT) * TS_CHUNK * 4;   // values, then neighbour ids
 constexpr int TS_MAXSTAGE = 8;
 constexpr long long TS_WAIT_LIMIT = 1LL << 22;
+constexpr int TS_ILP = 4;                                          // positions per thread in the run's gathers
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -176,10 +177,27 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     for (int q = 0; q < TS_MAXSTAGE; q++) s_last[q] = -1;
     for (int q = 0; q < nstage && q < nchunks; q++) issue(q);
   }
-  // r starts as b (the chunks subtract K x)
-  for (int l = tid; l < P1 - P0; l += blockDim.x) {
-    const size_t n = posNode[P0 + l];
-    sr[3 * l] = b[3 * n]; sr[3 * l + 1] = b[3 * n + 1]; sr[3 * l + 2] = b[3 * n + 2];
+  // r starts as b (the chunks subtract K x); a thread takes up to TS_ILP positions and issues
+  // their loads together (the node ids, then b), so that the gathers' latencies overlap
+  const int nrun = P1 - P0;
+  for (int l0 = tid; l0 < nrun; l0 += TS_ILP * blockDim.x) {
+    size_t nd[TS_ILP];
+    float v[TS_ILP][3];
+#pragma unroll
+    for (int u = 0; u < TS_ILP; u++) {
+      const int l = l0 + u * blockDim.x;
+      nd[u] = l < nrun ? (size_t)posNode[P0 + l] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < TS_ILP; u++)
+      if (l0 + u * (int)blockDim.x < nrun) {
+        v[u][0] = b[3 * nd[u]]; v[u][1] = b[3 * nd[u] + 1]; v[u][2] = b[3 * nd[u] + 2];
+      }
+#pragma unroll
+    for (int u = 0; u < TS_ILP; u++) {
+      const int l = l0 + u * blockDim.x;
+      if (l < nrun) { sr[3 * l] = v[u][0]; sr[3 * l + 1] = v[u][1]; sr[3 * l + 2] = v[u][2]; }
+    }
   }
   __syncthreads();
   // two warp groups take alternate chunks, so that one group's gathers of x overlap the other's;
@@ -265,50 +283,94 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     __syncthreads();
     return;
   }
-  // one thread per column: block-tridiagonal forward and backward substitution
+  // one thread per column: block-tridiagonal forward and backward substitution. A node's 18
+  // factor entries are read as 9 float2 (node rows are 72 bytes, 8-byte aligned), the next node's
+  // ahead of the current node's arithmetic; the backward pass keeps the factors of node l+1 from
+  // the previous iteration. Entry i of a node is pair i/2, component i%2.
   for (int q = tid; q < c1 - c0; q += blockDim.x) {
     const int cp0 = colPos[c0 + q], len = colPos[c0 + q + 1] - cp0;
+    if (len <= 0) continue;
     float* rr = sr + 3 * (size_t)(cp0 - P0);
-    const float* Fc = sF + 18 * (size_t)(cp0 - Q0);
+    const float2* Fc = reinterpret_cast<const float2*>(sF + 18 * (size_t)(cp0 - Q0));
+    float2 f[9], fn[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) f[j] = Fc[j];
     float p0v = 0, p1v = 0, p2v = 0;
     for (int l = 0; l < len; l++) {
-      const float* f = Fc + 18 * l;
+      if (l + 1 < len) {
+#pragma unroll
+        for (int j = 0; j < 9; j++) fn[j] = Fc[9 * (l + 1) + j];
+      }
       float b0 = rr[3 * l], b1 = rr[3 * l + 1], b2 = rr[3 * l + 2];
       if (l > 0) {
-        b0 -= f[9] * p0v + f[10] * p1v + f[11] * p2v;
-        b1 -= f[12] * p0v + f[13] * p1v + f[14] * p2v;
-        b2 -= f[15] * p0v + f[16] * p1v + f[17] * p2v;
+        b0 -= f[4].y * p0v + f[5].x * p1v + f[5].y * p2v;   // entries 9, 10, 11
+        b1 -= f[6].x * p0v + f[6].y * p1v + f[7].x * p2v;   // 12, 13, 14
+        b2 -= f[7].y * p0v + f[8].x * p1v + f[8].y * p2v;   // 15, 16, 17
       }
-      const float y0 = b0 * f[1];
-      const float y1 = (b1 - f[3] * y0) * f[2];
-      const float y2 = (b2 - f[6] * y0 - f[7] * y1) * f[5];
+      const float y0 = b0 * f[0].y;                                  // 1
+      const float y1 = (b1 - f[1].y * y0) * f[1].x;                  // 3, 2
+      const float y2 = (b2 - f[3].x * y0 - f[3].y * y1) * f[2].y;    // 6, 7, 5
       rr[3 * l] = y0; rr[3 * l + 1] = y1; rr[3 * l + 2] = y2;
       p0v = y0; p1v = y1; p2v = y2;
+#pragma unroll
+      for (int j = 0; j < 9; j++) f[j] = fn[j];
     }
+    float2 g[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) f[j] = Fc[9 * (len - 1) + j];
     float q0 = 0, q1 = 0, q2 = 0;
     for (int l = len - 1; l >= 0; l--) {
-      const float* f = Fc + 18 * l;
-      float b0 = rr[3 * l], b1 = rr[3 * l + 1], b2 = rr[3 * l + 2];
-      if (l + 1 < len) {
-        const float* g = Fc + 18 * (l + 1);
-        b0 -= g[9] * q0 + g[12] * q1 + g[15] * q2;
-        b1 -= g[10] * q0 + g[13] * q1 + g[16] * q2;
-        b2 -= g[11] * q0 + g[14] * q1 + g[17] * q2;
+      if (l > 0) {
+#pragma unroll
+        for (int j = 0; j < 9; j++) fn[j] = Fc[9 * (l - 1) + j];
       }
-      const float z2 = b2 * f[5];
-      const float z1 = (b1 - f[7] * z2) * f[2];
-      const float z0 = (b0 - f[3] * z1 - f[6] * z2) * f[1];
+      float b0 = rr[3 * l], b1 = rr[3 * l + 1], b2 = rr[3 * l + 2];
+      if (l + 1 < len) {   // g: node l+1
+        b0 -= g[4].y * q0 + g[6].x * q1 + g[7].y * q2;   // entries 9, 12, 15
+        b1 -= g[5].x * q0 + g[6].y * q1 + g[8].x * q2;   // 10, 13, 16
+        b2 -= g[5].y * q0 + g[7].x * q1 + g[8].y * q2;   // 11, 14, 17
+      }
+      const float z2 = b2 * f[2].y;                                  // 5
+      const float z1 = (b1 - f[3].y * z2) * f[1].x;                  // 7, 2
+      const float z0 = (b0 - f[1].y * z1 - f[3].x * z2) * f[0].y;    // 3, 6, 1
       rr[3 * l] = z0; rr[3 * l + 1] = z1; rr[3 * l + 2] = z2;
       q0 = z0; q1 = z1; q2 = z2;
+#pragma unroll
+      for (int j = 0; j < 9; j++) {
+        g[j] = f[j];
+        f[j] = fn[j];
+      }
     }
   }
   __syncthreads();
-  for (int l = tid; l < P1 - P0; l += blockDim.x) {
-    const size_t n = posNode[P0 + l];
+  // x of the run (node ids, then x, then the stores, TS_ILP positions per thread)
+  for (int l0 = tid; l0 < nrun; l0 += TS_ILP * blockDim.x) {
+    size_t nd[TS_ILP];
+#pragma unroll
+    for (int u = 0; u < TS_ILP; u++) {
+      const int l = l0 + u * blockDim.x;
+      nd[u] = l < nrun ? (size_t)posNode[P0 + l] : 0;
+    }
     if (zeroGuess) {
-      x[3 * n] = sr[3 * l]; x[3 * n + 1] = sr[3 * l + 1]; x[3 * n + 2] = sr[3 * l + 2];
+#pragma unroll
+      for (int u = 0; u < TS_ILP; u++) {
+        const int l = l0 + u * blockDim.x;
+        if (l < nrun) { x[3 * nd[u]] = sr[3 * l]; x[3 * nd[u] + 1] = sr[3 * l + 1]; x[3 * nd[u] + 2] = sr[3 * l + 2]; }
+      }
     } else {
-      x[3 * n] += sr[3 * l]; x[3 * n + 1] += sr[3 * l + 1]; x[3 * n + 2] += sr[3 * l + 2];
+      float v[TS_ILP][3];
+#pragma unroll
+      for (int u = 0; u < TS_ILP; u++)
+        if (l0 + u * (int)blockDim.x < nrun) {
+          v[u][0] = x[3 * nd[u]]; v[u][1] = x[3 * nd[u] + 1]; v[u][2] = x[3 * nd[u] + 2];
+        }
+#pragma unroll
+      for (int u = 0; u < TS_ILP; u++) {
+        const int l = l0 + u * blockDim.x;
+        if (l < nrun) {
+          x[3 * nd[u]] = v[u][0] + sr[3 * l]; x[3 * nd[u] + 1] = v[u][1] + sr[3 * l + 1]; x[3 * nd[u] + 2] = v[u][2] + sr[3 * l + 2];
+        }
+      }
     }
   }
 }
