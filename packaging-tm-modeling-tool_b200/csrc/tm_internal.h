@@ -259,10 +259,8 @@ struct Context {
   int pinStages = 0;                   // pinned TMA stage count (0: the planner's)
   int tsParts = 0, tsMaxNodes = 0, tsStages = 0;
   DBuf<int> d_tsPart[4];
-  alignas(64) unsigned char tsMapVal[128];
-  alignas(64) unsigned char tsMapNbr[128];
-  const void* tsValPtr = nullptr;
-  const void* tsNbrPtr = nullptr;
+  DBuf<float> d_val32p;                // position-major FP32 operator (243 values per position)
+  DBuf<int> d_nbrp;                    // position-major neighbour ids (27 per position)
   DBuf<int> d_err;                     // set by a bounded device wait that ran out
   // level-0 column panels: the columns of one colour packed into groups of at most panelCap nodes,
   // one CTA per group (group g holds colour columns grpStart[g] .. grpStart[g+1]-1); colPos holds
@@ -385,6 +383,7 @@ void launch_div_scalar(Context& c, double* v, double d, size_t n);              
 // ---- level-0 sweep of the FP32 V-cycle with TMA-streamed operator rows (tm_sweep_tma.cu)
 void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st);
 bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float* x);   // false: not available
+void launch_val_to_f32(Context& c);   // FP32 level-0 operator (and its position-major copy for the TMA sweep)
 size_t sweep_tma_smem(int maxNodes, int nstage);   // shared memory of the TMA sweep (~0: does not fit)
 
 // ---- Anand (tm_anand.cu) ---------------------------------------------------------------------

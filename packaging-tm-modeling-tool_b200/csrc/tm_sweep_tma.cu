@@ -4,9 +4,10 @@
 //  * every CTA (one per SM) owns a contiguous run of whole columns of the colour (about 1/148 of
 //    the colour's nodes; the colour's positions are contiguous, so the run is one position range);
 //  * the run's operator rows (243 values per position) and neighbour ids (27) stream through
-//    shared memory in chunks of 64 positions, each chunk one pair of 2-D TMA tensor loads
-//    (cp.async.bulk.tensor, no multicast) completing on an mbarrier, in a ring of stages so that
-//    the loads of later chunks are in flight while a chunk's residual rows are computed;
+//    shared memory in chunks of 64 positions, each chunk one pair of TMA bulk copies
+//    (cp.async.bulk, no multicast) of the position-major copies of the operator and the ids (a
+//    chunk is one contiguous range of each), completing on an mbarrier, in a ring of stages so
+//    that the loads of later chunks are in flight while a chunk's residual rows are computed;
 //  * r starts as the run's b in shared memory; two warp groups take alternate chunks (one
 //    group's gathers of x overlap the other's); in a group 4 threads per position take the 27
 //    slots (a warp takes 32 consecutive positions of one slot group, conflict-free), their
@@ -19,7 +20,6 @@
 // Columns of one colour do not couple, so runs never read each other's updates. Every wait on
 // an mbarrier is bounded: a wait that runs out sets the error flag, waits (bounded) for the
 // copies still in flight and leaves; the host reports TM_TIMEOUT.
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -113,23 +113,22 @@ __device__ __forceinline__ float ld_keep(const float* p, uint64_t pol) {
   return v;
 }
 
-// box of a 2-D tensor map at (x, y) into shared memory, completing on bar
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar, uint64_t pol) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(pol)
-      : "memory");
-}
 // contiguous bytes into shared memory (16-byte aligned source, destination and size)
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)), "l"(src),
                "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+// the same with an L2 policy
+__device__ __forceinline__ void bulk_load_hint(void* dst, const void* src, unsigned bytes, uint64_t* bar, uint64_t pol) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+               : "memory");
+}
 
 __global__ void __launch_bounds__(TS_THREADS, 1)
-    k_sweep_tma(const __grid_constant__ CUtensorMap tmVal, const __grid_constant__ CUtensorMap tmNbr, const int* __restrict__ partCol,
+    k_sweep_tma(const float* __restrict__ valPm, const int* __restrict__ nbrPm, const int* __restrict__ partCol,
                 const int* __restrict__ colPos, const int* __restrict__ posNode, const float* __restrict__ F, const float* __restrict__ b,
                 float* __restrict__ x, int maxNodes, int nstage, int zeroGuess, int nn, int zlo, int zhi, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smraw_t[];
@@ -165,11 +164,15 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
   const uint64_t polStream = policy_evict_first(), polKeep = policy_evict_last();
   __shared__ int s_fail;
   __shared__ int s_last[TS_MAXSTAGE];   // last chunk issued into each stage
+  // chunk k: positions Q0 + 64k .. (the last chunk up to QE; both multiples of 4, so every copy
+  // starts on a 16-byte boundary and moves a multiple of 16 bytes)
   auto issue = [&](int k) {
     float* dst = reinterpret_cast<float*>(smt + (size_t)(k % nstage) * TS_STAGE_BYTES);
-    mbar_expect_tx(&bars[k % nstage], TS_STAGE_BYTES);
-    tma_load_2d(dst, &tmVal, Q0 + k * TS_CHUNK, 0, &bars[k % nstage], polStream);
-    tma_load_2d(dst + TS_ROWS * TS_CHUNK, &tmNbr, Q0 + k * TS_CHUNK, 0, &bars[k % nstage], polStream);
+    const int q0 = Q0 + k * TS_CHUNK, np = min(TS_CHUNK, QE - q0);
+    const unsigned bv = (unsigned)np * TS_ROWS * 4, bi = (unsigned)np * NSLOT * 4;
+    mbar_expect_tx(&bars[k % nstage], bv + bi);
+    bulk_load_hint(dst, valPm + (size_t)q0 * TS_ROWS, bv, &bars[k % nstage], polStream);
+    bulk_load_hint(dst + TS_ROWS * TS_CHUNK, nbrPm + (size_t)q0 * NSLOT, bi, &bars[k % nstage], polStream);
     s_last[k % nstage] = k;
   };
   if (tid == 0) {
@@ -201,7 +204,8 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
   }
   __syncthreads();
   // two warp groups take alternate chunks, so that one group's gathers of x overlap the other's;
-  // a warp takes 32 consecutive positions of one slot group: conflict-free shared-memory rows
+  // a warp takes 32 consecutive positions of one slot group: position rows are 243 values and 27
+  // ids long (odd strides), so the warp's shared-memory accesses fall in 32 different banks
   const int grp = tid / TS_GTHREADS, gtid = tid % TS_GTHREADS;
   const int pl = gtid % TS_CHUNK, sub = gtid / TS_CHUNK;
   float* gred = red + (size_t)grp * TS_TPP * TS_CHUNK * 3;
@@ -223,13 +227,13 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       for (int h = 0; h < (NSLOT + TS_TPP - 1) / TS_TPP; h++) {
         const int s = sub + TS_TPP * h;
         if (s < NSLOT) {
-          const int jj = sn[s * TS_CHUNK + pl];
+          const int jj = sn[pl * NSLOT + s];
           const size_t j = jj < 0 ? 0 : jj;   // absent slots hold zeros
           const float x0 = ld_keep(x + 3 * j, polKeep), x1 = ld_keep(x + 3 * j + 1, polKeep), x2 = ld_keep(x + 3 * j + 2, polKeep);
-          const float* v = sv + s * 9 * TS_CHUNK + pl;
-          a0 += v[0] * x0 + v[TS_CHUNK] * x1 + v[2 * TS_CHUNK] * x2;
-          a1 += v[3 * TS_CHUNK] * x0 + v[4 * TS_CHUNK] * x1 + v[5 * TS_CHUNK] * x2;
-          a2 += v[6 * TS_CHUNK] * x0 + v[7 * TS_CHUNK] * x1 + v[8 * TS_CHUNK] * x2;
+          const float* v = sv + pl * TS_ROWS + s * 9;
+          a0 += v[0] * x0 + v[1] * x1 + v[2] * x2;
+          a1 += v[3] * x0 + v[4] * x1 + v[5] * x2;
+          a2 += v[6] * x0 + v[7] * x1 + v[8] * x2;
         }
       }
     }
@@ -375,35 +379,41 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
   }
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
-                                  const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    TM_CUDA_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    if (q != cudaDriverEntryPointSuccess || !p) fail(TM_CUDA, "cuTensorMapEncodeTiled is not available");
-    fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
-  return fn;
-}
-
-// 2-D map over a slot-major array of `rows` rows of nnp 4-byte entries, box of TS_CHUNK
-// positions x all rows
-void encode_rows(CUtensorMap* map, CUtensorMapDataType type, const void* base, int nnp, int rows) {
-  const cuuint64_t dims[2] = {(cuuint64_t)nnp, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)nnp * 4};
-  const cuuint32_t box[2] = {(cuuint32_t)TS_CHUNK, (cuuint32_t)rows};
-  const cuuint32_t elem[2] = {1, 1};
-  const CUresult r = encode_fn()(map, type, 2, const_cast<void*>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) fail(TM_CUDA, "cuTensorMapEncodeTiled failed");
-}
-
 }  // namespace
+
+inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
+
+// FP32 copies of the level-0 operator in one pass over the FP64 one: slot-major (rows of nnp
+// positions, as the FP64 operator; the apply and the panel sweep read it) and, when vpm is
+// given, position-major (the 243 values of a position contiguous, the layout the TMA sweep
+// streams). A block takes 32 positions: coalesced row reads, a shared-memory transpose, one
+// contiguous write.
+__global__ void __launch_bounds__(256) k_val_to_f32(int nnp, const double* __restrict__ val, float* __restrict__ v32,
+                                                    float* __restrict__ vpm) {
+  __shared__ float tile[32 * TS_ROWS];
+  const int p0 = blockIdx.x * 32, pl = threadIdx.x & 31, p = p0 + pl;
+  for (int r = threadIdx.x >> 5; r < TS_ROWS; r += 8) {
+    float f = 0.f;
+    if (p < nnp) {
+      f = (float)val[(size_t)r * nnp + p];
+      v32[(size_t)r * nnp + p] = f;
+    }
+    tile[pl * TS_ROWS + r] = f;   // bank (19 pl + r) mod 32: conflict-free
+  }
+  if (!vpm) return;
+  __syncthreads();
+  const int np = min(32, nnp - p0);
+  float* out = vpm + (size_t)p0 * TS_ROWS;
+  for (int j = threadIdx.x; j < np * TS_ROWS; j += blockDim.x) out[j] = tile[j];
+}
+
+// position-major copy of the neighbour ids (27 per position)
+__global__ void k_nbr_pm(int nnp, const int* __restrict__ nbr, int* __restrict__ npm) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)nnp * NSLOT) return;
+  const int p = (int)(t / NSLOT), s = (int)(t % NSLOT);
+  npm[t] = nbr[(size_t)s * nnp + p];
+}
 
 // shared memory of the sweep for the longest run; 0 when even two stages do not fit
 size_t sweep_tma_smem(int maxNodes, int nstage) {
@@ -442,25 +452,32 @@ void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st)
     if (sweep_tma_smem(c.tsMaxNodes, ns) + staticSmem <= (size_t)smemMax) c.tsStages = ns;
   c.tsPlanned = c.tsStages;
   c.tsReady = TM_SWEEP_TMA && c.tsStages > 0;
+  if (c.tsReady) {
+    c.d_nbrp.alloc((size_t)NSLOT * c.nnp);
+    k_nbr_pm<<<grid_for((size_t)NSLOT * c.nnp, 256), 256, 0, st>>>(c.nnp, c.d_nbr.p, c.d_nbrp.p);
+    note_launch();
+    TM_CUDA_CHECK(cudaGetLastError());
+  }
 }
 
 bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float* x) {
   if (!c.tsReady) return false;
-  if (c.tsValPtr != c.d_val32.p || c.tsNbrPtr != c.d_nbr.p) {
-    static_assert(sizeof(CUtensorMap) <= sizeof(c.tsMapVal), "tensor map storage");
-    encode_rows(reinterpret_cast<CUtensorMap*>(c.tsMapVal), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, c.d_val32.p, c.nnp, TS_ROWS);
-    encode_rows(reinterpret_cast<CUtensorMap*>(c.tsMapNbr), CU_TENSOR_MAP_DATA_TYPE_INT32, c.d_nbr.p, c.nnp, NSLOT);
-    c.tsValPtr = c.d_val32.p;
-    c.tsNbrPtr = c.d_nbr.p;
-  }
   const size_t smem = sweep_tma_smem(c.tsMaxNodes, c.tsStages);
   TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const CUtensorMap* mv = reinterpret_cast<const CUtensorMap*>(c.tsMapVal);
-  const CUtensorMap* mn = reinterpret_cast<const CUtensorMap*>(c.tsMapNbr);
-  k_sweep_tma<<<c.tsParts, TS_THREADS, smem, c.stream>>>(*mv, *mn, c.d_tsPart[col].p, c.d_colPos[col].p, c.d_posNode.p, c.d_F32.p, b, x,
-      c.tsMaxNodes, c.tsStages, zeroGuess, c.nn, c.colourPos[col], c.colourPos[col + 1], c.d_err.p);
+  k_sweep_tma<<<c.tsParts, TS_THREADS, smem, c.stream>>>(c.d_val32p.p, c.d_nbrp.p, c.d_tsPart[col].p, c.d_colPos[col].p, c.d_posNode.p,
+                                                        c.d_F32.p, b, x, c.tsMaxNodes, c.tsStages, zeroGuess, c.nn, c.colourPos[col],
+                                                        c.colourPos[col + 1], c.d_err.p);
   note_launch();
   return true;
+}
+
+void launch_val_to_f32(Context& c) {
+  const size_t n = (size_t)TS_ROWS * c.nnp;
+  c.d_val32.alloc(n);
+  if (c.tsReady) c.d_val32p.alloc(n);
+  k_val_to_f32<<<(c.nnp + 31) / 32, 256, 0, c.stream>>>(c.nnp, c.d_val.p, c.d_val32.p, c.tsReady ? c.d_val32p.p : nullptr);
+  note_launch();
+  TM_CUDA_CHECK(cudaGetLastError());
 }
 
 }  // namespace tmg
