@@ -31,7 +31,7 @@ for p in (ROOT, PKG):
 METRIC = "PCG-MG solve s & MDOF·iter/s, mixed vs FP64 GPU at ≤1e-6 warpage err; HBM GB/s"
 UNIT = "MDOF·iter/s"
 WORKLOAD = "lidded_c2 160x160x32 (8-2-8 layered substrate, die, TIM, Cu hat lid), 150->25 degC step, tol 1e-8"
-DOMINANT = "sweep_solid"   # the level-0 z-column smoother: largest share of the ncu launch list
+DOMINANT = "sweep_solid"   # the level-0 z-column smoother: the largest bandwidth-bound share of the ncu launch list
 
 
 def parse():
@@ -43,12 +43,15 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--inplane", type=int, default=160)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile", action="store_true", help="one assemble + one solve only (for ncu captures); prints no bench line")
+    ap.add_argument("--profile", action="store_true",
+                    help="a warm-up assemble + solve, then one assemble + solve (for ncu captures); prints no bench line")
     return ap.parse_args()
 
 
 def run_profile(a):
-    """The smallest run of the hot path for ncu: model creation, one assembly, one solve."""
+    """The smallest run of the hot path for ncu: model creation, then two steps of one assembly and
+    one solve each. The first step builds what a hierarchy builds once (the launch-shape tuning, the
+    captured V-cycle); the second is the step the launch list summarises (from its k_assemble on)."""
     import torch
     from tmsolve.packages import lidded_c2
     from tmsolve.solver import DeviceModel
@@ -57,8 +60,9 @@ def run_profile(a):
     dm = DeviceModel(pkg)
     f = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
     u = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
-    dm.assemble_step_device(pkg.step(), f.data_ptr())
-    r = dm.solve_device(f.data_ptr(), u.data_ptr(), tol=1e-8, warm=0, key=1, precision=a.precision)
+    for key in (1, 2):
+        dm.assemble_step_device(pkg.step(), f.data_ptr())
+        r = dm.solve_device(f.data_ptr(), u.data_ptr(), tol=1e-8, warm=0, key=key, precision=a.precision)
     torch.cuda.synchronize()
     print(json.dumps({"profile": True, "dof": dm.ndof, "iters": r["iters"], "converged": r["converged"], "ms": r["ms"]}))
 
@@ -291,8 +295,8 @@ def run_ours(a):
     hbm, hbm_kind = peaks()
     achieved = per_launch / (kms / kcount / 1e3) / 1e9 if kcount else None
     traffic = profile_traffic(DOMINANT, a.precision)
-    kname = ("k_sweep_tma (level-0 z-column smoother, one colour: operator rows streamed by TMA through shared memory, "
-             "block-tridiagonal column solves per SM run)") if a.precision == "mixed" else \
+    kname = ("k_sweep_tma (level-0 z-column smoother, one colour: position-major operator rows streamed by TMA bulk copies "
+             "through shared memory, block-tridiagonal column solves per SM run)") if a.precision == "mixed" else \
         "k_sweep_panel<double> (level-0 z-column block-tridiagonal smoother on packed column panels, one colour)"
     roof = {"kernel": kname, "bound": "hbm", "achieved": achieved,
             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None, "traffic": traffic,
