@@ -356,8 +356,12 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
                                                       const T* __restrict__ b, const T* __restrict__ x, bool zeroGuess,
                                                       T* part, T* r, int* rp) {
   const int m = 6 * na;
+  // the column's b is loaded with the block rows, not after them
+  const T* bc = b + 6 * (size_t)n0;
+  const T bo0 = lane < m ? bc[lane] : (T)0, bo1 = lane + 32 < m ? bc[lane + 32] : (T)0;
+  auto bval = [&](int e) { return e == lane ? bo0 : e == lane + 32 ? bo1 : bc[e]; };
   if (zeroGuess) {
-    for (int e = lane; e < m; e += 32) r[e] = b[6 * (size_t)n0 + e];
+    for (int e = lane; e < m; e += 32) r[e] = bval(e);
     __syncwarp();
     return;
   }
@@ -374,7 +378,7 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
   __syncwarp();
   for (int e = lane; e < m; e += 32) {
     const int a = e / 6, p = e % 6;
-    T s = b[6 * (size_t)n0 + e];
+    T s = bval(e);
     for (int k = rp[a]; k < rp[a + 1]; k++) s -= part[6 * k + p];
     r[e] = s;
   }
@@ -382,9 +386,11 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
 }
 
 // one column of a shell-level sweep by one warp: r = b - K x over the column's rows, then
-// x_col += A_cc^-1 r with the explicit inverse Ai (entry (e, k) at k*m + e). For blocks of at most
-// SH_PRE rows every lane fetches its row of the inverse before the residual, so that those loads
-// overlap the residual's.
+// x_col += A_cc^-1 r with the explicit inverse Ai (entry (e, k) at k*m + e). Every lane fetches
+// its row of the inverse (blocks of at most SH_PRE rows) and its entries of the column's own x
+// before the residual, so that those loads overlap the residual's instead of following it: no
+// other warp writes this column's x during the launch (a colour's columns do not couple), and
+// this warp writes it only at the end.
 template <class T>
 __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* __restrict__ Ai, const int* __restrict__ rowPtr,
                                                    const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ b,
@@ -394,6 +400,8 @@ __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* _
   const bool pre = m <= SH_PRE;
 #pragma unroll
   for (int k = 0; k < SH_PRE; k++) a[k] = (pre && lane < m && k < m) ? Ai[(size_t)k * m + lane] : (T)0;
+  T* xc = x + 6 * (size_t)n0;
+  const T xo0 = lane < m ? xc[lane] : (T)0, xo1 = lane + 32 < m ? xc[lane + 32] : (T)0;
   shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, zeroGuess, part, r, rp);
   if (pre) {
     if (lane < m) {
@@ -401,7 +409,7 @@ __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* _
 #pragma unroll
       for (int k = 0; k < SH_PRE; k++)
         if (k < m) acc += a[k] * r[k];
-      x[6 * (size_t)n0 + lane] += acc;
+      xc[lane] = xo0 + acc;
     }
     return;
   }
@@ -409,7 +417,7 @@ __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* _
     T acc = 0;
 #pragma unroll 6
     for (int k = 0; k < m; k++) acc += Ai[(size_t)k * m + e] * r[k];
-    x[6 * (size_t)n0 + e] += acc;
+    xc[e] = (e == lane ? xo0 : e == lane + 32 ? xo1 : xc[e]) + acc;
   }
 }
 
