@@ -287,63 +287,43 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     __syncthreads();
     return;
   }
-  // one thread per column: block-tridiagonal forward and backward substitution. A node's 18
-  // factor entries are read as 9 float2 (node rows are 72 bytes, 8-byte aligned), the next node's
-  // ahead of the current node's arithmetic; the backward pass keeps the factors of node l+1 from
-  // the previous iteration. Entry i of a node is pair i/2, component i%2.
+  // one thread per column: block-tridiagonal forward and backward substitution (scalar loads: a
+  // float2 version of the factor reads measured slower, 6.3 against 4.9 µs per launch, as the
+  // 8-byte accesses of neighbouring columns conflict in more banks)
   for (int q = tid; q < c1 - c0; q += blockDim.x) {
     const int cp0 = colPos[c0 + q], len = colPos[c0 + q + 1] - cp0;
-    if (len <= 0) continue;
     float* rr = sr + 3 * (size_t)(cp0 - P0);
-    const float2* Fc = reinterpret_cast<const float2*>(sF + 18 * (size_t)(cp0 - Q0));
-    float2 f[9], fn[9];
-#pragma unroll
-    for (int j = 0; j < 9; j++) f[j] = Fc[j];
+    const float* Fc = sF + 18 * (size_t)(cp0 - Q0);
     float p0v = 0, p1v = 0, p2v = 0;
     for (int l = 0; l < len; l++) {
-      if (l + 1 < len) {
-#pragma unroll
-        for (int j = 0; j < 9; j++) fn[j] = Fc[9 * (l + 1) + j];
-      }
+      const float* f = Fc + 18 * l;
       float b0 = rr[3 * l], b1 = rr[3 * l + 1], b2 = rr[3 * l + 2];
       if (l > 0) {
-        b0 -= f[4].y * p0v + f[5].x * p1v + f[5].y * p2v;   // entries 9, 10, 11
-        b1 -= f[6].x * p0v + f[6].y * p1v + f[7].x * p2v;   // 12, 13, 14
-        b2 -= f[7].y * p0v + f[8].x * p1v + f[8].y * p2v;   // 15, 16, 17
+        b0 -= f[9] * p0v + f[10] * p1v + f[11] * p2v;
+        b1 -= f[12] * p0v + f[13] * p1v + f[14] * p2v;
+        b2 -= f[15] * p0v + f[16] * p1v + f[17] * p2v;
       }
-      const float y0 = b0 * f[0].y;                                  // 1
-      const float y1 = (b1 - f[1].y * y0) * f[1].x;                  // 3, 2
-      const float y2 = (b2 - f[3].x * y0 - f[3].y * y1) * f[2].y;    // 6, 7, 5
+      const float y0 = b0 * f[1];
+      const float y1 = (b1 - f[3] * y0) * f[2];
+      const float y2 = (b2 - f[6] * y0 - f[7] * y1) * f[5];
       rr[3 * l] = y0; rr[3 * l + 1] = y1; rr[3 * l + 2] = y2;
       p0v = y0; p1v = y1; p2v = y2;
-#pragma unroll
-      for (int j = 0; j < 9; j++) f[j] = fn[j];
     }
-    float2 g[9];
-#pragma unroll
-    for (int j = 0; j < 9; j++) f[j] = Fc[9 * (len - 1) + j];
     float q0 = 0, q1 = 0, q2 = 0;
     for (int l = len - 1; l >= 0; l--) {
-      if (l > 0) {
-#pragma unroll
-        for (int j = 0; j < 9; j++) fn[j] = Fc[9 * (l - 1) + j];
-      }
+      const float* f = Fc + 18 * l;
       float b0 = rr[3 * l], b1 = rr[3 * l + 1], b2 = rr[3 * l + 2];
-      if (l + 1 < len) {   // g: node l+1
-        b0 -= g[4].y * q0 + g[6].x * q1 + g[7].y * q2;   // entries 9, 12, 15
-        b1 -= g[5].x * q0 + g[6].y * q1 + g[8].x * q2;   // 10, 13, 16
-        b2 -= g[5].y * q0 + g[7].x * q1 + g[8].y * q2;   // 11, 14, 17
+      if (l + 1 < len) {
+        const float* g = Fc + 18 * (l + 1);
+        b0 -= g[9] * q0 + g[12] * q1 + g[15] * q2;
+        b1 -= g[10] * q0 + g[13] * q1 + g[16] * q2;
+        b2 -= g[11] * q0 + g[14] * q1 + g[17] * q2;
       }
-      const float z2 = b2 * f[2].y;                                  // 5
-      const float z1 = (b1 - f[3].y * z2) * f[1].x;                  // 7, 2
-      const float z0 = (b0 - f[1].y * z1 - f[3].x * z2) * f[0].y;    // 3, 6, 1
+      const float z2 = b2 * f[5];
+      const float z1 = (b1 - f[7] * z2) * f[2];
+      const float z0 = (b0 - f[3] * z1 - f[6] * z2) * f[1];
       rr[3 * l] = z0; rr[3 * l + 1] = z1; rr[3 * l + 2] = z2;
       q0 = z0; q1 = z1; q2 = z2;
-#pragma unroll
-      for (int j = 0; j < 9; j++) {
-        g[j] = f[j];
-        f[j] = fn[j];
-      }
     }
   }
   __syncthreads();
