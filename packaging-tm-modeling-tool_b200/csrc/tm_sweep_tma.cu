@@ -8,10 +8,10 @@
 //    (cp.async.bulk, no multicast) of the position-major copies of the operator and the ids (a
 //    chunk is one contiguous range of each), completing on an mbarrier, in a ring of stages so
 //    that the loads of later chunks are in flight while a chunk's residual rows are computed;
-//  * r starts as the run's b in shared memory; two warp groups take alternate chunks (one
-//    group's gathers of x overlap the other's); in a group 4 threads per position take the 27
-//    slots (a warp takes 32 consecutive positions of one slot group, conflict-free), their
-//    partial rows are added in a fixed order and subtracted from r;
+//  * two warp groups take alternate chunks (one group's gathers of x overlap the other's); in a
+//    group 4 threads per position take the 27 slots (a warp takes 32 consecutive positions of one
+//    slot group, conflict-free), their partial rows are added in a fixed order and the run's
+//    residual rows r = b - K x are written to shared memory (b fetched by the chunk itself);
 //  * the run's column factors then arrive with one bulk copy into the freed stage memory;
 //  * one thread per column then runs the block-tridiagonal forward/backward substitution and
 //    the run's x is updated (on the cycle's first sweep, x is assigned and the other colours'
@@ -180,10 +180,11 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     for (int q = 0; q < TS_MAXSTAGE; q++) s_last[q] = -1;
     for (int q = 0; q < nstage && q < nchunks; q++) issue(q);
   }
-  // r starts as b (the chunks subtract K x); a thread takes up to TS_ILP positions and issues
-  // their loads together (the node ids, then b), so that the gathers' latencies overlap
+  // r = b - K x: each chunk loads its positions' b while it waits for its stage and computes, and
+  // writes r once. On the cycle's first sweep (x = 0, no chunks) r = b, loaded here: a thread
+  // takes up to TS_ILP positions and issues their loads together (the node ids, then b)
   const int nrun = P1 - P0;
-  for (int l0 = tid; l0 < nrun; l0 += TS_ILP * blockDim.x) {
+  for (int l0 = tid; zeroGuess && l0 < nrun; l0 += TS_ILP * blockDim.x) {
     size_t nd[TS_ILP];
     float v[TS_ILP][3];
 #pragma unroll
@@ -210,6 +211,10 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
   const int pl = gtid % TS_CHUNK, sub = gtid / TS_CHUNK;
   float* gred = red + (size_t)grp * TS_TPP * TS_CHUNK * 3;
   for (int k = grp; k < nchunks; k += TS_GROUPS) {
+    // b of the position and component this thread adds the partial rows of (see below)
+    const int rq = gtid / 3, rc = gtid % 3, rp = Q0 + k * TS_CHUNK + rq;
+    const bool rlive = gtid < 3 * TS_CHUNK && rp >= P0 && rp < P1;
+    const float bv = rlive ? b[3 * (size_t)posNode[rp] + rc] : 0.f;
     // the chunk's loads must have been issued before its stage is waited on: the previous chunk
     // of the stage belongs to the other group, and a wait one phase early would see that phase
     bool ok = false;
@@ -249,15 +254,12 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
       fence_proxy_async();   // the stage being refilled was last read by the threads
       issue(k + nstage);
     }
-    // the slot groups' partial rows of a position, added in group order
-    if (gtid < 3 * TS_CHUNK) {
-      const int pq = gtid / 3, q = gtid % 3, pp = Q0 + k * TS_CHUNK + pq;
-      if (pp >= P0 && pp < P1) {
-        float acc = gred[3 * pq + q];
+    // the slot groups' partial rows of a position, added in group order: r = b - (K x)
+    if (rlive) {
+      float acc = gred[3 * rq + rc];
 #pragma unroll
-        for (int g = 1; g < TS_TPP; g++) acc += gred[3 * (g * TS_CHUNK + pq) + q];
-        sr[3 * (pp - P0) + q] -= acc;
-      }
+      for (int g = 1; g < TS_TPP; g++) acc += gred[3 * (g * TS_CHUNK + rq) + rc];
+      sr[3 * (rp - P0) + rc] = bv - acc;
     }
     group_sync(grp);
   }
