@@ -404,6 +404,22 @@ typedef struct {
   const double* subD;
   const double* subF;
   double nuMax, zt, zaf;
+  /* homogenized-layer consistency mode, BumpSubmodel opts.uniformMaterial (13-fatigue.js:538,
+   * 556, 711-748, 757; the V7 check), 0: off. The bump layer's solder and underfill cells become
+   * one material: solder columns (columnD) and underfill (isoD clamped at nuMaxGlobal) with
+   * volume fractions density and 1 - density. Every substrate element layer takes the step-mean
+   * stiffness of the top substrate band's sub-layer at its mid-height, with the band's
+   * through-thickness response (Voigt thickness modulus, Turner-weighted thermal strain). The band
+   * section (buildBandSection, 04-homogenize.js:139-183): nsec sub-layers, secZ (z0, z1 per
+   * sub-layer, ascending), secD (36 x TGRID_N per sub-layer: its shell stiffness table), secF
+   * (3 x TGRID_N per sub-layer: its thermal strain table). There are no Anand points in this
+   * mode: tm_submodel_step works, tm_submodel_run refuses. */
+  int32_t uniformMaterial;
+  double density, nuMaxGlobal;
+  int32_t nsec;
+  const double* secZ;
+  const double* secD;
+  const double* secF;
 } tm_submodel_spec;
 typedef struct tm_sub tm_sub;
 tm_status tm_submodel_create(const tm_submodel_spec* spec, tm_sub** out);

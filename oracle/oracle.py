@@ -76,8 +76,9 @@ def lib():
     L.orc_sub_create.restype = vp
     L.orc_sub_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _ip, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int, _ip,
                                  _dp, _dp, _dp, _dp, C.c_int, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, C.c_double,
-                                 C.c_double, C.c_double]
+                                 C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp]
     L.orc_sub_destroy.argtypes = [vp]
+    L.orc_sub_elastic.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp]
     L.orc_sub_sizes.argtypes = [vp, _ip]
     L.orc_sub_step.argtypes = [vp, C.c_double, C.c_double, _ip, _dp]
     L.orc_sub_get_u.argtypes = [vp, _dp]
@@ -295,7 +296,8 @@ class OracleSubmodel:
                                   spec.nglob, len(spec.ts), f(spec.ts), f(spec.fields), f(spec.u25), nb, i32(spec.bGlob).reshape(-1),
                                   f(spec.bW).reshape(-1), f(spec.anand), f(spec.solder_E), f(spec.solder_F), int(spec.elastic_solder),
                                   f(spec.uf_E), f(spec.uf_F), float(spec.uf_nu), f(spec.si_D), f(spec.si_F), f(spec.sub_D),
-                                  f(spec.sub_F), float(spec.nu_max), float(spec.zt), float(spec.zaf))
+                                  f(spec.sub_F), float(spec.nu_max), float(spec.zt), float(spec.zaf), int(spec.uniform),
+                                  float(spec.density), float(spec.nu_max_global), spec.nsec, *spec.section_arrays())
         if not self.h:
             raise ValueError("boundary node count does not match the cell")
         sz = np.zeros(4, np.int32)
@@ -307,6 +309,13 @@ class OracleSubmodel:
         if getattr(self, "h", None):
             lib().orc_sub_destroy(self.h)
             self.h = None
+
+    def elastic(self, mat, Ta, Tb, sub_z=0.0):
+        """_elastic (13-fatigue.js:702-757) of material mat (0 substrate, 1 solder, 2 underfill,
+        3 silicon) over the step from Ta to Tb: (D 36, thermal stress increment 6)."""
+        D, sth = np.zeros(36), np.zeros(6)
+        lib().orc_sub_elastic(self.h, int(mat), float(sub_z), float(Ta), float(Tb), D, sth)
+        return D, sth
 
     def step(self, T, dt):
         """stepTo (13-fatigue.js:924-956): (converged, newton, dMax)."""

@@ -1855,7 +1855,23 @@ struct SubInput {
   dvec ufE, ufF; double ufNu = 0.35;
   dvec siD, siF; dvec subD, subF;
   double nuMax = 0.49, zt = 0, zaf = 0;
+  // homogenized-layer consistency mode (opts.uniformMaterial, 13-fatigue.js:516, 538, 556,
+  // 711-748, 757): solder volume fraction of the bump layer (die.density), the global Poisson
+  // clamp, and the top substrate band's section (buildBandSection, 04-homogenize.js:139-183):
+  // per sub-layer its z range, shell stiffness table (36 x TGRID_N) and thermal strain table
+  // (3 x TGRID_N)
+  int uniform = 0; double density = 0, nuMaxGlobal = 0.45;
+  int nsec = 0; dvec secZ, secD, secF;
 };
+
+// columnD (03-materials.js:259-266): the solder phase as separate columns, in-plane terms at
+// COLUMN_INPLANE_FRACTION (00-constants.js:25) of the axial ones
+void columnD(double E, double nu, double* out) {
+  const double fl = 1e-3, G = E / (2 * (1 + nu));
+  for (int q = 0; q < 36; q++) out[q] = 0;
+  out[0] = out[7] = fl * E; out[21] = fl * G;
+  out[14] = E; out[28] = G; out[35] = G;
+}
 
 struct Submodel {
   enum { SUB = 0, SOLDER = 1, UF = 2, SI = 3 };
@@ -1871,12 +1887,18 @@ struct Submodel {
   dvec u, uN, sigE, eFn, eK, eF, val, vals, s_;
   double Tn = 25;
   bool haveStepKey = false; double keyTn = 0, keyT = 0;
-  bool elasValid[4] = {false, false, false, false}; double elasD[4][36], elasS[4][6];
+  // step records of the elastic materials: 4 materials, then (consistency mode) one per
+  // substrate element layer
+  std::vector<char> elasValid; dvec elasD, elasS;
   std::unique_ptr<ICPC> pc; bool pcStale = false; int pcIters = 0;
 
   explicit Submodel(const SubInput& inp) : in(inp) {
     m.nx = in.nx; m.ny = in.ny; m.nz = in.nz; m.xs = in.xs; m.ys = in.ys; m.zs = in.zs;
     const int ncells = (in.nx - 1) * (in.ny - 1) * (in.nz - 1);
+    // consistency mode: the bump layer's phases are one homogenized material (13-fatigue.js:538)
+    if (in.uniform)
+      for (int& c : in.cellMat)
+        if (c == SOLDER) c = UF;
     ivec cg(2 * ncells, -1), cp(2 * ncells, 0); dvec cs(2 * ncells, 0.0);
     for (int c = 0; c < ncells; c++) { cg[2 * c] = in.cellMat[c]; cp[2 * c] = in.cellMat[c]; cs[2 * c] = 1; }
     buildStructuredMesh(m, cg.data(), cp.data(), cs.data());
@@ -1924,6 +1946,8 @@ struct Submodel {
         eBb[e] = idx;
       } else eBb[e] = it->second;
     }
+    const int nrec = 4 + (in.nz - 1);
+    elasValid.assign(nrec, 0); elasD.assign(36 * (size_t)nrec, 0.0); elasS.assign(6 * (size_t)nrec, 0.0);
     u.assign(ndof, 0.0); uN.assign(ndof, 0.0);
     sigE.assign((size_t)m.ne * 48, 0.0); eFn.assign((size_t)m.ne * 24, 0.0);
     eK.assign((size_t)m.ne * 576, 0.0); eF.assign((size_t)m.ne * 24, 0.0);
@@ -1949,9 +1973,25 @@ struct Submodel {
     }
   }
 
-  // _elastic (13-fatigue.js:702-757) without the homogenized-layer consistency mode
-  void elastic(int mat, double Ta, double Tb, double* D, double* sth) const {
+  // _elastic (13-fatigue.js:702-757); subZ: the element layer's mid-height for the substrate
+  // slice in the consistency mode
+  void elastic(int mat, double Ta, double Tb, double* D, double* sth, double subZ = 0) const {
     auto rowSum = [&](int r) { return D[r * 6] + D[r * 6 + 1] + D[r * 6 + 2]; };
+    auto rowSumOf = [](const double* Dx, int r) { return Dx[r * 6] + Dx[r * 6 + 1] + Dx[r * 6 + 2]; };
+    if (in.uniform && mat == UF) {
+      // solder columns (columnD) and underfill superposed with volume fractions fb, 1 - fb
+      const double fb = in.density;
+      double Es, Eu, Ds[36], Du[36];
+      gridMean(in.solderE.data(), 1, 1, Ta, Tb, &Es);
+      gridMean(in.ufE.data(), 1, 1, Ta, Tb, &Eu);
+      columnD(Es, in.anand.nu, Ds);
+      isoD(Eu, in.ufNu, in.nuMaxGlobal, Du);
+      const double fs = gridModulusStrainIncrement(in.solderE.data(), in.solderF.data(), Ta, Tb) / Es;
+      const double fu = gridModulusStrainIncrement(in.ufE.data(), in.ufF.data(), Ta, Tb) / Eu;
+      for (int q = 0; q < 36; q++) D[q] = fb * Ds[q] + (1 - fb) * Du[q];
+      for (int r = 0; r < 6; r++) sth[r] = fb * rowSumOf(Ds, r) * fs + (1 - fb) * rowSumOf(Du, r) * fu;
+      return;
+    }
     auto isoStep = [&](const dvec& E, const dvec& F, double nu) {
       double Em;
       gridMean(E.data(), 1, 1, Ta, Tb, &Em);
@@ -1967,14 +2007,45 @@ struct Submodel {
     }
     if (mat == UF) { isoStep(in.ufE, in.ufF, in.ufNu); return; }
     if (mat == SOLDER) { isoStep(in.solderE, in.solderF, in.anand.nu); return; }
+    if (in.uniform) {
+      // the top band's own sub-layer stiffness at this height, with the through-thickness
+      // response of the whole band: Voigt thickness modulus and Turner-weighted thermal strain
+      const size_t DN = 36 * (size_t)TGRID_N, FN = 3 * (size_t)TGRID_N;
+      int sl = in.nsec - 1;
+      for (int q = 0; q < in.nsec; q++)
+        if (subZ <= in.secZ[2 * q + 1] + 1e-12) { sl = q; break; }
+      gridMean(in.secD.data() + DN * sl, 36, 36, Ta, Tb, D);
+      const double* Fsl = in.secF.data() + FN * sl;
+      double dF[3];
+      for (int c = 0; c < 2; c++) dF[c] = gridAtS(Fsl, Tb, 3, c) - gridAtS(Fsl, Ta, 3, c);
+      double Ez = 0, EzF = 0, tt = 0, Dq[36], sq[6];
+      for (int q = 0; q < in.nsec; q++) {
+        const double ts = in.secZ[2 * q + 1] - in.secZ[2 * q];
+        gridMean(in.secD.data() + DN * q, 36, 36, Ta, Tb, Dq);
+        const double* Fq = in.secF.data() + FN * q;
+        const double fx = gridAtS(Fq, Tb, 3, 0) - gridAtS(Fq, Ta, 3, 0), fy = gridAtS(Fq, Tb, 3, 1) - gridAtS(Fq, Ta, 3, 1);
+        gridStressIncrement(in.secD.data() + DN * q, Fq, Ta, Tb, sq);
+        Ez += ts * Dq[14]; EzF += ts * (sq[2] - Dq[12] * fx - Dq[13] * fy); tt += ts;
+      }
+      D[14] = Ez / tt; dF[2] = EzF / Ez;
+      for (int r = 0; r < 6; r++) sth[r] = D[r * 6] * dF[0] + D[r * 6 + 1] * dF[1] + D[r * 6 + 2] * dF[2];
+      return;
+    }
     gridMean(in.subD.data(), 36, 36, Ta, Tb, D);
     gridStressIncrement(in.subD.data(), in.subF.data(), Ta, Tb, sth);
   }
 
-  // _elasRec (13-fatigue.js:760-773): per material, cached for the step from Tn to T
-  void elasRec(int mat, double T, const double** D, const double** sth) {
-    if (!elasValid[mat]) { elastic(mat, Tn, T, elasD[mat], elasS[mat]); elasValid[mat] = true; }
-    *D = elasD[mat]; *sth = elasS[mat];
+  // _elasRec (13-fatigue.js:760-773): per material (per substrate layer in the consistency
+  // mode), cached for the step from Tn to T
+  void elasRec(int e, double T, const double** D, const double** sth) {
+    const int mat = m.eGroup[e], k = m.eIJK[3 * e + 2];
+    const bool perLayer = in.uniform && mat == SUB;
+    const int key = perLayer ? 4 + k : mat;
+    if (!elasValid[key]) {
+      elastic(mat, Tn, T, &elasD[36 * (size_t)key], &elasS[6 * (size_t)key], perLayer ? 0.5 * (m.zs[k] + m.zs[k + 1]) : 0);
+      elasValid[key] = 1;
+    }
+    *D = &elasD[36 * (size_t)key]; *sth = &elasS[6 * (size_t)key];
   }
 
   // assemble (13-fatigue.js:776-853): tangent (wantK) and internal force at u; returns max dEbar
@@ -1982,7 +2053,7 @@ struct Submodel {
     if (wantK) std::fill(val.begin(), val.end(), 0.0);
     std::fill(rint.begin(), rint.end(), 0.0);
     const bool fresh = !(haveStepKey && keyTn == Tn && keyT == T);
-    if (fresh) for (auto& v : elasValid) v = false;
+    if (fresh) std::fill(elasValid.begin(), elasValid.end(), 0);
     AnandPoint kAn(in.anand, in.solderE.data());
     const StepK kc = kAn.stepConstants(T, dt);
     const double fSolder = gridAt(in.solderF.data(), T) - gridAt(in.solderF.data(), 25);
@@ -1996,7 +2067,7 @@ struct Submodel {
         double* Kc = eK.data() + 576 * (size_t)e; double* fc = eF.data() + 24 * (size_t)e;
         if (fresh) {
           const double *D, *sth;
-          elasRec(m.eGroup[e], T, &D, &sth);
+          elasRec(e, T, &D, &sth);
           std::fill(Kc, Kc + 576, 0.0); std::fill(fc, fc + 24, 0.0);
           for (int g = 0; g < 8; g++) {
             const double* Bb = Ball + 144 * g;
@@ -2048,7 +2119,7 @@ struct Submodel {
     for (int e = 0; e < m.ne; e++) {
       if (anand[(size_t)e * 8]) continue;
       const double *D, *sth;
-      elasRec(m.eGroup[e], T, &D, &sth);
+      elasRec(e, T, &D, &sth);
       const double* Ball = bbB[eBb[e]].data(); const double w = bbW[eBb[e]];
       for (int a = 0; a < 8; a++) { const int n = m.conn[8 * e + a]; for (int c = 0; c < 3; c++) due[3 * a + c] = u[3 * n + c] - uN[3 * n + c]; }
       double* fn = eFn.data() + 24 * (size_t)e;
@@ -2595,7 +2666,8 @@ orc_sub* orc_sub_create(int nx, int ny, int nz, const double* xs, const double* 
                         int nglob, int nt, const double* ts, const double* fields, const double* u25, int nb, const int* bGlob,
                         const double* bW, const double* anand, const double* solderE, const double* solderF, int elasticSolder,
                         const double* ufE, const double* ufF, double ufNu, const double* siD, const double* siF, const double* subD,
-                        const double* subF, double nuMax, double zt, double zaf) {
+                        const double* subF, double nuMax, double zt, double zaf, int uniform, double density, double nuMaxGlobal,
+                        int nsec, const double* secZ, const double* secD, const double* secF) {
   SubInput in;
   in.nx = nx; in.ny = ny; in.nz = nz;
   in.xs.assign(xs, xs + nx); in.ys.assign(ys, ys + ny); in.zs.assign(zs, zs + nz);
@@ -2610,6 +2682,14 @@ orc_sub* orc_sub_create(int nx, int ny, int nz, const double* xs, const double* 
   in.siD.assign(siD, siD + 36); in.siF.assign(siF, siF + TGRID_N);
   in.subD.assign(subD, subD + 36 * TGRID_N); in.subF.assign(subF, subF + 3 * TGRID_N);
   in.nuMax = nuMax; in.zt = zt; in.zaf = zaf;
+  in.uniform = uniform; in.density = density; in.nuMaxGlobal = nuMaxGlobal;
+  if (uniform) {
+    if (nsec < 1) return nullptr;
+    in.nsec = nsec;
+    in.secZ.assign(secZ, secZ + 2 * (size_t)nsec);
+    in.secD.assign(secD, secD + 36 * (size_t)TGRID_N * nsec);
+    in.secF.assign(secF, secF + 3 * (size_t)TGRID_N * nsec);
+  }
   auto* o = new orc_sub();
   o->S.reset(new Submodel(in));
   if ((int)o->S->bNodes.size() != nb) { delete o; return nullptr; }
@@ -2617,6 +2697,11 @@ orc_sub* orc_sub_create(int nx, int ny, int nz, const double* xs, const double* 
 }
 
 void orc_sub_destroy(orc_sub* o) { delete o; }
+// _elastic of one material over the step from Ta to Tb (subZ: the layer mid-height for the
+// substrate slice in the consistency mode): D (36) and the thermal stress increment (6)
+void orc_sub_elastic(orc_sub* o, int mat, double subZ, double Ta, double Tb, double* D, double* sth) {
+  o->S->elastic(mat, Ta, Tb, D, sth, subZ);
+}
 // nn, ne, boundary nodes, solder Gauss points
 void orc_sub_sizes(orc_sub* o, int* out) {
   int ns = 0;

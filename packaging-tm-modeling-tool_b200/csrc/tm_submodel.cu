@@ -101,6 +101,16 @@ double grid_modulus_strain_increment(const double* E, const double* F, double Ta
   });
   return sg * s;
 }
+// columnD (03-materials.js:259-266): the solder phase of the bump layer as separate columns,
+// in-plane terms at COLUMN_INPLANE_FRACTION (00-constants.js:25) of the axial ones
+void column_d(double E, double nu, double* out) {
+  const double fl = 1e-3, G = E / (2 * (1 + nu));
+  for (int q = 0; q < 36; q++) out[q] = 0;
+  out[0] = out[7] = fl * E;
+  out[21] = fl * G;
+  out[14] = E; out[28] = G; out[35] = G;
+}
+
 // isoD through isoEC and orthoD (03-materials.js:222-249), invDense (01-util.js:110-134)
 void iso_d(double E, double nu, double nuMax, double* out) {
   const double nc = std::min(nu, nuMax);
@@ -555,7 +565,15 @@ struct SubModel {
   double ufNu = 0, nuMax = 0, zt = 0, zaf = 0;
   AnandConst P{};
   int elasticSolder = 0;
-  std::vector<int> conn, eIJK, eMat, eAn, rowPtr, col, diag, blkRow;
+  // homogenized-layer consistency mode: bump-layer solder fraction, global Poisson clamp, the top
+  // substrate band's section (z ranges, stiffness and thermal strain tables per sub-layer)
+  int uniform = 0, nsec = 0;
+  double density = 0, nuMaxGlobal = 0.45;
+  std::vector<double> secZ, secD, secF;
+  // elastic material records: 4 materials, then (consistency mode) one per substrate element layer;
+  // eRec is each element's record (d_eMat on the device)
+  int nrec = 4;
+  std::vector<int> conn, eIJK, eMat, eRec, eAn, rowPtr, col, diag, blkRow;
   std::vector<uint8_t> isC;
   int nglob = 0;
   // device
@@ -590,9 +608,48 @@ struct SubModel {
     TM_CUDA_CHECK(cudaStreamSynchronize(st));
   }
 
-  // _elastic (13-fatigue.js:702-757), without the homogenized-layer consistency mode
-  void elastic(int mat, double Ta, double Tb, double* D, double* sth) const {
+  // _elastic (13-fatigue.js:702-757); subZ: the element layer's mid-height for the substrate
+  // slice in the consistency mode
+  void elastic(int mat, double Ta, double Tb, double* D, double* sth, double subZ = 0) const {
     auto rowSum = [&](int r) { return D[r * 6] + D[r * 6 + 1] + D[r * 6 + 2]; };
+    auto rowSumOf = [](const double* Dx, int r) { return Dx[r * 6] + Dx[r * 6 + 1] + Dx[r * 6 + 2]; };
+    if (uniform && mat == M_UF) {
+      // solder columns (columnD) and underfill superposed with volume fractions fb, 1 - fb
+      double Es, Eu, Ds[36], Du[36];
+      grid_mean(solderE.data(), 1, 1, Ta, Tb, &Es);
+      grid_mean(ufE.data(), 1, 1, Ta, Tb, &Eu);
+      column_d(Es, P.nu, Ds);
+      iso_d(Eu, ufNu, nuMaxGlobal, Du);
+      const double fs = grid_modulus_strain_increment(solderE.data(), solderF.data(), Ta, Tb) / Es;
+      const double fu = grid_modulus_strain_increment(ufE.data(), ufF.data(), Ta, Tb) / Eu;
+      for (int q = 0; q < 36; q++) D[q] = density * Ds[q] + (1 - density) * Du[q];
+      for (int r = 0; r < 6; r++) sth[r] = density * rowSumOf(Ds, r) * fs + (1 - density) * rowSumOf(Du, r) * fu;
+      return;
+    }
+    if (uniform && mat == M_SUB) {
+      // the top band's own sub-layer stiffness at this height, with the through-thickness
+      // response of the whole band: Voigt thickness modulus and Turner-weighted thermal strain
+      const size_t DN = 36 * (size_t)TGRID_N, FN = 3 * (size_t)TGRID_N;
+      int sl = nsec - 1;
+      for (int q = 0; q < nsec; q++)
+        if (subZ <= secZ[2 * q + 1] + 1e-12) { sl = q; break; }
+      grid_mean(secD.data() + DN * sl, 36, 36, Ta, Tb, D);
+      const double* Fsl = secF.data() + FN * sl;
+      double dF[3];
+      for (int c = 0; c < 2; c++) dF[c] = grid_at_s(Fsl, Tb, 3, c) - grid_at_s(Fsl, Ta, 3, c);
+      double Ez = 0, EzF = 0, tt = 0, Dq[36], sq[6];
+      for (int q = 0; q < nsec; q++) {
+        const double tq = secZ[2 * q + 1] - secZ[2 * q];
+        grid_mean(secD.data() + DN * q, 36, 36, Ta, Tb, Dq);
+        const double* Fq = secF.data() + FN * q;
+        const double fx = grid_at_s(Fq, Tb, 3, 0) - grid_at_s(Fq, Ta, 3, 0), fy = grid_at_s(Fq, Tb, 3, 1) - grid_at_s(Fq, Ta, 3, 1);
+        grid_stress_increment(secD.data() + DN * q, Fq, Ta, Tb, sq);
+        Ez += tq * Dq[14]; EzF += tq * (sq[2] - Dq[12] * fx - Dq[13] * fy); tt += tq;
+      }
+      D[14] = Ez / tt; dF[2] = EzF / Ez;
+      for (int r = 0; r < 6; r++) sth[r] = D[r * 6] * dF[0] + D[r * 6 + 1] * dF[1] + D[r * 6 + 2] * dF[2];
+      return;
+    }
     auto isoStep = [&](const std::vector<double>& E, const std::vector<double>& F, double nu) {
       double Em;
       grid_mean(E.data(), 1, 1, Ta, Tb, &Em);
@@ -634,11 +691,7 @@ struct SubModel {
   // assemble (13-fatigue.js:776-853); returns the largest plastic increment
   double assemble(double T, double dt, bool wantK) {
     const bool fresh = !(haveKey && keyTn == Tn && keyT == T);
-    if (fresh) {
-      double h[4 * 42];
-      for (int m = 0; m < 4; m++) elastic(m, Tn, T, h + 42 * m, h + 42 * m + 36);
-      d_elas.upload(h, 4 * 42, st);
-    }
+    if (fresh) upload_records(T);
     // the solder constants of the step and its thermal strain from 25 degC
     const double E = grid_at_s(solderE.data(), T, 1, 0), nu = P.nu;
     const double expQ = std::exp(P.QR / (T + 273.15));
@@ -709,13 +762,18 @@ struct SubModel {
     return it;
   }
 
+  // the elastic material records of the step from Tn to T (_elasRec, 13-fatigue.js:760-773): the
+  // 4 materials, then per substrate element layer in the consistency mode
+  void upload_records(double T) {
+    std::vector<double> h(42 * (size_t)nrec, 0.0);
+    for (int m = 0; m < 4; m++) elastic(m, Tn, T, &h[42 * m], &h[42 * m + 36]);
+    for (int k = 0; k + 4 < nrec; k++) elastic(M_SUB, Tn, T, &h[42 * (4 + k)], &h[42 * (4 + k) + 36], 0.5 * (zs[k] + zs[k + 1]));
+    d_elas.upload(h, st);
+  }
+
   void commit_elastic(double T) {
     // the step's material records are those of the assembly from Tn to T
-    if (!(haveKey && keyTn == Tn && keyT == T)) {
-      double h[4 * 42];
-      for (int m = 0; m < 4; m++) elastic(m, Tn, T, h + 42 * m, h + 42 * m + 36);
-      d_elas.upload(h, 4 * 42, st);
-    }
+    if (!(haveKey && keyTn == Tn && keyT == T)) upload_records(T);
     note_launch();
     k_sub_commit_elastic<<<blocks_for(ne, SA_WARPS), 32 * SA_WARPS, 0, st>>>(ne, d_conn.p, d_eMat.p, d_eBb.p, d_Bm.p, d_Bw.p, d_eAn.p, d_u.p,
                                                                             d_uN.p, d_elas.p, d_sigE.p, d_eFn.p);
@@ -874,6 +932,18 @@ SubModel* submodel_create(const tm_submodel_spec& sp) {
   m.siD.assign(sp.siD, sp.siD + 36); m.siF.assign(sp.siF, sp.siF + TGRID_N);
   m.subD.assign(sp.subD, sp.subD + 36 * TGRID_N); m.subF.assign(sp.subF, sp.subF + 3 * TGRID_N);
   m.ufNu = sp.ufNu; m.nuMax = sp.nuMax; m.zt = sp.zt; m.zaf = sp.zaf;
+  if (sp.uniformMaterial) {
+    if (sp.nsec < 1 || !sp.secZ || !sp.secD || !sp.secF) fail(TM_BAD_INPUT, "submodel: the consistency mode needs the band section");
+    if (!(sp.density >= 0 && sp.density <= 1)) fail(TM_BAD_INPUT, "submodel: bump density outside [0, 1]");
+    m.uniform = 1;
+    m.density = sp.density;
+    m.nuMaxGlobal = sp.nuMaxGlobal;
+    m.nsec = sp.nsec;
+    m.secZ.assign(sp.secZ, sp.secZ + 2 * (size_t)sp.nsec);
+    m.secD.assign(sp.secD, sp.secD + 36 * (size_t)TGRID_N * sp.nsec);
+    m.secF.assign(sp.secF, sp.secF + 3 * (size_t)TGRID_N * sp.nsec);
+    m.nrec = 4 + (sp.nz - 1);
+  }
   m.P = AnandConst{sp.solder.A, sp.solder.QR, sp.solder.xi, sp.solder.m, sp.solder.shat, sp.solder.n, sp.solder.h0, sp.solder.a,
                    sp.solder.s0, sp.solder.nu};
   m.elasticSolder = sp.elasticSolder;
@@ -884,13 +954,15 @@ SubModel* submodel_create(const tm_submodel_spec& sp) {
   m.ne = (nx - 1) * ncy * ncz;
   m.ndof = 3 * m.nn;
   const int LOC[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
-  m.conn.resize(8 * (size_t)m.ne); m.eIJK.resize(3 * (size_t)m.ne); m.eMat.resize(m.ne); m.eAn.assign(m.ne, -1);
+  m.conn.resize(8 * (size_t)m.ne); m.eIJK.resize(3 * (size_t)m.ne); m.eMat.resize(m.ne); m.eRec.resize(m.ne); m.eAn.assign(m.ne, -1);
   for (int i = 0, e = 0; i < nx - 1; i++)
     for (int j = 0; j < ncy; j++)
       for (int k = 0; k < ncz; k++, e++) {
-        const int mat = sp.cellMat[e];
+        int mat = sp.cellMat[e];
         if (mat < 0 || mat > 3) fail(TM_BAD_INPUT, "submodel: cell material out of range");
+        if (m.uniform && mat == M_SOLDER) mat = M_UF;   // the bump layer's phases homogenized (13-fatigue.js:538)
         m.eMat[e] = mat;
+        m.eRec[e] = m.uniform && mat == M_SUB ? 4 + k : mat;
         m.eIJK[3 * e] = i; m.eIJK[3 * e + 1] = j; m.eIJK[3 * e + 2] = k;
         for (int a = 0; a < 8; a++) m.conn[8 * (size_t)e + a] = ((i + LOC[a][0]) * ny + j + LOC[a][1]) * nz + k + LOC[a][2];
         if (mat == M_SOLDER && !m.elasticSolder) m.eAn[e] = m.nsolderE++;
@@ -992,7 +1064,7 @@ SubModel* submodel_create(const tm_submodel_spec& sp) {
   }
   // device copies and state
   cudaStream_t st = m.st;
-  m.d_conn.upload(m.conn, st); m.d_eMat.upload(m.eMat, st); m.d_eBb.upload(eBb, st); m.d_eAn.upload(m.eAn, st);
+  m.d_conn.upload(m.conn, st); m.d_eMat.upload(m.eRec, st); m.d_eBb.upload(eBb, st); m.d_eAn.upload(m.eAn, st);
   m.d_rowPtr.upload(m.rowPtr, st); m.d_col.upload(m.col, st); m.d_diag.upload(m.diag, st); m.d_blkRow.upload(m.blkRow, st);
   m.d_blkStart.upload(bcnt, st); m.d_blkList.upload(blist, st); m.d_nodeStart.upload(ncnt, st); m.d_nodeList.upload(nlist, st);
   m.d_bNodes.upload(bNodes, st); m.d_bGlob.upload(sp.bGlob, 8 * (size_t)sp.nb, st); m.d_bW.upload(sp.bW, 8 * (size_t)sp.nb, st);

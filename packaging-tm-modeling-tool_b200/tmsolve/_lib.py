@@ -79,7 +79,8 @@ class TmSubmodelSpec(C.Structure):
                 ("nglob", C.c_int32), ("nt", C.c_int32), ("ts", dp), ("fields", dp), ("u25", dp), ("nb", C.c_int32),
                 ("bGlob", ip), ("bW", dp), ("solder", TmAnandMaterial), ("elasticSolder", C.c_int32), ("ufE", dp), ("ufF", dp),
                 ("ufNu", C.c_double), ("siD", dp), ("siF", dp), ("subD", dp), ("subF", dp), ("nuMax", C.c_double),
-                ("zt", C.c_double), ("zaf", C.c_double)]
+                ("zt", C.c_double), ("zaf", C.c_double), ("uniformMaterial", C.c_int32), ("density", C.c_double),
+                ("nuMaxGlobal", C.c_double), ("nsec", C.c_int32), ("secZ", dp), ("secD", dp), ("secF", dp)]
 
 
 _lib = None

@@ -24,7 +24,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, load
-from .materials import TGRID_N
+from .materials import NU_MAX_GLOBAL, TGRID_N
 
 SUB_T_AVG = 0.025       # 00-constants.js:114
 SUB_MARGIN = 0.05       # 00-constants.js:115
@@ -190,10 +190,30 @@ class SubmodelSpec:
     zaf: float
     elastic_solder: bool = False
     nu_max: float = NU_MAX_SUBMODEL
+    # homogenized-layer consistency mode (opts.uniformMaterial, 13-fatigue.js:538, 556, 711-748):
+    # the bump layer as one material (solder columns with volume fraction `density`, underfill),
+    # every substrate element layer from the top substrate band's section: per sub-layer its z
+    # range (sec_z, nsec x 2), shell stiffness table (sec_D, nsec x 381 x 36) and thermal strain
+    # table (sec_F, nsec x 381 x 3)
+    uniform: bool = False
+    density: float = 0.0
+    nu_max_global: float = NU_MAX_GLOBAL
+    sec_z: Optional[np.ndarray] = None
+    sec_D: Optional[np.ndarray] = None
+    sec_F: Optional[np.ndarray] = None
 
     @property
     def nglob(self) -> int:
         return self.u25.size // 3
+
+    @property
+    def nsec(self) -> int:
+        return 0 if self.sec_z is None else int(np.asarray(self.sec_z).size // 2)
+
+    def section_arrays(self):
+        """(sec_z, sec_D, sec_F) as contiguous float64 arrays (one zero each without a section)."""
+        f = lambda a: np.ascontiguousarray(np.zeros(1) if a is None else np.asarray(a).reshape(-1), np.float64)
+        return f(self.sec_z), f(self.sec_D), f(self.sec_F)
 
 
 def synthetic_spec(nxy: int = 16, nz: int = 14, site=(2.4, 1.2), shear: float = 2e-5, seed: int = 20261203,
@@ -240,6 +260,31 @@ def synthetic_spec(nxy: int = 16, nz: int = 14, site=(2.4, 1.2), shear: float = 
                         sub_D=sub_D, sub_F=sub_F, zt=zt, zaf=zaf, elastic_solder=elastic_solder)
 
 
+def uniform_spec(spec: SubmodelSpec, density: float = 0.35, seed: int = 20261204) -> SubmodelSpec:
+    """The consistency-mode variant of a spec (opts.uniformMaterial, the V7 check): the bump layer
+    homogenized with solder volume fraction `density`, and a synthetic top substrate band of three
+    sub-layers (a resin layer, a copper-rich layer, a resin layer) whose top is the cell's zt; the
+    sub-layers' shell stiffness tables (isoD clamped at NU_MAX_GLOBAL, then sublayerShellD) and
+    thermal strain tables (in-plane and through-thickness CTEs) on the 1 degC grid."""
+    import dataclasses
+    from .materials import NU_MAX_GLOBAL, T_STRAIN_ORIGIN, TGRID_MIN, grid_table, interp_table_linear, iso_d, sublayer_shell_d
+    rng = np.random.default_rng(seed)
+    zt, z0 = spec.zt, float(spec.zs[0])
+    h = zt - z0
+    bounds = [z0 - 0.5 * h, z0 + 0.4 * h, z0 + 0.75 * h, zt]
+    layers = [(9000.0, 6000.0, 0.35, 45e-6, 60e-6), (60000.0, 52000.0, 0.33, 16e-6, 30e-6), (12000.0, 9000.0, 0.34, 35e-6, 55e-6)]
+    sec_D, sec_F = [], []
+    for (e_lo, e_hi, nu, a_xy, a_z) in layers:
+        j = rng.uniform(0.95, 1.05)
+        E_of = lambda T: j * interp_table_linear([-40.0, 125.0], [e_lo, e_hi], float(T))
+        Dtab = np.concatenate([sublayer_shell_d(iso_d(E_of(TGRID_MIN + i), nu, NU_MAX_GLOBAL)) for i in range(TGRID_N)])
+        Ftab = np.stack([grid_table(lambda T, a=a: a * (T - T_STRAIN_ORIGIN)) for a in (a_xy, a_xy, a_z)], axis=1).reshape(-1)
+        sec_D.append(Dtab); sec_F.append(Ftab)
+    sec_z = np.array([[bounds[q], bounds[q + 1]] for q in range(3)], np.float64)
+    return dataclasses.replace(spec, uniform=True, density=float(density), nu_max_global=NU_MAX_GLOBAL, sec_z=sec_z,
+                               sec_D=np.concatenate(sec_D), sec_F=np.concatenate(sec_F))
+
+
 class DeviceSubmodel:
     """BumpSubmodel on the GPU (tm_submodel_*): step (stepTo), run, and the state readers."""
 
@@ -249,7 +294,7 @@ class DeviceSubmodel:
         i32 = lambda a: np.ascontiguousarray(a, np.int32)
         keep = [f(spec.xs), f(spec.ys), f(spec.zs), i32(spec.cell_mat), f(spec.ts), f(spec.fields), f(spec.u25),
                 i32(spec.bGlob).reshape(-1), f(spec.bW).reshape(-1), f(spec.solder_E), f(spec.solder_F), f(spec.uf_E),
-                f(spec.uf_F), f(spec.si_D), f(spec.si_F), f(spec.sub_D), f(spec.sub_F)]
+                f(spec.uf_F), f(spec.si_D), f(spec.si_F), f(spec.sub_D), f(spec.sub_F), *spec.section_arrays()]
         P = spec.anand
         dpp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
         mat = _lib.TmAnandMaterial(A=P[0], QR=P[1], xi=P[2], m=P[3], shat=P[4], n=P[5], h0=P[6], a=P[7], s0=P[8], nu=P[9],
@@ -260,7 +305,10 @@ class DeviceSubmodel:
                                  u25=dpp(keep[6]), nb=len(spec.bGlob), bGlob=ipp(keep[7]), bW=dpp(keep[8]), solder=mat,
                                  elasticSolder=int(spec.elastic_solder), ufE=dpp(keep[11]), ufF=dpp(keep[12]), ufNu=float(spec.uf_nu),
                                  siD=dpp(keep[13]), siF=dpp(keep[14]), subD=dpp(keep[15]), subF=dpp(keep[16]),
-                                 nuMax=float(spec.nu_max), zt=float(spec.zt), zaf=float(spec.zaf))
+                                 nuMax=float(spec.nu_max), zt=float(spec.zt), zaf=float(spec.zaf),
+                                 uniformMaterial=int(spec.uniform), density=float(spec.density),
+                                 nuMaxGlobal=float(spec.nu_max_global), nsec=spec.nsec, secZ=dpp(keep[17]), secD=dpp(keep[18]),
+                                 secF=dpp(keep[19]))
         h = C.c_void_p()
         check(L.tm_submodel_create(C.byref(sp), C.byref(h)))
         self.h = h

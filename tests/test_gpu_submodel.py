@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from tmsolve.anand import cycle_history
-from tmsolve.submodel import DeviceSubmodel, synthetic_spec
+from tmsolve.submodel import DeviceSubmodel, synthetic_spec, uniform_spec
 
 pytestmark = pytest.mark.gpu
 
@@ -73,3 +73,15 @@ def test_submodel_batch_equals_single_runs(oracle_lib):
             assert recs[q][k] == one[k], (q, k)
         assert np.array_equal(recs[q]["loop"], one["loop"])
 
+
+
+def test_submodel_uniform_matches_oracle(oracle_lib):
+    """The homogenized-layer consistency mode (opts.uniformMaterial, the V7 check) on the GPU:
+    solder cells as the homogenized bump layer, substrate layers from the top band's section."""
+    spec = uniform_spec(synthetic_spec(nxy=6, nz=8))
+    dm, om = DeviceSubmodel(spec), oracle_lib.OracleSubmodel(spec)
+    assert dm.npoints == 0 and om.nsolder == 0
+    for T in (60.0, 125.0, -40.0):
+        g, o = dm.step(T, 60.0), om.step(T, 60.0)
+        assert g[0] and o[0] and abs(g[1] - o[1]) <= 1 and g[2] == 0
+        assert _rel(dm.u(), om.u()) <= 1e-7

@@ -11,8 +11,9 @@
 import numpy as np
 import pytest
 
-from tmsolve.materials import SAC305, anand_params_array, elastic_tables, iso_d, sac305_tables
-from tmsolve.submodel import NU_MAX_SUBMODEL, SubmodelSpec, boundary_weights, synthetic_spec
+from tmsolve.materials import (NU_MAX_GLOBAL, SAC305, TGRID_MIN, anand_params_array, column_d, elastic_tables, iso_d,
+                               sac305_tables)
+from tmsolve.submodel import NU_MAX_SUBMODEL, SubmodelSpec, boundary_weights, synthetic_spec, uniform_spec
 
 GCONN = [0, 4, 6, 2, 1, 5, 7, 3]
 
@@ -97,3 +98,94 @@ def test_submodel_run_small_cell(oracle_lib):
     assert r["dWdie"] > 0 and r["dWsub"] > 0 and r["steps"] >= len(hist["t"]) - 1
     assert r["dW"] == max(r["dWdie"], r["dWsub"])
     assert np.all(np.isfinite(r["loop"][:, 0]))
+
+
+# ---- homogenized-layer consistency mode (opts.uniformMaterial, 13-fatigue.js:538, 711-748) ----
+# A restatement of the grid integrals for whole-degree step ends (03-materials.js:370-418):
+# values at the segment midpoints, by linear interpolation in the 1 degC tables.
+def _at(tab, T, stride=1, comp=0):
+    x = T - TGRID_MIN
+    i = min(int(np.floor(x)), len(tab) // stride - 2)
+    t = x - i
+    return tab[i * stride + comp] + t * (tab[(i + 1) * stride + comp] - tab[i * stride + comp])
+
+
+def _segments(Ta, Tb):
+    lo, hi = min(Ta, Tb), max(Ta, Tb)
+    return [(t0 + 0.5, t0, t0 + 1) for t0 in range(int(lo), int(hi))], (1.0 if Tb >= Ta else -1.0), hi - lo
+
+
+def _mean(tab, Ta, Tb, n=1):
+    seg, _, L = _segments(Ta, Tb)
+    return np.array([sum(_at(tab, tm, n, c) for tm, _, _ in seg) / L for c in range(n)])
+
+
+def _modulus_strain(E, F, Ta, Tb):
+    seg, sg, _ = _segments(Ta, Tb)
+    return sg * sum(_at(E, tm) * (_at(F, t1) - _at(F, t0)) for tm, t0, t1 in seg)
+
+
+def _stress_increment(Dtab, Ftab, Ta, Tb):
+    seg, sg, _ = _segments(Ta, Tb)
+    out = np.zeros(6)
+    for tm, t0, t1 in seg:
+        D = np.array([_at(Dtab, tm, 36, q) for q in range(36)]).reshape(6, 6)
+        dF = np.array([_at(Ftab, t1, 3, c) - _at(Ftab, t0, 3, c) for c in range(3)])
+        out += sg * D[:, :3] @ dF
+    return out
+
+
+@pytest.mark.parametrize("Ta, Tb", [(25, 125), (125, 60), (-40, 25)])
+def test_submodel_uniform_records(oracle_lib, Ta, Tb):
+    """The consistency mode's elastic records against a restatement of _elastic's branches: the
+    bump layer as solder columns (columnD) plus underfill (isoD at NU_MAX_GLOBAL) with volume
+    fractions fb, 1 - fb; each substrate layer as its sub-layer of the top band, with the band's
+    Voigt thickness modulus and Turner-weighted through-thickness thermal strain."""
+    spec = uniform_spec(synthetic_spec(nxy=4, nz=8), density=0.3)
+    om = oracle_lib.OracleSubmodel(spec)
+    assert om.nsolder == 0                      # the solder cells are underfill in this mode
+    # bump layer
+    fb, nu_s = spec.density, spec.anand[9]
+    Es, Eu = _mean(spec.solder_E, Ta, Tb)[0], _mean(spec.uf_E, Ta, Tb)[0]
+    Ds, Du = column_d(Es, nu_s), iso_d(Eu, spec.uf_nu, NU_MAX_GLOBAL)
+    fs = _modulus_strain(spec.solder_E, spec.solder_F, Ta, Tb) / Es
+    fu = _modulus_strain(spec.uf_E, spec.uf_F, Ta, Tb) / Eu
+    Dw = fb * Ds + (1 - fb) * Du
+    sw = np.array([fb * Ds[6 * r:6 * r + 3].sum() * fs + (1 - fb) * Du[6 * r:6 * r + 3].sum() * fu for r in range(6)])
+    D, sth = om.elastic(2, Ta, Tb)
+    assert np.allclose(D, Dw, rtol=1e-12, atol=0) and np.allclose(sth, sw, rtol=1e-12, atol=1e-300)
+    # substrate layers at heights in each sub-layer
+    ns = spec.nsec
+    secD = spec.sec_D.reshape(ns, -1); secF = spec.sec_F.reshape(ns, -1)
+    Dm = [_mean(secD[q], Ta, Tb, 36) for q in range(ns)]
+    Ez = EzF = tt = 0.0
+    for q in range(ns):
+        tq = spec.sec_z[q][1] - spec.sec_z[q][0]
+        fx = _at(secF[q], Tb, 3, 0) - _at(secF[q], Ta, 3, 0)
+        fy = _at(secF[q], Tb, 3, 1) - _at(secF[q], Ta, 3, 1)
+        sq = _stress_increment(secD[q], secF[q], Ta, Tb)
+        Ez += tq * Dm[q][14]; EzF += tq * (sq[2] - Dm[q][12] * fx - Dm[q][13] * fy); tt += tq
+    for q in range(ns):
+        z = 0.5 * (spec.sec_z[q][0] + spec.sec_z[q][1])
+        Dw = Dm[q].copy(); Dw[14] = Ez / tt
+        dF = np.array([_at(secF[q], Tb, 3, 0) - _at(secF[q], Ta, 3, 0), _at(secF[q], Tb, 3, 1) - _at(secF[q], Ta, 3, 1),
+                       EzF / Ez])
+        sw = Dw.reshape(6, 6)[:, :3] @ dF
+        D, sth = om.elastic(0, Ta, Tb, z)
+        assert np.allclose(D, Dw, rtol=1e-12, atol=1e-300), q
+        assert np.allclose(sth, sw, rtol=1e-10, atol=1e-12 * np.abs(sw).max()), q
+    # without the mode the bump layer's underfill is the plain isotropic step
+    D0, _ = oracle_lib.OracleSubmodel(synthetic_spec(nxy=4, nz=8)).elastic(2, Ta, Tb)
+    assert np.allclose(D0, iso_d(Eu, spec.uf_nu, NU_MAX_SUBMODEL), rtol=1e-12, atol=0)
+
+
+def test_submodel_uniform_cell_steps(oracle_lib):
+    """A consistency-mode cell steps like an elastic body: one tangent solve per temperature (the
+    increment test then passes), no plastic work, a finite field that follows the boundary."""
+    spec = uniform_spec(synthetic_spec(nxy=4, nz=8))
+    om = oracle_lib.OracleSubmodel(spec)
+    for T in (60.0, 125.0, -40.0):
+        ok, newton, dmax = om.step(T, 60.0)
+        assert ok and newton <= 3 and dmax == 0
+    u = om.u()
+    assert np.all(np.isfinite(u)) and np.abs(u).max() > 0
