@@ -438,6 +438,16 @@ tm_status tm_submodel_get(tm_sub* sm, double* u, double* W, double* ebar);
  * site's direction from the die centre. A step that fails after 8 cutbacks is TM_NOT_CONVERGED. */
 tm_status tm_submodel_run(tm_sub* sm, int32_t nsteps, const double* t, const double* T, const int32_t* cycle, int32_t cycles,
                           double cphi, double sphi, double* out10, double* perCycle, double* loop);
+/* tm_submodel_run with the result's section record (13-fatigue.js:1053-1078, 1098-1101): phase
+ * (per history point, cycleHistory's phase) marks the ramps and dwells; at the end of each of
+ * them in the last cycle a stress snapshot is taken. *nSnaps counts them; up to maxSnaps are
+ * written: snapMeta (4 each: T, t, cycle, phase) and snapSig (48 floats per element each). */
+tm_status tm_submodel_run_sections(tm_sub* sm, int32_t nsteps, const double* t, const double* T, const int32_t* cycle,
+                                   const int32_t* phase, int32_t cycles, double cphi, double sphi, double* out10, double* perCycle,
+                                   double* loop, int32_t maxSnaps, int32_t* nSnaps, double* snapMeta, float* snapSig);
+/* _stressSnapshot (13-fatigue.js:965-989) of the current state at temperature T: per element the
+ * 8 nodes' 6 stresses (float32), extrapolated from the Gauss points (GP_TO_NODE). */
+tm_status tm_submodel_stress_snapshot(tm_sub* sm, double T, float* out);
 
 /* n submodels over the same history at once (the screened sites of a die): out10, perCycle
  * and loop hold n consecutive records; status[i] is each run's status (TM_OK or the failure),

@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libtmoracle.so")
 
 _dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _lib = None
 
@@ -83,7 +84,8 @@ def lib():
     L.orc_sub_step.argtypes = [vp, C.c_double, C.c_double, _ip, _dp]
     L.orc_sub_get_u.argtypes = [vp, _dp]
     L.orc_sub_get_points.argtypes = [vp, _dp, _dp]
-    L.orc_sub_run.argtypes = [vp, C.c_int, _dp, _dp, _ip, _ip, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp]
+    L.orc_sub_run.argtypes = [vp, C.c_int, _dp, _dp, _ip, _ip, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, C.c_int, _ip, _dp, _fp]
+    L.orc_sub_stress_snapshot.argtypes = [vp, C.c_double, _fp]
     L.orc_last_error.restype = C.c_char_p
     L.orc_last_error.argtypes = [vp]
     _lib = L
@@ -333,18 +335,30 @@ class OracleSubmodel:
         lib().orc_sub_get_points(self.h, W, E)
         return W, E
 
-    def run(self, hist, cphi=1.0, sphi=0.0):
+    def run(self, hist, cphi=1.0, sphi=0.0, max_snaps=0):
         """run (13-fatigue.js:1004-1104): dict of dW, dWdie, dWsub, dE, dEdie, dEsub, stabChange,
-        steps, cutbacks, newtonPerStep, perCycle (cycles x 2), loop (points x 4)."""
+        steps, cutbacks, newtonPerStep, perCycle (cycles x 2), loop (points x 4); with max_snaps,
+        the stress snapshots of the last cycle: snaps_meta (T, t, cycle, phase) and snaps
+        (float32, n x ne x 8 x 6)."""
         n, nc = len(hist["t"]), int(hist["cycles"])
         out = np.zeros(10); pc = np.zeros(2 * nc); loop = np.zeros(4 * n)
+        ns = np.zeros(1, np.int32); meta = np.zeros(4 * max(max_snaps, 1)); sig = np.zeros(48 * self.ne * max(max_snaps, 1), np.float32)
         rc = lib().orc_sub_run(self.h, n, np.ascontiguousarray(hist["t"], np.float64), np.ascontiguousarray(hist["T"], np.float64),
                                np.ascontiguousarray(hist["cycle"], np.int32), np.ascontiguousarray(hist["phase"], np.int32), nc,
-                               float(cphi), float(sphi), out, pc, loop)
+                               float(cphi), float(sphi), out, pc, loop, int(max_snaps), ns, meta, sig)
         if rc:
             raise RuntimeError("submodel run failed")
         keys = ["dW", "dWdie", "dWsub", "dE", "dEdie", "dEsub", "stabChange", "steps", "cutbacks", "newtonPerStep"]
         rec = {k: float(out[i]) for i, k in enumerate(keys)}
         rec["perCycle"] = pc.reshape(nc, 2); rec["loop"] = loop.reshape(n, 4)
+        k = min(int(ns[0]), max_snaps)
+        rec["nsnaps"] = int(ns[0])
+        rec["snaps_meta"] = meta[:4 * k].reshape(k, 4); rec["snaps"] = sig[:48 * self.ne * k].reshape(k, self.ne, 8, 6)
         return rec
+
+    def stress_snapshot(self, T):
+        """_stressSnapshot (13-fatigue.js:965-989) of the current state: float32 (ne, 8, 6)."""
+        out = np.zeros(48 * self.ne, np.float32)
+        lib().orc_sub_stress_snapshot(self.h, float(T), out)
+        return out.reshape(self.ne, 8, 6)
 

@@ -2237,12 +2237,56 @@ struct Submodel {
     }
   }
 
+  // _stressSnapshot (13-fatigue.js:965-989): nodal stresses of every element (48: 8 nodes x 6,
+  // float32) extrapolated from its Gauss points with GP_TO_NODE (07-element.js:227-234): the
+  // committed Gauss-point stresses of elastic elements, and at solder points the stress of the
+  // current displacement at the committed plastic strain (AnandPoint.stressAt, :221-227)
+  void stressSnapshot(double T, float* out) const {
+    double M[64];
+    const double s3 = std::sqrt(3.0);
+    for (int n = 0; n < 8; n++) {
+      const double xi = HEX_XI[n] * s3, eta = HEX_ETA[n] * s3, zeta = HEX_ZETA[n] * s3;
+      for (int g = 0; g < 8; g++) M[n * 8 + g] = 0.125 * (1 + HEX_XI[g] * xi) * (1 + HEX_ETA[g] * eta) * (1 + HEX_ZETA[g] * zeta);
+    }
+    double ue[24], eps[6], gp[48];
+    for (int e = 0; e < m.ne; e++) {
+      const double* Ball = bbB[eBb[e]].data();
+      if (!anand[(size_t)e * 8]) {
+        for (int q = 0; q < 48; q++) gp[q] = sigE[48 * (size_t)e + q];
+      } else {
+        for (int a = 0; a < 8; a++) { const int n = m.conn[8 * e + a]; ue[3 * a] = u[3 * n]; ue[3 * a + 1] = u[3 * n + 1]; ue[3 * a + 2] = u[3 * n + 2]; }
+        for (int g = 0; g < 8; g++) {
+          const double* Bb = Ball + 144 * g;
+          for (int r = 0; r < 6; r++) { double sm = 0; for (int c = 0; c < 24; c++) sm += Bb[r * 24 + c] * ue[c]; eps[r] = sm; }
+          const AnandPoint& pt = *anand[(size_t)e * 8 + g];
+          const double f = gridAt(in.solderF.data(), T) - gridAt(in.solderF.data(), 25);
+          eps[0] -= f; eps[1] -= f; eps[2] -= f;
+          const double E = gridAt(in.solderE.data(), T), nu = in.anand.nu;
+          const double G = E / (2 * (1 + nu)), K = E / (3 * (1 - 2 * nu));
+          const double vol = (eps[0] + eps[1] + eps[2]) / 3, smv = 3 * K * vol;
+          for (int i = 0; i < 3; i++) gp[6 * g + i] = 2 * G * (eps[i] - vol - pt.ep[i]) + smv;
+          for (int i = 3; i < 6; i++) gp[6 * g + i] = 2 * G * (0.5 * eps[i] - pt.ep[i]);
+        }
+      }
+      for (int a = 0; a < 8; a++)
+        for (int c = 0; c < 6; c++) {
+          double v = 0;
+          for (int g = 0; g < 8; g++) v += M[a * 8 + g] * gp[6 * g + c];
+          out[48 * (size_t)e + 6 * a + c] = (float)v;
+        }
+    }
+  }
+
   // run (13-fatigue.js:1004-1104): the cycle history with adaptive sub-steps, the hysteresis
   // sampler of the two interface layers and the per-cycle inelastic work. out (10): dW, dWdie,
   // dWsub, dE, dEdie, dEsub, stabChange, steps, cutbacks, newtonPerStep; perCycle: dWdie, dWsub
-  // per cycle; loop (4 per history point): tau, gamma (die side), tauSub, gammaSub.
+  // per cycle; loop (4 per history point): tau, gamma (die side), tauSub, gammaSub. Stress
+  // snapshots at the end of each ramp and dwell of the last cycle (:1053-1078): *nSnaps of them,
+  // up to maxSnaps written, meta (4 each: T, t, cycle, phase) and 48 ne floats each.
   void run(int nsteps, const double* ht, const double* hT, const int* hcycle, const int* hphase, int cycles, double cphi, double sphi,
-           double* out, double* perCycle, double* loop) {
+           double* out, double* perCycle, double* loop, int maxSnaps = 0, int* nSnaps = nullptr, double* snapMeta = nullptr,
+           float* snapSig = nullptr) {
+    if (nSnaps) *nSnaps = 0;
     struct Rec { int idx; double w; };
     std::vector<Rec> dieLayer, subLayer;
     for (int e = 0; e < m.ne; e++) {
@@ -2308,6 +2352,14 @@ struct Submodel {
       if (!done) throw std::runtime_error("Submodel step failed to converge after cutbacks");
       sampleLoop(T1);
       const int c = hcycle[k];
+      if (nSnaps && c == cycles && (k == nsteps - 1 || hphase[k + 1] != hphase[k])) {
+        const int q = (*nSnaps)++;
+        if (q < maxSnaps) {
+          double* mt = snapMeta + 4 * (size_t)q;
+          mt[0] = T1; mt[1] = t1s; mt[2] = c; mt[3] = hphase[k];
+          stressSnapshot(T1, snapSig + 48 * (size_t)m.ne * q);
+        }
+      }
       Wdie[c] = avg(dieLayer, true); Wsub[c] = avg(subLayer, true);
       Edie[c] = avg(dieLayer, false); Esub[c] = avg(subLayer, false);
     }
@@ -2717,12 +2769,15 @@ void orc_sub_get_points(orc_sub* o, double* W, double* ebar) {
   for (auto& p : o->S->anand) if (p) { W[q] = p->W; ebar[q] = p->ebar; q++; }
 }
 int orc_sub_run(orc_sub* o, int nsteps, const double* t, const double* T, const int* cycle, const int* phase, int cycles, double cphi,
-                double sphi, double* out, double* perCycle, double* loop) {
+                double sphi, double* out, double* perCycle, double* loop, int maxSnaps, int* nSnaps, double* snapMeta, float* snapSig) {
   try {
-    o->S->run(nsteps, t, T, cycle, phase, cycles, cphi, sphi, out, perCycle, loop);
+    o->S->run(nsteps, t, T, cycle, phase, cycles, cphi, sphi, out, perCycle, loop, maxSnaps, nSnaps, snapMeta, snapSig);
     return 0;
   } catch (std::exception& e) { o->err = e.what(); return 1; }
 }
+
+// _stressSnapshot of the current state at temperature T (48 floats per element)
+void orc_sub_stress_snapshot(orc_sub* o, double T, float* out) { o->S->stressSnapshot(T, out); }
 
 // pc.apply(r, z) of the preconditioner the last solve built (scaled space); 1 when none
 int orc_pc_apply(orc_model* o, const double* r, double* z) {

@@ -1290,4 +1290,21 @@ tm_status tm_submodel_run(tm_sub* sm, int32_t nsteps, const double* t, const dou
   });
 }
 
+tm_status tm_submodel_run_sections(tm_sub* sm, int32_t nsteps, const double* t, const double* T, const int32_t* cycle,
+                                   const int32_t* phase, int32_t cycles, double cphi, double sphi, double* out10, double* perCycle,
+                                   double* loop, int32_t maxSnaps, int32_t* nSnaps, double* snapMeta, float* snapSig) {
+  return guarded([&] {
+    if (!sm || !t || !T || !cycle || !phase || !out10 || !perCycle || !loop || !nSnaps) fail(TM_BAD_INPUT, "null argument");
+    submodel_run(*reinterpret_cast<SubModel*>(sm), nsteps, t, T, cycle, cycles, cphi, sphi, out10, perCycle, loop, phase, maxSnaps, nSnaps,
+                 snapMeta, snapSig);
+  });
+}
+
+tm_status tm_submodel_stress_snapshot(tm_sub* sm, double T, float* out) {
+  return guarded([&] {
+    if (!sm || !out) fail(TM_BAD_INPUT, "null argument");
+    submodel_stress_snapshot(*reinterpret_cast<SubModel*>(sm), T, out);
+  });
+}
+
 }  // extern "C"

@@ -402,6 +402,8 @@ bool submodel_step(SubModel& s, double T, double dt, int* newton, double* dMax);
 void submodel_get(SubModel& s, double* u, double* W, double* ebar);
 void submodel_sizes(SubModel& s, int64_t* out);
 void submodel_run(SubModel& s, int nsteps, const double* t, const double* T, const int* cycle, int cycles, double cphi, double sphi,
-                  double* out, double* perCycle, double* loop);
+                  double* out, double* perCycle, double* loop, const int* phase = nullptr, int maxSnaps = 0, int* nSnaps = nullptr,
+                  double* snapMeta = nullptr, float* snapSig = nullptr);
+void submodel_stress_snapshot(SubModel& s, double T, float* out);
 
 }  // namespace tmg

@@ -497,6 +497,56 @@ __global__ void k_sub_commit_points(int np, Point* __restrict__ pts) {
   if (i < np) commit(pts[i]);
 }
 
+// GP_TO_NODE (07-element.js:227-234): nodal value = sum_g N_g(sqrt3 x node natural coords) v_g
+struct GpToNode {
+  double M[64];
+};
+
+// _stressSnapshot (13-fatigue.js:965-989), thread per element: the 48 nodal stresses (float32)
+// extrapolated from the Gauss points: the committed Gauss-point stresses of elastic elements, and
+// at solder points the stress of the current displacement at the committed plastic strain
+// (AnandPoint.stressAt, :221-227); f the solder's thermal strain from 25 degC, E its modulus at T
+__global__ void __launch_bounds__(128) k_sub_stress_snapshot(int ne, const int* __restrict__ conn, const int* __restrict__ eAn,
+                                                             const int* __restrict__ eBb, const double* __restrict__ Bm,
+                                                             const Point* __restrict__ pts, const double* __restrict__ u,
+                                                             const double* __restrict__ sigE, double E, double nu, double f,
+                                                             const GpToNode G2N, float* __restrict__ out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  double gp[48];
+  if (eAn[e] < 0) {
+    for (int q = 0; q < 48; q++) gp[q] = sigE[48 * (size_t)e + q];
+  } else {
+    double ue[24];
+    for (int a = 0; a < 8; a++) {
+      const int n = conn[8 * (size_t)e + a];
+      ue[3 * a] = u[3 * (size_t)n]; ue[3 * a + 1] = u[3 * (size_t)n + 1]; ue[3 * a + 2] = u[3 * (size_t)n + 2];
+    }
+    const double G = E / (2 * (1 + nu)), K = E / (3 * (1 - 2 * nu));
+    const double* Ball = Bm + (size_t)eBb[e] * 8 * 144;
+    for (int g = 0; g < 8; g++) {
+      const double* Bb = Ball + 144 * g;
+      double eps[6];
+      for (int r = 0; r < 6; r++) {
+        double sm = 0;
+        for (int c = 0; c < 24; c++) sm += Bb[r * 24 + c] * ue[c];
+        eps[r] = sm;
+      }
+      eps[0] -= f; eps[1] -= f; eps[2] -= f;
+      const Point& pt = pts[8 * (size_t)eAn[e] + g];
+      const double vol = (eps[0] + eps[1] + eps[2]) / 3, smv = 3 * K * vol;
+      for (int i = 0; i < 3; i++) gp[6 * g + i] = 2 * G * (eps[i] - vol - pt.ep[i]) + smv;
+      for (int i = 3; i < 6; i++) gp[6 * g + i] = 2 * G * (0.5 * eps[i] - pt.ep[i]);
+    }
+  }
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 6; c++) {
+      double v = 0;
+      for (int g = 0; g < 8; g++) v += G2N.M[a * 8 + g] * gp[6 * g + c];
+      out[48 * (size_t)e + 6 * a + c] = (float)v;
+    }
+}
+
 // _snapshot / _restore of the solder points' committed state (ep, s, ebar, W, sigEq)
 __global__ void k_sub_points_copy(int np, const Point* __restrict__ from, Point* __restrict__ to) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -584,6 +634,7 @@ struct SubModel {
   DBuf<double> d_u, d_uN, d_sigE, d_eFn, d_eK, d_eF, d_fe, d_dmax, d_val, d_vals, d_s, d_rint, d_b, d_r, d_z, d_p, d_q, d_x, d_sums, d_pcg;
   DBuf<Point> d_pts, d_snapPts;
   DBuf<double> d_snapU, d_snapSig, d_snapFn;
+  DBuf<float> d_snapOut;                // a stress snapshot (48 per element)
   IcFactor ic;
   bool pcBuilt = false, pcStale = false;
   int pcIters = 0;
@@ -862,9 +913,32 @@ struct SubModel {
   }
 
   // run (13-fatigue.js:1004-1104)
+  // _stressSnapshot at temperature T into host memory (48 floats per element)
+  void stress_snapshot(double T, float* host) {
+    GpToNode G2N;
+    const double s3 = std::sqrt(3.0);
+    for (int n = 0; n < 8; n++) {
+      const double xi = HX[n] * s3, eta = HY[n] * s3, zeta = HZ[n] * s3;
+      for (int g = 0; g < 8; g++) G2N.M[n * 8 + g] = 0.125 * (1 + HX[g] * xi) * (1 + HY[g] * eta) * (1 + HZ[g] * zeta);
+    }
+    const double E = grid_at_s(solderE.data(), T, 1, 0);
+    const double f = grid_at_s(solderF.data(), T, 1, 0) - grid_at_s(solderF.data(), 25, 1, 0);
+    d_snapOut.alloc(48 * (size_t)ne);
+    note_launch();
+    k_sub_stress_snapshot<<<blocks_for(ne, 128), 128, 0, st>>>(ne, d_conn.p, d_eAn.p, d_eBb.p, d_Bm.p, d_pts.p, d_u.p, d_sigE.p, E, P.nu, f,
+                                                              G2N, d_snapOut.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+    TM_CUDA_CHECK(cudaMemcpyAsync(host, d_snapOut.p, 48 * (size_t)ne * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TM_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+
+  // run; with hphase, the stress snapshots at the end of each ramp and dwell of the last cycle
+  // (13-fatigue.js:1053-1078): *nSnaps of them, up to maxSnaps written (meta: T, t, cycle, phase)
   void run(int nsteps, const double* ht, const double* hT, const int* hcycle, int cycles, double cphi, double sphi, double* out,
-           double* perCycle, double* loop) {
+           double* perCycle, double* loop, const int* hphase = nullptr, int maxSnaps = 0, int* nSnaps = nullptr, double* snapMeta = nullptr,
+           float* snapSig = nullptr) {
     if (!nsolderE || elasticSolder) fail(TM_BAD_INPUT, "submodel run needs Anand solder points");
+    if (nSnaps) *nSnaps = 0;
     std::vector<double> Wdie(cycles + 1, 0.0), Wsub(cycles + 1, 0.0), Edie(cycles + 1, 0.0), Esub(cycles + 1, 0.0);
     long long totalNewton = 0;
     int cutbacks = 0, steps = 0, nsubNext = 1, sample = 0;
@@ -902,6 +976,14 @@ struct SubModel {
       d_avg.download(avg, 4, st);
       TM_CUDA_CHECK(cudaStreamSynchronize(st));
       const int c = hcycle[k];
+      if (hphase && nSnaps && c == cycles && (k == nsteps - 1 || hphase[k + 1] != hphase[k])) {
+        const int q = (*nSnaps)++;
+        if (q < maxSnaps) {
+          double* mt = snapMeta + 4 * (size_t)q;
+          mt[0] = T1; mt[1] = t1s; mt[2] = c; mt[3] = hphase[k];
+          stress_snapshot(T1, snapSig + 48 * (size_t)ne * q);
+        }
+      }
       Wdie[c] = avg[0]; Edie[c] = avg[1]; Wsub[c] = avg[2]; Esub[c] = avg[3];
     }
     const int nc = cycles;
@@ -1122,10 +1204,14 @@ void submodel_sizes(SubModel& s, int64_t* out) {
 }
 
 void submodel_run(SubModel& s, int nsteps, const double* t, const double* T, const int* cycle, int cycles, double cphi, double sphi,
-                  double* out, double* perCycle, double* loop) {
+                  double* out, double* perCycle, double* loop, const int* phase, int maxSnaps, int* nSnaps, double* snapMeta,
+                  float* snapSig) {
   if (nsteps < 2 || cycles < 1) fail(TM_BAD_INPUT, "submodel run: need >= 2 history points and >= 1 cycle");
   for (int k = 0; k < nsteps; k++) if (cycle[k] < 0 || cycle[k] > cycles) fail(TM_BAD_INPUT, "submodel run: cycle index out of range");
-  s.run(nsteps, t, T, cycle, cycles, cphi, sphi, out, perCycle, loop);
+  if (maxSnaps > 0 && (!snapMeta || !snapSig)) fail(TM_BAD_INPUT, "submodel run: snapshot buffers missing");
+  s.run(nsteps, t, T, cycle, cycles, cphi, sphi, out, perCycle, loop, phase, maxSnaps, nSnaps, snapMeta, snapSig);
 }
+
+void submodel_stress_snapshot(SubModel& s, double T, float* out) { s.stress_snapshot(T, out); }
 
 }  // namespace tmg

@@ -344,18 +344,36 @@ class DeviceSubmodel:
         check(load().tm_submodel_get(self.h, None, W.ctypes.data_as(C.c_void_p), E.ctypes.data_as(C.c_void_p)))
         return W, E
 
-    def run(self, hist, cphi=1.0, sphi=0.0) -> dict:
-        """run over a cycle history (cycle_history): the reference's result record's numbers."""
+    def run(self, hist, cphi=1.0, sphi=0.0, max_snaps=0) -> dict:
+        """run over a cycle history (cycle_history): the reference's result record's numbers; with
+        max_snaps, the section record's stress snapshots of the last cycle (tm_submodel_run_sections):
+        snaps_meta (T, t, cycle, phase) and snaps (float32, n x ne x 8 x 6)."""
         n, nc = len(hist["t"]), int(hist["cycles"])
         t = np.ascontiguousarray(hist["t"], np.float64); T = np.ascontiguousarray(hist["T"], np.float64)
         cyc = np.ascontiguousarray(hist["cycle"], np.int32)
         out = np.zeros(10); pc = np.zeros(2 * nc); loop = np.zeros(4 * n)
         vp = lambda a: a.ctypes.data_as(C.c_void_p)
-        check(load().tm_submodel_run(self.h, n, vp(t), vp(T), vp(cyc), nc, float(cphi), float(sphi), vp(out), vp(pc), vp(loop)))
+        if max_snaps:
+            ph = np.ascontiguousarray(hist["phase"], np.int32)
+            ns = np.zeros(1, np.int32); meta = np.zeros(4 * max_snaps); sig = np.zeros(48 * self.ne * max_snaps, np.float32)
+            check(load().tm_submodel_run_sections(self.h, n, vp(t), vp(T), vp(cyc), vp(ph), nc, float(cphi), float(sphi), vp(out), vp(pc),
+                                                  vp(loop), int(max_snaps), vp(ns), vp(meta), vp(sig)))
+        else:
+            check(load().tm_submodel_run(self.h, n, vp(t), vp(T), vp(cyc), nc, float(cphi), float(sphi), vp(out), vp(pc), vp(loop)))
         keys = ["dW", "dWdie", "dWsub", "dE", "dEdie", "dEsub", "stabChange", "steps", "cutbacks", "newtonPerStep"]
         rec = {k: float(out[i]) for i, k in enumerate(keys)}
         rec["perCycle"] = pc.reshape(nc, 2); rec["loop"] = loop.reshape(n, 4)
+        if max_snaps:
+            k = min(int(ns[0]), max_snaps)
+            rec["nsnaps"] = int(ns[0])
+            rec["snaps_meta"] = meta[:4 * k].reshape(k, 4); rec["snaps"] = sig[:48 * self.ne * k].reshape(k, self.ne, 8, 6)
         return rec
+
+    def stress_snapshot(self, T) -> np.ndarray:
+        """_stressSnapshot (13-fatigue.js:965-989) of the current state: float32 (ne, 8, 6)."""
+        out = np.zeros(48 * self.ne, np.float32)
+        check(load().tm_submodel_stress_snapshot(self.h, float(T), out.ctypes.data_as(C.c_void_p)))
+        return out.reshape(self.ne, 8, 6)
 
 
 def run_batch(models, hist, cphi, sphi) -> list:

@@ -85,3 +85,24 @@ def test_submodel_uniform_matches_oracle(oracle_lib):
         g, o = dm.step(T, 60.0), om.step(T, 60.0)
         assert g[0] and o[0] and abs(g[1] - o[1]) <= 1 and g[2] == 0
         assert _rel(dm.u(), om.u()) <= 1e-7
+
+
+def test_stress_snapshots_match_oracle(oracle_lib):
+    """The section record's stress snapshots (_stressSnapshot): after single steps, and the ones
+    run takes at the end of every ramp and dwell of the last cycle. The states agree to the
+    solver tolerances, so the float32 nodal stresses do too (1e-6 of the largest after steps,
+    1e-5 after a run)."""
+    spec = synthetic_spec(nxy=6, nz=8)
+    dm, om = DeviceSubmodel(spec), oracle_lib.OracleSubmodel(spec)
+    for T in (30.0, 35.0, 40.0):
+        assert dm.step(T, 30.0)[0] and om.step(T, 30.0)[0]
+        g, o = dm.stress_snapshot(T), om.stress_snapshot(T)
+        assert g.shape == o.shape == (om.ne, 8, 6)
+        assert _rel(g.astype(np.float64), o.astype(np.float64)) <= 1e-6
+    spec = synthetic_spec(nxy=4, nz=8)
+    hist = cycle_history(-40.0, 125.0, 33.0, 5.0, 1)
+    rg = DeviceSubmodel(spec).run(hist, 0.8, 0.6, max_snaps=8)
+    ro = oracle_lib.OracleSubmodel(spec).run(hist, 0.8, 0.6, max_snaps=8)
+    assert rg["nsnaps"] == ro["nsnaps"] >= 4
+    assert np.array_equal(rg["snaps_meta"], ro["snaps_meta"])
+    assert _rel(rg["snaps"].astype(np.float64), ro["snaps"].astype(np.float64)) <= 1e-5

@@ -189,3 +189,56 @@ def test_submodel_uniform_cell_steps(oracle_lib):
         assert ok and newton <= 3 and dmax == 0
     u = om.u()
     assert np.all(np.isfinite(u)) and np.abs(u).max() > 0
+
+
+# ---- stress snapshots of the cross-section view (_stressSnapshot, 13-fatigue.js:965-989) ----
+def _voigt(Em):
+    return np.array([Em[0, 0], Em[1, 1], Em[2, 2], 2 * Em[0, 1], 2 * Em[1, 2], 2 * Em[0, 2]])
+
+
+def test_snapshot_elastic_patch(oracle_lib):
+    """An elastic cell under a uniform strain field: the committed Gauss-point stresses are D eps
+    everywhere, and GP_TO_NODE carries a constant field to every node unchanged."""
+    spec = _uniform_spec(2, lambda T, x: (T - 25.0) / 100.0 * (E @ x))
+    om = oracle_lib.OracleSubmodel(spec)
+    ok, _, _ = om.step(125.0, 60.0)
+    assert ok
+    snap = om.stress_snapshot(125.0)
+    assert snap.dtype == np.float32 and snap.shape == (om.ne, 8, 6)
+    want = iso_d(8000.0, 0.35, NU_MAX_SUBMODEL).reshape(6, 6) @ _voigt(E)
+    assert np.abs(snap - want).max() <= 1e-6 * np.abs(want).max()
+
+
+def test_snapshot_solder_points(oracle_lib):
+    """An all-solder cell under a uniform strain history: every node carries the stress of one
+    Anand point driven by that strain, at its committed plastic strain (AnandPoint.stressAt)."""
+    Et, Ft = sac305_tables()
+    P = anand_params_array(SAC305)
+    spec = _uniform_spec(1, lambda T, x: (T - 25.0) / 100.0 * (E @ x), n=2, nz=2)
+    om = oracle_lib.OracleSubmodel(spec)
+    state = np.zeros(12); state[6] = SAC305["s0"]
+    for T in (45.0, 65.0, 85.0):
+        ok, _, _ = om.step(T, 120.0)
+        assert ok
+        f = float(np.interp(T, np.arange(-80, 301), Ft)) - float(np.interp(25.0, np.arange(-80, 301), Ft))
+        eps = _voigt((T - 25.0) / 100.0 * E) - np.array([f, f, f, 0, 0, 0])
+        _, sig, _ = oracle_lib.anand_step(P, Et, state, eps, T, 120.0)
+    snap = om.stress_snapshot(85.0).astype(np.float64)
+    # the Gauss-point strains carry the Newton tolerance (SUB_RES_TOL 1e-6 on the residual)
+    assert np.abs(snap - sig).max() <= 1e-4 * np.abs(sig).max()
+
+
+def test_run_snapshots_last_cycle(oracle_lib):
+    """run records a snapshot at the end of every ramp and dwell of the last cycle."""
+    from tmsolve.anand import cycle_history
+    spec = synthetic_spec(nxy=4, nz=8)
+    om = oracle_lib.OracleSubmodel(spec)
+    hist = cycle_history(-40.0, 125.0, 33.0, 5.0, 2)
+    r = om.run(hist, 0.8, 0.6, max_snaps=8)
+    ph, cy = np.asarray(hist["phase"]), np.asarray(hist["cycle"])
+    n = len(ph)
+    ends = [k for k in range(1, n) if cy[k] == 2 and (k == n - 1 or ph[k + 1] != ph[k])]
+    assert r["nsnaps"] == len(ends) >= 4
+    assert np.array_equal(r["snaps_meta"][:, 0], np.asarray(hist["T"])[ends][:8])
+    assert np.array_equal(r["snaps_meta"][:, 3], ph[ends][:8])
+    assert np.all(np.isfinite(r["snaps"])) and np.abs(r["snaps"]).max() > 0
