@@ -150,7 +150,7 @@ def test_zero_load():
 @pytest.mark.parametrize("precision", ["mixed", "mixed_ir"])
 def test_mixed_precision(make, precision):
     """FP32 multigrid (and, for mixed_ir, the FP32 apply) inside FP64 iterations: same FP64
-    residual target; RMS warpage within 1e-6 relative of the FP64 GPU solve,
+    residual target; RMS warpage within 1e-6 relative of the FP64 GPU solve (the bar of the mixed path),
     displacements within 1e-5 (both solutions carry the 1e-10 residual of the solve)."""
     from tmsolve.solver import DeviceModel
     pkg = make()
