@@ -208,6 +208,15 @@ tm_status tm_vcycle_shapes(tm_ctx* ctx, int cap, int* nlevels, int* wpb_sweep, i
  * nlevels < 0 returns to autotuning. Takes effect at the next FP32 V-cycle; the shapes change
  * no arithmetic. */
 tm_status tm_set_vcycle_shapes(tm_ctx* ctx, int nlevels, const int* wpb_sweep, const int* wpb_apply, int tma_stages);
+/* The multigrid hierarchy built for the mesh (MultigridPC's levels, src/core/10-solver.js:620-662:
+ * the solid level, buildShellLevel :248-335, then buildCoarseShellLevel :356-471 down to the
+ * coarsest), for checks: per level, fine to coarse, 4 values (grid lines nx and ny of its
+ * columns, nodes or aggregates nn, DOFs per node or aggregate b: 3 solid, 6 shell), up to cap
+ * levels written into out4, *nlevels = all levels. */
+tm_status tm_mg_levels(tm_ctx* ctx, int32_t cap, int32_t* out4, int32_t* nlevels);
+/* The level-1 aggregate of every node (nn values): the solid-to-shell grouping of
+ * buildShellLevel (src/core/10-solver.js:260-334) as the multigrid preconditioner uses it. */
+tm_status tm_mg_node_agg(tm_ctx* ctx, int32_t* out);
 
 /* ---- element DOF histories at screening sites ---- */
 /* Loads the per-step data that the DOF histories read (the shape matrices of every property set

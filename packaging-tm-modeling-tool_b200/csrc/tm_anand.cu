@@ -10,7 +10,9 @@
 //   _dsdd                :209-218
 //   screenJoints loop    :395-451  strain interpolation, in-plane guesses, per-cycle W and ebar
 // Compiled without fused multiply-add, like the reference's JavaScript arithmetic.
+#include <atomic>
 #include <cmath>
+#include <exception>
 #include <vector>
 
 #include "tm_internal.h"
@@ -311,21 +313,25 @@ constexpr size_t NA_BYTES = NA_FTAB + NA_ALIGN(sizeof(double) * TGRID_N);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
-// device address of g_noalloc_scratch per device, looked up once per device with it current
+// device address of g_noalloc_scratch per device, looked up once per device with it current;
+// atomic, since two host threads may make their first call on a device at the same moment (both
+// store the same address)
 constexpr int NA_MAX_DEVICES = 64;
-unsigned char* g_noalloc_addr[NA_MAX_DEVICES] = {nullptr};
+std::atomic<unsigned char*> g_noalloc_addr[NA_MAX_DEVICES];
 
 unsigned char* noalloc_scratch_address() {
   int dev = 0;
   TM_CUDA_CHECK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= NA_MAX_DEVICES) fail(TM_BAD_INPUT, "device index beyond the no-allocation scratch table");
-  if (!g_noalloc_addr[dev]) {
+  unsigned char* a = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!a) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) fail(TM_CUDA, std::string("cudaGetSymbolAddress of the screening scratch: ") + cudaGetErrorString(e));
-    g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    a = static_cast<unsigned char*>(p);
+    g_noalloc_addr[dev].store(a, std::memory_order_release);
   }
-  return g_noalloc_addr[dev];
+  return a;
 }
 
 // per-step interpolation weights and thermal strains of screenJoints (13-fatigue.js:395-401), on the device
@@ -367,6 +373,7 @@ extern "C" tm_status tm_anand_screen_noalloc(const tm_anand_material* mat, int32
     if (nsites <= 0) return TM_OK;
     int i25 = -1;
     for (int i = 0; i < ntemps; i++) if (temps[i] == 25) { i25 = i; break; }
+    require_device();
     unsigned char* base = noalloc_scratch_address();
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     StepK* kc = reinterpret_cast<StepK*>(base + NA_KC);
@@ -399,5 +406,8 @@ extern "C" tm_status tm_anand_screen_noalloc(const tm_anand_material* mat, int32
   } catch (const Error& e) {
     set_last_error(e.msg);
     return e.status;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return TM_CUDA;
   }
 }

@@ -36,6 +36,17 @@ void cuda_check(cudaError_t e, const char* what) {
 
 long long launch_count();
 
+// the path has no CPU fallback: a usable sm_100 device or TM_NO_DEVICE
+void require_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) fail(TM_NO_DEVICE, "no CUDA device: the solve path has no CPU fallback");
+  int dev = 0;
+  TM_CUDA_CHECK(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  TM_CUDA_CHECK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) fail(TM_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100: this library is built for B200 (sm_100a) only");
+}
+
 Context::~Context() {
   for (auto* L : shells) delete L;
   for (auto* b : basis) delete b;
@@ -66,15 +77,6 @@ tm_status guarded(F&& f) {
   }
 }
 
-void require_device() {
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) fail(TM_NO_DEVICE, "no CUDA device: the solve path has no CPU fallback");
-  int dev = 0;
-  TM_CUDA_CHECK(cudaGetDevice(&dev));
-  cudaDeviceProp prop;
-  TM_CUDA_CHECK(cudaGetDeviceProperties(&prop, dev));
-  if (prop.major < 10) fail(TM_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100: this library is built for B200 (sm_100a) only");
-}
 
 // numeric set-up of a preconditioner for the current scaled operator (_buildPC, 10-solver.js:868-882):
 // MultigridPC constructor / update, ICPC, or nothing for Jacobi (the scaled operator's diagonal is 1)
@@ -964,6 +966,31 @@ tm_status tm_vcycle_shapes(tm_ctx* ctx, int cap, int* nlevels, int* wpb_sweep, i
     }
     if (nlevels) *nlevels = k;
     if (tma_stages) *tma_stages = c.tsReady ? c.tsStages : 0;
+  });
+}
+
+tm_status tm_mg_levels(tm_ctx* ctx, int32_t cap, int32_t* out4, int32_t* nlevels) {
+  return guarded([&] {
+    if (!ctx) fail(TM_BAD_INPUT, "null context");
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!c.hierarchy) fail(TM_BAD_INPUT, "no multigrid hierarchy");
+    const int L = 1 + (int)c.shells.size();
+    if (nlevels) *nlevels = L;
+    if (!out4) return;
+    for (int l = 0; l < L && l < cap; l++) {
+      int32_t* o = out4 + 4 * l;
+      if (l == 0) { o[0] = c.nx; o[1] = c.ny; o[2] = c.nn; o[3] = 3; }
+      else { const ShellLevel& S = *c.shells[l - 1]; o[0] = S.nx; o[1] = S.ny; o[2] = S.nn; o[3] = 6; }
+    }
+  });
+}
+
+tm_status tm_mg_node_agg(tm_ctx* ctx, int32_t* out) {
+  return guarded([&] {
+    if (!ctx || !out) fail(TM_BAD_INPUT, "null argument");
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!c.hierarchy) fail(TM_BAD_INPUT, "no multigrid hierarchy");
+    std::copy(c.nodeAgg.begin(), c.nodeAgg.end(), out);
   });
 }
 

@@ -19,6 +19,7 @@ struct Error {
 [[noreturn]] void fail(tm_status st, const std::string& msg);
 void set_last_error(const std::string& msg);
 void cuda_check(cudaError_t e, const char* what);
+void require_device();   // TM_NO_DEVICE unless the current device is an sm_100 GPU
 #define TM_CUDA_CHECK(x) ::tmg::cuda_check((x), #x)
 
 // ---- device buffers ---------------------------------------------------------------------

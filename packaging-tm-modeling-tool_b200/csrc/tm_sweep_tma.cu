@@ -430,8 +430,10 @@ void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st)
   }
   const size_t staticSmem = 256;   // the kernel's barriers and flags
   c.tsStages = 0;
-  for (int ns = 3; ns >= 2 && !c.tsStages; ns--)
-    if (sweep_tma_smem(c.tsMaxNodes, ns) + staticSmem <= (size_t)smemMax) c.tsStages = ns;
+  for (int ns = 3; ns >= 2 && !c.tsStages; ns--) {
+    const size_t need = sweep_tma_smem(c.tsMaxNodes, ns);   // ~0 (does not fit) must not wrap when the static part is added
+    if (need != ~(size_t)0 && need + staticSmem <= (size_t)smemMax) c.tsStages = ns;
+  }
   c.tsPlanned = c.tsStages;
   c.tsReady = TM_SWEEP_TMA && c.tsStages > 0;
   if (c.tsReady) {

@@ -239,6 +239,20 @@ class DeviceModel:
         k = min(n.value, cap)
         return dict(wpb_sweep=list(ws[:k]), wpb_apply=list(wa[:k]), tma_stages=st.value)
 
+    def mg_levels(self) -> list:
+        """The multigrid hierarchy, fine to coarse: (nx, ny, nn, b) per level (MultigridPC's levels)."""
+        cap = 64
+        n = C.c_int32(0)
+        out = np.zeros(4 * cap, np.int32)
+        check(load().tm_mg_levels(self.h, cap, out.ctypes.data_as(C.c_void_p), C.byref(n)))
+        return [tuple(int(v) for v in out[4 * l:4 * l + 4]) for l in range(min(n.value, cap))]
+
+    def mg_node_agg(self) -> np.ndarray:
+        """Level-1 aggregate of every node (buildShellLevel's grouping)."""
+        out = np.zeros(self.nn, np.int32)
+        check(load().tm_mg_node_agg(self.h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def set_vcycle_shapes(self, wpb_sweep=None, wpb_apply=None, tma_stages=0):
         """Pin the FP32 V-cycle's launch shapes (as vcycle_shapes returns them); None: autotune."""
         if wpb_sweep is None:

@@ -59,3 +59,7 @@ def test_point_step_parity(oracle_lib):
         d, so, Do = oracle_lib.anand_step(P, Et, st, eps[q], 75.0, 30.0)
         assert np.allclose(sig[q], so, rtol=1e-9, atol=1e-9)
         assert np.allclose(state[q, :11], st[:11], rtol=1e-9, atol=1e-12)
+        # the consistent tangent (_dsdd, 13-fatigue.js:209-218) that the submodel's Newton uses:
+        # within 1e-8 of its largest entry
+        assert np.allclose(D[q], Do, rtol=0, atol=1e-8 * np.abs(Do).max()), np.abs(D[q] - Do).max()
+    assert np.any(state[:, 7] > 0)      # some points flowed plastically (the tangent is not the elastic one)

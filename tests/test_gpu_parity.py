@@ -211,3 +211,78 @@ def test_vcycle_autotuned_shapes():
     dm.set_vcycle_shapes(None)      # back to autotuning
     r2 = dm.solve(f, tol=1e-10, warm=0, key=4, precision="mixed")
     assert np.array_equal(r2["u"], r["u"])
+
+
+@pytest.mark.parametrize("make", [fcbga_c1, lambda: lidded_c2(n_inplane=48)], ids=["c1", "c2_48"])
+def test_hierarchy_matches_oracle(make, oracle_lib):
+    """The device multigrid hierarchy is the reference's: the same levels (grid lines, nodes or
+    aggregates, DOFs per unit) down to the coarsest, and the same solid-to-shell aggregate of every
+    node (buildShellLevel, including its classification of the last node row by the flat cell index,
+    10-solver.js:270-287)."""
+    pkg = make()
+    dm, om = _models(pkg, oracle_lib)
+    fo = om.assemble(pkg.step())
+    om.solve(fo, tol=1e-8)           # the oracle builds its hierarchy with the first preconditioner
+    lg, lo = dm.mg_levels(), om.mg_levels()
+    assert len(lg) >= 3
+    assert lg == [tuple(int(v) for v in l) for l in lo]
+    assert np.array_equal(dm.mg_node_agg(), om.mg_node_agg())
+
+
+def test_warm_start_matches_oracle(oracle_lib):
+    """_warmStart (10-solver.js:885-915) against the oracle's: after one stored solution, a second
+    load that is not a multiple of the first starts from the same Galerkin projection (the relative
+    residual of the initial guess agrees), keeps the same number of stored solutions and converges
+    to the same displacements."""
+    pkg = fcbga_c1()
+    dm, om = _models(pkg, oracle_lib)
+    step = pkg.step()
+    r1 = dm.solve(dm.assemble_step(step), tol=1e-12, key=0)
+    ro1 = om.solve(om.assemble(step), tol=1e-12, key=0)
+    assert r1["warm"] == ro1["warm"] == 1
+    step2 = pkg.step(25.0, 125.0)
+    rng = np.random.default_rng(5)
+    g = np.zeros(dm.ndof)
+    g[3 * rng.choice(dm.nn, 64, replace=False) + 2] = 1e3 * rng.standard_normal(64)
+    g[np.asarray(pkg.mesh.constraints)] = 0
+    f2 = dm.assemble_step(step2) + g
+    fo2 = om.assemble(step2) + g
+    r2 = dm.solve(f2, tol=1e-12, key=1)
+    ro2 = om.solve(fo2, tol=1e-12, key=1)
+    assert r2["converged"] and ro2["converged"]
+    assert r2["warm"] == ro2["warm"] == 2
+    assert 0 < ro2["iters0"] < 1
+    assert abs(r2["iters0"] / ro2["iters0"] - 1) <= 1e-5, (r2["iters0"], ro2["iters0"])
+    assert np.linalg.norm(r2["u"] - ro2["u"]) / np.linalg.norm(ro2["u"]) <= 1e-8
+    assert abs(r2["iters"] - ro2["iters"]) <= max(3, ro2["iters"] // 4)
+
+
+def test_bench_workload_parity(oracle_lib):
+    """The benchmark workload itself (lidded C2 160x160x32, 2,065,539 DOF) on the GPU in FP64 and in
+    mixed precision against the oracle's FP64 solve, all to relative residual 1e-12: displacements
+    within 1e-8 (FP64) and 1e-5 (mixed), RMS and signed JEITA warpage within 1e-8 and 1e-6."""
+    from tmsolve import post
+    from tmsolve.solver import DeviceModel
+    pkg = lidded_c2()
+    om = oracle_lib.OracleModel(pkg)
+    step = pkg.step()
+    ro = om.solve(om.assemble(step), tol=1e-12)
+    assert ro["converged"]
+    uo = ro["u"]
+    b = post.bga_sites(**pkg.meta["bga"])
+    z = b["zone"]
+    wo = om.warpage_jeita(uo, b["x"], b["y"], [z["x0"], z["x1"], z["y0"], z["y1"]])
+    rms_o = rms_warpage(pkg.mesh, uo)
+    del om
+    dm = DeviceModel(pkg)
+    for key, (precision, bar_u, bar_w) in enumerate((("fp64", 1e-8, 1e-8), ("mixed", 1e-5, 1e-6))):
+        r = dm.solve(dm.assemble_step(step), tol=1e-12, warm=0, key=key, precision=precision)
+        assert r["converged"], precision
+        u = r["u"]
+        du = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+        assert du <= bar_u, (precision, du)
+        assert abs(rms_warpage(pkg.mesh, u) / rms_o - 1) <= bar_w, precision
+        w = post.warpage_jeita(b, lambda x, y: dm.sample_plane(u, 0, 2, x, y))
+        assert w["sign"] == wo["sign"]
+        assert abs(w["signed"] / wo["signed"] - 1) <= bar_w, (precision, w["signed"], wo["signed"])
+        assert abs(w["mag"] / wo["mag"] - 1) <= bar_w, precision

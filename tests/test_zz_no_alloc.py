@@ -7,6 +7,8 @@ tables live in a fixed array of the library instead of fresh allocations. This t
 it twice in a row through the C-ABI, with the strain table and the outputs in device
 memory that the caller (torch) allocated, and checks both results against the regular
 entry point tm_anand_screen at the tolerance of the other Anand tests (1e-8 relative).
+Around the second call (the library is loaded and the array's address looked up by then) the
+device's free memory, as cudaMemGetInfo reports it, must not change.
 The file is named so that pytest collects it last.
 """
 import ctypes as C
@@ -43,11 +45,16 @@ def test_noalloc_screen_matches_regular_entry_point_twice():
         dW = torch.full((ns,), -1.0, dtype=torch.float64, device="cuda")
         dE = torch.full((ns,), -1.0, dtype=torch.float64, device="cuda")
         st = torch.full((ns,), -1.0, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
         rc = L.tm_anand_screen_noalloc(C.byref(m), ns, len(temps), vp(temps), C.c_void_p(d_table.data_ptr()), len(t), vp(t), vp(T),
                                       vp(cyc), vp(ph), int(hist["cycles"]), C.c_void_p(dW.data_ptr()), C.c_void_p(dE.data_ptr()),
                                       C.c_void_p(st.data_ptr()), C.c_void_p(stream))
         assert rc == _lib.TM_OK, _lib.last_error()
         torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        if call == 1:
+            assert free1 == free0, (free0, free1)
         assert np.allclose(dW.cpu().numpy(), ref_dW, rtol=1e-8, atol=0), call
         assert np.allclose(dE.cpu().numpy(), ref_dE, rtol=1e-8, atol=0), call
         assert np.allclose(st.cpu().numpy(), ref_st, rtol=1e-8, atol=0), call
