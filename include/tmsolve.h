@@ -217,6 +217,10 @@ tm_status tm_mg_levels(tm_ctx* ctx, int32_t cap, int32_t* out4, int32_t* nlevels
 /* The level-1 aggregate of every node (nn values): the solid-to-shell grouping of
  * buildShellLevel (src/core/10-solver.js:260-334) as the multigrid preconditioner uses it. */
 tm_status tm_mg_node_agg(tm_ctx* ctx, int32_t* out);
+/* CUDA-core fused multiply-add throughput of the current device in TFLOP/s, FP32 and FP64 (no
+ * counterpart in the reference): the denominators of the compute roofline of the matrix-free level-0
+ * kernels. Runs about a hundred milliseconds of arithmetic; either pointer may be NULL. */
+tm_status tm_device_peaks(double* fp32_tflops, double* fp64_tflops);
 
 /* ---- element DOF histories at screening sites ---- */
 /* Loads the per-step data that the DOF histories read (the shape matrices of every property set

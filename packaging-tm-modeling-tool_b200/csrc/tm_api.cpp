@@ -372,6 +372,7 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
   c.pcKey = o.key;
   if (!c.scaled) {
     launch_scale(c);
+    launch_mf_scales(c, true);
     c.scaled = true;
     c.fp32Ready = false;
   }
@@ -623,10 +624,14 @@ tm_status tm_assemble_step(tm_ctx* ctx, const tm_step* st, double* rhs_out) {
     check_step(c, *st);
     launch_shape_matrices(c, *st);
     launch_class_condense(c);
+    mf_build_cells(c, st->stage);
+    launch_mf_combine(c);
     launch_assemble(c);
     launch_constraints(c);
     c.assembled = true;
     c.scaled = false;
+    c.mf = c.mfAvailable;
+    launch_mf_scales(c, false);
     if (rhs_out) {
       c.d_rhs.download(rhs_out, 3 * (size_t)c.nn, c.stream);
     }
@@ -666,6 +671,7 @@ tm_status tm_set_bcsr(tm_ctx* ctx, const int32_t* rowPtr, const int32_t* col, co
     c.d_constr.upload(c.constr, c.stream);
     c.assembled = true;
     c.scaled = false;
+    c.mf = false;   // a caller-assembled operator has no element classes: the stencil path
     TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   });
 }
@@ -965,7 +971,7 @@ tm_status tm_vcycle_shapes(tm_ctx* ctx, int cap, int* nlevels, int* wpb_sweep, i
       k++;
     }
     if (nlevels) *nlevels = k;
-    if (tma_stages) *tma_stages = c.tsReady ? c.tsStages : 0;
+    if (tma_stages) *tma_stages = c.tsReady && !c.mf ? c.tsStages : 0;
   });
 }
 

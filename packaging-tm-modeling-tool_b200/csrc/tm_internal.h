@@ -84,6 +84,11 @@ struct DBuf {
 #ifndef TM_APPLY32_MINB
 #define TM_APPLY32_MINB 10
 #endif
+// level-0 operator from the cell-class table (tm_mf.cu) instead of the assembled stencil, for
+// operators assembled by tm_assemble_step (0: the assembled stencil everywhere)
+#ifndef TM_MATRIX_FREE
+#define TM_MATRIX_FREE 1
+#endif
 #define TM_STR_(x) #x
 #define TM_UNROLL(n) _Pragma(TM_STR_(unroll n))
 
@@ -210,6 +215,21 @@ struct Context {
   DBuf<double> d_psetM;                // 6*1089 per property set
   DBuf<double> d_clsF33;               // 33 per class: uncondensed element thermal load (elementFth)
   DBuf<int> d_psetLayered, d_psetBorn;
+  // matrix-free level 0 (tm_mf.cu): per mesh cell one cell class (the (class, scale) pairs of its
+  // elements) whose combined condensed matrix is formed per step; per DOF the gather scale gs (S,
+  // zero at constrained DOFs), the row scale os (S) and the kept diagonal cd of constrained rows
+  bool mf = false;                     // level 0 is applied from the cell-class table (operator from tm_assemble_step)
+  bool mfBuilt = false, mfAvailable = false;
+  int mfStage = 0;                     // stage the cell classes were built for (element birth scales)
+  int ncc = 0;
+  DBuf<uint16_t> d_cellCls;            // per cell, 0xFFFF: no element
+  DBuf<int> d_ccInfo;                  // per cell class: the element classes (second -1 when single)
+  DBuf<double> d_ccScale;              // per cell class: the elements' assembly scales
+  DBuf<double> d_ccK;                  // 576 per cell class
+  DBuf<float> d_ccK32;
+  DBuf<double> d_gs, d_os, d_cd;
+  DBuf<float> d_gs32, d_os32, d_cd32;
+  DBuf<int> d_colP0;                   // per node column: position of its first node (-1: empty)
   IcFactor ic;                         // the IC(0) preconditioner (tm_ic0.cu)
   int pcKind = -1;                     // kind of the preconditioner built last (TM_PC_*)
   bool stepReady = false;              // shape matrices and thermal loads of an assembled step are on the device
@@ -386,6 +406,16 @@ void plan_sweep_tma(Context& c, const std::vector<int>* colPos, cudaStream_t st)
 bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float* x);   // false: not available
 void launch_val_to_f32(Context& c);   // FP32 level-0 operator (and its position-major copy for the TMA sweep)
 size_t sweep_tma_smem(int maxNodes, int nstage);   // shared memory of the TMA sweep (~0: does not fit)
+
+// ---- matrix-free level 0 (tm_mf.cu) --------------------------------------------------------------
+void mf_build_cells(Context& c, int stage);                 // cell classes for a stage (host, on a stage change)
+void launch_mf_combine(Context& c);                         // combined cell matrices of the step (after the condensation)
+void launch_mf_scales(Context& c, bool scaled);             // gs, os, cd of the unscaled or the scaled operator
+void launch_mf_apply(Context& c, const double* x, double* y, const double* b);   // y = Ks x, or b - Ks x
+void launch_mf_apply32(Context& c, const float* x, float* y, const float* b);
+void launch_mf_sweep32(Context& c, int col, int zeroGuess, const float* b, float* x);   // one colour of the level-0 sweep
+void launch_mf_sweep64(Context& c, int col, int zeroGuess, const double* b, double* x);
+size_t mf_sweep_smem(int nz);
 
 // ---- Anand (tm_anand.cu) ---------------------------------------------------------------------
 void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps_h,

@@ -1089,7 +1089,7 @@ void launch_to_fp32(Context& c) {
     b.alloc(a.n);
     if (a.n) { k_to_f32<<<grid_for(a.n, 256), 256, 0, c.stream>>>(a.n, a.p, b.p); note_launch(); }
   };
-  launch_val_to_f32(c);
+  if (!c.mf) launch_val_to_f32(c);   // the matrix-free level 0 reads no FP32 stencil
   conv(c.d_F, c.d_F32);
   conv(c.d_W01, c.d_W01_32);
   c.d_res0_32.alloc(3 * (size_t)c.nn);

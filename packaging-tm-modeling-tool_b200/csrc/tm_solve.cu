@@ -580,11 +580,16 @@ void vcycle(Context& c, const T* r, T* z) {
   const int nn = c.nn;
   const size_t smem0 = (size_t)21 * c.panelCap * sizeof(T) + (size_t)(c.panelMaxCols + 1) * sizeof(int);
   // the iterate starts at zero (the TMA sweep clears it itself on the first sweep)
-  if (sizeof(T) == 8 || !c.tsReady) TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(T), st));
+  if (sizeof(T) == 8 || !c.tsReady || c.mf) TM_CUDA_CHECK(cudaMemsetAsync(z, 0, 3 * (size_t)nn * sizeof(T), st));
   if (smem0 > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
   auto sweep0 = [&](int col, int zero) {
     if (!c.grpCount[col]) return;
     TimedLaunch tl(c, K_SWEEP_SOLID);
+    if (c.mf) {   // level 0 from the cell-class table
+      if constexpr (sizeof(T) == 4) launch_mf_sweep32(c, col, zero, (const float*)r, (float*)z);
+      else launch_mf_sweep64(c, col, zero, (const double*)r, (double*)z);
+      return;
+    }
     if constexpr (sizeof(T) == 4)
       if (launch_sweep_tma(c, col, zero, r, z)) return;
     k_sweep_panel<T><<<c.grpCount[col], TM_PANEL_THREADS, smem0, st>>>(c.d_grpStart[col].p, c.d_colPos[col].p, c.d_posNode.p, c.nnp,
@@ -619,7 +624,12 @@ void vcycle(Context& c, const T* r, T* z) {
     }
   {
     TimedLaunch tl(c, K_APPLY0);
-    apply0_range<T, T>(c, B::val0(c), 0, nn, z, B::res0(c), r);
+    if (c.mf) {
+      if constexpr (sizeof(T) == 4) launch_mf_apply32(c, (const float*)z, (float*)B::res0(c), (const float*)r);
+      else launch_mf_apply(c, (const double*)z, (double*)B::res0(c), (const double*)r);
+    } else {
+      apply0_range<T, T>(c, B::val0(c), 0, nn, z, B::res0(c), r);
+    }
   }
   ShellLevel& L1 = *c.shells[0];
   k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, B::W01(c), B::res0(c), B::b(L1), B::x(L1));
@@ -692,6 +702,7 @@ TimedLaunch::~TimedLaunch() {
 
 void launch_apply0(Context& c, const double* x, double* y, const double* b) {
   TimedLaunch tl(c, K_APPLY0);
+  if (c.mf) { launch_mf_apply(c, x, y, b); return; }
   apply0_range<double, double>(c, c.d_val.p, 0, c.nn, x, y, b);
   TM_CUDA_CHECK(cudaGetLastError());
 }
@@ -703,6 +714,7 @@ void launch_apply0_f32(Context& c, const double* x, double* y, const double* b) 
 
 void launch_apply0_32(Context& c, const float* x, float* y, const float* b) {
   TimedLaunch tl(c, K_APPLY0);
+  if (c.mf) { launch_mf_apply32(c, x, y, b); return; }
   apply0_range<float, float>(c, c.d_val32.p, 0, c.nn, x, y, b);
   TM_CUDA_CHECK(cudaGetLastError());
 }
@@ -817,7 +829,8 @@ void vcycle_graph(Context& c, const T* r, T* z) {
   }
   const int idx = sizeof(T) == 4 ? 1 : 0;
   size_t key = 1469598103934665603ull;
-  for (size_t v : {(size_t)r, (size_t)z, (size_t)c.structEpoch, (size_t)c.shapeEpoch, (size_t)Bufs<T>::val0(c), (size_t)c.stream})
+  for (size_t v : {(size_t)r, (size_t)z, (size_t)c.structEpoch, (size_t)c.shapeEpoch, (size_t)Bufs<T>::val0(c), (size_t)c.stream,
+                   (size_t)c.mf, (size_t)c.d_ccK32.p, (size_t)c.d_gs32.p, (size_t)c.d_gs.p})
     key = (key ^ v) * 1099511628211ull;
   if (!c.vcGraph[idx] || c.vcKey[idx] != key) {
     if (c.vcGraph[idx]) {
@@ -925,7 +938,7 @@ void autotune_vcycle32(Context& c) {
       if (tA < 0.97 * bestA) { bestA = tA; L.wpbApply = wpb; }
     }
   }
-  if (c.tsReady && c.colorCount[0]) {
+  if (c.tsReady && c.colorCount[0] && !c.mf) {
     const size_t n = 3 * (size_t)c.nn;
     DBuf<float> sx, sb;
     sx.alloc(n); sx.zero(st);

@@ -345,3 +345,10 @@ def launch_count() -> int:
 
 
 __all__ = ["DeviceModel", "TmError", "launch_count"]
+
+
+def device_peaks() -> dict:
+    """CUDA-core FMA throughput of the current device (TFLOP/s, FP32 and FP64)."""
+    f32, f64 = C.c_double(), C.c_double()
+    check(load().tm_device_peaks(C.byref(f32), C.byref(f64)))
+    return dict(fp32_tflops=f32.value, fp64_tflops=f64.value)
