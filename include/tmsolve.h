@@ -221,6 +221,12 @@ tm_status tm_mg_node_agg(tm_ctx* ctx, int32_t* out);
  * counterpart in the reference): the denominators of the compute roofline of the matrix-free level-0
  * kernels. Runs about a hundred milliseconds of arithmetic; either pointer may be NULL. */
 tm_status tm_device_peaks(double* fp32_tflops, double* fp64_tflops);
+/* Test hook of the timeout path (no counterpart in the reference). Every device wait of the library
+ * is bounded: a wait that runs out makes the kernel flag the error, let its copies in flight land
+ * and return, and the call fails with TM_TIMEOUT while the context stays usable. While on != 0,
+ * the level-0 TMA sweep (used for operators loaded with tm_set_bcsr in mixed precision) waits,
+ * with a short limit, for a stage flag that nothing sets, so that path can be exercised. */
+tm_status tm_set_wait_test(tm_ctx* ctx, int32_t on);
 
 /* ---- element DOF histories at screening sites ---- */
 /* Loads the per-step data that the DOF histories read (the shape matrices of every property set

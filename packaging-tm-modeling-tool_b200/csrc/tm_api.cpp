@@ -1000,6 +1000,13 @@ tm_status tm_mg_node_agg(tm_ctx* ctx, int32_t* out) {
   });
 }
 
+tm_status tm_set_wait_test(tm_ctx* ctx, int32_t on) {
+  return guarded([&] {
+    if (!ctx) fail(TM_BAD_INPUT, "null context");
+    reinterpret_cast<Context*>(ctx)->waitTest = on != 0;
+  });
+}
+
 tm_status tm_pc_apply(tm_ctx* ctx, const double* r, double* z) {
   return guarded([&] {
     Context& c = *reinterpret_cast<Context*>(ctx);

@@ -40,6 +40,7 @@ constexpr int TS_ROWS = NSLOT * 9;                                 // operator r
 constexpr int TS_STAGE_BYTES = (TS_ROWS + NSLOT) * TS_CHUNK * 4;   // values, then neighbour ids
 constexpr int TS_MAXSTAGE = 8;
 constexpr long long TS_WAIT_LIMIT = 1LL << 22;
+constexpr long long TS_TEST_LIMIT = 1LL << 12;                     // the timeout test's wait (see waitTest)
 constexpr int TS_ILP = 4;                                          // positions per thread in the run's gathers
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -130,7 +131,8 @@ __device__ __forceinline__ void bulk_load_hint(void* dst, const void* src, unsig
 __global__ void __launch_bounds__(TS_THREADS, 1)
     k_sweep_tma(const float* __restrict__ valPm, const int* __restrict__ nbrPm, const int* __restrict__ partCol,
                 const int* __restrict__ colPos, const int* __restrict__ posNode, const float* __restrict__ F, const float* __restrict__ b,
-                float* __restrict__ x, int maxNodes, int nstage, int zeroGuess, int nn, int zlo, int zhi, int* __restrict__ err) {
+                float* __restrict__ x, int maxNodes, int nstage, int zeroGuess, int nn, int zlo, int zhi, int* __restrict__ err,
+                int waitTest) {
   extern __shared__ __align__(16) unsigned char smraw_t[];
   __shared__ __align__(8) uint64_t bars[TS_MAXSTAGE + 1];   // chunk stages, then the factors
   // 128-byte aligned start of the stages (the launch adds 128 bytes for this)
@@ -217,9 +219,13 @@ __global__ void __launch_bounds__(TS_THREADS, 1)
     const float bv = rlive ? b[3 * (size_t)posNode[rp] + rc] : 0.f;
     // the chunk's loads must have been issued before its stage is waited on: the previous chunk
     // of the stage belongs to the other group, and a wait one phase early would see that phase
+    // (waitTest: the test hook of the timeout path waits, with a short limit, for a stage number that
+    // is never issued)
     bool ok = false;
-    for (long long it = 0; it < TS_WAIT_LIMIT; it++)
-      if (*(volatile int*)&s_last[k % nstage] == k) { ok = true; break; }
+    const int want = waitTest ? -2 : k;
+    const long long limit = waitTest ? TS_TEST_LIMIT : TS_WAIT_LIMIT;
+    for (long long it = 0; it < limit; it++)
+      if (*(volatile int*)&s_last[k % nstage] == want) { ok = true; break; }
     if (ok) ok = mbar_wait(&bars[k % nstage], (unsigned)(k / nstage) & 1u);
     if (!ok) s_fail = 1;
     const float* sv = reinterpret_cast<const float*>(smt + (size_t)(k % nstage) * TS_STAGE_BYTES);
@@ -450,7 +456,7 @@ bool launch_sweep_tma(Context& c, int col, int zeroGuess, const float* b, float*
   TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_sweep_tma<<<c.tsParts, TS_THREADS, smem, c.stream>>>(c.d_val32p.p, c.d_nbrp.p, c.d_tsPart[col].p, c.d_colPos[col].p, c.d_posNode.p,
                                                         c.d_F32.p, b, x, c.tsMaxNodes, c.tsStages, zeroGuess, c.nn, c.colourPos[col],
-                                                        c.colourPos[col + 1], c.d_err.p);
+                                                        c.colourPos[col + 1], c.d_err.p, c.waitTest ? 1 : 0);
   note_launch();
   return true;
 }

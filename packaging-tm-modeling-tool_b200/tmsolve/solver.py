@@ -239,6 +239,10 @@ class DeviceModel:
         k = min(n.value, cap)
         return dict(wpb_sweep=list(ws[:k]), wpb_apply=list(wa[:k]), tma_stages=st.value)
 
+    def set_wait_test(self, on: bool):
+        """Test hook of the timeout path: the level-0 TMA sweep waits for a flag that nothing sets."""
+        check(load().tm_set_wait_test(self.h, 1 if on else 0))
+
     def mg_levels(self) -> list:
         """The multigrid hierarchy, fine to coarse: (nx, ny, nn, b) per level (MultigridPC's levels)."""
         cap = 64
@@ -263,12 +267,18 @@ class DeviceModel:
         check(load().tm_set_vcycle_shapes(self.h, n, ws, wa, int(tma_stages)))
 
     def solve(self, f, label=None, key=-1, tol=1e-8, maxit=2000, warm=20, precond="mg", precision="fp64",
-              out: Optional[np.ndarray] = None) -> dict:
-        """LinearSolver.solve with host arrays; the displacement goes to `out` when given."""
+              out: Optional[np.ndarray] = None, progress=None, progress_every: int = 1) -> dict:
+        """LinearSolver.solve with host arrays; the displacement goes to `out` when given.
+        progress(it, relres), when given, is called between PCG iterations every progress_every
+        iterations, on this thread (the reference's LIVE.post progress, 10-solver.js:1033)."""
         f = np.ascontiguousarray(f, np.float64)
         u = _out_array(out, self.ndof)
         info = TmSolveInfo()
         o = self.make_opts(tol, maxit, warm, precond, precision, key)
+        if progress is not None:
+            cb = _lib.PROGRESS_FN(lambda user, it, rel: progress(int(it), float(rel)))
+            o.progress = cb
+            o.progress_every = int(progress_every)
         check(load().tm_solve(self.h, f.ctypes.data_as(C.c_void_p), u.ctypes.data_as(C.c_void_p), C.byref(o), C.byref(info)),
               allow_not_converged=True)
         rec = self.record(info, label, precond)
