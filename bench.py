@@ -40,12 +40,20 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default=None, choices=["mixed", "fp64"], help="default: mixed (c2), fp64 (c1)")
     ap.add_argument("--inplane", type=int, default=160)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="a warm-up assemble + solve, then one assemble + solve (for ncu captures); prints no bench line")
-    return ap.parse_args()
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "screen"],
+                    help="c2: the lidded 160x160x32 solve (the headline); c1: the plain FP64 FCBGA 48x48x20 solve; "
+                         "screen: Anand screening of the 17,424 bumps of a die over three -40/125 degC cycles")
+    ap.add_argument("--sites", type=int, default=17424, help="screen: bump sites")
+    a = ap.parse_args()
+    a.precision_default = a.precision is None
+    if a.precision is None:
+        a.precision = "mixed"
+    return a
 
 
 def run_profile(a):
@@ -53,10 +61,9 @@ def run_profile(a):
     one solve each. The first step builds what a hierarchy builds once (the launch-shape tuning, the
     captured V-cycle); the second is the step the launch list summarises (from its k_assemble on)."""
     import torch
-    from tmsolve.packages import lidded_c2
     from tmsolve.solver import DeviceModel
     torch.cuda.set_device(0)
-    pkg = lidded_c2(n_inplane=a.inplane)
+    pkg = make_package(a.workload, a.inplane)
     dm = DeviceModel(pkg)
     f = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
     u = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
@@ -122,14 +129,18 @@ class Clocks:
 _CPU = {}
 
 
-def cpu_init(inplane):
+def make_package(workload, inplane):
+    from tmsolve.packages import fcbga_c1, lidded_c2
+    return fcbga_c1() if workload == "c1" else lidded_c2(n_inplane=inplane)
+
+
+def cpu_init(workload, inplane):
     """Worker set-up (untimed): the package and the oracle's FEModel + LinearSolver of the workload."""
     for p in (ROOT, PKG):
         if p not in sys.path:
             sys.path.insert(0, p)
     from oracle import oracle
-    from tmsolve.packages import lidded_c2
-    pkg = lidded_c2(n_inplane=inplane)
+    pkg = make_package(workload, inplane)
     _CPU.update(pkg=pkg, om=oracle.OracleModel(pkg), key=0)
 
 
@@ -168,7 +179,7 @@ def run_reference(a):
     oracle.build()
     procs = min(reference_procs(), max(1, a.steps))
     ctx = mp.get_context("spawn")
-    with ctx.Pool(procs, initializer=cpu_init, initargs=(a.inplane,)) as pool:
+    with ctx.Pool(procs, initializer=cpu_init, initargs=(a.workload, a.inplane)) as pool:
         pool.map(cpu_step, range(max(1, min(a.warmup, procs))), chunksize=1)
         t0 = time.perf_counter()
         res = pool.map(cpu_step, range(a.steps), chunksize=1)
@@ -199,7 +210,7 @@ def run_ours(a):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         from oracle import oracle
         oracle.build()
-        cpu_init(a.inplane)
+        cpu_init(a.workload, a.inplane)
         nd, it, dt, conv = cpu_step()
         _CPU.clear()
         cpu = {"value": nd * it / 1e6 / dt, "unit": UNIT, "cores": 1, "kind": "port",
@@ -212,9 +223,9 @@ def run_ours(a):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from tmsolve.packages import lidded_c2, rms_warpage
+    from tmsolve.packages import rms_warpage
     from tmsolve.solver import DeviceModel, launch_count
-    pkg = lidded_c2(n_inplane=a.inplane)
+    pkg = make_package(a.workload, a.inplane)
     dm = DeviceModel(pkg)
     stream = torch.cuda.current_stream()
     dm.set_stream(stream.cuda_stream)
@@ -343,8 +354,112 @@ def profile_traffic(kernel, precision):
     return None
 
 
+# ---- Anand screening ------------------------------------------------------------------------------
+SCREEN_METRIC = "Anand screening throughput: bump sites x time steps per second (screenJoints, FP64 return map)"
+SCREEN_UNIT = "Msite-steps/s"
+
+
+def screen_inputs(nsites):
+    from tmsolve.anand import cycle_history, cycling_temps, synthetic_strain_table
+    from tmsolve.materials import SAC305_MODULE, anand_tables
+    hist = cycle_history(-40.0, 125.0, 11.0, 15.0, 3)      # 15-min ramps (11 degC/min) and dwells, 3 cycles
+    temps = cycling_temps(-40.0, 125.0)
+    table, _, _ = synthetic_strain_table(nsites, temps, die_half=12.5)
+    Et, Ft = anand_tables(SAC305_MODULE)
+    return hist, temps, table, Et, Ft
+
+
+def run_screen(a):
+    """Anand screening of one die's bumps: every site runs the whole three-cycle history (its table
+    of strains at the cycling temperatures interpolated per time step, the in-plane Newton, the FP64
+    return map) and reports the last cycle's dW and dE."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from oracle import oracle
+    from tmsolve._lib import check, load
+    from tmsolve.anand import material
+    from tmsolve.materials import SAC305_MODULE, anand_params_array
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    hist, temps, table, Et, Ft = screen_inputs(a.sites)
+    ns, nt, nsteps = a.sites, len(temps), len(hist["t"])
+    unit_work = ns * nsteps / 1e6
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        oracle.build()
+        sample = min(ns, 512)
+        t0 = time.perf_counter()
+        oracle.anand_screen(anand_params_array(SAC305_MODULE), Et, Ft, temps, table[:sample].ravel(), hist)
+        dt = time.perf_counter() - t0
+        cpu = {"value": sample * nsteps / 1e6 / dt, "unit": SCREEN_UNIT, "cores": 1, "kind": "port",
+               "sample": f"the first {sample} of the {ns} sites, all {nsteps} time steps, on one core ({dt:.1f} s)"}
+    torch.cuda.set_device(local)
+    m, keep = material(SAC305_MODULE, Et, Ft)
+    vp = lambda x: x.ctypes.data_as(C.c_void_p)
+    t = np.ascontiguousarray(hist["t"]); T = np.ascontiguousarray(hist["T"])
+    cyc = np.ascontiguousarray(hist["cycle"], np.int32); ph = np.ascontiguousarray(hist["phase"], np.int32)
+    temps = np.ascontiguousarray(temps)
+    d_table = torch.from_numpy(np.ascontiguousarray(table).ravel()).cuda()
+    d_out = torch.empty(3, ns, dtype=torch.float64, device="cuda")
+    L = load()
+
+    def dev_run():
+        check(L.tm_anand_screen_device(C.byref(m), ns, nt, vp(temps), C.c_void_p(d_table.data_ptr()), nsteps, vp(t), vp(T), vp(cyc),
+                                       vp(ph), int(hist["cycles"]), C.c_void_p(d_out[0].data_ptr()), C.c_void_p(d_out[1].data_ptr()),
+                                       C.c_void_p(d_out[2].data_ptr())))
+    for _ in range(a.warmup):
+        dev_run()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as ck:
+        e0.record(stream)
+        for _ in range(a.steps):
+            dev_run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    # end to end: the host API with host arrays (table in, dW/dE/stab out)
+    hW = np.zeros(ns); hE = np.zeros(ns); hS = np.zeros(ns)
+    tab = np.ascontiguousarray(table).ravel()
+    e0.record(stream)
+    for _ in range(a.steps):
+        check(L.tm_anand_screen(C.byref(m), ns, nt, vp(temps), vp(tab), nsteps, vp(t), vp(T), vp(cyc), vp(ph), int(hist["cycles"]),
+                                vp(hW), vp(hE), vp(hS)))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / a.steps
+    # accuracy against the oracle on a sample of sites
+    dW = d_out[0].cpu().numpy()
+    sample = np.arange(0, ns, max(1, ns // 64))
+    oW, _, _ = oracle.anand_screen(anand_params_array(SAC305_MODULE), Et, Ft, temps, table[sample].ravel(), hist)
+    err = float(np.max(np.abs(dW[sample] / oW - 1)))
+    if rank == 0:
+        print(json.dumps({
+            "metric": SCREEN_METRIC, "value": unit_work / (ms / 1e3), "unit": SCREEN_UNIT, "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"Anand screening, {ns} bump sites (132 x 132 grid over a 25 mm die), SAC305 module constants, "
+                                   f"3 cycles -40/125 degC, 15-min ramps and dwells, {nsteps} time steps",
+                       "sites": ns, "time_steps": nsteps, "l2": "inputs smaller than L2: the kernel is bound by FP64 arithmetic"},
+            "screen": {"seconds_per_screening": ms / 1e3, "reference_published_s": 15.0,
+                       "dW_max_rel_err_vs_oracle_64_sites": err, "dW_mean_mj_per_mm3": float(np.nanmean(dW))},
+            "e2e": {"value": unit_work / (ms_e2e / 1e3), "unit": SCREEN_UNIT, "h2d_bytes_per_step": int(tab.nbytes),
+                    "d2h_bytes_per_step": int(3 * 8 * ns)},
+            "cpu_baseline": cpu, "clocks": ck.summary()}))
+
+
 def main():
     a = parse()
+    if a.workload == "screen":
+        run_screen(a)
+        return
+    if a.workload == "c1":
+        global WORKLOAD
+        WORKLOAD = "fcbga_c1 48x48x20 (plain FP64 linear-elastic FCBGA, 150->25 degC step), tol 1e-8"
+        if a.precision_default:
+            a.precision = "fp64"
     if a.profile:
         run_profile(a)
     elif a.impl == "reference":

@@ -92,8 +92,16 @@ typedef struct {
   int32_t nfeatureX, nfeatureY;  /* feature lines kept at every multigrid level (06-mesher.js:504) */
   const int32_t* featureX;
   const int32_t* featureY;
+  int32_t nmodconstr;            /* stacked modules: each module's 3-2-1 support DOFs (mesh.moduleConstraints,
+                                    06-mesher.js:535-545); 0 for a package without modules */
+  const int32_t* modconstr;
 } tm_mesh;
 
+/* Stacked-module stages (stage < 0 on a mesh with module supports, 09-assembly.js:392-443): only the
+ * elements born in the stage are assembled, the constrained DOFs are the package's and every module's
+ * 3-2-1 supports plus all DOFs of the nodes no born element touches, and the multigrid hierarchy is
+ * built over the born elements and the nodes they touch (10-solver.js:260-266); the first solve after
+ * the active set changes builds that hierarchy. */
 /* Per-step property sets (FEModel.prepareStep's output, 09-assembly.js:346-365):
  * homogeneous: mean stiffness D (36) and thermal stress increment s0 (6);
  * layered: step-mean weights W_j (3 x 36) and thermal weights V_j (3 x 6). */

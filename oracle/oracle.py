@@ -38,6 +38,7 @@ def lib():
                                    C.c_int, _ip, _ip, _ip, _ip, C.c_int, C.c_int, _ip, C.c_double,
                                    C.c_int, _ip, C.c_int, _ip]
     L.orc_model_destroy.argtypes = [vp]
+    L.orc_set_module_constraints.argtypes = [vp, C.c_int, _ip]
     L.orc_model_sizes.argtypes = [vp, np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")]
     L.orc_model_mesh.argtypes = [vp] + [vp] * 8
     L.orc_assemble.argtypes = [vp, C.c_int, _ip, _dp, _dp, _dp, _dp, _ip, _dp, C.c_int]
@@ -117,6 +118,9 @@ class OracleModel:
                                     np.ascontiguousarray(pkg.sec_of_layer, np.int32), int(pkg.npset),
                                     len(con), con, 0.0, len(fx), fx if len(fx) else np.zeros(1, np.int32),
                                     len(fy), fy if len(fy) else np.zeros(1, np.int32))
+        mc = getattr(m, "moduleConstraints", None)
+        if mc is not None and len(mc):
+            L.orc_set_module_constraints(self.h, len(mc), np.ascontiguousarray(mc, np.int32))
         sz = np.zeros(5, np.int64)
         L.orc_model_sizes(self.h, sz)
         self.nn, self.ne, self.nb, self.ndof, self.ncon = (int(v) for v in sz)

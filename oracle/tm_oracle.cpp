@@ -595,7 +595,31 @@ struct Model {
   std::vector<PropSet> psets;
   int stage = 0;
   bool assembled = false;
+  // stacked modules (09-assembly.js:227, 392-443): the package's then the modules' 3-2-1 supports,
+  // and for a module stage assembled last its born elements and the nodes they touch
+  ivec moduleConstraints;
+  bool moduleStage = false;
+  std::vector<uint8_t> actElem, actNode;
 };
+
+// moduleStageSet / moduleStageConstraints (09-assembly.js:427-440): the elements born in the stage,
+// the nodes they touch, and the module constraints plus every DOF of the other nodes (sorted)
+ivec moduleStageSet(Model& M, int stage) {
+  const Mesh& m = M.mesh;
+  M.actElem.assign(m.ne, 0);
+  M.actNode.assign(m.nn, 0);
+  for (int e = 0; e < m.ne; e++) {
+    if (M.groupStage[m.eGroup[e]] > stage) continue;
+    M.actElem[e] = 1;
+    for (int a = 0; a < 8; a++) M.actNode[m.conn[8 * e + a]] = 1;
+  }
+  std::vector<uint8_t> fixed(M.ndof, 0);
+  for (int d : M.moduleConstraints) fixed[d] = 1;
+  for (int n = 0; n < m.nn; n++) if (!M.actNode[n]) fixed[3 * n] = fixed[3 * n + 1] = fixed[3 * n + 2] = 1;
+  ivec dofs;
+  for (int d = 0; d < M.ndof; d++) if (fixed[d]) dofs.push_back(d);
+  return dofs;
+}
 
 void blockMap(Model& M) {
   const Mesh& m = M.mesh; const Pattern& P = M.pattern;
@@ -630,9 +654,15 @@ void assembleStep(Model& M, double* rhs, bool noConstraints) {
   for (auto& ps : M.psets) shapeMatrices(ps.layered ? ps.W : nullptr, ps.layered ? nullptr : ps.D, ps.M);
   std::fill(M.val.begin(), M.val.end(), 0.0);
   std::fill(rhs, rhs + M.ndof, 0.0);
+  // a stacked-module stage assembles the born parts only (09-assembly.js:397-402)
+  M.moduleStage = M.stage < 0 && !M.moduleConstraints.empty();
+  ivec stageDofs;
+  if (M.moduleStage) stageDofs = moduleStageSet(M, M.stage);
+  else { M.actElem.clear(); M.actNode.clear(); }
   double K33[1089], f33[33], Kc[576], fc[24];
   for (int e = 0; e < m.ne; e++) {
     const bool born = M.groupStage[m.eGroup[e]] <= M.stage;
+    if (M.moduleStage && !born) continue;
     const double scale = m.eScale[e] * (born ? 1 : UNBORN_SCALE);
     const PropSet& ps = M.psets[M.ePset[e]];
     const int i = m.eIJK[3 * e], j = m.eIJK[3 * e + 1], k = m.eIJK[3 * e + 2];
@@ -657,7 +687,7 @@ void assembleStep(Model& M, double* rhs, bool noConstraints) {
       }
     }
   }
-  if (!noConstraints) applyConstraints(M, rhs, M.constraints);
+  if (!noConstraints) applyConstraints(M, rhs, M.moduleStage ? stageDofs : M.constraints);
   M.assembled = true;
 }
 
@@ -884,8 +914,13 @@ int cellElemAt(const Mesh& mesh, long c, int q) {
   return mesh.cellElems[idx];
 }
 
-// buildShellLevel :260-334 (no stacked-module active set); s = Jacobi scaling
-void buildShellLevel(Level& L, Level& C, const Mesh& mesh, const double* s, const char* mergeSingles) {
+// buildShellLevel :260-334; s = Jacobi scaling. act (stacked-module stages, :262-266): when actElem is
+// not empty, the elements not born in the stage count as void and the nodes they alone touch stay
+// out of every aggregate
+void buildShellLevel(Level& L, Level& C, const Mesh& mesh, const double* s, const char* mergeSingles,
+                     const std::vector<uint8_t>& actElem, const std::vector<uint8_t>& actNode) {
+  const bool act = !actElem.empty();
+  auto elemOn = [&](int e) { return e >= 0 && (!act || actElem[e]); };
   const int nx = L.nx, ny = L.ny, nz = L.nz, ncy = ny - 1, ncz = nz - 1;
   const int ncol = nx * ny;
   C.colStart.assign(ncol + 1, 0);
@@ -897,7 +932,7 @@ void buildShellLevel(Level& L, Level& C, const Mesh& mesh, const double* s, cons
     bool any = false, stiff = false;
     for (int q = 0; q < 2; q++) {
       const int e = cellElemAt(mesh, c, q);
-      if (e < 0) continue;
+      if (!elemOn(e)) continue;
       any = true;
       if (!is_compliant_part(mesh.ePart[e])) stiff = true;
     }
@@ -905,7 +940,7 @@ void buildShellLevel(Level& L, Level& C, const Mesh& mesh, const double* s, cons
   };
   auto hasElem = [&](int i, int j, int k) {
     const long c = ((long)i * ncy + j) * ncz + k;
-    return cellElemAt(mesh, c, 0) >= 0 || cellElemAt(mesh, c, 1) >= 0;
+    return elemOn(cellElemAt(mesh, c, 0)) || elemOn(cellElemAt(mesh, c, 1));
   };
   auto elemClass = [&](int i, int j, int k) -> int {
     return (k < 0 || k >= ncz || !hasElem(i, j, k)) ? 0 : (isCompliant(i, j, k) ? 1 : 2);
@@ -919,7 +954,7 @@ void buildShellLevel(Level& L, Level& C, const Mesh& mesh, const double* s, cons
     int cur = -1, prevK = -2, prevType = 0;   // cur: index of the current run, -1 = none
     for (int k = 0; k < nz; k++) {
       const int n = mesh.nodeId[(size_t)c * nz + k];
-      if (n < 0) { cur = -1; prevK = -2; continue; }
+      if (n < 0 || (act && !actNode[n])) { cur = -1; prevK = -2; continue; }
       const int below = elemClass(i, j, k - 1), above = elemClass(i, j, k);
       const int type = (below == 2 || above == 2) ? 2 : 1;
       bool joined = false;
@@ -1205,7 +1240,8 @@ struct MultigridPC : Precond {
   bool symmetric = false;
   int colJitter = 0, shellJitter = 0;
 
-  MultigridPC(const Mesh& mesh, const Pattern& P, const dvec& val, const dvec& s) {
+  MultigridPC(const Mesh& mesh, const Pattern& P, const dvec& val, const dvec& s, const std::vector<uint8_t>& actElem,
+              const std::vector<uint8_t>& actNode) {
     const double t0 = now_ms();
     auto fine = std::make_unique<Level>();
     fine->solid = true; fine->b = 3; fine->nx = mesh.nx; fine->ny = mesh.ny; fine->nz = mesh.nz; fine->nn = mesh.nn;
@@ -1217,7 +1253,7 @@ struct MultigridPC : Precond {
     colJitter = fine->colJitter;
     levels.push_back(std::move(fine));
     auto lv = std::make_unique<Level>();
-    buildShellLevel(*levels[0], *lv, mesh, s.data(), "below");
+    buildShellLevel(*levels[0], *lv, mesh, s.data(), "below", actElem, actNode);
     levels.push_back(std::move(lv));
     for (int guard = 0; guard < 20; guard++) {
       Level& cur = *levels.back();
@@ -1384,10 +1420,10 @@ struct LinearSolver {
     }
   }
 
-  // _buildPC :868-882 (a new hierarchy each time: the oracle has no stacked-module stages)
+  // _buildPC :868-882 (a new hierarchy each time, over the active set of a stacked-module stage)
   double buildPC(int kind) {
     const double t0 = now_ms();
-    if (kind == 0) pc.reset(new MultigridPC(model->mesh, model->pattern, model->val, s));
+    if (kind == 0) pc.reset(new MultigridPC(model->mesh, model->pattern, model->val, s, model->actElem, model->actNode));
     else pc.reset(new ICPC(model->pattern, model->val));
     pcKind = kind;
     needRebuild = false;
@@ -2646,6 +2682,15 @@ orc_model* orc_model_create(int nx, int ny, int nz, const double* xs, const doub
 }
 
 void orc_model_destroy(orc_model* o) { delete o; }
+
+// the stacked modules' 3-2-1 support DOFs (mesh.moduleConstraints): the model's module constraints are
+// the package's constraints followed by these (09-assembly.js:227)
+void orc_set_module_constraints(orc_model* o, int n, const int* dofs) {
+  Model& M = o->M;
+  M.moduleConstraints = M.constraints;
+  M.moduleConstraints.insert(M.moduleConstraints.end(), dofs, dofs + n);
+  if (n <= 0) M.moduleConstraints.clear();
+}
 
 // sizes: nn, ne, nb, ndof, nconstr
 void orc_model_sizes(orc_model* o, long* out) {

@@ -572,6 +572,12 @@ tm_status tm_create(const tm_mesh* m, tm_ctx** out) {
       c->constr.assign(m->constr, m->constr + m->nconstr);
       if (m->nfeatureX > 0) c->featureX.assign(m->featureX, m->featureX + m->nfeatureX);
       if (m->nfeatureY > 0) c->featureY.assign(m->featureY, m->featureY + m->nfeatureY);
+      c->meshConstr = c->constr;
+      if (m->nmodconstr > 0) {   // the model's module constraints: the package's then the modules' (09-assembly.js:227)
+        if (!m->modconstr) fail(TM_BAD_INPUT, "module constraints: null list");
+        c->modConstr = c->constr;
+        c->modConstr.insert(c->modConstr.end(), m->modconstr, m->modconstr + m->nmodconstr);
+      }
       // index validation (no device access is made with unchecked indices)
       for (int v : c->conn) if (v < 0 || v >= c->nn) fail(TM_BAD_INPUT, "conn index out of range");
       for (int v : c->nodeId) if (v >= c->nn) fail(TM_BAD_INPUT, "nodeId out of range");
@@ -579,6 +585,7 @@ tm_status tm_create(const tm_mesh* m, tm_ctx** out) {
       for (int v : c->eGroup) if (v < 0 || v >= c->ngroups) fail(TM_BAD_INPUT, "eGroup out of range");
       for (int v : c->ePset) if (v < 0 || v >= c->npset) fail(TM_BAD_INPUT, "ePset out of range");
       for (int v : c->constr) if (v < 0 || v >= 3 * c->nn) fail(TM_BAD_INPUT, "constraint DOF out of range");
+      for (int v : c->modConstr) if (v < 0 || v >= 3 * c->nn) fail(TM_BAD_INPUT, "module constraint DOF out of range");
       if (c->colStart.back() != c->nn) fail(TM_BAD_INPUT, "colStart does not cover the nodes");
       build_stencil(*c);
       build_classes(*c);
@@ -607,6 +614,46 @@ void check_step(const Context& c, const tm_step& st) {
 }
 }  // namespace
 
+namespace {
+// the active set and constraints of a stage (moduleStageSet / moduleStageConstraints,
+// 09-assembly.js:427-443): in a stacked-module stage the born elements, the nodes they touch and
+// the module constraints plus every DOF of the other nodes (sorted); otherwise the whole package
+// with the mesh's constraints. A change of the active set rebuilds the hierarchy (the reference's
+// _buildPC keyed on activeKey, 10-solver.js:868-876).
+void set_active_stage(Context& c, int stage) {
+  const bool moduleStage = stage < 0 && !c.modConstr.empty();
+  c.moduleStage = moduleStage;
+  const int key = moduleStage ? stage : 0;
+  if (moduleStage) {
+    c.actElem.assign(c.ne, 0);
+    c.actNode.assign(c.nn, 0);
+    for (int e = 0; e < c.ne; e++) {
+      if (c.groupStage[c.eGroup[e]] > stage) continue;
+      c.actElem[e] = 1;
+      for (int a = 0; a < 8; a++) c.actNode[c.conn[8 * (size_t)e + a]] = 1;
+    }
+    std::vector<uint8_t> fixed(3 * (size_t)c.nn, 0);
+    for (int d : c.modConstr) fixed[d] = 1;
+    for (int n = 0; n < c.nn; n++)
+      if (!c.actNode[n]) fixed[3 * (size_t)n] = fixed[3 * (size_t)n + 1] = fixed[3 * (size_t)n + 2] = 1;
+    c.constr.clear();
+    for (int d = 0; d < 3 * c.nn; d++) if (fixed[d]) c.constr.push_back(d);
+  } else {
+    c.actElem.clear();
+    c.actNode.clear();
+    c.constr = c.meshConstr;   // (a caller-assembled operator, tm_set_bcsr, may have loaded its own list)
+  }
+  c.d_constr.upload(c.constr, c.stream);
+  if (key != c.hierKey) {
+    c.activeKey = key;
+    build_hierarchy(c);
+    c.hierKey = key;
+    c.needRebuild = true;
+    c.pcReady = false;
+  }
+}
+}  // namespace
+
 tm_status tm_prepare_step(tm_ctx* ctx, const tm_step* st) {
   return guarded([&] {
     if (!ctx || !st) fail(TM_BAD_INPUT, "null argument");
@@ -624,6 +671,7 @@ tm_status tm_assemble_step(tm_ctx* ctx, const tm_step* st, double* rhs_out) {
     check_step(c, *st);
     launch_shape_matrices(c, *st);
     launch_class_condense(c);
+    set_active_stage(c, st->stage);
     mf_build_cells(c, st->stage);
     launch_mf_combine(c);
     launch_assemble(c);

@@ -250,7 +250,9 @@ void galerkin_lists01(Context& c, cudaStream_t st) {
       for (int ps = 0; ps < nn; ps++) {
         const int i = c.posNode[ps];
         if (!(c.slotMask[i] >> s & 1)) continue;
-        const int k = block_of(L1, c.nodeAgg[i], c.nodeAgg[c.nbr[(size_t)s * nn + i]]);
+        const int I = c.nodeAgg[i], J = c.nodeAgg[c.nbr[(size_t)s * nn + i]];
+        if (I < 0 || J < 0) continue;   // held nodes have no prolongation
+        const int k = block_of(L1, I, J);
         if (k < 0) fail(TM_BAD_INPUT, "level-1 Galerkin pattern misses a stencil coupling");
         emit(k, ps * NSLOT + s);
       }
@@ -408,7 +410,11 @@ void build_hierarchy(Context& c) {
   const int nx = c.nx, ny = c.ny, nz = c.nz, ncy = ny - 1, ncz = nz - 1, nn = c.nn;
   for (auto* L : c.shells) delete L;
   c.shells.clear();
-  // ---- level 1: buildShellLevel (10-solver.js:260-334), mergeSingles 'below' (:626)
+  // ---- level 1: buildShellLevel (10-solver.js:260-334), mergeSingles 'below' (:626). In a
+  // stacked-module stage (c.actElem / c.actNode set, 10-solver.js:262-266) the elements not born in
+  // the stage count as void and the nodes they alone touch (held) stay out of every aggregate.
+  const bool act = !c.actElem.empty();
+  auto elemOn = [&](int e) { return e >= 0 && (!act || c.actElem[e]); };
   ShellLevel* L1 = new ShellLevel();
   L1->nx = nx; L1->ny = ny; L1->xs = c.xs; L1->ys = c.ys;
   L1->colStart.assign((size_t)nx * ny + 1, 0);
@@ -418,7 +424,7 @@ void build_hierarchy(Context& c) {
     bool any = false, stiff = false;
     for (int q = 0; q < 2; q++) {
       const int e = cell_elem_at(c, cell, q);
-      if (e < 0) continue;
+      if (!elemOn(e)) continue;
       any = true;
       if (!compliant_part(c.ePart[e])) stiff = true;
     }
@@ -426,7 +432,7 @@ void build_hierarchy(Context& c) {
   };
   auto hasElem = [&](int i, int j, int k) {
     const long cell = ((long)i * ncy + j) * ncz + k;
-    return cell_elem_at(c, cell, 0) >= 0 || cell_elem_at(c, cell, 1) >= 0;
+    return elemOn(cell_elem_at(c, cell, 0)) || elemOn(cell_elem_at(c, cell, 1));
   };
   auto elemClass = [&](int i, int j, int k) -> int {
     return (k < 0 || k >= ncz || !hasElem(i, j, k)) ? 0 : (isCompliant(i, j, k) ? 1 : 2);
@@ -440,7 +446,7 @@ void build_hierarchy(Context& c) {
     int cur = -1, prevK = -2, prevType = 0;
     for (int k = 0; k < nz; k++) {
       const int n = c.nodeId[(size_t)col * nz + k];
-      if (n < 0) { cur = -1; prevK = -2; continue; }
+      if (n < 0 || (act && !c.actNode[n])) { cur = -1; prevK = -2; continue; }
       const int below = elemClass(i, j, k - 1), above = elemClass(i, j, k);
       const int type = (below == 2 || above == 2) ? 2 : 1;
       bool joined = false;
@@ -465,16 +471,28 @@ void build_hierarchy(Context& c) {
   }
   L1->colStart[(size_t)nx * ny] = na;
   L1->nn = na;
-  // every node is in exactly one aggregate and aggregates are contiguous node ranges
-  c.aggStart.assign(na + 1, 0);
+  // every node outside the held ones is in exactly one aggregate; the members of aggregate I are
+  // aggNodes[aggPtr[I] .. aggPtr[I+1]-1] in ascending node order (a contiguous node range unless held
+  // nodes lie between them)
+  c.aggPtr.assign(na + 1, 0);
   for (int n = 0; n < nn; n++) {
-    if (c.nodeAgg[n] < 0) fail(TM_BAD_INPUT, "node outside every multigrid aggregate");
-    if (n > 0 && c.nodeAgg[n] != c.nodeAgg[n - 1] && c.nodeAgg[n] != c.nodeAgg[n - 1] + 1) fail(TM_BAD_INPUT, "aggregates are not contiguous");
-    if (n == 0 || c.nodeAgg[n] != c.nodeAgg[n - 1]) c.aggStart[c.nodeAgg[n]] = n;
+    const int a = c.nodeAgg[n];
+    if (a < 0) {
+      if (!act || c.actNode[n]) fail(TM_BAD_INPUT, "node outside every multigrid aggregate");
+      continue;
+    }
+    c.aggPtr[a + 1]++;
   }
-  c.aggStart[na] = nn;
+  for (int a = 0; a < na; a++) c.aggPtr[a + 1] += c.aggPtr[a];
+  c.aggNodes.assign(c.aggPtr[na], 0);
+  {
+    std::vector<int> fill(c.aggPtr.begin(), c.aggPtr.end() - 1);
+    for (int n = 0; n < nn; n++)
+      if (c.nodeAgg[n] >= 0) c.aggNodes[fill[c.nodeAgg[n]]++] = n;
+  }
   c.zp.assign(nn, 0.0);
-  for (int n = 0; n < nn; n++) c.zp[n] = c.coords[3 * (size_t)n + 2] - L1->zref[c.nodeAgg[n]];
+  for (int n = 0; n < nn; n++)
+    if (c.nodeAgg[n] >= 0) c.zp[n] = c.coords[3 * (size_t)n + 2] - L1->zref[c.nodeAgg[n]];
   L1->hasKeep = !c.featureX.empty() || !c.featureY.empty();
   L1->keepX = c.featureX; L1->keepY = c.featureY;
   // Galerkin pattern 0 -> 1 over the block pattern of the solid level
@@ -484,11 +502,13 @@ void build_hierarchy(Context& c) {
     int maxr = 0;
     for (int I = 0; I < na; I++) {
       touched.clear();
-      for (int i = c.aggStart[I]; i < c.aggStart[I + 1]; i++) {
+      for (int q = c.aggPtr[I]; q < c.aggPtr[I + 1]; q++) {
+        const int i = c.aggNodes[q];
         const int mask = c.slotMask[i];
         for (int s = 0; s < NSLOT; s++) {
           if (!(mask >> s & 1)) continue;
           const int J = c.nodeAgg[c.nbr[(size_t)s * nn + i]];
+          if (J < 0) continue;   // a held neighbour (no prolongation)
           if (mark[J] != I) { mark[J] = I; touched.push_back(J); }
         }
       }
@@ -566,7 +586,8 @@ void build_hierarchy(Context& c) {
   if (c.colourPos[4] != nn) fail(TM_BAD_INPUT, "colours do not cover the positions");
   plan_sweep_tma(c, colPos, st);
   c.d_nodeAgg.upload(c.nodeAgg, st);
-  c.d_aggStart.upload(c.aggStart, st);
+  c.d_aggPtr.upload(c.aggPtr, st);
+  c.d_aggNodes.upload(c.aggNodes, st);
   galerkin_lists01(c, st);
   for (size_t l = 0; l + 1 < c.shells.size(); l++) galerkin_lists_shell(*c.shells[l], *c.shells[l + 1], st);
   c.d_zp.upload(c.zp, st);

@@ -219,7 +219,7 @@ struct Context {
   // elements) whose combined condensed matrix is formed per step; per DOF the gather scale gs (S,
   // zero at constrained DOFs), the row scale os (S) and the kept diagonal cd of constrained rows
   bool mf = false;                     // level 0 is applied from the cell-class table (operator from tm_assemble_step)
-  bool mfBuilt = false, mfAvailable = false;
+  bool mfBuilt = false, mfAvailable = false, mfModule = false;
   int mfStage = 0;                     // stage the cell classes were built for (element birth scales)
   int ncc = 0;
   DBuf<uint16_t> d_cellCls;            // per cell, 0xFFFF: no element
@@ -291,9 +291,16 @@ struct Context {
   DBuf<int> d_grpStart[4], d_colPos[4];
   int colourPos[5] = {0, 0, 0, 0, 0};  // colour k occupies positions colourPos[k] .. colourPos[k+1]-1
   int grpCount[4] = {0, 0, 0, 0};
-  std::vector<int> nodeAgg, aggStart;  // level 0 -> 1
+  std::vector<int> nodeAgg, aggPtr, aggNodes;   // level 0 -> 1 (nodeAgg -1: a held node of a module stage)
   std::vector<double> zp;              // z of node minus zref of its aggregate
-  DBuf<int> d_nodeAgg, d_aggStart;
+  DBuf<int> d_nodeAgg, d_aggPtr, d_aggNodes;
+  // stacked-module stages (09-assembly.js:397-443): the constraints of those stages (the package's
+  // 3-2-1 plus each module's own), and for the stage assembled last its born elements and the nodes
+  // they touch (empty outside module stages); the hierarchy is built for activeKey (0: the whole package)
+  std::vector<int> modConstr, meshConstr;
+  std::vector<uint8_t> actElem, actNode;
+  int activeKey = 0, hierKey = 0;
+  bool moduleStage = false;            // the step assembled last is a stacked-module stage (unborn elements skipped)
   // Galerkin contributions of the solid operator to the level-1 blocks: per block the
   // (position, slot) pairs, coded position*27 + slot, in (slot, position) order
   DBuf<int> d_g01Start, d_g01List;

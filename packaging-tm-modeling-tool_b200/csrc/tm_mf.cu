@@ -455,7 +455,7 @@ void mf_apply(Context& c, const T* ccK, const T* gs, const T* os, const T* cd, c
 // cell classes of the mesh at a stage: (class, scale) of each of the cell's elements, scale = eScale
 // (times 1e-6 before the element's group is born, 09-assembly.js:401-403)
 void mf_build_cells(Context& c, int stage) {
-  if (c.mfStage == stage && c.mfBuilt) return;
+  if (c.mfStage == stage && c.mfBuilt && c.mfModule == c.moduleStage) return;
   const int ncy = c.ny - 1, ncz = c.nz - 1;
   const size_t ncells = (size_t)(c.nx - 1) * ncy * ncz;
   std::map<std::tuple<int, double, int, double>, int> key;
@@ -470,8 +470,10 @@ void mf_build_cells(Context& c, int stage) {
     for (int e2 = 0; e2 < 2; e2++) {
       const int e = c.cellElems[2 * cell + e2];
       if (e < 0) continue;
+      const bool born = c.groupStage[c.eGroup[e]] <= stage;
+      if (c.moduleStage && !born) continue;   // module stages assemble the born parts only
       cl[q] = c.eClass[e];
-      sc[q] = c.eScale[e] * (c.groupStage[c.eGroup[e]] <= stage ? 1.0 : 1e-6);
+      sc[q] = c.eScale[e] * (born ? 1.0 : 1e-6);
       q++;
     }
     if (!q) continue;
@@ -493,6 +495,7 @@ void mf_build_cells(Context& c, int stage) {
   TM_CUDA_CHECK(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.dev));
   c.mfBuilt = true;
   c.mfStage = stage;
+  c.mfModule = c.moduleStage;
   // the colour sweep stages whole node columns: meshes with too many node planes keep the stencil
   c.mfAvailable = ok && !key.empty() && TM_MATRIX_FREE && mf_sweep_smem(c.nz) <= (size_t)smemMax &&
                   mf_apply_smem<double>(apply_dims(c).ks) <= (size_t)smemMax;

@@ -345,7 +345,7 @@ __device__ __forceinline__ int loc_index(int a, int b, int c) {
 __global__ void k_assemble(int nn, int S, int nx, int ny, int nz, const int* __restrict__ posNode, const int* __restrict__ nodeIJK,
                            const int* __restrict__ nbr, const int* __restrict__ cellElems, const int* __restrict__ eClass,
                            const double* __restrict__ eScale, const int* __restrict__ eGroup, const int* __restrict__ groupStage, int stage,
-                           const double* __restrict__ clsKc, double* __restrict__ val) {
+                           int moduleStage, const double* __restrict__ clsKc, double* __restrict__ val) {
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= (size_t)NSLOT * S) return;
   const int s = (int)(t / S), ps = (int)(t % S);
@@ -373,6 +373,7 @@ __global__ void k_assemble(int nn, int S, int nx, int ny, int nz, const int* __r
             const int e = cellElems[2 * cell + q];
             if (e < 0) continue;
             const bool born = groupStage[eGroup[e]] <= stage;
+            if (moduleStage && !born) continue;   // module stages assemble the born parts only
             const double scale = eScale[e] * (born ? 1.0 : 1e-6);
             const double* Kc = clsKc + (size_t)eClass[e] * 576;
             for (int p = 0; p < 3; p++) {
@@ -390,7 +391,7 @@ __global__ void k_assemble(int nn, int S, int nx, int ny, int nz, const int* __r
 // thermal load, thread per node (assembleStep's rhs, 09-assembly.js:417-420)
 __global__ void k_assemble_rhs(int nn, int nx, int ny, int nz, const int* __restrict__ nodeIJK, const int* __restrict__ cellElems,
                                const int* __restrict__ eClass, const double* __restrict__ eScale, const int* __restrict__ eGroup,
-                               const int* __restrict__ groupStage, int stage, const int* __restrict__ clsBorn,
+                               const int* __restrict__ groupStage, int stage, int moduleStage, const int* __restrict__ clsBorn,
                                const double* __restrict__ clsFc, double* __restrict__ rhs) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nn) return;
@@ -408,6 +409,7 @@ __global__ void k_assemble_rhs(int nn, int nx, int ny, int nz, const int* __rest
           const int cls = eClass[e];
           if (!clsBorn[cls]) continue;
           const bool born = groupStage[eGroup[e]] <= stage;
+          if (moduleStage && !born) continue;
           const double scale = eScale[e] * (born ? 1.0 : 1e-6);
           const double* fc = clsFc + (size_t)cls * 24;
           acc0 += scale * fc[3 * a];
@@ -1017,13 +1019,13 @@ void launch_assemble(Context& c) {
   {
   TimedLaunch tl(c, K_ASSEMBLE);
   k_assemble<<<grid_for(tot, 256), 256, 0, c.stream>>>(c.nn, c.nnp, c.nx, c.ny, c.nz, c.d_posNode.p, c.d_nodeIJK.p, c.d_nbr.p, c.d_cellElems.p,
-                                                      c.d_eClass.p, c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsKc.p,
-                                                      c.d_val.p);
+                                                      c.d_eClass.p, c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.moduleStage ? 1 : 0,
+                                                      c.d_clsKc.p, c.d_val.p);
   }
   TM_CUDA_CHECK(cudaGetLastError());
   k_assemble_rhs<<<grid_for(c.nn, 256), 256, 0, c.stream>>>(c.nn, c.nx, c.ny, c.nz, c.d_nodeIJK.p, c.d_cellElems.p, c.d_eClass.p,
-                                                           c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.d_clsBorn.p,
-                                                           c.d_clsFc.p, c.d_rhs.p);
+                                                           c.d_eScale.p, c.d_eGroup.p, c.d_groupStage.p, c.stage, c.moduleStage ? 1 : 0,
+                                                           c.d_clsBorn.p, c.d_clsFc.p, c.d_rhs.p);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 

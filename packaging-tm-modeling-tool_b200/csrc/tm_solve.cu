@@ -278,16 +278,17 @@ __global__ void __launch_bounds__(TM_PANEL_THREADS, PanelMinBlocks<T>::value)
   }
 }
 
-// restriction 0 -> 1: rc = P^T res, thread per aggregate (children are a contiguous node range)
+// restriction 0 -> 1: rc = P^T res, thread per aggregate over its member nodes (ascending)
 template <class T>
-__global__ void k_restrict0(int na, const int* __restrict__ aggStart, const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc,
-                            T* __restrict__ xc) {
+__global__ void k_restrict0(int na, const int* __restrict__ aggPtr, const int* __restrict__ aggNodes, const T* __restrict__ W,
+                            const T* __restrict__ res, T* __restrict__ rc, T* __restrict__ xc) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= na) return;
 #pragma unroll
   for (int a = 0; a < 6; a++) xc[6 * (size_t)I + a] = 0;   // the level's iterate starts at zero
   T acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int f = aggStart[I]; f < aggStart[I + 1]; f++) {
+  for (int q = aggPtr[I]; q < aggPtr[I + 1]; q++) {
+    const int f = aggNodes[q];
     const T* w = W + 18 * (size_t)f;
     const T r0 = res[3 * f], r1 = res[3 * f + 1], r2 = res[3 * f + 2];
 #pragma unroll
@@ -302,8 +303,10 @@ template <class T>
 __global__ void k_prolong0(int nn, const int* __restrict__ nodeAgg, const T* __restrict__ W, const T* __restrict__ ec, T* __restrict__ x) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nn) return;
+  const int a = nodeAgg[n];
+  if (a < 0) return;   // a held node of a module stage: no prolongation
   const T* w = W + 18 * (size_t)n;
-  const T* e = ec + 6 * (size_t)nodeAgg[n];
+  const T* e = ec + 6 * (size_t)a;
 #pragma unroll
   for (int p = 0; p < 3; p++) {
     T s = 0;
@@ -632,7 +635,8 @@ void vcycle(Context& c, const T* r, T* z) {
     }
   }
   ShellLevel& L1 = *c.shells[0];
-  k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggStart.p, B::W01(c), B::res0(c), B::b(L1), B::x(L1));
+  k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggPtr.p, c.d_aggNodes.p, B::W01(c), B::res0(c), B::b(L1),
+                                                                  B::x(L1));
   note_launch();
   const size_t nl = c.shells.size();
   for (size_t l = 0; l < nl; l++) {

@@ -42,7 +42,8 @@ class TmMesh(C.Structure):
                 ("coords", dp), ("nodeId", ip), ("conn", ip), ("eIJK", ip), ("colStart", ip), ("cellElems", ip),
                 ("eGroup", ip), ("ePart", C.POINTER(C.c_int8)), ("eScale", dp), ("ngroups", C.c_int32), ("groupStage", ip),
                 ("npset", C.c_int32), ("ePset", ip), ("nconstr", C.c_int32), ("constr", ip),
-                ("nfeatureX", C.c_int32), ("nfeatureY", C.c_int32), ("featureX", ip), ("featureY", ip)]
+                ("nfeatureX", C.c_int32), ("nfeatureY", C.c_int32), ("featureX", ip), ("featureY", ip),
+                ("nmodconstr", C.c_int32), ("modconstr", ip)]
 
 
 class TmStep(C.Structure):

@@ -204,6 +204,23 @@ def sac305_tables():
     return Et, Ft
 
 
+# SAC305 Anand constant set of the stacked-module thermal-cycle workload (s0 = 45.9 MPa, Q/R = 7460 K,
+# A = 5.87e6 1/s, xi = 2, m = 0.0942, h0 = 9350 MPa, s_hat = 58.3 MPa, n = 0.015, a = 1.5) with a
+# linear E(T) through the database's end points (57.4 GPa at -40 degC, 30.0 GPa at 125 degC)
+SAC305_MODULE = dict(A=5.87e6, QR=7460.0, xi=2.0, m=0.0942, shat=58.3, n=0.015, h0=9350.0, a=1.5, s0=45.9, nu=0.4,
+                     E_T=[-40.0, 125.0], E_GPa=[57.4, 30.0], solidus=217.0, cte=22.5e-6)
+
+
+def anand_tables(p: dict):
+    """E(T) (MPa, linear table with linear extrapolation, 1 % above the solidus) and F(T) = alpha (T - 25)
+    on the 1 degC grid for an Anand parameter set with E_T / E_GPa / solidus / cte entries."""
+    def E(T):
+        if T > p["solidus"]:
+            return 0.01 * interp_table_linear(p["E_T"], p["E_GPa"], p["solidus"]) * 1000.0
+        return interp_table_linear(p["E_T"], p["E_GPa"], T) * 1000.0
+    return grid_table(E), grid_table(lambda T: p["cte"] * (T - T_STRAIN_ORIGIN))
+
+
 def anand_params_array(p: dict) -> np.ndarray:
     """Parameter vector (A, Q/R, xi, m, s_hat, n, h0, a, s0, nu) of the Anand entry points."""
     return np.array([p["A"], p["QR"], p["xi"], p["m"], p["shat"], p["n"], p["h0"], p["a"], p["s0"], p["nu"]], np.float64)

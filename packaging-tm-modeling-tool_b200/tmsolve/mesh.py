@@ -11,9 +11,12 @@ contract of the boundary:
   local node order ``loc`` (06-mesher.js:49); column c = i*ny + j holds the
   contiguous node range colStart[c] .. colStart[c+1]-1.
 * ``constraints321`` (06-mesher.js:112-116) with ``nearestNodeOnPlane`` (:75-84).
+* ``module_support`` (``moduleSupport``, 06-mesher.js:92-109): the three support nodes of a
+  stacked module on its base bottom plane.
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -49,6 +52,9 @@ class Mesh:
     featureX: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     featureY: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     constraints: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    # stacked modules: each module's 3-2-1 support DOFs on its base bottom (mesh.moduleConstraints,
+    # 06-mesher.js:535-545), None for a package without modules
+    moduleConstraints: np.ndarray = None
 
     @property
     def ndof(self) -> int:
@@ -134,3 +140,37 @@ def constraints321(mesh: Mesh, a: float) -> np.ndarray:
     n1 = nearest_node_on_plane(mesh, a, 0.0, 0)
     n2 = nearest_node_on_plane(mesh, 0.0, a, 0)
     return np.array([3 * n0, 3 * n0 + 1, 3 * n0 + 2, 3 * n1 + 1, 3 * n1 + 2, 3 * n2 + 2], np.int32)
+
+
+def module_support(mesh: Mesh, rect: dict, cx: float, cy: float, k: int):
+    """moduleSupport (06-mesher.js:92-109): three nodes of plane k inside rect (x0, x1, y0, y1):
+    a the nearest to (cx, cy), b on a's row farthest from it in x, c off that row, farthest in y
+    (ties to the smaller x distance); None when there are too few."""
+    tol = 1e-9
+    cand = []
+    for i in range(mesh.nx):
+        x = float(mesh.xs[i])
+        if x < rect["x0"] - tol or x > rect["x1"] + tol:
+            continue
+        for j in range(mesh.ny):
+            y = float(mesh.ys[j])
+            nid = int(mesh.nodeId[(i * mesh.ny + j) * mesh.nz + k])
+            if nid >= 0 and rect["y0"] - tol <= y <= rect["y1"] + tol:
+                cand.append((nid, x, y))
+    if len(cand) < 3:
+        return None
+
+    def pick(score, ok):
+        best, bs = None, -math.inf
+        for c in cand:
+            if ok(c):
+                s = score(c)
+                if s > bs + tol:
+                    bs, best = s, c
+        return best
+    a = pick(lambda c: -math.hypot(c[1] - cx, c[2] - cy), lambda c: True)
+    b = pick(lambda c: abs(c[1] - a[1]), lambda c: abs(c[2] - a[2]) < tol and c[0] != a[0])
+    if b is None:
+        return None
+    c = pick(lambda c: abs(c[2] - a[2]) - 1e-6 * abs(c[1] - a[1]), lambda c: abs(c[2] - a[2]) > tol)
+    return None if c is None else [a[0], b[0], c[0]]

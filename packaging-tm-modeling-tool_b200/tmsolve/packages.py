@@ -26,7 +26,7 @@ from typing import Callable, List, Optional
 import numpy as np
 
 from .materials import column_d, iso_d, layered_section, thermal_stress_const
-from .mesh import PART, Mesh, build_structured_mesh, constraints321
+from .mesh import PART, Mesh, build_structured_mesh, constraints321, module_support
 
 CONSTRAINT_SPAN = 0.4   # 00-constants.js:52
 
@@ -71,8 +71,23 @@ class Package:
         lay = self.group_layered[m.eGroup] != 0
         return np.where(lay, self.sec_of_layer[k], self.group_pset[m.eGroup]).astype(np.int32)
 
-    def step(self, Ta: Optional[float] = None, Tb: Optional[float] = None) -> StepData:
-        return self.step_fn(self.Ta if Ta is None else Ta, self.Tb if Tb is None else Tb)
+    def step(self, Ta: Optional[float] = None, Tb: Optional[float] = None, stage: int = 0) -> StepData:
+        """prepareStep's property sets from Ta to Tb in a stage: a set's thermal load is on when one
+        of its groups is born in the stage (09-assembly.js:346-365, isBorn :339)."""
+        st = self.step_fn(self.Ta if Ta is None else Ta, self.Tb if Tb is None else Tb)
+        st.stage = int(stage)
+        if stage != 0 or np.any(self.group_stage != 0):
+            born = np.zeros(self.npset, np.int32)
+            k = self.mesh.eIJK[2::3]
+            for g in range(len(self.group_stage)):
+                if self.group_stage[g] > stage:
+                    continue
+                if self.group_layered[g]:
+                    born[np.unique(self.sec_of_layer[k[self.mesh.eGroup == g]])] = 1
+                else:
+                    born[self.group_pset[g]] = 1
+            st.born = born
+        return st
 
 
 def _homog_step(mats, Ta, Tb, npset=None, layered_fn=None) -> StepData:
@@ -280,6 +295,108 @@ def lidded_c2(n_inplane: int = 160, seed: int = 20261203) -> Package:
                              die=dict(cx=0.0, cy=0.0, w=25.0, h=25.0, keepout=0.2, px=0.15, py=0.15),
                              bga=dict(sx=L, sy=L, inset=1.0, pitch=1.0),
                              bump_layer=dict(zmid=z0 + 0.5 * t_bump, part=PART["SOLDER"])))
+
+
+def stacked_module(n_inplane: int = 192) -> Package:
+    """Stacked-module package under a thermal cycle: 45 x 45 x 1.0 mm substrate, SAC305 bump layer
+    (0.08 mm, solder columns 30 % with underfill) under a 30 x 30 x 0.1 mm Si base die, a 0.03 mm
+    microbump / wafer-underfill layer, four 12 x 12 x 0.6 mm chiplets (2 x 2, 2 mm apart) in wafer
+    mold. The module (base die, microbumps, chiplets, mold) is born in stage -1 and stands on its own
+    3-2-1 support on the base die bottom; the substrate and the bump layer are born in stage 0.
+    n x n uniform in-plane cells, 15 element layers; n = 192 gives about 1.2M DOF. Solder E falls
+    linearly with temperature (57.4 GPa at -40 degC, 30.0 GPa at 125 degC); the other materials are
+    database-like 25 degC constants."""
+    n = n_inplane
+    L = 45.0
+    xs = np.array([-L / 2 + L * q / n for q in range(n + 1)])
+    ys = xs.copy()
+    t_sub, t_bump, t_base, t_mb, t_chip = 1.0, 0.08, 0.1, 0.03, 0.6
+    zs = _graded_lines([(0.0, t_sub, 6), (t_sub, t_sub + t_bump, 2), (t_sub + t_bump, t_sub + t_bump + t_base, 2),
+                        (t_sub + t_bump + t_base, t_sub + t_bump + t_base + t_mb, 1),
+                        (t_sub + t_bump + t_base + t_mb, t_sub + t_bump + t_base + t_mb + t_chip, 4)])
+    nz = len(zs)
+    ncz = nz - 1
+    idx = lambda x: int(round((x + L / 2) / L * n))
+    b0, b1 = idx(-15.0), idx(15.0)
+    chips = [(idx(-13.0), idx(-1.0)), (idx(1.0), idx(13.0))]
+    ncells = n * n * ncz
+    cg = np.full(2 * ncells, -1, np.int32); cp = np.zeros(2 * ncells, np.int32); cs = np.zeros(2 * ncells)
+    I, J, K = np.meshgrid(np.arange(n), np.arange(n), np.arange(ncz), indexing="ij")
+    c = ((I * n + J) * ncz + K).ravel(); I = I.ravel(); J = J.ravel(); K = K.ravel()
+    in_base = (I >= b0) & (I < b1) & (J >= b0) & (J < b1)
+    in_chip = np.zeros_like(in_base)
+    for (x0, x1) in chips:
+        for (y0, y1) in chips:
+            in_chip |= (I >= x0) & (I < x1) & (J >= y0) & (J < y1)
+    G = dict(sub=0, solder=1, uf=2, base=3, ddi=4, fill=5, chip=6, mold=7)
+
+    def put(mask, g, part, scale=1.0, q=0):
+        cc = c[mask]
+        cg[2 * cc + q] = g; cp[2 * cc + q] = part; cs[2 * cc + q] = scale
+    put(K < 6, G["sub"], PART["SUB"])
+    put((K >= 6) & (K < 8) & in_base, G["solder"], PART["SOLDER"], 0.3, 0)
+    put((K >= 6) & (K < 8) & in_base, G["uf"], PART["UF_BUMP"], 0.7, 1)
+    put((K >= 8) & (K < 10) & in_base, G["base"], PART["BASE_SI"])
+    put((K == 10) & in_chip, G["ddi"], PART["DDI_SOLDER"], 0.3, 0)
+    put((K == 10) & in_chip, G["fill"], PART["DDI_FILL"], 0.7, 1)
+    put((K == 10) & in_base & ~in_chip, G["mold"], PART["MOLD"])
+    put((K > 10) & in_chip, G["chip"], PART["CHIPLET"])
+    put((K > 10) & in_base & ~in_chip, G["mold"], PART["MOLD"])
+    feat = sorted({b0, b1, chips[0][0], chips[0][1], chips[1][0], chips[1][1]})
+    mesh = build_structured_mesh(xs, ys, zs, cg, cp, cs, featureX=feat, featureY=feat)
+    mesh.constraints = constraints321(mesh, CONSTRAINT_SPAN * L / 2)
+    kb = 8   # node plane of the base die bottom
+    sup = module_support(mesh, dict(x0=-15.0, x1=15.0, y0=-15.0, y1=15.0), 0.0, 0.0, kb)
+    mesh.moduleConstraints = np.array([3 * sup[0], 3 * sup[0] + 1, 3 * sup[0] + 2, 3 * sup[1] + 1, 3 * sup[1] + 2, 3 * sup[2] + 2],
+                                      np.int32)
+    # property sets, one per group: E (MPa), nu, CTE
+    const = [(iso_d(25000.0, 0.3), 15e-6), None, (iso_d(8000.0, 0.35), 30e-6), (iso_d(130000.0, 0.28), 2.6e-6),
+             None, (iso_d(8000.0, 0.35), 30e-6), (iso_d(130000.0, 0.28), 2.6e-6), (iso_d(20000.0, 0.3), 10e-6)]
+
+    def solder_E(T):   # linear E(T) of the module's SAC305 (MPa)
+        return 57400.0 + (30000.0 - 57400.0) * (T + 40.0) / 165.0
+
+    def step_fn(Ta, Tb):
+        Es = solder_E(0.5 * (Ta + Tb))   # the step mean of a linear E(T)
+        mats = []
+        for p, m in enumerate(const):
+            if m is None:
+                mats.append((column_d(Es, 0.4), 22.5e-6, 22.5e-6))
+            else:
+                mats.append((m[0], m[1], m[1]))
+        return _homog_step(mats, Ta, Tb)
+    return Package(name="stacked_module", mesh=mesh, group_layered=np.zeros(8, np.int32),
+                   group_stage=np.array([0, 0, 0, -1, -1, -1, -1, -1], np.int32), group_pset=np.arange(8, dtype=np.int32),
+                   sec_of_layer=np.zeros(ncz, np.int32), npset=8, step_fn=step_fn, Ta=217.0, Tb=25.0,
+                   meta=dict(workload=f"stacked_module {n}x{n}x{ncz}", bottom_plane=0,
+                             # process: the module is stress-free at the mold cure (175 degC), attached at the
+                             # solder reflow (217 degC)
+                             T_module=175.0, T_attach=217.0,
+                             die=dict(cx=0.0, cy=0.0, w=30.0, h=30.0, keepout=0.2, px=0.15, py=0.15),
+                             bga=dict(sx=L, sy=L, inset=1.0, pitch=1.0),
+                             bump_layer=dict(zmid=t_sub + 0.5 * t_bump, part=PART["SOLDER"])))
+
+
+def module_path_steps(pkg: Package, max_dt: float = 30.0, cycle_dt: float = 10.0, Tmin: float = -40.0, Tmax: float = 125.0):
+    """The thermal path of a stacked-module package: the module alone (stage -1) from its
+    stress-free temperature to the attach temperature, the whole package (stage 0) from there down to
+    25 degC in steps of at most max_dt, then the two cycling branches 25 -> Tmax and 25 -> Tmin in
+    steps of cycle_dt (the cycling sample temperatures). Returns (steps, Tb, chain, up, down)."""
+    T0, Ta = pkg.meta["T_module"], pkg.meta["T_attach"]
+    steps, Tb = [pkg.step(T0, Ta, stage=-1)], [Ta]
+    nch = max(1, int(np.ceil((Ta - 25.0) / max_dt - 1e-9)))
+    for q in range(nch):
+        a, b = Ta - (Ta - 25.0) * q / nch, Ta - (Ta - 25.0) * (q + 1) / nch
+        steps.append(pkg.step(a, b)); Tb.append(b)
+    chain = list(range(len(steps)))
+    up, down = [], []
+    for end, br in ((Tmax, up), (Tmin, down)):
+        T = 25.0
+        while T != end:
+            nxt = min(T + cycle_dt, end) if end > T else max(T - cycle_dt, end)
+            br.append(len(steps)); steps.append(pkg.step(T, nxt)); Tb.append(nxt)
+            T = nxt
+    return steps, Tb, chain, up, down
 
 
 def rms_warpage(mesh: Mesh, u: np.ndarray, k: int = 0) -> float:

@@ -51,6 +51,7 @@ class DeviceModel:
         xs, ys, zs = keep(m.xs, np.float64), keep(m.ys, np.float64), keep(m.zs, np.float64)
         con = keep(m.constraints if constraints is None else constraints, np.int32)
         fx = keep(m.featureX, np.int32); fy = keep(m.featureY, np.int32)
+        mc = keep(getattr(m, "moduleConstraints", None) if getattr(m, "moduleConstraints", None) is not None else [], np.int32)
         mesh = TmMesh(nx=m.nx, ny=m.ny, nz=m.nz, xs=_p(xs, C.c_double), ys=_p(ys, C.c_double), zs=_p(zs, C.c_double),
                       nn=m.nn, ne=m.ne, coords=_p(keep(m.coords, np.float64), C.c_double),
                       nodeId=_p(keep(m.nodeId, np.int32), C.c_int32), conn=_p(keep(m.conn, np.int32), C.c_int32),
@@ -60,7 +61,8 @@ class DeviceModel:
                       ngroups=len(pkg.group_stage), groupStage=_p(keep(pkg.group_stage, np.int32), C.c_int32),
                       npset=int(pkg.npset), ePset=_p(keep(pkg.e_pset, np.int32), C.c_int32),
                       nconstr=len(con), constr=_p(con, C.c_int32), nfeatureX=len(fx), nfeatureY=len(fy),
-                      featureX=_p(fx, C.c_int32) if len(fx) else None, featureY=_p(fy, C.c_int32) if len(fy) else None)
+                      featureX=_p(fx, C.c_int32) if len(fx) else None, featureY=_p(fy, C.c_int32) if len(fy) else None,
+                      nmodconstr=len(mc), modconstr=_p(mc, C.c_int32) if len(mc) else None)
         h = C.c_void_p()
         check(L.tm_create(C.byref(mesh), C.byref(h)))
         self.h = h
