@@ -145,6 +145,10 @@ class OracleModel:
                            np.ascontiguousarray(step.born, np.int32), rhs, int(no_constraints))
         return rhs
 
+    def prepare_step(self, step):
+        """The step's shape matrices and thermal loads for the DOF histories (an assembly here)."""
+        self.assemble(step)
+
     def bcsr(self):
         rowPtr = np.zeros(self.nn + 1, np.int32); col = np.zeros(self.nb, np.int32)
         val = np.zeros(9 * self.nb); isC = np.zeros(self.ndof, np.uint8)

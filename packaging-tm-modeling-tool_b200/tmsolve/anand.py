@@ -24,14 +24,18 @@ DWELL_MIN_STEPS = 10   # 00-constants.js:112
 PHASES = {"start": 0, "ramp up": 1, "dwell hot": 2, "ramp down": 3, "dwell cold": 4}
 
 
-def cycle_history(Tmin: float, Tmax: float, ramp_c_per_min: float, dwell_min: float, cycles: int) -> dict:
+def cycle_history(Tmin: float, Tmax: float, ramp_c_per_min: float, dwell_min: float, cycles: int,
+                  ramp_max_dt: float = RAMP_MAX_DT, dwell_steps: int = DWELL_MIN_STEPS) -> dict:
+    """cycleHistory (13-fatigue.js:275-293) with its step rules as parameters (the reference's
+    RAMP_MAX_DT and DWELL_MIN_STEPS by default; ramp_max_dt = 10, dwell_steps = 3 gives 40 load steps
+    per -40/125 degC cycle)."""
     rate = ramp_c_per_min / 60.0
     dwell = dwell_min * 60.0
     t, T, cyc, ph = [0.0], [25.0], [0], [0]
     time = [0.0]
 
     def ramp(frm, to, c):
-        n = max(1, math.ceil(abs(to - frm) / RAMP_MAX_DT))
+        n = max(1, math.ceil(abs(to - frm) / ramp_max_dt))
         dur = abs(to - frm) / rate
         for k in range(1, n + 1):
             time[0] += dur / n
@@ -39,8 +43,8 @@ def cycle_history(Tmin: float, Tmax: float, ramp_c_per_min: float, dwell_min: fl
             ph.append(PHASES["ramp up"] if to > frm else PHASES["ramp down"])
 
     def hold(Tv, c, label):
-        for _ in range(DWELL_MIN_STEPS):
-            time[0] += dwell / DWELL_MIN_STEPS
+        for _ in range(dwell_steps):
+            time[0] += dwell / dwell_steps
             t.append(time[0]); T.append(Tv); cyc.append(c); ph.append(PHASES[label])
 
     for c in range(1, cycles + 1):

@@ -377,11 +377,14 @@ def stacked_module(n_inplane: int = 192) -> Package:
                              bump_layer=dict(zmid=t_sub + 0.5 * t_bump, part=PART["SOLDER"])))
 
 
-def module_path_steps(pkg: Package, max_dt: float = 30.0, cycle_dt: float = 10.0, Tmin: float = -40.0, Tmax: float = 125.0):
+def module_path_steps(pkg: Package, max_dt: float = 30.0, temps=None):
     """The thermal path of a stacked-module package: the module alone (stage -1) from its
     stress-free temperature to the attach temperature, the whole package (stage 0) from there down to
-    25 degC in steps of at most max_dt, then the two cycling branches 25 -> Tmax and 25 -> Tmin in
-    steps of cycle_dt (the cycling sample temperatures). Returns (steps, Tb, chain, up, down)."""
+    25 degC in steps of at most max_dt, then the two cycling branches from 25 degC through the
+    cycling sample temperatures (default every 10 degC from -40 to 125 degC, with 25 and both ends)
+    up to the highest and down to the lowest. Returns (steps, Tb, chain, up, down)."""
+    if temps is None:
+        temps = sorted(set(np.arange(-40.0, 125.0 + 1e-9, 10.0).round(9).tolist()) | {-40.0, 125.0, 25.0})
     T0, Ta = pkg.meta["T_module"], pkg.meta["T_attach"]
     steps, Tb = [pkg.step(T0, Ta, stage=-1)], [Ta]
     nch = max(1, int(np.ceil((Ta - 25.0) / max_dt - 1e-9)))
@@ -390,12 +393,11 @@ def module_path_steps(pkg: Package, max_dt: float = 30.0, cycle_dt: float = 10.0
         steps.append(pkg.step(a, b)); Tb.append(b)
     chain = list(range(len(steps)))
     up, down = [], []
-    for end, br in ((Tmax, up), (Tmin, down)):
+    for seq, br in ((sorted(t for t in temps if t > 25.0), up), (sorted((t for t in temps if t < 25.0), reverse=True), down)):
         T = 25.0
-        while T != end:
-            nxt = min(T + cycle_dt, end) if end > T else max(T - cycle_dt, end)
-            br.append(len(steps)); steps.append(pkg.step(T, nxt)); Tb.append(nxt)
-            T = nxt
+        for nxt in seq:
+            br.append(len(steps)); steps.append(pkg.step(T, float(nxt))); Tb.append(float(nxt))
+            T = float(nxt)
     return steps, Tb, chain, up, down
 
 
