@@ -45,9 +45,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="a warm-up assemble + solve, then one assemble + solve (for ncu captures); prints no bench line")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "screen"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "screen", "c3"],
                     help="c2: the lidded 160x160x32 solve (the headline); c1: the plain FP64 FCBGA 48x48x20 solve; "
-                         "screen: Anand screening of the 17,424 bumps of a die over three -40/125 degC cycles")
+                         "screen: Anand screening of the 17,424 bumps of a die over three -40/125 degC cycles; "
+                         "c3: the stacked-module thermal-cycle analysis (module stage, process chain, cycling branches, "
+                         "bump strain tables, Anand screening at 40 load steps per cycle), about 1.2M DOF")
     ap.add_argument("--sites", type=int, default=17424, help="screen: bump sites")
     a = ap.parse_args()
     a.precision_default = a.precision is None
@@ -450,10 +452,78 @@ def run_screen(a):
             "cpu_baseline": cpu, "clocks": ck.summary()}))
 
 
+# ---- stacked-module thermal-cycle analysis ----------------------------------------------------------
+C3_METRIC = "stacked-module thermal-cycle analysis (module stage + process chain + cycling branches + bump strain tables + Anand screening)"
+
+
+def run_c3(a):
+    """One analysis = every step of the module's thermal path solved on the device (module stage -1,
+    stage 0 from the attach temperature to 25 degC, the cycling branches through the sample
+    temperatures), the bump-layer strain table at the screened die bump sites from the steps' float32
+    increments, and the Anand screening of those sites over three -40/125 degC cycles at 40 load steps
+    per cycle. Timed end to end (host API), device and host work included."""
+    import numpy as np
+    import torch
+    from tmsolve import post
+    from tmsolve.anand import cycle_history, cycling_temps, screen
+    from tmsolve.materials import SAC305_MODULE, anand_tables
+    from tmsolve.packages import module_path_steps, stacked_module
+    from tmsolve.solver import DeviceModel
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    n_in = a.inplane if a.inplane != 160 else 192
+    pkg = stacked_module(n_in)
+    temps = cycling_temps(-40.0, 125.0)
+    steps, Tb, chain, up, down = module_path_steps(pkg, temps=temps)
+    sites = post.screening_sites(post.bump_field(**pkg.meta["die"]))["sites"]
+    hist = cycle_history(-40.0, 125.0, 11.0, 15.0, 3, ramp_max_dt=10.0, dwell_steps=3)
+    Et, Ft = anand_tables(SAC305_MODULE)
+    bl = pkg.meta["bump_layer"]
+    dm = DeviceModel(pkg)
+
+    def analysis(key0):
+        t0 = time.perf_counter()
+        du, its = [], 0
+        for k, st in enumerate(steps):
+            r = dm.solve(dm.assemble_step(st), tol=1e-8, key=key0 + k, precision=a.precision)
+            du.append(r["u"].astype(np.float32).astype(np.float64))
+            its += r["iters"]
+        t1 = time.perf_counter()
+        table = post.site_strain_table(dm, post.ThermalPath(steps, Tb, du, chain, up, down), sites, temps, bl["zmid"], bl["part"])
+        t2 = time.perf_counter()
+        dW, dE, stab = screen(SAC305_MODULE, Et, Ft, temps, table, hist)
+        t3 = time.perf_counter()
+        return dict(solve_s=t1 - t0, table_s=t2 - t1, screen_s=t3 - t2, total_s=t3 - t0, iters=its, dW=dW)
+    for w in range(a.warmup):
+        analysis(1000 * (w + 1))
+    torch.cuda.synchronize()
+    with Clocks(local) as ck:
+        runs = [analysis(100000 * (q + 1)) for q in range(a.steps)]
+    tot = sum(r["total_s"] for r in runs) / a.steps
+    last = runs[-1]
+    n = dm.ndof
+    print(json.dumps({
+        "metric": C3_METRIC, "value": tot, "unit": "s per analysis", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * tot, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 apply/smoother + f64 refinement; f64 return map" if a.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"stacked module {n_in}x{n_in}x15 ({n} DOF), {len(steps)} path steps (module stage, "
+                               f"{len(chain) - 1} chain steps, {len(up)}+{len(down)} cycling steps), {len(sites['x'])} screened bump sites, "
+                               f"3 cycles -40/125 degC at 40 load steps per cycle", "dof": n, "precision": a.precision,
+                   "l2": "working set larger than L2"},
+        "analysis": {"solve_s": last["solve_s"], "table_s": last["table_s"], "screen_s": last["screen_s"],
+                     "pcg_iters": last["iters"], "solve_mdof_iter_per_s": n * last["iters"] / 1e6 / last["solve_s"],
+                     "dW_mean": float(np.nanmean(last["dW"])), "dW_max": float(np.nanmax(last["dW"]))},
+        "e2e": {"value": tot, "unit": "s per analysis", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "clocks": ck.summary()}))
+
+
 def main():
     a = parse()
     if a.workload == "screen":
         run_screen(a)
+        return
+    if a.workload == "c3":
+        run_c3(a)
         return
     if a.workload == "c1":
         global WORKLOAD

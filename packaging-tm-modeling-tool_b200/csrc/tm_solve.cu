@@ -338,6 +338,8 @@ __device__ __forceinline__ void load_block36(const double* __restrict__ p, doubl
 
 // rows of the column inverse a lane keeps in registers when the column block is small
 constexpr int SH_PRE = 18;
+// larger column inverses are staged in the warp's shared memory up to this size
+constexpr size_t SH_AI_MAX = 12 * 1024;
 
 // per-warp shared staging of the shell column kernels: the 6 partial sums of every block of the
 // column's rows, the m residual rows (at least SH_PRE) and the local row starts
@@ -347,12 +349,25 @@ __host__ __device__ inline size_t shell_stage_bytes(int maxm, int maxBlk) {
   const size_t b = sizeof(T) * (6 * (size_t)maxBlk + rlen) + sizeof(int) * ((size_t)maxm / 6 + 1);
   return (b + 15) / 16 * 16;
 }
+// whether a level's column inverses are staged in shared memory by the sweep, and the sweep's
+// per-warp staging
+template <class T>
+__host__ __device__ inline bool shell_stage_ai(int maxm) {
+  return maxm > SH_PRE && (size_t)maxm * maxm * sizeof(T) <= SH_AI_MAX;
+}
+template <class T>
+__host__ __device__ inline size_t shell_sweep_bytes(int maxm, int maxBlk, bool stageAi) {
+  return shell_stage_bytes<T>(maxm, maxBlk) + (stageAi ? ((size_t)maxm * maxm * sizeof(T) + 15) / 16 * 16 : 0);
+}
 
 // residual rows r = b - K x of the column whose aggregates are n0 .. n0+na-1 (blocks k0 ..
 // k0+nblk-1), by one warp: the
 // lanes take the column's blocks (all rows together), each lane's 6 products of a block land in
 // shared memory, and lane e then subtracts its row's block sums in block order, as the serial
-// row loop of columnSweep (10-solver.js:535-553) does
+// row loop of columnSweep (10-solver.js:535-553) does. A lane's blocks are taken SH_BPL at a time:
+// first all their column indices, then all their neighbour values, then the block values and the
+// products, so that each of these steps is one round of loads rather than one per block.
+constexpr int SH_BPL = 4;
 template <class T>
 __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, int k0, int nblk, const int* __restrict__ rowPtr,
                                                       const int* __restrict__ col, const T* __restrict__ val,
@@ -369,14 +384,31 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
     return;
   }
   for (int q = lane; q <= na; q += 32) rp[q] = rowPtr[n0 + q] - k0;
-  for (int e = lane; e < nblk; e += 32) {
-    const T* xj = x + 6 * (size_t)col[k0 + e];
-    T v[36];
-    load_block36(val + 36 * (size_t)(k0 + e), v);
-    const T x0 = xj[0], x1 = xj[1], x2 = xj[2], x3 = xj[3], x4 = xj[4], x5 = xj[5];
+  for (int e0 = 0; e0 < nblk; e0 += 32 * SH_BPL) {
+    int cj[SH_BPL];
 #pragma unroll
-    for (int p = 0; p < 6; p++)
-      part[6 * e + p] = v[6 * p] * x0 + v[6 * p + 1] * x1 + v[6 * p + 2] * x2 + v[6 * p + 3] * x3 + v[6 * p + 4] * x4 + v[6 * p + 5] * x5;
+    for (int u = 0; u < SH_BPL; u++) {
+      const int e = e0 + lane + 32 * u;
+      cj[u] = e < nblk ? col[k0 + e] : -1;
+    }
+    T xv[SH_BPL][6];
+#pragma unroll
+    for (int u = 0; u < SH_BPL; u++) {
+      const T* xj = x + 6 * (size_t)(cj[u] < 0 ? 0 : cj[u]);
+#pragma unroll
+      for (int q = 0; q < 6; q++) xv[u][q] = cj[u] >= 0 ? xj[q] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < SH_BPL; u++) {
+      const int e = e0 + lane + 32 * u;
+      if (e >= nblk) break;
+      T v[36];
+      load_block36(val + 36 * (size_t)(k0 + e), v);
+#pragma unroll
+      for (int p = 0; p < 6; p++)
+        part[6 * e + p] = v[6 * p] * xv[u][0] + v[6 * p + 1] * xv[u][1] + v[6 * p + 2] * xv[u][2] + v[6 * p + 3] * xv[u][3] +
+                          v[6 * p + 4] * xv[u][4] + v[6 * p + 5] * xv[u][5];
+    }
   }
   __syncwarp();
   for (int e = lane; e < m; e += 32) {
@@ -388,21 +420,34 @@ __device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, 
   __syncwarp();
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 // one column of a shell-level sweep by one warp: r = b - K x over the column's rows, then
-// x_col += A_cc^-1 r with the explicit inverse Ai (entry (e, k) at k*m + e). Every lane fetches
-// its row of the inverse (blocks of at most SH_PRE rows) and its entries of the column's own x
-// before the residual, so that those loads overlap the residual's instead of following it: no
-// other warp writes this column's x during the launch (a colour's columns do not couple), and
-// this warp writes it only at the end.
+// x_col += A_cc^-1 r with the explicit inverse Ai (entry (e, k) at k*m + e). The inverse reaches the
+// lanes before the residual is done: rows of at most SH_PRE entries in registers, larger blocks
+// copied asynchronously into the warp's shared memory (aiSm, when the level's blocks fit there) and
+// otherwise read from global memory after it. Every lane fetches its entries of the column's own x
+// before the residual too: no other warp writes this column's x during the launch (a colour's
+// columns do not couple), and this warp writes it only at the end.
 template <class T>
 __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* __restrict__ Ai, const int* __restrict__ rowPtr,
                                                    const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ b,
-                                                   T* __restrict__ x, bool zeroGuess, T* part, T* r, int* rp) {
+                                                   T* __restrict__ x, bool zeroGuess, T* part, T* r, int* rp, T* aiSm) {
   const int n0 = mt.x, na = mt.y - mt.x, m = 6 * na;
   T a[SH_PRE];
   const bool pre = m <= SH_PRE;
 #pragma unroll
   for (int k = 0; k < SH_PRE; k++) a[k] = (pre && lane < m && k < m) ? Ai[(size_t)k * m + lane] : (T)0;
+  const bool staged = !pre && aiSm != nullptr;
+  if (staged) {
+    // m*m values, a multiple of 36: 16-byte pieces (the block starts on a 16-byte boundary)
+    const int pieces = m * m * (int)sizeof(T) / 16;
+    for (int q = lane; q < pieces; q += 32) cp_async16(reinterpret_cast<unsigned char*>(aiSm) + 16 * q, reinterpret_cast<const unsigned char*>(Ai) + 16 * q);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
   T* xc = x + 6 * (size_t)n0;
   const T xo0 = lane < m ? xc[lane] : (T)0, xo1 = lane + 32 < m ? xc[lane + 32] : (T)0;
   shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, zeroGuess, part, r, rp);
@@ -416,10 +461,16 @@ __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* _
     }
     return;
   }
+  const T* A = Ai;
+  if (staged) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncwarp();
+    A = aiSm;
+  }
   for (int e = lane; e < m; e += 32) {
     T acc = 0;
 #pragma unroll 6
-    for (int k = 0; k < m; k++) acc += Ai[(size_t)k * m + e] * r[k];
+    for (int k = 0; k < m; k++) acc += A[(size_t)k * m + e] * r[k];
     xc[e] = (e == lane ? xo0 : e == lane + 32 ? xo1 : xc[e]) + acc;
   }
 }
@@ -452,16 +503,17 @@ template <class T>
 __global__ void __launch_bounds__(256) k_sweep_shell(int ncolc, const int4* __restrict__ meta, const long long* __restrict__ cfOff,
                                                      const int* __restrict__ rowPtr, const int* __restrict__ col,
                                                      const T* __restrict__ val, const T* __restrict__ cf, const T* __restrict__ b,
-                                                     T* __restrict__ x, int maxm, int maxBlk, int zeroGuess) {
+                                                     T* __restrict__ x, int maxm, int maxBlk, int zeroGuess, int stageAi) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
   if (gw >= ncolc) return;
-  unsigned char* base = smraw + (size_t)warp * shell_stage_bytes<T>(maxm, maxBlk);
+  unsigned char* base = smraw + (size_t)warp * shell_sweep_bytes<T>(maxm, maxBlk, stageAi != 0);
   T* part = reinterpret_cast<T*>(base);
   T* r = part + 6 * (size_t)maxBlk;
   int* rp = reinterpret_cast<int*>(r + (maxm > SH_PRE ? maxm : SH_PRE));
-  shell_sweep_column<T>(lane, meta[gw], cf + cfOff[gw], rowPtr, col, val, b, x, zeroGuess != 0, part, r, rp);
+  T* aiSm = stageAi ? reinterpret_cast<T*>(base + shell_stage_bytes<T>(maxm, maxBlk)) : nullptr;
+  shell_sweep_column<T>(lane, meta[gw], cf + cfOff[gw], rowPtr, col, val, b, x, zeroGuess != 0, part, r, rp, aiSm);
 }
 
 // shell restriction: rc = P^T res (children lists, transposeProl order)
@@ -604,17 +656,20 @@ void vcycle(Context& c, const T* r, T* z) {
   auto wpbA = [&](const ShellLevel& L) { return sizeof(T) == 4 ? L.wpbApply : 4; };
   size_t smemS = 0;
   for (auto& Lp : c.shells)
-    smemS = std::max(smemS, (size_t)std::max(wpbS(*Lp), wpbA(*Lp)) * shell_stage_bytes<T>(Lp->maxm, Lp->maxColBlocks));
+    smemS = std::max(smemS, (size_t)std::max(wpbS(*Lp), wpbA(*Lp)) *
+                                shell_sweep_bytes<T>(Lp->maxm, Lp->maxColBlocks, shell_stage_ai<T>(Lp->maxm)));
   if (smemS > 48 * 1024) {
     TM_CUDA_CHECK(cudaFuncSetAttribute(k_sweep_shell<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemS));
     TM_CUDA_CHECK(cudaFuncSetAttribute(k_apply_shell<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemS));
   }
   auto sweepS = [&](ShellLevel& L, int col, int zero) {
-    const size_t per = shell_stage_bytes<T>(L.maxm, L.maxColBlocks);
+    const bool sai = shell_stage_ai<T>(L.maxm);
+    const size_t per = shell_sweep_bytes<T>(L.maxm, L.maxColBlocks, sai);
     const int wpb = wpbS(L);
     TimedLaunch tl(c, K_SWEEP_SHELL);
     k_sweep_shell<T><<<grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st>>>(L.colorCount[col], L.d_colorMeta[col].p,
-        (const long long*)L.d_colorCf[col].p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::cf(L), B::b(L), B::x(L), L.maxm, L.maxColBlocks, zero);
+        (const long long*)L.d_colorCf[col].p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::cf(L), B::b(L), B::x(L), L.maxm, L.maxColBlocks, zero,
+        sai ? 1 : 0);
     note_launch();
   };
   // ---- level 0 pre-smoothing: 2 sweeps in colours 0..3
@@ -916,7 +971,8 @@ void autotune_vcycle32(Context& c) {
   const int cands[3] = {4, 2, 8};   // the default first
   for (ShellLevel* Lp : swept) {
     ShellLevel& L = *Lp;
-    const size_t per = shell_stage_bytes<float>(L.maxm, L.maxColBlocks);
+    const bool sai = shell_stage_ai<float>(L.maxm);
+    const size_t per = shell_sweep_bytes<float>(L.maxm, L.maxColBlocks, sai);
     DBuf<float> sx, sb, sr;
     sx.alloc(6 * (size_t)L.nn); sx.zero(st);
     sb.alloc(6 * (size_t)L.nn); sb.zero(st);
@@ -931,7 +987,8 @@ void autotune_vcycle32(Context& c) {
       TM_CUDA_CHECK(cudaFuncSetAttribute(k_apply_shell<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, attr));
       const double tS = timed([&] {
         k_sweep_shell<float><<<grid_for(L.colorCount[0], wpb), 32 * wpb, smem, st>>>(L.colorCount[0], L.d_colorMeta[0].p,
-            (const long long*)L.d_colorCf[0].p, L.d_rowPtr.p, L.d_col.p, L.d_val32.p, L.d_cfInv32.p, sb.p, sx.p, L.maxm, L.maxColBlocks, 0);
+            (const long long*)L.d_colorCf[0].p, L.d_rowPtr.p, L.d_col.p, L.d_val32.p, L.d_cfInv32.p, sb.p, sx.p, L.maxm, L.maxColBlocks, 0,
+            sai ? 1 : 0);
       });
       const int ncol = L.nx * L.ny;
       const double tA = timed([&] {
