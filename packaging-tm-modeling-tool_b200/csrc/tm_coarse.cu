@@ -175,21 +175,22 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
   if (tid == 0) s_fix = 0;
   __syncthreads();
   if (tid < 32) {
+    // right-looking, lane i owning row i: column j is scaled once its pivot is known, then every
+    // later row subtracts its rank-1 part (independent updates instead of a serial dot per entry)
     const int lane = tid;
     const double jitter = jit[0];
     int fixes = 0;
     for (int j = 0; j < nbk; j++) {
-      const double ss = warp_sum(lane < j ? Ds[j][lane] * Ds[j][lane] : 0.0);
-      double d = Ds[j][j] - ss;
+      double d = Ds[j][j];
       if (!(d > jitter)) { d = fmax(fabs(d), jitter); fixes++; }
       const double ljj = sqrt(d), inv = 1 / ljj;
       __syncwarp();
       if (lane == 0) Ds[j][j] = ljj;
-      if (lane > j && lane < nbk) {
-        double s2 = Ds[lane][j];
-        for (int t = 0; t < j; t++) s2 -= Ds[lane][t] * Ds[j][t];
-        Ds[lane][j] = s2 * inv;
-      }
+      double lij = 0;
+      if (lane > j && lane < nbk) { lij = Ds[lane][j] * inv; Ds[lane][j] = lij; }
+      __syncwarp();
+      if (lane > j && lane < nbk)
+        for (int k = j + 1; k <= lane; k++) Ds[lane][k] -= lij * Ds[k][j];
       __syncwarp();
     }
     if (lane == 0) s_fix = fixes;
@@ -209,15 +210,24 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
   }
   __syncthreads();
   if (tid < 64) {
+    // right-looking in registers: P[k] is final once the columns before it are subtracted
     const int which = tid >> 5, r = tid & 31;
     const int tile = which ? tj : ti;
     double* P = which ? &Pj[r][0] : &Pi[r][0];
     if (!(which == 1 && ti == tj) && tile * CN + r < R) {
-      for (int k = 0; k < nbk; k++) {
-        double a = P[k];
-        for (int t = 0; t < k; t++) a -= P[t] * Ds[k][t];
-        P[k] = a / Ds[k][k];
+      double p[CN];
+#pragma unroll
+      for (int k = 0; k < CN; k++) p[k] = k < nbk ? P[k] : 0.0;
+#pragma unroll
+      for (int k = 0; k < CN; k++) {
+        if (k >= nbk) break;
+        const double pk = p[k] / Ds[k][k];
+        p[k] = pk;
+#pragma unroll
+        for (int t = k + 1; t < CN; t++) p[t] -= pk * Ds[t][k];
       }
+#pragma unroll
+      for (int k = 0; k < CN; k++) if (k < nbk) P[k] = p[k];
     }
   }
   __syncthreads();
