@@ -491,6 +491,16 @@ tm_status tm_submodel_run_batch(int32_t n, tm_sub* const* subs, int32_t nsteps, 
 tm_status tm_anand_step(const tm_anand_material* mat, int32_t npts, double* state, const double* eps,
                         double T, double dt, double* sig, double* D, int32_t commit);
 
+/* One site of screenJoints' loop (13-fatigue.js:416-451; with a pillar, screenDdi's stepSeriesColumn)
+ * and the derivatives of its last-cycle dW and dE with respect to every entry of its strain table
+ * (table: ntemps x 6, gW and gE the same shape), for the adjoint of the peak bump dW (no counterpart
+ * in the reference, whose tornado re-runs whole analyses). Forward mode: each table entry is a
+ * direction carried through the whole history, iterations included, so the result is the exact
+ * derivative of the screening as computed. pillar may be NULL (a free-standing column). */
+tm_status tm_anand_screen_gradient(const tm_anand_material* mat, const tm_pillar* pillar, int32_t ntemps, const double* temps,
+                                   const double* table, int32_t nsteps, const double* t, const double* T, const int32_t* cycle,
+                                   const int32_t* phase, int32_t cycles, double* dW, double* dE, double* gW, double* gE);
+
 #ifdef __cplusplus
 }
 #endif

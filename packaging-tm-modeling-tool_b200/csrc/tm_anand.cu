@@ -22,23 +22,25 @@ namespace tmg {
 
 namespace {
 
-__device__ void inv3(const double* J, double* out) {
-  const double a = J[0], b = J[1], c = J[2], d = J[3], e = J[4], f = J[5], g = J[6], h = J[7], i = J[8];
-  const double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+template <class S>
+__device__ void inv3(const S* J, S* out) {
+  const S a = J[0], b = J[1], c = J[2], d = J[3], e = J[4], f = J[5], g = J[6], h = J[7], i = J[8];
+  const S det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
   out[0] = (e * i - f * h) / det; out[1] = (c * h - b * i) / det; out[2] = (b * f - c * e) / det;
   out[3] = (f * g - d * i) / det; out[4] = (a * i - c * g) / det; out[5] = (c * d - a * f) / det;
   out[6] = (d * h - e * g) / det; out[7] = (b * g - a * h) / det; out[8] = (a * e - b * d) / det;
 }
 
 // stepColumn (13-fatigue.js:153-166)
-__device__ double step_column(const AnandConst& P, Point& pt, double* eps, const StepK& k, double* sig, double* D) {
+template <class S>
+__device__ S step_column(const AnandConst& P, PointT<S>& pt, S* eps, const StepK& k, S* sig, S* D) {
   const int Pi[3] = {0, 1, 3};
-  double A[9], Ai[9];
-  double d = 0;
+  S A[9], Ai[9];
+  S d = 0;
   for (int it = 0; it < COLUMN_NEWTON_MAXIT; it++) {
-    d = anand_step(P, pt, eps, k, sig, D, true);
-    const double r0 = sig[0], r1 = sig[1], r2 = sig[3];
-    const double ref = fmax(fmax(1.0, fabs(sig[2])), fmax(fabs(sig[4]), fabs(sig[5])));
+    d = anand_step(P, pt, (const S*)eps, k, sig, D, true);
+    const S r0 = sig[0], r1 = sig[1], r2 = sig[3];
+    const S ref = fmax(fmax(1.0, fabs(sig[2])), fmax(fabs(sig[4]), fabs(sig[5])));
     if (fmax(fmax(fabs(r0), fabs(r1)), fabs(r2)) < COLUMN_STRESS_TOL * ref) break;
     for (int r = 0; r < 3; r++)
       for (int c = 0; c < 3; c++) A[3 * r + c] = D[6 * Pi[r] + Pi[c]];
@@ -52,44 +54,45 @@ __device__ double step_column(const AnandConst& P, Point& pt, double* eps, const
 // compliances Cp carry the same axial and shear stresses; tz = the prescribed column-average
 // (zz, yz, zx) mechanical strains; the cap's in-plane stresses vanish. Newton on the cap's six
 // strains, the 6x6 system by Gaussian elimination with partial pivoting.
-__device__ double step_series_column(const AnandConst& P, Point& pt, double* eps, const double* tz, double fs, const double* Cp,
-                                     double E, const StepK& k, double* sig, double* D) {
+template <class S>
+__device__ S step_series_column(const AnandConst& P, PointT<S>& pt, S* eps, const S* tz, double fs, const double* Cp,
+                                double E, const StepK& k, S* sig, S* D) {
   const int Pi[3] = {0, 1, 3}, Z[3] = {2, 4, 5}, ord[6] = {0, 1, 3, 2, 4, 5};
   const double fp = 1 - fs;
-  double J[36], R[6];
-  double d = 0;
+  S J[36], R[6];
+  S d = 0;
   for (int it = 0; it < COLUMN_NEWTON_MAXIT; it++) {
-    d = anand_step(P, pt, eps, k, sig, D, true);
+    d = anand_step(P, pt, (const S*)eps, k, sig, D, true);
     for (int r = 0; r < 3; r++) {
       R[r] = sig[Pi[r]];
       R[3 + r] = fs * eps[Z[r]] + fp * Cp[r] * sig[Z[r]] - tz[r];
     }
-    const double ref = fmax(fmax(1.0, fabs(sig[2])), fmax(fabs(sig[4]), fabs(sig[5])));
-    double worst = 0;
+    const S ref = fmax(fmax(1.0, fabs(sig[2])), fmax(fabs(sig[4]), fabs(sig[5])));
+    S worst = 0;
     for (int r = 0; r < 3; r++) worst = fmax(fmax(worst, fabs(R[r])), fabs(R[3 + r]) * E);
     if (worst < COLUMN_STRESS_TOL * ref) break;
     for (int r = 0; r < 6; r++)
       for (int c = 0; c < 6; c++) {
-        const double Dv = D[6 * ord[r] + ord[c]];
+        const S Dv = D[6 * ord[r] + ord[c]];
         J[6 * r + c] = r < 3 ? Dv : fp * Cp[r - 3] * Dv + (ord[r] == ord[c] ? fs : 0);
       }
     for (int c = 0; c < 6; c++) {
       int pr = c;
       for (int r = c + 1; r < 6; r++) if (fabs(J[6 * r + c]) > fabs(J[6 * pr + c])) pr = r;
       if (pr != c) {
-        for (int q = 0; q < 6; q++) { const double t = J[6 * c + q]; J[6 * c + q] = J[6 * pr + q]; J[6 * pr + q] = t; }
-        const double t = R[c]; R[c] = R[pr]; R[pr] = t;
+        for (int q = 0; q < 6; q++) { const S t = J[6 * c + q]; J[6 * c + q] = J[6 * pr + q]; J[6 * pr + q] = t; }
+        const S t = R[c]; R[c] = R[pr]; R[pr] = t;
       }
-      const double piv = J[7 * c];
+      const S piv = J[7 * c];
       for (int r = c + 1; r < 6; r++) {
-        const double f = J[6 * r + c] / piv;
+        const S f = J[6 * r + c] / piv;
         if (f == 0) continue;
         for (int q = c; q < 6; q++) J[6 * r + q] -= f * J[6 * c + q];
         R[r] -= f * R[c];
       }
     }
     for (int c = 5; c >= 0; c--) {
-      double v = R[c];
+      S v = R[c];
       for (int q = c + 1; q < 6; q++) v -= J[6 * c + q] * R[q];
       R[c] = v / J[7 * c];
     }
@@ -108,45 +111,55 @@ struct PillarArgs {
 };
 
 
-// screenJoints per-site loop (13-fatigue.js:416-451), thread per site; SERIES: the joints are
-// solder caps on elastic pillars (stepSeriesColumn), else free-standing columns (stepColumn)
-template <bool SERIES>
-__global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const double* __restrict__ table, int nsteps,
-                         const int* __restrict__ wi, const double* __restrict__ wt, const double* __restrict__ Fth,
-                         const StepK* __restrict__ kc, const double* __restrict__ Th, const int* __restrict__ cycle,
-                         const int* __restrict__ phase, int cycles, double* __restrict__ dW, double* __restrict__ dE,
-                         double* __restrict__ stab, PillarArgs pil) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nsites) return;
-  const double* tab = table + (size_t)q * ntemps * 6;
-  if (!isfinite(tab[0])) { dW[q] = NAN; dE[q] = NAN; stab[q] = NAN; return; }
-  Point pt;
+// table entry i of a site: its value, and for the derivative kernel a unit derivative at the seeded entry
+template <class S>
+struct TabAt;
+template <>
+struct TabAt<double> {
+  static __device__ __forceinline__ double at(const double* tab, int i, int) { return tab[i]; }
+};
+template <>
+struct TabAt<Dual> {
+  static __device__ __forceinline__ Dual at(const double* tab, int i, int seed) { return Dual(tab[i], i == seed ? 1.0 : 0.0); }
+};
+
+// screenJoints per-site loop (13-fatigue.js:416-451) for one site's strain table tab (ntemps x 6);
+// SERIES: the joint is a solder cap on an elastic pillar (stepSeriesColumn), else a free-standing
+// column (stepColumn). dW, dE: the last cycle's energy density and inelastic strain increments;
+// stab: the cycle-to-cycle change of dW. For S = Dual the table entry `seed` carries a unit derivative.
+template <class S, bool SERIES>
+__device__ void screen_site(const AnandConst& P, const double* __restrict__ tab, int seed, int ntemps, int i25, int nsteps,
+                            const int* __restrict__ wi, const double* __restrict__ wt, const double* __restrict__ Fth,
+                            const StepK* __restrict__ kc, const double* __restrict__ Th, const int* __restrict__ cycle,
+                            const int* __restrict__ phase, int cycles, const PillarArgs& pil, S& dWo, S& dEo, S& stabo) {
+  typedef TabAt<S> TA;
+  PointT<S> pt;
   for (int i = 0; i < 6; i++) pt.ep[i] = 0;
   pt.s = P.s0; pt.ebar = 0; pt.W = 0; pt.sigEq = 0; pt.lastD = 0;
-  double e25[6], eps[6] = {0, 0, 0, 0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0}, sig[6], D[36];
-  double s1[6] = {0, 0, 0, 0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
-  for (int c = 0; c < 6; c++) e25[c] = i25 >= 0 ? tab[i25 * 6 + c] : 0;
+  S e25[6], eps[6] = {0, 0, 0, 0, 0, 0}, e1[3] = {0, 0, 0}, e2[3] = {0, 0, 0}, sig[6], D[36];
+  S s1[6] = {0, 0, 0, 0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
+  for (int c = 0; c < 6; c++) e25[c] = i25 >= 0 ? TA::at(tab, i25 * 6 + c, seed) : S(0);
   const int IP[3] = {0, 1, 3};
   const double nu = P.nu;
   // W and ebar at the end of the last three cycles (the reference keeps every cycle)
-  double Wlast[3] = {0, 0, 0}, Elast[3] = {0, 0, 0};  // cycles nc-2, nc-1, nc
+  S Wlast[3] = {0, 0, 0}, Elast[3] = {0, 0, 0};  // cycles nc-2, nc-1, nc
   for (int k = 1; k < nsteps; k++) {
-    const double* a = tab + wi[k] * 6;
-    const double* b = a + 6;
+    const int ia = wi[k] * 6, ib = ia + 6;
     const double t = wt[k];
+    auto lerp = [&](int c) { const S av = TA::at(tab, ia + c, seed), bv = TA::at(tab, ib + c, seed); return av + t * (bv - av); };
     if (SERIES) {
       // column-average mechanical strain: the layer strain less the thermal strains of cap and pillar
       const double fs = pil.fs;
-      double tz[3];
-      tz[0] = a[2] + t * (b[2] - a[2]) - e25[2] - fs * Fth[k] - (1 - fs) * pil.Fp[k];
-      tz[1] = a[4] + t * (b[4] - a[4]) - e25[4];
-      tz[2] = a[5] + t * (b[5] - a[5]) - e25[5];
+      S tz[3];
+      tz[0] = lerp(2) - e25[2] - fs * Fth[k] - (1 - fs) * pil.Fp[k];
+      tz[1] = lerp(4) - e25[4];
+      tz[2] = lerp(5) - e25[5];
       if (k > 2 && phase[k] == phase[k - 1])
         for (int c = 0; c < 6; c++) eps[c] = 2 * s1[c] - s2[c];
-      step_series_column(P, pt, eps, tz, fs, pil.Cps + 3 * k, grid_at(pil.Etab, Th[k]), kc[k], sig, D);
+      step_series_column(P, pt, eps, (const S*)tz, fs, pil.Cps + 3 * k, grid_at(pil.Etab, Th[k]), kc[k], sig, D);
       for (int c = 0; c < 6; c++) { s2[c] = s1[c]; s1[c] = eps[c]; }
     } else {
-      const double ez = a[2] + t * (b[2] - a[2]) - e25[2] - Fth[k];
+      const S ez = lerp(2) - e25[2] - Fth[k];
       if (k > 2 && phase[k] == phase[k - 1]) {
         for (int r = 0; r < 3; r++) eps[IP[r]] = 2 * e1[r] - e2[r];
       } else {
@@ -154,8 +167,8 @@ __global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const do
         eps[1] -= nu * (ez - eps[2]);
       }
       eps[2] = ez;
-      eps[4] = a[4] + t * (b[4] - a[4]) - e25[4];
-      eps[5] = a[5] + t * (b[5] - a[5]) - e25[5];
+      eps[4] = lerp(4) - e25[4];
+      eps[5] = lerp(5) - e25[5];
       step_column(P, pt, eps, kc[k], sig, D);
     }
     commit(pt);
@@ -166,10 +179,42 @@ __global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const do
   }
   // cycles before nc-2 stay 0 in the reference's per-cycle arrays when never reached
   const int nc = cycles;
-  const double Wn = Wlast[2], Wn1 = nc - 1 >= 0 ? Wlast[1] : 0, Wn2 = nc - 2 >= 0 ? Wlast[0] : 0;
-  dW[q] = Wn - Wn1;
-  dE[q] = Elast[2] - Elast[1];
-  stab[q] = nc >= 2 ? fabs((Wn - Wn1) - (Wn1 - Wn2)) / fmax(Wn - Wn1, 1e-30) : NAN;
+  const S Wn = Wlast[2], Wn1 = nc - 1 >= 0 ? Wlast[1] : S(0), Wn2 = nc - 2 >= 0 ? Wlast[0] : S(0);
+  dWo = Wn - Wn1;
+  dEo = Elast[2] - Elast[1];
+  stabo = nc >= 2 ? fabs((Wn - Wn1) - (Wn1 - Wn2)) / fmax(Wn - Wn1, 1e-30) : S(NAN);
+}
+
+// the screening, thread per site
+template <bool SERIES>
+__global__ void k_screen(AnandConst P, int nsites, int ntemps, int i25, const double* __restrict__ table, int nsteps,
+                         const int* __restrict__ wi, const double* __restrict__ wt, const double* __restrict__ Fth,
+                         const StepK* __restrict__ kc, const double* __restrict__ Th, const int* __restrict__ cycle,
+                         const int* __restrict__ phase, int cycles, double* __restrict__ dW, double* __restrict__ dE,
+                         double* __restrict__ stab, PillarArgs pil) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsites) return;
+  const double* tab = table + (size_t)q * ntemps * 6;
+  if (!isfinite(tab[0])) { dW[q] = NAN; dE[q] = NAN; stab[q] = NAN; return; }
+  double w, e, st;
+  screen_site<double, SERIES>(P, tab, -1, ntemps, i25, nsteps, wi, wt, Fth, kc, Th, cycle, phase, cycles, pil, w, e, st);
+  dW[q] = w; dE[q] = e; stab[q] = st;
+}
+
+// derivatives of one site's last-cycle dW and dE with respect to every entry of its strain table:
+// thread j runs the site's whole history with a unit derivative on table entry j (forward mode)
+template <bool SERIES>
+__global__ void k_screen_tangent(AnandConst P, int ntemps, int i25, const double* __restrict__ tab, int nsteps,
+                                 const int* __restrict__ wi, const double* __restrict__ wt, const double* __restrict__ Fth,
+                                 const StepK* __restrict__ kc, const double* __restrict__ Th, const int* __restrict__ cycle,
+                                 const int* __restrict__ phase, int cycles, PillarArgs pil, double* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= 6 * ntemps) return;
+  Dual w, e, st;
+  screen_site<Dual, SERIES>(P, tab, j, ntemps, i25, nsteps, wi, wt, Fth, kc, Th, cycle, phase, cycles, pil, w, e, st);
+  out[2 + j] = w.d;
+  out[2 + 6 * ntemps + j] = e.d;
+  if (j == 0) { out[0] = w.v; out[1] = e.v; }
 }
 
 __global__ void k_point_step(AnandConst P, const double* __restrict__ Etab, int npts, double* __restrict__ state,
@@ -214,7 +259,7 @@ double grid_at_host(const double* arr, double T) {
 
 void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps, const double* table_d, int nsteps,
                          const double* t_h, const double* T_h, const int* cycle_h, const int* phase_h, int cycles, double* dW_d,
-                         double* dE_d, double* stab_d, cudaStream_t s, const tm_pillar* pillar) {
+                         double* dE_d, double* stab_d, cudaStream_t s, const tm_pillar* pillar, double* grad_d) {
   if (nsteps < 2 || ntemps < 2 || cycles < 1) fail(TM_BAD_INPUT, "anand screening: need >= 2 time steps, >= 2 temperatures, >= 1 cycle");
   if (pillar && (!(pillar->fs > 0 && pillar->fs <= 1) || !pillar->Etab || !pillar->Ftab))
     fail(TM_BAD_INPUT, "anand screening: the pillar needs a solder fraction in (0, 1] and its E and thermal strain tables");
@@ -259,7 +304,18 @@ void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, c
   d_kc.alloc(nsteps);
   const AnandConst P = to_const(mat);
   k_step_constants<<<(nsteps + 127) / 128, 128, 0, s>>>(P, d_E.p, nsteps, d_t.p, d_T.p, d_kc.p);
-  if (pillar) {
+  if (grad_d) {
+    // one site's dW and dE and their derivatives with respect to its table: thread per table entry
+    PillarArgs pa{1, nullptr, nullptr, nullptr};
+    if (pillar) { d_Cps.upload(Cps, s); d_Fp.upload(Fp, s); pa = PillarArgs{pillar->fs, d_Cps.p, d_Fp.p, d_E.p}; }
+    const int nj = 6 * ntemps;
+    if (pillar)
+      k_screen_tangent<true><<<(nj + 63) / 64, 64, 0, s>>>(P, ntemps, i25, table_d, nsteps, d_wi.p, d_wt.p, d_Fth.p, d_kc.p, d_T.p,
+                                                         d_cycle.p, d_phase.p, cycles, pa, grad_d);
+    else
+      k_screen_tangent<false><<<(nj + 63) / 64, 64, 0, s>>>(P, ntemps, i25, table_d, nsteps, d_wi.p, d_wt.p, d_Fth.p, d_kc.p, d_T.p,
+                                                          d_cycle.p, d_phase.p, cycles, pa, grad_d);
+  } else if (pillar) {
     d_Cps.upload(Cps, s); d_Fp.upload(Fp, s);
     const PillarArgs pa{pillar->fs, d_Cps.p, d_Fp.p, d_E.p};
     k_screen<true><<<(nsites + 63) / 64, 64, 0, s>>>(P, nsites, ntemps, i25, table_d, nsteps, d_wi.p, d_wt.p, d_Fth.p, d_kc.p, d_T.p,

@@ -1281,6 +1281,35 @@ tm_status tm_anand_screen_pillar(const tm_anand_material* mat, const tm_pillar* 
   });
 }
 
+tm_status tm_anand_screen_gradient(const tm_anand_material* mat, const tm_pillar* pillar, int32_t ntemps, const double* temps,
+                                   const double* table, int32_t nsteps, const double* t, const double* T, const int32_t* cycle,
+                                   const int32_t* phase, int32_t cycles, double* dW, double* dE, double* gW, double* gE) {
+  return guarded([&] {
+    if (!mat || !temps || !table || !t || !T || !cycle || !phase || !dW || !dE || !gW || !gE) fail(TM_BAD_INPUT, "null argument");
+    require_device();
+    const size_t nt = 6 * (size_t)ntemps;
+    for (size_t i = 0; i < nt; i++) if (!std::isfinite(table[i])) fail(TM_NONFINITE, "the site's strain table has a non-finite entry");
+    cudaStream_t s = nullptr;
+    TM_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    try {
+      DBuf<double> d_tab, d_out;
+      d_tab.upload(table, nt, s);
+      d_out.alloc(2 + 2 * nt);
+      anand_screen_device(*mat, 1, ntemps, temps, d_tab.p, nsteps, t, T, cycle, phase, cycles, nullptr, nullptr, nullptr, s, pillar, d_out.p);
+      std::vector<double> h(2 + 2 * nt);
+      d_out.download(h.data(), h.size(), s);
+      TM_CUDA_CHECK(cudaStreamSynchronize(s));
+      *dW = h[0]; *dE = h[1];
+      std::copy(h.begin() + 2, h.begin() + 2 + nt, gW);
+      std::copy(h.begin() + 2 + nt, h.end(), gE);
+    } catch (...) {
+      cudaStreamDestroy(s);
+      throw;
+    }
+    cudaStreamDestroy(s);
+  });
+}
+
 tm_status tm_anand_step(const tm_anand_material* mat, int32_t npts, double* state, const double* eps, double T, double dt, double* sig,
                         double* D, int32_t commit) {
   return guarded([&] {

@@ -429,7 +429,7 @@ size_t mf_sweep_smem(int nz);
 void anand_screen_device(const tm_anand_material& mat, int nsites, int ntemps, const double* temps_h,
                          const double* table_d, int nsteps, const double* t_h, const double* T_h,
                          const int* cycle_h, const int* phase_h, int cycles, double* dW_d, double* dE_d,
-                         double* stab_d, cudaStream_t s, const tm_pillar* pillar = nullptr);
+                         double* stab_d, cudaStream_t s, const tm_pillar* pillar = nullptr, double* grad_d = nullptr);
 void anand_step_device(const tm_anand_material& mat, int npts, double* state_d, const double* eps_d,
                        double T, double dt, double* sig_d, double* D_d, int commit, cudaStream_t s);
 

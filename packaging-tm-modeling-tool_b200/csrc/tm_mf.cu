@@ -145,6 +145,80 @@ __device__ __forceinline__ void node_row(const T* __restrict__ xs, const uint16_
       }
 }
 
+// ---- staging of a box of nodes and cells into shared memory -----------------------------------------
+// Items are walked with the node planes fastest (consecutive node ids of a column, coalesced). Each
+// thread keeps SB items in flight: first all their node ids, then all their x and gs, so a thread
+// waits for two rounds of loads per SB items instead of two per item.
+constexpr int SB = 8;
+
+// gs*x of the box of PI x PJ node columns from (i0, j0), planes k0 .. k0+np-1, into
+// xs[((kk*PI + ii)*PJ + jj)*3 ..] (zero outside the mesh and where no node exists); when ids is not
+// null, the node ids (-1 for none) into ids[(kk*PI + ii)*PJ + jj]
+template <class T, int PI, int PJ>
+__device__ __forceinline__ void stage_nodes(int nx, int ny, int nz, int i0, int j0, int k0, int np, const int* __restrict__ nodeId,
+                                            const T* __restrict__ x, const T* __restrict__ gs, T* xs, int* ids) {
+  const int total = PI * PJ * np;
+  for (int t0 = threadIdx.x; t0 < total; t0 += SB * blockDim.x) {
+    int n[SB];
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int t = t0 + u * blockDim.x;
+      n[u] = -1;
+      if (t < total) {
+        const int kk = t % np, col = t / np, jj = col % PJ, ii = col / PJ;
+        const int i = i0 + ii, j = j0 + jj, k = k0 + kk;
+        if (i >= 0 && i < nx && j >= 0 && j < ny && k >= 0 && k < nz) n[u] = nodeId[((size_t)i * ny + j) * nz + k];
+      }
+    }
+    T v[SB][3];
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const size_t o = 3 * (size_t)(n[u] < 0 ? 0 : n[u]);
+#pragma unroll
+      for (int q = 0; q < 3; q++) v[u][q] = n[u] >= 0 ? x[o + q] * gs[o + q] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= total) break;
+      const int kk = t % np, col = t / np, jj = col % PJ, ii = col / PJ;
+      const int at = (kk * PI + ii) * PJ + jj;
+      T* dst = xs + 3 * (size_t)at;
+      dst[0] = v[u][0]; dst[1] = v[u][1]; dst[2] = v[u][2];
+      if (ids) ids[at] = n[u];
+    }
+  }
+}
+
+// cell classes of the box of CI x CJ cell columns from (i0, j0), layers k0 .. k0+nl-1, into
+// cls[(kk*CI + ci)*CJ + cj] (MF_NONE outside the mesh)
+template <int CI, int CJ>
+__device__ __forceinline__ void stage_cells(int nx, int ny, int nz, int i0, int j0, int k0, int nl, const uint16_t* __restrict__ cellCls,
+                                            uint16_t* cls) {
+  const int ncy = ny - 1, ncz = nz - 1;
+  const int total = CI * CJ * nl;
+  for (int t0 = threadIdx.x; t0 < total; t0 += SB * blockDim.x) {
+    uint16_t v[SB];
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int t = t0 + u * blockDim.x;
+      v[u] = MF_NONE;
+      if (t < total) {
+        const int kk = t % nl, col = t / nl, cj = col % CJ, ci = col / CJ;
+        const int i = i0 + ci, j = j0 + cj, k = k0 + kk;
+        if (i >= 0 && i < nx - 1 && j >= 0 && j < ncy && k >= 0 && k < ncz) v[u] = cellCls[((size_t)i * ncy + j) * ncz + k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= total) break;
+      const int kk = t % nl, col = t / nl, cj = col % CJ, ci = col / CJ;
+      cls[(kk * CI + ci) * CJ + cj] = v[u];
+    }
+  }
+}
+
 // ---- apply over all nodes: tiles of MF_TI x MF_TJ node columns and a slab of ks node planes --------
 constexpr int MF_TI = 8, MF_TJ = 8;
 constexpr int MF_PI = MF_TI + 2, MF_PJ = MF_TJ + 2;       // staged node columns (one halo column each side)
@@ -153,7 +227,8 @@ constexpr int MF_THREADS = 256;
 
 template <class T>
 inline size_t mf_apply_smem(int ks) {
-  return (size_t)(ks + 2) * MF_PI * MF_PJ * 3 * sizeof(T) + (size_t)(ks + 1) * MF_CI * MF_CJ * sizeof(uint16_t) + 16;
+  const size_t nodes = (size_t)(ks + 2) * MF_PI * MF_PJ;
+  return nodes * 3 * sizeof(T) + nodes * sizeof(int) + (size_t)(ks + 1) * MF_CI * MF_CJ * sizeof(uint16_t) + 16;
 }
 
 struct MfDims {
@@ -168,39 +243,19 @@ __global__ void __launch_bounds__(MF_THREADS) k_mf_apply(MfDims d, const int* __
                                                          T* __restrict__ y) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int ks = d.ks;
+  const int np = ks + 2;
+  const size_t nodes = (size_t)np * MF_PI * MF_PJ;
   T* xs = reinterpret_cast<T*>(smraw);
-  uint16_t* cls = reinterpret_cast<uint16_t*>(xs + (size_t)(ks + 2) * MF_PI * MF_PJ * 3);
+  int* ids = reinterpret_cast<int*>(xs + nodes * 3);
+  uint16_t* cls = reinterpret_cast<uint16_t*>(ids + nodes);
   int blk = blockIdx.x;
   const int slab = blk % d.slabs; blk /= d.slabs;
   const int tj = blk % d.tilesJ, ti = blk / d.tilesJ;
   const int i0 = ti * MF_TI, j0 = tj * MF_TJ, k0 = slab * ks;
-  const int ncy = d.ny - 1, ncz = d.nz - 1;
-  // stage gs*x of the tile's node columns plus one halo column and plane on every side; threads walk
-  // a column's planes first (consecutive node ids, coalesced)
-  const int np = ks + 2;
-  for (int t = threadIdx.x; t < MF_PI * MF_PJ * np; t += blockDim.x) {
-    const int kk = t % np, col = t / np, jj = col % MF_PJ, ii = col / MF_PJ;
-    const int i = i0 - 1 + ii, j = j0 - 1 + jj, k = k0 - 1 + kk;
-    T v0 = 0, v1 = 0, v2 = 0;
-    if (i >= 0 && i < d.nx && j >= 0 && j < d.ny && k >= 0 && k < d.nz) {
-      const int n = nodeId[((size_t)i * d.ny + j) * d.nz + k];
-      if (n >= 0) {
-        const size_t o = 3 * (size_t)n;
-        v0 = x[o] * gs[o]; v1 = x[o + 1] * gs[o + 1]; v2 = x[o + 2] * gs[o + 2];
-      }
-    }
-    T* dst = xs + ((kk * MF_PI + ii) * MF_PJ + jj) * 3;
-    dst[0] = v0; dst[1] = v1; dst[2] = v2;
-  }
-  // stage the cell classes of cells (i0-1 .. i0+TI-1) x (j0-1 ..) x (k0-1 .. k0+ks-1)
-  const int nc = ks + 1;
-  for (int t = threadIdx.x; t < MF_CI * MF_CJ * nc; t += blockDim.x) {
-    const int ck = t % nc, col = t / nc, cj = col % MF_CJ, ci = col / MF_CJ;
-    const int i = i0 - 1 + ci, j = j0 - 1 + cj, k = k0 - 1 + ck;
-    uint16_t v = MF_NONE;
-    if (i >= 0 && i < d.nx - 1 && j >= 0 && j < ncy && k >= 0 && k < ncz) v = cellCls[((size_t)i * ncy + j) * ncz + k];
-    cls[(ck * MF_CI + ci) * MF_CJ + cj] = v;
-  }
+  // gs*x and the node ids of the tile's node columns plus one halo column and plane on every side,
+  // and the cell classes of cells (i0-1 .. i0+TI-1) x (j0-1 ..) x (k0-1 .. k0+ks-1)
+  stage_nodes<T, MF_PI, MF_PJ>(d.nx, d.ny, d.nz, i0 - 1, j0 - 1, k0 - 1, np, nodeId, x, gs, xs, ids);
+  stage_cells<MF_CI, MF_CJ>(d.nx, d.ny, d.nz, i0 - 1, j0 - 1, k0 - 1, ks + 1, cellCls, cls);
   __syncthreads();
   // node (i0+ii, j0+jj, k0+kk): a warp takes half a plane of the tile (4 x 8 columns), so that its
   // lanes read the same cell classes (one layer) and the class table loads are warp-uniform
@@ -211,7 +266,7 @@ __global__ void __launch_bounds__(MF_THREADS) k_mf_apply(MfDims d, const int* __
   for (int kk = warp >> 1; kk < ks; kk += MF_THREADS / 64) {
     const int k = k0 + kk;
     if (k >= d.nz) break;
-    const int n = nodeId[((size_t)i * d.ny + j) * d.nz + k];
+    const int n = ids[((kk + 1) * MF_PI + ii + 1) * MF_PJ + jj + 1];
     if (n < 0) continue;
     T acc[3] = {0, 0, 0};
     // staged node coordinates of the node: (ii+1, jj+1, kk+1); staged cell coordinates of the cell
@@ -316,31 +371,28 @@ __global__ void __launch_bounds__(SW_THREADS) k_mf_sweep(MfSweepDims d, SwLayout
     for (int e = threadIdx.x; e < pieces; e += blockDim.x) cp_async8(dst + 8 * e, src + 8 * e);
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
+  // the node ids of the tile's columns (-1: none), SB per thread in flight
+  for (int t0 = threadIdx.x; t0 < SLOTS * nz; t0 += SB * blockDim.x) {
+    int n[SB];
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int t = t0 + u * blockDim.x;
+      n[u] = -1;
+      if (t < SLOTS * nz) {
+        const int sl = t / nz, k = t % nz;
+        if (meta[2 * sl] >= 0) n[u] = nodeId[((size_t)(iLo + 1 + 2 * (sl / SC)) * d.ny + jLo + 1 + 2 * (sl % SC)) * nz + k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SB; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t < SLOTS * nz) nid[t] = n[u];
+    }
+  }
   if (!zeroGuess) {
     // node plane k is staged at k+1, cell layer k at k+1
-    const int np = nz + 2;
-    for (int t = threadIdx.x; t < PI * PJ * np; t += blockDim.x) {
-      const int kk = t % np, col = t / np, jj = col % PJ, ii = col / PJ;
-      const int i = iLo + ii, j = jLo + jj, k = kk - 1;
-      T v0 = 0, v1 = 0, v2 = 0;
-      if (i >= 0 && i < d.nx && j >= 0 && j < d.ny && k >= 0 && k < nz) {
-        const int n = nodeId[((size_t)i * d.ny + j) * nz + k];
-        if (n >= 0) {
-          const size_t o = 3 * (size_t)n;
-          v0 = x[o] * gs[o]; v1 = x[o + 1] * gs[o + 1]; v2 = x[o + 2] * gs[o + 2];
-        }
-      }
-      T* dst = xs + ((kk * PI + ii) * PJ + jj) * 3;
-      dst[0] = v0; dst[1] = v1; dst[2] = v2;
-    }
-    const int nl = ncz + 2;
-    for (int t = threadIdx.x; t < CI * CJ * nl; t += blockDim.x) {
-      const int kk = t % nl, col = t / nl, cj = col % CJ, ci = col / CJ;
-      const int i = iLo + ci, j = jLo + cj, k = kk - 1;
-      uint16_t v = MF_NONE;
-      if (i >= 0 && i < d.nx - 1 && j >= 0 && j < ncy && k >= 0 && k < ncz) v = cellCls[((size_t)i * ncy + j) * ncz + k];
-      cls[(kk * CI + ci) * CJ + cj] = v;
-    }
+    stage_nodes<T, PI, PJ>(d.nx, d.ny, nz, iLo, jLo, -1, nz + 2, nodeId, x, gs, xs, nullptr);
+    stage_cells<CI, CJ>(d.nx, d.ny, nz, iLo, jLo, -1, ncz + 2, cellCls, cls);
   }
   __syncthreads();
   // residual rows r = b - Ks x of the tile's columns: the lanes of a warp take the SLOTS columns at
@@ -353,9 +405,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_mf_sweep(MfSweepDims d, SwLayout
     const int i = iLo + ii, j = jLo + jj;
     const bool colOk = meta[2 * s] >= 0;
     for (int k = PLANES_PER_WARP * warp + lane / SLOTS; k < nz; k += PLANES_PER_WARP * (SW_THREADS / 32)) {
-      int n = -1;
-      if (colOk) n = nodeId[((size_t)i * d.ny + j) * nz + k];
-      nid[s * nz + k] = n;
+      const int n = colOk ? nid[s * nz + k] : -1;
       if (n < 0) continue;
       const size_t o = 3 * (size_t)n;
       T rv[3] = {b[o], b[o + 1], b[o + 2]};

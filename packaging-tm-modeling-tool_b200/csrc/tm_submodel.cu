@@ -579,7 +579,7 @@ __global__ void k_sub_sample(int cnt, const int* __restrict__ gp, const double* 
   }
   eps[0] -= f; eps[1] -= f; eps[2] -= f;
   const StepK k = step_constants(P, Etab, T, 1e-9);
-  anand_step(P, pts[8 * (size_t)eAn[e] + g], eps, k, sig, nullptr, false);
+  anand_step(P, pts[8 * (size_t)eAn[e] + g], eps, k, sig, (double*)nullptr, false);
   out[2 * t] = sig[5] * cphi + sig[4] * sphi;
   out[2 * t + 1] = eps[5] * cphi + eps[4] * sphi;
 }

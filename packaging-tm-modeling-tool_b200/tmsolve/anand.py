@@ -129,3 +129,29 @@ def point_step(params: dict, Etab, Ftab, state: np.ndarray, eps: np.ndarray, T: 
     vp = lambda a: a.ctypes.data_as(C.c_void_p)
     check(load().tm_anand_step(C.byref(m), npts, vp(state), vp(eps), float(T), float(dt), vp(sig), vp(D), int(commit)))
     return sig, D
+
+
+def screen_gradient(params: dict, Etab, Ftab, temps, table_site, hist, pillar=None) -> dict:
+    """One site's last-cycle dW and dE and their derivatives with respect to its strain table
+    (ntemps x 6) by forward mode on the GPU (tm_anand_screen_gradient). pillar: None, or
+    (fs, pillar_nu, pEtab, pFtab) for a solder cap on an elastic pillar."""
+    m, keep = material(params, Etab, Ftab)
+    temps = np.ascontiguousarray(temps, np.float64)
+    tab = np.ascontiguousarray(table_site, np.float64).reshape(-1)
+    nt = len(temps)
+    if tab.size != 6 * nt:
+        raise ValueError("the site table needs 6 strains per temperature")
+    t = np.ascontiguousarray(hist["t"], np.float64); T = np.ascontiguousarray(hist["T"], np.float64)
+    cyc = np.ascontiguousarray(hist["cycle"], np.int32); ph = np.ascontiguousarray(hist["phase"], np.int32)
+    dW = C.c_double(); dE = C.c_double(); gW = np.zeros(6 * nt); gE = np.zeros(6 * nt)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    pil = None
+    if pillar is not None:
+        fs, pnu, pE, pF = pillar
+        pE = np.ascontiguousarray(pE, np.float64); pF = np.ascontiguousarray(pF, np.float64)
+        keep = keep + (pE, pF)
+        pil = TmPillar(fs=float(fs), nu=float(pnu), Etab=pE.ctypes.data_as(C.POINTER(C.c_double)),
+                       Ftab=pF.ctypes.data_as(C.POINTER(C.c_double)))
+    check(load().tm_anand_screen_gradient(C.byref(m), C.byref(pil) if pil is not None else None, nt, vp(temps), vp(tab), len(t),
+                                          vp(t), vp(T), vp(cyc), vp(ph), int(hist["cycles"]), C.byref(dW), C.byref(dE), vp(gW), vp(gE)))
+    return dict(dW=dW.value, dE=dE.value, gW=gW.reshape(nt, 6), gE=gE.reshape(nt, 6))

@@ -4,8 +4,11 @@ bump-layer strain table at the die bump sites from those increments (siteStrainT
 Anand screening of the sites over three -40/125 degC cycles at 40 load steps per cycle with the
 module's SAC305 constants.
 
-Bars: every step's displacement increment within 1e-8 (relres 1e-12 on both sides), the strain
-tables within 1e-7 of their largest entry, and per-site dW and dE of the last cycle within 1e-6.
+Bars: every step's displacement increment within 1e-8 (relres 1e-12 on both sides). The analysis
+keeps the increments as float32 (11-analysis.js:256), so two increments that agree to 1e-8 can
+round to neighbouring floats: the strain tables built from each side's own increments agree to 1e-6
+of their largest entry, and per-site dW and dE of the last cycle to 1e-5. From the same increments
+the GPU and the oracle build the same table to 1e-12.
 """
 import numpy as np
 import pytest
@@ -38,7 +41,9 @@ def test_module_thermal_cycle_matches_oracle(oracle_lib):
     to = post.site_strain_table(om, post.ThermalPath(steps, Tb, do, chain, up, down), sites, temps, bl["zmid"], bl["part"])
     ok = np.isfinite(to)
     assert ok.mean() > 0.9 and np.array_equal(ok, np.isfinite(tg))
-    assert np.abs(tg[ok] - to[ok]).max() <= 1e-7 * np.abs(to[ok]).max()
+    assert np.abs(tg[ok] - to[ok]).max() <= 1e-6 * np.abs(to[ok]).max()
+    tgo = post.site_strain_table(om, post.ThermalPath(steps, Tb, dg, chain, up, down), sites, temps, bl["zmid"], bl["part"])
+    assert np.abs(tg[ok] - tgo[ok]).max() <= 1e-12 * np.abs(tgo[ok]).max()
     hist = cycle_history(-40.0, 125.0, 11.0, 15.0, 3, ramp_max_dt=10.0, dwell_steps=3)
     Et, Ft = anand_tables(SAC305_MODULE)
     dW, dE, _ = screen(SAC305_MODULE, Et, Ft, temps, tg, hist)
@@ -46,5 +51,5 @@ def test_module_thermal_cycle_matches_oracle(oracle_lib):
     fin = np.isfinite(oW)
     assert fin.mean() > 0.9 and np.array_equal(fin, np.isfinite(dW))
     assert np.all(oW[fin] > 0)
-    assert np.allclose(dW[fin], oW[fin], rtol=1e-6, atol=0)
-    assert np.allclose(dE[fin], oE[fin], rtol=1e-6, atol=0)
+    assert np.allclose(dW[fin], oW[fin], rtol=1e-5, atol=0)
+    assert np.allclose(dE[fin], oE[fin], rtol=1e-5, atol=0)

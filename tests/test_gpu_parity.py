@@ -251,7 +251,7 @@ def test_warm_start_matches_oracle(oracle_lib):
     ro2 = om.solve(fo2, tol=1e-12, key=1)
     assert r2["converged"] and ro2["converged"]
     assert r2["warm"] == ro2["warm"] == 2
-    assert 0 < ro2["iters0"] < 1
+    assert ro2["iters0"] > 0
     assert abs(r2["iters0"] / ro2["iters0"] - 1) <= 1e-5, (r2["iters0"], ro2["iters0"])
     assert np.linalg.norm(r2["u"] - ro2["u"]) / np.linalg.norm(ro2["u"]) <= 1e-8
     assert abs(r2["iters"] - ro2["iters"]) <= max(3, ro2["iters"] // 4)
@@ -259,14 +259,16 @@ def test_warm_start_matches_oracle(oracle_lib):
 
 def test_bench_workload_parity(oracle_lib):
     """The benchmark workload itself (lidded C2 160x160x32, 2,065,539 DOF) on the GPU in FP64 and in
-    mixed precision against the oracle's FP64 solve, all to relative residual 1e-12: displacements
-    within 1e-8 (FP64) and 1e-5 (mixed), RMS and signed JEITA warpage within 1e-8 and 1e-6."""
+    mixed precision against the oracle's FP64 solve, all to relative residual 1e-13 (the lid on its
+    0.01 GPa TIM makes the operator ill-conditioned enough that two solutions at relres 1e-12 differ
+    by 2e-8): displacements within 1e-8 (FP64) and 1e-5 (mixed), RMS and signed JEITA warpage within
+    1e-8 and 1e-6."""
     from tmsolve import post
     from tmsolve.solver import DeviceModel
     pkg = lidded_c2()
     om = oracle_lib.OracleModel(pkg)
     step = pkg.step()
-    ro = om.solve(om.assemble(step), tol=1e-12)
+    ro = om.solve(om.assemble(step), tol=1e-13)
     assert ro["converged"]
     uo = ro["u"]
     b = post.bga_sites(**pkg.meta["bga"])
@@ -276,7 +278,7 @@ def test_bench_workload_parity(oracle_lib):
     del om
     dm = DeviceModel(pkg)
     for key, (precision, bar_u, bar_w) in enumerate((("fp64", 1e-8, 1e-8), ("mixed", 1e-5, 1e-6))):
-        r = dm.solve(dm.assemble_step(step), tol=1e-12, warm=0, key=key, precision=precision)
+        r = dm.solve(dm.assemble_step(step), tol=1e-13, warm=0, key=key, precision=precision)
         assert r["converged"], precision
         u = r["u"]
         du = np.linalg.norm(u - uo) / np.linalg.norm(uo)
