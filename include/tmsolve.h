@@ -258,6 +258,26 @@ tm_status tm_accumulate_q_device(tm_ctx* ctx, const double* du_dev, int32_t nel,
 tm_status tm_element_strains_device(tm_ctx* ctx, int32_t npts, const int32_t* elem_dev, const double* q_dev,
                                     const double* nat_dev, double* eps_dev);
 
+/* The transposes of the two steps from a step's displacement increment to the strain at a site,
+ * for the adjoint of a function of the site strains (the peak bump dW; no counterpart in the
+ * reference, whose tornado re-runs whole analyses):
+ * tm_element_strains_adjoint: gq (33 per point) = B^T g, B the strain operator of
+ * tm_element_strains at elem[p], nat[3 p ..] and g (6 per point) the function's derivative with
+ * respect to the strains. tm_accumulate_q_adjoint: for the step loaded last (tm_prepare_step) and
+ * gq (33 per element) the derivative with respect to the element DOF increment (du at the nodes,
+ * dalpha = K_aa^-1 (f_a - K_au du)), gdu (24 per element) its derivative with respect to du at the
+ * element's nodes and gA (one per element) its derivative with respect to the logarithm of the
+ * thermal strain of the element's property set through dalpha. Host pointers. */
+tm_status tm_element_strains_adjoint(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* nat, const double* g, double* gq);
+tm_status tm_accumulate_q_adjoint(tm_ctx* ctx, int32_t nel, const int32_t* elems, const double* gq, double* gdu, double* gA);
+/* The adjoint solve of the step assembled last for an adjoint load g (3*nn, the derivative of a
+ * function with respect to the step's displacement increment u), and per property set m the
+ * function's derivatives through that increment: dlogE[m] with respect to the logarithm of the set's
+ * stiffness (lambda^T (f_m - K_m u)) and dlogA[m] with respect to the logarithm of its thermal strain
+ * (lambda^T f_m), lambda = K^-1 g (the same MG-PCG; no counterpart in the reference). */
+tm_status tm_adjoint_sensitivity(tm_ctx* ctx, const double* g, const double* u, const tm_solve_opts* opts, double* dlogE,
+                                 double* dlogA, tm_solve_info* info);
+
 /* ---- element stress histories ---- */
 /* The sub-layers of the layered property sets for the step loaded last, which the stress
  * histories read (per sub-layer s of a section: sectionSubMeanD and sectionSubStress,

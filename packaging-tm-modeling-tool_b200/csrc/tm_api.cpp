@@ -945,6 +945,45 @@ tm_status tm_element_strains(tm_ctx* ctx, int32_t npts, const int32_t* elem, con
   });
 }
 
+// ---- the transposes of the strain recovery, for adjoints of functions of the site strains --------------
+tm_status tm_element_strains_adjoint(tm_ctx* ctx, int32_t npts, const int32_t* elem, const double* nat, const double* g, double* gq) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (npts < 0 || (npts > 0 && (!elem || !nat || !g || !gq))) fail(TM_BAD_INPUT, "tm_element_strains_adjoint: bad arguments");
+    if (npts == 0) return;
+    check_elems(c, npts, elem);
+    DBuf<int> de;
+    DBuf<double> dn, dg, dgq;
+    de.upload(elem, npts, c.stream);
+    dn.upload(nat, 3 * (size_t)npts, c.stream);
+    dg.upload(g, 6 * (size_t)npts, c.stream);
+    dgq.alloc(33 * (size_t)npts);
+    launch_element_strains_adjoint(c, npts, de.p, dn.p, dg.p, dgq.p);
+    dgq.download(gq, 33 * (size_t)npts, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
+tm_status tm_accumulate_q_adjoint(tm_ctx* ctx, int32_t nel, const int32_t* elems, const double* gq, double* gdu, double* gA) {
+  return guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (nel < 0 || (nel > 0 && (!elems || !gq || !gdu || !gA))) fail(TM_BAD_INPUT, "tm_accumulate_q_adjoint: bad arguments");
+    if (nel == 0) return;
+    check_elems(c, nel, elems);
+    recovery_ready(c);
+    DBuf<int> de;
+    DBuf<double> dgq, dgdu, dgA;
+    de.upload(elems, nel, c.stream);
+    dgq.upload(gq, 33 * (size_t)nel, c.stream);
+    dgdu.alloc(24 * (size_t)nel);
+    dgA.alloc(nel);
+    launch_accumulate_q_adjoint(c, nel, de.p, dgq.p, dgdu.p, dgA.p);
+    dgdu.download(gdu, 24 * (size_t)nel, c.stream);
+    dgA.download(gA, nel, c.stream);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  });
+}
+
 // ---- samplePlane at points ------------------------------------------------------------------------
 tm_status tm_sample_plane_device(tm_ctx* ctx, const double* u, int32_t k, int32_t comp, int32_t npts, const double* x,
                                  const double* y, double* out) {
@@ -1125,6 +1164,30 @@ tm_status tm_solve_f32(tm_ctx* ctx, const double* f, float* u32, const tm_solve_
 // (free DOFs); per property set m, with K_m and f_m the set's share of the assembled operator and
 // load, dJ/dlog(E_m) = lambda^T (f_m - K_m u) (K_m and f_m scale with the set's stiffness) and
 // dJ/dlog(alpha_m) = lambda^T f_m (f_m scales with its thermal strain)
+namespace {
+// the adjoint solve K lambda = g (no warm start, nothing stored; constrained DOFs of g zeroed) and,
+// per property set m with K_m and f_m its share of the step's operator and load, dlogE_m =
+// lambda^T (f_m - K_m u) and dlogA_m = lambda^T f_m, summed per element on the device
+tm_status adjoint_sums(Context& c, const double* g, const double* u, const tm_solve_opts* opts, double* dlogE, double* dlogA,
+                       tm_solve_info* info) {
+  const size_t n = 3 * (size_t)c.nn;
+  tm_solve_opts o;
+  if (opts) o = *opts; else tm_default_solve_opts(&o);
+  o.warm = 0;
+  c.d_f.upload(g, n, c.stream);
+  launch_zero_constrained(c, c.d_f.p);
+  c.d_sensLam.alloc(n);
+  const tm_status st = solve_impl(c, c.d_f.p, c.d_sensLam.p, o, info);
+  c.d_sensU.upload(u, n, c.stream);
+  if (!c.d_conn.p) c.d_conn.upload(c.conn, c.stream);
+  std::vector<double> sums(2 * (size_t)c.npset);
+  launch_sens(c, c.d_sensU.p, c.d_sensLam.p, sums.data());
+  for (int p = 0; p < c.npset; p++) { dlogE[p] = sums[2 * p + 1] - sums[2 * p]; dlogA[p] = sums[2 * p + 1]; }
+  c.sensReady = true;
+  return st;
+}
+}  // namespace
+
 tm_status tm_warpage_sensitivity(tm_ctx* ctx, const double* u, int32_t k, const tm_solve_opts* opts, double* J, double* dlogE,
                                  double* dlogA, tm_solve_info* info) {
   tm_status st = TM_OK;
@@ -1159,22 +1222,22 @@ tm_status tm_warpage_sensitivity(tm_ctx* ctx, const double* u, int32_t k, const 
       gr[3 * (size_t)q + 2] = 2 * r / N;
     }
     *J = Jv / N;
-    // the adjoint solve (no warm start, nothing stored)
-    tm_solve_opts o;
-    if (opts) o = *opts; else tm_default_solve_opts(&o);
-    o.warm = 0;
-    c.d_f.upload(gr.data(), n, c.stream);
-    launch_zero_constrained(c, c.d_f.p);
-    c.d_sensLam.alloc(n);
-    st = solve_impl(c, c.d_f.p, c.d_sensLam.p, o, info);
-    c.d_sensU.upload(u, n, c.stream);
-    if (!c.d_conn.p) c.d_conn.upload(c.conn, c.stream);
-    std::vector<double> sums(2 * (size_t)c.npset);
-    launch_sens(c, c.d_sensU.p, c.d_sensLam.p, sums.data());
-    for (int p = 0; p < c.npset; p++) { dlogE[p] = sums[2 * p + 1] - sums[2 * p]; dlogA[p] = sums[2 * p + 1]; }
-    c.sensReady = true;
+    st = adjoint_sums(c, gr.data(), u, opts, dlogE, dlogA, info);
   });
   return g != TM_OK ? g : st;
+}
+
+tm_status tm_adjoint_sensitivity(tm_ctx* ctx, const double* g, const double* u, const tm_solve_opts* opts, double* dlogE, double* dlogA,
+                                 tm_solve_info* info) {
+  tm_status st = TM_OK;
+  tm_status gs = guarded([&] {
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!g || !u || !dlogE || !dlogA) fail(TM_BAD_INPUT, "null argument");
+    if (!c.assembled || !c.stepReady || !c.d_clsKc.p) fail(TM_BAD_INPUT, "sensitivities need a step assembled by tm_assemble_step");
+    for (size_t q = 0; q < 3 * (size_t)c.nn; q++) if (!std::isfinite(g[q])) fail(TM_NONFINITE, "non-finite adjoint load");
+    st = adjoint_sums(c, g, u, opts, dlogE, dlogA, info);
+  });
+  return gs != TM_OK ? gs : st;
 }
 
 tm_status tm_sensitivity_direction(tm_ctx* ctx, const tm_step* base, const tm_step* dir, double* dJ) {

@@ -356,6 +356,8 @@ void launch_to_fp32(Context& c);
 // element DOF histories and strains at points (device pointers; elems/elem, q, nat, eps on the device)
 void launch_accumulate_q(Context& c, const double* du, int nel, const int* elems, double* q);
 void launch_element_strains(Context& c, int np, const int* elem, const double* q, const double* nat, double* eps);
+void launch_element_strains_adjoint(Context& c, int np, const int* elem, const double* nat, const double* g, double* gq);
+void launch_accumulate_q_adjoint(Context& c, int nel, const int* elems, const double* gq, double* gdu, double* gA);
 void launch_sample_plane(Context& c, const double* u, int k, int comp, int npts, const double* x, const double* y, double* out);
 void launch_accumulate_state(Context& c, const double* du, int nel, const int* elems, int stride, double* state);
 void launch_sens(Context& c, const double* u, const double* lam, double* outHost);

@@ -81,15 +81,11 @@ __global__ void k_mf_scales(int nn, int S, const int* __restrict__ pos, const ui
 }
 
 // ---- the row of one node from its 8 cells ---------------------------------------------------------
-// xs: staged gs*x, 3 values per node, node (ii, jj, kk) at ((kk*PI + ii)*PJ + jj)*3; cls: staged cell
-// classes, cell (ci, cj, ck) at (ck*CI + ci)*CJ + cj, where the node's own cell-corner indices are
-// (ii-1, jj-1, kk-1) .. (ii, jj, kk) in staged-cell coordinates shifted by one (cell (ii-1+a) is staged
-// at ii-1+a + co, co = the cell-coordinate offset of the stage)
 template <class T>
 struct KRow;
 template <>
 struct KRow<float> {
-  // 24 values of row r of cell class cc
+  // the 24 values of one row of a cell matrix
   static __device__ __forceinline__ void load(const float* __restrict__ K, float (&k)[24]) {
     const float4* q = reinterpret_cast<const float4*>(K);
 #pragma unroll
@@ -111,26 +107,35 @@ struct KRow<double> {
   }
 };
 
-// acc += (K x) rows of the node at staged node coordinates (ii, jj, kk); staged cell (ci, cj, ck) of
-// the cell whose corner at offsets (1-a, 1-b, 1-c) is this node sits at (ii-1+a+cio, jj-1+b+cjo, kk-1+c+cko)
+// acc += the node's rows of K x. Staged gs*x is stored by component (structure of arrays):
+// component q of the node at staged (kk, ii, jj) is xs[q*NS + (kk*PI + ii)*PJ + jj], so a warp whose
+// lanes take consecutive (or every other) jj reads 32 different banks. (ii, jj, kk): the node's
+// staged coordinates; (ci0, cj0, ck0): the staged coordinates of cell (i-1, j-1, k-1), cells stored at
+// (ck*CI + ci)*CJ + cj. Per cell layer c the node's 18 neighbours on its two node planes are loaded
+// once into registers and serve that layer's four cells (the cell whose corner (1-a, 1-b, 1-c) is the
+// node, its 8 nodes in the local order of the element matrix).
 template <class T, int PI, int PJ, int CI, int CJ>
-__device__ __forceinline__ void node_row(const T* __restrict__ xs, const uint16_t* __restrict__ cls, const T* __restrict__ ccK, int ii, int jj,
-                                         int kk, int ci0, int cj0, int ck0, T (&acc)[3]) {
+__device__ __forceinline__ void node_row(const T* __restrict__ xs, int NS, const uint16_t* __restrict__ cls, const T* __restrict__ ccK,
+                                         int ii, int jj, int kk, int ci0, int cj0, int ck0, T (&acc)[3]) {
 #pragma unroll
-  for (int c = 0; c < 2; c++)
+  for (int c = 0; c < 2; c++) {
+    T xv[2][3][3][3];
+#pragma unroll
+    for (int dk = 0; dk < 2; dk++)
+#pragma unroll
+      for (int di = 0; di < 3; di++)
+#pragma unroll
+        for (int dj = 0; dj < 3; dj++) {
+          const int at = ((kk - 1 + c + dk) * PI + ii - 1 + di) * PJ + jj - 1 + dj;
+#pragma unroll
+          for (int q = 0; q < 3; q++) xv[dk][di][dj][q] = xs[q * NS + at];
+        }
 #pragma unroll
     for (int b = 0; b < 2; b++)
 #pragma unroll
       for (int a = 0; a < 2; a++) {
         const int cc = cls[((ck0 + c) * CI + ci0 + a) * CJ + cj0 + b];
         if (cc == MF_NONE) continue;
-        // the cell's 8 nodes, gathered in the local order of the element matrix
-        T xv[24];
-#pragma unroll
-        for (int M = 0; M < 8; M++) {
-          const T* xp = xs + (((kk - 1 + c + loc_c(M)) * PI + ii - 1 + a + loc_a(M)) * PJ + jj - 1 + b + loc_b(M)) * 3;
-          xv[3 * M] = xp[0]; xv[3 * M + 1] = xp[1]; xv[3 * M + 2] = xp[2];
-        }
         const int Lrow = loc_of(1 - a, 1 - b, 1 - c);
         const T* K = ccK + (size_t)cc * 576 + 3 * Lrow * 24;
 #pragma unroll
@@ -139,10 +144,13 @@ __device__ __forceinline__ void node_row(const T* __restrict__ xs, const uint16_
           KRow<T>::load(K + 24 * p, k);
           T s = 0;
 #pragma unroll
-          for (int q = 0; q < 24; q++) s += k[q] * xv[q];
+          for (int M = 0; M < 8; M++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) s += k[3 * M + q] * xv[loc_c(M)][a + loc_a(M)][b + loc_b(M)][q];
           acc[p] += s;
         }
       }
+  }
 }
 
 // ---- staging of a box of nodes and cells into shared memory -----------------------------------------
@@ -151,9 +159,9 @@ __device__ __forceinline__ void node_row(const T* __restrict__ xs, const uint16_
 // waits for two rounds of loads per SB items instead of two per item.
 constexpr int SB = 8;
 
-// gs*x of the box of PI x PJ node columns from (i0, j0), planes k0 .. k0+np-1, into
-// xs[((kk*PI + ii)*PJ + jj)*3 ..] (zero outside the mesh and where no node exists); when ids is not
-// null, the node ids (-1 for none) into ids[(kk*PI + ii)*PJ + jj]
+// gs*x of the box of PI x PJ node columns from (i0, j0), planes k0 .. k0+np-1, by component into
+// xs[q*NS + (kk*PI + ii)*PJ + jj], NS = np*PI*PJ (zero outside the mesh and where no node exists);
+// when ids is not null, the node ids (-1 for none) into ids[(kk*PI + ii)*PJ + jj]
 template <class T, int PI, int PJ>
 __device__ __forceinline__ void stage_nodes(int nx, int ny, int nz, int i0, int j0, int k0, int np, const int* __restrict__ nodeId,
                                             const T* __restrict__ x, const T* __restrict__ gs, T* xs, int* ids) {
@@ -183,8 +191,7 @@ __device__ __forceinline__ void stage_nodes(int nx, int ny, int nz, int i0, int 
       if (t >= total) break;
       const int kk = t % np, col = t / np, jj = col % PJ, ii = col / PJ;
       const int at = (kk * PI + ii) * PJ + jj;
-      T* dst = xs + 3 * (size_t)at;
-      dst[0] = v[u][0]; dst[1] = v[u][1]; dst[2] = v[u][2];
+      xs[at] = v[u][0]; xs[total + at] = v[u][1]; xs[2 * total + at] = v[u][2];
       if (ids) ids[at] = n[u];
     }
   }
@@ -220,10 +227,13 @@ __device__ __forceinline__ void stage_cells(int nx, int ny, int nz, int i0, int 
 }
 
 // ---- apply over all nodes: tiles of MF_TI x MF_TJ node columns and a slab of ks node planes --------
-constexpr int MF_TI = 8, MF_TJ = 8;
+// A warp takes one row of the tile's 32 node columns in one plane (lane = jj): its lanes read
+// consecutive words of the staged x and the same cell layer, so the class-table loads are uniform.
+constexpr int MF_TI = 4, MF_TJ = 32;
 constexpr int MF_PI = MF_TI + 2, MF_PJ = MF_TJ + 2;       // staged node columns (one halo column each side)
 constexpr int MF_CI = MF_TI + 1, MF_CJ = MF_TJ + 1;       // staged cell columns
 constexpr int MF_THREADS = 256;
+constexpr int MF_PLANES = MF_THREADS / 32 / MF_TI;        // planes per pass of the CTA's warps
 
 template <class T>
 inline size_t mf_apply_smem(int ks) {
@@ -244,10 +254,10 @@ __global__ void __launch_bounds__(MF_THREADS) k_mf_apply(MfDims d, const int* __
   extern __shared__ __align__(16) unsigned char smraw[];
   const int ks = d.ks;
   const int np = ks + 2;
-  const size_t nodes = (size_t)np * MF_PI * MF_PJ;
+  const int NS = np * MF_PI * MF_PJ;
   T* xs = reinterpret_cast<T*>(smraw);
-  int* ids = reinterpret_cast<int*>(xs + nodes * 3);
-  uint16_t* cls = reinterpret_cast<uint16_t*>(ids + nodes);
+  int* ids = reinterpret_cast<int*>(xs + 3 * (size_t)NS);
+  uint16_t* cls = reinterpret_cast<uint16_t*>(ids + NS);
   int blk = blockIdx.x;
   const int slab = blk % d.slabs; blk /= d.slabs;
   const int tj = blk % d.tilesJ, ti = blk / d.tilesJ;
@@ -257,21 +267,18 @@ __global__ void __launch_bounds__(MF_THREADS) k_mf_apply(MfDims d, const int* __
   stage_nodes<T, MF_PI, MF_PJ>(d.nx, d.ny, d.nz, i0 - 1, j0 - 1, k0 - 1, np, nodeId, x, gs, xs, ids);
   stage_cells<MF_CI, MF_CJ>(d.nx, d.ny, d.nz, i0 - 1, j0 - 1, k0 - 1, ks + 1, cellCls, cls);
   __syncthreads();
-  // node (i0+ii, j0+jj, k0+kk): a warp takes half a plane of the tile (4 x 8 columns), so that its
-  // lanes read the same cell classes (one layer) and the class table loads are warp-uniform
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ii = (warp & 1) * 4 + (lane >> 3), jj = lane & 7;
+  const int ii = warp % MF_TI, jj = lane;
   const int i = i0 + ii, j = j0 + jj;
   if (i >= d.nx || j >= d.ny) return;
-  for (int kk = warp >> 1; kk < ks; kk += MF_THREADS / 64) {
+  for (int kk = warp / MF_TI; kk < ks; kk += MF_PLANES) {
     const int k = k0 + kk;
     if (k >= d.nz) break;
     const int n = ids[((kk + 1) * MF_PI + ii + 1) * MF_PJ + jj + 1];
     if (n < 0) continue;
     T acc[3] = {0, 0, 0};
-    // staged node coordinates of the node: (ii+1, jj+1, kk+1); staged cell coordinates of the cell
-    // (i-1+a, j-1+b, k-1+c): (ii+a, jj+b, kk+c)
-    node_row<T, MF_PI, MF_PJ, MF_CI, MF_CJ>(xs, cls, ccK, ii + 1, jj + 1, kk + 1, ii, jj, kk, acc);
+    // staged node coordinates of the node: (ii+1, jj+1, kk+1); of cell (i-1, j-1, k-1): (ii, jj, kk)
+    node_row<T, MF_PI, MF_PJ, MF_CI, MF_CJ>(xs, NS, cls, ccK, ii + 1, jj + 1, kk + 1, ii, jj, kk, acc);
     const size_t o = 3 * (size_t)n;
 #pragma unroll
     for (int p = 0; p < 3; p++) {
@@ -282,217 +289,187 @@ __global__ void __launch_bounds__(MF_THREADS) k_mf_apply(MfDims d, const int* __
   }
 }
 
-// ---- colour sweep: tiles of SR x SC columns of one colour -------------------------------------------
-// The tile's columns are (pi + 2 r, pj + 2 c) for r < SR, c < SC (colour rows and columns of the
-// tile); their neighbours span 2 SR + 1 x 2 SC + 1 node columns, staged over all node planes. The
-// column factors of the tile's columns are copied into shared memory asynchronously while the
-// residual rows are computed. FP32: 2 x 8 columns (the 32 lanes of a warp take two planes); FP64:
-// 1 x 8 (four planes per warp), which keeps two CTAs per SM.
-constexpr int SW_SC = 8;
-constexpr int SW_THREADS = 256;
-template <class T>
-struct SwShape { static constexpr int SR = sizeof(T) == 4 ? 2 : 1; };
+// ---- one colour of the level-0 sweep: residual rows, then the column solves -----------------------------
+// Residual: a CTA takes one colour row of RS_SC colour columns (i = pi + 2 tr, j = pj + 2 (RS_SC tc + c))
+// over all planes; their neighbours span 3 x (2 RS_SC + 1) node columns. Lanes 0-15 take the 16
+// columns at one plane (every other staged column: 16 banks), lanes 16-31 the next plane (an odd
+// plane stride away: the other 16 banks). r = b - Ks x goes to a global buffer in node order.
+constexpr int RS_SC = 16;
+constexpr int RS_PI = 3, RS_PJ = 2 * RS_SC + 1, RS_CI = 2, RS_CJ = 2 * RS_SC;
+constexpr int RS_THREADS = 256;
 
-struct SwLayout {
-  size_t xs, cls, F, r, nid, meta, total;
-};
 template <class T>
-inline SwLayout sw_layout(int nz) {
-  constexpr int SR = SwShape<T>::SR, SLOTS = SR * SW_SC;
-  constexpr int PI = 2 * SR + 1, PJ = 2 * SW_SC + 1, CI = 2 * SR, CJ = 2 * SW_SC;
-  SwLayout L;
-  size_t o = 0;
-  auto take = [&](size_t bytes) { const size_t at = o; o = (o + bytes + 15) / 16 * 16; return at; };
-  // node planes -1 .. nz and cell layers -1 .. nz-1, zero / no class outside the mesh
-  L.xs = take((size_t)(nz + 2) * PI * PJ * 3 * sizeof(T));
-  L.cls = take((size_t)(nz + 1) * CI * CJ * sizeof(uint16_t));
-  L.F = take((size_t)SLOTS * nz * 18 * sizeof(T));
-  L.r = take((size_t)SLOTS * nz * 3 * sizeof(T));
-  L.nid = take((size_t)SLOTS * nz * sizeof(int));
-  L.meta = take((size_t)SLOTS * 2 * sizeof(int));
-  L.total = o;
-  return L;
+inline size_t mf_resid_smem(int nz) {
+  const size_t nodes = (size_t)(nz + 2) * RS_PI * RS_PJ;
+  return nodes * 3 * sizeof(T) + (size_t)(nz + 1) * RS_CI * RS_CJ * sizeof(uint16_t) + (size_t)RS_SC * nz * sizeof(int) + 32;
 }
 
-struct MfSweepDims {
+struct MfColDims {
   int nx, ny, nz;
   int pi, pj;          // colour parities
   int rows, cols;      // colour rows / columns of the colour
   int tilesJ;          // tiles along the colour columns
 };
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
 template <class T>
-__global__ void __launch_bounds__(SW_THREADS) k_mf_sweep(MfSweepDims d, SwLayout lay, const int* __restrict__ nodeId,
-                                                         const int* __restrict__ colStart, const int* __restrict__ colP0,
-                                                         const uint16_t* __restrict__ cellCls, const T* __restrict__ ccK,
-                                                         const T* __restrict__ gs, const T* __restrict__ os, const T* __restrict__ cd,
-                                                         const T* __restrict__ F, const T* __restrict__ b, T* __restrict__ x,
-                                                         int zeroGuess) {
-  constexpr int SR = SwShape<T>::SR, SC = SW_SC, SLOTS = SR * SC;
-  constexpr int PI = 2 * SR + 1, PJ = 2 * SC + 1, CI = 2 * SR, CJ = 2 * SC;
-  constexpr int PLANES_PER_WARP = 32 / SLOTS;
+__global__ void __launch_bounds__(RS_THREADS) k_mf_resid(MfColDims d, const int* __restrict__ nodeId, const uint16_t* __restrict__ cellCls,
+                                                         const T* __restrict__ ccK, const T* __restrict__ gs, const T* __restrict__ os,
+                                                         const T* __restrict__ cd, const T* __restrict__ b, const T* __restrict__ x,
+                                                         T* __restrict__ r) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* xs = reinterpret_cast<T*>(smraw + lay.xs);
-  uint16_t* cls = reinterpret_cast<uint16_t*>(smraw + lay.cls);
-  T* Fs = reinterpret_cast<T*>(smraw + lay.F);
-  T* rs = reinterpret_cast<T*>(smraw + lay.r);
-  int* nid = reinterpret_cast<int*>(smraw + lay.nid);
-  int* meta = reinterpret_cast<int*>(smraw + lay.meta);
-  const int nz = d.nz, ncy = d.ny - 1, ncz = d.nz - 1;
+  const int nz = d.nz;
+  const int NS = (nz + 2) * RS_PI * RS_PJ;
+  T* xs = reinterpret_cast<T*>(smraw);
+  uint16_t* cls = reinterpret_cast<uint16_t*>(xs + 3 * (size_t)NS);
+  int* nid = reinterpret_cast<int*>(smraw + ((3 * (size_t)NS * sizeof(T) + (size_t)(nz + 1) * RS_CI * RS_CJ * sizeof(uint16_t) + 15) / 16) * 16);
   const int tr = blockIdx.x / d.tilesJ, tc = blockIdx.x % d.tilesJ;
-  const int iLo = d.pi + 2 * SR * tr - 1, jLo = d.pj + 2 * SC * tc - 1;   // first staged node column
-  // the tile's columns: first position and length
-  if (threadIdx.x < SLOTS) {
-    const int r = threadIdx.x / SC, c = threadIdx.x % SC;
-    const int cr = SR * tr + r, ccol = SC * tc + c;
-    int p0 = -1, len = 0;
-    if (cr < d.rows && ccol < d.cols) {
-      const int col = (d.pi + 2 * cr) * d.ny + d.pj + 2 * ccol;
-      len = colStart[col + 1] - colStart[col];
-      p0 = len > 0 ? colP0[col] : -1;
-    }
-    meta[2 * threadIdx.x] = p0;
-    meta[2 * threadIdx.x + 1] = len;
-  }
-  __syncthreads();
-  // column factors (18 per node, position order) -> Fs[slot][l][18], asynchronously in 8-byte pieces
-  for (int s = 0; s < SLOTS; s++) {
-    const int p0 = meta[2 * s], len = meta[2 * s + 1];
-    if (p0 < 0) continue;
-    const unsigned char* src = reinterpret_cast<const unsigned char*>(F + 18 * (size_t)p0);
-    unsigned char* dst = reinterpret_cast<unsigned char*>(Fs + (size_t)s * nz * 18);
-    const int pieces = (int)(18 * sizeof(T) / 8) * len;
-    for (int e = threadIdx.x; e < pieces; e += blockDim.x) cp_async8(dst + 8 * e, src + 8 * e);
-  }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  const int i = d.pi + 2 * tr;
+  const int iLo = i - 1, jLo = d.pj + 2 * RS_SC * tc - 1;   // first staged node column
   // the node ids of the tile's columns (-1: none), SB per thread in flight
-  for (int t0 = threadIdx.x; t0 < SLOTS * nz; t0 += SB * blockDim.x) {
+  for (int t0 = threadIdx.x; t0 < RS_SC * nz; t0 += SB * blockDim.x) {
     int n[SB];
 #pragma unroll
     for (int u = 0; u < SB; u++) {
       const int t = t0 + u * blockDim.x;
       n[u] = -1;
-      if (t < SLOTS * nz) {
-        const int sl = t / nz, k = t % nz;
-        if (meta[2 * sl] >= 0) n[u] = nodeId[((size_t)(iLo + 1 + 2 * (sl / SC)) * d.ny + jLo + 1 + 2 * (sl % SC)) * nz + k];
+      if (t < RS_SC * nz) {
+        const int c = t / nz, k = t % nz;
+        if (RS_SC * tc + c < d.cols) n[u] = nodeId[((size_t)i * d.ny + jLo + 1 + 2 * c) * nz + k];
       }
     }
 #pragma unroll
     for (int u = 0; u < SB; u++) {
       const int t = t0 + u * blockDim.x;
-      if (t < SLOTS * nz) nid[t] = n[u];
+      if (t < RS_SC * nz) nid[t] = n[u];
     }
   }
-  if (!zeroGuess) {
-    // node plane k is staged at k+1, cell layer k at k+1
-    stage_nodes<T, PI, PJ>(d.nx, d.ny, nz, iLo, jLo, -1, nz + 2, nodeId, x, gs, xs, nullptr);
-    stage_cells<CI, CJ>(d.nx, d.ny, nz, iLo, jLo, -1, ncz + 2, cellCls, cls);
-  }
+  // node plane k is staged at k+1, cell layer k at k+1
+  stage_nodes<T, RS_PI, RS_PJ>(d.nx, d.ny, nz, iLo, jLo, -1, nz + 2, nodeId, x, gs, xs, nullptr);
+  stage_cells<RS_CI, RS_CJ>(d.nx, d.ny, nz, iLo, jLo, -1, nz + 1, cellCls, cls);
   __syncthreads();
-  // residual rows r = b - Ks x of the tile's columns: the lanes of a warp take the SLOTS columns at
-  // PLANES_PER_WARP consecutive planes
-  {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = lane % SLOTS;
-    const int r = s / SC, c = s % SC;
-    const int ii = 1 + 2 * r, jj = 1 + 2 * c;   // staged coordinates of the column
-    const int i = iLo + ii, j = jLo + jj;
-    const bool colOk = meta[2 * s] >= 0;
-    for (int k = PLANES_PER_WARP * warp + lane / SLOTS; k < nz; k += PLANES_PER_WARP * (SW_THREADS / 32)) {
-      const int n = colOk ? nid[s * nz + k] : -1;
-      if (n < 0) continue;
-      const size_t o = 3 * (size_t)n;
-      T rv[3] = {b[o], b[o + 1], b[o + 2]};
-      if (!zeroGuess) {
-        T acc[3] = {0, 0, 0};
-        // cell (i-1+a, j-1+b, k-1+c) is staged at (ii-1+a, jj-1+b, k+c); node (i, j, k) at (ii, jj, k+1)
-        node_row<T, PI, PJ, CI, CJ>(xs, cls, ccK, ii, jj, k + 1, ii - 1, jj - 1, k, acc);
-#pragma unroll
-        for (int p = 0; p < 3; p++) {
-          const T g = gs[o + p];
-          rv[p] -= g != (T)0 ? os[o + p] * acc[p] : cd[o + p] * x[o + p];
-        }
-      }
-      T* rp = rs + ((size_t)s * nz + k) * 3;
-      rp[0] = rv[0]; rp[1] = rv[1]; rp[2] = rv[2];
-    }
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  // block-tridiagonal solve of every column (solveColumn, 10-solver.js:71-104), one thread per column,
-  // with the reciprocal pivots stored in the factors' upper slots; absent planes are skipped
-  if (threadIdx.x < SLOTS && meta[2 * threadIdx.x] >= 0) {
-    const int s = threadIdx.x;
-    const T* Fc = Fs + (size_t)s * nz * 18;
-    T* rc = rs + (size_t)s * nz * 3;
-    const int* nc = nid + s * nz;
-    T p0 = 0, p1 = 0, p2 = 0;
-    int l = 0;
-    for (int k = 0; k < nz; k++) {
-      if (nc[k] < 0) continue;
-      const T* f = Fc + 18 * l;
-      T b0 = rc[3 * k], b1 = rc[3 * k + 1], b2 = rc[3 * k + 2];
-      if (l > 0) {
-        b0 -= f[9] * p0 + f[10] * p1 + f[11] * p2;
-        b1 -= f[12] * p0 + f[13] * p1 + f[14] * p2;
-        b2 -= f[15] * p0 + f[16] * p1 + f[17] * p2;
-      }
-      p0 = b0 * f[1];
-      p1 = (b1 - f[3] * p0) * f[2];
-      p2 = (b2 - f[6] * p0 - f[7] * p1) * f[5];
-      rc[3 * k] = p0; rc[3 * k + 1] = p1; rc[3 * k + 2] = p2;
-      l++;
-    }
-    T q0 = 0, q1 = 0, q2 = 0;
-    const T* g = nullptr;
-    for (int k = nz - 1; k >= 0; k--) {
-      if (nc[k] < 0) continue;
-      l--;
-      const T* f = Fc + 18 * l;
-      T b0 = rc[3 * k], b1 = rc[3 * k + 1], b2 = rc[3 * k + 2];
-      if (g) {
-        b0 -= g[9] * q0 + g[12] * q1 + g[15] * q2;
-        b1 -= g[10] * q0 + g[13] * q1 + g[16] * q2;
-        b2 -= g[11] * q0 + g[14] * q1 + g[17] * q2;
-      }
-      q2 = b2 * f[5];
-      q1 = (b1 - f[7] * q2) * f[2];
-      q0 = (b0 - f[3] * q1 - f[6] * q2) * f[1];
-      rc[3 * k] = q0; rc[3 * k + 1] = q1; rc[3 * k + 2] = q2;
-      g = f;
-    }
-  }
-  __syncthreads();
-  // x += dx
-  for (int t = threadIdx.x; t < SLOTS * nz; t += blockDim.x) {
-    const int n = nid[t];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = lane & (RS_SC - 1), jj = 1 + 2 * c;
+  for (int k = 2 * warp + (lane >> 4); k < nz; k += 2 * (RS_THREADS / 32)) {
+    const int n = nid[c * nz + k];
     if (n < 0) continue;
-    const T* rp = rs + (size_t)t * 3;
+    T acc[3] = {0, 0, 0};
+    // node (i, j, k) at staged (1, jj, k+1); cell (i-1, j-1, k-1) at staged (0, jj-1, k)
+    node_row<T, RS_PI, RS_PJ, RS_CI, RS_CJ>(xs, NS, cls, ccK, 1, jj, k + 1, 0, jj - 1, k, acc);
     const size_t o = 3 * (size_t)n;
-    if (zeroGuess) { x[o] = rp[0]; x[o + 1] = rp[1]; x[o + 2] = rp[2]; }
-    else { x[o] += rp[0]; x[o + 1] += rp[1]; x[o + 2] += rp[2]; }
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      const T g = gs[o + p];
+      r[o + p] = b[o + p] - (g != (T)0 ? os[o + p] * acc[p] : cd[o + p] * x[o + p]);
+    }
   }
 }
 
-MfDims apply_dims(const Context& c) {
+// Column solves: a warp per column of the colour's list; lane l holds the positions l, l+32, ... of
+// the column (its factors, 15 of the 18 values, and its residual rows, coalesced loads), and the
+// block-tridiagonal forward and backward substitutions of solveColumn (10-solver.js:71-104) run down
+// and up the column with the neighbour's values broadcast by warp shuffles. x += dx (x = dx on the
+// cycle's first sweep, whose residual is b itself).
+constexpr int CS_MAXS = 4;   // up to 128 nodes per column
+template <class T>
+__global__ void __launch_bounds__(256) k_col_solve(int ncols, const int* __restrict__ colPos, const int* __restrict__ posNode,
+                                                   const T* __restrict__ F, const T* __restrict__ r, T* __restrict__ x, int zeroGuess) {
+  const int lane = threadIdx.x & 31;
+  const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= ncols) return;
+  const int p0 = colPos[q], len = colPos[q + 1] - p0;
+  T f[CS_MAXS][15], v[CS_MAXS][3];
+  int nd[CS_MAXS];
+#pragma unroll
+  for (int s = 0; s < CS_MAXS; s++) {
+    const int pos = 32 * s + lane;
+    nd[s] = -1;
+    if (pos < len) {
+      const T* fp = F + 18 * (size_t)(p0 + pos);
+      f[s][0] = fp[1]; f[s][1] = fp[2]; f[s][2] = fp[3]; f[s][3] = fp[5]; f[s][4] = fp[6]; f[s][5] = fp[7];
+#pragma unroll
+      for (int t = 0; t < 9; t++) f[s][6 + t] = fp[9 + t];
+      const int n = posNode[p0 + pos];
+      nd[s] = n;
+      v[s][0] = r[3 * (size_t)n]; v[s][1] = r[3 * (size_t)n + 1]; v[s][2] = r[3 * (size_t)n + 2];
+    } else {
+#pragma unroll
+      for (int t = 0; t < 15; t++) f[s][t] = 0;
+      v[s][0] = v[s][1] = v[s][2] = 0;
+    }
+  }
+  // forward: y = L_pp^-1 (r - L_p,p-1 y_prev); f[0..5] = (1/l00, 1/l11, l10, 1/l22, l20, l21), f[6..14] = L_p,p-1
+  T y0 = 0, y1 = 0, y2 = 0;
+#pragma unroll
+  for (int s = 0; s < CS_MAXS; s++) {
+    if (32 * s >= len) break;
+    for (int l = 0; l < 32; l++) {
+      const int pos = 32 * s + l;
+      if (pos >= len) break;
+      if (lane == l) {
+        T b0 = v[s][0], b1 = v[s][1], b2 = v[s][2];
+        if (pos > 0) {
+          b0 -= f[s][6] * y0 + f[s][7] * y1 + f[s][8] * y2;
+          b1 -= f[s][9] * y0 + f[s][10] * y1 + f[s][11] * y2;
+          b2 -= f[s][12] * y0 + f[s][13] * y1 + f[s][14] * y2;
+        }
+        const T n0 = b0 * f[s][0];
+        const T n1 = (b1 - f[s][2] * n0) * f[s][1];
+        const T n2 = (b2 - f[s][4] * n0 - f[s][5] * n1) * f[s][3];
+        v[s][0] = n0; v[s][1] = n1; v[s][2] = n2;
+        y0 = n0; y1 = n1; y2 = n2;
+      }
+      y0 = __shfl_sync(0xffffffffu, y0, l);
+      y1 = __shfl_sync(0xffffffffu, y1, l);
+      y2 = __shfl_sync(0xffffffffu, y2, l);
+    }
+  }
+  // backward: z = L_pp^-T (y - L_p+1,p^T z_next), the product with L_p+1,p formed by the next position's lane
+  T t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+  for (int s = CS_MAXS - 1; s >= 0; s--) {
+    if (32 * s >= len) continue;
+    for (int l = 31; l >= 0; l--) {
+      const int pos = 32 * s + l;
+      if (pos >= len) continue;
+      if (lane == l) {
+        T b0 = v[s][0], b1 = v[s][1], b2 = v[s][2];
+        if (pos + 1 < len) { b0 -= t0; b1 -= t1; b2 -= t2; }
+        const T z2 = b2 * f[s][3];
+        const T z1 = (b1 - f[s][5] * z2) * f[s][1];
+        const T z0 = (b0 - f[s][2] * z1 - f[s][4] * z2) * f[s][0];
+        v[s][0] = z0; v[s][1] = z1; v[s][2] = z2;
+        t0 = f[s][6] * z0 + f[s][9] * z1 + f[s][12] * z2;
+        t1 = f[s][7] * z0 + f[s][10] * z1 + f[s][13] * z2;
+        t2 = f[s][8] * z0 + f[s][11] * z1 + f[s][14] * z2;
+      }
+      t0 = __shfl_sync(0xffffffffu, t0, l);
+      t1 = __shfl_sync(0xffffffffu, t1, l);
+      t2 = __shfl_sync(0xffffffffu, t2, l);
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < CS_MAXS; s++) {
+    if (nd[s] < 0) continue;
+    const size_t o = 3 * (size_t)nd[s];
+    if (zeroGuess) { x[o] = v[s][0]; x[o + 1] = v[s][1]; x[o + 2] = v[s][2]; }
+    else { x[o] += v[s][0]; x[o + 1] += v[s][1]; x[o + 2] += v[s][2]; }
+  }
+}
+
+MfDims apply_dims(const Context& c, bool fp64) {
   MfDims d;
   d.nx = c.nx; d.ny = c.ny; d.nz = c.nz;
   d.tilesI = (c.nx + MF_TI - 1) / MF_TI;
   d.tilesJ = (c.ny + MF_TJ - 1) / MF_TJ;
-  d.slabs = (c.nz + 15) / 16;
+  const int maxKs = fp64 ? 8 : 16;
+  d.slabs = (c.nz + maxKs - 1) / maxKs;
   d.ks = (c.nz + d.slabs - 1) / d.slabs;
   return d;
 }
 
 template <class T, bool RES>
 void mf_apply(Context& c, const T* ccK, const T* gs, const T* os, const T* cd, const T* x, const T* b, T* y) {
-  const MfDims d = apply_dims(c);
+  const MfDims d = apply_dims(c, sizeof(T) == 8);
   const size_t smem = mf_apply_smem<T>(d.ks);
   if (smem > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_mf_apply<T, RES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_mf_apply<T, RES><<<d.tilesI * d.tilesJ * d.slabs, MF_THREADS, smem, c.stream>>>(d, c.d_nodeId.p, c.d_cellCls.p, ccK, gs, os, cd, x, b, y);
@@ -548,7 +525,7 @@ void mf_build_cells(Context& c, int stage) {
   c.mfModule = c.moduleStage;
   // the colour sweep stages whole node columns: meshes with too many node planes keep the stencil
   c.mfAvailable = ok && !key.empty() && TM_MATRIX_FREE && mf_sweep_smem(c.nz) <= (size_t)smemMax &&
-                  mf_apply_smem<double>(apply_dims(c).ks) <= (size_t)smemMax;
+                  mf_apply_smem<double>(apply_dims(c, true).ks) <= (size_t)smemMax && c.maxColLen <= 32 * CS_MAXS;
   if (!c.mfAvailable) return;
   c.ncc = (int)key.size();
   cudaStream_t st = c.stream;
@@ -594,35 +571,41 @@ void launch_mf_apply32(Context& c, const float* x, float* y, const float* b) {
   else mf_apply<float, false>(c, c.d_ccK32.p, c.d_gs32.p, c.d_os32.p, c.d_cd32.p, x, nullptr, y);
 }
 
-size_t mf_sweep_smem(int nz) { return std::max(sw_layout<float>(nz).total, sw_layout<double>(nz).total); }
+size_t mf_sweep_smem(int nz) { return std::max(mf_resid_smem<float>(nz), mf_resid_smem<double>(nz)); }
 
 namespace {
+// one colour of the level-0 sweep: the colour's residual rows (not on the cycle's first sweep,
+// whose residual is b), then a warp per column solves and updates x
 template <class T>
-void mf_sweep(Context& c, int col, int zeroGuess, const T* ccK, const T* gs, const T* os, const T* cd, const T* F, const T* b, T* x) {
-  constexpr int SR = SwShape<T>::SR;
-  MfSweepDims d;
+void mf_sweep(Context& c, int col, int zeroGuess, const T* ccK, const T* gs, const T* os, const T* cd, const T* F, const T* b, T* x,
+              T* res) {
+  MfColDims d;
   d.nx = c.nx; d.ny = c.ny; d.nz = c.nz;
   d.pi = col >> 1; d.pj = col & 1;
   d.rows = (c.nx - d.pi + 1) / 2;
   d.cols = (c.ny - d.pj + 1) / 2;
-  if (d.rows <= 0 || d.cols <= 0) return;
-  d.tilesJ = (d.cols + SW_SC - 1) / SW_SC;
-  const int tilesI = (d.rows + SR - 1) / SR;
-  const SwLayout lay = sw_layout<T>(c.nz);
-  if (lay.total > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_mf_sweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total));
-  k_mf_sweep<T><<<tilesI * d.tilesJ, SW_THREADS, lay.total, c.stream>>>(d, lay, c.d_nodeId.p, c.d_colStart.p, c.d_colP0.p, c.d_cellCls.p,
-                                                                      ccK, gs, os, cd, F, b, x, zeroGuess);
+  if (d.rows <= 0 || d.cols <= 0 || !c.colorCount[col]) return;
+  d.tilesJ = (d.cols + RS_SC - 1) / RS_SC;
+  if (!zeroGuess) {
+    const size_t smem = mf_resid_smem<T>(c.nz);
+    if (smem > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_mf_resid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_mf_resid<T><<<d.rows * d.tilesJ, RS_THREADS, smem, c.stream>>>(d, c.d_nodeId.p, c.d_cellCls.p, ccK, gs, os, cd, b, x, res);
+    note_launch();
+  }
+  const int ncols = c.colorCount[col];
+  k_col_solve<T><<<grid_for((size_t)ncols * 32, 256), 256, 0, c.stream>>>(ncols, c.d_colPos[col].p, c.d_posNode.p, F, zeroGuess ? b : res,
+                                                                         x, zeroGuess);
   note_launch();
   TM_CUDA_CHECK(cudaGetLastError());
 }
 }  // namespace
 
 void launch_mf_sweep32(Context& c, int col, int zeroGuess, const float* b, float* x) {
-  mf_sweep<float>(c, col, zeroGuess, c.d_ccK32.p, c.d_gs32.p, c.d_os32.p, c.d_cd32.p, c.d_F32.p, b, x);
+  mf_sweep<float>(c, col, zeroGuess, c.d_ccK32.p, c.d_gs32.p, c.d_os32.p, c.d_cd32.p, c.d_F32.p, b, x, c.d_res0_32.p);
 }
 
 void launch_mf_sweep64(Context& c, int col, int zeroGuess, const double* b, double* x) {
-  mf_sweep<double>(c, col, zeroGuess, c.d_ccK.p, c.d_gs.p, c.d_os.p, c.d_cd.p, c.d_F.p, b, x);
+  mf_sweep<double>(c, col, zeroGuess, c.d_ccK.p, c.d_gs.p, c.d_os.p, c.d_cd.p, c.d_F.p, b, x, c.d_res0.p);
 }
 
 }  // namespace tmg

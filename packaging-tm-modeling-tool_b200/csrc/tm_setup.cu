@@ -931,6 +931,95 @@ __global__ void k_element_strains(int np, int ne, const int* __restrict__ elem, 
   o[0] = e0; o[1] = e1; o[2] = e2; o[3] = e3; o[4] = e4; o[5] = e5;
 }
 
+// the transpose of boxStrainAt (07-element.js:127-142), thread per point: gq[33 t ..] = B(nat)^T
+// g[6 t ..] with B the strain operator of k_element_strains (the derivative of a function of the
+// strains with respect to the element DOFs)
+__global__ void k_element_strains_adjoint(int np, int ne, const int* __restrict__ elem, const int* __restrict__ eClass,
+                                          const double* __restrict__ clsH, const double* __restrict__ nat, const double* __restrict__ g,
+                                          double* __restrict__ gq) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np) return;
+  double* o = gq + 33 * (size_t)t;
+  const int e = elem[t];
+  if (e < 0 || e >= ne) {
+    for (int r = 0; r < 33; r++) o[r] = CUDART_NAN;
+    return;
+  }
+  const int cls = eClass[e];
+  const double sx = 2 / clsH[3 * cls], sy = 2 / clsH[3 * cls + 1], sz = 2 / clsH[3 * cls + 2];
+  const double xi = nat[3 * (size_t)t], eta = nat[3 * (size_t)t + 1], zeta = nat[3 * (size_t)t + 2];
+  const double* gv = g + 6 * (size_t)t;
+  const double g0 = gv[0], g1 = gv[1], g2 = gv[2], g3 = gv[3], g4 = gv[4], g5 = gv[5];
+  for (int b = 0; b < 11; b++) {
+    double dx, dy, dz;
+    if (b < 8) {
+      const double xa = node_xi(b), ya = node_eta(b), za = node_zeta(b);
+      dx = xa * (1 + ya * eta) * (1 + za * zeta) * 0.125 * sx;
+      dy = ya * (1 + xa * xi) * (1 + za * zeta) * 0.125 * sy;
+      dz = za * (1 + xa * xi) * (1 + ya * eta) * 0.125 * sz;
+    } else {
+      dx = b == 8 ? -2 * xi * sx : 0;
+      dy = b == 9 ? -2 * eta * sy : 0;
+      dz = b == 10 ? -2 * zeta * sz : 0;
+    }
+    o[3 * b] = dx * g0 + dy * g3 + dz * g5;
+    o[3 * b + 1] = dy * g1 + dx * g3 + dz * g4;
+    o[3 * b + 2] = dz * g2 + dy * g4 + dx * g5;
+  }
+}
+
+// the transpose of one step of k_accumulate_q, warp per listed element: with the step's
+// q increment dq = (du_e, alpha), alpha = K_aa^-1 (f_a - K_au du_e), and gq (33) the derivative of
+// a function with respect to dq, gdu (24) = gq_u - K_au^T K_aa^-1 gq_a is its derivative with
+// respect to du_e, and gA = (K_aa^-1 gq_a)^T f_a its derivative with respect to the logarithm of the
+// thermal strain of the element's property set through alpha (alpha does not change when the set's
+// stiffness is scaled)
+__global__ void k_accumulate_q_adjoint(int nel, int ne, const int* __restrict__ elems, const int* __restrict__ eClass,
+                                       const int* __restrict__ clsPset, const double* __restrict__ clsH, const double* __restrict__ psetM,
+                                       const double* __restrict__ clsF33, const double* __restrict__ gq, double* __restrict__ gdu,
+                                       double* __restrict__ gA) {
+  __shared__ double sm[4][420];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * 4 + warp;
+  if (t >= nel) return;
+  double* Kr = sm[warp];               // 297
+  double* Kaa = Kr + 297;              // 81
+  double* w = Kaa + 81;                // 9
+  const int e = elems[t];
+  if (e < 0 || e >= ne) {
+    for (int o = lane; o < 24; o += 32) gdu[24 * (size_t)t + o] = CUDART_NAN;
+    if (lane == 0) gA[t] = CUDART_NAN;
+    return;
+  }
+  const int cls = eClass[e];
+  const double hx = clsH[3 * cls], hy = clsH[3 * cls + 1], hz = clsH[3 * cls + 2];
+  const double V8 = hx * hy * hz / 8;
+  const double c0 = V8 * 4 / (hx * hx), c1 = V8 * 4 / (hy * hy), c2 = V8 * 4 / (hz * hz);
+  const double c3 = V8 * 4 / (hx * hy), c4 = V8 * 4 / (hy * hz), c5 = V8 * 4 / (hz * hx);
+  const double* Ma = psetM + (size_t)clsPset[cls] * 6 * 1089 + 24 * 33;
+  for (int r = lane; r < 297; r += 32)
+    Kr[r] = c0 * Ma[r] + c1 * Ma[1089 + r] + c2 * Ma[2178 + r] + c3 * Ma[3267 + r] + c4 * Ma[4356 + r] + c5 * Ma[5445 + r];
+  if (lane < 9) w[lane] = gq[33 * (size_t)t + 24 + lane];
+  __syncwarp();
+  for (int o = lane; o < 81; o += 32) Kaa[o] = Kr[(o / 9) * 33 + 24 + o % 9];
+  __syncwarp();
+  if (lane == 0) {
+    chol_dense9(Kaa, 1e-14);
+    chol_solve9(Kaa, w);   // K_aa is symmetric: K_aa^-T gq_a = K_aa^-1 gq_a
+  }
+  __syncwarp();
+  if (lane < 24) {
+    double s = gq[33 * (size_t)t + lane];
+    for (int r = 0; r < 9; r++) s -= Kr[r * 33 + lane] * w[r];
+    gdu[24 * (size_t)t + lane] = s;
+  }
+  if (lane == 0) {
+    double a = 0;
+    for (int r = 0; r < 9; r++) a += w[r] * clsF33[(size_t)cls * 33 + 24 + r];
+    gA[t] = a;
+  }
+}
+
 // findInterval (01-util.js:12-22): i with a[i] <= x < a[i+1], clamped to [0, n-2]
 __device__ int find_interval(const double* __restrict__ a, int n, double x) {
   if (x <= a[0]) return 0;
@@ -1114,6 +1203,21 @@ void launch_accumulate_q(Context& c, const double* du, int nel, const int* elems
   note_launch();
   k_accumulate_q<<<(nel + 3) / 4, 128, 0, c.stream>>>(nel, c.ne, elems, c.d_conn.p, c.d_eClass.p, c.d_clsPset.p, c.d_clsH.p, c.d_psetM.p,
                                                       c.d_clsF33.p, du, q);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_element_strains_adjoint(Context& c, int np, const int* elem, const double* nat, const double* g, double* gq) {
+  if (np <= 0) return;
+  note_launch();
+  k_element_strains_adjoint<<<grid_for(np, 128), 128, 0, c.stream>>>(np, c.ne, elem, c.d_eClass.p, c.d_clsH.p, nat, g, gq);
+  TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void launch_accumulate_q_adjoint(Context& c, int nel, const int* elems, const double* gq, double* gdu, double* gA) {
+  if (nel <= 0) return;
+  note_launch();
+  k_accumulate_q_adjoint<<<(nel + 3) / 4, 128, 0, c.stream>>>(nel, c.ne, elems, c.d_eClass.p, c.d_clsPset.p, c.d_clsH.p, c.d_psetM.p,
+                                                               c.d_clsF33.p, gq, gdu, gA);
   TM_CUDA_CHECK(cudaGetLastError());
 }
 

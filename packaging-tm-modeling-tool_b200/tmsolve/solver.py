@@ -159,6 +159,39 @@ class DeviceModel:
                                         nat.ctypes.data_as(C.c_void_p), eps.ctypes.data_as(C.c_void_p)))
         return eps.reshape(-1, 6)
 
+    def element_strains_adjoint(self, elem, nat, g) -> np.ndarray:
+        """The transpose of element_strains: (npts, 33) B^T g for strain derivatives g (npts, 6)."""
+        elem = np.ascontiguousarray(elem, np.int32)
+        nat = np.ascontiguousarray(nat, np.float64).reshape(-1); g = np.ascontiguousarray(g, np.float64).reshape(-1)
+        if nat.size != 3 * len(elem) or g.size != 6 * len(elem):
+            raise ValueError("nat needs 3 and g 6 values per point")
+        gq = np.zeros(33 * len(elem))
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(load().tm_element_strains_adjoint(self.h, len(elem), vp(elem), vp(nat), vp(g), vp(gq)))
+        return gq.reshape(-1, 33)
+
+    def accumulate_q_adjoint(self, elems, gq):
+        """The transpose of one accumulate_q step (the step loaded last): (gdu (nel, 24), gA (nel,))."""
+        elems = np.ascontiguousarray(elems, np.int32)
+        gq = np.ascontiguousarray(gq, np.float64).reshape(-1)
+        if gq.size != 33 * len(elems):
+            raise ValueError("gq needs 33 values per element")
+        gdu = np.zeros(24 * len(elems)); gA = np.zeros(len(elems))
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(load().tm_accumulate_q_adjoint(self.h, len(elems), vp(elems), vp(gq), vp(gdu), vp(gA)))
+        return gdu.reshape(-1, 24), gA
+
+    def adjoint_sensitivity(self, g, u, tol=1e-12, maxit=2000, precond="mg") -> dict:
+        """For the step assembled last and its solution u: lambda = K^-1 g and per property set the
+        derivatives through u with respect to log stiffness (dlogE) and log thermal strain (dlogA)."""
+        g = np.ascontiguousarray(g, np.float64); u = np.ascontiguousarray(u, np.float64)
+        dE = np.zeros(self.pkg.npset); dA = np.zeros(self.pkg.npset)
+        info = TmSolveInfo()
+        o = self.make_opts(tol, maxit, 0, precond, "fp64", -1)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(load().tm_adjoint_sensitivity(self.h, vp(g), vp(u), C.byref(o), vp(dE), vp(dA), C.byref(info)), allow_not_converged=True)
+        return dict(dlogE=dE, dlogA=dA, adjoint=self.record(info, "adjoint", precond))
+
     def set_sublayers(self, step: StepData):
         """The step's sub-layers of the layered property sets, for the stress histories (call
         after prepare_step / assemble_step of that step)."""
