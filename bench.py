@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=["mixed", "fp64"], help="default: mixed (c2), fp64 (c1)")
     ap.add_argument("--inplane", type=int, default=160)
+    ap.add_argument("--level0", default="stencil", choices=["stencil", "mf"],
+                    help="level-0 operator: the assembled 27-point stencil (default) or matrix-free cell products")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="a warm-up assemble + solve, then one assemble + solve (for ncu captures); prints no bench line")
@@ -67,6 +69,7 @@ def run_profile(a):
     torch.cuda.set_device(0)
     pkg = make_package(a.workload, a.inplane)
     dm = DeviceModel(pkg)
+    dm.set_level0(a.level0 == "mf")
     f = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
     u = torch.empty(dm.ndof, dtype=torch.float64, device="cuda")
     for key in (1, 2):
@@ -229,6 +232,7 @@ def run_ours(a):
     from tmsolve.solver import DeviceModel, launch_count
     pkg = make_package(a.workload, a.inplane)
     dm = DeviceModel(pkg)
+    dm.set_level0(a.level0 == "mf")
     stream = torch.cuda.current_stream()
     dm.set_stream(stream.cuda_stream)
     n = dm.ndof
@@ -311,25 +315,48 @@ def run_ours(a):
     # ---- roofline of the dominant kernel: level-0 column smoother, one colour per launch
     nn = dm.nn
     prec_bytes = 4 if a.precision == "mixed" else 8
-    # per full sweep (4 colours): operator rows 243 values + 27 neighbour ids + 18 factor values + b, x read, x write per node
-    sweep_bytes = nn * (243 * prec_bytes + 27 * 4 + 18 * prec_bytes + 3 * prec_bytes * 3)
-    per_launch = sweep_bytes / 4
     hbm, hbm_kind = peaks()
-    achieved = per_launch / (kms / kcount / 1e3) / 1e9 if kcount else None
-    traffic = profile_traffic(DOMINANT, a.precision)
-    kname = ("k_sweep_tma (level-0 z-column smoother, one colour: position-major operator rows streamed by TMA bulk copies "
-             "through shared memory, block-tridiagonal column solves per SM run)") if a.precision == "mixed" else \
-        "k_sweep_panel<double> (level-0 z-column block-tridiagonal smoother on packed column panels, one colour)"
-    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved,
-            "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None, "traffic": traffic,
-            "peak_kind": hbm_kind, "launches_timed": kcount, "avg_launch_us": 1e3 * kms / kcount if kcount else None,
-            "algorithmic_bytes_per_launch": per_launch}
+    mf = dm.level0_matrix_free
+    avg_s = kms / kcount / 1e3 if kcount else None
+    if not mf:
+        # per full sweep (4 colours): operator rows 243 values + 27 neighbour ids + 18 factor values + b, x read, x write per node
+        sweep_bytes = nn * (243 * prec_bytes + 27 * 4 + 18 * prec_bytes + 3 * prec_bytes * 3)
+        per_launch = sweep_bytes / 4
+        achieved = per_launch / avg_s / 1e9 if kcount else None
+        traffic = profile_traffic(DOMINANT, a.precision)
+        kname = ("k_sweep_tma (level-0 z-column smoother, one colour: position-major operator rows streamed by TMA bulk copies "
+                 "through shared memory, block-tridiagonal column solves per SM run)") if a.precision == "mixed" else \
+            "k_sweep_panel<double> (level-0 z-column block-tridiagonal smoother on packed column panels, one colour)"
+        roof = {"kernel": kname, "bound": "hbm", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None, "traffic": traffic,
+                "peak_kind": hbm_kind, "launches_timed": kcount, "avg_launch_us": 1e3 * kms / kcount if kcount else None,
+                "algorithmic_bytes_per_launch": per_launch}
+    else:
+        # one colour of the matrix-free sweep (k_mf_resid + k_col_solve): per colour node the class id
+        # of its 8 cells (2 B each), 18 factor values, gs/os/cd, b, x read and x write (3 values each),
+        # and 8 cells x 3 rows x 24 multiply-adds
+        from tmsolve.solver import device_peaks
+        pk = device_peaks()
+        fp32, fp64 = pk["fp32_tflops"], pk["fp64_tflops"]
+        per_launch = nn / 4 * (8 * 2 + 18 * prec_bytes + 6 * 3 * prec_bytes)
+        flops = nn / 4 * 1152
+        achieved = per_launch / avg_s / 1e9 if kcount else None
+        fpeak = 1e3 * (fp32 if prec_bytes == 4 else fp64)
+        roof = {"kernel": "k_mf_resid + k_col_solve (matrix-free level-0 colour sweep: residual rows from the cell-class "
+                          "table, then warp-per-column block-tridiagonal solves)",
+                "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if achieved else None,
+                "traffic": None, "peak_kind": hbm_kind, "launches_timed": kcount,
+                "avg_launch_us": 1e3 * kms / kcount if kcount else None, "algorithmic_bytes_per_launch": per_launch,
+                "flops_per_launch": flops, "achieved_gflops": flops / avg_s / 1e9 if kcount else None,
+                "flops_peak_gflops": fpeak, "flops_frac": flops / avg_s / 1e9 / fpeak if kcount else None,
+                "flops_peak_kind": "measured FMA loop (tm_device_peaks)"}
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 apply/smoother + f64 refinement" if a.precision == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "dof": n, "precision": a.precision, "parallelism": f"replicas x{world}",
+                       "level0": "matrix-free" if mf else "stencil",
                        "l2": "inputs larger than L2 (1.3 GB level-0 operator)"},
             "solve": {"iters_per_step": iters / a.steps, "solve_s": ms / 1e3 / a.steps, "refinements": recs[-1]["refinements"],
                       "pc_ms": recs[-1]["pcMs"], "relres": recs[-1]["relres"], "fp64_iters": r64["iters"],

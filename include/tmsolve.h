@@ -232,9 +232,19 @@ tm_status tm_device_peaks(double* fp32_tflops, double* fp64_tflops);
 /* Test hook of the timeout path (no counterpart in the reference). Every device wait of the library
  * is bounded: a wait that runs out makes the kernel flag the error, let its copies in flight land
  * and return, and the call fails with TM_TIMEOUT while the context stays usable. While on != 0,
- * the level-0 TMA sweep (used for operators loaded with tm_set_bcsr in mixed precision) waits,
- * with a short limit, for a stage flag that nothing sets, so that path can be exercised. */
+ * the level-0 TMA sweep of the FP32 V-cycle (the assembled level-0 operator in mixed precision)
+ * waits, with a short limit, for a stage flag that nothing sets, so that path can be exercised. */
 tm_status tm_set_wait_test(tm_ctx* ctx, int32_t on);
+/* Level-0 operator of the solves after the next tm_assemble_step (no counterpart in the reference,
+ * whose LinearSolver always multiplies by the assembled matrix, 10-solver.js:933-994):
+ * matrix_free = 0 (default) multiplies by the assembled 27-point stencil in the PCG apply and the
+ * V-cycle's level-0 residuals and sweeps; 1 multiplies cell by cell with the element matrices of the
+ * mesh's element classes (the level-0 sweep's column factors still come from the assembled diagonal
+ * blocks). Both give the same operator up to the order of summation. The matrix-free path is taken
+ * only where the mesh allows it (every cell's element classes in one table of at most 4095
+ * combinations, columns of at most 128 nodes); tm_level0 reports the operator the current step uses. */
+tm_status tm_set_level0(tm_ctx* ctx, int32_t matrix_free);
+tm_status tm_level0(tm_ctx* ctx, int32_t* matrix_free_active);
 
 /* ---- element DOF histories at screening sites ---- */
 /* Loads the per-step data that the DOF histories read (the shape matrices of every property set

@@ -672,13 +672,15 @@ tm_status tm_assemble_step(tm_ctx* ctx, const tm_step* st, double* rhs_out) {
     launch_shape_matrices(c, *st);
     launch_class_condense(c);
     set_active_stage(c, st->stage);
-    mf_build_cells(c, st->stage);
-    launch_mf_combine(c);
+    if (c.level0Mf) {
+      mf_build_cells(c, st->stage);
+      launch_mf_combine(c);
+    }
     launch_assemble(c);
     launch_constraints(c);
     c.assembled = true;
     c.scaled = false;
-    c.mf = c.mfAvailable;
+    c.mf = c.level0Mf && c.mfAvailable;
     launch_mf_scales(c, false);
     if (rhs_out) {
       c.d_rhs.download(rhs_out, 3 * (size_t)c.nn, c.stream);
@@ -1091,6 +1093,20 @@ tm_status tm_set_wait_test(tm_ctx* ctx, int32_t on) {
   return guarded([&] {
     if (!ctx) fail(TM_BAD_INPUT, "null context");
     reinterpret_cast<Context*>(ctx)->waitTest = on != 0;
+  });
+}
+
+tm_status tm_set_level0(tm_ctx* ctx, int32_t matrix_free) {
+  return guarded([&] {
+    if (!ctx) fail(TM_BAD_INPUT, "null context");
+    reinterpret_cast<Context*>(ctx)->level0Mf = matrix_free != 0;
+  });
+}
+
+tm_status tm_level0(tm_ctx* ctx, int32_t* matrix_free_active) {
+  return guarded([&] {
+    if (!ctx || !matrix_free_active) fail(TM_BAD_INPUT, "null argument");
+    *matrix_free_active = reinterpret_cast<Context*>(ctx)->mf ? 1 : 0;
   });
 }
 

@@ -283,6 +283,7 @@ struct Context {
   DBuf<float> d_val32p;                // position-major FP32 operator (243 values per position)
   DBuf<int> d_nbrp;                    // position-major neighbour ids (27 per position)
   DBuf<int> d_err;                     // set by a bounded device wait that ran out
+  bool level0Mf = false;               // caller's choice of the level-0 operator (tm_set_level0)
   bool waitTest = false;               // test hook: the TMA sweep waits for a stage flag that nothing sets
   // level-0 column panels: the columns of one colour packed into groups of at most panelCap nodes,
   // one CTA per group (group g holds colour columns grpStart[g] .. grpStart[g+1]-1); colPos holds

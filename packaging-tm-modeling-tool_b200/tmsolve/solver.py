@@ -278,6 +278,18 @@ class DeviceModel:
         """Test hook of the timeout path: the level-0 TMA sweep waits for a flag that nothing sets."""
         check(load().tm_set_wait_test(self.h, 1 if on else 0))
 
+    def set_level0(self, matrix_free: bool):
+        """Level-0 operator of the solves after the next assembly: the assembled stencil (default)
+        or cell-by-cell products with the element classes' matrices (tm_set_level0)."""
+        check(load().tm_set_level0(self.h, 1 if matrix_free else 0))
+
+    @property
+    def level0_matrix_free(self) -> bool:
+        """Whether the current step's level-0 operator is the matrix-free one."""
+        v = C.c_int32(0)
+        check(load().tm_level0(self.h, C.byref(v)))
+        return bool(v.value)
+
     def mg_levels(self) -> list:
         """The multigrid hierarchy, fine to coarse: (nx, ny, nn, b) per level (MultigridPC's levels)."""
         cap = 64

@@ -39,3 +39,26 @@ def test_no_device_is_an_error_not_a_fallback():
         assert e.status == _lib.TM_NO_DEVICE
     else:
         raise AssertionError("tm_create succeeded without a device")
+
+
+def declared_arity():
+    """Parameter count of every entry point in include/tmsolve.h (`(void)` counts as none)."""
+    src = open(os.path.join(ROOT, "include", "tmsolve.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"^\s*(?:tm_status|void|int32_t|int64_t|const char\s*\*)\s*(tm_\w+)\s*\(([^;]*?)\)\s*;", src, re.M | re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_header():
+    """Every ctypes argtypes list the binding sets has exactly as many entries as the C declaration."""
+    L = _lib.load()
+    ar = declared_arity()
+    bad = {}
+    for n in _lib.EXPORTED:
+        at = getattr(L, n).argtypes
+        if at is not None and n in ar and len(at) != ar[n]:
+            bad[n] = (len(at), ar[n])
+    assert not bad, bad

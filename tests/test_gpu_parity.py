@@ -259,29 +259,38 @@ def test_warm_start_matches_oracle(oracle_lib):
 
 def test_bench_workload_parity(oracle_lib):
     """The benchmark workload itself (lidded C2 160x160x32, 2,065,539 DOF) on the GPU in FP64 and in
-    mixed precision against the oracle's FP64 solve, all to relative residual 1e-13 (the lid on its
-    0.01 GPa TIM makes the operator ill-conditioned enough that two solutions at relres 1e-12 differ
-    by 2e-8): displacements within 1e-8 (FP64) and 1e-5 (mixed), RMS and signed JEITA warpage within
-    1e-8 and 1e-6."""
+    mixed precision against the oracle's FP64 solve, all to relative residual 1e-13.
+
+    Each GPU solution solves the oracle's own assembled system: its residual under the oracle's
+    operator is within 1e-12 of the load (measured 5.6e-13). Displacements within 1e-8 (FP64; measured
+    7e-11) and 1e-5 (mixed), RMS and signed JEITA warpage within 1e-8 and 1e-6. The lid on its 0.01
+    GPa TIM next to silicon and copper makes this operator ill-conditioned: an operator summed in
+    another order (the matrix-free level 0, tm_set_level0) moves the FP64 solution by about 2e-8
+    however far the residual is driven, which is why the default assembled path is the one pinned
+    here to 1e-8."""
     from tmsolve import post
     from tmsolve.solver import DeviceModel
     pkg = lidded_c2()
     om = oracle_lib.OracleModel(pkg)
     step = pkg.step()
-    ro = om.solve(om.assemble(step), tol=1e-13)
+    fo = om.assemble(step)
+    ro = om.solve(fo, tol=1e-13)
     assert ro["converged"]
     uo = ro["u"]
     b = post.bga_sites(**pkg.meta["bga"])
     z = b["zone"]
     wo = om.warpage_jeita(uo, b["x"], b["y"], [z["x0"], z["x1"], z["y0"], z["y1"]])
     rms_o = rms_warpage(pkg.mesh, uo)
-    del om
+    om.assemble(step)   # the solve scales the oracle's values in place: assemble the operator again
     dm = DeviceModel(pkg)
     for key, (precision, bar_u, bar_w) in enumerate((("fp64", 1e-8, 1e-8), ("mixed", 1e-5, 1e-6))):
         r = dm.solve(dm.assemble_step(step), tol=1e-13, warm=0, key=key, precision=precision)
         assert r["converged"], precision
         u = r["u"]
+        res = np.linalg.norm(fo - om.matvec(u)) / np.linalg.norm(fo)
         du = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+        print(f"{precision}: relres under the oracle's operator {res:.2e}, displacement difference {du:.2e}")
+        assert res <= 1e-12, (precision, res)
         assert du <= bar_u, (precision, du)
         assert abs(rms_warpage(pkg.mesh, u) / rms_o - 1) <= bar_w, precision
         w = post.warpage_jeita(b, lambda x, y: dm.sample_plane(u, 0, 2, x, y))
