@@ -47,11 +47,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="a warm-up assemble + solve, then one assemble + solve (for ncu captures); prints no bench line")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "screen", "c3"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "screen", "c3", "tornado", "c4"],
                     help="c2: the lidded 160x160x32 solve (the headline); c1: the plain FP64 FCBGA 48x48x20 solve; "
                          "screen: Anand screening of the 17,424 bumps of a die over three -40/125 degC cycles; "
                          "c3: the stacked-module thermal-cycle analysis (module stage, process chain, cycling branches, "
-                         "bump strain tables, Anand screening at 40 load steps per cycle), about 1.2M DOF")
+                         "bump strain tables, Anand screening at 40 load steps per cycle), about 1.2M DOF; "
+                         "tornado: the 24 perturbed-material cases of the c2 package in one warm-started solve loop; "
+                         "c4: 64 bump submodels of 20^3-48^3 voxels in one batch over the first history points of a "
+                         "40-step -40/125 degC cycle")
+    ap.add_argument("--c4-cells", type=int, default=64, help="c4: submodels in the batch")
+    ap.add_argument("--c4-points", type=int, default=6, help="c4: history points of the timed sample")
+    ap.add_argument("--c4-precond", default="line", choices=["line", "ic"], help="c4: inner-solve preconditioner")
     ap.add_argument("--sites", type=int, default=17424, help="screen: bump sites")
     a = ap.parse_args()
     a.precision_default = a.precision is None
@@ -544,8 +550,152 @@ def run_c3(a):
         "clocks": ck.summary()}))
 
 
+TORNADO_METRIC = "tornado batch: base + 24 perturbed-material solves of lidded C2 (matE x6, matCTE x6 at -/+10 %), signed JEITA warpage per case"
+
+
+def run_tornado(a):
+    """One batch = the base case and the 24 cases of tornado_cases() on the c2 package, each assembled,
+    solved to tol 1e-8 from the previous case's solution (warm start) and its JEITA warpage sampled
+    (host API, end to end). The same loop with every case started from zero, as the reference's
+    tornado runs its cases, is timed once beside it."""
+    import torch
+    from tmsolve.packages import lidded_c2
+    from tmsolve.sensitivity import tornado, tornado_cases
+    from tmsolve.solver import DeviceModel
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pkg = lidded_c2(a.inplane)
+    cases = tornado_cases()
+    dm = DeviceModel(pkg)
+    dm.set_level0(a.level0 == "mf")
+    for w in range(a.warmup):
+        dm.clear_warm()
+        tornado(dm, cases, precision=a.precision, key=1000 * (w + 1))
+    torch.cuda.synchronize()
+    runs = []
+    with Clocks(local) as ck:
+        for q in range(a.steps):
+            dm.clear_warm()
+            t0 = time.perf_counter()
+            res = tornado(dm, cases, precision=a.precision, key=100000 * (q + 1))
+            torch.cuda.synchronize()
+            runs.append((time.perf_counter() - t0, res))
+    secs = sum(t for t, _ in runs) / a.steps
+    res = runs[-1][1]
+    # the reference's way: every case from zero (no stored solutions), the same loop otherwise
+    dm.clear_warm()
+    t0 = time.perf_counter()
+    fresh = tornado(dm, cases, precision=a.precision, key=10000000, warm=0)
+    torch.cuda.synchronize()
+    cold = time.perf_counter() - t0
+    cold_iters = sum(c["iters"] for c in [fresh["base"]] + fresh["cases"])
+    iters = sum(c["iters"] for c in [res["base"]] + res["cases"])
+    n = dm.ndof
+    print(json.dumps({
+        "metric": TORNADO_METRIC, "value": secs, "unit": "s per 25-solve batch", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * secs, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 apply/smoother + f64 refinement" if a.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"lidded_c2 {a.inplane}x{a.inplane}x32 ({n} DOF), base + 24 cases, tol 1e-8", "dof": n,
+                   "precision": a.precision, "l2": "inputs larger than L2"},
+        "batch": {"pcg_iters": iters, "rebuilds": sum(c["rebuilt"] for c in [res["base"]] + res["cases"]),
+                  "mdof_iter_per_s": n * iters / 1e6 / secs, "base_signed_warpage_mm": res["base"]["signed"],
+                  "largest_swing": max(res["swing"], key=lambda s: s["span"])},
+        "cases_from_zero": {"s": cold, "pcg_iters": cold_iters, "speedup_of_warm_batch": cold / secs},
+        "e2e": {"value": secs, "unit": "s per 25-solve batch", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "clocks": ck.summary()}))
+
+
+C4_METRIC = "batched bump submodels (BumpSubmodel.run: B-bar voxels, Anand solder, Newton with PCG inner solves, adaptive sub-steps)"
+
+
+def c4_specs(n, seed=20261203):
+    """n bump cells with k x k x k voxels, k ~ U{20..48}, at sites spread over a 20 mm die (the
+    joints away from the centre see more shear)."""
+    import numpy as np
+    from tmsolve.submodel import synthetic_spec
+    rng = np.random.default_rng(seed)
+    ks = rng.integers(20, 49, n)
+    xy = rng.uniform(-10.0, 10.0, (n, 2))
+    specs = []
+    for q in range(n):
+        r = float(np.hypot(*xy[q]))
+        specs.append(synthetic_spec(nxy=int(ks[q]), nz=int(ks[q]), site=(float(xy[q, 0]), float(xy[q, 1])), shear=2e-6 * r,
+                                    seed=seed + q))
+    return specs, ks, xy
+
+
+def run_c4(a):
+    """The batch of --c4-cells submodels over the first --c4-points points of the 40-step cycle
+    history (cycle_history with 10 degC ramp steps and 3 dwell steps), timed end to end through
+    tm_submodel_run_batch. The unit of work is one voxel element through one accepted sub-step;
+    the CPU baseline is the oracle's BumpSubmodel on one core for the smallest cell over the same
+    points."""
+    import numpy as np
+    import torch
+    from tmsolve.anand import cycle_history
+    from tmsolve.submodel import DeviceSubmodel, run_batch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    specs, ks, xy = c4_specs(a.c4_cells)
+    full = cycle_history(-40.0, 125.0, 11.0, 15.0, 1, ramp_max_dt=10.0, dwell_steps=3)
+    P = min(a.c4_points + 1, len(full["t"]))
+    hist = dict(t=full["t"][:P], T=full["T"][:P], cycle=full["cycle"][:P], phase=full["phase"][:P], cycles=1)
+    ang = np.arctan2(xy[:, 1], xy[:, 0])
+    cph, sph = np.cos(ang), np.sin(ang)
+
+    def batch():
+        models = [DeviceSubmodel(sp) for sp in specs]
+        for m in models:
+            m.set_precond(a.c4_precond)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        recs = run_batch(models, hist, cph, sph)
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        ne = np.array([m.ne for m in models])
+        for m in models:
+            m.close()
+        return secs, recs, ne
+    for _ in range(a.warmup):
+        batch()
+    with Clocks(local) as ck:
+        runs = [batch() for _ in range(a.steps)]
+    secs = sum(r[0] for r in runs) / a.steps
+    _, recs, ne = runs[-1]
+    steps = np.array([r["steps"] for r in recs])
+    work = float((ne * steps).sum())
+    cpu = None
+    if not a.no_cpu_baseline:
+        import oracle.oracle as orc
+        q = int(np.argmin(ks))
+        t0 = time.perf_counter()
+        ro = orc.OracleSubmodel(specs[q]).run(hist, float(cph[q]), float(sph[q]))
+        cs = time.perf_counter() - t0
+        cpu = {"value": int(ne[q]) * ro["steps"] / cs, "unit": "voxel-element sub-steps/s", "cores": 1, "kind": "port",
+               "sample": f"the oracle's BumpSubmodel run of the smallest cell ({int(ks[q])}^3, {int(ne[q])} elements) over the same "
+                         f"{P} history points on one core: {int(ro['steps'])} sub-steps in {cs:.1f} s"}
+    print(json.dumps({
+        "metric": C4_METRIC, "value": work / secs, "unit": "voxel-element sub-steps/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * secs, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(specs)} bump cells k^3 voxels, k ~ U{{20..48}} (seed 20261203, {int(ne.sum())} elements), "
+                               f"first {P} points of a 40-step -40/125 degC cycle, {a.c4_precond} inner preconditioner",
+                   "cells": len(specs), "elements": int(ne.sum()), "history_points": P, "precond": a.c4_precond,
+                   "l2": "working set larger than L2"},
+        "batch": {"s": secs, "substeps": int(steps.sum()), "max_substeps": int(steps.max()),
+                  "newton_per_step_mean": float(np.mean([r["newtonPerStep"] for r in recs])),
+                  "cutbacks": int(sum(r["cutbacks"] for r in recs))},
+        "e2e": {"value": work / secs, "unit": "voxel-element sub-steps/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "cpu_baseline": cpu, "clocks": ck.summary()}))
+
+
 def main():
     a = parse()
+    if a.workload == "c4":
+        run_c4(a)
+        return
+    if a.workload == "tornado":
+        run_tornado(a)
+        return
     if a.workload == "screen":
         run_screen(a)
         return

@@ -244,6 +244,9 @@ tm_status tm_set_wait_test(tm_ctx* ctx, int32_t on);
  * only where the mesh allows it (every cell's element classes in one table of at most 4095
  * combinations, columns of at most 128 nodes); tm_level0 reports the operator the current step uses. */
 tm_status tm_set_level0(tm_ctx* ctx, int32_t matrix_free);
+/* Drops the stored solutions of the warm start (a new LinearSolver's empty _warm list,
+ * 10-solver.js:885-926): the next solve starts from zero. */
+tm_status tm_clear_warm(tm_ctx* ctx);
 tm_status tm_level0(tm_ctx* ctx, int32_t* matrix_free_active);
 
 /* ---- element DOF histories at screening sites ---- */
@@ -480,6 +483,16 @@ typedef struct {
 } tm_submodel_spec;
 typedef struct tm_sub tm_sub;
 tm_status tm_submodel_create(const tm_submodel_spec* spec, tm_sub** out);
+/* Preconditioner of the Newton steps' inner PCG solves: TM_SUB_PC_IC, the reference's IC(0)
+ * (_solve, 13-fatigue.js:886-917; the default), or TM_SUB_PC_LINE, a z-line block Jacobi (the
+ * cell's node columns' 3x3-block tridiagonal parts factored exactly; one launch per apply, where
+ * IC(0) runs one launch per level set). The inner solves stop at the same relative residual
+ * either way, so the Newton iterates agree to that tolerance. */
+#define TM_SUB_PC_IC 0
+#define TM_SUB_PC_LINE 1
+tm_status tm_submodel_set_precond(tm_sub* sm, int32_t kind);
+/* Work counters of the submodel so far: inner solves, and their PCG iterations summed. */
+tm_status tm_submodel_counters(tm_sub* sm, int64_t* out2);
 tm_status tm_submodel_destroy(tm_sub* sm);
 /* nn, ne, boundary nodes, solder Gauss points */
 tm_status tm_submodel_sizes(tm_sub* sm, int64_t* out4);
@@ -508,8 +521,11 @@ tm_status tm_submodel_stress_snapshot(tm_sub* sm, double T, float* out);
 
 /* n submodels over the same history at once (the screened sites of a die): out10, perCycle
  * and loop hold n consecutive records; status[i] is each run's status (TM_OK or the failure),
- * and the call returns the first failure. Runs the submodels concurrently from host threads,
- * each on its own stream. */
+ * and the call returns the first failure. The submodels advance together in groups of up to 64:
+ * each phase of their Newton steps (boundary, assembly and gathers, norms, the inner solves'
+ * products, reductions and preconditioner, commits) is one launch over every submodel in that
+ * phase, while each keeps its own sub-steps, cutbacks and Newton iterations; a submodel's result
+ * equals its tm_submodel_run result with the same preconditioner. */
 tm_status tm_submodel_run_batch(int32_t n, tm_sub* const* subs, int32_t nsteps, const double* t, const double* T,
                                 const int32_t* cycle, int32_t cycles, const double* cphi, const double* sphi, double* out10,
                                 double* perCycle, double* loop, int32_t* status);

@@ -230,18 +230,25 @@ void warm_start(Context& c, const double* fs, double* x) {
   const int m = (int)c.basis.size();
   TM_CUDA_CHECK(cudaMemsetAsync(x, 0, n * sizeof(double), c.stream));
   if (!m) return;
-  std::vector<DBuf<double>> KV(m);
+  if (c.d_warmKV.n < (size_t)m * n) c.d_warmKV.alloc((size_t)m * n);
+  std::vector<const double*> V(m), W(m + 1);
   for (int i = 0; i < m; i++) {
-    KV[i].alloc(n);
+    double* kv = c.d_warmKV.p + (size_t)i * n;
     launch_scale_vec(c, c.basis[i]->p, c.d_s.p, c.d_tmp.p, true, n);
     launch_apply0(c, c.d_tmp.p, c.d_tmp2.p, nullptr);
-    launch_scale_vec(c, c.d_tmp2.p, c.d_s.p, KV[i].p, true, n);
+    launch_scale_vec(c, c.d_tmp2.p, c.d_s.p, kv, true, n);
+    V[i] = c.basis[i]->p;
+    W[i] = kv;
   }
-  std::vector<double> A((size_t)m * m), b(m), cc;
   launch_scale_vec(c, fs, c.d_s.p, c.d_tmp.p, true, n);
+  W[m] = c.d_tmp.p;
+  // A[i][j] = v_i . K v_j and b[i] = v_i . f: one batched launch, every dot independent as in the
+  // reference's loops
+  std::vector<double> AB((size_t)m * (m + 1)), A((size_t)m * m), b(m), cc;
+  multi_dot_host(c, V, W, n, AB.data());
   for (int i = 0; i < m; i++) {
-    b[i] = dot_host(c, c.basis[i]->p, c.d_tmp.p, n);
-    for (int j = 0; j < m; j++) A[i * m + j] = dot_host(c, c.basis[i]->p, KV[j].p, n);
+    for (int j = 0; j < m; j++) A[i * m + j] = AB[(size_t)i * (m + 1) + j];
+    b[i] = AB[(size_t)i * (m + 1) + m];
   }
   for (int i = 0; i < m; i++)
     for (int j = i + 1; j < m; j++) { const double v = 0.5 * (A[i * m + j] + A[j * m + i]); A[i * m + j] = A[j * m + i] = v; }
@@ -1096,6 +1103,16 @@ tm_status tm_set_wait_test(tm_ctx* ctx, int32_t on) {
   });
 }
 
+tm_status tm_clear_warm(tm_ctx* ctx) {
+  return guarded([&] {
+    if (!ctx) fail(TM_BAD_INPUT, "null context");
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    for (auto* b : c.basis) delete b;
+    c.basis.clear();
+  });
+}
+
 tm_status tm_set_level0(tm_ctx* ctx, int32_t matrix_free) {
   return guarded([&] {
     if (!ctx) fail(TM_BAD_INPUT, "null context");
@@ -1416,6 +1433,20 @@ tm_status tm_submodel_create(const tm_submodel_spec* spec, tm_sub** out) {
   });
 }
 
+tm_status tm_submodel_set_precond(tm_sub* sm, int32_t kind) {
+  return guarded([&] {
+    if (!sm) fail(TM_BAD_INPUT, "null argument");
+    submodel_set_precond(*reinterpret_cast<SubModel*>(sm), kind);
+  });
+}
+
+tm_status tm_submodel_counters(tm_sub* sm, int64_t* out2) {
+  return guarded([&] {
+    if (!sm || !out2) fail(TM_BAD_INPUT, "null argument");
+    submodel_counters(*reinterpret_cast<SubModel*>(sm), out2);
+  });
+}
+
 tm_status tm_submodel_destroy(tm_sub* sm) {
   return guarded([&] { submodel_destroy(reinterpret_cast<SubModel*>(sm)); });
 }
@@ -1446,33 +1477,22 @@ tm_status tm_submodel_get(tm_sub* sm, double* u, double* W, double* ebar) {
   });
 }
 
-// independent submodels (the sites of one die) run concurrently: one host thread per submodel
-// (up to the hardware threads), each on its submodel's own stream, so the GPU overlaps their
-// latency-bound Newton and PCG chains
+// independent submodels (the sites of one die) over one history: the batched engine advances them
+// together, every phase one launch over all of them
 tm_status tm_submodel_run_batch(int32_t n, tm_sub* const* subs, int32_t nsteps, const double* t, const double* T, const int32_t* cycle,
                                 int32_t cycles, const double* cphi, const double* sphi, double* out10, double* perCycle, double* loop,
                                 int32_t* status) {
   return guarded([&] {
     if (n < 0 || (n > 0 && (!subs || !t || !T || !cycle || !cphi || !sphi || !out10 || !perCycle || !loop || !status)))
       fail(TM_BAD_INPUT, "null argument");
-    int dev = 0;
-    TM_CUDA_CHECK(cudaGetDevice(&dev));
-    std::atomic<int> next(0);
-    auto worker = [&] {
-      cudaSetDevice(dev);
-      for (int i = next++; i < n; i = next++) {
-        const tm_status st = guarded([&] {
-          if (!subs[i]) fail(TM_BAD_INPUT, "null submodel");
-          submodel_run(*reinterpret_cast<SubModel*>(subs[i]), nsteps, t, T, cycle, cycles, cphi[i], sphi[i], out10 + 10 * (size_t)i,
-                       perCycle + 2 * (size_t)cycles * i, loop + 4 * (size_t)nsteps * i);
-        });
-        status[i] = st;
-      }
-    };
-    const int nth = std::max(1, std::min<int>(n, (int)std::max(1u, std::thread::hardware_concurrency())));
-    std::vector<std::thread> pool;
-    for (int q = 0; q < nth; q++) pool.emplace_back(worker);
-    for (auto& th : pool) th.join();
+    std::vector<SubModel*> v(n);
+    for (int i = 0; i < n; i++) {
+      if (!subs[i]) fail(TM_BAD_INPUT, "null submodel");
+      for (int j = 0; j < i; j++)
+        if (subs[j] == subs[i]) fail(TM_BAD_INPUT, "a submodel appears twice in the batch");
+      v[i] = reinterpret_cast<SubModel*>(subs[i]);
+    }
+    submodel_run_batch(v, nsteps, t, T, cycle, cycles, cphi, sphi, out10, perCycle, loop, status);
     for (int i = 0; i < n; i++)
       if (status[i] != TM_OK) fail((tm_status)status[i], "submodel " + std::to_string(i) + " of the batch failed");
   });

@@ -262,6 +262,8 @@ struct Context {
   // solver state
   DBuf<double> d_s, d_f, d_uio, d_bs, d_x, d_r, d_z, d_p, d_q, d_tmp, d_tmp2;
   DBuf<double> d_partial, d_scalars;
+  DBuf<uintptr_t> d_mdPtr;             // vector tables of the batched dot products
+  DBuf<double> d_mdPart, d_warmKV;     // their partial sums; K times the warm-start basis
   DBuf<int> d_jitter;
   // level 0 smoother and transfer
   DBuf<double> d_F;                    // 18 per node (column block-tridiagonal factors)
@@ -390,6 +392,9 @@ struct TimedLaunch {   // brackets one launch with events when the context times
 void launch_apply0(Context& c, const double* x, double* y, const double* b);   // y = K x, or b - K x when b != nullptr
 void launch_apply0_f32(Context& c, const double* x, double* y, const double* b);
 void launch_dot(Context& c, const double* a, const double* b, size_t n, double* out_dev);
+// every dot a_i . b_j (n entries) into out[i * b.size() + j] on the host: one launch pair and one
+// synchronization per 512 pairs
+void multi_dot_host(Context& c, const std::vector<const double*>& a, const std::vector<const double*>& b, size_t n, double* out);
 void launch_axpy2(Context& c, const double* alpha_dev, const double* p, double* x, const double* q, double* r, size_t n);
 void launch_xpby(Context& c, const double* z, const double* beta_dev, double* p, size_t n);
 void launch_zero_constrained(Context& c, double* v);
@@ -447,5 +452,9 @@ void submodel_run(SubModel& s, int nsteps, const double* t, const double* T, con
                   double* out, double* perCycle, double* loop, const int* phase = nullptr, int maxSnaps = 0, int* nSnaps = nullptr,
                   double* snapMeta = nullptr, float* snapSig = nullptr);
 void submodel_stress_snapshot(SubModel& s, double T, float* out);
+void submodel_set_precond(SubModel& s, int kind);
+void submodel_counters(SubModel& s, int64_t* out);
+void submodel_run_batch(const std::vector<SubModel*>& subs, int nsteps, const double* t, const double* T, const int* cycle, int cycles,
+                        const double* cphi, const double* sphi, double* out10, double* perCycle, double* loop, int32_t* status);
 
 }  // namespace tmg

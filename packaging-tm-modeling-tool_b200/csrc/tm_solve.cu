@@ -154,6 +154,58 @@ __global__ void k_reduce_final(int np, const double* __restrict__ partial, doubl
   if (threadIdx.x == 0) *out = s;
 }
 
+// all dots a_i . b_j of ma vectors a and mb vectors b (n entries each): each CTA walks chunks of
+// MD_CHUNK entries (chunk c, c + grid, ...), stages the chunk of every vector in shared memory and
+// adds the chunk's products to its threads' pairs (a thread starts its pair's row at its own
+// offset, so the threads of a warp read different banks); partial[cta * np + p] then holds the
+// CTA's sum of pair p = i * mb + j, and k_multi_dot_final adds the CTAs in order.
+constexpr int MD_CHUNK = 128;
+constexpr int MD_THREADS = 256;
+constexpr int MD_MAXP = 2 * MD_THREADS;   // pairs per launch (two per thread)
+constexpr int MD_MAXV = 200;              // vectors staged per launch (1 KB of shared memory each)
+__global__ void __launch_bounds__(MD_THREADS) k_multi_dot_partial(size_t n, int ma, const double* const* __restrict__ A, int mb,
+                                                                  const double* const* __restrict__ B, double* __restrict__ partial) {
+  extern __shared__ double sh[];
+  const int nv = ma + mb, np = ma * mb;
+  double acc[2] = {0, 0};
+  const size_t nchunks = (n + MD_CHUNK - 1) / MD_CHUNK;
+  for (size_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const size_t r0 = ch * MD_CHUNK;
+    const int len = (int)min((size_t)MD_CHUNK, n - r0);
+    for (int e = threadIdx.x; e < nv * MD_CHUNK; e += MD_THREADS) {
+      const int v = e / MD_CHUNK, t = e % MD_CHUNK;
+      const double* src = v < ma ? A[v] : B[v - ma];
+      sh[e] = t < len ? src[r0 + t] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int p = threadIdx.x + u * MD_THREADS;
+      if (p >= np) continue;
+      const double* a = sh + (p / mb) * MD_CHUNK;
+      const double* b = sh + (ma + p % mb) * MD_CHUNK;
+      double s = 0;
+      for (int t = 0; t < MD_CHUNK; t++) {
+        const int q = (t + threadIdx.x) & (MD_CHUNK - 1);
+        s += a[q] * b[q];
+      }
+      acc[u] += s;
+    }
+    __syncthreads();
+  }
+  for (int u = 0; u < 2; u++) {
+    const int p = threadIdx.x + u * MD_THREADS;
+    if (p < np) partial[(size_t)blockIdx.x * np + p] = acc[u];
+  }
+}
+__global__ void k_multi_dot_final(int nblk, int np, const double* __restrict__ partial, double* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  double s = 0;
+  for (int b = 0; b < nblk; b++) s += partial[(size_t)b * np + p];
+  out[p] = s;
+}
+
 // x += alpha p ; r -= alpha q ; partial sums of r.r
 template <class T>
 __global__ void k_axpy2(size_t n, const double* __restrict__ alpha, const T* __restrict__ p, T* __restrict__ x, const T* __restrict__ q,
@@ -783,6 +835,37 @@ void launch_dot(Context& c, const double* a, const double* b, size_t n, double* 
   k_reduce_final<<<1, 1024, 0, c.stream>>>(RED_BLOCKS, c.d_partial.p, out_dev);
   note_launch(2);
   TM_CUDA_CHECK(cudaGetLastError());
+}
+
+void multi_dot_host(Context& c, const std::vector<const double*>& a, const std::vector<const double*>& b, size_t n, double* out) {
+  const int ma = (int)a.size(), mb = (int)b.size(), np = ma * mb;
+  if (!np) return;
+  // a launch holds at most MD_MAXP pairs and MD_MAXV staged vectors (MD_MAXV KB of shared memory)
+  if (mb > MD_MAXV / 2) fail(TM_BAD_INPUT, "too many vectors for one batched dot launch");
+  const int rows = std::min(MD_MAXP / mb, MD_MAXV - mb);
+  if (ma > rows) {   // rows of a in groups that fit one launch
+    for (int i0 = 0; i0 < ma; i0 += rows) {
+      const std::vector<const double*> part(a.begin() + i0, a.begin() + std::min(ma, i0 + rows));
+      multi_dot_host(c, part, b, n, out + (size_t)i0 * mb);
+    }
+    return;
+  }
+  std::vector<const double*> ptr(a);
+  ptr.insert(ptr.end(), b.begin(), b.end());
+  if (c.d_mdPtr.n < (size_t)MD_MAXV) c.d_mdPtr.alloc(MD_MAXV);
+  TM_CUDA_CHECK(cudaMemcpyAsync(c.d_mdPtr.p, ptr.data(), ptr.size() * sizeof(uintptr_t), cudaMemcpyHostToDevice, c.stream));
+  const int blocks = RED_BLOCKS / 2;
+  c.d_mdPart.alloc((size_t)blocks * MD_MAXP + MD_MAXP);
+  const double* const* P = reinterpret_cast<const double* const*>(c.d_mdPtr.p);
+  const size_t smem = (size_t)(ma + mb) * MD_CHUNK * sizeof(double);
+  if (smem > 48 * 1024) TM_CUDA_CHECK(cudaFuncSetAttribute(k_multi_dot_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  double* fin = c.d_mdPart.p + (size_t)blocks * MD_MAXP;
+  k_multi_dot_partial<<<blocks, MD_THREADS, smem, c.stream>>>(n, ma, P, mb, P + ma, c.d_mdPart.p);
+  k_multi_dot_final<<<grid_for(np, 128), 128, 0, c.stream>>>(blocks, np, c.d_mdPart.p, fin);
+  note_launch(2);
+  TM_CUDA_CHECK(cudaGetLastError());
+  TM_CUDA_CHECK(cudaMemcpyAsync(out, fin, np * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
 }
 
 void launch_dot32(Context& c, const float* a, const float* b, size_t n, double* out_dev) {

@@ -169,12 +169,11 @@ void bbar_matrix(double hx, double hy, double hz, double xi, double eta, double 
 // ---- device kernels ------------------------------------------------------------------------------
 constexpr unsigned FULLMASK = 0xffffffffu;
 
-// prescribe: thread per boundary node, fieldAt blended between global temperatures i and i+1
-__global__ void k_sub_prescribe(int nb, const int* __restrict__ bNodes, const int* __restrict__ bGlob, const double* __restrict__ bW,
-                                const double* __restrict__ fa, const double* __restrict__ fb, double t, const double* __restrict__ u25,
-                                double* __restrict__ u) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nb) return;
+// prescribe: boundary node q, fieldAt blended between global temperatures i and i+1
+__device__ __forceinline__ void sub_prescribe_node(int q, const int* __restrict__ bNodes, const int* __restrict__ bGlob,
+                                                   const double* __restrict__ bW, const double* __restrict__ fa,
+                                                   const double* __restrict__ fb, double t, const double* __restrict__ u25,
+                                                   double* __restrict__ u) {
   double ux = 0, uy = 0, uz = 0;
   for (int c = 0; c < 8; c++) {
     const int gn = bGlob[8 * q + c];
@@ -186,27 +185,32 @@ __global__ void k_sub_prescribe(int nb, const int* __restrict__ bNodes, const in
   const int n = bNodes[q];
   u[3 * n] = ux; u[3 * n + 1] = uy; u[3 * n + 2] = uz;
 }
+__global__ void k_sub_prescribe(int nb, const int* __restrict__ bNodes, const int* __restrict__ bGlob, const double* __restrict__ bW,
+                                const double* __restrict__ fa, const double* __restrict__ fb, double t, const double* __restrict__ u25,
+                                double* __restrict__ u) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < nb) sub_prescribe_node(q, bNodes, bGlob, bW, fa, fb, t, u25, u);
+}
 
-// assemble, warp per element: elastic elements build K_e, f_th once per step (fresh) and give
+// the per-warp shared work space of the element assembly
+struct AsmSmem {
+  double K[576], DB[144], Sig[48], D[288], Ue[24];
+};
+
+// assemble element e by one warp: elastic elements build K_e, f_th once per step (fresh) and give
 // f_e = f_n + K_e (u_e - u_n,e) - f_th; solder elements step their 8 Anand points (one lane each)
 // and sum f_e and, with wantK, K_e = sum_g w B^T D_g B
-__global__ void __launch_bounds__(32 * SA_WARPS)
-k_sub_assemble(int ne, const int* __restrict__ conn, const int* __restrict__ eMat, const int* __restrict__ eBb, const double* __restrict__ Bm,
-               const double* __restrict__ Bw, const int* __restrict__ eAn, Point* __restrict__ pts, const double* __restrict__ u,
-               const double* __restrict__ uN, const double* __restrict__ eFn, double* __restrict__ eK, double* __restrict__ eF,
-               double* __restrict__ fe, double* __restrict__ dmaxE, const double* __restrict__ elas, int fresh, int wantK, AnandConst P,
-               StepK kc, double fSolder) {
-  __shared__ double sK[SA_WARPS][576];
-  __shared__ double sDB[SA_WARPS][144];
-  __shared__ double sSig[SA_WARPS][48];
-  __shared__ double sD[SA_WARPS][288];
-  __shared__ double sUe[SA_WARPS][24];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int e = blockIdx.x * SA_WARPS + w;
-  if (e >= ne) return;
-  double* K = sK[w];
-  double* DB = sDB[w];
-  double* ue = sUe[w];
+__device__ __forceinline__ void sub_assemble_element(int e, int lane, AsmSmem& sm, const int* __restrict__ conn,
+                                                     const int* __restrict__ eMat, const int* __restrict__ eBb,
+                                                     const double* __restrict__ Bm, const double* __restrict__ Bw,
+                                                     const int* __restrict__ eAn, Point* __restrict__ pts, const double* __restrict__ u,
+                                                     const double* __restrict__ uN, const double* __restrict__ eFn,
+                                                     double* __restrict__ eK, double* __restrict__ eF, double* __restrict__ fe,
+                                                     double* __restrict__ dmaxE, const double* __restrict__ elas, int fresh, int wantK,
+                                                     const AnandConst& P, const StepK& kc, double fSolder) {
+  double* K = sm.K;
+  double* DB = sm.DB;
+  double* ue = sm.Ue;
   const double* B = Bm + (size_t)eBb[e] * 8 * 144;
   const double wt = Bw[eBb[e]];
   const int an = eAn[e];
@@ -272,7 +276,7 @@ k_sub_assemble(int ne, const int* __restrict__ conn, const int* __restrict__ eMa
       eps[r] = s;
     }
     eps[0] -= fSolder; eps[1] -= fSolder; eps[2] -= fSolder;
-    d = anand_step(P, pts[8 * (size_t)an + lane], eps, kc, sSig[w] + 6 * lane, sD[w] + 36 * lane, wantK != 0);
+    d = anand_step(P, pts[8 * (size_t)an + lane], eps, kc, sm.Sig + 6 * lane, sm.D + 36 * lane, wantK != 0);
   }
   for (int off = 16; off > 0; off >>= 1) d = fmax(d, __shfl_xor_sync(FULLMASK, d, off));
   if (lane == 0) dmaxE[e] = d;
@@ -281,7 +285,7 @@ k_sub_assemble(int ne, const int* __restrict__ conn, const int* __restrict__ eMa
     double f = 0;
     for (int g = 0; g < 8; g++) {
       const double* Bb = B + 144 * g;
-      const double* sig = sSig[w] + 6 * g;
+      const double* sig = sm.Sig + 6 * g;
       double s = 0;
       for (int r = 0; r < 6; r++) s += Bb[r * 24 + lane] * sig[r];
       f += wt * s;
@@ -293,7 +297,7 @@ k_sub_assemble(int ne, const int* __restrict__ conn, const int* __restrict__ eMa
   __syncwarp();
   for (int g = 0; g < 8; g++) {
     const double* Bb = B + 144 * g;
-    const double* Dg = sD[w] + 36 * g;
+    const double* Dg = sm.D + 36 * g;
     for (int o = lane; o < 144; o += 32) {
       const int r = o / 24, c = o % 24;
       double s = 0;
@@ -316,14 +320,25 @@ k_sub_assemble(int ne, const int* __restrict__ conn, const int* __restrict__ eMa
     Ke[o] = b < a ? K[b * 24 + a] : K[o];
   }
 }
+__global__ void __launch_bounds__(32 * SA_WARPS)
+k_sub_assemble(int ne, const int* __restrict__ conn, const int* __restrict__ eMat, const int* __restrict__ eBb, const double* __restrict__ Bm,
+               const double* __restrict__ Bw, const int* __restrict__ eAn, Point* __restrict__ pts, const double* __restrict__ u,
+               const double* __restrict__ uN, const double* __restrict__ eFn, double* __restrict__ eK, double* __restrict__ eF,
+               double* __restrict__ fe, double* __restrict__ dmaxE, const double* __restrict__ elas, int fresh, int wantK, AnandConst P,
+               StepK kc, double fSolder) {
+  __shared__ AsmSmem sm[SA_WARPS];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * SA_WARPS + w;
+  if (e >= ne) return;
+  sub_assemble_element(e, lane, sm[w], conn, eMat, eBb, Bm, Bw, eAn, pts, u, uN, eFn, eK, eF, fe, dmaxE, elas, fresh, wantK, P, kc, fSolder);
+}
 
 // the tangent's blocks, thread per block: the element contributions in element order, then the
 // constrained rows and columns zeroed off the diagonal (_constrain)
-__global__ void k_sub_gather_val(int nb, const int* __restrict__ blkRow, const int* __restrict__ col, const int* __restrict__ start,
-                                 const int* __restrict__ list, const double* __restrict__ eK, const uint8_t* __restrict__ isC,
-                                 double* __restrict__ val) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nb) return;
+__device__ __forceinline__ void sub_gather_val_block(int k, const int* __restrict__ blkRow, const int* __restrict__ col,
+                                                     const int* __restrict__ start, const int* __restrict__ list,
+                                                     const double* __restrict__ eK, const uint8_t* __restrict__ isC,
+                                                     double* __restrict__ val) {
   const int i = blkRow[k], j = col[k];
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int l = start[k]; l < start[k + 1]; l++) {
@@ -339,12 +354,16 @@ __global__ void k_sub_gather_val(int nb, const int* __restrict__ blkRow, const i
       val[9 * (size_t)k + 3 * p + q] = v[3 * p + q];
     }
 }
+__global__ void k_sub_gather_val(int nb, const int* __restrict__ blkRow, const int* __restrict__ col, const int* __restrict__ start,
+                                 const int* __restrict__ list, const double* __restrict__ eK, const uint8_t* __restrict__ isC,
+                                 double* __restrict__ val) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nb) sub_gather_val_block(k, blkRow, col, start, list, eK, isC, val);
+}
 
 // internal force, thread per DOF: the element forces in element order
-__global__ void k_sub_gather_rint(int ndof, const int* __restrict__ start, const int* __restrict__ list, const double* __restrict__ fe,
-                                  double* __restrict__ rint) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= ndof) return;
+__device__ __forceinline__ void sub_gather_rint_dof(int q, const int* __restrict__ start, const int* __restrict__ list,
+                                                    const double* __restrict__ fe, double* __restrict__ rint) {
   const int n = q / 3, p = q % 3;
   double s = 0;
   for (int l = start[n]; l < start[n + 1]; l++) {
@@ -353,16 +372,21 @@ __global__ void k_sub_gather_rint(int ndof, const int* __restrict__ start, const
   }
   rint[q] = s;
 }
+__global__ void k_sub_gather_rint(int ndof, const int* __restrict__ start, const int* __restrict__ list, const double* __restrict__ fe,
+                                  double* __restrict__ rint) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < ndof) sub_gather_rint_dof(q, start, list, fe, rint);
+}
 
 // deterministic sums over one block: out[0..m) = sums of m products (pairs of arrays, or with a mask)
 // kind 0: a.a over the free DOFs, a.a over all (the Newton residual norms)
 // kind 1: a.b
 // kind 2: after u += du on the free DOFs: du.du over the free DOFs, u.u over all
-__global__ void __launch_bounds__(1024) k_sub_sums(int n, int kind, const double* __restrict__ a, double* __restrict__ b,
-                                                   const uint8_t* __restrict__ isC, double* __restrict__ out) {
-  __shared__ double s0[1024], s1[1024];
+constexpr int SUMS_THREADS = 1024;
+__device__ __forceinline__ void sub_block_sums(int n, int kind, const double* __restrict__ a, double* __restrict__ b,
+                                               const uint8_t* __restrict__ isC, double* __restrict__ out, double* s0, double* s1) {
   double x0 = 0, x1 = 0;
-  for (int q = threadIdx.x; q < n; q += 1024) {
+  for (int q = threadIdx.x; q < n; q += SUMS_THREADS) {
     if (kind == 0) {
       const double v = a[q];
       if (!isC[q]) x0 += v * v;
@@ -376,42 +400,56 @@ __global__ void __launch_bounds__(1024) k_sub_sums(int n, int kind, const double
   }
   s0[threadIdx.x] = x0; s1[threadIdx.x] = x1;
   __syncthreads();
-  for (int h = 512; h > 0; h >>= 1) {
+  for (int h = SUMS_THREADS / 2; h > 0; h >>= 1) {
     if ((int)threadIdx.x < h) { s0[threadIdx.x] += s0[threadIdx.x + h]; s1[threadIdx.x] += s1[threadIdx.x + h]; }
     __syncthreads();
   }
   if (threadIdx.x == 0) { out[0] = s0[0]; out[1] = s1[0]; }
 }
+__global__ void __launch_bounds__(SUMS_THREADS) k_sub_sums(int n, int kind, const double* __restrict__ a, double* __restrict__ b,
+                                                           const uint8_t* __restrict__ isC, double* __restrict__ out) {
+  __shared__ double s0[SUMS_THREADS], s1[SUMS_THREADS];
+  sub_block_sums(n, kind, a, b, isC, out, s0, s1);
+}
 
 // _solve's scaling: s from the tangent's diagonal, the scaled copy, b = rhs s with rhs = -rint
 // on the free DOFs
-__global__ void k_sub_scale_s(int nn, const int* __restrict__ diag, const double* __restrict__ val, double* __restrict__ s) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nn) return;
+__device__ __forceinline__ void sub_scale_s_node(int i, const int* __restrict__ diag, const double* __restrict__ val,
+                                                 double* __restrict__ s) {
   const double* v = val + 9 * (size_t)diag[i];
   s[3 * i] = 1 / sqrt(fmax(v[0], 1e-300)); s[3 * i + 1] = 1 / sqrt(fmax(v[4], 1e-300)); s[3 * i + 2] = 1 / sqrt(fmax(v[8], 1e-300));
 }
-__global__ void k_sub_scale_vals(int nb, const int* __restrict__ blkRow, const int* __restrict__ col, const double* __restrict__ s,
-                                 const double* __restrict__ val, double* __restrict__ vals) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nb) return;
+__global__ void k_sub_scale_s(int nn, const int* __restrict__ diag, const double* __restrict__ val, double* __restrict__ s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nn) sub_scale_s_node(i, diag, val, s);
+}
+__device__ __forceinline__ void sub_scale_vals_block(int k, const int* __restrict__ blkRow, const int* __restrict__ col,
+                                                     const double* __restrict__ s, const double* __restrict__ val,
+                                                     double* __restrict__ vals) {
   const int i = blkRow[k], j = col[k];
   for (int p = 0; p < 3; p++)
     for (int q = 0; q < 3; q++) vals[9 * (size_t)k + 3 * p + q] = val[9 * (size_t)k + 3 * p + q] * (s[3 * i + p] * s[3 * j + q]);
 }
-__global__ void k_sub_rhs(int n, const double* __restrict__ rint, const uint8_t* __restrict__ isC, const double* __restrict__ s,
-                          double* __restrict__ b, double* __restrict__ r, double* __restrict__ x) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
+__global__ void k_sub_scale_vals(int nb, const int* __restrict__ blkRow, const int* __restrict__ col, const double* __restrict__ s,
+                                 const double* __restrict__ val, double* __restrict__ vals) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nb) sub_scale_vals_block(k, blkRow, col, s, val, vals);
+}
+__device__ __forceinline__ void sub_rhs_dof(int q, const double* __restrict__ rint, const uint8_t* __restrict__ isC,
+                                            const double* __restrict__ s, double* __restrict__ b, double* __restrict__ r,
+                                            double* __restrict__ x) {
   const double rhs = isC[q] ? 0 : -rint[q];
   const double v = rhs * s[q];
   b[q] = v; r[q] = v; x[q] = 0;
 }
-// fullMatVec (09-assembly.js:151-165), thread per node
-__global__ void k_sub_spmv(int nn, const int* __restrict__ rowPtr, const int* __restrict__ col, const double* __restrict__ val,
-                           const double* __restrict__ x, double* __restrict__ y) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nn) return;
+__global__ void k_sub_rhs(int n, const double* __restrict__ rint, const uint8_t* __restrict__ isC, const double* __restrict__ s,
+                          double* __restrict__ b, double* __restrict__ r, double* __restrict__ x) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) sub_rhs_dof(q, rint, isC, s, b, r, x);
+}
+// fullMatVec (09-assembly.js:151-165), node i
+__device__ __forceinline__ void sub_spmv_node(int i, const int* __restrict__ rowPtr, const int* __restrict__ col,
+                                              const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y) {
   double y0 = 0, y1 = 0, y2 = 0;
   for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
     const int j = col[k];
@@ -423,43 +461,143 @@ __global__ void k_sub_spmv(int nn, const int* __restrict__ rowPtr, const int* __
   }
   y[3 * i] = y0; y[3 * i + 1] = y1; y[3 * i + 2] = y2;
 }
+__global__ void k_sub_spmv(int nn, const int* __restrict__ rowPtr, const int* __restrict__ col, const double* __restrict__ val,
+                           const double* __restrict__ x, double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nn) sub_spmv_node(i, rowPtr, col, val, x, y);
+}
 // the PCG updates with their scalars read on the device: alpha = rz / (p.q), beta = rz2 / rz
+__device__ __forceinline__ void sub_axpy2_dof(int i, double rz, double pq, const double* __restrict__ p, const double* __restrict__ q,
+                                              double* __restrict__ x, double* __restrict__ r) {
+  const double alpha = rz / pq;
+  x[i] += alpha * p[i];
+  r[i] += -alpha * q[i];
+}
 __global__ void k_sub_axpy2(int n, const double* __restrict__ rz, const double* __restrict__ pq, const double* __restrict__ p,
                             const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double alpha = *rz / *pq;
-  x[i] += alpha * p[i];
-  r[i] += -alpha * q[i];
+  if (i < n) sub_axpy2_dof(i, *rz, *pq, p, q, x, r);
+}
+__device__ __forceinline__ void sub_xpby_dof(int i, double rz2, double rz, const double* __restrict__ z, double* __restrict__ p) {
+  const double beta = rz2 / rz;
+  p[i] = z[i] + beta * p[i];
 }
 __global__ void k_sub_xpby(int n, const double* __restrict__ z, const double* __restrict__ rz2, const double* __restrict__ rz,
                            double* __restrict__ p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double beta = *rz2 / *rz;
-  p[i] = z[i] + beta * p[i];
+  if (i < n) sub_xpby_dof(i, *rz2, *rz, z, p);
 }
+// ---- z-line block-Jacobi preconditioner of the scaled tangent --------------------------------------
+// The cell's nodes (i ny + j) nz + k form columns of nz consecutive ids. Per column the 3x3-block
+// tridiagonal part of the scaled tangent (diagonal blocks and the couplings to the node below) is
+// factored as L L^T, L block lower bidiagonal, and applied by a forward and a backward block
+// substitution; all columns are independent, so one thread takes one column and one launch applies
+// the whole preconditioner (an SPD block-Jacobi splitting: a valid PCG preconditioner). Per node
+// 15 values: 1/l00, 1/l11, l10, 1/l22, l20, l21 of the diagonal factor, then the 3x3 coupling
+// L_{k,k-1} row-major. A pivot that is not positive (the scaled tangent's diagonal is 1) is taken
+// as 1e-12, so the factor exists for any tangent.
+constexpr int LF_VALS = 15;
+constexpr double LF_PIVOT_MIN = 1e-12;
+
+__device__ __forceinline__ void sub_line_factor_column(int c, int nz, const int* __restrict__ diag, const int* __restrict__ subBlk,
+                                                       const double* __restrict__ vals, double* __restrict__ lf) {
+  double L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // previous node's diagonal factor (lower, row-major)
+  for (int k = 0; k < nz; k++) {
+    const int n = c * nz + k;
+    const double* A = vals + 9 * (size_t)diag[n];
+    double a00 = A[0], a10 = A[3], a11 = A[4], a20 = A[6], a21 = A[7], a22 = A[8];
+    double X[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (k > 0) {
+      // X = C L_prev^-T: each row x of X solves L_prev x^T = c^T for the row c of C = A_{k,k-1}
+      const double* Cb = vals + 9 * (size_t)subBlk[n];
+      for (int r = 0; r < 3; r++) {
+        const double c0 = Cb[3 * r], c1 = Cb[3 * r + 1], c2 = Cb[3 * r + 2];
+        const double x0 = c0 / L[0];
+        const double x1 = (c1 - L[3] * x0) / L[4];
+        const double x2 = (c2 - L[6] * x0 - L[7] * x1) / L[8];
+        X[3 * r] = x0; X[3 * r + 1] = x1; X[3 * r + 2] = x2;
+      }
+      a00 -= X[0] * X[0] + X[1] * X[1] + X[2] * X[2];
+      a10 -= X[3] * X[0] + X[4] * X[1] + X[5] * X[2];
+      a11 -= X[3] * X[3] + X[4] * X[4] + X[5] * X[5];
+      a20 -= X[6] * X[0] + X[7] * X[1] + X[8] * X[2];
+      a21 -= X[6] * X[3] + X[7] * X[4] + X[8] * X[5];
+      a22 -= X[6] * X[6] + X[7] * X[7] + X[8] * X[8];
+    }
+    const double l00 = sqrt(fmax(a00, LF_PIVOT_MIN));
+    const double l10 = a10 / l00, l20 = a20 / l00;
+    const double l11 = sqrt(fmax(a11 - l10 * l10, LF_PIVOT_MIN));
+    const double l21 = (a21 - l20 * l10) / l11;
+    const double l22 = sqrt(fmax(a22 - l20 * l20 - l21 * l21, LF_PIVOT_MIN));
+    double* f = lf + LF_VALS * (size_t)n;
+    f[0] = 1 / l00; f[1] = 1 / l11; f[2] = l10; f[3] = 1 / l22; f[4] = l20; f[5] = l21;
+    for (int q = 0; q < 9; q++) f[6 + q] = X[q];
+    L[0] = l00; L[3] = l10; L[4] = l11; L[6] = l20; L[7] = l21; L[8] = l22;
+  }
+}
+
+// z = M^-1 r on one column: y = L^-1 r downwards, z = L^-T y upwards
+__device__ __forceinline__ void sub_line_apply_column(int c, int nz, const double* __restrict__ lf, const double* __restrict__ r,
+                                                      double* __restrict__ z) {
+  double y0 = 0, y1 = 0, y2 = 0;
+  for (int k = 0; k < nz; k++) {
+    const size_t n = (size_t)c * nz + k;
+    const double* f = lf + LF_VALS * n;
+    double b0 = r[3 * n], b1 = r[3 * n + 1], b2 = r[3 * n + 2];
+    if (k > 0) {
+      b0 -= f[6] * y0 + f[7] * y1 + f[8] * y2;
+      b1 -= f[9] * y0 + f[10] * y1 + f[11] * y2;
+      b2 -= f[12] * y0 + f[13] * y1 + f[14] * y2;
+    }
+    y0 = b0 * f[0];
+    y1 = (b1 - f[2] * y0) * f[1];
+    y2 = (b2 - f[4] * y0 - f[5] * y1) * f[3];
+    z[3 * n] = y0; z[3 * n + 1] = y1; z[3 * n + 2] = y2;
+  }
+  double t0 = 0, t1 = 0, t2 = 0;   // L_{k+1,k}^T z_{k+1}
+  for (int k = nz - 1; k >= 0; k--) {
+    const size_t n = (size_t)c * nz + k;
+    const double* f = lf + LF_VALS * n;
+    const double b0 = z[3 * n] - t0, b1 = z[3 * n + 1] - t1, b2 = z[3 * n + 2] - t2;
+    const double z2 = b2 * f[3];
+    const double z1 = (b1 - f[5] * z2) * f[1];
+    const double z0 = (b0 - f[2] * z1 - f[4] * z2) * f[0];
+    z[3 * n] = z0; z[3 * n + 1] = z1; z[3 * n + 2] = z2;
+    t0 = f[6] * z0 + f[9] * z1 + f[12] * z2;
+    t1 = f[7] * z0 + f[10] * z1 + f[13] * z2;
+    t2 = f[8] * z0 + f[11] * z1 + f[14] * z2;
+  }
+}
+__global__ void k_sub_line_factor(int ncol, int nz, const int* __restrict__ diag, const int* __restrict__ subBlk,
+                                  const double* __restrict__ vals, double* __restrict__ lf) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncol) sub_line_factor_column(c, nz, diag, subBlk, vals, lf);
+}
+__global__ void k_sub_line_apply(int ncol, int nz, const double* __restrict__ lf, const double* __restrict__ r, double* __restrict__ z) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncol) sub_line_apply_column(c, nz, lf, r, z);
+}
+
 __global__ void k_sub_mul(int n, const double* __restrict__ s, double* __restrict__ x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] *= s[i];
 }
 
 // _commitElastic, warp per elastic element: Gauss-point stresses and the element's internal force
-__global__ void __launch_bounds__(32 * SA_WARPS)
-k_sub_commit_elastic(int ne, const int* __restrict__ conn, const int* __restrict__ eMat, const int* __restrict__ eBb,
-                     const double* __restrict__ Bm, const double* __restrict__ Bw, const int* __restrict__ eAn, const double* __restrict__ u,
-                     const double* __restrict__ uN, const double* __restrict__ elas, double* __restrict__ sigE, double* __restrict__ eFn) {
-  __shared__ double sDue[SA_WARPS][24];
-  __shared__ double sSg[SA_WARPS][6];
-  __shared__ double sDe[SA_WARPS][6];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int e = blockIdx.x * SA_WARPS + w;
-  if (e >= ne || eAn[e] >= 0) return;
+struct CommitSmem {
+  double Due[24], Sg[6], De[6];
+};
+__device__ __forceinline__ void sub_commit_elastic_element(int e, int lane, CommitSmem& sm, const int* __restrict__ conn,
+                                                           const int* __restrict__ eMat, const int* __restrict__ eBb,
+                                                           const double* __restrict__ Bm, const double* __restrict__ Bw,
+                                                           const double* __restrict__ u, const double* __restrict__ uN,
+                                                           const double* __restrict__ elas, double* __restrict__ sigE,
+                                                           double* __restrict__ eFn) {
   const double* D = elas + 42 * eMat[e];
   const double* sth = D + 36;
   const double* B = Bm + (size_t)eBb[e] * 8 * 144;
   const double wt = Bw[eBb[e]];
-  double* due = sDue[w];
+  double* due = sm.Due;
   if (lane < 24) {
     const size_t n = 3 * (size_t)conn[8 * (size_t)e + lane / 3] + lane % 3;
     due[lane] = u[n] - uN[n];
@@ -472,24 +610,34 @@ k_sub_commit_elastic(int ne, const int* __restrict__ conn, const int* __restrict
     if (lane < 6) {
       double s2 = 0;
       for (int c = 0; c < 24; c++) s2 += Bb[lane * 24 + c] * due[c];
-      sDe[w][lane] = s2;
+      sm.De[lane] = s2;
     }
     __syncwarp();
     if (lane < 6) {
       double s2 = -sth[lane];
-      for (int c = 0; c < 6; c++) s2 += D[lane * 6 + c] * sDe[w][c];
+      for (int c = 0; c < 6; c++) s2 += D[lane * 6 + c] * sm.De[c];
       so[lane] += s2;
-      sSg[w][lane] = so[lane];
+      sm.Sg[lane] = so[lane];
     }
     __syncwarp();
     if (lane < 24) {
       double s2 = 0;
-      for (int r = 0; r < 6; r++) s2 += Bb[r * 24 + lane] * sSg[w][r];
+      for (int r = 0; r < 6; r++) s2 += Bb[r * 24 + lane] * sm.Sg[r];
       fn += wt * s2;
     }
     __syncwarp();
   }
   if (lane < 24) eFn[24 * (size_t)e + lane] = fn;
+}
+__global__ void __launch_bounds__(32 * SA_WARPS)
+k_sub_commit_elastic(int ne, const int* __restrict__ conn, const int* __restrict__ eMat, const int* __restrict__ eBb,
+                     const double* __restrict__ Bm, const double* __restrict__ Bw, const int* __restrict__ eAn, const double* __restrict__ u,
+                     const double* __restrict__ uN, const double* __restrict__ elas, double* __restrict__ sigE, double* __restrict__ eFn) {
+  __shared__ CommitSmem sm[SA_WARPS];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * SA_WARPS + w;
+  if (e >= ne || eAn[e] >= 0) return;
+  sub_commit_elastic_element(e, lane, sm[w], conn, eMat, eBb, Bm, Bw, u, uN, elas, sigE, eFn);
 }
 
 __global__ void k_sub_commit_points(int np, Point* __restrict__ pts) {
@@ -638,6 +786,11 @@ struct SubModel {
   IcFactor ic;
   bool pcBuilt = false, pcStale = false;
   int pcIters = 0;
+  // preconditioner of the inner solves: IC(0) as the reference, or the z-line block Jacobi
+  int precond = TM_SUB_PC_IC;
+  long long pcgSolves = 0, pcgIters = 0;   // inner solves and their PCG iterations so far
+  DBuf<int> d_subBlk;                   // per node the block (n, n-1) of its column (-1 at the bottom)
+  DBuf<double> d_lf;                    // z-line factors (LF_VALS per node)
   double Tn = 25;
   bool haveKey = false;
   double keyTn = 0, keyT = 0;
@@ -720,7 +873,8 @@ struct SubModel {
     grid_stress_increment(subD.data(), subF.data(), Ta, Tb, sth);
   }
 
-  void prescribe(double T) {
+  // fieldAt's two global temperatures around T and the blend between them
+  void prescribe_args(double T, const double** fa, const double** fb, double* tOut) const {
     int i;
     const int n = (int)ts.size();
     if (T <= ts[0]) i = 0;
@@ -733,21 +887,36 @@ struct SubModel {
     double t = (T - ts[i]) / (ts[i + 1] - ts[i]);
     t = t < 0 ? 0 : (t > 1 ? 1 : t);
     const size_t G = 3 * (size_t)nglob;
+    *fa = d_fields.p + G * i;
+    *fb = d_fields.p + G * (i + 1);
+    *tOut = t;
+  }
+  void prescribe(double T) {
+    const double *fa, *fb;
+    double t;
+    prescribe_args(T, &fa, &fb, &t);
     note_launch();
-    k_sub_prescribe<<<blocks_for(nbnd, 128), 128, 0, st>>>(nbnd, d_bNodes.p, d_bGlob.p, d_bW.p, d_fields.p + G * i, d_fields.p + G * (i + 1), t,
-                                                          d_u25.p, d_u.p);
+    k_sub_prescribe<<<blocks_for(nbnd, 128), 128, 0, st>>>(nbnd, d_bNodes.p, d_bGlob.p, d_bW.p, fa, fb, t, d_u25.p, d_u.p);
     TM_CUDA_CHECK(cudaGetLastError());
   }
 
-  // assemble (13-fatigue.js:776-853); returns the largest plastic increment
-  double assemble(double T, double dt, bool wantK) {
-    const bool fresh = !(haveKey && keyTn == Tn && keyT == T);
-    if (fresh) upload_records(T);
-    // the solder constants of the step and its thermal strain from 25 degC
+  // the solder's step constants at T over dt and its thermal strain from 25 degC
+  void step_params(double T, double dt, StepK* kc, double* fSolder) const {
     const double E = grid_at_s(solderE.data(), T, 1, 0), nu = P.nu;
     const double expQ = std::exp(P.QR / (T + 273.15));
-    const StepK kc{E / (2 * (1 + nu)), E / (3 * (1 - 2 * nu)), expQ, dt * P.A / expQ, dt};
-    const double fSolder = grid_at_s(solderF.data(), T, 1, 0) - grid_at_s(solderF.data(), 25, 1, 0);
+    *kc = StepK{E / (2 * (1 + nu)), E / (3 * (1 - 2 * nu)), expQ, dt * P.A / expQ, dt};
+    *fSolder = grid_at_s(solderF.data(), T, 1, 0) - grid_at_s(solderF.data(), 25, 1, 0);
+  }
+  // whether the step from Tn to T needs its element matrices and material records built
+  bool fresh_for(double T) const { return !(haveKey && keyTn == Tn && keyT == T); }
+
+  // assemble (13-fatigue.js:776-853); returns the largest plastic increment
+  double assemble(double T, double dt, bool wantK) {
+    const bool fresh = fresh_for(T);
+    if (fresh) upload_records(T);
+    StepK kc;
+    double fSolder;
+    step_params(T, dt, &kc, &fSolder);
     note_launch(wantK ? 3 : 2);
     k_sub_assemble<<<blocks_for(ne, SA_WARPS), 32 * SA_WARPS, 0, st>>>(ne, d_conn.p, d_eMat.p, d_eBb.p, d_Bm.p, d_Bw.p, d_eAn.p, d_pts.p, d_u.p,
                                                                       d_uN.p, d_eFn.p, d_eK.p, d_eF.p, d_fe.p, d_dmax.p, d_elas.p, fresh,
@@ -773,12 +942,18 @@ struct SubModel {
     k_sub_scale_vals<<<blocks_for(nbk, 128), 128, 0, st>>>(nbk, d_blkRow.p, d_col.p, d_s.p, d_val.p, d_vals.p);
     k_sub_rhs<<<blocks_for(ndof, 256), 256, 0, st>>>(ndof, d_rint.p, d_isC.p, d_s.p, d_b.p, d_r.p, d_x.p);
     TM_CUDA_CHECK(cudaGetLastError());
-    if (!pcBuilt || pcStale) { ic_factor(ic, d_vals.p, st); pcBuilt = true; pcStale = false; pcIters = 0; }
+    if (precond == TM_SUB_PC_LINE) {
+      note_launch();
+      k_sub_line_factor<<<blocks_for((size_t)nx * ny, 128), 128, 0, st>>>(nx * ny, nz, d_diag.p, d_subBlk.p, d_vals.p, d_lf.p);
+      TM_CUDA_CHECK(cudaGetLastError());
+    } else if (!pcBuilt || pcStale) {
+      ic_factor(ic, d_vals.p, st); pcBuilt = true; pcStale = false; pcIters = 0;
+    }
     double h[2];
     sums(ndof, 1, d_b.p, d_b.p, h);
     const double bn = std::sqrt(h[0]);
     if (bn == 0) return 0;
-    ic_apply(ic, d_r.p, d_z.p, st);
+    pc_apply(d_r.p, d_z.p);
     TM_CUDA_CHECK(cudaMemcpyAsync(d_p.p, d_z.p, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
     // device scalars (k_sub_sums writes two values per result): rz at a, the next rz at 2 - a,
     // p.q at 4, r.r at 6; one host synchronization per iteration, for the convergence test
@@ -798,7 +973,7 @@ struct SubModel {
       TM_CUDA_CHECK(cudaMemcpyAsync(&rr, S + 6, sizeof(double), cudaMemcpyDeviceToHost, st));
       TM_CUDA_CHECK(cudaStreamSynchronize(st));
       if (std::sqrt(rr) / bn < tol) break;
-      ic_apply(ic, d_r.p, d_z.p, st);
+      pc_apply(d_r.p, d_z.p);
       note_launch(2);
       k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_r.p, d_z.p, d_isC.p, S + (2 - a));
       k_sub_xpby<<<nb, 256, 0, st>>>(ndof, d_z.p, S + (2 - a), S + a, d_p.p);
@@ -808,17 +983,34 @@ struct SubModel {
     note_launch();
     k_sub_mul<<<nb, 256, 0, st>>>(ndof, d_s.p, d_x.p);
     TM_CUDA_CHECK(cudaGetLastError());
+    pcgSolves++;
+    pcgIters += it;
     if (!pcIters) pcIters = it;
     else if (it > 2 * pcIters) pcStale = true;
     return it;
   }
 
+  // z = M^-1 r with the submodel's preconditioner
+  void pc_apply(const double* r, double* z) {
+    if (precond == TM_SUB_PC_LINE) {
+      note_launch();
+      k_sub_line_apply<<<blocks_for((size_t)nx * ny, 128), 128, 0, st>>>(nx * ny, nz, d_lf.p, r, z);
+      TM_CUDA_CHECK(cudaGetLastError());
+    } else {
+      ic_apply(ic, r, z, st);
+    }
+  }
+
   // the elastic material records of the step from Tn to T (_elasRec, 13-fatigue.js:760-773): the
   // 4 materials, then per substrate element layer in the consistency mode
-  void upload_records(double T) {
-    std::vector<double> h(42 * (size_t)nrec, 0.0);
+  void fill_records(double T, double* h) const {
+    for (int q = 0; q < 42 * nrec; q++) h[q] = 0;
     for (int m = 0; m < 4; m++) elastic(m, Tn, T, &h[42 * m], &h[42 * m + 36]);
     for (int k = 0; k + 4 < nrec; k++) elastic(M_SUB, Tn, T, &h[42 * (4 + k)], &h[42 * (4 + k) + 36], 0.5 * (zs[k] + zs[k + 1]));
+  }
+  void upload_records(double T) {
+    std::vector<double> h(42 * (size_t)nrec, 0.0);
+    fill_records(T, h.data());
     d_elas.upload(h, st);
   }
 
@@ -912,7 +1104,17 @@ struct SubModel {
     L[2] = s[5] != 0 ? s[3] / s[5] : NAN; L[3] = s[5] != 0 ? s[4] / s[5] : NAN;
   }
 
-  // run (13-fatigue.js:1004-1104)
+  // W and ebar averaged over the two interface layers (avg of run, 13-fatigue.js:1020): die W, die
+  // ebar, substrate W, substrate ebar
+  void layer_avg(double* avg) {
+    note_launch();
+    k_sub_layer_avg<<<1, 1, 0, st>>>((int)dieGp.size(), d_dieGp.p, d_dieW.p, (int)subGp.size(), d_subGp.p, d_subW.p, d_pts.p, d_eAn.p,
+                                    d_avg.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+    d_avg.download(avg, 4, st);
+    TM_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+
   // _stressSnapshot at temperature T into host memory (48 floats per element)
   void stress_snapshot(double T, float* host) {
     GpToNode G2N;
@@ -969,12 +1171,7 @@ struct SubModel {
       nsubNext = dLast > 0.5 * INELASTIC_STEP_MAX ? std::min(nsub * 2, 64) : (dLast < 0.2 * INELASTIC_STEP_MAX ? std::max(1, nsub >> 1) : nsub);
       if (!done) fail(TM_NOT_CONVERGED, "submodel step failed to converge after cutbacks");
       sample_loop(T1, cphi, sphi, loop + 4 * (size_t)sample++);
-      note_launch();
-      k_sub_layer_avg<<<1, 1, 0, st>>>((int)dieGp.size(), d_dieGp.p, d_dieW.p, (int)subGp.size(), d_subGp.p, d_subW.p, d_pts.p, d_eAn.p,
-                                      d_avg.p);
-      TM_CUDA_CHECK(cudaGetLastError());
-      d_avg.download(avg, 4, st);
-      TM_CUDA_CHECK(cudaStreamSynchronize(st));
+      layer_avg(avg);
       const int c = hcycle[k];
       if (hphase && nSnaps && c == cycles && (k == nsteps - 1 || hphase[k + 1] != hphase[k])) {
         const int q = (*nSnaps)++;
@@ -1176,6 +1373,13 @@ SubModel* submodel_create(const tm_submodel_spec& sp) {
   m.d_dieGp.upload(m.dieGp, st); m.d_subGp.upload(m.subGp, st); m.d_dieW.upload(m.dieW, st); m.d_subW.upload(m.subW, st);
   m.d_dieB.upload(dieB, st); m.d_subB.upload(subB, st);
   m.d_sample.alloc(2 * std::max(m.dieGp.size(), m.subGp.size()) + 2);
+  // the z-line preconditioner's column couplings
+  std::vector<int> subBlk(m.nn, -1);
+  for (int n = 0; n < m.nn; n++)
+    if (n % nz)
+      for (int k = m.rowPtr[n]; k < m.rowPtr[n + 1]; k++) if (m.col[k] == n - 1) { subBlk[n] = k; break; }
+  m.d_subBlk.upload(subBlk, st);
+  m.d_lf.alloc((size_t)LF_VALS * m.nn);
   // IC(0) structure of the tangent's pattern (values at 9k + 3p + q)
   std::vector<long long> vbase(m.nbk);
   for (int k = 0; k < m.nbk; k++) vbase[k] = 9LL * k;
@@ -1203,6 +1407,10 @@ void submodel_sizes(SubModel& s, int64_t* out) {
   out[0] = s.nn; out[1] = s.ne; out[2] = s.nbnd; out[3] = 8LL * s.nsolderE;
 }
 
+void submodel_counters(SubModel& s, int64_t* out) {
+  out[0] = s.pcgSolves; out[1] = s.pcgIters;
+}
+
 void submodel_run(SubModel& s, int nsteps, const double* t, const double* T, const int* cycle, int cycles, double cphi, double sphi,
                   double* out, double* perCycle, double* loop, const int* phase, int maxSnaps, int* nSnaps, double* snapMeta,
                   float* snapSig) {
@@ -1213,5 +1421,567 @@ void submodel_run(SubModel& s, int nsteps, const double* t, const double* T, con
 }
 
 void submodel_stress_snapshot(SubModel& s, double T, float* out) { s.stress_snapshot(T, out); }
+
+void submodel_set_precond(SubModel& s, int kind) {
+  if (kind != TM_SUB_PC_IC && kind != TM_SUB_PC_LINE) fail(TM_BAD_INPUT, "submodel: unknown preconditioner kind");
+  s.precond = kind;
+  s.pcBuilt = false;
+}
+
+
+// ---- batched submodels ------------------------------------------------------------------------------
+// Submodels over the same cycle history advance together: each phase of their Newton steps
+// (prescription, assembly and gathers, residual norms, the inner PCG's products, updates,
+// preconditioner and reductions, commits) is one launch over every submodel in that phase, its
+// CTAs mapped to (submodel, block of items) through a segment table passed by value. Every
+// submodel keeps its own sub-step, cutback and Newton state on the host (run(), 13-fatigue.js:
+// 1004-1104, stepTo :924-956) and takes exactly the operations of the single engine, so with the
+// same preconditioner a batched submodel's result is the single engine's bit for bit.
+namespace {
+
+constexpr int SB_MAX = 64;   // submodels per batch
+
+// one submodel's device arrays as the batched kernels read them
+struct SubView {
+  int ne, nn, ndof, nbk, nbnd, ncol, nz, npts;
+  const int *conn, *eMat, *eBb, *eAn, *rowPtr, *col, *diag, *blkRow, *blkStart, *blkList, *nodeStart, *nodeList, *bNodes, *bGlob, *subBlk;
+  const uint8_t* isC;
+  const double *Bm, *Bw, *bW, *u25, *elas;
+  double *u, *uN, *sigE, *eFn, *eK, *eF, *fe, *dmax, *val, *vals, *s, *rint, *b, *r, *z, *p, *q, *x, *lf;
+  Point* pts;
+};
+// one submodel's parameters of the current phase
+struct SubRound {
+  AnandConst P;
+  StepK kc;
+  double fSolder, t;
+  const double *fa, *fb;
+  int fresh, wantK;
+};
+// the submodels of one launch and the first CTA of each
+struct Seg {
+  int n;
+  int sub[SB_MAX];
+  int start[SB_MAX + 1];
+};
+
+__device__ __forceinline__ int seg_find(const Seg& g, int blk) {
+  int lo = 0, hi = g.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (g.start[mid] <= blk) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+// the CTA's submodel and the index of its thread's item (items of `per` per CTA, one per thread)
+#define SB_ITEM(per)                                              \
+  const int sq_ = seg_find(g, blockIdx.x);                        \
+  const int sub = g.sub[sq_];                                     \
+  const SubView& v = V[sub];                                      \
+  const int item = (blockIdx.x - g.start[sq_]) * (per) + threadIdx.x
+
+__global__ void kb_prescribe(Seg g, const SubView* __restrict__ V, const SubRound* __restrict__ R) {
+  SB_ITEM(blockDim.x);
+  if (item < v.nbnd) sub_prescribe_node(item, v.bNodes, v.bGlob, v.bW, R[sub].fa, R[sub].fb, R[sub].t, v.u25, v.u);
+}
+__global__ void __launch_bounds__(32 * SA_WARPS) kb_assemble(Seg g, const SubView* __restrict__ V, const SubRound* __restrict__ R) {
+  __shared__ AsmSmem sm[SA_WARPS];
+  const int sq = seg_find(g, blockIdx.x), sub = g.sub[sq];
+  const SubView& v = V[sub];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = (blockIdx.x - g.start[sq]) * SA_WARPS + w;
+  if (e >= v.ne) return;
+  const SubRound& r = R[sub];
+  sub_assemble_element(e, lane, sm[w], v.conn, v.eMat, v.eBb, v.Bm, v.Bw, v.eAn, v.pts, v.u, v.uN, v.eFn, v.eK, v.eF, v.fe, v.dmax, v.elas,
+                       r.fresh, r.wantK, r.P, r.kc, r.fSolder);
+}
+__global__ void kb_gather_rint(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ndof) sub_gather_rint_dof(item, v.nodeStart, v.nodeList, v.fe, v.rint);
+}
+__global__ void kb_gather_val(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.nbk) sub_gather_val_block(item, v.blkRow, v.col, v.blkStart, v.blkList, v.eK, v.isC, v.val);
+}
+// the largest plastic increment of each submodel (CTA per submodel)
+__global__ void __launch_bounds__(256) kb_dmax(Seg g, const SubView* __restrict__ V, double* __restrict__ out) {
+  __shared__ double red[256];
+  const int sub = g.sub[blockIdx.x];
+  const SubView& v = V[sub];
+  double m = 0;
+  for (int e = threadIdx.x; e < v.ne; e += 256) {
+    const double d = v.dmax[e];
+    if (d > m) m = d;
+  }
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h && red[threadIdx.x + h] > red[threadIdx.x]) red[threadIdx.x] = red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[sub] = red[0];
+}
+// the sums of the single engine, CTA per submodel, into out[8 sub + slot]
+enum SumWhat { SUM_RINT, SUM_BB, SUM_RZ, SUM_PQ, SUM_RR, SUM_UPD };
+__global__ void __launch_bounds__(SUMS_THREADS) kb_sums(Seg g, const SubView* __restrict__ V, int what, double* __restrict__ out, int slot) {
+  __shared__ double s0[SUMS_THREADS], s1[SUMS_THREADS];
+  const int sub = g.sub[blockIdx.x];
+  const SubView& v = V[sub];
+  double* o = out + 8 * sub + slot;
+  switch (what) {
+    case SUM_RINT: sub_block_sums(v.ndof, 0, v.rint, nullptr, v.isC, o, s0, s1); break;
+    case SUM_BB: sub_block_sums(v.ndof, 1, v.b, v.b, v.isC, o, s0, s1); break;
+    case SUM_RZ: sub_block_sums(v.ndof, 1, v.r, v.z, v.isC, o, s0, s1); break;
+    case SUM_PQ: sub_block_sums(v.ndof, 1, v.p, v.q, v.isC, o, s0, s1); break;
+    case SUM_RR: sub_block_sums(v.ndof, 1, v.r, v.r, v.isC, o, s0, s1); break;
+    default: sub_block_sums(v.ndof, 2, v.x, v.u, v.isC, o, s0, s1); break;
+  }
+}
+__global__ void kb_scale_s(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.nn) sub_scale_s_node(item, v.diag, v.val, v.s);
+}
+__global__ void kb_scale_vals(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.nbk) sub_scale_vals_block(item, v.blkRow, v.col, v.s, v.val, v.vals);
+}
+__global__ void kb_rhs(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ndof) sub_rhs_dof(item, v.rint, v.isC, v.s, v.b, v.r, v.x);
+}
+__global__ void kb_spmv(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.nn) sub_spmv_node(item, v.rowPtr, v.col, v.vals, v.p, v.q);
+}
+// alpha = rz / pq from the submodel's scalars S[a] and S[4]
+__global__ void kb_axpy2(Seg g, const SubView* __restrict__ V, const double* __restrict__ S, int a) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ndof) sub_axpy2_dof(item, S[8 * sub + a], S[8 * sub + 4], v.p, v.q, v.x, v.r);
+}
+// beta = S[2 - a] / S[a]
+__global__ void kb_xpby(Seg g, const SubView* __restrict__ V, const double* __restrict__ S, int a) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ndof) sub_xpby_dof(item, S[8 * sub + 2 - a], S[8 * sub + a], v.z, v.p);
+}
+__global__ void kb_copy_zp(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ndof) v.p[item] = v.z[item];
+}
+__global__ void kb_mul(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ndof) v.x[item] *= v.s[item];
+}
+__global__ void kb_line_factor(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ncol) sub_line_factor_column(item, v.nz, v.diag, v.subBlk, v.vals, v.lf);
+}
+__global__ void kb_line_apply(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ncol) sub_line_apply_column(item, v.nz, v.lf, v.r, v.z);
+}
+__global__ void kb_commit_points(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.npts) commit(v.pts[item]);
+}
+__global__ void __launch_bounds__(32 * SA_WARPS) kb_commit_elastic(Seg g, const SubView* __restrict__ V) {
+  __shared__ CommitSmem sm[SA_WARPS];
+  const int sq = seg_find(g, blockIdx.x), sub = g.sub[sq];
+  const SubView& v = V[sub];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = (blockIdx.x - g.start[sq]) * SA_WARPS + w;
+  if (e >= v.ne || v.eAn[e] >= 0) return;
+  sub_commit_elastic_element(e, lane, sm[w], v.conn, v.eMat, v.eBb, v.Bm, v.Bw, v.u, v.uN, v.elas, v.sigE, v.eFn);
+}
+__global__ void kb_copy_uN(Seg g, const SubView* __restrict__ V) {
+  SB_ITEM(blockDim.x);
+  if (item < v.ndof) v.uN[item] = v.u[item];
+}
+#undef SB_ITEM
+
+// per submodel: where it is in run()'s history loop and in its current stepTo
+enum RunPhase { RP_START, RP_NEWTON, RP_DONE, RP_FAILED };
+struct RunState {
+  RunPhase ph = RP_START;
+  int k = 1, nsub = 1, nsubNext = 1, attempt = 0, sIdx = 1, sample = 0;
+  double snapTn = 0, dLast = 0;
+  long long totalNewton = 0;
+  int cutbacks = 0, steps = 0;
+  std::vector<double> Wdie, Wsub, Edie, Esub;
+  double T = 0, dt = 0, rPrev = INFINITY, dMax = 0, tol = 0, bn = 0;
+  int it = 1;
+  bool haveK = false, wantK = false;
+  tm_status status = TM_OK;
+};
+
+struct Batch {
+  std::vector<SubModel*> M;
+  int B = 0;
+  cudaStream_t st = nullptr;
+  std::vector<cudaStream_t> own;         // the submodels' own streams, restored at the end
+  DBuf<SubView> dV;
+  DBuf<SubRound> dR;
+  DBuf<double> dS, dN, dDmax, dElas;     // PCG scalars (8 per submodel), norms (8 per), plastic increments, records
+  std::vector<SubRound> R;
+  std::vector<double> hS, hN, hDmax, hElas;
+  int recMax = 0;
+
+  explicit Batch(const std::vector<SubModel*>& subs) : M(subs), B((int)subs.size()) {
+    TM_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (SubModel* m : M) {
+      TM_CUDA_CHECK(cudaStreamSynchronize(m->st));
+      own.push_back(m->st);
+      m->st = st;                         // the submodel's own operations join the batch's stream
+      recMax = std::max(recMax, m->nrec);
+    }
+    hElas.assign((size_t)B * recMax * 42, 0.0);
+    dElas.alloc(hElas.size());
+    std::vector<SubView> hv(B);
+    for (int s = 0; s < B; s++) {
+      SubModel& m = *M[s];
+      SubView& v = hv[s];
+      v.ne = m.ne; v.nn = m.nn; v.ndof = m.ndof; v.nbk = m.nbk; v.nbnd = m.nbnd; v.ncol = m.nx * m.ny; v.nz = m.nz;
+      v.npts = 8 * m.nsolderE;
+      v.conn = m.d_conn.p; v.eMat = m.d_eMat.p; v.eBb = m.d_eBb.p; v.eAn = m.d_eAn.p; v.rowPtr = m.d_rowPtr.p; v.col = m.d_col.p;
+      v.diag = m.d_diag.p; v.blkRow = m.d_blkRow.p; v.blkStart = m.d_blkStart.p; v.blkList = m.d_blkList.p;
+      v.nodeStart = m.d_nodeStart.p; v.nodeList = m.d_nodeList.p; v.bNodes = m.d_bNodes.p; v.bGlob = m.d_bGlob.p; v.subBlk = m.d_subBlk.p;
+      v.isC = m.d_isC.p; v.Bm = m.d_Bm.p; v.Bw = m.d_Bw.p; v.bW = m.d_bW.p; v.u25 = m.d_u25.p;
+      v.elas = dElas.p + (size_t)s * recMax * 42;
+      v.u = m.d_u.p; v.uN = m.d_uN.p; v.sigE = m.d_sigE.p; v.eFn = m.d_eFn.p; v.eK = m.d_eK.p; v.eF = m.d_eF.p; v.fe = m.d_fe.p;
+      v.dmax = m.d_dmax.p; v.val = m.d_val.p; v.vals = m.d_vals.p; v.s = m.d_s.p; v.rint = m.d_rint.p; v.b = m.d_b.p; v.r = m.d_r.p;
+      v.z = m.d_z.p; v.p = m.d_p.p; v.q = m.d_q.p; v.x = m.d_x.p; v.lf = m.d_lf.p; v.pts = m.d_pts.p;
+      // the batch owns the material records: the single engine uploads its own again when next used
+      m.haveKey = false;
+    }
+    dV.upload(hv, st);
+    R.assign(B, SubRound{});
+    dR.alloc(B);
+    hS.assign(8 * (size_t)B, 0.0); dS.alloc(hS.size());
+    hN.assign(8 * (size_t)B, 0.0); dN.alloc(hN.size());
+    hDmax.assign(B, 0.0); dDmax.alloc(B);
+  }
+  ~Batch() {
+    cudaStreamSynchronize(st);
+    for (int s = 0; s < B; s++) { M[s]->st = own[s]; M[s]->haveKey = false; }
+    cudaStreamDestroy(st);
+  }
+
+  // a segment over the listed submodels, count(s) items each, per items per CTA; false when empty
+  template <class F>
+  static bool seg(Seg& g, const std::vector<int>& subs, F count, int per) {
+    g.n = 0;
+    long long tot = 0;
+    for (int s : subs) {
+      const long long c = count(s);
+      if (c <= 0) continue;
+      g.sub[g.n] = s;
+      g.start[g.n] = (int)tot;
+      tot += (c + per - 1) / per;
+      g.n++;
+    }
+    if (tot >= (1LL << 31)) fail(TM_BAD_INPUT, "submodel batch too large for one launch");
+    g.start[g.n] = (int)tot;
+    return tot > 0;
+  }
+  static Seg one_each(const std::vector<int>& subs) {
+    Seg g;
+    g.n = (int)subs.size();
+    for (int q = 0; q < g.n; q++) { g.sub[q] = subs[q]; g.start[q] = q; }
+    g.start[g.n] = g.n;
+    return g;
+  }
+  void upload_rounds() { TM_CUDA_CHECK(cudaMemcpyAsync(dR.p, R.data(), B * sizeof(SubRound), cudaMemcpyHostToDevice, st)); }
+
+  void prescribe(const std::vector<int>& subs) {
+    Seg g;
+    if (!seg(g, subs, [&](int s) { return M[s]->nbnd; }, 128)) return;
+    upload_rounds();
+    note_launch();
+    kb_prescribe<<<g.start[g.n], 128, 0, st>>>(g, dV.p, dR.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+  }
+
+  // assemble (13-fatigue.js:776-853) of the listed submodels with their R[s]; the plastic
+  // increments go to dDmax
+  void assemble(const std::vector<int>& subs, bool anyFresh) {
+    upload_rounds();
+    if (anyFresh) TM_CUDA_CHECK(cudaMemcpyAsync(dElas.p, hElas.data(), hElas.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    Seg g;
+    note_launch(3);
+    if (seg(g, subs, [&](int s) { return M[s]->ne; }, SA_WARPS)) kb_assemble<<<g.start[g.n], 32 * SA_WARPS, 0, st>>>(g, dV.p, dR.p);
+    if (seg(g, subs, [&](int s) { return M[s]->ndof; }, 256)) kb_gather_rint<<<g.start[g.n], 256, 0, st>>>(g, dV.p);
+    std::vector<int> wk;
+    for (int s : subs) if (R[s].wantK) wk.push_back(s);
+    if (seg(g, wk, [&](int s) { return M[s]->nbk; }, 128)) { note_launch(); kb_gather_val<<<g.start[g.n], 128, 0, st>>>(g, dV.p); }
+    kb_dmax<<<(int)subs.size(), 256, 0, st>>>(one_each(subs), dV.p, dDmax.p);
+    TM_CUDA_CHECK(cudaGetLastError());
+  }
+
+  void sums(const std::vector<int>& subs, int what, DBuf<double>& out, int slot) {
+    if (subs.empty()) return;
+    note_launch();
+    kb_sums<<<(int)subs.size(), SUMS_THREADS, 0, st>>>(one_each(subs), dV.p, what, out.p, slot);
+    TM_CUDA_CHECK(cudaGetLastError());
+  }
+  void fetch(DBuf<double>& d, std::vector<double>& h) {
+    TM_CUDA_CHECK(cudaMemcpyAsync(h.data(), d.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TM_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+  template <class K>
+  void each_dof(const std::vector<int>& subs, K kern) {
+    Seg g;
+    if (seg(g, subs, [&](int s) { return M[s]->ndof; }, 256)) { note_launch(); kern<<<g.start[g.n], 256, 0, st>>>(g, dV.p); }
+  }
+
+  // z = M^-1 r: the z-line submodels in one launch, the IC(0) ones through their level launches
+  void pc_apply(const std::vector<int>& subs) {
+    std::vector<int> line;
+    for (int s : subs) {
+      if (M[s]->precond == TM_SUB_PC_LINE) line.push_back(s);
+      else M[s]->pc_apply(M[s]->d_r.p, M[s]->d_z.p);
+    }
+    Seg g;
+    if (seg(g, line, [&](int s) { return (long long)M[s]->nx * M[s]->ny; }, 128)) {
+      note_launch();
+      kb_line_apply<<<g.start[g.n], 128, 0, st>>>(g, dV.p);
+    }
+    TM_CUDA_CHECK(cudaGetLastError());
+  }
+
+  // _solve (13-fatigue.js:886-917) for the listed submodels, each to its RunState tol: d_x = the
+  // Newton increment
+  void solve(const std::vector<int>& subs, std::vector<RunState>& rs) {
+    Seg g;
+    note_launch(3);
+    if (seg(g, subs, [&](int s) { return M[s]->nn; }, 128)) kb_scale_s<<<g.start[g.n], 128, 0, st>>>(g, dV.p);
+    if (seg(g, subs, [&](int s) { return M[s]->nbk; }, 128)) kb_scale_vals<<<g.start[g.n], 128, 0, st>>>(g, dV.p);
+    each_dof(subs, kb_rhs);
+    std::vector<int> line;
+    for (int s : subs) {
+      SubModel& m = *M[s];
+      if (m.precond == TM_SUB_PC_LINE) line.push_back(s);
+      else if (!m.pcBuilt || m.pcStale) { ic_factor(m.ic, m.d_vals.p, st); m.pcBuilt = true; m.pcStale = false; m.pcIters = 0; }
+    }
+    if (seg(g, line, [&](int s) { return (long long)M[s]->nx * M[s]->ny; }, 128)) {
+      note_launch();
+      kb_line_factor<<<g.start[g.n], 128, 0, st>>>(g, dV.p);
+    }
+    sums(subs, SUM_BB, dN, 0);
+    fetch(dN, hN);
+    std::vector<int> act;
+    for (int s : subs) {
+      rs[s].bn = std::sqrt(hN[8 * s]);
+      if (rs[s].bn != 0) act.push_back(s);
+    }
+    if (act.empty()) return;
+    const std::vector<int> solved = act;
+    pc_apply(act);
+    each_dof(act, kb_copy_zp);
+    int a = 0;
+    sums(act, SUM_RZ, dS, a);
+    std::vector<int> its(B, 0);
+    int it;
+    for (it = 1; it <= 2000 && !act.empty(); it++) {
+      Seg ga;
+      if (seg(ga, act, [&](int s) { return M[s]->nn; }, 128)) { note_launch(); kb_spmv<<<ga.start[ga.n], 128, 0, st>>>(ga, dV.p); }
+      sums(act, SUM_PQ, dS, 4);
+      if (seg(ga, act, [&](int s) { return M[s]->ndof; }, 256)) { note_launch(); kb_axpy2<<<ga.start[ga.n], 256, 0, st>>>(ga, dV.p, dS.p, a); }
+      sums(act, SUM_RR, dS, 6);
+      fetch(dS, hS);
+      std::vector<int> next;
+      for (int s : act) {
+        if (std::sqrt(hS[8 * s + 6]) / rs[s].bn < rs[s].tol) its[s] = it;
+        else next.push_back(s);
+      }
+      act.swap(next);
+      if (act.empty()) break;
+      pc_apply(act);
+      sums(act, SUM_RZ, dS, 2 - a);
+      if (seg(ga, act, [&](int s) { return M[s]->ndof; }, 256)) { note_launch(); kb_xpby<<<ga.start[ga.n], 256, 0, st>>>(ga, dV.p, dS.p, a); }
+      a = 2 - a;
+    }
+    for (int s : act) its[s] = 2001;   // the loop's bound, as the single engine's counter ends
+    each_dof(solved, kb_mul);
+    TM_CUDA_CHECK(cudaGetLastError());
+    for (int s : solved) {
+      SubModel& m = *M[s];
+      m.pcgSolves++;
+      m.pcgIters += its[s];
+      if (m.precond == TM_SUB_PC_LINE) continue;
+      if (!m.pcIters) m.pcIters = its[s];
+      else if (its[s] > 2 * m.pcIters) m.pcStale = true;
+    }
+  }
+
+  // the end of a converged stepTo: the solder points' trial states become committed, the elastic
+  // elements' stresses and forces are updated and u_n = u
+  void commit(const std::vector<int>& subs) {
+    Seg g;
+    if (seg(g, subs, [&](int s) { return 8LL * M[s]->nsolderE; }, 128)) { note_launch(); kb_commit_points<<<g.start[g.n], 128, 0, st>>>(g, dV.p); }
+    if (seg(g, subs, [&](int s) { return M[s]->ne; }, SA_WARPS)) {
+      note_launch();
+      kb_commit_elastic<<<g.start[g.n], 32 * SA_WARPS, 0, st>>>(g, dV.p);
+    }
+    each_dof(subs, kb_copy_uN);
+    TM_CUDA_CHECK(cudaGetLastError());
+  }
+};
+
+}  // namespace
+
+void submodel_run_batch(const std::vector<SubModel*>& subs, int nsteps, const double* ht, const double* hT, const int* hcycle, int cycles,
+                        const double* cphi, const double* sphi, double* out10, double* perCycle, double* loop, int32_t* status) {
+  const int n = (int)subs.size();
+  if (nsteps < 2 || cycles < 1) fail(TM_BAD_INPUT, "submodel run: need >= 2 history points and >= 1 cycle");
+  for (int k = 0; k < nsteps; k++) if (hcycle[k] < 0 || hcycle[k] > cycles) fail(TM_BAD_INPUT, "submodel run: cycle index out of range");
+  for (int b0 = 0; b0 < n; b0 += SB_MAX) {
+    const int nb = std::min(SB_MAX, n - b0);
+    std::vector<SubModel*> part(subs.begin() + b0, subs.begin() + b0 + nb);
+    Batch bt(part);
+    std::vector<RunState> rs(nb);
+    auto begin_substep = [&](int s) {
+      RunState& r = rs[s];
+      const double T0 = hT[r.k - 1], T1 = hT[r.k], t0s = ht[r.k - 1], t1s = ht[r.k];
+      r.T = T0 + (T1 - T0) * r.sIdx / r.nsub;
+      r.dt = (t1s - t0s) / r.nsub;
+      r.ph = RP_START;
+    };
+    auto begin_attempt = [&](int s) {
+      rs[s].snapTn = part[s]->Tn;
+      part[s]->snapshot();
+      rs[s].sIdx = 1;
+      begin_substep(s);
+    };
+    auto finish = [&](int s) {
+      RunState& r = rs[s];
+      const int nc = cycles;
+      const double dWdie = r.Wdie[nc] - r.Wdie[nc - 1], dWsub = r.Wsub[nc] - r.Wsub[nc - 1];
+      const double dEdie = r.Edie[nc] - r.Edie[nc - 1], dEsub = r.Esub[nc] - r.Esub[nc - 1];
+      const double dW = std::max(dWdie, dWsub), dE = dWdie >= dWsub ? dEdie : dEsub;
+      const double prev = nc >= 2 ? std::max(r.Wdie[nc - 1] - r.Wdie[nc - 2], r.Wsub[nc - 1] - r.Wsub[nc - 2]) : NAN;
+      const double stab = std::isfinite(prev) && prev > 0 ? std::fabs(dW - prev) / prev : NAN;
+      const double o[10] = {dW, dWdie, dWsub, dE, dEdie, dEsub, stab, (double)r.steps, (double)r.cutbacks,
+                            (double)r.totalNewton / std::max(r.steps, 1)};
+      std::copy(o, o + 10, out10 + 10 * (size_t)(b0 + s));
+      double* pc = perCycle + 2 * (size_t)cycles * (b0 + s);
+      for (int c = 1; c <= nc; c++) { pc[2 * (c - 1)] = r.Wdie[c] - r.Wdie[c - 1]; pc[2 * (c - 1) + 1] = r.Wsub[c] - r.Wsub[c - 1]; }
+      r.ph = RP_DONE;
+    };
+    auto attempt_failed = [&](int s) {
+      RunState& r = rs[s];
+      part[s]->restore(r.snapTn);
+      r.nsub *= 2;
+      r.cutbacks++;
+      if (++r.attempt >= 8) { r.status = TM_NOT_CONVERGED; r.ph = RP_FAILED; return; }
+      begin_attempt(s);
+    };
+    auto substep_done = [&](int s) {
+      RunState& r = rs[s];
+      if (++r.sIdx <= r.nsub) { begin_substep(s); return; }
+      // the history step is complete
+      r.nsubNext = r.dLast > 0.5 * INELASTIC_STEP_MAX ? std::min(r.nsub * 2, 64)
+                                                        : (r.dLast < 0.2 * INELASTIC_STEP_MAX ? std::max(1, r.nsub >> 1) : r.nsub);
+      double avg[4];
+      part[s]->sample_loop(hT[r.k], cphi[b0 + s], sphi[b0 + s], loop + 4 * (size_t)nsteps * (b0 + s) + 4 * (size_t)r.sample++);
+      part[s]->layer_avg(avg);
+      const int c = hcycle[r.k];
+      r.Wdie[c] = avg[0]; r.Edie[c] = avg[1]; r.Wsub[c] = avg[2]; r.Esub[c] = avg[3];
+      if (++r.k >= nsteps) { finish(s); return; }
+      r.nsub = r.nsubNext;
+      r.attempt = 0;
+      begin_attempt(s);
+    };
+    for (int s = 0; s < nb; s++) {
+      RunState& r = rs[s];
+      if (!part[s]->nsolderE || part[s]->elasticSolder) { r.status = TM_BAD_INPUT; r.ph = RP_FAILED; continue; }
+      r.Wdie.assign(cycles + 1, 0.0); r.Wsub = r.Wdie; r.Edie = r.Wdie; r.Esub = r.Wdie;
+      part[s]->sample_loop(25, cphi[b0 + s], sphi[b0 + s], loop + 4 * (size_t)nsteps * (b0 + s) + 4 * (size_t)r.sample++);
+      begin_attempt(s);
+    }
+    for (;;) {
+      // stepTo's start: prescribe the cut boundary
+      std::vector<int> start, newton;
+      for (int s = 0; s < nb; s++)
+        if (rs[s].ph == RP_START) {
+          RunState& r = rs[s];
+          part[s]->prescribe_args(r.T, &bt.R[s].fa, &bt.R[s].fb, &bt.R[s].t);
+          r.ph = RP_NEWTON; r.it = 1; r.rPrev = INFINITY; r.haveK = false;
+          start.push_back(s);
+        }
+      bt.prescribe(start);
+      for (int s = 0; s < nb; s++) if (rs[s].ph == RP_NEWTON) newton.push_back(s);
+      if (newton.empty()) break;
+      // one Newton iteration of every submodel in a stepTo
+      bool anyFresh = false;
+      for (int s : newton) {
+        RunState& r = rs[s];
+        SubModel& m = *part[s];
+        r.wantK = r.it <= 2 || !r.haveK;
+        SubRound& R = bt.R[s];
+        R.fresh = m.fresh_for(r.T);
+        if (R.fresh) { m.fill_records(r.T, bt.hElas.data() + (size_t)s * bt.recMax * 42); anyFresh = true; }
+        m.step_params(r.T, r.dt, &R.kc, &R.fSolder);
+        R.P = m.P;
+        R.wantK = r.wantK;
+      }
+      bt.assemble(newton, anyFresh);
+      for (int s : newton) {
+        RunState& r = rs[s];
+        SubModel& m = *part[s];
+        if (r.wantK) r.haveK = true;
+        m.haveKey = true; m.keyTn = m.Tn; m.keyT = r.T;
+      }
+      bt.sums(newton, SUM_RINT, bt.dN, 0);
+      bt.fetch(bt.dN, bt.hN);
+      bt.fetch(bt.dDmax, bt.hDmax);
+      std::vector<int> conv, solve, refresh;
+      for (int s : newton) {
+        RunState& r = rs[s];
+        r.dMax = bt.hDmax[s];
+        const double rn = std::sqrt(bt.hN[8 * s]), fn = std::sqrt(bt.hN[8 * s + 1]);
+        const double ref = std::max(fn, 1e-30);
+        if (rn / ref < SUB_RES_TOL) { conv.push_back(s); continue; }
+        if (!r.wantK && rn > 0.5 * r.rPrev) refresh.push_back(s);   // stalled with the frozen tangent: refresh it
+        r.rPrev = rn;
+        r.tol = std::max(SUB_INNER_TOL, std::min(1e-3, 0.01 * SUB_RES_TOL * ref / std::max(rn, 1e-300)));
+        solve.push_back(s);
+      }
+      if (!refresh.empty()) {
+        for (int s : refresh) { bt.R[s].fresh = 0; bt.R[s].wantK = 1; }
+        bt.assemble(refresh, false);
+      }
+      if (!solve.empty()) {
+        bt.solve(solve, rs);
+        bt.sums(solve, SUM_UPD, bt.dN, 0);   // u += du on the free DOFs
+        bt.fetch(bt.dN, bt.hN);
+        for (int s : solve) {
+          RunState& r = rs[s];
+          const bool done = std::sqrt(bt.hN[8 * s]) < SUB_DU_TOL * std::max(std::sqrt(bt.hN[8 * s + 1]), 1e-30);
+          r.it++;
+          if (done) conv.push_back(s);
+          else if (r.it > SUB_NEWTON_MAXIT) {   // not converged: the attempt fails
+            r.totalNewton += r.it; r.steps++; r.dLast = r.dMax;
+            attempt_failed(s);
+          }
+        }
+      }
+      if (conv.empty()) continue;
+      // converged stepTo: the final assembly and the commit
+      for (int s : conv) { bt.R[s].fresh = 0; bt.R[s].wantK = 0; }
+      bt.assemble(conv, false);
+      bt.commit(conv);
+      bt.fetch(bt.dDmax, bt.hDmax);
+      for (int s : conv) {
+        RunState& r = rs[s];
+        part[s]->Tn = r.T;
+        r.totalNewton += r.it; r.steps++;
+        r.dLast = bt.hDmax[s];
+        if (r.dLast > INELASTIC_STEP_MAX) attempt_failed(s);
+        else substep_done(s);
+      }
+    }
+    for (int s = 0; s < nb; s++) status[b0 + s] = rs[s].status;
+  }
+}
 
 }  // namespace tmg

@@ -28,7 +28,7 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_warpage_sensitivity", "tm_sensitivity_direction", "tm_vcycle_shapes", "tm_set_vcycle_shapes", "tm_submodel_run_sections", "tm_submodel_stress_snapshot",
             "tm_mg_levels", "tm_mg_node_agg", "tm_device_peaks",
             "tm_set_wait_test", "tm_anand_screen_gradient",
-            "tm_element_strains_adjoint", "tm_accumulate_q_adjoint", "tm_adjoint_sensitivity", "tm_set_level0", "tm_level0"]
+            "tm_element_strains_adjoint", "tm_accumulate_q_adjoint", "tm_adjoint_sensitivity", "tm_set_level0", "tm_level0", "tm_clear_warm", "tm_submodel_set_precond", "tm_submodel_counters"]
 PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
 PRECOND_NAMES = {v: k for k, v in PRECONDS.items()}
 KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
@@ -115,6 +115,8 @@ def load():
     L.tm_pc_apply.argtypes = [vp, vp, vp]
     L.tm_submodel_create.argtypes = [C.POINTER(TmSubmodelSpec), C.POINTER(vp)]
     L.tm_submodel_destroy.argtypes = [vp]
+    L.tm_submodel_set_precond.argtypes = [vp, C.c_int32]
+    L.tm_submodel_counters.argtypes = [vp, vp]
     L.tm_submodel_sizes.argtypes = [vp, vp]
     L.tm_submodel_step.argtypes = [vp, C.c_double, C.c_double, vp, vp, vp]
     L.tm_submodel_get.argtypes = [vp, vp, vp, vp]
@@ -132,6 +134,7 @@ def load():
     L.tm_set_wait_test.argtypes = [vp, C.c_int32]
     L.tm_set_level0.argtypes = [vp, C.c_int32]
     L.tm_level0.argtypes = [vp, vp]
+    L.tm_clear_warm.argtypes = [vp]
     L.tm_element_strains_adjoint.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
     L.tm_accumulate_q_adjoint.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
     L.tm_adjoint_sensitivity.argtypes = [vp, vp, vp, C.POINTER(TmSolveOpts), vp, vp, C.POINTER(TmSolveInfo)]

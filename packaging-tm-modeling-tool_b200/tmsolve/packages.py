@@ -63,6 +63,14 @@ class Package:
     Ta: float = 150.0
     Tb: float = 25.0
     meta: dict = field(default_factory=dict)
+    # step data with named materials' moduli and expansion coefficients scaled,
+    # scales {material: (E factor, CTE factor)} (applySensitivity's matE / matCTE, 14-sensitivity.js:89-110)
+    material_step_fn: Optional[Callable[[dict, float, float], StepData]] = None
+
+    def material_step(self, scales: dict, Ta: Optional[float] = None, Tb: Optional[float] = None) -> StepData:
+        if self.material_step_fn is None:
+            raise ValueError(f"package {self.name} has no named materials to scale")
+        return self.material_step_fn(scales, self.Ta if Ta is None else Ta, self.Tb if Tb is None else Tb)
 
     @property
     def e_pset(self) -> np.ndarray:
@@ -261,28 +269,28 @@ def lidded_c2(n_inplane: int = 160, seed: int = 20261203) -> Package:
     mesh = build_structured_mesh(xs, ys, zs, cg, cp, cs, featureX=feat, featureY=feat)
     mesh.constraints = constraints321(mesh, CONSTRAINT_SPAN * L / 2)
     # property sets: 0..11 layered bands, then the homogeneous groups
-    def row_mat(nm):
-        E, nu, a = mat[nm]
-        return iso_d(E, nu), a, a
-    band_subs = []
-    for (b0, b1) in bands:
-        subs = []
-        for q, (nm, _) in enumerate(rows):
-            a, bb = max(b0, zr[q]), min(b1, zr[q + 1])
-            if bb - a > 1e-12:
-                D, axy, az = row_mat(nm)
-                subs.append((a, bb, D, axy, az))
-        band_subs.append((b0, b1, subs))
-    hom = [row_mat("core")]  # placeholder for pset ordering below
     hom_names = ["solder", "uf", "die", "tim", "adh", "lid"]
-    mats: List = [None] * nb
-    for nm in hom_names:
-        E, nu, a = mat[nm]
-        mats.append((column_d(E, nu) if nm == "solder" else iso_d(E, nu), a, a))
-    del hom
-    def layered_fn(p, Ta, Tb):
-        b0, b1, subs = band_subs[p]
-        return layered_section(b0, b1, subs, Ta, Tb, with_subs=True)
+
+    def make_step(scales, Ta, Tb):
+        m = {k: (mat[k][0] * scales.get(k, (1.0, 1.0))[0], mat[k][1], mat[k][2] * scales.get(k, (1.0, 1.0))[1]) for k in names}
+        band_subs = []
+        for (b0, b1) in bands:
+            subs = []
+            for q, (nm, _) in enumerate(rows):
+                a, bb = max(b0, zr[q]), min(b1, zr[q + 1])
+                if bb - a > 1e-12:
+                    E, nu, al = m[nm]
+                    subs.append((a, bb, iso_d(E, nu), al, al))
+            band_subs.append((b0, b1, subs))
+        mats: List = [None] * nb
+        for nm in hom_names:
+            E, nu, al = m[nm]
+            mats.append((column_d(E, nu) if nm == "solder" else iso_d(E, nu), al, al))
+
+        def layered_fn(p, Ta, Tb):
+            b0, b1, subs = band_subs[p]
+            return layered_section(b0, b1, subs, Ta, Tb, with_subs=True)
+        return _homog_step(mats, Ta, Tb, layered_fn=layered_fn)
     ng = 7
     group_layered = np.array([1, 0, 0, 0, 0, 0, 0], np.int32)
     group_pset = np.array([0, nb + 0, nb + 1, nb + 2, nb + 3, nb + 4, nb + 5], np.int32)
@@ -290,8 +298,8 @@ def lidded_c2(n_inplane: int = 160, seed: int = 20261203) -> Package:
     sec_of_layer[:nb] = np.arange(nb)
     return Package(name="lidded_c2", mesh=mesh, group_layered=group_layered, group_stage=np.zeros(ng, np.int32),
                    group_pset=group_pset, sec_of_layer=sec_of_layer, npset=nb + len(hom_names),
-                   step_fn=lambda Ta, Tb: _homog_step(mats, Ta, Tb, layered_fn=layered_fn), Ta=150.0, Tb=25.0,
-                   meta=dict(workload=f"lidded_c2 {n}x{n}x32", bottom_plane=0, seed=seed,
+                   step_fn=lambda Ta, Tb: make_step({}, Ta, Tb), Ta=150.0, Tb=25.0, material_step_fn=make_step,
+                   meta=dict(workload=f"lidded_c2 {n}x{n}x32", bottom_plane=0, seed=seed, materials=list(names),
                              die=dict(cx=0.0, cy=0.0, w=25.0, h=25.0, keepout=0.2, px=0.15, py=0.15),
                              bga=dict(sx=L, sy=L, inset=1.0, pitch=1.0),
                              bump_layer=dict(zmid=z0 + 0.5 * t_bump, part=PART["SOLDER"])))

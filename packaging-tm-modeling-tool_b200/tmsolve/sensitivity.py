@@ -1,4 +1,6 @@
-"""Adjoint gradient of a bump site's last-cycle dW with respect to the property sets' stiffness and
+"""Sensitivities on the device: the tornado batch of perturbed materials (the reference's
+applySensitivity / runSensitivityCase, src/core/14-sensitivity.js:89-156) and the adjoint gradient of a
+bump site's last-cycle dW with respect to the property sets' stiffness and
 thermal strain (the peak-bump half of the adjoint sensitivities; the reference's tornado,
 src/core/14-sensitivity.js, re-runs a whole analysis per input instead).
 
@@ -27,6 +29,64 @@ import numpy as np
 
 from . import post
 from .anand import screen_gradient
+
+SENS_REL = 0.10    # relative perturbation of a sensitivity input (00-constants.js:129)
+# the inputs of the C2 tornado: the moduli of six materials, then the expansion coefficients of six
+TORNADO_E = ("sr", "diel", "cu", "corecu", "core", "solder")
+TORNADO_CTE = ("uf", "die", "tim", "adh", "lid", "cu")
+
+
+def tornado_cases(e_materials=TORNADO_E, cte_materials=TORNADO_CTE, rel: float = SENS_REL) -> list:
+    """The perturbed cases: every listed material's modulus (matE), then every listed material's
+    expansion coefficient (matCTE), at the low and the high bound, factors 1 -/+ rel
+    (sensitivityBounds, 14-sensitivity.js:113-119)."""
+    cases = []
+    for kind, names in (("E", e_materials), ("CTE", cte_materials)):
+        for nm in names:
+            for f in (1.0 - rel, 1.0 + rel):
+                cases.append(dict(material=nm, kind=kind, factor=f))
+    return cases
+
+
+def case_scales(case: dict) -> dict:
+    """The package's material scales {name: (E factor, CTE factor)} of one case (None: the base)."""
+    if case is None:
+        return {}
+    f = float(case["factor"])
+    return {case["material"]: (f, 1.0) if case["kind"] == "E" else (1.0, f)}
+
+
+def tornado(model, cases, tol: float = 1e-8, precision: str = "mixed", warm: int = 1, key: int = 0,
+            Ta=None, Tb=None) -> dict:
+    """The base case, then every case of `cases`, in one solve loop on one device model. Each case's
+    step is assembled with its materials scaled, gets its own multigrid hierarchy (key + case
+    index: a hierarchy kept across a 10 % change of one material needs about twice the
+    iterations, which costs more than the set-up) and is solved from the Galerkin projection onto
+    the `warm` most recent solutions (the warm start, 10-solver.js:885-926; one stored solution
+    costs one operator apply and two dot products, and the previous case is already close). Per
+    case: the signed JEITA warpage of the bottom surface over the BGA zone and the RMS warpage of the
+    bottom plane, with the solve's record; `swing` lists per input the low and high warpage
+    (tornadoFromCases)."""
+    pkg = model.pkg
+    bga = post.bga_sites(**pkg.meta["bga"])
+    from .packages import rms_warpage
+    out = []
+    for q, case in enumerate([None] + list(cases)):
+        st = pkg.material_step(case_scales(case), Ta, Tb)
+        r = model.solve(model.assemble_step(st), tol=tol, warm=warm, key=key + q, precision=precision)
+        if not r["converged"]:
+            raise RuntimeError(f"tornado case {case} did not converge")
+        u = r["u"]
+        w = post.warpage_jeita(bga, lambda x, y: model.sample_plane(u, 0, 2, x, y))
+        out.append(dict(case=case, signed=float(w["signed"]), rms=float(rms_warpage(pkg.mesh, u)), iters=int(r["iters"]),
+                        iters0=float(r["iters0"]), warm=int(r["warm"]), rebuilt=bool(r["rebuilt"]), ms=float(r["ms"])))
+    base, rest = out[0], out[1:]
+    swing = []
+    for q in range(0, len(rest) - 1, 2):
+        lo, hi = rest[q], rest[q + 1]
+        swing.append(dict(material=lo["case"]["material"], kind=lo["case"]["kind"], lo=lo["signed"], hi=hi["signed"],
+                          span=abs(hi["signed"] - lo["signed"])))
+    return dict(base=base, cases=rest, swing=swing)
 
 
 def _branch_h(path: post.ThermalPath, gq: dict) -> dict:

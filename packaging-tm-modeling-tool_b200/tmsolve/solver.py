@@ -278,6 +278,10 @@ class DeviceModel:
         """Test hook of the timeout path: the level-0 TMA sweep waits for a flag that nothing sets."""
         check(load().tm_set_wait_test(self.h, 1 if on else 0))
 
+    def clear_warm(self):
+        """Drops the warm start's stored solutions (tm_clear_warm)."""
+        check(load().tm_clear_warm(self.h))
+
     def set_level0(self, matrix_free: bool):
         """Level-0 operator of the solves after the next assembly: the assembled stencil (default)
         or cell-by-cell products with the element classes' matrices (tm_set_level0)."""

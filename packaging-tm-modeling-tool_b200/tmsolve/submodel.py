@@ -30,6 +30,7 @@ SUB_T_AVG = 0.025       # 00-constants.js:114
 SUB_MARGIN = 0.05       # 00-constants.js:115
 NU_MAX_SUBMODEL = 0.49  # 00-constants.js:20
 MAT = dict(SUB=0, SOLDER=1, UF=2, SI=3)
+SUB_PRECONDS = dict(ic=0, line=1)    # TM_SUB_PC_IC, TM_SUB_PC_LINE
 HEX_XI = (-1, 1, 1, -1, -1, 1, 1, -1)
 HEX_ETA = (-1, -1, 1, 1, -1, -1, 1, 1)
 HEX_ZETA = (-1, -1, -1, -1, 1, 1, 1, 1)
@@ -328,6 +329,17 @@ class DeviceSubmodel:
         except Exception:
             pass
 
+    def set_precond(self, kind: str):
+        """Preconditioner of the inner PCG solves: "ic" (IC(0), the reference's; the default) or
+        "line" (z-line block Jacobi, one launch per apply)."""
+        check(load().tm_submodel_set_precond(self.h, SUB_PRECONDS[kind]))
+
+    def counters(self) -> dict:
+        """Inner solves so far and their PCG iterations summed."""
+        out = np.zeros(2, np.int64)
+        check(load().tm_submodel_counters(self.h, out.ctypes.data_as(C.c_void_p)))
+        return dict(solves=int(out[0]), pcg_iters=int(out[1]))
+
     def step(self, T, dt):
         """stepTo: (converged, newton, dMax)."""
         cv = C.c_int32(); nw = C.c_int32(); dm = C.c_double()
@@ -377,7 +389,8 @@ class DeviceSubmodel:
 
 
 def run_batch(models, hist, cphi, sphi) -> list:
-    """run of several DeviceSubmodels over one history at once (tm_submodel_run_batch): a record per model."""
+    """run of several DeviceSubmodels over one history at once (tm_submodel_run_batch: every phase
+    of their Newton steps one launch over all of them): a record per model."""
     n, m, nc = len(models), len(hist["t"]), int(hist["cycles"])
     t = np.ascontiguousarray(hist["t"], np.float64); T = np.ascontiguousarray(hist["T"], np.float64)
     cyc = np.ascontiguousarray(hist["cycle"], np.int32)

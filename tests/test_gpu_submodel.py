@@ -60,18 +60,46 @@ def test_submodel_run_matches_oracle(oracle_lib):
     assert np.allclose(rg["loop"], ro["loop"], rtol=1e-5, atol=1e-9)
 
 
-def test_submodel_batch_equals_single_runs(oracle_lib):
-    """Three sites at once (concurrent streams) give each site's single-run record."""
+def _batch_specs():
+    # cells of different sizes, so the batched launches map CTAs to uneven submodels
+    return [synthetic_spec(nxy=4 + 2 * (q % 2), nz=6 + q, site=(0.3 * q, -0.2 * q), shear=1e-5 * (q + 1), seed=q) for q in range(3)]
+
+
+@pytest.mark.parametrize("precond", ["ic", "line"])
+def test_submodel_batch_equals_single_runs(precond):
+    """Three sites of different cell sizes in one batch (every Newton phase one launch over all
+    three) give each site's single-run record bit for bit, with either preconditioner."""
     from tmsolve.submodel import run_batch
     hist = cycle_history(-40.0, 125.0, 66.0, 2.0, 1)
-    specs = [synthetic_spec(nxy=4, nz=6, site=(0.3 * q, -0.2 * q), shear=1e-5 * (q + 1), seed=q) for q in range(3)]
+    specs = _batch_specs()
     cph, sph = [1.0, 0.6, 0.0], [0.0, 0.8, 1.0]
-    recs = run_batch([DeviceSubmodel(s) for s in specs], hist, cph, sph)
+    models = [DeviceSubmodel(s) for s in specs]
+    for m in models:
+        m.set_precond(precond)
+    recs = run_batch(models, hist, cph, sph)
     for q in range(3):
-        one = DeviceSubmodel(specs[q]).run(hist, cph[q], sph[q])
-        for k in ("dW", "dWdie", "dWsub", "dE", "steps", "cutbacks"):
-            assert recs[q][k] == one[k], (q, k)
-        assert np.array_equal(recs[q]["loop"], one["loop"])
+        one = DeviceSubmodel(specs[q])
+        one.set_precond(precond)
+        r1 = one.run(hist, cph[q], sph[q])
+        for k in ("dW", "dWdie", "dWsub", "dE", "steps", "cutbacks", "newtonPerStep"):
+            assert recs[q][k] == r1[k], (q, k)
+        assert np.array_equal(recs[q]["loop"], r1["loop"])
+        assert np.array_equal(models[q].u(), one.u())
+
+
+def test_submodel_line_preconditioner_matches_oracle(oracle_lib):
+    """The z-line block-Jacobi inner solves against the oracle's IC(0) ones: the inner solves stop
+    at the same relative residual, so the Newton iterates agree to the solver tolerances; the run's
+    dW, dWdie, dWsub and dE within 1e-6 relative (the submodel bar) with the same sub-steps."""
+    spec = synthetic_spec(nxy=4, nz=8)
+    hist = cycle_history(-40.0, 125.0, 33.0, 5.0, 1)
+    dm = DeviceSubmodel(spec)
+    dm.set_precond("line")
+    rg = dm.run(hist, 0.8, 0.6)
+    ro = oracle_lib.OracleSubmodel(spec).run(hist, 0.8, 0.6)
+    for k in ("dW", "dWdie", "dWsub", "dE", "dEdie", "dEsub"):
+        assert abs(rg[k] - ro[k]) <= 1e-6 * abs(ro[k]), (k, rg[k], ro[k])
+    assert rg["steps"] == ro["steps"] and rg["cutbacks"] == ro["cutbacks"]
 
 
 
