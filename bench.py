@@ -56,7 +56,7 @@ def parse():
                          "c4: 64 bump submodels of 20^3-48^3 voxels in one batch over the first history points of a "
                          "40-step -40/125 degC cycle")
     ap.add_argument("--c4-cells", type=int, default=64, help="c4: submodels in the batch")
-    ap.add_argument("--c4-points", type=int, default=6, help="c4: history points of the timed sample")
+    ap.add_argument("--c4-points", type=int, default=1, help="c4: history points of the timed sample")
     ap.add_argument("--c4-precond", default="line", choices=["line", "ic"], help="c4: inner-solve preconditioner")
     ap.add_argument("--sites", type=int, default=17424, help="screen: bump sites")
     a = ap.parse_args()

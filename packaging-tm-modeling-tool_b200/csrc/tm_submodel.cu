@@ -382,11 +382,26 @@ __global__ void k_sub_gather_rint(int ndof, const int* __restrict__ start, const
 // kind 0: a.a over the free DOFs, a.a over all (the Newton residual norms)
 // kind 1: a.b
 // kind 2: after u += du on the free DOFs: du.du over the free DOFs, u.u over all
-constexpr int SUMS_THREADS = 1024;
-__device__ __forceinline__ void sub_block_sums(int n, int kind, const double* __restrict__ a, double* __restrict__ b,
-                                               const uint8_t* __restrict__ isC, double* __restrict__ out, double* s0, double* s1) {
+// deterministic sums over n entries: the entries are cut into sums_parts(n) contiguous slices (a
+// function of n only), a CTA sums one slice by a strided loop and a fixed tree, and the slices'
+// partial sums are added in slice order; two results per call (out[0], out[1]):
+// kind 0: a.a over the free DOFs, a.a over all (the Newton residual norms)
+// kind 1: a.b
+// kind 2: after u += du on the free DOFs: du.du over the free DOFs, u.u over all
+constexpr int SUMS_THREADS = 256;
+constexpr int SUMS_SLICE = 16384;        // entries per slice, before the cap on the slice count
+constexpr int SUMS_MAXP = 64;            // slices at most
+__host__ __device__ inline int sums_parts(int n) {
+  const int p = (n + SUMS_SLICE - 1) / SUMS_SLICE;
+  return p < 1 ? 1 : (p > SUMS_MAXP ? SUMS_MAXP : p);
+}
+// slice c of n entries into part[2c], part[2c + 1]
+__device__ __forceinline__ void sub_sums_slice(int n, int c, int kind, const double* __restrict__ a, double* __restrict__ b,
+                                               const uint8_t* __restrict__ isC, double* __restrict__ part, double* s0, double* s1) {
+  const int parts = sums_parts(n), len = (n + parts - 1) / parts;
+  const int q0 = c * len, q1 = min(n, q0 + len);
   double x0 = 0, x1 = 0;
-  for (int q = threadIdx.x; q < n; q += SUMS_THREADS) {
+  for (int q = q0 + threadIdx.x; q < q1; q += SUMS_THREADS) {
     if (kind == 0) {
       const double v = a[q];
       if (!isC[q]) x0 += v * v;
@@ -404,12 +419,20 @@ __device__ __forceinline__ void sub_block_sums(int n, int kind, const double* __
     if ((int)threadIdx.x < h) { s0[threadIdx.x] += s0[threadIdx.x + h]; s1[threadIdx.x] += s1[threadIdx.x + h]; }
     __syncthreads();
   }
-  if (threadIdx.x == 0) { out[0] = s0[0]; out[1] = s1[0]; }
+  if (threadIdx.x == 0) { part[2 * c] = s0[0]; part[2 * c + 1] = s1[0]; }
 }
-__global__ void __launch_bounds__(SUMS_THREADS) k_sub_sums(int n, int kind, const double* __restrict__ a, double* __restrict__ b,
-                                                           const uint8_t* __restrict__ isC, double* __restrict__ out) {
+__device__ __forceinline__ void sub_sums_final(int n, const double* __restrict__ part, double* __restrict__ out) {
+  double x0 = 0, x1 = 0;
+  for (int c = 0; c < sums_parts(n); c++) { x0 += part[2 * c]; x1 += part[2 * c + 1]; }
+  out[0] = x0; out[1] = x1;
+}
+__global__ void __launch_bounds__(SUMS_THREADS) k_sub_sums_slice(int n, int kind, const double* __restrict__ a, double* __restrict__ b,
+                                                                 const uint8_t* __restrict__ isC, double* __restrict__ part) {
   __shared__ double s0[SUMS_THREADS], s1[SUMS_THREADS];
-  sub_block_sums(n, kind, a, b, isC, out, s0, s1);
+  sub_sums_slice(n, blockIdx.x, kind, a, b, isC, part, s0, s1);
+}
+__global__ void k_sub_sums_final(int n, const double* __restrict__ part, double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) sub_sums_final(n, part, out);
 }
 
 // _solve's scaling: s from the tangent's diagonal, the scaled copy, b = rhs s with rhs = -rint
@@ -780,6 +803,7 @@ struct SubModel {
   DBuf<uint8_t> d_isC;
   DBuf<double> d_Bm, d_Bw, d_bW, d_fields, d_u25, d_solderE, d_elas;
   DBuf<double> d_u, d_uN, d_sigE, d_eFn, d_eK, d_eF, d_fe, d_dmax, d_val, d_vals, d_s, d_rint, d_b, d_r, d_z, d_p, d_q, d_x, d_sums, d_pcg;
+  DBuf<double> d_sumPart;               // the slices' partial sums (2 per slice)
   DBuf<Point> d_pts, d_snapPts;
   DBuf<double> d_snapU, d_snapSig, d_snapFn;
   DBuf<float> d_snapOut;                // a stress snapshot (48 per element)
@@ -804,10 +828,15 @@ struct SubModel {
     if (st) cudaStreamDestroy(st);
   }
 
-  void sums(int n, int kind, const double* a, double* b, double* h) {
-    note_launch();
-    k_sub_sums<<<1, 1024, 0, st>>>(n, kind, a, b, d_isC.p, d_sums.p);
+  // the two sums of `kind` into out (device)
+  void sums_dev(int n, int kind, const double* a, double* b, double* out) {
+    note_launch(2);
+    k_sub_sums_slice<<<sums_parts(n), SUMS_THREADS, 0, st>>>(n, kind, a, b, d_isC.p, d_sumPart.p);
+    k_sub_sums_final<<<1, 32, 0, st>>>(n, d_sumPart.p, out);
     TM_CUDA_CHECK(cudaGetLastError());
+  }
+  void sums(int n, int kind, const double* a, double* b, double* h) {
+    sums_dev(n, kind, a, b, d_sums.p);
     TM_CUDA_CHECK(cudaMemcpyAsync(h, d_sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     TM_CUDA_CHECK(cudaStreamSynchronize(st));
   }
@@ -959,23 +988,22 @@ struct SubModel {
     // p.q at 4, r.r at 6; one host synchronization per iteration, for the convergence test
     double* S = d_pcg.p;
     int a = 0;
-    note_launch();
-    k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_r.p, d_z.p, d_isC.p, S + a);
+    sums_dev(ndof, 1, d_r.p, d_z.p, S + a);
     int it;
     const int nb = blocks_for(ndof, 256);
     double rr = 0;
     for (it = 1; it <= 2000; it++) {
-      note_launch(4);
+      note_launch(2);
       k_sub_spmv<<<blocks_for(nn, 128), 128, 0, st>>>(nn, d_rowPtr.p, d_col.p, d_vals.p, d_p.p, d_q.p);
-      k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_p.p, d_q.p, d_isC.p, S + 4);
+      sums_dev(ndof, 1, d_p.p, d_q.p, S + 4);
       k_sub_axpy2<<<nb, 256, 0, st>>>(ndof, S + a, S + 4, d_p.p, d_q.p, d_x.p, d_r.p);
-      k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_r.p, d_r.p, d_isC.p, S + 6);
+      sums_dev(ndof, 1, d_r.p, d_r.p, S + 6);
       TM_CUDA_CHECK(cudaMemcpyAsync(&rr, S + 6, sizeof(double), cudaMemcpyDeviceToHost, st));
       TM_CUDA_CHECK(cudaStreamSynchronize(st));
       if (std::sqrt(rr) / bn < tol) break;
       pc_apply(d_r.p, d_z.p);
-      note_launch(2);
-      k_sub_sums<<<1, 1024, 0, st>>>(ndof, 1, d_r.p, d_z.p, d_isC.p, S + (2 - a));
+      note_launch();
+      sums_dev(ndof, 1, d_r.p, d_z.p, S + (2 - a));
       k_sub_xpby<<<nb, 256, 0, st>>>(ndof, d_z.p, S + (2 - a), S + a, d_p.p);
       a = 2 - a;
     }
@@ -1359,7 +1387,7 @@ SubModel* submodel_create(const tm_submodel_spec& sp) {
   m.d_snapSig.alloc(48 * (size_t)m.ne); m.d_snapFn.alloc(24 * (size_t)m.ne);
   m.d_eK.alloc(576 * (size_t)m.ne); m.d_eF.alloc(24 * (size_t)m.ne); m.d_fe.alloc(24 * (size_t)m.ne); m.d_dmax.alloc(m.ne);
   m.d_val.alloc(9 * (size_t)m.nbk); m.d_vals.alloc(9 * (size_t)m.nbk);
-  m.d_sums.alloc(2); m.d_avg.alloc(4); m.d_pcg.alloc(8);
+  m.d_sums.alloc(2); m.d_avg.alloc(4); m.d_pcg.alloc(8); m.d_sumPart.alloc(2 * SUMS_MAXP);
   if (m.nsolderE) {
     std::vector<Point> pts(8 * (size_t)m.nsolderE);
     for (Point& p : pts) {
@@ -1447,7 +1475,7 @@ struct SubView {
   const int *conn, *eMat, *eBb, *eAn, *rowPtr, *col, *diag, *blkRow, *blkStart, *blkList, *nodeStart, *nodeList, *bNodes, *bGlob, *subBlk;
   const uint8_t* isC;
   const double *Bm, *Bw, *bW, *u25, *elas;
-  double *u, *uN, *sigE, *eFn, *eK, *eF, *fe, *dmax, *val, *vals, *s, *rint, *b, *r, *z, *p, *q, *x, *lf;
+  double *u, *uN, *sigE, *eFn, *eK, *eF, *fe, *dmax, *val, *vals, *s, *rint, *b, *r, *z, *p, *q, *x, *lf, *sumPart;
   Point* pts;
 };
 // one submodel's parameters of the current phase
@@ -1522,21 +1550,28 @@ __global__ void __launch_bounds__(256) kb_dmax(Seg g, const SubView* __restrict_
   }
   if (threadIdx.x == 0) out[sub] = red[0];
 }
-// the sums of the single engine, CTA per submodel, into out[8 sub + slot]
+// the sums of the single engine (the same slices, CTA per slice), then per submodel the slices
+// added in order into out[8 sub + slot]
 enum SumWhat { SUM_RINT, SUM_BB, SUM_RZ, SUM_PQ, SUM_RR, SUM_UPD };
-__global__ void __launch_bounds__(SUMS_THREADS) kb_sums(Seg g, const SubView* __restrict__ V, int what, double* __restrict__ out, int slot) {
+__global__ void __launch_bounds__(SUMS_THREADS) kb_sums_slice(Seg g, const SubView* __restrict__ V, int what) {
   __shared__ double s0[SUMS_THREADS], s1[SUMS_THREADS];
-  const int sub = g.sub[blockIdx.x];
+  const int sq = seg_find(g, blockIdx.x), sub = g.sub[sq];
   const SubView& v = V[sub];
-  double* o = out + 8 * sub + slot;
+  const int c = blockIdx.x - g.start[sq];
   switch (what) {
-    case SUM_RINT: sub_block_sums(v.ndof, 0, v.rint, nullptr, v.isC, o, s0, s1); break;
-    case SUM_BB: sub_block_sums(v.ndof, 1, v.b, v.b, v.isC, o, s0, s1); break;
-    case SUM_RZ: sub_block_sums(v.ndof, 1, v.r, v.z, v.isC, o, s0, s1); break;
-    case SUM_PQ: sub_block_sums(v.ndof, 1, v.p, v.q, v.isC, o, s0, s1); break;
-    case SUM_RR: sub_block_sums(v.ndof, 1, v.r, v.r, v.isC, o, s0, s1); break;
-    default: sub_block_sums(v.ndof, 2, v.x, v.u, v.isC, o, s0, s1); break;
+    case SUM_RINT: sub_sums_slice(v.ndof, c, 0, v.rint, nullptr, v.isC, v.sumPart, s0, s1); break;
+    case SUM_BB: sub_sums_slice(v.ndof, c, 1, v.b, v.b, v.isC, v.sumPart, s0, s1); break;
+    case SUM_RZ: sub_sums_slice(v.ndof, c, 1, v.r, v.z, v.isC, v.sumPart, s0, s1); break;
+    case SUM_PQ: sub_sums_slice(v.ndof, c, 1, v.p, v.q, v.isC, v.sumPart, s0, s1); break;
+    case SUM_RR: sub_sums_slice(v.ndof, c, 1, v.r, v.r, v.isC, v.sumPart, s0, s1); break;
+    default: sub_sums_slice(v.ndof, c, 2, v.x, v.u, v.isC, v.sumPart, s0, s1); break;
   }
+}
+__global__ void kb_sums_final(Seg g, const SubView* __restrict__ V, double* __restrict__ out, int slot) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  const int sub = g.sub[q];
+  sub_sums_final(V[sub].ndof, V[sub].sumPart, out + 8 * sub + slot);
 }
 __global__ void kb_scale_s(Seg g, const SubView* __restrict__ V) {
   SB_ITEM(blockDim.x);
@@ -1649,7 +1684,7 @@ struct Batch {
       v.elas = dElas.p + (size_t)s * recMax * 42;
       v.u = m.d_u.p; v.uN = m.d_uN.p; v.sigE = m.d_sigE.p; v.eFn = m.d_eFn.p; v.eK = m.d_eK.p; v.eF = m.d_eF.p; v.fe = m.d_fe.p;
       v.dmax = m.d_dmax.p; v.val = m.d_val.p; v.vals = m.d_vals.p; v.s = m.d_s.p; v.rint = m.d_rint.p; v.b = m.d_b.p; v.r = m.d_r.p;
-      v.z = m.d_z.p; v.p = m.d_p.p; v.q = m.d_q.p; v.x = m.d_x.p; v.lf = m.d_lf.p; v.pts = m.d_pts.p;
+      v.z = m.d_z.p; v.p = m.d_p.p; v.q = m.d_q.p; v.x = m.d_x.p; v.lf = m.d_lf.p; v.sumPart = m.d_sumPart.p; v.pts = m.d_pts.p;
       // the batch owns the material records: the single engine uploads its own again when next used
       m.haveKey = false;
     }
@@ -1718,9 +1753,11 @@ struct Batch {
   }
 
   void sums(const std::vector<int>& subs, int what, DBuf<double>& out, int slot) {
-    if (subs.empty()) return;
-    note_launch();
-    kb_sums<<<(int)subs.size(), SUMS_THREADS, 0, st>>>(one_each(subs), dV.p, what, out.p, slot);
+    Seg g;
+    if (!seg(g, subs, [&](int s) { return sums_parts(M[s]->ndof); }, 1)) return;
+    note_launch(2);
+    kb_sums_slice<<<g.start[g.n], SUMS_THREADS, 0, st>>>(g, dV.p, what);
+    kb_sums_final<<<1, SB_MAX, 0, st>>>(one_each(subs), dV.p, out.p, slot);
     TM_CUDA_CHECK(cudaGetLastError());
   }
   void fetch(DBuf<double>& d, std::vector<double>& h) {
