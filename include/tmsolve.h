@@ -360,6 +360,10 @@ int64_t tm_launch_count(void);
 #define TM_K_ASSEMBLE 3      /* stencil assembly (assembleStep) */
 #define TM_K_GALERKIN01 4    /* Galerkin product solid -> shell (galerkinProduct) */
 #define TM_K_APPLY_SHELL 5   /* shell-level residual (blockMatVec, b = 6) */
+#define TM_K_SETUP_LEVEL0 6  /* multigrid set-up: level-0 column factors and transfer weights (factorColumns) */
+#define TM_K_SETUP_SHELL 7   /* multigrid set-up: shell column factors, inverses and the Galerkin products between shells */
+#define TM_K_SETUP_COARSEST 8 /* multigrid set-up: banded factor and explicit inverse of the coarsest level */
+#define TM_K_TO_FP32 9       /* FP32 copies of the V-cycle's operators, factors and weights */
 /* Brackets every following launch of one kernel class with CUDA events on the context's
  * stream (kernel = -1 switches the timer off); tm_kernel_timer_read returns the launches and
  * their summed device time since, and resets them. */

@@ -91,12 +91,20 @@ double build_pc(Context& c, int kind) {
     return now_ms() - t0;
   }
   c.d_jitter.zero(c.stream);
-  launch_factor_columns(c);
-  launch_w01(c);
+  {
+    TimedLaunch tl(c, K_SETUP_LEVEL0);
+    launch_factor_columns(c);
+    launch_w01(c);
+  }
   launch_galerkin01(c);
   for (size_t l = 0; l < c.shells.size(); l++) {
     ShellLevel& L = *c.shells[l];
-    if (L.coarsest) { launch_factor_coarsest(c, L); break; }
+    if (L.coarsest) {
+      TimedLaunch tl(c, K_SETUP_COARSEST);
+      launch_factor_coarsest(c, L);
+      break;
+    }
+    TimedLaunch tl(c, K_SETUP_SHELL);
     launch_factor_shell(c, L);
     launch_galerkin_shell(c, (int)l);
   }
@@ -406,7 +414,10 @@ tm_status solve_impl(Context& c, const double* f_dev, double* u_dev, const tm_so
     rebuilt = true;
     if (mixed) {
       const double t1 = now_ms();
-      launch_to_fp32(c);
+      {
+        TimedLaunch tl(c, K_TO_FP32);
+        launch_to_fp32(c);
+      }
       autotune_vcycle32(c);
       TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
       pcMs += now_ms() - t1;

@@ -378,7 +378,10 @@ void ic_factor(IcFactor& F, const double* val, cudaStream_t st);
 void ic_apply(IcFactor& F, const double* r, double* z, cudaStream_t st);
 
 // ---- launch accounting ------------------------------------------------------------------------
-enum KernelId { K_APPLY0 = 0, K_SWEEP_SOLID = 1, K_SWEEP_SHELL = 2, K_ASSEMBLE = 3, K_GALERKIN01 = 4, K_APPLY_SHELL = 5, K_NKERNEL };
+enum KernelId {
+  K_APPLY0 = 0, K_SWEEP_SOLID = 1, K_SWEEP_SHELL = 2, K_ASSEMBLE = 3, K_GALERKIN01 = 4, K_APPLY_SHELL = 5,
+  K_SETUP_LEVEL0 = 6, K_SETUP_SHELL = 7, K_SETUP_COARSEST = 8, K_TO_FP32 = 9, K_NKERNEL
+};
 void note_launch(int count = 1);
 struct TimedLaunch {   // brackets one launch with events when the context times this kernel class
   Context& c;

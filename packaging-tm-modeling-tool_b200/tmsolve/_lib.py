@@ -31,7 +31,8 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_element_strains_adjoint", "tm_accumulate_q_adjoint", "tm_adjoint_sensitivity", "tm_set_level0", "tm_level0", "tm_clear_warm", "tm_submodel_set_precond", "tm_submodel_counters"]
 PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
 PRECOND_NAMES = {v: k for k, v in PRECONDS.items()}
-KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5)
+KERNELS = dict(apply0=0, sweep_solid=1, sweep_shell=2, assemble=3, galerkin01=4, apply_shell=5, setup_level0=6, setup_shell=7,
+               setup_coarsest=8, to_fp32=9)
 
 dp = C.POINTER(C.c_double)
 ip = C.POINTER(C.c_int32)
