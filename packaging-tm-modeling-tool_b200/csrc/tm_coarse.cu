@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
   __shared__ double Ds[CN][CN_LD];
   __shared__ double Pi[CN][CN_LD];
   __shared__ double Pj[CN][CN_LD];
+  __shared__ double Dv[CN];   // reciprocals of the factor's diagonal
   __shared__ int s_fix;
   const int w = bw + 1, tid = threadIdx.x, nthr = blockDim.x;
   const int nbk = min(CN, n - jb);
@@ -175,24 +176,35 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
   if (tid == 0) s_fix = 0;
   __syncthreads();
   if (tid < 32) {
-    // right-looking, lane i owning row i: column j is scaled once its pivot is known, then every
-    // later row subtracts its rank-1 part (independent updates instead of a serial dot per entry)
+    // right-looking in registers, lane r owning row r: column j's pivot comes from lane j, the
+    // column is scaled by the reciprocal square root, and every later row subtracts its rank-1
+    // part with the column entries of the other rows brought by shuffles (no shared-memory
+    // round trip and no division on the chain)
     const int lane = tid;
     const double jitter = jit[0];
     int fixes = 0;
-    for (int j = 0; j < nbk; j++) {
-      double d = Ds[j][j];
+    double a[CN];
+#pragma unroll
+    for (int k = 0; k < CN; k++) a[k] = Ds[lane][k];
+    double dv = 0;
+#pragma unroll
+    for (int j = 0; j < CN; j++) {
+      if (j >= nbk) break;
+      double d = __shfl_sync(0xffffffffu, a[j], j);
       if (!(d > jitter)) { d = fmax(fabs(d), jitter); fixes++; }
-      const double ljj = sqrt(d), inv = 1 / ljj;
-      __syncwarp();
-      if (lane == 0) Ds[j][j] = ljj;
-      double lij = 0;
-      if (lane > j && lane < nbk) { lij = Ds[lane][j] * inv; Ds[lane][j] = lij; }
-      __syncwarp();
-      if (lane > j && lane < nbk)
-        for (int k = j + 1; k <= lane; k++) Ds[lane][k] -= lij * Ds[k][j];
-      __syncwarp();
+      const double inv = rsqrt(d);
+      const double l = lane > j ? a[j] * inv : (lane == j ? d * inv : 0.0);
+      if (lane >= j) a[j] = l;
+      if (lane == j) dv = inv;
+#pragma unroll
+      for (int k = j + 1; k < CN; k++) {
+        const double lk = __shfl_sync(0xffffffffu, l, k);
+        if (k <= lane) a[k] -= l * lk;
+      }
     }
+#pragma unroll
+    for (int k = 0; k < CN; k++) Ds[lane][k] = (lane < nbk && k <= lane) ? a[k] : 0.0;
+    Dv[lane] = lane < nbk ? dv : 0.0;
     if (lane == 0) s_fix = fixes;
   }
   __syncthreads();
@@ -221,7 +233,7 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
 #pragma unroll
       for (int k = 0; k < CN; k++) {
         if (k >= nbk) break;
-        const double pk = p[k] / Ds[k][k];
+        const double pk = p[k] * Dv[k];
         p[k] = pk;
 #pragma unroll
         for (int t = k + 1; t < CN; t++) p[t] -= pk * Ds[t][k];
@@ -254,7 +266,7 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
         if (r >= c && r < nbk) {
           double s = (r == c) ? 1.0 : 0.0;
           for (int t = c; t < r; t++) s -= Ds[r][t] * Pj[t][c];
-          x = s / Ds[r][r];
+          x = s * Dv[r];
         }
         Pj[r][c] = x;
       }

@@ -420,15 +420,19 @@ __global__ void k_assemble_rhs(int nn, int nx, int ny, int nz, const int* __rest
   rhs[3 * n] = acc0; rhs[3 * n + 1] = acc1; rhs[3 * n + 2] = acc2;
 }
 
-// applyConstraints (09-assembly.js:445-464), one thread walking the DOFs in order (nn: the
-// row stride of the slot-major arrays)
+// applyConstraints (09-assembly.js:445-464), thread per constrained DOF (nn: the row stride of the
+// slot-major arrays). The reference walks the DOFs in order, but the result does not depend on
+// the order: a DOF's row and column entries off the diagonal are set to zero (by every DOF that
+// reaches them, all writing the same zero), and its diagonal, which no other DOF writes, is set to
+// one only if it is zero.
 __global__ void k_constraints(int nn, int ncon, const int* __restrict__ dofs, const int* __restrict__ pos, const int* __restrict__ nbr,
                               const int* __restrict__ slotMask, double* __restrict__ val, double* __restrict__ rhs,
                               uint8_t* __restrict__ isC) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  for (int t = 0; t < ncon; t++) isC[dofs[t]] = 1;
-  for (int t = 0; t < ncon; t++) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncon) return;
+  {
     const int d = dofs[t], i = d / 3, p = d % 3, pi = pos[i];
+    isC[d] = 1;
     const int mask = slotMask[i];
     for (int s = 0; s < NSLOT; s++) {
       if (!(mask >> s & 1)) continue;
@@ -1124,7 +1128,9 @@ void launch_constraints(Context& c) {
   DBuf<int> d;
   d.upload(c.constr, c.stream);
   note_launch();
-  k_constraints<<<1, 1, 0, c.stream>>>(c.nnp, (int)c.constr.size(), d.p, c.d_pos.p, c.d_nbr.p, c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
+  if (!c.constr.empty())
+    k_constraints<<<grid_for(c.constr.size(), 128), 128, 0, c.stream>>>(c.nnp, (int)c.constr.size(), d.p, c.d_pos.p, c.d_nbr.p,
+                                                                       c.d_slotMask.p, c.d_val.p, c.d_rhs.p, c.d_isC.p);
   TM_CUDA_CHECK(cudaGetLastError());
   TM_CUDA_CHECK(cudaStreamSynchronize(c.stream));
   c.isC.assign(3 * (size_t)c.nn, 0);
