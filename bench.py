@@ -544,7 +544,10 @@ def run_c3(a):
                                f"3 cycles -40/125 degC at 40 load steps per cycle", "dof": n, "precision": a.precision,
                    "l2": "working set larger than L2"},
         "analysis": {"solve_s": last["solve_s"], "table_s": last["table_s"], "screen_s": last["screen_s"],
-                     "pcg_iters": last["iters"], "solve_mdof_iter_per_s": n * last["iters"] / 1e6 / last["solve_s"],
+                     "pcg_iters": last["iters"],
+                     "solve_mdof_iter_per_s": n * last["iters"] / 1e6 / last["solve_s"] if last["iters"] else None,
+                     "warm_start": "up to 20 stored solutions (WARM_START_MAX): a step whose increment is a combination of "
+                                   "earlier ones is solved by the projection alone, in 0 PCG iterations",
                      "dW_mean": float(np.nanmean(last["dW"])), "dW_max": float(np.nanmax(last["dW"]))},
         "e2e": {"value": tot, "unit": "s per analysis", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
         "clocks": ck.summary()}))
