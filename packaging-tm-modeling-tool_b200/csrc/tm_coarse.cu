@@ -314,17 +314,7 @@ __global__ void __launch_bounds__(1024) k_band_inverse(int n, int bw, const doub
       if (r < nbk) {
         const int gr = r0 + r;
         const int kbeg = max(rs, gr - bw);
-        // two accumulators, so that two rounds of band loads are in flight
-        const double* lrow = Lb + (size_t)gr * w + bw - gr;
-        double s1 = 0;
-        int k = kbeg + part;
-#pragma unroll 4
-        for (; k + S < r0; k += 2 * S) {
-          s += lrow[k] * Y[(size_t)k * NR + c];
-          s1 += lrow[k + S] * Y[(size_t)(k + S) * NR + c];
-        }
-        if (k < r0) s += lrow[k] * Y[(size_t)k * NR + c];
-        s += s1;
+        for (int k = kbeg + part; k < r0; k += S) s += Lb[(size_t)gr * w + (k - gr + bw)] * Y[(size_t)k * NR + c];
       }
 #pragma unroll
       for (int q = S / 2; q > 0; q >>= 1) s += __shfl_down_sync(0xffffffffu, s, q, S);
@@ -346,15 +336,7 @@ __global__ void __launch_bounds__(1024) k_band_inverse(int n, int bw, const doub
       if (r < nbk) {
         const int gr = r0 + r;
         const int kend = min(n, gr + bw + 1);
-        double s1 = 0;
-        int k = r0 + nbk + part;
-#pragma unroll 4
-        for (; k + S < kend; k += 2 * S) {
-          s += Lb[(size_t)k * w + (gr - k + bw)] * Y[(size_t)k * NR + c];
-          s1 += Lb[(size_t)(k + S) * w + (gr - k - S + bw)] * Y[(size_t)(k + S) * NR + c];
-        }
-        if (k < kend) s += Lb[(size_t)k * w + (gr - k + bw)] * Y[(size_t)k * NR + c];
-        s += s1;
+        for (int k = r0 + nbk + part; k < kend; k += S) s += Lb[(size_t)k * w + (gr - k + bw)] * Y[(size_t)k * NR + c];
       }
 #pragma unroll
       for (int q = S / 2; q > 0; q >>= 1) s += __shfl_down_sync(0xffffffffu, s, q, S);
@@ -461,9 +443,7 @@ void launch_factor_coarsest(Context& c, ShellLevel& L) {
     note_launch();
   }
   TM_CUDA_CHECK(cudaGetLastError());
-  // four unit vectors per group: twice the CTAs of eight (two resident per SM), each with half the
-  // products per output
-  if (!try_band_inverse<4>(c, L) && !try_band_inverse<2>(c, L) && !try_band_inverse<1>(c, L)) {
+  if (!try_band_inverse<8>(c, L) && !try_band_inverse<4>(c, L) && !try_band_inverse<2>(c, L) && !try_band_inverse<1>(c, L)) {
     k_band_inverse_warp<<<grid_for(n, 4), 128, 0, c.stream>>>(n, bw, L.d_bandL.p, L.d_inv.p);
     note_launch();
   }
