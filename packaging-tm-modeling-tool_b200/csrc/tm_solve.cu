@@ -330,24 +330,23 @@ __global__ void __launch_bounds__(TM_PANEL_THREADS, PanelMinBlocks<T>::value)
   }
 }
 
-// restriction 0 -> 1: rc = P^T res, thread per aggregate over its member nodes (ascending)
+// restriction 0 -> 1: rc = P^T res, thread per (aggregate, component) over the aggregate's member
+// nodes (ascending): the six threads of an aggregate share the members' residual loads and read
+// adjacent weights, and each sums its component in the same order as a thread per aggregate would
 template <class T>
 __global__ void k_restrict0(int na, const int* __restrict__ aggPtr, const int* __restrict__ aggNodes, const T* __restrict__ W,
                             const T* __restrict__ res, T* __restrict__ rc, T* __restrict__ xc) {
-  const int I = blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= na) return;
-#pragma unroll
-  for (int a = 0; a < 6; a++) xc[6 * (size_t)I + a] = 0;   // the level's iterate starts at zero
-  T acc[6] = {0, 0, 0, 0, 0, 0};
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= 6 * (size_t)na) return;
+  const int I = (int)(t / 6), a = (int)(t % 6);
+  xc[t] = 0;   // the level's iterate starts at zero
+  T acc = 0;
   for (int q = aggPtr[I]; q < aggPtr[I + 1]; q++) {
     const int f = aggNodes[q];
     const T* w = W + 18 * (size_t)f;
-    const T r0 = res[3 * f], r1 = res[3 * f + 1], r2 = res[3 * f + 2];
-#pragma unroll
-    for (int a = 0; a < 6; a++) acc[a] += w[a] * r0 + w[6 + a] * r1 + w[12 + a] * r2;
+    acc += w[a] * res[3 * f] + w[6 + a] * res[3 * f + 1] + w[12 + a] * res[3 * f + 2];
   }
-#pragma unroll
-  for (int a = 0; a < 6; a++) rc[6 * (size_t)I + a] = acc[a];
+  rc[t] = acc;
 }
 
 // prolongation 1 -> 0: x += P ec, thread per node
@@ -742,8 +741,8 @@ void vcycle(Context& c, const T* r, T* z) {
     }
   }
   ShellLevel& L1 = *c.shells[0];
-  k_restrict0<T><<<grid_for(L1.nn, 128), 128, 0, st>>>(L1.nn, c.d_aggPtr.p, c.d_aggNodes.p, B::W01(c), B::res0(c), B::b(L1),
-                                                                  B::x(L1));
+  k_restrict0<T><<<grid_for(6 * (size_t)L1.nn, 192), 192, 0, st>>>(L1.nn, c.d_aggPtr.p, c.d_aggNodes.p, B::W01(c), B::res0(c),
+                                                                     B::b(L1), B::x(L1));
   note_launch();
   const size_t nl = c.shells.size();
   for (size_t l = 0; l < nl; l++) {
