@@ -23,6 +23,32 @@ constexpr int RED_THREADS = 256;
 
 inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
 
+// Programmatic dependent launch. A grid launched by launch_pdl may start while the previous
+// kernel of the stream drains: it first reads only data that no kernel of the V-cycle writes
+// (operator blocks, ids, inverses), then waits in grid_dep_wait until every earlier kernel has
+// completed and its writes are visible (a no-op in a grid launched without the attribute).
+// grid_dep_launch lets the next such grid start once every CTA of this one has issued it.
+// The wait does not clear the SM's L1, which CTAs of the earlier grids running on the same SM
+// may have filled with lines that other SMs wrote since: what earlier kernels write (iterates,
+// right-hand sides) is read after the wait with ld.global.cg (L2, the point of coherence).
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+template <class... KArgs, class... Args>
+void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  TM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
 // ---- level-0 stencil apply: y = K x or y = b - K x over the positions p0 .. p1-1 -------------
 // nn positions, slot-major arrays of row stride `stride`. Absent stencil slots hold exact zeros,
 // so they read the node's own x (branch-free). NPT = 1:
@@ -336,6 +362,7 @@ __global__ void __launch_bounds__(TM_PANEL_THREADS, PanelMinBlocks<T>::value)
 template <class T>
 __global__ void k_restrict0(int na, const int* __restrict__ aggPtr, const int* __restrict__ aggNodes, const T* __restrict__ W,
                             const T* __restrict__ res, T* __restrict__ rc, T* __restrict__ xc) {
+  grid_dep_launch();
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= 6 * (size_t)na) return;
   const int I = (int)(t / 6), a = (int)(t % 6);
@@ -412,42 +439,63 @@ __host__ __device__ inline size_t shell_sweep_bytes(int maxm, int maxBlk, bool s
 }
 
 // residual rows r = b - K x of the column whose aggregates are n0 .. n0+na-1 (blocks k0 ..
-// k0+nblk-1), by one warp: the
-// lanes take the column's blocks (all rows together), each lane's 6 products of a block land in
-// shared memory, and lane e then subtracts its row's block sums in block order, as the serial
-// row loop of columnSweep (10-solver.js:535-553) does. A lane's blocks are taken SH_BPL at a time:
-// first all their column indices, then all their neighbour values, then the block values and the
-// products, so that each of these steps is one round of loads rather than one per block.
+// k0+nblk-1), by one warp: the lanes take the column's blocks (all rows together), each lane's 6
+// products of a block land in shared memory, and lane e then subtracts its row's block sums in
+// block order, as the serial row loop of columnSweep (10-solver.js:535-553) does. A lane's blocks
+// are taken SH_BPL at a time: first all their column indices, then all their neighbour values,
+// then the block values and the products, so that each of these steps is one round of loads
+// rather than one per block.
+//
+// Two parts. shell_column_static reads what the V-cycle never writes: the local row starts, the
+// first round of block column indices (cj0) and an L2 prefetch of the first round's blocks; it
+// runs before the grid-dependency wait. shell_column_residual runs after it (b and x).
 constexpr int SH_BPL = 4;
 template <class T>
-__device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, int k0, int nblk, const int* __restrict__ rowPtr,
-                                                      const int* __restrict__ col, const T* __restrict__ val,
-                                                      const T* __restrict__ b, const T* __restrict__ x, bool zeroGuess,
-                                                      T* part, T* r, int* rp) {
+__device__ __forceinline__ void shell_column_static(int lane, int n0, int na, int k0, int nblk, const int* __restrict__ rowPtr,
+                                                    const int* __restrict__ col, const T* __restrict__ val, bool zeroGuess,
+                                                    int* rp, int (&cj0)[SH_BPL]) {
+#pragma unroll
+  for (int u = 0; u < SH_BPL; u++) cj0[u] = -1;
+  if (zeroGuess) return;
+  for (int q = lane; q <= na; q += 32) rp[q] = rowPtr[n0 + q] - k0;
+#pragma unroll
+  for (int u = 0; u < SH_BPL; u++) {
+    const int e = lane + 32 * u;
+    if (e < nblk) {
+      cj0[u] = col[k0 + e];
+      const char* blk = reinterpret_cast<const char*>(val + 36 * (size_t)(k0 + e));
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(blk));
+      asm volatile("prefetch.global.L2 [%0];\n" ::"l"(blk + 36 * sizeof(T) - 1));
+    }
+  }
+}
+template <class T>
+__device__ __forceinline__ void shell_column_residual(int lane, int n0, int na, int k0, int nblk, const int* __restrict__ col,
+                                                      const T* __restrict__ val, const T* __restrict__ b, const T* __restrict__ x,
+                                                      bool zeroGuess, const int (&cj0)[SH_BPL], T* part, T* r, const int* rp) {
   const int m = 6 * na;
   // the column's b is loaded with the block rows, not after them
   const T* bc = b + 6 * (size_t)n0;
-  const T bo0 = lane < m ? bc[lane] : (T)0, bo1 = lane + 32 < m ? bc[lane + 32] : (T)0;
-  auto bval = [&](int e) { return e == lane ? bo0 : e == lane + 32 ? bo1 : bc[e]; };
+  const T bo0 = lane < m ? __ldcg(bc + lane) : (T)0, bo1 = lane + 32 < m ? __ldcg(bc + lane + 32) : (T)0;
+  auto bval = [&](int e) { return e == lane ? bo0 : e == lane + 32 ? bo1 : __ldcg(bc + e); };
   if (zeroGuess) {
     for (int e = lane; e < m; e += 32) r[e] = bval(e);
     __syncwarp();
     return;
   }
-  for (int q = lane; q <= na; q += 32) rp[q] = rowPtr[n0 + q] - k0;
   for (int e0 = 0; e0 < nblk; e0 += 32 * SH_BPL) {
     int cj[SH_BPL];
 #pragma unroll
     for (int u = 0; u < SH_BPL; u++) {
       const int e = e0 + lane + 32 * u;
-      cj[u] = e < nblk ? col[k0 + e] : -1;
+      cj[u] = e0 == 0 ? cj0[u] : e < nblk ? col[k0 + e] : -1;
     }
     T xv[SH_BPL][6];
 #pragma unroll
     for (int u = 0; u < SH_BPL; u++) {
       const T* xj = x + 6 * (size_t)(cj[u] < 0 ? 0 : cj[u]);
 #pragma unroll
-      for (int q = 0; q < 6; q++) xv[u][q] = cj[u] >= 0 ? xj[q] : (T)0;
+      for (int q = 0; q < 6; q++) xv[u][q] = cj[u] >= 0 ? __ldcg(xj + q) : (T)0;
     }
 #pragma unroll
     for (int u = 0; u < SH_BPL; u++) {
@@ -480,9 +528,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 // x_col += A_cc^-1 r with the explicit inverse Ai (entry (e, k) at k*m + e). The inverse reaches the
 // lanes before the residual is done: rows of at most SH_PRE entries in registers, larger blocks
 // copied asynchronously into the warp's shared memory (aiSm, when the level's blocks fit there) and
-// otherwise read from global memory after it. Every lane fetches its entries of the column's own x
-// before the residual too: no other warp writes this column's x during the launch (a colour's
-// columns do not couple), and this warp writes it only at the end.
+// otherwise read from global memory after it. The inverse, the row starts and the first block
+// columns are read before the grid-dependency wait (no kernel of the V-cycle writes them); b and x
+// after it. Every lane fetches its entries of the column's own x right after the wait: no other
+// warp writes this column's x during the launch (a colour's columns do not couple), and this warp
+// writes it only at the end.
 template <class T>
 __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* __restrict__ Ai, const int* __restrict__ rowPtr,
                                                    const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ b,
@@ -499,9 +549,12 @@ __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* _
     for (int q = lane; q < pieces; q += 32) cp_async16(reinterpret_cast<unsigned char*>(aiSm) + 16 * q, reinterpret_cast<const unsigned char*>(Ai) + 16 * q);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
+  int cj0[SH_BPL];
+  shell_column_static(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, zeroGuess, rp, cj0);
+  grid_dep_wait();
   T* xc = x + 6 * (size_t)n0;
-  const T xo0 = lane < m ? xc[lane] : (T)0, xo1 = lane + 32 < m ? xc[lane + 32] : (T)0;
-  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, zeroGuess, part, r, rp);
+  const T xo0 = lane < m ? __ldcg(xc + lane) : (T)0, xo1 = lane + 32 < m ? __ldcg(xc + lane + 32) : (T)0;
+  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, col, val, b, x, zeroGuess, cj0, part, r, rp);
   if (pre) {
     if (lane < m) {
       T acc = 0;
@@ -522,17 +575,19 @@ __device__ __forceinline__ void shell_sweep_column(int lane, int4 mt, const T* _
     T acc = 0;
 #pragma unroll 6
     for (int k = 0; k < m; k++) acc += A[(size_t)k * m + e] * r[k];
-    xc[e] = (e == lane ? xo0 : e == lane + 32 ? xo1 : xc[e]) + acc;
+    xc[e] = (e == lane ? xo0 : e == lane + 32 ? xo1 : __ldcg(xc + e)) + acc;
   }
 }
 
 // shell-level residual res = b - K x over all columns, warp per column (meta: first and
-// one-past-last aggregate and block of every column)
+// one-past-last aggregate and block of every column); launched with a programmatic dependency on
+// the level's last sweep
 template <class T>
 __global__ void __launch_bounds__(256) k_apply_shell(int ncol, const int4* __restrict__ meta, const int* __restrict__ rowPtr,
                                                      const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ x,
                                                      const T* __restrict__ b, T* __restrict__ y, int maxm, int maxBlk) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  grid_dep_launch();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x * (blockDim.x >> 5) + warp;
   if (c >= ncol) return;
@@ -542,20 +597,25 @@ __global__ void __launch_bounds__(256) k_apply_shell(int ncol, const int4* __res
   int* rp = reinterpret_cast<int*>(r + (maxm > SH_PRE ? maxm : SH_PRE));
   const int4 mt = meta[c];
   const int n0 = mt.x, na = mt.y - mt.x;
-  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, b, x, false, part, r, rp);
+  int cj0[SH_BPL];
+  shell_column_static(lane, n0, na, mt.z, mt.w - mt.z, rowPtr, col, val, false, rp, cj0);
+  grid_dep_wait();
+  shell_column_residual(lane, n0, na, mt.z, mt.w - mt.z, col, val, b, x, false, cj0, part, r, rp);
   for (int e = lane; e < 6 * na; e += 32) y[6 * (size_t)n0 + e] = r[e];
 }
 
 // shell-level column sweep, warp per column of one colour (columnSweep shell branch,
 // 10-solver.js:535-553): r = b - K x over the column's rows, then x_col += A_cc^-1 r with the
 // explicit inverse of the column block. The colour's column list carries each column's aggregate
-// and block ranges and the offset of its inverse (one load).
+// and block ranges and the offset of its inverse (one load). Launched with a programmatic
+// dependency on the previous kernel, so its reads of the column structure overlap that kernel.
 template <class T>
 __global__ void __launch_bounds__(256) k_sweep_shell(int ncolc, const int4* __restrict__ meta, const long long* __restrict__ cfOff,
                                                      const int* __restrict__ rowPtr, const int* __restrict__ col,
                                                      const T* __restrict__ val, const T* __restrict__ cf, const T* __restrict__ b,
                                                      T* __restrict__ x, int maxm, int maxBlk, int zeroGuess, int stageAi) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  grid_dep_launch();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * (blockDim.x >> 5) + warp;
   if (gw >= ncolc) return;
@@ -571,6 +631,7 @@ __global__ void __launch_bounds__(256) k_sweep_shell(int ncolc, const int4* __re
 template <class T>
 __global__ void k_restrict_shell(int nnc, const int* __restrict__ chPtr, const int* __restrict__ chIdx, const int* __restrict__ chW,
                                  const T* __restrict__ W, const T* __restrict__ res, T* __restrict__ rc, T* __restrict__ xc) {
+  grid_dep_launch();
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= 6 * (size_t)nnc) return;
   xc[t] = 0;   // the coarse level's iterate starts at zero
@@ -589,6 +650,7 @@ __global__ void k_restrict_shell(int nnc, const int* __restrict__ chPtr, const i
 template <class T>
 __global__ void k_prolong_shell(int nnf, const int* __restrict__ prolPtr, const int* __restrict__ prolIdx, const T* __restrict__ W,
                                 const T* __restrict__ ec, T* __restrict__ x) {
+  grid_dep_launch();
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= 6 * (size_t)nnf) return;
   const int f = (int)(t / 6), p = (int)(t % 6);
@@ -718,9 +780,9 @@ void vcycle(Context& c, const T* r, T* z) {
     const size_t per = shell_sweep_bytes<T>(L.maxm, L.maxColBlocks, sai);
     const int wpb = wpbS(L);
     TimedLaunch tl(c, K_SWEEP_SHELL);
-    k_sweep_shell<T><<<grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st>>>(L.colorCount[col], L.d_colorMeta[col].p,
-        (const long long*)L.d_colorCf[col].p, L.d_rowPtr.p, L.d_col.p, B::val(L), B::cf(L), B::b(L), B::x(L), L.maxm, L.maxColBlocks, zero,
-        sai ? 1 : 0);
+    launch_pdl(k_sweep_shell<T>, grid_for(L.colorCount[col], wpb), 32 * wpb, wpb * per, st, L.colorCount[col],
+               (const int4*)L.d_colorMeta[col].p, (const long long*)L.d_colorCf[col].p, (const int*)L.d_rowPtr.p, (const int*)L.d_col.p,
+               (const T*)B::val(L), (const T*)B::cf(L), (const T*)B::b(L), B::x(L), L.maxm, L.maxColBlocks, zero, sai ? 1 : 0);
     note_launch();
   };
   // ---- level 0 pre-smoothing: 2 sweeps in colours 0..3
@@ -764,8 +826,9 @@ void vcycle(Context& c, const T* r, T* z) {
       TimedLaunch tl(c, K_APPLY_SHELL);
       const int ncol = L.nx * L.ny;
       const int wpb = wpbA(L);
-      k_apply_shell<T><<<grid_for(ncol, wpb), 32 * wpb, wpb * shell_stage_bytes<T>(L.maxm, L.maxColBlocks), st>>>(ncol, L.d_colMeta.p,
-          L.d_rowPtr.p, L.d_col.p, B::val(L), B::x(L), B::b(L), B::res(L), L.maxm, L.maxColBlocks);
+      launch_pdl(k_apply_shell<T>, grid_for(ncol, wpb), 32 * wpb, wpb * shell_stage_bytes<T>(L.maxm, L.maxColBlocks), st, ncol,
+                 (const int4*)L.d_colMeta.p, (const int*)L.d_rowPtr.p, (const int*)L.d_col.p, (const T*)B::val(L), (const T*)B::x(L),
+                 (const T*)B::b(L), B::res(L), L.maxm, L.maxColBlocks);
       note_launch();
     }
     ShellLevel& C = *c.shells[l + 1];
