@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "tm_internal.h"
+#include "tm_pdl.cuh"
 
 namespace tmg {
 
@@ -22,32 +23,6 @@ constexpr int RED_BLOCKS = 592;   // 4 x 148 SMs
 constexpr int RED_THREADS = 256;
 
 inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
-
-// Programmatic dependent launch. A grid launched by launch_pdl may start while the previous
-// kernel of the stream drains: it first reads only data that no kernel of the V-cycle writes
-// (operator blocks, ids, inverses), then waits in grid_dep_wait until every earlier kernel has
-// completed and its writes are visible (a no-op in a grid launched without the attribute).
-// grid_dep_launch lets the next such grid start once every CTA of this one has issued it.
-// The wait does not clear the SM's L1, which CTAs of the earlier grids running on the same SM
-// may have filled with lines that other SMs wrote since: what earlier kernels write (iterates,
-// right-hand sides) is read after the wait with ld.global.cg (L2, the point of coherence).
-__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-
-template <class... KArgs, class... Args>
-void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  TM_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kern, args...));
-}
 
 // ---- level-0 stencil apply: y = K x or y = b - K x over the positions p0 .. p1-1 -------------
 // nn positions, slot-major arrays of row stride `stride`. Absent stencil slots hold exact zeros,
@@ -379,6 +354,7 @@ __global__ void k_restrict0(int na, const int* __restrict__ aggPtr, const int* _
 // prolongation 1 -> 0: x += P ec, thread per node
 template <class T>
 __global__ void k_prolong0(int nn, const int* __restrict__ nodeAgg, const T* __restrict__ W, const T* __restrict__ ec, T* __restrict__ x) {
+  grid_dep_launch();
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nn) return;
   const int a = nodeAgg[n];
