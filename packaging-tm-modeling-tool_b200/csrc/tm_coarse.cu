@@ -32,6 +32,7 @@
 #include <algorithm>
 
 #include "tm_internal.h"
+#include "tm_pdl.cuh"
 
 namespace tmg {
 
@@ -39,6 +40,7 @@ namespace {
 
 constexpr int CN = 32;          // block size of the blocked factor
 constexpr int CN_LD = CN + 1;   // padded shared-memory row
+constexpr int CHOL_THREADS = 256;
 
 inline int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
 
@@ -154,16 +156,21 @@ __global__ void k_band_jitter(int n, int bw, const double* __restrict__ A, doubl
   }
 }
 
-// one block column jb .. jb+nbk-1 of the blocked band Cholesky (see the file comment)
-__global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, double* __restrict__ A, double* __restrict__ Lb,
-                                                        double* __restrict__ Dinv, const double* __restrict__ jit,
-                                                        int* __restrict__ jitterCount) {
+// one block column jb .. jb+nbk-1 of the blocked band Cholesky (see the file comment). Launched
+// with a programmatic dependency on the previous step (its launch overlaps that step); the working
+// band is read through L2 after the wait (tm_pdl.cuh).
+__global__ void __launch_bounds__(CHOL_THREADS) k_band_chol_step(int n, int bw, int jb, double* __restrict__ A, double* __restrict__ Lb,
+                                                                 double* __restrict__ Dinv, const double* __restrict__ jit,
+                                                                 int* __restrict__ jitterCount) {
   __shared__ double Ds[CN][CN_LD];
   __shared__ double Pi[CN][CN_LD];
   __shared__ double Pj[CN][CN_LD];
   __shared__ double Dv[CN];   // reciprocals of the factor's diagonal
   __shared__ int s_fix;
-  const int w = bw + 1, tid = threadIdx.x, nthr = blockDim.x;
+  grid_dep_launch();
+  grid_dep_wait();
+  const int w = bw + 1, tid = threadIdx.x;
+  constexpr int nthr = CHOL_THREADS;
   const int nbk = min(CN, n - jb);
   const int i0 = jb + nbk, R = min(n, jb + nbk + bw) - i0;
   int ti = 0, tj = blockIdx.x;
@@ -171,22 +178,23 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
   // 1. the diagonal block and its factor (warp 0; the same arithmetic in every CTA)
   for (int e = tid; e < CN * CN; e += nthr) {
     const int r = e / CN, cc = e % CN;
-    Ds[r][cc] = (r < nbk && cc <= r && r - cc <= bw) ? A[(size_t)(jb + r) * w + (cc - r + bw)] : 0.0;
+    Ds[r][cc] = (r < nbk && cc <= r && r - cc <= bw) ? __ldcg(A + (size_t)(jb + r) * w + (cc - r + bw)) : 0.0;
   }
   if (tid == 0) s_fix = 0;
   __syncthreads();
+  // lane r of warp 0 owns row r of the diagonal block through step 2 (its factor row in a[])
+  double a[CN];
+  double dv = 0;
   if (tid < 32) {
     // right-looking in registers, lane r owning row r: column j's pivot comes from lane j, the
     // column is scaled by the reciprocal square root, and every later row subtracts its rank-1
     // part with the column entries of the other rows brought by shuffles (no shared-memory
     // round trip and no division on the chain)
     const int lane = tid;
-    const double jitter = jit[0];
+    const double jitter = __ldcg(jit);
     int fixes = 0;
-    double a[CN];
 #pragma unroll
     for (int k = 0; k < CN; k++) a[k] = Ds[lane][k];
-    double dv = 0;
 #pragma unroll
     for (int j = 0; j < CN; j++) {
       if (j >= nbk) break;
@@ -210,20 +218,21 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
   __syncthreads();
   // 2. panel rows of the tiles ti and tj: first the rows of A (all threads, zero outside the
   //    band and the window), then P[r][k] = (A[g][jb+k] - sum_t<k P[r][t] L[k][t]) / L[k][k],
-  //    thread per row, in shared memory
+  //    thread per row (warps 2 and 3), in shared memory. Meanwhile warp 0 of CTA 0 forms the
+  //    inverse of the diagonal block from the rows it holds.
   for (int e = tid; e < 2 * CN * CN; e += nthr) {
     const int which = e / (CN * CN), r = (e / CN) % CN, k = e % CN;
     if (which == 1 && ti == tj) continue;
     const int tile = which ? tj : ti;
     const int g = i0 + tile * CN + r, kk = jb + k;
-    double a = 0;
-    if (tile * CN + r < R && k < nbk && g - kk <= bw) a = A[(size_t)g * w + (kk - g + bw)];
-    (which ? Pj : Pi)[r][k] = a;
+    double v = 0;
+    if (tile * CN + r < R && k < nbk && g - kk <= bw) v = __ldcg(A + (size_t)g * w + (kk - g + bw));
+    (which ? Pj : Pi)[r][k] = v;
   }
   __syncthreads();
-  if (tid < 64) {
+  if (tid >= 64 && tid < 128) {
     // right-looking in registers: P[k] is final once the columns before it are subtracted
-    const int which = tid >> 5, r = tid & 31;
+    const int which = (tid - 64) >> 5, r = tid & 31;
     const int tile = which ? tj : ti;
     double* P = which ? &Pj[r][0] : &Pi[r][0];
     if (!(which == 1 && ti == tj) && tile * CN + r < R) {
@@ -242,9 +251,29 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
       for (int k = 0; k < CN; k++) if (k < nbk) P[k] = p[k];
     }
   }
+  if (blockIdx.x == 0 && tid < 32) {
+    // column `lane` of L_D^-1 (lower triangular), right-looking: x starts as e_lane, x[k] is
+    // final once scaled by 1/L[k][k], and every later x[t] then subtracts L[t][k] x[k] (a[k] of
+    // lane t). Each x[t] thus subtracts its terms in the order k = lane, lane+1, ..., t-1.
+    const int lane = tid;
+    double xv[CN];
+#pragma unroll
+    for (int r = 0; r < CN; r++) xv[r] = r == lane ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < CN; k++) {
+      if (k >= nbk) break;
+      const double xk = xv[k] * __shfl_sync(0xffffffffu, dv, k);
+      xv[k] = xk;
+#pragma unroll
+      for (int t = k + 1; t < CN; t++) xv[t] -= __shfl_sync(0xffffffffu, a[k], t) * xk;
+    }
+    double* Db = Dinv + (size_t)(jb / CN) * CN * CN;
+#pragma unroll
+    for (int r = 0; r < CN; r++) Db[r * CN + lane] = (r >= lane && r < nbk) ? xv[r] : 0.0;
+  }
   __syncthreads();
-  // 3. stores of the factor: panel rows by the diagonal tiles, the diagonal block, its inverse and
-  //    the pivot fixes by CTA 0
+  // 3. stores of the factor: panel rows by the diagonal tiles, the diagonal block and the pivot
+  //    fixes by CTA 0
   if (ti == tj) {
     for (int e = tid; e < CN * CN; e += nthr) {
       const int r = e / CN, k = e % CN;
@@ -257,35 +286,151 @@ __global__ void __launch_bounds__(256) k_band_chol_step(int n, int bw, int jb, d
       const int r = e / CN, cc = e % CN;
       if (r < nbk && cc <= r && r - cc <= bw) Lb[(size_t)(jb + r) * w + (cc - r + bw)] = Ds[r][cc];
     }
-    // column c of the inverse of the diagonal block (lower triangular), thread per column; Pj is
-    // free in CTA 0 (its tile pair is (0, 0)) and holds the columns
-    if (tid < CN) {
-      const int c = tid;
-      for (int r = 0; r < CN; r++) {
-        double x = 0;
-        if (r >= c && r < nbk) {
-          double s = (r == c) ? 1.0 : 0.0;
-          for (int t = c; t < r; t++) s -= Ds[r][t] * Pj[t][c];
-          x = s * Dv[r];
-        }
-        Pj[r][c] = x;
+    if (tid == 0 && s_fix) atomicAdd(jitterCount, s_fix);
+  }
+  // 4. trailing update of the tile (ti, tj): thread per column cc and four rows rb + 8q, the four
+  //    dot products interleaved (each in the order k = 0 .. nbk-1)
+  const double(*PJ)[CN_LD] = (ti == tj) ? Pi : Pj;
+  static_assert(CHOL_THREADS == 8 * CN, "four rows per thread");
+  {
+    const int cc = tid % CN, rb = tid / CN;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < nbk; k++) {
+      const double pj = PJ[cc][k];
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] += Pi[rb + 8 * q][k] * pj;
+    }
+    const int gk = i0 + tj * CN + cc;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int r = rb + 8 * q, gi = i0 + ti * CN + r;
+      if (ti * CN + r < R && tj * CN + cc < R && gk <= gi && gi - gk <= bw) {
+        double* ap = A + (size_t)gi * w + (gk - gi + bw);
+        *ap = __ldcg(ap) - acc[q];
+      }
+    }
+  }
+}
+
+// the factor's band transposed: Lt[i*w + d] = L[i+d][i] (d = 0 .. bw; zero past the last row)
+__global__ void k_band_transpose(int n, int bw, const double* __restrict__ Lb, double* __restrict__ Lt) {
+  const int w = bw + 1;
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * w) return;
+  const int i = (int)(t / w), d = (int)(t % w);
+  Lt[t] = i + d < n ? Lb[(size_t)(i + d) * w + (bw - d)] : 0.0;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// Explicit inverse from the blocked factor with the band rows staged in shared memory. The same
+// substitutions as k_band_inverse (forward with L, backward with L^T, groups of NR unit vectors,
+// pairs g, G-1-g per CTA), but each block step reads its 32 band rows (of L forward, of L^T
+// backward: both contiguous, Lb + r0*w and Lt + r0*w) and the diagonal block's inverse from a
+// shared-memory buffer that cp.async filled while the previous block step computed: the
+// substitution chain waits on no L2 round trip. The buffers and Y take
+// 2 * (32 w + 1024) + (n + 32) NR doubles (the launcher checks the fit).
+template <int NR>
+__global__ void __launch_bounds__(1024) k_band_inverse_staged(int n, int bw, const double* __restrict__ Lb, const double* __restrict__ Lt,
+                                                              const double* __restrict__ Dinv, int ngroups, double* __restrict__ inv) {
+  constexpr int S = 32 / NR;   // partial sums per output
+  extern __shared__ __align__(16) double sms[];
+  const int w = bw + 1, tid = threadIdx.x;
+  const size_t bufLen = ((size_t)CN * w + CN * CN + 1) & ~(size_t)1;   // 16-byte multiple
+  double* buf[2] = {sms, sms + bufLen};
+  double* Y = sms + 2 * bufLen;       // n x NR, row-major
+  double* Z = Y + (size_t)n * NR;     // CN x NR
+  const int o = tid / S, part = tid % S;   // output (r, c) and its part
+  const int r = o / NR, c = o % NR;        // blockDim = CN * NR * S = 1024
+  const int nblk = (n + CN - 1) / CN;
+  // block b's band rows (of L or of L^T) and its diagonal inverse into buf[b & 1]; every copy is
+  // 16 bytes between 16-byte boundaries (row blocks start at multiples of 32 w doubles); the last
+  // block's rows are rounded up to 16 bytes, which stays inside the band's allocation padding
+  auto stage = [&](int b, const double* band) {
+    double* dst = buf[b & 1];
+    const int rows = min(CN, n - b * CN);
+    const int pieces = (int)(((size_t)rows * w * sizeof(double) + 15) / 16);
+    const double* src = band + (size_t)b * CN * w;
+    for (int q = tid; q < pieces; q += blockDim.x) cp_async16(dst + 2 * q, src + 2 * q);
+    const double* db = Dinv + (size_t)b * CN * CN;
+    for (int q = tid; q < CN * CN / 2; q += blockDim.x) cp_async16(dst + (size_t)CN * w + 2 * q, db + 2 * q);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  auto noStage = [] { asm volatile("cp.async.commit_group;\n" ::: "memory"); };
+  auto waitStaged = [] { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); };
+  for (int pass = 0; pass < 2; pass++) {
+    const int g = pass == 0 ? (int)blockIdx.x : ngroups - 1 - (int)blockIdx.x;
+    if (pass == 1 && g <= (int)blockIdx.x) break;
+    const int j0 = g * NR, nr = min(NR, n - j0);
+    const int b0 = j0 / CN, rs = b0 * CN;
+    // forward: Y = L^-1 E on rows rs .. n-1
+    stage(b0, Lb);
+    for (int b = b0; b < nblk; b++) {
+      if (b + 1 < nblk) stage(b + 1, Lb); else noStage();
+      waitStaged();
+      __syncthreads();
+      const double* Lr = buf[b & 1];
+      const double* Db = Lr + (size_t)CN * w;
+      const int r0 = b * CN, nbk = min(CN, n - r0);
+      double sacc = 0;
+      if (r < nbk) {
+        const int gr = r0 + r;
+        const int kbeg = max(rs, gr - bw);
+        for (int k = kbeg + part; k < r0; k += S) sacc += Lr[(size_t)r * w + (k - gr + bw)] * Y[(size_t)k * NR + c];
+      }
+#pragma unroll
+      for (int q = S / 2; q > 0; q >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, q, S);
+      if (part == 0) Z[r * NR + c] = (r < nbk ? ((r0 + r == j0 + c && c < nr) ? 1.0 : 0.0) : 0.0) - sacc;
+      __syncthreads();
+      double y = 0;
+      if (r < nbk)
+        for (int t = part; t <= r; t += S) y += Db[r * CN + t] * Z[t * NR + c];
+#pragma unroll
+      for (int q = S / 2; q > 0; q >>= 1) y += __shfl_down_sync(0xffffffffu, y, q, S);
+      if (part == 0 && r < nbk) Y[(size_t)(r0 + r) * NR + c] = y;
+      __syncthreads();   // the buffer is refilled two steps on
+    }
+    // backward: X = L^-T Y on rows n-1 .. rs (X overwrites Y block by block)
+    stage(nblk - 1, Lt);
+    for (int b = nblk - 1; b >= b0; b--) {
+      if (b - 1 >= b0) stage(b - 1, Lt); else noStage();
+      waitStaged();
+      __syncthreads();
+      const double* Ur = buf[b & 1];
+      const double* Db = Ur + (size_t)CN * w;
+      const int r0 = b * CN, nbk = min(CN, n - r0);
+      double sacc = 0;
+      if (r < nbk) {
+        const int gr = r0 + r;
+        const int kend = min(n, gr + bw + 1);
+        for (int k = r0 + nbk + part; k < kend; k += S) sacc += Ur[(size_t)r * w + (k - gr)] * Y[(size_t)k * NR + c];
+      }
+#pragma unroll
+      for (int q = S / 2; q > 0; q >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, q, S);
+      if (part == 0) Z[r * NR + c] = (r < nbk ? Y[(size_t)(r0 + r) * NR + c] : 0.0) - sacc;
+      __syncthreads();
+      double x = 0;
+      if (r < nbk)
+        for (int t = r + part; t < nbk; t += S) x += Db[t * CN + r] * Z[t * NR + c];
+#pragma unroll
+      for (int q = S / 2; q > 0; q >>= 1) x += __shfl_down_sync(0xffffffffu, x, q, S);
+      if (part == 0 && r < nbk) Y[(size_t)(r0 + r) * NR + c] = x;
+      __syncthreads();
+    }
+    // rows i >= j of column j = j0 + cc, on both sides of the diagonal
+    for (size_t e = tid; e < (size_t)(n - rs) * NR; e += blockDim.x) {
+      const int i = rs + (int)(e / NR), cc = (int)(e % NR);
+      const int j = j0 + cc;
+      if (cc < nr && i >= j) {
+        const double v = Y[e + (size_t)rs * NR];
+        inv[(size_t)i * n + j] = v;
+        inv[(size_t)j * n + i] = v;
       }
     }
     __syncthreads();
-    double* Db = Dinv + (size_t)(jb / CN) * CN * CN;
-    for (int e = tid; e < CN * CN; e += nthr) Db[e] = Pj[e / CN][e % CN];
-    if (tid == 0 && s_fix) atomicAdd(jitterCount, s_fix);
-  }
-  // 4. trailing update of the tile (ti, tj) (CTA 0 reused Pj above; its tile pair reads Pi only)
-  const double(*PJ)[CN_LD] = (ti == tj) ? Pi : Pj;
-  for (int e = tid; e < CN * CN; e += nthr) {
-    const int r = e / CN, cc = e % CN;
-    const int gi = i0 + ti * CN + r, gk = i0 + tj * CN + cc;
-    if (ti * CN + r < R && tj * CN + cc < R && gk <= gi && gi - gk <= bw) {
-      double s = 0;
-      for (int k = 0; k < nbk; k++) s += Pi[r][k] * PJ[cc][k];
-      A[(size_t)gi * w + (gk - gi + bw)] -= s;
-    }
   }
 }
 
@@ -393,6 +538,23 @@ __global__ void k_band_inverse_warp(int n, int bw, const double* __restrict__ A,
 }
 
 template <int NR>
+bool try_band_inverse_staged(Context& c, ShellLevel& L) {
+  const int n = L.denseN, bw = L.bandBw, w = bw + 1;
+  const size_t bufLen = ((size_t)CN * w + CN * CN + 1) & ~(size_t)1;
+  const size_t smem = (2 * bufLen + (size_t)(n + CN) * NR) * sizeof(double);
+  int smemMax = 0;
+  TM_CUDA_CHECK(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.dev));
+  if (smem > (size_t)smemMax) return false;
+  L.d_bandLt.alloc((size_t)n * w);
+  k_band_transpose<<<grid_for((size_t)n * w, 256), 256, 0, c.stream>>>(n, bw, L.d_bandL.p, L.d_bandLt.p);
+  TM_CUDA_CHECK(cudaFuncSetAttribute(k_band_inverse_staged<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int ngroups = (n + NR - 1) / NR;
+  k_band_inverse_staged<NR><<<(ngroups + 1) / 2, 1024, smem, c.stream>>>(n, bw, L.d_bandL.p, L.d_bandLt.p, L.d_dinv.p, ngroups, L.d_inv.p);
+  note_launch(2);
+  return true;
+}
+
+template <int NR>
 bool try_band_inverse(Context& c, ShellLevel& L) {
   const int n = L.denseN;
   const size_t smem = ((size_t)n * NR + (size_t)CN * NR) * sizeof(double);
@@ -439,11 +601,13 @@ void launch_factor_coarsest(Context& c, ShellLevel& L) {
     const int R = std::min(n, jb + nbk + bw) - (jb + nbk);
     const int T = (R + CN - 1) / CN;
     const int ncta = std::max(1, T * (T + 1) / 2);
-    k_band_chol_step<<<ncta, 256, 0, c.stream>>>(n, bw, jb, L.d_band.p, L.d_bandL.p, L.d_dinv.p, L.d_jit.p, c.d_jitter.p);
+    launch_pdl(k_band_chol_step, ncta, CHOL_THREADS, 0, c.stream, n, bw, jb, L.d_band.p, L.d_bandL.p, L.d_dinv.p, (const double*)L.d_jit.p,
+               c.d_jitter.p);
     note_launch();
   }
   TM_CUDA_CHECK(cudaGetLastError());
-  if (!try_band_inverse<8>(c, L) && !try_band_inverse<4>(c, L) && !try_band_inverse<2>(c, L) && !try_band_inverse<1>(c, L)) {
+  if (!try_band_inverse_staged<4>(c, L) && !try_band_inverse_staged<2>(c, L) && !try_band_inverse<8>(c, L) && !try_band_inverse<4>(c, L) &&
+      !try_band_inverse<2>(c, L) && !try_band_inverse<1>(c, L)) {
     k_band_inverse_warp<<<grid_for(n, 4), 128, 0, c.stream>>>(n, bw, L.d_bandL.p, L.d_inv.p);
     note_launch();
   }

@@ -178,6 +178,7 @@ struct ShellLevel {
   int bandBw = 0, denseN = 0;
   DBuf<double> d_band;                 // denseN*(bw+1): the operator's lower band, then its Schur complements
   DBuf<double> d_bandL;                // denseN*(bw+1): the banded Cholesky factor
+  DBuf<double> d_bandLt;               // denseN*(bw+1): its transpose, row i holding L[i..i+bw][i]
   DBuf<double> d_dinv;                 // inverses of the factor's 32x32 diagonal blocks
   DBuf<double> d_jit;                  // pivot floor of the factor
   DBuf<double> d_inv;                  // denseN*denseN
