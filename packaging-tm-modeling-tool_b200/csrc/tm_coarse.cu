@@ -330,37 +330,55 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 // substitutions as k_band_inverse (forward with L, backward with L^T, groups of NR unit vectors,
 // pairs g, G-1-g per CTA), but each block step reads its 32 band rows (of L forward, of L^T
 // backward: both contiguous, Lb + r0*w and Lt + r0*w) and the diagonal block's inverse from a
-// shared-memory buffer that cp.async filled while the previous block step computed: the
-// substitution chain waits on no L2 round trip. The buffers and Y take
+// shared-memory buffer that cp.async filled while the previous block step computed, so the
+// substitution chain waits on no L2 round trip. Warp r takes row r of the block, lane q the
+// terms k = q (mod 32) of its sums for all NR vectors at once (one band value, NR products), and
+// the NR sums are reduced over the warp by a fixed butterfly. The buffers and Y take
 // 2 * (32 w + 1024) + (n + 32) NR doubles (the launcher checks the fit).
+template <int NR>
+__device__ __forceinline__ void warp_sum_n(double (&v)[NR]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int c = 0; c < NR; c++) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+}
 template <int NR>
 __global__ void __launch_bounds__(1024) k_band_inverse_staged(int n, int bw, const double* __restrict__ Lb, const double* __restrict__ Lt,
                                                               const double* __restrict__ Dinv, int ngroups, double* __restrict__ inv) {
-  constexpr int S = 32 / NR;   // partial sums per output
+  static_assert(NR == 2 || NR == 4, "row of Y loaded as double2 pieces");
   extern __shared__ __align__(16) double sms[];
   const int w = bw + 1, tid = threadIdx.x;
   const size_t bufLen = ((size_t)CN * w + CN * CN + 1) & ~(size_t)1;   // 16-byte multiple
-  double* buf[2] = {sms, sms + bufLen};
+  auto buf = [&](int b) { return sms + (size_t)(b & 1) * bufLen; };
   double* Y = sms + 2 * bufLen;       // n x NR, row-major
   double* Z = Y + (size_t)n * NR;     // CN x NR
-  const int o = tid / S, part = tid % S;   // output (r, c) and its part
-  const int r = o / NR, c = o % NR;        // blockDim = CN * NR * S = 1024
+  const int r = tid >> 5, q = tid & 31;   // blockDim = 1024: warp per block row, lane per term class
   const int nblk = (n + CN - 1) / CN;
-  // block b's band rows (of L or of L^T) and its diagonal inverse into buf[b & 1]; every copy is
+  // block b's band rows (of L or of L^T) and its diagonal inverse into buffer b & 1; every copy is
   // 16 bytes between 16-byte boundaries (row blocks start at multiples of 32 w doubles); the last
   // block's rows are rounded up to 16 bytes, which stays inside the band's allocation padding
   auto stage = [&](int b, const double* band) {
-    double* dst = buf[b & 1];
+    double* dst = buf(b);
     const int rows = min(CN, n - b * CN);
     const int pieces = (int)(((size_t)rows * w * sizeof(double) + 15) / 16);
     const double* src = band + (size_t)b * CN * w;
-    for (int q = tid; q < pieces; q += blockDim.x) cp_async16(dst + 2 * q, src + 2 * q);
+    for (int e = tid; e < pieces; e += blockDim.x) cp_async16(dst + 2 * e, src + 2 * e);
     const double* db = Dinv + (size_t)b * CN * CN;
-    for (int q = tid; q < CN * CN / 2; q += blockDim.x) cp_async16(dst + (size_t)CN * w + 2 * q, db + 2 * q);
+    for (int e = tid; e < CN * CN / 2; e += blockDim.x) cp_async16(dst + (size_t)CN * w + 2 * e, db + 2 * e);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
   auto noStage = [] { asm volatile("cp.async.commit_group;\n" ::: "memory"); };
   auto waitStaged = [] { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); };
+  // acc[c] += v * Y[k][c] for the NR vectors (the row of Y as double2 loads)
+  auto fmaRow = [&](double (&acc)[NR], double v, int k) {
+    const double2* yk = reinterpret_cast<const double2*>(Y + (size_t)k * NR);
+#pragma unroll
+    for (int h = 0; h < NR / 2; h++) {
+      const double2 t = yk[h];
+      acc[2 * h] += v * t.x;
+      acc[2 * h + 1] += v * t.y;
+    }
+  };
   for (int pass = 0; pass < 2; pass++) {
     const int g = pass == 0 ? (int)blockIdx.x : ngroups - 1 - (int)blockIdx.x;
     if (pass == 1 && g <= (int)blockIdx.x) break;
@@ -372,25 +390,38 @@ __global__ void __launch_bounds__(1024) k_band_inverse_staged(int n, int bw, con
       if (b + 1 < nblk) stage(b + 1, Lb); else noStage();
       waitStaged();
       __syncthreads();
-      const double* Lr = buf[b & 1];
+      const double* Lr = buf(b);
       const double* Db = Lr + (size_t)CN * w;
       const int r0 = b * CN, nbk = min(CN, n - r0);
-      double sacc = 0;
-      if (r < nbk) {
-        const int gr = r0 + r;
-        const int kbeg = max(rs, gr - bw);
-        for (int k = kbeg + part; k < r0; k += S) sacc += Lr[(size_t)r * w + (k - gr + bw)] * Y[(size_t)k * NR + c];
-      }
+      const int gr = r0 + r;
+      double acc[NR];
 #pragma unroll
-      for (int q = S / 2; q > 0; q >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, q, S);
-      if (part == 0) Z[r * NR + c] = (r < nbk ? ((r0 + r == j0 + c && c < nr) ? 1.0 : 0.0) : 0.0) - sacc;
-      __syncthreads();
-      double y = 0;
+      for (int c = 0; c < NR; c++) acc[c] = 0;
       if (r < nbk)
-        for (int t = part; t <= r; t += S) y += Db[r * CN + t] * Z[t * NR + c];
+        for (int k = max(rs, gr - bw) + q; k < r0; k += 32) fmaRow(acc, Lr[(size_t)r * w + (k - gr + bw)], k);
+      warp_sum_n<NR>(acc);
+      if (q < NR) {
+        double a = acc[0];
 #pragma unroll
-      for (int q = S / 2; q > 0; q >>= 1) y += __shfl_down_sync(0xffffffffu, y, q, S);
-      if (part == 0 && r < nbk) Y[(size_t)(r0 + r) * NR + c] = y;
+        for (int c = 1; c < NR; c++) if (q == c) a = acc[c];
+        Z[r * NR + q] = (r < nbk ? ((gr == j0 + q && q < nr) ? 1.0 : 0.0) : 0.0) - a;
+      }
+      __syncthreads();
+      double y[NR];
+#pragma unroll
+      for (int c = 0; c < NR; c++) y[c] = 0;
+      if (r < nbk && q <= r) {
+        const double d = Db[r * CN + q];
+#pragma unroll
+        for (int c = 0; c < NR; c++) y[c] = d * Z[q * NR + c];
+      }
+      warp_sum_n<NR>(y);
+      if (q < NR && r < nbk) {
+        double a = y[0];
+#pragma unroll
+        for (int c = 1; c < NR; c++) if (q == c) a = y[c];
+        Y[(size_t)gr * NR + q] = a;
+      }
       __syncthreads();   // the buffer is refilled two steps on
     }
     // backward: X = L^-T Y on rows n-1 .. rs (X overwrites Y block by block)
@@ -399,25 +430,40 @@ __global__ void __launch_bounds__(1024) k_band_inverse_staged(int n, int bw, con
       if (b - 1 >= b0) stage(b - 1, Lt); else noStage();
       waitStaged();
       __syncthreads();
-      const double* Ur = buf[b & 1];
+      const double* Ur = buf(b);
       const double* Db = Ur + (size_t)CN * w;
       const int r0 = b * CN, nbk = min(CN, n - r0);
-      double sacc = 0;
+      const int gr = r0 + r;
+      double acc[NR];
+#pragma unroll
+      for (int c = 0; c < NR; c++) acc[c] = 0;
       if (r < nbk) {
-        const int gr = r0 + r;
         const int kend = min(n, gr + bw + 1);
-        for (int k = r0 + nbk + part; k < kend; k += S) sacc += Ur[(size_t)r * w + (k - gr)] * Y[(size_t)k * NR + c];
+        for (int k = r0 + nbk + q; k < kend; k += 32) fmaRow(acc, Ur[(size_t)r * w + (k - gr)], k);
       }
+      warp_sum_n<NR>(acc);
+      if (q < NR) {
+        double a = acc[0];
 #pragma unroll
-      for (int q = S / 2; q > 0; q >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, q, S);
-      if (part == 0) Z[r * NR + c] = (r < nbk ? Y[(size_t)(r0 + r) * NR + c] : 0.0) - sacc;
+        for (int c = 1; c < NR; c++) if (q == c) a = acc[c];
+        Z[r * NR + q] = (r < nbk ? Y[(size_t)gr * NR + q] : 0.0) - a;
+      }
       __syncthreads();
-      double x = 0;
-      if (r < nbk)
-        for (int t = r + part; t < nbk; t += S) x += Db[t * CN + r] * Z[t * NR + c];
+      double x[NR];
 #pragma unroll
-      for (int q = S / 2; q > 0; q >>= 1) x += __shfl_down_sync(0xffffffffu, x, q, S);
-      if (part == 0 && r < nbk) Y[(size_t)(r0 + r) * NR + c] = x;
+      for (int c = 0; c < NR; c++) x[c] = 0;
+      if (r < nbk && q >= r && q < nbk) {
+        const double d = Db[q * CN + r];
+#pragma unroll
+        for (int c = 0; c < NR; c++) x[c] = d * Z[q * NR + c];
+      }
+      warp_sum_n<NR>(x);
+      if (q < NR && r < nbk) {
+        double a = x[0];
+#pragma unroll
+        for (int c = 1; c < NR; c++) if (q == c) a = x[c];
+        Y[(size_t)gr * NR + q] = a;
+      }
       __syncthreads();
     }
     // rows i >= j of column j = j0 + cc, on both sides of the diagonal
