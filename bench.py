@@ -281,6 +281,22 @@ def run_ours(a):
     torch.cuda.synchronize()
     kcount, kms = dm.kernel_time()
     dm.time_kernel(None)
+    # and of the shell-level column sweeps (all shell levels; FP32 cycle only)
+    shell = None
+    if a.precision == "mixed" and not dm.level0_matrix_free:
+        dm.time_kernel("sweep_shell")
+        one(a.precision, u)
+        torch.cuda.synchronize()
+        scount, sms = dm.kernel_time()
+        dm.time_kernel(None)
+        sbytes, spc = dm.shell_sweep_bytes()
+        if scount and spc:
+            cycles = scount / spc
+            shell = {"kernel": "k_sweep_shell<float> (shell-level z-column sweeps, warp per column, all levels)",
+                     "bound": "latency (dependent loads per column; bandwidth figure for reference)",
+                     "achieved": sbytes * cycles / (sms / 1e3) / 1e9, "unit": "GB/s",
+                     "algorithmic_bytes_per_cycle": sbytes, "launches_per_cycle": spc, "launches_timed": scount,
+                     "avg_launch_us": 1e3 * sms / scount}
     clocks = ck.summary()
     wmix = rms_warpage(pkg.mesh, u.cpu().numpy())
     iters = sum(r["iters"] for r in recs)
@@ -356,6 +372,10 @@ def run_ours(a):
                 "flops_per_launch": flops, "achieved_gflops": flops / avg_s / 1e9 if kcount else None,
                 "flops_peak_gflops": fpeak, "flops_frac": flops / avg_s / 1e9 / fpeak if kcount else None,
                 "flops_peak_kind": "measured FMA loop (tm_device_peaks)"}
+    if shell is not None:
+        shell["peak"] = hbm
+        shell["frac"] = shell["achieved"] / hbm
+        roof["shell_sweeps"] = shell
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,

@@ -222,6 +222,14 @@ tm_status tm_set_vcycle_shapes(tm_ctx* ctx, int nlevels, const int* wpb_sweep, c
  * columns, nodes or aggregates nn, DOFs per node or aggregate b: 3 solid, 6 shell), up to cap
  * levels written into out4, *nlevels = all levels. */
 tm_status tm_mg_levels(tm_ctx* ctx, int32_t cap, int32_t* out4, int32_t* nlevels);
+/* Algorithmic bytes of the shell-level column sweeps of one FP32 V-cycle (no counterpart in the
+ * reference; for the bandwidth figure of the sweeps): per swept shell level, 2 sweeps before and 2
+ * after the coarse correction, each over all columns in 4 colours; a sweep reads the level's 6x6
+ * blocks (36 floats and a column index each), the columns' explicit inverses, b and x and writes
+ * x (the cycle's first colour launch on a level starts from x = 0 and reads neither its
+ * columns' blocks nor their x), plus the column lists (24 bytes per column). *launches_per_cycle = the sweep launches of one cycle
+ * (one per non-empty colour and sweep). Needs the multigrid hierarchy. */
+tm_status tm_shell_sweep_bytes(tm_ctx* ctx, double* bytes_per_cycle, int32_t* launches_per_cycle);
 /* The level-1 aggregate of every node (nn values): the solid-to-shell grouping of
  * buildShellLevel (src/core/10-solver.js:260-334) as the multigrid preconditioner uses it. */
 tm_status tm_mg_node_agg(tm_ctx* ctx, int32_t* out);

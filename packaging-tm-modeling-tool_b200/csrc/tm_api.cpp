@@ -1098,6 +1098,42 @@ tm_status tm_mg_levels(tm_ctx* ctx, int32_t cap, int32_t* out4, int32_t* nlevels
   });
 }
 
+tm_status tm_shell_sweep_bytes(tm_ctx* ctx, double* bytes_per_cycle, int32_t* launches_per_cycle) {
+  return guarded([&] {
+    if (!ctx) fail(TM_BAD_INPUT, "null context");
+    Context& c = *reinterpret_cast<Context*>(ctx);
+    if (!c.hierarchy) fail(TM_BAD_INPUT, "no multigrid hierarchy");
+    double bytes = 0;
+    int launches = 0;
+    for (const ShellLevel* Lp : c.shells) {
+      const ShellLevel& L = *Lp;
+      if (L.coarsest) break;
+      const double f = sizeof(float), ncol = (double)L.nx * L.ny;
+      const double inverses = f * (L.cfPtr.empty() ? 0.0 : (double)L.cfPtr.back());
+      const double vec = f * 6.0 * L.nn;          // one level vector
+      const double lists = 24.0 * ncol;           // per column: aggregate/block ranges, inverse offset
+      const double full = (36.0 * f + 4.0) * L.nb + inverses + 3.0 * vec + lists;   // b, x read, x write
+      // the cycle's first launch on the level (the first non-empty colour, i = j = 0 mod 2 when
+      // present) starts from x = 0 and reads neither the blocks nor x of its columns
+      int k0 = 0;
+      while (k0 < 4 && !L.colorCount[k0]) k0++;
+      double blk0 = 0, agg0 = 0;
+      for (int cc = 0; cc < L.nx * L.ny; cc++) {
+        const int i = cc / L.ny, j = cc % L.ny;
+        if ((i & 1) * 2 + (j & 1) != k0) continue;
+        blk0 += L.rowPtr[L.colStart[cc + 1]] - L.rowPtr[L.colStart[cc]];
+        agg0 += L.colStart[cc + 1] - L.colStart[cc];
+      }
+      bytes += 4.0 * full - (36.0 * f + 4.0) * blk0 - f * 6.0 * agg0;
+      int colours = 0;
+      for (int k = 0; k < 4; k++) colours += L.colorCount[k] ? 1 : 0;
+      launches += 4 * colours;
+    }
+    if (bytes_per_cycle) *bytes_per_cycle = bytes;
+    if (launches_per_cycle) *launches_per_cycle = launches;
+  });
+}
+
 tm_status tm_mg_node_agg(tm_ctx* ctx, int32_t* out) {
   return guarded([&] {
     if (!ctx || !out) fail(TM_BAD_INPUT, "null argument");

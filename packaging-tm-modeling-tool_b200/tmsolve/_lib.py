@@ -26,7 +26,7 @@ EXPORTED = ["tm_default_solve_opts", "tm_create", "tm_assemble_step", "tm_set_bc
             "tm_submodel_run", "tm_submodel_run_batch", "tm_set_sublayers", "tm_accumulate_state",
             "tm_accumulate_state_device", "tm_state_stress", "tm_state_stress_device", "tm_solve_f32",
             "tm_warpage_sensitivity", "tm_sensitivity_direction", "tm_vcycle_shapes", "tm_set_vcycle_shapes", "tm_submodel_run_sections", "tm_submodel_stress_snapshot",
-            "tm_mg_levels", "tm_mg_node_agg", "tm_device_peaks",
+            "tm_mg_levels", "tm_mg_node_agg", "tm_shell_sweep_bytes", "tm_device_peaks",
             "tm_set_wait_test", "tm_anand_screen_gradient",
             "tm_element_strains_adjoint", "tm_accumulate_q_adjoint", "tm_adjoint_sensitivity", "tm_set_level0", "tm_level0", "tm_clear_warm", "tm_submodel_set_precond", "tm_submodel_counters"]
 PRECONDS = {"mg": 0, "jacobi": 1, "ic": 2}
@@ -130,6 +130,7 @@ def load():
     L.tm_vcycle_shapes.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
     L.tm_set_vcycle_shapes.argtypes = [vp, C.c_int32, vp, vp, C.c_int32]
     L.tm_mg_levels.argtypes = [vp, C.c_int32, vp, vp]
+    L.tm_shell_sweep_bytes.argtypes = [vp, vp, vp]
     L.tm_mg_node_agg.argtypes = [vp, vp]
     L.tm_device_peaks.argtypes = [vp, vp]
     L.tm_set_wait_test.argtypes = [vp, C.c_int32]

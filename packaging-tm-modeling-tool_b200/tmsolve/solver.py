@@ -302,6 +302,12 @@ class DeviceModel:
         check(load().tm_mg_levels(self.h, cap, out.ctypes.data_as(C.c_void_p), C.byref(n)))
         return [tuple(int(v) for v in out[4 * l:4 * l + 4]) for l in range(min(n.value, cap))]
 
+    def shell_sweep_bytes(self):
+        """(algorithmic bytes, launches) of the shell-level column sweeps of one FP32 V-cycle."""
+        b = C.c_double(); n = C.c_int32()
+        check(load().tm_shell_sweep_bytes(self.h, C.byref(b), C.byref(n)))
+        return float(b.value), int(n.value)
+
     def mg_node_agg(self) -> np.ndarray:
         """Level-1 aggregate of every node (buildShellLevel's grouping)."""
         out = np.zeros(self.nn, np.int32)

@@ -321,3 +321,17 @@ def test_module_stage_matches_oracle(oracle_lib):
             assert np.linalg.norm(r["u"] - ro["u"]) / np.linalg.norm(ro["u"]) <= 1e-8, (k, prec)
         assert dm.mg_levels() == [tuple(int(v) for v in l) for l in om.mg_levels()]
         assert np.array_equal(dm.mg_node_agg(), om.mg_node_agg())
+
+
+def test_shell_sweep_bytes():
+    """The shell sweeps' byte count: 16 launches per swept level and cycle (2 + 2 sweeps in 4
+    colours), and more bytes than the swept levels' 6x6 blocks read in the three sweeps that read
+    every colour's blocks."""
+    from tmsolve.packages import fcbga_c1
+    from tmsolve.solver import DeviceModel
+    dm = DeviceModel(fcbga_c1())
+    levels = dm.mg_levels()
+    b, n = dm.shell_sweep_bytes()
+    assert n == 16 * (len(levels) - 2)
+    blocks_floor = sum(3 * 144 * nn for (_, _, nn, _) in levels[1:-1])   # at least one block per aggregate row
+    assert b > blocks_floor
