@@ -305,6 +305,84 @@ def lidded_c2(n_inplane: int = 160, seed: int = 20261203) -> Package:
                              bump_layer=dict(zmid=z0 + 0.5 * t_bump, part=PART["SOLDER"])))
 
 
+# database-like 25 degC constants (E MPa, nu, CTE 1/degC) of the reference package's materials, by
+# role: substrate row types, then the package groups
+REF_PKG_MATERIALS = {
+    "sr": (3000.0, 0.35, 50e-6), "diel": (5000.0, 0.34, 40e-6), "cu": (60000.0, 0.32, 17e-6), "core": (28000.0, 0.2, 12e-6),
+    "solder": (40000.0, 0.4, 22.5e-6), "uf": (8000.0, 0.35, 30e-6), "die": (130000.0, 0.28, 2.6e-6), "tim": (10.0, 0.45, 100e-6),
+    "lid": (117000.0, 0.34, 17e-6), "lidadh": (2000.0, 0.4, 60e-6), "stiff": (117000.0, 0.34, 17e-6), "stiffadh": (2000.0, 0.4, 60e-6),
+}
+
+
+def reference_package(preset: str = "draft", cfg: Optional[dict] = None, Ta: float = 150.0, Tb: float = 25.0) -> Package:
+    """A package on the reference's own mesh: ``buildPackageMesh`` restated (``pkgmesh``) for the
+    reference's default lidded single die (``defaultConfig``) or a given configuration of
+    monolithic dies, at a mesh preset (Draft 65k, Standard 314k, Fine 1.18M DOF on the default
+    package). The substrate is one layered group whose element layers map to its bands (the rows
+    of the band as sub-layers); solder (column phase), underfill (bump layer and fillet, the fillet
+    cells scaled by their filled fraction), dies, TIM, lid and adhesive as homogeneous groups with
+    database-like 25 degC constants (``REF_PKG_MATERIALS``; not the reference's temperature tables)."""
+    from .pkgmesh import build_package_mesh, default_config
+    cfg = cfg or default_config()
+    mesh, info = build_package_mesh(cfg, {"preset": preset})
+    g = info["geometry"]
+    names = info["groups"]
+    sub = g["sub"]
+    bands = [(b["z0"], b["z1"]) for b in sub["bands"]]
+    nb = len(bands)
+    ncz = mesh.nz - 1
+    sec_of_layer = np.zeros(ncz, np.int32)
+    for k in range(ncz):
+        zc = 0.5 * (mesh.zs[k] + mesh.zs[k + 1])
+        for b, (b0, b1) in enumerate(bands):
+            if b0 < zc < b1:
+                sec_of_layer[k] = b
+    roles = ["sub", "solder", "uf"] + ["die"] * len(g["dies"])
+    if g["lid"]:
+        roles += ["tim", "lid", "lidadh"]
+    if g["stiff"]:
+        roles += ["stiff", "stiffadh"]
+    assert len(roles) == len(names)
+    hom = roles[1:]
+    rows = sub["rows"]     # bottom-up, with z ranges
+
+    def make_step(scales, Ta_, Tb_):
+        m = {k: (v[0] * scales.get(k, (1.0, 1.0))[0], v[1], v[2] * scales.get(k, (1.0, 1.0))[1]) for k, v in REF_PKG_MATERIALS.items()}
+        band_subs = []
+        for (b0, b1) in bands:
+            subs = []
+            for r in rows:
+                a, bb = max(b0, r["z0"]), min(b1, r["z1"])
+                if bb - a > 1e-12:
+                    E, nu, al = m[r["row"]["type"]]
+                    subs.append((a, bb, iso_d(E, nu), al, al))
+            band_subs.append((b0, b1, subs))
+        mats: List = [None] * nb
+        for role in hom:
+            E, nu, al = m[role]
+            mats.append((column_d(E, nu) if role == "solder" else iso_d(E, nu), al, al))
+
+        def layered_fn(p, Ta2, Tb2):
+            b0, b1, subs = band_subs[p]
+            return layered_section(b0, b1, subs, Ta2, Tb2, with_subs=True)
+        return _homog_step(mats, Ta_, Tb_, layered_fn=layered_fn)
+
+    ng = len(names)
+    group_layered = np.zeros(ng, np.int32)
+    group_layered[0] = 1
+    group_pset = np.array([0] + [nb + q for q in range(ng - 1)], np.int32)
+    d0 = g["dies"][0]
+    return Package(name=f"reference_{preset}", mesh=mesh, group_layered=group_layered, group_stage=np.zeros(ng, np.int32),
+                   group_pset=group_pset, sec_of_layer=sec_of_layer, npset=nb + ng - 1,
+                   step_fn=lambda Ta_, Tb_: make_step({}, Ta_, Tb_), Ta=Ta, Tb=Tb, material_step_fn=make_step,
+                   meta=dict(workload=f"reference default package, {info['preset']} mesh", bottom_plane=0, mesh_info=info,
+                             materials=sorted(REF_PKG_MATERIALS),
+                             die=dict(cx=d0["cx"], cy=d0["cy"], w=d0["w"], h=d0["h"], keepout=cfg["dies"][0]["bump"]["keepout"],
+                                      px=d0["px"], py=d0["py"]),
+                             bga=dict(sx=cfg["substrate"]["sx"], sy=cfg["substrate"]["sy"], inset=1.0, pitch=1.0),
+                             bump_layer=dict(zmid=g["zt"] + 0.5 * g["so"], part=PART["SOLDER"])))
+
+
 def stacked_module(n_inplane: int = 192) -> Package:
     """Stacked-module package under a thermal cycle: 45 x 45 x 1.0 mm substrate, SAC305 bump layer
     (0.08 mm, solder columns 30 % with underfill) under a 30 x 30 x 0.1 mm Si base die, a 0.03 mm
