@@ -114,6 +114,37 @@ def default_config() -> dict:
     )
 
 
+def preset_config(which: str, variant: Optional[str] = None) -> dict:
+    """presetConfig (02-config.js:169-243) for the presets of monolithic dies, geometry fields:
+    'default', 'bare', 'stiffener2' (two dies side by side, stiffener ring), 'offset' (an offset
+    bare die) and 'coreStudy' (variant 'A': 0.4 mm core, 'B': 0.8 mm core)."""
+    c = default_config()
+    if which == "default":
+        pass
+    elif which == "bare":
+        c["packageType"] = "bare"
+    elif which == "stiffener2":
+        c["packageType"] = "stiffener"
+        c["substrate"]["sx"] = c["substrate"]["sy"] = 55
+        gap, w = 0.20, 16.0
+        d1, d2 = default_die("D1", -(w + gap) / 2, 0), default_die("D2", (w + gap) / 2, 0)
+        for d in (d1, d2):
+            d["sx"], d["sy"] = 16.0, 24.0
+        c["dies"] = [d1, d2]
+        c["stiffener"] = dict(ox=53.0, oy=53.0, ringW=4.0, t=0.8, adhT=0.050)
+    elif which == "offset":
+        c["packageType"] = "bare"
+        c["dies"][0].update(sx=15, sy=15, x=8, y=6)
+    elif which == "coreStudy":
+        v = "A" if variant == "A" else "B"
+        c["packageType"] = "bare"
+        c["substrate"]["sx"] = c["substrate"]["sy"] = 40
+        c["substrate"]["layers"] = generate_stack(n=3, dielT=0.020, cuT=0.015, srT=0.019, coreT=0.4 if v == "A" else 0.8, coreCuT=0.015)
+    else:
+        raise ValueError(f"preset {which!r} is not one of monolithic dies")
+    return c
+
+
 # ---- geometry ------------------------------------------------------------------------------
 
 def substrate_bands(rows_top_down: list, nb: int) -> dict:

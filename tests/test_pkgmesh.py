@@ -73,3 +73,38 @@ def test_oracle_solves_reference_draft(oracle_lib):
     r = om.solve(om.assemble(pkg.step()), tol=1e-10)
     assert r["converged"] and r["relres"] <= 1e-10
     assert r["iters"] < 60, r["iters"]
+
+
+def test_published_v17_package():
+    """V17's small bare-die package (12 x 12 mm substrate, 5 x 5 mm die offset to (0.5, -0.3), Draft
+    with a 6k DOF cap, src/core/15-verify.js:536-540): printed as 5.9k DOF under its 6k cap
+    (README.md:365), after the cap loop enlarged h_min."""
+    cfg = pm.preset_config("bare")
+    cfg["substrate"]["sx"] = cfg["substrate"]["sy"] = 12
+    cfg["dies"][0].update(sx=5, sy=5, x=0.5, y=-0.3)
+    m, info = pm.build_package_mesh(cfg, {"preset": "draft", "cap": 6000})
+    assert info["scaled"] and not info["ringRefined"]
+    assert info["nDof"] <= 6000 and round(info["nDof"] / 100) == 59, info["nDof"]
+
+
+@pytest.mark.parametrize("which, variant, parts", [
+    ("bare", None, ("SUB", "SOLDER", "UF_BUMP", "UF_FILLET", "DIE")),
+    ("stiffener2", None, ("SUB", "SOLDER", "UF_FILLET", "DIE", "STIFF", "STIFFADH")),
+    ("offset", None, ("SUB", "DIE", "UF_FILLET")),
+    ("coreStudy", "A", ("SUB", "DIE")),
+])
+def test_preset_packages(which, variant, parts):
+    """The reference's presets of monolithic dies mesh at Draft: the parts of each package are there,
+    bare packages have no lid, and the two side-by-side dies' 0.2 mm gap (narrower than the fillet
+    width) is filled to the fillet height (wedgeHeight's gap rule)."""
+    cfg = pm.preset_config(which, variant)
+    m, info = pm.build_package_mesh(cfg, {"preset": "draft"})
+    for p in parts:
+        assert (m.ePart == PART[p]).any(), (which, p)
+    if cfg["packageType"] == "bare":
+        assert not (m.ePart == PART["LID"]).any() and not info["ringRefined"]
+    if which == "stiffener2":
+        g = info["geometry"]
+        assert len(g["dies"]) == 2
+        h, inside = pm.wedge_height(g["dies"], g["uf"]["Wf"], g["uf"]["Hf"], 0.0, 0.0)
+        assert inside and abs(h - 0.7 * 0.775) < 1e-12
