@@ -213,6 +213,21 @@ def run_reference(a):
 
 
 # ---- GPU -----------------------------------------------------------------------------------------
+def over_ranks(secs, work, device):
+    """Whole-job figures of the replicas: the slowest rank's seconds and all ranks' work (MAX and
+    SUM over the process group; a rank's own figures when it runs alone)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(secs), float(work)
+    t = torch.tensor([secs, work], dtype=torch.float64, device=device)
+    tmax = t[:1].clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    wsum = t[1:].clone()
+    dist.all_reduce(wsum, op=dist.ReduceOp.SUM)
+    return float(tmax), float(wsum)
+
+
 def run_ours(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -301,13 +316,7 @@ def run_ours(a):
     wmix = rms_warpage(pkg.mesh, u.cpu().numpy())
     iters = sum(r["iters"] for r in recs)
     work = n * iters / 1e6
-    t = torch.tensor([ms / 1e3, work], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tmax = t[:1].clone(); dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        wsum = t[1:].clone(); dist.all_reduce(wsum, op=dist.ReduceOp.SUM)
-        secs, work_all = float(tmax), float(wsum)
-    else:
-        secs, work_all = ms / 1e3, work
+    secs, work_all = over_ranks(ms / 1e3, work, "cuda")
     value = work_all / secs
     # ---- end to end through the host API (pinned host buffers)
     fh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
@@ -326,13 +335,8 @@ def run_ours(a):
     e3.record(stream)
     torch.cuda.synchronize()
     e2e_s = e2.elapsed_time(e3) / 1e3
-    t = torch.tensor([e2e_s, n * e2_iters / 1e6], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tm_ = t[:1].clone(); dist.all_reduce(tm_, op=dist.ReduceOp.MAX)
-        ws_ = t[1:].clone(); dist.all_reduce(ws_, op=dist.ReduceOp.SUM)
-        e2e_val = float(ws_) / float(tm_)
-    else:
-        e2e_val = n * e2_iters / 1e6 / e2e_s
+    e2e_secs, e2e_work = over_ranks(e2e_s, n * e2_iters / 1e6, "cuda")
+    e2e_val = e2e_work / e2e_secs
     step_bytes = sum(getattr(step, k).nbytes for k in ("layered", "D", "s0", "W", "V", "born"))
     # ---- roofline of the dominant kernel: level-0 column smoother, one colour per launch
     nn = dm.nn
