@@ -80,6 +80,99 @@ def iso_d(E, nu, nu_max=NU_MAX_GLOBAL) -> np.ndarray:
     return ortho_d(E, E, E, G, G, G, nu_c, nu_c, nu_c, nu_max)
 
 
+def iso_ec(E, nu, a) -> dict:
+    """isoEC (03-materials.js:241-244): isotropic engineering constants."""
+    G = E / (2 * (1 + nu))
+    return dict(Ex=E, Ey=E, Ez=E, Gxy=G, Gxz=G, Gyz=G, nuxy=nu, nuxz=nu, nuyz=nu, ax=a, ay=a, az=a)
+
+
+def ec_d(ec: dict, nu_max=NU_MAX_GLOBAL) -> np.ndarray:
+    """orthoD of an engineering-constants record."""
+    return ortho_d(ec["Ex"], ec["Ey"], ec["Ez"], ec["Gxy"], ec["Gxz"], ec["Gyz"], ec["nuxy"], ec["nuxz"], ec["nuyz"], nu_max)
+
+
+def mix_cu_ec(cu: dict, d: dict, r: float, inplane_rule: str) -> dict:
+    """The Cu-pattern mixing rules of a substrate row (mixCuEC, src/core/04-homogenize.js:14-27):
+    a Cu phase of area fraction r beside a matrix phase, both through the row's thickness.
+    Through-thickness modulus and shears: Voigt, X = r X_c + (1 - r) X_d. In-plane moduli and
+    shear: Voigt for a plane layer ('plane'), the mean of Voigt and Reuss (1/X = r/X_c +
+    (1 - r)/X_d) for a signal layer. Poisson ratios by the rule of mixtures; each direction's CTE
+    by Turner's rule, (r E_c a_c + (1 - r) E_d a_d) / (r E_c + (1 - r) E_d) with that direction's
+    moduli."""
+    voigt = lambda xc, xd: r * xc + (1 - r) * xd
+    reuss = lambda xc, xd: 1 / (r / xc + (1 - r) / xd)
+    inpl = (lambda xc, xd: voigt(xc, xd)) if inplane_rule == "plane" else (lambda xc, xd: 0.5 * (voigt(xc, xd) + reuss(xc, xd)))
+    turner = lambda Ec, ac, Ed, ad: (r * Ec * ac + (1 - r) * Ed * ad) / (r * Ec + (1 - r) * Ed)
+    return dict(Ex=inpl(cu["Ex"], d["Ex"]), Ey=inpl(cu["Ey"], d["Ey"]), Ez=voigt(cu["Ez"], d["Ez"]),
+                Gxy=inpl(cu["Gxy"], d["Gxy"]), Gxz=voigt(cu["Gxz"], d["Gxz"]), Gyz=voigt(cu["Gyz"], d["Gyz"]),
+                nuxy=voigt(cu["nuxy"], d["nuxy"]), nuxz=voigt(cu["nuxz"], d["nuxz"]), nuyz=voigt(cu["nuyz"], d["nuyz"]),
+                ax=turner(cu["Ex"], cu["ax"], d["Ex"], d["ax"]), ay=turner(cu["Ey"], cu["ay"], d["Ey"], d["ay"]),
+                az=turner(cu["Ez"], cu["az"], d["Ez"], d["az"]))
+
+
+def substrate_row_ec(row: dict, mats: dict) -> dict:
+    """substrateRowEC (04-homogenize.js:35-54) at one temperature, with the materials' engineering
+    constants given (mats: name -> record, 'cu' the pattern copper): solder resist and dielectric
+    rows as their material (a dielectric with via Cu mixed by the signal rule), Cu rows as the Cu
+    pattern of residual ratio r in the fill dielectric (plane or signal rule), the core with its
+    plated-through-hole Cu by the plane rule."""
+    cu = mats["cu"]
+    t = row["type"]
+    if t == "sr":
+        return dict(mats[row["mat"]])
+    if t == "diel":
+        d = mats[row["mat"]]
+        return mix_cu_ec(cu, d, row["via"], "signal") if row.get("via", 0) > 0 else dict(d)
+    if t == "cu":
+        return mix_cu_ec(cu, mats[row["fill"]], row["r"], "plane" if row["kind"] == "plane" else "signal")
+    if t == "core":
+        d = mats[row["mat"]]
+        return mix_cu_ec(cu, d, row["pth"], "plane") if row.get("pth", 0) > 0 else dict(d)
+    raise ValueError(f"unknown substrate row type {t!r}")
+
+
+# silicon's cubic constants (MPa): the literature values of (100) silicon
+SI_C11, SI_C12, SI_C44 = 165.7e3, 63.9e3, 79.6e3
+
+
+def cubic_rotated_d(C11: float, C12: float, C44: float, theta: float) -> np.ndarray:
+    """Stiffness of a cubic crystal rotated by theta about z (cubicRotatedD, 03-materials.js:272-294;
+    theta = 45 degrees puts x along <110>, the die edges of (100) silicon): the fourth-order tensor
+    C'_ijkl = R_ip R_jq R_kr R_ls C_pqrs in Voigt order (xx yy zz xy yz zx)."""
+    c, s = np.cos(theta), np.sin(theta)
+    R = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+    C = np.zeros((3, 3, 3, 3))
+    for i in range(3):
+        for k in range(3):
+            C[i, i, k, k] = C11 if i == k else C12
+    for i in range(3):
+        for j in range(3):
+            if i != j:
+                C[i, j, i, j] = C[i, j, j, i] = C44
+    Cr = np.einsum("ip,jq,kr,ls,pqrs->ijkl", R, R, R, R, C)
+    vo = [(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (2, 0)]
+    return np.array([Cr[i, j, k, l] for (i, j) in vo for (k, l) in vo])
+
+
+def directional_modulus(D: np.ndarray, n) -> float:
+    """Young's modulus along the unit direction n from a 6x6 stiffness (directionalModulus,
+    03-materials.js:297-307): the normal strain along n under a unit uniaxial stress along n."""
+    S = np.linalg.inv(np.asarray(D, np.float64).reshape(6, 6))
+    n = np.asarray(n, np.float64)
+    sv = np.array([n[0] * n[0], n[1] * n[1], n[2] * n[2], n[0] * n[1], n[1] * n[2], n[2] * n[0]])
+    ev = S @ sv
+    e = ev[0] * n[0] * n[0] + ev[1] * n[1] * n[1] + ev[2] * n[2] * n[2] + ev[3] * n[0] * n[1] + ev[4] * n[1] * n[2] + ev[5] * n[2] * n[0]
+    return 1.0 / e
+
+
+def silicon_d(model: str = "aniso") -> np.ndarray:
+    """siliconD (03-materials.js:310-314): 'aniso' the cubic constants rotated by 45 degrees (die
+    edges along <110>), 'iso' E = 130 GPa, nu = 0.28."""
+    if model == "iso":
+        return iso_d(130e3, 0.28)
+    return cubic_rotated_d(SI_C11, SI_C12, SI_C44, np.pi / 4)
+
+
 def column_d(E, nu) -> np.ndarray:
     """columnD (03-materials.js:259-266): solder phase of the bump layer as separate columns."""
     D = np.zeros(36)

@@ -25,7 +25,7 @@ from typing import Callable, List, Optional
 
 import numpy as np
 
-from .materials import column_d, iso_d, layered_section, thermal_stress_const
+from .materials import column_d, ec_d, iso_d, iso_ec, layered_section, silicon_d, substrate_row_ec, thermal_stress_const
 from .mesh import PART, Mesh, build_structured_mesh, constraints321, module_support
 
 CONSTRAINT_SPAN = 0.4   # 00-constants.js:52
@@ -314,14 +314,25 @@ REF_PKG_MATERIALS = {
 }
 
 
-def reference_package(preset: str = "draft", cfg: Optional[dict] = None, Ta: float = 150.0, Tb: float = 25.0) -> Package:
+# the substrate materials of the reference's default stack by database id (roles above), and the
+# 25 degC expansion of (100) silicon (the reference's Si CTE formula at 25 degC: 2.553 ppm/K)
+REF_PKG_MATERIAL_IDS = {"psr4000": "sr", "abf_gl": "diel", "mcl_e_795g": "core", "cu": "cu"}
+SI_CTE_25C = 2.553e-6
+
+
+def reference_package(preset: str = "draft", cfg: Optional[dict] = None, Ta: float = 150.0, Tb: float = 25.0,
+                      homogenize: bool = False) -> Package:
     """A package on the reference's own mesh: ``buildPackageMesh`` restated (``pkgmesh``) for the
     reference's default lidded single die (``defaultConfig``) or a given configuration of
     monolithic dies, at a mesh preset (Draft 65k, Standard 314k, Fine 1.18M DOF on the default
     package). The substrate is one layered group whose element layers map to its bands (the rows
     of the band as sub-layers); solder (column phase), underfill (bump layer and fillet, the fillet
     cells scaled by their filled fraction), dies, TIM, lid and adhesive as homogeneous groups with
-    database-like 25 degC constants (``REF_PKG_MATERIALS``; not the reference's temperature tables)."""
+    database-like 25 degC constants (``REF_PKG_MATERIALS``; not the reference's temperature tables).
+    With homogenize, the substrate rows follow the reference's homogenization (``substrateRowEC``:
+    Cu patterns of their residual ratios in the fill dielectric, the core with its plated
+    through-hole Cu) and the dies take the rotated cubic stiffness of (100) silicon (``siliconD``
+    'aniso') with its 25 degC expansion."""
     from .pkgmesh import build_package_mesh, default_config
     cfg = cfg or default_config()
     mesh, info = build_package_mesh(cfg, {"preset": preset})
@@ -348,19 +359,27 @@ def reference_package(preset: str = "draft", cfg: Optional[dict] = None, Ta: flo
 
     def make_step(scales, Ta_, Tb_):
         m = {k: (v[0] * scales.get(k, (1.0, 1.0))[0], v[1], v[2] * scales.get(k, (1.0, 1.0))[1]) for k, v in REF_PKG_MATERIALS.items()}
+        ecs = {mid: iso_ec(m[role][0], m[role][1], m[role][2]) for mid, role in REF_PKG_MATERIAL_IDS.items()}
         band_subs = []
         for (b0, b1) in bands:
             subs = []
             for r in rows:
                 a, bb = max(b0, r["z0"]), min(b1, r["z1"])
                 if bb - a > 1e-12:
-                    E, nu, al = m[r["row"]["type"]]
-                    subs.append((a, bb, iso_d(E, nu), al, al))
+                    if homogenize:
+                        ec = substrate_row_ec(r["row"], ecs)
+                        subs.append((a, bb, ec_d(ec), ec["ax"], ec["az"]))
+                    else:
+                        E, nu, al = m[r["row"]["type"]]
+                        subs.append((a, bb, iso_d(E, nu), al, al))
             band_subs.append((b0, b1, subs))
         mats: List = [None] * nb
         for role in hom:
             E, nu, al = m[role]
-            mats.append((column_d(E, nu) if role == "solder" else iso_d(E, nu), al, al))
+            if homogenize and role == "die":
+                mats.append((silicon_d("aniso"), SI_CTE_25C, SI_CTE_25C))
+            else:
+                mats.append((column_d(E, nu) if role == "solder" else iso_d(E, nu), al, al))
 
         def layered_fn(p, Ta2, Tb2):
             b0, b1, subs = band_subs[p]
@@ -372,7 +391,7 @@ def reference_package(preset: str = "draft", cfg: Optional[dict] = None, Ta: flo
     group_layered[0] = 1
     group_pset = np.array([0] + [nb + q for q in range(ng - 1)], np.int32)
     d0 = g["dies"][0]
-    return Package(name=f"reference_{preset}", mesh=mesh, group_layered=group_layered, group_stage=np.zeros(ng, np.int32),
+    return Package(name=f"reference_{preset}" + ("_homogenized" if homogenize else ""), mesh=mesh, group_layered=group_layered, group_stage=np.zeros(ng, np.int32),
                    group_pset=group_pset, sec_of_layer=sec_of_layer, npset=nb + ng - 1,
                    step_fn=lambda Ta_, Tb_: make_step({}, Ta_, Tb_), Ta=Ta, Tb=Tb, material_step_fn=make_step,
                    meta=dict(workload=f"reference default package, {info['preset']} mesh", bottom_plane=0, mesh_info=info,

@@ -108,3 +108,16 @@ def test_preset_packages(which, variant, parts):
         assert len(g["dies"]) == 2
         h, inside = pm.wedge_height(g["dies"], g["uf"]["Wf"], g["uf"]["Hf"], 0.0, 0.0)
         assert inside and abs(h - 0.7 * 0.775) < 1e-12
+
+
+def test_oracle_solves_reference_draft_homogenized(oracle_lib):
+    """The same mesh with the reference's substrate-row homogenization (Cu patterns of their
+    residual ratios, core with PTH Cu: orthotropic sub-layers) and anisotropic (100) silicon dies:
+    the sections differ from the constant-row ones, and the oracle's MG-PCG converges on them."""
+    from tmsolve.packages import reference_package
+    pkg0, pkg = reference_package("draft"), reference_package("draft", homogenize=True)
+    s0, s1 = pkg0.step(), pkg.step()
+    assert s1.W.shape == s0.W.shape and not np.allclose(s1.W, s0.W)
+    om = oracle_lib.OracleModel(pkg)
+    r = om.solve(om.assemble(s1), tol=1e-10)
+    assert r["converged"] and r["iters"] < 60, r["iters"]
