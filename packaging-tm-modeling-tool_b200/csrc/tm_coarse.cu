@@ -14,13 +14,17 @@
 //
 // Band layout: row i holds K[i][k] for k in [i-bw, i] at A[i*w + (k - i + bw)], w = bw + 1.
 //
-// Factor: right-looking blocked Cholesky in steps of CN columns, one launch per step. A step's
+// Factor: right-looking blocked Cholesky in steps of CN columns, one launch per step (each launched
+// with a programmatic dependency on the previous one, so its launch overlaps that step). A step's
 // CTAs each own one CN x CN tile of the trailing window (the rows within bw of the step's
 // columns); every CTA factors the step's diagonal block itself, solves the panel rows of its two
-// row tiles and subtracts their product from its tile, so no CTA waits on another inside a step.
-// The Schur complement stays in the working band; the factor goes to a second band.
+// row tiles and subtracts their product from its tile, so no CTA waits on another inside a step;
+// CTA 0 also forms the inverse of the diagonal block, in the registers of the warp that factored
+// it. The Schur complement stays in the working band; the factor goes to a second band.
 //
-// Inverse: CTA per pair of groups of NR unit vectors e_j (pairs g, G-1-g balance the work). A
+// Inverse: CTA per pair of groups of NR unit vectors e_j (pairs g, G-1-g balance the work); the
+// staged kernel reads each block step's band rows (of L, and of a transposed copy for the
+// backward pass) from shared memory filled by cp.async one step ahead. A
 // group's forward substitution starts at its first column's block (L^-1 e_j vanishes above j);
 // every block of CN rows is one product with the preceding bw rows followed by one product with
 // the inverse of the diagonal block, so there is no serial row loop. The backward substitution
