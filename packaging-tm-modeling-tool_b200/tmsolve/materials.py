@@ -326,3 +326,119 @@ def elastic_tables(E_T, E_MPa, cte: float):
     Ft = grid_table(lambda T: cte * (T - T_STRAIN_ORIGIN))
     return Et, Ft
 
+
+
+# ---- temperature-dependent properties of a database record -----------------------------------
+# (the caller's side in the tool; restated for the host-side known-answer tests and packages)
+
+SIGMOID_W_DEFAULT = 8.0       # 00-constants.js:22
+CTE_SMOOTH_DELTA = 3.0        # 00-constants.js:23
+PPM = 1e-6
+GPA = 1000.0
+
+
+def _pv(p):
+    return p["v"] if isinstance(p, dict) else p
+
+
+def _mod_mpa(p) -> float:
+    """modMPa (03-materials.js:21-25): a modulus parameter in MPa by its unit."""
+    u = (p.get("u") if isinstance(p, dict) else None) or "GPa"
+    return _pv(p) if u == "MPa" else _pv(p) * GPA
+
+
+def modulus_at(edef: dict, T: float) -> float:
+    """evalEdef (03-materials.js:88-107) for constant and glass-transition (sigmoid) moduli:
+    E(T) = E_r + (E_g - E_r) / (1 + exp((T - Tg_DMA) / w))."""
+    t = edef["type"]
+    if t == "const":
+        return _mod_mpa(edef["E"])
+    if t == "sigmoid":
+        Eg, Er = _mod_mpa(edef["Eg"]), _mod_mpa(edef["Er"])
+        w = _pv(edef.get("w")) or SIGMOID_W_DEFAULT
+        return Er + (Eg - Er) / (1 + np.exp((T - _pv(edef["TgDMA"])) / w))
+    raise ValueError(f"modulus type {t!r} not restated")
+
+
+def _softplus(x: float) -> float:
+    return x if x > 30 else float(np.log1p(np.exp(x)))
+
+
+def cte_at(cdef: dict, T: float) -> float:
+    """cteAlpha (03-materials.js:138-156), constant and bilinear kinds: the bilinear CTE switches
+    from a1 to a2 around Tg_TMA by a logistic step of width delta."""
+    t = cdef["type"]
+    if t == "const":
+        return _pv(cdef["a"]) * PPM
+    if t == "bilinear":
+        a1, a2 = _pv(cdef["a1"]) * PPM, _pv(cdef["a2"]) * PPM
+        d = _pv(cdef.get("delta")) or CTE_SMOOTH_DELTA
+        return a1 + (a2 - a1) / (1 + np.exp(-(T - _pv(cdef["TgTMA"])) / d))
+    raise ValueError(f"CTE type {t!r} not restated")
+
+
+def thermal_strain_at(cdef: dict, T: float) -> float:
+    """thermalStrain (03-materials.js:167-195), constant and bilinear kinds: the cumulative
+    thermal strain F(T) from 25 degC in closed form (the logistic term integrates to
+    (a2 - a1) delta ln(1 + exp((T - Tg) / delta)))."""
+    T0 = T_STRAIN_ORIGIN
+    t = cdef["type"]
+    if t == "const":
+        return _pv(cdef["a"]) * PPM * (T - T0)
+    if t == "bilinear":
+        a1, a2 = _pv(cdef["a1"]) * PPM, _pv(cdef["a2"]) * PPM
+        d = _pv(cdef.get("delta")) or CTE_SMOOTH_DELTA
+        Tg = _pv(cdef["TgTMA"])
+        return a1 * (T - T0) + (a2 - a1) * d * (_softplus((T - Tg) / d) - _softplus((T0 - Tg) / d))
+    raise ValueError(f"CTE type {t!r} not restated")
+
+
+def iso_tables(mat: dict) -> dict:
+    """isoTables (03-materials.js:424-433) of an isotropic record: E(T) in MPa and F(T) on the
+    1 degC grid, and nu."""
+    E = grid_table(lambda T: modulus_at(mat["elastic"]["E"], T))
+    cte = mat.get("cteXY") or mat["cte"]
+    F = grid_table(lambda T: thermal_strain_at(cte, T))
+    return dict(E=E, F=F, nu=_pv(mat["elastic"]["nu"]))
+
+
+def material_tgs(mat: dict) -> list:
+    """materialTgs (03-materials.js:203-216): the glass transitions of a record (the thermal path
+    takes smaller steps around them)."""
+    out = []
+    el = mat.get("elastic", {})
+    if el.get("E", {}).get("type") == "sigmoid":
+        out.append(float(_pv(el["E"]["TgDMA"])))
+    for c in {id(x): x for x in (mat.get("cteXY") or mat.get("cte"), mat.get("cteZ")) if x}.values():
+        if c.get("type") == "bilinear":
+            out.append(float(_pv(c["TgTMA"])))
+    return out
+
+
+def for_grid_segments(Ta: float, Tb: float, fn) -> None:
+    """forGridSegments (03-materials.js:370-377): the pieces of [Ta, Tb] between 1 degC grid points."""
+    lo, hi = min(Ta, Tb), max(Ta, Tb)
+    t0 = lo
+    while t0 < hi - 1e-12:
+        t1 = min(hi, TGRID_MIN + np.floor(t0 - TGRID_MIN + 1e-9) + 1)
+        fn(0.5 * (t0 + t1), t0, t1)
+        t0 = t1
+
+
+def grid_mean(arr: np.ndarray, Ta: float, Tb: float) -> float:
+    """gridMean (03-materials.js:380-387) of a scalar grid: the mean over the step [Ta, Tb]."""
+    L = abs(Tb - Ta)
+    if L < 1e-12:
+        return grid_at(arr, Ta)
+    acc = [0.0]
+    for_grid_segments(Ta, Tb, lambda tm, t0, t1: acc.__setitem__(0, acc[0] + (t1 - t0) / L * grid_at(arr, tm)))
+    return acc[0]
+
+
+def grid_modulus_strain_increment(E: np.ndarray, F: np.ndarray, Ta: float, Tb: float) -> float:
+    """gridModulusStrainIncrement (03-materials.js:413-418): the integral from Ta to Tb of
+    E(T) dF(T), exact for the interpolated tables (midpoint modulus per grid piece)."""
+    sg = 1.0 if Tb >= Ta else -1.0
+    acc = [0.0]
+    for_grid_segments(Ta, Tb, lambda tm, t0, t1: acc.__setitem__(0, acc[0] + grid_at(E, tm) * (grid_at(F, t1) - grid_at(F, t0))))
+    return sg * acc[0]

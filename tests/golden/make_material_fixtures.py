@@ -1,0 +1,35 @@
+"""Writes materials_subset.json: the records of the reference's material database
+(src/materials-db.json of the reference) that the host-side material tests use, with each
+parameter reduced to its value and unit. Run in a container that holds the reference:
+
+    python tests/golden/make_material_fixtures.py /path/to/reference/src/materials-db.json
+"""
+import json
+import os
+import sys
+
+IDS = ["uf9000ae"]
+
+
+def values(o):
+    if isinstance(o, dict):
+        if "v" in o:
+            return {"v": o["v"], "u": o.get("u")}
+        return {k: values(v) for k, v in o.items() if k not in ("s", "c", "n", "r")}
+    if isinstance(o, list):
+        return [values(v) for v in o]
+    return o
+
+
+def main(path):
+    db = json.load(open(path))
+    out = {m["id"]: {k: values(m[k]) for k in ("elastic", "cte", "cteXY", "cteZ", "solidus") if k in m}
+           for m in db["materials"] if m["id"] in IDS}
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "materials_subset.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print("wrote", dst, sorted(out))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

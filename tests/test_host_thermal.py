@@ -1,0 +1,99 @@
+"""Temperature-dependent materials and incremental thermoelasticity on the host and the oracle,
+against the reference's own check V16 (src/core/15-verify.js:492-529; README.md:364: "free
+9.0e-14 x E alpha dT; held 45.52 vs 45.52 MPa exact (0.00 %); a secant form gives 125.47 MPa"):
+the default underfill (UF9000AE record of the reference's material database, from
+tests/golden/materials_subset.json) cooled from its 165 degC cure through its glass transition
+to 25 degC along the tool's thermal path.
+
+* its 1 degC tables give the exact held stress -integral E / (1 - nu) dF = 45.52 MPa and the
+  secant value 125.47 MPa (printed digits);
+* a block of it (2 x 2 x 2 elements), stepped along the path with each step's mean stiffness and
+  thermal stress increment and solved by the oracle: free, it stays stress-free (below 1e-8 x
+  E alpha dT); held at its sides, its in-plane stress is the exact value within 0.1 % and its
+  through-thickness stress vanishes (1e-6)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tmsolve import post
+from tmsolve.materials import NU_MAX_GLOBAL, grid_at, iso_tables, material_tgs
+from tmsolve.packages import linspace
+from tmsolve.thermal import table_box_package, thermal_path_points
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "materials_subset.json")
+Ta, Tb = 165.0, 25.0
+
+
+@pytest.fixture(scope="module")
+def uf():
+    return json.load(open(GOLDEN))["uf9000ae"]
+
+
+def _exact_and_secant(tab):
+    nu = min(tab["nu"], NU_MAX_GLOBAL)
+    exact, T = 0.0, Ta
+    while T > Tb + 1e-9:      # 0.01 degC steps, as the check itself integrates
+        exact -= grid_at(tab["E"], T - 0.005) / (1 - nu) * (grid_at(tab["F"], T - 0.01) - grid_at(tab["F"], T))
+        T -= 0.01
+    secant = -grid_at(tab["E"], Tb) / (1 - nu) * (grid_at(tab["F"], Tb) - grid_at(tab["F"], Ta))
+    return exact, secant
+
+
+def test_v16_tables(uf):
+    exact, secant = _exact_and_secant(iso_tables(uf))
+    assert round(exact, 2) == 45.52 and round(secant, 2) == 125.47, (exact, secant)
+    assert material_tgs(uf) == [111.0, 112.0]
+
+
+def test_thermal_path_points():
+    # 30 degC steps, 10 degC while a step would reach within 15 degC of a Tg
+    assert thermal_path_points(Ta, Tb, [111.0, 112.0]) == [165.0, 135.0, 125.0, 115.0, 105.0, 95.0, 65.0, 35.0, 25.0]
+    assert thermal_path_points(25.0, 125.0, []) == [25.0, 55.0, 85.0, 115.0, 125.0]
+    assert thermal_path_points(25.0, 125.0, [], stops=[60.0]) == [25.0, 55.0, 60.0, 90.0, 120.0, 125.0]
+    assert thermal_path_points(25.0, 25.0, [111.0]) == [25.0]
+
+
+def _block(uf, held, oracle_lib):
+    xs, ys, zs = linspace(0, 1, 2), linspace(0, 1, 2), linspace(0, 0.5, 2)
+    cons = None
+    if held:
+        # roller supports: ux = 0 on both x faces, uy = 0 on both y faces, uz = 0 at one node
+        m = table_box_package(uf, xs, ys, zs).mesh
+        c = m.coords.reshape(-1, 3)
+        dofs = []
+        for n in range(m.nn):
+            if c[n, 0] < 1e-9 or c[n, 0] > 1 - 1e-9:
+                dofs.append(3 * n)
+            if c[n, 1] < 1e-9 or c[n, 1] > 1 - 1e-9:
+                dofs.append(3 * n + 1)
+        dofs.append(2)
+        cons = np.array(dofs, np.int32)
+    pkg = table_box_package(uf, xs, ys, zs, constraints=cons)
+    om = oracle_lib.OracleModel(pkg)
+    m = pkg.mesh
+    elems = np.arange(m.ne, dtype=np.int32)
+    pts = thermal_path_points(Ta, Tb, material_tgs(uf))
+    stride = post.state_stride(pkg.step(pts[0], pts[1]))
+    S = np.zeros(stride * m.ne)
+    for a, b in zip(pts[:-1], pts[1:]):
+        st = pkg.step(a, b)
+        r = om.solve(om.assemble(st), tol=1e-13)
+        assert r["converged"]
+        om.set_sublayers(st)
+        om.accumulate_state(r["u"], elems, stride, S)
+    _, sig = om.state_stress(elems, S, stride, np.zeros((m.ne, 3)))
+    return sig
+
+
+def test_v16_blocks(uf, oracle_lib):
+    tab = iso_tables(uf)
+    exact, _ = _exact_and_secant(tab)
+    sref = grid_at(tab["E"], Tb) * abs(grid_at(tab["F"], Tb) - grid_at(tab["F"], Ta))
+    free = _block(uf, False, oracle_lib)
+    assert np.abs(free).max() < 1e-8 * sref
+    held = _block(uf, True, oracle_lib)
+    sx = held[:, 0].mean()
+    assert abs(sx / exact - 1) < 1e-3 and round(sx, 2) == 45.52, sx
+    assert np.abs(held[:, 2]).max() < 1e-6 * abs(exact)
