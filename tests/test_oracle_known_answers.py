@@ -138,6 +138,57 @@ def test_v3_bimaterial_curvature(oracle_lib):
     assert f"{-kxx:.4e}" == known()["V3"]["fe_curvature"]
 
 
+def clt_curvature(layers, dT):
+    """Free thermal curvature of a laminate by classical lamination theory (cltCurvature,
+    15-verify.js:49-67): plane-stress stiffnesses Q of the layers (bottom to top), their A, B, D
+    integrals and thermal resultants, then the 6 x 6 system for mid-plane strains and curvatures."""
+    A, B, D = np.zeros((3, 3)), np.zeros((3, 3)), np.zeros((3, 3))
+    NT, MT = np.zeros(3), np.zeros(3)
+    z0 = -sum(L["t"] for L in layers) / 2
+    for L in layers:
+        z1 = z0 + L["t"]
+        nu21 = L["nu12"] * L["E2"] / L["E1"]
+        den = 1 - L["nu12"] * nu21
+        Q = np.array([[L["E1"] / den, L["nu12"] * L["E2"] / den, 0], [L["nu12"] * L["E2"] / den, L["E2"] / den, 0], [0, 0, L["G12"]]])
+        a = np.array([L["a1"], L["a2"], 0.0])
+        h1, h2, h3 = z1 - z0, (z1 ** 2 - z0 ** 2) / 2, (z1 ** 3 - z0 ** 3) / 3
+        A += Q * h1; B += Q * h2; D += Q * h3
+        s = Q @ a * dT
+        NT += s * h1; MT += s * h2
+        z0 = z1
+    M = np.block([[A, B], [B, D]])
+    x = np.linalg.solve(M, np.concatenate([NT, MT]))
+    return x[3], x[4]
+
+
+def v4_package(n=28):
+    """V4's asymmetric three-layer laminate (15-verify.js:183-203): an orthotropic layer (Ex 36,
+    Ey 20, Ez 12 GPa; Gxy 8, Gxz = Gyz = 5 GPa; nu 0.15 / 0.3 / 0.3; CTE 4 ppm in-plane, 12
+    through the thickness) under Cu and Si, two element layers each, cooled by 100 degC."""
+    from tmsolve.materials import ortho_d
+    O = ortho_d(36000.0, 20000.0, 12000.0, 8000.0, 5000.0, 5000.0, 0.15, 0.3, 0.3, 0.45)
+    mats = [(O, 4e-6, 12e-6), (iso_d(110000.0, 0.34), 16.4e-6, 16.4e-6), (iso_d(130000.0, 0.28), 2.6e-6, 2.6e-6)]
+    return box_package(linspace(-20, 20, n), linspace(-20, 20, n), [0, 0.15, 0.3, 0.4, 0.5, 0.75, 1.0], mats,
+                       lambda i, j, k: 0 if k < 2 else (1 if k < 4 else 2), Ta=25.0, Tb=-75.0)
+
+
+def test_v4_laminate_vs_clt(oracle_lib):
+    pkg = v4_package()
+    om = oracle_lib.OracleModel(pkg)
+    r = om.solve(om.assemble(pkg.step()), tol=1e-10)
+    assert r["converged"]
+    kxx, kyy = centre_curvature(pkg.mesh, r["u"])
+    kx, ky = clt_curvature([
+        dict(t=0.3, E1=36000, E2=20000, nu12=0.15, G12=8000, a1=4e-6, a2=4e-6),
+        dict(t=0.2, E1=110000, E2=110000, nu12=0.34, G12=110000 / 2.68, a1=16.4e-6, a2=16.4e-6),
+        dict(t=0.5, E1=130000, E2=130000, nu12=0.28, G12=130000 / 2.56, a1=2.6e-6, a2=2.6e-6),
+    ], -100)
+    ex, ey = abs(-kxx / kx - 1), abs(-kyy / ky - 1)
+    assert ex < 0.03 and ey < 0.03
+    # the reference's published deviations, at their printed precision
+    assert f"{100 * ex:.2f}" == known()["V4"]["kx_err_pct"] and f"{100 * ey:.2f}" == known()["V4"]["ky_err_pct"], (ex, ey)
+
+
 @pytest.mark.parametrize("case", [0, 1, 2])
 def test_v6_anand_saturation(oracle_lib, case):
     T, rate, ref_pub, cf_pub = known()["V6"]["cases"][case]
