@@ -365,11 +365,19 @@ def _softplus(x: float) -> float:
 
 
 def cte_at(cdef: dict, T: float) -> float:
-    """cteAlpha (03-materials.js:138-156), constant and bilinear kinds: the bilinear CTE switches
-    from a1 to a2 around Tg_TMA by a logistic step of width delta."""
+    """cteAlpha (03-materials.js:138-156), constant, bilinear and tabulated kinds: the bilinear CTE
+    switches from a1 to a2 around Tg_TMA by a logistic step of width delta; a table is
+    interpolated piecewise linearly (linear extrapolation unless it says 'hold')."""
     t = cdef["type"]
     if t == "const":
         return _pv(cdef["a"]) * PPM
+    if t == "table":
+        xs, ys = cdef["T"], cdef["v"]
+        xs = xs["v"] if isinstance(xs, dict) else xs
+        ys = ys["v"] if isinstance(ys, dict) else ys
+        if (cdef.get("extrap") or "linear") != "linear" and len(xs) > 1:
+            T = min(max(T, xs[0]), xs[-1])
+        return interp_table_linear(xs, ys, T) * PPM
     if t == "bilinear":
         a1, a2 = _pv(cdef["a1"]) * PPM, _pv(cdef["a2"]) * PPM
         d = _pv(cdef.get("delta")) or CTE_SMOOTH_DELTA
@@ -442,3 +450,33 @@ def grid_modulus_strain_increment(E: np.ndarray, F: np.ndarray, Ta: float, Tb: f
     acc = [0.0]
     for_grid_segments(Ta, Tb, lambda tm, t0, t1: acc.__setitem__(0, acc[0] + grid_at(E, tm) * (grid_at(F, t1) - grid_at(F, t0))))
     return sg * acc[0]
+
+
+def ortho_factor(el: dict, T: float) -> float:
+    """orthoFactor (03-materials.js:119-126): the glass-transition factor on every orthotropic
+    modulus, r + (1 - r) / (1 + exp((T - Tg) / w)) with the rubbery ratio r (1 without one)."""
+    r, Tg = _pv(el.get("rubberyRatio")), _pv(el.get("TgDMA"))
+    if r is None or Tg is None:
+        return 1.0
+    w = _pv(el.get("w")) or SIGMOID_W_DEFAULT
+    return r + (1 - r) / (1 + np.exp((T - Tg) / w))
+
+
+def material_ec(mat: dict, T: float) -> dict:
+    """materialEC (03-materials.js:317-340): engineering constants (MPa, 1/degC) of a database
+    record at T, for homogenization: isotropic records with their E(T), orthotropic ones with
+    their moduli times the glass-transition factor; in-plane and through-thickness CTEs."""
+    el = mat["elastic"]
+    cxy = mat.get("cteXY") or mat["cte"]
+    cz = mat.get("cteZ") or cxy
+    axy, az = cte_at(cxy, T), cte_at(cz, T)
+    if el["type"] == "iso":
+        ec = iso_ec(modulus_at(el["E"], T), _pv(el["nu"]), axy)
+        ec["az"] = az
+        return ec
+    if el["type"] == "ortho":
+        f = ortho_factor(el, T)
+        return dict(Ex=f * _mod_mpa(el["Ex"]), Ey=f * _mod_mpa(el["Ey"]), Ez=f * _mod_mpa(el["Ez"]), Gxy=f * _mod_mpa(el["Gxy"]),
+                    Gxz=f * _mod_mpa(el["Gxz"]), Gyz=f * _mod_mpa(el["Gyz"]), nuxy=_pv(el["nuxy"]), nuxz=_pv(el["nuxz"]),
+                    nuyz=_pv(el["nuyz"]), ax=axy, ay=axy, az=az)
+    raise ValueError(f"elastic type {el['type']!r} not restated")

@@ -8,12 +8,12 @@ import json
 import os
 import sys
 
-IDS = ["uf9000ae"]
+IDS = ["uf9000ae", "abf_gl", "cu", "mcl_e_795g", "psr4000"]
 
 
 def values(o):
     if isinstance(o, dict):
-        if "v" in o:
+        if "v" in o and not isinstance(o["v"], list):
             return {"v": o["v"], "u": o.get("u")}
         return {k: values(v) for k, v in o.items() if k not in ("s", "c", "n", "r")}
     if isinstance(o, list):

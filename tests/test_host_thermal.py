@@ -97,3 +97,43 @@ def test_v16_blocks(uf, oracle_lib):
     sx = held[:, 0].mean()
     assert abs(sx / exact - 1) < 1e-3 and round(sx, 2) == 45.52, sx
     assert np.abs(held[:, 2]).max() < 1e-6 * abs(exact)
+
+
+def _bottom_warpage(pkg, u):
+    """The free box's bottom-face warpage of V5: the z displacement on the bottom plane minus its
+    least-squares plane, peak to valley (planeGrid and fitPlane, src/core/12-post.js:40-47)."""
+    m = pkg.mesh
+    X, Y, W = [], [], []
+    for i in range(m.nx):
+        for j in range(m.ny):
+            n = m.nodeId[(i * m.ny + j) * m.nz]
+            X.append(m.xs[i]); Y.append(m.ys[j]); W.append(u[3 * n + 2])
+    c0, c1, c2 = post.fit_plane(X, Y, W)
+    r = [w - c0 - c1 * x - c2 * y for x, y, w in zip(X, Y, W)]
+    return max(r) - min(r)
+
+
+def test_v5_layered_band_vs_per_row(oracle_lib):
+    """The reference's check V5 (src/core/15-verify.js:205-235; README.md:353: "104.55 vs 104.47 um
+    (0.08 %)"): the default stack without its bottom build-up (asymmetric, so that it warps), its
+    rows from the database records of the default package's substrate materials, heated from 25 to
+    125 degC on a free 20 x 20 mm box of 16 x 16 elements: one layered element layer per substrate
+    band (Draft, one band per group) against one element layer per physical row."""
+    from tmsolve.pkgmesh import generate_stack
+    from tmsolve.thermal import substrate_box
+    recs = json.load(open(GOLDEN))
+    rows = generate_stack()
+    core = next(q for q, r in enumerate(rows) if r["type"] == "core")
+    asym = rows[:core + 2] + [rows[-1]]
+    xs, ys = linspace(-10, 10, 16), linspace(-10, 10, 16)
+    w = []
+    for per_row in (False, True):
+        pkg = substrate_box(xs, ys, asym, recs, 1, per_row=per_row)
+        om = oracle_lib.OracleModel(pkg)
+        r = om.solve(om.assemble(pkg.step(25.0, 125.0)), tol=1e-10)
+        assert r["converged"]
+        w.append(_bottom_warpage(pkg, r["u"]))
+    assert abs(w[0] / w[1] - 1) < 0.01                          # the check's criterion
+    # the reference's published values, at their printed precision
+    assert f"{1000 * w[0]:.2f}" == "104.55" and f"{1000 * w[1]:.2f}" == "104.47", w
+    assert f"{100 * abs(w[0] / w[1] - 1):.2f}" == "0.08"
