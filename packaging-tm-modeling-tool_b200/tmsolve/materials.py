@@ -353,11 +353,49 @@ def modulus_at(edef: dict, T: float) -> float:
     t = edef["type"]
     if t == "const":
         return _mod_mpa(edef["E"])
+    if t == "table":
+        scale = 1.0 if edef.get("u") == "MPa" else GPA
+        xs, ys = list(edef["T"]), list(edef["v"])
+        if (edef.get("extrap") or "hold") != "linear" and len(xs) > 1:
+            T = min(max(T, xs[0]), xs[-1])
+        if edef.get("interp") == "log":
+            return float(np.exp(interp_table_linear(xs, [float(np.log(v)) for v in ys], T))) * scale
+        return interp_table_linear(xs, ys, T) * scale
     if t == "sigmoid":
         Eg, Er = _mod_mpa(edef["Eg"]), _mod_mpa(edef["Er"])
         w = _pv(edef.get("w")) or SIGMOID_W_DEFAULT
         return Er + (Eg - Er) / (1 + np.exp((T - _pv(edef["TgDMA"])) / w))
     raise ValueError(f"modulus type {t!r} not restated")
+
+
+KELVIN = 273.15
+CTE_INTEGRATION_SUBSTEPS = 8   # 00-constants.js:14
+
+
+def iso_modulus(mat: dict, T: float) -> float:
+    """isoE (03-materials.js:109-116): the record's E(T), above a solder's solidus 1 % of its
+    modulus at the solidus (SOLDER_MOLTEN_FRACTION)."""
+    if mat.get("solidus") is not None:
+        Ts = _pv(mat["solidus"])
+        if T > Ts:
+            return 0.01 * modulus_at(mat["elastic"]["E"], Ts)
+    return modulus_at(mat["elastic"]["E"], T)
+
+
+def silicon_alpha(T: float) -> float:
+    """Instantaneous CTE of silicon, Okada and Tokumaru (1984) (siliconAlpha, 03-materials.js:132-135)."""
+    TK = T + KELVIN
+    return (3.725 * (1 - np.exp(-5.88e-3 * (TK - 124))) + 5.548e-4 * TK) * 1e-6
+
+
+def _simpson(f, a, b, n):
+    if n % 2:
+        n += 1
+    h = (b - a) / n
+    s = f(a) + f(b)
+    for i in range(1, n):
+        s += f(a + i * h) * (4 if i % 2 else 2)
+    return s * h / 3
 
 
 def _softplus(x: float) -> float:
@@ -371,6 +409,8 @@ def cte_at(cdef: dict, T: float) -> float:
     t = cdef["type"]
     if t == "const":
         return _pv(cdef["a"]) * PPM
+    if t == "silicon":
+        return silicon_alpha(T)
     if t == "table":
         xs, ys = cdef["T"], cdef["v"]
         xs = xs["v"] if isinstance(xs, dict) else xs
@@ -398,13 +438,24 @@ def thermal_strain_at(cdef: dict, T: float) -> float:
         d = _pv(cdef.get("delta")) or CTE_SMOOTH_DELTA
         Tg = _pv(cdef["TgTMA"])
         return a1 * (T - T0) + (a2 - a1) * d * (_softplus((T - Tg) / d) - _softplus((T0 - Tg) / d))
+    if t == "table":
+        # piecewise-linear alpha: trapezoids between the break points are exact
+        lo, hi = min(T, T0), max(T, T0)
+        pts = [lo] + [float(x) for x in cdef["T"] if lo < x < hi] + [hi]
+        s = 0.0
+        for i in range(len(pts) - 1):
+            s += 0.5 * (pts[i + 1] - pts[i]) * (cte_at(cdef, pts[i]) + cte_at(cdef, pts[i + 1]))
+        return s if T >= T0 else -s
+    if t == "silicon":
+        n = max(2, 2 * int(np.ceil(abs(T - T0) * CTE_INTEGRATION_SUBSTEPS / 2)))
+        return _simpson(silicon_alpha, T0, T, n)
     raise ValueError(f"CTE type {t!r} not restated")
 
 
 def iso_tables(mat: dict) -> dict:
     """isoTables (03-materials.js:424-433) of an isotropic record: E(T) in MPa and F(T) on the
     1 degC grid, and nu."""
-    E = grid_table(lambda T: modulus_at(mat["elastic"]["E"], T))
+    E = grid_table(lambda T: iso_modulus(mat, T))
     cte = mat.get("cteXY") or mat["cte"]
     F = grid_table(lambda T: thermal_strain_at(cte, T))
     return dict(E=E, F=F, nu=_pv(mat["elastic"]["nu"]))

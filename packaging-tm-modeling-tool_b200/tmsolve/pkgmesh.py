@@ -104,21 +104,25 @@ def generate_stack(**o) -> list:
 
 def default_die(did: str, x: float, y: float) -> dict:
     """defaultDie (02-config.js:58-63), geometry fields."""
-    return dict(id=did, name="Die " + did.lstrip("D"), x=x, y=y, sx=20.0, sy=20.0, t=0.775, rot=0,
+    return dict(id=did, name="Die " + did.lstrip("D"), x=x, y=y, sx=20.0, sy=20.0, t=0.775, rot=0, si="aniso",
                 bump=dict(type="full", rows=3, px=0.150, py=0.150, keepout=0.150, ubm=0.085, sro=0.090, dmax=0.105))
 
 
 def default_config() -> dict:
-    """defaultConfig (02-config.js:140-166): the lidded single-die package, geometry fields."""
+    """defaultConfig (02-config.js:140-166): the lidded single-die package, its geometry, the
+    material ids of its parts, the process temperatures and the BGA grid (materials database,
+    reflow, cycling and post-processing settings are the caller's)."""
     return dict(
         substrate=dict(sx=45.0, sy=45.0, layers=generate_stack()),
+        bga=dict(pitch=1.0, ballH=0.50, inset=1.0),
         packageType="lid",
-        bump=dict(standoff=0.075),
+        bump=dict(standoff=0.075, solder="sac305"),
         dies=[default_die("D1", 0.0, 0.0)],
         modules=[],
-        underfill=dict(Wf=0.8, Hf=0.7),
-        lid=dict(ox=43.0, oy=43.0, tPlate=1.0, footW=3.0, adhT=0.100, blt=0.050),
-        stiffener=dict(ox=53.0, oy=53.0, ringW=4.0, t=0.8, adhT=0.050),
+        underfill=dict(mat="uf9000ae", Wf=0.8, Hf=0.7),
+        lid=dict(mat="cu", ox=43.0, oy=43.0, tPlate=1.0, footW=3.0, adhMat="eccobond3005", adhT=0.100, timMat="tim_gel", blt=0.050),
+        stiffener=dict(mat="cu", ox=53.0, oy=53.0, ringW=4.0, t=0.8, adhMat="eccobond3005", adhT=0.050),
+        process=dict(Tsub=217, Tjoin=217, Tuf=165, Tattach=150),
         mesh=dict(preset="standard"),
     )
 
@@ -140,7 +144,7 @@ def preset_config(which: str, variant: Optional[str] = None) -> dict:
         for d in (d1, d2):
             d["sx"], d["sy"] = 16.0, 24.0
         c["dies"] = [d1, d2]
-        c["stiffener"] = dict(ox=53.0, oy=53.0, ringW=4.0, t=0.8, adhT=0.050)
+        c["stiffener"] = dict(mat="cu", ox=53.0, oy=53.0, ringW=4.0, t=0.8, adhMat="eccobond3005", adhT=0.050)
     elif which == "offset":
         c["packageType"] = "bare"
         c["dies"][0].update(sx=15, sy=15, x=8, y=6)

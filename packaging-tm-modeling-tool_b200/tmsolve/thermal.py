@@ -22,9 +22,9 @@ from typing import Optional
 
 import numpy as np
 
-from .materials import (NU_MAX_GLOBAL, TGRID_MIN, TGRID_N, T_STRAIN_ORIGIN, ec_d, for_grid_segments, grid_mean,
-                        grid_modulus_strain_increment, iso_d, iso_tables, lagrange3_integrals, material_ec,
-                        sublayer_shell_d, substrate_row_ec)
+from .materials import (NU_MAX_GLOBAL, TGRID_MIN, TGRID_N, T_STRAIN_ORIGIN, column_d, ec_d, for_grid_segments, grid_mean,
+                        grid_modulus_strain_increment, iso_d, iso_modulus, iso_tables, lagrange3_integrals, material_ec,
+                        material_tgs, silicon_d, sublayer_shell_d, substrate_row_ec, thermal_strain_at)
 from .mesh import build_structured_mesh, constraints321
 from .packages import CONSTRAINT_SPAN, Package, StepData, box_package
 
@@ -219,3 +219,41 @@ def substrate_box(xs, ys, rows_top_down: list, recs: dict, nb: int, per_row: boo
     return Package(name="substrate box" + (" per row" if per_row else ""), mesh=mesh, group_layered=layered,
                    group_stage=np.zeros(ng, np.int32), group_pset=np.arange(ng, dtype=np.int32), sec_of_layer=sec_of_layer,
                    npset=n, step_fn=step_fn, Ta=25.0, Tb=125.0)
+
+
+# ---- homogeneous groups of database records ----------------------------------------------------
+
+def group_tables(mat: dict, column: bool = False, si_model: str = "aniso", nu_max: float = NU_MAX_GLOBAL) -> dict:
+    """FEModel._prepareGroup (09-assembly.js:253-284) for a homogeneous group of one record: the
+    thermal strains F(T) (TGRID_N, 3: in-plane twice, through-thickness) and either a constant
+    stiffness (cubic silicon, an isotropic record of constant modulus without a solidus) or a
+    stiffness grid (TGRID_N, 36): isotropic D(E(T), nu) (the solder phase as separate columns,
+    ``column``), orthotropic from the record's constants at T."""
+    cxy = mat.get("cteXY") or mat["cte"]
+    cz = mat.get("cteZ") or cxy
+    F = np.zeros((TGRID_N, 3))
+    for i in range(TGRID_N):
+        T = float(TGRID_MIN + i)
+        fxy = thermal_strain_at(cxy, T)
+        F[i] = (fxy, fxy, fxy if cz is cxy else thermal_strain_at(cz, T))
+    el = mat["elastic"]
+    if el["type"] == "cubic":
+        return dict(Dconst=silicon_d(si_model), F=F)
+    if el["type"] == "iso":
+        nu = el["nu"]["v"] if isinstance(el["nu"], dict) else el["nu"]
+        mk = (lambda E: column_d(E, nu)) if column else (lambda E: iso_d(E, nu, nu_max))
+        if el["E"]["type"] == "const" and mat.get("solidus") is None:
+            return dict(Dconst=mk(iso_modulus(mat, float(TGRID_MIN))), F=F)
+        return dict(Dgrid=np.array([mk(iso_modulus(mat, float(TGRID_MIN + i))) for i in range(TGRID_N)]), F=F)
+    if el["type"] == "ortho":
+        return dict(Dgrid=np.array([ec_d(material_ec(mat, float(TGRID_MIN + i)), nu_max) for i in range(TGRID_N)]), F=F)
+    raise ValueError(f"elastic type {el['type']!r} not restated")
+
+
+def group_step(tab: dict, Ta: float, Tb: float):
+    """prepareStep (09-assembly.js:346-365) for a homogeneous group: (D 36, s0 6) of the step."""
+    if "Dconst" in tab:
+        Dc = tab["Dconst"].reshape(6, 6)
+        f = _grid_vec(tab["F"], Tb) - _grid_vec(tab["F"], Ta)
+        return tab["Dconst"].copy(), Dc[:, 0] * f[0] + Dc[:, 1] * f[1] + Dc[:, 2] * f[2]
+    return grid_mean_vec(tab["Dgrid"], Ta, Tb), grid_stress_increment(tab["Dgrid"], tab["F"], Ta, Tb)

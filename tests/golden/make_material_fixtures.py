@@ -8,7 +8,7 @@ import json
 import os
 import sys
 
-IDS = ["uf9000ae", "abf_gl", "cu", "mcl_e_795g", "psr4000"]
+IDS = ["uf9000ae", "abf_gl", "cu", "mcl_e_795g", "psr4000", "sac305", "si", "tim_gel", "eccobond3005"]
 
 
 def values(o):
