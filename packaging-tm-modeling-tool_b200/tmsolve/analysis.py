@@ -135,15 +135,28 @@ def process_chain(pkg: Package, recs: dict) -> list:
     return steps
 
 
-def solve_chain(model, pkg: Package, steps: list, tol: float = 1e-8, **solve_kw):
+def solve_chain(model, pkg: Package, steps: list, tol: float = 1e-8, state_elems=None, **solve_kw):
     """Each step assembled and solved on a model (``assemble``/``assemble_step`` and ``solve``:
-    the oracle's ``OracleModel`` or the library's ``DeviceModel``), increments summed: the state at
-    the chain's end (25 degC), and the solve records."""
+    the oracle's ``OracleModel`` or the library's ``DeviceModel``). The increments are kept as
+    float32, as the analysis stores them (src/core/11-analysis.js:256), and summed: the state at
+    the chain's end (25 degC). With state_elems, the element history states of those elements are
+    marched along (``accumulateStep``), rows of ``post.state_stride`` values. Returns (u, solve
+    records, states or None)."""
+    from .post import state_stride
     assemble = getattr(model, "assemble_step", None) or model.assemble
     u = np.zeros(3 * pkg.mesh.nn)
-    recs = []
+    recs, S, stride = [], None, 0
+    if state_elems is not None:
+        state_elems = np.ascontiguousarray(state_elems, np.int32)
+        stride = state_stride(pkg.step(steps[0][0], steps[0][1], stage=steps[0][2]))
+        S = np.zeros(stride * len(state_elems))
     for k, (a, b, st) in enumerate(steps):
-        r = model.solve(assemble(pkg.step(a, b, stage=st)), tol=tol, key=k, **solve_kw)
-        u += r["u"]
+        step = pkg.step(a, b, stage=st)
+        r = model.solve(assemble(step), tol=tol, key=k, **solve_kw)
+        du = r["u"].astype(np.float32).astype(np.float64)
+        u += du
         recs.append(r)
-    return u, recs
+        if S is not None:
+            model.set_sublayers(step)
+            model.accumulate_state(du, state_elems, stride, S)
+    return u, recs, (S.reshape(-1, stride) if S is not None else None)

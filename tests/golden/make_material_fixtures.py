@@ -4,11 +4,13 @@ parameter reduced to its value and unit. Run in a container that holds the refer
 
     python tests/golden/make_material_fixtures.py /path/to/reference/src/materials-db.json
 """
+import copy
 import json
 import os
 import sys
 
-IDS = ["uf9000ae", "abf_gl", "cu", "mcl_e_795g", "psr4000", "sac305", "si", "tim_gel", "eccobond3005"]
+IDS = ["uf9000ae", "abf_gl", "cu", "mcl_e_795g", "psr4000", "sac305", "si", "tim_gel", "eccobond3005", "mcl_e_705g",
+       "mcl_e_795g_lh"]
 
 
 def values(o):
@@ -21,10 +23,31 @@ def values(o):
     return o
 
 
+def expand(m, by_id):
+    """A preset record (presetOf + override) as its complete record, as the tool's
+    buildMaterialLibrary expands it: the base record, the preset's own fields, then each override
+    path set."""
+    if not m.get("presetOf"):
+        return m
+    r = copy.deepcopy(by_id[m["presetOf"]])
+    r.update({k: copy.deepcopy(v) for k, v in m.items() if k != "override"})
+    for path, val in (m.get("override") or {}).items():
+        o = r
+        ks = path.split(".")
+        for k in ks[:-1]:
+            o = o.setdefault(k, {})
+        o[ks[-1]] = copy.deepcopy(val)
+    return r
+
+
 def main(path):
     db = json.load(open(path))
-    out = {m["id"]: {k: values(m[k]) for k in ("elastic", "cte", "cteXY", "cteZ", "solidus") if k in m}
-           for m in db["materials"] if m["id"] in IDS}
+    by_id = {m["id"]: m for m in db["materials"]}
+    out = {}
+    for m in db["materials"]:
+        if m["id"] in IDS:
+            m = expand(m, by_id)
+            out[m["id"]] = {k: values(m[k]) for k in ("elastic", "cte", "cteXY", "cteZ", "solidus") if k in m}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "materials_subset.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

@@ -37,9 +37,55 @@ def test_default_package_rt_warpage(oracle_lib):
     cfg = default_config()
     pkg = process_package(cfg, recs, "draft")
     om = oracle_lib.OracleModel(pkg)
-    u, rs = solve_chain(om, pkg, process_chain(pkg, recs))
+    u, rs, _ = solve_chain(om, pkg, process_chain(pkg, recs))
     assert all(r["converged"] for r in rs)
     b = post.bga_sites(sx=cfg["substrate"]["sx"], sy=cfg["substrate"]["sy"], inset=cfg["bga"]["inset"], pitch=cfg["bga"]["pitch"])
     z = b["zone"]
     w = om.warpage_jeita(u, b["x"], b["y"], [z["x0"], z["x1"], z["y0"], z["y1"]])
     assert f"{1000 * w['signed']:.2f}" == "-69.34", w["signed"]
+
+
+def _rt(oracle_lib, cfg, recs, die_stress=False):
+    """The as-assembled 25 degC state of a configuration at Draft on the oracle: the signed JEITA
+    warpage (mm) and, with die_stress, the first die's backside (top face) stress reader."""
+    from tmsolve.mesh import PART
+    pkg = process_package(cfg, recs, "draft")
+    om = oracle_lib.OracleModel(pkg)
+    elems, d, group = None, None, None
+    if die_stress:
+        d = pkg.meta["mesh_info"]["geometry"]["dies"][0]
+        group = 3                                # packageGroups: substrate, solder, underfill, then the dies
+        kp = post.plane_index(pkg.mesh, d["ztop"])
+        elems = np.array([e for (_, _, e) in post.die_elements(pkg.mesh, d["rect"], kp - 1, PART["DIE"], group)[0]], np.int32)
+    u, rs, S = solve_chain(om, pkg, process_chain(pkg, recs), state_elems=elems)
+    assert all(r["converged"] for r in rs)
+    b = post.bga_sites(sx=cfg["substrate"]["sx"], sy=cfg["substrate"]["sy"], inset=cfg["bga"]["inset"], pitch=cfg["bga"]["pitch"])
+    z = b["zone"]
+    w = om.warpage_jeita(u, b["x"], b["y"], [z["x0"], z["x1"], z["y0"], z["y1"]])["signed"]
+    ds = None
+    if die_stress:
+        ds = post.die_surface_stress(om, S, elems, S.shape[1], d["rect"], d["ztop"], d["zaf"], PART["DIE"], group, "top")
+    return w, ds
+
+
+def test_v9_presets(oracle_lib):
+    """The reference's check V9 (src/core/15-verify.js:339-357) at Draft, its published values
+    (README.md:358: "bare RT +222.7 um convex; backside +65.8 MPa tensile; 0.8 mm core 166.0 vs
+    285.8 um; 795G LH 169.5 vs 705G 263.6 um") to their printed digits: the bare-die preset's
+    room-temperature warpage and die backside interior peak stress, the core-thickness study's
+    two variants, and the bare package with the 705G and the 795G Type LH cores."""
+    from tmsolve.pkgmesh import preset_config
+    recs = json.load(open(GOLDEN))
+    w, ds = _rt(oracle_lib, preset_config("bare"), recs, die_stress=True)
+    assert f"{1000 * w:.1f}" == "222.7" and f"{ds['peakInterior']:.1f}" == "65.8", (w, ds["peakInterior"])
+    wa, _ = _rt(oracle_lib, preset_config("coreStudy", "A"), recs)
+    wb, _ = _rt(oracle_lib, preset_config("coreStudy", "B"), recs)
+    assert f"{1000 * wa:.1f}" == "285.8" and f"{1000 * wb:.1f}" == "166.0", (wa, wb)
+    cores = {}
+    for core in ("mcl_e_705g", "mcl_e_795g_lh"):
+        cfg = preset_config("bare")
+        for r in cfg["substrate"]["layers"]:
+            if r["type"] == "core":
+                r["mat"] = core
+        cores[core], _ = _rt(oracle_lib, cfg, recs)
+    assert f"{1000 * cores['mcl_e_705g']:.1f}" == "263.6" and f"{1000 * cores['mcl_e_795g_lh']:.1f}" == "169.5", cores
