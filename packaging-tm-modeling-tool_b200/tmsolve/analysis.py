@@ -18,6 +18,7 @@ oracle) and sums the increments.
 """
 from __future__ import annotations
 
+import math
 from typing import Optional
 
 import numpy as np
@@ -133,6 +134,96 @@ def process_chain(pkg: Package, recs: dict) -> list:
         pts = thermal_path_points(float(Ta), float(Tb), stage_tgs(pkg, recs, st), stops)
         steps += [(a, b, st) for a, b in zip(pts[:-1], pts[1:])]
     return steps
+
+
+CYCLE_DT_STEP, CYCLE_DT_FINE, CYCLE_TG_BAND = 10.0, 5.0, 15.0     # 00-constants.js:106-108
+REFLOW_DT, REFLOW_DT_FINE = 15.0, 10.0
+
+
+def _js_round(x: float) -> float:
+    return math.floor(x + 0.5)
+
+
+def temperature_samples(Tmin: float, Tmax: float, tgs, extras=()) -> list:
+    """temperatureSamples (11-analysis.js:29-40): every 10 degC, every 5 degC within 15 degC of a
+    glass transition, both ends and the extras, rounded to 1e-3 degC, ascending."""
+    out = set()
+
+    def add(T):
+        if Tmin - 1e-9 <= T <= Tmax + 1e-9:
+            out.add(_js_round(T * 1000) / 1000)
+    add(Tmin)
+    add(Tmax)
+    T = math.ceil(Tmin / CYCLE_DT_STEP) * CYCLE_DT_STEP
+    while T <= Tmax:
+        add(T)
+        T += CYCLE_DT_STEP
+    for tg in tgs:
+        T = math.ceil((tg - CYCLE_TG_BAND) / CYCLE_DT_FINE) * CYCLE_DT_FINE
+        while T <= tg + CYCLE_TG_BAND:
+            add(T)
+            T += CYCLE_DT_FINE
+    for T in extras:
+        add(T)
+    return sorted(out)
+
+
+def _solidus(pkg: Package, recs: dict) -> float:
+    sol = recs[pkg.meta["cfg"]["bump"]["solder"]].get("solidus")
+    return float(sol["v"] if isinstance(sol, dict) else sol) if sol is not None else SOLIDUS_DEFAULT
+
+
+def evaluation_temperatures(pkg: Package, recs: dict) -> dict:
+    """evaluationTemperatures (11-analysis.js:132-144) of a full analysis: the cycling samples
+    (with 25 degC) and the reflow sweep above the cycling range (every 15 degC, 10 degC near a
+    glass transition, the solidus and one degree above it, the report temperatures, the peak)."""
+    cfg = pkg.meta["cfg"]
+    tgs = stage_tgs(pkg, recs)
+    cyc = temperature_samples(cfg["cycling"]["Tmin"], cfg["cycling"]["Tmax"], tgs, [25])
+    peak = cfg["reflow"]["peak"]
+    sol = _solidus(pkg, recs)
+    ref = {25, peak, sol, sol + 1, *cfg["reflow"]["reportTemps"]}
+    T = math.ceil(cfg["cycling"]["Tmax"] / REFLOW_DT) * REFLOW_DT
+    while T <= peak:
+        ref.add(T)
+        T += REFLOW_DT
+    for tg in tgs:
+        T = math.ceil((tg - CYCLE_TG_BAND) / REFLOW_DT_FINE) * REFLOW_DT_FINE
+        while T <= tg + CYCLE_TG_BAND:
+            ref.add(T)
+            T += REFLOW_DT_FINE
+    ref = sorted(float(T) for T in ref if 25 <= T <= peak)
+    return dict(all=sorted(set(cyc) | set(ref)), cycling=cyc, reflow=ref)
+
+
+def full_path(pkg: Package, recs: dict) -> dict:
+    """buildPath (11-analysis.js:146-175) of a full analysis of monolithic dies, in its solve order:
+    the chain's S0 and S1 steps, the chip-join branch (T_UF -> 25 degC in S1), the rest of the
+    chain, then the sweep branches in the final stage from 25 degC down to the coldest and up to
+    the hottest evaluation temperature, stopping at every one. Returns dict(steps: [(Ta, Tb,
+    stage, branch)], chain, cpi, down, up: step indices, temps)."""
+    cfg = pkg.meta["cfg"]
+    p = cfg["process"]
+    fin = 2 if cfg["packageType"] == "bare" else 3
+    temps = evaluation_temperatures(pkg, recs)
+    solidi = [_solidus(pkg, recs)]
+    steps = []
+
+    def seg(Ta, Tb, stage, branch, stops=()):
+        pts = thermal_path_points(float(Ta), float(Tb), stage_tgs(pkg, recs, stage), list(stops) + solidi)
+        ids = []
+        for a, b in zip(pts[:-1], pts[1:]):
+            steps.append((a, b, stage, branch))
+            ids.append(len(steps) - 1)
+        return ids
+    s0 = seg(p["Tsub"], p["Tjoin"], 0, "chain") if abs(p["Tsub"] - p["Tjoin"]) > 1e-9 else []
+    s1 = seg(p["Tjoin"], p["Tuf"], 1, "chain")
+    cpi = seg(p["Tuf"], 25, 1, "cpi")
+    rest = seg(p["Tuf"], p["Tattach"], 2, "chain") + seg(p["Tattach"], 25, 3, "chain") if fin == 3 else seg(p["Tuf"], 25, 2, "chain")
+    ev = temps["all"]
+    down = seg(25, min([25] + ev), fin, "down", ev)
+    up = seg(25, max([25] + ev), fin, "up", ev)
+    return dict(steps=steps, chain=s0 + s1 + rest, cpi=cpi, down=down, up=up, temps=temps)
 
 
 def solve_chain(model, pkg: Package, steps: list, tol: float = 1e-8, state_elems=None, **solve_kw):

@@ -89,3 +89,21 @@ def test_v9_presets(oracle_lib):
                 r["mat"] = core
         cores[core], _ = _rt(oracle_lib, cfg, recs)
     assert f"{1000 * cores['mcl_e_705g']:.1f}" == "263.6" and f"{1000 * cores['mcl_e_795g_lh']:.1f}" == "169.5", cores
+
+
+def test_default_package_full_path():
+    """A full analysis of the default package solves one step per piece of its thermal path: 67
+    steps (README.md:370), the chain (15), the chip-join branch T_UF -> 25 degC in S1, and the sweeps
+    from 25 degC down to -40 and up to the 260 degC reflow peak through every evaluation
+    temperature (the cycling samples every 10 degC, 5 near a Tg; the reflow sweep; the solidus)."""
+    from tmsolve.analysis import full_path
+    recs = json.load(open(GOLDEN))
+    fp = full_path(process_package(default_config(), recs, "draft"), recs)
+    assert len(fp["steps"]) == 67
+    assert len(fp["chain"]) == 15 and len(fp["cpi"]) == 10
+    t = fp["temps"]
+    assert t["all"][0] == -40.0 and t["all"][-1] == 260.0 and 217.0 in t["all"] and 218.0 in t["all"]
+    assert fp["steps"][fp["down"][-1]][1] == -40.0 and fp["steps"][fp["up"][-1]][1] == 260.0
+    # every evaluation temperature is the end of a sweep step
+    ends = {fp["steps"][k][1] for k in fp["down"] + fp["up"]}
+    assert set(t["all"]) - {25.0} <= ends
