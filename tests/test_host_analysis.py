@@ -107,3 +107,31 @@ def test_default_package_full_path():
     # every evaluation temperature is the end of a sweep step
     ends = {fp["steps"][k][1] for k in fp["down"] + fp["up"]}
     assert set(t["all"]) - {25.0} <= ends
+
+
+def test_v11_solver_integrity(oracle_lib):
+    """The reference's check V11 (src/core/15-verify.js:368-393; README.md:360: "residual 7.5e-11
+    (20 iterations), reactions 2.3e-10 of the force scale, energy balance 5.7e-14"): the default
+    package's chain at Draft with the solver at 1e-10, each step keyed by its index (so that it
+    warm-starts from the stored solutions of the steps before it). The last step (S3 30 -> 25 degC)
+    takes the published 20 iterations to the published residual; a re-solve from the stored
+    solution, against the unconstrained operator and load, leaves the published reactions at the
+    supports; the energy balance is at rounding level (the published 5.7e-14 is one rounding)."""
+    recs = json.load(open(GOLDEN))
+    pkg = process_package(default_config(), recs, "draft")
+    om = oracle_lib.OracleModel(pkg)
+    steps = process_chain(pkg, recs)
+    _, rs, _ = solve_chain(om, pkg, steps, tol=1e-10)
+    last = rs[-1]
+    assert steps[-1] == (30.0, 25.0, 3)
+    assert last["iters"] == 20 and f"{last['relres']:.1e}" == "7.5e-11", (last["iters"], last["relres"])
+    a, b, st = steps[-1]
+    step = pkg.step(a, b, stage=st)
+    u = om.solve(om.assemble(step), tol=1e-10, key=len(steps) - 1)["u"]
+    f = om.assemble(step, no_constraints=True)
+    Ku = om.matvec(u)
+    fscale = max(np.abs(Ku).max(), np.abs(f).max())
+    con = pkg.mesh.constraints
+    reac = np.abs(Ku[con] - f[con]).max() / fscale
+    assert f"{reac:.1e}" == "2.3e-10", reac
+    assert abs(u @ Ku - f @ u) / abs(f @ u) < 1e-12
