@@ -6,9 +6,13 @@
 // CPU baseline of bench.py; nothing in the product links or calls it.
 //
 // Parity is pinned by the reference's own analytic known-answer tests
-// (src/core/15-verify.js V1, V2, V3, V6, V16, V18(4)), re-implemented in
-// tests/test_oracle_known_answers.py; the reference publishes no golden
-// vector files and its JavaScript cannot be run here (no JS engine).
+// (src/core/15-verify.js V1, V2, V3, V4, V6, V16, V18(4)), re-implemented in
+// tests/test_oracle_known_answers.py, and by its published whole-package
+// results on its own models (V5, V9, V11, the default package's room-
+// temperature warpage), reproduced through the host's restated model building
+// in tests/test_host_analysis.py and tests/test_host_thermal.py; the reference
+// publishes no golden vector files and its JavaScript cannot be run here (no
+// JS engine).
 //
 // Loop orders follow the reference line by line so that the summation order
 // of every dot product, matvec and factorisation is the same; the file is
