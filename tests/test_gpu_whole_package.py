@@ -1,0 +1,76 @@
+"""The tool's process chain solved on the GPU, on the reference's own models built by the restated
+model-building side (the mesher, the substrate bands, the parts' tables from the database records
+of tests/golden/materials_subset.json, the chain's stages with their births).
+
+* The default package at Draft (65,322 DOF, 15 steps 217 -> 165 -> 150 -> 25 degC): every step's
+  increment within 1e-8 of the oracle's in FP64 and 1e-5 in mixed precision (both solved to
+  relative residual 1e-12; the oracle takes about a minute on one core), and the room-temperature
+  JEITA warpage at the reference's published -69.34 um (README.md:91) to its printed digits.
+* The bare-die preset (V9, src/core/15-verify.js:339-357; README.md:358): the warpage +222.7 um
+  and the die backside interior peak +65.8 MPa from the die's element states marched on the
+  device (accumulateStep, stateStress), to their printed digits."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tmsolve import post
+from tmsolve.analysis import process_chain, process_package, solve_chain
+from tmsolve.pkgmesh import default_config, preset_config
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "materials_subset.json")
+
+
+def _bga(cfg):
+    return post.bga_sites(sx=cfg["substrate"]["sx"], sy=cfg["substrate"]["sy"], inset=cfg["bga"]["inset"], pitch=cfg["bga"]["pitch"])
+
+
+def test_default_package_chain_on_gpu(oracle_lib):
+    from tmsolve.solver import DeviceModel
+    recs = json.load(open(GOLDEN))
+    cfg = default_config()
+    pkg = process_package(cfg, recs, "draft")
+    steps = process_chain(pkg, recs)
+    b = _bga(cfg)
+    z = b["zone"]
+    om = oracle_lib.OracleModel(pkg)
+    uo, ro, _ = solve_chain(om, pkg, steps, tol=1e-12)
+    assert all(r["converged"] for r in ro)
+    wo = om.warpage_jeita(uo, b["x"], b["y"], [z["x0"], z["x1"], z["y0"], z["y1"]])["signed"]
+    for precision, bar in (("fp64", 1e-8), ("mixed", 1e-5)):
+        dm = DeviceModel(pkg)                    # its own stored solutions: the same warm starts as the oracle's
+        try:
+            u, rs, _ = solve_chain(dm, pkg, steps, tol=1e-12, precision=precision)
+            assert all(r["converged"] for r in rs), (precision, [r["relres"] for r in rs])
+            for k, (r, o) in enumerate(zip(rs, ro)):
+                assert np.linalg.norm(r["u"] - o["u"]) <= bar * np.linalg.norm(o["u"]), (precision, k)
+            w = post.warpage_jeita(b, lambda x, y: dm.sample_plane(u, 0, 2, x, y))["signed"]
+        finally:
+            dm.close()
+        assert abs(w / wo - 1) <= bar, (precision, w, wo)
+        assert f"{1000 * w:.2f}" == "-69.34", (precision, w)
+
+
+def test_bare_die_v9_on_gpu():
+    from tmsolve.mesh import PART
+    from tmsolve.solver import DeviceModel
+    recs = json.load(open(GOLDEN))
+    cfg = preset_config("bare")
+    pkg = process_package(cfg, recs, "draft")
+    d = pkg.meta["mesh_info"]["geometry"]["dies"][0]
+    group = 3                                    # packageGroups: substrate, solder, underfill, then the dies
+    kp = post.plane_index(pkg.mesh, d["ztop"])
+    elems = np.array([e for (_, _, e) in post.die_elements(pkg.mesh, d["rect"], kp - 1, PART["DIE"], group)[0]], np.int32)
+    b = _bga(cfg)
+    dm = DeviceModel(pkg)
+    try:
+        u, rs, S = solve_chain(dm, pkg, process_chain(pkg, recs), state_elems=elems)
+        assert all(r["converged"] for r in rs)
+        w = post.warpage_jeita(b, lambda x, y: dm.sample_plane(u, 0, 2, x, y))["signed"]
+        ds = post.die_surface_stress(dm, S, elems, S.shape[1], d["rect"], d["ztop"], d["zaf"], PART["DIE"], group, "top")
+    finally:
+        dm.close()
+    assert f"{1000 * w:.1f}" == "222.7" and f"{ds['peakInterior']:.1f}" == "65.8", (w, ds["peakInterior"])
