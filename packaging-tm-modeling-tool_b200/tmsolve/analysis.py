@@ -1,4 +1,4 @@
-"""The process chain of the tool's analysis for packages of monolithic dies, on the host: the
+"""The process chain of the tool's analysis, on the host: the
 model that ``Analysis.build`` makes (src/core/11-analysis.js:100-113: ``buildPackageMesh``, then
 ``FEModel`` with the configuration's materials) and the chain of ``buildPath`` (:146-175), whose
 summed increments are the as-assembled state at 25 degC:
@@ -25,25 +25,41 @@ import numpy as np
 
 from .materials import material_tgs
 from .packages import Package, StepData
-from .pkgmesh import build_package_mesh
+from .pkgmesh import STAGE, build_package_mesh
 from .thermal import band_section, group_step, group_tables, section_step, thermal_path_points
 
 SOLIDUS_DEFAULT = 217.0
 
 
 def _groups(cfg: dict, g: dict) -> list:
-    """(record id, birth stage, column phase, silicon model) of the homogeneous groups in packageGroups order
-    (06-mesher.js:310-322): solder (stage 1, separate columns), underfill (2), the dies (1), then
-    TIM, lid and lid adhesive or stiffener and its adhesive (3)."""
-    out = [(cfg["bump"]["solder"], 1, True, None), (cfg["underfill"]["mat"], 2, False, None)]
-    for d, dc in zip(g["dies"], cfg["dies"]):
-        out.append(("si", 1, False, dc.get("si", "aniso")))
+    """The homogeneous groups in packageGroups order (06-mesher.js:310-345), each dict(mat: record
+    id, stage: birth stage, column: separate columns, si: silicon model, series: (record id, height
+    fraction) of a second material in series along the columns): solder (stage 1, columns),
+    underfill (2), the dies (1), then TIM, lid and lid adhesive or stiffener and its adhesive (3);
+    with stacked modules, per module its chiplets, Si base and TSV Cu, then the DDI microbumps (a
+    solder cap on a Cu pillar), all born at chiplet join (-3), the wafer underfill (-2) and the
+    wafer mold (-1)."""
+    grp = lambda mat, stage, column=False, si=None, series=None: dict(mat=mat, stage=stage, column=column, si=si, series=series)
+    out = [grp(cfg["bump"]["solder"], 1, True), grp(cfg["underfill"]["mat"], 2)]
+    for dc in cfg["dies"]:
+        out.append(grp("si", 1, si=dc.get("si", "aniso")))
     if g["lid"]:
         L = cfg["lid"]
-        out += [(L["timMat"], 3, False, None), (L["mat"], 3, False, None), (L["adhMat"], 3, False, None)]
+        out += [grp(L["timMat"], 3), grp(L["mat"], 3), grp(L["adhMat"], 3)]
     if g["stiff"]:
         S = cfg["stiffener"]
-        out += [(S["mat"], 3, False, None), (S["adhMat"], 3, False, None)]
+        out += [grp(S["mat"], 3), grp(S["adhMat"], 3)]
+    if g["modules"]:
+        st, S = cfg["stack"], STAGE
+        for m in g["modules"]:
+            out += [grp("si", S["DDI"], si=c["si"]) for c in m["chiplets"]]
+            out.append(grp("si", S["DDI"], si=m["si"]))
+            if m["tsv"] > 0:
+                out.append(grp("cu", S["DDI"]))
+        out.append(grp(st["ddi"]["solder"], S["DDI"], column=True, series=("cu", st["ddi"]["pillarH"] / st["ddi"]["standoff"])))
+        if g["wcuf"]:
+            out.append(grp(st["wcuf"]["mat"], S["WCUF"]))
+        out.append(grp(st["moldMat"], S["MOLD"]))
     return out
 
 
@@ -68,7 +84,8 @@ def process_package(cfg: dict, recs: dict, preset: str = "draft", override: Opti
             if b["z0"] < zc < b["z1"]:
                 sec_of_layer[k] = q
     hom = _groups(cfg, g)
-    tabs = [group_tables(recs[mid], column=col, si_model=si or "aniso") for (mid, _, col, si) in hom]
+    tabs = [group_tables(recs[h["mat"]], column=h["column"], si_model=h["si"] or "aniso",
+                         series=(recs[h["series"][0]], h["series"][1]) if h["series"] else None) for h in hom]
     n = nb + len(hom)
 
     def step_fn(Ta, Tb):
@@ -85,7 +102,7 @@ def process_package(cfg: dict, recs: dict, preset: str = "draft", override: Opti
 
     return Package(name=f"process model, {info['preset']} mesh", mesh=mesh,
                    group_layered=np.array([1] + [0] * len(hom), np.int32),
-                   group_stage=np.array([0] + [st for (_, st, _, _) in hom], np.int32),
+                   group_stage=np.array([0] + [h["stage"] for h in hom], np.int32),
                    group_pset=np.array([0] + [nb + q for q in range(len(hom))], np.int32), sec_of_layer=sec_of_layer,
                    npset=n, step_fn=step_fn, Ta=float(cfg["process"]["Tattach"]), Tb=25.0,
                    meta=dict(mesh_info=info, cfg=cfg, groups=hom, bottom_plane=0,
@@ -103,9 +120,9 @@ def stage_tgs(pkg: Package, recs: dict, stage: Optional[int] = None) -> list:
         if mid and mid not in seen:
             seen.add(mid)
             out.extend(material_tgs(recs[mid]))
-    for (mid, st, _, _) in pkg.meta["groups"]:
-        if stage is None or st <= stage:
-            add(mid)
+    for h in pkg.meta["groups"]:
+        if stage is None or h["stage"] <= stage:
+            add(h["mat"])
     if stage is None or stage >= 0:
         for r in cfg["substrate"]["layers"]:
             add(r.get("mat"))
@@ -113,15 +130,31 @@ def stage_tgs(pkg: Package, recs: dict, stage: Optional[int] = None) -> list:
     return out
 
 
+def _module_segments(cfg: dict) -> tuple:
+    """buildPath's stacked-module segments (11-analysis.js:169-175): chiplet join T_ddi -> T_fill
+    (the wafer underfill's cure temperature, or the mold's for a mold-only fill) in stage DDI, then
+    T_wcuf -> T_mold in stage WCUF (wafer underfill only) and T_mold -> T_sub in stage MOLD.
+    Returns (the join segment, the segments after it)."""
+    if not cfg.get("modules"):
+        return [], []
+    st, S = cfg["stack"], STAGE
+    mp = st["process"]
+    wcuf = st["fill"] == "wcuf"
+    join = [(mp["Tddi"], mp["Twcuf"] if wcuf else mp["Tmold"], S["DDI"])]
+    rest = ([(mp["Twcuf"], mp["Tmold"], S["WCUF"])] if wcuf else []) + [(mp["Tmold"], cfg["process"]["Tsub"], S["MOLD"])]
+    return join, rest
+
+
 def process_chain(pkg: Package, recs: dict) -> list:
-    """The chain of buildPath (11-analysis.js:146-175): (Ta, Tb, stage) of every step from the
-    substrate's stress-free temperature to 25 degC."""
+    """The chain of buildPath (11-analysis.js:146-182): (Ta, Tb, stage) of every step from the
+    first process temperature to 25 degC: the stacked modules' stages first (when the package
+    has any), then the substrate's."""
     cfg = pkg.meta["cfg"]
     p = cfg["process"]
-    sol = recs[cfg["bump"]["solder"]].get("solidus")
-    stops = [float(sol["v"] if isinstance(sol, dict) else sol) if sol is not None else SOLIDUS_DEFAULT]
+    stops = _solidi(pkg, recs)
     final = 2 if cfg["packageType"] == "bare" else 3
-    segs = []
+    join, mrest = _module_segments(cfg)
+    segs = join + mrest
     if abs(p["Tsub"] - p["Tjoin"]) > 1e-9:
         segs.append((p["Tsub"], p["Tjoin"], 0))
     segs.append((p["Tjoin"], p["Tuf"], 1))
@@ -173,6 +206,18 @@ def _solidus(pkg: Package, recs: dict) -> float:
     return float(sol["v"] if isinstance(sol, dict) else sol) if sol is not None else SOLIDUS_DEFAULT
 
 
+def _solidi(pkg: Package, recs: dict) -> list:
+    """The path's solidus stops (11-analysis.js:127-130): the flip chip solder's, and the DDI
+    microbump solder's when the package has stacked modules and its record gives one."""
+    out = [_solidus(pkg, recs)]
+    cfg = pkg.meta["cfg"]
+    if cfg.get("modules"):
+        sol = recs[cfg["stack"]["ddi"]["solder"]].get("solidus")
+        if sol is not None:
+            out.append(float(sol["v"] if isinstance(sol, dict) else sol))
+    return out
+
+
 def evaluation_temperatures(pkg: Package, recs: dict) -> dict:
     """evaluationTemperatures (11-analysis.js:132-144) of a full analysis: the cycling samples
     (with 25 degC) and the reflow sweep above the cycling range (every 15 degC, 10 degC near a
@@ -181,8 +226,9 @@ def evaluation_temperatures(pkg: Package, recs: dict) -> dict:
     tgs = stage_tgs(pkg, recs)
     cyc = temperature_samples(cfg["cycling"]["Tmin"], cfg["cycling"]["Tmax"], tgs, [25])
     peak = cfg["reflow"]["peak"]
-    sol = _solidus(pkg, recs)
-    ref = {25, peak, sol, sol + 1, *cfg["reflow"]["reportTemps"]}
+    ref = {25, peak, *cfg["reflow"]["reportTemps"]}
+    for sol in _solidi(pkg, recs):
+        ref |= {sol, sol + 1}
     T = math.ceil(cfg["cycling"]["Tmax"] / REFLOW_DT) * REFLOW_DT
     while T <= peak:
         ref.add(T)
@@ -197,16 +243,18 @@ def evaluation_temperatures(pkg: Package, recs: dict) -> dict:
 
 
 def full_path(pkg: Package, recs: dict) -> dict:
-    """buildPath (11-analysis.js:146-175) of a full analysis of monolithic dies, in its solve order:
-    the chain's S0 and S1 steps, the chip-join branch (T_UF -> 25 degC in S1), the rest of the
-    chain, then the sweep branches in the final stage from 25 degC down to the coldest and up to
-    the hottest evaluation temperature, stopping at every one. Returns dict(steps: [(Ta, Tb,
-    stage, branch)], chain, cpi, down, up: step indices, temps)."""
+    """buildPath (11-analysis.js:146-182) of a full analysis, in its solve order: the stacked
+    modules' chiplet join, its 'ddi' branch (T_fill -> 25 degC in stage DDI) and the module fill
+    and mold cures (when the package has modules), the chain's S0 and S1 steps, the chip-join
+    branch (T_UF -> 25 degC in S1), the rest of the chain, then the sweep branches in the final
+    stage from 25 degC down to the coldest and up to the hottest evaluation temperature, stopping
+    at every one. Returns dict(steps: [(Ta, Tb, stage, branch)], chain, cpi, down, up, ddiJoin,
+    ddi: step indices, temps)."""
     cfg = pkg.meta["cfg"]
     p = cfg["process"]
     fin = 2 if cfg["packageType"] == "bare" else 3
     temps = evaluation_temperatures(pkg, recs)
-    solidi = [_solidus(pkg, recs)]
+    solidi = _solidi(pkg, recs)
     steps = []
 
     def seg(Ta, Tb, stage, branch, stops=()):
@@ -216,6 +264,12 @@ def full_path(pkg: Package, recs: dict) -> dict:
             steps.append((a, b, stage, branch))
             ids.append(len(steps) - 1)
         return ids
+    # stacked modules first: chiplet join, the 'ddi' branch (the joined module cooled to 25 degC before
+    # its fill is born), then the fill and mold cures up to the substrate's stress-free temperature
+    join, mrest = _module_segments(cfg)
+    sm_join = [k for (Ta, Tb, st) in join for k in seg(Ta, Tb, st, "chain")]
+    ddi = seg(join[0][1], 25, STAGE["DDI"], "ddi") if join else []
+    sm = sm_join + [k for (Ta, Tb, st) in mrest for k in seg(Ta, Tb, st, "chain")]
     s0 = seg(p["Tsub"], p["Tjoin"], 0, "chain") if abs(p["Tsub"] - p["Tjoin"]) > 1e-9 else []
     s1 = seg(p["Tjoin"], p["Tuf"], 1, "chain")
     cpi = seg(p["Tuf"], 25, 1, "cpi")
@@ -223,16 +277,18 @@ def full_path(pkg: Package, recs: dict) -> dict:
     ev = temps["all"]
     down = seg(25, min([25] + ev), fin, "down", ev)
     up = seg(25, max([25] + ev), fin, "up", ev)
-    return dict(steps=steps, chain=s0 + s1 + rest, cpi=cpi, down=down, up=up, temps=temps)
+    return dict(steps=steps, chain=sm + s0 + s1 + rest, cpi=cpi, down=down, up=up, temps=temps, ddiJoin=sm_join, ddi=ddi)
 
 
-def solve_chain(model, pkg: Package, steps: list, tol: float = 1e-8, state_elems=None, **solve_kw):
+def solve_chain(model, pkg: Package, steps: list, tol: float = 1e-8, state_elems=None, state_f32: bool = True, **solve_kw):
     """Each step assembled and solved on a model (``assemble``/``assemble_step`` and ``solve``:
-    the oracle's ``OracleModel`` or the library's ``DeviceModel``). The increments are kept as
-    float32, as the analysis stores them (src/core/11-analysis.js:256), and summed: the state at
-    the chain's end (25 degC). With state_elems, the element history states of those elements are
-    marched along (``accumulateStep``), rows of ``post.state_stride`` values. Returns (u, solve
-    records, states or None)."""
+    the oracle's ``OracleModel`` or the library's ``DeviceModel``), as ``Analysis.run`` does
+    (src/core/11-analysis.js:209-214, ``finishPath`` :230-256): the increments summed in double
+    precision give the state at the chain's end (25 degC). With state_elems, the element history
+    states of those elements are marched along (``accumulateStep``), rows of
+    ``post.state_stride`` values, from the increments as the analysis keeps them for its element
+    histories: rounded to float32 (``finishPath``), or in double precision with state_f32=False
+    (the increments of ``solveStep`` used directly). Returns (u, solve records, states or None)."""
     from .post import state_stride
     assemble = getattr(model, "assemble_step", None) or model.assemble
     u = np.zeros(3 * pkg.mesh.nn)
@@ -244,10 +300,10 @@ def solve_chain(model, pkg: Package, steps: list, tol: float = 1e-8, state_elems
     for k, (a, b, st) in enumerate(steps):
         step = pkg.step(a, b, stage=st)
         r = model.solve(assemble(step), tol=tol, key=k, **solve_kw)
-        du = r["u"].astype(np.float32).astype(np.float64)
-        u += du
+        u += r["u"]
         recs.append(r)
         if S is not None:
+            du = r["u"].astype(np.float32).astype(np.float64) if state_f32 else r["u"]
             model.set_sublayers(step)
             model.accumulate_state(du, state_elems, stride, S)
     return u, recs, (S.reshape(-1, stride) if S is not None else None)

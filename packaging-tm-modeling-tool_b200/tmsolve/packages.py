@@ -348,7 +348,7 @@ def reference_package(preset: str = "draft", cfg: Optional[dict] = None, Ta: flo
         for b, (b0, b1) in enumerate(bands):
             if b0 < zc < b1:
                 sec_of_layer[k] = b
-    roles = ["sub", "solder", "uf"] + ["die"] * len(g["dies"])
+    roles = ["sub", "solder", "uf"] + ["die"] * len(g["monoDies"])
     if g["lid"]:
         roles += ["tim", "lid", "lidadh"]
     if g["stiff"]:

@@ -1,4 +1,4 @@
-"""The tool's package mesher for packages of monolithic dies: the host-side restatement of
+"""The tool's package mesher: the host-side restatement of
 ``buildPackageMesh`` (src/core/06-mesher.js:468-563) and what it needs, so that the reference's
 own packages (its default lidded single die, its lid and stiffener variants) can be built and
 solved through the library.
@@ -11,16 +11,19 @@ decides a grid line or an element:
   process and post-processing settings are the caller's);
 * ``substrateBands`` (src/core/04-homogenize.js:64-105): the build-up and core groups of the
   substrate, each split into ``layers`` bands of equal thickness;
-* ``deriveGeometry`` (src/core/05-geometry.js:98-175) for monolithic dies: z levels, bump fields
+* ``deriveGeometry`` (src/core/05-geometry.js:98-175): z levels, bump fields
   (``bumpAxis``, ``bumpFieldRects``, :23-58), underfill fillet, lid and stiffener footprints;
   ``wedgeHeight`` (:216-240), ``dieAt`` (:255-258), ``cellBumpFraction`` (:205-211);
 * the mesher's in-plane grid (``axisFeatures`` :196-248, ``mergeFeatures`` :121-134,
   ``gridLines`` :142-189), z planes (``zPlanes`` :253-305), groups (``packageGroups`` :310-322),
-  cell assignment (``makePackageAssign`` :344-453, monolithic dies) and the DOF-cap loop of
+  cell assignment (``makePackageAssign`` :344-453) and the DOF-cap loop of
   ``buildPackageMesh`` with its final refinement at the lid foot or stiffener ring edges.
 
-Stacked modules (chiplets on a base) are not restated here: ``stacked_module`` in
-``packages.py`` builds the library's own module workload.
+Stacked modules with a Si base (``defaultModule``, ``defaultChiplet``, ``defaultStack``,
+02-config.js:82-117; their geometry, feature lines, planes, groups, cells and three-point supports,
+06-mesher.js:87-109, :209-222, :246-251, :281-286, :328-343, :376-427, :477-482, :534-545) are
+restated too; organic RDL interposer bases are not (``stacked_module`` in ``packages.py`` is the
+library's own module workload).
 """
 from __future__ import annotations
 
@@ -29,7 +32,7 @@ from typing import Optional
 
 import numpy as np
 
-from .mesh import PART, Mesh, build_structured_mesh, constraints321
+from .mesh import PART, Mesh, build_structured_mesh, constraints321, module_support
 
 # the mesher's constants (src/core/00-constants.js:34-55)
 FEATURE_SNAP_TOL = 0.010
@@ -47,6 +50,8 @@ SIZE_SAMPLES = 256
 CAP_GROWTH_PAD = 1.03
 CAP_MAX_ITER = 12
 CONSTRAINT_SPAN = 0.4
+MODULE_HMIN_PER_HEIGHT = 4
+STAGE = dict(DDI=-3, WCUF=-2, MOLD=-1)      # the module process stages before the substrate's (00-constants.js:27)
 MESH_PRESETS = {
     "draft": dict(label="Draft", hmin=0.6, hmax=3.0, cap=75000, layers=1),
     "standard": dict(label="Standard", hmin=0.25, hmax=1.5, cap=330000, layers=2),
@@ -108,6 +113,30 @@ def default_die(did: str, x: float, y: float) -> dict:
                 bump=dict(type="full", rows=3, px=0.150, py=0.150, keepout=0.150, ubm=0.085, sro=0.090, dmax=0.105))
 
 
+def default_chiplet(cid: str, x: float, y: float, sx: float = 10.0, sy: float = 10.0) -> dict:
+    """defaultChiplet (02-config.js:82-84): a chiplet placed relative to its module."""
+    return dict(id=cid, name="Chiplet " + cid.lstrip("C"), x=x, y=y, sx=sx, sy=sy, rot=0, si="aniso",
+                ddi=dict(type="full", rows=3, keepout=0.050))
+
+
+def default_module(mid: str, x: float, y: float) -> dict:
+    """defaultModule (02-config.js:92-100) with a Si base: a 22 x 16 mm base 0.100 mm thick with
+    1 % TSV Cu, on the flip chip bumps, carrying two 10 x 14 mm chiplets."""
+    return dict(id=mid, name="Module " + mid.lstrip("M"), x=x, y=y, sx=22.0, sy=16.0, rot=0, base="si", tBase=0.100,
+                si="aniso", tsv=0.01,
+                bump=dict(type="full", rows=3, px=0.150, py=0.150, keepout=0.150, ubm=0.085, sro=0.090, dmax=0.105),
+                chiplets=[default_chiplet("C1", -5.4, 0, 10.0, 14.0), default_chiplet("C2", 5.4, 0, 10.0, 14.0)])
+
+
+def default_stack() -> dict:
+    """defaultStack (02-config.js:108-117): the package-wide module technology (chiplet thickness,
+    the DDI microbump: a Cu pillar under a solder cap, the DDI fill, the module process
+    temperatures)."""
+    return dict(chipletT=0.700, ddi=dict(standoff=0.025, pillarH=0.012, d=0.025, px=0.040, py=0.040, solder="sn35ag"),
+                fill="wcuf", wcuf=dict(mat="cv5300", Wf=0.30, Hf=0.5), moldMat="ei6042",
+                process=dict(Tddi=221, Twcuf=150, Tmold=180))
+
+
 def default_config() -> dict:
     """defaultConfig (02-config.js:140-166): the lidded single-die package, its geometry, the
     material ids of its parts, the process temperatures and the BGA grid (materials database,
@@ -119,6 +148,7 @@ def default_config() -> dict:
         bump=dict(standoff=0.075, solder="sac305"),
         dies=[default_die("D1", 0.0, 0.0)],
         modules=[],
+        stack=default_stack(),
         underfill=dict(mat="uf9000ae", Wf=0.8, Hf=0.7),
         lid=dict(mat="cu", ox=43.0, oy=43.0, tPlate=1.0, footW=3.0, adhMat="eccobond3005", adhT=0.100, timMat="tim_gel", blt=0.050),
         stiffener=dict(mat="cu", ox=53.0, oy=53.0, ringW=4.0, t=0.8, adhMat="eccobond3005", adhT=0.050),
@@ -256,9 +286,12 @@ def bump_field_rects(cx, cy, w, h, rect, bump, px, py) -> dict:
 
 
 def derive_geometry(cfg: dict, layers: int) -> dict:
-    """deriveGeometry (05-geometry.js:98-175) for monolithic dies."""
-    if cfg.get("modules"):
-        raise ValueError("stacked modules are not part of this mesher restatement")
+    """deriveGeometry (05-geometry.js:98-175): the monolithic dies, then the stacked modules (Si
+    base only) with their chiplets; ``dies`` holds both (the objects on the flip chip bump layer),
+    ``monoDies`` and ``modules`` each kind."""
+    for m in cfg.get("modules") or []:
+        if m.get("base", "si") == "rdl":
+            raise ValueError("modules on an organic RDL interposer are not part of this mesher restatement")
     sub = substrate_bands(cfg["substrate"]["layers"], layers)
     zt = sub["total"]
     so = cfg["bump"]["standoff"]
@@ -278,9 +311,49 @@ def derive_geometry(cfg: dict, layers: int) -> dict:
         o.update(index=i, kind="die", name=d["name"], rect=rect, cx=d["x"], cy=d["y"], w=w, h=h, px=px, py=py,
                  t=d["t"], zaf=zaf, ztop=zaf + d["t"], deff=deff, density=abump / (px * py))
         dies.append(o)
-    tmax = max((d["t"] for d in dies), default=0.0)
-    g = dict(cfg=cfg, layers=layers, sub=sub, zt=zt, zaf=zaf, so=so, substrate=substrate, dies=dies, tmax=tmax,
-             uf=dict(Wf=cfg["underfill"]["Wf"], Hf=cfg["underfill"]["Hf"]), lid=None, stiff=None)
+    mods = cfg.get("modules") or []
+    st = cfg["stack"] if mods else None
+    modules = []
+    for mi, m in enumerate(mods):
+        rot = m.get("rot", 0) == 90
+        w, h = (m["sy"], m["sx"]) if rot else (m["sx"], m["sy"])
+        b = m["bump"]
+        px, py = (b["py"], b["px"]) if rot else (b["px"], b["py"])
+        rect = dict(x0=m["x"] - w / 2, x1=m["x"] + w / 2, y0=m["y"] - h / 2, y1=m["y"] + h / 2)
+        o = bump_field_rects(m["x"], m["y"], w, h, rect, b, px, py)
+        deff = bump_profile_deff(b["ubm"], b["sro"], b["dmax"], so)
+        abump = math.pi * deff * deff / 4
+        t_base = m["tBase"]
+        z_base_top = zaf + t_base
+        z_ddi_top = z_base_top + st["ddi"]["standoff"]
+        H = t_base + st["ddi"]["standoff"] + st["chipletT"]
+        o.update(index=len(cfg["dies"]) + mi, kind="module", modIndex=mi, name=m["name"], rect=rect, cx=m["x"], cy=m["y"], w=w,
+                 h=h, px=px, py=py, t=H, zaf=zaf, ztop=zaf + H, deff=deff, density=abump / (px * py), base="si",
+                 tBase=t_base, zBaseTop=z_base_top, zDdiTop=z_ddi_top, si=m.get("si") or "aniso", tsv=max(0.0, m.get("tsv") or 0.0))
+        # chiplets: centres rotated with the module, sizes and DDI pitch swapped by the module and the chiplet rotation
+        dpx, dpy = st["ddi"]["px"], st["ddi"]["py"]
+        a_ddi = math.pi * st["ddi"]["d"] * st["ddi"]["d"] / 4
+        chips = []
+        for ci, c in enumerate(m["chiplets"]):
+            ccx, ccy = m["x"] + (-c["y"] if rot else c["x"]), m["y"] + (c["x"] if rot else c["y"])
+            swap = rot != (c.get("rot", 0) == 90)
+            cw, ch = (c["sy"], c["sx"]) if swap else (c["sx"], c["sy"])
+            cpx, cpy = (dpy, dpx) if swap else (dpx, dpy)
+            crect = dict(x0=ccx - cw / 2, x1=ccx + cw / 2, y0=ccy - ch / 2, y1=ccy + ch / 2)
+            f = bump_field_rects(ccx, ccy, cw, ch, crect, c["ddi"], cpx, cpy)
+            f.update(index=ci, modIndex=mi, name=m["name"] + " / " + c["name"], cx=ccx, cy=ccy, w=cw, h=ch, rect=crect, px=cpx,
+                     py=cpy, t=st["chipletT"], si=c.get("si") or "aniso", zaf=z_ddi_top, zb=z_ddi_top,
+                     ztop=z_ddi_top + st["chipletT"], deff=st["ddi"]["d"], density=a_ddi / (cpx * cpy), kind="chiplet")
+            chips.append(f)
+        o["chiplets"] = chips
+        modules.append(o)
+    objs = dies + modules
+    tmax = max((d["t"] for d in objs), default=0.0)
+    g = dict(cfg=cfg, layers=layers, sub=sub, zt=zt, zaf=zaf, so=so, substrate=substrate, dies=objs, monoDies=dies,
+             modules=modules, tmax=tmax, stack=st, uf=dict(Wf=cfg["underfill"]["Wf"], Hf=cfg["underfill"]["Hf"]), lid=None,
+             stiff=None, wcuf=None)
+    if st and st["fill"] == "wcuf":
+        g["wcuf"] = dict(Wf=st["wcuf"]["Wf"], Hf=st["wcuf"]["Hf"])
     if cfg["packageType"] == "lid":
         L = cfg["lid"]
         outer = dict(x0=-L["ox"] / 2, x1=L["ox"] / 2, y0=-L["oy"] / 2, y1=L["oy"] / 2)
@@ -437,8 +510,8 @@ def grid_lines(lines, edges, hmin, hmax, spans) -> list:
 
 
 def axis_features(g: dict, axis: str) -> dict:
-    """axisFeatures (06-mesher.js:196-248) for monolithic dies: feature lines, refined die edges,
-    ring and fillet spans, and the lid foot or stiffener ring edges."""
+    """axisFeatures (06-mesher.js:196-248): feature lines, refined die and chiplet edges, ring,
+    underfill and wafer underfill fillet spans, and the lid foot or stiffener ring edges."""
     sb = g["substrate"]
     lo, hi = (sb["x0"], sb["x1"]) if axis == "x" else (sb["y0"], sb["y1"])
     k0, k1 = ("x0", "x1") if axis == "x" else ("y0", "y1")
@@ -465,6 +538,25 @@ def axis_features(g: dict, axis: str) -> dict:
         if d["inner"]:
             add(d["inner"][k0], 1, d["name"] + " bump ring")
             add(d["inner"][k1], 1, d["name"] + " bump ring")
+        if d["kind"] != "module":
+            continue
+        # chiplet edges refine like die edges; the wafer underfill fillet gets its own columns, clipped at
+        # the base edge (the DDI microbump fields are not grid lines: cells take their area overlap)
+        for c in d["chiplets"]:
+            add(c["rect"][k0], 2, c["name"] + " edge")
+            add(c["rect"][k1], 2, c["name"] + " edge")
+            edges.append(dict(v=c["rect"][k0], zone=REFINE_ZONE_FACTOR * c["t"]))
+            edges.append(dict(v=c["rect"][k1], zone=REFINE_ZONE_FACTOR * c["t"]))
+            if not g["wcuf"]:
+                continue
+            wa = max(d["rect"][k0], c["rect"][k0] - g["wcuf"]["Wf"])
+            wb = min(d["rect"][k1], c["rect"][k1] + g["wcuf"]["Wf"])
+            add(wa, 1, c["name"] + " wCUF fillet")
+            add(wb, 1, c["name"] + " wCUF fillet")
+            if c["rect"][k0] - wa > 1e-9:
+                spans.append(dict(a=wa, b=c["rect"][k0], fillet=True, min=1))
+            if wb - c["rect"][k1] > 1e-9:
+                spans.append(dict(a=c["rect"][k1], b=wb, fillet=True, min=1))
     ring = g["lid"] or g["stiff"]
     if ring:
         what = "lid" if g["lid"] else "stiffener"
@@ -483,7 +575,8 @@ def axis_features(g: dict, axis: str) -> dict:
 # ---- z planes ------------------------------------------------------------------------------
 
 def z_planes(g: dict) -> dict:
-    """zPlanes (06-mesher.js:253-305) for monolithic dies: merged structural planes, then element
+    """zPlanes (06-mesher.js:253-305): merged structural planes (module base tops, chiplet bottoms
+    and wafer underfill fillet tops included), then element
     layers per band (die bands except slivers and the lid plate start at half the preset minimum,
     every region then gets at least the preset minimum, each extra layer to the band of the
     region with the thickest elements; substrate bands keep one layer)."""
@@ -497,6 +590,12 @@ def z_planes(g: dict) -> dict:
         pl.append(dict(v=d["ztop"], label=d["name"] + " top", prio=2))
         if 0 < Hf < 1:
             pl.append(dict(v=g["zaf"] + Hf * d["t"], label=d["name"] + " fillet top", prio=1))
+    wc = g["wcuf"]
+    for m in g["modules"]:
+        pl.append(dict(v=m["zBaseTop"], label=m["name"] + " base top", prio=2))
+        pl.append(dict(v=m["zDdiTop"], label=m["name"] + " chiplet bottom", prio=2))
+        if wc and 0 < wc["Hf"] < 1:
+            pl.append(dict(v=m["zDdiTop"] + wc["Hf"] * g["stack"]["chipletT"], label=m["name"] + " wCUF fillet top", prio=1))
     lid, stiff = g["lid"], g["stiff"]
     if lid:
         pl += [dict(v=lid["zAdhTop"], label="lid adhesive top", prio=2), dict(v=lid["zLidBot"], label="lid underside", prio=2),
@@ -527,6 +626,11 @@ def z_planes(g: dict) -> dict:
         regions.append((g["zaf"], d["ztop"]))
         if Hf > 0:
             regions.append((g["zaf"], g["zaf"] + min(1, Hf) * d["t"]))
+    # stacked modules: the base, the DDI gap, the chiplets and mold, the wafer underfill fillet
+    for m in g["modules"]:
+        regions += [(g["zaf"], m["zBaseTop"]), (m["zBaseTop"], m["zDdiTop"]), (m["zDdiTop"], m["ztop"])]
+        if wc and wc["Hf"] > 0:
+            regions.append((m["zDdiTop"], m["zDdiTop"] + min(1, wc["Hf"]) * g["stack"]["chipletT"]))
     if lid:
         regions += [(g["zt"], lid["zAdhTop"]), (lid["zAdhTop"], lid["zLidBot"]), (lid["zLidBot"], lid["zLidTop"])]
     if stiff:
@@ -554,7 +658,10 @@ def z_planes(g: dict) -> dict:
 # ---- groups and cell assignment --------------------------------------------------------------
 
 def package_groups(g: dict) -> dict:
-    """packageGroups (06-mesher.js:310-322) for monolithic dies: group index per role."""
+    """packageGroups (06-mesher.js:310-345): group index per role. Stacked modules add, per
+    module, its chiplets, its Si base and the TSV Cu, then the DDI microbumps, the wafer underfill
+    and the wafer mold (G['chip'][mi][ci], G['base'][mi], G['tsv'][mi], G['ddi'], G['wcuf'],
+    G['mold'])."""
     G, names = {}, []
 
     def add(key, name):
@@ -563,13 +670,30 @@ def package_groups(g: dict) -> dict:
 
     add("sub", "Substrate"); add("solder", "Solder phase"); add("uf", "Underfill")
     G["die"] = []
-    for i, d in enumerate(g["dies"]):
+    for i, d in enumerate(g["monoDies"]):
         G["die"].append(len(names))
         names.append(d["name"])
     if g["lid"]:
         add("tim", "TIM1"); add("lid", "Lid"); add("lidadh", "Lid adhesive")
     if g["stiff"]:
         add("stiff", "Stiffener"); add("stiffadh", "Stiffener adhesive")
+    if g["modules"]:
+        G["chip"], G["base"], G["tsv"] = [], [], []
+        for m in g["modules"]:
+            G["chip"].append([])
+            for c in m["chiplets"]:
+                G["chip"][-1].append(len(names))
+                names.append(c["name"])
+            G["base"].append(len(names))
+            names.append(m["name"] + " Si base")
+            G["tsv"].append(None)
+            if m["tsv"] > 0:
+                G["tsv"][-1] = len(names)
+                names.append(m["name"] + " TSV Cu")
+        add("ddi", "DDI microbumps")
+        if g["wcuf"]:
+            add("wcuf", "Wafer underfill")
+        add("mold", "Wafer mold")
     return dict(G=G, names=names)
 
 
@@ -581,8 +705,68 @@ def _fill_fraction(hs, z_base, z0, z1) -> float:
     return f / len(hs)
 
 
+def wcuf_height(g, m, x, y):
+    """wcufHeight (05-geometry.js:250-253): the wafer underfill fillet height above the chiplet
+    bottom at (x, y) on module m outside its chiplets (the wedge rule around the chiplets, within
+    the base footprint), and whether (x, y) is in a fillet footprint."""
+    if not g["wcuf"] or not _point_in_rect(m["rect"], x, y):
+        return 0.0, False
+    return wedge_height(m["chiplets"], g["wcuf"]["Wf"], g["wcuf"]["Hf"], x, y)
+
+
+def chiplet_at(m, x, y):
+    """chipletAt (05-geometry.js:262-265): the chiplet of module m whose footprint strictly holds (x, y)."""
+    for c in m["chiplets"]:
+        r = c["rect"]
+        if r["x0"] < x < r["x1"] and r["y0"] < y < r["y1"]:
+            return c
+    return None
+
+
+def _module_cell(g, G, d, chip, fbd, wc_in, hsw, z, z0, z1, put):
+    """makePackageAssign's module branch (06-mesher.js:402-428) for a cell above the active face:
+    the Si base (with the TSV Cu superposed by its fraction), the DDI gap (microbump columns
+    superposed on the fill under a chiplet; wafer underfill fillet or mold between chiplets), the
+    chiplet layer (chiplet, or the fillet wedge and mold by their volume fractions), the TIM above."""
+    mi = d["modIndex"]
+    if z < d["zBaseTop"]:
+        if d["tsv"] > 0:
+            put(0, G["base"][mi], PART["BASE_SI"], 1 - d["tsv"])
+            put(1, G["tsv"][mi], PART["TSV"], d["tsv"])
+        else:
+            put(0, G["base"][mi], PART["BASE_SI"], 1.0)
+    elif z < d["zDdiTop"]:
+        fill = G["wcuf"] if "wcuf" in G else G["mold"]
+        if chip:
+            if fbd > 1e-12:
+                put(0, G["ddi"], PART["DDI_SOLDER"], fbd)
+                put(1, fill, PART["DDI_FILL"], 1 - fbd)
+            else:
+                put(0, fill, PART["DDI_FILL"], 1.0)
+        elif wc_in:
+            put(0, G["wcuf"], PART["WCUF_FILLET"], 1.0)
+        else:
+            put(0, G["mold"], PART["MOLD"], 1.0)
+    elif z < d["ztop"]:
+        if chip:
+            put(0, G["chip"][mi][chip["index"]], PART["CHIPLET"], 1.0)
+            return
+        if wc_in:
+            f = _fill_fraction(hsw, d["zDdiTop"], z0, z1)
+            if f > 1 - FILLET_FILL_MIN:
+                put(0, G["wcuf"], PART["WCUF_FILLET"], 1.0)
+                return
+            if f >= FILLET_FILL_MIN:
+                put(0, G["wcuf"], PART["WCUF_FILLET"], f)
+                put(1, G["mold"], PART["MOLD"], 1 - f)
+                return
+        put(0, G["mold"], PART["MOLD"], 1.0)
+    elif g["lid"] and z < g["lid"]["zLidBot"]:
+        put(0, G["tim"], PART["TIM"], 1.0)
+
+
 def package_cells(g: dict, xs, ys, zs, G: dict):
-    """makePackageAssign (06-mesher.js:344-453) for monolithic dies, evaluated for every cell:
+    """makePackageAssign (06-mesher.js:344-453), evaluated for every cell:
     per-cell phase arrays (group, part, scale; two slots per cell, -1 = none) in the cell order of
     buildStructuredMesh. Column descriptors first (die under the centroid, bump fraction, fillet
     footprint and surface samples, lid and stiffener footprints), then each layer of the column."""
@@ -613,6 +797,15 @@ def package_cells(g: dict, xs, ys, zs, G: dict):
                     hs = [wedge_height(g["dies"], g["uf"]["Wf"], g["uf"]["Hf"],
                                        xs[i] + (xs[i + 1] - xs[i]) * (a + 0.5) / S, ys[j] + (ys[j + 1] - ys[j]) * (b + 0.5) / S)[0]
                           for a in range(S) for b in range(S)]
+            chip, fbd, wc_in, hsw = None, 0.0, False, None
+            if die and die["kind"] == "module":
+                chip = chiplet_at(die, xc, yc)
+                fbd = cell_bump_fraction(chip, cell) if chip else 0.0
+                if not chip:
+                    _, wc_in = wcuf_height(g, die, xc, yc)
+                    if wc_in:
+                        hsw = [wcuf_height(g, die, xs[i] + (xs[i + 1] - xs[i]) * (a + 0.5) / S,
+                                           ys[j] + (ys[j + 1] - ys[j]) * (b + 0.5) / S)[0] for a in range(S) for b in range(S)]
             lid_outer = lid_foot = ring = False
             if lid:
                 lid_outer = _point_in_rect(lid["outer"], xc, yc)
@@ -635,6 +828,8 @@ def package_cells(g: dict, xs, ys, zs, G: dict):
                             put(i, j, k, 1, G["uf"], PART["UF_BUMP"], 1 - fb)
                         else:
                             put(i, j, k, 0, G["uf"], PART["UF_BUMP"], 1.0)
+                    elif die["kind"] == "module":
+                        _module_cell(g, G, die, chip, fbd, wc_in, hsw, z, zs[k], zs[k + 1], lambda *a: put(i, j, k, *a))
                     elif z < die["ztop"]:
                         put(i, j, k, 0, G["die"][die["index"]], PART["DIE"], 1.0)
                     elif lid and z < lid["zLidBot"]:
@@ -675,7 +870,7 @@ def preset_params(cfg: dict, override: Optional[dict] = None) -> dict:
 
 
 def build_package_mesh(cfg: dict, override: Optional[dict] = None):
-    """buildPackageMesh (06-mesher.js:468-563) for monolithic dies: the grid from the preset's
+    """buildPackageMesh (06-mesher.js:468-563): the grid from the preset's
     h_min and h_max, both enlarged by sqrt(DOF / cap) x 1.03 until the DOF (3 per node) is under
     the preset cap (at most 12 times, h_min at most the preset h_max), then rebuilt with the lid
     foot or stiffener ring edges refined to the same h_min. Returns (Mesh, info)."""
@@ -688,7 +883,9 @@ def build_package_mesh(cfg: dict, override: Optional[dict] = None):
     G = grp["G"]
     hmin, hmax = pre["hmin"], pre["hmax"]
     scaled = floor = False
-    hmin_limit = max(pre["hmin"], min(pre["hmax"], math.inf))
+    # with stacked modules h_min grows at most to MODULE_HMIN_PER_HEIGHT times the lowest module's height
+    mod_h = [d["t"] for d in g["dies"] if d["kind"] == "module"]
+    hmin_limit = max(pre["hmin"], min(pre["hmax"], MODULE_HMIN_PER_HEIGHT * min(mod_h) if mod_h else math.inf))
 
     def build(ring):
         xs = grid_lines(mx["lines"], fx["edges"] + fx["ringEdges"] if ring else fx["edges"], hmin, hmax, fx["spans"])
@@ -730,7 +927,18 @@ def build_package_mesh(cfg: dict, override: Optional[dict] = None):
     mesh.featureY = feat_idx(my["lines"], my["labels"], mesh.ys)
     sb = g["substrate"]
     mesh.constraints = constraints321(mesh, CONSTRAINT_SPAN * min(sb["x1"], sb["y1"]))
+    # stacked modules are free bodies in their own process stages: a 3-2-1 support on each base bottom
+    if g["modules"]:
+        kb = next(k for k, z in enumerate(zp["zs"]) if abs(z - g["zaf"]) < 1e-9)
+        dofs = []
+        for m in g["modules"]:
+            sup = module_support(mesh, m["rect"], m["cx"], m["cy"], kb)
+            if sup is None:
+                raise ValueError(m["name"] + ": too few mesh nodes under the module base for its support in the module stages")
+            dofs += [3 * sup[0], 3 * sup[0] + 1, 3 * sup[0] + 2, 3 * sup[1] + 1, 3 * sup[1] + 2, 3 * sup[2] + 2]
+        mesh.moduleConstraints = np.asarray(dofs, np.int32)
     info = dict(preset=pre["label"], hmin=hmin, hmax=hmax, cap=pre["cap"], scaled=scaled, capDof=cap_dof, capFloor=floor,
+                hminLimit=hmin_limit, moduleLimited=hmin_limit < pre["hmax"],
                 ringRefined=ring_refined, nx=mesh.nx, ny=mesh.ny, nz=mesh.nz, nNodes=mesh.nn, nElem=mesh.ne, nDof=3 * mesh.nn,
                 layerBand=np.asarray(zp["layerBand"], np.int32), basePlanes=zp["basePlanes"], planeLabels=zp["baseLabels"],
                 groups=grp["names"], geometry=g)

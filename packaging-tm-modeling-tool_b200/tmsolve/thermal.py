@@ -223,12 +223,16 @@ def substrate_box(xs, ys, rows_top_down: list, recs: dict, nb: int, per_row: boo
 
 # ---- homogeneous groups of database records ----------------------------------------------------
 
-def group_tables(mat: dict, column: bool = False, si_model: str = "aniso", nu_max: float = NU_MAX_GLOBAL) -> dict:
+def group_tables(mat: dict, column: bool = False, si_model: str = "aniso", nu_max: float = NU_MAX_GLOBAL,
+                 series: Optional[tuple] = None) -> dict:
     """FEModel._prepareGroup (09-assembly.js:253-284) for a homogeneous group of one record: the
     thermal strains F(T) (TGRID_N, 3: in-plane twice, through-thickness) and either a constant
     stiffness (cubic silicon, an isotropic record of constant modulus without a solidus) or a
     stiffness grid (TGRID_N, 36): isotropic D(E(T), nu) (the solder phase as separate columns,
-    ``column``), orthotropic from the record's constants at T."""
+    ``column``), orthotropic from the record's constants at T. ``series`` = (record, f): the
+    columns are a cap of this record on a pillar of the other over the height fraction f
+    (``_seriesColumn``, :288-305): compliances add by height, 1/E = (1 - f)/E_s + f/E_p and
+    1/G likewise, columnD(E, E / 2G - 1), F = (1 - f) F_s + f F_p."""
     cxy = mat.get("cteXY") or mat["cte"]
     cz = mat.get("cteZ") or cxy
     F = np.zeros((TGRID_N, 3))
@@ -242,6 +246,17 @@ def group_tables(mat: dict, column: bool = False, si_model: str = "aniso", nu_ma
     if el["type"] == "iso":
         nu = el["nu"]["v"] if isinstance(el["nu"], dict) else el["nu"]
         mk = (lambda E: column_d(E, nu)) if column else (lambda E: iso_d(E, nu, nu_max))
+        if series is not None:
+            tp, fp = iso_tables(series[0]), series[1]
+            Dg = np.zeros((TGRID_N, 36))
+            for i in range(TGRID_N):
+                Es, Ep = iso_modulus(mat, float(TGRID_MIN + i)), tp["E"][i]
+                Gs, Gp = Es / (2 * (1 + nu)), Ep / (2 * (1 + tp["nu"]))
+                E = 1 / ((1 - fp) / Es + fp / Ep)
+                G = 1 / ((1 - fp) / Gs + fp / Gp)
+                Dg[i] = column_d(E, E / (2 * G) - 1)
+                F[i] = (1 - fp) * F[i] + fp * tp["F"][i]
+            return dict(Dgrid=Dg, F=F)
         if el["E"]["type"] == "const" and mat.get("solidus") is None:
             return dict(Dconst=mk(iso_modulus(mat, float(TGRID_MIN))), F=F)
         return dict(Dgrid=np.array([mk(iso_modulus(mat, float(TGRID_MIN + i))) for i in range(TGRID_N)]), F=F)

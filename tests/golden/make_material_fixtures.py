@@ -10,7 +10,7 @@ import os
 import sys
 
 IDS = ["uf9000ae", "abf_gl", "cu", "mcl_e_795g", "psr4000", "sac305", "si", "tim_gel", "eccobond3005", "mcl_e_705g",
-       "mcl_e_795g_lh"]
+       "mcl_e_795g_lh", "sn35ag", "cv5300", "ei6042"]
 
 
 def values(o):
