@@ -282,7 +282,8 @@ def bump_field_rects(cx, cy, w, h, rect, bump, px, py) -> dict:
     if field and bump["type"] == "peripheral" and ax["n"] > 2 * N and ay["n"] > 2 * N:
         inner = dict(x0=ax["first"] + (N - 0.5) * px, x1=ax["last"] - (N - 0.5) * px,
                      y0=ay["first"] + (N - 0.5) * py, y1=ay["last"] - (N - 0.5) * py)
-    return dict(nbx=ax["n"], nby=ay["n"], field=field, inner=inner, rows=N, peripheral=inner is not None)
+    return dict(nbx=ax["n"], nby=ay["n"], bx0=ax["first"], by0=ay["first"], field=field, inner=inner, rows=N,
+                peripheral=inner is not None)
 
 
 def derive_geometry(cfg: dict, layers: int) -> dict:
@@ -343,7 +344,7 @@ def derive_geometry(cfg: dict, layers: int) -> dict:
             f = bump_field_rects(ccx, ccy, cw, ch, crect, c["ddi"], cpx, cpy)
             f.update(index=ci, modIndex=mi, name=m["name"] + " / " + c["name"], cx=ccx, cy=ccy, w=cw, h=ch, rect=crect, px=cpx,
                      py=cpy, t=st["chipletT"], si=c.get("si") or "aniso", zaf=z_ddi_top, zb=z_ddi_top,
-                     ztop=z_ddi_top + st["chipletT"], deff=st["ddi"]["d"], density=a_ddi / (cpx * cpy), kind="chiplet")
+                     ztop=z_ddi_top + st["chipletT"], deff=st["ddi"]["d"], abump=a_ddi, density=a_ddi / (cpx * cpy), kind="chiplet")
             chips.append(f)
         o["chiplets"] = chips
         modules.append(o)

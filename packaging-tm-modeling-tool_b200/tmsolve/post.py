@@ -27,6 +27,10 @@ Every function follows one reference function (paths within the reference projec
   eig_sym3, max_principal  eigSym3 / maxPrincipal, src/core/01-util.js:148-173
   joint_loads            jointLoads / bumpLoads, src/core/12-post.js:245-299
   die_surface_stress     dieSurfaceStress, src/core/12-post.js:178-243
+  ddi_loads              ddiLoads, src/core/12-post.js:265-276 (jointLoads of a chiplet's microbumps)
+  die_corners            dieCorners, src/core/12-post.js:316-323
+  perimeter_tractions    perimeterTractions, src/core/12-post.js:349-412 (uf_tractions: ufTractions
+                         :331-334; wcuf_tractions: wcufTractions :336-346)
 
 Arithmetic is plain Python floats in the reference's order of operations, so the results are
 the reference's to the last bit for the same sampled values.
@@ -48,7 +52,9 @@ SCREEN_MAX_BUMPS = 20000
 SCREEN_MAX_DDI = 5000
 SCREEN_KEEP_ROWS = 3
 SCREEN_CORNER_BLOCK = 10
-DIE_EDGE_BAND = 0.5      # 00-constants.js:86-88
+DIE_EDGE_BAND = 0.5      # 00-constants.js:86-90
+TRACTION_PATCH = 0.05    # mm: the side of a traction patch
+TRACTION_SAMPLES = 3     # samples per patch side
 CORNER_PATCH = 0.1
 PATCH_SAMPLES = 5
 GP2 = 1 / math.sqrt(3)
@@ -604,3 +610,147 @@ def die_surface_stress(model, states: np.ndarray, state_elems, stride: int, rect
     return dict(which=which, xs=np.array(gxs), ys=np.array(gys), nx=nxd, ny=nyd, smax=smax, sxx=sxx, syy=syy, peakInterior=peak,
                 peakX=px, peakY=py, gpPeakInterior=gpPeak, gpPeakAll=gpPeakAll, corners=corner_vals, midEdges=mid)
 
+
+
+# ---- stacked-module readers and interface tractions --------------------------------------------
+
+def ddi_loads(model, states: np.ndarray, state_elems, stride: int, g: dict, mi: int, ci: int) -> dict:
+    """Per-microbump axial and shear forces of chiplet ci of module mi: joint_loads of its DDI
+    sites at mid-height of the DDI gap in the microbump phase (a Cu pillar and a solder cap in
+    series, so its stresses are those of both)."""
+    from .mesh import PART
+    m = g["modules"][mi]
+    c = m["chiplets"][ci]
+    r = joint_loads(model, states, state_elems, stride, die_bump_sites(c), 0.5 * (m["zBaseTop"] + m["zDdiTop"]),
+                    PART["DDI_SOLDER"], c["abump"])
+    r.update(module=mi, chiplet=ci)
+    return r
+
+
+def ddi_elements(mesh, g: dict, mi: int, ci: int) -> np.ndarray:
+    """The microbump-phase elements under chiplet ci of module mi that ddi_loads reads."""
+    from .mesh import PART
+    m = g["modules"][mi]
+    sites = die_bump_sites(m["chiplets"][ci])
+    elem, _ = site_elements(mesh, sites["x"], sites["y"], 0.5 * (m["zBaseTop"] + m["zDdiTop"]), PART["DDI_SOLDER"])
+    return np.unique(elem[elem >= 0])
+
+
+def die_corners(r: dict) -> list:
+    """The corner numbering of the tool: 1 to 4 clockwise seen from the top, from (+x, -y)."""
+    return [dict(n=1, x=r["x1"], y=r["y0"], sx=1, sy=-1), dict(n=2, x=r["x0"], y=r["y0"], sx=-1, sy=-1),
+            dict(n=3, x=r["x0"], y=r["y1"], sx=-1, sy=1), dict(n=4, x=r["x1"], y=r["y1"], sx=1, sy=1)]
+
+
+def _perimeter_samples(mesh, r: dict, z0: float, side_parts, face_part) -> dict:
+    """The sample points of perimeter_tractions with their elements: per patch (walked clockwise
+    from corner 1, TRACTION_PATCH long), TRACTION_SAMPLES^2 points on the sidewall just outside
+    the edge from z0 up by one patch (the first of side_parts found in the cell, else any part)
+    and as many on the face just below z0, one patch deep inside the edge (face_part)."""
+    step, ns, eps = TRACTION_PATCH, TRACTION_SAMPLES, 1e-6
+    xs, ys, zs = [float(v) for v in mesh.xs], [float(v) for v in mesh.ys], [float(v) for v in mesh.zs]
+
+    def elem_at(x, y, z, part):
+        return element_in_cell(mesh, find_interval(xs, x), find_interval(ys, y), find_interval(zs, z), part)
+
+    def side_elem(x, y, z):
+        for p in side_parts:
+            e = elem_at(x, y, z, p)
+            if e >= 0:
+                return e
+        return elem_at(x, y, z, None)
+    cs = die_corners(r)
+    patches, corners, s0 = [], [0.0], 0.0
+    for k, c in enumerate(cs):
+        e2 = cs[(k + 1) % 4]
+        nx, ny = (c["sx"] if c["sx"] == e2["sx"] else 0), (c["sy"] if c["sy"] == e2["sy"] else 0)
+        L = math.hypot(e2["x"] - c["x"], e2["y"] - c["y"])
+        tx, ty = (e2["x"] - c["x"]) / L, (e2["y"] - c["y"]) / L
+        m = max(1, math.floor(L / step + 0.5))
+        for p in range(m):
+            sc = (p + 0.5) * L / m
+            xc, yc = c["x"] + tx * sc, c["y"] + ty * sc
+            side, face = [], []
+            for a in range(ns):
+                for b in range(ns):
+                    ds = (a + 0.5) / ns * step - step / 2
+                    x, y = xc + tx * ds, yc + ty * ds
+                    zS = z0 + (b + 0.5) / ns * step
+                    e = side_elem(x + nx * eps, y + ny * eps, zS)
+                    if e >= 0:
+                        side.append((e, x + nx * eps, y + ny * eps, zS))
+                    ix, iy = x - nx * (b + 0.5) / ns * step, y - ny * (b + 0.5) / ns * step
+                    e = elem_at(ix, iy, z0 - eps, face_part)
+                    if e >= 0:
+                        face.append((e, ix, iy, z0 - eps))
+            patches.append(dict(s=s0 + sc, x=xc, y=yc, nx=nx, ny=ny, side=side, face=face))
+        s0 += L
+        corners.append(s0)
+    return dict(patches=patches, corners=corners)
+
+
+def perimeter_elements(mesh, r: dict, z0: float, side_parts, face_part) -> np.ndarray:
+    """The elements that perimeter_tractions reads."""
+    smp = _perimeter_samples(mesh, r, z0, side_parts, face_part)
+    return np.unique(np.array([q[0] for p in smp["patches"] for q in p["side"] + p["face"]], np.int32))
+
+
+def perimeter_tractions(model, states: np.ndarray, state_elems, stride: int, name: str, r: dict, z0: float, side_parts,
+                        face_part) -> dict:
+    """Tractions along the perimeter of rectangle r on the sidewall just outside it (t = sigma n with
+    the outward normal n; peel = its normal part, shear = the rest) and on the face just below z0
+    (peel szz, shear |(tyz, tzx)|), each averaged over a patch's samples, with their maxima."""
+    mesh = model.pkg.mesh
+    smp = _perimeter_samples(mesh, r, z0, side_parts, face_part)
+    pts = [q for p in smp["patches"] for q in p["side"] + p["face"]]
+    sig = np.zeros((0, 6))
+    if pts:
+        E = np.array([q[0] for q in pts], np.int32)
+        nat = np.array([natural_coords(mesh, int(q[0]), q[1], q[2], q[3]) for q in pts])
+        row = {int(e): t for t, e in enumerate(np.asarray(state_elems))}
+        _, sig = model.state_stress(E, states[np.array([row[int(e)] for e in E])], stride, nat)
+    out = dict(s=[], x=[], y=[], peelSide=[], shearSide=[], peelFace=[], shearFace=[])
+    t = 0
+    for p in smp["patches"]:
+        nx, ny = p["nx"], p["ny"]
+        pS = vS = pF = vF = 0.0
+        for _ in p["side"]:
+            sg = sig[t]; t += 1
+            t0, t1, t2 = sg[0] * nx + sg[3] * ny, sg[3] * nx + sg[1] * ny, sg[5] * nx + sg[4] * ny
+            tn = t0 * nx + t1 * ny
+            pS += tn
+            vS += math.hypot(t0 - tn * nx, t1 - tn * ny, t2)
+        for _ in p["face"]:
+            sf = sig[t]; t += 1
+            pF += sf[2]
+            vF += math.hypot(sf[4], sf[5])
+        cS, cF = len(p["side"]), len(p["face"])
+        out["s"].append(p["s"]); out["x"].append(p["x"]); out["y"].append(p["y"])
+        out["peelSide"].append(pS / cS if cS else math.nan); out["shearSide"].append(vS / cS if cS else math.nan)
+        out["peelFace"].append(pF / cF if cF else math.nan); out["shearFace"].append(vF / cF if cF else math.nan)
+    mx = lambda a: max([v for v in a if math.isfinite(v)], default=-math.inf)
+    res = {k: np.array(v) for k, v in out.items()}
+    res.update(die=name, corners=smp["corners"], maxPeelSide=mx(out["peelSide"]), maxShearSide=mx(out["shearSide"]),
+               maxPeelFace=mx(out["peelFace"]), maxShearFace=mx(out["shearFace"]))
+    return res
+
+
+def uf_tractions(model, states: np.ndarray, state_elems, stride: int, g: dict, die: int) -> dict:
+    """Underfill tractions along the perimeter of a die (or module base) on the flip chip layer: the
+    sidewall to the fillet, the active face to the underfill near the edge."""
+    from .mesh import PART
+    d = g["dies"][die]
+    return perimeter_tractions(model, states, state_elems, stride, d["name"], d["rect"], d["zaf"], [PART["UF_FILLET"]],
+                               PART["UF_BUMP"])
+
+
+def wcuf_tractions(model, states: np.ndarray, state_elems, stride: int, g: dict, mi: int, ci: int) -> dict:
+    """Wafer underfill (or wafer mold) tractions around chiplet ci of module mi: the chiplet
+    sidewall to the fillet or mold, the chiplet's active face to the DDI fill near the edge."""
+    from .mesh import PART
+    m = g["modules"][mi]
+    c = m["chiplets"][ci]
+    r = perimeter_tractions(model, states, state_elems, stride, c["name"], c["rect"], m["zDdiTop"],
+                            [PART["WCUF_FILLET"], PART["MOLD"]], PART["DDI_FILL"])
+    r.update(module=mi, chiplet=ci, fill="wcuf" if g["wcuf"] else "mold")
+    return r

@@ -11,8 +11,9 @@ of tests/golden/materials_subset.json, the chain's stages with their births).
   device (accumulateStep, stateStress), to their printed digits.
 * V18's bare module package (15-verify.js:573-636; README.md:366: a Si-base module with two
   chiplets, its module stages free on their three-point support, then the substrate's): the RT
-  warpage +11.04 um and the whole-face Gauss-point peaks of the chiplets 49.6 / 5.3 MPa and of the
-  Si base 20.2 / 18.3 MPa, to their printed digits."""
+  warpage +11.04 um, the whole-face Gauss-point peaks of the chiplets 49.6 / 5.3 MPa and of the Si
+  base 20.2 / 18.3 MPa, the worst DDI microbump shear 75.3 mN and the wafer underfill sidewall shear
+  4.43 MPa, to their printed digits."""
 import json
 import os
 
@@ -81,17 +82,14 @@ def test_bare_die_v9_on_gpu():
 
 
 def test_v18_module_package_on_gpu():
-    from test_host_modules import V18_OPTS, v18_config, v18_results
+    from test_host_modules import V18_OPTS, check_v18, v18_config, v18_results
     from tmsolve.solver import DeviceModel
     recs = json.load(open(GOLDEN))
     cfg = v18_config()
     pkg = process_package(cfg, recs, "draft", V18_OPTS)
     dm = DeviceModel(pkg)
     try:
-        w, peaks = v18_results(dm, pkg, recs, cfg, lambda u, b: post.warpage_jeita(b, lambda x, y: dm.sample_plane(u, 0, 2, x, y)))
+        res = v18_results(dm, pkg, recs, cfg, lambda u, b: post.warpage_jeita(b, lambda x, y: dm.sample_plane(u, 0, 2, x, y)))
     finally:
         dm.close()
-    assert w["sign"] > 0 and f"{1000 * w['signed']:.2f}" == "11.04", w["signed"]
-    fmt = lambda tb: tuple(f"{v:.1f}" for v in tb)
-    assert fmt(peaks["Module 1 / Chiplet 1"]) == ("49.6", "5.3") and fmt(peaks["Module 1 / Chiplet 2"]) == ("49.6", "5.3"), peaks
-    assert fmt(peaks["Module 1 Si base"]) == ("20.2", "18.3"), peaks
+    check_v18(res)

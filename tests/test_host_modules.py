@@ -6,7 +6,8 @@ Published values pinned here to their printed digits: the uniform-CTE module (ev
 material given silicon's CTE) left stressed at 3.87e-5 of E alpha dT after its process stages;
 the module support's reactions on the first module step at 6.95e-11 of the force scale; the RT
 warpage of the bare module package, +11.04 um convex; the whole-face Gauss-point peaks of the
-chiplets (top / bottom) 49.6 / 5.3 MPa and of the Si base 20.2 / 18.3 MPa."""
+chiplets (top / bottom) 49.6 / 5.3 MPa and of the Si base 20.2 / 18.3 MPa; the worst DDI microbump
+shear 75.3 mN and the wafer underfill sidewall shear 4.43 MPa."""
 import copy
 import json
 import os
@@ -116,30 +117,53 @@ def v18_silicon_parts(pkg):
 
 
 def v18_state_elements(pkg):
-    """The elements of the top and bottom element layers of every silicon part."""
+    """The elements that the readers need: the top and bottom element layers of every silicon part,
+    the chiplets' microbump-phase elements and the elements around their perimeters."""
+    g = pkg.meta["mesh_info"]["geometry"]
+    m = g["modules"][0]
     sel = set()
     for (_, rect, zt, zb, part, grp) in v18_silicon_parts(pkg):
         for k in (post.plane_index(pkg.mesh, zt) - 1, post.plane_index(pkg.mesh, zb)):
             sel |= {e for (_, _, e) in post.die_elements(pkg.mesh, rect, k, part, grp)[0]}
+    for ci, c in enumerate(m["chiplets"]):
+        sel |= set(post.ddi_elements(pkg.mesh, g, 0, ci).tolist())
+        sel |= set(post.perimeter_elements(pkg.mesh, c["rect"], m["zDdiTop"], [PART["WCUF_FILLET"], PART["MOLD"]],
+                                           PART["DDI_FILL"]).tolist())
     return np.array(sorted(sel), np.int32)
 
 
 def v18_results(model, pkg, recs, cfg, sampler):
-    """The bare module package's 25 degC state through the model: the signed JEITA warpage (mm)
-    and the whole-face Gauss-point peaks (top, bottom) of each silicon part."""
+    """The bare module package's 25 degC state through the model: the JEITA warpage, the
+    whole-face Gauss-point peaks (top, bottom) of each silicon part, and per chiplet the worst
+    microbump shear force (N) and the largest wafer underfill sidewall shear traction (MPa)."""
+    g = pkg.meta["mesh_info"]["geometry"]
     elems = v18_state_elements(pkg)
     u, rs, S = solve_chain(model, pkg, process_chain(pkg, recs), state_elems=elems)
     assert all(r["converged"] for r in rs)
     b = post.bga_sites(sx=cfg["substrate"]["sx"], sy=cfg["substrate"]["sy"], inset=cfg["bga"]["inset"], pitch=cfg["bga"]["pitch"])
     w = sampler(u, b)
-    peaks = {nm: tuple(post.die_surface_stress(model, S, elems, S.shape[1], rect, zt, zb, part, grp, which)["gpPeakAll"]
-                       for which in ("top", "bottom"))
+    st = (S, elems, S.shape[1])
+    peaks = {nm: tuple(post.die_surface_stress(model, *st, rect, zt, zb, part, grp, which)["gpPeakAll"] for which in ("top", "bottom"))
              for (nm, rect, zt, zb, part, grp) in v18_silicon_parts(pkg)}
-    return w, peaks
+    ddi = [post.ddi_loads(model, *st, g, 0, ci)["worstV"] for ci in range(2)]
+    wct = [post.wcuf_tractions(model, *st, g, 0, ci)["maxShearSide"] for ci in range(2)]
+    return dict(w=w, peaks=peaks, ddiV=ddi, wcufShear=wct)
+
+
+def check_v18(res):
+    """V18's published 25 degC values (README.md:366) to their printed digits."""
+    w, peaks = res["w"], res["peaks"]
+    assert w["sign"] > 0 and f"{1000 * w['signed']:.2f}" == "11.04", w["signed"]
+    fmt = lambda tb: tuple(f"{v:.1f}" for v in tb)
+    assert fmt(peaks["Module 1 / Chiplet 1"]) == ("49.6", "5.3") and fmt(peaks["Module 1 / Chiplet 2"]) == ("49.6", "5.3"), peaks
+    assert fmt(peaks["Module 1 Si base"]) == ("20.2", "18.3"), peaks
+    assert [f"{1000 * v:.1f}" for v in res["ddiV"]] == ["75.3", "75.3"], res["ddiV"]
+    assert [f"{v:.2f}" for v in res["wcufShear"]] == ["4.43", "4.43"], res["wcufShear"]
 
 
 def test_v18_bare_module_package(oracle_lib):
-    """V18 (3): the whole path of the bare module package at 25 degC."""
+    """V18 (3): the whole path of the bare module package at 25 degC: warpage, silicon stresses,
+    DDI microbump loads (ddiLoads) and wafer underfill tractions (wcufTractions)."""
     recs = json.load(open(GOLDEN))
     cfg = v18_config()
     pkg = process_package(cfg, recs, "draft", V18_OPTS)
@@ -148,8 +172,4 @@ def test_v18_bare_module_package(oracle_lib):
     def jeita(u, b):
         z = b["zone"]
         return om.warpage_jeita(u, b["x"], b["y"], [z["x0"], z["x1"], z["y0"], z["y1"]])
-    w, peaks = v18_results(om, pkg, recs, cfg, jeita)
-    assert w["sign"] > 0 and f"{1000 * w['signed']:.2f}" == "11.04", w["signed"]
-    fmt = lambda tb: tuple(f"{v:.1f}" for v in tb)
-    assert fmt(peaks["Module 1 / Chiplet 1"]) == ("49.6", "5.3") and fmt(peaks["Module 1 / Chiplet 2"]) == ("49.6", "5.3"), peaks
-    assert fmt(peaks["Module 1 Si base"]) == ("20.2", "18.3"), peaks
+    check_v18(v18_results(om, pkg, recs, cfg, jeita))
