@@ -93,3 +93,17 @@ def test_v18_module_package_on_gpu():
     finally:
         dm.close()
     check_v18(res)
+
+
+def test_v8_symmetry_on_gpu():
+    """The reference's check V8 (src/core/15-verify.js:312-337) with the chains solved on the GPU:
+    the centred bare die's residual field symmetric in x, y and across the diagonal, and the offset
+    die's mirrored with its floorplan, to 1e-6 of the warpage magnitude (the GPU sweeps its columns
+    in four colours, so no sweep order favours a side)."""
+    from test_host_analysis import v8_symmetry
+    from tmsolve.solver import DeviceModel
+
+    def jeita(model, pkg, u):
+        return post.warpage_jeita(_bga(pkg.meta["cfg"]), lambda x, y: model.sample_plane(u, 0, 2, x, y))
+    rel = v8_symmetry(DeviceModel, jeita)
+    assert max(rel) < 1e-6, rel
