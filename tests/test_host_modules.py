@@ -173,3 +173,22 @@ def test_v18_bare_module_package(oracle_lib):
         z = b["zone"]
         return om.warpage_jeita(u, b["x"], b["y"], [z["x0"], z["x1"], z["y0"], z["y1"]])
     check_v18(v18_results(om, pkg, recs, cfg, jeita))
+
+
+def test_foveros_preset_meshes():
+    """The reference's Foveros-S-like preset (02-config.js:200-208: a 21 x 16 mm Si base die 0.150 mm
+    thick with three chiplets, lidded) meshes with every module part under the lid and the
+    module's support; its Draft size is a regression value of this restatement (the reference
+    publishes only a Fine size, 1.16M DOF, quoted beside a timing run, README.md:420; this mesher
+    gives 1,147,032 there)."""
+    recs = json.load(open(GOLDEN))
+    pkg = process_package(pm.preset_config("foveros"), recs, "draft")
+    info = pkg.meta["mesh_info"]
+    assert info["nDof"] == 77544 and info["ringRefined"]
+    assert info["groups"][6:] == ["Base die 1 / Chiplet 1", "Base die 1 / Chiplet 2", "Base die 1 / Chiplet 3", "Base die 1 Si base",
+                                  "Base die 1 TSV Cu", "DDI microbumps", "Wafer underfill", "Wafer mold"]
+    for part in ("CHIPLET", "BASE_SI", "TSV", "DDI_SOLDER", "WCUF_FILLET", "MOLD", "TIM", "LID", "LIDADH"):
+        assert (pkg.mesh.ePart == PART[part]).any(), part
+    assert len(pkg.mesh.moduleConstraints) == 6
+    steps = process_chain(pkg, recs)
+    assert [s[2] for s in steps[:8]] == [-3, -3, -3, -3, -2, -1, -1, -1] and steps[-1] == (30.0, 25.0, 3)
