@@ -59,6 +59,8 @@ def lib():
     L.orc_general_derivs.argtypes = [_dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
     L.orc_anand_step.restype = C.c_double
     L.orc_anand_step.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double, _dp, _dp, C.c_int, C.c_int]
+    L.orc_anand_series_step.restype = C.c_double
+    L.orc_anand_series_step.argtypes = [_dp, _dp, _dp, _dp, _dp, C.c_double, _dp, C.c_double, C.c_double, _dp, _dp, C.c_int]
     L.orc_anand_uniaxial.restype = C.c_double
     L.orc_anand_uniaxial.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int]
     L.orc_anand_screen.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _ip, _ip, C.c_int,
@@ -251,6 +253,16 @@ def fit_plane(x, y, w):
     lib().orc_fit_plane(len(w), np.ascontiguousarray(x, np.float64), np.ascontiguousarray(y, np.float64),
                         np.ascontiguousarray(w, np.float64), c)
     return c
+
+
+def anand_series_step(params, Etab, state, eps, tz, fs, Cp, T, dt, commit=True):
+    """stepSeriesColumn of one point: (plastic increment, sig, D); eps (the cap's strain) and
+    state are updated in place."""
+    sig = np.zeros(6); D = np.zeros(36)
+    d = lib().orc_anand_series_step(np.ascontiguousarray(params, np.float64), np.ascontiguousarray(Etab, np.float64), state, eps,
+                                    np.ascontiguousarray(tz, np.float64), float(fs), np.ascontiguousarray(Cp, np.float64),
+                                    float(T), float(dt), sig, D, int(commit))
+    return d, sig, D
 
 
 def anand_uniaxial(params, Etab, T, rate, eps_max, nsteps):

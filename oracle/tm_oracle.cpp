@@ -2886,6 +2886,22 @@ double orc_anand_step(const double* params, const double* Etab, double* state, c
   return d;
 }
 
+// stepSeriesColumn (13-fatigue.js:178-206) of one point: the cap's strain eps (guess in, solution
+// out) for the prescribed column-average (zz, yz, zx) strains tz, cap fraction fs and pillar
+// compliances Cp; the state as in orc_anand_step; returns the plastic increment
+double orc_anand_series_step(const double* params, const double* Etab, double* state, double* eps, const double* tz, double fs,
+                             const double* Cp, double T, double dt, double* sig, double* D, int commit) {
+  AnandParams P{params[0], params[1], params[2], params[3], params[4], params[5], params[6], params[7], params[8], params[9]};
+  AnandPoint pt(P, Etab);
+  for (int i = 0; i < 6; i++) pt.ep[i] = state[i];
+  pt.s = state[6]; pt.ebar = state[7]; pt.W = state[8]; pt.sigEq = state[9]; pt.lastD = state[10];
+  const double d = pt.stepSeriesColumn(eps, tz, fs, Cp, T, dt, sig, D, nullptr);
+  if (commit) pt.commit();
+  for (int i = 0; i < 6; i++) state[i] = pt.ep[i];
+  state[6] = pt.s; state[7] = pt.ebar; state[8] = pt.W; state[9] = pt.sigEq; state[10] = pt.lastD;
+  return d;
+}
+
 // anandUniaxial (13-fatigue.js:252-272): returns the final stress
 double orc_anand_uniaxial(const double* params, const double* Etab, double T, double rate, double epsMax, int nsteps) {
   AnandParams P{params[0], params[1], params[2], params[3], params[4], params[5], params[6], params[7], params[8], params[9]};

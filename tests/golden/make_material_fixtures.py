@@ -17,7 +17,8 @@ def values(o):
     if isinstance(o, dict):
         if "v" in o and not isinstance(o["v"], list):
             return {"v": o["v"], "u": o.get("u")}
-        return {k: values(v) for k, v in o.items() if k not in ("s", "c", "n", "r")}
+        # s, c, n, r: a parameter's sources, confidence, note and remark (the Anand exponent n is a parameter)
+        return {k: values(v) for k, v in o.items() if k not in ("s", "c", "n", "r") or isinstance(v, dict)}
     if isinstance(o, list):
         return [values(v) for v in o]
     return o
@@ -47,7 +48,7 @@ def main(path):
     for m in db["materials"]:
         if m["id"] in IDS:
             m = expand(m, by_id)
-            out[m["id"]] = {k: values(m[k]) for k in ("elastic", "cte", "cteXY", "cteZ", "solidus") if k in m}
+            out[m["id"]] = {k: values(m[k]) for k in ("elastic", "cte", "cteXY", "cteZ", "solidus", "anand") if k in m}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "materials_subset.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
