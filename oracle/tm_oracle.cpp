@@ -8,9 +8,10 @@
 // Parity is pinned by the reference's own analytic known-answer tests
 // (src/core/15-verify.js V1, V2, V3, V4, V6, V16, V18(4)), re-implemented in
 // tests/test_oracle_known_answers.py, and by its published whole-package
-// results on its own models (V5, V9, V11, the default package's room-
+// results on its own models (V5, V8, V9, V11, V18, the default package's room-
 // temperature warpage), reproduced through the host's restated model building
-// in tests/test_host_analysis.py and tests/test_host_thermal.py; the reference
+// in tests/test_host_analysis.py, tests/test_host_thermal.py and
+// tests/test_host_modules.py (V18's series column of one point there); the reference
 // publishes no golden vector files and its JavaScript cannot be run here (no
 // JS engine).
 //
