@@ -1134,7 +1134,7 @@ void factorShellColumns(Level& L) {
 
 // columnSweep :512-555
 void columnSweep(Level& L, const double* bvec, double* x, bool backward) {
-  const Pattern& P = L.P; const double* val = L.val.data(); const int ncol = (int)L.colStart.size() - 1, b = L.b;
+  const Pattern& P = L.P; const double* val = L.val.data(); const int ncol = (int)L.colStart.size() - 1;
   double* r = L.r.data(); double* dx = L.dx.data();
   for (int cc = 0; cc < ncol; cc++) {
     const int c = backward ? ncol - 1 - cc : cc;
@@ -1845,7 +1845,7 @@ void isoD(double E, double nu, double nuMax, double* out) {
   const double nc = std::min(nu, nuMax);
   const double G = E / (2 * (1 + nc));
   const double nxy = std::min(nc, nuMax), nxz = nxy, nyz = nxy;
-  double S[9] = {0}, C[9];
+  double S[9] = {0}, C[9] = {0};
   S[0] = 1 / E; S[4] = 1 / E; S[8] = 1 / E;
   S[1] = S[3] = -nxy / E;
   S[2] = S[6] = -nxz / E;
