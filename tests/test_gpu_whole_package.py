@@ -9,6 +9,8 @@ of tests/golden/materials_subset.json, the chain's stages with their births).
 * The bare-die preset (V9, src/core/15-verify.js:339-357; README.md:358): the warpage +222.7 um
   and the die backside interior peak +65.8 MPa from the die's element states marched on the
   device (accumulateStep, stateStress), to their printed digits.
+* V10's Standard half (README.md:358): the default package at Standard (314,385 DOF), -69.3 um
+  and the die interior peak 72.6 MPa.
 * V18's bare module package (15-verify.js:573-636; README.md:366: a Si-base module with two
   chiplets, its module stages free on their three-point support, then the substrate's): the RT
   warpage +11.04 um, the whole-face Gauss-point peaks of the chiplets 49.6 / 5.3 MPa and of the Si
@@ -59,12 +61,13 @@ def test_default_package_chain_on_gpu(oracle_lib):
         assert f"{1000 * w:.2f}" == "-69.34", (precision, w)
 
 
-def test_bare_die_v9_on_gpu():
+def _die_rt_on_gpu(cfg, preset):
+    """The chain of a single-die configuration solved on the GPU: the signed JEITA warpage (mm) and
+    the die's top-face stress record from its element states marched on the device."""
     from tmsolve.mesh import PART
     from tmsolve.solver import DeviceModel
     recs = json.load(open(GOLDEN))
-    cfg = preset_config("bare")
-    pkg = process_package(cfg, recs, "draft")
+    pkg = process_package(cfg, recs, preset)
     d = pkg.meta["mesh_info"]["geometry"]["dies"][0]
     group = 3                                    # packageGroups: substrate, solder, underfill, then the dies
     kp = post.plane_index(pkg.mesh, d["ztop"])
@@ -78,7 +81,19 @@ def test_bare_die_v9_on_gpu():
         ds = post.die_surface_stress(dm, S, elems, S.shape[1], d["rect"], d["ztop"], d["zaf"], PART["DIE"], group, "top")
     finally:
         dm.close()
+    return w, ds
+
+
+def test_bare_die_v9_on_gpu():
+    w, ds = _die_rt_on_gpu(preset_config("bare"), "draft")
     assert f"{1000 * w:.1f}" == "222.7" and f"{ds['peakInterior']:.1f}" == "65.8", (w, ds["peakInterior"])
+
+
+def test_default_package_v10_standard_on_gpu():
+    """V10's Standard half (15-verify.js; README.md:358: -69.3 um and a die interior peak of
+    72.6 MPa at Standard, 314k DOF with 2 layers per region) with the chain on the GPU."""
+    w, ds = _die_rt_on_gpu(default_config(), "standard")
+    assert f"{1000 * w:.1f}" == "-69.3" and f"{ds['peakInterior']:.1f}" == "72.6", (w, ds["peakInterior"])
 
 
 def test_v18_module_package_on_gpu():
