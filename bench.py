@@ -47,14 +47,15 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="a warm-up assemble + solve, then one assemble + solve (for ncu captures); prints no bench line")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "screen", "c3", "tornado", "c4"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "screen", "c3", "tornado", "c4", "analysis"],
                     help="c2: the lidded 160x160x32 solve (the headline); c1: the plain FP64 FCBGA 48x48x20 solve; "
                          "screen: Anand screening of the 17,424 bumps of a die over three -40/125 degC cycles; "
                          "c3: the stacked-module thermal-cycle analysis (module stage, process chain, cycling branches, "
                          "bump strain tables, Anand screening at 40 load steps per cycle), about 1.2M DOF; "
                          "tornado: the 24 perturbed-material cases of the c2 package in one warm-started solve loop; "
                          "c4: 64 bump submodels of 20^3-48^3 voxels in one batch over the first history points of a "
-                         "40-step -40/125 degC cycle")
+                         "40-step -40/125 degC cycle; analysis: every step of the full thermal path of the tool's "
+                         "default package at Standard (the reference's 'Full Standard analysis')")
     ap.add_argument("--c4-cells", type=int, default=64, help="c4: submodels in the batch")
     ap.add_argument("--c4-points", type=int, default=1, help="c4: history points of the timed sample")
     ap.add_argument("--c4-precond", default="line", choices=["line", "ic"], help="c4: inner-solve preconditioner")
@@ -577,6 +578,67 @@ def run_c3(a):
         "clocks": ck.summary()}))
 
 
+ANALYSIS_METRIC = "full thermal-path analysis of the tool's default package (every step of buildPath solved), seconds per analysis"
+
+
+def run_analysis(a):
+    """The reference's 'Full Standard analysis' (its README's timing table: 611 s at 314k DOF on
+    three workers): the tool's default lidded package built by the restated model-building side at
+    the Standard preset (untimed, reported as build_s), then every step of its full thermal path
+    (the chain, the chip-join branch, the cycling and reflow sweeps: 67 steps) assembled and solved
+    through the host API from a fresh solver (no stored solutions), with the room-temperature JEITA
+    warpage read at the end. Timed end to end on the host clock around device-synchronising calls."""
+    import numpy as np
+    import torch
+    from tmsolve import post
+    from tmsolve.analysis import full_path, process_package
+    from tmsolve.pkgmesh import default_config
+    from tmsolve.solver import DeviceModel
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    recs = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "materials_subset.json")))
+    cfg = default_config()
+    t0 = time.perf_counter()
+    pkg = process_package(cfg, recs, "standard")
+    fp = full_path(pkg, recs)
+    build_s = time.perf_counter() - t0
+    steps = fp["steps"]
+    b = post.bga_sites(sx=cfg["substrate"]["sx"], sy=cfg["substrate"]["sy"], inset=cfg["bga"]["inset"], pitch=cfg["bga"]["pitch"])
+    dm = DeviceModel(pkg)
+
+    def analysis():
+        dm.clear_warm()
+        t0 = time.perf_counter()
+        u, its = np.zeros(dm.ndof), 0
+        for k, (Ta, Tb, st, _) in enumerate(steps):
+            r = dm.solve(dm.assemble_step(pkg.step(Ta, Tb, stage=st)), tol=1e-8, key=k, precision=a.precision)
+            if not r["converged"]:
+                raise RuntimeError(f"step {k} ({Ta} -> {Tb} degC) did not converge: relres {r['relres']:.2e}")
+            if k in fp["chain"]:
+                u += r["u"]
+            its += r["iters"]
+        w = post.warpage_jeita(b, lambda x, y: dm.sample_plane(u, 0, 2, x, y))
+        return dict(total_s=time.perf_counter() - t0, iters=its, w=w["signed"])
+    for _ in range(a.warmup):
+        analysis()
+    torch.cuda.synchronize()
+    with Clocks(local) as ck:
+        runs = [analysis() for _ in range(a.steps)]
+    tot = sum(r["total_s"] for r in runs) / a.steps
+    n = dm.ndof
+    print(json.dumps({
+        "metric": ANALYSIS_METRIC, "value": tot, "unit": "s per analysis", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * tot / len(steps), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 apply/smoother + f64 refinement" if a.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"default lidded package at Standard ({n} DOF), {len(steps)} path steps, tol 1e-8, fresh solver",
+                   "dof": n, "precision": a.precision, "l2": "working set larger than L2"},
+        "analysis": {"build_s": build_s, "pcg_iters": runs[-1]["iters"], "rt_warpage_um": 1000 * runs[-1]["w"],
+                     "reference_s": 611.0, "reference_note": "README timing table: 611 s at 314k DOF, Chromium, 3 workers"},
+        "e2e": {"value": tot, "unit": "s per analysis", "h2d_bytes_per_step": 8 * n * len(steps),
+                "d2h_bytes_per_step": 8 * n * len(steps)},
+        "clocks": ck.summary()}))
+
+
 TORNADO_METRIC = "tornado batch: base + 24 perturbed-material solves of lidded C2 (matE x6, matCTE x6 at -/+10 %), signed JEITA warpage per case"
 
 
@@ -728,6 +790,9 @@ def main():
         return
     if a.workload == "c3":
         run_c3(a)
+        return
+    if a.workload == "analysis":
+        run_analysis(a)
         return
     if a.workload == "c1":
         global WORKLOAD
