@@ -1,6 +1,7 @@
 """The tool's process chain solved on the GPU, on the reference's own models built by the restated
-model-building side (named to run after the kernel-level GPU tests: it drives whole analyses) (the mesher, the substrate bands, the parts' tables from the database records
-of tests/golden/materials_subset.json, the chain's stages with their births).
+model-building side (the mesher, the substrate bands, the parts' tables from the database records
+of tests/golden/materials_subset.json, the chain's stages with their births). The file runs after
+the kernel-level GPU tests: it drives whole analyses.
 
 * The default package at Draft (65,322 DOF, 15 steps 217 -> 165 -> 150 -> 25 degC): every step's
   increment within 1e-8 of the oracle's in FP64 and 1e-5 in mixed precision (both solved to
